@@ -1,0 +1,203 @@
+/*
+ * pib200.h — C ABI of libpib200, the B200 (sm_100a) model time step of PlanktonIndividuals.jl.
+ *
+ * The reference has no FFI: its public surface is the Julia API (src/PlanktonIndividuals.jl:7-42)
+ * RectilinearGrid → PlanktonModel → PlanktonSimulation → update!, with TimeStep! underneath.
+ * Each entry point below names the reference function whose job it takes over. A Julia `ccall`
+ * shim and the Python package `PlanktonIndividuals` in this repository bind
+ * exactly these symbols.
+ *
+ * Conventions
+ *  - Arrays cross the boundary as host pointers in Julia column-major order (x fastest), with the
+ *    shapes the reference uses: grid fields are (Nx+2Hx, Ny+2Hy, Nz+2Hz) including halos,
+ *    individual attributes are `capacity` long (max_individuals, src/Model/models.jl:54).
+ *  - Host pointers are borrowed for the duration of the call and copied; calls are synchronous
+ *    unless stated. The library owns all device memory of a handle. A handle belongs to one host
+ *    thread at a time and runs on its own CUDA stream of the device that was current at
+ *    pi_create.
+ *  - Every call returns PI_OK or an error code; pi_last_error gives the message. Messages of
+ *    validation errors repeat the reference's ArgumentError texts.
+ *  - Quantities are Float64 at the boundary. PI_FP64 models compute in Float64 (the plain
+ *    drop-in); PI_FP32 models store and compute the bulk of the step in Float32.
+ *  - Indices (xi, yi, zi) are the reference's 1-based Julia indices including the halo offset.
+ */
+#ifndef PIB200_H
+#define PIB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t pi_status;
+
+#define PI_OK            0
+#define PI_ERR_ARG       1   /* bad argument, NULL pointer, unsupported option            */
+#define PI_ERR_SHAPE     2   /* dimension mismatch (src/Simulation/utils.jl:213-304)      */
+#define PI_ERR_PARAM     3   /* parameter value rejected (src/Parameters/param_update.jl) */
+#define PI_ERR_CAPACITY  4   /* division overflow (QuotaMode/plankton_update.jl:20-22)    */
+#define PI_ERR_CUDA      5   /* CUDA runtime error or no usable device                    */
+#define PI_ERR_TIMEOUT   6   /* a bounded device-side wait gave up                        */
+#define PI_ERR_NAN       7   /* NaN found by pi_check_finite                              */
+#define PI_ERR_DOMAIN    8   /* an individual's cell index left the halo-padded grid      */
+#define PI_ERR_NOMEM     9   /* device allocation failed                                  */
+#define PI_ERR_STATE    10   /* call not valid in the handle's current state              */
+
+#define PI_FP64 0
+#define PI_FP32 1
+
+#define PI_PERIODIC 0
+#define PI_BOUNDED  1
+
+/* Tracer order of the reference (src/Biogeochemistry/Biogeochemistry.jl:20). */
+enum {
+    PI_DIC = 0, PI_NH4, PI_NO3, PI_PO4, PI_DFe, PI_DOC, PI_DON, PI_DOP,
+    PI_PFe_inorg, PI_POC, PI_PON, PI_POP, PI_PFe_bio, PI_Dust, PI_NTRACERS
+};
+
+/* Flux boundary faces and kinds (src/Biogeochemistry/HaloRegions/apply_bcs.jl:87-98). */
+enum { PI_WEST = 0, PI_EAST, PI_SOUTH, PI_NORTH, PI_BOTTOM, PI_TOP };
+enum { PI_BC_NONE = 0, PI_BC_CONST, PI_BC_ARRAY2D, PI_BC_ARRAY3D };
+
+/* Diagnostics kept by TimeStep! (src/Diagnostics/diagnostics_struct.jl:23-105 defaults). */
+enum { PI_DIAG_PAR = 0, PI_DIAG_NUM, PI_DIAG_GRAZ, PI_DIAG_MORT, PI_DIAG_DVID };
+
+/* RectilinearGrid (src/Grids/rectilinear_grid.jl:1-25). Metrics are passed as the reference
+ * stores them after construction (rectilinear_grid.jl:57-122), halos included. */
+typedef struct {
+    int32_t Nx, Ny, Nz;
+    int32_t Hx, Hy, Hz;
+    int32_t topo[3];            /* PI_PERIODIC or PI_BOUNDED for x, y, z                   */
+    double  dx, dy;             /* Δx, Δy                                                  */
+    const double*  dzF;         /* Nz+2Hz, g.dzF                                           */
+    const double*  dzC;         /* Nz+2Hz, g.dzC                                           */
+    const uint8_t* landmask;    /* (Nx+2Hx)(Ny+2Hy)(Nz+2Hz) with halos (Grids/utils.jl:92-129),
+                                   NULL = all water                                        */
+} pi_grid;
+
+/* Biogeochemical parameters, names and meaning of bgc_params_default
+ * (src/Parameters/param_default.jl:44-71). */
+typedef struct {
+    double kw, kc, kDOC, Nit, kDON, kDOP, kPOC, kPON, kPOP;
+    double kappa_h, kappa_v, kappa_hP, kappa_vP;     /* κh, κv, κhP, κvP */
+    double shared_graz;
+    double w_sink_org, w_sink_inorg;
+    double lambda_POC, lambda_min, kdiss, lambda_dust, lambda_Fe, ligand, DFeFrac;
+} pi_bgc_params;
+
+/* QuotaMode phytoplankton parameters of one species, in the reference's param_names order
+ * (src/Individuals/Plankton/QuotaMode/plankton_generation.jl:16-20). */
+typedef struct {
+    double Nsuper, Cquota, mean, var, Chl2Cint, alpha, Phi, Topt, Tmax, Ea;
+    double PCmax, VDOCmax, VNO3max, VNH4max, VPO4max;
+    double KsatDOC, KsatNH4, KsatNO3, KsatPO4, Cqmax, Nqmax, Pqmax;
+    double Chl2N, R_NC, R_PC, k_mtb, respir, grz_P, dvid_type, dvid_P, dvid_reg, dvid_reg2;
+    double mort_P, mort_reg, grazFracC, grazFracN, grazFracP, mortFracC, mortFracN, mortFracP;
+} pi_quota_params;
+
+/* The persistent per-individual state of one species (QuotaMode struct-of-arrays,
+ * plankton_generation.jl:2-13). Every array is `capacity` long. graz/mort/dvid carry the 0/1
+ * decisions drawn at the end of a step and applied at the start of the next. For
+ * pi_set_individuals every member is required; for pi_get_individuals NULL members are skipped. */
+typedef struct {
+    double  *x, *y, *z;
+    int64_t *xi, *yi, *zi;
+    double  *Sz, *Bm, *Cq, *Nq, *Pq, *Chl, *gen, *age;
+    uint8_t *ac;
+    double  *graz, *mort, *dvid;
+} pi_individuals;
+
+typedef struct pi_model pi_model;
+typedef struct pi_sim   pi_sim;
+
+/* PlanktonModel(arch, grid; FT, mode = QuotaMode(), max_individuals, bgc_params, phyto)
+ * (src/Model/models.jl:51-155) and timestepper(...) (src/Model/timestepper.jl:23-60): allocates
+ * the model state and scratch on the current CUDA device. Individuals start inactive and
+ * tracers at zero until set. `seed` keys the model's random draws. */
+pi_status pi_create(const pi_grid* grid, const pi_bgc_params* bgc,
+                    const pi_quota_params* species, int32_t nspecies, int64_t capacity,
+                    int32_t precision, uint64_t seed, pi_model** out);
+
+/* Releases every device allocation of the handle. */
+pi_status pi_destroy(pi_model* m);
+
+/* Individuals of species `sp` (0-based), as set by initialize_plankton!
+ * (plankton_generation.jl:35-72) or read back for output/checkpoint. */
+pi_status pi_set_individuals(pi_model* m, int32_t sp, const pi_individuals* in);
+pi_status pi_get_individuals(pi_model* m, int32_t sp, pi_individuals* out);
+
+/* Tracer `idx` (PI_DIC..PI_Dust) with halos, as model.tracers[name].data
+ * (src/Biogeochemistry/tracer_fields.jl:60-101). */
+pi_status pi_set_tracer(pi_model* m, int32_t idx, const double* data);
+pi_status pi_get_tracer(pi_model* m, int32_t idx, double* out);
+
+/* vel_copy!(vel₁, u, v, w, grid) (src/Simulation/utils.jl:5-11): interior velocities, sized
+ * (Nx[+1], Ny[+1], Nz[+1]) with the +1 on Bounded axes; halos are filled as fill_halo_vel!
+ * (src/Biogeochemistry/HaloRegions/halo_regions.jl:64-99). */
+pi_status pi_set_velocity(pi_model* m, const double* u, const double* v, const double* w);
+
+/* copyto!(timestepper.PARF, PARF) (src/Simulation/update.jl:23): surface PAR, Nx*Ny. */
+pi_status pi_set_PARF(pi_model* m, const double* parf);
+
+/* copy_interior!(timestepper.temp, temp) (src/Simulation/update.jl:26): Nx*Ny*Nz. */
+pi_status pi_set_temp(pi_model* m, const double* temp);
+
+/* set_bc!(model; tracer, pos, bc_value) (HaloRegions/boundary_conditions.jl:21-31): flux
+ * boundary condition of one tracer face. kind PI_BC_CONST reads values[0]; PI_BC_ARRAY2D reads
+ * the face's (n1, n2) array; PI_BC_ARRAY3D reads (n1, n2, nt), indexed by model.iteration. */
+pi_status pi_set_flux_bc(pi_model* m, int32_t tracer, int32_t face, int32_t kind,
+                         const double* values, int64_t nt);
+
+/* TimeStep!(model, ΔT, diags) (src/Model/time_step.jl:12-180), QuotaMode physiology. Advances
+ * model.iteration by one and model.t to iteration·ΔT. Returns PI_ERR_CAPACITY with the
+ * reference's message when divisions exceed the free slots. */
+pi_status pi_time_step(pi_model* m, double dT);
+
+/* model.iteration and model.t. */
+pi_status pi_get_time(pi_model* m, int64_t* iteration, double* t);
+pi_status pi_set_time(pi_model* m, int64_t iteration, double t);
+
+/* Number of active individuals of species `sp` (calc_active_individuals, models.jl:157-164). */
+pi_status pi_count_active(pi_model* m, int32_t sp, int64_t* n);
+
+/* Diagnostics accumulated by TimeStep! since the last reset: PI_DIAG_PAR (sp ignored) or the
+ * per-species PI_DIAG_NUM/GRAZ/MORT/DVID fields, (Nx+2Hx)(Ny+2Hy)(Nz+2Hz) each. */
+pi_status pi_get_diag(pi_model* m, int32_t kind, int32_t sp, double* out);
+pi_status pi_reset_diags(pi_model* m);
+
+/* PlanktonSimulation(model; ΔT, iterations, PARF, temp, vels, ΔT_vel, ΔT_PAR, ΔT_temp)
+ * (src/Simulation/simulations.jl:98-142) with the shape and time-step validation of
+ * src/Simulation/utils.jl:213-304. The forcing series are copied to device memory once:
+ * u, v, w are (Nx[+1], Ny[+1], Nz[+1], nvel) (NULL when no velocities are given), PARF is
+ * (Nx, Ny, npar), temp is (Nx, Ny, Nz, ntemp). */
+pi_status pi_sim_create(pi_model* m, double dT, int64_t iterations,
+                        const double* u, const double* v, const double* w, int64_t nvel,
+                        double dT_vel,
+                        const double* parf, int64_t npar, double dT_PAR,
+                        const double* temp, int64_t ntemp, double dT_temp,
+                        pi_sim** out);
+
+/* update!(sim; time_offset) (src/Simulation/update.jl:11-48): `iterations` steps, each binding
+ * that step's forcing snapshot and calling TimeStep!. Bits 0/1/2 of time_offset select the
+ * vels/PARF/temp time offsets. Runs asynchronously on the model's stream unless `sync`. */
+pi_status pi_sim_update(pi_sim* s, int32_t time_offset, int32_t sync);
+
+pi_status pi_sim_destroy(pi_sim* s);
+
+/* Blocks until all work queued on the model's stream is done and reports any device-side error
+ * (capacity overflow, index out of domain) raised since the last call. */
+pi_status pi_synchronize(pi_model* m);
+
+/* Message of the last error of the handle (or of the last failed pi_create when m is NULL). */
+pi_status pi_last_error(pi_model* m, char* buf, size_t len);
+
+/* Static description of a status code. */
+const char* pi_status_string(pi_status code);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PIB200_H */

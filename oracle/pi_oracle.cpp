@@ -1,0 +1,1140 @@
+/*
+ * pi_oracle.cpp — CPU oracle for the model time step of PlanktonIndividuals.jl (QuotaMode).
+ *
+ * TEST INFRASTRUCTURE ONLY. Nothing in the product library links or calls this file; it is the
+ * checker the tests, smoke() and the CPU-baseline leg of bench.py compare the CUDA path against.
+ *
+ * This is a plain Float64 restatement of the reference's TimeStep! written pass by pass in the
+ * order of the Julia kernels, each pass citing the file:line it follows (paths relative to the
+ * reference repository root). Summation of scatters is in ascending slot order, species in
+ * order — the order a single-threaded KernelAbstractions CPU run of the reference takes.
+ *
+ * Parity status: the reference (Julia 1.12, KernelAbstractions) cannot run in this environment,
+ * so step outputs are "parity unpinned" against the reference itself. What pins the restatement:
+ * the reference's own known-answer tests for the grid metrics, halo rules and flux boundary
+ * condition (test/grid_test.jl:5-67, test/field_test.jl:21-122), the 14-tracer order
+ * (test/field_test.jl:8), and its total-P conservation invariant (test/example_2D_test.jl:19-47),
+ * all re-run against this code by tests/test_oracle_kats.py. Random draws come from the shared
+ * counter-based generator in include/pi_numerics.h instead of the reference's unseeded
+ * MersenneTwister (src/Architectures.jl:33); exp and integer powers come from the same header.
+ *
+ * Out-of-domain indices (which the reference would read out of bounds under @inbounds) are
+ * clamped into the halo-padded grid and reported as PI_ERR_DOMAIN, the same rule as the CUDA path.
+ *
+ * The elementwise passes are OpenMP-parallel; scatters, scans and column sweeps are sequential,
+ * so the result does not depend on the thread count.
+ */
+#include "../include/pib200.h"
+#include "../include/pi_numerics.h"
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+typedef std::vector<double> dvec;
+
+/* Float32 literals of the reference that appear inside Float64 arithmetic. */
+const double F_1em30 = (double)1.0e-30f;   /* 1.0f-30  */
+const double F_RGAS  = (double)8.3145f;    /* 8.3145f0 */
+const double F_T0    = (double)273.15f;    /* 273.15f0 */
+const double F_4em2  = (double)4.0e-2f;    /* 4.0f-2   */
+const double F_1em4  = (double)1.0e-4f;    /* 1.0f-4   */
+const double F_1em2  = (double)1.0e-2f;    /* 1.0f-2   */
+const double F_1em1  = (double)1.0e-1f;    /* 1.0f-1   */
+const double F_2em3  = (double)2.0e-3f;    /* 2.0f-3   */
+const double F_1em3  = (double)1.0e-3f;    /* 1.0f-3   */
+const double F_1em5  = (double)1.0e-5f;    /* 1.0f-5   */
+const double F_THMAX = (double)1.0e20f;    /* θmax = 1.0f20, DST3FL.jl:2 */
+const double F_1em20 = (double)1.0e-20f;   /* 1.0f-20  */
+
+const uint32_t ERR_DOMAIN = 1u, ERR_CAPACITY = 2u;
+
+struct Grid {
+    int Nx, Ny, Nz, Hx, Hy, Hz, Gx, Gy, Gz;
+    int tx, ty, tz;
+    double dx, dy;
+    dvec dzF, dzC;               /* 1-based access through f(k) below */
+    std::vector<uint8_t> lm;     /* landmask with halos */
+    size_t G;
+    inline size_t id(long i, long j, long k) const {   /* 1-based Julia indices */
+        return (size_t)(i - 1) + (size_t)Gx * ((size_t)(j - 1) + (size_t)Gy * (size_t)(k - 1));
+    }
+    inline double dzF1(long k) const { return dzF[k - 1]; }
+    inline double dzC1(long k) const { return dzC[k - 1]; }
+    inline double vol(long k) const { return dx * dy * dzF1(k); }      /* volume = Δx*Δy*dzF[k] */
+    inline double Axk(long k) const { return dy * dzF1(k); }           /* Ax = Δy*dzF[k] */
+    inline double Ayk(long k) const { return dx * dzF1(k); }           /* Ay = Δx*dzF[k] */
+    inline double Az() const { return dx * dy; }                        /* Az = Δx*Δy     */
+    inline int L(long i, long j, long k) const { return lm[id(i, j, k)]; }
+};
+
+struct Species {
+    pi_quota_params p;
+    dvec x, y, z;
+    std::vector<int64_t> xi, yi, zi, idx;
+    dvec Sz, Bm, Cq, Nq, Pq, Chl, gen, age;
+    std::vector<uint8_t> ac;
+    dvec PS, VDOC, VNH4, VNO3, VPO4, rChl, resp, BS, exu, graz, mort, dvid;
+    /* diagnostics (diags.phytos[sp]) */
+    dvec d_num, d_graz, d_mort, d_dvid;
+};
+
+struct FluxBC { int kind = PI_BC_NONE; dvec v; int64_t nt = 0; };
+
+}  // namespace
+
+struct orc_model {
+    Grid g;
+    pi_bgc_params bgc;
+    int nsp;
+    int64_t C;
+    uint64_t seed;
+    std::vector<Species> sp;
+    std::vector<dvec> tr, Gcs, tt, plk;      /* 14 fields each */
+    dvec u0, v0, w0, u1, v1, w1, uh, vh, wh; /* vel₀, vel₁, vel½ */
+    dvec PARF, temp, flux_sink, par, par0, Chl, pop;
+    /* C-length scratch: rnd, velos, trs (timestepper.jl:40-55) */
+    dvec rx, ry, rz;
+    dvec vx, vy, vz, vu1, vv1, vw1, vu2, vv2, vw2;
+    dvec tNH4, tNO3, tPO4, tDOC, tDFe, tpar, tT, tpop, tdpar, tidc;
+    std::vector<int64_t> tidc_int;
+    dvec d_PAR;
+    FluxBC bc[PI_NTRACERS][6];
+    int64_t iteration;
+    double t;
+    uint32_t err_flags;
+    std::string err;
+};
+
+namespace {
+
+/* Clamp a 1-based index into [lo, hi], recording an out-of-domain access. */
+inline long clampi(orc_model* m, long v, long lo, long hi) {
+    if (v < lo) { m->err_flags |= ERR_DOMAIN; return lo; }
+    if (v > hi) { m->err_flags |= ERR_DOMAIN; return hi; }
+    return v;
+}
+
+/* ---------------------------------------------------------------------------------------- */
+/* Halo rules, src/Biogeochemistry/HaloRegions/halo_regions.jl:2-62. Each fill reads its whole */
+/* source range before writing, as Julia's broadcast unaliases overlapping views.              */
+/* ---------------------------------------------------------------------------------------- */
+
+/* axis 0/1/2 = x/y/z; face 0 = low (west/south/top), 1 = high (east/north/bottom). */
+/* mode: 0 tracer rule, 1 velocity rule for the high face (fill_halo_*_vel!), 2 Gc rule for the
+ * high face (fill_halo_*_Gc!). */
+void fill_face(const Grid& g, dvec& c, int axis, int face, int mode) {
+    int N = axis == 0 ? g.Nx : axis == 1 ? g.Ny : g.Nz;
+    int H = axis == 0 ? g.Hx : axis == 1 ? g.Hy : g.Hz;
+    int topo = axis == 0 ? g.tx : axis == 1 ? g.ty : g.tz;
+    int n1 = axis == 0 ? g.Gy : g.Gx;              /* the two other axes, full range */
+    int n2 = axis == 2 ? g.Gy : g.Gz;
+    auto at = [&](long a, long b1, long b2) -> double& {   /* a along axis, 1-based */
+        if (axis == 0) return c[g.id(a, b1, b2)];
+        if (axis == 1) return c[g.id(b1, a, b2)];
+        return c[g.id(b1, b2, a)];
+    };
+    std::vector<long> dst, src;
+    bool zero = false;
+    if (face == 0) {
+        for (int h = 1; h <= H; ++h) dst.push_back(h);
+        if (topo == PI_PERIODIC) for (int h = 1; h <= H; ++h) src.push_back(N + h);      /* c[1:H] = c[N+1:N+H] */
+        else for (int h = 1; h <= H; ++h) src.push_back(H + 1);                          /* c[1:H] = c[H+1]    */
+    } else {
+        if (mode == 1 && topo == PI_BOUNDED) {
+            for (int h = N + H + 2; h <= N + 2 * H; ++h) { dst.push_back(h); src.push_back(N + H + 1); }
+        } else if (mode == 2 && topo == PI_BOUNDED) {
+            for (int h = N + H + 1; h <= N + 2 * H; ++h) dst.push_back(h);
+            zero = true;
+        } else if (topo == PI_PERIODIC) {
+            for (int h = 1; h <= H; ++h) { dst.push_back(N + H + h); src.push_back(H + h); }  /* c[N+H+1:N+2H] = c[1+H:2H] */
+        } else {
+            for (int h = 1; h <= H; ++h) { dst.push_back(N + H + h); src.push_back(N + H); }  /* c[N+H+1:N+2H] = c[N+H] */
+        }
+    }
+    std::vector<double> tmp(dst.size());
+    for (int b2 = 1; b2 <= n2; ++b2)
+        for (int b1 = 1; b1 <= n1; ++b1) {
+            if (!zero) for (size_t q = 0; q < dst.size(); ++q) tmp[q] = at(src[q], b1, b2);
+            for (size_t q = 0; q < dst.size(); ++q) at(dst[q], b1, b2) = zero ? 0.0 : tmp[q];
+        }
+}
+
+void fill_halo_tracer(const Grid& g, dvec& c) {          /* halo_regions.jl:37-47 */
+    fill_face(g, c, 0, 0, 0); fill_face(g, c, 0, 1, 0);
+    fill_face(g, c, 1, 0, 0); fill_face(g, c, 1, 1, 0);
+    fill_face(g, c, 2, 0, 0); fill_face(g, c, 2, 1, 0);
+}
+void fill_halo_Gc(const Grid& g, dvec& c) {              /* halo_regions.jl:49-56 */
+    fill_face(g, c, 0, 1, 2); fill_face(g, c, 1, 1, 2); fill_face(g, c, 2, 1, 2);
+}
+void fill_halo_u(const Grid& g, dvec& c) {               /* halo_regions.jl:64-72 */
+    fill_face(g, c, 0, 1, 1); fill_face(g, c, 0, 0, 0);
+    fill_face(g, c, 1, 0, 0); fill_face(g, c, 1, 1, 0);
+    fill_face(g, c, 2, 0, 0); fill_face(g, c, 2, 1, 0);
+}
+void fill_halo_v(const Grid& g, dvec& c) {               /* halo_regions.jl:74-82 */
+    fill_face(g, c, 1, 1, 1); fill_face(g, c, 0, 0, 0); fill_face(g, c, 0, 1, 0);
+    fill_face(g, c, 1, 0, 0); fill_face(g, c, 2, 0, 0); fill_face(g, c, 2, 1, 0);
+}
+void fill_halo_w(const Grid& g, dvec& c) {               /* halo_regions.jl:84-92 */
+    fill_face(g, c, 2, 1, 1); fill_face(g, c, 0, 0, 0); fill_face(g, c, 0, 1, 0);
+    fill_face(g, c, 1, 0, 0); fill_face(g, c, 1, 1, 0); fill_face(g, c, 2, 0, 0);
+}
+
+/* ---------------------------------------------------------------------------------------- */
+/* Particle advection, src/Individuals/Advection/ (all files)                                         */
+/* ---------------------------------------------------------------------------------------- */
+
+/* particle_boundary_condition, particle_advection_kernels.jl:2-11 */
+inline double bc_pos(double x, double xr, int topo) {
+    const double xl = 0.0;
+    if (topo == PI_PERIODIC) {
+        if (x > xr) return xl + (x - xr);
+        if (x < xl) return xr - (xl - x);
+        return x;
+    }
+    if (x > xr) return xr - (x - xr) * 1.0;
+    if (x < xl) return xl + (xl - x) * 1.0;
+    return x;
+}
+
+/* normalized trilinear interpolation, interpolation.jl:12-83. comp 0/1/2 = u/v/w. The face
+ * coordinate along the component's own axis uses +1, the others +0.5. */
+double itpl(orc_model* m, const dvec& f, int comp, double x, double y, double z, int ac) {
+    const Grid& g = m->g;
+    double fx = jl_mulb(comp == 0 ? x + 1.0 : x + 0.5, ac);
+    double fy = jl_mulb(comp == 1 ? y + 1.0 : y + 0.5, ac);
+    double fz = jl_mulb(comp == 2 ? z + 1.0 : z + 0.5, ac);
+    double xd = jl_mod1(fx); long xi = (long)jl_trunc(fx);
+    double yd = jl_mod1(fy); long yi = (long)jl_trunc(fy);
+    double zd = jl_mod1(fz); long zi = (long)jl_trunc(fz);
+    long i = clampi(m, xi + g.Hx, 1, g.Gx - 1);
+    long j = clampi(m, yi + g.Hy, 1, g.Gy - 1);
+    long k = clampi(m, zi + g.Hz, 1, g.Gz - 1);
+    double w000 = (1.0 - xd) * (1.0 - yd) * (1.0 - zd);
+    double w001 = (1.0 - xd) * (1.0 - yd) * zd;
+    double w010 = (1.0 - xd) * yd * (1.0 - zd);
+    double w011 = (1.0 - xd) * yd * zd;
+    double w100 = xd * (1.0 - yd) * (1.0 - zd);
+    double w101 = xd * (1.0 - yd) * zd;
+    double w110 = xd * yd * (1.0 - zd);
+    double w111 = xd * yd * zd;
+    double d0, d1;   /* ΔxC / ΔyC are constant; ΔzC depends on the corner's k */
+    if (comp == 0) { d0 = g.dx; d1 = g.dx; }
+    else if (comp == 1) { d0 = g.dy; d1 = g.dy; }
+    else { d0 = g.dzC1(k); d1 = g.dzC1(k + 1); }
+    return w000 * f[g.id(i, j, k)] / d0
+         + w001 * f[g.id(i, j, k + 1)] / d1
+         + w010 * f[g.id(i, j + 1, k)] / d0
+         + w011 * f[g.id(i, j + 1, k + 1)] / d1
+         + w100 * f[g.id(i + 1, j, k)] / d0
+         + w101 * f[g.id(i + 1, j, k + 1)] / d1
+         + w110 * f[g.id(i + 1, j + 1, k)] / d0
+         + w111 * f[g.id(i + 1, j + 1, k + 1)] / d1;
+}
+
+/* vel_interpolate_kernel!, particle_advection_kernels.jl:26-31 */
+void vel_interpolate(orc_model* m, Species& s, const dvec& X, const dvec& Y, const dvec& Z,
+                     const dvec& U, const dvec& V, const dvec& W) {
+    int64_t C = m->C;
+    for (int64_t i = 0; i < C; ++i) {
+        int ac = s.ac[i];
+        m->vu1[i] = jl_mulb(itpl(m, U, 0, X[i], Y[i], Z[i], ac), ac);
+        m->vv1[i] = jl_mulb(itpl(m, V, 1, X[i], Y[i], Z[i], ac), ac);
+        m->vw1[i] = jl_mulb(itpl(m, W, 2, X[i], Y[i], Z[i], ac), ac);
+    }
+}
+
+/* calc_coord_kernel!, particle_advection_kernels.jl:40-45 */
+void calc_coord(orc_model* m, Species& s, dvec& oX, dvec& oY, dvec& oZ,
+                const dvec& U, const dvec& V, const dvec& W, double dT, double weight) {
+    int64_t C = m->C;
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < C; ++i) {
+        int ac = s.ac[i];
+        double x = s.x[i], y = s.y[i], z = s.z[i];
+        oX[i] = x + jl_mulb(weight * U[i] * dT, ac);
+        oY[i] = y + jl_mulb(weight * V[i] * dT, ac);
+        oZ[i] = z - jl_mulb(weight * W[i] * dT, ac);
+    }
+}
+
+/* particle_boundaries_kernel!, particle_advection_kernels.jl:13-17 */
+void particle_boundaries(orc_model* m, Species& s, dvec& X, dvec& Y, dvec& Z) {
+    const Grid& g = m->g;
+    int64_t C = m->C;
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < C; ++i) {
+        int ac = s.ac[i];
+        X[i] = jl_mulb(bc_pos(X[i], (double)g.Nx, g.tx), ac);
+        Y[i] = jl_mulb(bc_pos(Y[i], (double)g.Ny, g.ty), ac);
+        Z[i] = jl_mulb(bc_pos(Z[i], (double)g.Nz, g.tz), ac);
+    }
+}
+
+/* particle_advection!, particle_advection.jl:2-56 (RK4) */
+void particle_advection(orc_model* m, Species& s, double dT) {
+    int64_t C = m->C;
+    vel_interpolate(m, s, s.x, s.y, s.z, m->u0, m->v0, m->w0);
+    for (int64_t i = 0; i < C; ++i) { m->vu2[i] = m->vu1[i]; m->vv2[i] = m->vv1[i]; m->vw2[i] = m->vw1[i]; }
+    calc_coord(m, s, m->vx, m->vy, m->vz, m->vu1, m->vv1, m->vw1, dT, 0.5);
+    particle_boundaries(m, s, m->vx, m->vy, m->vz);
+    /* stage 2 */
+    vel_interpolate(m, s, m->vx, m->vy, m->vz, m->uh, m->vh, m->wh);
+    for (int64_t i = 0; i < C; ++i) {
+        m->vu2[i] = m->vu2[i] + m->vu1[i] * 2.0; m->vv2[i] = m->vv2[i] + m->vv1[i] * 2.0;
+        m->vw2[i] = m->vw2[i] + m->vw1[i] * 2.0;
+    }
+    calc_coord(m, s, m->vx, m->vy, m->vz, m->vu1, m->vv1, m->vw1, dT, 0.5);
+    particle_boundaries(m, s, m->vx, m->vy, m->vz);
+    /* stage 3 */
+    vel_interpolate(m, s, m->vx, m->vy, m->vz, m->uh, m->vh, m->wh);
+    for (int64_t i = 0; i < C; ++i) {
+        m->vu2[i] = m->vu2[i] + m->vu1[i] * 2.0; m->vv2[i] = m->vv2[i] + m->vv1[i] * 2.0;
+        m->vw2[i] = m->vw2[i] + m->vw1[i] * 2.0;
+    }
+    calc_coord(m, s, m->vx, m->vy, m->vz, m->vu1, m->vv1, m->vw1, dT, 1.0);
+    particle_boundaries(m, s, m->vx, m->vy, m->vz);
+    /* stage 4 */
+    vel_interpolate(m, s, m->vx, m->vy, m->vz, m->u1, m->v1, m->w1);
+    for (int64_t i = 0; i < C; ++i) {
+        m->vu2[i] = m->vu2[i] + m->vu1[i]; m->vv2[i] = m->vv2[i] + m->vv1[i];
+        m->vw2[i] = m->vw2[i] + m->vw1[i];
+    }
+    for (int64_t i = 0; i < C; ++i) {
+        m->vu2[i] = m->vu2[i] / 6.0; m->vv2[i] = m->vv2[i] / 6.0; m->vw2[i] = m->vw2[i] / 6.0;
+    }
+    calc_coord(m, s, s.x, s.y, s.z, m->vu2, m->vv2, m->vw2, dT, 1.0);
+    particle_boundaries(m, s, s.x, s.y, s.z);
+}
+
+/* particle_diffusion!, particle_diffusion.jl:16-33 */
+void particle_diffusion(orc_model* m, Species& s, int spi, double dT) {
+    const Grid& g = m->g;
+    int64_t C = m->C;
+    double kx = m->bgc.kappa_hP, ky = m->bgc.kappa_hP, kz = m->bgc.kappa_vP;
+    for (int64_t i = 0; i < C; ++i)
+        pi_draw3(m->seed, (uint32_t)m->iteration, (uint32_t)spi, PI_DRAW_DIFFUSION, (uint32_t)i,
+                 &m->rx[i], &m->ry[i], &m->rz[i]);
+    for (int64_t i = 0; i < C; ++i) {
+        m->rx[i] = (m->rx[i] - 0.5) * 2.0; m->ry[i] = (m->ry[i] - 0.5) * 2.0; m->rz[i] = (m->rz[i] - 0.5) * 2.0;
+    }
+    for (int64_t i = 0; i < C; ++i) {   /* calc_diffusion_kernel!, :2-8; ΔzC at zi+Hz of the stored zi */
+        long kk = clampi(m, (long)s.zi[i] + g.Hz, 1, g.Gz);
+        m->rx[i] = m->rx[i] * sqrt(kx * dT) / g.dx;
+        m->ry[i] = m->ry[i] * sqrt(ky * dT) / g.dy;
+        m->rz[i] = m->rz[i] * sqrt(kz * dT) / g.dzC1(kk);
+    }
+    for (int64_t i = 0; i < C; ++i) {
+        int ac = s.ac[i];
+        s.x[i] = s.x[i] + jl_mulb(m->rx[i], ac);
+        s.y[i] = s.y[i] + jl_mulb(m->ry[i], ac);
+        s.z[i] = s.z[i] + jl_mulb(m->rz[i], ac);
+    }
+    particle_boundaries(m, s, s.x, s.y, s.z);
+}
+
+/* ---------------------------------------------------------------------------------------- */
+/* Particle-grid coupling, src/Individuals/utils.jl                                            */
+/* ---------------------------------------------------------------------------------------- */
+
+void find_inds(orc_model* m, Species& s) {     /* utils.jl:2-7 */
+    const Grid& g = m->g;
+    for (int64_t i = 0; i < m->C; ++i) {
+        int ac = s.ac[i];
+        s.xi[i] = clampi(m, (long)jl_trunc(jl_mulb(s.x[i] + 1.0, ac)) + g.Hx, 1, g.Gx);
+        s.yi[i] = clampi(m, (long)jl_trunc(jl_mulb(s.y[i] + 1.0, ac)) + g.Hy, 1, g.Gy);
+        s.zi[i] = clampi(m, (long)jl_trunc(jl_mulb(s.z[i] + 1.0, ac)) + g.Hz, 1, g.Gz);
+    }
+}
+
+inline size_t cell_of(orc_model* m, const Species& s, int64_t i) {
+    const Grid& g = m->g;
+    long a = clampi(m, (long)s.xi[i], 1, g.Gx);
+    long b = clampi(m, (long)s.yi[i], 1, g.Gy);
+    long c = clampi(m, (long)s.zi[i], 1, g.Gz);
+    return g.id(a, b, c);
+}
+
+void acc_chl(orc_model* m, Species& s) {       /* utils.jl:33-36 */
+    for (int64_t i = 0; i < m->C; ++i) m->Chl[cell_of(m, s, i)] += jl_mulb(s.Chl[i], s.ac[i]);
+}
+void acc_counts(orc_model* m, Species& s) {    /* utils.jl:44-47 */
+    for (int64_t i = 0; i < m->C; ++i) m->pop[cell_of(m, s, i)] += (double)s.ac[i];
+}
+
+void calc_par(orc_model* m, int ki) {          /* utils.jl:55-63 */
+    const Grid& g = m->g;
+    for (int j = 1; j <= g.Ny; ++j)
+        for (int i = 1; i <= g.Nx; ++i) {
+            long ii = i + g.Hx, jj = j + g.Hy, kk = ki + g.Hz;
+            size_t c = g.id(ii, jj, kk);
+            size_t f = (size_t)(i - 1) + (size_t)g.Nx * (size_t)(j - 1);
+            double atten = (m->Chl[c] / g.vol(kk) * m->bgc.kc + m->bgc.kw) * g.dzF1(kk);
+            m->par[c] = m->PARF[f] * (1.0 - pi_exp(-atten)) / atten;
+            m->PARF[f] = m->PARF[f] * pi_exp(-atten);
+        }
+}
+
+void find_NPT(orc_model* m, Species& s) {      /* utils.jl:14-25 */
+    for (int64_t i = 0; i < m->C; ++i) {
+        size_t c = cell_of(m, s, i);
+        int ac = s.ac[i];
+        m->tNH4[i] = jl_mulb(jl_max(0.0, m->tr[PI_NH4][c]), ac);
+        m->tNO3[i] = jl_mulb(jl_max(0.0, m->tr[PI_NO3][c]), ac);
+        m->tPO4[i] = jl_mulb(jl_max(0.0, m->tr[PI_PO4][c]), ac);
+        m->tDOC[i] = jl_mulb(jl_max(0.0, m->tr[PI_DOC][c]), ac);
+        m->tDFe[i] = jl_mulb(jl_max(0.0, m->tr[PI_DFe][c]), ac);
+        m->tpar[i] = jl_mulb(m->par[c], ac);
+        m->tdpar[i] = jl_mulb(m->par[c] - m->par0[c], ac);
+        m->tT[i] = jl_mulb(m->temp[c], ac);
+        m->tpop[i] = jl_mulb(m->pop[c], ac);
+    }
+}
+
+/* ---------------------------------------------------------------------------------------- */
+/* QuotaMode physiology, src/Individuals/Plankton/QuotaMode/ (all files)                             */
+/* ---------------------------------------------------------------------------------------- */
+
+/* shape functions, Individuals/utils.jl:109-121 */
+inline double shape_func_dec(double x, double xmax, double k, int pw) {
+    double fx = jl_max(0.0, jl_min(1.0, 1.0 - x / xmax));
+    return pi_pow_int(fx, pw) / (k + pi_pow_int(fx, pw));
+}
+inline double shape_func_inc(double x, double xmax, double k, int pw) {
+    double fx = jl_max(0.0, jl_min(1.0, 1.0 - x / xmax));
+    double reg = pi_pow_int(fx, pw) / (k + pi_pow_int(fx, pw));
+    return 1.0 - reg;
+}
+
+inline double tempFunc_PS(double T, const pi_quota_params& p) {   /* growth_kernels.jl:2-9 */
+    double x = T - p.Topt, xmax = p.Tmax - p.Topt;
+    double regT = shape_func_dec(x, xmax, F_4em2, 4);
+    double k = pi_exp(-p.Ea / (F_RGAS * (T + F_T0))) * regT;
+    k = jl_max(0.0, k);
+    double OGT_rate = pi_exp(-p.Ea / (F_RGAS * (p.Topt + F_T0)));
+    return jl_min(1.0, k / OGT_rate);
+}
+inline double tempFunc(double T, const pi_quota_params& p) {      /* growth_kernels.jl:12-17 */
+    double k = pi_exp(-p.Ea / (F_RGAS * (T + F_T0)));
+    k = jl_max(0.0, k);
+    double OGT_rate = pi_exp(-p.Ea / (F_RGAS * (p.Topt + F_T0)));
+    return jl_min(1.0, k / OGT_rate);
+}
+
+void plankton_growth(orc_model* m, Species& s, int spi, double dT, double t) {
+    const pi_quota_params& p = s.p;
+    int64_t C = m->C;
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < C; ++i) {
+        int ac = s.ac[i];
+        double par = m->tpar[i], T = m->tT[i], pop = m->tpop[i];
+        double NH4 = m->tNH4[i], NO3 = m->tNO3[i], PO4 = m->tPO4[i], DOC = m->tDOC[i];
+        /* calc_inorganic_uptake_kernel!, growth_kernels.jl:48-56 with calc_PS :20-25 and
+         * calc_NP_uptake :28-39 */
+        {
+            double aI = par * p.alpha * p.Phi;
+            double PCm = p.PCmax * tempFunc_PS(T, p);
+            double PS = PCm * (1.0 - pi_exp(-aI / jl_max(F_1em30, PCm) * s.Chl[i] / jl_max(F_1em30, s.Bm[i]))) * s.Bm[i];
+            s.PS[i] = jl_mulb(PS, ac);
+            double Bm = s.Bm[i], Cq = s.Cq[i], Nq = s.Nq[i], Pq = s.Pq[i];
+            double Qn = (Nq + Bm * p.R_NC) / jl_max(F_1em30, Bm + Cq);
+            double Qp = (Pq + Bm * p.R_PC) / jl_max(F_1em30, Bm + Cq);
+            double regQN = shape_func_dec(Qn, p.Nqmax, F_1em4, 4);
+            double regQP = shape_func_dec(Qp, p.Pqmax, F_1em4, 4);
+            double VNH4 = jl_mulb(p.VNH4max * regQN * NH4 / jl_max(F_1em30, NH4 + p.KsatNH4) * tempFunc(T, p) * Bm, ac);
+            double VNO3 = jl_mulb(p.VNO3max * regQN * NO3 / jl_max(F_1em30, NO3 + p.KsatNO3) * tempFunc(T, p) * Bm, ac);
+            double VPO4 = jl_mulb(p.VPO4max * regQP * PO4 / jl_max(F_1em30, PO4 + p.KsatPO4) * tempFunc(T, p) * Bm, ac);
+            s.VNH4[i] = jl_min(VNH4, NH4 / dT / jl_max(1.0, pop));
+            s.VNO3[i] = jl_min(VNO3, NO3 / dT / jl_max(1.0, pop));
+            s.VPO4[i] = jl_min(VPO4, PO4 / dT / jl_max(1.0, pop));
+        }
+        /* update_quotas_1_kernel!, :64-69 */
+        s.Cq[i] += s.PS[i] * dT;
+        s.Pq[i] += s.VPO4[i] * dT;
+        s.Nq[i] += (s.VNH4[i] + s.VNO3[i]) * dT;
+        /* calc_organic_uptake_kernel!, :78-84 with calc_DOC_uptake :41-46 */
+        {
+            double Cq = s.Cq[i], Bm = s.Bm[i];
+            double Qc = Cq / jl_max(F_1em30, Bm + Cq);
+            double regQ = shape_func_dec(Qc, p.Cqmax, F_1em4, 4);
+            double VN = p.VDOCmax * regQ * DOC / jl_max(F_1em30, DOC + p.KsatDOC) * tempFunc(T, p) * Bm;
+            double VDOC = jl_mulb(jl_min(VN, DOC / dT / jl_max(1.0, pop)), ac);
+            s.VDOC[i] = jl_mulb(VDOC, jl_isless(F_1em2, s.PS[i] / (VDOC + s.PS[i])));
+        }
+        /* calc_ρChl_kernel!, :92-97 */
+        s.rChl[i] = jl_mulb(jl_mulb(s.PS[i] / jl_max(F_1em30, s.Bm[i]) * p.Chl2N /
+                                    jl_max(F_1em30, par * p.alpha * p.Phi * s.Chl[i] / s.Bm[i]),
+                                    jl_isless(F_1em1, par)), ac);
+        /* calc_respir_kernel!, :105-108 */
+        s.resp[i] = jl_mulb(p.respir * s.Bm[i] * tempFunc(T, p), ac);
+        /* update_quotas_2_kernel!, :117-124 */
+        s.Cq[i] = s.Cq[i] + (s.VDOC[i] - s.resp[i]) * dT;
+        s.Bm[i] = s.Bm[i] - jl_max(0.0, (0.0 - s.Cq[i]));
+        s.Nq[i] = s.Nq[i] + jl_max(0.0, (0.0 - s.Cq[i])) * p.R_NC;
+        s.Pq[i] = s.Pq[i] + jl_max(0.0, (0.0 - s.Cq[i])) * p.R_PC;
+        s.Cq[i] = s.Cq[i] + jl_max(0.0, (0.0 - s.Cq[i]));
+        /* calc_BS_kernel!, :132-138 */
+        {
+            double mn = jl_min(jl_min(s.Cq[i], s.Nq[i] / p.R_NC), s.Pq[i] / p.R_PC);
+            s.BS[i] = jl_mulb(mn * p.k_mtb, ac);
+            double mn2 = jl_min(jl_min(s.Cq[i], s.Nq[i] / p.R_NC), s.Pq[i] / p.R_PC);
+            s.exu[i] = jl_mulb(jl_max(0.0, s.Cq[i] - mn2) * p.k_mtb, ac);
+        }
+        /* update_biomass_kernel!, :146-154 */
+        s.Bm[i] += dT * s.BS[i];
+        s.Cq[i] -= dT * (s.BS[i] + s.exu[i]);
+        s.Nq[i] -= dT * s.BS[i] * p.R_NC;
+        s.Pq[i] -= dT * s.BS[i] * p.R_PC;
+        s.Chl[i] += dT * s.BS[i] * p.R_NC * s.rChl[i];
+        s.age[i] += jl_mulb(dT / 3600.0, ac);
+        /* update_cellsize_kernel!, :163-166 */
+        s.Sz[i] = s.Bm[i] / (p.Cquota * p.Nsuper);
+        /* calc_graz_quadratic_kernel!, division_death_probability.jl:49-52 */
+        s.graz[i] = jl_mulb(pop * p.grz_P, ac);
+        /* calc_mort_kernel!, :60-63 */
+        s.mort[i] = jl_mulb(p.mort_P * shape_func_dec(s.Sz[i], p.mort_reg, F_1em5, 4), ac);
+        /* calc_dvid_kernel!, :26-30 with calc_division :7-12 */
+        {
+            double dv;
+            int ty = (int)p.dvid_type;
+            if (ty == 1) dv = p.dvid_P * shape_func_inc(s.Sz[i], p.dvid_reg, F_2em3, 2);
+            else if (ty == 2) dv = p.dvid_P * shape_func_inc(fmod(t, 86400.0) / 3600.0, p.dvid_reg, F_1em5, 4);
+            else dv = p.dvid_P * shape_func_inc(s.Sz[i], p.dvid_reg, F_1em3, 4)
+                      * shape_func_inc(fmod(t, 86400.0) / 3600.0, p.dvid_reg2, F_1em5, 4);
+            s.dvid[i] = jl_mulb(dv, ac);
+        }
+    }
+    /* get_probability!, division_death_probability.jl:95-107 */
+    for (int64_t i = 0; i < C; ++i) {
+        double r0, r1, r2;
+        pi_draw3(m->seed, (uint32_t)m->iteration, (uint32_t)spi, PI_DRAW_DECISION, (uint32_t)i, &r0, &r1, &r2);
+        m->rx[i] = r0; m->ry[i] = r1; m->rz[i] = r2;
+    }
+    for (int64_t i = 0; i < C; ++i) {
+        int ac = s.ac[i];
+        s.graz[i] = (double)(jl_isless(m->rx[i], s.graz[i] * dT) && ac);
+        s.mort[i] = (double)(jl_isless(m->ry[i], s.mort[i] * dT) && ac);
+        s.dvid[i] = (double)(jl_isless(m->rz[i], s.dvid[i] * dT) && ac);
+    }
+}
+
+/* calc_loss_kernel!, QuotaMode/consume_loss.jl:17-26, then inactivate!, utils.jl:103-105 */
+void calc_loss(orc_model* m, Species& s, const dvec& loss, double fC, double fN, double fP) {
+    const pi_quota_params& p = s.p;
+    for (int64_t i = 0; i < m->C; ++i) {
+        size_t c = cell_of(m, s, i);
+        int ac = s.ac[i];
+        double Bm = s.Bm[i], Cq = s.Cq[i], Nq = s.Nq[i], Pq = s.Pq[i], l = loss[i];
+        m->plk[PI_DOC][c] += jl_mulb((Bm + Cq) * fC, ac) * l;
+        m->plk[PI_DON][c] += jl_mulb((Bm * p.R_NC + Nq) * fN, ac) * l;
+        m->plk[PI_DOP][c] += jl_mulb((Bm * p.R_PC + Pq) * fP, ac) * l;
+        m->plk[PI_POC][c] += jl_mulb((Bm + Cq) * (1.0 - fC), ac) * l;
+        m->plk[PI_PON][c] += jl_mulb((Bm * p.R_NC + Nq) * (1.0 - fN), ac) * l;
+        m->plk[PI_POP][c] += jl_mulb((Bm * p.R_PC + Pq) * (1.0 - fP), ac) * l;
+    }
+    for (int64_t i = 0; i < m->C; ++i) s.ac[i] = (uint8_t)(s.ac[i] && jl_isless(loss[i], 1.0));
+}
+
+/* diags_proc_kernel!, Diagnostics/diagnostics_kernels.jl:4-7 */
+void diags_proc(orc_model* m, Species& s, dvec& d, const dvec* proc) {
+    for (int64_t i = 0; i < m->C; ++i) {
+        size_t c = cell_of(m, s, i);
+        d[c] += proc ? jl_mulb((*proc)[i], s.ac[i]) : (double)(s.ac[i] && s.ac[i]);
+    }
+}
+
+/* plankton_update!, QuotaMode/plankton_update.jl:1-34 */
+bool plankton_update(orc_model* m, Species& s, int spi, double dT, double t) {
+    const pi_quota_params& p = s.p;
+    int64_t C = m->C;
+    diags_proc(m, s, s.d_graz, &s.graz);
+    calc_loss(m, s, s.graz, p.grazFracC, p.grazFracN, p.grazFracP);          /* grazing!   */
+    diags_proc(m, s, s.d_mort, &s.mort);
+    calc_loss(m, s, s.mort, p.mortFracC, p.mortFracN, p.mortFracP);          /* mortality! */
+    for (int64_t i = 0; i < C; ++i) s.dvid[i] = jl_mulb(s.dvid[i], s.ac[i]);
+    diags_proc(m, s, s.d_dvid, &s.dvid);
+    double dvidnum = 0.0;
+    std::vector<int64_t> free_slots;
+    for (int64_t i = 0; i < C; ++i) {
+        dvidnum += s.dvid[i] * (double)s.ac[i];
+        if (!s.ac[i]) free_slots.push_back(i + 1);                          /* 1-based */
+    }
+    if (dvidnum > (double)free_slots.size()) {
+        char buf[160];
+        snprintf(buf, sizeof buf, "number of individual exceeds the capacity at timestep %s days",
+                 std::to_string(t / 86400.0).c_str());
+        m->err = buf;
+        m->err_flags |= ERR_CAPACITY;
+        return false;
+    }
+    /* divide!, QuotaMode/division_death.jl:69-77 */
+    double acc = 0.0;
+    for (int64_t i = 0; i < C; ++i) { acc += s.dvid[i]; m->tidc[i] = acc; m->tidc_int[i] = (int64_t)acc; }
+    for (int64_t i = 0; i < C; ++i)                                           /* get_tind!   */
+        if (s.dvid[i] == 1.0) s.idx[i] = free_slots[(size_t)m->tidc_int[i] - 1];
+    for (int64_t i = 0; i < C; ++i)                                           /* copy :28-45 */
+        if (s.dvid[i] == 1.0 && s.idx[i] != 0) {
+            int64_t d = s.idx[i] - 1;
+            s.x[d] = s.x[i]; s.y[d] = s.y[i]; s.z[d] = s.z[i];
+            s.Sz[d] = s.Sz[i]; s.Bm[d] = s.Bm[i]; s.Cq[d] = s.Cq[i]; s.Nq[d] = s.Nq[i]; s.Pq[d] = s.Pq[i];
+            s.Chl[d] = s.Chl[i]; s.gen[d] = s.gen[i]; s.ac[d] = s.ac[i]; s.dvid[d] = s.dvid[i];
+        }
+    for (int64_t i = 0; i < C; ++i) {                                         /* divide_to_half :53-63 */
+        double f = (2.0 - s.dvid[i]) / 2.0;
+        s.Sz[i] *= f; s.Bm[i] *= f; s.Cq[i] *= f; s.Nq[i] *= f; s.Pq[i] *= f; s.Chl[i] *= f;
+        s.gen[i] += s.dvid[i];
+        s.age[i] *= (1.0 - s.dvid[i]);
+    }
+    for (int64_t i = 0; i < C; ++i) s.idx[i] = 0;
+    plankton_growth(m, s, spi, dT, t);
+    /* calc_consume_kernel!, consume_loss.jl:2-9 */
+    for (int64_t i = 0; i < C; ++i) {
+        size_t c = cell_of(m, s, i);
+        int ac = s.ac[i];
+        m->plk[PI_DIC][c] += jl_mulb((s.resp[i] - s.PS[i]) * dT, ac);
+        m->plk[PI_DOC][c] += jl_mulb((s.exu[i] - s.VDOC[i]) * dT, ac);
+        m->plk[PI_NH4][c] += jl_mulb(-s.VNH4[i] * dT, ac);
+        m->plk[PI_NO3][c] += jl_mulb(-s.VNO3[i] * dT, ac);
+        m->plk[PI_PO4][c] += jl_mulb(-s.VPO4[i] * dT, ac);
+    }
+    diags_proc(m, s, s.d_num, nullptr);
+    return true;
+}
+
+/* ---------------------------------------------------------------------------------------- */
+/* Tracer update, src/Biogeochemistry/ (all files)                                                       */
+/* ---------------------------------------------------------------------------------------- */
+
+/* Difference operators with landmask, Advection/operaters.jl:1-14 */
+struct Ops {
+    const Grid& g;
+    inline double dxp(const dvec& c, long i, long j, long k) const { return jl_mulb(jl_mulb(c[g.id(i + 1, j, k)] - c[g.id(i, j, k)], g.L(i + 1, j, k)), g.L(i, j, k)); }
+    inline double dyp(const dvec& c, long i, long j, long k) const { return jl_mulb(jl_mulb(c[g.id(i, j + 1, k)] - c[g.id(i, j, k)], g.L(i, j + 1, k)), g.L(i, j, k)); }
+    inline double dzp(const dvec& c, long i, long j, long k) const { return jl_mulb(jl_mulb(c[g.id(i, j, k)] - c[g.id(i, j, k + 1)], g.L(i, j, k + 1)), g.L(i, j, k)); }
+    inline double dx0(const dvec& c, long i, long j, long k) const { return jl_mulb(jl_mulb(c[g.id(i, j, k)] - c[g.id(i - 1, j, k)], g.L(i, j, k)), g.L(i - 1, j, k)); }
+    inline double dy0(const dvec& c, long i, long j, long k) const { return jl_mulb(jl_mulb(c[g.id(i, j, k)] - c[g.id(i, j - 1, k)], g.L(i, j, k)), g.L(i, j - 1, k)); }
+    inline double dz0(const dvec& c, long i, long j, long k) const { return jl_mulb(jl_mulb(c[g.id(i, j, k - 1)] - c[g.id(i, j, k)], g.L(i, j, k)), g.L(i, j, k - 1)); }
+    inline double dxm(const dvec& c, long i, long j, long k) const { return jl_mulb(jl_mulb(c[g.id(i - 1, j, k)] - c[g.id(i - 2, j, k)], g.L(i - 1, j, k)), g.L(i - 2, j, k)); }
+    inline double dym(const dvec& c, long i, long j, long k) const { return jl_mulb(jl_mulb(c[g.id(i, j - 1, k)] - c[g.id(i, j - 2, k)], g.L(i, j - 1, k)), g.L(i, j - 2, k)); }
+    inline double dzm(const dvec& c, long i, long j, long k) const { return jl_mulb(jl_mulb(c[g.id(i, j, k - 2)] - c[g.id(i, j, k - 1)], g.L(i, j, k - 1)), g.L(i, j, k - 2)); }
+};
+
+/* θ and Ψ of DST3FL.jl:19-53 */
+inline double theta(double dnum, double d0) {
+    return fabs(d0) * F_THMAX <= fabs(dnum) ? copysign(F_THMAX, dnum * d0) : dnum / d0;
+}
+inline double psi_lim(double cfl, double th) {
+    double d0 = (2.0 - cfl) * (1.0 - cfl) / 6.0;
+    double d1 = (1.0 - cfl * cfl) / 6.0;
+    return jl_max(0.0, jl_min(jl_min(1.0, d0 + d1 * th), th * (1.0 - cfl) / (cfl + F_1em20)));
+}
+
+/* adv_flux_x/y/z, DST3FL.jl:63-73 */
+double adv_flux_x(const Grid& g, const Ops& o, long i, long j, long k, const dvec& u, const dvec& c, double dT) {
+    double uu = u[g.id(i, j, k)];
+    double cfl = fabs(uu * dT / g.dx);
+    double tr = g.Axk(k) * uu;
+    double d0 = o.dx0(c, i, j, k);
+    double psp = psi_lim(cfl, theta(o.dxm(c, i, j, k), d0));
+    double psm = psi_lim(cfl, theta(o.dxp(c, i, j, k), d0));
+    return 0.5 * (tr + fabs(tr)) * (c[g.id(i - 1, j, k)] + psp * d0)
+         + 0.5 * (tr - fabs(tr)) * (c[g.id(i, j, k)] - psm * d0);
+}
+double adv_flux_y(const Grid& g, const Ops& o, long i, long j, long k, const dvec& v, const dvec& c, double dT) {
+    double vv = v[g.id(i, j, k)];
+    double cfl = fabs(vv * dT / g.dy);
+    double tr = g.Ayk(k) * vv;
+    double d0 = o.dy0(c, i, j, k);
+    double psp = psi_lim(cfl, theta(o.dym(c, i, j, k), d0));
+    double psm = psi_lim(cfl, theta(o.dyp(c, i, j, k), d0));
+    return 0.5 * (tr + fabs(tr)) * (c[g.id(i, j - 1, k)] + psp * d0)
+         + 0.5 * (tr - fabs(tr)) * (c[g.id(i, j, k)] - psm * d0);
+}
+double adv_flux_z(const Grid& g, const Ops& o, long i, long j, long k, const dvec& w, const dvec& c, double dT) {
+    double ww = w[g.id(i, j, k)];
+    double cfl = fabs(ww * dT / g.dzC1(k));
+    double tr = g.Az() * ww;
+    double d0 = o.dz0(c, i, j, k);
+    double psp = psi_lim(cfl, theta(o.dzm(c, i, j, k), d0));   /* Ψz⁺ uses θz⁺ = δz⁻/δz⁰ */
+    double psm = psi_lim(cfl, theta(o.dzp(c, i, j, k), d0));   /* Ψz⁻ uses θz⁻ = δz⁺/δz⁰ */
+    return 0.5 * (tr + fabs(tr)) * (c[g.id(i, j, k)] + psm * d0)
+         + 0.5 * (tr - fabs(tr)) * (c[g.id(i, j, k - 1)] - psp * d0);
+}
+
+/* tracer_advection!, Advection/multi_dim_adv.jl:111-135 */
+void tracer_advection(orc_model* m, double dT) {
+    const Grid& g = m->g;
+    Ops o{g};
+    for (int n = 0; n < PI_NTRACERS; ++n) m->tt[n] = m->tr[n];
+    for (int dir = 0; dir < 3; ++dir) {
+        const dvec& vel = dir == 0 ? m->u1 : dir == 1 ? m->v1 : m->w1;
+        #pragma omp parallel for schedule(static)
+        for (int n = 0; n < PI_NTRACERS; ++n) {
+            dvec& Gc = m->Gcs[n];
+            const dvec& cT = m->tt[n];
+            for (long k = g.Hz + 1; k <= g.Hz + g.Nz; ++k)       /* calc_Gcˣ/ʸ/ᶻ_kernel! */
+                for (long j = g.Hy + 1; j <= g.Hy + g.Ny; ++j)
+                    for (long i = g.Hx + 1; i <= g.Hx + g.Nx; ++i)
+                        Gc[g.id(i, j, k)] = dir == 0 ? adv_flux_x(g, o, i, j, k, vel, cT, dT)
+                                          : dir == 1 ? adv_flux_y(g, o, i, j, k, vel, cT, dT)
+                                                     : adv_flux_z(g, o, i, j, k, vel, cT, dT);
+        }
+        for (int n = 0; n < PI_NTRACERS; ++n) fill_halo_Gc(g, m->Gcs[n]);
+        #pragma omp parallel for schedule(static)
+        for (int n = 0; n < PI_NTRACERS; ++n) {                    /* multi_dim_x/y/z_kernel! */
+            dvec& ct = m->tt[n];
+            const dvec& Gc = m->Gcs[n];
+            const dvec& c = m->tr[n];
+            for (long k = g.Hz + 1; k <= g.Hz + g.Nz; ++k)
+                for (long j = g.Hy + 1; j <= g.Hy + g.Ny; ++j)
+                    for (long i = g.Hx + 1; i <= g.Hx + g.Nx; ++i) {
+                        size_t q = g.id(i, j, k);
+                        double ftr;
+                        double dG;
+                        if (dir == 0) {
+                            dG = o.dxp(Gc, i, j, k);
+                            ftr = jl_mulb(jl_mulb(g.Axk(k) * vel[g.id(i + 1, j, k)] - g.Axk(k) * vel[q], g.L(i + 1, j, k)), g.L(i, j, k));
+                        } else if (dir == 1) {
+                            dG = o.dyp(Gc, i, j, k);
+                            ftr = jl_mulb(jl_mulb(g.Ayk(k) * vel[g.id(i, j + 1, k)] - g.Ayk(k) * vel[q], g.L(i, j + 1, k)), g.L(i, j, k));
+                        } else {
+                            dG = o.dzp(Gc, i, j, k);
+                            ftr = jl_mulb(jl_mulb(g.Az() * vel[q] - g.Az() * vel[g.id(i, j, k + 1)], g.L(i, j, k + 1)), g.L(i, j, k));
+                        }
+                        ct[q] -= dT / g.vol(k) * (dG - c[q] * ftr);
+                    }
+        }
+        for (int n = 0; n < PI_NTRACERS; ++n) fill_halo_tracer(g, m->tt[n]);
+    }
+    for (int n = 0; n < PI_NTRACERS; ++n)                          /* calc_tracer_tendency! */
+        for (size_t q = 0; q < g.G; ++q) m->Gcs[n][q] = m->tt[n][q] - m->tr[n][q];
+}
+
+/* tracer_diffusion!, Advection/tracer_diffusion.jl:1-30 */
+void tracer_diffusion(orc_model* m, double dT) {
+    const Grid& g = m->g;
+    Ops o{g};
+    double kx = m->bgc.kappa_h, ky = m->bgc.kappa_h, kz = m->bgc.kappa_v;
+    #pragma omp parallel for schedule(static)
+    for (int n = 0; n < PI_NTRACERS; ++n) {
+        const dvec& c = m->tr[n];
+        dvec& Gc = m->Gcs[n];
+        auto fx = [&](long i, long j, long k) { return kx * g.Axk(k) * (o.dx0(c, i, j, k) / g.dx); };
+        auto fy = [&](long i, long j, long k) { return ky * g.Ayk(k) * (o.dy0(c, i, j, k) / g.dy); };
+        auto fz = [&](long i, long j, long k) { return kz * g.Az() * (o.dz0(c, i, j, k) / g.dzF1(k)); };
+        for (long k = g.Hz + 1; k <= g.Hz + g.Nz; ++k)
+            for (long j = g.Hy + 1; j <= g.Hy + g.Ny; ++j)
+                for (long i = g.Hx + 1; i <= g.Hx + g.Nx; ++i) {
+                    double ax = jl_mulb(jl_mulb(fx(i + 1, j, k) - fx(i, j, k), g.L(i + 1, j, k)), g.L(i, j, k));
+                    double ay = jl_mulb(jl_mulb(fy(i, j + 1, k) - fy(i, j, k), g.L(i, j + 1, k)), g.L(i, j, k));
+                    double az = jl_mulb(jl_mulb(fz(i, j, k) - fz(i, j, k + 1), g.L(i, j, k + 1)), g.L(i, j, k));
+                    double lap = 1.0 / g.vol(k) * (ax + ay + az);
+                    size_t q = g.id(i, j, k);
+                    Gc[q] = Gc[q] + lap * dT;
+                }
+    }
+}
+
+/* tracer_sinking!, Advection/tracer_sinking.jl:1-42 */
+void tracer_sinking(orc_model* m, double dT) {
+    const Grid& g = m->g;
+    const int names[3] = { PI_PFe_inorg, PI_Dust, PI_PFe_bio };
+    for (int q3 = 0; q3 < 3; ++q3) {
+        int n = names[q3];
+        double wsink = q3 < 2 ? m->bgc.w_sink_inorg : m->bgc.w_sink_org;
+        for (size_t q = 0; q < g.G; ++q) m->flux_sink[q] = wsink * m->tr[n][q];
+        for (int j = 1; j <= g.Gy; ++j)                  /* fill_halo_flux_sink!, halo_regions.jl:58-62 */
+            for (int i = 1; i <= g.Gx; ++i) {
+                for (int k = 1; k <= g.Hz; ++k) m->flux_sink[g.id(i, j, k)] = 0.0;
+                for (int k = g.Nz + g.Hz; k <= g.Nz + 2 * g.Hz; ++k) m->flux_sink[g.id(i, j, k)] = 0.0;
+            }
+        dvec& Gc = m->Gcs[n];
+        for (long k = 1; k <= g.Nz; ++k)
+            for (long j = 1; j <= g.Ny; ++j)
+                for (long i = 1; i <= g.Nx; ++i) {
+                    long ii = i + g.Hx, jj = j + g.Hy, kk = k + g.Hz;
+                    size_t q = g.id(ii, jj, kk);
+                    Gc[q] = Gc[q] + (m->flux_sink[g.id(ii, jj, kk - 1)] - m->flux_sink[q]) / g.dzC1(k) * dT;
+                }
+    }
+}
+
+/* tracer_forcing!, tracer_forcings.jl:2-50 (interior; the halo part of Gcs is never read) */
+void tracer_forcing(orc_model* m, double dT) {
+    const Grid& g = m->g;
+    const pi_bgc_params& b = m->bgc;
+    #pragma omp parallel for schedule(static)
+    for (long k = g.Hz + 1; k <= g.Hz + g.Nz; ++k)
+        for (long j = g.Hy + 1; j <= g.Hy + g.Ny; ++j)
+            for (long i = g.Hx + 1; i <= g.Hx + g.Nx; ++i) {
+                size_t q = g.id(i, j, k);
+                double T[PI_NTRACERS];
+                for (int n = 0; n < PI_NTRACERS; ++n) T[n] = jl_max(0.0, m->tr[n][q]);
+                std::vector<dvec>& F = m->Gcs;
+                F[PI_DIC][q] = F[PI_DIC][q] + T[PI_DOC] * b.kDOC * dT;
+                F[PI_DOC][q] = F[PI_DOC][q] - T[PI_DOC] * b.kDOC * dT + T[PI_POC] * b.kPOC * dT;
+                F[PI_POC][q] = F[PI_POC][q] - T[PI_POC] * b.kPOC * dT;
+                F[PI_NH4][q] = F[PI_NH4][q] + T[PI_DON] * b.kDON * dT - T[PI_NH4] * b.Nit * dT;
+                F[PI_NO3][q] = F[PI_NO3][q] + T[PI_NH4] * b.Nit * dT;
+                F[PI_DON][q] = F[PI_DON][q] - T[PI_DON] * b.kDON * dT + T[PI_PON] * b.kPON * dT;
+                F[PI_PON][q] = F[PI_PON][q] - T[PI_PON] * b.kPON * dT;
+                F[PI_PO4][q] = F[PI_PO4][q] + T[PI_DOP] * b.kDOP * dT;
+                F[PI_DOP][q] = F[PI_DOP][q] - T[PI_DOP] * b.kDOP * dT + T[PI_POP] * b.kPOP * dT;
+                F[PI_POP][q] = F[PI_POP][q] - T[PI_POP] * b.kPOP * dT;
+                F[PI_DFe][q] = F[PI_DFe][q] + T[PI_PFe_bio] * b.kPOC * dT
+                             - (b.lambda_POC * T[PI_POC] + b.lambda_min + b.lambda_dust * T[PI_Dust]) * T[PI_DFe] * b.DFeFrac * dT
+                             + T[PI_PFe_inorg] * b.kdiss * dT
+                             - jl_max((T[PI_DFe] - b.ligand), 0.0) * T[PI_DFe] * b.DFeFrac * b.lambda_Fe * dT;
+                F[PI_PFe_bio][q] = F[PI_PFe_bio][q] + T[PI_POC] * T[PI_DFe] * b.DFeFrac * b.lambda_POC * dT
+                                 - b.kPOC * T[PI_PFe_bio] * dT;
+                F[PI_PFe_inorg][q] = F[PI_PFe_inorg][q] - T[PI_PFe_inorg] * b.kdiss * dT
+                                   + (b.lambda_min + b.lambda_dust * T[PI_Dust]) * T[PI_DFe] * b.DFeFrac * dT
+                                   + jl_max((T[PI_DFe] - b.ligand), 0.0) * T[PI_DFe] * b.DFeFrac * b.lambda_Fe * dT;
+            }
+}
+
+/* getbc, HaloRegions/boundary_conditions.jl:44-52 (a, b are 1-based face indices) */
+inline double getbc(const FluxBC& bc, int n1, int n2, long a, long b, int64_t it) {
+    if (bc.kind == PI_BC_CONST) return bc.v[0];
+    if (bc.kind == PI_BC_ARRAY2D) return bc.v[(size_t)(a - 1) + (size_t)n1 * (size_t)(b - 1)];
+    return bc.v[(size_t)(a - 1) + (size_t)n1 * ((size_t)(b - 1) + (size_t)n2 * (size_t)(it - 1))];
+}
+
+/* apply_bcs!, HaloRegions/apply_bcs.jl:4-98 */
+void apply_bcs(orc_model* m, double dT) {
+    const Grid& g = m->g;
+    int64_t it = m->iteration;
+    for (int n = 0; n < PI_NTRACERS; ++n) {
+        dvec& Gc = m->Gcs[n];
+        const FluxBC* b = m->bc[n];
+        if (b[PI_WEST].kind) for (long k = 1; k <= g.Nz; ++k) for (long j = 1; j <= g.Ny; ++j) {
+            long jj = j + g.Hy, kk = k + g.Hz;
+            Gc[g.id(1 + g.Hx, jj, kk)] += getbc(b[PI_WEST], g.Ny, g.Nz, j, k, it) * dT * g.Axk(kk) / g.vol(kk);
+        }
+        if (b[PI_EAST].kind) for (long k = 1; k <= g.Nz; ++k) for (long j = 1; j <= g.Ny; ++j) {
+            long jj = j + g.Hy, kk = k + g.Hz;
+            Gc[g.id(g.Nx + g.Hx, jj, kk)] -= getbc(b[PI_EAST], g.Ny, g.Nz, j, k, it) * dT * g.Axk(kk) / g.vol(kk);
+        }
+        if (b[PI_SOUTH].kind) for (long k = 1; k <= g.Nz; ++k) for (long i = 1; i <= g.Nx; ++i) {
+            long ii = i + g.Hx, kk = k + g.Hz;
+            Gc[g.id(ii, 1 + g.Hy, kk)] += getbc(b[PI_SOUTH], g.Nx, g.Nz, i, k, it) * dT * g.Ayk(kk) / g.vol(kk);
+        }
+        if (b[PI_NORTH].kind) for (long k = 1; k <= g.Nz; ++k) for (long i = 1; i <= g.Nx; ++i) {
+            long ii = i + g.Hx, kk = k + g.Hz;
+            Gc[g.id(ii, g.Ny + g.Hy, kk)] -= getbc(b[PI_NORTH], g.Nx, g.Nz, i, k, it) * dT * g.Ayk(kk) / g.vol(kk);
+        }
+        if (b[PI_BOTTOM].kind) for (long j = 1; j <= g.Ny; ++j) for (long i = 1; i <= g.Nx; ++i) {
+            long ii = i + g.Hx, jj = j + g.Hy, kk = g.Nz + g.Hz;
+            Gc[g.id(ii, jj, kk)] += getbc(b[PI_BOTTOM], g.Nx, g.Ny, i, j, it) * dT * g.Az() / g.vol(kk);
+        }
+        if (b[PI_TOP].kind) for (long j = 1; j <= g.Ny; ++j) for (long i = 1; i <= g.Nx; ++i) {
+            long ii = i + g.Hx, jj = j + g.Hy, kk = 1 + g.Hz;
+            Gc[g.id(ii, jj, kk)] -= getbc(b[PI_TOP], g.Nx, g.Ny, i, j, it) * dT * g.Az() / g.vol(kk);
+        }
+    }
+}
+
+/* apply_tendency!, tracer_update.jl:6-13 */
+void apply_tendency(orc_model* m) {
+    const Grid& g = m->g;
+    #pragma omp parallel for schedule(static)
+    for (int n = 0; n < PI_NTRACERS; ++n)
+        for (long k = g.Hz + 1; k <= g.Hz + g.Nz; ++k)
+            for (long j = g.Hy + 1; j <= g.Hy + g.Ny; ++j)
+                for (long i = g.Hx + 1; i <= g.Hx + g.Nx; ++i) {
+                    size_t q = g.id(i, j, k);
+                    m->tr[n][q] += m->Gcs[n][q] + m->plk[n][q] / g.vol(k);
+                }
+}
+
+/* tracer_update!, tracer_update.jl:22-43 */
+void tracer_update(orc_model* m, double dT) {
+    tracer_advection(m, dT);
+    tracer_diffusion(m, dT);
+    tracer_sinking(m, dT);
+    tracer_forcing(m, dT);     /* zero_fields!(tracer_temp) + the forcing broadcasts */
+    apply_bcs(m, dT);
+    apply_tendency(m);
+    for (int n = 0; n < PI_NTRACERS; ++n) fill_halo_tracer(m->g, m->tr[n]);
+}
+
+void zero(dvec& v) { std::fill(v.begin(), v.end(), 0.0); }
+
+}  // namespace
+
+/* ============================================================================================ */
+/* C entry points (orc_* mirror the pi_* entry points of include/pib200.h)                       */
+/* ============================================================================================ */
+
+static std::string g_create_err;
+
+extern "C" {
+
+int orc_create(const pi_grid* grid, const pi_bgc_params* bgc, const pi_quota_params* species,
+               int32_t nspecies, int64_t capacity, uint64_t seed, orc_model** out) {
+    if (!grid || !bgc || !species || !out || nspecies < 1 || capacity < 1 || !grid->dzF || !grid->dzC) {
+        g_create_err = "orc_create: bad argument"; return PI_ERR_ARG;
+    }
+    if (grid->topo[2] != PI_BOUNDED) { g_create_err = "z topology must be Bounded"; return PI_ERR_ARG; }
+    orc_model* m = new orc_model();
+    Grid& g = m->g;
+    g.Nx = grid->Nx; g.Ny = grid->Ny; g.Nz = grid->Nz; g.Hx = grid->Hx; g.Hy = grid->Hy; g.Hz = grid->Hz;
+    g.Gx = g.Nx + 2 * g.Hx; g.Gy = g.Ny + 2 * g.Hy; g.Gz = g.Nz + 2 * g.Hz;
+    g.tx = grid->topo[0]; g.ty = grid->topo[1]; g.tz = grid->topo[2];
+    g.dx = grid->dx; g.dy = grid->dy;
+    g.dzF.assign(grid->dzF, grid->dzF + g.Gz);
+    g.dzC.assign(grid->dzC, grid->dzC + g.Gz);
+    g.G = (size_t)g.Gx * g.Gy * g.Gz;
+    g.lm.assign(g.G, 1);
+    if (grid->landmask) g.lm.assign(grid->landmask, grid->landmask + g.G);
+    m->bgc = *bgc; m->nsp = nspecies; m->C = capacity; m->seed = seed;
+    m->sp.resize(nspecies);
+    size_t C = (size_t)capacity;
+    for (int s = 0; s < nspecies; ++s) {
+        Species& S = m->sp[s];
+        S.p = species[s];
+        for (dvec* v : { &S.x, &S.y, &S.z, &S.Sz, &S.Bm, &S.Cq, &S.Nq, &S.Pq, &S.Chl, &S.gen, &S.age,
+                         &S.PS, &S.VDOC, &S.VNH4, &S.VNO3, &S.VPO4, &S.rChl, &S.resp, &S.BS, &S.exu,
+                         &S.graz, &S.mort, &S.dvid }) v->assign(C, 0.0);
+        S.xi.assign(C, 0); S.yi.assign(C, 0); S.zi.assign(C, 0); S.idx.assign(C, 0);
+        S.ac.assign(C, 0);
+        for (dvec* v : { &S.d_num, &S.d_graz, &S.d_mort, &S.d_dvid }) v->assign(g.G, 0.0);
+    }
+    m->tr.assign(PI_NTRACERS, dvec(g.G, 0.0));
+    m->Gcs.assign(PI_NTRACERS, dvec(g.G, 0.0));
+    m->tt.assign(PI_NTRACERS, dvec(g.G, 0.0));
+    m->plk.assign(PI_NTRACERS, dvec(g.G, 0.0));
+    for (dvec* v : { &m->u0, &m->v0, &m->w0, &m->u1, &m->v1, &m->w1, &m->uh, &m->vh, &m->wh,
+                     &m->temp, &m->flux_sink, &m->par, &m->par0, &m->Chl, &m->pop, &m->d_PAR }) v->assign(g.G, 0.0);
+    m->PARF.assign((size_t)g.Nx * g.Ny, 0.0);
+    for (dvec* v : { &m->rx, &m->ry, &m->rz, &m->vx, &m->vy, &m->vz, &m->vu1, &m->vv1, &m->vw1,
+                     &m->vu2, &m->vv2, &m->vw2, &m->tNH4, &m->tNO3, &m->tPO4, &m->tDOC, &m->tDFe,
+                     &m->tpar, &m->tT, &m->tpop, &m->tdpar, &m->tidc }) v->assign(C, 0.0);
+    m->tidc_int.assign(C, 0);
+    m->iteration = 0; m->t = 0.0; m->err_flags = 0;
+    *out = m;
+    return PI_OK;
+}
+
+int orc_destroy(orc_model* m) { delete m; return PI_OK; }
+
+int orc_set_individuals(orc_model* m, int32_t sp, const pi_individuals* in) {
+    if (!m || sp < 0 || sp >= m->nsp || !in) return PI_ERR_ARG;
+    Species& S = m->sp[sp];
+    size_t C = (size_t)m->C;
+    auto cp = [&](dvec& d, const double* s) { d.assign(s, s + C); };
+    cp(S.x, in->x); cp(S.y, in->y); cp(S.z, in->z);
+    S.xi.assign(in->xi, in->xi + C); S.yi.assign(in->yi, in->yi + C); S.zi.assign(in->zi, in->zi + C);
+    cp(S.Sz, in->Sz); cp(S.Bm, in->Bm); cp(S.Cq, in->Cq); cp(S.Nq, in->Nq); cp(S.Pq, in->Pq);
+    cp(S.Chl, in->Chl); cp(S.gen, in->gen); cp(S.age, in->age);
+    S.ac.assign(in->ac, in->ac + C);
+    cp(S.graz, in->graz); cp(S.mort, in->mort); cp(S.dvid, in->dvid);
+    return PI_OK;
+}
+
+int orc_get_individuals(orc_model* m, int32_t sp, pi_individuals* out) {
+    if (!m || sp < 0 || sp >= m->nsp || !out) return PI_ERR_ARG;
+    Species& S = m->sp[sp];
+    auto cp = [&](double* d, const dvec& s) { if (d) std::copy(s.begin(), s.end(), d); };
+    auto ci = [&](int64_t* d, const std::vector<int64_t>& s) { if (d) std::copy(s.begin(), s.end(), d); };
+    cp(out->x, S.x); cp(out->y, S.y); cp(out->z, S.z);
+    ci(out->xi, S.xi); ci(out->yi, S.yi); ci(out->zi, S.zi);
+    cp(out->Sz, S.Sz); cp(out->Bm, S.Bm); cp(out->Cq, S.Cq); cp(out->Nq, S.Nq); cp(out->Pq, S.Pq);
+    cp(out->Chl, S.Chl); cp(out->gen, S.gen); cp(out->age, S.age);
+    if (out->ac) std::copy(S.ac.begin(), S.ac.end(), out->ac);
+    cp(out->graz, S.graz); cp(out->mort, S.mort); cp(out->dvid, S.dvid);
+    return PI_OK;
+}
+
+/* Physiological rates of the last step (PS, VDOC, VNH4, VNO3, VPO4, ρChl, resp, BS, exu). */
+int orc_get_rates(orc_model* m, int32_t sp, double* out9) {
+    if (!m || sp < 0 || sp >= m->nsp || !out9) return PI_ERR_ARG;
+    Species& S = m->sp[sp];
+    const dvec* r[9] = { &S.PS, &S.VDOC, &S.VNH4, &S.VNO3, &S.VPO4, &S.rChl, &S.resp, &S.BS, &S.exu };
+    for (int q = 0; q < 9; ++q) std::copy(r[q]->begin(), r[q]->end(), out9 + (size_t)q * m->C);
+    return PI_OK;
+}
+
+int orc_set_tracer(orc_model* m, int32_t idx, const double* data) {
+    if (!m || idx < 0 || idx >= PI_NTRACERS || !data) return PI_ERR_ARG;
+    m->tr[idx].assign(data, data + m->g.G);
+    return PI_OK;
+}
+int orc_get_tracer(orc_model* m, int32_t idx, double* out) {
+    if (!m || idx < 0 || idx >= PI_NTRACERS || !out) return PI_ERR_ARG;
+    std::copy(m->tr[idx].begin(), m->tr[idx].end(), out);
+    return PI_OK;
+}
+
+/* Scratch fields for tests: 0 par, 1 Chl, 2 pop, 3..16 plk[0..13], 17..30 Gcs[0..13],
+ * 31 u1, 32 v1, 33 w1, 34 u0, 35 temp. */
+int orc_get_field(orc_model* m, int32_t which, double* out) {
+    if (!m || !out) return PI_ERR_ARG;
+    const dvec* f = nullptr;
+    if (which == 0) f = &m->par; else if (which == 1) f = &m->Chl; else if (which == 2) f = &m->pop;
+    else if (which >= 3 && which < 17) f = &m->plk[which - 3];
+    else if (which >= 17 && which < 31) f = &m->Gcs[which - 17];
+    else if (which == 31) f = &m->u1; else if (which == 32) f = &m->v1; else if (which == 33) f = &m->w1;
+    else if (which == 34) f = &m->u0; else if (which == 35) f = &m->temp;
+    if (!f) return PI_ERR_ARG;
+    std::copy(f->begin(), f->end(), out);
+    return PI_OK;
+}
+
+/* vel_copy!, Simulation/utils.jl:5-34 */
+int orc_set_velocity(orc_model* m, const double* u, const double* v, const double* w) {
+    if (!m || !u || !v || !w) return PI_ERR_ARG;
+    const Grid& g = m->g;
+    int ex = g.tx == PI_BOUNDED, ey = g.ty == PI_BOUNDED, ez = g.tz == PI_BOUNDED;
+    auto copy_in = [&](dvec& f, const double* s, int nx, int ny, int nz) {
+        for (int k = 1; k <= nz; ++k) for (int j = 1; j <= ny; ++j) for (int i = 1; i <= nx; ++i)
+            f[g.id(i + g.Hx, j + g.Hy, k + g.Hz)] = s[(size_t)(i - 1) + (size_t)nx * ((size_t)(j - 1) + (size_t)ny * (size_t)(k - 1))];
+    };
+    copy_in(m->u1, u, g.Nx + ex, g.Ny, g.Nz);
+    copy_in(m->v1, v, g.Nx, g.Ny + ey, g.Nz);
+    copy_in(m->w1, w, g.Nx, g.Ny, g.Nz + ez);
+    fill_halo_u(g, m->u1); fill_halo_v(g, m->v1); fill_halo_w(g, m->w1);
+    return PI_OK;
+}
+
+int orc_set_PARF(orc_model* m, const double* parf) {
+    if (!m || !parf) return PI_ERR_ARG;
+    m->PARF.assign(parf, parf + (size_t)m->g.Nx * m->g.Ny);
+    return PI_OK;
+}
+
+int orc_set_temp(orc_model* m, const double* temp) {   /* copy_interior!, Simulation/utils.jl:13-15 */
+    if (!m || !temp) return PI_ERR_ARG;
+    const Grid& g = m->g;
+    for (int k = 1; k <= g.Nz; ++k) for (int j = 1; j <= g.Ny; ++j) for (int i = 1; i <= g.Nx; ++i)
+        m->temp[g.id(i + g.Hx, j + g.Hy, k + g.Hz)] = temp[(size_t)(i - 1) + (size_t)g.Nx * ((size_t)(j - 1) + (size_t)g.Ny * (size_t)(k - 1))];
+    return PI_OK;
+}
+
+int orc_set_flux_bc(orc_model* m, int32_t tracer, int32_t face, int32_t kind, const double* values, int64_t nt) {
+    if (!m || tracer < 0 || tracer >= PI_NTRACERS || face < 0 || face > 5 || kind < 0 || kind > 3) return PI_ERR_ARG;
+    const Grid& g = m->g;
+    FluxBC& b = m->bc[tracer][face];
+    b.kind = kind; b.nt = nt; b.v.clear();
+    size_t n1 = face <= PI_EAST ? g.Ny : g.Nx, n2 = face <= PI_NORTH ? g.Nz : g.Ny;
+    size_t n = kind == PI_BC_CONST ? 1 : kind == PI_BC_ARRAY2D ? n1 * n2 : kind == PI_BC_ARRAY3D ? n1 * n2 * (size_t)nt : 0;
+    if (n && !values) return PI_ERR_ARG;
+    if (n) b.v.assign(values, values + n);
+    return PI_OK;
+}
+
+/* TimeStep!, Model/time_step.jl:12-180 (QuotaMode, no abiotic particles) */
+int orc_time_step(orc_model* m, double dT) {
+    if (!m) return PI_ERR_ARG;
+    const Grid& g = m->g;
+    m->iteration = m->iteration + 1;
+    m->t = (double)m->iteration * dT;
+    for (size_t q = 0; q < g.G; ++q) {                                           /* :17-19 */
+        m->uh[q] = (m->u0[q] + m->u1[q]) * 0.5;
+        m->vh[q] = (m->v0[q] + m->v1[q]) * 0.5;
+        m->wh[q] = (m->w0[q] + m->w1[q]) * 0.5;
+    }
+    for (int n = 0; n < PI_NTRACERS; ++n) zero(m->plk[n]);                        /* :21-22 */
+    zero(m->Chl);
+    bool ok = true;
+    if (m->bgc.shared_graz == 1.0) {
+        zero(m->pop);
+        for (int s = 0; s < m->nsp; ++s) {
+            particle_advection(m, m->sp[s], dT);
+            particle_diffusion(m, m->sp[s], s, dT);
+            find_inds(m, m->sp[s]);
+            acc_chl(m, m->sp[s]);
+            acc_counts(m, m->sp[s]);
+        }
+        for (int ki = 1; ki <= g.Nz; ++ki) calc_par(m, ki);
+        for (int s = 0; s < m->nsp && ok; ++s) {
+            find_NPT(m, m->sp[s]);
+            ok = plankton_update(m, m->sp[s], s, dT, m->t);
+        }
+    } else {
+        for (int s = 0; s < m->nsp; ++s) {
+            particle_advection(m, m->sp[s], dT);
+            particle_diffusion(m, m->sp[s], s, dT);
+            find_inds(m, m->sp[s]);
+            acc_chl(m, m->sp[s]);
+        }
+        for (int ki = 1; ki <= g.Nz; ++ki) calc_par(m, ki);
+        for (int s = 0; s < m->nsp && ok; ++s) {
+            zero(m->pop);
+            acc_counts(m, m->sp[s]);
+            find_NPT(m, m->sp[s]);
+            ok = plankton_update(m, m->sp[s], s, dT, m->t);
+        }
+    }
+    if (!ok) return PI_ERR_CAPACITY;
+    tracer_update(m, dT);
+    for (size_t q = 0; q < g.G; ++q) m->d_PAR[q] += m->par[q];                  /* :167 */
+    m->u0 = m->u1; m->v0 = m->v1; m->w0 = m->w1;                                  /* :174-177 */
+    m->par0 = m->par;
+    if (m->err_flags & ERR_DOMAIN) { m->err = "an individual left the halo-padded grid"; return PI_ERR_DOMAIN; }
+    return PI_OK;
+}
+
+int orc_get_time(orc_model* m, int64_t* it, double* t) {
+    if (!m) return PI_ERR_ARG;
+    if (it) *it = m->iteration;
+    if (t) *t = m->t;
+    return PI_OK;
+}
+int orc_set_time(orc_model* m, int64_t it, double t) { if (!m) return PI_ERR_ARG; m->iteration = it; m->t = t; return PI_OK; }
+
+int orc_count_active(orc_model* m, int32_t sp, int64_t* n) {
+    if (!m || sp < 0 || sp >= m->nsp || !n) return PI_ERR_ARG;
+    int64_t c = 0;
+    for (uint8_t a : m->sp[sp].ac) c += a;
+    *n = c;
+    return PI_OK;
+}
+
+int orc_get_diag(orc_model* m, int32_t kind, int32_t sp, double* out) {
+    if (!m || !out) return PI_ERR_ARG;
+    const dvec* f = nullptr;
+    if (kind == PI_DIAG_PAR) f = &m->d_PAR;
+    else {
+        if (sp < 0 || sp >= m->nsp) return PI_ERR_ARG;
+        Species& S = m->sp[sp];
+        f = kind == PI_DIAG_NUM ? &S.d_num : kind == PI_DIAG_GRAZ ? &S.d_graz
+          : kind == PI_DIAG_MORT ? &S.d_mort : kind == PI_DIAG_DVID ? &S.d_dvid : nullptr;
+    }
+    if (!f) return PI_ERR_ARG;
+    std::copy(f->begin(), f->end(), out);
+    return PI_OK;
+}
+
+int orc_last_error(orc_model* m, char* buf, size_t len) {
+    const std::string& e = m ? m->err : g_create_err;
+    if (buf && len) { size_t n = std::min(len - 1, e.size()); memcpy(buf, e.c_str(), n); buf[n] = 0; }
+    return PI_OK;
+}
+
+int orc_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+/* Numeric primitives exposed for tests of the shared header. */
+double orc_exp(double x) { return pi_exp(x); }
+double orc_pow_int(double x, int n) { return pi_pow_int(x, n); }
+void orc_draw3(uint64_t seed, uint32_t it, uint32_t sp, uint32_t purpose, uint32_t slot, double* r) {
+    pi_draw3(seed, it, sp, purpose, slot, &r[0], &r[1], &r[2]);
+}
+
+}  // extern "C"

@@ -1,0 +1,111 @@
+"""ctypes mirror of include/pib200.h (structs, constants and prototypes)."""
+import ctypes as ct
+
+PI_OK, PI_ERR_ARG, PI_ERR_SHAPE, PI_ERR_PARAM, PI_ERR_CAPACITY = 0, 1, 2, 3, 4
+PI_ERR_CUDA, PI_ERR_TIMEOUT, PI_ERR_NAN, PI_ERR_DOMAIN, PI_ERR_NOMEM, PI_ERR_STATE = 5, 6, 7, 8, 9, 10
+PI_FP64, PI_FP32 = 0, 1
+PI_PERIODIC, PI_BOUNDED = 0, 1
+
+# Tracer order of the reference, src/Biogeochemistry/Biogeochemistry.jl:20
+tracer_names = ("DIC", "NH4", "NO3", "PO4", "DFe", "DOC", "DON", "DOP",
+                "PFe_inorg", "POC", "PON", "POP", "PFe_bio", "Dust")
+NTRACERS = len(tracer_names)
+
+FACES = {"west": 0, "east": 1, "south": 2, "north": 3, "bottom": 4, "top": 5}
+PI_BC_NONE, PI_BC_CONST, PI_BC_ARRAY2D, PI_BC_ARRAY3D = 0, 1, 2, 3
+PI_DIAG_PAR, PI_DIAG_NUM, PI_DIAG_GRAZ, PI_DIAG_MORT, PI_DIAG_DVID = 0, 1, 2, 3, 4
+
+_dp = ct.POINTER(ct.c_double)
+_i64p = ct.POINTER(ct.c_int64)
+_u8p = ct.POINTER(ct.c_uint8)
+
+
+class pi_grid(ct.Structure):
+    _fields_ = [("Nx", ct.c_int32), ("Ny", ct.c_int32), ("Nz", ct.c_int32),
+                ("Hx", ct.c_int32), ("Hy", ct.c_int32), ("Hz", ct.c_int32),
+                ("topo", ct.c_int32 * 3),
+                ("dx", ct.c_double), ("dy", ct.c_double),
+                ("dzF", _dp), ("dzC", _dp), ("landmask", _u8p)]
+
+
+# bgc_params_default keys (src/Parameters/param_default.jl:44-71) in struct order
+BGC_FIELDS = [("kw", "kw"), ("kc", "kc"), ("kDOC", "kDOC"), ("Nit", "Nit"), ("kDON", "kDON"),
+              ("kDOP", "kDOP"), ("kPOC", "kPOC"), ("kPON", "kPON"), ("kPOP", "kPOP"),
+              ("kappa_h", "κh"), ("kappa_v", "κv"), ("kappa_hP", "κhP"), ("kappa_vP", "κvP"),
+              ("shared_graz", "shared_graz"), ("w_sink_org", "w_sink_org"),
+              ("w_sink_inorg", "w_sink_inorg"), ("lambda_POC", "lambda_POC"),
+              ("lambda_min", "lambda_min"), ("kdiss", "kdiss"), ("lambda_dust", "lambda_dust"),
+              ("lambda_Fe", "lambda_Fe"), ("ligand", "ligand"), ("DFeFrac", "DFeFrac")]
+
+
+class pi_bgc_params(ct.Structure):
+    _fields_ = [(c, ct.c_double) for c, _ in BGC_FIELDS]
+
+
+# QuotaMode param_names (src/Individuals/Plankton/QuotaMode/plankton_generation.jl:16-20)
+QUOTA_FIELDS = [("Nsuper", "Nsuper"), ("Cquota", "Cquota"), ("mean", "mean"), ("var", "var"),
+                ("Chl2Cint", "Chl2Cint"), ("alpha", "α"), ("Phi", "Φ"), ("Topt", "Topt"),
+                ("Tmax", "Tmax"), ("Ea", "Ea"), ("PCmax", "PCmax"), ("VDOCmax", "VDOCmax"),
+                ("VNO3max", "VNO3max"), ("VNH4max", "VNH4max"), ("VPO4max", "VPO4max"),
+                ("KsatDOC", "KsatDOC"), ("KsatNH4", "KsatNH4"), ("KsatNO3", "KsatNO3"),
+                ("KsatPO4", "KsatPO4"), ("Cqmax", "Cqmax"), ("Nqmax", "Nqmax"),
+                ("Pqmax", "Pqmax"), ("Chl2N", "Chl2N"), ("R_NC", "R_NC"), ("R_PC", "R_PC"),
+                ("k_mtb", "k_mtb"), ("respir", "respir"), ("grz_P", "grz_P"),
+                ("dvid_type", "dvid_type"), ("dvid_P", "dvid_P"), ("dvid_reg", "dvid_reg"),
+                ("dvid_reg2", "dvid_reg2"), ("mort_P", "mort_P"), ("mort_reg", "mort_reg"),
+                ("grazFracC", "grazFracC"), ("grazFracN", "grazFracN"),
+                ("grazFracP", "grazFracP"), ("mortFracC", "mortFracC"),
+                ("mortFracN", "mortFracN"), ("mortFracP", "mortFracP")]
+
+
+class pi_quota_params(ct.Structure):
+    _fields_ = [(c, ct.c_double) for c, _ in QUOTA_FIELDS]
+
+
+IND_DOUBLE = ("x", "y", "z", "Sz", "Bm", "Cq", "Nq", "Pq", "Chl", "gen", "age", "graz", "mort", "dvid")
+IND_INT = ("xi", "yi", "zi")
+
+
+class pi_individuals(ct.Structure):
+    _fields_ = [("x", _dp), ("y", _dp), ("z", _dp),
+                ("xi", _i64p), ("yi", _i64p), ("zi", _i64p),
+                ("Sz", _dp), ("Bm", _dp), ("Cq", _dp), ("Nq", _dp), ("Pq", _dp),
+                ("Chl", _dp), ("gen", _dp), ("age", _dp),
+                ("ac", _u8p),
+                ("graz", _dp), ("mort", _dp), ("dvid", _dp)]
+
+
+def declare(lib, prefix):
+    """Attach argtypes/restype for the pi_* (or mirrored) entry points found in `lib`."""
+    P = ct.c_void_p
+    protos = {
+        "create": (ct.c_int32, [ct.POINTER(pi_grid), ct.POINTER(pi_bgc_params),
+                                ct.POINTER(pi_quota_params), ct.c_int32, ct.c_int64]),
+        "destroy": (ct.c_int32, [P]),
+        "set_individuals": (ct.c_int32, [P, ct.c_int32, ct.POINTER(pi_individuals)]),
+        "get_individuals": (ct.c_int32, [P, ct.c_int32, ct.POINTER(pi_individuals)]),
+        "set_tracer": (ct.c_int32, [P, ct.c_int32, _dp]),
+        "get_tracer": (ct.c_int32, [P, ct.c_int32, _dp]),
+        "set_velocity": (ct.c_int32, [P, _dp, _dp, _dp]),
+        "set_PARF": (ct.c_int32, [P, _dp]),
+        "set_temp": (ct.c_int32, [P, _dp]),
+        "set_flux_bc": (ct.c_int32, [P, ct.c_int32, ct.c_int32, ct.c_int32, _dp, ct.c_int64]),
+        "time_step": (ct.c_int32, [P, ct.c_double]),
+        "get_time": (ct.c_int32, [P, _i64p, _dp]),
+        "set_time": (ct.c_int32, [P, ct.c_int64, ct.c_double]),
+        "count_active": (ct.c_int32, [P, ct.c_int32, _i64p]),
+        "get_diag": (ct.c_int32, [P, ct.c_int32, ct.c_int32, _dp]),
+        "last_error": (ct.c_int32, [P, ct.c_char_p, ct.c_size_t]),
+    }
+    for name, (res, args) in protos.items():
+        fn = getattr(lib, prefix + name, None)
+        if fn is None:
+            continue
+        if name == "create":
+            if prefix == "pi_":
+                args = args + [ct.c_int32, ct.c_uint64, ct.POINTER(P)]
+            else:
+                args = args + [ct.c_uint64, ct.POINTER(P)]
+        fn.restype = res
+        fn.argtypes = args
+    return lib

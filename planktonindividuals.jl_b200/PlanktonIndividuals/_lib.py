@@ -1,0 +1,48 @@
+"""Loads libpib200.so, the CUDA (sm_100a) implementation behind this package.
+
+There is no CPU fallback: if the library is missing or no CUDA device can be used, model
+construction raises. Build it with `python planktonindividuals.jl_b200/build.py`."""
+import ctypes as ct
+import os
+
+from . import _abi
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libpib200.so")
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"libpib200.so not found at {LIB_PATH}; build it with "
+                          f"`python planktonindividuals.jl_b200/build.py` (the package has no CPU fallback)")
+    lib = ct.CDLL(LIB_PATH)
+    _abi.declare(lib, "pi_")
+    P = ct.c_void_p
+    dp = ct.POINTER(ct.c_double)
+    lib.pi_sim_create.restype = ct.c_int32
+    lib.pi_sim_create.argtypes = [P, ct.c_double, ct.c_int64, dp, dp, dp, ct.c_int64, ct.c_double,
+                                  dp, ct.c_int64, ct.c_double, dp, ct.c_int64, ct.c_double,
+                                  ct.POINTER(P)]
+    lib.pi_sim_update.restype = ct.c_int32
+    lib.pi_sim_update.argtypes = [P, ct.c_int32, ct.c_int32]
+    lib.pi_sim_destroy.restype = ct.c_int32
+    lib.pi_sim_destroy.argtypes = [P]
+    lib.pi_synchronize.restype = ct.c_int32
+    lib.pi_synchronize.argtypes = [P]
+    lib.pi_reset_diags.restype = ct.c_int32
+    lib.pi_reset_diags.argtypes = [P]
+    lib.pi_status_string.restype = ct.c_char_p
+    lib.pi_status_string.argtypes = [ct.c_int32]
+    _lib = lib
+    return lib
+
+
+# Exported entry points of include/pib200.h (checked by the CPU test suite).
+EXPORTS = ("pi_create", "pi_destroy", "pi_set_individuals", "pi_get_individuals", "pi_set_tracer",
+           "pi_get_tracer", "pi_set_velocity", "pi_set_PARF", "pi_set_temp", "pi_set_flux_bc",
+           "pi_time_step", "pi_get_time", "pi_set_time", "pi_count_active", "pi_get_diag",
+           "pi_reset_diags", "pi_sim_create", "pi_sim_update", "pi_sim_destroy", "pi_synchronize",
+           "pi_last_error", "pi_status_string")

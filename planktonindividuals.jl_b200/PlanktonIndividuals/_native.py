@@ -1,0 +1,233 @@
+"""Thin object wrapper over a C library that exports the pib200.h entry points.
+
+`CModel` owns one model handle and converts numpy arrays (Julia column-major layout) to the
+pointer arguments of the C ABI. The product package instantiates it over libpib200 only.
+"""
+import ctypes as ct
+
+import numpy as np
+
+from . import _abi
+from ._abi import (IND_DOUBLE, IND_INT, NTRACERS, PI_OK, pi_bgc_params, pi_grid, pi_individuals,
+                   pi_quota_params, BGC_FIELDS, QUOTA_FIELDS)
+
+
+class PIError(RuntimeError):
+    """Error returned by the C ABI; `.code` is the pi_status value."""
+
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+
+
+class CapacityError(PIError, ValueError):
+    """Division overflow, the reference's ArgumentError at QuotaMode/plankton_update.jl:20-22."""
+
+
+def _dptr(a):
+    return a.ctypes.data_as(ct.POINTER(ct.c_double))
+
+
+def _f64(a, shape=None):
+    a = np.asarray(a, dtype=np.float64)
+    if shape is not None and a.shape != tuple(shape):
+        raise ValueError(f"expected shape {tuple(shape)}, got {a.shape}")
+    return np.asfortranarray(a)
+
+
+def make_grid_struct(grid):
+    g = pi_grid()
+    g.Nx, g.Ny, g.Nz = grid.Nx, grid.Ny, grid.Nz
+    g.Hx, g.Hy, g.Hz = grid.Hx, grid.Hy, grid.Hz
+    for a in range(3):
+        g.topo[a] = grid.topo[a]
+    g.dx, g.dy = float(grid.Δx), float(grid.Δy)
+    keep = [np.ascontiguousarray(grid.dzF, dtype=np.float64),
+            np.ascontiguousarray(grid.dzC, dtype=np.float64),
+            np.asfortranarray(grid.landmask, dtype=np.uint8)]
+    g.dzF = _dptr(keep[0])
+    g.dzC = _dptr(keep[1])
+    g.landmask = keep[2].ctypes.data_as(ct.POINTER(ct.c_uint8))
+    return g, keep
+
+
+def make_bgc_struct(params):
+    b = pi_bgc_params()
+    for cname, key in BGC_FIELDS:
+        setattr(b, cname, float(params[key]))
+    return b
+
+
+def make_species_structs(phyt_params, nsp):
+    arr = (pi_quota_params * nsp)()
+    for s in range(nsp):
+        for cname, key in QUOTA_FIELDS:
+            v = phyt_params[key]
+            v = v[s] if hasattr(v, "__len__") else v
+            setattr(arr[s], cname, float(v))
+    return arr
+
+
+class CModel:
+    """One model handle of a library exporting `<prefix>create` ... `<prefix>last_error`."""
+
+    def __init__(self, lib, prefix, grid, bgc_params, phyt_params, nsp, capacity, seed,
+                 precision=None):
+        self.lib = _abi.declare(lib, prefix)
+        self.prefix = prefix
+        self.grid = grid
+        self.nsp = int(nsp)
+        self.capacity = int(capacity)
+        g, self._keep = make_grid_struct(grid)
+        b = make_bgc_struct(bgc_params)
+        sp = make_species_structs(phyt_params, self.nsp)
+        h = ct.c_void_p()
+        fn = self._fn("create")
+        if precision is None:
+            rc = fn(ct.byref(g), ct.byref(b), sp, self.nsp, self.capacity, ct.c_uint64(seed), ct.byref(h))
+        else:
+            rc = fn(ct.byref(g), ct.byref(b), sp, self.nsp, self.capacity, int(precision),
+                    ct.c_uint64(seed), ct.byref(h))
+        if rc != PI_OK:
+            raise PIError(rc, f"{prefix}create failed ({rc}): {self._errmsg(None)}")
+        self.h = h
+
+    def _fn(self, name):
+        return getattr(self.lib, self.prefix + name)
+
+    def _errmsg(self, h):
+        buf = ct.create_string_buffer(512)
+        self._fn("last_error")(h, buf, 512)
+        return buf.value.decode(errors="replace")
+
+    def _check(self, rc, what):
+        if rc != PI_OK:
+            msg = self._errmsg(self.h)
+            if rc == _abi.PI_ERR_CAPACITY:
+                raise CapacityError(rc, msg)
+            raise PIError(rc, f"{what}: status {rc}: {msg}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._fn("destroy")(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def G(self):
+        g = self.grid
+        return (g.Nx + 2 * g.Hx) * (g.Ny + 2 * g.Hy) * (g.Nz + 2 * g.Hz)
+
+    @property
+    def gshape(self):
+        return self.grid.total_size
+
+    # ---- individuals ---------------------------------------------------------------------
+    def set_individuals(self, sp, data):
+        C = self.capacity
+        keep = {}
+        st = pi_individuals()
+        for k in IND_DOUBLE:
+            a = np.ascontiguousarray(data[k], dtype=np.float64)
+            if a.shape != (C,):
+                raise ValueError(f"individual attribute {k} must have length {C}")
+            keep[k] = a
+            setattr(st, k, _dptr(a))
+        for k in IND_INT:
+            a = np.ascontiguousarray(data[k], dtype=np.int64)
+            if a.shape != (C,):
+                raise ValueError(f"individual attribute {k} must have length {C}")
+            keep[k] = a
+            setattr(st, k, a.ctypes.data_as(ct.POINTER(ct.c_int64)))
+        ac = np.ascontiguousarray(data["ac"], dtype=np.uint8)
+        keep["ac"] = ac
+        st.ac = ac.ctypes.data_as(ct.POINTER(ct.c_uint8))
+        self._check(self._fn("set_individuals")(self.h, int(sp), ct.byref(st)), "set_individuals")
+
+    def get_individuals(self, sp):
+        C = self.capacity
+        out = {k: np.empty(C, dtype=np.float64) for k in IND_DOUBLE}
+        out.update({k: np.empty(C, dtype=np.int64) for k in IND_INT})
+        out["ac"] = np.empty(C, dtype=np.uint8)
+        st = pi_individuals()
+        for k in IND_DOUBLE:
+            setattr(st, k, _dptr(out[k]))
+        for k in IND_INT:
+            setattr(st, k, out[k].ctypes.data_as(ct.POINTER(ct.c_int64)))
+        st.ac = out["ac"].ctypes.data_as(ct.POINTER(ct.c_uint8))
+        self._check(self._fn("get_individuals")(self.h, int(sp), ct.byref(st)), "get_individuals")
+        out["ac"] = out["ac"].astype(bool)
+        return out
+
+    # ---- fields ----------------------------------------------------------------------------
+    def set_tracer(self, idx, data):
+        a = _f64(data, self.gshape)
+        self._check(self._fn("set_tracer")(self.h, int(idx), _dptr(a.ravel(order="F"))), "set_tracer")
+
+    def get_tracer(self, idx):
+        out = np.empty(self.G, dtype=np.float64)
+        self._check(self._fn("get_tracer")(self.h, int(idx), _dptr(out)), "get_tracer")
+        return out.reshape(self.gshape, order="F")
+
+    def set_velocity(self, u, v, w):
+        g = self.grid
+        b = [int(t == _abi.PI_BOUNDED) for t in g.topo]
+        u = _f64(u, (g.Nx + b[0], g.Ny, g.Nz))
+        v = _f64(v, (g.Nx, g.Ny + b[1], g.Nz))
+        w = _f64(w, (g.Nx, g.Ny, g.Nz + b[2]))
+        self._check(self._fn("set_velocity")(self.h, _dptr(u.ravel(order="F")), _dptr(v.ravel(order="F")),
+                                             _dptr(w.ravel(order="F"))), "set_velocity")
+
+    def set_PARF(self, parf):
+        a = _f64(parf, (self.grid.Nx, self.grid.Ny))
+        self._check(self._fn("set_PARF")(self.h, _dptr(a.ravel(order="F"))), "set_PARF")
+
+    def set_temp(self, temp):
+        a = _f64(temp, self.grid.size)
+        self._check(self._fn("set_temp")(self.h, _dptr(a.ravel(order="F"))), "set_temp")
+
+    def set_flux_bc(self, tracer, face, kind, values=None, nt=0):
+        if values is None:
+            p = ct.POINTER(ct.c_double)()
+        else:
+            values = np.asfortranarray(np.atleast_1d(np.asarray(values, dtype=np.float64)))
+            self._keep.append(values)
+            p = _dptr(values.ravel(order="F"))
+        self._check(self._fn("set_flux_bc")(self.h, int(tracer), int(face), int(kind), p, int(nt)),
+                    "set_flux_bc")
+
+    # ---- stepping ----------------------------------------------------------------------------
+    def time_step(self, dT):
+        self._check(self._fn("time_step")(self.h, float(dT)), "time_step")
+
+    def get_time(self):
+        it = ct.c_int64()
+        t = ct.c_double()
+        self._check(self._fn("get_time")(self.h, ct.byref(it), ct.byref(t)), "get_time")
+        return it.value, t.value
+
+    def set_time(self, iteration, t):
+        self._check(self._fn("set_time")(self.h, int(iteration), float(t)), "set_time")
+
+    def count_active(self, sp):
+        n = ct.c_int64()
+        self._check(self._fn("count_active")(self.h, int(sp), ct.byref(n)), "count_active")
+        return n.value
+
+    def get_diag(self, kind, sp=0):
+        out = np.empty(self.G, dtype=np.float64)
+        self._check(self._fn("get_diag")(self.h, int(kind), int(sp), _dptr(out)), "get_diag")
+        return out.reshape(self.gshape, order="F")
+
+    def set_state(self, individuals, tracers):
+        """Upload a full initial state: individuals = list (per species) of attribute dicts,
+        tracers = sequence of NTRACERS halo-padded arrays."""
+        for s, d in enumerate(individuals):
+            self.set_individuals(s, d)
+        for n in range(NTRACERS):
+            self.set_tracer(n, tracers[n])

@@ -1,0 +1,83 @@
+"""Initial conditions on the host: initialize_plankton! and generate_tracers
+(src/Individuals/Plankton/QuotaMode/plankton_generation.jl:35-72,
+src/Biogeochemistry/tracer_fields.jl:60-101) with a seeded generator instead of the reference's
+unseeded one. Arrays are float64 (the C ABI type)."""
+import numpy as np
+
+from ._abi import tracer_names
+from .grids import fill_halo_tracer
+
+
+def empty_individuals(C):
+    d = {k: np.zeros(C, dtype=np.float64) for k in
+         ("x", "y", "z", "Sz", "Bm", "Cq", "Nq", "Pq", "Chl", "gen", "age", "graz", "mort", "dvid")}
+    for k in ("xi", "yi", "zi"):
+        d[k] = np.zeros(C, dtype=np.int64)
+    d["ac"] = np.zeros(C, dtype=bool)
+    return d
+
+
+def species_param(p, key, s):
+    v = p[key]
+    return float(v[s] if hasattr(v, "__len__") else v)
+
+
+def initialize_plankton(grid, p, s, N, C, rng):
+    """initialize_plankton! for species s (0-based) with N active individuals out of C slots."""
+    if N > C:
+        raise ValueError("PlanktonModel: number of individuals exceeds max_individuals")
+    d = empty_individuals(C)
+    ac = np.zeros(C, dtype=bool)
+    ac[:N] = True
+    mean, var = species_param(p, "mean", s), species_param(p, "var", s)
+    Cquota, Nsuper = species_param(p, "Cquota", s), species_param(p, "Nsuper", s)
+    cqmax, nqmax, pqmax = (species_param(p, k, s) for k in ("Cqmax", "Nqmax", "Pqmax"))
+    R_NC, R_PC, Chl2Cint = (species_param(p, k, s) for k in ("R_NC", "R_PC", "Chl2Cint"))
+    Sz = rng.standard_normal(C)
+    x, y, z = rng.random(C), rng.random(C), rng.random(C)
+    Cq, Nq, Pq = rng.random(C), rng.random(C), rng.random(C)
+    d["ac"] = ac
+    d["gen"][:N] = 1.0
+    d["age"][:N] = 0.0
+    d["x"] = (x * grid.Nx) * ac
+    d["y"] = (y * grid.Ny) * ac
+    d["z"] = (z * grid.Nz) * ac
+    d["Sz"] = np.maximum(1.0, Sz * var + mean) * ac
+    d["Bm"] = Cquota * d["Sz"] * Nsuper
+    d["Cq"] = Cq * cqmax * d["Bm"]
+    d["Nq"] = Nq * (nqmax * (d["Bm"] + d["Cq"]) - d["Bm"] * R_NC)
+    d["Pq"] = Pq * (pqmax * (d["Bm"] + d["Cq"]) - d["Bm"] * R_PC)
+    d["Chl"] = d["Bm"] * Chl2Cint
+    mask_individuals(d, grid, N)
+    return d
+
+
+def mask_individuals(d, grid, N):
+    """mask_individuals! (Individuals/utils.jl:89-100)."""
+    ac = d["ac"][:N]
+    xi = np.trunc((d["x"][:N] + 1) * ac).astype(np.int64) + grid.Hx
+    yi = np.trunc((d["y"][:N] + 1) * ac).astype(np.int64) + grid.Hy
+    zi = np.trunc((d["z"][:N] + 1) * ac).astype(np.int64) + grid.Hz
+    lm = grid.landmask[xi - 1, yi - 1, zi - 1]
+    d["ac"][:N] = lm & ac
+
+
+def generate_tracers(grid, source, rng):
+    """generate_tracers for a NamedTuple-style source {initial_condition, rand_noise}: each tracer
+    is its value times a draw from lower:1.0e-4:upper, masked by land, halos filled."""
+    shape = grid.total_size
+    out = []
+    ic, noise = source["initial_condition"], source["rand_noise"]
+    for name in tracer_names:
+        if name not in ic:
+            raise ValueError(f"TRAC_INIT: tracer not found {name}")
+        if ic[name] < 0.0:
+            raise ValueError("TRAC_INIT:  The initial condition should be none-negetive.")
+        lower, upper = 1.0 - noise[name], 1.0 + noise[name]
+        nsteps = int(round((upper - lower) / 1.0e-4))
+        lattice = lower + 1.0e-4 * rng.integers(0, nsteps + 1, size=shape)
+        a = np.asfortranarray(float(ic[name]) * lattice)
+        a *= grid.landmask
+        fill_halo_tracer(a, grid)
+        out.append(a)
+    return out

@@ -1,0 +1,250 @@
+"""Seeded synthetic workloads with the shapes of the benchmark configurations.
+
+config1: 2D horizontal, 128×128×1, dx=dy=1 km, dz=10 m, 1 species × 16384 individuals,
+         steady double-gyre velocity (peak 0.1 m/s), dt = 60 s.
+config2: 3D 256×256×64, dx=dy=50 m, dz=2 m, 2 species × 2,097,152 individuals seeded in the top
+         40 m, divergence-free random-Fourier velocity (256 modes, k^-5/3, rms 0.05 m/s) refreshed
+         every 60 steps, linear NO3 gradient with depth, dt = 30 s.
+config3: 3D 512×512×128, 4 species × 16,777,216 individuals, lognormal sizes with
+         μ ∈ {-0.5, 0, 0.5, 1}, σ = 0.25, random-Fourier velocity, dt = 20 s.
+Every size can be scaled down for tests with the keyword arguments.
+
+Individuals: positions uniform in the seeded region; size Sz ~ LogNormal(μ, σ);
+Bm = Cquota·Sz·Nsuper; quotas at half their maximum (the mean of the reference's uniform
+initialisation, plankton_generation.jl:64-68) times U(0.8, 1.2); Chl = Chl2Cint·Bm; gen = 1,
+age = 0; capacity = 2 × initial population. Tracers: DIC 20, NH4 0.5, NO3 0.8, PO4 0.10,
+DOC 10, DON 0.1, DOP 0.05, POC/PON/POP 0, each × U(0.9, 1.1); DFe, PFe_inorg, PFe_bio and Dust
+are 0. Light: 1000·max(0, sin(2π(t/86400 − 1/4))) µmol m⁻² s⁻¹ sampled at the middle of each
+hour (ΔT_PAR = 3600 s). Temperature: default_temperature (param_default.jl:22-38).
+"""
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from ._abi import tracer_names
+from .grids import Bounded, Periodic, RectilinearGrid, fill_halo_tracer
+from .init import empty_individuals
+from .parameters import default_temperature, update_bgc_params, update_phyt_params
+
+
+@dataclass
+class Workload:
+    name: str
+    grid: RectilinearGrid
+    bgc: dict
+    phyt: dict
+    nsp: int
+    capacity: int
+    N: list
+    individuals: list
+    tracers: list
+    dT: float
+    steps: int
+    dT_vel: float
+    n_vel: int
+    vel_fn: object            # vel_fn(snapshot_index) -> (u, v, w)
+    parf: np.ndarray          # (Nx, Ny, npar)
+    dT_PAR: float
+    temp: np.ndarray          # (Nx, Ny, Nz, ntemp)
+    dT_temp: float
+    seed: int
+    meta: dict = field(default_factory=dict)
+
+    def velocity(self, t):
+        return self.vel_fn(t)
+
+    def snapshots_needed(self, iterations):
+        """Velocity snapshots that `iterations` steps from t = 0 read (update.jl:18)."""
+        return int(np.floor((iterations - 1) * self.dT / self.dT_vel)) + 1 if iterations > 0 else 1
+
+
+def diel_parf(Nx, Ny, hours, peak=1000.0, phase=0.0):
+    h = np.arange(hours, dtype=np.float64)
+    t = (h + 0.5) * 3600.0 + phase
+    val = peak * np.maximum(0.0, np.sin(2.0 * np.pi * (t / 86400.0 - 0.25)))
+    return np.asfortranarray(np.broadcast_to(val[None, None, :], (Nx, Ny, hours)).copy(order="F"))
+
+
+def make_individuals(grid, phyt, s, N, C, rng, zmax=None, mu=0.0, sigma=0.2):
+    p = {k: (v[s] if hasattr(v, "__len__") else v) for k, v in phyt.items()}
+    d = empty_individuals(C)
+    zmax = grid.Nz if zmax is None else zmax
+    d["ac"][:N] = True
+    d["x"][:N] = rng.random(N) * grid.Nx
+    d["y"][:N] = rng.random(N) * grid.Ny
+    d["z"][:N] = rng.random(N) * zmax
+    Sz = np.exp(rng.normal(mu, sigma, N))
+    Bm = float(p["Cquota"]) * Sz * float(p["Nsuper"])
+    Cq = 0.5 * float(p["Cqmax"]) * Bm * rng.uniform(0.8, 1.2, N)
+    Nq = 0.5 * (float(p["Nqmax"]) * (Bm + Cq) - Bm * float(p["R_NC"])) * rng.uniform(0.8, 1.2, N)
+    Pq = 0.5 * (float(p["Pqmax"]) * (Bm + Cq) - Bm * float(p["R_PC"])) * rng.uniform(0.8, 1.2, N)
+    d["Sz"][:N] = Sz
+    d["Bm"][:N] = Bm
+    d["Cq"][:N] = Cq
+    d["Nq"][:N] = Nq
+    d["Pq"][:N] = Pq
+    d["Chl"][:N] = float(p["Chl2Cint"]) * Bm
+    d["gen"][:N] = 1.0
+    return d
+
+
+TRACER_INIT = dict(DIC=20.0, NH4=0.5, NO3=0.8, PO4=0.10, DOC=10.0, DON=0.1, DOP=0.05,
+                   POC=0.0, PON=0.0, POP=0.0)
+
+
+def make_tracers(grid, rng, no3_gradient_depth=None):
+    out = []
+    shape = grid.total_size
+    zc = -np.asarray(grid.zC, dtype=np.float64)   # depth of cell centres, with halos
+    for name in tracer_names:
+        v0 = TRACER_INIT.get(name, 0.0)
+        a = np.asfortranarray(v0 * rng.uniform(0.9, 1.1, shape))
+        if name == "NO3" and no3_gradient_depth:
+            a *= (1.0 + zc / no3_gradient_depth)[None, None, :]
+        a *= grid.landmask
+        fill_halo_tracer(a, grid)
+        out.append(np.asfortranarray(a))
+    return out
+
+
+def double_gyre(grid, peak=0.1):
+    """Steady double gyre on the C-grid from a corner streamfunction, following the recipe of the
+    reference's examples/helper_functions.jl:38-59: ψ = 0.3 sin(πx/L) sin(2πy/L) +
+    0.7 sin(2πx/L) sin(πy/L), u = -δyψ, v = δxψ, w = 0; scaled so max(|u|, |v|) = peak."""
+    Nx, Ny, Nz = grid.Nx, grid.Ny, grid.Nz
+    xs = np.arange(Nx + 1, dtype=np.float64)[:, None]
+    ys = np.arange(Ny + 1, dtype=np.float64)[None, :]
+    phi = 0.3 * np.sin(np.pi * xs / Nx) * np.sin(2 * np.pi * ys / Ny) + \
+        0.7 * np.sin(2 * np.pi * xs / Nx) * np.sin(np.pi * ys / Ny)
+    uu = -(phi[:, 1:] - phi[:, :-1])[:-1, :]
+    vv = (phi[1:, :] - phi[:-1, :])[:, :-1]
+    s = peak / max(np.abs(uu).max(), np.abs(vv).max())
+    u = np.asfortranarray(np.repeat((uu * s)[:, :, None], Nz, axis=2))
+    v = np.asfortranarray(np.repeat((vv * s)[:, :, None], Nz, axis=2))
+    w = np.zeros((Nx, Ny, Nz + 1), order="F")
+    return u, v, w
+
+
+class FourierVelocity:
+    """Divergence-free velocity u = ∇×A on the C-grid from a vector potential of `nmodes` random
+    Fourier modes per component. Horizontal wavenumbers are integers (periodic in x and y) with
+    |k| uniform in [1, kmax]; potential amplitudes scale as |k|^(-11/6), so the velocity energy
+    spectrum follows k^(-5/3). A_x and A_y vary as sin(nπ d/H) with depth d so w = 0 at the
+    surface and the bottom (Bounded z); A_z varies as cos(nπ d/H). The discrete divergence
+    (u[i+1]-u[i])/Δx + (v[j+1]-v[j])/Δy + (w[k]-w[k+1])/Δz is zero up to rounding. Each snapshot
+    is scaled to the requested rms speed."""
+
+    def __init__(self, grid, nmodes=256, rms=0.05, seed=0, kmax=None, vert_ratio=0.3):
+        self.g = grid
+        self.nmodes, self.rms, self.seed = nmodes, rms, seed
+        self.kmax = kmax or max(2, min(grid.Nx, grid.Ny) // 8)
+        self.vert_ratio = vert_ratio
+
+    def _modes(self, snap, comp):
+        rng = np.random.default_rng([self.seed, snap, comp])
+        M = self.nmodes
+        kabs = rng.uniform(1.0, self.kmax, M)
+        ang = rng.uniform(0, 2 * np.pi, M)
+        nx = np.rint(kabs * np.cos(ang)).astype(int)
+        ny = np.rint(kabs * np.sin(ang)).astype(int)
+        zero = (nx == 0) & (ny == 0)
+        nx[zero] = 1
+        nz = rng.integers(1, 4, M) if comp < 2 else rng.integers(0, 3, M)
+        amp = np.hypot(nx, ny) ** (-11.0 / 6.0)
+        phase = rng.uniform(0, 2 * np.pi, M)
+        return nx, ny, nz, amp, phase
+
+    def _potential(self, snap, comp, xpos, ypos, dpos):
+        """Σ_m a_m sin(kx x + ky y + φ) Z_m(d) at x (cells), y (cells), depth d (cells)."""
+        g = self.g
+        nx, ny, nz, amp, phase = self._modes(snap, comp)
+        X = np.exp(1j * (2 * np.pi * np.outer(nx, xpos) / g.Nx))          # (M, nx)
+        Y = np.exp(1j * (2 * np.pi * np.outer(ny, ypos) / g.Ny))          # (M, ny)
+        if comp < 2:
+            Z = np.sin(np.pi * np.outer(nz, dpos) / g.Nz)                  # (M, nd)
+        else:
+            Z = np.cos(np.pi * np.outer(nz, dpos) / g.Nz)
+        W = (amp * np.exp(1j * phase))[:, None] * Z                        # (M, nd)
+        out = np.empty((len(xpos), len(ypos), len(dpos)))
+        step = max(1, int(2 ** 22 // max(1, len(xpos) * self.nmodes)))
+        for j0 in range(0, len(ypos), step):
+            j1 = min(len(ypos), j0 + step)
+            XY = (X[:, :, None] * Y[:, None, j0:j1]).reshape(self.nmodes, -1)   # (M, nx*nyc)
+            F = XY.T @ W                                                         # (nx*nyc, nd)
+            out[:, j0:j1, :] = F.imag.reshape(len(xpos), j1 - j0, len(dpos))
+        return out
+
+    def __call__(self, snap):
+        g = self.g
+        Nx, Ny, Nz = g.Nx, g.Ny, g.Nz
+        dx, dy = g.Δx, g.Δy
+        dz = float(np.asarray(g.dzF)[g.Hz])
+        xf, xc = np.arange(Nx + 1, dtype=float), np.arange(Nx + 1, dtype=float) + 0.5
+        yf, yc = np.arange(Ny + 1, dtype=float), np.arange(Ny + 1, dtype=float) + 0.5
+        df, dc = np.arange(Nz + 1, dtype=float), np.arange(Nz, dtype=float) + 0.5
+        r = self.vert_ratio
+        Ah = self._potential(snap, 2, xf, yf, dc)              # (x face, y face, d centre)
+        Ay = r * self._potential(snap, 1, xf, yc, df)          # (x face, y centre, d face)
+        Ax = r * self._potential(snap, 0, xc, yf, df)          # (x centre, y face, d face)
+        Ay[:, :, 0] = 0.0; Ay[:, :, -1] = 0.0
+        Ax[:, :, 0] = 0.0; Ax[:, :, -1] = 0.0
+        # u at (x face i, y centre j, d centre k); v at (x centre, y face, d centre); w at d faces
+        u = (Ah[:Nx, 1:Ny + 1, :] - Ah[:Nx, :Ny, :]) / dy - (Ay[:Nx, :Ny, :-1] - Ay[:Nx, :Ny, 1:]) / dz
+        v = (Ax[:Nx, :Ny, :-1] - Ax[:Nx, :Ny, 1:]) / dz - (Ah[1:Nx + 1, :Ny, :] - Ah[:Nx, :Ny, :]) / dx
+        w = (Ay[1:Nx + 1, :Ny, :] - Ay[:Nx, :Ny, :]) / dx - (Ax[:Nx, 1:Ny + 1, :] - Ax[:Nx, :Ny, :]) / dy
+        s = self.rms / np.sqrt(np.mean(u ** 2) + np.mean(v ** 2) + np.mean(w[:, :, :Nz] ** 2))
+        return (np.asfortranarray(u * s), np.asfortranarray(v * s), np.asfortranarray(w * s))
+
+
+def _finish(name, grid, nsp, N, C, phyt_over, bgc_over, dT, steps, rng, vel_fn, n_vel, dT_vel, zmax,
+            mus, sigma, seed, no3_grad=None, parf_peak=1000.0):
+    FT = np.float64
+    bgc = update_bgc_params(bgc_over or {}, FT)
+    phyt = update_phyt_params(phyt_over or {}, FT, N=nsp)
+    inds = [make_individuals(grid, phyt, s, N[s], C, rng, zmax=zmax, mu=mus[s], sigma=sigma)
+            for s in range(nsp)]
+    trs = make_tracers(grid, rng, no3_gradient_depth=no3_grad)
+    hours = int(np.ceil(steps * dT / 3600.0)) + 1
+    parf = diel_parf(grid.Nx, grid.Ny, hours, peak=parf_peak)
+    temp = default_temperature(grid, dT, steps)
+    return Workload(name, grid, bgc, phyt, nsp, C, list(N), inds, trs, dT, steps, dT_vel, n_vel,
+                    vel_fn, parf, 3600.0, temp, 3600.0, seed)
+
+
+def config1(n=128, N=16384, steps=1440, dT=60.0, seed=1, capacity=None, phyt_over=None):
+    """Plain FP64, 2D horizontal (n×n×1, 1 km cells, 10 m deep)."""
+    rng = np.random.default_rng(seed)
+    grid = RectilinearGrid(size=(n, n, 1), x=(0.0, n * 1000.0), y=(0.0, n * 1000.0), z=(0.0, -10.0),
+                           FT=np.float64, topology=(Periodic, Periodic, Bounded))
+    u, v, w = double_gyre(grid, 0.1)
+    C = capacity or 2 * N
+    return _finish("config1", grid, 1, [N], C, phyt_over, None, dT, steps, rng,
+                   lambda t: (u, v, w), 1, dT * steps, None, [0.0], 0.2, seed)
+
+
+def config2(nx=256, nz=64, N_per_species=2_097_152, nsp=2, steps=1000, dT=30.0, seed=2,
+            nmodes=256, capacity=None, phyt_over=None):
+    """FP64/FP32 3D (nx×nx×nz, 50 m × 50 m × 2 m), individuals in the top 40 m."""
+    rng = np.random.default_rng(seed)
+    grid = RectilinearGrid(size=(nx, nx, nz), x=(0.0, nx * 50.0), y=(0.0, nx * 50.0),
+                           z=(0.0, -2.0 * nz), FT=np.float64, topology=(Periodic, Periodic, Bounded))
+    vel = FourierVelocity(grid, nmodes=nmodes, rms=0.05, seed=seed)
+    C = capacity or 2 * N_per_species
+    zmax = min(nz, 20)
+    n_vel = int(np.ceil(steps / 60)) + 1
+    return _finish("config2", grid, nsp, [N_per_species] * nsp, C, phyt_over, None, dT, steps, rng,
+                   vel, n_vel, 60 * dT, zmax, [0.0] * nsp, 0.2, seed, no3_grad=2.0 * nz)
+
+
+def config3(nx=512, nz=128, N_per_species=16_777_216, nsp=4, steps=1000, dT=20.0, seed=3,
+            nmodes=256, capacity=None):
+    """Mixed precision at scale (nx×nx×nz), 4 species with their own size distributions."""
+    rng = np.random.default_rng(seed)
+    grid = RectilinearGrid(size=(nx, nx, nz), x=(0.0, nx * 50.0), y=(0.0, nx * 50.0),
+                           z=(0.0, -2.0 * nz), FT=np.float64, topology=(Periodic, Periodic, Bounded))
+    vel = FourierVelocity(grid, nmodes=nmodes, rms=0.05, seed=seed)
+    C = capacity or 2 * N_per_species
+    mus = [-0.5, 0.0, 0.5, 1.0][:nsp]
+    n_vel = int(np.ceil(steps / 60)) + 1
+    return _finish("config3", grid, nsp, [N_per_species] * nsp, C, None, None, dT, steps, rng,
+                   vel, n_vel, 60 * dT, min(nz, 20), mus, 0.25, seed, no3_grad=2.0 * nz)

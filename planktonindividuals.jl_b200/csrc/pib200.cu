@@ -1,0 +1,843 @@
+// libpib200 — C ABI (include/pib200.h) and step orchestration of the B200 model time step.
+//
+// One handle = one PlanktonModel on the CUDA device current at pi_create, with its own stream.
+// A step (TimeStep!, src/Model/time_step.jl:12-180) is this sequence of launches:
+//   k_particles          RK4 + diffusion + find_inds! for every species; per-cell counts
+//   scan(cnt) → off      cell offsets of the binned individuals
+//   radix sort           (cell, species·C + slot) order = the order of a sequential reference run
+//   k_setpos             position of each individual in the cell-sorted list
+//   k_par                Chl per cell, calc_par! down each column, PAR diagnostic
+//   per species:         k_decide → scan(flags) → k_lists → k_daughters → k_physiology
+//   k_sweep_x/y          DST3FL sweeps on tracer_temp
+//   k_sweep_z_final      z sweep + tendency, diffusion, sinking, forcing, BCs, particle terms
+//   k_halo<x,y,z>        fill_halo_tracer! on the new tracers
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kernels_fp64.cuh"
+
+using namespace pib;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct HostGrid {
+    int Nx, Ny, Nz, Hx, Hy, Hz, Gx, Gy, Gz;
+    int topo[3];
+    double dx, dy;
+    std::vector<double> dzF, dzC;
+    std::vector<uint8_t> lm;
+    long long G;
+    size_t id(long i, long j, long k) const {
+        return (size_t)(i - 1) + (size_t)Gx * ((size_t)(j - 1) + (size_t)Gy * (size_t)(k - 1));
+    }
+};
+
+// Host halo rules for velocities (HaloRegions/halo_regions.jl:2-99), used by vel_copy!.
+// mode 0 tracer rule, 1 velocity rule on the high face.
+void host_fill_face(const HostGrid& g, std::vector<double>& c, int axis, int face, int mode) {
+    int N = axis == 0 ? g.Nx : axis == 1 ? g.Ny : g.Nz;
+    int H = axis == 0 ? g.Hx : axis == 1 ? g.Hy : g.Hz;
+    int topo = g.topo[axis];
+    int n1 = axis == 0 ? g.Gy : g.Gx, n2 = axis == 2 ? g.Gy : g.Gz;
+    std::vector<long> dst, src;
+    if (face == 0) {
+        for (int h = 1; h <= H; ++h) { dst.push_back(h); src.push_back(topo == PI_PERIODIC ? N + h : H + 1); }
+    } else if (mode == 1 && topo == PI_BOUNDED) {
+        for (int h = N + H + 2; h <= N + 2 * H; ++h) { dst.push_back(h); src.push_back(N + H + 1); }
+    } else {
+        for (int h = 1; h <= H; ++h) { dst.push_back(N + H + h); src.push_back(topo == PI_PERIODIC ? H + h : N + H); }
+    }
+    std::vector<double> tmp(dst.size());
+    for (int b2 = 1; b2 <= n2; ++b2)
+        for (int b1 = 1; b1 <= n1; ++b1) {
+            auto at = [&](long a) -> double& {
+                if (axis == 0) return c[g.id(a, b1, b2)];
+                if (axis == 1) return c[g.id(b1, a, b2)];
+                return c[g.id(b1, b2, a)];
+            };
+            for (size_t q = 0; q < dst.size(); ++q) tmp[q] = at(src[q]);
+            for (size_t q = 0; q < dst.size(); ++q) at(dst[q]) = tmp[q];
+        }
+}
+
+void host_fill_halo_vel(const HostGrid& g, std::vector<double>& u, std::vector<double>& v, std::vector<double>& w) {
+    host_fill_face(g, u, 0, 1, 1); host_fill_face(g, u, 0, 0, 0);
+    host_fill_face(g, u, 1, 0, 0); host_fill_face(g, u, 1, 1, 0);
+    host_fill_face(g, u, 2, 0, 0); host_fill_face(g, u, 2, 1, 0);
+    host_fill_face(g, v, 1, 1, 1); host_fill_face(g, v, 0, 0, 0); host_fill_face(g, v, 0, 1, 0);
+    host_fill_face(g, v, 1, 0, 0); host_fill_face(g, v, 2, 0, 0); host_fill_face(g, v, 2, 1, 0);
+    host_fill_face(g, w, 2, 1, 1); host_fill_face(g, w, 0, 0, 0); host_fill_face(g, w, 0, 1, 0);
+    host_fill_face(g, w, 1, 0, 0); host_fill_face(g, w, 1, 1, 0); host_fill_face(g, w, 2, 0, 0);
+}
+
+// Interior velocity snapshot (reference array layout) → halo-padded fields (vel_copy!).
+void host_vel_copy(const HostGrid& g, const double* u, const double* v, const double* w,
+                   std::vector<double>& U, std::vector<double>& V, std::vector<double>& W) {
+    U.assign(g.G, 0.0); V.assign(g.G, 0.0); W.assign(g.G, 0.0);
+    int ex = g.topo[0] == PI_BOUNDED, ey = g.topo[1] == PI_BOUNDED, ez = g.topo[2] == PI_BOUNDED;
+    auto copy_in = [&](std::vector<double>& f, const double* s, int nx, int ny, int nz) {
+        for (int k = 1; k <= nz; ++k) for (int j = 1; j <= ny; ++j) for (int i = 1; i <= nx; ++i)
+            f[g.id(i + g.Hx, j + g.Hy, k + g.Hz)] =
+                s[(size_t)(i - 1) + (size_t)nx * ((size_t)(j - 1) + (size_t)ny * (size_t)(k - 1))];
+    };
+    copy_in(U, u, g.Nx + ex, g.Ny, g.Nz);
+    copy_in(V, v, g.Nx, g.Ny + ey, g.Nz);
+    copy_in(W, w, g.Nx, g.Ny, g.Nz + ez);
+    host_fill_halo_vel(g, U, V, W);
+}
+
+// Julia's string(x::Float64) for the capacity message: shortest round-trip digits.
+std::string julia_float(double x) {
+    char buf[64];
+    for (int p = 1; p <= 17; ++p) {
+        snprintf(buf, sizeof buf, "%.*g", p, x);
+        if (strtod(buf, nullptr) == x) break;
+    }
+    std::string s(buf);
+    size_t e = s.find('e');
+    if (e == std::string::npos) {
+        if (s.find('.') == std::string::npos && s.find("inf") == std::string::npos && s.find("nan") == std::string::npos) s += ".0";
+        return s;
+    }
+    std::string mant = s.substr(0, e), ex = s.substr(e + 1);
+    if (mant.find('.') == std::string::npos) mant += ".0";
+    int ev = atoi(ex.c_str());
+    return mant + "e" + std::to_string(ev);
+}
+
+struct DevBC {
+    int kind = PI_BC_NONE;
+    long long nt = 0;
+    double* v = nullptr;
+};
+
+}  // namespace
+
+struct pi_model {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    HostGrid hg;
+    DGrid dg;
+    pi_bgc_params bgc;
+    std::vector<pi_quota_params> sp;
+    int nsp = 0;
+    long long C = 0;
+    uint64_t seed = 0;
+    int precision = PI_FP64;
+    int64_t iteration = 0;
+    double t = 0.0;
+    double last_dT = 0.0;
+    std::string err;
+    std::vector<void*> allocs;
+
+    // device state
+    std::vector<SpcDev> h_spc;
+    SpcDev* d_spc = nullptr;
+    double* tr = nullptr;        // 14 × G
+    double* tr_next = nullptr;   // 14 × G
+    double* tta = nullptr;       // 14 × G
+    double* ttb = nullptr;       // 14 × G
+    double* velbuf[2][3] = {{nullptr}};
+    const double* vel0[3] = {nullptr, nullptr, nullptr};
+    const double* vel1[3] = {nullptr, nullptr, nullptr};
+    int vel1_buf = 1;            // own buffer that vel1 points to, -1 when bound to a series
+    double* zeros = nullptr;     // G zeros (vel₀ before the first step)
+    double* par = nullptr;       // G
+    double* PARF = nullptr;      // Nx·Ny
+    double* temp_own = nullptr;  // G
+    const double* temp = nullptr;
+    double* diag_par = nullptr;  // G
+    double* diag_sp = nullptr;   // nsp × 4 × G (num, graz, mort, dvid)
+    double* dzF = nullptr;
+    double* dzC = nullptr;
+    uint8_t* lm = nullptr;
+    StepBufs sb{};
+    uint32_t* iota = nullptr;    // nsp·C
+    void* cub_tmp = nullptr;
+    size_t cub_bytes = 0;
+    int key_bits = 1;
+    DevBC bcs[PI_NTRACERS][6];
+    FluxBCDev* d_bcs = nullptr;
+    int any_bc = 0;
+};
+
+struct pi_sim {
+    pi_model* m = nullptr;
+    double dT = 0.0;
+    int64_t iterations = 0;
+    int has_vel = 0;
+    int64_t nvel = 0, npar = 0, ntemp = 0;
+    double dT_vel = 0.0, dT_PAR = 0.0, dT_temp = 0.0;
+    std::vector<double*> vel;     // 3 × nvel halo-padded fields
+    double* parf = nullptr;       // Nx·Ny × npar
+    std::vector<double*> temp;    // ntemp halo-padded fields
+};
+
+namespace {
+
+pi_status fail(pi_model* m, pi_status code, const std::string& msg) {
+    if (m) m->err = msg; else g_create_error = msg;
+    return code;
+}
+
+pi_status cuda_fail(pi_model* m, cudaError_t e, const char* what) {
+    std::string msg = std::string(what) + ": " + cudaGetErrorString(e);
+    return fail(m, e == cudaErrorMemoryAllocation ? PI_ERR_NOMEM : PI_ERR_CUDA, msg);
+}
+
+#define CK(call, what)                                              \
+    do {                                                            \
+        cudaError_t e_ = (call);                                    \
+        if (e_ != cudaSuccess) return cuda_fail(m, e_, what);       \
+    } while (0)
+
+template <typename T>
+pi_status dalloc(pi_model* m, T** p, size_t n, const char* what) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess) return cuda_fail(m, e, what);
+    m->allocs.push_back(q);
+    *p = (T*)q;
+    return PI_OK;
+}
+
+#define AL(ptr, n) do { pi_status s_ = dalloc(m, &(ptr), (size_t)(n), #ptr); if (s_) return s_; } while (0)
+
+void free_all(pi_model* m) {
+    for (void* p : m->allocs) cudaFree(p);
+    m->allocs.clear();
+    for (int n = 0; n < PI_NTRACERS; ++n)
+        for (int f = 0; f < 6; ++f)
+            if (m->bcs[n][f].v) { cudaFree(m->bcs[n][f].v); m->bcs[n][f].v = nullptr; }
+}
+
+inline unsigned nblk(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+// Reads and clears the device error word; converts it to a status.
+pi_status check_device_errors(pi_model* m) {
+    uint32_t err = 0;
+    int64_t it = 0;
+    CK(cudaMemcpyAsync(&err, m->sb.err, sizeof err, cudaMemcpyDeviceToHost, m->stream), "read error word");
+    CK(cudaMemcpyAsync(&it, m->sb.err_iter, sizeof it, cudaMemcpyDeviceToHost, m->stream), "read error iteration");
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    if (!err) return PI_OK;
+    CK(cudaMemsetAsync(m->sb.err, 0, sizeof(uint32_t), m->stream), "clear error word");
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    if (err & PI_DEVERR_CAPACITY) {
+        double tf = (double)it * m->last_dT;    // model.t of the failing step
+        return fail(m, PI_ERR_CAPACITY, "number of individual exceeds the capacity at timestep " +
+                                            julia_float(tf / 86400.0) + " days");
+    }
+    return fail(m, PI_ERR_DOMAIN, "an individual left the halo-padded grid (cell index out of range)");
+}
+
+// Enqueues one TimeStep! on the model's stream (no synchronisation).
+pi_status enqueue_step(pi_model* m, double dT) {
+    m->iteration += 1;
+    m->t = (double)m->iteration * dT;
+    m->last_dT = dT;
+    const DGrid& g = m->dg;
+    const long long G = g.G, C = m->C, NC = (long long)m->nsp * C;
+    const uint32_t iter = (uint32_t)m->iteration;
+    cudaStream_t st = m->stream;
+    StepBufs& sb = m->sb;
+    const int BS = 256;
+
+    CK(cudaMemsetAsync(sb.cnt, 0, (G + 1) * sizeof(uint32_t), st), "zero counts");
+    VelPtrs vp{m->vel0[0], m->vel0[1], m->vel0[2], m->vel1[0], m->vel1[1], m->vel1[2]};
+    k_particles<<<nblk(NC, BS), BS, 0, st>>>(g, m->d_spc, m->nsp, C, dT, m->seed, iter, vp,
+                                             m->bgc.kappa_hP, m->bgc.kappa_vP, sb.cnt, sb.key,
+                                             (uint32_t)G, sb.err);
+    CK(cudaGetLastError(), "k_particles");
+    size_t tb = m->cub_bytes;
+    CK(cub::DeviceScan::ExclusiveSum(m->cub_tmp, tb, sb.cnt, sb.off, (int)(G + 1), st), "scan counts");
+    tb = m->cub_bytes;
+    CK(cub::DeviceRadixSort::SortPairs(m->cub_tmp, tb, sb.key, sb.key_sorted, m->iota, sb.gid_sorted,
+                                       (int64_t)NC, 0, m->key_bits, st), "sort by cell");
+    k_setpos<<<nblk(NC, BS), BS, 0, st>>>(sb.off, G, sb.gid_sorted, sb.pos, NC, sb.err);
+    CK(cudaGetLastError(), "k_setpos");
+    {
+        dim3 grid(nblk(g.Nx, 128), g.Ny);
+        k_par<<<grid, 128, 0, st>>>(g, m->d_spc, C, sb.off, sb.gid_sorted, m->PARF, m->PARF, m->par,
+                                    m->diag_par, m->bgc.kc, m->bgc.kw, sb.err);
+        CK(cudaGetLastError(), "k_par");
+    }
+    const int shared = m->bgc.shared_graz == 1.0;
+    for (int s = 0; s < m->nsp; ++s) {
+        double* dsp = m->diag_sp + (size_t)s * 4 * G;
+        k_decide<<<nblk(C, BS), BS, 0, st>>>(g, m->h_spc[s], m->sp[s], C, s, sb.pos, sb.loss, sb.evk,
+                                             sb.flag64, dsp + 1 * G, dsp + 2 * G, dsp + 3 * G, sb.err);
+        CK(cudaGetLastError(), "k_decide");
+        tb = m->cub_bytes;
+        CK(cub::DeviceScan::ExclusiveSum(m->cub_tmp, tb, sb.flag64, sb.rank64, (int64_t)C, st), "scan division flags");
+        k_lists<<<nblk(C, BS), BS, 0, st>>>(sb.flag64, sb.rank64, C, sb.divlist, sb.freelist, sb.ndiv,
+                                            sb.err, sb.err_iter, m->iteration);
+        CK(cudaGetLastError(), "k_lists");
+        k_daughters<<<148 * 4, 256, 0, st>>>(m->h_spc[s], sb.divlist, sb.freelist, sb.ndiv, sb.err);
+        CK(cudaGetLastError(), "k_daughters");
+        const double* trp = m->tr;
+        k_physiology<<<nblk(C, BS), BS, 0, st>>>(g, m->h_spc[s], m->sp[s], C, s, dT, m->t, m->seed, iter,
+                                                 shared, trp + PI_NH4 * G, trp + PI_NO3 * G,
+                                                 trp + PI_PO4 * G, trp + PI_DOC * G, m->par, m->temp,
+                                                 sb.off, sb.gid_sorted, sb.pos, sb.contrib,
+                                                 dsp + 0 * G, sb.err);
+        CK(cudaGetLastError(), "k_physiology");
+    }
+    {
+        dim3 grid(nblk(g.Nx, 128), g.Ny, g.Nz);
+        k_sweep_x<<<grid, 128, 0, st>>>(g, m->tr, m->tta, m->vel1[0], dT, sb.err);
+        CK(cudaGetLastError(), "k_sweep_x");
+        k_sweep_y<<<grid, 128, 0, st>>>(g, m->tr, m->tta, m->ttb, m->vel1[1], dT, sb.err);
+        CK(cudaGetLastError(), "k_sweep_y");
+        ZFinalArgs za;
+        za.g = g; za.tr = m->tr; za.ttb = m->ttb; za.tr_next = m->tr_next; za.w = m->vel1[2];
+        za.dT = dT; za.b = m->bgc;
+        za.diffuse = (m->bgc.kappa_h != 0.0 || m->bgc.kappa_v != 0.0);
+        za.any_bc = m->any_bc; za.bcs = m->d_bcs; za.iter = m->iteration;
+        za.spc = m->d_spc; za.C = C; za.off = sb.off; za.gid_sorted = sb.gid_sorted; za.evk = sb.evk;
+        za.loss = sb.loss; za.contrib = sb.contrib; za.nsp = m->nsp; za.err = sb.err;
+        dim3 g2(nblk(g.Nx, 64), g.Ny);
+        k_sweep_z_final<<<g2, 64, 0, st>>>(za);
+        CK(cudaGetLastError(), "k_sweep_z_final");
+        // tracers are only replaced when the step completed (a capacity error leaves them)
+        k_halo<0><<<dim3(nblk(g.Gy, 64), g.Gz, PI_NTRACERS), 64, 0, st>>>(g, m->tr_next, PI_NTRACERS, sb.err);
+        k_halo<1><<<dim3(nblk(g.Gx, 64), g.Gz, PI_NTRACERS), 64, 0, st>>>(g, m->tr_next, PI_NTRACERS, sb.err);
+        k_halo<2><<<dim3(nblk(g.Gx, 64), g.Gy, PI_NTRACERS), 64, 0, st>>>(g, m->tr_next, PI_NTRACERS, sb.err);
+        CK(cudaGetLastError(), "k_halo");
+        k_copy_if_err<<<148 * 4, 256, 0, st>>>(m->tr_next, m->tr, PI_NTRACERS * G, sb.err);
+        CK(cudaGetLastError(), "k_copy_if_err");
+    }
+    std::swap(m->tr, m->tr_next);
+    for (int c = 0; c < 3; ++c) m->vel0[c] = m->vel1[c];    // vel₀ .= vel₁ (time_step.jl:174-176)
+    return PI_OK;
+}
+
+pi_status upload_bcs(pi_model* m) {
+    std::vector<FluxBCDev> h(PI_NTRACERS * 6);
+    m->any_bc = 0;
+    const HostGrid& g = m->hg;
+    for (int n = 0; n < PI_NTRACERS; ++n)
+        for (int f = 0; f < 6; ++f) {
+            FluxBCDev& d = h[n * 6 + f];
+            d.kind = m->bcs[n][f].kind;
+            d.nt = m->bcs[n][f].nt;
+            d.v = m->bcs[n][f].v;
+            d.n1 = f <= PI_EAST ? g.Ny : g.Nx;
+            d.n2 = f <= PI_NORTH ? g.Nz : g.Ny;
+            if (d.kind) m->any_bc = 1;
+        }
+    CK(cudaMemcpyAsync(m->d_bcs, h.data(), h.size() * sizeof(FluxBCDev), cudaMemcpyHostToDevice, m->stream), "upload bcs");
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    return PI_OK;
+}
+
+pi_status validate_quota(const pi_quota_params& p, int s, std::string& msg) {
+    int ty = (int)p.dvid_type;
+    if ((double)ty != p.dvid_type || ty < 1 || ty > 3) {
+        msg = "Wrong cell division type, must be in 1 to 3 (species " + std::to_string(s + 1) + ")";
+        return PI_ERR_PARAM;
+    }
+    return PI_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* pi_status_string(pi_status code) {
+    switch (code) {
+        case PI_OK: return "ok";
+        case PI_ERR_ARG: return "invalid argument";
+        case PI_ERR_SHAPE: return "dimension mismatch";
+        case PI_ERR_PARAM: return "invalid parameter";
+        case PI_ERR_CAPACITY: return "number of individuals exceeds the capacity";
+        case PI_ERR_CUDA: return "CUDA error";
+        case PI_ERR_TIMEOUT: return "device wait timed out";
+        case PI_ERR_NAN: return "NaN found";
+        case PI_ERR_DOMAIN: return "individual outside the grid";
+        case PI_ERR_NOMEM: return "out of device memory";
+        case PI_ERR_STATE: return "invalid state";
+        default: return "unknown status";
+    }
+}
+
+pi_status pi_last_error(pi_model* m, char* buf, size_t len) {
+    const std::string& e = m ? m->err : g_create_error;
+    if (buf && len) {
+        size_t n = std::min(len - 1, e.size());
+        memcpy(buf, e.c_str(), n);
+        buf[n] = 0;
+    }
+    return PI_OK;
+}
+
+pi_status pi_create(const pi_grid* grid, const pi_bgc_params* bgc, const pi_quota_params* species,
+                    int32_t nspecies, int64_t capacity, int32_t precision, uint64_t seed, pi_model** out) {
+    if (!out) return fail(nullptr, PI_ERR_ARG, "pi_create: out is NULL");
+    *out = nullptr;
+    if (!grid || !bgc || !species || nspecies < 1 || capacity < 1 || !grid->dzF || !grid->dzC)
+        return fail(nullptr, PI_ERR_ARG, "pi_create: NULL argument, nspecies < 1 or capacity < 1");
+    if (precision != PI_FP64)
+        return fail(nullptr, PI_ERR_ARG, "pi_create: this build provides the FP64 form (PI_FP64) only");
+    if (grid->Nx < 1 || grid->Ny < 1 || grid->Nz < 1)
+        return fail(nullptr, PI_ERR_ARG, "pi_create: grid size must be at least 1 in every direction");
+    if (grid->Hx < 2 || grid->Hy < 2 || grid->Hz < 2 || grid->Hx > 8 || grid->Hy > 8 || grid->Hz > 8)
+        return fail(nullptr, PI_ERR_ARG, "pi_create: halo must be 2..8 points (DST3FL needs at least 2)");
+    for (int a = 0; a < 3; ++a)
+        if (grid->topo[a] != PI_PERIODIC && grid->topo[a] != PI_BOUNDED)
+            return fail(nullptr, PI_ERR_ARG, "pi_create: topology must be Periodic or Bounded");
+    if (grid->topo[2] != PI_BOUNDED)
+        return fail(nullptr, PI_ERR_ARG, "pi_create: z must be Bounded (tracer sinking has no Periodic rule)");
+    long long Gx = grid->Nx + 2LL * grid->Hx, Gy = grid->Ny + 2LL * grid->Hy, Gz = grid->Nz + 2LL * grid->Hz;
+    if (Gx * Gy * Gz >= (1LL << 31) - 2 || (Gx + 1) * (Gy + 1) * (Gz + 1) >= (1LL << 31))
+        return fail(nullptr, PI_ERR_ARG, "pi_create: grid too large for 32-bit cell indices");
+    if ((long long)nspecies * capacity >= (1LL << 31))
+        return fail(nullptr, PI_ERR_ARG, "pi_create: nspecies × capacity must be below 2^31");
+    for (int s = 0; s < nspecies; ++s) {
+        std::string msg;
+        pi_status st = validate_quota(species[s], s, msg);
+        if (st) return fail(nullptr, st, msg);
+    }
+    pi_model* m = new pi_model();
+    if (cudaGetDevice(&m->device) != cudaSuccess) {
+        delete m;
+        return fail(nullptr, PI_ERR_CUDA, "pi_create: no CUDA device");
+    }
+    auto bail = [&](pi_status st) { g_create_error = m->err; free_all(m); if (m->stream) cudaStreamDestroy(m->stream); delete m; return st; };
+    if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        m->err = "pi_create: stream creation failed"; return bail(PI_ERR_CUDA);
+    }
+    HostGrid& hg = m->hg;
+    hg.Nx = grid->Nx; hg.Ny = grid->Ny; hg.Nz = grid->Nz; hg.Hx = grid->Hx; hg.Hy = grid->Hy; hg.Hz = grid->Hz;
+    hg.Gx = (int)Gx; hg.Gy = (int)Gy; hg.Gz = (int)Gz;
+    for (int a = 0; a < 3; ++a) hg.topo[a] = grid->topo[a];
+    hg.dx = grid->dx; hg.dy = grid->dy;
+    hg.dzF.assign(grid->dzF, grid->dzF + Gz);
+    hg.dzC.assign(grid->dzC, grid->dzC + Gz);
+    hg.G = Gx * Gy * Gz;
+    hg.lm.assign(hg.G, 1);
+    int all_water = 1;
+    if (grid->landmask) {
+        hg.lm.assign(grid->landmask, grid->landmask + hg.G);
+        for (uint8_t v : hg.lm) if (v != 1) { all_water = 0; break; }
+        for (uint8_t& v : hg.lm) v = v ? 1 : 0;
+    }
+    m->bgc = *bgc;
+    m->sp.assign(species, species + nspecies);
+    m->nsp = nspecies; m->C = capacity; m->seed = seed; m->precision = precision;
+    const long long G = hg.G, C = capacity, NC = (long long)nspecies * capacity;
+    pi_status st;
+#define ALB(ptr, n) do { st = dalloc(m, &(ptr), (size_t)(n), #ptr); if (st) return bail(st); } while (0)
+    ALB(m->dzF, Gz); ALB(m->dzC, Gz); ALB(m->lm, G);
+    ALB(m->tr, PI_NTRACERS * G); ALB(m->tr_next, PI_NTRACERS * G);
+    ALB(m->tta, PI_NTRACERS * G); ALB(m->ttb, PI_NTRACERS * G);
+    for (int b = 0; b < 2; ++b) for (int c = 0; c < 3; ++c) ALB(m->velbuf[b][c], G);
+    ALB(m->zeros, G); ALB(m->par, G); ALB(m->PARF, (long long)hg.Nx * hg.Ny); ALB(m->temp_own, G);
+    ALB(m->diag_par, G); ALB(m->diag_sp, 4LL * nspecies * G);
+    StepBufs& sb = m->sb;
+    ALB(sb.cnt, G + 1); ALB(sb.off, G + 1); ALB(sb.key, NC); ALB(sb.key_sorted, NC);
+    ALB(sb.gid_sorted, NC); ALB(sb.pos, NC); ALB(sb.contrib, 5 * NC); ALB(sb.loss, 6 * NC);
+    ALB(sb.evk, NC); ALB(sb.flag64, C); ALB(sb.rank64, C); ALB(sb.divlist, C); ALB(sb.freelist, C);
+    ALB(sb.ndiv, 1); ALB(sb.err, 1); ALB(sb.err_iter, 1);
+    ALB(m->iota, NC);
+    ALB(m->d_bcs, PI_NTRACERS * 6);
+    m->h_spc.resize(nspecies);
+    for (int s = 0; s < nspecies; ++s) {
+        SpcDev& P = m->h_spc[s];
+        ALB(P.x, C); ALB(P.y, C); ALB(P.z, C); ALB(P.Sz, C); ALB(P.Bm, C); ALB(P.Cq, C); ALB(P.Nq, C);
+        ALB(P.Pq, C); ALB(P.Chl, C); ALB(P.gen, C); ALB(P.age, C); ALB(P.flags, C); ALB(P.cell, C);
+        ALB(P.stat, C);
+    }
+    ALB(m->d_spc, nspecies);
+#undef ALB
+    cudaStream_t s0 = m->stream;
+    bool ok = true;
+    ok = ok && cudaMemcpyAsync(m->dzF, hg.dzF.data(), Gz * sizeof(double), cudaMemcpyHostToDevice, s0) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync(m->dzC, hg.dzC.data(), Gz * sizeof(double), cudaMemcpyHostToDevice, s0) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync(m->lm, hg.lm.data(), G, cudaMemcpyHostToDevice, s0) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync(m->d_spc, m->h_spc.data(), nspecies * sizeof(SpcDev), cudaMemcpyHostToDevice, s0) == cudaSuccess;
+    for (void* p : { (void*)m->tr, (void*)m->tr_next, (void*)m->tta, (void*)m->ttb })
+        ok = ok && cudaMemsetAsync(p, 0, PI_NTRACERS * G * sizeof(double), s0) == cudaSuccess;
+    for (int b = 0; b < 2; ++b) for (int c = 0; c < 3; ++c)
+        ok = ok && cudaMemsetAsync(m->velbuf[b][c], 0, G * sizeof(double), s0) == cudaSuccess;
+    for (void* p : { (void*)m->zeros, (void*)m->par, (void*)m->temp_own, (void*)m->diag_par })
+        ok = ok && cudaMemsetAsync(p, 0, G * sizeof(double), s0) == cudaSuccess;
+    ok = ok && cudaMemsetAsync(m->PARF, 0, hg.Nx * (size_t)hg.Ny * sizeof(double), s0) == cudaSuccess;
+    ok = ok && cudaMemsetAsync(m->diag_sp, 0, 4 * nspecies * G * sizeof(double), s0) == cudaSuccess;
+    ok = ok && cudaMemsetAsync(sb.cnt, 0, (G + 1) * sizeof(uint32_t), s0) == cudaSuccess;
+    ok = ok && cudaMemsetAsync(sb.err, 0, sizeof(uint32_t), s0) == cudaSuccess;
+    ok = ok && cudaMemsetAsync(sb.err_iter, 0, sizeof(int64_t), s0) == cudaSuccess;
+    for (int s = 0; s < nspecies; ++s) {
+        const SpcDev& P = m->h_spc[s];
+        for (double* p : { P.x, P.y, P.z, P.Sz, P.Bm, P.Cq, P.Nq, P.Pq, P.Chl, P.gen, P.age })
+            ok = ok && cudaMemsetAsync(p, 0, C * sizeof(double), s0) == cudaSuccess;
+        ok = ok && cudaMemsetAsync(P.flags, 0, C, s0) == cudaSuccess;
+        ok = ok && cudaMemsetAsync(P.stat, 0, C, s0) == cudaSuccess;
+        ok = ok && cudaMemsetAsync(P.cell, 0, C * sizeof(int32_t), s0) == cudaSuccess;  // (0,0,0) as constructed
+    }
+    {
+        std::vector<uint32_t> io(NC);
+        for (long long q = 0; q < NC; ++q) io[q] = (uint32_t)q;
+        ok = ok && cudaMemcpyAsync(m->iota, io.data(), NC * sizeof(uint32_t), cudaMemcpyHostToDevice, s0) == cudaSuccess;
+        ok = ok && cudaStreamSynchronize(s0) == cudaSuccess;
+    }
+    if (!ok) { m->err = "pi_create: device initialisation failed"; return bail(PI_ERR_CUDA); }
+    // vel₀ = vel₁ = 0 until set (timestepper.jl:24-26)
+    for (int c = 0; c < 3; ++c) { m->vel0[c] = m->velbuf[0][c]; m->vel1[c] = m->velbuf[1][c]; }
+    m->vel1_buf = 1;
+    m->temp = m->temp_own;
+    m->key_bits = 1;
+    while ((1LL << m->key_bits) <= G) ++m->key_bits;
+    // CUB scratch: the largest of the three uses
+    size_t b1 = 0, b2 = 0, b3 = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, b1, sb.cnt, sb.off, (int)(G + 1), s0);
+    cub::DeviceRadixSort::SortPairs(nullptr, b2, sb.key, sb.key_sorted, m->iota, sb.gid_sorted, (int64_t)NC, 0, m->key_bits, s0);
+    cub::DeviceScan::ExclusiveSum(nullptr, b3, sb.flag64, sb.rank64, (int64_t)C, s0);
+    m->cub_bytes = std::max(b1, std::max(b2, b3));
+    st = dalloc(m, (char**)&m->cub_tmp, m->cub_bytes, "cub scratch");
+    if (st) return bail(st);
+    m->dg = DGrid{hg.Nx, hg.Ny, hg.Nz, hg.Hx, hg.Hy, hg.Hz, hg.Gx, hg.Gy, hg.Gz,
+                  hg.topo[0], hg.topo[1], hg.topo[2], all_water, hg.dx, hg.dy, m->dzF, m->dzC, m->lm, G};
+    st = upload_bcs(m);
+    if (st) return bail(st);
+    *out = m;
+    return PI_OK;
+}
+
+pi_status pi_destroy(pi_model* m) {
+    if (!m) return PI_OK;
+    cudaStreamSynchronize(m->stream);
+    free_all(m);
+    cudaStreamDestroy(m->stream);
+    delete m;
+    return PI_OK;
+}
+
+pi_status pi_set_individuals(pi_model* m, int32_t sp, const pi_individuals* in) {
+    if (!m || !in || sp < 0 || sp >= m->nsp) return fail(m, PI_ERR_ARG, "pi_set_individuals: bad argument");
+    const double* dcols[] = { in->x, in->y, in->z, in->Sz, in->Bm, in->Cq, in->Nq, in->Pq, in->Chl, in->gen, in->age,
+                              in->graz, in->mort, in->dvid };
+    for (const double* p : dcols) if (!p) return fail(m, PI_ERR_ARG, "pi_set_individuals: NULL attribute");
+    if (!in->xi || !in->yi || !in->zi || !in->ac) return fail(m, PI_ERR_ARG, "pi_set_individuals: NULL attribute");
+    const long long C = m->C;
+    const HostGrid& g = m->hg;
+    std::vector<uint8_t> flags(C);
+    std::vector<int32_t> cell(C);
+    for (long long i = 0; i < C; ++i) {
+        if (in->ac[i] > 1) return fail(m, PI_ERR_PARAM, "pi_set_individuals: ac must be 0 or 1");
+        double d3[3] = { in->graz[i], in->mort[i], in->dvid[i] };
+        for (double d : d3)
+            if (d != 0.0 && d != 1.0) return fail(m, PI_ERR_PARAM, "pi_set_individuals: graz/mort/dvid must be 0 or 1");
+        if (in->xi[i] < 0 || in->xi[i] > g.Gx || in->yi[i] < 0 || in->yi[i] > g.Gy || in->zi[i] < 0 || in->zi[i] > g.Gz)
+            return fail(m, PI_ERR_PARAM, "pi_set_individuals: xi/yi/zi outside 0..G");
+        flags[i] = (uint8_t)((in->ac[i] ? FL_AC : 0) | (in->graz[i] == 1.0 ? FL_GRAZ : 0) |
+                             (in->mort[i] == 1.0 ? FL_MORT : 0) | (in->dvid[i] == 1.0 ? FL_DVID : 0));
+        cell[i] = pack_cell(m->dg, (int)in->xi[i], (int)in->yi[i], (int)in->zi[i]);
+    }
+    const SpcDev& P = m->h_spc[sp];
+    double* dptr[] = { P.x, P.y, P.z, P.Sz, P.Bm, P.Cq, P.Nq, P.Pq, P.Chl, P.gen, P.age };
+    for (int q = 0; q < 11; ++q)
+        CK(cudaMemcpyAsync(dptr[q], dcols[q], C * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload individuals");
+    CK(cudaMemcpyAsync(P.flags, flags.data(), C, cudaMemcpyHostToDevice, m->stream), "upload flags");
+    CK(cudaMemcpyAsync(P.cell, cell.data(), C * sizeof(int32_t), cudaMemcpyHostToDevice, m->stream), "upload cells");
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    return PI_OK;
+}
+
+pi_status pi_get_individuals(pi_model* m, int32_t sp, pi_individuals* out) {
+    if (!m || !out || sp < 0 || sp >= m->nsp) return fail(m, PI_ERR_ARG, "pi_get_individuals: bad argument");
+    const long long C = m->C;
+    const SpcDev& P = m->h_spc[sp];
+    double* hptr[] = { out->x, out->y, out->z, out->Sz, out->Bm, out->Cq, out->Nq, out->Pq, out->Chl, out->gen, out->age };
+    const double* dptr[] = { P.x, P.y, P.z, P.Sz, P.Bm, P.Cq, P.Nq, P.Pq, P.Chl, P.gen, P.age };
+    for (int q = 0; q < 11; ++q)
+        if (hptr[q]) CK(cudaMemcpyAsync(hptr[q], dptr[q], C * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download individuals");
+    std::vector<uint8_t> flags(C);
+    std::vector<int32_t> cell(C);
+    CK(cudaMemcpyAsync(flags.data(), P.flags, C, cudaMemcpyDeviceToHost, m->stream), "download flags");
+    CK(cudaMemcpyAsync(cell.data(), P.cell, C * sizeof(int32_t), cudaMemcpyDeviceToHost, m->stream), "download cells");
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    for (long long i = 0; i < C; ++i) {
+        uint8_t f = flags[i];
+        if (out->ac) out->ac[i] = (f & FL_AC) ? 1 : 0;
+        if (out->graz) out->graz[i] = (f & FL_GRAZ) ? 1.0 : 0.0;
+        if (out->mort) out->mort[i] = (f & FL_MORT) ? 1.0 : 0.0;
+        if (out->dvid) out->dvid[i] = (f & FL_DVID) ? 1.0 : 0.0;
+        int xi, yi, zi;
+        unpack_cell(m->dg, cell[i], xi, yi, zi);
+        if (out->xi) out->xi[i] = xi;
+        if (out->yi) out->yi[i] = yi;
+        if (out->zi) out->zi[i] = zi;
+    }
+    return PI_OK;
+}
+
+pi_status pi_set_tracer(pi_model* m, int32_t idx, const double* data) {
+    if (!m || !data || idx < 0 || idx >= PI_NTRACERS) return fail(m, PI_ERR_ARG, "pi_set_tracer: bad argument");
+    CK(cudaMemcpyAsync(m->tr + (size_t)idx * m->hg.G, data, m->hg.G * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload tracer");
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    return PI_OK;
+}
+
+pi_status pi_get_tracer(pi_model* m, int32_t idx, double* out) {
+    if (!m || !out || idx < 0 || idx >= PI_NTRACERS) return fail(m, PI_ERR_ARG, "pi_get_tracer: bad argument");
+    CK(cudaMemcpyAsync(out, m->tr + (size_t)idx * m->hg.G, m->hg.G * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download tracer");
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    return PI_OK;
+}
+
+pi_status pi_set_velocity(pi_model* m, const double* u, const double* v, const double* w) {
+    if (!m || !u || !v || !w) return fail(m, PI_ERR_ARG, "pi_set_velocity: NULL argument");
+    std::vector<double> U, V, W;
+    host_vel_copy(m->hg, u, v, w, U, V, W);
+    // write into the own buffer that vel₀ does not alias
+    int b = (m->vel0[0] == m->velbuf[0][0]) ? 1 : 0;
+    const size_t bytes = m->hg.G * sizeof(double);
+    CK(cudaMemcpyAsync(m->velbuf[b][0], U.data(), bytes, cudaMemcpyHostToDevice, m->stream), "upload u");
+    CK(cudaMemcpyAsync(m->velbuf[b][1], V.data(), bytes, cudaMemcpyHostToDevice, m->stream), "upload v");
+    CK(cudaMemcpyAsync(m->velbuf[b][2], W.data(), bytes, cudaMemcpyHostToDevice, m->stream), "upload w");
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    for (int c = 0; c < 3; ++c) m->vel1[c] = m->velbuf[b][c];
+    m->vel1_buf = b;
+    return PI_OK;
+}
+
+pi_status pi_set_PARF(pi_model* m, const double* parf) {
+    if (!m || !parf) return fail(m, PI_ERR_ARG, "pi_set_PARF: NULL argument");
+    CK(cudaMemcpyAsync(m->PARF, parf, (size_t)m->hg.Nx * m->hg.Ny * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload PARF");
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    return PI_OK;
+}
+
+pi_status pi_set_temp(pi_model* m, const double* temp) {
+    if (!m || !temp) return fail(m, PI_ERR_ARG, "pi_set_temp: NULL argument");
+    const HostGrid& g = m->hg;
+    std::vector<double> T(g.G, 0.0);
+    for (int k = 1; k <= g.Nz; ++k) for (int j = 1; j <= g.Ny; ++j) for (int i = 1; i <= g.Nx; ++i)
+        T[g.id(i + g.Hx, j + g.Hy, k + g.Hz)] = temp[(size_t)(i - 1) + (size_t)g.Nx * ((size_t)(j - 1) + (size_t)g.Ny * (size_t)(k - 1))];
+    CK(cudaMemcpyAsync(m->temp_own, T.data(), g.G * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload temp");
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    m->temp = m->temp_own;
+    return PI_OK;
+}
+
+pi_status pi_set_flux_bc(pi_model* m, int32_t tracer, int32_t face, int32_t kind, const double* values, int64_t nt) {
+    if (!m || tracer < 0 || tracer >= PI_NTRACERS || face < 0 || face > 5 || kind < 0 || kind > 3)
+        return fail(m, PI_ERR_ARG, "pi_set_flux_bc: bad argument");
+    const HostGrid& g = m->hg;
+    size_t n1 = face <= PI_EAST ? g.Ny : g.Nx, n2 = face <= PI_NORTH ? g.Nz : g.Ny;
+    size_t n = kind == PI_BC_CONST ? 1 : kind == PI_BC_ARRAY2D ? n1 * n2 : kind == PI_BC_ARRAY3D ? n1 * n2 * (size_t)std::max<int64_t>(nt, 0) : 0;
+    if (kind == PI_BC_ARRAY3D && nt < 1) return fail(m, PI_ERR_SHAPE, "BC: time-dependent flux needs nt >= 1");
+    if (n && !values) return fail(m, PI_ERR_ARG, "pi_set_flux_bc: NULL values");
+    DevBC& b = m->bcs[tracer][face];
+    if (b.v) { cudaFree(b.v); b.v = nullptr; }
+    b.kind = kind; b.nt = nt;
+    if (n) {
+        CK(cudaMalloc(&b.v, n * sizeof(double)), "bc values");
+        CK(cudaMemcpyAsync(b.v, values, n * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload bc");
+    }
+    return upload_bcs(m);
+}
+
+pi_status pi_time_step(pi_model* m, double dT) {
+    if (!m) return fail(m, PI_ERR_ARG, "pi_time_step: NULL model");
+    pi_status st = enqueue_step(m, dT);
+    if (st) return st;
+    return check_device_errors(m);
+}
+
+pi_status pi_synchronize(pi_model* m) {
+    if (!m) return fail(m, PI_ERR_ARG, "pi_synchronize: NULL model");
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    return check_device_errors(m);
+}
+
+pi_status pi_get_time(pi_model* m, int64_t* iteration, double* t) {
+    if (!m) return fail(m, PI_ERR_ARG, "pi_get_time: NULL model");
+    if (iteration) *iteration = m->iteration;
+    if (t) *t = m->t;
+    return PI_OK;
+}
+
+pi_status pi_set_time(pi_model* m, int64_t iteration, double t) {
+    if (!m) return fail(m, PI_ERR_ARG, "pi_set_time: NULL model");
+    m->iteration = iteration; m->t = t;
+    return PI_OK;
+}
+
+pi_status pi_count_active(pi_model* m, int32_t sp, int64_t* n) {
+    if (!m || !n || sp < 0 || sp >= m->nsp) return fail(m, PI_ERR_ARG, "pi_count_active: bad argument");
+    std::vector<uint8_t> flags(m->C);
+    CK(cudaMemcpyAsync(flags.data(), m->h_spc[sp].flags, m->C, cudaMemcpyDeviceToHost, m->stream), "download flags");
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    int64_t c = 0;
+    for (uint8_t f : flags) c += (f & FL_AC) ? 1 : 0;
+    *n = c;
+    return PI_OK;
+}
+
+pi_status pi_get_diag(pi_model* m, int32_t kind, int32_t sp, double* out) {
+    if (!m || !out) return fail(m, PI_ERR_ARG, "pi_get_diag: bad argument");
+    const long long G = m->hg.G;
+    const double* src = nullptr;
+    if (kind == PI_DIAG_PAR) src = m->diag_par;
+    else {
+        if (sp < 0 || sp >= m->nsp || kind < PI_DIAG_NUM || kind > PI_DIAG_DVID) return fail(m, PI_ERR_ARG, "pi_get_diag: bad kind/species");
+        src = m->diag_sp + ((size_t)sp * 4 + (kind - PI_DIAG_NUM)) * G;
+    }
+    CK(cudaMemcpyAsync(out, src, G * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download diag");
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    return PI_OK;
+}
+
+pi_status pi_reset_diags(pi_model* m) {
+    if (!m) return fail(m, PI_ERR_ARG, "pi_reset_diags: NULL model");
+    const long long G = m->hg.G;
+    CK(cudaMemsetAsync(m->diag_par, 0, G * sizeof(double), m->stream), "reset diags");
+    CK(cudaMemsetAsync(m->diag_sp, 0, 4 * m->nsp * G * sizeof(double), m->stream), "reset diags");
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    return PI_OK;
+}
+
+// ---- PlanktonSimulation / update! -------------------------------------------------------------
+
+pi_status pi_sim_create(pi_model* m, double dT, int64_t iterations,
+                        const double* u, const double* v, const double* w, int64_t nvel, double dT_vel,
+                        const double* parf, int64_t npar, double dT_PAR,
+                        const double* temp, int64_t ntemp, double dT_temp, pi_sim** out) {
+    if (!m || !out) return fail(m, PI_ERR_ARG, "pi_sim_create: NULL argument");
+    *out = nullptr;
+    if (!parf || !temp || npar < 1 || ntemp < 1 || iterations < 0)
+        return fail(m, PI_ERR_ARG, "pi_sim_create: PARF and temp series are required");
+    const HostGrid& g = m->hg;
+    int has_vel = (u != nullptr);
+    // validate_velocity / validate_PARF / validate_temp (Simulation/utils.jl:213-304)
+    if (has_vel) {
+        if (!v || !w || nvel < 1) return fail(m, PI_ERR_ARG, "pi_sim_create: u, v and w are required together");
+        if (std::floor(dT_vel / dT) * dT != dT_vel)
+            return fail(m, PI_ERR_SHAPE, "ΔT_vel must be an integer times of " + julia_float(dT) + ".");
+        if ((double)nvel < std::floor((double)iterations * dT / dT_vel))
+            return fail(m, PI_ERR_SHAPE, "Velocities provided cannot cover the time period of (iterations+1)*ΔT (" +
+                                          julia_float((double)iterations * dT) + " seconds) with ΔT_vel = " + julia_float(dT_vel) + ".");
+    }
+    if (std::floor(dT_PAR / dT) * dT != dT_PAR)
+        return fail(m, PI_ERR_SHAPE, "ΔT_PAR must be an integer times of " + julia_float(dT) + ".");
+    if ((double)npar < std::floor((double)iterations * dT / dT_PAR))
+        return fail(m, PI_ERR_SHAPE, "Surface PAR provided cannot cover the time period of (iterations+1)*ΔT (" +
+                                      julia_float((double)iterations * dT) + " seconds) with ΔT_PAR = " + julia_float(dT_PAR) + ".");
+    if (std::floor(dT_temp / dT) * dT != dT_temp)
+        return fail(m, PI_ERR_SHAPE, "ΔT_temp must be an integer times of " + julia_float(dT) + ".");
+    if ((double)ntemp < std::floor((double)iterations * dT / dT_temp))
+        return fail(m, PI_ERR_SHAPE, "Temperature provided cannot cover the time period of (iterations+1)*ΔT (" +
+                                      julia_float((double)iterations * dT) + " seconds) with ΔT_temp = " + julia_float(dT_temp) + ".");
+    pi_sim* s = new pi_sim();
+    s->m = m; s->dT = dT; s->iterations = iterations; s->has_vel = has_vel;
+    s->nvel = nvel; s->npar = npar; s->ntemp = ntemp; s->dT_vel = dT_vel; s->dT_PAR = dT_PAR; s->dT_temp = dT_temp;
+    auto cleanup = [&](pi_status st) { pi_sim_destroy(s); return st; };
+    const size_t bytes = g.G * sizeof(double);
+    if (has_vel) {
+        int ex = g.topo[0] == PI_BOUNDED, ey = g.topo[1] == PI_BOUNDED, ez = g.topo[2] == PI_BOUNDED;
+        size_t nu = (size_t)(g.Nx + ex) * g.Ny * g.Nz, nv = (size_t)g.Nx * (g.Ny + ey) * g.Nz, nw = (size_t)g.Nx * g.Ny * (g.Nz + ez);
+        std::vector<double> U, V, W;
+        for (int64_t t = 0; t < nvel; ++t) {
+            host_vel_copy(g, u + t * nu, v + t * nv, w + t * nw, U, V, W);
+            for (auto* hv : { &U, &V, &W }) {
+                double* d = nullptr;
+                if (cudaMalloc(&d, bytes) != cudaSuccess) return cleanup(fail(m, PI_ERR_NOMEM, "pi_sim_create: velocity series"));
+                s->vel.push_back(d);
+                if (cudaMemcpyAsync(d, hv->data(), bytes, cudaMemcpyHostToDevice, m->stream) != cudaSuccess)
+                    return cleanup(fail(m, PI_ERR_CUDA, "pi_sim_create: upload velocity"));
+                if (cudaStreamSynchronize(m->stream) != cudaSuccess) return cleanup(fail(m, PI_ERR_CUDA, "pi_sim_create: synchronize"));
+            }
+        }
+    }
+    size_t nf = (size_t)g.Nx * g.Ny;
+    if (cudaMalloc(&s->parf, nf * npar * sizeof(double)) != cudaSuccess) return cleanup(fail(m, PI_ERR_NOMEM, "pi_sim_create: PARF series"));
+    if (cudaMemcpyAsync(s->parf, parf, nf * npar * sizeof(double), cudaMemcpyHostToDevice, m->stream) != cudaSuccess)
+        return cleanup(fail(m, PI_ERR_CUDA, "pi_sim_create: upload PARF"));
+    std::vector<double> T(g.G, 0.0);
+    size_t nt = (size_t)g.Nx * g.Ny * g.Nz;
+    for (int64_t q = 0; q < ntemp; ++q) {
+        const double* src = temp + q * nt;
+        for (int k = 1; k <= g.Nz; ++k) for (int j = 1; j <= g.Ny; ++j) for (int i = 1; i <= g.Nx; ++i)
+            T[g.id(i + g.Hx, j + g.Hy, k + g.Hz)] = src[(size_t)(i - 1) + (size_t)g.Nx * ((size_t)(j - 1) + (size_t)g.Ny * (size_t)(k - 1))];
+        double* d = nullptr;
+        if (cudaMalloc(&d, bytes) != cudaSuccess) return cleanup(fail(m, PI_ERR_NOMEM, "pi_sim_create: temperature series"));
+        s->temp.push_back(d);
+        if (cudaMemcpyAsync(d, T.data(), bytes, cudaMemcpyHostToDevice, m->stream) != cudaSuccess)
+            return cleanup(fail(m, PI_ERR_CUDA, "pi_sim_create: upload temperature"));
+        if (cudaStreamSynchronize(m->stream) != cudaSuccess) return cleanup(fail(m, PI_ERR_CUDA, "pi_sim_create: synchronize"));
+    }
+    *out = s;
+    return PI_OK;
+}
+
+pi_status pi_sim_update(pi_sim* s, int32_t time_offset, int32_t sync) {
+    if (!s || !s->m) return PI_ERR_ARG;
+    pi_model* m = s->m;
+    const HostGrid& g = m->hg;
+    const size_t nf = (size_t)g.Nx * g.Ny;
+    for (int64_t i = 1; i <= s->iterations; ++i) {
+        double tv = (time_offset & 1) ? (double)(i - 1) * s->dT : m->t;
+        double tp = (time_offset & 2) ? (double)(i - 1) * s->dT : m->t;
+        double tt = (time_offset & 4) ? (double)(i - 1) * s->dT : m->t;
+        if (s->has_vel) {
+            int64_t t_vel = (int64_t)std::floor(tv / s->dT_vel) + 1;
+            if (t_vel < 1 || t_vel > s->nvel) return fail(m, PI_ERR_SHAPE, "BoundsError: velocity snapshot " + std::to_string(t_vel) + " not provided");
+            for (int c = 0; c < 3; ++c) m->vel1[c] = s->vel[(size_t)(t_vel - 1) * 3 + c];
+            m->vel1_buf = -1;
+        }
+        int64_t t_par = (int64_t)std::floor(tp / s->dT_PAR) + 1;
+        if (t_par < 1 || t_par > s->npar) return fail(m, PI_ERR_SHAPE, "BoundsError: PARF snapshot " + std::to_string(t_par) + " not provided");
+        CK(cudaMemcpyAsync(m->PARF, s->parf + (size_t)(t_par - 1) * nf, nf * sizeof(double), cudaMemcpyDeviceToDevice, m->stream), "PARF copy");
+        int64_t t_temp = (int64_t)std::floor(tt / s->dT_temp) + 1;
+        if (t_temp < 1 || t_temp > s->ntemp) return fail(m, PI_ERR_SHAPE, "BoundsError: temperature snapshot " + std::to_string(t_temp) + " not provided");
+        m->temp = s->temp[(size_t)(t_temp - 1)];
+        pi_status st = enqueue_step(m, s->dT);
+        if (st) return st;
+    }
+    if (sync) return pi_synchronize(m);
+    return PI_OK;
+}
+
+pi_status pi_sim_destroy(pi_sim* s) {
+    if (!s) return PI_OK;
+    pi_model* m = s->m;
+    if (m) {
+        cudaStreamSynchronize(m->stream);
+        // the model must not keep pointers into the series
+        bool bound = false;
+        for (double* d : s->vel) for (int c = 0; c < 3; ++c) if (m->vel1[c] == d || m->vel0[c] == d) bound = true;
+        if (bound) {
+            // copy the bound snapshot into own buffers so the model stays usable
+            for (int c = 0; c < 3; ++c) {
+                int b = 0;
+                cudaMemcpyAsync(m->velbuf[b][c], m->vel1[c], m->hg.G * sizeof(double), cudaMemcpyDeviceToDevice, m->stream);
+                m->vel1[c] = m->velbuf[b][c];
+                m->vel0[c] = m->velbuf[b][c];
+            }
+            m->vel1_buf = 0;
+        }
+        for (double* d : s->temp) if (m->temp == d) {
+            cudaMemcpyAsync(m->temp_own, d, m->hg.G * sizeof(double), cudaMemcpyDeviceToDevice, m->stream);
+            m->temp = m->temp_own;
+        }
+        cudaStreamSynchronize(m->stream);
+    }
+    for (double* d : s->vel) cudaFree(d);
+    for (double* d : s->temp) cudaFree(d);
+    if (s->parf) cudaFree(s->parf);
+    delete s;
+    return PI_OK;
+}
+
+}  // extern "C"
