@@ -190,6 +190,18 @@ pi_status pi_sim_destroy(pi_sim* s);
  * (capacity overflow, index out of domain) raised since the last call. */
 pi_status pi_synchronize(pi_model* m);
 
+/* The CUDA stream (cudaStream_t) the handle launches on, for callers that record events or order
+ * their own work against the model's. */
+pi_status pi_get_stream(pi_model* m, void** stream);
+
+/* Per-kernel device timing. While enabled, every kernel launch of a step is bracketed by CUDA
+ * events on the model's stream; pi_profile_read synchronises and returns, for up to `max`
+ * kernels, the name (NUL-separated in `names`, `names_len` bytes), the number of launches and
+ * the summed milliseconds since profiling was enabled. `*n` receives the number of kernels. */
+pi_status pi_profile_enable(pi_model* m, int32_t on);
+pi_status pi_profile_read(pi_model* m, int32_t max, char* names, size_t names_len,
+                          int64_t* launches, double* ms, int32_t* n);
+
 /* Message of the last error of the handle (or of the last failed pi_create when m is NULL). */
 pi_status pi_last_error(pi_model* m, char* buf, size_t len);
 

@@ -118,8 +118,8 @@ namespace {
 
 /* Clamp a 1-based index into [lo, hi], recording an out-of-domain access. */
 inline long clampi(orc_model* m, long v, long lo, long hi) {
-    if (v < lo) { m->err_flags |= ERR_DOMAIN; return lo; }
-    if (v > hi) { m->err_flags |= ERR_DOMAIN; return hi; }
+    if (v < lo) { __atomic_or_fetch(&m->err_flags, ERR_DOMAIN, __ATOMIC_RELAXED); return lo; }
+    if (v > hi) { __atomic_or_fetch(&m->err_flags, ERR_DOMAIN, __ATOMIC_RELAXED); return hi; }
     return v;
 }
 
@@ -246,6 +246,7 @@ double itpl(orc_model* m, const dvec& f, int comp, double x, double y, double z,
 void vel_interpolate(orc_model* m, Species& s, const dvec& X, const dvec& Y, const dvec& Z,
                      const dvec& U, const dvec& V, const dvec& W) {
     int64_t C = m->C;
+    #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < C; ++i) {
         int ac = s.ac[i];
         m->vu1[i] = jl_mulb(itpl(m, U, 0, X[i], Y[i], Z[i], ac), ac);
@@ -322,12 +323,14 @@ void particle_diffusion(orc_model* m, Species& s, int spi, double dT) {
     const Grid& g = m->g;
     int64_t C = m->C;
     double kx = m->bgc.kappa_hP, ky = m->bgc.kappa_hP, kz = m->bgc.kappa_vP;
+    #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < C; ++i)
         pi_draw3(m->seed, (uint32_t)m->iteration, (uint32_t)spi, PI_DRAW_DIFFUSION, (uint32_t)i,
                  &m->rx[i], &m->ry[i], &m->rz[i]);
     for (int64_t i = 0; i < C; ++i) {
         m->rx[i] = (m->rx[i] - 0.5) * 2.0; m->ry[i] = (m->ry[i] - 0.5) * 2.0; m->rz[i] = (m->rz[i] - 0.5) * 2.0;
     }
+    #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < C; ++i) {   /* calc_diffusion_kernel!, :2-8; ΔzC at zi+Hz of the stored zi */
         long kk = clampi(m, (long)s.zi[i] + g.Hz, 1, g.Gz);
         m->rx[i] = m->rx[i] * sqrt(kx * dT) / g.dx;
@@ -349,6 +352,7 @@ void particle_diffusion(orc_model* m, Species& s, int spi, double dT) {
 
 void find_inds(orc_model* m, Species& s) {     /* utils.jl:2-7 */
     const Grid& g = m->g;
+    #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < m->C; ++i) {
         int ac = s.ac[i];
         s.xi[i] = clampi(m, (long)jl_trunc(jl_mulb(s.x[i] + 1.0, ac)) + g.Hx, 1, g.Gx);
@@ -374,6 +378,7 @@ void acc_counts(orc_model* m, Species& s) {    /* utils.jl:44-47 */
 
 void calc_par(orc_model* m, int ki) {          /* utils.jl:55-63 */
     const Grid& g = m->g;
+    #pragma omp parallel for schedule(static)
     for (int j = 1; j <= g.Ny; ++j)
         for (int i = 1; i <= g.Nx; ++i) {
             long ii = i + g.Hx, jj = j + g.Hy, kk = ki + g.Hz;
@@ -386,6 +391,7 @@ void calc_par(orc_model* m, int ki) {          /* utils.jl:55-63 */
 }
 
 void find_NPT(orc_model* m, Species& s) {      /* utils.jl:14-25 */
+    #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < m->C; ++i) {
         size_t c = cell_of(m, s, i);
         int ac = s.ac[i];
@@ -515,6 +521,7 @@ void plankton_growth(orc_model* m, Species& s, int spi, double dT, double t) {
         }
     }
     /* get_probability!, division_death_probability.jl:95-107 */
+    #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < C; ++i) {
         double r0, r1, r2;
         pi_draw3(m->seed, (uint32_t)m->iteration, (uint32_t)spi, PI_DRAW_DECISION, (uint32_t)i, &r0, &r1, &r2);
@@ -678,10 +685,10 @@ void tracer_advection(orc_model* m, double dT) {
     for (int n = 0; n < PI_NTRACERS; ++n) m->tt[n] = m->tr[n];
     for (int dir = 0; dir < 3; ++dir) {
         const dvec& vel = dir == 0 ? m->u1 : dir == 1 ? m->v1 : m->w1;
-        #pragma omp parallel for schedule(static)
         for (int n = 0; n < PI_NTRACERS; ++n) {
             dvec& Gc = m->Gcs[n];
             const dvec& cT = m->tt[n];
+            #pragma omp parallel for schedule(static)
             for (long k = g.Hz + 1; k <= g.Hz + g.Nz; ++k)       /* calc_Gcˣ/ʸ/ᶻ_kernel! */
                 for (long j = g.Hy + 1; j <= g.Hy + g.Ny; ++j)
                     for (long i = g.Hx + 1; i <= g.Hx + g.Nx; ++i)
@@ -690,11 +697,11 @@ void tracer_advection(orc_model* m, double dT) {
                                                      : adv_flux_z(g, o, i, j, k, vel, cT, dT);
         }
         for (int n = 0; n < PI_NTRACERS; ++n) fill_halo_Gc(g, m->Gcs[n]);
-        #pragma omp parallel for schedule(static)
         for (int n = 0; n < PI_NTRACERS; ++n) {                    /* multi_dim_x/y/z_kernel! */
             dvec& ct = m->tt[n];
             const dvec& Gc = m->Gcs[n];
             const dvec& c = m->tr[n];
+            #pragma omp parallel for schedule(static)
             for (long k = g.Hz + 1; k <= g.Hz + g.Nz; ++k)
                 for (long j = g.Hy + 1; j <= g.Hy + g.Ny; ++j)
                     for (long i = g.Hx + 1; i <= g.Hx + g.Nx; ++i) {
@@ -716,8 +723,10 @@ void tracer_advection(orc_model* m, double dT) {
         }
         for (int n = 0; n < PI_NTRACERS; ++n) fill_halo_tracer(g, m->tt[n]);
     }
-    for (int n = 0; n < PI_NTRACERS; ++n)                          /* calc_tracer_tendency! */
+    for (int n = 0; n < PI_NTRACERS; ++n) {                        /* calc_tracer_tendency! */
+        #pragma omp parallel for schedule(static)
         for (size_t q = 0; q < g.G; ++q) m->Gcs[n][q] = m->tt[n][q] - m->tr[n][q];
+    }
 }
 
 /* tracer_diffusion!, Advection/tracer_diffusion.jl:1-30 */
@@ -847,8 +856,8 @@ void apply_bcs(orc_model* m, double dT) {
 /* apply_tendency!, tracer_update.jl:6-13 */
 void apply_tendency(orc_model* m) {
     const Grid& g = m->g;
-    #pragma omp parallel for schedule(static)
     for (int n = 0; n < PI_NTRACERS; ++n)
+        #pragma omp parallel for schedule(static)
         for (long k = g.Hz + 1; k <= g.Hz + g.Nz; ++k)
             for (long j = g.Hy + 1; j <= g.Hy + g.Ny; ++j)
                 for (long i = g.Hx + 1; i <= g.Hx + g.Nx; ++i) {
@@ -1039,6 +1048,7 @@ int orc_time_step(orc_model* m, double dT) {
     const Grid& g = m->g;
     m->iteration = m->iteration + 1;
     m->t = (double)m->iteration * dT;
+    #pragma omp parallel for schedule(static)
     for (size_t q = 0; q < g.G; ++q) {                                           /* :17-19 */
         m->uh[q] = (m->u0[q] + m->u1[q]) * 0.5;
         m->vh[q] = (m->v0[q] + m->v1[q]) * 0.5;

@@ -34,6 +34,13 @@ def load():
     lib.pi_synchronize.argtypes = [P]
     lib.pi_reset_diags.restype = ct.c_int32
     lib.pi_reset_diags.argtypes = [P]
+    lib.pi_get_stream.restype = ct.c_int32
+    lib.pi_get_stream.argtypes = [P, ct.POINTER(ct.c_void_p)]
+    lib.pi_profile_enable.restype = ct.c_int32
+    lib.pi_profile_enable.argtypes = [P, ct.c_int32]
+    lib.pi_profile_read.restype = ct.c_int32
+    lib.pi_profile_read.argtypes = [P, ct.c_int32, ct.c_char_p, ct.c_size_t, ct.POINTER(ct.c_int64),
+                                    dp, ct.POINTER(ct.c_int32)]
     lib.pi_status_string.restype = ct.c_char_p
     lib.pi_status_string.argtypes = [ct.c_int32]
     _lib = lib
@@ -45,4 +52,4 @@ EXPORTS = ("pi_create", "pi_destroy", "pi_set_individuals", "pi_get_individuals"
            "pi_get_tracer", "pi_set_velocity", "pi_set_PARF", "pi_set_temp", "pi_set_flux_bc",
            "pi_time_step", "pi_get_time", "pi_set_time", "pi_count_active", "pi_get_diag",
            "pi_reset_diags", "pi_sim_create", "pi_sim_update", "pi_sim_destroy", "pi_synchronize",
-           "pi_last_error", "pi_status_string")
+           "pi_last_error", "pi_status_string", "pi_get_stream", "pi_profile_enable", "pi_profile_read")

@@ -828,6 +828,61 @@ __global__ void k_halo(DGrid g, double* __restrict__ f, int nfields, const uint3
     }
 }
 
+// Interior array (reference layout nx×ny×nz, x fastest) into a halo-padded field at offset
+// (Hx, Hy, Hz): copy_interior! / copy_interior_u! (Simulation/utils.jl:13-34).
+__global__ void k_scatter_interior(DGrid g, double* __restrict__ dst, const double* __restrict__ src,
+                                   int nx, int ny, int nz) {
+    long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long n = (long long)nx * ny * nz;
+    if (q >= n) return;
+    int i = (int)(q % nx);
+    long long r = q / nx;
+    int j = (int)(r % ny);
+    int k = (int)(r / ny);
+    dst[gidx(g, i + 1 + g.Hx, j + 1 + g.Hy, k + 1 + g.Hz)] = src[q];
+}
+
+// Velocity halo rule along one axis (fill_halo_u/v/w!, halo_regions.jl:64-99) when the field is a
+// face field on that axis and the axis is Bounded: the high halo copies the extra face N+H+1.
+// Otherwise the tracer rule. One thread per line; sources are read before writes.
+template <int AXIS>
+__global__ void k_halo_vel(DGrid g, double* __restrict__ c, int face_axis) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    int b = blockIdx.y + 1;
+    int na = AXIS == 0 ? g.Gy : g.Gx;
+    if (a > na) return;
+    int N = AXIS == 0 ? g.Nx : AXIS == 1 ? g.Ny : g.Nz;
+    int H = AXIS == 0 ? g.Hx : AXIS == 1 ? g.Hy : g.Hz;
+    int topo = AXIS == 0 ? g.tx : AXIS == 1 ? g.ty : g.tz;
+    auto at = [&](int t) -> double& {
+        if (AXIS == 0) return c[gidx(g, t, a, b)];
+        if (AXIS == 1) return c[gidx(g, a, t, b)];
+        return c[gidx(g, a, b, t)];
+    };
+    double wv[8], ev[8];
+    int velrule = (face_axis == AXIS) && topo == PI_BOUNDED;
+    for (int h = 1; h <= H; ++h) {
+        wv[h - 1] = topo == PI_PERIODIC ? at(N + h) : at(H + 1);
+        ev[h - 1] = topo == PI_PERIODIC ? at(H + h) : at(N + H);
+    }
+    double face = velrule ? at(N + H + 1) : 0.0;
+    for (int h = 1; h <= H; ++h) at(h) = wv[h - 1];
+    if (velrule) {
+        for (int h = N + H + 2; h <= N + 2 * H; ++h) at(h) = face;
+    } else {
+        for (int h = 1; h <= H; ++h) at(N + H + h) = ev[h - 1];
+    }
+}
+
+// Active individuals of one species (calc_active_individuals, models.jl:157-164).
+__global__ void k_count_active(const uint8_t* __restrict__ flags, long long C, unsigned long long* out) {
+    unsigned long long n = 0;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < C; q += (long long)gridDim.x * blockDim.x)
+        n += (flags[q] & FL_AC) ? 1 : 0;
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_down_sync(0xffffffffu, n, o);
+    if ((threadIdx.x & 31) == 0 && n) atomicAdd(out, n);
+}
+
 // After a capacity error the step stops where the reference throws: the tracers keep their
 // values, so the buffer that becomes current is a copy of the old one.
 __global__ void k_copy_if_err(double* __restrict__ dst, const double* __restrict__ src, long long n,

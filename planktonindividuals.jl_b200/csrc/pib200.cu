@@ -154,6 +154,7 @@ struct pi_model {
     double* par = nullptr;       // G
     double* PARF = nullptr;      // Nx·Ny
     double* temp_own = nullptr;  // G
+    double* stage = nullptr;     // 3 × G staging for interior uploads
     const double* temp = nullptr;
     double* diag_par = nullptr;  // G
     double* diag_sp = nullptr;   // nsp × 4 × G (num, graz, mort, dvid)
@@ -168,6 +169,14 @@ struct pi_model {
     DevBC bcs[PI_NTRACERS][6];
     FluxBCDev* d_bcs = nullptr;
     int any_bc = 0;
+    // optional per-kernel event timing
+    int profiling = 0;
+    struct Mark { const char* name; cudaEvent_t a, b; };
+    std::vector<Mark> marks;            // recorded, not yet read
+    std::vector<cudaEvent_t> event_pool;
+    std::vector<std::string> prof_names;
+    std::vector<int64_t> prof_count;
+    std::vector<double> prof_ms;
 };
 
 struct pi_sim {
@@ -222,6 +231,45 @@ void free_all(pi_model* m) {
 
 inline unsigned nblk(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
+cudaEvent_t take_event(pi_model* m) {
+    if (!m->event_pool.empty()) { cudaEvent_t e = m->event_pool.back(); m->event_pool.pop_back(); return e; }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Brackets one kernel launch (or library call) with events when profiling is on.
+struct ProfScope {
+    pi_model* m;
+    pi_model::Mark mk;
+    ProfScope(pi_model* m_, const char* name) : m(m_) {
+        if (!m->profiling) return;
+        mk.name = name; mk.a = take_event(m); mk.b = take_event(m);
+        cudaEventRecord(mk.a, m->stream);
+    }
+    ~ProfScope() {
+        if (!m->profiling) return;
+        cudaEventRecord(mk.b, m->stream);
+        m->marks.push_back(mk);
+    }
+};
+
+void drain_marks(pi_model* m) {
+    for (auto& mk : m->marks) {
+        float ms = 0.f;
+        cudaEventSynchronize(mk.b);
+        cudaEventElapsedTime(&ms, mk.a, mk.b);
+        size_t q = 0;
+        while (q < m->prof_names.size() && m->prof_names[q] != mk.name) ++q;
+        if (q == m->prof_names.size()) { m->prof_names.push_back(mk.name); m->prof_count.push_back(0); m->prof_ms.push_back(0.0); }
+        m->prof_count[q] += 1;
+        m->prof_ms[q] += ms;
+        m->event_pool.push_back(mk.a);
+        m->event_pool.push_back(mk.b);
+    }
+    m->marks.clear();
+}
+
 // Reads and clears the device error word; converts it to a status.
 pi_status check_device_errors(pi_model* m) {
     uint32_t err = 0;
@@ -254,19 +302,24 @@ pi_status enqueue_step(pi_model* m, double dT) {
 
     CK(cudaMemsetAsync(sb.cnt, 0, (G + 1) * sizeof(uint32_t), st), "zero counts");
     VelPtrs vp{m->vel0[0], m->vel0[1], m->vel0[2], m->vel1[0], m->vel1[1], m->vel1[2]};
+    { ProfScope ps_(m, "k_particles");
     k_particles<<<nblk(NC, BS), BS, 0, st>>>(g, m->d_spc, m->nsp, C, dT, m->seed, iter, vp,
                                              m->bgc.kappa_hP, m->bgc.kappa_vP, sb.cnt, sb.key,
                                              (uint32_t)G, sb.err);
-    CK(cudaGetLastError(), "k_particles");
+    CK(cudaGetLastError(), "k_particles"); }
     size_t tb = m->cub_bytes;
-    CK(cub::DeviceScan::ExclusiveSum(m->cub_tmp, tb, sb.cnt, sb.off, (int)(G + 1), st), "scan counts");
+    { ProfScope ps_(m, "cub_scan_cells");
+    CK(cub::DeviceScan::ExclusiveSum(m->cub_tmp, tb, sb.cnt, sb.off, (int)(G + 1), st), "scan counts"); }
     tb = m->cub_bytes;
+    { ProfScope ps_(m, "cub_sort_cells");
     CK(cub::DeviceRadixSort::SortPairs(m->cub_tmp, tb, sb.key, sb.key_sorted, m->iota, sb.gid_sorted,
-                                       (int64_t)NC, 0, m->key_bits, st), "sort by cell");
+                                       (int64_t)NC, 0, m->key_bits, st), "sort by cell"); }
+    { ProfScope ps_(m, "k_setpos");
     k_setpos<<<nblk(NC, BS), BS, 0, st>>>(sb.off, G, sb.gid_sorted, sb.pos, NC, sb.err);
-    CK(cudaGetLastError(), "k_setpos");
+    CK(cudaGetLastError(), "k_setpos"); }
     {
         dim3 grid(nblk(g.Nx, 128), g.Ny);
+        ProfScope ps_(m, "k_par");
         k_par<<<grid, 128, 0, st>>>(g, m->d_spc, C, sb.off, sb.gid_sorted, m->PARF, m->PARF, m->par,
                                     m->diag_par, m->bgc.kc, m->bgc.kw, sb.err);
         CK(cudaGetLastError(), "k_par");
@@ -274,30 +327,37 @@ pi_status enqueue_step(pi_model* m, double dT) {
     const int shared = m->bgc.shared_graz == 1.0;
     for (int s = 0; s < m->nsp; ++s) {
         double* dsp = m->diag_sp + (size_t)s * 4 * G;
+        { ProfScope ps_(m, "k_decide");
         k_decide<<<nblk(C, BS), BS, 0, st>>>(g, m->h_spc[s], m->sp[s], C, s, sb.pos, sb.loss, sb.evk,
                                              sb.flag64, dsp + 1 * G, dsp + 2 * G, dsp + 3 * G, sb.err);
-        CK(cudaGetLastError(), "k_decide");
+        CK(cudaGetLastError(), "k_decide"); }
         tb = m->cub_bytes;
-        CK(cub::DeviceScan::ExclusiveSum(m->cub_tmp, tb, sb.flag64, sb.rank64, (int64_t)C, st), "scan division flags");
+        { ProfScope ps_(m, "cub_scan_slots");
+        CK(cub::DeviceScan::ExclusiveSum(m->cub_tmp, tb, sb.flag64, sb.rank64, (int64_t)C, st), "scan division flags"); }
+        { ProfScope ps_(m, "k_lists");
         k_lists<<<nblk(C, BS), BS, 0, st>>>(sb.flag64, sb.rank64, C, sb.divlist, sb.freelist, sb.ndiv,
                                             sb.err, sb.err_iter, m->iteration);
-        CK(cudaGetLastError(), "k_lists");
+        CK(cudaGetLastError(), "k_lists"); }
+        { ProfScope ps_(m, "k_daughters");
         k_daughters<<<148 * 4, 256, 0, st>>>(m->h_spc[s], sb.divlist, sb.freelist, sb.ndiv, sb.err);
-        CK(cudaGetLastError(), "k_daughters");
+        CK(cudaGetLastError(), "k_daughters"); }
         const double* trp = m->tr;
+        { ProfScope ps_(m, "k_physiology");
         k_physiology<<<nblk(C, BS), BS, 0, st>>>(g, m->h_spc[s], m->sp[s], C, s, dT, m->t, m->seed, iter,
                                                  shared, trp + PI_NH4 * G, trp + PI_NO3 * G,
                                                  trp + PI_PO4 * G, trp + PI_DOC * G, m->par, m->temp,
                                                  sb.off, sb.gid_sorted, sb.pos, sb.contrib,
                                                  dsp + 0 * G, sb.err);
-        CK(cudaGetLastError(), "k_physiology");
+        CK(cudaGetLastError(), "k_physiology"); }
     }
     {
         dim3 grid(nblk(g.Nx, 128), g.Ny, g.Nz);
+        { ProfScope ps_(m, "k_sweep_x");
         k_sweep_x<<<grid, 128, 0, st>>>(g, m->tr, m->tta, m->vel1[0], dT, sb.err);
-        CK(cudaGetLastError(), "k_sweep_x");
+        CK(cudaGetLastError(), "k_sweep_x"); }
+        { ProfScope ps_(m, "k_sweep_y");
         k_sweep_y<<<grid, 128, 0, st>>>(g, m->tr, m->tta, m->ttb, m->vel1[1], dT, sb.err);
-        CK(cudaGetLastError(), "k_sweep_y");
+        CK(cudaGetLastError(), "k_sweep_y"); }
         ZFinalArgs za;
         za.g = g; za.tr = m->tr; za.ttb = m->ttb; za.tr_next = m->tr_next; za.w = m->vel1[2];
         za.dT = dT; za.b = m->bgc;
@@ -306,13 +366,15 @@ pi_status enqueue_step(pi_model* m, double dT) {
         za.spc = m->d_spc; za.C = C; za.off = sb.off; za.gid_sorted = sb.gid_sorted; za.evk = sb.evk;
         za.loss = sb.loss; za.contrib = sb.contrib; za.nsp = m->nsp; za.err = sb.err;
         dim3 g2(nblk(g.Nx, 64), g.Ny);
+        { ProfScope ps_(m, "k_sweep_z_final");
         k_sweep_z_final<<<g2, 64, 0, st>>>(za);
-        CK(cudaGetLastError(), "k_sweep_z_final");
+        CK(cudaGetLastError(), "k_sweep_z_final"); }
         // tracers are only replaced when the step completed (a capacity error leaves them)
+        { ProfScope ps_(m, "k_halo");
         k_halo<0><<<dim3(nblk(g.Gy, 64), g.Gz, PI_NTRACERS), 64, 0, st>>>(g, m->tr_next, PI_NTRACERS, sb.err);
         k_halo<1><<<dim3(nblk(g.Gx, 64), g.Gz, PI_NTRACERS), 64, 0, st>>>(g, m->tr_next, PI_NTRACERS, sb.err);
         k_halo<2><<<dim3(nblk(g.Gx, 64), g.Gy, PI_NTRACERS), 64, 0, st>>>(g, m->tr_next, PI_NTRACERS, sb.err);
-        CK(cudaGetLastError(), "k_halo");
+        CK(cudaGetLastError(), "k_halo"); }
         k_copy_if_err<<<148 * 4, 256, 0, st>>>(m->tr_next, m->tr, PI_NTRACERS * G, sb.err);
         CK(cudaGetLastError(), "k_copy_if_err");
     }
@@ -441,6 +503,7 @@ pi_status pi_create(const pi_grid* grid, const pi_bgc_params* bgc, const pi_quot
     ALB(m->tr, PI_NTRACERS * G); ALB(m->tr_next, PI_NTRACERS * G);
     ALB(m->tta, PI_NTRACERS * G); ALB(m->ttb, PI_NTRACERS * G);
     for (int b = 0; b < 2; ++b) for (int c = 0; c < 3; ++c) ALB(m->velbuf[b][c], G);
+    ALB(m->stage, 3 * G);
     ALB(m->zeros, G); ALB(m->par, G); ALB(m->PARF, (long long)hg.Nx * hg.Ny); ALB(m->temp_own, G);
     ALB(m->diag_par, G); ALB(m->diag_sp, 4LL * nspecies * G);
     StepBufs& sb = m->sb;
@@ -516,6 +579,8 @@ pi_status pi_create(const pi_grid* grid, const pi_bgc_params* bgc, const pi_quot
 pi_status pi_destroy(pi_model* m) {
     if (!m) return PI_OK;
     cudaStreamSynchronize(m->stream);
+    drain_marks(m);
+    for (cudaEvent_t e : m->event_pool) cudaEventDestroy(e);
     free_all(m);
     cudaStreamDestroy(m->stream);
     delete m;
@@ -595,16 +660,47 @@ pi_status pi_get_tracer(pi_model* m, int32_t idx, double* out) {
     return PI_OK;
 }
 
+// vel_copy! on the device: interior arrays go to staging, then scatter + halo fill there. When an
+// axis has fewer cells than halo points the reference's aliased halo copy reads stale values, so
+// that case keeps the exact host-side fill.
+static pi_status device_vel_copy(pi_model* m, const double* u, const double* v, const double* w,
+                                 double* U, double* V, double* W) {
+    const HostGrid& g = m->hg;
+    const DGrid& dg = m->dg;
+    cudaStream_t st = m->stream;
+    int b[3] = { g.topo[0] == PI_BOUNDED, g.topo[1] == PI_BOUNDED, g.topo[2] == PI_BOUNDED };
+    int dims[3][3] = { { g.Nx + b[0], g.Ny, g.Nz }, { g.Nx, g.Ny + b[1], g.Nz }, { g.Nx, g.Ny, g.Nz + b[2] } };
+    const double* src[3] = { u, v, w };
+    double* dst[3] = { U, V, W };
+    for (int c = 0; c < 3; ++c) {
+        size_t n = (size_t)dims[c][0] * dims[c][1] * dims[c][2];
+        double* sg = m->stage + (size_t)c * g.G;
+        CK(cudaMemcpyAsync(sg, src[c], n * sizeof(double), cudaMemcpyDefault, st), "upload velocity");
+        k_scatter_interior<<<nblk((long long)n, 256), 256, 0, st>>>(dg, dst[c], sg, dims[c][0], dims[c][1], dims[c][2]);
+        k_halo_vel<0><<<dim3(nblk(g.Gy, 64), g.Gz), 64, 0, st>>>(dg, dst[c], c);
+        k_halo_vel<1><<<dim3(nblk(g.Gx, 64), g.Gz), 64, 0, st>>>(dg, dst[c], c);
+        k_halo_vel<2><<<dim3(nblk(g.Gx, 64), g.Gy), 64, 0, st>>>(dg, dst[c], c);
+        CK(cudaGetLastError(), "velocity halo");
+    }
+    return PI_OK;
+}
+
 pi_status pi_set_velocity(pi_model* m, const double* u, const double* v, const double* w) {
     if (!m || !u || !v || !w) return fail(m, PI_ERR_ARG, "pi_set_velocity: NULL argument");
-    std::vector<double> U, V, W;
-    host_vel_copy(m->hg, u, v, w, U, V, W);
     // write into the own buffer that vel₀ does not alias
     int b = (m->vel0[0] == m->velbuf[0][0]) ? 1 : 0;
-    const size_t bytes = m->hg.G * sizeof(double);
-    CK(cudaMemcpyAsync(m->velbuf[b][0], U.data(), bytes, cudaMemcpyHostToDevice, m->stream), "upload u");
-    CK(cudaMemcpyAsync(m->velbuf[b][1], V.data(), bytes, cudaMemcpyHostToDevice, m->stream), "upload v");
-    CK(cudaMemcpyAsync(m->velbuf[b][2], W.data(), bytes, cudaMemcpyHostToDevice, m->stream), "upload w");
+    const HostGrid& g = m->hg;
+    if (g.Nx >= g.Hx && g.Ny >= g.Hy && g.Nz >= g.Hz) {
+        pi_status st = device_vel_copy(m, u, v, w, m->velbuf[b][0], m->velbuf[b][1], m->velbuf[b][2]);
+        if (st) return st;
+    } else {
+        std::vector<double> U, V, W;
+        host_vel_copy(g, u, v, w, U, V, W);
+        const size_t bytes = g.G * sizeof(double);
+        CK(cudaMemcpyAsync(m->velbuf[b][0], U.data(), bytes, cudaMemcpyHostToDevice, m->stream), "upload u");
+        CK(cudaMemcpyAsync(m->velbuf[b][1], V.data(), bytes, cudaMemcpyHostToDevice, m->stream), "upload v");
+        CK(cudaMemcpyAsync(m->velbuf[b][2], W.data(), bytes, cudaMemcpyHostToDevice, m->stream), "upload w");
+    }
     CK(cudaStreamSynchronize(m->stream), "synchronize");
     for (int c = 0; c < 3; ++c) m->vel1[c] = m->velbuf[b][c];
     m->vel1_buf = b;
@@ -613,7 +709,7 @@ pi_status pi_set_velocity(pi_model* m, const double* u, const double* v, const d
 
 pi_status pi_set_PARF(pi_model* m, const double* parf) {
     if (!m || !parf) return fail(m, PI_ERR_ARG, "pi_set_PARF: NULL argument");
-    CK(cudaMemcpyAsync(m->PARF, parf, (size_t)m->hg.Nx * m->hg.Ny * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload PARF");
+    CK(cudaMemcpyAsync(m->PARF, parf, (size_t)m->hg.Nx * m->hg.Ny * sizeof(double), cudaMemcpyDefault, m->stream), "upload PARF");
     CK(cudaStreamSynchronize(m->stream), "synchronize");
     return PI_OK;
 }
@@ -621,10 +717,11 @@ pi_status pi_set_PARF(pi_model* m, const double* parf) {
 pi_status pi_set_temp(pi_model* m, const double* temp) {
     if (!m || !temp) return fail(m, PI_ERR_ARG, "pi_set_temp: NULL argument");
     const HostGrid& g = m->hg;
-    std::vector<double> T(g.G, 0.0);
-    for (int k = 1; k <= g.Nz; ++k) for (int j = 1; j <= g.Ny; ++j) for (int i = 1; i <= g.Nx; ++i)
-        T[g.id(i + g.Hx, j + g.Hy, k + g.Hz)] = temp[(size_t)(i - 1) + (size_t)g.Nx * ((size_t)(j - 1) + (size_t)g.Ny * (size_t)(k - 1))];
-    CK(cudaMemcpyAsync(m->temp_own, T.data(), g.G * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload temp");
+    size_t n = (size_t)g.Nx * g.Ny * g.Nz;
+    // copy_interior!: only the interior is written; the halo of timestepper.temp stays zero
+    CK(cudaMemcpyAsync(m->stage, temp, n * sizeof(double), cudaMemcpyDefault, m->stream), "upload temp");
+    k_scatter_interior<<<nblk((long long)n, 256), 256, 0, m->stream>>>(m->dg, m->temp_own, m->stage, g.Nx, g.Ny, g.Nz);
+    CK(cudaGetLastError(), "scatter temp");
     CK(cudaStreamSynchronize(m->stream), "synchronize");
     m->temp = m->temp_own;
     return PI_OK;
@@ -655,6 +752,40 @@ pi_status pi_time_step(pi_model* m, double dT) {
     return check_device_errors(m);
 }
 
+pi_status pi_get_stream(pi_model* m, void** stream) {
+    if (!m || !stream) return fail(m, PI_ERR_ARG, "pi_get_stream: NULL argument");
+    *stream = (void*)m->stream;
+    return PI_OK;
+}
+
+pi_status pi_profile_enable(pi_model* m, int32_t on) {
+    if (!m) return fail(m, PI_ERR_ARG, "pi_profile_enable: NULL model");
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    drain_marks(m);
+    m->prof_names.clear(); m->prof_count.clear(); m->prof_ms.clear();
+    m->profiling = on ? 1 : 0;
+    return PI_OK;
+}
+
+pi_status pi_profile_read(pi_model* m, int32_t max, char* names, size_t names_len,
+                          int64_t* launches, double* ms, int32_t* n) {
+    if (!m || !n) return fail(m, PI_ERR_ARG, "pi_profile_read: NULL argument");
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    drain_marks(m);
+    int32_t k = (int32_t)m->prof_names.size();
+    *n = k;
+    size_t off = 0;
+    for (int32_t q = 0; q < k && q < max; ++q) {
+        if (launches) launches[q] = m->prof_count[q];
+        if (ms) ms[q] = m->prof_ms[q];
+        if (names) {
+            const std::string& nm = m->prof_names[q];
+            if (off + nm.size() + 1 <= names_len) { memcpy(names + off, nm.c_str(), nm.size() + 1); off += nm.size() + 1; }
+        }
+    }
+    return PI_OK;
+}
+
 pi_status pi_synchronize(pi_model* m) {
     if (!m) return fail(m, PI_ERR_ARG, "pi_synchronize: NULL model");
     CK(cudaStreamSynchronize(m->stream), "synchronize");
@@ -676,12 +807,14 @@ pi_status pi_set_time(pi_model* m, int64_t iteration, double t) {
 
 pi_status pi_count_active(pi_model* m, int32_t sp, int64_t* n) {
     if (!m || !n || sp < 0 || sp >= m->nsp) return fail(m, PI_ERR_ARG, "pi_count_active: bad argument");
-    std::vector<uint8_t> flags(m->C);
-    CK(cudaMemcpyAsync(flags.data(), m->h_spc[sp].flags, m->C, cudaMemcpyDeviceToHost, m->stream), "download flags");
+    unsigned long long* d = (unsigned long long*)m->sb.rank64;   // scratch between steps
+    unsigned long long h = 0;
+    CK(cudaMemsetAsync(d, 0, sizeof h, m->stream), "zero count");
+    k_count_active<<<148 * 2, 256, 0, m->stream>>>(m->h_spc[sp].flags, m->C, d);
+    CK(cudaGetLastError(), "k_count_active");
+    CK(cudaMemcpyAsync(&h, d, sizeof h, cudaMemcpyDeviceToHost, m->stream), "download count");
     CK(cudaStreamSynchronize(m->stream), "synchronize");
-    int64_t c = 0;
-    for (uint8_t f : flags) c += (f & FL_AC) ? 1 : 0;
-    *n = c;
+    *n = (int64_t)h;
     return PI_OK;
 }
 
