@@ -202,6 +202,23 @@ pi_status pi_profile_enable(pi_model* m, int32_t on);
 pi_status pi_profile_read(pi_model* m, int32_t max, char* names, size_t names_len,
                           int64_t* launches, double* ms, int32_t* n);
 
+/* DST3FL advection tendency of one tracer field, computed without allocating any device memory.
+ * No counterpart in the reference: it serves callers that cannot allocate device memory (a host
+ * runtime that owns all device allocations through its own pool, or a loop that must not allocate
+ * after start-up). `c`, `u`, `v`, `w` and `Gc` are caller-owned DEVICE pointers to halo-padded
+ * fields in the layout of pi_set_tracer, with halos already filled; the grid's dzF, dzC and
+ * landmask are host pointers as in pi_create. On return the work is queued on `stream`
+ * (a cudaStream_t, NULL for the default stream) and Gc's interior holds tracer_temp − tracer after
+ * the x, y and z sweeps of tracer_advection! (multi_dim_adv.jl:111-135); Gc's halo is not written.
+ * The sweeps' intermediates live in one fixed device array shared by all calls on a device:
+ * grids above 524,288 halo-padded cells or 4,096 levels are rejected with PI_ERR_ARG; calls that
+ * overlap on the GPU race on that array; the first call on a device looks up its address and
+ * should come before any stream capture. Errors are reported by pi_noalloc_last_error. */
+pi_status pi_tracer_advection_noalloc(const pi_grid* grid, const double* c, const double* u,
+                                      const double* v, const double* w, double dT, double* Gc,
+                                      void* stream);
+pi_status pi_noalloc_last_error(char* buf, size_t len);
+
 /* Message of the last error of the handle (or of the last failed pi_create when m is NULL). */
 pi_status pi_last_error(pi_model* m, char* buf, size_t len);
 

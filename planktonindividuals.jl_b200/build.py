@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "PlanktonIndividuals", "libpib200.so")
 SOURCES = ["pib200.cu"]
-DEPS = ["pib200.cu", "kernels_fp64.cuh", "pib200_internal.h"]
+DEPS = ["pib200.cu", "kernels_fp64.cuh", "pib200_internal.h", "noalloc.cu"]
 
 
 def nvcc():

@@ -974,3 +974,7 @@ pi_status pi_sim_destroy(pi_sim* s) {
 }
 
 }  // extern "C"
+
+// Allocation-free tracer advection entry point (its own file; compiled in this translation unit
+// so the kernels above are shared rather than defined twice).
+#include "noalloc.cu"
