@@ -110,23 +110,29 @@ def dist_setup():
 # ------------------------------------------------------------------------------------------
 
 def algorithmic_bytes(name, wl, n_active_total):
+    """Bytes each launch must move at minimum (Float64 form); see DESIGN.md section 4."""
     g = wl.grid
     V = g.Nx * g.Ny * g.Nz
     NC = wl.nsp * wl.capacity
     inactive = NC - n_active_total
     occupied_layers = min(g.Nz, 20)
     vel_cells = g.Nx * g.Ny * occupied_layers
+    if name == "k_particles_sorted":
+        # per individual: list entry, flags, stat, cell, x, y, z read; x, y, z, cell, key written;
+        # one count update; vel₀, vel½, vel₁ (9 fields) read once over the occupied layers
+        return n_active_total * (4 + 1 + 1 + 4 + 24 + 24 + 4 + 4 + 8) + 9 * 8 * vel_cells
     if name == "k_particles":
-        # active: x,y,z,flags,cell read; x,y,z,cell,key written; one count update;
-        # inactive: flags,cell read, cell,key written; vel₀ and vel₁ read once where individuals are
-        return n_active_total * (29 + 32 + 8) + inactive * (5 + 8) + 6 * 8 * vel_cells
+        # slot pass: flags, stat for every slot; inactive slots: cell, x, y, z read, cell, key written
+        return NC * 2 + inactive * (4 + 24 + 8)
     if name == "k_sweep_x":
         return V * (14 * 8 * 2 + 8)
     if name == "k_sweep_y":
         return V * (14 * 8 * 3 + 8)
-    if name == "k_sweep_z_final":
-        # tracer_temp, tracer, new tracer, w, offsets + each entry's 5 consumption terms
-        return V * (14 * 8 * 3 + 8 + 4) + n_active_total * (4 + 1 + 40)
+    if name == "k_sweep_z":
+        return V * (14 * 8 * 3 + 8)
+    if name == "k_tracer_tail":
+        # advective tendency + tracer read, new tracer written, offsets, each entry's 5 terms
+        return V * (14 * 8 * 3 + 4) + n_active_total * (4 + 1 + 40)
     if name == "k_physiology":
         # per species launch over C slots: state r/w (Bm,Cq,Nq,Pq,Chl,age r; +Sz w), flags, stat,
         # cell, pos, 7 gathers, 5 consumption terms
@@ -210,6 +216,44 @@ def run_ours(args):
     cell_steps = ws * K * cells / (t_max / 1e3)
 
     # ---- per-kernel profile (CUDA events around each launch, separate pass) ----
+    prof, roof, tot_ms = {}, None, 1.0
+    if args.profile_steps > 0:
+        prof, roof, tot_ms = kernel_profile(lib, m, wl, args, step_async)
+    # ---- end to end through the C-ABI with pinned host buffers ----
+    lib.pi_sim_destroy(sim)
+    e2e = None
+    if args.e2e_steps > 0:
+        e2e = run_e2e(m, wl, snaps, nsnap, args, stream)
+
+    out = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline and ws == 1:
+            cpu = cpu_baseline(args.cpu_steps)
+        out = {
+            "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": ws, "steps": K,
+            "warmup": Wm, "ms_per_step": round(t_max / K, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": "config2: 256x256x64 grid, 2 species x 2,097,152 individuals, "
+                                   "random-Fourier velocity, dt=30 s, FP64 plain",
+                       "form": "fp64", "l2": "inputs larger than L2 (state ~1.5 GB per model)",
+                       "parallelism": f"replicas x{ws}"},
+            "cell_steps_per_s": round(cell_steps, 1),
+            "individuals": int(n0),
+            "kernel_profile_ms_per_step": {k: round(v[1] / args.profile_steps, 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
+            "profile_share": {k: round(v[1] / tot_ms, 4) for k, v in prof.items()},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": ck,
+            "gpu_launches": K * (12 + 4 * wl.nsp),
+        }
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    m.close()
+    return out
+
+
+def kernel_profile(lib, m, wl, args, step_async):
+    import ctypes as ct
     lib.pi_profile_enable(m.h, 1)
     for _ in range(args.profile_steps):
         step_async()
@@ -235,66 +279,42 @@ def run_ours(args):
                 "peak_source": peak_kind, "unit": "GB/s", "frac": round(ach / hbm, 4),
                 "traffic": None, "algorithmic_bytes_per_launch": int(byts),
                 "avg_launch_ms": round(per_launch_ms, 4)}
+    return prof, roof, tot_ms
 
-    # ---- end to end through the C-ABI with pinned host buffers ----
-    lib.pi_sim_destroy(sim)
-    e2e = None
-    if args.e2e_steps > 0:
-        g = wl.grid
-        pin = lambda shape: torch.empty(int(np.prod(shape)), dtype=torch.float64, pin_memory=True).numpy().reshape(shape, order="F")
-        hu, hv, hw = pin(snaps[0][0].shape), pin(snaps[0][1].shape), pin(snaps[0][2].shape)
-        hp, ht = pin((g.Nx, g.Ny)), pin((g.Nx, g.Ny, g.Nz))
-        h2d = (hu.nbytes + hv.nbytes + hw.nbytes + hp.nbytes + ht.nbytes)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ee0.record(stream)
-        ne = 0
-        for _ in range(args.e2e_steps):
-            it, tnow = m.get_time()
-            tv = int(np.floor(tnow / wl.dT_vel)); tp = int(np.floor(tnow / wl.dT_PAR)); tt = int(np.floor(tnow / wl.dT_temp))
-            src = snaps[min(tv, nsnap - 1)]
-            hu[...] = src[0]; hv[...] = src[1]; hw[...] = src[2]
-            hp[...] = wl.parf[:, :, tp]; ht[...] = wl.temp[:, :, :, tt]
-            m.set_velocity(hu, hv, hw)
-            m.set_PARF(hp)
-            m.set_temp(ht)
-            m.time_step(wl.dT)
-            ne += sum(m.count_active(s) for s in range(wl.nsp))
-        ee1.record(stream)
-        ee1.synchronize()
-        wall = time.perf_counter() - t0
-        ev_ms = ee0.elapsed_time(ee1)
-        e2e = {"value": round(ne / (ev_ms / 1e3), 1), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": 8 * wl.nsp, "steps": args.e2e_steps,
-               "ms_per_step": round(ev_ms / args.e2e_steps, 3), "wall_ms_per_step": round(1e3 * wall / args.e2e_steps, 3),
-               "note": "host numpy snapshot copied into pinned buffers outside the device copy; "
-                       "timed with CUDA events on the model stream around upload+step+readback"}
 
-    out = None
-    if rank == 0:
-        cpu = None
-        if not args.no_cpu_baseline and ws == 1:
-            cpu = cpu_baseline(args.cpu_steps)
-        out = {
-            "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": ws, "steps": K,
-            "warmup": Wm, "ms_per_step": round(t_max / K, 4), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": {"workload": "config2: 256x256x64 grid, 2 species x 2,097,152 individuals, "
-                                   "random-Fourier velocity, dt=30 s, FP64 plain",
-                       "form": "fp64", "l2": "inputs larger than L2 (state ~1.5 GB per model)",
-                       "parallelism": f"replicas x{ws}"},
-            "cell_steps_per_s": round(cell_steps, 1),
-            "individuals": int(n0), "kernel_profile_ms_per_step": {k: round(v[1] / args.profile_steps, 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
-            "profile_share": {k: round(v[1] / tot_ms, 4) for k, v in prof.items()},
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": ck,
-            "gpu_launches": K * (10 + 4 * wl.nsp),
-        }
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
-    m.close()
-    return out
+def run_e2e(m, wl, snaps, nsnap, args, stream):
+    import torch
+    g = wl.grid
+    pin = lambda shape: torch.empty(int(np.prod(shape)), dtype=torch.float64, pin_memory=True).numpy().reshape(shape, order="F")
+    hu, hv, hw = pin(snaps[0][0].shape), pin(snaps[0][1].shape), pin(snaps[0][2].shape)
+    hp, ht = pin((g.Nx, g.Ny)), pin((g.Nx, g.Ny, g.Nz))
+    h2d = (hu.nbytes + hv.nbytes + hw.nbytes + hp.nbytes + ht.nbytes)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ee0.record(stream)
+    ne = 0
+    for _ in range(args.e2e_steps):
+        it, tnow = m.get_time()
+        tv = int(np.floor(tnow / wl.dT_vel)); tp = int(np.floor(tnow / wl.dT_PAR)); tt = int(np.floor(tnow / wl.dT_temp))
+        src = snaps[min(tv, nsnap - 1)]
+        hu[...] = src[0]; hv[...] = src[1]; hw[...] = src[2]
+        hp[...] = wl.parf[:, :, tp]; ht[...] = wl.temp[:, :, :, tt]
+        m.set_velocity(hu, hv, hw)
+        m.set_PARF(hp)
+        m.set_temp(ht)
+        m.time_step(wl.dT)
+        ne += sum(m.count_active(s) for s in range(wl.nsp))
+    ee1.record(stream)
+    ee1.synchronize()
+    wall = time.perf_counter() - t0
+    ev_ms = ee0.elapsed_time(ee1)
+    return {"value": round(ne / (ev_ms / 1e3), 1), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": 8 * wl.nsp, "steps": args.e2e_steps,
+            "ms_per_step": round(ev_ms / args.e2e_steps, 3), "wall_ms_per_step": round(1e3 * wall / args.e2e_steps, 3),
+            "note": "each step copies its snapshot into pinned host buffers, uploads it (vel_copy!, "
+                    "copyto!, copy_interior!), runs pi_time_step and reads the population counts; "
+                    "CUDA events on the model stream bracket the whole loop"}
 
 
 def cpu_sample_workload():

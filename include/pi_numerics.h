@@ -74,9 +74,11 @@ PI_HD int jl_isless(double x, double y) {
 /* Julia x * b for x::Float64, b::Bool: ifelse(b, x, copysign(0.0, x)). */
 PI_HD double jl_mulb(double x, int b) { return b ? x : copysign(0.0, x); }
 
-/* Julia mod(x, 1.0): r = rem(x, 1); r == 0 ? copysign(r, 1) : (r < 0 ? r + 1 : r). */
+/* Julia mod(x, 1.0): r = rem(x, 1); r == 0 ? copysign(r, 1) : (r < 0 ? r + 1 : r).
+ * rem(x, 1) is computed as x - trunc(x): exact for finite x (Sterbenz: trunc(x) is within a factor
+ * of two of x when |x| >= 1, and 0 otherwise), NaN for infinite or NaN x, like fmod. */
 PI_HD double jl_mod1(double x) {
-    double r = fmod(x, 1.0);
+    double r = x - trunc(x);
     if (r == 0.0) return 0.0;
     if ((r > 0.0) != (1.0 > 0.0)) return r + 1.0;
     return r;

@@ -138,6 +138,10 @@ pi_status pi_get_tracer(pi_model* m, int32_t idx, double* out);
  * (src/Biogeochemistry/HaloRegions/halo_regions.jl:64-99). */
 pi_status pi_set_velocity(pi_model* m, const double* u, const double* v, const double* w);
 
+/* vel₀ of the timestepper (the previous step's velocity, time_step.jl:174-176), same layout as
+ * pi_set_velocity. Only needed to restart from a checkpoint in a fresh handle. */
+pi_status pi_set_velocity0(pi_model* m, const double* u, const double* v, const double* w);
+
 /* copyto!(timestepper.PARF, PARF) (src/Simulation/update.jl:23): surface PAR, Nx*Ny. */
 pi_status pi_set_PARF(pi_model* m, const double* parf);
 

@@ -577,10 +577,19 @@ bool plankton_update(orc_model* m, Species& s, int spi, double dT, double t) {
         if (!s.ac[i]) free_slots.push_back(i + 1);                          /* 1-based */
     }
     if (dvidnum > (double)free_slots.size()) {
-        char buf[160];
-        snprintf(buf, sizeof buf, "number of individual exceeds the capacity at timestep %s days",
-                 std::to_string(t / 86400.0).c_str());
-        m->err = buf;
+        /* Julia prints the Float64 with the shortest digits that round-trip */
+        char num[64];
+        double d = t / 86400.0;
+        for (int p = 1; p <= 17; ++p) { snprintf(num, sizeof num, "%.*g", p, d); if (strtod(num, nullptr) == d) break; }
+        std::string ns(num);
+        if (ns.find('e') != std::string::npos) {
+            std::string mant = ns.substr(0, ns.find('e')), ex = ns.substr(ns.find('e') + 1);
+            if (mant.find('.') == std::string::npos) mant += ".0";
+            ns = mant + "e" + std::to_string(atoi(ex.c_str()));
+        } else if (ns.find('.') == std::string::npos) {
+            ns += ".0";
+        }
+        m->err = "number of individual exceeds the capacity at timestep " + ns + " days";
         m->err_flags |= ERR_CAPACITY;
         return false;
     }
@@ -1014,6 +1023,15 @@ int orc_set_velocity(orc_model* m, const double* u, const double* v, const doubl
     copy_in(m->w1, w, g.Nx, g.Ny, g.Nz + ez);
     fill_halo_u(g, m->u1); fill_halo_v(g, m->v1); fill_halo_w(g, m->w1);
     return PI_OK;
+}
+
+int orc_set_velocity0(orc_model* m, const double* u, const double* v, const double* w) {
+    if (!m) return PI_ERR_ARG;
+    dvec su = m->u1, sv = m->v1, sw = m->w1;
+    int r = orc_set_velocity(m, u, v, w);
+    std::swap(m->u0, m->u1); std::swap(m->v0, m->v1); std::swap(m->w0, m->w1);
+    m->u1 = su; m->v1 = sv; m->w1 = sw;
+    return r;
 }
 
 int orc_set_PARF(orc_model* m, const double* parf) {

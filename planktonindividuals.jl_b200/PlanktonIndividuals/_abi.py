@@ -87,6 +87,7 @@ def declare(lib, prefix):
         "set_tracer": (ct.c_int32, [P, ct.c_int32, _dp]),
         "get_tracer": (ct.c_int32, [P, ct.c_int32, _dp]),
         "set_velocity": (ct.c_int32, [P, _dp, _dp, _dp]),
+        "set_velocity0": (ct.c_int32, [P, _dp, _dp, _dp]),
         "set_PARF": (ct.c_int32, [P, _dp]),
         "set_temp": (ct.c_int32, [P, _dp]),
         "set_flux_bc": (ct.c_int32, [P, ct.c_int32, ct.c_int32, ct.c_int32, _dp, ct.c_int64]),

@@ -49,7 +49,7 @@ def load():
 
 # Exported entry points of include/pib200.h (checked by the CPU test suite).
 EXPORTS = ("pi_create", "pi_destroy", "pi_set_individuals", "pi_get_individuals", "pi_set_tracer",
-           "pi_get_tracer", "pi_set_velocity", "pi_set_PARF", "pi_set_temp", "pi_set_flux_bc",
+           "pi_get_tracer", "pi_set_velocity", "pi_set_velocity0", "pi_set_PARF", "pi_set_temp", "pi_set_flux_bc",
            "pi_time_step", "pi_get_time", "pi_set_time", "pi_count_active", "pi_get_diag",
            "pi_reset_diags", "pi_sim_create", "pi_sim_update", "pi_sim_destroy", "pi_synchronize",
            "pi_last_error", "pi_status_string", "pi_get_stream", "pi_profile_enable", "pi_profile_read")

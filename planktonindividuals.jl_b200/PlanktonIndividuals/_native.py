@@ -183,6 +183,16 @@ class CModel:
         self._check(self._fn("set_velocity")(self.h, _dptr(u.ravel(order="F")), _dptr(v.ravel(order="F")),
                                              _dptr(w.ravel(order="F"))), "set_velocity")
 
+    def set_velocity0(self, u, v, w):
+        """vel₀ (previous step's velocity), for restarting from a checkpoint."""
+        g = self.grid
+        b = [int(t == _abi.PI_BOUNDED) for t in g.topo]
+        u = _f64(u, (g.Nx + b[0], g.Ny, g.Nz))
+        v = _f64(v, (g.Nx, g.Ny + b[1], g.Nz))
+        w = _f64(w, (g.Nx, g.Ny, g.Nz + b[2]))
+        self._check(self._fn("set_velocity0")(self.h, _dptr(u.ravel(order="F")), _dptr(v.ravel(order="F")),
+                                              _dptr(w.ravel(order="F"))), "set_velocity0")
+
     def set_PARF(self, parf):
         a = _f64(parf, (self.grid.Nx, self.grid.Ny))
         self._check(self._fn("set_PARF")(self.h, _dptr(a.ravel(order="F"))), "set_PARF")

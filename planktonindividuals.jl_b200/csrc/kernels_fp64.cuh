@@ -80,35 +80,34 @@ __device__ __forceinline__ double itpl(const DGrid& g, const double* __restrict_
          + w100 * c100 / d0 + w101 * c101 / d1 + w110 * c110 / d0 + w111 * c111 / d1;
 }
 
-struct VelPtrs { const double *u0, *v0, *w0, *u1, *v1, *w1; };
 
-// One thread per (species, slot). Writes the new position, the packed cell of find_inds!, the
-// binning key and the per-cell count of active individuals.
-__global__ void k_particles(DGrid g, const SpcDev* __restrict__ spc, int nsp, long long C,
-                            double dT, uint64_t seed, uint32_t iter, VelPtrs vel,
-                            double kappa_h, double kappa_v, uint32_t* __restrict__ cnt,
-                            uint32_t* __restrict__ key, uint32_t sentinel, uint32_t* err) {
-    long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= (long long)nsp * C) return;
+// vel½ = (vel₀ + vel₁) * 0.5 (time_step.jl:17-19), once per step for the three components.
+__global__ void k_velhalf(long long G, const double* __restrict__ u0, const double* __restrict__ v0,
+                          const double* __restrict__ w0, const double* __restrict__ u1,
+                          const double* __restrict__ v1, const double* __restrict__ w1,
+                          double* __restrict__ uh, double* __restrict__ vh, double* __restrict__ wh,
+                          const uint32_t* err) {
     if (*err & PI_DEVERR_CAPACITY) return;
-    int s = (int)(gid / C);
-    long long slot = gid - (long long)s * C;
-    const SpcDev& P = spc[s];
-    int ac = P.flags[slot] & FL_AC;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < G; q += (long long)gridDim.x * blockDim.x) {
+        uh[q] = (u0[q] + u1[q]) * 0.5;
+        vh[q] = (v0[q] + v1[q]) * 0.5;
+        wh[q] = (w0[q] + w1[q]) * 0.5;
+    }
+}
+
+struct VelPtrs { const double *u0, *v0, *w0, *uh, *vh, *wh, *u1, *v1, *w1; };
+
+// RK4 + diffusion + find_inds! of one active individual; writes its position, packed cell, binning
+// key and count.
+__device__ __forceinline__ void particle_step(const DGrid& g, const SpcDev& P, int s, long long slot,
+                                              long long gid, double dT, uint64_t seed, uint32_t iter,
+                                              const VelPtrs& vel, double kappa_h, double kappa_v,
+                                              uint32_t* __restrict__ cnt, uint32_t* __restrict__ key,
+                                              uint32_t* err) {
+    const int ac = 1;
     int oxi, oyi, ozi;
     unpack_cell(g, P.cell[slot], oxi, oyi, ozi);
-    // ΔzC at the stored zi + Hz (particle_diffusion.jl:5), checked for every slot
-    int kdz = clamp_idx((long long)ozi + g.Hz, 1, g.Gz, err);
-    if (!ac) {
-        // Inactive slots: every stage multiplies by ac, so positions end as zeros and the cell
-        // is (Hx, Hy, Hz).
-        if (P.x[slot] != 0.0) P.x[slot] = 0.0;
-        if (P.y[slot] != 0.0) P.y[slot] = 0.0;
-        if (P.z[slot] != 0.0) P.z[slot] = 0.0;
-        P.cell[slot] = pack_cell(g, g.Hx, g.Hy, g.Hz);
-        key[gid] = sentinel;
-        return;
-    }
+    int kdz = clamp_idx((long long)ozi + g.Hz, 1, g.Gz, err);   // ΔzC at the stored zi + Hz
     const double X = P.x[slot], Y = P.y[slot], Z = P.z[slot];
     const double NX = (double)g.Nx, NY = (double)g.Ny, NZ = (double)g.Nz;
     // stage 1 at vel₀
@@ -121,18 +120,18 @@ __global__ void k_particles(DGrid g, const SpcDev* __restrict__ spc, int nsp, lo
     double vz = Z - jl_mulb(0.5 * w1 * dT, ac);
     vx = jl_mulb(bc_pos(vx, NX, g.tx), ac); vy = jl_mulb(bc_pos(vy, NY, g.ty), ac); vz = jl_mulb(bc_pos(vz, NZ, g.tz), ac);
     // stage 2 at vel½
-    u1 = jl_mulb(itpl<0, 1>(g, vel.u0, vel.u1, vx, vy, vz, ac, err), ac);
-    v1 = jl_mulb(itpl<1, 1>(g, vel.v0, vel.v1, vx, vy, vz, ac, err), ac);
-    w1 = jl_mulb(itpl<2, 1>(g, vel.w0, vel.w1, vx, vy, vz, ac, err), ac);
+    u1 = jl_mulb(itpl<0, 0>(g, vel.uh, vel.uh, vx, vy, vz, ac, err), ac);
+    v1 = jl_mulb(itpl<1, 0>(g, vel.vh, vel.vh, vx, vy, vz, ac, err), ac);
+    w1 = jl_mulb(itpl<2, 0>(g, vel.wh, vel.wh, vx, vy, vz, ac, err), ac);
     u2 = u2 + u1 * 2.0; v2 = v2 + v1 * 2.0; w2 = w2 + w1 * 2.0;
     vx = X + jl_mulb(0.5 * u1 * dT, ac);
     vy = Y + jl_mulb(0.5 * v1 * dT, ac);
     vz = Z - jl_mulb(0.5 * w1 * dT, ac);
     vx = jl_mulb(bc_pos(vx, NX, g.tx), ac); vy = jl_mulb(bc_pos(vy, NY, g.ty), ac); vz = jl_mulb(bc_pos(vz, NZ, g.tz), ac);
     // stage 3 at vel½
-    u1 = jl_mulb(itpl<0, 1>(g, vel.u0, vel.u1, vx, vy, vz, ac, err), ac);
-    v1 = jl_mulb(itpl<1, 1>(g, vel.v0, vel.v1, vx, vy, vz, ac, err), ac);
-    w1 = jl_mulb(itpl<2, 1>(g, vel.w0, vel.w1, vx, vy, vz, ac, err), ac);
+    u1 = jl_mulb(itpl<0, 0>(g, vel.uh, vel.uh, vx, vy, vz, ac, err), ac);
+    v1 = jl_mulb(itpl<1, 0>(g, vel.vh, vel.vh, vx, vy, vz, ac, err), ac);
+    w1 = jl_mulb(itpl<2, 0>(g, vel.wh, vel.wh, vx, vy, vz, ac, err), ac);
     u2 = u2 + u1 * 2.0; v2 = v2 + v1 * 2.0; w2 = w2 + w1 * 2.0;
     vx = X + jl_mulb(1.0 * u1 * dT, ac);
     vy = Y + jl_mulb(1.0 * v1 * dT, ac);
@@ -166,6 +165,54 @@ __global__ void k_particles(DGrid g, const SpcDev* __restrict__ spc, int nsp, lo
     int c = gidx(g, xi, yi, zi);
     key[gid] = (uint32_t)c;
     atomicAdd(&cnt[c], 1u);
+}
+
+// Slot-order pass over every (species, slot): inactive slots (every stage multiplies by ac, so
+// their positions end as zeros and their cell is (Hx, Hy, Hz)), and active individuals that were
+// not binned in the previous step (new daughters, uploaded state). The others are moved by
+// k_particles_sorted in cell order.
+__global__ void k_particles(DGrid g, const SpcDev* __restrict__ spc, int nsp, long long C,
+                            double dT, uint64_t seed, uint32_t iter, VelPtrs vel,
+                            double kappa_h, double kappa_v, uint32_t* __restrict__ cnt,
+                            uint32_t* __restrict__ key, uint32_t sentinel, uint32_t* err) {
+    long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (long long)nsp * C) return;
+    if (*err & PI_DEVERR_CAPACITY) return;
+    int s = (int)(gid / C);
+    long long slot = gid - (long long)s * C;
+    const SpcDev& P = spc[s];
+    if (!(P.flags[slot] & FL_AC)) {
+        int oxi, oyi, ozi;
+        unpack_cell(g, P.cell[slot], oxi, oyi, ozi);
+        clamp_idx((long long)ozi + g.Hz, 1, g.Gz, err);
+        if (P.x[slot] != 0.0) P.x[slot] = 0.0;
+        if (P.y[slot] != 0.0) P.y[slot] = 0.0;
+        if (P.z[slot] != 0.0) P.z[slot] = 0.0;
+        P.cell[slot] = pack_cell(g, g.Hx, g.Hy, g.Hz);
+        key[gid] = sentinel;
+        return;
+    }
+    if (P.stat[slot] & ST_AC0) return;                // moved by k_particles_sorted
+    particle_step(g, P, s, slot, gid, dT, seed, iter, vel, kappa_h, kappa_v, cnt, key, err);
+}
+
+// Cell-order pass: the individuals binned in the previous step (prev_sorted[0 .. off[G]), which
+// were active then) that are still active. Neighbouring threads interpolate in neighbouring cells.
+__global__ void k_particles_sorted(DGrid g, const SpcDev* __restrict__ spc, long long C,
+                                   const uint32_t* __restrict__ prev_sorted,
+                                   const uint32_t* __restrict__ prev_off, long long Gcells,
+                                   double dT, uint64_t seed, uint32_t iter, VelPtrs vel,
+                                   double kappa_h, double kappa_v, uint32_t* __restrict__ cnt,
+                                   uint32_t* __restrict__ key, uint32_t* err) {
+    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (*err & PI_DEVERR_CAPACITY) return;
+    if (p >= (long long)prev_off[Gcells]) return;
+    uint32_t gd = prev_sorted[p];
+    int s = (int)(gd / C);
+    long long slot = gd - (long long)s * C;
+    const SpcDev& P = spc[s];
+    if (!(P.flags[slot] & FL_AC) || !(P.stat[slot] & ST_AC0)) return;
+    particle_step(g, P, s, slot, gd, dT, seed, iter, vel, kappa_h, kappa_v, cnt, key, err);
 }
 
 // pos[gid] = position of gid in the cell-sorted entry list.
@@ -526,91 +573,152 @@ __device__ __forceinline__ int wrap_axis(int a, int N, int H, int topo) {
     return a < H + 1 ? H + 1 : (a > N + H ? N + H : a);
 }
 
-// x sweep: calc_Gcˣ + fill_halo_Gcs + multi_dim_x on tracer_temp = tracer.
-__global__ void k_sweep_x(DGrid g, const double* __restrict__ tr, double* __restrict__ tta,
-                          const double* __restrict__ u, double dT, const uint32_t* err) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x + 1 + g.Hx;
-    int j = blockIdx.y + 1 + g.Hy;
-    int k = blockIdx.z + 1 + g.Hz;
-    if (i > g.Nx + g.Hx) return;
+// Per-face quantities of DST3FL that do not depend on the tracer (CFL, transport, d₀ and d₁ of
+// DST3FL.jl:5-11, the factors of adv_flux): computed once per face and shared by the 14 tracers.
+// Each is the same IEEE expression the per-tracer formula evaluates, so results are unchanged.
+struct FaceCoef { double d0c, d1c, omc, cpe, hp, hm; };
+
+__device__ __forceinline__ FaceCoef face_coef(double vel, double area, double dxc, double dT) {
+    FaceCoef f;
+    double cfl = fabs(vel * dT / dxc);
+    double tr = area * vel;
+    f.d0c = (2.0 - cfl) * (1.0 - cfl) / 6.0;
+    f.d1c = (1.0 - cfl * cfl) / 6.0;
+    f.omc = 1.0 - cfl;
+    f.cpe = cfl + F_1em20;
+    f.hp = 0.5 * (tr + fabs(tr));
+    f.hm = 0.5 * (tr - fabs(tr));
+    return f;
+}
+__device__ __forceinline__ double psi_c(const FaceCoef& f, double th) {
+    return jl_max(0.0, jl_min(jl_min(1.0, f.d0c + f.d1c * th), th * f.omc / f.cpe));
+}
+// adv_flux_x / adv_flux_y at face i from c[i-2], c[i-1], c[i], c[i+1]
+__device__ __forceinline__ double flux_xy_c(const FaceCoef& f, double cm2, double cm1, double c0, double cp1,
+                                            int lm2, int lm1, int l0, int lp1) {
+    double d0 = jl_mulb(jl_mulb(c0 - cm1, l0), lm1);
+    double dm = jl_mulb(jl_mulb(cm1 - cm2, lm1), lm2);
+    double dp = jl_mulb(jl_mulb(cp1 - c0, lp1), l0);
+    double psp = psi_c(f, theta(dm, d0));
+    double psm = psi_c(f, theta(dp, d0));
+    return f.hp * (cm1 + psp * d0) + f.hm * (c0 - psm * d0);
+}
+// adv_flux_z at face k from c[k-2], c[k-1], c[k], c[k+1] (index grows downward)
+__device__ __forceinline__ double flux_z_c(const FaceCoef& f, double cm2, double cm1, double c0, double cp1,
+                                           int lm2, int lm1, int l0, int lp1) {
+    double d0 = jl_mulb(jl_mulb(cm1 - c0, l0), lm1);
+    double dm = jl_mulb(jl_mulb(cm2 - cm1, lm1), lm2);
+    double dp = jl_mulb(jl_mulb(c0 - cp1, lp1), l0);
+    double psp = psi_c(f, theta(dm, d0));
+    double psm = psi_c(f, theta(dp, d0));
+    return f.hp * (c0 + psm * d0) + f.hm * (cm1 - psp * d0);
+}
+
+// x sweep (calc_Gcˣ + fill_halo_Gcs + multi_dim_x on tracer_temp = tracer). Each warp owns 31
+// cells of one row and 32 faces: lane l computes the flux of face i0 + l once, and the east-face
+// flux of its cell comes from lane l + 1 by shuffle. The face after the last interior cell follows
+// fill_halo_Gcs!: the periodic image of face H+1, or zero when Bounded.
+#define SWX_WARPS 4
+__global__ void __launch_bounds__(32 * SWX_WARPS) k_sweep_x(DGrid g, const double* __restrict__ tr,
+                                                            double* __restrict__ tta,
+                                                            const double* __restrict__ u, double dT,
+                                                            const uint32_t* err) {
     if (*err & PI_DEVERR_CAPACITY) return;
+    const int lane = threadIdx.x & 31;
+    const int wid = blockIdx.x * SWX_WARPS + (threadIdx.x >> 5);
+    const int i0 = wid * 31 + 1 + g.Hx;
+    if (i0 > g.Nx + g.Hx) return;                    // uniform per warp
+    const int j = blockIdx.y + 1 + g.Hy, k = blockIdx.z + 1 + g.Hz;
+    const int f = i0 + lane;                         // this lane's face (west face of cell f)
+    const int last = g.Nx + g.Hx;
+    const bool has_face = f <= last + 1;
+    const bool has_cell = lane < 31 && f <= last;
+    const bool special = f == last + 1;
+    const bool zero_face = !has_face || (special && g.tx != PI_PERIODIC);
+    const int fs = special ? g.Hx + 1 : f;           // face whose stencil gives the flux
     const long long G = g.G;
-    int q = gidx(g, i, j, k);
-    double ax = g.dy * dzF1(g, k);
-    double volk = vol(g, k);
-    double ui = u[q], up = u[q + 1];
-    int last = (i == g.Nx + g.Hx);
-    int lm2 = lmask(g, i - 2, j, k), lm1 = lmask(g, i - 1, j, k), l0 = lmask(g, i, j, k);
-    int lp1 = lmask(g, i + 1, j, k), lp2 = last ? 0 : lmask(g, i + 2, j, k);
-    int qw = gidx(g, g.Hx + 1, j, k);
-    double ftr = jl_mulb(jl_mulb(ax * up - ax * ui, lp1), l0);
+    const double ax = g.dy * dzF1(g, k);
+    const int qf = gidx(g, has_face ? fs : i0, j, k);
+    FaceCoef fc{};
+    int lm2 = 1, lm1 = 1, l0 = 1, lp1 = 1;
+    if (!zero_face) {
+        fc = face_coef(u[qf], ax, g.dx, dT);
+        lm2 = lmask(g, fs - 2, j, k); lm1 = lmask(g, fs - 1, j, k); l0 = lmask(g, fs, j, k); lp1 = lmask(g, fs + 1, j, k);
+    }
+    const int qc = gidx(g, has_cell ? f : i0, j, k);
+    double ftr = 0.0, dtv = 0.0;
+    int cl0 = 1, clp = 1;
+    if (has_cell) {
+        cl0 = lmask(g, f, j, k); clp = lmask(g, f + 1, j, k);
+        ftr = jl_mulb(jl_mulb(ax * u[qc + 1] - ax * u[qc], clp), cl0);
+        dtv = dT / vol(g, k);
+    }
+#pragma unroll 2
     for (int n = 0; n < PI_NTRACERS; ++n) {
         const double* c = tr + n * G;
-        double cm2 = c[q - 2], cm1 = c[q - 1], c0 = c[q], cp1 = c[q + 1];
-        double Fi = dst3_flux_xy(cm2, cm1, c0, cp1, lm2, lm1, l0, lp1, ui, ax, g.dx, dT);
-        double Fp;
-        if (!last) {
-            Fp = dst3_flux_xy(cm1, c0, cp1, c[q + 2], lm1, l0, lp1, lp2, up, ax, g.dx, dT);
-        } else if (g.tx == PI_PERIODIC) {
-            Fp = dst3_flux_xy(c[qw - 2], c[qw - 1], c[qw], c[qw + 1],
-                              lmask(g, g.Hx - 1, j, k), lmask(g, g.Hx, j, k), lmask(g, g.Hx + 1, j, k),
-                              lmask(g, g.Hx + 2, j, k), u[qw], ax, g.dx, dT);
-        } else {
-            Fp = 0.0;
+        double F = zero_face ? 0.0 : flux_xy_c(fc, c[qf - 2], c[qf - 1], c[qf], c[qf + 1], lm2, lm1, l0, lp1);
+        double Fe = __shfl_down_sync(0xffffffffu, F, 1);
+        if (has_cell) {
+            double c0 = c[qc];
+            double dG = jl_mulb(jl_mulb(Fe - F, clp), cl0);
+            tta[n * G + qc] = c0 - dtv * (dG - c0 * ftr);
         }
-        double dG = jl_mulb(jl_mulb(Fp - Fi, lp1), l0);
-        tta[n * G + q] = c0 - dT / volk * (dG - c0 * ftr);
     }
 }
 
-// y sweep on tracer_temp after x; original tracer c in the update term.
-__global__ void k_sweep_y(DGrid g, const double* __restrict__ tr, const double* __restrict__ tta,
-                          double* __restrict__ ttb, const double* __restrict__ v, double dT,
-                          const uint32_t* err) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x + 1 + g.Hx;
-    int j = blockIdx.y + 1 + g.Hy;
-    int k = blockIdx.z + 1 + g.Hz;
-    if (i > g.Nx + g.Hx) return;
+// y sweep on tracer_temp after x (multi_dim_y, original tracer in the update term). Each thread
+// walks SWY_L cells along y carrying the face flux (each face computed once, plus one shared face
+// per segment), tracer by tracer so a thread holds one running flux; lanes run along x for
+// coalesced access. Rows outside the interior are read through the periodic or clamped map the
+// halo fill of tracer_temp produces.
+#define SWY_L 8
+#define SWY_TY 4
+__device__ __forceinline__ double yface_flux(const DGrid& g, const double* __restrict__ c,
+                                             const double* __restrict__ v, int i, int f, int k,
+                                             double ay, double dT) {
+    const bool special = f == g.Ny + g.Hy + 1;
+    if (special && g.ty != PI_PERIODIC) return 0.0;            // fill_halo_north_Gc! (Bounded)
+    const int fs = special ? g.Hy + 1 : f;                      // periodic: Gc[N+H+1] = Gc[H+1]
+    FaceCoef fc = face_coef(v[gidx(g, i, fs, k)], ay, g.dy, dT);
+    int r0 = gidx(g, i, wrap_axis(fs - 2, g.Ny, g.Hy, g.ty), k), r1 = gidx(g, i, wrap_axis(fs - 1, g.Ny, g.Hy, g.ty), k);
+    int r2 = gidx(g, i, wrap_axis(fs, g.Ny, g.Hy, g.ty), k), r3 = gidx(g, i, wrap_axis(fs + 1, g.Ny, g.Hy, g.ty), k);
+    return flux_xy_c(fc, c[r0], c[r1], c[r2], c[r3], lmask(g, i, fs - 2, k), lmask(g, i, fs - 1, k),
+                     lmask(g, i, fs, k), lmask(g, i, fs + 1, k));
+}
+
+__global__ void __launch_bounds__(32 * SWY_TY, 8) k_sweep_y(DGrid g, const double* __restrict__ tr,
+                                                         const double* __restrict__ tta,
+                                                         double* __restrict__ ttb,
+                                                         const double* __restrict__ v, double dT,
+                                                         const uint32_t* err) {
     if (*err & PI_DEVERR_CAPACITY) return;
+    const int i = blockIdx.x * 32 + threadIdx.x + 1 + g.Hx;
+    const int j0 = (blockIdx.y * SWY_TY + threadIdx.y) * SWY_L + 1 + g.Hy;
+    const int k = blockIdx.z + 1 + g.Hz;
+    if (i > g.Nx + g.Hx || j0 > g.Ny + g.Hy) return;
+    const int jend = min(j0 + SWY_L - 1, g.Ny + g.Hy);
     const long long G = g.G;
-    int q = gidx(g, i, j, k);
-    int last = (j == g.Ny + g.Hy);
-    double ay = g.dx * dzF1(g, k);
-    double volk = vol(g, k);
-    double vj = v[q], vp = v[q + g.Gx];
-    int jm2 = wrap_axis(j - 2, g.Ny, g.Hy, g.ty), jm1 = wrap_axis(j - 1, g.Ny, g.Hy, g.ty);
-    int jp1 = wrap_axis(j + 1, g.Ny, g.Hy, g.ty), jp2 = wrap_axis(j + 2, g.Ny, g.Hy, g.ty);
-    int lm2 = lmask(g, i, j - 2, k), lm1 = lmask(g, i, j - 1, k), l0 = lmask(g, i, j, k);
-    int lp1 = lmask(g, i, j + 1, k), lp2 = last ? 0 : lmask(g, i, j + 2, k);
-    double ftr = jl_mulb(jl_mulb(ay * vp - ay * vj, lp1), l0);
-    int qm2 = gidx(g, i, jm2, k), qm1 = gidx(g, i, jm1, k), qp1 = gidx(g, i, jp1, k), qp2 = gidx(g, i, jp2, k);
-    int js = g.Hy + 1;
-    int qs = gidx(g, i, js, k);
-    int qsm2 = gidx(g, i, wrap_axis(js - 2, g.Ny, g.Hy, g.ty), k);
-    int qsm1 = gidx(g, i, wrap_axis(js - 1, g.Ny, g.Hy, g.ty), k);
-    int qsp1 = gidx(g, i, wrap_axis(js + 1, g.Ny, g.Hy, g.ty), k);
-    for (int n = 0; n < PI_NTRACERS; ++n) {
-        const double* c = tta + n * G;
-        double cm2 = c[qm2], cm1 = c[qm1], c0 = c[q], cp1 = c[qp1];
-        double Fj = dst3_flux_xy(cm2, cm1, c0, cp1, lm2, lm1, l0, lp1, vj, ay, g.dy, dT);
-        double Fp;
-        if (!last) {
-            Fp = dst3_flux_xy(cm1, c0, cp1, c[qp2], lm1, l0, lp1, lp2, vp, ay, g.dy, dT);
-        } else if (g.ty == PI_PERIODIC) {
-            Fp = dst3_flux_xy(c[qsm2], c[qsm1], c[qs], c[qsp1],
-                              lmask(g, i, js - 2, k), lmask(g, i, js - 1, k), lmask(g, i, js, k),
-                              lmask(g, i, js + 1, k), v[qs], ay, g.dy, dT);
-        } else {
-            Fp = 0.0;
+    const double ay = g.dx * dzF1(g, k);
+    const double dtv = dT / vol(g, k);
+#pragma unroll 1
+    for (int t = 0; t < PI_NTRACERS; ++t) {
+        const double* c = tta + t * G;
+        double Ft = yface_flux(g, c, v, i, j0, k, ay, dT);
+        for (int jj = j0; jj <= jend; ++jj) {
+            double Fb = yface_flux(g, c, v, i, jj + 1, k, ay, dT);
+            const int q = gidx(g, i, jj, k);
+            const int cl0 = lmask(g, i, jj, k), clp = lmask(g, i, jj + 1, k);
+            const double ftr = jl_mulb(jl_mulb(ay * v[q + g.Gx] - ay * v[q], clp), cl0);
+            double dG = jl_mulb(jl_mulb(Fb - Ft, clp), cl0);
+            ttb[t * G + q] = c[q] - dtv * (dG - tr[t * G + q] * ftr);
+            Ft = Fb;
         }
-        double dG = jl_mulb(jl_mulb(Fp - Fj, lp1), l0);
-        double cc = tr[n * G + q];
-        ttb[n * G + q] = c0 - dT / volk * (dG - cc * ftr);
     }
 }
 
 struct ZFinalArgs {
     DGrid g;
+    const double* gadv;      // 14 × G, advective tendency from k_sweep_z
     const double* tr;        // 14 × G, current tracers
     const double* ttb;       // 14 × G, tracer_temp after x and y
     double* tr_next;         // 14 × G
@@ -639,162 +747,185 @@ __device__ __forceinline__ double getbc_dev(const FluxBCDev& b, int a, int c, in
     return b.v[(a - 1) + (long long)b.n1 * ((c - 1) + (long long)b.n2 * (it - 1))];
 }
 
-// z sweep + calc_tracer_tendency + diffusion + sinking + forcing + flux BCs + apply_tendency.
-// One thread per water column (i, j), walking k downward so each z face flux is computed once.
-__global__ void k_sweep_z_final(ZFinalArgs a) {
-    const DGrid& g = a.g;
-    int i = blockIdx.x * blockDim.x + threadIdx.x + 1 + g.Hx;
-    int j = blockIdx.y + 1 + g.Hy;
-    if (i > g.Nx + g.Hx) return;
-    if (*a.err & PI_DEVERR_CAPACITY) return;
+#define SWZ_L 8
+#define SWZ_TZ 4
+// z sweep of multi_dim_z then calc_tracer_tendency!: Gc_adv = tracer_temp - tracer, written to
+// `gadv`. Each thread walks SWZ_L levels of one column carrying the z face flux, tracer by tracer;
+// levels outside the interior are read through the clamped map of the Bounded halo fill.
+__device__ __forceinline__ double zface_flux(const DGrid& g, const double* __restrict__ c,
+                                             const double* __restrict__ w, int i, int j, int f,
+                                             int qcol, int slab, double az, double dT) {
+    if (f == g.Nz + g.Hz + 1) return 0.0;                      // fill_halo_bottom_Gc! (Bounded)
+    FaceCoef fc = face_coef(w[qcol + (f - 1) * slab], az, dzC1(g, f), dT);
+    auto lev = [&](int kk) { return qcol + (wrap_axis(kk, g.Nz, g.Hz, PI_BOUNDED) - 1) * slab; };
+    return flux_z_c(fc, c[lev(f - 2)], c[lev(f - 1)], c[lev(f)], c[lev(f + 1)], lmask(g, i, j, f - 2),
+                    lmask(g, i, j, f - 1), lmask(g, i, j, f), lmask(g, i, j, f + 1));
+}
+
+__global__ void __launch_bounds__(32 * SWZ_TZ, 8) k_sweep_z(DGrid g, const double* __restrict__ tr,
+                                                         const double* __restrict__ ttb,
+                                                         double* __restrict__ gadv,
+                                                         const double* __restrict__ w, double dT,
+                                                         const uint32_t* err) {
+    if (*err & PI_DEVERR_CAPACITY) return;
+    const int i = blockIdx.x * 32 + threadIdx.x + 1 + g.Hx;
+    const int j = blockIdx.y + 1 + g.Hy;
+    const int k0 = (blockIdx.z * SWZ_TZ + threadIdx.y) * SWZ_L + 1 + g.Hz;
+    if (i > g.Nx + g.Hx || k0 > g.Nz + g.Hz) return;
+    const int kend = min(k0 + SWZ_L - 1, g.Nz + g.Hz);
     const long long G = g.G;
-    const double dT = a.dT;
-    const pi_bgc_params& b = a.b;
     const double az = g.dx * g.dy;
-    const int k0 = g.Hz + 1, k1 = g.Nz + g.Hz;
-    double Ftop[PI_NTRACERS];
-    // flux at the top face of cell k0
-    {
-        int k = k0;
-        double wk = a.w[gidx(g, i, j, k)];
-        int lm2 = lmask(g, i, j, k - 2), lm1 = lmask(g, i, j, k - 1), l0 = lmask(g, i, j, k), lp1 = lmask(g, i, j, k + 1);
-        int km2 = gidx(g, i, j, wrap_axis(k - 2, g.Nz, g.Hz, PI_BOUNDED));
-        int km1 = gidx(g, i, j, wrap_axis(k - 1, g.Nz, g.Hz, PI_BOUNDED));
-        int kc = gidx(g, i, j, k);
-        int kp1 = gidx(g, i, j, wrap_axis(k + 1, g.Nz, g.Hz, PI_BOUNDED));
-        for (int n = 0; n < PI_NTRACERS; ++n) {
-            const double* c = a.ttb + n * G;
-            Ftop[n] = dst3_flux_z(c[km2], c[km1], c[kc], c[kp1], lm2, lm1, l0, lp1, wk, az, dzC1(g, k), dT);
+    const int slab = g.Gx * g.Gy;
+    const int qcol = gidx(g, i, j, 1);
+#pragma unroll 1
+    for (int t = 0; t < PI_NTRACERS; ++t) {
+        const double* c = ttb + t * G;
+        double Ft = zface_flux(g, c, w, i, j, k0, qcol, slab, az, dT);
+        for (int k = k0; k <= kend; ++k) {
+            double Fb = zface_flux(g, c, w, i, j, k + 1, qcol, slab, az, dT);
+            const int q = qcol + (k - 1) * slab;
+            const int cl0 = lmask(g, i, j, k), clp = lmask(g, i, j, k + 1);
+            const double ftr = jl_mulb(jl_mulb(az * w[q] - az * w[q + slab], clp), cl0);
+            const double dG = jl_mulb(jl_mulb(Ft - Fb, clp), cl0);
+            const double cc = tr[t * G + q];
+            const double ct = c[q] - dT / vol(g, k) * (dG - cc * ftr);
+            gadv[t * G + q] = ct - cc;                          // calc_tracer_tendency!
+            Ft = Fb;
         }
     }
-    for (int k = k0; k <= k1; ++k) {
-        int q = gidx(g, i, j, k);
-        double volk = vol(g, k);
-        double wk = a.w[q], wp = a.w[q + g.Gx * g.Gy];
-        int l0 = lmask(g, i, j, k), lp1 = lmask(g, i, j, k + 1);
-        double ftr = jl_mulb(jl_mulb(az * wk - az * wp, lp1), l0);
-        double Gc[PI_NTRACERS];
-        {
-            int last = (k == k1);
-            int lm1 = l0, lp2 = last ? 0 : lmask(g, i, j, k + 2);
-            int kc = q;
-            int kp1 = gidx(g, i, j, wrap_axis(k + 1, g.Nz, g.Hz, PI_BOUNDED));
-            int kp2 = gidx(g, i, j, wrap_axis(k + 2, g.Nz, g.Hz, PI_BOUNDED));
-            int km1 = gidx(g, i, j, wrap_axis(k - 1, g.Nz, g.Hz, PI_BOUNDED));
-            for (int n = 0; n < PI_NTRACERS; ++n) {
-                const double* c = a.ttb + n * G;
-                double Fb;
-                if (!last) {
-                    // face k+1: c[k-1], c[k], c[k+1], c[k+2]
-                    Fb = dst3_flux_z(c[km1], c[kc], c[kp1], c[kp2], lmask(g, i, j, k - 1), lm1, lp1, lp2,
-                                     wp, az, dzC1(g, k + 1), dT);
-                } else {
-                    Fb = 0.0;   // fill_halo_bottom_Gc! (Bounded)
-                }
-                double dG = jl_mulb(jl_mulb(Ftop[n] - Fb, lp1), l0);
-                double cc = a.tr[n * G + q];
-                double ct = c[kc] - dT / volk * (dG - cc * ftr);
-                Gc[n] = ct - cc;                         // calc_tracer_tendency!
-                Ftop[n] = Fb;
+}
+
+__device__ __forceinline__ void z_final_cell(const ZFinalArgs& a, int i, int j, int k, int q, double volk, double* Gc);
+
+// Per interior cell: diffusion, sinking, forcing, flux BCs, particle terms and apply_tendency!
+// on top of the advective tendency of k_sweep_z (tracer_update.jl:22-43).
+__global__ void __launch_bounds__(128, 6) k_tracer_tail(ZFinalArgs a) {
+    const DGrid& g = a.g;
+    if (*a.err & PI_DEVERR_CAPACITY) return;
+    const int i = blockIdx.x * 128 + threadIdx.x + 1 + g.Hx;
+    const int j = blockIdx.y + 1 + g.Hy;
+    const int k = blockIdx.z + 1 + g.Hz;
+    if (i > g.Nx + g.Hx) return;
+    const int q = gidx(g, i, j, k);
+    const long long G = g.G;
+    double Gc[PI_NTRACERS];
+#pragma unroll
+    for (int t = 0; t < PI_NTRACERS; ++t) Gc[t] = a.gadv[t * G + q];
+    z_final_cell(a, i, j, k, q, vol(g, k), Gc);
+}
+
+// The rest of tracer_update! for one interior cell, given its advective tendency Gc.
+__device__ __forceinline__ void z_final_cell(const ZFinalArgs& a, int i, int j, int k, int q, double volk, double* Gc) {
+    const DGrid& g = a.g;
+    const long long G = g.G;
+    const double dT = a.dT;
+    const double az = g.dx * g.dy;
+    const int slab = g.Gx * g.Gy;
+    const pi_bgc_params& b = a.b;
+    // tracer_diffusion! (κ∇², tracer_diffusion.jl:1-21) on the original tracer
+    if (a.diffuse) {
+        double kx = b.kappa_h, ky = b.kappa_h, kz = b.kappa_v;
+        double axk = g.dy * dzF1(g, k), ayk = g.dx * dzF1(g, k);
+        int li = lmask(g, i, j, k);
+#pragma unroll
+        for (int n = 0; n < PI_NTRACERS; ++n) {
+            const double* c = a.tr + n * G;
+            auto dx0 = [&](int ii) { return jl_mulb(jl_mulb(c[gidx(g, ii, j, k)] - c[gidx(g, ii - 1, j, k)], lmask(g, ii, j, k)), lmask(g, ii - 1, j, k)); };
+            auto dy0 = [&](int jj) { return jl_mulb(jl_mulb(c[gidx(g, i, jj, k)] - c[gidx(g, i, jj - 1, k)], lmask(g, i, jj, k)), lmask(g, i, jj - 1, k)); };
+            auto dz0 = [&](int kk) { return jl_mulb(jl_mulb(c[gidx(g, i, j, kk - 1)] - c[gidx(g, i, j, kk)], lmask(g, i, j, kk)), lmask(g, i, j, kk - 1)); };
+            double fx1 = kx * axk * (dx0(i + 1) / g.dx), fx0 = kx * axk * (dx0(i) / g.dx);
+            double fy1 = ky * ayk * (dy0(j + 1) / g.dy), fy0 = ky * ayk * (dy0(j) / g.dy);
+            double fz0 = kz * az * (dz0(k) / dzF1(g, k)), fz1 = kz * az * (dz0(k + 1) / dzF1(g, k + 1));
+            double ax_ = jl_mulb(jl_mulb(fx1 - fx0, lmask(g, i + 1, j, k)), li);
+            double ay_ = jl_mulb(jl_mulb(fy1 - fy0, lmask(g, i, j + 1, k)), li);
+            double az_ = jl_mulb(jl_mulb(fz0 - fz1, lmask(g, i, j, k + 1)), li);
+            double lap = 1.0 / volk * (ax_ + ay_ + az_);
+            Gc[n] = Gc[n] + lap * dT;
+        }
+    }
+    // tracer_sinking! (tracer_sinking.jl:1-42); flux_sink is zero on k <= Hz and k >= Nz+Hz
+    {
+        auto sink = [&](int n, double ws) {
+            const double* c = a.tr + n * G;
+            double fup = (k - 1 <= g.Hz || k - 1 >= g.Nz + g.Hz) ? 0.0 : ws * c[q - slab];
+            double fdn = (k >= g.Nz + g.Hz) ? 0.0 : ws * c[q];
+            return (fup - fdn) / dzC1(g, k - g.Hz) * dT;
+        };
+        Gc[PI_PFe_inorg] = Gc[PI_PFe_inorg] + sink(PI_PFe_inorg, b.w_sink_inorg);
+        Gc[PI_Dust] = Gc[PI_Dust] + sink(PI_Dust, b.w_sink_inorg);
+        Gc[PI_PFe_bio] = Gc[PI_PFe_bio] + sink(PI_PFe_bio, b.w_sink_org);
+    }
+    // tracer_forcing! (tracer_forcings.jl:2-50) on max(0, tracer)
+    {
+        double T[PI_NTRACERS];
+#pragma unroll
+        for (int n = 0; n < PI_NTRACERS; ++n) T[n] = jl_max(0.0, a.tr[n * G + q]);
+        Gc[PI_DIC] = Gc[PI_DIC] + T[PI_DOC] * b.kDOC * dT;
+        Gc[PI_DOC] = Gc[PI_DOC] - T[PI_DOC] * b.kDOC * dT + T[PI_POC] * b.kPOC * dT;
+        Gc[PI_POC] = Gc[PI_POC] - T[PI_POC] * b.kPOC * dT;
+        Gc[PI_NH4] = Gc[PI_NH4] + T[PI_DON] * b.kDON * dT - T[PI_NH4] * b.Nit * dT;
+        Gc[PI_NO3] = Gc[PI_NO3] + T[PI_NH4] * b.Nit * dT;
+        Gc[PI_DON] = Gc[PI_DON] - T[PI_DON] * b.kDON * dT + T[PI_PON] * b.kPON * dT;
+        Gc[PI_PON] = Gc[PI_PON] - T[PI_PON] * b.kPON * dT;
+        Gc[PI_PO4] = Gc[PI_PO4] + T[PI_DOP] * b.kDOP * dT;
+        Gc[PI_DOP] = Gc[PI_DOP] - T[PI_DOP] * b.kDOP * dT + T[PI_POP] * b.kPOP * dT;
+        Gc[PI_POP] = Gc[PI_POP] - T[PI_POP] * b.kPOP * dT;
+        Gc[PI_DFe] = Gc[PI_DFe] + T[PI_PFe_bio] * b.kPOC * dT
+                   - (b.lambda_POC * T[PI_POC] + b.lambda_min + b.lambda_dust * T[PI_Dust]) * T[PI_DFe] * b.DFeFrac * dT
+                   + T[PI_PFe_inorg] * b.kdiss * dT
+                   - jl_max((T[PI_DFe] - b.ligand), 0.0) * T[PI_DFe] * b.DFeFrac * b.lambda_Fe * dT;
+        Gc[PI_PFe_bio] = Gc[PI_PFe_bio] + T[PI_POC] * T[PI_DFe] * b.DFeFrac * b.lambda_POC * dT
+                       - b.kPOC * T[PI_PFe_bio] * dT;
+        Gc[PI_PFe_inorg] = Gc[PI_PFe_inorg] - T[PI_PFe_inorg] * b.kdiss * dT
+                         + (b.lambda_min + b.lambda_dust * T[PI_Dust]) * T[PI_DFe] * b.DFeFrac * dT
+                         + jl_max((T[PI_DFe] - b.ligand), 0.0) * T[PI_DFe] * b.DFeFrac * b.lambda_Fe * dT;
+    }
+    // apply_bcs! (apply_bcs.jl:4-98), faces in the reference's order
+    if (a.any_bc) {
+        int ii = i - g.Hx, jj = j - g.Hy, kk = k - g.Hz;
+        double axk = g.dy * dzF1(g, k), ayk = g.dx * dzF1(g, k);
+#pragma unroll
+        for (int n = 0; n < PI_NTRACERS; ++n) {
+            const FluxBCDev* B = a.bcs + n * 6;
+            if (B[PI_WEST].kind && i == 1 + g.Hx) Gc[n] += getbc_dev(B[PI_WEST], jj, kk, a.iter) * dT * axk / volk;
+            if (B[PI_EAST].kind && i == g.Nx + g.Hx) Gc[n] -= getbc_dev(B[PI_EAST], jj, kk, a.iter) * dT * axk / volk;
+            if (B[PI_SOUTH].kind && j == 1 + g.Hy) Gc[n] += getbc_dev(B[PI_SOUTH], ii, kk, a.iter) * dT * ayk / volk;
+            if (B[PI_NORTH].kind && j == g.Ny + g.Hy) Gc[n] -= getbc_dev(B[PI_NORTH], ii, kk, a.iter) * dT * ayk / volk;
+            if (B[PI_BOTTOM].kind && k == g.Nz + g.Hz) Gc[n] += getbc_dev(B[PI_BOTTOM], ii, jj, a.iter) * dT * az / volk;
+            if (B[PI_TOP].kind && k == 1 + g.Hz) Gc[n] -= getbc_dev(B[PI_TOP], ii, jj, a.iter) * dT * az / volk;
+        }
+    }
+    // plk: per-cell particle losses and consumption in reference summation order
+    double plk_DIC = 0.0, plk_NH4 = 0.0, plk_NO3 = 0.0, plk_PO4 = 0.0, plk_DOC = 0.0;
+    double plk_DON = 0.0, plk_DOP = 0.0, plk_POC = 0.0, plk_PON = 0.0, plk_POP = 0.0;
+    {
+        uint32_t p0 = a.off[q], p1 = a.off[q + 1];
+        uint32_t p = p0;
+        while (p < p1) {
+            uint32_t s = a.gid_sorted[p] / (uint32_t)a.C;
+            uint32_t e = p;
+            while (e < p1 && a.gid_sorted[e] / (uint32_t)a.C == s) ++e;
+            for (int pass = 1; pass <= 2; ++pass)
+                for (uint32_t r = p; r < e; ++r)
+                    if (a.evk[r] == pass) {
+                        const double* L = a.loss + (long long)r * 6;
+                        plk_DOC += L[0]; plk_DON += L[1]; plk_DOP += L[2];
+                        plk_POC += L[3]; plk_PON += L[4]; plk_POP += L[5];
+                    }
+            for (uint32_t r = p; r < e; ++r) {
+                const double* K = a.contrib + (long long)r * 5;
+                plk_DIC += K[0]; plk_DOC += K[1]; plk_NH4 += K[2]; plk_NO3 += K[3]; plk_PO4 += K[4];
             }
+            p = e;
         }
-        // tracer_diffusion! (κ∇², tracer_diffusion.jl:1-21) on the original tracer
-        if (a.diffuse) {
-            double kx = b.kappa_h, ky = b.kappa_h, kz = b.kappa_v;
-            double axk = g.dy * dzF1(g, k), ayk = g.dx * dzF1(g, k);
-            int li = lmask(g, i, j, k);
-            for (int n = 0; n < PI_NTRACERS; ++n) {
-                const double* c = a.tr + n * G;
-                auto dx0 = [&](int ii) { return jl_mulb(jl_mulb(c[gidx(g, ii, j, k)] - c[gidx(g, ii - 1, j, k)], lmask(g, ii, j, k)), lmask(g, ii - 1, j, k)); };
-                auto dy0 = [&](int jj) { return jl_mulb(jl_mulb(c[gidx(g, i, jj, k)] - c[gidx(g, i, jj - 1, k)], lmask(g, i, jj, k)), lmask(g, i, jj - 1, k)); };
-                auto dz0 = [&](int kk) { return jl_mulb(jl_mulb(c[gidx(g, i, j, kk - 1)] - c[gidx(g, i, j, kk)], lmask(g, i, j, kk)), lmask(g, i, j, kk - 1)); };
-                double fx1 = kx * axk * (dx0(i + 1) / g.dx), fx0 = kx * axk * (dx0(i) / g.dx);
-                double fy1 = ky * ayk * (dy0(j + 1) / g.dy), fy0 = ky * ayk * (dy0(j) / g.dy);
-                double fz0 = kz * az * (dz0(k) / dzF1(g, k)), fz1 = kz * az * (dz0(k + 1) / dzF1(g, k + 1));
-                double ax_ = jl_mulb(jl_mulb(fx1 - fx0, lmask(g, i + 1, j, k)), li);
-                double ay_ = jl_mulb(jl_mulb(fy1 - fy0, lmask(g, i, j + 1, k)), li);
-                double az_ = jl_mulb(jl_mulb(fz0 - fz1, lmask(g, i, j, k + 1)), li);
-                double lap = 1.0 / volk * (ax_ + ay_ + az_);
-                Gc[n] = Gc[n] + lap * dT;
-            }
-        }
-        // tracer_sinking! (tracer_sinking.jl:1-42); flux_sink is zero on k <= Hz and k >= Nz+Hz
-        {
-            const int names[3] = { PI_PFe_inorg, PI_Dust, PI_PFe_bio };
-            for (int m = 0; m < 3; ++m) {
-                int n = names[m];
-                double ws = m < 2 ? b.w_sink_inorg : b.w_sink_org;
-                const double* c = a.tr + n * G;
-                double fup = (k - 1 <= g.Hz || k - 1 >= g.Nz + g.Hz) ? 0.0 : ws * c[q - g.Gx * g.Gy];
-                double fdn = (k >= g.Nz + g.Hz) ? 0.0 : ws * c[q];
-                Gc[n] = Gc[n] + (fup - fdn) / dzC1(g, k - g.Hz) * dT;
-            }
-        }
-        // tracer_forcing! (tracer_forcings.jl:2-50) on max(0, tracer)
-        {
-            double T[PI_NTRACERS];
-            for (int n = 0; n < PI_NTRACERS; ++n) T[n] = jl_max(0.0, a.tr[n * G + q]);
-            Gc[PI_DIC] = Gc[PI_DIC] + T[PI_DOC] * b.kDOC * dT;
-            Gc[PI_DOC] = Gc[PI_DOC] - T[PI_DOC] * b.kDOC * dT + T[PI_POC] * b.kPOC * dT;
-            Gc[PI_POC] = Gc[PI_POC] - T[PI_POC] * b.kPOC * dT;
-            Gc[PI_NH4] = Gc[PI_NH4] + T[PI_DON] * b.kDON * dT - T[PI_NH4] * b.Nit * dT;
-            Gc[PI_NO3] = Gc[PI_NO3] + T[PI_NH4] * b.Nit * dT;
-            Gc[PI_DON] = Gc[PI_DON] - T[PI_DON] * b.kDON * dT + T[PI_PON] * b.kPON * dT;
-            Gc[PI_PON] = Gc[PI_PON] - T[PI_PON] * b.kPON * dT;
-            Gc[PI_PO4] = Gc[PI_PO4] + T[PI_DOP] * b.kDOP * dT;
-            Gc[PI_DOP] = Gc[PI_DOP] - T[PI_DOP] * b.kDOP * dT + T[PI_POP] * b.kPOP * dT;
-            Gc[PI_POP] = Gc[PI_POP] - T[PI_POP] * b.kPOP * dT;
-            Gc[PI_DFe] = Gc[PI_DFe] + T[PI_PFe_bio] * b.kPOC * dT
-                       - (b.lambda_POC * T[PI_POC] + b.lambda_min + b.lambda_dust * T[PI_Dust]) * T[PI_DFe] * b.DFeFrac * dT
-                       + T[PI_PFe_inorg] * b.kdiss * dT
-                       - jl_max((T[PI_DFe] - b.ligand), 0.0) * T[PI_DFe] * b.DFeFrac * b.lambda_Fe * dT;
-            Gc[PI_PFe_bio] = Gc[PI_PFe_bio] + T[PI_POC] * T[PI_DFe] * b.DFeFrac * b.lambda_POC * dT
-                           - b.kPOC * T[PI_PFe_bio] * dT;
-            Gc[PI_PFe_inorg] = Gc[PI_PFe_inorg] - T[PI_PFe_inorg] * b.kdiss * dT
-                             + (b.lambda_min + b.lambda_dust * T[PI_Dust]) * T[PI_DFe] * b.DFeFrac * dT
-                             + jl_max((T[PI_DFe] - b.ligand), 0.0) * T[PI_DFe] * b.DFeFrac * b.lambda_Fe * dT;
-        }
-        // apply_bcs! (apply_bcs.jl:4-98), faces in the reference's order
-        if (a.any_bc) {
-            int ii = i - g.Hx, jj = j - g.Hy, kk = k - g.Hz;
-            double axk = g.dy * dzF1(g, k), ayk = g.dx * dzF1(g, k);
-            for (int n = 0; n < PI_NTRACERS; ++n) {
-                const FluxBCDev* B = a.bcs + n * 6;
-                if (B[PI_WEST].kind && i == 1 + g.Hx) Gc[n] += getbc_dev(B[PI_WEST], jj, kk, a.iter) * dT * axk / volk;
-                if (B[PI_EAST].kind && i == g.Nx + g.Hx) Gc[n] -= getbc_dev(B[PI_EAST], jj, kk, a.iter) * dT * axk / volk;
-                if (B[PI_SOUTH].kind && j == 1 + g.Hy) Gc[n] += getbc_dev(B[PI_SOUTH], ii, kk, a.iter) * dT * ayk / volk;
-                if (B[PI_NORTH].kind && j == g.Ny + g.Hy) Gc[n] -= getbc_dev(B[PI_NORTH], ii, kk, a.iter) * dT * ayk / volk;
-                if (B[PI_BOTTOM].kind && k == g.Nz + g.Hz) Gc[n] += getbc_dev(B[PI_BOTTOM], ii, jj, a.iter) * dT * az / volk;
-                if (B[PI_TOP].kind && k == 1 + g.Hz) Gc[n] -= getbc_dev(B[PI_TOP], ii, jj, a.iter) * dT * az / volk;
-            }
-        }
-        // plk: per-cell particle losses and consumption in reference summation order
-        double plk[PI_NTRACERS];
-        for (int n = 0; n < PI_NTRACERS; ++n) plk[n] = 0.0;
-        {
-            uint32_t p0 = a.off[q], p1 = a.off[q + 1];
-            uint32_t p = p0;
-            while (p < p1) {
-                uint32_t s = a.gid_sorted[p] / (uint32_t)a.C;
-                uint32_t e = p;
-                while (e < p1 && a.gid_sorted[e] / (uint32_t)a.C == s) ++e;
-                for (int pass = 1; pass <= 2; ++pass)
-                    for (uint32_t r = p; r < e; ++r)
-                        if (a.evk[r] == pass) {
-                            const double* L = a.loss + (long long)r * 6;
-                            plk[PI_DOC] += L[0]; plk[PI_DON] += L[1]; plk[PI_DOP] += L[2];
-                            plk[PI_POC] += L[3]; plk[PI_PON] += L[4]; plk[PI_POP] += L[5];
-                        }
-                for (uint32_t r = p; r < e; ++r) {
-                    const double* K = a.contrib + (long long)r * 5;
-                    plk[PI_DIC] += K[0]; plk[PI_DOC] += K[1]; plk[PI_NH4] += K[2];
-                    plk[PI_NO3] += K[3]; plk[PI_PO4] += K[4];
-                }
-                p = e;
-            }
-        }
-        for (int n = 0; n < PI_NTRACERS; ++n)            // apply_tendency!
-            a.tr_next[n * G + q] = a.tr[n * G + q] + (Gc[n] + plk[n] / volk);
+    }
+    // apply_tendency!: tracer += Gc + plk / volume
+#pragma unroll
+    for (int n = 0; n < PI_NTRACERS; ++n) {
+        double pk = n == PI_DIC ? plk_DIC : n == PI_NH4 ? plk_NH4 : n == PI_NO3 ? plk_NO3 : n == PI_PO4 ? plk_PO4
+                  : n == PI_DOC ? plk_DOC : n == PI_DON ? plk_DON : n == PI_DOP ? plk_DOP : n == PI_POC ? plk_POC
+                  : n == PI_PON ? plk_PON : n == PI_POP ? plk_POP : 0.0;
+        a.tr_next[n * G + q] = a.tr[n * G + q] + (Gc[n] + pk / volk);
     }
 }
 

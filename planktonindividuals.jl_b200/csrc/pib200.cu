@@ -9,7 +9,8 @@
 //   k_par                Chl per cell, calc_par! down each column, PAR diagnostic
 //   per species:         k_decide → scan(flags) → k_lists → k_daughters → k_physiology
 //   k_sweep_x/y          DST3FL sweeps on tracer_temp
-//   k_sweep_z_final      z sweep + tendency, diffusion, sinking, forcing, BCs, particle terms
+//   k_sweep_z            z sweep and the advective tendency
+//   k_tracer_tail        diffusion, sinking, forcing, BCs, particle terms, apply_tendency!
 //   k_halo<x,y,z>        fill_halo_tracer! on the new tracers
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
@@ -155,6 +156,7 @@ struct pi_model {
     double* PARF = nullptr;      // Nx·Ny
     double* temp_own = nullptr;  // G
     double* stage = nullptr;     // 3 × G staging for interior uploads
+    double* velh[3] = {nullptr, nullptr, nullptr};   // vel½
     const double* temp = nullptr;
     double* diag_par = nullptr;  // G
     double* diag_sp = nullptr;   // nsp × 4 × G (num, graz, mort, dvid)
@@ -301,7 +303,16 @@ pi_status enqueue_step(pi_model* m, double dT) {
     const int BS = 256;
 
     CK(cudaMemsetAsync(sb.cnt, 0, (G + 1) * sizeof(uint32_t), st), "zero counts");
-    VelPtrs vp{m->vel0[0], m->vel0[1], m->vel0[2], m->vel1[0], m->vel1[1], m->vel1[2]};
+    { ProfScope ps_(m, "k_velhalf");
+    k_velhalf<<<148 * 8, 256, 0, st>>>(G, m->vel0[0], m->vel0[1], m->vel0[2], m->vel1[0], m->vel1[1], m->vel1[2],
+                                       m->velh[0], m->velh[1], m->velh[2], sb.err);
+    CK(cudaGetLastError(), "k_velhalf"); }
+    VelPtrs vp{m->vel0[0], m->vel0[1], m->vel0[2], m->velh[0], m->velh[1], m->velh[2],
+               m->vel1[0], m->vel1[1], m->vel1[2]};
+    { ProfScope ps_(m, "k_particles_sorted");
+    k_particles_sorted<<<nblk(NC, 128), 128, 0, st>>>(g, m->d_spc, C, sb.gid_sorted, sb.off, G, dT, m->seed, iter, vp,
+                                                      m->bgc.kappa_hP, m->bgc.kappa_vP, sb.cnt, sb.key, sb.err);
+    CK(cudaGetLastError(), "k_particles_sorted"); }
     { ProfScope ps_(m, "k_particles");
     k_particles<<<nblk(NC, BS), BS, 0, st>>>(g, m->d_spc, m->nsp, C, dT, m->seed, iter, vp,
                                              m->bgc.kappa_hP, m->bgc.kappa_vP, sb.cnt, sb.key,
@@ -351,12 +362,11 @@ pi_status enqueue_step(pi_model* m, double dT) {
         CK(cudaGetLastError(), "k_physiology"); }
     }
     {
-        dim3 grid(nblk(g.Nx, 128), g.Ny, g.Nz);
         { ProfScope ps_(m, "k_sweep_x");
-        k_sweep_x<<<grid, 128, 0, st>>>(g, m->tr, m->tta, m->vel1[0], dT, sb.err);
+        k_sweep_x<<<dim3(nblk(nblk(g.Nx, 31), SWX_WARPS), g.Ny, g.Nz), 32 * SWX_WARPS, 0, st>>>(g, m->tr, m->tta, m->vel1[0], dT, sb.err);
         CK(cudaGetLastError(), "k_sweep_x"); }
         { ProfScope ps_(m, "k_sweep_y");
-        k_sweep_y<<<grid, 128, 0, st>>>(g, m->tr, m->tta, m->ttb, m->vel1[1], dT, sb.err);
+        k_sweep_y<<<dim3(nblk(g.Nx, 32), nblk(nblk(g.Ny, SWY_L), SWY_TY), g.Nz), dim3(32, SWY_TY), 0, st>>>(g, m->tr, m->tta, m->ttb, m->vel1[1], dT, sb.err);
         CK(cudaGetLastError(), "k_sweep_y"); }
         ZFinalArgs za;
         za.g = g; za.tr = m->tr; za.ttb = m->ttb; za.tr_next = m->tr_next; za.w = m->vel1[2];
@@ -365,10 +375,14 @@ pi_status enqueue_step(pi_model* m, double dT) {
         za.any_bc = m->any_bc; za.bcs = m->d_bcs; za.iter = m->iteration;
         za.spc = m->d_spc; za.C = C; za.off = sb.off; za.gid_sorted = sb.gid_sorted; za.evk = sb.evk;
         za.loss = sb.loss; za.contrib = sb.contrib; za.nsp = m->nsp; za.err = sb.err;
-        dim3 g2(nblk(g.Nx, 64), g.Ny);
-        { ProfScope ps_(m, "k_sweep_z_final");
-        k_sweep_z_final<<<g2, 64, 0, st>>>(za);
-        CK(cudaGetLastError(), "k_sweep_z_final"); }
+        za.gadv = m->tta;      // the x-sweep output is no longer needed
+        { ProfScope ps_(m, "k_sweep_z");
+        k_sweep_z<<<dim3(nblk(g.Nx, 32), g.Ny, nblk(nblk(g.Nz, SWZ_L), SWZ_TZ)), dim3(32, SWZ_TZ), 0, st>>>(
+            g, m->tr, m->ttb, m->tta, m->vel1[2], dT, sb.err);
+        CK(cudaGetLastError(), "k_sweep_z"); }
+        { ProfScope ps_(m, "k_tracer_tail");
+        k_tracer_tail<<<dim3(nblk(g.Nx, 128), g.Ny, g.Nz), 128, 0, st>>>(za);
+        CK(cudaGetLastError(), "k_tracer_tail"); }
         // tracers are only replaced when the step completed (a capacity error leaves them)
         { ProfScope ps_(m, "k_halo");
         k_halo<0><<<dim3(nblk(g.Gy, 64), g.Gz, PI_NTRACERS), 64, 0, st>>>(g, m->tr_next, PI_NTRACERS, sb.err);
@@ -504,6 +518,7 @@ pi_status pi_create(const pi_grid* grid, const pi_bgc_params* bgc, const pi_quot
     ALB(m->tta, PI_NTRACERS * G); ALB(m->ttb, PI_NTRACERS * G);
     for (int b = 0; b < 2; ++b) for (int c = 0; c < 3; ++c) ALB(m->velbuf[b][c], G);
     ALB(m->stage, 3 * G);
+    for (int c = 0; c < 3; ++c) ALB(m->velh[c], G);
     ALB(m->zeros, G); ALB(m->par, G); ALB(m->PARF, (long long)hg.Nx * hg.Ny); ALB(m->temp_own, G);
     ALB(m->diag_par, G); ALB(m->diag_sp, 4LL * nspecies * G);
     StepBufs& sb = m->sb;
@@ -537,6 +552,7 @@ pi_status pi_create(const pi_grid* grid, const pi_bgc_params* bgc, const pi_quot
     ok = ok && cudaMemsetAsync(m->PARF, 0, hg.Nx * (size_t)hg.Ny * sizeof(double), s0) == cudaSuccess;
     ok = ok && cudaMemsetAsync(m->diag_sp, 0, 4 * nspecies * G * sizeof(double), s0) == cudaSuccess;
     ok = ok && cudaMemsetAsync(sb.cnt, 0, (G + 1) * sizeof(uint32_t), s0) == cudaSuccess;
+    ok = ok && cudaMemsetAsync(sb.off, 0, (G + 1) * sizeof(uint32_t), s0) == cudaSuccess;
     ok = ok && cudaMemsetAsync(sb.err, 0, sizeof(uint32_t), s0) == cudaSuccess;
     ok = ok && cudaMemsetAsync(sb.err_iter, 0, sizeof(int64_t), s0) == cudaSuccess;
     for (int s = 0; s < nspecies; ++s) {
@@ -614,6 +630,7 @@ pi_status pi_set_individuals(pi_model* m, int32_t sp, const pi_individuals* in) 
         CK(cudaMemcpyAsync(dptr[q], dcols[q], C * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload individuals");
     CK(cudaMemcpyAsync(P.flags, flags.data(), C, cudaMemcpyHostToDevice, m->stream), "upload flags");
     CK(cudaMemcpyAsync(P.cell, cell.data(), C * sizeof(int32_t), cudaMemcpyHostToDevice, m->stream), "upload cells");
+    CK(cudaMemsetAsync(P.stat, 0, C, m->stream), "reset step status");
     CK(cudaStreamSynchronize(m->stream), "synchronize");
     return PI_OK;
 }
@@ -704,6 +721,27 @@ pi_status pi_set_velocity(pi_model* m, const double* u, const double* v, const d
     CK(cudaStreamSynchronize(m->stream), "synchronize");
     for (int c = 0; c < 3; ++c) m->vel1[c] = m->velbuf[b][c];
     m->vel1_buf = b;
+    return PI_OK;
+}
+
+pi_status pi_set_velocity0(pi_model* m, const double* u, const double* v, const double* w) {
+    if (!m || !u || !v || !w) return fail(m, PI_ERR_ARG, "pi_set_velocity0: NULL argument");
+    // write into the own buffer that vel₁ does not alias
+    int b = (m->vel1[0] == m->velbuf[0][0]) ? 1 : 0;
+    const HostGrid& g = m->hg;
+    if (g.Nx >= g.Hx && g.Ny >= g.Hy && g.Nz >= g.Hz) {
+        pi_status st = device_vel_copy(m, u, v, w, m->velbuf[b][0], m->velbuf[b][1], m->velbuf[b][2]);
+        if (st) return st;
+    } else {
+        std::vector<double> U, V, W;
+        host_vel_copy(g, u, v, w, U, V, W);
+        const size_t bytes = g.G * sizeof(double);
+        CK(cudaMemcpyAsync(m->velbuf[b][0], U.data(), bytes, cudaMemcpyHostToDevice, m->stream), "upload u");
+        CK(cudaMemcpyAsync(m->velbuf[b][1], V.data(), bytes, cudaMemcpyHostToDevice, m->stream), "upload v");
+        CK(cudaMemcpyAsync(m->velbuf[b][2], W.data(), bytes, cudaMemcpyHostToDevice, m->stream), "upload w");
+    }
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    for (int c = 0; c < 3; ++c) m->vel0[c] = m->velbuf[b][c];
     return PI_OK;
 }
 
