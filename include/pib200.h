@@ -229,6 +229,92 @@ pi_status pi_last_error(pi_model* m, char* buf, size_t len);
 /* Static description of a status code. */
 const char* pi_status_string(pi_status code);
 
+/* ---------------------------------------------------------------------------------------------
+ * Batched FP32 form. A batch holds independent members, each a PlanktonModel of its own (grid,
+ * parameters, capacity, individuals, tracers, forcing, seed), that are advanced together: every
+ * phase of TimeStep! is one launch over all members, and the step is replayed from a CUDA graph.
+ * The reference runs such ensembles as separate models one after another (no batch API); each
+ * member here computes what pi_create(..., PI_FP32, ...) followed by the same calls computes for
+ * it alone, bit for bit. All members share nspecies and the time step ΔT.
+ * --------------------------------------------------------------------------------------------- */
+typedef struct pi_batch pi_batch;
+
+typedef struct {
+    const pi_grid* grid;
+    const pi_bgc_params* bgc;
+    const pi_quota_params* species;   /* nspecies entries */
+    int64_t capacity;                 /* max_individuals per species */
+    uint64_t seed;                    /* key of the member's random draws */
+} pi_member;
+
+/* PlanktonModel(...) for every member (src/Model/models.jl:51-155), FP32 form. */
+pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t nspecies, pi_batch** out);
+pi_status pi_batch_destroy(pi_batch* b);
+
+/* As pi_set_individuals / pi_get_individuals for one member. */
+pi_status pi_batch_set_individuals(pi_batch* b, int32_t member, int32_t sp, const pi_individuals* in);
+pi_status pi_batch_get_individuals(pi_batch* b, int32_t member, int32_t sp, pi_individuals* out);
+/* As pi_set_tracer / pi_get_tracer for one member (halo-padded, Float64 at the boundary). */
+pi_status pi_batch_set_tracer(pi_batch* b, int32_t member, int32_t idx, const double* data);
+pi_status pi_batch_get_tracer(pi_batch* b, int32_t member, int32_t idx, double* out);
+/* As pi_set_velocity / pi_set_velocity0 / pi_set_PARF / pi_set_temp / pi_set_flux_bc. */
+pi_status pi_batch_set_velocity(pi_batch* b, int32_t member, const double* u, const double* v, const double* w);
+pi_status pi_batch_set_velocity0(pi_batch* b, int32_t member, const double* u, const double* v, const double* w);
+pi_status pi_batch_set_PARF(pi_batch* b, int32_t member, const double* parf);
+pi_status pi_batch_set_temp(pi_batch* b, int32_t member, const double* temp);
+pi_status pi_batch_set_flux_bc(pi_batch* b, int32_t member, int32_t tracer, int32_t face, int32_t kind,
+                               const double* values, int64_t nt);
+
+/* PlanktonSimulation's forcing arrays for one member (src/Model/simulations.jl:51-97), kept on the
+ * device: u, v, w snapshots (nvel; NULL for none), PARF (npar snapshots of Nx*Ny) and temperature
+ * (ntemp snapshots of Nx*Ny*Nz), each with its own interval. Every following step picks its
+ * snapshots as update! does (src/Simulation/update.jl:14-26) from model.t, or from the step index
+ * within the pi_batch_step call for the bits of `time_offset` set (1 vel, 2 PAR, 4 temp). */
+pi_status pi_batch_set_series(pi_batch* b, int32_t member,
+                              const double* u, const double* v, const double* w, int64_t nvel, double dT_vel,
+                              const double* parf, int64_t npar, double dT_PAR,
+                              const double* temp, int64_t ntemp, double dT_temp, int32_t time_offset);
+/* update!(sim; time_offset) for the following steps: bits 1 vel, 2 PAR, 4 temp index the series by
+ * the step within the pi_batch_step call instead of model.t. */
+pi_status pi_batch_set_time_offset(pi_batch* b, int32_t member, int32_t time_offset);
+/* Drops a member's series; the snapshots bound for the next step are kept as its own fields. */
+pi_status pi_batch_clear_series(pi_batch* b, int32_t member);
+
+/* `nsteps` TimeStep!s of every member (graph replay). With sync = 0 the call returns after
+ * queueing; pi_batch_synchronize reports errors. A division overflow in any member stops the
+ * whole batch at that step with PI_ERR_CAPACITY and the reference's message. */
+pi_status pi_batch_step(pi_batch* b, double dT, int64_t nsteps, int32_t sync);
+pi_status pi_batch_synchronize(pi_batch* b);
+
+/* model.iteration and model.t (shared by all members). */
+pi_status pi_batch_get_time(pi_batch* b, int64_t* iteration, double* t);
+pi_status pi_batch_set_time(pi_batch* b, int64_t iteration, double t);
+
+/* Active individuals of one member and species (sp = -1: all species; member = -1: all members). */
+pi_status pi_batch_count_active(pi_batch* b, int32_t member, int32_t sp, int64_t* n);
+/* As pi_get_diag / pi_reset_diags. */
+pi_status pi_batch_get_diag(pi_batch* b, int32_t member, int32_t kind, int32_t sp, double* out);
+pi_status pi_batch_reset_diags(pi_batch* b);
+
+/* FP64 mass budgets of one member (mmol): out[0..2] = Σ volume·tracer over the interior for
+ * carbon (DIC+DOC+POC), nitrogen (NH4+NO3+DON+PON) and phosphorus (PO4+DOP+POP); out[3..5] = the
+ * active individuals' C (Bm+Cq), N (Bm·R_NC+Nq) and P (Bm·R_PC+Pq). No counterpart in the
+ * reference, which has no budget call. */
+pi_status pi_batch_budget(pi_batch* b, int32_t member, double out[6]);
+
+/* Launch-shape autotuner (no counterpart in the reference): times `steps_per_candidate` real
+ * steps of ΔT for each candidate block size, tiles-per-block mode and sweep segment length, and
+ * keeps the fastest per kernel. The steps it takes are ordinary steps of the model (results do
+ * not depend on launch shapes). `report` (may be NULL) receives one line per choice. */
+pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t steps_per_candidate, char* report, size_t report_len);
+
+/* As pi_get_stream / pi_profile_enable / pi_profile_read / pi_last_error. */
+pi_status pi_batch_get_stream(pi_batch* b, void** stream);
+pi_status pi_batch_profile_enable(pi_batch* b, int32_t on);
+pi_status pi_batch_profile_read(pi_batch* b, int32_t max, char* names, size_t names_len,
+                                int64_t* launches, double* ms, int32_t* n);
+pi_status pi_batch_last_error(pi_batch* b, char* buf, size_t len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -825,7 +825,8 @@ void tracer_forcing(orc_model* m, double dT) {
 inline double getbc(const FluxBC& bc, int n1, int n2, long a, long b, int64_t it) {
     if (bc.kind == PI_BC_CONST) return bc.v[0];
     if (bc.kind == PI_BC_ARRAY2D) return bc.v[(size_t)(a - 1) + (size_t)n1 * (size_t)(b - 1)];
-    return bc.v[(size_t)(a - 1) + (size_t)n1 * ((size_t)(b - 1) + (size_t)n2 * (size_t)(it - 1))];
+    const int64_t t = it < 1 ? 1 : (it > bc.nt ? bc.nt : it);   /* Julia would raise a BoundsError */
+    return bc.v[(size_t)(a - 1) + (size_t)n1 * ((size_t)(b - 1) + (size_t)n2 * (size_t)(t - 1))];
 }
 
 /* apply_bcs!, HaloRegions/apply_bcs.jl:4-98 */

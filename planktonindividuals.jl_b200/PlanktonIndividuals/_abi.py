@@ -75,6 +75,11 @@ class pi_individuals(ct.Structure):
                 ("graz", _dp), ("mort", _dp), ("dvid", _dp)]
 
 
+class pi_member(ct.Structure):
+    _fields_ = [("grid", ct.POINTER(pi_grid)), ("bgc", ct.POINTER(pi_bgc_params)),
+                ("species", ct.POINTER(pi_quota_params)), ("capacity", ct.c_int64), ("seed", ct.c_uint64)]
+
+
 def declare(lib, prefix):
     """Attach argtypes/restype for the pi_* (or mirrored) entry points found in `lib`."""
     P = ct.c_void_p

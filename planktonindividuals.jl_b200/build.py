@@ -2,8 +2,12 @@
 
     python planktonindividuals.jl_b200/build.py
 
--fmad=false keeps every multiply and add separately rounded so the Float64 path produces the
-same bits as the CPU oracle, which is compiled with -ffp-contract=off.
+Each translation unit has its own floating-point flags:
+  pib200.cu  (FP64 form)  -fmad=false keeps every multiply and add separately rounded so the
+                          Float64 path produces the same bits as the CPU oracle, which is compiled
+                          with -ffp-contract=off;
+  fp32.cu    (FP32 form)  default contraction: fused multiply-adds are faster and more accurate,
+                          and the FP32 form is compared with the oracle within a tolerance.
 """
 import os
 import shutil
@@ -13,8 +17,11 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "PlanktonIndividuals", "libpib200.so")
-SOURCES = ["pib200.cu"]
-DEPS = ["pib200.cu", "kernels_fp64.cuh", "pib200_internal.h", "noalloc.cu"]
+SOURCES = {"pib200.cu": ["-fmad=false", "-Xcompiler", "-ffp-contract=off"],
+           "fp32.cu": []}
+DEPS = ["pib200.cu", "kernels_fp64.cuh", "pib200_internal.h", "noalloc.cu", "host_common.h",
+        "fp32.cu", "kernels_fp32.cuh", "fp32_internal.h"]
+BUILD_DIR = os.path.join(HERE, "_build")
 
 
 def nvcc():
@@ -44,16 +51,22 @@ def needs_build():
 def build(force=False, verbose=False):
     if not force and not needs_build():
         return OUT
-    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-fmad=false",
-           "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-shared",
-           "-o", OUT] + [os.path.join(CSRC, s) for s in SOURCES]
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    base = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
+            "-Xcompiler", "-fPIC"]
     hc = host_compiler()
     if hc:
-        cmd[1:1] = ["-ccbin", hc]
-    if verbose:
-        cmd.append("-Xptxas=-v")
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+        base[1:1] = ["-ccbin", hc]
+    objs = []
+    for src, flags in SOURCES.items():
+        obj = os.path.join(BUILD_DIR, src.replace(".cu", ".o"))
+        cmd = base + flags + ["-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            cmd.append("-Xptxas=-v")
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        objs.append(obj)
+    subprocess.run(base + ["-shared", "-o", OUT] + objs, check=True)
     return OUT
 
 

@@ -1,0 +1,1277 @@
+// libpib200 — FP32 form: batches of independent members stepped together (pi_batch_* of
+// include/pib200.h). A PlanktonModel created with PI_FP32 is a batch of one member.
+//
+// One step is this sequence of launches, each covering every member:
+//   k32_bind             forcing of the step from device-resident series; vel½ buffer choice
+//   k32_velhalf          vel½ for members whose vel₀ and vel₁ differ
+//   k32_move             RK4 + diffusion + find_inds!, pop/Chl sums, previous decisions, tile counts
+//   k32_par              calc_par! down each column
+//   scan(tile counts)    division and free-slot offsets of every tile
+//   k32_assign           k-th divider → k-th free slot per (member, species) segment
+//   k32_daughters        copy_daughter_individuals! + divide_to_half!
+//   k32_physiology       QuotaMode growth, consumption sums, decisions for the next step
+//   k32_sweep_x/y/z      DST3FL sweeps, advective tendency
+//   k32_tail             diffusion, sinking, forcing, BCs, particle terms, apply_tendency!
+//   k32_halo<x,y,z>      fill_halo_tracer!
+//   k32_end_step         vel₀ ← vel₁, iteration and t
+// Nothing in a step reads a host value, so the step is captured once as a CUDA graph (one per
+// tracer-buffer parity) and replayed. The results do not depend on block shapes, tile-per-block
+// assignment or sweep segment lengths (integer sums commute; every other value is computed by
+// exactly one thread from the same inputs), which lets the autotuner time real steps.
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kernels_fp32.cuh"
+#include "host_common.h"
+
+using namespace p32;
+using namespace pih;
+
+namespace {
+
+thread_local std::string g_batch_error;
+
+inline unsigned nblk(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+struct HostBC {
+    int kind = PI_BC_NONE;
+    long long nt = 0;
+    float* v = nullptr;
+};
+
+struct MemberHost {
+    HostGrid g;
+    long long C = 0;
+    uint64_t seed = 0;
+    pi_bgc_params bgc{};
+    std::vector<pi_quota_params> sp;
+    int all_water = 1;
+    // device-resident forcing series (owned), or none
+    float* ser_vel = nullptr;
+    float* ser_parf = nullptr;
+    float* ser_temp = nullptr;
+    HostBC bcs[PI_NTRACERS][6];
+};
+
+struct Tuning {
+    int bs_move = 256, bs_phys = 256, bs_assign = 256;
+    int persist_move = 0, persist_phys = 0;   // 0: one tile per block; k: k blocks per SM, looping
+    int Ly = 8, Lz = 8;
+    int wpb_x = 4, wpb_y = 4, wpb_z = 4, wpb_tail = 4, wpb_par = 4;
+};
+
+}  // namespace
+
+struct pi_batch {
+    int device = 0;
+    int nsm = 148;
+    cudaStream_t stream = nullptr;
+    int nm = 0, nsp = 0, nseg = 0;
+    std::vector<MemberHost> mh;
+    std::vector<MemberDev> mdh;
+    std::vector<MemberSeries> serh;
+    std::vector<FluxBC32> bch;
+    std::string err;
+    std::vector<void*> allocs;
+    long long Gtot = 0, Stot = 0, ncol = 0, maxG = 0;
+    int nlev = 0;
+    // device
+    MemberDev* md = nullptr;
+    SpeciesDev32* sp = nullptr;
+    BgcDev32* bgc = nullptr;
+    FluxBC32* bcs = nullptr;
+    MemberForcing* F = nullptr;
+    MemberSeries* S = nullptr;
+    StepState* st = nullptr;
+    uint32_t* errw = nullptr;
+    float* trbuf[2] = {nullptr, nullptr};
+    int cur = 0;                    // trbuf[cur] holds the current tracers
+    float *ta = nullptr, *tb = nullptr;
+    float *par = nullptr, *diag_par = nullptr, *PARF = nullptr;
+    float *dzF = nullptr, *dzC = nullptr;
+    uint8_t* lm = nullptr;
+    float* velown = nullptr;        // 6 planes of Gtot: buffer b, component c at (b*3+c)*Gtot
+    float* velh = nullptr;          // 3 planes of Gtot
+    float* tempown = nullptr;       // Gtot
+    uint32_t* dcnt = nullptr;
+    int* pop = nullptr;
+    int* pop_sp = nullptr;
+    unsigned long long* acc = nullptr;
+    unsigned long long* chl_acc = nullptr;
+    IndDev32 P{};
+    int ntiles = 0;
+    int2* tiles = nullptr;
+    int* seg_tile0 = nullptr;
+    unsigned long long *tile_cnt = nullptr, *tile_off = nullptr;
+    int *divlist = nullptr, *freelist = nullptr;
+    uint32_t* ndiv = nullptr;
+    long long* line_off[3] = {nullptr, nullptr, nullptr};
+    long long nlines[3] = {0, 0, 0};
+    double last_dT = 0.0;
+    char* cub_tmp = nullptr;
+    size_t cub_bytes = 0;
+    double* stage = nullptr;        // maxG doubles of upload staging
+    double* partial = nullptr;      // budget partials
+    unsigned long long* scratch = nullptr;
+    // work tables (device) built for the current tuning
+    Tab32 T{};
+    std::vector<void*> table_allocs;
+    int tables_Ly = -1, tables_Lz = -1;
+    Tuning tune;
+    // graphs
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    double graph_dT = -1.0;
+    int use_graph = 1;
+    // profiling
+    int profiling = 0;
+    struct Mark { const char* name; cudaEvent_t a, b; };
+    std::vector<Mark> marks;
+    std::vector<cudaEvent_t> event_pool;
+    std::vector<std::string> prof_names;
+    std::vector<int64_t> prof_count;
+    std::vector<double> prof_ms;
+};
+
+namespace {
+
+pi_status bfail(pi_batch* b, pi_status code, const std::string& msg) {
+    if (b) b->err = msg; else g_batch_error = msg;
+    return code;
+}
+pi_status bcuda(pi_batch* b, cudaError_t e, const char* what) {
+    return bfail(b, e == cudaErrorMemoryAllocation ? PI_ERR_NOMEM : PI_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define BK(call, what)                                              \
+    do {                                                            \
+        cudaError_t e_ = (call);                                    \
+        if (e_ != cudaSuccess) return bcuda(b, e_, what);           \
+    } while (0)
+
+template <typename T>
+pi_status balloc(pi_batch* b, T** p, size_t n, const char* what, std::vector<void*>* list = nullptr) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess) return bcuda(b, e, what);
+    (list ? *list : b->allocs).push_back(q);
+    *p = (T*)q;
+    return PI_OK;
+}
+
+cudaEvent_t take_event(pi_batch* b) {
+    if (!b->event_pool.empty()) { cudaEvent_t e = b->event_pool.back(); b->event_pool.pop_back(); return e; }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+
+struct BScope {
+    pi_batch* b;
+    pi_batch::Mark mk;
+    bool on;
+    BScope(pi_batch* b_, const char* name) : b(b_), on(b_->profiling != 0) {
+        if (!on) return;
+        mk.name = name; mk.a = take_event(b); mk.b = take_event(b);
+        cudaEventRecord(mk.a, b->stream);
+    }
+    ~BScope() {
+        if (!on) return;
+        cudaEventRecord(mk.b, b->stream);
+        b->marks.push_back(mk);
+    }
+};
+
+void drain(pi_batch* b) {
+    for (auto& mk : b->marks) {
+        float ms = 0.f;
+        cudaEventSynchronize(mk.b);
+        cudaEventElapsedTime(&ms, mk.a, mk.b);
+        size_t q = 0;
+        while (q < b->prof_names.size() && b->prof_names[q] != mk.name) ++q;
+        if (q == b->prof_names.size()) { b->prof_names.push_back(mk.name); b->prof_count.push_back(0); b->prof_ms.push_back(0.0); }
+        b->prof_count[q] += 1;
+        b->prof_ms[q] += ms;
+        b->event_pool.push_back(mk.a);
+        b->event_pool.push_back(mk.b);
+    }
+    b->marks.clear();
+}
+
+void free_graphs(pi_batch* b) {
+    for (int p = 0; p < 2; ++p)
+        if (b->gexec[p]) { cudaGraphExecDestroy(b->gexec[p]); b->gexec[p] = nullptr; }
+    b->graph_dT = -1.0;
+}
+
+void free_tables(pi_batch* b) {
+    for (void* p : b->table_allocs) cudaFree(p);
+    b->table_allocs.clear();
+    b->tables_Ly = b->tables_Lz = -1;
+}
+
+void free_series(MemberHost& h) {
+    if (h.ser_vel) cudaFree(h.ser_vel);
+    if (h.ser_parf) cudaFree(h.ser_parf);
+    if (h.ser_temp) cudaFree(h.ser_temp);
+    h.ser_vel = h.ser_parf = h.ser_temp = nullptr;
+}
+
+void free_batch(pi_batch* b) {
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    free_graphs(b);
+    free_tables(b);
+    for (auto& h : b->mh) {
+        free_series(h);
+        for (int n = 0; n < PI_NTRACERS; ++n) for (int f = 0; f < 6; ++f) if (h.bcs[n][f].v) cudaFree(h.bcs[n][f].v);
+    }
+    for (void* p : b->allocs) cudaFree(p);
+    b->allocs.clear();
+    for (cudaEvent_t e : b->event_pool) cudaEventDestroy(e);
+    b->event_pool.clear();
+    if (b->stream) cudaStreamDestroy(b->stream);
+    b->stream = nullptr;
+}
+
+SpeciesDev32 to_dev(const pi_quota_params& p) {
+    SpeciesDev32 d;
+    d.Nsuper = (float)p.Nsuper; d.Cquota = (float)p.Cquota; d.Chl2Cint = (float)p.Chl2Cint;
+    d.alpha = (float)p.alpha; d.Phi = (float)p.Phi; d.Topt = (float)p.Topt; d.Tmax = (float)p.Tmax;
+    d.Ea = (float)p.Ea; d.PCmax = (float)p.PCmax; d.VDOCmax = (float)p.VDOCmax; d.VNO3max = (float)p.VNO3max;
+    d.VNH4max = (float)p.VNH4max; d.VPO4max = (float)p.VPO4max; d.KsatDOC = (float)p.KsatDOC;
+    d.KsatNH4 = (float)p.KsatNH4; d.KsatNO3 = (float)p.KsatNO3; d.KsatPO4 = (float)p.KsatPO4;
+    d.Cqmax = (float)p.Cqmax; d.Nqmax = (float)p.Nqmax; d.Pqmax = (float)p.Pqmax; d.Chl2N = (float)p.Chl2N;
+    d.R_NC = (float)p.R_NC; d.R_PC = (float)p.R_PC; d.k_mtb = (float)p.k_mtb; d.respir = (float)p.respir;
+    d.grz_P = (float)p.grz_P; d.dvid_P = (float)p.dvid_P; d.dvid_reg = (float)p.dvid_reg;
+    d.dvid_reg2 = (float)p.dvid_reg2; d.mort_P = (float)p.mort_P; d.mort_reg = (float)p.mort_reg;
+    d.grazFracC = (float)p.grazFracC; d.grazFracN = (float)p.grazFracN; d.grazFracP = (float)p.grazFracP;
+    d.mortFracC = (float)p.mortFracC; d.mortFracN = (float)p.mortFracN; d.mortFracP = (float)p.mortFracP;
+    d.dvid_type = (int)p.dvid_type;
+    // tempFunc's normaliser (growth_kernels.jl:2-16), a constant of the species
+    d.OGT_rate = (float)std::exp(-(double)d.Ea / (8.3145 * ((double)d.Topt + 273.15)));
+    return d;
+}
+
+BgcDev32 to_dev(const pi_bgc_params& p) {
+    BgcDev32 d;
+    d.kw = (float)p.kw; d.kc = (float)p.kc; d.kDOC = (float)p.kDOC; d.Nit = (float)p.Nit; d.kDON = (float)p.kDON;
+    d.kDOP = (float)p.kDOP; d.kPOC = (float)p.kPOC; d.kPON = (float)p.kPON; d.kPOP = (float)p.kPOP;
+    d.kappa_h = (float)p.kappa_h; d.kappa_v = (float)p.kappa_v; d.kappa_hP = (float)p.kappa_hP;
+    d.kappa_vP = (float)p.kappa_vP; d.shared_graz = p.shared_graz == 1.0;
+    d.w_sink_org = (float)p.w_sink_org; d.w_sink_inorg = (float)p.w_sink_inorg; d.lambda_POC = (float)p.lambda_POC;
+    d.lambda_min = (float)p.lambda_min; d.kdiss = (float)p.kdiss; d.lambda_dust = (float)p.lambda_dust;
+    d.lambda_Fe = (float)p.lambda_Fe; d.ligand = (float)p.ligand; d.DFeFrac = (float)p.DFeFrac;
+    return d;
+}
+
+pi_status check_member(const pi_member& mb, int nsp, std::string& msg) {
+    const pi_grid* grid = mb.grid;
+    if (!grid || !mb.bgc || !mb.species || mb.capacity < 1 || !grid->dzF || !grid->dzC) { msg = "NULL grid/params or capacity < 1"; return PI_ERR_ARG; }
+    if (grid->Nx < 1 || grid->Ny < 1 || grid->Nz < 1) { msg = "grid size must be at least 1 in every direction"; return PI_ERR_ARG; }
+    if (grid->Hx < 2 || grid->Hy < 2 || grid->Hz < 2 || grid->Hx > 8 || grid->Hy > 8 || grid->Hz > 8) { msg = "halo must be 2..8 points (DST3FL needs at least 2)"; return PI_ERR_ARG; }
+    for (int a = 0; a < 3; ++a)
+        if (grid->topo[a] != PI_PERIODIC && grid->topo[a] != PI_BOUNDED) { msg = "topology must be Periodic or Bounded"; return PI_ERR_ARG; }
+    if (grid->topo[2] != PI_BOUNDED) { msg = "z must be Bounded (tracer sinking has no Periodic rule)"; return PI_ERR_ARG; }
+    long long Gx = grid->Nx + 2LL * grid->Hx, Gy = grid->Ny + 2LL * grid->Hy, Gz = grid->Nz + 2LL * grid->Hz;
+    if (Gx * Gy * Gz >= (1LL << 31) - 2 || (Gx + 1) * (Gy + 1) * (Gz + 1) >= (1LL << 31)) { msg = "grid too large for 32-bit cell indices"; return PI_ERR_ARG; }
+    if (mb.capacity >= (1LL << 31)) { msg = "capacity must be below 2^31"; return PI_ERR_ARG; }
+    for (int s = 0; s < nsp; ++s) {
+        const pi_quota_params& p = mb.species[s];
+        int ty = (int)p.dvid_type;
+        if ((double)ty != p.dvid_type || ty < 1 || ty > 3) { msg = "dvid_type must be 1 (Sizer), 2 (Timer) or 3 (Sizer_Timer)"; return PI_ERR_PARAM; }
+        if (!(p.Cquota > 0.0) || !(p.Nsuper > 0.0)) { msg = "Cquota and Nsuper must be positive"; return PI_ERR_PARAM; }
+    }
+    return PI_OK;
+}
+
+// Work tables for the current tuning (sweep segment lengths) on the device.
+pi_status build_tables(pi_batch* b) {
+    const int Ly = b->tune.Ly, Lz = b->tune.Lz;
+    if (b->tables_Ly == Ly && b->tables_Lz == Lz) return PI_OK;
+    free_tables(b);
+    std::vector<int4> ix, iy, iz, ic, icol;
+    for (int m = 0; m < b->nm; ++m) {
+        const HostGrid& g = b->mh[m].g;
+        for (int k = 1 + g.Hz; k <= g.Nz + g.Hz; ++k)
+            for (int j = 1 + g.Hy; j <= g.Ny + g.Hy; ++j) {
+                for (int i0 = 1 + g.Hx; i0 <= g.Nx + g.Hx; i0 += 31) ix.push_back(make_int4(m, j, k, i0));
+                for (int i0 = 1 + g.Hx; i0 <= g.Nx + g.Hx; i0 += 32) ic.push_back(make_int4(m, i0, j, k));
+            }
+        for (int k = 1 + g.Hz; k <= g.Nz + g.Hz; ++k)
+            for (int j0 = 1 + g.Hy; j0 <= g.Ny + g.Hy; j0 += Ly)
+                for (int i0 = 1 + g.Hx; i0 <= g.Nx + g.Hx; i0 += 32) iy.push_back(make_int4(m, i0, j0, k));
+        for (int k0 = 1 + g.Hz; k0 <= g.Nz + g.Hz; k0 += Lz)
+            for (int j = 1 + g.Hy; j <= g.Ny + g.Hy; ++j)
+                for (int i0 = 1 + g.Hx; i0 <= g.Nx + g.Hx; i0 += 32) iz.push_back(make_int4(m, i0, j, k0));
+        for (int j = 1; j <= g.Ny; ++j)
+            for (int i0 = 1; i0 <= g.Nx; i0 += 32) icol.push_back(make_int4(m, i0, j, 0));
+    }
+    auto up = [&](std::vector<int4>& v, const int4** dst, int* n) -> pi_status {
+        int4* d = nullptr;
+        pi_status s = balloc(b, &d, v.size(), "work table", &b->table_allocs);
+        if (s) return s;
+        BK(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(int4), cudaMemcpyHostToDevice, b->stream), "upload work table");
+        *dst = d; *n = (int)v.size();
+        return PI_OK;
+    };
+    pi_status s;
+    if ((s = up(ix, &b->T.ix, &b->T.nix))) return s;
+    if ((s = up(iy, &b->T.iy, &b->T.niy))) return s;
+    if ((s = up(iz, &b->T.iz, &b->T.niz))) return s;
+    if ((s = up(ic, &b->T.ic, &b->T.nic))) return s;
+    if ((s = up(icol, &b->T.icol, &b->T.nicol))) return s;
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    b->T.Ly = Ly; b->T.Lz = Lz;
+    b->tables_Ly = Ly; b->tables_Lz = Lz;
+    return PI_OK;
+}
+
+float* velown(pi_batch* b, int m, int buf, int c) { return b->velown + ((long long)(buf * 3 + c)) * b->Gtot + b->mdh[m].cell_off; }
+
+// Launch grid of a tile kernel: one block per tile, or a persistent grid of k blocks per SM.
+unsigned tile_grid(pi_batch* b, int persist) {
+    if (!persist) return (unsigned)std::max(1, b->ntiles);
+    return (unsigned)std::max(1, std::min(b->ntiles, persist * b->nsm));
+}
+unsigned warp_grid(long long nitems, int wpb) { return std::max(1u, nblk(nitems, wpb)); }
+
+// Enqueues one step on the batch stream (eager launches, or the body of a graph capture).
+pi_status enqueue_step(pi_batch* b, double dT, int cur) {
+    cudaStream_t s = b->stream;
+    const long long G = b->Gtot;
+    const float fdT = (float)dT;
+    float* tr = b->trbuf[cur];
+    float* trn = b->trbuf[cur ^ 1];
+    BK(cudaMemsetAsync(b->pop, 0, G * sizeof(int), s), "zero pop");
+    if (b->pop_sp) BK(cudaMemsetAsync(b->pop_sp, 0, (size_t)b->nsp * G * sizeof(int), s), "zero pop");
+    { BScope sc(b, "k32_bind");
+      k32_bind<<<b->nm, 128, 0, s>>>(b->nm, b->md, b->S, b->F, b->st, dT, b->PARF, b->errw); }
+    { BScope sc(b, "k32_velhalf");
+      unsigned gx = std::min<unsigned>(nblk(b->maxG, 256), 64);
+      k32_velhalf<<<dim3(gx, b->nm), 256, 0, s>>>(b->md, b->F, b->errw); }
+    {
+        MoveArgs a;
+        a.T = b->T; a.P = b->P; a.sp = b->sp; a.bgc = b->bgc; a.F = b->F; a.dzC = b->dzC; a.st = b->st;
+        a.dT = fdT; a.Gtot = G; a.pop = b->pop; a.pop_sp = b->pop_sp; a.chl_acc = b->chl_acc; a.acc = b->acc;
+        a.dcnt = b->dcnt; a.tile_cnt = b->tile_cnt; a.err = b->errw;
+        BScope sc(b, "k32_move");
+        k32_move<<<tile_grid(b, b->tune.persist_move), b->tune.bs_move, 0, s>>>(a);
+    }
+    { BScope sc(b, "k32_par");
+      k32_par<<<warp_grid(b->T.nicol, b->tune.wpb_par), 32 * b->tune.wpb_par, 0, s>>>(b->T, b->dzF, b->bgc, b->chl_acc, b->PARF,
+                                                                                   b->par, b->diag_par, b->errw); }
+    { BScope sc(b, "cub_scan_tiles");
+      size_t tb = b->cub_bytes;
+      BK(cub::DeviceScan::ExclusiveSum(b->cub_tmp, tb, b->tile_cnt, b->tile_off, b->ntiles, s), "scan tiles"); }
+    { BScope sc(b, "k32_assign");
+      k32_assign<<<tile_grid(b, 0), b->tune.bs_assign, 0, s>>>(b->T, b->P, b->tile_cnt, b->tile_off, b->divlist,
+                                                               b->freelist, b->ndiv, b->st, b->errw); }
+    { BScope sc(b, "k32_daughters");
+      k32_daughters<<<dim3(4, b->nseg), 128, 0, s>>>(b->T, b->P, b->divlist, b->freelist, b->ndiv, b->errw); }
+    {
+        PhysArgs a;
+        a.T = b->T; a.P = b->P; a.sp = b->sp; a.F = b->F; a.st = b->st; a.dT = fdT; a.Gtot = G; a.tr = tr;
+        a.par = b->par; a.pop = b->pop; a.pop_sp = b->pop_sp; a.acc = b->acc; a.dcnt = b->dcnt; a.err = b->errw;
+        BScope sc(b, "k32_physiology");
+        k32_physiology<<<tile_grid(b, b->tune.persist_phys), b->tune.bs_phys, 0, s>>>(a);
+    }
+    SweepArgs sw;
+    sw.T = b->T; sw.lm = b->lm; sw.dzF = b->dzF; sw.dzC = b->dzC; sw.F = b->F; sw.Gtot = G; sw.tr = tr;
+    sw.dT = fdT; sw.err = b->errw;
+    { sw.src = tr; sw.dst = b->ta;
+      BScope sc(b, "k32_sweep_x");
+      k32_sweep_x<<<warp_grid(b->T.nix, b->tune.wpb_x), 32 * b->tune.wpb_x, 0, s>>>(sw); }
+    { sw.src = b->ta; sw.dst = b->tb;
+      BScope sc(b, "k32_sweep_y");
+      k32_sweep_y<<<warp_grid(b->T.niy, b->tune.wpb_y), 32 * b->tune.wpb_y, 0, s>>>(sw); }
+    { sw.src = b->tb; sw.dst = b->ta;
+      BScope sc(b, "k32_sweep_z");
+      k32_sweep_z<<<warp_grid(b->T.niz, b->tune.wpb_z), 32 * b->tune.wpb_z, 0, s>>>(sw); }
+    {
+        TailArgs a;
+        a.T = b->T; a.lm = b->lm; a.dzF = b->dzF; a.dzC = b->dzC; a.bgc = b->bgc; a.bcs = b->bcs; a.st = b->st;
+        a.Gtot = G; a.tr = tr; a.gadv = b->ta; a.tr_next = trn; a.acc = b->acc; a.pop = b->pop; a.dT = fdT;
+        a.err = b->errw;
+        BScope sc(b, "k32_tail");
+        k32_tail<<<warp_grid(b->T.nic, b->tune.wpb_tail), 32 * b->tune.wpb_tail, 0, s>>>(a);
+    }
+    { BScope sc(b, "k32_halo");
+      k32_halo<0><<<std::min<unsigned>(nblk(b->nlines[0], 128), 148 * 8), 128, 0, s>>>(b->md, b->line_off[0], b->nm, G, trn, PI_NTRACERS, b->errw);
+      k32_halo<1><<<std::min<unsigned>(nblk(b->nlines[1], 128), 148 * 8), 128, 0, s>>>(b->md, b->line_off[1], b->nm, G, trn, PI_NTRACERS, b->errw);
+      k32_halo<2><<<std::min<unsigned>(nblk(b->nlines[2], 128), 148 * 8), 128, 0, s>>>(b->md, b->line_off[2], b->nm, G, trn, PI_NTRACERS, b->errw); }
+    k32_copy_if_err<<<148 * 4, 256, 0, s>>>(trn, tr, (long long)PI_NTRACERS * G, b->errw);
+    k32_end_step<<<nblk(b->nm, 128), 128, 0, s>>>(b->nm, b->F, b->st, dT, b->errw);
+    BK(cudaGetLastError(), "step launch");
+    return PI_OK;
+}
+
+pi_status capture_graphs(pi_batch* b, double dT) {
+    free_graphs(b);
+    for (int p = 0; p < 2; ++p) {
+        cudaGraph_t g = nullptr;
+        BK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        pi_status st = enqueue_step(b, dT, p);
+        cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+        if (st) { if (g) cudaGraphDestroy(g); return st; }
+        if (e != cudaSuccess) return bcuda(b, e, "end capture");
+        e = cudaGraphInstantiate(&b->gexec[p], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return bcuda(b, e, "instantiate graph");
+    }
+    b->graph_dT = dT;
+    return PI_OK;
+}
+
+pi_status check_errors(pi_batch* b) {
+    uint32_t e = 0;
+    StepState hs{};
+    BK(cudaMemcpyAsync(&e, b->errw, sizeof e, cudaMemcpyDeviceToHost, b->stream), "read error word");
+    BK(cudaMemcpyAsync(&hs, b->st, sizeof hs, cudaMemcpyDeviceToHost, b->stream), "read step state");
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    if (!e) return PI_OK;
+    BK(cudaMemsetAsync(b->errw, 0, sizeof(uint32_t), b->stream), "clear error word");
+    if (e & F32_ERR_CAPACITY) {
+        // the step stopped after the decisions: drop the unconsumed loss sums
+        BK(cudaMemsetAsync(b->acc, 0, (size_t)ACC_N * b->Gtot * sizeof(unsigned long long), b->stream), "clear sums");
+        BK(cudaStreamSynchronize(b->stream), "synchronize");
+        // TimeStep! advanced model.iteration and model.t before it threw (time_step.jl:14-15)
+        hs.iteration = hs.err_iter;
+        hs.t = (double)hs.err_iter * b->last_dT;
+        BK(cudaMemcpyAsync(b->st, &hs, sizeof hs, cudaMemcpyHostToDevice, b->stream), "write step state");
+        BK(cudaStreamSynchronize(b->stream), "synchronize");
+        const double tf = hs.t;
+        std::string msg = "number of individual exceeds the capacity at timestep " + julia_float(tf / 86400.0) + " days";
+        if (b->nm > 1) msg += " (member " + std::to_string(hs.err_member) + ")";
+        return bfail(b, PI_ERR_CAPACITY, msg);
+    }
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    if (e & F32_ERR_FORCING) return bfail(b, PI_ERR_SHAPE, "BoundsError: forcing snapshot not provided for the step time");
+    return bfail(b, PI_ERR_DOMAIN, "an individual left the halo-padded grid (cell index out of range)");
+}
+
+}  // namespace
+
+extern "C" {
+
+pi_status pi_batch_last_error(pi_batch* b, char* buf, size_t len) {
+    const std::string& e = b ? b->err : g_batch_error;
+    if (buf && len) {
+        size_t n = std::min(len - 1, e.size());
+        memcpy(buf, e.c_str(), n);
+        buf[n] = 0;
+    }
+    return PI_OK;
+}
+
+pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t nspecies, pi_batch** out) {
+    if (!out) return bfail(nullptr, PI_ERR_ARG, "pi_batch_create: out is NULL");
+    *out = nullptr;
+    if (!members || nmembers < 1 || nspecies < 1) return bfail(nullptr, PI_ERR_ARG, "pi_batch_create: no members or nspecies < 1");
+    if ((long long)nmembers * nspecies > 65535) return bfail(nullptr, PI_ERR_ARG, "pi_batch_create: members × species must be at most 65535");
+    for (int m = 0; m < nmembers; ++m) {
+        std::string msg;
+        pi_status st = check_member(members[m], nspecies, msg);
+        if (st) return bfail(nullptr, st, "pi_batch_create: member " + std::to_string(m) + ": " + msg);
+    }
+    pi_batch* b = new pi_batch();
+    auto bail = [&](pi_status st) { g_batch_error = b->err; free_batch(b); delete b; return st; };
+    if (cudaGetDevice(&b->device) != cudaSuccess) { b->err = "pi_batch_create: no CUDA device"; return bail(PI_ERR_CUDA); }
+    cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, b->device);
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) { b->err = "pi_batch_create: stream"; return bail(PI_ERR_CUDA); }
+    b->nm = nmembers; b->nsp = nspecies; b->nseg = nmembers * nspecies;
+    b->mh.resize(nmembers);
+    b->mdh.resize(nmembers);
+    std::vector<SpeciesDev32> sph;
+    std::vector<BgcDev32> bgch;
+    std::vector<float> dzF, dzC;
+    std::vector<int2> tiles;
+    std::vector<int> seg_tile0;
+    long long cell = 0, slot = 0, col = 0;
+    int lev = 0;
+    bool any_land = false;
+    for (int m = 0; m < nmembers; ++m) {
+        const pi_member& mb = members[m];
+        const pi_grid* grid = mb.grid;
+        MemberHost& h = b->mh[m];
+        HostGrid& g = h.g;
+        g.Nx = grid->Nx; g.Ny = grid->Ny; g.Nz = grid->Nz; g.Hx = grid->Hx; g.Hy = grid->Hy; g.Hz = grid->Hz;
+        g.Gx = g.Nx + 2 * g.Hx; g.Gy = g.Ny + 2 * g.Hy; g.Gz = g.Nz + 2 * g.Hz;
+        for (int a = 0; a < 3; ++a) g.topo[a] = grid->topo[a];
+        g.dx = grid->dx; g.dy = grid->dy;
+        g.dzF.assign(grid->dzF, grid->dzF + g.Gz);
+        g.dzC.assign(grid->dzC, grid->dzC + g.Gz);
+        g.G = (long long)g.Gx * g.Gy * g.Gz;
+        h.all_water = 1;
+        if (grid->landmask) {
+            g.lm.assign(grid->landmask, grid->landmask + g.G);
+            for (uint8_t& v : g.lm) { v = v ? 1 : 0; if (!v) h.all_water = 0; }
+            if (!h.all_water) any_land = true;
+        }
+        h.C = mb.capacity; h.seed = mb.seed; h.bgc = *mb.bgc;
+        h.sp.assign(mb.species, mb.species + nspecies);
+        MemberDev& d = b->mdh[m];
+        d.Nx = g.Nx; d.Ny = g.Ny; d.Nz = g.Nz; d.Hx = g.Hx; d.Hy = g.Hy; d.Hz = g.Hz;
+        d.Gx = g.Gx; d.Gy = g.Gy; d.Gz = g.Gz; d.tx = g.topo[0]; d.ty = g.topo[1]; d.tz = g.topo[2];
+        d.all_water = h.all_water; d.any_bc = 0;
+        d.dx = (float)g.dx; d.dy = (float)g.dy;
+        d.cell_off = cell; d.G = g.G; d.col_off = col; d.slot_off = slot; d.C = h.C;
+        d.dz_off = lev; d.bc_off = m * PI_NTRACERS * 6; d.seed = h.seed;
+        double cmin = 1e300, chlmin = 1e300;
+        for (int s = 0; s < nspecies; ++s) {
+            const pi_quota_params& p = h.sp[s];
+            cmin = std::min(cmin, p.Cquota * p.Nsuper);
+            if (p.Chl2Cint > 0.0) chlmin = std::min(chlmin, p.Chl2Cint * p.Cquota * p.Nsuper);
+            sph.push_back(to_dev(p));
+        }
+        if (chlmin > 1e299) chlmin = cmin;
+        // 2^40 units per nominal individual: sums of up to ~2^22 individuals per cell fit in 63 bits
+        d.fx_unit = cmin * 0x1p-40;
+        d.chl_unit = chlmin * 0x1p-40;
+        bgch.push_back(to_dev(h.bgc));
+        for (int k = 0; k < g.Gz; ++k) { dzF.push_back((float)g.dzF[k]); dzC.push_back((float)g.dzC[k]); }
+        for (int s = 0; s < nspecies; ++s) {
+            seg_tile0.push_back((int)tiles.size());
+            for (long long t0 = 0; t0 < h.C; t0 += F32_TILE) tiles.push_back(make_int2(m * nspecies + s, (int)t0));
+        }
+        cell += (g.G + 63) / 64 * 64;       // members start on 256-byte boundaries
+        slot += (long long)nspecies * h.C;
+        col += (long long)g.Nx * g.Ny;
+        lev += g.Gz;
+        b->maxG = std::max(b->maxG, g.G);
+    }
+    seg_tile0.push_back((int)tiles.size());
+    if (tiles.size() >= (size_t)INT32_MAX) { b->err = "pi_batch_create: too many slots"; return bail(PI_ERR_ARG); }
+    b->Gtot = cell; b->Stot = slot; b->ncol = col; b->nlev = lev; b->ntiles = (int)tiles.size();
+    const long long G = b->Gtot, S = b->Stot;
+    pi_status st;
+#define BA(ptr, n) do { st = balloc(b, &(ptr), (size_t)(n), #ptr); if (st) return bail(st); } while (0)
+    BA(b->md, nmembers); BA(b->sp, sph.size()); BA(b->bgc, nmembers); BA(b->bcs, (size_t)nmembers * PI_NTRACERS * 6);
+    BA(b->F, nmembers); BA(b->S, nmembers); BA(b->st, 1); BA(b->errw, 1);
+    BA(b->trbuf[0], PI_NTRACERS * G); BA(b->trbuf[1], PI_NTRACERS * G); BA(b->ta, PI_NTRACERS * G); BA(b->tb, PI_NTRACERS * G);
+    BA(b->par, G); BA(b->diag_par, G); BA(b->PARF, std::max<long long>(col, 1));
+    BA(b->dzF, lev); BA(b->dzC, lev);
+    if (any_land) BA(b->lm, G);
+    BA(b->velown, 6 * G); BA(b->velh, 3 * G); BA(b->tempown, G);
+    BA(b->dcnt, (size_t)nspecies * 4 * G); BA(b->pop, G);
+    bool shared = true;
+    for (auto& h : b->mh) if (h.bgc.shared_graz != 1.0) shared = false;
+    if (!shared) BA(b->pop_sp, (size_t)nspecies * G);
+    BA(b->acc, (size_t)ACC_N * G); BA(b->chl_acc, G);
+    IndDev32& P = b->P;
+    BA(P.cell, S); BA(P.scell, S); BA(P.ox, S); BA(P.oy, S); BA(P.oz, S); BA(P.Bm, S); BA(P.Cq, S);
+    BA(P.Nq, S); BA(P.Pq, S); BA(P.Chl, S); BA(P.age, S); BA(P.gen, S); BA(P.flags, S); BA(P.stat, S);
+    BA(b->tiles, tiles.size()); BA(b->seg_tile0, seg_tile0.size());
+    BA(b->tile_cnt, tiles.size()); BA(b->tile_off, tiles.size());
+    BA(b->divlist, S); BA(b->freelist, S); BA(b->ndiv, b->nseg);
+    for (int a = 0; a < 3; ++a) BA(b->line_off[a], nmembers + 1);
+    BA(b->stage, std::max<long long>(b->maxG, col));
+    BA(b->partial, 3 * 1024); BA(b->scratch, 4);
+    size_t cb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, cb, b->tile_cnt, b->tile_off, b->ntiles, b->stream);
+    b->cub_bytes = cb;
+    BA(b->cub_tmp, cb);
+#undef BA
+    // series and forcing tables
+    b->serh.assign(nmembers, MemberSeries{});
+    std::vector<MemberForcing> Fh(nmembers);
+    for (int m = 0; m < nmembers; ++m) {
+        for (int c = 0; c < 3; ++c) {
+            b->serh[m].velh_buf[c] = b->velh + (long long)c * G + b->mdh[m].cell_off;
+            Fh[m].vel0[c] = velown(b, m, 0, c);
+            Fh[m].vel1[c] = velown(b, m, 1, c);
+            Fh[m].velh[c] = b->serh[m].velh_buf[c];
+        }
+        Fh[m].temp = b->tempown + b->mdh[m].cell_off;
+        b->serh[m].dT_vel = b->serh[m].dT_PAR = b->serh[m].dT_temp = 1.0;
+    }
+    b->bch.assign((size_t)nmembers * PI_NTRACERS * 6, FluxBC32{PI_BC_NONE, 0, 0, 0, nullptr});
+    std::vector<long long> lo[3];
+    for (int a = 0; a < 3; ++a) lo[a].assign(nmembers + 1, 0);
+    for (int m = 0; m < nmembers; ++m) {
+        const HostGrid& g = b->mh[m].g;
+        lo[0][m + 1] = lo[0][m] + (long long)g.Gy * g.Gz;
+        lo[1][m + 1] = lo[1][m] + (long long)g.Gx * g.Gz;
+        lo[2][m + 1] = lo[2][m] + (long long)g.Gx * g.Gy;
+    }
+    for (int a = 0; a < 3; ++a) b->nlines[a] = lo[a][nmembers];
+    cudaStream_t s0 = b->stream;
+    bool ok = true;
+    auto H2D = [&](void* d, const void* h, size_t n) { ok = ok && cudaMemcpyAsync(d, h, n, cudaMemcpyHostToDevice, s0) == cudaSuccess; };
+    auto Z = [&](void* d, size_t n) { ok = ok && cudaMemsetAsync(d, 0, n, s0) == cudaSuccess; };
+    H2D(b->md, b->mdh.data(), nmembers * sizeof(MemberDev));
+    H2D(b->sp, sph.data(), sph.size() * sizeof(SpeciesDev32));
+    H2D(b->bgc, bgch.data(), bgch.size() * sizeof(BgcDev32));
+    H2D(b->bcs, b->bch.data(), b->bch.size() * sizeof(FluxBC32));
+    H2D(b->F, Fh.data(), nmembers * sizeof(MemberForcing));
+    H2D(b->S, b->serh.data(), nmembers * sizeof(MemberSeries));
+    H2D(b->dzF, dzF.data(), dzF.size() * sizeof(float));
+    H2D(b->dzC, dzC.data(), dzC.size() * sizeof(float));
+    H2D(b->tiles, tiles.data(), tiles.size() * sizeof(int2));
+    H2D(b->seg_tile0, seg_tile0.data(), seg_tile0.size() * sizeof(int));
+    for (int a = 0; a < 3; ++a) H2D(b->line_off[a], lo[a].data(), (nmembers + 1) * sizeof(long long));
+    if (b->lm) {
+        std::vector<uint8_t> lmh(G, 1);
+        for (int m = 0; m < nmembers; ++m)
+            if (!b->mh[m].g.lm.empty()) std::copy(b->mh[m].g.lm.begin(), b->mh[m].g.lm.end(), lmh.begin() + b->mdh[m].cell_off);
+        H2D(b->lm, lmh.data(), G);
+        ok = ok && cudaStreamSynchronize(s0) == cudaSuccess;
+    }
+    Z(b->st, sizeof(StepState)); Z(b->errw, sizeof(uint32_t));
+    for (int q = 0; q < 2; ++q) Z(b->trbuf[q], PI_NTRACERS * G * sizeof(float));
+    Z(b->ta, PI_NTRACERS * G * sizeof(float)); Z(b->tb, PI_NTRACERS * G * sizeof(float));
+    Z(b->par, G * sizeof(float)); Z(b->diag_par, G * sizeof(float)); Z(b->PARF, std::max<long long>(col, 1) * sizeof(float));
+    Z(b->velown, 6 * G * sizeof(float)); Z(b->velh, 3 * G * sizeof(float)); Z(b->tempown, G * sizeof(float));
+    Z(b->dcnt, (size_t)nspecies * 4 * G * sizeof(uint32_t)); Z(b->pop, G * sizeof(int));
+    if (b->pop_sp) Z(b->pop_sp, (size_t)nspecies * G * sizeof(int));
+    Z(b->acc, (size_t)ACC_N * G * 8); Z(b->chl_acc, G * 8);
+    for (void* p : { (void*)P.ox, (void*)P.oy, (void*)P.oz, (void*)P.Bm, (void*)P.Cq, (void*)P.Nq, (void*)P.Pq,
+                     (void*)P.Chl, (void*)P.age, (void*)P.gen }) Z(p, S * sizeof(float));
+    Z(P.flags, S); Z(P.stat, S); Z(P.scell, S * sizeof(int32_t));
+    // constructor state: inactive, find_inds! cell (0, 0, 0) (plankton_generation.jl:3)
+    ok = ok && cudaMemsetAsync(P.cell, 0xff, S * sizeof(int32_t), s0) == cudaSuccess;
+    ok = ok && cudaStreamSynchronize(s0) == cudaSuccess;
+    if (!ok) { b->err = "pi_batch_create: device initialisation failed"; return bail(PI_ERR_CUDA); }
+    b->T.md = b->md; b->T.nsp = nspecies; b->T.tiles = b->tiles; b->T.ntiles = b->ntiles; b->T.seg_tile0 = b->seg_tile0;
+    st = build_tables(b);
+    if (st) return bail(st);
+    *out = b;
+    return PI_OK;
+}
+
+pi_status pi_batch_destroy(pi_batch* b) {
+    if (!b) return PI_OK;
+    drain(b);
+    free_batch(b);
+    delete b;
+    return PI_OK;
+}
+
+static pi_status check_mem(pi_batch* b, int32_t member, const char* fn) {
+    if (!b) return bfail(b, PI_ERR_ARG, std::string(fn) + ": NULL batch");
+    if (member < 0 || member >= b->nm) return bfail(b, PI_ERR_ARG, std::string(fn) + ": member out of range");
+    return PI_OK;
+}
+
+pi_status pi_batch_set_individuals(pi_batch* b, int32_t member, int32_t sp, const pi_individuals* in) {
+    pi_status e = check_mem(b, member, "pi_set_individuals");
+    if (e) return e;
+    if (!in || sp < 0 || sp >= b->nsp) return bfail(b, PI_ERR_ARG, "pi_set_individuals: bad argument");
+    const double* dcols[] = { in->x, in->y, in->z, in->Bm, in->Cq, in->Nq, in->Pq, in->Chl, in->gen, in->age,
+                              in->graz, in->mort, in->dvid };
+    for (const double* p : dcols) if (!p) return bfail(b, PI_ERR_ARG, "pi_set_individuals: NULL attribute");
+    if (!in->xi || !in->yi || !in->zi || !in->ac) return bfail(b, PI_ERR_ARG, "pi_set_individuals: NULL attribute");
+    const MemberHost& h = b->mh[member];
+    const HostGrid& g = h.g;
+    const MemberDev& d = b->mdh[member];
+    const long long C = h.C;
+    std::vector<int32_t> cell(C), scell(C, 0);
+    std::vector<float> o[3], f[7];
+    for (auto& v : o) v.assign(C, 0.0f);
+    for (auto& v : f) v.assign(C, 0.0f);
+    std::vector<uint8_t> flags(C), stat(C, 0);
+    const double* pos[3] = { in->x, in->y, in->z };
+    const int N[3] = { g.Nx, g.Ny, g.Nz }, Hh[3] = { g.Hx, g.Hy, g.Hz }, Gg[3] = { g.Gx, g.Gy, g.Gz };
+    const int64_t* idx[3] = { in->xi, in->yi, in->zi };
+    for (long long i = 0; i < C; ++i) {
+        if (in->ac[i] > 1) return bfail(b, PI_ERR_PARAM, "pi_set_individuals: ac must be 0 or 1");
+        double d3[3] = { in->graz[i], in->mort[i], in->dvid[i] };
+        for (double v : d3) if (v != 0.0 && v != 1.0) return bfail(b, PI_ERR_PARAM, "pi_set_individuals: graz/mort/dvid must be 0 or 1");
+        for (int a = 0; a < 3; ++a)
+            if (idx[a][i] < 0 || idx[a][i] > Gg[a]) return bfail(b, PI_ERR_PARAM, "pi_set_individuals: xi/yi/zi outside 0..G");
+        flags[i] = (uint8_t)((in->ac[i] ? F32_AC : 0) | (in->graz[i] == 1.0 ? F32_GRAZ : 0) |
+                             (in->mort[i] == 1.0 ? F32_MORT : 0) | (in->dvid[i] == 1.0 ? F32_DVID : 0));
+        const double* cols[7] = { in->Bm, in->Cq, in->Nq, in->Pq, in->Chl, in->age, in->gen };
+        for (int q = 0; q < 7; ++q) f[q][i] = (float)cols[q][i];
+        if (!in->ac[i]) { cell[i] = -1; continue; }
+        int c[3];
+        for (int a = 0; a < 3; ++a) {
+            const double x = pos[a][i];
+            if (!(x >= 0.0 && x <= (double)N[a])) return bfail(b, PI_ERR_PARAM, "pi_set_individuals: position outside [0, N] of an active individual");
+            double fl = std::floor(x);
+            c[a] = (int)fl;
+            float of = (float)(x - fl);
+            if (of >= 1.0f) { c[a] += 1; of = 0.0f; }
+            o[a][i] = of;
+        }
+        cell[i] = c[0] + (g.Nx + 1) * (c[1] + (g.Ny + 1) * c[2]);
+        bool same = true;
+        for (int a = 0; a < 3; ++a) same = same && idx[a][i] == c[a] + 1 + Hh[a];
+        if (!same) {
+            stat[i] = F32_ST_STALE;
+            scell[i] = (int32_t)(in->xi[i] + (g.Gx + 1) * (in->yi[i] + (g.Gy + 1) * in->zi[i]));
+        }
+    }
+    const long long g0 = d.slot_off + (long long)sp * C;
+    const IndDev32& P = b->P;
+    cudaStream_t s = b->stream;
+    BK(cudaMemcpyAsync(P.cell + g0, cell.data(), C * 4, cudaMemcpyHostToDevice, s), "upload individuals");
+    BK(cudaMemcpyAsync(P.scell + g0, scell.data(), C * 4, cudaMemcpyHostToDevice, s), "upload individuals");
+    float* od[3] = { P.ox, P.oy, P.oz };
+    for (int a = 0; a < 3; ++a) BK(cudaMemcpyAsync(od[a] + g0, o[a].data(), C * 4, cudaMemcpyHostToDevice, s), "upload individuals");
+    float* fd[7] = { P.Bm, P.Cq, P.Nq, P.Pq, P.Chl, P.age, P.gen };
+    for (int q = 0; q < 7; ++q) BK(cudaMemcpyAsync(fd[q] + g0, f[q].data(), C * 4, cudaMemcpyHostToDevice, s), "upload individuals");
+    BK(cudaMemcpyAsync(P.flags + g0, flags.data(), C, cudaMemcpyHostToDevice, s), "upload individuals");
+    BK(cudaMemcpyAsync(P.stat + g0, stat.data(), C, cudaMemcpyHostToDevice, s), "upload individuals");
+    BK(cudaStreamSynchronize(s), "synchronize");
+    return PI_OK;
+}
+
+pi_status pi_batch_get_individuals(pi_batch* b, int32_t member, int32_t sp, pi_individuals* out) {
+    pi_status e = check_mem(b, member, "pi_get_individuals");
+    if (e) return e;
+    if (!out || sp < 0 || sp >= b->nsp) return bfail(b, PI_ERR_ARG, "pi_get_individuals: bad argument");
+    const MemberHost& h = b->mh[member];
+    const HostGrid& g = h.g;
+    const long long C = h.C;
+    const long long g0 = b->mdh[member].slot_off + (long long)sp * C;
+    std::vector<int32_t> cell(C), scell(C);
+    std::vector<float> o[3], f[7];
+    std::vector<uint8_t> flags(C), stat(C);
+    const IndDev32& P = b->P;
+    cudaStream_t s = b->stream;
+    BK(cudaMemcpyAsync(cell.data(), P.cell + g0, C * 4, cudaMemcpyDeviceToHost, s), "download individuals");
+    BK(cudaMemcpyAsync(scell.data(), P.scell + g0, C * 4, cudaMemcpyDeviceToHost, s), "download individuals");
+    const float* od[3] = { P.ox, P.oy, P.oz };
+    for (int a = 0; a < 3; ++a) { o[a].resize(C); BK(cudaMemcpyAsync(o[a].data(), od[a] + g0, C * 4, cudaMemcpyDeviceToHost, s), "download individuals"); }
+    const float* fd[7] = { P.Bm, P.Cq, P.Nq, P.Pq, P.Chl, P.age, P.gen };
+    for (int q = 0; q < 7; ++q) { f[q].resize(C); BK(cudaMemcpyAsync(f[q].data(), fd[q] + g0, C * 4, cudaMemcpyDeviceToHost, s), "download individuals"); }
+    BK(cudaMemcpyAsync(flags.data(), P.flags + g0, C, cudaMemcpyDeviceToHost, s), "download individuals");
+    BK(cudaMemcpyAsync(stat.data(), P.stat + g0, C, cudaMemcpyDeviceToHost, s), "download individuals");
+    BK(cudaStreamSynchronize(s), "synchronize");
+    const pi_quota_params& p = h.sp[sp];
+    const float cq_ns = (float)p.Cquota * (float)p.Nsuper;
+    for (long long i = 0; i < C; ++i) {
+        const uint8_t fl = flags[i];
+        int ci = 0, cj = 0, ck = 0;
+        if (cell[i] >= 0) { ci = cell[i] % (g.Nx + 1); int r = cell[i] / (g.Nx + 1); cj = r % (g.Ny + 1); ck = r / (g.Ny + 1); }
+        const double xyz[3] = { cell[i] < 0 ? 0.0 : ci + (double)o[0][i], cell[i] < 0 ? 0.0 : cj + (double)o[1][i],
+                                cell[i] < 0 ? 0.0 : ck + (double)o[2][i] };
+        int64_t xi, yi, zi;
+        if (stat[i] & F32_ST_STALE) {
+            xi = scell[i] % (g.Gx + 1); int r = scell[i] / (g.Gx + 1); yi = r % (g.Gy + 1); zi = r / (g.Gy + 1);
+        } else if (cell[i] < 0) { xi = g.Hx; yi = g.Hy; zi = g.Hz; }
+        else { xi = ci + 1 + g.Hx; yi = cj + 1 + g.Hy; zi = ck + 1 + g.Hz; }
+        if (out->x) out->x[i] = xyz[0];
+        if (out->y) out->y[i] = xyz[1];
+        if (out->z) out->z[i] = xyz[2];
+        if (out->xi) out->xi[i] = xi;
+        if (out->yi) out->yi[i] = yi;
+        if (out->zi) out->zi[i] = zi;
+        double* cols[7] = { out->Bm, out->Cq, out->Nq, out->Pq, out->Chl, out->age, out->gen };
+        for (int q = 0; q < 7; ++q) if (cols[q]) cols[q][i] = (double)f[q][i];
+        if (out->Sz) out->Sz[i] = (double)(f[0][i] / cq_ns);
+        if (out->ac) out->ac[i] = (fl & F32_AC) ? 1 : 0;
+        if (out->graz) out->graz[i] = (fl & F32_GRAZ) ? 1.0 : 0.0;
+        if (out->mort) out->mort[i] = (fl & F32_MORT) ? 1.0 : 0.0;
+        if (out->dvid) out->dvid[i] = (fl & F32_DVID) ? 1.0 : 0.0;
+    }
+    return PI_OK;
+}
+
+pi_status pi_batch_set_tracer(pi_batch* b, int32_t member, int32_t idx, const double* data) {
+    pi_status e = check_mem(b, member, "pi_set_tracer");
+    if (e) return e;
+    if (!data || idx < 0 || idx >= PI_NTRACERS) return bfail(b, PI_ERR_ARG, "pi_set_tracer: bad argument");
+    const long long G = b->mdh[member].G;
+    BK(cudaMemcpyAsync(b->stage, data, G * sizeof(double), cudaMemcpyHostToDevice, b->stream), "upload tracer");
+    k32_d2f<<<std::min<unsigned>(nblk(G, 256), 1024), 256, 0, b->stream>>>(b->trbuf[b->cur] + idx * b->Gtot + b->mdh[member].cell_off, b->stage, G);
+    BK(cudaGetLastError(), "convert tracer");
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    return PI_OK;
+}
+
+pi_status pi_batch_get_tracer(pi_batch* b, int32_t member, int32_t idx, double* out) {
+    pi_status e = check_mem(b, member, "pi_get_tracer");
+    if (e) return e;
+    if (!out || idx < 0 || idx >= PI_NTRACERS) return bfail(b, PI_ERR_ARG, "pi_get_tracer: bad argument");
+    const long long G = b->mdh[member].G;
+    k32_f2d<<<std::min<unsigned>(nblk(G, 256), 1024), 256, 0, b->stream>>>(b->stage, b->trbuf[b->cur] + idx * b->Gtot + b->mdh[member].cell_off, G);
+    BK(cudaGetLastError(), "convert tracer");
+    BK(cudaMemcpyAsync(out, b->stage, G * sizeof(double), cudaMemcpyDeviceToHost, b->stream), "download tracer");
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    return PI_OK;
+}
+
+// Interior velocity snapshot (reference layout) into three halo-padded FP32 member fields
+// (vel_copy!, Simulation/utils.jl:5-34 with fill_halo_vel!).
+static pi_status vel_copy32(pi_batch* b, int m, const double* u, const double* v, const double* w,
+                            float* U, float* V, float* W) {
+    const HostGrid& g = b->mh[m].g;
+    const MemberDev& d = b->mdh[m];
+    cudaStream_t s = b->stream;
+    if (g.Nx >= g.Hx && g.Ny >= g.Hy && g.Nz >= g.Hz) {
+        int bd[3] = { g.topo[0] == PI_BOUNDED, g.topo[1] == PI_BOUNDED, g.topo[2] == PI_BOUNDED };
+        int dims[3][3] = { { g.Nx + bd[0], g.Ny, g.Nz }, { g.Nx, g.Ny + bd[1], g.Nz }, { g.Nx, g.Ny, g.Nz + bd[2] } };
+        const double* src[3] = { u, v, w };
+        float* dst[3] = { U, V, W };
+        for (int c = 0; c < 3; ++c) {
+            size_t n = (size_t)dims[c][0] * dims[c][1] * dims[c][2];
+            BK(cudaMemsetAsync(dst[c], 0, g.G * sizeof(float), s), "clear velocity");
+            BK(cudaMemcpyAsync(b->stage, src[c], n * sizeof(double), cudaMemcpyDefault, s), "upload velocity");
+            k32_scatter_interior<<<std::min<unsigned>(nblk((long long)n, 256), 1024), 256, 0, s>>>(d, dst[c], b->stage, dims[c][0], dims[c][1], dims[c][2]);
+            k32_halo_vel<0><<<std::min<unsigned>(nblk((long long)g.Gy * g.Gz, 128), 1024), 128, 0, s>>>(d, dst[c], c);
+            k32_halo_vel<1><<<std::min<unsigned>(nblk((long long)g.Gx * g.Gz, 128), 1024), 128, 0, s>>>(d, dst[c], c);
+            k32_halo_vel<2><<<std::min<unsigned>(nblk((long long)g.Gx * g.Gy, 128), 1024), 128, 0, s>>>(d, dst[c], c);
+            BK(cudaGetLastError(), "velocity halo");
+            BK(cudaStreamSynchronize(s), "synchronize");
+        }
+    } else {
+        std::vector<double> Ud, Vd, Wd;
+        host_vel_copy(g, u, v, w, Ud, Vd, Wd);
+        std::vector<float> tmp(g.G);
+        const std::vector<double>* hv[3] = { &Ud, &Vd, &Wd };
+        float* dst[3] = { U, V, W };
+        for (int c = 0; c < 3; ++c) {
+            for (long long q = 0; q < g.G; ++q) tmp[q] = (float)(*hv[c])[q];
+            BK(cudaMemcpyAsync(dst[c], tmp.data(), g.G * sizeof(float), cudaMemcpyHostToDevice, s), "upload velocity");
+            BK(cudaStreamSynchronize(s), "synchronize");
+        }
+    }
+    return PI_OK;
+}
+
+static pi_status read_forcing(pi_batch* b, int m, MemberForcing& f) {
+    BK(cudaMemcpyAsync(&f, b->F + m, sizeof f, cudaMemcpyDeviceToHost, b->stream), "read forcing");
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    return PI_OK;
+}
+static pi_status write_forcing(pi_batch* b, int m, const MemberForcing& f) {
+    BK(cudaMemcpyAsync(b->F + m, &f, sizeof f, cudaMemcpyHostToDevice, b->stream), "write forcing");
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    return PI_OK;
+}
+
+pi_status pi_batch_set_velocity(pi_batch* b, int32_t member, const double* u, const double* v, const double* w) {
+    pi_status e = check_mem(b, member, "pi_set_velocity");
+    if (e) return e;
+    if (!u || !v || !w) return bfail(b, PI_ERR_ARG, "pi_set_velocity: NULL argument");
+    MemberForcing f;
+    if ((e = read_forcing(b, member, f))) return e;
+    const int buf = (f.vel0[0] == velown(b, member, 0, 0)) ? 1 : 0;   // the own buffer vel₀ does not alias
+    if ((e = vel_copy32(b, member, u, v, w, velown(b, member, buf, 0), velown(b, member, buf, 1), velown(b, member, buf, 2)))) return e;
+    for (int c = 0; c < 3; ++c) f.vel1[c] = velown(b, member, buf, c);
+    return write_forcing(b, member, f);
+}
+
+pi_status pi_batch_set_velocity0(pi_batch* b, int32_t member, const double* u, const double* v, const double* w) {
+    pi_status e = check_mem(b, member, "pi_set_velocity0");
+    if (e) return e;
+    if (!u || !v || !w) return bfail(b, PI_ERR_ARG, "pi_set_velocity0: NULL argument");
+    MemberForcing f;
+    if ((e = read_forcing(b, member, f))) return e;
+    const int buf = (f.vel1[0] == velown(b, member, 0, 0)) ? 1 : 0;   // the own buffer vel₁ does not alias
+    if ((e = vel_copy32(b, member, u, v, w, velown(b, member, buf, 0), velown(b, member, buf, 1), velown(b, member, buf, 2)))) return e;
+    for (int c = 0; c < 3; ++c) f.vel0[c] = velown(b, member, buf, c);
+    return write_forcing(b, member, f);
+}
+
+pi_status pi_batch_set_PARF(pi_batch* b, int32_t member, const double* parf) {
+    pi_status e = check_mem(b, member, "pi_set_PARF");
+    if (e) return e;
+    if (!parf) return bfail(b, PI_ERR_ARG, "pi_set_PARF: NULL argument");
+    const long long n = (long long)b->mdh[member].Nx * b->mdh[member].Ny;
+    BK(cudaMemcpyAsync(b->stage, parf, n * sizeof(double), cudaMemcpyDefault, b->stream), "upload PARF");
+    k32_d2f<<<std::min<unsigned>(nblk(n, 256), 1024), 256, 0, b->stream>>>(b->PARF + b->mdh[member].col_off, b->stage, n);
+    BK(cudaGetLastError(), "convert PARF");
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    return PI_OK;
+}
+
+pi_status pi_batch_set_temp(pi_batch* b, int32_t member, const double* temp) {
+    pi_status e = check_mem(b, member, "pi_set_temp");
+    if (e) return e;
+    if (!temp) return bfail(b, PI_ERR_ARG, "pi_set_temp: NULL argument");
+    const MemberDev& d = b->mdh[member];
+    const long long n = (long long)d.Nx * d.Ny * d.Nz;
+    float* dst = b->tempown + d.cell_off;
+    // copy_interior!: only the interior is written; the halo stays zero
+    BK(cudaMemcpyAsync(b->stage, temp, n * sizeof(double), cudaMemcpyDefault, b->stream), "upload temp");
+    k32_scatter_interior<<<std::min<unsigned>(nblk(n, 256), 1024), 256, 0, b->stream>>>(d, dst, b->stage, d.Nx, d.Ny, d.Nz);
+    BK(cudaGetLastError(), "scatter temp");
+    MemberForcing f;
+    if ((e = read_forcing(b, member, f))) return e;
+    f.temp = dst;
+    return write_forcing(b, member, f);
+}
+
+pi_status pi_batch_set_flux_bc(pi_batch* b, int32_t member, int32_t tracer, int32_t face, int32_t kind,
+                               const double* values, int64_t nt) {
+    pi_status e = check_mem(b, member, "pi_set_flux_bc");
+    if (e) return e;
+    if (tracer < 0 || tracer >= PI_NTRACERS || face < 0 || face > 5 || kind < 0 || kind > 3)
+        return bfail(b, PI_ERR_ARG, "pi_set_flux_bc: bad argument");
+    MemberHost& h = b->mh[member];
+    const HostGrid& g = h.g;
+    size_t n1 = face <= PI_EAST ? g.Ny : g.Nx, n2 = face <= PI_NORTH ? g.Nz : g.Ny;
+    size_t n = kind == PI_BC_CONST ? 1 : kind == PI_BC_ARRAY2D ? n1 * n2 : kind == PI_BC_ARRAY3D ? n1 * n2 * (size_t)std::max<int64_t>(nt, 0) : 0;
+    if (kind == PI_BC_ARRAY3D && nt < 1) return bfail(b, PI_ERR_SHAPE, "BC: time-dependent flux needs nt >= 1");
+    if (n && !values) return bfail(b, PI_ERR_ARG, "pi_set_flux_bc: NULL values");
+    HostBC& hb = h.bcs[tracer][face];
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    if (hb.v) { cudaFree(hb.v); hb.v = nullptr; }
+    hb.kind = kind; hb.nt = nt;
+    if (n) {
+        std::vector<float> tmp(n);
+        for (size_t q = 0; q < n; ++q) tmp[q] = (float)values[q];
+        BK(cudaMalloc(&hb.v, n * sizeof(float)), "bc values");
+        BK(cudaMemcpyAsync(hb.v, tmp.data(), n * sizeof(float), cudaMemcpyHostToDevice, b->stream), "upload bc");
+    }
+    FluxBC32& d = b->bch[(size_t)b->mdh[member].bc_off + tracer * 6 + face];
+    d.kind = kind; d.nt = nt; d.v = hb.v; d.n1 = (int)n1; d.n2 = (int)n2;
+    int any = 0;
+    for (int q = 0; q < PI_NTRACERS * 6; ++q) if (b->bch[(size_t)b->mdh[member].bc_off + q].kind) any = 1;
+    b->mdh[member].any_bc = any;
+    BK(cudaMemcpyAsync(b->bcs, b->bch.data(), b->bch.size() * sizeof(FluxBC32), cudaMemcpyHostToDevice, b->stream), "upload bcs");
+    BK(cudaMemcpyAsync(b->md + member, &b->mdh[member], sizeof(MemberDev), cudaMemcpyHostToDevice, b->stream), "upload member");
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    return PI_OK;
+}
+
+pi_status pi_batch_set_series(pi_batch* b, int32_t member,
+                              const double* u, const double* v, const double* w, int64_t nvel, double dT_vel,
+                              const double* parf, int64_t npar, double dT_PAR,
+                              const double* temp, int64_t ntemp, double dT_temp, int32_t time_offset) {
+    pi_status e = check_mem(b, member, "pi_batch_set_series");
+    if (e) return e;
+    const int has_vel = u != nullptr;
+    if (!parf || !temp || npar < 1 || ntemp < 1 || (has_vel && (!v || !w || nvel < 1)))
+        return bfail(b, PI_ERR_ARG, "pi_batch_set_series: PARF and temp series are required; u, v, w together");
+    if (!(dT_PAR > 0) || !(dT_temp > 0) || (has_vel && !(dT_vel > 0))) return bfail(b, PI_ERR_ARG, "pi_batch_set_series: intervals must be positive");
+    if ((e = pi_batch_clear_series(b, member))) return e;
+    MemberHost& h = b->mh[member];
+    const HostGrid& g = h.g;
+    const MemberDev& d = b->mdh[member];
+    cudaStream_t s = b->stream;
+    MemberSeries& se = b->serh[member];
+    if (has_vel) {
+        BK(cudaMalloc(&h.ser_vel, (size_t)nvel * 3 * g.G * sizeof(float)), "velocity series");
+        int ex = g.topo[0] == PI_BOUNDED, ey = g.topo[1] == PI_BOUNDED, ez = g.topo[2] == PI_BOUNDED;
+        size_t nu = (size_t)(g.Nx + ex) * g.Ny * g.Nz, nv = (size_t)g.Nx * (g.Ny + ey) * g.Nz, nw = (size_t)g.Nx * g.Ny * (g.Nz + ez);
+        for (int64_t t = 0; t < nvel; ++t) {
+            float* base = h.ser_vel + (size_t)t * 3 * g.G;
+            if ((e = vel_copy32(b, member, u + t * nu, v + t * nv, w + t * nw, base, base + g.G, base + 2 * g.G))) return e;
+        }
+    }
+    const long long nf = (long long)g.Nx * g.Ny;
+    BK(cudaMalloc(&h.ser_parf, (size_t)npar * nf * sizeof(float)), "PARF series");
+    for (int64_t t = 0; t < npar; ++t) {
+        BK(cudaMemcpyAsync(b->stage, parf + t * nf, nf * sizeof(double), cudaMemcpyDefault, s), "upload PARF");
+        k32_d2f<<<std::min<unsigned>(nblk(nf, 256), 1024), 256, 0, s>>>(h.ser_parf + t * nf, b->stage, nf);
+        BK(cudaStreamSynchronize(s), "synchronize");
+    }
+    const long long nt3 = (long long)g.Nx * g.Ny * g.Nz;
+    BK(cudaMalloc(&h.ser_temp, (size_t)ntemp * g.G * sizeof(float)), "temperature series");
+    BK(cudaMemsetAsync(h.ser_temp, 0, (size_t)ntemp * g.G * sizeof(float), s), "clear temperature series");
+    for (int64_t t = 0; t < ntemp; ++t) {
+        BK(cudaMemcpyAsync(b->stage, temp + t * nt3, nt3 * sizeof(double), cudaMemcpyDefault, s), "upload temp");
+        k32_scatter_interior<<<std::min<unsigned>(nblk(nt3, 256), 1024), 256, 0, s>>>(d, h.ser_temp + t * g.G, b->stage, g.Nx, g.Ny, g.Nz);
+        BK(cudaStreamSynchronize(s), "synchronize");
+    }
+    BK(cudaGetLastError(), "upload series");
+    se.vel = h.ser_vel; se.nvel = has_vel ? nvel : 0; se.dT_vel = has_vel ? dT_vel : 1.0;
+    se.parf = h.ser_parf; se.npar = npar; se.dT_PAR = dT_PAR;
+    se.temp = h.ser_temp; se.ntemp = ntemp; se.dT_temp = dT_temp;
+    se.has_series = 1; se.has_vel = has_vel; se.time_offset = time_offset;
+    BK(cudaMemcpyAsync(b->S + member, &se, sizeof se, cudaMemcpyHostToDevice, s), "upload series table");
+    BK(cudaStreamSynchronize(s), "synchronize");
+    return PI_OK;
+}
+
+pi_status pi_batch_clear_series(pi_batch* b, int32_t member) {
+    pi_status e = check_mem(b, member, "pi_batch_clear_series");
+    if (e) return e;
+    MemberHost& h = b->mh[member];
+    MemberSeries& se = b->serh[member];
+    if (!se.has_series) return PI_OK;
+    MemberForcing f;
+    if ((e = read_forcing(b, member, f))) return e;
+    const long long G = h.g.G;
+    cudaStream_t s = b->stream;
+    // keep the bound snapshots as the member's own fields
+    auto in_series = [&](const float* p) {
+        return h.ser_vel && p >= h.ser_vel && p < h.ser_vel + (size_t)se.nvel * 3 * G;
+    };
+    const bool v1s = in_series(f.vel1[0]), v0s = in_series(f.vel0[0]);
+    if (v1s) {
+        for (int c = 0; c < 3; ++c) BK(cudaMemcpyAsync(velown(b, member, 1, c), f.vel1[c], G * sizeof(float), cudaMemcpyDeviceToDevice, s), "keep velocity");
+        if (v0s && f.vel0[0] == f.vel1[0]) for (int c = 0; c < 3; ++c) f.vel0[c] = velown(b, member, 1, c);
+        for (int c = 0; c < 3; ++c) f.vel1[c] = velown(b, member, 1, c);
+    }
+    if (in_series(f.vel0[0])) {
+        for (int c = 0; c < 3; ++c) BK(cudaMemcpyAsync(velown(b, member, 0, c), f.vel0[c], G * sizeof(float), cudaMemcpyDeviceToDevice, s), "keep velocity");
+        for (int c = 0; c < 3; ++c) f.vel0[c] = velown(b, member, 0, c);
+    }
+    if (h.ser_temp && f.temp >= h.ser_temp && f.temp < h.ser_temp + (size_t)se.ntemp * G) {
+        BK(cudaMemcpyAsync(b->tempown + b->mdh[member].cell_off, f.temp, G * sizeof(float), cudaMemcpyDeviceToDevice, s), "keep temperature");
+        f.temp = b->tempown + b->mdh[member].cell_off;
+    }
+    if ((e = write_forcing(b, member, f))) return e;
+    free_series(h);
+    float* keep[3] = { se.velh_buf[0], se.velh_buf[1], se.velh_buf[2] };
+    se = MemberSeries{};
+    for (int c = 0; c < 3; ++c) se.velh_buf[c] = keep[c];
+    se.dT_vel = se.dT_PAR = se.dT_temp = 1.0;
+    BK(cudaMemcpyAsync(b->S + member, &se, sizeof se, cudaMemcpyHostToDevice, s), "upload series table");
+    BK(cudaStreamSynchronize(s), "synchronize");
+    return PI_OK;
+}
+
+pi_status pi_batch_set_time_offset(pi_batch* b, int32_t member, int32_t time_offset) {
+    pi_status e = check_mem(b, member, "pi_batch_set_time_offset");
+    if (e) return e;
+    b->serh[member].time_offset = time_offset;
+    BK(cudaMemcpyAsync(b->S + member, &b->serh[member], sizeof(MemberSeries), cudaMemcpyHostToDevice, b->stream), "upload series table");
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    return PI_OK;
+}
+
+pi_status pi_batch_synchronize(pi_batch* b) {
+    if (!b) return bfail(b, PI_ERR_ARG, "pi_batch_synchronize: NULL batch");
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    return check_errors(b);
+}
+
+pi_status pi_batch_step(pi_batch* b, double dT, int64_t nsteps, int32_t sync) {
+    if (!b) return bfail(b, PI_ERR_ARG, "pi_batch_step: NULL batch");
+    if (!(dT > 0) || nsteps < 0) return bfail(b, PI_ERR_ARG, "pi_batch_step: ΔT must be positive and nsteps >= 0");
+    pi_status e = build_tables(b);
+    if (e) return e;
+    bool any3d = false;
+    for (const auto& h : b->mh)
+        for (int n = 0; n < PI_NTRACERS; ++n) for (int f = 0; f < 6; ++f) any3d = any3d || h.bcs[n][f].kind == PI_BC_ARRAY3D;
+    if (any3d) {
+        // getbc(bc, i, j, t) of a time-dependent flux reads bc[i, j, iteration] (boundary_conditions.jl:44-52)
+        int64_t it = 0;
+        if ((e = pi_batch_get_time(b, &it, nullptr))) return e;
+        for (const auto& h : b->mh)
+            for (int n = 0; n < PI_NTRACERS; ++n)
+                for (int f = 0; f < 6; ++f)
+                    if (h.bcs[n][f].kind == PI_BC_ARRAY3D && h.bcs[n][f].nt < it + nsteps)
+                        return bfail(b, PI_ERR_SHAPE, "BoundsError: time-dependent flux boundary condition has " +
+                                                          std::to_string(h.bcs[n][f].nt) + " snapshots, step " +
+                                                          std::to_string(it + nsteps) + " needs more");
+    }
+    b->last_dT = dT;
+    BK(cudaMemsetAsync(&b->st->call_step, 0, sizeof(int64_t), b->stream), "reset call step");
+    if (b->profiling || !b->use_graph) {
+        for (int64_t i = 0; i < nsteps; ++i) {
+            if ((e = enqueue_step(b, dT, b->cur))) return e;
+            b->cur ^= 1;
+        }
+    } else {
+        if (b->graph_dT != dT || !b->gexec[0]) { if ((e = capture_graphs(b, dT))) return e; }
+        for (int64_t i = 0; i < nsteps; ++i) {
+            BK(cudaGraphLaunch(b->gexec[b->cur], b->stream), "graph launch");
+            b->cur ^= 1;
+        }
+    }
+    if (sync) return pi_batch_synchronize(b);
+    return PI_OK;
+}
+
+pi_status pi_batch_get_time(pi_batch* b, int64_t* iteration, double* t) {
+    if (!b) return bfail(b, PI_ERR_ARG, "pi_get_time: NULL batch");
+    StepState hs{};
+    BK(cudaMemcpyAsync(&hs, b->st, sizeof hs, cudaMemcpyDeviceToHost, b->stream), "read step state");
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    if (iteration) *iteration = hs.iteration;
+    if (t) *t = hs.t;
+    return PI_OK;
+}
+
+pi_status pi_batch_set_time(pi_batch* b, int64_t iteration, double t) {
+    if (!b) return bfail(b, PI_ERR_ARG, "pi_set_time: NULL batch");
+    StepState hs{};
+    BK(cudaMemcpyAsync(&hs, b->st, sizeof hs, cudaMemcpyDeviceToHost, b->stream), "read step state");
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    hs.iteration = iteration; hs.t = t;
+    BK(cudaMemcpyAsync(b->st, &hs, sizeof hs, cudaMemcpyHostToDevice, b->stream), "write step state");
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    return PI_OK;
+}
+
+pi_status pi_batch_count_active(pi_batch* b, int32_t member, int32_t sp, int64_t* n) {
+    if (!b || !n || member < -1 || member >= b->nm || sp < -1 || sp >= b->nsp) return bfail(b, PI_ERR_ARG, "pi_count_active: bad argument");
+    long long first, count;
+    if (member < 0) { first = 0; count = b->Stot; }
+    else {
+        const MemberDev& d = b->mdh[member];
+        first = d.slot_off + (sp < 0 ? 0 : (long long)sp * d.C);
+        count = sp < 0 ? (long long)b->nsp * d.C : d.C;
+    }
+    unsigned long long h = 0;
+    BK(cudaMemsetAsync(b->scratch, 0, sizeof h, b->stream), "zero count");
+    k32_count_active<<<std::max(1u, std::min<unsigned>(nblk(count, 256), 148 * 4)), 256, 0, b->stream>>>(b->P.flags + first, count, b->scratch);
+    BK(cudaGetLastError(), "k32_count_active");
+    BK(cudaMemcpyAsync(&h, b->scratch, sizeof h, cudaMemcpyDeviceToHost, b->stream), "download count");
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    *n = (int64_t)h;
+    return PI_OK;
+}
+
+pi_status pi_batch_get_diag(pi_batch* b, int32_t member, int32_t kind, int32_t sp, double* out) {
+    pi_status e = check_mem(b, member, "pi_get_diag");
+    if (e) return e;
+    if (!out) return bfail(b, PI_ERR_ARG, "pi_get_diag: bad argument");
+    const MemberDev& d = b->mdh[member];
+    const long long G = d.G;
+    const unsigned grid = std::min<unsigned>(nblk(G, 256), 1024);
+    if (kind == PI_DIAG_PAR) k32_f2d<<<grid, 256, 0, b->stream>>>(b->stage, b->diag_par + d.cell_off, G);
+    else {
+        if (sp < 0 || sp >= b->nsp || kind < PI_DIAG_NUM || kind > PI_DIAG_DVID) return bfail(b, PI_ERR_ARG, "pi_get_diag: bad kind/species");
+        k32_u2d<<<grid, 256, 0, b->stream>>>(b->stage, b->dcnt + ((long long)sp * 4 + (kind - PI_DIAG_NUM)) * b->Gtot + d.cell_off, G);
+    }
+    BK(cudaGetLastError(), "convert diag");
+    BK(cudaMemcpyAsync(out, b->stage, G * sizeof(double), cudaMemcpyDeviceToHost, b->stream), "download diag");
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    return PI_OK;
+}
+
+pi_status pi_batch_reset_diags(pi_batch* b) {
+    if (!b) return bfail(b, PI_ERR_ARG, "pi_reset_diags: NULL batch");
+    BK(cudaMemsetAsync(b->diag_par, 0, b->Gtot * sizeof(float), b->stream), "reset diags");
+    BK(cudaMemsetAsync(b->dcnt, 0, (size_t)b->nsp * 4 * b->Gtot * sizeof(uint32_t), b->stream), "reset diags");
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    return PI_OK;
+}
+
+pi_status pi_batch_budget(pi_batch* b, int32_t member, double out[6]) {
+    pi_status e = check_mem(b, member, "pi_batch_budget");
+    if (e) return e;
+    if (!out) return bfail(b, PI_ERR_ARG, "pi_batch_budget: NULL out");
+    const MemberDev& d = b->mdh[member];
+    const int nb = 512;
+    std::vector<double> h(3 * nb);
+    k32_budget_cells<<<nb, 256, 0, b->stream>>>(d, b->trbuf[b->cur], b->dzF, b->Gtot, b->partial);
+    BK(cudaGetLastError(), "k32_budget_cells");
+    BK(cudaMemcpyAsync(h.data(), b->partial, 3 * nb * sizeof(double), cudaMemcpyDeviceToHost, b->stream), "download budget");
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    for (int r = 0; r < 3; ++r) { double s = 0.0; for (int q = 0; q < nb; ++q) s += h[q * 3 + r]; out[r] = s; }
+    k32_budget_inds<<<nb, 256, 0, b->stream>>>(d, b->nsp, b->sp + (size_t)member * b->nsp, b->P, b->partial);
+    BK(cudaGetLastError(), "k32_budget_inds");
+    BK(cudaMemcpyAsync(h.data(), b->partial, 3 * nb * sizeof(double), cudaMemcpyDeviceToHost, b->stream), "download budget");
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    for (int r = 0; r < 3; ++r) { double s = 0.0; for (int q = 0; q < nb; ++q) s += h[q * 3 + r]; out[3 + r] = s; }
+    return PI_OK;
+}
+
+pi_status pi_batch_get_stream(pi_batch* b, void** stream) {
+    if (!b || !stream) return bfail(b, PI_ERR_ARG, "pi_get_stream: NULL argument");
+    *stream = (void*)b->stream;
+    return PI_OK;
+}
+
+pi_status pi_batch_profile_enable(pi_batch* b, int32_t on) {
+    if (!b) return bfail(b, PI_ERR_ARG, "pi_profile_enable: NULL batch");
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    drain(b);
+    b->prof_names.clear(); b->prof_count.clear(); b->prof_ms.clear();
+    b->profiling = on ? 1 : 0;
+    return PI_OK;
+}
+
+pi_status pi_batch_profile_read(pi_batch* b, int32_t max, char* names, size_t names_len,
+                                int64_t* launches, double* ms, int32_t* n) {
+    if (!b || !n) return bfail(b, PI_ERR_ARG, "pi_profile_read: NULL argument");
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    drain(b);
+    int32_t k = (int32_t)b->prof_names.size();
+    *n = k;
+    size_t off = 0;
+    for (int32_t q = 0; q < k && q < max; ++q) {
+        if (launches) launches[q] = b->prof_count[q];
+        if (ms) ms[q] = b->prof_ms[q];
+        if (names) {
+            const std::string& nm = b->prof_names[q];
+            if (off + nm.size() + 1 <= names_len) { memcpy(names + off, nm.c_str(), nm.size() + 1); off += nm.size() + 1; }
+        }
+    }
+    return PI_OK;
+}
+
+// Times `k` eager steps per candidate with per-kernel events and keeps, for each knob, the value
+// whose kernel ran fastest. Knobs are tuned one after another (coordinate descent).
+pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t k, char* report, size_t report_len) {
+    if (!b || !(dT > 0) || k < 1) return bfail(b, PI_ERR_ARG, "pi_batch_autotune: bad argument");
+    const int was = b->profiling;
+    std::string rep;
+    auto kernel_ms = [&](const char* name, double& out) -> pi_status {
+        pi_status e;
+        b->profiling = 1;
+        b->prof_names.clear(); b->prof_count.clear(); b->prof_ms.clear();
+        b->last_dT = dT;
+        if ((e = build_tables(b))) return e;
+        for (int i = 0; i < k; ++i) { if ((e = enqueue_step(b, dT, b->cur))) return e; b->cur ^= 1; }
+        BK(cudaStreamSynchronize(b->stream), "synchronize");
+        drain(b);
+        if ((e = check_errors(b))) return e;
+        out = 0.0;
+        for (size_t q = 0; q < b->prof_names.size(); ++q) if (b->prof_names[q] == name) out = b->prof_ms[q] / k;
+        return PI_OK;
+    };
+    struct Knob { const char* kernel; int* field; std::vector<int> values; const char* label; int threads_per_value; };
+    Tuning& t = b->tune;
+    std::vector<Knob> knobs = {
+        { "k32_move", &t.bs_move, {128, 256, 512, 1024}, "move block", 1 },
+        { "k32_move", &t.persist_move, {0, 2, 4, 8}, "move blocks/SM (0 = one tile per block)", 0 },
+        { "k32_physiology", &t.bs_phys, {128, 256, 512, 1024}, "physiology block", 1 },
+        { "k32_physiology", &t.persist_phys, {0, 2, 4, 8}, "physiology blocks/SM (0 = one tile per block)", 0 },
+        { "k32_assign", &t.bs_assign, {128, 256, 512, 1024}, "assign block", 1 },
+        { "k32_sweep_x", &t.wpb_x, {2, 4, 8}, "sweep_x warps/block", 32 },
+        { "k32_sweep_y", &t.Ly, {4, 8, 16, 32}, "sweep_y rows per warp", 0 },
+        { "k32_sweep_y", &t.wpb_y, {2, 4, 8}, "sweep_y warps/block", 32 },
+        { "k32_sweep_z", &t.Lz, {4, 8, 16, 32}, "sweep_z levels per warp", 0 },
+        { "k32_sweep_z", &t.wpb_z, {2, 4, 8}, "sweep_z warps/block", 32 },
+        { "k32_tail", &t.wpb_tail, {2, 4, 8}, "tail warps/block", 32 },
+        { "k32_par", &t.wpb_par, {1, 2, 4, 8}, "par warps/block", 32 },
+    };
+    // the largest block each kernel can be launched with (registers per thread)
+    auto max_threads = [](const char* kernel) -> int {
+        cudaFuncAttributes fa{};
+        const void* f = nullptr;
+        if (!strcmp(kernel, "k32_move")) f = (const void*)k32_move;
+        else if (!strcmp(kernel, "k32_physiology")) f = (const void*)k32_physiology;
+        else if (!strcmp(kernel, "k32_assign")) f = (const void*)k32_assign;
+        else if (!strcmp(kernel, "k32_sweep_x")) f = (const void*)k32_sweep_x;
+        else if (!strcmp(kernel, "k32_sweep_y")) f = (const void*)k32_sweep_y;
+        else if (!strcmp(kernel, "k32_sweep_z")) f = (const void*)k32_sweep_z;
+        else if (!strcmp(kernel, "k32_tail")) f = (const void*)k32_tail;
+        else if (!strcmp(kernel, "k32_par")) f = (const void*)k32_par;
+        if (!f || cudaFuncGetAttributes(&fa, f) != cudaSuccess) return 256;
+        return fa.maxThreadsPerBlock;
+    };
+    free_graphs(b);
+    for (auto& kb : knobs) {
+        int best = *kb.field;
+        double best_ms = 1e300;
+        const int lim = max_threads(kb.kernel);
+        for (int v : kb.values) {
+            if (kb.threads_per_value && v * kb.threads_per_value > lim) continue;
+            *kb.field = v;
+            double ms = 0.0;
+            pi_status e = kernel_ms(kb.kernel, ms);
+            if (e) { b->profiling = was; return e; }
+            if (ms < best_ms) { best_ms = ms; best = v; }
+        }
+        *kb.field = best;
+        char line[160];
+        snprintf(line, sizeof line, "%s = %d (%.4f ms)\n", kb.label, best, best_ms);
+        rep += line;
+    }
+    b->profiling = was;
+    b->prof_names.clear(); b->prof_count.clear(); b->prof_ms.clear();
+    pi_status e = build_tables(b);
+    if (e) return e;
+    if (report && report_len) {
+        size_t n = std::min(report_len - 1, rep.size());
+        memcpy(report, rep.c_str(), n);
+        report[n] = 0;
+    }
+    return PI_OK;
+}
+
+}  // extern "C"

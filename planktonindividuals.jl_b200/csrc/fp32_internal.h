@@ -1,0 +1,121 @@
+// FP32 form: declarations shared by the FP32 kernels and their host orchestration.
+//
+// A batch is a set of independent members (each with its own grid, individuals, tracers, forcing
+// and seed) that step together: every phase of the step is one launch over all members. A single
+// FP32 model is a batch of one member.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/pib200.h"
+#include "../../include/pi_numerics.h"
+
+// Individual flag byte (carried between steps): ac and the three decisions of get_probability!.
+#define F32_AC   1u
+#define F32_GRAZ 2u
+#define F32_MORT 4u
+#define F32_DVID 8u
+// Status byte: ac at cell-lookup time in this step, and "the find_inds! cell differs from the
+// cell of the position" (daughters in their birth step, uploaded states).
+#define F32_ST_AC0   1u
+#define F32_ST_STALE 2u
+
+// Device error word bits.
+#define F32_ERR_DOMAIN   1u
+#define F32_ERR_CAPACITY 2u
+#define F32_ERR_FORCING  4u
+
+// Slots are processed in tiles of this many consecutive slots of one (member, species) segment.
+#define F32_TILE 1024
+
+// Per-member description used by the kernels.
+struct MemberDev {
+    int Nx, Ny, Nz, Hx, Hy, Hz, Gx, Gy, Gz;
+    int tx, ty, tz;
+    int all_water;
+    int any_bc;
+    float dx, dy;
+    long long cell_off;     // first cell of the member's halo-padded grid in the batch cell space
+    long long G;            // (Nx+2Hx)(Ny+2Hy)(Nz+2Hz)
+    long long col_off;      // first of the member's Nx*Ny surface columns
+    long long slot_off;     // first slot of species 0; species s starts at slot_off + s*C
+    long long C;            // capacity per species
+    int dz_off;             // first of the member's Gz levels in dzF/dzC
+    int bc_off;             // first of the member's 14*6 flux boundary conditions
+    uint64_t seed;
+    double fx_unit;         // mmol per fixed-point unit of the particle→grid mass sums
+    double chl_unit;        // mg Chl per fixed-point unit of the Chl sums
+};
+
+// Forcing of a member for the current step.
+struct MemberForcing {
+    const float* vel0[3];   // halo-padded velocity of the previous step
+    const float* vel1[3];   // halo-padded velocity of this step
+    const float* velh[3];   // (vel0 + vel1) / 2, or vel1 itself when vel0 and vel1 are the same field
+    const float* temp;      // halo-padded temperature
+};
+
+// Forcing time series resident on the device (PlanktonSimulation's arrays), or none.
+struct MemberSeries {
+    const float* vel;       // nvel snapshots of 3 halo-padded fields (u, v, w), G each
+    long long nvel;
+    double dT_vel;
+    const float* parf;      // npar snapshots of Nx*Ny
+    long long npar;
+    double dT_PAR;
+    const float* temp;      // ntemp halo-padded snapshots
+    long long ntemp;
+    double dT_temp;
+    int has_series;
+    int has_vel;
+    int time_offset;        // bit 0 vel, bit 1 PAR, bit 2 temp: index by the step within the call
+    float* velh_buf[3];     // scratch for vel½ (member-local fields)
+};
+
+// Step counters on the device (graph replay needs no host argument).
+struct StepState {
+    int64_t iteration;      // model.iteration
+    double t;               // model.t
+    int64_t call_step;      // steps taken in the current update! call (time_offset indexing)
+    int64_t err_iter;       // iteration at which a capacity error occurred
+    int32_t err_member;     // member of that error
+    int32_t pad;
+};
+
+// Individuals of all members and species.
+struct IndDev32 {
+    int32_t* cell;          // interior cell of the position: ci + (Nx+1)(cj + (Ny+1) ck); -1 inactive
+    int32_t* scell;         // find_inds! cell (xi + (Gx+1)(yi + (Gy+1) zi)) when F32_ST_STALE
+    float *ox, *oy, *oz;    // in-cell offsets, in [0, 1)
+    float *Bm, *Cq, *Nq, *Pq, *Chl, *age, *gen;
+    uint8_t* flags;
+    uint8_t* stat;
+};
+
+struct SpeciesDev32 {
+    float Nsuper, Cquota, Chl2Cint, alpha, Phi, Topt, Tmax, Ea;
+    float PCmax, VDOCmax, VNO3max, VNH4max, VPO4max;
+    float KsatDOC, KsatNH4, KsatNO3, KsatPO4, Cqmax, Nqmax, Pqmax;
+    float Chl2N, R_NC, R_PC, k_mtb, respir, grz_P, dvid_P, dvid_reg, dvid_reg2;
+    float mort_P, mort_reg, grazFracC, grazFracN, grazFracP, mortFracC, mortFracN, mortFracP;
+    int dvid_type;
+    float OGT_rate;         // exp(-Ea / (R (Topt + 273.15))), a constant of the species
+};
+
+struct BgcDev32 {
+    float kw, kc, kDOC, Nit, kDON, kDOP, kPOC, kPON, kPOP;
+    float kappa_h, kappa_v, kappa_hP, kappa_vP;
+    int shared_graz;
+    float w_sink_org, w_sink_inorg, lambda_POC, lambda_min, kdiss, lambda_dust, lambda_Fe, ligand, DFeFrac;
+};
+
+struct FluxBC32 {
+    int kind;
+    int n1, n2;
+    long long nt;
+    const float* v;
+};
+
+// Per-cell fixed-point accumulators of the particle→grid sums (zeroed as they are consumed).
+enum { ACC_DIC = 0, ACC_NH4, ACC_NO3, ACC_PO4, ACC_DOC, ACC_DON, ACC_DOP, ACC_POC, ACC_PON, ACC_POP, ACC_N };

@@ -1,0 +1,1143 @@
+// FP32 form: kernels. Every launch covers all members of a batch; blocks and warps find their
+// member through work tables built when the batch is created.
+//
+// The formulas are those of the FP64 kernels (and of the reference lines they cite) evaluated in
+// Float32, with three changes of representation:
+//  - a position is an interior cell (ci, cj, ck) plus an in-cell offset in [0, 1): find_inds! is
+//    the cell itself, interpolation weights come straight from the offsets, and the precision of a
+//    position does not degrade with the size of the grid;
+//  - particle→grid sums (Chl for light, consumption, grazing and mortality losses) are 64-bit
+//    fixed-point integers added with atomics; integer addition commutes, so the sums do not depend
+//    on the order in which individuals are visited and no sort is needed for determinism; pop and
+//    the diagnostic counts are exact integer counts;
+//  - Sz is not stored: it is Bm / (Cquota Nsuper), as update_cellsize_kernel! sets it.
+// FP64 is used for the fixed-point conversions, the mass budgets and the DST3FL limiter ratio
+// where the centred gradient is within a few FP32 ulps of zero.
+#pragma once
+
+#include "fp32_internal.h"
+
+namespace p32 {
+
+#define THMAX_F 1.0e20f
+#define EPS20_F 1.0e-20f
+
+struct Tab32 {
+    const MemberDev* md;
+    int nsp;
+    const int2* tiles;        // {segment = member*nsp + species, first slot}, F32_TILE slots each
+    int ntiles;
+    const int* seg_tile0;     // first tile of each segment (nseg + 1 entries)
+    const int4* ix; int nix;  // x sweep warps {m, j, k, i0}: 31 cells from i0
+    const int4* iy; int niy;  // y sweep warps {m, i0, j0, k}: 32 columns × Ly rows
+    const int4* iz; int niz;  // z sweep warps {m, i0, j, k0}: 32 columns × Lz levels
+    const int4* ic; int nic;  // cell-row warps {m, i0, j, k}: 32 cells from i0
+    const int4* icol; int nicol;  // column warps {m, i0, j, 0}
+    int Ly, Lz;
+};
+
+__device__ __forceinline__ int gid3(const MemberDev& m, int i, int j, int k) {   // 1-based, member-local
+    return (i - 1) + m.Gx * ((j - 1) + m.Gy * (k - 1));
+}
+__device__ __forceinline__ int lm32(const MemberDev& m, const uint8_t* __restrict__ lm, int i, int j, int k) {
+    return m.all_water ? 1 : (int)lm[m.cell_off + gid3(m, i, j, k)];
+}
+__device__ __forceinline__ float mulbf(float x, int b) { return b ? x : copysignf(0.0f, x); }
+__device__ __forceinline__ void seterr(uint32_t* err, uint32_t bit) { atomicOr(err, bit); }
+__device__ __forceinline__ bool stopped(const uint32_t* err) {
+    return (*(volatile const uint32_t*)err & F32_ERR_CAPACITY) != 0;
+}
+__device__ __forceinline__ void seg_of(const Tab32& T, int seg, int& m, int& s) { m = seg / T.nsp; s = seg - m * T.nsp; }
+
+// ------------------------------------------------------------------------------------------
+// cells and positions
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ void unpack_int(const MemberDev& m, int32_t code, int& ci, int& cj, int& ck) {
+    ci = code % (m.Nx + 1);
+    const int r = code / (m.Nx + 1);
+    cj = r % (m.Ny + 1);
+    ck = r / (m.Ny + 1);
+}
+__device__ __forceinline__ int32_t pack_int(const MemberDev& m, int ci, int cj, int ck) {
+    return ci + (m.Nx + 1) * (cj + (m.Ny + 1) * ck);
+}
+__device__ __forceinline__ int32_t pack_halo(const MemberDev& m, int xi, int yi, int zi) {
+    return xi + (m.Gx + 1) * (yi + (m.Gy + 1) * zi);
+}
+__device__ __forceinline__ void unpack_halo(const MemberDev& m, int32_t c, int& xi, int& yi, int& zi) {
+    xi = c % (m.Gx + 1);
+    const int r = c / (m.Gx + 1);
+    yi = r % (m.Gy + 1);
+    zi = r / (m.Gy + 1);
+}
+// halo-inclusive member-local cell of an interior position cell (find_inds!, Individuals/utils.jl:2-7)
+__device__ __forceinline__ int q_of(const MemberDev& m, int ci, int cj, int ck) {
+    return gid3(m, ci + 1 + m.Hx, cj + 1 + m.Hy, ck + 1 + m.Hz);
+}
+__device__ __forceinline__ bool interior_q(const MemberDev& m, int q) {
+    const int i = q % m.Gx + 1, r = q / m.Gx, j = r % m.Gy + 1, k = r / m.Gy + 1;
+    return i > m.Hx && i <= m.Nx + m.Hx && j > m.Hy && j <= m.Ny + m.Hy && k > m.Hz && k <= m.Nz + m.Hz;
+}
+
+struct Ax1 { int c; float o; };
+
+// particle_boundary_condition (particle_advection_kernels.jl:2-11) on x = c + o
+__device__ __forceinline__ void bc_axis(Ax1& a, int N, int topo) {
+    const bool above = a.c > N || (a.c == N && a.o > 0.0f);
+    const bool below = a.c < 0;
+    if (topo == PI_PERIODIC) {
+        if (above) a.c -= N;
+        else if (below) a.c += N;
+    } else if (above || below) {              // x → 2N − x or x → −x
+        const int pivot = above ? 2 * N : 0;
+        if (a.o > 0.0f) { a.c = pivot - a.c - 1; a.o = 1.0f - a.o; } else { a.c = pivot - a.c; }
+        if (a.o >= 1.0f) { a.c += 1; a.o = 0.0f; }
+    }
+}
+__device__ __forceinline__ void move(Ax1& a, float d, int N, int topo) {
+    const float o = a.o + d;
+    const float n = floorf(o);
+    a.c += (int)n;
+    a.o = o - n;
+    if (a.o >= 1.0f) { a.c += 1; a.o = 0.0f; }
+    bc_axis(a, N, topo);
+}
+
+// index and weight along one axis for a face-centred (own axis) or cell-centred field
+// (interpolation.jl:3-83: x + 1 or x + 0.5 split into trunc and mod)
+__device__ __forceinline__ void axis_iw(const Ax1& a, int H, bool face, int& idx, float& w) {
+    if (face) { idx = a.c + 1 + H; w = a.o; }
+    else if (a.o < 0.5f) { idx = a.c + H; w = a.o + 0.5f; }
+    else { idx = a.c + 1 + H; w = a.o - 0.5f; }
+}
+__device__ __forceinline__ int clampi(int v, int lo, int hi, uint32_t* err) {
+    if (v < lo) { seterr(err, F32_ERR_DOMAIN); return lo; }
+    if (v > hi) { seterr(err, F32_ERR_DOMAIN); return hi; }
+    return v;
+}
+
+// trilinear interpolation of one velocity component (member-local field pointer)
+template <int COMP>
+__device__ __forceinline__ float itpl32(const MemberDev& m, const float* __restrict__ f,
+                                        const float* __restrict__ dzC, const Ax1& X, const Ax1& Y,
+                                        const Ax1& Z, uint32_t* err) {
+    int i, j, k;
+    float xd, yd, zd;
+    axis_iw(X, m.Hx, COMP == 0, i, xd);
+    axis_iw(Y, m.Hy, COMP == 1, j, yd);
+    axis_iw(Z, m.Hz, COMP == 2, k, zd);
+    i = clampi(i, 1, m.Gx - 1, err); j = clampi(j, 1, m.Gy - 1, err); k = clampi(k, 1, m.Gz - 1, err);
+    const int q = gid3(m, i, j, k);
+    const int sy = m.Gx, sz = m.Gx * m.Gy;
+    const float a0 = (1.0f - xd) * (1.0f - yd), a1 = (1.0f - xd) * yd, a2 = xd * (1.0f - yd), a3 = xd * yd;
+    const float lo = a0 * __ldg(f + q) + a1 * __ldg(f + q + sy) + a2 * __ldg(f + q + 1) + a3 * __ldg(f + q + 1 + sy);
+    const float hi = a0 * __ldg(f + q + sz) + a1 * __ldg(f + q + sy + sz) + a2 * __ldg(f + q + 1 + sz) + a3 * __ldg(f + q + 1 + sy + sz);
+    if (COMP == 0) return ((1.0f - zd) * lo + zd * hi) / m.dx;
+    if (COMP == 1) return ((1.0f - zd) * lo + zd * hi) / m.dy;
+    return (1.0f - zd) * lo / dzC[m.dz_off + k - 1] + zd * hi / dzC[m.dz_off + k];
+}
+
+// the draws of the FP64 form (same keys, same numbers; lattice values are exact in float)
+__device__ __forceinline__ void draw3f(uint64_t seed, uint32_t iter, uint32_t sp, uint32_t purpose,
+                                       uint32_t slot, float& r0, float& r1, float& r2) {
+    uint32_t ctr[4] = { slot, iter, (sp & 0xFFFFu) | (purpose << 16), 0x706c6b74u };
+    uint32_t key[2] = { (uint32_t)seed, (uint32_t)(seed >> 32) };
+    uint32_t o[4];
+    pi_philox4x32_10(ctr, key, o);
+    r0 = (float)(o[0] >> 8) * 0x1p-24f;
+    r1 = (float)(o[1] >> 8) * 0x1p-24f;
+    r2 = (float)(o[2] >> 8) * 0x1p-24f;
+}
+
+__device__ __forceinline__ void add_fixed(unsigned long long* a, float v, double unit) {
+    const long long x = __double2ll_rn((double)v / unit);
+    if (x) atomicAdd(a, (unsigned long long)x);
+}
+
+// ------------------------------------------------------------------------------------------
+// step prologue: forcing of the step, vel½
+// ------------------------------------------------------------------------------------------
+
+// update!'s forcing selection (Simulation/update.jl:14-26) for members with device-resident
+// series, from model.t before the step (or the step index of the call with time_offset), and the
+// choice of the vel½ buffer. One block per member.
+__global__ void k32_bind(int nm, const MemberDev* __restrict__ md, const MemberSeries* __restrict__ S,
+                         MemberForcing* __restrict__ F, const StepState* __restrict__ st, double dT,
+                         float* __restrict__ PARF, uint32_t* err) {
+    const int m = blockIdx.x;
+    if (m >= nm || stopped(err)) return;
+    const MemberSeries& s = S[m];
+    const MemberDev& M = md[m];
+    __shared__ long long tp_sh;
+    if (threadIdx.x == 0) {
+        MemberForcing f = F[m];
+        if (s.has_series) {
+            const double tm = st->t, tc = (double)st->call_step * dT;
+            if (s.has_vel) {
+                long long tv = (long long)floor(((s.time_offset & 1) ? tc : tm) / s.dT_vel);
+                if (tv < 0 || tv >= s.nvel) { seterr(err, F32_ERR_FORCING); tv = tv < 0 ? 0 : s.nvel - 1; }
+                for (int c = 0; c < 3; ++c) f.vel1[c] = s.vel + (tv * 3 + c) * M.G;
+            }
+            long long tt = (long long)floor(((s.time_offset & 4) ? tc : tm) / s.dT_temp);
+            if (tt < 0 || tt >= s.ntemp) { seterr(err, F32_ERR_FORCING); tt = tt < 0 ? 0 : s.ntemp - 1; }
+            f.temp = s.temp + tt * M.G;
+            long long tp = (long long)floor(((s.time_offset & 2) ? tc : tm) / s.dT_PAR);
+            if (tp < 0 || tp >= s.npar) { seterr(err, F32_ERR_FORCING); tp = tp < 0 ? 0 : s.npar - 1; }
+            tp_sh = tp;
+        }
+        for (int c = 0; c < 3; ++c) f.velh[c] = (f.vel0[c] == f.vel1[c]) ? f.vel1[c] : s.velh_buf[c];
+        F[m] = f;
+    }
+    __syncthreads();
+    if (!s.has_series) return;
+    const long long n = (long long)M.Nx * M.Ny;
+    const float* src = s.parf + tp_sh * n;
+    for (long long q = threadIdx.x; q < n; q += blockDim.x) PARF[M.col_off + q] = src[q];
+}
+
+// vel½ = (vel₀ + vel₁) * 0.5 (time_step.jl:17-19) for members whose two fields differ.
+// Grid: (x blocks, members).
+__global__ void k32_velhalf(const MemberDev* __restrict__ md, const MemberForcing* __restrict__ F,
+                            const uint32_t* err) {
+    const int m = blockIdx.y;
+    if (stopped(err)) return;
+    const MemberForcing& f = F[m];
+    if (f.velh[0] == f.vel1[0]) return;
+    const long long G = md[m].G;
+    float* h0 = (float*)f.velh[0];
+    float* h1 = (float*)f.velh[1];
+    float* h2 = (float*)f.velh[2];
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < G; q += (long long)gridDim.x * blockDim.x) {
+        h0[q] = (f.vel0[0][q] + f.vel1[0][q]) * 0.5f;
+        h1[q] = (f.vel0[1][q] + f.vel1[1][q]) * 0.5f;
+        h2[q] = (f.vel0[2][q] + f.vel1[2][q]) * 0.5f;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// (a)+(e) particles: RK4 + diffusion + find_inds!, pop and Chl into the per-cell sums, then the
+// grazing/mortality decisions of the previous step (inactivate!, calc_loss!, diagnostics) and the
+// division/free counts of each tile of slots for the compaction.
+// ------------------------------------------------------------------------------------------
+struct MoveArgs {
+    Tab32 T;
+    IndDev32 P;
+    const SpeciesDev32* sp;        // [member * nsp + species]
+    const BgcDev32* bgc;           // [member]
+    const MemberForcing* F;
+    const float* dzC;
+    const StepState* st;
+    float dT;
+    long long Gtot;
+    int* pop;                      // Gtot: all species
+    int* pop_sp;                   // nsp × Gtot when grazing is not shared, else null
+    unsigned long long* chl_acc;   // Gtot
+    unsigned long long* acc;       // ACC_N × Gtot
+    uint32_t* dcnt;                // nsp × 4 × Gtot: num, graz, mort, dvid
+    unsigned long long* tile_cnt;  // ntiles: (dividers << 32) | free slots
+    uint32_t* err;
+};
+
+__device__ __forceinline__ void move_one(const MoveArgs& a, const MemberDev& m, int mi, int s, long long slot,
+                                         long long g, uint32_t iter, int& is_div, int& is_free) {
+    const IndDev32& P = a.P;
+    const uint8_t fl = P.flags[g];
+    if (!(fl & F32_AC)) {
+        // every stage multiplies by ac: the position becomes (0, 0, 0) and the cell (Hx, Hy, Hz)
+        if (P.cell[g] != -1) {
+            P.cell[g] = -1;
+            P.ox[g] = 0.0f; P.oy[g] = 0.0f; P.oz[g] = 0.0f;
+        }
+        if (P.stat[g]) P.stat[g] = 0;
+        is_div = 0; is_free = 1;
+        return;
+    }
+    uint32_t* err = a.err;
+    const uint8_t stt = P.stat[g];
+    int ci, cj, ck;
+    unpack_int(m, P.cell[g], ci, cj, ck);
+    // ΔzC at the find_inds! zi of the previous step, plus Hz (particle_diffusion.jl:26-28)
+    int zi = ck + 1 + m.Hz;
+    if (stt & F32_ST_STALE) { int a0, a1; unpack_halo(m, P.scell[g], a0, a1, zi); }
+    const int kdz = clampi(zi + m.Hz, 1, m.Gz, err);
+    const MemberForcing& f = a.F[mi];
+    const Ax1 X0{ci, P.ox[g]}, Y0{cj, P.oy[g]}, Z0{ck, P.oz[g]};
+    const float dT = a.dT;
+    const float* dzC = a.dzC;
+    float u1 = itpl32<0>(m, f.vel0[0], dzC, X0, Y0, Z0, err);
+    float v1 = itpl32<1>(m, f.vel0[1], dzC, X0, Y0, Z0, err);
+    float w1 = itpl32<2>(m, f.vel0[2], dzC, X0, Y0, Z0, err);
+    float u2 = u1, v2 = v1, w2 = w1;
+    Ax1 X = X0, Y = Y0, Z = Z0;
+    move(X, 0.5f * u1 * dT, m.Nx, m.tx); move(Y, 0.5f * v1 * dT, m.Ny, m.ty); move(Z, -(0.5f * w1 * dT), m.Nz, m.tz);
+    u1 = itpl32<0>(m, f.velh[0], dzC, X, Y, Z, err); v1 = itpl32<1>(m, f.velh[1], dzC, X, Y, Z, err);
+    w1 = itpl32<2>(m, f.velh[2], dzC, X, Y, Z, err);
+    u2 += u1 * 2.0f; v2 += v1 * 2.0f; w2 += w1 * 2.0f;
+    X = X0; Y = Y0; Z = Z0;
+    move(X, 0.5f * u1 * dT, m.Nx, m.tx); move(Y, 0.5f * v1 * dT, m.Ny, m.ty); move(Z, -(0.5f * w1 * dT), m.Nz, m.tz);
+    u1 = itpl32<0>(m, f.velh[0], dzC, X, Y, Z, err); v1 = itpl32<1>(m, f.velh[1], dzC, X, Y, Z, err);
+    w1 = itpl32<2>(m, f.velh[2], dzC, X, Y, Z, err);
+    u2 += u1 * 2.0f; v2 += v1 * 2.0f; w2 += w1 * 2.0f;
+    X = X0; Y = Y0; Z = Z0;
+    move(X, u1 * dT, m.Nx, m.tx); move(Y, v1 * dT, m.Ny, m.ty); move(Z, -(w1 * dT), m.Nz, m.tz);
+    u1 = itpl32<0>(m, f.vel1[0], dzC, X, Y, Z, err); v1 = itpl32<1>(m, f.vel1[1], dzC, X, Y, Z, err);
+    w1 = itpl32<2>(m, f.vel1[2], dzC, X, Y, Z, err);
+    u2 = (u2 + u1) / 6.0f; v2 = (v2 + v1) / 6.0f; w2 = (w2 + w1) / 6.0f;
+    X = X0; Y = Y0; Z = Z0;
+    move(X, u2 * dT, m.Nx, m.tx); move(Y, v2 * dT, m.Ny, m.ty); move(Z, -(w2 * dT), m.Nz, m.tz);
+    // random-walk diffusion (particle_diffusion.jl:16-33); a zero κ moves nothing
+    const BgcDev32& b = a.bgc[mi];
+    if (b.kappa_hP != 0.0f || b.kappa_vP != 0.0f) {
+        float r0, r1, r2;
+        draw3f(m.seed, iter, (uint32_t)s, PI_DRAW_DIFFUSION, (uint32_t)slot, r0, r1, r2);
+        move(X, (r0 - 0.5f) * 2.0f * sqrtf(b.kappa_hP * dT) / m.dx, m.Nx, m.tx);
+        move(Y, (r1 - 0.5f) * 2.0f * sqrtf(b.kappa_hP * dT) / m.dy, m.Ny, m.ty);
+        move(Z, (r2 - 0.5f) * 2.0f * sqrtf(b.kappa_vP * dT) / dzC[m.dz_off + kdz - 1], m.Nz, m.tz);
+    }
+    if (X.c < 0 || X.c > m.Nx) { seterr(err, F32_ERR_DOMAIN); X.c = X.c < 0 ? 0 : m.Nx; X.o = 0.0f; }
+    if (Y.c < 0 || Y.c > m.Ny) { seterr(err, F32_ERR_DOMAIN); Y.c = Y.c < 0 ? 0 : m.Ny; Y.o = 0.0f; }
+    if (Z.c < 0 || Z.c > m.Nz) { seterr(err, F32_ERR_DOMAIN); Z.c = Z.c < 0 ? 0 : m.Nz; Z.o = 0.0f; }
+    P.ox[g] = X.o; P.oy[g] = Y.o; P.oz[g] = Z.o;
+    P.cell[g] = pack_int(m, X.c, Y.c, Z.c);
+    const int q = q_of(m, X.c, Y.c, Z.c);
+    const long long cq = m.cell_off + q;
+    const long long G = a.Gtot;
+    const bool inside = X.c < m.Nx && Y.c < m.Ny && Z.c < m.Nz;
+    atomicAdd(&a.pop[cq], 1);
+    if (a.pop_sp) atomicAdd(&a.pop_sp[(long long)s * G + cq], 1);
+    if (inside) add_fixed(&a.chl_acc[cq], P.Chl[g], m.chl_unit);
+    // previous step's decisions (plankton_update.jl:5-16, division_death.jl:2-25)
+    const int gz = (fl & F32_GRAZ) != 0, mt = (fl & F32_MORT) != 0, dv = (fl & F32_DVID) != 0;
+    const int ac1 = !gz, ac2 = ac1 && !mt, dv2 = dv && ac2;
+    uint32_t* dc = a.dcnt + (long long)s * 4 * G + cq;
+    if (gz) atomicAdd(dc + 1 * G, 1u);
+    if (ac1 && mt) atomicAdd(dc + 2 * G, 1u);
+    if (dv2) atomicAdd(dc + 3 * G, 1u);
+    const int kind = gz ? 1 : (ac1 && mt) ? 2 : 0;
+    if (kind && inside) {
+        const SpeciesDev32& p = a.sp[mi * a.T.nsp + s];
+        const float fC = kind == 1 ? p.grazFracC : p.mortFracC;
+        const float fN = kind == 1 ? p.grazFracN : p.mortFracN;
+        const float fP = kind == 1 ? p.grazFracP : p.mortFracP;
+        const float Bm = P.Bm[g], Cq = P.Cq[g], Nq = P.Nq[g], Pq = P.Pq[g];
+        const double u = m.fx_unit;
+        add_fixed(&a.acc[ACC_DOC * G + cq], (Bm + Cq) * fC, u);
+        add_fixed(&a.acc[ACC_DON * G + cq], (Bm * p.R_NC + Nq) * fN, u);
+        add_fixed(&a.acc[ACC_DOP * G + cq], (Bm * p.R_PC + Pq) * fP, u);
+        add_fixed(&a.acc[ACC_POC * G + cq], (Bm + Cq) * (1.0f - fC), u);
+        add_fixed(&a.acc[ACC_PON * G + cq], (Bm * p.R_NC + Nq) * (1.0f - fN), u);
+        add_fixed(&a.acc[ACC_POP * G + cq], (Bm * p.R_PC + Pq) * (1.0f - fP), u);
+    }
+    P.flags[g] = (uint8_t)((ac2 ? F32_AC : 0) | (dv2 ? F32_DVID : 0));
+    P.stat[g] = F32_ST_AC0;
+    is_div = dv2; is_free = !ac2;
+}
+
+__global__ void k32_move(MoveArgs a) {
+    if (stopped(a.err)) return;
+    __shared__ unsigned int sh_d, sh_f;
+    const int bs = blockDim.x, ppt = F32_TILE / bs;
+    const uint32_t iter = (uint32_t)(a.st->iteration + 1);
+    for (int t = blockIdx.x; t < a.T.ntiles; t += gridDim.x) {
+        const int2 tl = a.T.tiles[t];
+        int mi, s;
+        seg_of(a.T, tl.x, mi, s);
+        const MemberDev& m = a.T.md[mi];
+        const long long base = m.slot_off + (long long)s * m.C;
+        unsigned int nd = 0, nf = 0;
+        for (int p = 0; p < ppt; ++p) {
+            const long long slot = (long long)tl.y + p * bs + threadIdx.x;
+            if (slot < m.C) {
+                int d, f;
+                move_one(a, m, mi, s, slot, base + slot, iter, d, f);
+                nd += d; nf += f;
+            }
+        }
+        if (threadIdx.x == 0) { sh_d = 0; sh_f = 0; }
+        __syncthreads();
+        nd = __reduce_add_sync(0xffffffffu, nd);
+        nf = __reduce_add_sync(0xffffffffu, nf);
+        if ((threadIdx.x & 31) == 0) { atomicAdd(&sh_d, nd); atomicAdd(&sh_f, nf); }
+        __syncthreads();
+        if (threadIdx.x == 0) a.tile_cnt[t] = ((unsigned long long)sh_d << 32) | sh_f;
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// PAR down each column (calc_par!, Individuals/utils.jl:55-63); consumes the Chl sums
+// ------------------------------------------------------------------------------------------
+__global__ void k32_par(Tab32 T, const float* __restrict__ dzF, const BgcDev32* __restrict__ bgc,
+                        unsigned long long* __restrict__ chl_acc, float* __restrict__ PARF,
+                        float* __restrict__ par, float* __restrict__ diag_par, const uint32_t* err) {
+    if (stopped(err)) return;
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < T.nicol; w += nw) {
+        const int4 it = T.icol[w];
+        const MemberDev& m = T.md[it.x];
+        const int i = it.y + lane, j = it.z;     // 1-based interior column
+        if (i > m.Nx) continue;
+        const float kc = bgc[it.x].kc, kw = bgc[it.x].kw;
+        const long long fcol = m.col_off + (i - 1) + (long long)m.Nx * (j - 1);
+        float parf = PARF[fcol];
+        for (int k = 1; k <= m.Nz; ++k) {
+            const int kk = k + m.Hz;
+            const long long c = m.cell_off + gid3(m, i + m.Hx, j + m.Hy, kk);
+            const long long v = (long long)chl_acc[c];
+            if (v) chl_acc[c] = 0ull;
+            const float chl = (float)((double)v * m.chl_unit);
+            const float dz = dzF[m.dz_off + kk - 1];
+            const float volk = m.dx * m.dy * dz;
+            const float atten = (chl / volk * kc + kw) * dz;
+            const float e = expf(-atten);
+            const float pv = parf * (1.0f - e) / atten;
+            par[c] = pv;
+            parf = parf * e;
+            diag_par[c] += pv;
+        }
+        PARF[fcol] = parf;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// (e) division: k-th divider (slot order) → k-th free slot (findall(!ac), ascending), per segment
+// (get_tind!, Individuals/utils.jl:76-86), with the capacity check (plankton_update.jl:18-22).
+// Ranks inside a tile come from warp ballots, tile offsets from the scan of the tile counts.
+// Tiles with neither dividers nor needed free slots do nothing.
+// ------------------------------------------------------------------------------------------
+__global__ void k32_assign(Tab32 T, IndDev32 P, const unsigned long long* __restrict__ tile_cnt,
+                           const unsigned long long* __restrict__ tile_off, int* __restrict__ divlist,
+                           int* __restrict__ freelist, uint32_t* __restrict__ ndiv, StepState* st,
+                           uint32_t* err) {
+    if (stopped(err)) return;
+    __shared__ unsigned int wd[32], wf[32];
+    const int bs = blockDim.x, ppt = F32_TILE / bs, nwarp = bs >> 5;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
+        const int2 tl = T.tiles[t];
+        const int seg = tl.x;
+        int mi, s;
+        seg_of(T, seg, mi, s);
+        const MemberDev& m = T.md[mi];
+        const long long base = m.slot_off + (long long)s * m.C;
+        const int t0 = T.seg_tile0[seg], t1 = T.seg_tile0[seg + 1];
+        const unsigned long long b0 = tile_off[t0];
+        const unsigned long long tot = tile_off[t1 - 1] + tile_cnt[t1 - 1] - b0;
+        const unsigned int tdiv = (unsigned int)(tot >> 32), tfree = (unsigned int)(tot & 0xffffffffull);
+        if (tdiv > tfree) {
+            if (t == t0 && threadIdx.x == 0) {
+                ndiv[seg] = 0;
+                if (!(atomicOr(err, F32_ERR_CAPACITY) & F32_ERR_CAPACITY)) {
+                    st->err_iter = st->iteration + 1;
+                    st->err_member = mi;
+                }
+            }
+            continue;
+        }
+        if (t == t0 && threadIdx.x == 0) ndiv[seg] = tdiv;
+        const unsigned long long before = tile_off[t] - b0;
+        const unsigned int dbefore = (unsigned int)(before >> 32), fbefore = (unsigned int)(before & 0xffffffffull);
+        const unsigned long long c = tile_cnt[t];
+        const bool work = (c >> 32) != 0 || ((c & 0xffffffffull) != 0 && fbefore < tdiv);
+        if (!work) continue;                                        // uniform over the block
+        unsigned int rd = dbefore, rf = fbefore;
+        for (int p = 0; p < ppt; ++p) {
+            const long long slot = (long long)tl.y + p * bs + threadIdx.x;
+            const bool valid = slot < m.C;
+            const uint8_t fl = valid ? P.flags[base + slot] : (uint8_t)F32_AC;
+            const bool isd = (fl & F32_DVID) != 0, isf = !(fl & F32_AC);
+            const unsigned int bd = __ballot_sync(0xffffffffu, isd), bf = __ballot_sync(0xffffffffu, isf);
+            if (lane == 0) { wd[wid] = __popc(bd); wf[wid] = __popc(bf); }
+            __syncthreads();
+            unsigned int pd = 0, pf = 0, sd = 0, sf = 0;
+            for (int w = 0; w < nwarp; ++w) {
+                if (w < wid) { pd += wd[w]; pf += wf[w]; }
+                sd += wd[w]; sf += wf[w];
+            }
+            const unsigned int lt = (1u << lane) - 1u;
+            if (isd) divlist[base + rd + pd + __popc(bd & lt)] = (int)slot;
+            if (isf) {
+                const unsigned int kf = rf + pf + __popc(bf & lt);
+                if (kf < tdiv) freelist[base + kf] = (int)slot;
+            }
+            rd += sd; rf += sf;
+            __syncthreads();
+        }
+    }
+}
+
+// copy_daughter_individuals! and divide_to_half! (division_death.jl:28-63). Grid: (x, segments).
+__global__ void k32_daughters(Tab32 T, IndDev32 P, const int* __restrict__ divlist,
+                              const int* __restrict__ freelist, const uint32_t* __restrict__ ndiv,
+                              const uint32_t* err) {
+    if (stopped(err)) return;
+    const int seg = blockIdx.y;
+    int mi, s;
+    seg_of(T, seg, mi, s);
+    const MemberDev& m = T.md[mi];
+    const long long base = m.slot_off + (long long)s * m.C;
+    const uint32_t n = ndiv[seg];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const long long p = base + divlist[base + k], d = base + freelist[base + k];
+        // the daughter's slot keeps the cell find_inds! gave it this step
+        const int32_t cd = P.cell[d];
+        int32_t sc;
+        if (cd < 0) sc = pack_halo(m, m.Hx, m.Hy, m.Hz);
+        else { int a0, a1, a2; unpack_int(m, cd, a0, a1, a2); sc = pack_halo(m, a0 + 1 + m.Hx, a1 + 1 + m.Hy, a2 + 1 + m.Hz); }
+        P.scell[d] = sc;
+        P.cell[d] = P.cell[p];
+        P.ox[d] = P.ox[p]; P.oy[d] = P.oy[p]; P.oz[d] = P.oz[p];
+        const float Bm = P.Bm[p] * 0.5f, Cq = P.Cq[p] * 0.5f, Nq = P.Nq[p] * 0.5f, Pq = P.Pq[p] * 0.5f;
+        const float Chl = P.Chl[p] * 0.5f, gen = P.gen[p] + 1.0f;
+        P.Bm[d] = Bm; P.Cq[d] = Cq; P.Nq[d] = Nq; P.Pq[d] = Pq; P.Chl[d] = Chl; P.gen[d] = gen;
+        P.age[d] = P.age[d] * 0.0f;
+        P.Bm[p] = Bm; P.Cq[p] = Cq; P.Nq[p] = Nq; P.Pq[p] = Pq; P.Chl[p] = Chl; P.gen[p] = gen;
+        P.age[p] = P.age[p] * 0.0f;
+        P.flags[d] = F32_AC | F32_DVID;
+        P.stat[d] = (uint8_t)((P.stat[d] & F32_ST_AC0) | F32_ST_STALE);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// (b) QuotaMode physiology in Float32 (plankton_growth.jl:2-24, growth_kernels.jl:2-166,
+//     division_death_probability.jl:7-107, find_NPT!, calc_consume!, diags num)
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ float shape_dec_f(float x, float xmax, float k, int pw) {
+    const float fx = fmaxf(0.0f, fminf(1.0f, 1.0f - x / xmax));
+    const float p = pw == 2 ? fx * fx : (fx * fx) * (fx * fx);
+    return p / (k + p);
+}
+__device__ __forceinline__ float shape_inc_f(float x, float xmax, float k, int pw) {
+    return 1.0f - shape_dec_f(x, xmax, k, pw);
+}
+__device__ __forceinline__ float tempFunc_f(float T, const SpeciesDev32& p) {
+    const float k = fmaxf(0.0f, expf(-p.Ea / (8.3145f * (T + 273.15f))));
+    return fminf(1.0f, k / p.OGT_rate);
+}
+__device__ __forceinline__ float tempFunc_PS_f(float T, const SpeciesDev32& p) {
+    const float regT = shape_dec_f(T - p.Topt, p.Tmax - p.Topt, 4.0e-2f, 4);
+    const float k = fmaxf(0.0f, expf(-p.Ea / (8.3145f * (T + 273.15f))) * regT);
+    return fminf(1.0f, k / p.OGT_rate);
+}
+// Julia isless on floats without signed zeros: NaN orders last
+__device__ __forceinline__ bool jl_lessf(float x, float y) { return x < y || (y != y && x == x); }
+
+struct PhysArgs {
+    Tab32 T;
+    IndDev32 P;
+    const SpeciesDev32* sp;
+    const MemberForcing* F;
+    const StepState* st;
+    float dT;
+    long long Gtot;
+    const float* tr;
+    const float* par;
+    const int* pop;
+    const int* pop_sp;
+    unsigned long long* acc;
+    uint32_t* dcnt;
+    const uint32_t* err;
+};
+
+__device__ __forceinline__ void phys_one(const PhysArgs& a, const MemberDev& m, int mi, int s, long long slot,
+                                         long long g, uint32_t iter, double tnow) {
+    const IndDev32& P = a.P;
+    if (!(P.flags[g] & F32_AC)) return;
+    const uint8_t stt = P.stat[g];
+    const int ac0 = stt & F32_ST_AC0;
+    int q;
+    if (stt & F32_ST_STALE) { int xi, yi, zi; unpack_halo(m, P.scell[g], xi, yi, zi); q = gid3(m, xi, yi, zi); }
+    else { int ci, cj, ck; unpack_int(m, P.cell[g], ci, cj, ck); q = q_of(m, ci, cj, ck); }
+    const long long cq = m.cell_off + q;
+    const long long G = a.Gtot;
+    const SpeciesDev32& p = a.sp[mi * a.T.nsp + s];
+    const float dT = a.dT;
+    float NH4 = 0.0f, NO3 = 0.0f, PO4 = 0.0f, DOC = 0.0f, parv = 0.0f, Tm = 0.0f, popv = 0.0f;
+    if (ac0) {
+        NH4 = fmaxf(0.0f, a.tr[PI_NH4 * G + cq]); NO3 = fmaxf(0.0f, a.tr[PI_NO3 * G + cq]);
+        PO4 = fmaxf(0.0f, a.tr[PI_PO4 * G + cq]); DOC = fmaxf(0.0f, a.tr[PI_DOC * G + cq]);
+        parv = a.par[cq];
+        Tm = a.F[mi].temp[q];
+        popv = (float)(a.pop_sp ? a.pop_sp[(long long)s * G + cq] : a.pop[cq]);
+    }
+    float Bm = P.Bm[g], Cq = P.Cq[g], Nq = P.Nq[g], Pq = P.Pq[g], Chl = P.Chl[g];
+    const float tf = tempFunc_f(Tm, p);
+    // calc_inorganic_uptake_kernel! (:48-56)
+    const float aI = parv * p.alpha * p.Phi;
+    const float PCm = p.PCmax * tempFunc_PS_f(Tm, p);
+    const float PS = PCm * (1.0f - expf(-aI / fmaxf(1.0e-30f, PCm) * Chl / fmaxf(1.0e-30f, Bm))) * Bm;
+    const float Qn = (Nq + Bm * p.R_NC) / fmaxf(1.0e-30f, Bm + Cq);
+    const float Qp = (Pq + Bm * p.R_PC) / fmaxf(1.0e-30f, Bm + Cq);
+    const float regQN = shape_dec_f(Qn, p.Nqmax, 1.0e-4f, 4), regQP = shape_dec_f(Qp, p.Pqmax, 1.0e-4f, 4);
+    const float ipop = fmaxf(1.0f, popv);
+    const float VNH4 = fminf(p.VNH4max * regQN * NH4 / fmaxf(1.0e-30f, NH4 + p.KsatNH4) * tf * Bm, NH4 / dT / ipop);
+    const float VNO3 = fminf(p.VNO3max * regQN * NO3 / fmaxf(1.0e-30f, NO3 + p.KsatNO3) * tf * Bm, NO3 / dT / ipop);
+    const float VPO4 = fminf(p.VPO4max * regQP * PO4 / fmaxf(1.0e-30f, PO4 + p.KsatPO4) * tf * Bm, PO4 / dT / ipop);
+    // update_quotas_1_kernel! (:64-69)
+    Cq += PS * dT; Pq += VPO4 * dT; Nq += (VNH4 + VNO3) * dT;
+    // calc_organic_uptake_kernel! (:78-84)
+    const float Qc = Cq / fmaxf(1.0e-30f, Bm + Cq);
+    const float regQ = shape_dec_f(Qc, p.Cqmax, 1.0e-4f, 4);
+    float VDOC = fminf(p.VDOCmax * regQ * DOC / fmaxf(1.0e-30f, DOC + p.KsatDOC) * tf * Bm, DOC / dT / ipop);
+    VDOC = mulbf(VDOC, jl_lessf(1.0e-2f, PS / (VDOC + PS)));
+    // calc_ρChl_kernel! (:92-97)
+    const float rChl = mulbf(PS / fmaxf(1.0e-30f, Bm) * p.Chl2N / fmaxf(1.0e-30f, parv * p.alpha * p.Phi * Chl / Bm),
+                             jl_lessf(1.0e-1f, parv));
+    // calc_respir_kernel! (:105-108)
+    const float resp = p.respir * Bm * tf;
+    // update_quotas_2_kernel! (:117-124)
+    Cq = Cq + (VDOC - resp) * dT;
+    const float def = fmaxf(0.0f, 0.0f - Cq);
+    Bm = Bm - def; Nq = Nq + def * p.R_NC; Pq = Pq + def * p.R_PC; Cq = Cq + def;
+    // calc_BS_kernel! (:132-138)
+    const float mn = fminf(fminf(Cq, Nq / p.R_NC), Pq / p.R_PC);
+    const float BS = mn * p.k_mtb, exu = fmaxf(0.0f, Cq - mn) * p.k_mtb;
+    // update_biomass_kernel! (:146-154)
+    Bm += dT * BS; Cq -= dT * (BS + exu); Nq -= dT * BS * p.R_NC; Pq -= dT * BS * p.R_PC;
+    Chl += dT * BS * p.R_NC * rChl;
+    const float age = P.age[g] + dT / 3600.0f;
+    // update_cellsize_kernel! (:163-166) and the probabilities (division_death_probability.jl:7-68)
+    const float Sz = Bm / (p.Cquota * p.Nsuper);
+    const float graz = popv * p.grz_P;
+    const float mort = p.mort_P * shape_dec_f(Sz, p.mort_reg, 1.0e-5f, 4);
+    float dv;
+    if (p.dvid_type == 1) dv = p.dvid_P * shape_inc_f(Sz, p.dvid_reg, 2.0e-3f, 2);
+    else {
+        const float h = (float)(fmod(tnow, 86400.0) / 3600.0);
+        if (p.dvid_type == 2) dv = p.dvid_P * shape_inc_f(h, p.dvid_reg, 1.0e-5f, 4);
+        else dv = p.dvid_P * shape_inc_f(Sz, p.dvid_reg, 1.0e-3f, 4) * shape_inc_f(h, p.dvid_reg2, 1.0e-5f, 4);
+    }
+    // get_probability! (:95-107)
+    float r0, r1, r2;
+    draw3f(m.seed, iter, (uint32_t)s, PI_DRAW_DECISION, (uint32_t)slot, r0, r1, r2);
+    const int dg = jl_lessf(r0, graz * dT), dm = jl_lessf(r1, mort * dT), dd = jl_lessf(r2, dv * dT);
+    P.Bm[g] = Bm; P.Cq[g] = Cq; P.Nq[g] = Nq; P.Pq[g] = Pq; P.Chl[g] = Chl; P.age[g] = age;
+    P.flags[g] = (uint8_t)(F32_AC | (dg ? F32_GRAZ : 0) | (dm ? F32_MORT : 0) | (dd ? F32_DVID : 0));
+    // calc_consume_kernel! (consume_loss.jl:2-9): only individuals binned this step reach the grid
+    if (ac0 && interior_q(m, q)) {
+        const double u = m.fx_unit;
+        add_fixed(&a.acc[ACC_DIC * G + cq], (resp - PS) * dT, u);
+        add_fixed(&a.acc[ACC_DOC * G + cq], (exu - VDOC) * dT, u);
+        add_fixed(&a.acc[ACC_NH4 * G + cq], -VNH4 * dT, u);
+        add_fixed(&a.acc[ACC_NO3 * G + cq], -VNO3 * dT, u);
+        add_fixed(&a.acc[ACC_PO4 * G + cq], -VPO4 * dT, u);
+    }
+    atomicAdd(&a.dcnt[(long long)s * 4 * G + cq], 1u);      // diags num at the (possibly stale) cell
+}
+
+__global__ void k32_physiology(PhysArgs a) {
+    if (stopped(a.err)) return;
+    const int bs = blockDim.x, ppt = F32_TILE / bs;
+    const uint32_t iter = (uint32_t)(a.st->iteration + 1);
+    const double tnow = (double)(a.st->iteration + 1) * (double)a.dT;
+    for (int t = blockIdx.x; t < a.T.ntiles; t += gridDim.x) {
+        const int2 tl = a.T.tiles[t];
+        int mi, s;
+        seg_of(a.T, tl.x, mi, s);
+        const MemberDev& m = a.T.md[mi];
+        const long long base = m.slot_off + (long long)s * m.C;
+        for (int p = 0; p < ppt; ++p) {
+            const long long slot = (long long)tl.y + p * bs + threadIdx.x;
+            if (slot < m.C) phys_one(a, m, mi, s, slot, base + slot, iter, tnow);
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// (d) tracer update in Float32: DST3FL sweeps (DST3FL.jl:1-73, multi_dim_adv.jl:1-135), then
+//     diffusion, sinking, forcing, flux BCs, particle terms and apply_tendency!
+// ------------------------------------------------------------------------------------------
+struct FC32 { float d0c, d1c, omc, cpe, hp, hm; };
+__device__ __forceinline__ FC32 fc32(float vel, float area, float dxc, float dT) {
+    FC32 f;
+    const float cfl = fabsf(vel * dT / dxc);
+    const float tr = area * vel;
+    f.d0c = (2.0f - cfl) * (1.0f - cfl) / 6.0f;
+    f.d1c = (1.0f - cfl * cfl) / 6.0f;
+    f.omc = 1.0f - cfl;
+    f.cpe = cfl + EPS20_F;
+    f.hp = 0.5f * (tr + fabsf(tr));
+    f.hm = 0.5f * (tr - fabsf(tr));
+    return f;
+}
+// θ = δ⁻/δ⁰ limited at ±θmax (DST3FL.jl:2). Where δ⁰ is within 2^-22 of the values it was taken
+// from (a gradient near zero), the ratio, the limit test and the sign are formed in FP64.
+__device__ __forceinline__ float theta_f(float dn, float d0, float scale) {
+    if (fabsf(d0) <= scale * 0x1p-22f) {
+        const double D0 = d0, DN = dn;
+        const double th = fabs(D0) * 1.0e20 <= fabs(DN) ? copysign(1.0e20, DN * D0) : DN / D0;
+        return (float)th;
+    }
+    return fabsf(d0) * THMAX_F <= fabsf(dn) ? copysignf(THMAX_F, dn * d0) : dn / d0;
+}
+__device__ __forceinline__ float psi_f(const FC32& f, float th) {
+    return fmaxf(0.0f, fminf(fminf(1.0f, f.d0c + f.d1c * th), th * f.omc / f.cpe));
+}
+__device__ __forceinline__ float fxy32(const FC32& f, float cm2, float cm1, float c0, float cp1,
+                                       int lm2, int lm1, int l0, int lp1) {
+    const float d0 = mulbf(mulbf(c0 - cm1, l0), lm1), dm = mulbf(mulbf(cm1 - cm2, lm1), lm2);
+    const float dp = mulbf(mulbf(cp1 - c0, lp1), l0);
+    const float sc = fmaxf(fabsf(c0), fabsf(cm1));
+    return f.hp * (cm1 + psi_f(f, theta_f(dm, d0, sc)) * d0) + f.hm * (c0 - psi_f(f, theta_f(dp, d0, sc)) * d0);
+}
+__device__ __forceinline__ float fz32(const FC32& f, float cm2, float cm1, float c0, float cp1,
+                                      int lm2, int lm1, int l0, int lp1) {
+    const float d0 = mulbf(mulbf(cm1 - c0, l0), lm1), dm = mulbf(mulbf(cm2 - cm1, lm1), lm2);
+    const float dp = mulbf(mulbf(c0 - cp1, lp1), l0);
+    const float sc = fmaxf(fabsf(c0), fabsf(cm1));
+    return f.hp * (c0 + psi_f(f, theta_f(dp, d0, sc)) * d0) + f.hm * (cm1 - psi_f(f, theta_f(dm, d0, sc)) * d0);
+}
+__device__ __forceinline__ int wrap_ax(int a, int N, int H, int topo) {
+    if (topo == PI_PERIODIC) { while (a < H + 1) a += N; while (a > N + H) a -= N; return a; }
+    return a < H + 1 ? H + 1 : (a > N + H ? N + H : a);
+}
+
+struct SweepArgs {
+    Tab32 T;
+    const uint8_t* lm;
+    const float* dzF;
+    const float* dzC;
+    const MemberForcing* F;
+    long long Gtot;
+    const float* tr;       // tracers at the start of the step
+    const float* src;      // input of this sweep
+    float* dst;            // output of this sweep
+    float dT;
+    const uint32_t* err;
+};
+
+// x sweep: each warp owns 31 cells of one row and 32 faces; the east flux of a cell is the next
+// lane's west flux. The face after the last cell is the periodic image of face H+1, or zero.
+__global__ void k32_sweep_x(SweepArgs a) {
+    if (stopped(a.err)) return;
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < a.T.nix; w += nw) {
+        const int4 it = a.T.ix[w];
+        const MemberDev& m = a.T.md[it.x];
+        const int j = it.y, k = it.z, i0 = it.w;
+        const int f = i0 + lane, last = m.Nx + m.Hx;
+        const bool has_face = f <= last + 1, has_cell = lane < 31 && f <= last, special = f == last + 1;
+        const bool zero_face = !has_face || (special && m.tx != PI_PERIODIC);
+        const int fs = special ? m.Hx + 1 : f;
+        const float* u = a.F[it.x].vel1[0];
+        const float ax = m.dy * a.dzF[m.dz_off + k - 1];
+        const int qf = gid3(m, has_face ? fs : i0, j, k);
+        FC32 fc{};
+        int l2 = 1, l1 = 1, l0 = 1, lp = 1;
+        if (!zero_face) {
+            fc = fc32(u[qf], ax, m.dx, a.dT);
+            l2 = lm32(m, a.lm, fs - 2, j, k); l1 = lm32(m, a.lm, fs - 1, j, k);
+            l0 = lm32(m, a.lm, fs, j, k); lp = lm32(m, a.lm, fs + 1, j, k);
+        }
+        const int qc = gid3(m, has_cell ? f : i0, j, k);
+        float ftr = 0.0f, dtv = 0.0f;
+        int c0m = 1, cpm = 1;
+        if (has_cell) {
+            c0m = lm32(m, a.lm, f, j, k); cpm = lm32(m, a.lm, f + 1, j, k);
+            ftr = mulbf(mulbf(ax * u[qc + 1] - ax * u[qc], cpm), c0m);
+            dtv = a.dT / (m.dx * m.dy * a.dzF[m.dz_off + k - 1]);
+        }
+        const long long off = m.cell_off;
+#pragma unroll 2
+        for (int n = 0; n < PI_NTRACERS; ++n) {
+            const float* c = a.src + n * a.Gtot + off;
+            const float Fl = zero_face ? 0.0f : fxy32(fc, c[qf - 2], c[qf - 1], c[qf], c[qf + 1], l2, l1, l0, lp);
+            const float Fe = __shfl_down_sync(0xffffffffu, Fl, 1);
+            if (has_cell) {
+                const float cc = c[qc];
+                const float dG = mulbf(mulbf(Fe - Fl, cpm), c0m);
+                a.dst[n * a.Gtot + off + qc] = cc - dtv * (dG - cc * ftr);
+            }
+        }
+    }
+}
+
+// y sweep: lanes along x, each lane walks Ly rows carrying the face flux; rows outside the
+// interior are read through the map the halo fill of tracer_temp produces.
+__global__ void k32_sweep_y(SweepArgs a) {
+    if (stopped(a.err)) return;
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < a.T.niy; w += nw) {
+        const int4 it = a.T.iy[w];
+        const MemberDev& m = a.T.md[it.x];
+        const int i = it.y + lane, j0 = it.z, k = it.w;
+        if (i > m.Nx + m.Hx) continue;
+        const int jend = min(j0 + a.T.Ly - 1, m.Ny + m.Hy);
+        const float* v = a.F[it.x].vel1[1];
+        const float dz = a.dzF[m.dz_off + k - 1];
+        const float ay = m.dx * dz;
+        const float dtv = a.dT / (m.dx * m.dy * dz);
+        const long long off = m.cell_off;
+        auto face = [&](const float* c, int f) -> float {
+            const bool special = f == m.Ny + m.Hy + 1;
+            if (special && m.ty != PI_PERIODIC) return 0.0f;
+            const int fs = special ? m.Hy + 1 : f;
+            const FC32 fc = fc32(v[gid3(m, i, fs, k)], ay, m.dy, a.dT);
+            return fxy32(fc, c[gid3(m, i, wrap_ax(fs - 2, m.Ny, m.Hy, m.ty), k)], c[gid3(m, i, wrap_ax(fs - 1, m.Ny, m.Hy, m.ty), k)],
+                         c[gid3(m, i, wrap_ax(fs, m.Ny, m.Hy, m.ty), k)], c[gid3(m, i, wrap_ax(fs + 1, m.Ny, m.Hy, m.ty), k)],
+                         lm32(m, a.lm, i, fs - 2, k), lm32(m, a.lm, i, fs - 1, k), lm32(m, a.lm, i, fs, k), lm32(m, a.lm, i, fs + 1, k));
+        };
+#pragma unroll 1
+        for (int n = 0; n < PI_NTRACERS; ++n) {
+            const float* c = a.src + n * a.Gtot + off;
+            const float* c0 = a.tr + n * a.Gtot + off;
+            float Ft = face(c, j0);
+            for (int jj = j0; jj <= jend; ++jj) {
+                const float Fb = face(c, jj + 1);
+                const int q = gid3(m, i, jj, k);
+                const int c0m = lm32(m, a.lm, i, jj, k), cpm = lm32(m, a.lm, i, jj + 1, k);
+                const float ftr = mulbf(mulbf(ay * v[q + m.Gx] - ay * v[q], cpm), c0m);
+                const float dG = mulbf(mulbf(Fb - Ft, cpm), c0m);
+                a.dst[n * a.Gtot + off + q] = c[q] - dtv * (dG - c0[q] * ftr);
+                Ft = Fb;
+            }
+        }
+    }
+}
+
+// z sweep and calc_tracer_tendency!: writes Gc_adv = tracer_temp − tracer.
+__global__ void k32_sweep_z(SweepArgs a) {
+    if (stopped(a.err)) return;
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < a.T.niz; w += nw) {
+        const int4 it = a.T.iz[w];
+        const MemberDev& m = a.T.md[it.x];
+        const int i = it.y + lane, j = it.z, k0 = it.w;
+        if (i > m.Nx + m.Hx) continue;
+        const int kend = min(k0 + a.T.Lz - 1, m.Nz + m.Hz);
+        const float* wv = a.F[it.x].vel1[2];
+        const float az = m.dx * m.dy;
+        const int slab = m.Gx * m.Gy;
+        const int qcol = gid3(m, i, j, 1);
+        const long long off = m.cell_off;
+        auto face = [&](const float* c, int f) -> float {
+            if (f == m.Nz + m.Hz + 1) return 0.0f;
+            const FC32 fc = fc32(wv[qcol + (f - 1) * slab], az, a.dzC[m.dz_off + f - 1], a.dT);
+            auto lev = [&](int kk) { return qcol + (wrap_ax(kk, m.Nz, m.Hz, PI_BOUNDED) - 1) * slab; };
+            return fz32(fc, c[lev(f - 2)], c[lev(f - 1)], c[lev(f)], c[lev(f + 1)], lm32(m, a.lm, i, j, f - 2),
+                        lm32(m, a.lm, i, j, f - 1), lm32(m, a.lm, i, j, f), lm32(m, a.lm, i, j, f + 1));
+        };
+#pragma unroll 1
+        for (int n = 0; n < PI_NTRACERS; ++n) {
+            const float* c = a.src + n * a.Gtot + off;
+            const float* c0 = a.tr + n * a.Gtot + off;
+            float Ft = face(c, k0);
+            for (int k = k0; k <= kend; ++k) {
+                const float Fb = face(c, k + 1);
+                const int q = qcol + (k - 1) * slab;
+                const int c0m = lm32(m, a.lm, i, j, k), cpm = lm32(m, a.lm, i, j, k + 1);
+                const float ftr = mulbf(mulbf(az * wv[q] - az * wv[q + slab], cpm), c0m);
+                const float dG = mulbf(mulbf(Ft - Fb, cpm), c0m);
+                const float cc = c0[q];
+                const float ct = c[q] - a.dT / (m.dx * m.dy * a.dzF[m.dz_off + k - 1]) * (dG - cc * ftr);
+                a.dst[n * a.Gtot + off + q] = ct - cc;
+                Ft = Fb;
+            }
+        }
+    }
+}
+
+struct TailArgs {
+    Tab32 T;
+    const uint8_t* lm;
+    const float* dzF;
+    const float* dzC;
+    const BgcDev32* bgc;
+    const FluxBC32* bcs;   // [bc_off + tracer*6 + face]
+    const StepState* st;
+    long long Gtot;
+    const float* tr;
+    const float* gadv;
+    float* tr_next;
+    unsigned long long* acc;
+    const int* pop;
+    float dT;
+    const uint32_t* err;
+};
+
+__device__ __forceinline__ float getbc32(const FluxBC32& b, int a, int c, int64_t it) {
+    if (b.kind == PI_BC_CONST) return b.v[0];
+    if (b.kind == PI_BC_ARRAY2D) return b.v[(a - 1) + (long long)b.n1 * (c - 1)];
+    const int64_t t = it < 1 ? 1 : (it > b.nt ? b.nt : it);   // the host rejects steps past nt
+    return b.v[(a - 1) + (long long)b.n1 * ((c - 1) + (long long)b.n2 * (t - 1))];
+}
+
+__global__ void k32_tail(TailArgs a) {
+    if (stopped(a.err)) return;
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < a.T.nic; w += nw) {
+        const int4 it = a.T.ic[w];
+        const MemberDev& m = a.T.md[it.x];
+        const int i = it.y + lane, j = it.z, k = it.w;
+        if (i > m.Nx + m.Hx) continue;
+        const long long G = a.Gtot, off = m.cell_off;
+        const int q = gid3(m, i, j, k);
+        const long long cq = off + q;
+        const float dT = a.dT;
+        const float dz = a.dzF[m.dz_off + k - 1];
+        const float volk = m.dx * m.dy * dz;
+        const float az = m.dx * m.dy;
+        const int slab = m.Gx * m.Gy;
+        const BgcDev32& b = a.bgc[it.x];
+        float Gc[PI_NTRACERS];
+#pragma unroll
+        for (int n = 0; n < PI_NTRACERS; ++n) Gc[n] = a.gadv[n * G + cq];
+        // tracer_diffusion! (tracer_diffusion.jl:1-21)
+        if (b.kappa_h != 0.0f || b.kappa_v != 0.0f) {
+            const float axk = m.dy * dz, ayk = m.dx * dz;
+            const int li = lm32(m, a.lm, i, j, k);
+            for (int n = 0; n < PI_NTRACERS; ++n) {
+                const float* c = a.tr + n * G + off;
+                auto dx0 = [&](int ii) { return mulbf(mulbf(c[gid3(m, ii, j, k)] - c[gid3(m, ii - 1, j, k)], lm32(m, a.lm, ii, j, k)), lm32(m, a.lm, ii - 1, j, k)); };
+                auto dy0 = [&](int jj) { return mulbf(mulbf(c[gid3(m, i, jj, k)] - c[gid3(m, i, jj - 1, k)], lm32(m, a.lm, i, jj, k)), lm32(m, a.lm, i, jj - 1, k)); };
+                auto dz0 = [&](int kk) { return mulbf(mulbf(c[gid3(m, i, j, kk - 1)] - c[gid3(m, i, j, kk)], lm32(m, a.lm, i, j, kk)), lm32(m, a.lm, i, j, kk - 1)); };
+                const float fx1 = b.kappa_h * axk * (dx0(i + 1) / m.dx), fx0 = b.kappa_h * axk * (dx0(i) / m.dx);
+                const float fy1 = b.kappa_h * ayk * (dy0(j + 1) / m.dy), fy0 = b.kappa_h * ayk * (dy0(j) / m.dy);
+                const float fz0 = b.kappa_v * az * (dz0(k) / dz), fz1 = b.kappa_v * az * (dz0(k + 1) / a.dzF[m.dz_off + k]);
+                const float ax_ = mulbf(mulbf(fx1 - fx0, lm32(m, a.lm, i + 1, j, k)), li);
+                const float ay_ = mulbf(mulbf(fy1 - fy0, lm32(m, a.lm, i, j + 1, k)), li);
+                const float az_ = mulbf(mulbf(fz0 - fz1, lm32(m, a.lm, i, j, k + 1)), li);
+                Gc[n] = Gc[n] + 1.0f / volk * (ax_ + ay_ + az_) * dT;
+            }
+        }
+        // tracer_sinking! (tracer_sinking.jl:1-42)
+        {
+            auto sink = [&](int n, float ws) {
+                const float* c = a.tr + n * G + off;
+                const float fup = (k - 1 <= m.Hz || k - 1 >= m.Nz + m.Hz) ? 0.0f : ws * c[q - slab];
+                const float fdn = (k >= m.Nz + m.Hz) ? 0.0f : ws * c[q];
+                return (fup - fdn) / a.dzC[m.dz_off + k - m.Hz - 1] * dT;
+            };
+            Gc[PI_PFe_inorg] += sink(PI_PFe_inorg, b.w_sink_inorg);
+            Gc[PI_Dust] += sink(PI_Dust, b.w_sink_inorg);
+            Gc[PI_PFe_bio] += sink(PI_PFe_bio, b.w_sink_org);
+        }
+        // tracer_forcing! (tracer_forcings.jl:2-50) on max(0, tracer)
+        {
+            float Tt[PI_NTRACERS];
+#pragma unroll
+            for (int n = 0; n < PI_NTRACERS; ++n) Tt[n] = fmaxf(0.0f, a.tr[n * G + cq]);
+            Gc[PI_DIC] = Gc[PI_DIC] + Tt[PI_DOC] * b.kDOC * dT;
+            Gc[PI_DOC] = Gc[PI_DOC] - Tt[PI_DOC] * b.kDOC * dT + Tt[PI_POC] * b.kPOC * dT;
+            Gc[PI_POC] = Gc[PI_POC] - Tt[PI_POC] * b.kPOC * dT;
+            Gc[PI_NH4] = Gc[PI_NH4] + Tt[PI_DON] * b.kDON * dT - Tt[PI_NH4] * b.Nit * dT;
+            Gc[PI_NO3] = Gc[PI_NO3] + Tt[PI_NH4] * b.Nit * dT;
+            Gc[PI_DON] = Gc[PI_DON] - Tt[PI_DON] * b.kDON * dT + Tt[PI_PON] * b.kPON * dT;
+            Gc[PI_PON] = Gc[PI_PON] - Tt[PI_PON] * b.kPON * dT;
+            Gc[PI_PO4] = Gc[PI_PO4] + Tt[PI_DOP] * b.kDOP * dT;
+            Gc[PI_DOP] = Gc[PI_DOP] - Tt[PI_DOP] * b.kDOP * dT + Tt[PI_POP] * b.kPOP * dT;
+            Gc[PI_POP] = Gc[PI_POP] - Tt[PI_POP] * b.kPOP * dT;
+            const float fe = fmaxf(Tt[PI_DFe] - b.ligand, 0.0f) * Tt[PI_DFe] * b.DFeFrac * b.lambda_Fe * dT;
+            Gc[PI_DFe] = Gc[PI_DFe] + Tt[PI_PFe_bio] * b.kPOC * dT
+                       - (b.lambda_POC * Tt[PI_POC] + b.lambda_min + b.lambda_dust * Tt[PI_Dust]) * Tt[PI_DFe] * b.DFeFrac * dT
+                       + Tt[PI_PFe_inorg] * b.kdiss * dT - fe;
+            Gc[PI_PFe_bio] = Gc[PI_PFe_bio] + Tt[PI_POC] * Tt[PI_DFe] * b.DFeFrac * b.lambda_POC * dT - b.kPOC * Tt[PI_PFe_bio] * dT;
+            Gc[PI_PFe_inorg] = Gc[PI_PFe_inorg] - Tt[PI_PFe_inorg] * b.kdiss * dT
+                             + (b.lambda_min + b.lambda_dust * Tt[PI_Dust]) * Tt[PI_DFe] * b.DFeFrac * dT + fe;
+        }
+        // apply_bcs! (apply_bcs.jl:4-98)
+        if (m.any_bc) {
+            const int ii = i - m.Hx, jj = j - m.Hy, kk = k - m.Hz;
+            const float axk = m.dy * dz, ayk = m.dx * dz;
+            const int64_t itn = a.st->iteration + 1;
+            for (int n = 0; n < PI_NTRACERS; ++n) {
+                const FluxBC32* B = a.bcs + m.bc_off + n * 6;
+                if (B[PI_WEST].kind && i == 1 + m.Hx) Gc[n] += getbc32(B[PI_WEST], jj, kk, itn) * dT * axk / volk;
+                if (B[PI_EAST].kind && i == m.Nx + m.Hx) Gc[n] -= getbc32(B[PI_EAST], jj, kk, itn) * dT * axk / volk;
+                if (B[PI_SOUTH].kind && j == 1 + m.Hy) Gc[n] += getbc32(B[PI_SOUTH], ii, kk, itn) * dT * ayk / volk;
+                if (B[PI_NORTH].kind && j == m.Ny + m.Hy) Gc[n] -= getbc32(B[PI_NORTH], ii, kk, itn) * dT * ayk / volk;
+                if (B[PI_BOTTOM].kind && k == m.Nz + m.Hz) Gc[n] += getbc32(B[PI_BOTTOM], ii, jj, itn) * dT * az / volk;
+                if (B[PI_TOP].kind && k == 1 + m.Hz) Gc[n] -= getbc32(B[PI_TOP], ii, jj, itn) * dT * az / volk;
+            }
+        }
+        // plk from the fixed-point sums; only cells with binned individuals can hold any
+        float pk[ACC_N];
+#pragma unroll
+        for (int r = 0; r < ACC_N; ++r) pk[r] = 0.0f;
+        if (a.pop[cq] > 0) {
+#pragma unroll
+            for (int r = 0; r < ACC_N; ++r) {
+                const long long v = (long long)a.acc[r * G + cq];
+                if (v) { a.acc[r * G + cq] = 0ull; pk[r] = (float)((double)v * m.fx_unit); }
+            }
+        }
+        // apply_tendency! (tracer_update.jl:6-13)
+        const float plk[PI_NTRACERS] = { pk[ACC_DIC], pk[ACC_NH4], pk[ACC_NO3], pk[ACC_PO4], 0.0f, pk[ACC_DOC],
+                                         pk[ACC_DON], pk[ACC_DOP], 0.0f, pk[ACC_POC], pk[ACC_PON], pk[ACC_POP],
+                                         0.0f, 0.0f };
+#pragma unroll
+        for (int n = 0; n < PI_NTRACERS; ++n) a.tr_next[n * G + cq] = a.tr[n * G + cq] + (Gc[n] + plk[n] / volk);
+    }
+}
+
+// fill_halo_tracer! (halo_regions.jl:2-62): one thread per line along the axis over all members'
+// lines; sources are read before writes. line_off[m] = first line of member m.
+template <int AXIS>
+__global__ void k32_halo(const MemberDev* __restrict__ md, const long long* __restrict__ line_off, int nm,
+                         long long Gtot, float* __restrict__ f, int nfields, const uint32_t* err) {
+    if (err && stopped(err)) return;
+    const long long nlines = line_off[nm];
+    for (long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x; l < nlines; l += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = nm - 1;
+        while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (line_off[mid] <= l) lo = mid; else hi = mid - 1; }
+        const MemberDev& m = md[lo];
+        const long long ll = l - line_off[lo];
+        const int na = AXIS == 0 ? m.Gy : m.Gx;
+        const int a1 = (int)(ll % na) + 1, b1 = (int)(ll / na) + 1;
+        const int N = AXIS == 0 ? m.Nx : AXIS == 1 ? m.Ny : m.Nz;
+        const int H = AXIS == 0 ? m.Hx : AXIS == 1 ? m.Hy : m.Hz;
+        const int topo = AXIS == 0 ? m.tx : AXIS == 1 ? m.ty : m.tz;
+        for (int n = 0; n < nfields; ++n) {
+            float* c = f + n * Gtot + m.cell_off;
+            auto at = [&](int t) -> float& {
+                if (AXIS == 0) return c[gid3(m, t, a1, b1)];
+                if (AXIS == 1) return c[gid3(m, a1, t, b1)];
+                return c[gid3(m, a1, b1, t)];
+            };
+            float wv[8], ev[8];
+            for (int h = 1; h <= H; ++h) {
+                wv[h - 1] = topo == PI_PERIODIC ? at(N + h) : at(H + 1);
+                ev[h - 1] = topo == PI_PERIODIC ? at(H + h) : at(N + H);
+            }
+            for (int h = 1; h <= H; ++h) { at(h) = wv[h - 1]; at(N + H + h) = ev[h - 1]; }
+        }
+    }
+}
+
+// vel₀ .= vel₁ (time_step.jl:174-176), model.iteration += 1, model.t = iteration·ΔT. After a
+// capacity error nothing advances.
+__global__ void k32_end_step(int nm, MemberForcing* __restrict__ F, StepState* st, double dT, const uint32_t* err) {
+    if (stopped(err)) return;
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < nm) for (int c = 0; c < 3; ++c) F[m].vel0[c] = F[m].vel1[c];
+    if (m == 0) { st->iteration += 1; st->t = (double)st->iteration * dT; st->call_step += 1; }
+}
+
+// After a capacity error the tracers keep their values: the buffer that becomes current is a copy.
+__global__ void k32_copy_if_err(float* __restrict__ dst, const float* __restrict__ src, long long n, const uint32_t* err) {
+    if (!stopped(err)) return;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        dst[q] = src[q];
+}
+
+// ------------------------------------------------------------------------------------------
+// uploads, counts, budgets
+// ------------------------------------------------------------------------------------------
+
+// Interior array (reference layout, x fastest, FP64) into a member's halo-padded FP32 field.
+__global__ void k32_scatter_interior(MemberDev m, float* __restrict__ dst, const double* __restrict__ src,
+                                     int nx, int ny, int nz) {
+    const long long n = (long long)nx * ny * nz;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(q % nx);
+        const long long r = q / nx;
+        const int j = (int)(r % ny), k = (int)(r / ny);
+        dst[gid3(m, i + 1 + m.Hx, j + 1 + m.Hy, k + 1 + m.Hz)] = (float)src[q];
+    }
+}
+
+// Velocity halo rule along one axis (halo_regions.jl:64-99) on one member-local field.
+template <int AXIS>
+__global__ void k32_halo_vel(MemberDev m, float* __restrict__ c, int face_axis) {
+    const int na = AXIS == 0 ? m.Gy : m.Gx, nb = AXIS == 2 ? m.Gy : m.Gz;
+    const long long nl = (long long)na * nb;
+    for (long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x; l < nl; l += (long long)gridDim.x * blockDim.x) {
+        const int a1 = (int)(l % na) + 1, b1 = (int)(l / na) + 1;
+        const int N = AXIS == 0 ? m.Nx : AXIS == 1 ? m.Ny : m.Nz;
+        const int H = AXIS == 0 ? m.Hx : AXIS == 1 ? m.Hy : m.Hz;
+        const int topo = AXIS == 0 ? m.tx : AXIS == 1 ? m.ty : m.tz;
+        auto at = [&](int t) -> float& {
+            if (AXIS == 0) return c[gid3(m, t, a1, b1)];
+            if (AXIS == 1) return c[gid3(m, a1, t, b1)];
+            return c[gid3(m, a1, b1, t)];
+        };
+        float wv[8], ev[8];
+        const int velrule = (face_axis == AXIS) && topo == PI_BOUNDED;
+        for (int h = 1; h <= H; ++h) {
+            wv[h - 1] = topo == PI_PERIODIC ? at(N + h) : at(H + 1);
+            ev[h - 1] = topo == PI_PERIODIC ? at(H + h) : at(N + H);
+        }
+        const float face = velrule ? at(N + H + 1) : 0.0f;
+        for (int h = 1; h <= H; ++h) at(h) = wv[h - 1];
+        if (velrule) { for (int h = N + H + 2; h <= N + 2 * H; ++h) at(h) = face; }
+        else { for (int h = 1; h <= H; ++h) at(N + H + h) = ev[h - 1]; }
+    }
+}
+
+__global__ void k32_d2f(float* __restrict__ dst, const double* __restrict__ src, long long n) {
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        dst[q] = (float)src[q];
+}
+__global__ void k32_f2d(double* __restrict__ dst, const float* __restrict__ src, long long n) {
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        dst[q] = (double)src[q];
+}
+__global__ void k32_u2d(double* __restrict__ dst, const uint32_t* __restrict__ src, long long n) {
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        dst[q] = (double)src[q];
+}
+
+// Active individuals of a slot range (calc_active_individuals, models.jl:157-164).
+__global__ void k32_count_active(const uint8_t* __restrict__ flags, long long n, unsigned long long* out) {
+    unsigned long long c = 0;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        c += (flags[q] & F32_AC) ? 1 : 0;
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+}
+
+// FP64 mass budgets of one member: interior Σ c·vol of the C, N and P tracers (DIC+DOC+POC,
+// NH4+NO3+DON+PON, PO4+DOP+POP) and the individuals' C, N, P. Block partials (fixed order).
+__global__ void k32_budget_cells(MemberDev m, const float* __restrict__ tr, const float* __restrict__ dzF,
+                                 long long Gtot, double* __restrict__ partial) {
+    __shared__ double sh[3][256];
+    double c = 0.0, n = 0.0, p = 0.0;
+    const long long V = (long long)m.Nx * m.Ny * m.Nz;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < V; q += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(q % m.Nx) + 1 + m.Hx;
+        const long long r = q / m.Nx;
+        const int j = (int)(r % m.Ny) + 1 + m.Hy, k = (int)(r / m.Ny) + 1 + m.Hz;
+        const long long cq = m.cell_off + gid3(m, i, j, k);
+        const double vol = (double)m.dx * (double)m.dy * (double)dzF[m.dz_off + k - 1];
+        c += vol * ((double)tr[PI_DIC * Gtot + cq] + (double)tr[PI_DOC * Gtot + cq] + (double)tr[PI_POC * Gtot + cq]);
+        n += vol * ((double)tr[PI_NH4 * Gtot + cq] + (double)tr[PI_NO3 * Gtot + cq] + (double)tr[PI_DON * Gtot + cq] + (double)tr[PI_PON * Gtot + cq]);
+        p += vol * ((double)tr[PI_PO4 * Gtot + cq] + (double)tr[PI_DOP * Gtot + cq] + (double)tr[PI_POP * Gtot + cq]);
+    }
+    sh[0][threadIdx.x] = c; sh[1][threadIdx.x] = n; sh[2][threadIdx.x] = p;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) for (int r = 0; r < 3; ++r) sh[r][threadIdx.x] += sh[r][threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) for (int r = 0; r < 3; ++r) partial[blockIdx.x * 3 + r] = sh[r][0];
+}
+
+__global__ void k32_budget_inds(MemberDev m, int nsp, const SpeciesDev32* __restrict__ sp, IndDev32 P,
+                                double* __restrict__ partial) {
+    __shared__ double sh[3][256];
+    double c = 0.0, n = 0.0, p = 0.0;
+    const long long S = (long long)nsp * m.C;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < S; q += (long long)gridDim.x * blockDim.x) {
+        const long long g = m.slot_off + q;
+        if (!(P.flags[g] & F32_AC)) continue;
+        const SpeciesDev32& s = sp[q / m.C];
+        const double Bm = P.Bm[g];
+        c += Bm + (double)P.Cq[g];
+        n += Bm * (double)s.R_NC + (double)P.Nq[g];
+        p += Bm * (double)s.R_PC + (double)P.Pq[g];
+    }
+    sh[0][threadIdx.x] = c; sh[1][threadIdx.x] = n; sh[2][threadIdx.x] = p;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) for (int r = 0; r < 3; ++r) sh[r][threadIdx.x] += sh[r][threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) for (int r = 0; r < 3; ++r) partial[blockIdx.x * 3 + r] = sh[r][0];
+}
+
+}  // namespace p32

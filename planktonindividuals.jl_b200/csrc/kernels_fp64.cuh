@@ -744,7 +744,8 @@ struct ZFinalArgs {
 __device__ __forceinline__ double getbc_dev(const FluxBCDev& b, int a, int c, int64_t it) {
     if (b.kind == PI_BC_CONST) return b.v[0];
     if (b.kind == PI_BC_ARRAY2D) return b.v[(a - 1) + (long long)b.n1 * (c - 1)];
-    return b.v[(a - 1) + (long long)b.n1 * ((c - 1) + (long long)b.n2 * (it - 1))];
+    const int64_t t = it < 1 ? 1 : (it > b.nt ? b.nt : it);   // the host rejects steps past nt
+    return b.v[(a - 1) + (long long)b.n1 * ((c - 1) + (long long)b.n2 * (t - 1))];
 }
 
 #define SWZ_L 8

@@ -23,97 +23,14 @@
 #include <vector>
 
 #include "kernels_fp64.cuh"
+#include "host_common.h"
 
 using namespace pib;
+using namespace pih;
 
 namespace {
 
 thread_local std::string g_create_error;
-
-struct HostGrid {
-    int Nx, Ny, Nz, Hx, Hy, Hz, Gx, Gy, Gz;
-    int topo[3];
-    double dx, dy;
-    std::vector<double> dzF, dzC;
-    std::vector<uint8_t> lm;
-    long long G;
-    size_t id(long i, long j, long k) const {
-        return (size_t)(i - 1) + (size_t)Gx * ((size_t)(j - 1) + (size_t)Gy * (size_t)(k - 1));
-    }
-};
-
-// Host halo rules for velocities (HaloRegions/halo_regions.jl:2-99), used by vel_copy!.
-// mode 0 tracer rule, 1 velocity rule on the high face.
-void host_fill_face(const HostGrid& g, std::vector<double>& c, int axis, int face, int mode) {
-    int N = axis == 0 ? g.Nx : axis == 1 ? g.Ny : g.Nz;
-    int H = axis == 0 ? g.Hx : axis == 1 ? g.Hy : g.Hz;
-    int topo = g.topo[axis];
-    int n1 = axis == 0 ? g.Gy : g.Gx, n2 = axis == 2 ? g.Gy : g.Gz;
-    std::vector<long> dst, src;
-    if (face == 0) {
-        for (int h = 1; h <= H; ++h) { dst.push_back(h); src.push_back(topo == PI_PERIODIC ? N + h : H + 1); }
-    } else if (mode == 1 && topo == PI_BOUNDED) {
-        for (int h = N + H + 2; h <= N + 2 * H; ++h) { dst.push_back(h); src.push_back(N + H + 1); }
-    } else {
-        for (int h = 1; h <= H; ++h) { dst.push_back(N + H + h); src.push_back(topo == PI_PERIODIC ? H + h : N + H); }
-    }
-    std::vector<double> tmp(dst.size());
-    for (int b2 = 1; b2 <= n2; ++b2)
-        for (int b1 = 1; b1 <= n1; ++b1) {
-            auto at = [&](long a) -> double& {
-                if (axis == 0) return c[g.id(a, b1, b2)];
-                if (axis == 1) return c[g.id(b1, a, b2)];
-                return c[g.id(b1, b2, a)];
-            };
-            for (size_t q = 0; q < dst.size(); ++q) tmp[q] = at(src[q]);
-            for (size_t q = 0; q < dst.size(); ++q) at(dst[q]) = tmp[q];
-        }
-}
-
-void host_fill_halo_vel(const HostGrid& g, std::vector<double>& u, std::vector<double>& v, std::vector<double>& w) {
-    host_fill_face(g, u, 0, 1, 1); host_fill_face(g, u, 0, 0, 0);
-    host_fill_face(g, u, 1, 0, 0); host_fill_face(g, u, 1, 1, 0);
-    host_fill_face(g, u, 2, 0, 0); host_fill_face(g, u, 2, 1, 0);
-    host_fill_face(g, v, 1, 1, 1); host_fill_face(g, v, 0, 0, 0); host_fill_face(g, v, 0, 1, 0);
-    host_fill_face(g, v, 1, 0, 0); host_fill_face(g, v, 2, 0, 0); host_fill_face(g, v, 2, 1, 0);
-    host_fill_face(g, w, 2, 1, 1); host_fill_face(g, w, 0, 0, 0); host_fill_face(g, w, 0, 1, 0);
-    host_fill_face(g, w, 1, 0, 0); host_fill_face(g, w, 1, 1, 0); host_fill_face(g, w, 2, 0, 0);
-}
-
-// Interior velocity snapshot (reference array layout) → halo-padded fields (vel_copy!).
-void host_vel_copy(const HostGrid& g, const double* u, const double* v, const double* w,
-                   std::vector<double>& U, std::vector<double>& V, std::vector<double>& W) {
-    U.assign(g.G, 0.0); V.assign(g.G, 0.0); W.assign(g.G, 0.0);
-    int ex = g.topo[0] == PI_BOUNDED, ey = g.topo[1] == PI_BOUNDED, ez = g.topo[2] == PI_BOUNDED;
-    auto copy_in = [&](std::vector<double>& f, const double* s, int nx, int ny, int nz) {
-        for (int k = 1; k <= nz; ++k) for (int j = 1; j <= ny; ++j) for (int i = 1; i <= nx; ++i)
-            f[g.id(i + g.Hx, j + g.Hy, k + g.Hz)] =
-                s[(size_t)(i - 1) + (size_t)nx * ((size_t)(j - 1) + (size_t)ny * (size_t)(k - 1))];
-    };
-    copy_in(U, u, g.Nx + ex, g.Ny, g.Nz);
-    copy_in(V, v, g.Nx, g.Ny + ey, g.Nz);
-    copy_in(W, w, g.Nx, g.Ny, g.Nz + ez);
-    host_fill_halo_vel(g, U, V, W);
-}
-
-// Julia's string(x::Float64) for the capacity message: shortest round-trip digits.
-std::string julia_float(double x) {
-    char buf[64];
-    for (int p = 1; p <= 17; ++p) {
-        snprintf(buf, sizeof buf, "%.*g", p, x);
-        if (strtod(buf, nullptr) == x) break;
-    }
-    std::string s(buf);
-    size_t e = s.find('e');
-    if (e == std::string::npos) {
-        if (s.find('.') == std::string::npos && s.find("inf") == std::string::npos && s.find("nan") == std::string::npos) s += ".0";
-        return s;
-    }
-    std::string mant = s.substr(0, e), ex = s.substr(e + 1);
-    if (mant.find('.') == std::string::npos) mant += ".0";
-    int ev = atoi(ex.c_str());
-    return mant + "e" + std::to_string(ev);
-}
 
 struct DevBC {
     int kind = PI_BC_NONE;
@@ -134,6 +51,7 @@ struct pi_model {
     long long C = 0;
     uint64_t seed = 0;
     int precision = PI_FP64;
+    pi_batch* b32 = nullptr;     // PI_FP32: the model is a batch of one member
     int64_t iteration = 0;
     double t = 0.0;
     double last_dT = 0.0;
@@ -183,6 +101,7 @@ struct pi_model {
 
 struct pi_sim {
     pi_model* m = nullptr;
+    int fp32 = 0;
     double dT = 0.0;
     int64_t iterations = 0;
     int has_vel = 0;
@@ -198,6 +117,16 @@ namespace {
 pi_status fail(pi_model* m, pi_status code, const std::string& msg) {
     if (m) m->err = msg; else g_create_error = msg;
     return code;
+}
+
+// Result of a call forwarded to the FP32 batch of a PI_FP32 model, with its message.
+pi_status fwd32(pi_model* m, pi_status st) {
+    if (st != PI_OK) {
+        char buf[1024];
+        pi_batch_last_error(m->b32, buf, sizeof buf);
+        m->err = buf;
+    }
+    return st;
 }
 
 pi_status cuda_fail(pi_model* m, cudaError_t e, const char* what) {
@@ -292,6 +221,13 @@ pi_status check_device_errors(pi_model* m) {
 
 // Enqueues one TimeStep! on the model's stream (no synchronisation).
 pi_status enqueue_step(pi_model* m, double dT) {
+    // getbc(bc, i, j, t) of a time-dependent flux reads bc[i, j, iteration] (boundary_conditions.jl:44-52)
+    for (int n = 0; n < PI_NTRACERS; ++n)
+        for (int f = 0; f < 6; ++f)
+            if (m->bcs[n][f].kind == PI_BC_ARRAY3D && m->bcs[n][f].nt < m->iteration + 1)
+                return fail(m, PI_ERR_SHAPE, "BoundsError: time-dependent flux boundary condition has " +
+                                                 std::to_string(m->bcs[n][f].nt) + " snapshots, step " +
+                                                 std::to_string(m->iteration + 1) + " needs one more");
     m->iteration += 1;
     m->t = (double)m->iteration * dT;
     m->last_dT = dT;
@@ -462,8 +398,8 @@ pi_status pi_create(const pi_grid* grid, const pi_bgc_params* bgc, const pi_quot
     *out = nullptr;
     if (!grid || !bgc || !species || nspecies < 1 || capacity < 1 || !grid->dzF || !grid->dzC)
         return fail(nullptr, PI_ERR_ARG, "pi_create: NULL argument, nspecies < 1 or capacity < 1");
-    if (precision != PI_FP64)
-        return fail(nullptr, PI_ERR_ARG, "pi_create: this build provides the FP64 form (PI_FP64) only");
+    if (precision != PI_FP64 && precision != PI_FP32)
+        return fail(nullptr, PI_ERR_ARG, "pi_create: precision must be PI_FP64 or PI_FP32");
     if (grid->Nx < 1 || grid->Ny < 1 || grid->Nz < 1)
         return fail(nullptr, PI_ERR_ARG, "pi_create: grid size must be at least 1 in every direction");
     if (grid->Hx < 2 || grid->Hy < 2 || grid->Hz < 2 || grid->Hx > 8 || grid->Hy > 8 || grid->Hz > 8)
@@ -482,6 +418,27 @@ pi_status pi_create(const pi_grid* grid, const pi_bgc_params* bgc, const pi_quot
         std::string msg;
         pi_status st = validate_quota(species[s], s, msg);
         if (st) return fail(nullptr, st, msg);
+    }
+    if (precision == PI_FP32) {
+        pi_member mb{grid, bgc, species, capacity, seed};
+        pi_batch* b32 = nullptr;
+        pi_status st = pi_batch_create(&mb, 1, nspecies, &b32);
+        if (st) {
+            char buf[1024];
+            pi_batch_last_error(nullptr, buf, sizeof buf);
+            std::string msg = buf;
+            const std::string pre = "pi_batch_create: member 0: ";
+            if (msg.compare(0, pre.size(), pre) == 0) msg = "pi_create: " + msg.substr(pre.size());
+            return fail(nullptr, st, msg);
+        }
+        pi_model* m = new pi_model();
+        m->b32 = b32;
+        m->precision = PI_FP32;
+        m->nsp = nspecies; m->C = capacity; m->seed = seed;
+        m->bgc = *bgc;
+        m->sp.assign(species, species + nspecies);
+        *out = m;
+        return PI_OK;
     }
     pi_model* m = new pi_model();
     if (cudaGetDevice(&m->device) != cudaSuccess) {
@@ -594,6 +551,11 @@ pi_status pi_create(const pi_grid* grid, const pi_bgc_params* bgc, const pi_quot
 
 pi_status pi_destroy(pi_model* m) {
     if (!m) return PI_OK;
+    if (m->b32) {
+        pi_batch_destroy(m->b32);
+        delete m;
+        return PI_OK;
+    }
     cudaStreamSynchronize(m->stream);
     drain_marks(m);
     for (cudaEvent_t e : m->event_pool) cudaEventDestroy(e);
@@ -604,6 +566,7 @@ pi_status pi_destroy(pi_model* m) {
 }
 
 pi_status pi_set_individuals(pi_model* m, int32_t sp, const pi_individuals* in) {
+    if (m && m->b32) return fwd32(m, pi_batch_set_individuals(m->b32, 0, sp, in));
     if (!m || !in || sp < 0 || sp >= m->nsp) return fail(m, PI_ERR_ARG, "pi_set_individuals: bad argument");
     const double* dcols[] = { in->x, in->y, in->z, in->Sz, in->Bm, in->Cq, in->Nq, in->Pq, in->Chl, in->gen, in->age,
                               in->graz, in->mort, in->dvid };
@@ -636,6 +599,7 @@ pi_status pi_set_individuals(pi_model* m, int32_t sp, const pi_individuals* in) 
 }
 
 pi_status pi_get_individuals(pi_model* m, int32_t sp, pi_individuals* out) {
+    if (m && m->b32) return fwd32(m, pi_batch_get_individuals(m->b32, 0, sp, out));
     if (!m || !out || sp < 0 || sp >= m->nsp) return fail(m, PI_ERR_ARG, "pi_get_individuals: bad argument");
     const long long C = m->C;
     const SpcDev& P = m->h_spc[sp];
@@ -664,6 +628,7 @@ pi_status pi_get_individuals(pi_model* m, int32_t sp, pi_individuals* out) {
 }
 
 pi_status pi_set_tracer(pi_model* m, int32_t idx, const double* data) {
+    if (m && m->b32) return fwd32(m, pi_batch_set_tracer(m->b32, 0, idx, data));
     if (!m || !data || idx < 0 || idx >= PI_NTRACERS) return fail(m, PI_ERR_ARG, "pi_set_tracer: bad argument");
     CK(cudaMemcpyAsync(m->tr + (size_t)idx * m->hg.G, data, m->hg.G * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload tracer");
     CK(cudaStreamSynchronize(m->stream), "synchronize");
@@ -671,6 +636,7 @@ pi_status pi_set_tracer(pi_model* m, int32_t idx, const double* data) {
 }
 
 pi_status pi_get_tracer(pi_model* m, int32_t idx, double* out) {
+    if (m && m->b32) return fwd32(m, pi_batch_get_tracer(m->b32, 0, idx, out));
     if (!m || !out || idx < 0 || idx >= PI_NTRACERS) return fail(m, PI_ERR_ARG, "pi_get_tracer: bad argument");
     CK(cudaMemcpyAsync(out, m->tr + (size_t)idx * m->hg.G, m->hg.G * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download tracer");
     CK(cudaStreamSynchronize(m->stream), "synchronize");
@@ -703,6 +669,7 @@ static pi_status device_vel_copy(pi_model* m, const double* u, const double* v, 
 }
 
 pi_status pi_set_velocity(pi_model* m, const double* u, const double* v, const double* w) {
+    if (m && m->b32) return fwd32(m, pi_batch_set_velocity(m->b32, 0, u, v, w));
     if (!m || !u || !v || !w) return fail(m, PI_ERR_ARG, "pi_set_velocity: NULL argument");
     // write into the own buffer that vel₀ does not alias
     int b = (m->vel0[0] == m->velbuf[0][0]) ? 1 : 0;
@@ -725,6 +692,7 @@ pi_status pi_set_velocity(pi_model* m, const double* u, const double* v, const d
 }
 
 pi_status pi_set_velocity0(pi_model* m, const double* u, const double* v, const double* w) {
+    if (m && m->b32) return fwd32(m, pi_batch_set_velocity0(m->b32, 0, u, v, w));
     if (!m || !u || !v || !w) return fail(m, PI_ERR_ARG, "pi_set_velocity0: NULL argument");
     // write into the own buffer that vel₁ does not alias
     int b = (m->vel1[0] == m->velbuf[0][0]) ? 1 : 0;
@@ -746,6 +714,7 @@ pi_status pi_set_velocity0(pi_model* m, const double* u, const double* v, const 
 }
 
 pi_status pi_set_PARF(pi_model* m, const double* parf) {
+    if (m && m->b32) return fwd32(m, pi_batch_set_PARF(m->b32, 0, parf));
     if (!m || !parf) return fail(m, PI_ERR_ARG, "pi_set_PARF: NULL argument");
     CK(cudaMemcpyAsync(m->PARF, parf, (size_t)m->hg.Nx * m->hg.Ny * sizeof(double), cudaMemcpyDefault, m->stream), "upload PARF");
     CK(cudaStreamSynchronize(m->stream), "synchronize");
@@ -753,6 +722,7 @@ pi_status pi_set_PARF(pi_model* m, const double* parf) {
 }
 
 pi_status pi_set_temp(pi_model* m, const double* temp) {
+    if (m && m->b32) return fwd32(m, pi_batch_set_temp(m->b32, 0, temp));
     if (!m || !temp) return fail(m, PI_ERR_ARG, "pi_set_temp: NULL argument");
     const HostGrid& g = m->hg;
     size_t n = (size_t)g.Nx * g.Ny * g.Nz;
@@ -766,6 +736,7 @@ pi_status pi_set_temp(pi_model* m, const double* temp) {
 }
 
 pi_status pi_set_flux_bc(pi_model* m, int32_t tracer, int32_t face, int32_t kind, const double* values, int64_t nt) {
+    if (m && m->b32) return fwd32(m, pi_batch_set_flux_bc(m->b32, 0, tracer, face, kind, values, nt));
     if (!m || tracer < 0 || tracer >= PI_NTRACERS || face < 0 || face > 5 || kind < 0 || kind > 3)
         return fail(m, PI_ERR_ARG, "pi_set_flux_bc: bad argument");
     const HostGrid& g = m->hg;
@@ -784,6 +755,7 @@ pi_status pi_set_flux_bc(pi_model* m, int32_t tracer, int32_t face, int32_t kind
 }
 
 pi_status pi_time_step(pi_model* m, double dT) {
+    if (m && m->b32) return fwd32(m, pi_batch_step(m->b32, dT, 1, 1));
     if (!m) return fail(m, PI_ERR_ARG, "pi_time_step: NULL model");
     pi_status st = enqueue_step(m, dT);
     if (st) return st;
@@ -791,12 +763,14 @@ pi_status pi_time_step(pi_model* m, double dT) {
 }
 
 pi_status pi_get_stream(pi_model* m, void** stream) {
+    if (m && m->b32) return fwd32(m, pi_batch_get_stream(m->b32, stream));
     if (!m || !stream) return fail(m, PI_ERR_ARG, "pi_get_stream: NULL argument");
     *stream = (void*)m->stream;
     return PI_OK;
 }
 
 pi_status pi_profile_enable(pi_model* m, int32_t on) {
+    if (m && m->b32) return fwd32(m, pi_batch_profile_enable(m->b32, on));
     if (!m) return fail(m, PI_ERR_ARG, "pi_profile_enable: NULL model");
     CK(cudaStreamSynchronize(m->stream), "synchronize");
     drain_marks(m);
@@ -807,6 +781,7 @@ pi_status pi_profile_enable(pi_model* m, int32_t on) {
 
 pi_status pi_profile_read(pi_model* m, int32_t max, char* names, size_t names_len,
                           int64_t* launches, double* ms, int32_t* n) {
+    if (m && m->b32) return fwd32(m, pi_batch_profile_read(m->b32, max, names, names_len, launches, ms, n));
     if (!m || !n) return fail(m, PI_ERR_ARG, "pi_profile_read: NULL argument");
     CK(cudaStreamSynchronize(m->stream), "synchronize");
     drain_marks(m);
@@ -825,12 +800,14 @@ pi_status pi_profile_read(pi_model* m, int32_t max, char* names, size_t names_le
 }
 
 pi_status pi_synchronize(pi_model* m) {
+    if (m && m->b32) return fwd32(m, pi_batch_synchronize(m->b32));
     if (!m) return fail(m, PI_ERR_ARG, "pi_synchronize: NULL model");
     CK(cudaStreamSynchronize(m->stream), "synchronize");
     return check_device_errors(m);
 }
 
 pi_status pi_get_time(pi_model* m, int64_t* iteration, double* t) {
+    if (m && m->b32) return fwd32(m, pi_batch_get_time(m->b32, iteration, t));
     if (!m) return fail(m, PI_ERR_ARG, "pi_get_time: NULL model");
     if (iteration) *iteration = m->iteration;
     if (t) *t = m->t;
@@ -838,12 +815,17 @@ pi_status pi_get_time(pi_model* m, int64_t* iteration, double* t) {
 }
 
 pi_status pi_set_time(pi_model* m, int64_t iteration, double t) {
+    if (m && m->b32) return fwd32(m, pi_batch_set_time(m->b32, iteration, t));
     if (!m) return fail(m, PI_ERR_ARG, "pi_set_time: NULL model");
     m->iteration = iteration; m->t = t;
     return PI_OK;
 }
 
 pi_status pi_count_active(pi_model* m, int32_t sp, int64_t* n) {
+    if (m && m->b32) {
+        if (sp < 0 || sp >= m->nsp) return fail(m, PI_ERR_ARG, "pi_count_active: bad argument");
+        return fwd32(m, pi_batch_count_active(m->b32, 0, sp, n));
+    }
     if (!m || !n || sp < 0 || sp >= m->nsp) return fail(m, PI_ERR_ARG, "pi_count_active: bad argument");
     unsigned long long* d = (unsigned long long*)m->sb.rank64;   // scratch between steps
     unsigned long long h = 0;
@@ -857,6 +839,7 @@ pi_status pi_count_active(pi_model* m, int32_t sp, int64_t* n) {
 }
 
 pi_status pi_get_diag(pi_model* m, int32_t kind, int32_t sp, double* out) {
+    if (m && m->b32) return fwd32(m, pi_batch_get_diag(m->b32, 0, kind, sp, out));
     if (!m || !out) return fail(m, PI_ERR_ARG, "pi_get_diag: bad argument");
     const long long G = m->hg.G;
     const double* src = nullptr;
@@ -871,6 +854,7 @@ pi_status pi_get_diag(pi_model* m, int32_t kind, int32_t sp, double* out) {
 }
 
 pi_status pi_reset_diags(pi_model* m) {
+    if (m && m->b32) return fwd32(m, pi_batch_reset_diags(m->b32));
     if (!m) return fail(m, PI_ERR_ARG, "pi_reset_diags: NULL model");
     const long long G = m->hg.G;
     CK(cudaMemsetAsync(m->diag_par, 0, G * sizeof(double), m->stream), "reset diags");
@@ -910,6 +894,14 @@ pi_status pi_sim_create(pi_model* m, double dT, int64_t iterations,
     if ((double)ntemp < std::floor((double)iterations * dT / dT_temp))
         return fail(m, PI_ERR_SHAPE, "Temperature provided cannot cover the time period of (iterations+1)*ΔT (" +
                                       julia_float((double)iterations * dT) + " seconds) with ΔT_temp = " + julia_float(dT_temp) + ".");
+    if (m->b32) {
+        pi_status st = pi_batch_set_series(m->b32, 0, u, v, w, nvel, dT_vel, parf, npar, dT_PAR, temp, ntemp, dT_temp, 0);
+        if (st) return fwd32(m, st);
+        pi_sim* s = new pi_sim();
+        s->m = m; s->fp32 = 1; s->dT = dT; s->iterations = iterations; s->has_vel = has_vel;
+        *out = s;
+        return PI_OK;
+    }
     pi_sim* s = new pi_sim();
     s->m = m; s->dT = dT; s->iterations = iterations; s->has_vel = has_vel;
     s->nvel = nvel; s->npar = npar; s->ntemp = ntemp; s->dT_vel = dT_vel; s->dT_PAR = dT_PAR; s->dT_temp = dT_temp;
@@ -955,6 +947,11 @@ pi_status pi_sim_create(pi_model* m, double dT, int64_t iterations,
 pi_status pi_sim_update(pi_sim* s, int32_t time_offset, int32_t sync) {
     if (!s || !s->m) return PI_ERR_ARG;
     pi_model* m = s->m;
+    if (s->fp32) {
+        pi_status st = pi_batch_set_time_offset(m->b32, 0, time_offset);
+        if (st) return fwd32(m, st);
+        return fwd32(m, pi_batch_step(m->b32, s->dT, s->iterations, sync));
+    }
     const HostGrid& g = m->hg;
     const size_t nf = (size_t)g.Nx * g.Ny;
     for (int64_t i = 1; i <= s->iterations; ++i) {
@@ -983,6 +980,11 @@ pi_status pi_sim_update(pi_sim* s, int32_t time_offset, int32_t sync) {
 pi_status pi_sim_destroy(pi_sim* s) {
     if (!s) return PI_OK;
     pi_model* m = s->m;
+    if (s->fp32) {
+        pi_status st = m ? fwd32(m, pi_batch_clear_series(m->b32, 0)) : PI_OK;
+        delete s;
+        return st;
+    }
     if (m) {
         cudaStreamSynchronize(m->stream);
         // the model must not keep pointers into the series
