@@ -10,13 +10,14 @@
 //   k32_assign           k-th divider → k-th free slot per (member, species) segment
 //   k32_daughters        copy_daughter_individuals! + divide_to_half!
 //   k32_physiology       QuotaMode growth, consumption sums, decisions for the next step
-//   k32_sweep_x/y/z      DST3FL sweeps, advective tendency
-//   k32_tail             diffusion, sinking, forcing, BCs, particle terms, apply_tendency!
+//   k32_xy               DST3FL x and y sweeps of every tracer on level tiles in shared memory
+//   k32_ztail            z sweep walking columns, then diffusion, sinking, forcing, BCs, particle
+//                        terms and apply_tendency!
 //   k32_halo<x,y,z>      fill_halo_tracer!
 //   k32_end_step         vel₀ ← vel₁, iteration and t
 // Nothing in a step reads a host value, so the step is captured once as a CUDA graph (one per
 // tracer-buffer parity) and replayed. The results do not depend on block shapes, tile-per-block
-// assignment or sweep segment lengths (integer sums commute; every other value is computed by
+// assignment, tracer tile heights or z walk lengths (integer sums commute; every other value is computed by
 // exactly one thread from the same inputs), which lets the autotuner time real steps.
 #include <cub/device/device_scan.cuh>
 
@@ -62,8 +63,9 @@ struct MemberHost {
 struct Tuning {
     int bs_move = 256, bs_phys = 256, bs_assign = 256;
     int persist_move = 0, persist_phys = 0;   // 0: one tile per block; k: k blocks per SM, looping
-    int Ly = 8, Lz = 8;
-    int wpb_x = 4, wpb_y = 4, wpb_z = 4, wpb_tail = 4, wpb_par = 4;
+    int ty = 4;                               // rows of an x-y tracer tile (4 or 8)
+    int lz = 16;                              // levels walked by a z thread (8, 16 or 32)
+    int wpb_par = 4;
 };
 
 }  // namespace
@@ -79,7 +81,7 @@ struct pi_batch {
     std::vector<FluxBC32> bch;
     std::string err;
     std::vector<void*> allocs;
-    long long Gtot = 0, Stot = 0, ncol = 0, maxG = 0;
+    long long Gtot = 0, Stot = 0, ncol = 0, maxG = 0, maxcol = 0;
     int nlev = 0;
     // device
     MemberDev* md = nullptr;
@@ -92,7 +94,6 @@ struct pi_batch {
     uint32_t* errw = nullptr;
     float* trbuf[2] = {nullptr, nullptr};
     int cur = 0;                    // trbuf[cur] holds the current tracers
-    float *ta = nullptr, *tb = nullptr;
     float *par = nullptr, *diag_par = nullptr, *PARF = nullptr;
     float *dzF = nullptr, *dzC = nullptr;
     uint8_t* lm = nullptr;
@@ -122,7 +123,13 @@ struct pi_batch {
     // work tables (device) built for the current tuning
     Tab32 T{};
     std::vector<void*> table_allocs;
-    int tables_Ly = -1, tables_Lz = -1;
+    int tables_ty = -1, tables_lz = -1;
+    int4* xy_items = nullptr;
+    int nxy_items = 0;
+    int4* z_items = nullptr;
+    int nz_items = 0;
+    float* tb = nullptr;
+    float* rdzC = nullptr;
     Tuning tune;
     // graphs
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
@@ -211,7 +218,7 @@ void free_graphs(pi_batch* b) {
 void free_tables(pi_batch* b) {
     for (void* p : b->table_allocs) cudaFree(p);
     b->table_allocs.clear();
-    b->tables_Ly = b->tables_Lz = -1;
+    b->tables_ty = b->tables_lz = -1;
 }
 
 void free_series(MemberHost& h) {
@@ -288,29 +295,25 @@ pi_status check_member(const pi_member& mb, int nsp, std::string& msg) {
     return PI_OK;
 }
 
-// Work tables for the current tuning (sweep segment lengths) on the device.
+// Work tables for the current tuning (tracer tile height, z walk length) on the device.
 pi_status build_tables(pi_batch* b) {
-    const int Ly = b->tune.Ly, Lz = b->tune.Lz;
-    if (b->tables_Ly == Ly && b->tables_Lz == Lz) return PI_OK;
+    const int ty = b->tune.ty, lz = b->tune.lz;
+    if (b->tables_ty == ty && b->tables_lz == lz) return PI_OK;
     free_tables(b);
-    std::vector<int4> ix, iy, iz, ic, icol;
+    std::vector<int4> xy, zz, icol;
     for (int m = 0; m < b->nm; ++m) {
         const HostGrid& g = b->mh[m].g;
-        for (int k = 1 + g.Hz; k <= g.Nz + g.Hz; ++k)
-            for (int j = 1 + g.Hy; j <= g.Ny + g.Hy; ++j) {
-                for (int i0 = 1 + g.Hx; i0 <= g.Nx + g.Hx; i0 += 31) ix.push_back(make_int4(m, j, k, i0));
-                for (int i0 = 1 + g.Hx; i0 <= g.Nx + g.Hx; i0 += 32) ic.push_back(make_int4(m, i0, j, k));
-            }
-        for (int k = 1 + g.Hz; k <= g.Nz + g.Hz; ++k)
-            for (int j0 = 1 + g.Hy; j0 <= g.Ny + g.Hy; j0 += Ly)
-                for (int i0 = 1 + g.Hx; i0 <= g.Nx + g.Hx; i0 += 32) iy.push_back(make_int4(m, i0, j0, k));
-        for (int k0 = 1 + g.Hz; k0 <= g.Nz + g.Hz; k0 += Lz)
+        for (int L = 1 + g.Hz; L <= g.Nz + g.Hz; ++L)
+            for (int j0 = 1 + g.Hy; j0 <= g.Ny + g.Hy; j0 += ty)
+                for (int i0 = 1 + g.Hx; i0 <= g.Nx + g.Hx; i0 += 28) xy.push_back(make_int4(m, i0, j0, L));
+        for (int k0 = 1 + g.Hz; k0 <= g.Nz + g.Hz; k0 += lz)
             for (int j = 1 + g.Hy; j <= g.Ny + g.Hy; ++j)
-                for (int i0 = 1 + g.Hx; i0 <= g.Nx + g.Hx; i0 += 32) iz.push_back(make_int4(m, i0, j, k0));
+                for (int i0 = 1 + g.Hx; i0 <= g.Nx + g.Hx; i0 += 32) zz.push_back(make_int4(m, i0, j, k0));
         for (int j = 1; j <= g.Ny; ++j)
             for (int i0 = 1; i0 <= g.Nx; i0 += 32) icol.push_back(make_int4(m, i0, j, 0));
     }
-    auto up = [&](std::vector<int4>& v, const int4** dst, int* n) -> pi_status {
+    if (xy.size() >= (size_t)INT32_MAX || zz.size() >= (size_t)INT32_MAX) return bfail(b, PI_ERR_ARG, "work tables too large");
+    auto up = [&](std::vector<int4>& v, int4** dst, int* n) -> pi_status {
         int4* d = nullptr;
         pi_status s = balloc(b, &d, v.size(), "work table", &b->table_allocs);
         if (s) return s;
@@ -319,16 +322,17 @@ pi_status build_tables(pi_batch* b) {
         return PI_OK;
     };
     pi_status s;
-    if ((s = up(ix, &b->T.ix, &b->T.nix))) return s;
-    if ((s = up(iy, &b->T.iy, &b->T.niy))) return s;
-    if ((s = up(iz, &b->T.iz, &b->T.niz))) return s;
-    if ((s = up(ic, &b->T.ic, &b->T.nic))) return s;
-    if ((s = up(icol, &b->T.icol, &b->T.nicol))) return s;
+    int4* ic = nullptr;
+    if ((s = up(xy, &b->xy_items, &b->nxy_items))) return s;
+    if ((s = up(zz, &b->z_items, &b->nz_items))) return s;
+    if ((s = up(icol, &ic, &b->T.nicol))) return s;
+    b->T.icol = ic;
     BK(cudaStreamSynchronize(b->stream), "synchronize");
-    b->T.Ly = Ly; b->T.Lz = Lz;
-    b->tables_Ly = Ly; b->tables_Lz = Lz;
+    b->tables_ty = ty; b->tables_lz = lz;
     return PI_OK;
 }
+
+size_t xy_smem(int ty) { return (size_t)(3 * ty + 5) * PI_NTRACERS * 32 * sizeof(float); }
 
 float* velown(pi_batch* b, int m, int buf, int c) { return b->velown + ((long long)(buf * 3 + c)) * b->Gtot + b->mdh[m].cell_off; }
 
@@ -349,7 +353,8 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
     BK(cudaMemsetAsync(b->pop, 0, G * sizeof(int), s), "zero pop");
     if (b->pop_sp) BK(cudaMemsetAsync(b->pop_sp, 0, (size_t)b->nsp * G * sizeof(int), s), "zero pop");
     { BScope sc(b, "k32_bind");
-      k32_bind<<<b->nm, 128, 0, s>>>(b->nm, b->md, b->S, b->F, b->st, dT, b->PARF, b->errw); }
+      const unsigned gx = std::max(1u, std::min<unsigned>(nblk(b->maxcol, 256), 64));
+      k32_bind<<<dim3(gx, b->nm), 256, 0, s>>>(b->nm, b->md, b->S, b->F, b->st, dT, b->PARF, b->errw); }
     { BScope sc(b, "k32_velhalf");
       unsigned gx = std::min<unsigned>(nblk(b->maxG, 256), 64);
       k32_velhalf<<<dim3(gx, b->nm), 256, 0, s>>>(b->md, b->F, b->errw); }
@@ -379,25 +384,26 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
         BScope sc(b, "k32_physiology");
         k32_physiology<<<tile_grid(b, b->tune.persist_phys), b->tune.bs_phys, 0, s>>>(a);
     }
-    SweepArgs sw;
-    sw.T = b->T; sw.lm = b->lm; sw.dzF = b->dzF; sw.dzC = b->dzC; sw.F = b->F; sw.Gtot = G; sw.tr = tr;
-    sw.dT = fdT; sw.err = b->errw;
-    { sw.src = tr; sw.dst = b->ta;
-      BScope sc(b, "k32_sweep_x");
-      k32_sweep_x<<<warp_grid(b->T.nix, b->tune.wpb_x), 32 * b->tune.wpb_x, 0, s>>>(sw); }
-    { sw.src = b->ta; sw.dst = b->tb;
-      BScope sc(b, "k32_sweep_y");
-      k32_sweep_y<<<warp_grid(b->T.niy, b->tune.wpb_y), 32 * b->tune.wpb_y, 0, s>>>(sw); }
-    { sw.src = b->tb; sw.dst = b->ta;
-      BScope sc(b, "k32_sweep_z");
-      k32_sweep_z<<<warp_grid(b->T.niz, b->tune.wpb_z), 32 * b->tune.wpb_z, 0, s>>>(sw); }
     {
-        TailArgs a;
-        a.T = b->T; a.lm = b->lm; a.dzF = b->dzF; a.dzC = b->dzC; a.bgc = b->bgc; a.bcs = b->bcs; a.st = b->st;
-        a.Gtot = G; a.tr = tr; a.gadv = b->ta; a.tr_next = trn; a.acc = b->acc; a.pop = b->pop; a.dT = fdT;
-        a.err = b->errw;
-        BScope sc(b, "k32_tail");
-        k32_tail<<<warp_grid(b->T.nic, b->tune.wpb_tail), 32 * b->tune.wpb_tail, 0, s>>>(a);
+        TrArgs a;
+        a.T = b->T; a.lm = b->lm; a.dzF = b->dzF; a.dzC = b->dzC; a.rdzC = b->rdzC; a.bgc = b->bgc;
+        a.bcs = b->bcs; a.st = b->st; a.F = b->F; a.Gtot = G; a.tr = tr; a.tb = b->tb; a.tr_next = trn;
+        a.acc = b->acc; a.pop = b->pop; a.dT = fdT; a.err = b->errw;
+        {
+            a.items = b->xy_items; a.nitems = b->nxy_items;
+            BScope sc(b, "k32_xy");
+            const unsigned grid = (unsigned)std::max(1, b->nxy_items);
+            if (b->tune.ty == 8) k32_xy<8><<<grid, 32 * 12, xy_smem(8), s>>>(a);
+            else k32_xy<4><<<grid, 32 * 8, xy_smem(4), s>>>(a);
+        }
+        {
+            a.items = b->z_items; a.nitems = b->nz_items;
+            BScope sc(b, "k32_ztail");
+            const unsigned grid = warp_grid(b->nz_items, 4);
+            if (b->tune.lz == 8) k32_ztail<8><<<grid, 128, 0, s>>>(a);
+            else if (b->tune.lz == 32) k32_ztail<32><<<grid, 128, 0, s>>>(a);
+            else k32_ztail<16><<<grid, 128, 0, s>>>(a);
+        }
     }
     { BScope sc(b, "k32_halo");
       k32_halo<0><<<std::min<unsigned>(nblk(b->nlines[0], 128), 148 * 8), 128, 0, s>>>(b->md, b->line_off[0], b->nm, G, trn, PI_NTRACERS, b->errw);
@@ -542,6 +548,7 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
         col += (long long)g.Nx * g.Ny;
         lev += g.Gz;
         b->maxG = std::max(b->maxG, g.G);
+        b->maxcol = std::max(b->maxcol, (long long)g.Nx * g.Ny);
     }
     seg_tile0.push_back((int)tiles.size());
     if (tiles.size() >= (size_t)INT32_MAX) { b->err = "pi_batch_create: too many slots"; return bail(PI_ERR_ARG); }
@@ -551,9 +558,9 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
 #define BA(ptr, n) do { st = balloc(b, &(ptr), (size_t)(n), #ptr); if (st) return bail(st); } while (0)
     BA(b->md, nmembers); BA(b->sp, sph.size()); BA(b->bgc, nmembers); BA(b->bcs, (size_t)nmembers * PI_NTRACERS * 6);
     BA(b->F, nmembers); BA(b->S, nmembers); BA(b->st, 1); BA(b->errw, 1);
-    BA(b->trbuf[0], PI_NTRACERS * G); BA(b->trbuf[1], PI_NTRACERS * G); BA(b->ta, PI_NTRACERS * G); BA(b->tb, PI_NTRACERS * G);
+    BA(b->trbuf[0], PI_NTRACERS * G); BA(b->trbuf[1], PI_NTRACERS * G); BA(b->tb, PI_NTRACERS * G);
     BA(b->par, G); BA(b->diag_par, G); BA(b->PARF, std::max<long long>(col, 1));
-    BA(b->dzF, lev); BA(b->dzC, lev);
+    BA(b->dzF, lev); BA(b->dzC, lev); BA(b->rdzC, lev);
     if (any_land) BA(b->lm, G);
     BA(b->velown, 6 * G); BA(b->velh, 3 * G); BA(b->tempown, G);
     BA(b->dcnt, (size_t)nspecies * 4 * G); BA(b->pop, G);
@@ -610,6 +617,9 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     H2D(b->S, b->serh.data(), nmembers * sizeof(MemberSeries));
     H2D(b->dzF, dzF.data(), dzF.size() * sizeof(float));
     H2D(b->dzC, dzC.data(), dzC.size() * sizeof(float));
+    std::vector<float> rdzC(dzC.size());
+    for (size_t q = 0; q < dzC.size(); ++q) rdzC[q] = 1.0f / dzC[q];
+    H2D(b->rdzC, rdzC.data(), rdzC.size() * sizeof(float));
     H2D(b->tiles, tiles.data(), tiles.size() * sizeof(int2));
     H2D(b->seg_tile0, seg_tile0.data(), seg_tile0.size() * sizeof(int));
     for (int a = 0; a < 3; ++a) H2D(b->line_off[a], lo[a].data(), (nmembers + 1) * sizeof(long long));
@@ -622,7 +632,6 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     }
     Z(b->st, sizeof(StepState)); Z(b->errw, sizeof(uint32_t));
     for (int q = 0; q < 2; ++q) Z(b->trbuf[q], PI_NTRACERS * G * sizeof(float));
-    Z(b->ta, PI_NTRACERS * G * sizeof(float)); Z(b->tb, PI_NTRACERS * G * sizeof(float));
     Z(b->par, G * sizeof(float)); Z(b->diag_par, G * sizeof(float)); Z(b->PARF, std::max<long long>(col, 1) * sizeof(float));
     Z(b->velown, 6 * G * sizeof(float)); Z(b->velh, 3 * G * sizeof(float)); Z(b->tempown, G * sizeof(float));
     Z(b->dcnt, (size_t)nspecies * 4 * G * sizeof(uint32_t)); Z(b->pop, G * sizeof(int));
@@ -635,6 +644,8 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     ok = ok && cudaMemsetAsync(P.cell, 0xff, S * sizeof(int32_t), s0) == cudaSuccess;
     ok = ok && cudaStreamSynchronize(s0) == cudaSuccess;
     if (!ok) { b->err = "pi_batch_create: device initialisation failed"; return bail(PI_ERR_CUDA); }
+    cudaFuncSetAttribute(k32_xy<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xy_smem(8));
+    cudaFuncSetAttribute(k32_xy<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xy_smem(4));
     b->T.md = b->md; b->T.nsp = nspecies; b->T.tiles = b->tiles; b->T.ntiles = b->ntiles; b->T.seg_tile0 = b->seg_tile0;
     st = build_tables(b);
     if (st) return bail(st);
@@ -1221,12 +1232,8 @@ pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t k, char* report, siz
         { "k32_physiology", &t.bs_phys, {128, 256, 512, 1024}, "physiology block", 1 },
         { "k32_physiology", &t.persist_phys, {0, 2, 4, 8}, "physiology blocks/SM (0 = one tile per block)", 0 },
         { "k32_assign", &t.bs_assign, {128, 256, 512, 1024}, "assign block", 1 },
-        { "k32_sweep_x", &t.wpb_x, {2, 4, 8}, "sweep_x warps/block", 32 },
-        { "k32_sweep_y", &t.Ly, {4, 8, 16, 32}, "sweep_y rows per warp", 0 },
-        { "k32_sweep_y", &t.wpb_y, {2, 4, 8}, "sweep_y warps/block", 32 },
-        { "k32_sweep_z", &t.Lz, {4, 8, 16, 32}, "sweep_z levels per warp", 0 },
-        { "k32_sweep_z", &t.wpb_z, {2, 4, 8}, "sweep_z warps/block", 32 },
-        { "k32_tail", &t.wpb_tail, {2, 4, 8}, "tail warps/block", 32 },
+        { "k32_xy", &t.ty, {4, 8}, "x-y tracer tile rows", 0 },
+        { "k32_ztail", &t.lz, {8, 16, 32}, "z levels per thread", 0 },
         { "k32_par", &t.wpb_par, {1, 2, 4, 8}, "par warps/block", 32 },
     };
     // the largest block each kernel can be launched with (registers per thread)
@@ -1236,10 +1243,6 @@ pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t k, char* report, siz
         if (!strcmp(kernel, "k32_move")) f = (const void*)k32_move;
         else if (!strcmp(kernel, "k32_physiology")) f = (const void*)k32_physiology;
         else if (!strcmp(kernel, "k32_assign")) f = (const void*)k32_assign;
-        else if (!strcmp(kernel, "k32_sweep_x")) f = (const void*)k32_sweep_x;
-        else if (!strcmp(kernel, "k32_sweep_y")) f = (const void*)k32_sweep_y;
-        else if (!strcmp(kernel, "k32_sweep_z")) f = (const void*)k32_sweep_z;
-        else if (!strcmp(kernel, "k32_tail")) f = (const void*)k32_tail;
         else if (!strcmp(kernel, "k32_par")) f = (const void*)k32_par;
         if (!f || cudaFuncGetAttributes(&fa, f) != cudaSuccess) return 256;
         return fa.maxThreadsPerBlock;

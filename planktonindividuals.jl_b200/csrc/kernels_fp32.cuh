@@ -28,12 +28,7 @@ struct Tab32 {
     const int2* tiles;        // {segment = member*nsp + species, first slot}, F32_TILE slots each
     int ntiles;
     const int* seg_tile0;     // first tile of each segment (nseg + 1 entries)
-    const int4* ix; int nix;  // x sweep warps {m, j, k, i0}: 31 cells from i0
-    const int4* iy; int niy;  // y sweep warps {m, i0, j0, k}: 32 columns × Ly rows
-    const int4* iz; int niz;  // z sweep warps {m, i0, j, k0}: 32 columns × Lz levels
-    const int4* ic; int nic;  // cell-row warps {m, i0, j, k}: 32 cells from i0
     const int4* icol; int nicol;  // column warps {m, i0, j, 0}
-    int Ly, Lz;
 };
 
 __device__ __forceinline__ int gid3(const MemberDev& m, int i, int j, int k) {   // 1-based, member-local
@@ -116,11 +111,17 @@ __device__ __forceinline__ int clampi(int v, int lo, int hi, uint32_t* err) {
     return v;
 }
 
+// The 8 corner values of one velocity component around a position. The four RK stages of a step
+// sample points a small fraction of a cell apart, usually from the same field (vel₀ = vel½ = vel₁
+// between velocity refreshes), so a stage reuses the corners of the previous one when the field
+// and the base corner are the same: the values are identical, only the loads are saved.
+struct Corners { const float* f; int q; float v[8]; };
+
 // trilinear interpolation of one velocity component (member-local field pointer)
 template <int COMP>
 __device__ __forceinline__ float itpl32(const MemberDev& m, const float* __restrict__ f,
                                         const float* __restrict__ dzC, const Ax1& X, const Ax1& Y,
-                                        const Ax1& Z, uint32_t* err) {
+                                        const Ax1& Z, uint32_t* err, Corners& cc) {
     int i, j, k;
     float xd, yd, zd;
     axis_iw(X, m.Hx, COMP == 0, i, xd);
@@ -128,10 +129,16 @@ __device__ __forceinline__ float itpl32(const MemberDev& m, const float* __restr
     axis_iw(Z, m.Hz, COMP == 2, k, zd);
     i = clampi(i, 1, m.Gx - 1, err); j = clampi(j, 1, m.Gy - 1, err); k = clampi(k, 1, m.Gz - 1, err);
     const int q = gid3(m, i, j, k);
-    const int sy = m.Gx, sz = m.Gx * m.Gy;
+    if (cc.f != f || cc.q != q) {
+        const int sy = m.Gx, sz = m.Gx * m.Gy;
+        cc.f = f; cc.q = q;
+        cc.v[0] = __ldg(f + q); cc.v[1] = __ldg(f + q + sy); cc.v[2] = __ldg(f + q + 1); cc.v[3] = __ldg(f + q + 1 + sy);
+        cc.v[4] = __ldg(f + q + sz); cc.v[5] = __ldg(f + q + sy + sz); cc.v[6] = __ldg(f + q + 1 + sz);
+        cc.v[7] = __ldg(f + q + 1 + sy + sz);
+    }
     const float a0 = (1.0f - xd) * (1.0f - yd), a1 = (1.0f - xd) * yd, a2 = xd * (1.0f - yd), a3 = xd * yd;
-    const float lo = a0 * __ldg(f + q) + a1 * __ldg(f + q + sy) + a2 * __ldg(f + q + 1) + a3 * __ldg(f + q + 1 + sy);
-    const float hi = a0 * __ldg(f + q + sz) + a1 * __ldg(f + q + sy + sz) + a2 * __ldg(f + q + 1 + sz) + a3 * __ldg(f + q + 1 + sy + sz);
+    const float lo = a0 * cc.v[0] + a1 * cc.v[1] + a2 * cc.v[2] + a3 * cc.v[3];
+    const float hi = a0 * cc.v[4] + a1 * cc.v[5] + a2 * cc.v[6] + a3 * cc.v[7];
     if (COMP == 0) return ((1.0f - zd) * lo + zd * hi) / m.dx;
     if (COMP == 1) return ((1.0f - zd) * lo + zd * hi) / m.dy;
     return (1.0f - zd) * lo / dzC[m.dz_off + k - 1] + zd * hi / dzC[m.dz_off + k];
@@ -160,39 +167,42 @@ __device__ __forceinline__ void add_fixed(unsigned long long* a, float v, double
 
 // update!'s forcing selection (Simulation/update.jl:14-26) for members with device-resident
 // series, from model.t before the step (or the step index of the call with time_offset), and the
-// choice of the vel½ buffer. One block per member.
+// choice of the vel½ buffer. Grid: (x blocks, members); block x = 0 binds the fields, every block
+// copies its share of the surface PAR snapshot.
+__device__ __forceinline__ long long snap_index(double tm, double tc, int use_call, double dT_s, long long n,
+                                                uint32_t* err, bool flag) {
+    long long t = (long long)floor((use_call ? tc : tm) / dT_s);
+    if (t < 0 || t >= n) { if (flag) seterr(err, F32_ERR_FORCING); t = t < 0 ? 0 : n - 1; }
+    return t;
+}
+
 __global__ void k32_bind(int nm, const MemberDev* __restrict__ md, const MemberSeries* __restrict__ S,
                          MemberForcing* __restrict__ F, const StepState* __restrict__ st, double dT,
                          float* __restrict__ PARF, uint32_t* err) {
-    const int m = blockIdx.x;
+    const int m = blockIdx.y;
     if (m >= nm || stopped(err)) return;
     const MemberSeries& s = S[m];
     const MemberDev& M = md[m];
-    __shared__ long long tp_sh;
-    if (threadIdx.x == 0) {
+    const double tm = st->t, tc = (double)st->call_step * dT;
+    const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+    if (lead) {
         MemberForcing f = F[m];
         if (s.has_series) {
-            const double tm = st->t, tc = (double)st->call_step * dT;
             if (s.has_vel) {
-                long long tv = (long long)floor(((s.time_offset & 1) ? tc : tm) / s.dT_vel);
-                if (tv < 0 || tv >= s.nvel) { seterr(err, F32_ERR_FORCING); tv = tv < 0 ? 0 : s.nvel - 1; }
+                const long long tv = snap_index(tm, tc, s.time_offset & 1, s.dT_vel, s.nvel, err, true);
                 for (int c = 0; c < 3; ++c) f.vel1[c] = s.vel + (tv * 3 + c) * M.G;
             }
-            long long tt = (long long)floor(((s.time_offset & 4) ? tc : tm) / s.dT_temp);
-            if (tt < 0 || tt >= s.ntemp) { seterr(err, F32_ERR_FORCING); tt = tt < 0 ? 0 : s.ntemp - 1; }
-            f.temp = s.temp + tt * M.G;
-            long long tp = (long long)floor(((s.time_offset & 2) ? tc : tm) / s.dT_PAR);
-            if (tp < 0 || tp >= s.npar) { seterr(err, F32_ERR_FORCING); tp = tp < 0 ? 0 : s.npar - 1; }
-            tp_sh = tp;
+            f.temp = s.temp + snap_index(tm, tc, s.time_offset & 4, s.dT_temp, s.ntemp, err, true) * M.G;
         }
         for (int c = 0; c < 3; ++c) f.velh[c] = (f.vel0[c] == f.vel1[c]) ? f.vel1[c] : s.velh_buf[c];
         F[m] = f;
     }
-    __syncthreads();
     if (!s.has_series) return;
+    const long long tp = snap_index(tm, tc, s.time_offset & 2, s.dT_PAR, s.npar, err, lead);
     const long long n = (long long)M.Nx * M.Ny;
-    const float* src = s.parf + tp_sh * n;
-    for (long long q = threadIdx.x; q < n; q += blockDim.x) PARF[M.col_off + q] = src[q];
+    const float* src = s.parf + tp * n;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        PARF[M.col_off + q] = src[q];
 }
 
 // vel½ = (vel₀ + vel₁) * 0.5 (time_step.jl:17-19) for members whose two fields differ.
@@ -264,24 +274,25 @@ __device__ __forceinline__ void move_one(const MoveArgs& a, const MemberDev& m, 
     const Ax1 X0{ci, P.ox[g]}, Y0{cj, P.oy[g]}, Z0{ck, P.oz[g]};
     const float dT = a.dT;
     const float* dzC = a.dzC;
-    float u1 = itpl32<0>(m, f.vel0[0], dzC, X0, Y0, Z0, err);
-    float v1 = itpl32<1>(m, f.vel0[1], dzC, X0, Y0, Z0, err);
-    float w1 = itpl32<2>(m, f.vel0[2], dzC, X0, Y0, Z0, err);
+    Corners cu{nullptr, -1, {}}, cv{nullptr, -1, {}}, cw{nullptr, -1, {}};
+    float u1 = itpl32<0>(m, f.vel0[0], dzC, X0, Y0, Z0, err, cu);
+    float v1 = itpl32<1>(m, f.vel0[1], dzC, X0, Y0, Z0, err, cv);
+    float w1 = itpl32<2>(m, f.vel0[2], dzC, X0, Y0, Z0, err, cw);
     float u2 = u1, v2 = v1, w2 = w1;
     Ax1 X = X0, Y = Y0, Z = Z0;
     move(X, 0.5f * u1 * dT, m.Nx, m.tx); move(Y, 0.5f * v1 * dT, m.Ny, m.ty); move(Z, -(0.5f * w1 * dT), m.Nz, m.tz);
-    u1 = itpl32<0>(m, f.velh[0], dzC, X, Y, Z, err); v1 = itpl32<1>(m, f.velh[1], dzC, X, Y, Z, err);
-    w1 = itpl32<2>(m, f.velh[2], dzC, X, Y, Z, err);
+    u1 = itpl32<0>(m, f.velh[0], dzC, X, Y, Z, err, cu); v1 = itpl32<1>(m, f.velh[1], dzC, X, Y, Z, err, cv);
+    w1 = itpl32<2>(m, f.velh[2], dzC, X, Y, Z, err, cw);
     u2 += u1 * 2.0f; v2 += v1 * 2.0f; w2 += w1 * 2.0f;
     X = X0; Y = Y0; Z = Z0;
     move(X, 0.5f * u1 * dT, m.Nx, m.tx); move(Y, 0.5f * v1 * dT, m.Ny, m.ty); move(Z, -(0.5f * w1 * dT), m.Nz, m.tz);
-    u1 = itpl32<0>(m, f.velh[0], dzC, X, Y, Z, err); v1 = itpl32<1>(m, f.velh[1], dzC, X, Y, Z, err);
-    w1 = itpl32<2>(m, f.velh[2], dzC, X, Y, Z, err);
+    u1 = itpl32<0>(m, f.velh[0], dzC, X, Y, Z, err, cu); v1 = itpl32<1>(m, f.velh[1], dzC, X, Y, Z, err, cv);
+    w1 = itpl32<2>(m, f.velh[2], dzC, X, Y, Z, err, cw);
     u2 += u1 * 2.0f; v2 += v1 * 2.0f; w2 += w1 * 2.0f;
     X = X0; Y = Y0; Z = Z0;
     move(X, u1 * dT, m.Nx, m.tx); move(Y, v1 * dT, m.Ny, m.ty); move(Z, -(w1 * dT), m.Nz, m.tz);
-    u1 = itpl32<0>(m, f.vel1[0], dzC, X, Y, Z, err); v1 = itpl32<1>(m, f.vel1[1], dzC, X, Y, Z, err);
-    w1 = itpl32<2>(m, f.vel1[2], dzC, X, Y, Z, err);
+    u1 = itpl32<0>(m, f.vel1[0], dzC, X, Y, Z, err, cu); v1 = itpl32<1>(m, f.vel1[1], dzC, X, Y, Z, err, cv);
+    w1 = itpl32<2>(m, f.vel1[2], dzC, X, Y, Z, err, cw);
     u2 = (u2 + u1) / 6.0f; v2 = (v2 + v1) / 6.0f; w2 = (w2 + w1) / 6.0f;
     X = X0; Y = Y0; Z = Z0;
     move(X, u2 * dT, m.Nx, m.tx); move(Y, v2 * dT, m.Ny, m.ty); move(Z, -(w2 * dT), m.Nz, m.tz);
@@ -645,219 +656,73 @@ __global__ void k32_physiology(PhysArgs a) {
 }
 
 // ------------------------------------------------------------------------------------------
-// (d) tracer update in Float32: DST3FL sweeps (DST3FL.jl:1-73, multi_dim_adv.jl:1-135), then
-//     diffusion, sinking, forcing, flux BCs, particle terms and apply_tendency!
+// (d) tracer update in Float32: the three DST3FL sweeps (DST3FL.jl:1-73, multi_dim_adv.jl:1-135)
+//     and the rest of tracer_update! (tracer_update.jl:22-43) in two kernels: k32_xy (x and y
+//     sweeps of a level tile staged in shared memory) and k32_ztail (z sweep walking columns, then
+//     diffusion, sinking, forcing, boundary fluxes, particle terms and apply_tendency!). Both
+//     handle all 14 tracers per thread, so face coefficients and indices are formed once per face.
+//
+// The flux limiter is evaluated without forming θ: for the upwind side,
+//   ψ(δ/δ⁰)·δ⁰ = max(0, min(δ⁰, d₀δ⁰ + d₁δ, Rδ)) for δ⁰ ≥ 0 and min(0, max(δ⁰, d₀δ⁰ + d₁δ, Rδ))
+//   for δ⁰ < 0, R = (1 − cfl)/(cfl + 1e-20),
+// which equals ψ(θ)·δ⁰ (the θmax cap never changes ψ) and needs no division by δ⁰, so gradients
+// near zero are exact. The downwind term of the reference multiplies a zero transport and is
+// dropped.
 // ------------------------------------------------------------------------------------------
-struct FC32 { float d0c, d1c, omc, cpe, hp, hm; };
-__device__ __forceinline__ FC32 fc32(float vel, float area, float dxc, float dT) {
-    FC32 f;
-    const float cfl = fabsf(vel * dT / dxc);
-    const float tr = area * vel;
-    f.d0c = (2.0f - cfl) * (1.0f - cfl) / 6.0f;
-    f.d1c = (1.0f - cfl * cfl) / 6.0f;
-    f.omc = 1.0f - cfl;
-    f.cpe = cfl + EPS20_F;
-    f.hp = 0.5f * (tr + fabsf(tr));
-    f.hm = 0.5f * (tr - fabsf(tr));
+struct FCu { float tr, d0c, d1c, R; };
+
+__device__ __forceinline__ FCu fcu(float vel, float area, float rdxc, float dT) {
+    FCu f;
+    const float cfl = fabsf(vel * dT * rdxc);
+    f.tr = area * vel;
+    f.d0c = (2.0f - cfl) * (1.0f - cfl) * (1.0f / 6.0f);
+    f.d1c = (1.0f - cfl * cfl) * (1.0f / 6.0f);
+    f.R = __fdividef(1.0f - cfl, cfl + EPS20_F);
     return f;
 }
-// θ = δ⁻/δ⁰ limited at ±θmax (DST3FL.jl:2). Where δ⁰ is within 2^-22 of the values it was taken
-// from (a gradient near zero), the ratio, the limit test and the sign are formed in FP64.
-__device__ __forceinline__ float theta_f(float dn, float d0, float scale) {
-    if (fabsf(d0) <= scale * 0x1p-22f) {
-        const double D0 = d0, DN = dn;
-        const double th = fabs(D0) * 1.0e20 <= fabs(DN) ? copysign(1.0e20, DN * D0) : DN / D0;
-        return (float)th;
+__device__ __forceinline__ float psid0(float d0, float dn, const FCu& f) {
+    const float a = f.d0c * d0 + f.d1c * dn, b = f.R * dn;
+    return d0 >= 0.0f ? fmaxf(0.0f, fminf(fminf(d0, a), b)) : fminf(0.0f, fmaxf(fmaxf(d0, a), b));
+}
+// adv_flux_x / adv_flux_y at a face from c[f-2], c[f-1], c[f], c[f+1] and the landmask there
+__device__ __forceinline__ float flux_h(const FCu& f, float cm2, float cm1, float c0, float cp1,
+                                        int lm2, int lm1, int l0, int lp1) {
+    if (f.tr > 0.0f) {
+        const float d0 = mulbf(mulbf(c0 - cm1, l0), lm1), dm = mulbf(mulbf(cm1 - cm2, lm1), lm2);
+        return f.tr * (cm1 + psid0(d0, dm, f));
     }
-    return fabsf(d0) * THMAX_F <= fabsf(dn) ? copysignf(THMAX_F, dn * d0) : dn / d0;
+    if (f.tr < 0.0f) {
+        const float d0 = mulbf(mulbf(c0 - cm1, l0), lm1), dp = mulbf(mulbf(cp1 - c0, lp1), l0);
+        return f.tr * (c0 - psid0(d0, dp, f));
+    }
+    return 0.0f;
 }
-__device__ __forceinline__ float psi_f(const FC32& f, float th) {
-    return fmaxf(0.0f, fminf(fminf(1.0f, f.d0c + f.d1c * th), th * f.omc / f.cpe));
-}
-__device__ __forceinline__ float fxy32(const FC32& f, float cm2, float cm1, float c0, float cp1,
-                                       int lm2, int lm1, int l0, int lp1) {
-    const float d0 = mulbf(mulbf(c0 - cm1, l0), lm1), dm = mulbf(mulbf(cm1 - cm2, lm1), lm2);
-    const float dp = mulbf(mulbf(cp1 - c0, lp1), l0);
-    const float sc = fmaxf(fabsf(c0), fabsf(cm1));
-    return f.hp * (cm1 + psi_f(f, theta_f(dm, d0, sc)) * d0) + f.hm * (c0 - psi_f(f, theta_f(dp, d0, sc)) * d0);
-}
-__device__ __forceinline__ float fz32(const FC32& f, float cm2, float cm1, float c0, float cp1,
-                                      int lm2, int lm1, int l0, int lp1) {
-    const float d0 = mulbf(mulbf(cm1 - c0, l0), lm1), dm = mulbf(mulbf(cm2 - cm1, lm1), lm2);
-    const float dp = mulbf(mulbf(c0 - cp1, lp1), l0);
-    const float sc = fmaxf(fabsf(c0), fabsf(cm1));
-    return f.hp * (c0 + psi_f(f, theta_f(dp, d0, sc)) * d0) + f.hm * (cm1 - psi_f(f, theta_f(dm, d0, sc)) * d0);
+// adv_flux_z at face k from c[k-2], c[k-1], c[k], c[k+1] (the index grows downward)
+__device__ __forceinline__ float flux_v(const FCu& f, float cm2, float cm1, float c0, float cp1,
+                                        int lm2, int lm1, int l0, int lp1) {
+    if (f.tr > 0.0f) {
+        const float d0 = mulbf(mulbf(cm1 - c0, l0), lm1), dp = mulbf(mulbf(c0 - cp1, lp1), l0);
+        return f.tr * (c0 + psid0(d0, dp, f));
+    }
+    if (f.tr < 0.0f) {
+        const float d0 = mulbf(mulbf(cm1 - c0, l0), lm1), dm = mulbf(mulbf(cm2 - cm1, lm1), lm2);
+        return f.tr * (cm1 - psid0(d0, dm, f));
+    }
+    return 0.0f;
 }
 __device__ __forceinline__ int wrap_ax(int a, int N, int H, int topo) {
     if (topo == PI_PERIODIC) { while (a < H + 1) a += N; while (a > N + H) a -= N; return a; }
     return a < H + 1 ? H + 1 : (a > N + H ? N + H : a);
 }
 
-struct SweepArgs {
-    Tab32 T;
-    const uint8_t* lm;
-    const float* dzF;
-    const float* dzC;
-    const MemberForcing* F;
-    long long Gtot;
-    const float* tr;       // tracers at the start of the step
-    const float* src;      // input of this sweep
-    float* dst;            // output of this sweep
-    float dT;
-    const uint32_t* err;
-};
-
-// x sweep: each warp owns 31 cells of one row and 32 faces; the east flux of a cell is the next
-// lane's west flux. The face after the last cell is the periodic image of face H+1, or zero.
-__global__ void k32_sweep_x(SweepArgs a) {
-    if (stopped(a.err)) return;
-    const int lane = threadIdx.x & 31;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < a.T.nix; w += nw) {
-        const int4 it = a.T.ix[w];
-        const MemberDev& m = a.T.md[it.x];
-        const int j = it.y, k = it.z, i0 = it.w;
-        const int f = i0 + lane, last = m.Nx + m.Hx;
-        const bool has_face = f <= last + 1, has_cell = lane < 31 && f <= last, special = f == last + 1;
-        const bool zero_face = !has_face || (special && m.tx != PI_PERIODIC);
-        const int fs = special ? m.Hx + 1 : f;
-        const float* u = a.F[it.x].vel1[0];
-        const float ax = m.dy * a.dzF[m.dz_off + k - 1];
-        const int qf = gid3(m, has_face ? fs : i0, j, k);
-        FC32 fc{};
-        int l2 = 1, l1 = 1, l0 = 1, lp = 1;
-        if (!zero_face) {
-            fc = fc32(u[qf], ax, m.dx, a.dT);
-            l2 = lm32(m, a.lm, fs - 2, j, k); l1 = lm32(m, a.lm, fs - 1, j, k);
-            l0 = lm32(m, a.lm, fs, j, k); lp = lm32(m, a.lm, fs + 1, j, k);
-        }
-        const int qc = gid3(m, has_cell ? f : i0, j, k);
-        float ftr = 0.0f, dtv = 0.0f;
-        int c0m = 1, cpm = 1;
-        if (has_cell) {
-            c0m = lm32(m, a.lm, f, j, k); cpm = lm32(m, a.lm, f + 1, j, k);
-            ftr = mulbf(mulbf(ax * u[qc + 1] - ax * u[qc], cpm), c0m);
-            dtv = a.dT / (m.dx * m.dy * a.dzF[m.dz_off + k - 1]);
-        }
-        const long long off = m.cell_off;
-#pragma unroll 2
-        for (int n = 0; n < PI_NTRACERS; ++n) {
-            const float* c = a.src + n * a.Gtot + off;
-            const float Fl = zero_face ? 0.0f : fxy32(fc, c[qf - 2], c[qf - 1], c[qf], c[qf + 1], l2, l1, l0, lp);
-            const float Fe = __shfl_down_sync(0xffffffffu, Fl, 1);
-            if (has_cell) {
-                const float cc = c[qc];
-                const float dG = mulbf(mulbf(Fe - Fl, cpm), c0m);
-                a.dst[n * a.Gtot + off + qc] = cc - dtv * (dG - cc * ftr);
-            }
-        }
+__device__ __forceinline__ int acc_slot(int n) {
+    switch (n) {
+        case PI_DIC: return ACC_DIC; case PI_NH4: return ACC_NH4; case PI_NO3: return ACC_NO3;
+        case PI_PO4: return ACC_PO4; case PI_DOC: return ACC_DOC; case PI_DON: return ACC_DON;
+        case PI_DOP: return ACC_DOP; case PI_POC: return ACC_POC; case PI_PON: return ACC_PON;
+        case PI_POP: return ACC_POP; default: return -1;
     }
 }
-
-// y sweep: lanes along x, each lane walks Ly rows carrying the face flux; rows outside the
-// interior are read through the map the halo fill of tracer_temp produces.
-__global__ void k32_sweep_y(SweepArgs a) {
-    if (stopped(a.err)) return;
-    const int lane = threadIdx.x & 31;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < a.T.niy; w += nw) {
-        const int4 it = a.T.iy[w];
-        const MemberDev& m = a.T.md[it.x];
-        const int i = it.y + lane, j0 = it.z, k = it.w;
-        if (i > m.Nx + m.Hx) continue;
-        const int jend = min(j0 + a.T.Ly - 1, m.Ny + m.Hy);
-        const float* v = a.F[it.x].vel1[1];
-        const float dz = a.dzF[m.dz_off + k - 1];
-        const float ay = m.dx * dz;
-        const float dtv = a.dT / (m.dx * m.dy * dz);
-        const long long off = m.cell_off;
-        auto face = [&](const float* c, int f) -> float {
-            const bool special = f == m.Ny + m.Hy + 1;
-            if (special && m.ty != PI_PERIODIC) return 0.0f;
-            const int fs = special ? m.Hy + 1 : f;
-            const FC32 fc = fc32(v[gid3(m, i, fs, k)], ay, m.dy, a.dT);
-            return fxy32(fc, c[gid3(m, i, wrap_ax(fs - 2, m.Ny, m.Hy, m.ty), k)], c[gid3(m, i, wrap_ax(fs - 1, m.Ny, m.Hy, m.ty), k)],
-                         c[gid3(m, i, wrap_ax(fs, m.Ny, m.Hy, m.ty), k)], c[gid3(m, i, wrap_ax(fs + 1, m.Ny, m.Hy, m.ty), k)],
-                         lm32(m, a.lm, i, fs - 2, k), lm32(m, a.lm, i, fs - 1, k), lm32(m, a.lm, i, fs, k), lm32(m, a.lm, i, fs + 1, k));
-        };
-#pragma unroll 1
-        for (int n = 0; n < PI_NTRACERS; ++n) {
-            const float* c = a.src + n * a.Gtot + off;
-            const float* c0 = a.tr + n * a.Gtot + off;
-            float Ft = face(c, j0);
-            for (int jj = j0; jj <= jend; ++jj) {
-                const float Fb = face(c, jj + 1);
-                const int q = gid3(m, i, jj, k);
-                const int c0m = lm32(m, a.lm, i, jj, k), cpm = lm32(m, a.lm, i, jj + 1, k);
-                const float ftr = mulbf(mulbf(ay * v[q + m.Gx] - ay * v[q], cpm), c0m);
-                const float dG = mulbf(mulbf(Fb - Ft, cpm), c0m);
-                a.dst[n * a.Gtot + off + q] = c[q] - dtv * (dG - c0[q] * ftr);
-                Ft = Fb;
-            }
-        }
-    }
-}
-
-// z sweep and calc_tracer_tendency!: writes Gc_adv = tracer_temp − tracer.
-__global__ void k32_sweep_z(SweepArgs a) {
-    if (stopped(a.err)) return;
-    const int lane = threadIdx.x & 31;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < a.T.niz; w += nw) {
-        const int4 it = a.T.iz[w];
-        const MemberDev& m = a.T.md[it.x];
-        const int i = it.y + lane, j = it.z, k0 = it.w;
-        if (i > m.Nx + m.Hx) continue;
-        const int kend = min(k0 + a.T.Lz - 1, m.Nz + m.Hz);
-        const float* wv = a.F[it.x].vel1[2];
-        const float az = m.dx * m.dy;
-        const int slab = m.Gx * m.Gy;
-        const int qcol = gid3(m, i, j, 1);
-        const long long off = m.cell_off;
-        auto face = [&](const float* c, int f) -> float {
-            if (f == m.Nz + m.Hz + 1) return 0.0f;
-            const FC32 fc = fc32(wv[qcol + (f - 1) * slab], az, a.dzC[m.dz_off + f - 1], a.dT);
-            auto lev = [&](int kk) { return qcol + (wrap_ax(kk, m.Nz, m.Hz, PI_BOUNDED) - 1) * slab; };
-            return fz32(fc, c[lev(f - 2)], c[lev(f - 1)], c[lev(f)], c[lev(f + 1)], lm32(m, a.lm, i, j, f - 2),
-                        lm32(m, a.lm, i, j, f - 1), lm32(m, a.lm, i, j, f), lm32(m, a.lm, i, j, f + 1));
-        };
-#pragma unroll 1
-        for (int n = 0; n < PI_NTRACERS; ++n) {
-            const float* c = a.src + n * a.Gtot + off;
-            const float* c0 = a.tr + n * a.Gtot + off;
-            float Ft = face(c, k0);
-            for (int k = k0; k <= kend; ++k) {
-                const float Fb = face(c, k + 1);
-                const int q = qcol + (k - 1) * slab;
-                const int c0m = lm32(m, a.lm, i, j, k), cpm = lm32(m, a.lm, i, j, k + 1);
-                const float ftr = mulbf(mulbf(az * wv[q] - az * wv[q + slab], cpm), c0m);
-                const float dG = mulbf(mulbf(Ft - Fb, cpm), c0m);
-                const float cc = c0[q];
-                const float ct = c[q] - a.dT / (m.dx * m.dy * a.dzF[m.dz_off + k - 1]) * (dG - cc * ftr);
-                a.dst[n * a.Gtot + off + q] = ct - cc;
-                Ft = Fb;
-            }
-        }
-    }
-}
-
-struct TailArgs {
-    Tab32 T;
-    const uint8_t* lm;
-    const float* dzF;
-    const float* dzC;
-    const BgcDev32* bgc;
-    const FluxBC32* bcs;   // [bc_off + tracer*6 + face]
-    const StepState* st;
-    long long Gtot;
-    const float* tr;
-    const float* gadv;
-    float* tr_next;
-    unsigned long long* acc;
-    const int* pop;
-    float dT;
-    const uint32_t* err;
-};
 
 __device__ __forceinline__ float getbc32(const FluxBC32& b, int a, int c, int64_t it) {
     if (b.kind == PI_BC_CONST) return b.v[0];
@@ -866,112 +731,273 @@ __device__ __forceinline__ float getbc32(const FluxBC32& b, int a, int c, int64_
     return b.v[(a - 1) + (long long)b.n1 * ((c - 1) + (long long)b.n2 * (t - 1))];
 }
 
-__global__ void k32_tail(TailArgs a) {
+struct TrArgs {
+    Tab32 T;
+    const int4* items;          // k32_xy: {member, i0, j0, level}; k32_ztail: {member, i0, j, k0}
+    int nitems;
+    const uint8_t* lm;
+    const float* dzF;
+    const float* dzC;
+    const float* rdzC;          // 1 / dzC
+    const BgcDev32* bgc;
+    const FluxBC32* bcs;
+    const StepState* st;
+    const MemberForcing* F;
+    long long Gtot;
+    const float* tr;            // tracers at the start of the step
+    float* tb;                  // tracer_temp after the x and y sweeps
+    float* tr_next;
+    unsigned long long* acc;
+    const int* pop;
+    float dT;
+    const uint32_t* err;
+};
+
+// x and y sweeps of all 14 tracers on one level of a tile of 28 columns × TY rows. Warp w holds
+// row j0-2+w (TY+4 rows: the y sweep reads two rows on each side, outside the domain through the
+// halo-fill map), lane l column i0-2+l (28 cells and two halo columns on each side, exchanged by
+// shuffles). The face coefficients are computed once per face and shared by the 14 tracers.
+// Shared memory [row][tracer][lane]: TA (after x), FY (y face fluxes), TRs (tracer of the rows
+// the y sweep updates).
+template <int TY>
+__global__ void __launch_bounds__(32 * (TY + 4)) k32_xy(TrArgs a) {
+    if (stopped(a.err)) return;
+    extern __shared__ float sm[];
+    float* TA = sm;                                        // (TY+4) × 14 × 32
+    float* FY = TA + (TY + 4) * PI_NTRACERS * 32;          // (TY+1) × 14 × 32
+    float* TRs = FY + (TY + 1) * PI_NTRACERS * 32;         // TY × 14 × 32
+    auto at = [](float* base, int r, int n, int l) -> float& { return base[(r * PI_NTRACERS + n) * 32 + l]; };
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const long long G = a.Gtot;
+    const float dT = a.dT;
+    for (int item = blockIdx.x; item < a.nitems; item += gridDim.x) {
+        const int4 it = a.items[item];
+        const MemberDev& m = a.T.md[it.x];
+        const int i0 = it.y, j0 = it.z, L = it.w;
+        const long long off = m.cell_off;
+        const MemberForcing& F = a.F[it.x];
+        const float dz = a.dzF[m.dz_off + L - 1];
+        const float az = m.dx * m.dy, dtv = dT / (az * dz);
+        // ---- x sweep of row j0-2+wid
+        {
+            const int jj = wrap_ax(j0 - 2 + wid, m.Ny, m.Hy, m.ty);
+            const int i = i0 - 2 + lane;
+            const int ic = min(i, m.Gx);
+            const float ax = m.dy * dz;
+            const float* u = F.vel1[0];
+            const int q = gid3(m, ic, jj, L);
+            const float uw = u[q];
+            const float ue = __shfl_down_sync(0xffffffffu, uw, 1);
+            const FCu fc = fcu(uw, ax, 1.0f / m.dx, dT);
+            const int l0 = lm32(m, a.lm, ic, jj, L);
+            const int lm1 = __shfl_up_sync(0xffffffffu, l0, 1), lm2 = __shfl_up_sync(0xffffffffu, l0, 2);
+            const int lp1 = __shfl_down_sync(0xffffffffu, l0, 1);
+            const bool east_zero = i == m.Nx + m.Hx && m.tx != PI_PERIODIC;   // fill_halo_east_Gc! (Bounded)
+            const float ftr = mulbf(mulbf(ax * ue - ax * uw, lp1), l0);
+            const bool store_tr = wid >= 2 && wid < TY + 2;
+#pragma unroll
+            for (int n = 0; n < PI_NTRACERS; ++n) {
+                const float v = a.tr[n * G + off + q];
+                const float cm2 = __shfl_up_sync(0xffffffffu, v, 2), cm1 = __shfl_up_sync(0xffffffffu, v, 1);
+                const float cp1 = __shfl_down_sync(0xffffffffu, v, 1);
+                const float Fw = flux_h(fc, cm2, cm1, v, cp1, lm2, lm1, l0, lp1);
+                float Fe = __shfl_down_sync(0xffffffffu, Fw, 1);
+                if (east_zero) Fe = 0.0f;
+                const float dG = mulbf(mulbf(Fe - Fw, lp1), l0);
+                at(TA, wid, n, lane) = v - dtv * (dG - v * ftr);
+                if (store_tr) at(TRs, wid - 2, n, lane) = v;
+            }
+        }
+        __syncthreads();
+        // ---- y faces j0 + r, r = 0..TY
+        const int i = i0 - 2 + lane;
+        const bool col = lane >= 2 && lane < 30 && i <= m.Nx + m.Hx;
+        const float ay = m.dx * dz;
+        const float* vv = F.vel1[1];
+        if (wid <= TY) {
+            const int r = wid, f = j0 + r;
+            const bool special = f == m.Ny + m.Hy + 1;
+            const bool zero = !col || f > m.Ny + m.Hy + 1 || (special && m.ty != PI_PERIODIC);
+            const int fs = special ? m.Hy + 1 : min(f, m.Ny + m.Hy);
+            const int ic = min(i, m.Gx);
+            const FCu fc = fcu(zero ? 0.0f : vv[gid3(m, ic, fs, L)], ay, 1.0f / m.dy, dT);
+            const int L2 = lm32(m, a.lm, ic, fs - 2, L), L1 = lm32(m, a.lm, ic, fs - 1, L);
+            const int L0 = lm32(m, a.lm, ic, fs, L), Lp = lm32(m, a.lm, ic, fs + 1, L);
+#pragma unroll
+            for (int n = 0; n < PI_NTRACERS; ++n)
+                at(FY, r, n, lane) = zero ? 0.0f : flux_h(fc, at(TA, r, n, lane), at(TA, r + 1, n, lane), at(TA, r + 2, n, lane),
+                                                          at(TA, r + 3, n, lane), L2, L1, L0, Lp);
+        }
+        __syncthreads();
+        // ---- y update of row j0 + wid
+        if (wid < TY) {
+            const int j = j0 + wid;
+            if (col && j <= m.Ny + m.Hy) {
+                const int q = gid3(m, i, j, L);
+                const int c0m = lm32(m, a.lm, i, j, L), cpm = lm32(m, a.lm, i, j + 1, L);
+                const float ftr = mulbf(mulbf(ay * vv[q + m.Gx] - ay * vv[q], cpm), c0m);
+#pragma unroll
+                for (int n = 0; n < PI_NTRACERS; ++n) {
+                    const float dG = mulbf(mulbf(at(FY, wid + 1, n, lane) - at(FY, wid, n, lane), cpm), c0m);
+                    a.tb[n * G + off + q] = at(TA, wid + 2, n, lane) - dtv * (dG - at(TRs, wid, n, lane) * ftr);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// z sweep of all 14 tracers and the rest of tracer_update! for LZ levels of 32 columns: each
+// thread walks its column keeping, per tracer, the 4-level stencil window of tracer_temp and the
+// flux of the face above the current cell.
+template <int LZ>
+__global__ void __launch_bounds__(128) k32_ztail(TrArgs a) {
     if (stopped(a.err)) return;
     const int lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < a.T.nic; w += nw) {
-        const int4 it = a.T.ic[w];
+    const long long G = a.Gtot;
+    const float dT = a.dT;
+    const int64_t itn = a.st->iteration + 1;
+    for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < a.nitems; w += nw) {
+        const int4 it = a.items[w];
         const MemberDev& m = a.T.md[it.x];
-        const int i = it.y + lane, j = it.z, k = it.w;
+        const int i = it.y + lane, j = it.z, k0 = it.w;
         if (i > m.Nx + m.Hx) continue;
-        const long long G = a.Gtot, off = m.cell_off;
-        const int q = gid3(m, i, j, k);
-        const long long cq = off + q;
-        const float dT = a.dT;
-        const float dz = a.dzF[m.dz_off + k - 1];
-        const float volk = m.dx * m.dy * dz;
-        const float az = m.dx * m.dy;
+        const int top = m.Hz + 1, bot = m.Nz + m.Hz;
+        const int kend = min(k0 + LZ - 1, bot);
+        const long long off = m.cell_off;
         const int slab = m.Gx * m.Gy;
+        const int qcol = gid3(m, i, j, 1);
+        const float* wv = a.F[it.x].vel1[2];
         const BgcDev32& b = a.bgc[it.x];
-        float Gc[PI_NTRACERS];
-#pragma unroll
-        for (int n = 0; n < PI_NTRACERS; ++n) Gc[n] = a.gadv[n * G + cq];
-        // tracer_diffusion! (tracer_diffusion.jl:1-21)
-        if (b.kappa_h != 0.0f || b.kappa_v != 0.0f) {
-            const float axk = m.dy * dz, ayk = m.dx * dz;
-            const int li = lm32(m, a.lm, i, j, k);
-            for (int n = 0; n < PI_NTRACERS; ++n) {
-                const float* c = a.tr + n * G + off;
-                auto dx0 = [&](int ii) { return mulbf(mulbf(c[gid3(m, ii, j, k)] - c[gid3(m, ii - 1, j, k)], lm32(m, a.lm, ii, j, k)), lm32(m, a.lm, ii - 1, j, k)); };
-                auto dy0 = [&](int jj) { return mulbf(mulbf(c[gid3(m, i, jj, k)] - c[gid3(m, i, jj - 1, k)], lm32(m, a.lm, i, jj, k)), lm32(m, a.lm, i, jj - 1, k)); };
-                auto dz0 = [&](int kk) { return mulbf(mulbf(c[gid3(m, i, j, kk - 1)] - c[gid3(m, i, j, kk)], lm32(m, a.lm, i, j, kk)), lm32(m, a.lm, i, j, kk - 1)); };
-                const float fx1 = b.kappa_h * axk * (dx0(i + 1) / m.dx), fx0 = b.kappa_h * axk * (dx0(i) / m.dx);
-                const float fy1 = b.kappa_h * ayk * (dy0(j + 1) / m.dy), fy0 = b.kappa_h * ayk * (dy0(j) / m.dy);
-                const float fz0 = b.kappa_v * az * (dz0(k) / dz), fz1 = b.kappa_v * az * (dz0(k + 1) / a.dzF[m.dz_off + k]);
-                const float ax_ = mulbf(mulbf(fx1 - fx0, lm32(m, a.lm, i + 1, j, k)), li);
-                const float ay_ = mulbf(mulbf(fy1 - fy0, lm32(m, a.lm, i, j + 1, k)), li);
-                const float az_ = mulbf(mulbf(fz0 - fz1, lm32(m, a.lm, i, j, k + 1)), li);
-                Gc[n] = Gc[n] + 1.0f / volk * (ax_ + ay_ + az_) * dT;
-            }
-        }
-        // tracer_sinking! (tracer_sinking.jl:1-42)
+        const float az = m.dx * m.dy;
+        const bool diffuse = b.kappa_h != 0.0f || b.kappa_v != 0.0f;
+        auto lev = [&](int kk) { return qcol + (min(max(kk, top), bot) - 1) * slab; };
+        float win[PI_NTRACERS][4], Ft[PI_NTRACERS];
+        float wtop = wv[qcol + (k0 - 1) * slab];
         {
-            auto sink = [&](int n, float ws) {
-                const float* c = a.tr + n * G + off;
-                const float fup = (k - 1 <= m.Hz || k - 1 >= m.Nz + m.Hz) ? 0.0f : ws * c[q - slab];
-                const float fdn = (k >= m.Nz + m.Hz) ? 0.0f : ws * c[q];
-                return (fup - fdn) / a.dzC[m.dz_off + k - m.Hz - 1] * dT;
-            };
-            Gc[PI_PFe_inorg] += sink(PI_PFe_inorg, b.w_sink_inorg);
-            Gc[PI_Dust] += sink(PI_Dust, b.w_sink_inorg);
-            Gc[PI_PFe_bio] += sink(PI_PFe_bio, b.w_sink_org);
-        }
-        // tracer_forcing! (tracer_forcings.jl:2-50) on max(0, tracer)
-        {
-            float Tt[PI_NTRACERS];
+            const FCu fc = fcu(wtop, az, a.rdzC[m.dz_off + k0 - 1], dT);
+            const int l2 = lm32(m, a.lm, i, j, k0 - 2), l1 = lm32(m, a.lm, i, j, k0 - 1);
+            const int l0 = lm32(m, a.lm, i, j, k0), lp = lm32(m, a.lm, i, j, k0 + 1);
 #pragma unroll
-            for (int n = 0; n < PI_NTRACERS; ++n) Tt[n] = fmaxf(0.0f, a.tr[n * G + cq]);
-            Gc[PI_DIC] = Gc[PI_DIC] + Tt[PI_DOC] * b.kDOC * dT;
-            Gc[PI_DOC] = Gc[PI_DOC] - Tt[PI_DOC] * b.kDOC * dT + Tt[PI_POC] * b.kPOC * dT;
-            Gc[PI_POC] = Gc[PI_POC] - Tt[PI_POC] * b.kPOC * dT;
-            Gc[PI_NH4] = Gc[PI_NH4] + Tt[PI_DON] * b.kDON * dT - Tt[PI_NH4] * b.Nit * dT;
-            Gc[PI_NO3] = Gc[PI_NO3] + Tt[PI_NH4] * b.Nit * dT;
-            Gc[PI_DON] = Gc[PI_DON] - Tt[PI_DON] * b.kDON * dT + Tt[PI_PON] * b.kPON * dT;
-            Gc[PI_PON] = Gc[PI_PON] - Tt[PI_PON] * b.kPON * dT;
-            Gc[PI_PO4] = Gc[PI_PO4] + Tt[PI_DOP] * b.kDOP * dT;
-            Gc[PI_DOP] = Gc[PI_DOP] - Tt[PI_DOP] * b.kDOP * dT + Tt[PI_POP] * b.kPOP * dT;
-            Gc[PI_POP] = Gc[PI_POP] - Tt[PI_POP] * b.kPOP * dT;
-            const float fe = fmaxf(Tt[PI_DFe] - b.ligand, 0.0f) * Tt[PI_DFe] * b.DFeFrac * b.lambda_Fe * dT;
-            Gc[PI_DFe] = Gc[PI_DFe] + Tt[PI_PFe_bio] * b.kPOC * dT
-                       - (b.lambda_POC * Tt[PI_POC] + b.lambda_min + b.lambda_dust * Tt[PI_Dust]) * Tt[PI_DFe] * b.DFeFrac * dT
-                       + Tt[PI_PFe_inorg] * b.kdiss * dT - fe;
-            Gc[PI_PFe_bio] = Gc[PI_PFe_bio] + Tt[PI_POC] * Tt[PI_DFe] * b.DFeFrac * b.lambda_POC * dT - b.kPOC * Tt[PI_PFe_bio] * dT;
-            Gc[PI_PFe_inorg] = Gc[PI_PFe_inorg] - Tt[PI_PFe_inorg] * b.kdiss * dT
-                             + (b.lambda_min + b.lambda_dust * Tt[PI_Dust]) * Tt[PI_DFe] * b.DFeFrac * dT + fe;
-        }
-        // apply_bcs! (apply_bcs.jl:4-98)
-        if (m.any_bc) {
-            const int ii = i - m.Hx, jj = j - m.Hy, kk = k - m.Hz;
-            const float axk = m.dy * dz, ayk = m.dx * dz;
-            const int64_t itn = a.st->iteration + 1;
             for (int n = 0; n < PI_NTRACERS; ++n) {
-                const FluxBC32* B = a.bcs + m.bc_off + n * 6;
-                if (B[PI_WEST].kind && i == 1 + m.Hx) Gc[n] += getbc32(B[PI_WEST], jj, kk, itn) * dT * axk / volk;
-                if (B[PI_EAST].kind && i == m.Nx + m.Hx) Gc[n] -= getbc32(B[PI_EAST], jj, kk, itn) * dT * axk / volk;
-                if (B[PI_SOUTH].kind && j == 1 + m.Hy) Gc[n] += getbc32(B[PI_SOUTH], ii, kk, itn) * dT * ayk / volk;
-                if (B[PI_NORTH].kind && j == m.Ny + m.Hy) Gc[n] -= getbc32(B[PI_NORTH], ii, kk, itn) * dT * ayk / volk;
-                if (B[PI_BOTTOM].kind && k == m.Nz + m.Hz) Gc[n] += getbc32(B[PI_BOTTOM], ii, jj, itn) * dT * az / volk;
-                if (B[PI_TOP].kind && k == 1 + m.Hz) Gc[n] -= getbc32(B[PI_TOP], ii, jj, itn) * dT * az / volk;
+                const float* t = a.tb + n * G + off;
+                win[n][0] = t[lev(k0 - 2)]; win[n][1] = t[lev(k0 - 1)]; win[n][2] = t[lev(k0)]; win[n][3] = t[lev(k0 + 1)];
+                Ft[n] = flux_v(fc, win[n][0], win[n][1], win[n][2], win[n][3], l2, l1, l0, lp);
             }
         }
-        // plk from the fixed-point sums; only cells with binned individuals can hold any
-        float pk[ACC_N];
-#pragma unroll
-        for (int r = 0; r < ACC_N; ++r) pk[r] = 0.0f;
-        if (a.pop[cq] > 0) {
-#pragma unroll
-            for (int r = 0; r < ACC_N; ++r) {
-                const long long v = (long long)a.acc[r * G + cq];
-                if (v) { a.acc[r * G + cq] = 0ull; pk[r] = (float)((double)v * m.fx_unit); }
-            }
+        float sink_prev[3] = { 0.0f, 0.0f, 0.0f };   // tracer at k-1 of PFe_inorg, Dust, PFe_bio
+        if (k0 - 1 > m.Hz) {
+            sink_prev[0] = a.tr[PI_PFe_inorg * G + off + qcol + (k0 - 2) * slab];
+            sink_prev[1] = a.tr[PI_Dust * G + off + qcol + (k0 - 2) * slab];
+            sink_prev[2] = a.tr[PI_PFe_bio * G + off + qcol + (k0 - 2) * slab];
         }
-        // apply_tendency! (tracer_update.jl:6-13)
-        const float plk[PI_NTRACERS] = { pk[ACC_DIC], pk[ACC_NH4], pk[ACC_NO3], pk[ACC_PO4], 0.0f, pk[ACC_DOC],
-                                         pk[ACC_DON], pk[ACC_DOP], 0.0f, pk[ACC_POC], pk[ACC_PON], pk[ACC_POP],
-                                         0.0f, 0.0f };
+        for (int k = k0; k <= kend; ++k) {
+            const int f = k + 1;
+            const float wbot = wv[qcol + (f - 1) * slab];
+            const bool bottom = f == bot + 1;                  // fill_halo_bottom_Gc! (Bounded)
+            const FCu fc = fcu(bottom ? 0.0f : wbot, az, a.rdzC[m.dz_off + min(f, bot) - 1], dT);
+            const int l2 = lm32(m, a.lm, i, j, f - 2), l1 = lm32(m, a.lm, i, j, f - 1);
+            const int l0 = lm32(m, a.lm, i, j, f), lp = lm32(m, a.lm, i, j, f + 1);
+            const int q = qcol + (k - 1) * slab;
+            const long long cq = off + q;
+            const float dz = a.dzF[m.dz_off + k - 1];
+            const float volk = az * dz;
+            const int c0m = l1, cpm = l0;                      // landmask at k and k+1
+            const float ftr = mulbf(mulbf(az * wtop - az * wbot, cpm), c0m);
+            const bool occupied = a.pop[cq] > 0;
+            float cur[PI_NTRACERS];
 #pragma unroll
-        for (int n = 0; n < PI_NTRACERS; ++n) a.tr_next[n * G + cq] = a.tr[n * G + cq] + (Gc[n] + plk[n] / volk);
+            for (int n = 0; n < PI_NTRACERS; ++n) cur[n] = a.tr[n * G + cq];
+#pragma unroll
+            for (int n = 0; n < PI_NTRACERS; ++n) {
+                const float nw_ = a.tb[n * G + off + lev(k + 2)];
+                win[n][0] = win[n][1]; win[n][1] = win[n][2]; win[n][2] = win[n][3]; win[n][3] = nw_;
+                const float Fb = bottom ? 0.0f : flux_v(fc, win[n][0], win[n][1], win[n][2], win[n][3], l2, l1, l0, lp);
+                const float cc = cur[n];
+                const float dG = mulbf(mulbf(Ft[n] - Fb, cpm), c0m);
+                float Gc = (win[n][1] - dT / volk * (dG - cc * ftr)) - cc;
+                Ft[n] = Fb;
+                // tracer_diffusion! (tracer_diffusion.jl:1-21)
+                if (diffuse) {
+                    const float* c = a.tr + n * G + off;
+                    const float axk = m.dy * dz, ayk = m.dx * dz;
+                    auto dx0 = [&](int ii) { return mulbf(mulbf(c[gid3(m, ii, j, k)] - c[gid3(m, ii - 1, j, k)], lm32(m, a.lm, ii, j, k)), lm32(m, a.lm, ii - 1, j, k)); };
+                    auto dy0 = [&](int jj) { return mulbf(mulbf(c[gid3(m, i, jj, k)] - c[gid3(m, i, jj - 1, k)], lm32(m, a.lm, i, jj, k)), lm32(m, a.lm, i, jj - 1, k)); };
+                    auto dz0 = [&](int kk) { return mulbf(mulbf(c[gid3(m, i, j, kk - 1)] - c[gid3(m, i, j, kk)], lm32(m, a.lm, i, j, kk)), lm32(m, a.lm, i, j, kk - 1)); };
+                    const float fx1 = b.kappa_h * axk * (dx0(i + 1) / m.dx), fx0 = b.kappa_h * axk * (dx0(i) / m.dx);
+                    const float fy1 = b.kappa_h * ayk * (dy0(j + 1) / m.dy), fy0 = b.kappa_h * ayk * (dy0(j) / m.dy);
+                    const float fz0 = b.kappa_v * az * (dz0(k) / dz), fz1 = b.kappa_v * az * (dz0(k + 1) / a.dzF[m.dz_off + k]);
+                    const float ax_ = mulbf(mulbf(fx1 - fx0, lm32(m, a.lm, i + 1, j, k)), c0m);
+                    const float ay_ = mulbf(mulbf(fy1 - fy0, lm32(m, a.lm, i, j + 1, k)), c0m);
+                    const float az_ = mulbf(mulbf(fz0 - fz1, cpm), c0m);
+                    Gc += 1.0f / volk * (ax_ + ay_ + az_) * dT;
+                }
+                // tracer_sinking! (tracer_sinking.jl:1-42)
+                if (n == PI_PFe_inorg || n == PI_Dust || n == PI_PFe_bio) {
+                    const int si = n == PI_PFe_inorg ? 0 : n == PI_Dust ? 1 : 2;
+                    const float ws = n == PI_PFe_bio ? b.w_sink_org : b.w_sink_inorg;
+                    const float fup = (k - 1 <= m.Hz) ? 0.0f : ws * sink_prev[si];
+                    const float fdn = (k >= bot) ? 0.0f : ws * cc;
+                    Gc += (fup - fdn) / a.dzC[m.dz_off + k - m.Hz - 1] * dT;
+                    sink_prev[si] = cc;
+                }
+                // tracer_forcing! (tracer_forcings.jl:2-50)
+                {
+                    auto T = [&](int d) -> float { return fmaxf(0.0f, cur[d]); };
+                    float fo = 0.0f;
+                    switch (n) {
+                        case PI_DIC: fo = T(PI_DOC) * b.kDOC * dT; break;
+                        case PI_DOC: fo = -T(PI_DOC) * b.kDOC * dT + T(PI_POC) * b.kPOC * dT; break;
+                        case PI_POC: fo = -T(PI_POC) * b.kPOC * dT; break;
+                        case PI_NH4: fo = T(PI_DON) * b.kDON * dT - T(PI_NH4) * b.Nit * dT; break;
+                        case PI_NO3: fo = T(PI_NH4) * b.Nit * dT; break;
+                        case PI_DON: fo = -T(PI_DON) * b.kDON * dT + T(PI_PON) * b.kPON * dT; break;
+                        case PI_PON: fo = -T(PI_PON) * b.kPON * dT; break;
+                        case PI_PO4: fo = T(PI_DOP) * b.kDOP * dT; break;
+                        case PI_DOP: fo = -T(PI_DOP) * b.kDOP * dT + T(PI_POP) * b.kPOP * dT; break;
+                        case PI_POP: fo = -T(PI_POP) * b.kPOP * dT; break;
+                        case PI_DFe: {
+                            const float fe = fmaxf(T(PI_DFe) - b.ligand, 0.0f) * T(PI_DFe) * b.DFeFrac * b.lambda_Fe * dT;
+                            fo = T(PI_PFe_bio) * b.kPOC * dT
+                               - (b.lambda_POC * T(PI_POC) + b.lambda_min + b.lambda_dust * T(PI_Dust)) * T(PI_DFe) * b.DFeFrac * dT
+                               + T(PI_PFe_inorg) * b.kdiss * dT - fe;
+                            break;
+                        }
+                        case PI_PFe_bio: fo = T(PI_POC) * T(PI_DFe) * b.DFeFrac * b.lambda_POC * dT - b.kPOC * T(PI_PFe_bio) * dT; break;
+                        case PI_PFe_inorg: {
+                            const float fe = fmaxf(T(PI_DFe) - b.ligand, 0.0f) * T(PI_DFe) * b.DFeFrac * b.lambda_Fe * dT;
+                            fo = -T(PI_PFe_inorg) * b.kdiss * dT + (b.lambda_min + b.lambda_dust * T(PI_Dust)) * T(PI_DFe) * b.DFeFrac * dT + fe;
+                            break;
+                        }
+                        default: break;
+                    }
+                    Gc += fo;
+                }
+                // apply_bcs! (apply_bcs.jl:4-98)
+                if (m.any_bc) {
+                    const FluxBC32* B = a.bcs + m.bc_off + n * 6;
+                    const int ii = i - m.Hx, jj = j - m.Hy, kk = k - m.Hz;
+                    const float axk = m.dy * dz, ayk = m.dx * dz;
+                    if (B[PI_WEST].kind && i == 1 + m.Hx) Gc += getbc32(B[PI_WEST], jj, kk, itn) * dT * axk / volk;
+                    if (B[PI_EAST].kind && i == m.Nx + m.Hx) Gc -= getbc32(B[PI_EAST], jj, kk, itn) * dT * axk / volk;
+                    if (B[PI_SOUTH].kind && j == 1 + m.Hy) Gc += getbc32(B[PI_SOUTH], ii, kk, itn) * dT * ayk / volk;
+                    if (B[PI_NORTH].kind && j == m.Ny + m.Hy) Gc -= getbc32(B[PI_NORTH], ii, kk, itn) * dT * ayk / volk;
+                    if (B[PI_BOTTOM].kind && k == bot) Gc += getbc32(B[PI_BOTTOM], ii, jj, itn) * dT * az / volk;
+                    if (B[PI_TOP].kind && k == top) Gc -= getbc32(B[PI_TOP], ii, jj, itn) * dT * az / volk;
+                }
+                // particle terms from the fixed-point sums, apply_tendency! (tracer_update.jl:6-13)
+                float plk = 0.0f;
+                const int slot = acc_slot(n);
+                if (slot >= 0 && occupied) {
+                    unsigned long long* pa = a.acc + (long long)slot * G + cq;
+                    const long long vv = (long long)*pa;
+                    if (vv) { *pa = 0ull; plk = (float)((double)vv * m.fx_unit); }
+                }
+                a.tr_next[n * G + cq] = cc + (Gc + plk / volk);
+            }
+            wtop = wbot;
+        }
     }
 }
 

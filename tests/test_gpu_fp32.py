@@ -66,7 +66,7 @@ def errors_vs_oracle(ref, f32, wl):
                 rel = np.abs(a - b) / np.maximum(np.abs(a), 1e-30)
                 out["quota_rel"] = max(out["quota_rel"], float(rel.max()))
     out["cell_mismatch_frac"] = n_cell_bad / max(n_act, 1)
-    vol = g.dx * g.dy * np.asarray(g.dzF)[g.Hz:g.Hz + g.Nz]
+    vol = float(g.Δx) * float(g.Δy) * np.asarray(g.dzF)[g.Hz:g.Hz + g.Nz]
     for n, name in enumerate(_abi.tracer_names):
         a, b = interior(g, ref.get_tracer(n)), interior(g, f32.get_tracer(n))
         scale = max(float(np.abs(a).max()), 1e-300)
@@ -222,7 +222,7 @@ def test_fp32_capacity_error_message(gpu_lib):
     it, _ = f32.get_time()
     msg = str(ei.value)
     assert msg.startswith("number of individual exceeds the capacity at timestep ")
-    assert msg == f"number of individual exceeds the capacity at timestep {(it + 1) * wl.dT / 86400!r} days"
+    assert msg == f"number of individual exceeds the capacity at timestep {it * wl.dT / 86400!r} days"
 
 
 def test_fp32_budget_matches_downloaded_fields(gpu_lib):
@@ -233,7 +233,7 @@ def test_fp32_budget_matches_downloaded_fields(gpu_lib):
     _drive_batch(batch, wls, 5, [VelCache(wl)])
     bud = batch.budget(0)
     g = wl.grid
-    vol = g.dx * g.dy * np.asarray(g.dzF)[g.Hz:g.Hz + g.Nz]
+    vol = float(g.Δx) * float(g.Δy) * np.asarray(g.dzF)[g.Hz:g.Hz + g.Nz]
     tot = lambda names: sum(float(np.sum(interior(g, batch.get_tracer(0, _abi.tracer_names.index(n))) * vol)) for n in names)
     assert bud["tracer_C"] == pytest.approx(tot(("DIC", "DOC", "POC")), rel=1e-12)
     assert bud["tracer_N"] == pytest.approx(tot(("NH4", "NO3", "DON", "PON")), rel=1e-12)
