@@ -248,3 +248,55 @@ def config3(nx=512, nz=128, N_per_species=16_777_216, nsp=4, steps=1000, dT=20.0
     n_vel = int(np.ceil(steps / 60)) + 1
     return _finish("config3", grid, nsp, [N_per_species] * nsp, C, None, None, dT, steps, rng,
                    vel, n_vel, 60 * dT, min(nz, 20), mus, 0.25, seed, no3_grad=2.0 * nz)
+
+
+def config4(n_members=64, steps=500, dT=30.0, seed=4, nmodes=32, n_max=None):
+    """Batched ensemble: members with grids Nx, Ny ~ U{64..256}, Nz ~ U{16..32} (50 m × 50 m × 2 m
+    cells), populations round(2^U(14, 20)) of one species, config-2 physics (random-Fourier velocity
+    refreshed every 60 steps, NO3 gradient, individuals in the top 40 m) and their own seeds.
+    `nmodes` Fourier modes per member (fewer than config 2's 256 to keep host generation short;
+    the device work does not depend on it). `n_max` caps the member count for tests."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for m in range(n_members if n_max is None else min(n_members, n_max)):
+        nx, ny = int(rng.integers(64, 257)), int(rng.integers(64, 257))
+        nz = int(rng.integers(16, 33))
+        N = int(round(2.0 ** rng.uniform(14, 20)))
+        ms = seed * 1000 + m
+        r = np.random.default_rng(ms)
+        grid = RectilinearGrid(size=(nx, ny, nz), x=(0.0, nx * 50.0), y=(0.0, ny * 50.0),
+                               z=(0.0, -2.0 * nz), FT=np.float64, topology=(Periodic, Periodic, Bounded))
+        vel = FourierVelocity(grid, nmodes=nmodes, rms=0.05, seed=ms)
+        n_vel = int(np.ceil(steps / 60)) + 1
+        wl = _finish(f"config4[{m}]", grid, 1, [N], 2 * N, None, None, dT, steps, r, vel, n_vel, 60 * dT,
+                     min(nz, 20), [0.0], 0.2, ms, no3_grad=2.0 * nz)
+        out.append(wl)
+    return out
+
+
+def config5(n_boxes=4096, steps=2880, dT=60.0, seed=5, n_max=None):
+    """Batched 0D boxes (examples/0D_experiment.jl:35): 1×1×1 cells of 128 m × 128 m × 128 m, no
+    advection (zero velocity), populations round(2^U(8, 13)), light with a per-box phase offset
+    φ ~ U(0, 86400 s). Division by size with dvid_reg = 1.0 and dvid_P = 1.2e-5 s⁻¹ (≈ 1 d⁻¹ for
+    cells at nominal size); nitrate and ammonium start at 0.01 mmol m⁻³ (near their half-saturation
+    constants), so growth is nutrient-limited. Capacity 8 × the initial population."""
+    rng = np.random.default_rng(seed)
+    out = []
+    over = {"dvid_reg": [1.0], "dvid_P": [1.2e-5]}
+    for b in range(n_boxes if n_max is None else min(n_boxes, n_max)):
+        N = int(round(2.0 ** rng.uniform(8, 13)))
+        phase = float(rng.uniform(0.0, 86400.0))
+        ms = seed * 100000 + b
+        r = np.random.default_rng(ms)
+        grid = RectilinearGrid(size=(1, 1, 1), x=(0.0, 128.0), y=(0.0, 128.0), z=(0.0, -128.0),
+                               FT=np.float64, topology=(Periodic, Periodic, Bounded))
+        zero = (np.zeros((1, 1, 1), order="F"), np.zeros((1, 1, 1), order="F"), np.zeros((1, 1, 2), order="F"))
+        wl = _finish(f"config5[{b}]", grid, 1, [N], 8 * N, over, None, dT, steps, r, lambda t: zero, 1,
+                     dT * steps, None, [0.0], 0.2, ms)
+        for name in ("NO3", "NH4"):
+            a = wl.tracers[tracer_names.index(name)]
+            a[...] = 0.01
+        hours = wl.parf.shape[2]
+        wl.parf = diel_parf(1, 1, hours, peak=1000.0, phase=phase)
+        out.append(wl)
+    return out
