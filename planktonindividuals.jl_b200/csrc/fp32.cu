@@ -105,6 +105,7 @@ struct pi_batch {
     int* pop_sp = nullptr;
     unsigned long long* acc = nullptr;
     unsigned long long* chl_acc = nullptr;
+    float4* env = nullptr;          // 2 per cell: packed environment of occupied cells
     IndDev32 P{};
     int ntiles = 0;
     int2* tiles = nullptr;
@@ -368,7 +369,8 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
     }
     { BScope sc(b, "k32_par");
       k32_par<<<warp_grid(b->T.nicol, b->tune.wpb_par), 32 * b->tune.wpb_par, 0, s>>>(b->T, b->dzF, b->bgc, b->chl_acc, b->PARF,
-                                                                                   b->par, b->diag_par, b->errw); }
+                                                                                   b->par, b->diag_par, tr, G, b->F, b->pop,
+                                                                                   b->env, b->errw); }
     { BScope sc(b, "cub_scan_tiles");
       size_t tb = b->cub_bytes;
       BK(cub::DeviceScan::ExclusiveSum(b->cub_tmp, tb, b->tile_cnt, b->tile_off, b->ntiles, s), "scan tiles"); }
@@ -380,7 +382,8 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
     {
         PhysArgs a;
         a.T = b->T; a.P = b->P; a.sp = b->sp; a.F = b->F; a.st = b->st; a.dT = fdT; a.Gtot = G; a.tr = tr;
-        a.par = b->par; a.pop = b->pop; a.pop_sp = b->pop_sp; a.acc = b->acc; a.dcnt = b->dcnt; a.err = b->errw;
+        a.par = b->par; a.pop = b->pop; a.pop_sp = b->pop_sp; a.env = b->env; a.acc = b->acc; a.dcnt = b->dcnt;
+        a.err = b->errw;
         BScope sc(b, "k32_physiology");
         k32_physiology<<<tile_grid(b, b->tune.persist_phys), b->tune.bs_phys, 0, s>>>(a);
     }
@@ -399,10 +402,11 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
         {
             a.items = b->z_items; a.nitems = b->nz_items;
             BScope sc(b, "k32_ztail");
-            const unsigned grid = warp_grid(b->nz_items, 4);
-            if (b->tune.lz == 8) k32_ztail<8><<<grid, 128, 0, s>>>(a);
-            else if (b->tune.lz == 32) k32_ztail<32><<<grid, 128, 0, s>>>(a);
-            else k32_ztail<16><<<grid, 128, 0, s>>>(a);
+            const unsigned grid = (unsigned)std::max(1, b->nz_items);
+            const dim3 blk(32, PI_NTRACERS);
+            if (b->tune.lz == 8) k32_ztail<8><<<grid, blk, 0, s>>>(a);
+            else if (b->tune.lz == 32) k32_ztail<32><<<grid, blk, 0, s>>>(a);
+            else k32_ztail<16><<<grid, blk, 0, s>>>(a);
         }
     }
     { BScope sc(b, "k32_halo");
@@ -567,7 +571,7 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     bool shared = true;
     for (auto& h : b->mh) if (h.bgc.shared_graz != 1.0) shared = false;
     if (!shared) BA(b->pop_sp, (size_t)nspecies * G);
-    BA(b->acc, (size_t)ACC_N * G); BA(b->chl_acc, G);
+    BA(b->acc, (size_t)ACC_N * G); BA(b->chl_acc, G); BA(b->env, 2 * G);
     IndDev32& P = b->P;
     BA(P.cell, S); BA(P.scell, S); BA(P.ox, S); BA(P.oy, S); BA(P.oz, S); BA(P.Bm, S); BA(P.Cq, S);
     BA(P.Nq, S); BA(P.Pq, S); BA(P.Chl, S); BA(P.age, S); BA(P.gen, S); BA(P.flags, S); BA(P.stat, S);

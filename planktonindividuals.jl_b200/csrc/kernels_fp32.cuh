@@ -378,9 +378,15 @@ __global__ void k32_move(MoveArgs a) {
 // ------------------------------------------------------------------------------------------
 // PAR down each column (calc_par!, Individuals/utils.jl:55-63); consumes the Chl sums
 // ------------------------------------------------------------------------------------------
+//
+// For every interior cell holding individuals it also packs the environment physiology gathers
+// (find_NPT!, utils.jl:14-25: NH4, NO3, PO4, DOC, par, temperature, pop) into one 32-byte record,
+// so an individual reads one sector instead of seven.
 __global__ void k32_par(Tab32 T, const float* __restrict__ dzF, const BgcDev32* __restrict__ bgc,
                         unsigned long long* __restrict__ chl_acc, float* __restrict__ PARF,
-                        float* __restrict__ par, float* __restrict__ diag_par, const uint32_t* err) {
+                        float* __restrict__ par, float* __restrict__ diag_par, const float* __restrict__ tr,
+                        long long Gtot, const MemberForcing* __restrict__ F, const int* __restrict__ pop,
+                        float4* __restrict__ env, const uint32_t* err) {
     if (stopped(err)) return;
     const int lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -406,6 +412,12 @@ __global__ void k32_par(Tab32 T, const float* __restrict__ dzF, const BgcDev32* 
             par[c] = pv;
             parf = parf * e;
             diag_par[c] += pv;
+            const int pp = pop[c];
+            if (pp > 0) {
+                env[2 * c] = make_float4(tr[PI_NH4 * Gtot + c], tr[PI_NO3 * Gtot + c], tr[PI_PO4 * Gtot + c],
+                                         tr[PI_DOC * Gtot + c]);
+                env[2 * c + 1] = make_float4(pv, F[it.x].temp[c - m.cell_off], (float)pp, 0.0f);
+            }
         }
         PARF[fcol] = parf;
     }
@@ -546,6 +558,7 @@ struct PhysArgs {
     const float* par;
     const int* pop;
     const int* pop_sp;
+    const float4* env;          // packed environment of occupied interior cells
     unsigned long long* acc;
     uint32_t* dcnt;
     const uint32_t* err;
@@ -565,7 +578,14 @@ __device__ __forceinline__ void phys_one(const PhysArgs& a, const MemberDev& m, 
     const SpeciesDev32& p = a.sp[mi * a.T.nsp + s];
     const float dT = a.dT;
     float NH4 = 0.0f, NO3 = 0.0f, PO4 = 0.0f, DOC = 0.0f, parv = 0.0f, Tm = 0.0f, popv = 0.0f;
-    if (ac0) {
+    const bool inside = interior_q(m, q);
+    if (ac0 && inside) {
+        const float4 e0 = a.env[2 * cq], e1 = a.env[2 * cq + 1];
+        NH4 = fmaxf(0.0f, e0.x); NO3 = fmaxf(0.0f, e0.y); PO4 = fmaxf(0.0f, e0.z); DOC = fmaxf(0.0f, e0.w);
+        parv = e1.x; Tm = e1.y;
+        popv = a.pop_sp ? (float)a.pop_sp[(long long)s * G + cq] : e1.z;
+    } else if (ac0) {
+        // a cell on the halo face (a position exactly at x = Nx): read the fields themselves
         NH4 = fmaxf(0.0f, a.tr[PI_NH4 * G + cq]); NO3 = fmaxf(0.0f, a.tr[PI_NO3 * G + cq]);
         PO4 = fmaxf(0.0f, a.tr[PI_PO4 * G + cq]); DOC = fmaxf(0.0f, a.tr[PI_DOC * G + cq]);
         parv = a.par[cq];
@@ -626,7 +646,7 @@ __device__ __forceinline__ void phys_one(const PhysArgs& a, const MemberDev& m, 
     P.Bm[g] = Bm; P.Cq[g] = Cq; P.Nq[g] = Nq; P.Pq[g] = Pq; P.Chl[g] = Chl; P.age[g] = age;
     P.flags[g] = (uint8_t)(F32_AC | (dg ? F32_GRAZ : 0) | (dm ? F32_MORT : 0) | (dd ? F32_DVID : 0));
     // calc_consume_kernel! (consume_loss.jl:2-9): only individuals binned this step reach the grid
-    if (ac0 && interior_q(m, q)) {
+    if (ac0 && inside) {
         const double u = m.fx_unit;
         add_fixed(&a.acc[ACC_DIC * G + cq], (resp - PS) * dT, u);
         add_fixed(&a.acc[ACC_DOC * G + cq], (exu - VDOC) * dT, u);
@@ -847,18 +867,20 @@ __global__ void __launch_bounds__(32 * (TY + 4)) k32_xy(TrArgs a) {
     }
 }
 
-// z sweep of all 14 tracers and the rest of tracer_update! for LZ levels of 32 columns: each
-// thread walks its column keeping, per tracer, the 4-level stencil window of tracer_temp and the
-// flux of the face above the current cell.
+// z sweep and the rest of tracer_update! for LZ levels of 32 columns: warp y of the block takes
+// tracer y, each lane walks its column keeping the 4-level stencil window of tracer_temp and the
+// flux of the face above the current cell. The 14 warps walk the same cells, so the forcing terms'
+// reads of the other tracers at a cell hit the lines those warps load.
 template <int LZ>
-__global__ void __launch_bounds__(128) k32_ztail(TrArgs a) {
+__global__ void __launch_bounds__(32 * PI_NTRACERS, 2) k32_ztail(TrArgs a) {
     if (stopped(a.err)) return;
-    const int lane = threadIdx.x & 31;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
+    const int lane = threadIdx.x, n = threadIdx.y;
     const long long G = a.Gtot;
     const float dT = a.dT;
     const int64_t itn = a.st->iteration + 1;
-    for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < a.nitems; w += nw) {
+    const int slot = acc_slot(n);
+    const bool sinks = n == PI_PFe_inorg || n == PI_Dust || n == PI_PFe_bio;
+    for (int w = blockIdx.x; w < a.nitems; w += gridDim.x) {
         const int4 it = a.items[w];
         const MemberDev& m = a.T.md[it.x];
         const int i = it.y + lane, j = it.z, k0 = it.w;
@@ -871,132 +893,111 @@ __global__ void __launch_bounds__(128) k32_ztail(TrArgs a) {
         const float* wv = a.F[it.x].vel1[2];
         const BgcDev32& b = a.bgc[it.x];
         const float az = m.dx * m.dy;
-        const bool diffuse = b.kappa_h != 0.0f || b.kappa_v != 0.0f;
+        const float* t = a.tb + n * G + off;
+        const float* c = a.tr + n * G + off;
         auto lev = [&](int kk) { return qcol + (min(max(kk, top), bot) - 1) * slab; };
-        float win[PI_NTRACERS][4], Ft[PI_NTRACERS];
+        float w0 = t[lev(k0 - 2)], w1 = t[lev(k0 - 1)], w2 = t[lev(k0)], w3 = t[lev(k0 + 1)];
         float wtop = wv[qcol + (k0 - 1) * slab];
-        {
-            const FCu fc = fcu(wtop, az, a.rdzC[m.dz_off + k0 - 1], dT);
-            const int l2 = lm32(m, a.lm, i, j, k0 - 2), l1 = lm32(m, a.lm, i, j, k0 - 1);
-            const int l0 = lm32(m, a.lm, i, j, k0), lp = lm32(m, a.lm, i, j, k0 + 1);
-#pragma unroll
-            for (int n = 0; n < PI_NTRACERS; ++n) {
-                const float* t = a.tb + n * G + off;
-                win[n][0] = t[lev(k0 - 2)]; win[n][1] = t[lev(k0 - 1)]; win[n][2] = t[lev(k0)]; win[n][3] = t[lev(k0 + 1)];
-                Ft[n] = flux_v(fc, win[n][0], win[n][1], win[n][2], win[n][3], l2, l1, l0, lp);
-            }
-        }
-        float sink_prev[3] = { 0.0f, 0.0f, 0.0f };   // tracer at k-1 of PFe_inorg, Dust, PFe_bio
-        if (k0 - 1 > m.Hz) {
-            sink_prev[0] = a.tr[PI_PFe_inorg * G + off + qcol + (k0 - 2) * slab];
-            sink_prev[1] = a.tr[PI_Dust * G + off + qcol + (k0 - 2) * slab];
-            sink_prev[2] = a.tr[PI_PFe_bio * G + off + qcol + (k0 - 2) * slab];
-        }
+        float Ft = flux_v(fcu(wtop, az, a.rdzC[m.dz_off + k0 - 1], dT), w0, w1, w2, w3,
+                          lm32(m, a.lm, i, j, k0 - 2), lm32(m, a.lm, i, j, k0 - 1), lm32(m, a.lm, i, j, k0),
+                          lm32(m, a.lm, i, j, k0 + 1));
+        const float ws = n == PI_PFe_bio ? b.w_sink_org : b.w_sink_inorg;
+        float sink_prev = (sinks && k0 - 1 > m.Hz) ? c[qcol + (k0 - 2) * slab] : 0.0f;
         for (int k = k0; k <= kend; ++k) {
             const int f = k + 1;
-            const float wbot = wv[qcol + (f - 1) * slab];
-            const bool bottom = f == bot + 1;                  // fill_halo_bottom_Gc! (Bounded)
-            const FCu fc = fcu(bottom ? 0.0f : wbot, az, a.rdzC[m.dz_off + min(f, bot) - 1], dT);
-            const int l2 = lm32(m, a.lm, i, j, f - 2), l1 = lm32(m, a.lm, i, j, f - 1);
-            const int l0 = lm32(m, a.lm, i, j, f), lp = lm32(m, a.lm, i, j, f + 1);
             const int q = qcol + (k - 1) * slab;
             const long long cq = off + q;
+            const float cc = c[q];
+            const float nw_ = t[lev(k + 2)];
+            const float wbot = wv[qcol + (f - 1) * slab];
+            const bool bottom = f == bot + 1;                  // fill_halo_bottom_Gc! (Bounded)
+            const int l2 = lm32(m, a.lm, i, j, f - 2), l1 = lm32(m, a.lm, i, j, f - 1);
+            const int l0 = lm32(m, a.lm, i, j, f), lp = lm32(m, a.lm, i, j, f + 1);
+            w0 = w1; w1 = w2; w2 = w3; w3 = nw_;
+            const float Fb = bottom ? 0.0f : flux_v(fcu(wbot, az, a.rdzC[m.dz_off + f - 1], dT), w0, w1, w2, w3, l2, l1, l0, lp);
             const float dz = a.dzF[m.dz_off + k - 1];
             const float volk = az * dz;
             const int c0m = l1, cpm = l0;                      // landmask at k and k+1
             const float ftr = mulbf(mulbf(az * wtop - az * wbot, cpm), c0m);
-            const bool occupied = a.pop[cq] > 0;
-            float cur[PI_NTRACERS];
-#pragma unroll
-            for (int n = 0; n < PI_NTRACERS; ++n) cur[n] = a.tr[n * G + cq];
-#pragma unroll
-            for (int n = 0; n < PI_NTRACERS; ++n) {
-                const float nw_ = a.tb[n * G + off + lev(k + 2)];
-                win[n][0] = win[n][1]; win[n][1] = win[n][2]; win[n][2] = win[n][3]; win[n][3] = nw_;
-                const float Fb = bottom ? 0.0f : flux_v(fc, win[n][0], win[n][1], win[n][2], win[n][3], l2, l1, l0, lp);
-                const float cc = cur[n];
-                const float dG = mulbf(mulbf(Ft[n] - Fb, cpm), c0m);
-                float Gc = (win[n][1] - dT / volk * (dG - cc * ftr)) - cc;
-                Ft[n] = Fb;
-                // tracer_diffusion! (tracer_diffusion.jl:1-21)
-                if (diffuse) {
-                    const float* c = a.tr + n * G + off;
-                    const float axk = m.dy * dz, ayk = m.dx * dz;
-                    auto dx0 = [&](int ii) { return mulbf(mulbf(c[gid3(m, ii, j, k)] - c[gid3(m, ii - 1, j, k)], lm32(m, a.lm, ii, j, k)), lm32(m, a.lm, ii - 1, j, k)); };
-                    auto dy0 = [&](int jj) { return mulbf(mulbf(c[gid3(m, i, jj, k)] - c[gid3(m, i, jj - 1, k)], lm32(m, a.lm, i, jj, k)), lm32(m, a.lm, i, jj - 1, k)); };
-                    auto dz0 = [&](int kk) { return mulbf(mulbf(c[gid3(m, i, j, kk - 1)] - c[gid3(m, i, j, kk)], lm32(m, a.lm, i, j, kk)), lm32(m, a.lm, i, j, kk - 1)); };
-                    const float fx1 = b.kappa_h * axk * (dx0(i + 1) / m.dx), fx0 = b.kappa_h * axk * (dx0(i) / m.dx);
-                    const float fy1 = b.kappa_h * ayk * (dy0(j + 1) / m.dy), fy0 = b.kappa_h * ayk * (dy0(j) / m.dy);
-                    const float fz0 = b.kappa_v * az * (dz0(k) / dz), fz1 = b.kappa_v * az * (dz0(k + 1) / a.dzF[m.dz_off + k]);
-                    const float ax_ = mulbf(mulbf(fx1 - fx0, lm32(m, a.lm, i + 1, j, k)), c0m);
-                    const float ay_ = mulbf(mulbf(fy1 - fy0, lm32(m, a.lm, i, j + 1, k)), c0m);
-                    const float az_ = mulbf(mulbf(fz0 - fz1, cpm), c0m);
-                    Gc += 1.0f / volk * (ax_ + ay_ + az_) * dT;
-                }
-                // tracer_sinking! (tracer_sinking.jl:1-42)
-                if (n == PI_PFe_inorg || n == PI_Dust || n == PI_PFe_bio) {
-                    const int si = n == PI_PFe_inorg ? 0 : n == PI_Dust ? 1 : 2;
-                    const float ws = n == PI_PFe_bio ? b.w_sink_org : b.w_sink_inorg;
-                    const float fup = (k - 1 <= m.Hz) ? 0.0f : ws * sink_prev[si];
-                    const float fdn = (k >= bot) ? 0.0f : ws * cc;
-                    Gc += (fup - fdn) / a.dzC[m.dz_off + k - m.Hz - 1] * dT;
-                    sink_prev[si] = cc;
-                }
-                // tracer_forcing! (tracer_forcings.jl:2-50)
-                {
-                    auto T = [&](int d) -> float { return fmaxf(0.0f, cur[d]); };
-                    float fo = 0.0f;
-                    switch (n) {
-                        case PI_DIC: fo = T(PI_DOC) * b.kDOC * dT; break;
-                        case PI_DOC: fo = -T(PI_DOC) * b.kDOC * dT + T(PI_POC) * b.kPOC * dT; break;
-                        case PI_POC: fo = -T(PI_POC) * b.kPOC * dT; break;
-                        case PI_NH4: fo = T(PI_DON) * b.kDON * dT - T(PI_NH4) * b.Nit * dT; break;
-                        case PI_NO3: fo = T(PI_NH4) * b.Nit * dT; break;
-                        case PI_DON: fo = -T(PI_DON) * b.kDON * dT + T(PI_PON) * b.kPON * dT; break;
-                        case PI_PON: fo = -T(PI_PON) * b.kPON * dT; break;
-                        case PI_PO4: fo = T(PI_DOP) * b.kDOP * dT; break;
-                        case PI_DOP: fo = -T(PI_DOP) * b.kDOP * dT + T(PI_POP) * b.kPOP * dT; break;
-                        case PI_POP: fo = -T(PI_POP) * b.kPOP * dT; break;
-                        case PI_DFe: {
-                            const float fe = fmaxf(T(PI_DFe) - b.ligand, 0.0f) * T(PI_DFe) * b.DFeFrac * b.lambda_Fe * dT;
-                            fo = T(PI_PFe_bio) * b.kPOC * dT
-                               - (b.lambda_POC * T(PI_POC) + b.lambda_min + b.lambda_dust * T(PI_Dust)) * T(PI_DFe) * b.DFeFrac * dT
-                               + T(PI_PFe_inorg) * b.kdiss * dT - fe;
-                            break;
-                        }
-                        case PI_PFe_bio: fo = T(PI_POC) * T(PI_DFe) * b.DFeFrac * b.lambda_POC * dT - b.kPOC * T(PI_PFe_bio) * dT; break;
-                        case PI_PFe_inorg: {
-                            const float fe = fmaxf(T(PI_DFe) - b.ligand, 0.0f) * T(PI_DFe) * b.DFeFrac * b.lambda_Fe * dT;
-                            fo = -T(PI_PFe_inorg) * b.kdiss * dT + (b.lambda_min + b.lambda_dust * T(PI_Dust)) * T(PI_DFe) * b.DFeFrac * dT + fe;
-                            break;
-                        }
-                        default: break;
-                    }
-                    Gc += fo;
-                }
-                // apply_bcs! (apply_bcs.jl:4-98)
-                if (m.any_bc) {
-                    const FluxBC32* B = a.bcs + m.bc_off + n * 6;
-                    const int ii = i - m.Hx, jj = j - m.Hy, kk = k - m.Hz;
-                    const float axk = m.dy * dz, ayk = m.dx * dz;
-                    if (B[PI_WEST].kind && i == 1 + m.Hx) Gc += getbc32(B[PI_WEST], jj, kk, itn) * dT * axk / volk;
-                    if (B[PI_EAST].kind && i == m.Nx + m.Hx) Gc -= getbc32(B[PI_EAST], jj, kk, itn) * dT * axk / volk;
-                    if (B[PI_SOUTH].kind && j == 1 + m.Hy) Gc += getbc32(B[PI_SOUTH], ii, kk, itn) * dT * ayk / volk;
-                    if (B[PI_NORTH].kind && j == m.Ny + m.Hy) Gc -= getbc32(B[PI_NORTH], ii, kk, itn) * dT * ayk / volk;
-                    if (B[PI_BOTTOM].kind && k == bot) Gc += getbc32(B[PI_BOTTOM], ii, jj, itn) * dT * az / volk;
-                    if (B[PI_TOP].kind && k == top) Gc -= getbc32(B[PI_TOP], ii, jj, itn) * dT * az / volk;
-                }
-                // particle terms from the fixed-point sums, apply_tendency! (tracer_update.jl:6-13)
-                float plk = 0.0f;
-                const int slot = acc_slot(n);
-                if (slot >= 0 && occupied) {
-                    unsigned long long* pa = a.acc + (long long)slot * G + cq;
-                    const long long vv = (long long)*pa;
-                    if (vv) { *pa = 0ull; plk = (float)((double)vv * m.fx_unit); }
-                }
-                a.tr_next[n * G + cq] = cc + (Gc + plk / volk);
-            }
+            const float dG = mulbf(mulbf(Ft - Fb, cpm), c0m);
+            float Gc = (w1 - dT / volk * (dG - cc * ftr)) - cc;
+            Ft = Fb;
             wtop = wbot;
+            // tracer_diffusion! (tracer_diffusion.jl:1-21)
+            if (b.kappa_h != 0.0f || b.kappa_v != 0.0f) {
+                const float axk = m.dy * dz, ayk = m.dx * dz;
+                auto dx0 = [&](int ii) { return mulbf(mulbf(c[gid3(m, ii, j, k)] - c[gid3(m, ii - 1, j, k)], lm32(m, a.lm, ii, j, k)), lm32(m, a.lm, ii - 1, j, k)); };
+                auto dy0 = [&](int jj) { return mulbf(mulbf(c[gid3(m, i, jj, k)] - c[gid3(m, i, jj - 1, k)], lm32(m, a.lm, i, jj, k)), lm32(m, a.lm, i, jj - 1, k)); };
+                auto dz0 = [&](int kk) { return mulbf(mulbf(c[gid3(m, i, j, kk - 1)] - c[gid3(m, i, j, kk)], lm32(m, a.lm, i, j, kk)), lm32(m, a.lm, i, j, kk - 1)); };
+                const float fx1 = b.kappa_h * axk * (dx0(i + 1) / m.dx), fx0 = b.kappa_h * axk * (dx0(i) / m.dx);
+                const float fy1 = b.kappa_h * ayk * (dy0(j + 1) / m.dy), fy0 = b.kappa_h * ayk * (dy0(j) / m.dy);
+                const float fz0 = b.kappa_v * az * (dz0(k) / dz), fz1 = b.kappa_v * az * (dz0(k + 1) / a.dzF[m.dz_off + k]);
+                const float ax_ = mulbf(mulbf(fx1 - fx0, lm32(m, a.lm, i + 1, j, k)), c0m);
+                const float ay_ = mulbf(mulbf(fy1 - fy0, lm32(m, a.lm, i, j + 1, k)), c0m);
+                const float az_ = mulbf(mulbf(fz0 - fz1, cpm), c0m);
+                Gc += 1.0f / volk * (ax_ + ay_ + az_) * dT;
+            }
+            // tracer_sinking! (tracer_sinking.jl:1-42)
+            if (sinks) {
+                const float fup = (k - 1 <= m.Hz) ? 0.0f : ws * sink_prev;
+                const float fdn = (k >= bot) ? 0.0f : ws * cc;
+                Gc += (fup - fdn) / a.dzC[m.dz_off + k - m.Hz - 1] * dT;
+                sink_prev = cc;
+            }
+            // tracer_forcing! (tracer_forcings.jl:2-50) on max(0, tracer)
+            {
+                auto T = [&](int d) -> float { return d == n ? fmaxf(0.0f, cc) : fmaxf(0.0f, a.tr[d * G + cq]); };
+                float fo = 0.0f;
+                switch (n) {
+                    case PI_DIC: fo = T(PI_DOC) * b.kDOC * dT; break;
+                    case PI_DOC: fo = -T(PI_DOC) * b.kDOC * dT + T(PI_POC) * b.kPOC * dT; break;
+                    case PI_POC: fo = -T(PI_POC) * b.kPOC * dT; break;
+                    case PI_NH4: fo = T(PI_DON) * b.kDON * dT - T(PI_NH4) * b.Nit * dT; break;
+                    case PI_NO3: fo = T(PI_NH4) * b.Nit * dT; break;
+                    case PI_DON: fo = -T(PI_DON) * b.kDON * dT + T(PI_PON) * b.kPON * dT; break;
+                    case PI_PON: fo = -T(PI_PON) * b.kPON * dT; break;
+                    case PI_PO4: fo = T(PI_DOP) * b.kDOP * dT; break;
+                    case PI_DOP: fo = -T(PI_DOP) * b.kDOP * dT + T(PI_POP) * b.kPOP * dT; break;
+                    case PI_POP: fo = -T(PI_POP) * b.kPOP * dT; break;
+                    case PI_DFe: {
+                        const float dfe = T(PI_DFe);
+                        const float fe = fmaxf(dfe - b.ligand, 0.0f) * dfe * b.DFeFrac * b.lambda_Fe * dT;
+                        fo = T(PI_PFe_bio) * b.kPOC * dT
+                           - (b.lambda_POC * T(PI_POC) + b.lambda_min + b.lambda_dust * T(PI_Dust)) * dfe * b.DFeFrac * dT
+                           + T(PI_PFe_inorg) * b.kdiss * dT - fe;
+                        break;
+                    }
+                    case PI_PFe_bio: fo = T(PI_POC) * T(PI_DFe) * b.DFeFrac * b.lambda_POC * dT - b.kPOC * T(PI_PFe_bio) * dT; break;
+                    case PI_PFe_inorg: {
+                        const float dfe = T(PI_DFe);
+                        const float fe = fmaxf(dfe - b.ligand, 0.0f) * dfe * b.DFeFrac * b.lambda_Fe * dT;
+                        fo = -T(PI_PFe_inorg) * b.kdiss * dT + (b.lambda_min + b.lambda_dust * T(PI_Dust)) * dfe * b.DFeFrac * dT + fe;
+                        break;
+                    }
+                    default: break;
+                }
+                Gc += fo;
+            }
+            // apply_bcs! (apply_bcs.jl:4-98)
+            if (m.any_bc) {
+                const FluxBC32* B = a.bcs + m.bc_off + n * 6;
+                const int ii = i - m.Hx, jj = j - m.Hy, kk = k - m.Hz;
+                const float axk = m.dy * dz, ayk = m.dx * dz;
+                if (B[PI_WEST].kind && i == 1 + m.Hx) Gc += getbc32(B[PI_WEST], jj, kk, itn) * dT * axk / volk;
+                if (B[PI_EAST].kind && i == m.Nx + m.Hx) Gc -= getbc32(B[PI_EAST], jj, kk, itn) * dT * axk / volk;
+                if (B[PI_SOUTH].kind && j == 1 + m.Hy) Gc += getbc32(B[PI_SOUTH], ii, kk, itn) * dT * ayk / volk;
+                if (B[PI_NORTH].kind && j == m.Ny + m.Hy) Gc -= getbc32(B[PI_NORTH], ii, kk, itn) * dT * ayk / volk;
+                if (B[PI_BOTTOM].kind && k == bot) Gc += getbc32(B[PI_BOTTOM], ii, jj, itn) * dT * az / volk;
+                if (B[PI_TOP].kind && k == top) Gc -= getbc32(B[PI_TOP], ii, jj, itn) * dT * az / volk;
+            }
+            // particle terms from the fixed-point sums, apply_tendency! (tracer_update.jl:6-13)
+            float plk = 0.0f;
+            if (slot >= 0 && a.pop[cq] > 0) {
+                unsigned long long* pa = a.acc + (long long)slot * G + cq;
+                const long long vv = (long long)*pa;
+                if (vv) { *pa = 0ull; plk = (float)((double)vv * m.fx_unit); }
+            }
+            a.tr_next[n * G + cq] = cc + (Gc + plk / volk);
         }
     }
 }
