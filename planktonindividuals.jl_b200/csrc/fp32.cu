@@ -63,7 +63,7 @@ struct MemberHost {
 struct Tuning {
     int bs_move = 256, bs_phys = 256, bs_assign = 256;
     int persist_move = 0, persist_phys = 0;   // 0: one tile per block; k: k blocks per SM, looping
-    int ty = 4;                               // rows of an x-y tracer tile (4 or 8)
+    int ty = 8;                               // rows of an x-y tracer tile (4, 8 or 16)
     int lz = 16;                              // levels walked by a z thread (8, 16 or 32)
     int wpb_par = 4;
 };
@@ -396,7 +396,8 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
             a.items = b->xy_items; a.nitems = b->nxy_items;
             BScope sc(b, "k32_xy");
             const unsigned grid = (unsigned)std::max(1, b->nxy_items);
-            if (b->tune.ty == 8) k32_xy<8><<<grid, 32 * 12, xy_smem(8), s>>>(a);
+            if (b->tune.ty == 16) k32_xy<16><<<grid, 32 * 20, xy_smem(16), s>>>(a);
+            else if (b->tune.ty == 8) k32_xy<8><<<grid, 32 * 12, xy_smem(8), s>>>(a);
             else k32_xy<4><<<grid, 32 * 8, xy_smem(4), s>>>(a);
         }
         {
@@ -648,6 +649,7 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     ok = ok && cudaMemsetAsync(P.cell, 0xff, S * sizeof(int32_t), s0) == cudaSuccess;
     ok = ok && cudaStreamSynchronize(s0) == cudaSuccess;
     if (!ok) { b->err = "pi_batch_create: device initialisation failed"; return bail(PI_ERR_CUDA); }
+    cudaFuncSetAttribute(k32_xy<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xy_smem(16));
     cudaFuncSetAttribute(k32_xy<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xy_smem(8));
     cudaFuncSetAttribute(k32_xy<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xy_smem(4));
     b->T.md = b->md; b->T.nsp = nspecies; b->T.tiles = b->tiles; b->T.ntiles = b->ntiles; b->T.seg_tile0 = b->seg_tile0;
@@ -1236,7 +1238,7 @@ pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t k, char* report, siz
         { "k32_physiology", &t.bs_phys, {128, 256, 512, 1024}, "physiology block", 1 },
         { "k32_physiology", &t.persist_phys, {0, 2, 4, 8}, "physiology blocks/SM (0 = one tile per block)", 0 },
         { "k32_assign", &t.bs_assign, {128, 256, 512, 1024}, "assign block", 1 },
-        { "k32_xy", &t.ty, {4, 8}, "x-y tracer tile rows", 0 },
+        { "k32_xy", &t.ty, {4, 8, 16}, "x-y tracer tile rows", 0 },
         { "k32_ztail", &t.lz, {8, 16, 32}, "z levels per thread", 0 },
         { "k32_par", &t.wpb_par, {1, 2, 4, 8}, "par warps/block", 32 },
     };

@@ -704,30 +704,26 @@ __device__ __forceinline__ float psid0(float d0, float dn, const FCu& f) {
     const float a = f.d0c * d0 + f.d1c * dn, b = f.R * dn;
     return d0 >= 0.0f ? fmaxf(0.0f, fminf(fminf(d0, a), b)) : fminf(0.0f, fmaxf(fmaxf(d0, a), b));
 }
+// landmask product of a difference (δ·mask_a·mask_b); LM = false: every cell is water
+template <bool LM>
+__device__ __forceinline__ float mk(float x, int ma, int mb) { return LM ? mulbf(mulbf(x, ma), mb) : x; }
+
 // adv_flux_x / adv_flux_y at a face from c[f-2], c[f-1], c[f], c[f+1] and the landmask there
+template <bool LM>
 __device__ __forceinline__ float flux_h(const FCu& f, float cm2, float cm1, float c0, float cp1,
                                         int lm2, int lm1, int l0, int lp1) {
-    if (f.tr > 0.0f) {
-        const float d0 = mulbf(mulbf(c0 - cm1, l0), lm1), dm = mulbf(mulbf(cm1 - cm2, lm1), lm2);
-        return f.tr * (cm1 + psid0(d0, dm, f));
-    }
-    if (f.tr < 0.0f) {
-        const float d0 = mulbf(mulbf(c0 - cm1, l0), lm1), dp = mulbf(mulbf(cp1 - c0, lp1), l0);
-        return f.tr * (c0 - psid0(d0, dp, f));
-    }
+    const float d0 = mk<LM>(c0 - cm1, l0, lm1);
+    if (f.tr > 0.0f) return f.tr * (cm1 + psid0(d0, mk<LM>(cm1 - cm2, lm1, lm2), f));
+    if (f.tr < 0.0f) return f.tr * (c0 - psid0(d0, mk<LM>(cp1 - c0, lp1, l0), f));
     return 0.0f;
 }
 // adv_flux_z at face k from c[k-2], c[k-1], c[k], c[k+1] (the index grows downward)
+template <bool LM>
 __device__ __forceinline__ float flux_v(const FCu& f, float cm2, float cm1, float c0, float cp1,
                                         int lm2, int lm1, int l0, int lp1) {
-    if (f.tr > 0.0f) {
-        const float d0 = mulbf(mulbf(cm1 - c0, l0), lm1), dp = mulbf(mulbf(c0 - cp1, lp1), l0);
-        return f.tr * (c0 + psid0(d0, dp, f));
-    }
-    if (f.tr < 0.0f) {
-        const float d0 = mulbf(mulbf(cm1 - c0, l0), lm1), dm = mulbf(mulbf(cm2 - cm1, lm1), lm2);
-        return f.tr * (cm1 - psid0(d0, dm, f));
-    }
+    const float d0 = mk<LM>(cm1 - c0, l0, lm1);
+    if (f.tr > 0.0f) return f.tr * (c0 + psid0(d0, mk<LM>(c0 - cp1, lp1, l0), f));
+    if (f.tr < 0.0f) return f.tr * (cm1 - psid0(d0, mk<LM>(cm2 - cm1, lm1, lm2), f));
     return 0.0f;
 }
 __device__ __forceinline__ int wrap_ax(int a, int N, int H, int topo) {
@@ -779,10 +775,8 @@ struct TrArgs {
 // shuffles). The face coefficients are computed once per face and shared by the 14 tracers.
 // Shared memory [row][tracer][lane]: TA (after x), FY (y face fluxes), TRs (tracer of the rows
 // the y sweep updates).
-template <int TY>
-__global__ void __launch_bounds__(32 * (TY + 4)) k32_xy(TrArgs a) {
-    if (stopped(a.err)) return;
-    extern __shared__ float sm[];
+template <int TY, bool LM>
+__device__ __forceinline__ void xy_tile(const TrArgs& a, const MemberDev& m, const int4 it, float* sm) {
     float* TA = sm;                                        // (TY+4) × 14 × 32
     float* FY = TA + (TY + 4) * PI_NTRACERS * 32;          // (TY+1) × 14 × 32
     float* TRs = FY + (TY + 1) * PI_NTRACERS * 32;         // TY × 14 × 32
@@ -790,215 +784,254 @@ __global__ void __launch_bounds__(32 * (TY + 4)) k32_xy(TrArgs a) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const long long G = a.Gtot;
     const float dT = a.dT;
+    const int i0 = it.y, j0 = it.z, L = it.w;
+    const long long off = m.cell_off;
+    const MemberForcing& F = a.F[it.x];
+    const float dz = a.dzF[m.dz_off + L - 1];
+    const float az = m.dx * m.dy, dtv = dT / (az * dz);
+    // ---- x sweep of row j0-2+wid
+    {
+        const int jj = wrap_ax(j0 - 2 + wid, m.Ny, m.Hy, m.ty);
+        const int i = i0 - 2 + lane;
+        const int ic = min(i, m.Gx);
+        const float ax = m.dy * dz;
+        const int q = gid3(m, ic, jj, L);
+        const float uw = F.vel1[0][q];
+        const float ue = __shfl_down_sync(0xffffffffu, uw, 1);
+        const FCu fc = fcu(uw, ax, 1.0f / m.dx, dT);
+        int l0 = 1, lm1 = 1, lm2 = 1, lp1 = 1;
+        if (LM) {
+            l0 = lm32(m, a.lm, ic, jj, L);
+            lm1 = __shfl_up_sync(0xffffffffu, l0, 1); lm2 = __shfl_up_sync(0xffffffffu, l0, 2);
+            lp1 = __shfl_down_sync(0xffffffffu, l0, 1);
+        }
+        const bool east_zero = i == m.Nx + m.Hx && m.tx != PI_PERIODIC;   // fill_halo_east_Gc! (Bounded)
+        const float ftr = mk<LM>(ax * ue - ax * uw, lp1, l0);
+        const bool store_tr = wid >= 2 && wid < TY + 2;
+        const float* src = a.tr + off + q;
+#pragma unroll
+        for (int n = 0; n < PI_NTRACERS; ++n) {
+            const float v = src[n * G];
+            const float cm2 = __shfl_up_sync(0xffffffffu, v, 2), cm1 = __shfl_up_sync(0xffffffffu, v, 1);
+            const float cp1 = __shfl_down_sync(0xffffffffu, v, 1);
+            const float Fw = flux_h<LM>(fc, cm2, cm1, v, cp1, lm2, lm1, l0, lp1);
+            float Fe = __shfl_down_sync(0xffffffffu, Fw, 1);
+            if (east_zero) Fe = 0.0f;
+            at(TA, wid, n, lane) = v - dtv * (mk<LM>(Fe - Fw, lp1, l0) - v * ftr);
+            if (store_tr) at(TRs, wid - 2, n, lane) = v;
+        }
+    }
+    __syncthreads();
+    // ---- y faces j0 + r, r = 0..TY
+    const int i = i0 - 2 + lane;
+    const bool col = lane >= 2 && lane < 30 && i <= m.Nx + m.Hx;
+    const float ay = m.dx * dz;
+    const float* vv = F.vel1[1];
+    if (wid <= TY) {
+        const int r = wid, f = j0 + r;
+        const bool special = f == m.Ny + m.Hy + 1;
+        const bool zero = !col || f > m.Ny + m.Hy + 1 || (special && m.ty != PI_PERIODIC);
+        const int fs = special ? m.Hy + 1 : min(f, m.Ny + m.Hy);
+        const int ic = min(i, m.Gx);
+        const FCu fc = fcu(zero ? 0.0f : vv[gid3(m, ic, fs, L)], ay, 1.0f / m.dy, dT);
+        int L2 = 1, L1 = 1, L0 = 1, Lp = 1;
+        if (LM) {
+            L2 = lm32(m, a.lm, ic, fs - 2, L); L1 = lm32(m, a.lm, ic, fs - 1, L);
+            L0 = lm32(m, a.lm, ic, fs, L); Lp = lm32(m, a.lm, ic, fs + 1, L);
+        }
+#pragma unroll
+        for (int n = 0; n < PI_NTRACERS; ++n)
+            at(FY, r, n, lane) = zero ? 0.0f : flux_h<LM>(fc, at(TA, r, n, lane), at(TA, r + 1, n, lane), at(TA, r + 2, n, lane),
+                                                          at(TA, r + 3, n, lane), L2, L1, L0, Lp);
+    }
+    __syncthreads();
+    // ---- y update of row j0 + wid
+    if (wid < TY) {
+        const int j = j0 + wid;
+        if (col && j <= m.Ny + m.Hy) {
+            const int q = gid3(m, i, j, L);
+            const int c0m = LM ? lm32(m, a.lm, i, j, L) : 1, cpm = LM ? lm32(m, a.lm, i, j + 1, L) : 1;
+            const float ftr = mk<LM>(ay * vv[q + m.Gx] - ay * vv[q], cpm, c0m);
+            float* dst = a.tb + off + q;
+#pragma unroll
+            for (int n = 0; n < PI_NTRACERS; ++n) {
+                const float dG = mk<LM>(at(FY, wid + 1, n, lane) - at(FY, wid, n, lane), cpm, c0m);
+                dst[n * G] = at(TA, wid + 2, n, lane) - dtv * (dG - at(TRs, wid, n, lane) * ftr);
+            }
+        }
+    }
+    __syncthreads();
+}
+
+template <int TY>
+__global__ void __launch_bounds__(32 * (TY + 4)) k32_xy(TrArgs a) {
+    if (stopped(a.err)) return;
+    extern __shared__ float sm[];
     for (int item = blockIdx.x; item < a.nitems; item += gridDim.x) {
         const int4 it = a.items[item];
         const MemberDev& m = a.T.md[it.x];
-        const int i0 = it.y, j0 = it.z, L = it.w;
-        const long long off = m.cell_off;
-        const MemberForcing& F = a.F[it.x];
-        const float dz = a.dzF[m.dz_off + L - 1];
-        const float az = m.dx * m.dy, dtv = dT / (az * dz);
-        // ---- x sweep of row j0-2+wid
-        {
-            const int jj = wrap_ax(j0 - 2 + wid, m.Ny, m.Hy, m.ty);
-            const int i = i0 - 2 + lane;
-            const int ic = min(i, m.Gx);
-            const float ax = m.dy * dz;
-            const float* u = F.vel1[0];
-            const int q = gid3(m, ic, jj, L);
-            const float uw = u[q];
-            const float ue = __shfl_down_sync(0xffffffffu, uw, 1);
-            const FCu fc = fcu(uw, ax, 1.0f / m.dx, dT);
-            const int l0 = lm32(m, a.lm, ic, jj, L);
-            const int lm1 = __shfl_up_sync(0xffffffffu, l0, 1), lm2 = __shfl_up_sync(0xffffffffu, l0, 2);
-            const int lp1 = __shfl_down_sync(0xffffffffu, l0, 1);
-            const bool east_zero = i == m.Nx + m.Hx && m.tx != PI_PERIODIC;   // fill_halo_east_Gc! (Bounded)
-            const float ftr = mulbf(mulbf(ax * ue - ax * uw, lp1), l0);
-            const bool store_tr = wid >= 2 && wid < TY + 2;
-#pragma unroll
-            for (int n = 0; n < PI_NTRACERS; ++n) {
-                const float v = a.tr[n * G + off + q];
-                const float cm2 = __shfl_up_sync(0xffffffffu, v, 2), cm1 = __shfl_up_sync(0xffffffffu, v, 1);
-                const float cp1 = __shfl_down_sync(0xffffffffu, v, 1);
-                const float Fw = flux_h(fc, cm2, cm1, v, cp1, lm2, lm1, l0, lp1);
-                float Fe = __shfl_down_sync(0xffffffffu, Fw, 1);
-                if (east_zero) Fe = 0.0f;
-                const float dG = mulbf(mulbf(Fe - Fw, lp1), l0);
-                at(TA, wid, n, lane) = v - dtv * (dG - v * ftr);
-                if (store_tr) at(TRs, wid - 2, n, lane) = v;
-            }
-        }
-        __syncthreads();
-        // ---- y faces j0 + r, r = 0..TY
-        const int i = i0 - 2 + lane;
-        const bool col = lane >= 2 && lane < 30 && i <= m.Nx + m.Hx;
-        const float ay = m.dx * dz;
-        const float* vv = F.vel1[1];
-        if (wid <= TY) {
-            const int r = wid, f = j0 + r;
-            const bool special = f == m.Ny + m.Hy + 1;
-            const bool zero = !col || f > m.Ny + m.Hy + 1 || (special && m.ty != PI_PERIODIC);
-            const int fs = special ? m.Hy + 1 : min(f, m.Ny + m.Hy);
-            const int ic = min(i, m.Gx);
-            const FCu fc = fcu(zero ? 0.0f : vv[gid3(m, ic, fs, L)], ay, 1.0f / m.dy, dT);
-            const int L2 = lm32(m, a.lm, ic, fs - 2, L), L1 = lm32(m, a.lm, ic, fs - 1, L);
-            const int L0 = lm32(m, a.lm, ic, fs, L), Lp = lm32(m, a.lm, ic, fs + 1, L);
-#pragma unroll
-            for (int n = 0; n < PI_NTRACERS; ++n)
-                at(FY, r, n, lane) = zero ? 0.0f : flux_h(fc, at(TA, r, n, lane), at(TA, r + 1, n, lane), at(TA, r + 2, n, lane),
-                                                          at(TA, r + 3, n, lane), L2, L1, L0, Lp);
-        }
-        __syncthreads();
-        // ---- y update of row j0 + wid
-        if (wid < TY) {
-            const int j = j0 + wid;
-            if (col && j <= m.Ny + m.Hy) {
-                const int q = gid3(m, i, j, L);
-                const int c0m = lm32(m, a.lm, i, j, L), cpm = lm32(m, a.lm, i, j + 1, L);
-                const float ftr = mulbf(mulbf(ay * vv[q + m.Gx] - ay * vv[q], cpm), c0m);
-#pragma unroll
-                for (int n = 0; n < PI_NTRACERS; ++n) {
-                    const float dG = mulbf(mulbf(at(FY, wid + 1, n, lane) - at(FY, wid, n, lane), cpm), c0m);
-                    a.tb[n * G + off + q] = at(TA, wid + 2, n, lane) - dtv * (dG - at(TRs, wid, n, lane) * ftr);
-                }
-            }
-        }
-        __syncthreads();
+        if (m.all_water) xy_tile<TY, false>(a, m, it, sm);
+        else xy_tile<TY, true>(a, m, it, sm);
     }
 }
 
 // z sweep and the rest of tracer_update! for LZ levels of 32 columns: warp y of the block takes
-// tracer y, each lane walks its column keeping the 4-level stencil window of tracer_temp and the
-// flux of the face above the current cell. The 14 warps walk the same cells, so the forcing terms'
-// reads of the other tracers at a cell hit the lines those warps load.
-template <int LZ>
-__global__ void __launch_bounds__(32 * PI_NTRACERS, 2) k32_ztail(TrArgs a) {
-    if (stopped(a.err)) return;
+// tracer y and each lane walks its column keeping the 4-level stencil window of tracer_temp and
+// the flux of the face above the current cell. The face coefficients, the vertical velocity and
+// the cell counts of the block's LZ levels are formed once in shared memory for the 14 tracer
+// warps; as the warps walk the same cells, the forcing terms' reads of the other tracers at a
+// cell hit lines already loaded.
+template <int LZ, bool LM>
+__device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& m, const int4 it, const float4* sFC,
+                                       const float* sW, const int* sPop) {
     const int lane = threadIdx.x, n = threadIdx.y;
     const long long G = a.Gtot;
     const float dT = a.dT;
+    const int i = it.y + lane, j = it.z, k0 = it.w;
+    if (i > m.Nx + m.Hx) return;
     const int64_t itn = a.st->iteration + 1;
     const int slot = acc_slot(n);
     const bool sinks = n == PI_PFe_inorg || n == PI_Dust || n == PI_PFe_bio;
+    const int top = m.Hz + 1, bot = m.Nz + m.Hz;
+    const int kend = min(k0 + LZ - 1, bot);
+    const long long off = m.cell_off;
+    const int slab = m.Gx * m.Gy;
+    const int qcol = gid3(m, i, j, 1);
+    const BgcDev32& b = a.bgc[it.x];
+    const float az = m.dx * m.dy;
+    const float* t = a.tb + n * G + off;
+    const float* c = a.tr + n * G + off;
+    auto lev = [&](int kk) { return qcol + (min(max(kk, top), bot) - 1) * slab; };
+    auto fcz = [&](int f) { const float4 v = sFC[(f - k0) * 32 + lane]; FCu r; r.tr = v.x; r.d0c = v.y; r.d1c = v.z; r.R = v.w; return r; };
+    auto lmz = [&](int kk) { return LM ? lm32(m, a.lm, i, j, kk) : 1; };
+    float w0 = t[lev(k0 - 2)], w1 = t[lev(k0 - 1)], w2 = t[lev(k0)], w3 = t[lev(k0 + 1)];
+    float Ft = flux_v<LM>(fcz(k0), w0, w1, w2, w3, lmz(k0 - 2), lmz(k0 - 1), lmz(k0), lmz(k0 + 1));
+    const float ws = n == PI_PFe_bio ? b.w_sink_org : b.w_sink_inorg;
+    float sink_prev = (sinks && k0 - 1 > m.Hz) ? c[qcol + (k0 - 2) * slab] : 0.0f;
+    for (int k = k0; k <= kend; ++k) {
+        const int f = k + 1;
+        const int q = qcol + (k - 1) * slab;
+        const long long cq = off + q;
+        const float cc = c[q];
+        const float nw_ = t[lev(k + 2)];
+        const int l1 = lmz(k), l0 = lmz(k + 1);
+        w0 = w1; w1 = w2; w2 = w3; w3 = nw_;
+        const float Fb = flux_v<LM>(fcz(f), w0, w1, w2, w3, lmz(f - 2), l1, l0, lmz(f + 1));   // zero at the bottom
+        const float dz = a.dzF[m.dz_off + k - 1];
+        const float volk = az * dz;
+        const float ftr = mk<LM>(az * sW[(k - k0) * 32 + lane] - az * sW[(f - k0) * 32 + lane], l0, l1);
+        float Gc = (w1 - dT / volk * (mk<LM>(Ft - Fb, l0, l1) - cc * ftr)) - cc;
+        Ft = Fb;
+        // tracer_diffusion! (tracer_diffusion.jl:1-21)
+        if (b.kappa_h != 0.0f || b.kappa_v != 0.0f) {
+            const float axk = m.dy * dz, ayk = m.dx * dz;
+            auto dx0 = [&](int ii) { return mulbf(mulbf(c[gid3(m, ii, j, k)] - c[gid3(m, ii - 1, j, k)], lm32(m, a.lm, ii, j, k)), lm32(m, a.lm, ii - 1, j, k)); };
+            auto dy0 = [&](int jj) { return mulbf(mulbf(c[gid3(m, i, jj, k)] - c[gid3(m, i, jj - 1, k)], lm32(m, a.lm, i, jj, k)), lm32(m, a.lm, i, jj - 1, k)); };
+            auto dz0 = [&](int kk) { return mulbf(mulbf(c[gid3(m, i, j, kk - 1)] - c[gid3(m, i, j, kk)], lm32(m, a.lm, i, j, kk)), lm32(m, a.lm, i, j, kk - 1)); };
+            const float fx1 = b.kappa_h * axk * (dx0(i + 1) / m.dx), fx0 = b.kappa_h * axk * (dx0(i) / m.dx);
+            const float fy1 = b.kappa_h * ayk * (dy0(j + 1) / m.dy), fy0 = b.kappa_h * ayk * (dy0(j) / m.dy);
+            const float fz0 = b.kappa_v * az * (dz0(k) / dz), fz1 = b.kappa_v * az * (dz0(k + 1) / a.dzF[m.dz_off + k]);
+            const float ax_ = mulbf(mulbf(fx1 - fx0, lm32(m, a.lm, i + 1, j, k)), l1);
+            const float ay_ = mulbf(mulbf(fy1 - fy0, lm32(m, a.lm, i, j + 1, k)), l1);
+            const float az_ = mulbf(mulbf(fz0 - fz1, l0), l1);
+            Gc += 1.0f / volk * (ax_ + ay_ + az_) * dT;
+        }
+        // tracer_sinking! (tracer_sinking.jl:1-42)
+        if (sinks) {
+            const float fup = (k - 1 <= m.Hz) ? 0.0f : ws * sink_prev;
+            const float fdn = (k >= bot) ? 0.0f : ws * cc;
+            Gc += (fup - fdn) / a.dzC[m.dz_off + k - m.Hz - 1] * dT;
+            sink_prev = cc;
+        }
+        // tracer_forcing! (tracer_forcings.jl:2-50) on max(0, tracer)
+        {
+            auto T = [&](int d) -> float { return d == n ? fmaxf(0.0f, cc) : fmaxf(0.0f, a.tr[d * G + cq]); };
+            float fo = 0.0f;
+            switch (n) {
+                case PI_DIC: fo = T(PI_DOC) * b.kDOC * dT; break;
+                case PI_DOC: fo = -T(PI_DOC) * b.kDOC * dT + T(PI_POC) * b.kPOC * dT; break;
+                case PI_POC: fo = -T(PI_POC) * b.kPOC * dT; break;
+                case PI_NH4: fo = T(PI_DON) * b.kDON * dT - T(PI_NH4) * b.Nit * dT; break;
+                case PI_NO3: fo = T(PI_NH4) * b.Nit * dT; break;
+                case PI_DON: fo = -T(PI_DON) * b.kDON * dT + T(PI_PON) * b.kPON * dT; break;
+                case PI_PON: fo = -T(PI_PON) * b.kPON * dT; break;
+                case PI_PO4: fo = T(PI_DOP) * b.kDOP * dT; break;
+                case PI_DOP: fo = -T(PI_DOP) * b.kDOP * dT + T(PI_POP) * b.kPOP * dT; break;
+                case PI_POP: fo = -T(PI_POP) * b.kPOP * dT; break;
+                case PI_DFe: {
+                    const float dfe = T(PI_DFe);
+                    const float fe = fmaxf(dfe - b.ligand, 0.0f) * dfe * b.DFeFrac * b.lambda_Fe * dT;
+                    fo = T(PI_PFe_bio) * b.kPOC * dT
+                       - (b.lambda_POC * T(PI_POC) + b.lambda_min + b.lambda_dust * T(PI_Dust)) * dfe * b.DFeFrac * dT
+                       + T(PI_PFe_inorg) * b.kdiss * dT - fe;
+                    break;
+                }
+                case PI_PFe_bio: fo = T(PI_POC) * T(PI_DFe) * b.DFeFrac * b.lambda_POC * dT - b.kPOC * T(PI_PFe_bio) * dT; break;
+                case PI_PFe_inorg: {
+                    const float dfe = T(PI_DFe);
+                    const float fe = fmaxf(dfe - b.ligand, 0.0f) * dfe * b.DFeFrac * b.lambda_Fe * dT;
+                    fo = -T(PI_PFe_inorg) * b.kdiss * dT + (b.lambda_min + b.lambda_dust * T(PI_Dust)) * dfe * b.DFeFrac * dT + fe;
+                    break;
+                }
+                default: break;
+            }
+            Gc += fo;
+        }
+        // apply_bcs! (apply_bcs.jl:4-98)
+        if (m.any_bc) {
+            const FluxBC32* B = a.bcs + m.bc_off + n * 6;
+            const int ii = i - m.Hx, jj = j - m.Hy, kk = k - m.Hz;
+            const float axk = m.dy * dz, ayk = m.dx * dz;
+            if (B[PI_WEST].kind && i == 1 + m.Hx) Gc += getbc32(B[PI_WEST], jj, kk, itn) * dT * axk / volk;
+            if (B[PI_EAST].kind && i == m.Nx + m.Hx) Gc -= getbc32(B[PI_EAST], jj, kk, itn) * dT * axk / volk;
+            if (B[PI_SOUTH].kind && j == 1 + m.Hy) Gc += getbc32(B[PI_SOUTH], ii, kk, itn) * dT * ayk / volk;
+            if (B[PI_NORTH].kind && j == m.Ny + m.Hy) Gc -= getbc32(B[PI_NORTH], ii, kk, itn) * dT * ayk / volk;
+            if (B[PI_BOTTOM].kind && k == bot) Gc += getbc32(B[PI_BOTTOM], ii, jj, itn) * dT * az / volk;
+            if (B[PI_TOP].kind && k == top) Gc -= getbc32(B[PI_TOP], ii, jj, itn) * dT * az / volk;
+        }
+        // particle terms from the fixed-point sums, apply_tendency! (tracer_update.jl:6-13)
+        float plk = 0.0f;
+        if (slot >= 0 && sPop[(k - k0) * 32 + lane] > 0) {
+            unsigned long long* pa = a.acc + (long long)slot * G + cq;
+            const long long vv = (long long)*pa;
+            if (vv) { *pa = 0ull; plk = (float)((double)vv * m.fx_unit); }
+        }
+        a.tr_next[n * G + cq] = cc + (Gc + plk / volk);
+    }
+}
+
+template <int LZ>
+__global__ void __launch_bounds__(32 * PI_NTRACERS, 2) k32_ztail(TrArgs a) {
+    if (stopped(a.err)) return;
+    __shared__ float4 sFC[(LZ + 1) * 32];   // faces k0 .. k0+LZ of the 32 columns
+    __shared__ float sW[(LZ + 1) * 32];     // vertical velocity at those faces
+    __shared__ int sPop[LZ * 32];           // individuals in the cells k0 .. k0+LZ-1
+    const int tid = threadIdx.y * 32 + threadIdx.x;
     for (int w = blockIdx.x; w < a.nitems; w += gridDim.x) {
         const int4 it = a.items[w];
         const MemberDev& m = a.T.md[it.x];
-        const int i = it.y + lane, j = it.z, k0 = it.w;
-        if (i > m.Nx + m.Hx) continue;
-        const int top = m.Hz + 1, bot = m.Nz + m.Hz;
-        const int kend = min(k0 + LZ - 1, bot);
-        const long long off = m.cell_off;
-        const int slab = m.Gx * m.Gy;
-        const int qcol = gid3(m, i, j, 1);
+        const int k0 = it.w, bot = m.Nz + m.Hz;
         const float* wv = a.F[it.x].vel1[2];
-        const BgcDev32& b = a.bgc[it.x];
         const float az = m.dx * m.dy;
-        const float* t = a.tb + n * G + off;
-        const float* c = a.tr + n * G + off;
-        auto lev = [&](int kk) { return qcol + (min(max(kk, top), bot) - 1) * slab; };
-        float w0 = t[lev(k0 - 2)], w1 = t[lev(k0 - 1)], w2 = t[lev(k0)], w3 = t[lev(k0 + 1)];
-        float wtop = wv[qcol + (k0 - 1) * slab];
-        float Ft = flux_v(fcu(wtop, az, a.rdzC[m.dz_off + k0 - 1], dT), w0, w1, w2, w3,
-                          lm32(m, a.lm, i, j, k0 - 2), lm32(m, a.lm, i, j, k0 - 1), lm32(m, a.lm, i, j, k0),
-                          lm32(m, a.lm, i, j, k0 + 1));
-        const float ws = n == PI_PFe_bio ? b.w_sink_org : b.w_sink_inorg;
-        float sink_prev = (sinks && k0 - 1 > m.Hz) ? c[qcol + (k0 - 2) * slab] : 0.0f;
-        for (int k = k0; k <= kend; ++k) {
-            const int f = k + 1;
-            const int q = qcol + (k - 1) * slab;
-            const long long cq = off + q;
-            const float cc = c[q];
-            const float nw_ = t[lev(k + 2)];
-            const float wbot = wv[qcol + (f - 1) * slab];
-            const bool bottom = f == bot + 1;                  // fill_halo_bottom_Gc! (Bounded)
-            const int l2 = lm32(m, a.lm, i, j, f - 2), l1 = lm32(m, a.lm, i, j, f - 1);
-            const int l0 = lm32(m, a.lm, i, j, f), lp = lm32(m, a.lm, i, j, f + 1);
-            w0 = w1; w1 = w2; w2 = w3; w3 = nw_;
-            const float Fb = bottom ? 0.0f : flux_v(fcu(wbot, az, a.rdzC[m.dz_off + f - 1], dT), w0, w1, w2, w3, l2, l1, l0, lp);
-            const float dz = a.dzF[m.dz_off + k - 1];
-            const float volk = az * dz;
-            const int c0m = l1, cpm = l0;                      // landmask at k and k+1
-            const float ftr = mulbf(mulbf(az * wtop - az * wbot, cpm), c0m);
-            const float dG = mulbf(mulbf(Ft - Fb, cpm), c0m);
-            float Gc = (w1 - dT / volk * (dG - cc * ftr)) - cc;
-            Ft = Fb;
-            wtop = wbot;
-            // tracer_diffusion! (tracer_diffusion.jl:1-21)
-            if (b.kappa_h != 0.0f || b.kappa_v != 0.0f) {
-                const float axk = m.dy * dz, ayk = m.dx * dz;
-                auto dx0 = [&](int ii) { return mulbf(mulbf(c[gid3(m, ii, j, k)] - c[gid3(m, ii - 1, j, k)], lm32(m, a.lm, ii, j, k)), lm32(m, a.lm, ii - 1, j, k)); };
-                auto dy0 = [&](int jj) { return mulbf(mulbf(c[gid3(m, i, jj, k)] - c[gid3(m, i, jj - 1, k)], lm32(m, a.lm, i, jj, k)), lm32(m, a.lm, i, jj - 1, k)); };
-                auto dz0 = [&](int kk) { return mulbf(mulbf(c[gid3(m, i, j, kk - 1)] - c[gid3(m, i, j, kk)], lm32(m, a.lm, i, j, kk)), lm32(m, a.lm, i, j, kk - 1)); };
-                const float fx1 = b.kappa_h * axk * (dx0(i + 1) / m.dx), fx0 = b.kappa_h * axk * (dx0(i) / m.dx);
-                const float fy1 = b.kappa_h * ayk * (dy0(j + 1) / m.dy), fy0 = b.kappa_h * ayk * (dy0(j) / m.dy);
-                const float fz0 = b.kappa_v * az * (dz0(k) / dz), fz1 = b.kappa_v * az * (dz0(k + 1) / a.dzF[m.dz_off + k]);
-                const float ax_ = mulbf(mulbf(fx1 - fx0, lm32(m, a.lm, i + 1, j, k)), c0m);
-                const float ay_ = mulbf(mulbf(fy1 - fy0, lm32(m, a.lm, i, j + 1, k)), c0m);
-                const float az_ = mulbf(mulbf(fz0 - fz1, cpm), c0m);
-                Gc += 1.0f / volk * (ax_ + ay_ + az_) * dT;
-            }
-            // tracer_sinking! (tracer_sinking.jl:1-42)
-            if (sinks) {
-                const float fup = (k - 1 <= m.Hz) ? 0.0f : ws * sink_prev;
-                const float fdn = (k >= bot) ? 0.0f : ws * cc;
-                Gc += (fup - fdn) / a.dzC[m.dz_off + k - m.Hz - 1] * dT;
-                sink_prev = cc;
-            }
-            // tracer_forcing! (tracer_forcings.jl:2-50) on max(0, tracer)
-            {
-                auto T = [&](int d) -> float { return d == n ? fmaxf(0.0f, cc) : fmaxf(0.0f, a.tr[d * G + cq]); };
-                float fo = 0.0f;
-                switch (n) {
-                    case PI_DIC: fo = T(PI_DOC) * b.kDOC * dT; break;
-                    case PI_DOC: fo = -T(PI_DOC) * b.kDOC * dT + T(PI_POC) * b.kPOC * dT; break;
-                    case PI_POC: fo = -T(PI_POC) * b.kPOC * dT; break;
-                    case PI_NH4: fo = T(PI_DON) * b.kDON * dT - T(PI_NH4) * b.Nit * dT; break;
-                    case PI_NO3: fo = T(PI_NH4) * b.Nit * dT; break;
-                    case PI_DON: fo = -T(PI_DON) * b.kDON * dT + T(PI_PON) * b.kPON * dT; break;
-                    case PI_PON: fo = -T(PI_PON) * b.kPON * dT; break;
-                    case PI_PO4: fo = T(PI_DOP) * b.kDOP * dT; break;
-                    case PI_DOP: fo = -T(PI_DOP) * b.kDOP * dT + T(PI_POP) * b.kPOP * dT; break;
-                    case PI_POP: fo = -T(PI_POP) * b.kPOP * dT; break;
-                    case PI_DFe: {
-                        const float dfe = T(PI_DFe);
-                        const float fe = fmaxf(dfe - b.ligand, 0.0f) * dfe * b.DFeFrac * b.lambda_Fe * dT;
-                        fo = T(PI_PFe_bio) * b.kPOC * dT
-                           - (b.lambda_POC * T(PI_POC) + b.lambda_min + b.lambda_dust * T(PI_Dust)) * dfe * b.DFeFrac * dT
-                           + T(PI_PFe_inorg) * b.kdiss * dT - fe;
-                        break;
-                    }
-                    case PI_PFe_bio: fo = T(PI_POC) * T(PI_DFe) * b.DFeFrac * b.lambda_POC * dT - b.kPOC * T(PI_PFe_bio) * dT; break;
-                    case PI_PFe_inorg: {
-                        const float dfe = T(PI_DFe);
-                        const float fe = fmaxf(dfe - b.ligand, 0.0f) * dfe * b.DFeFrac * b.lambda_Fe * dT;
-                        fo = -T(PI_PFe_inorg) * b.kdiss * dT + (b.lambda_min + b.lambda_dust * T(PI_Dust)) * dfe * b.DFeFrac * dT + fe;
-                        break;
-                    }
-                    default: break;
+        for (int e = tid; e < (LZ + 1) * 32; e += 32 * PI_NTRACERS) {
+            const int f = k0 + e / 32, i = it.y + (e & 31);
+            float4 fc = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            float wf = 0.0f;
+            if (i <= m.Nx + m.Hx && f <= bot + 1) {
+                wf = wv[gid3(m, i, it.z, f)];
+                if (f <= bot) {                               // fill_halo_bottom_Gc!: zero flux at the bottom
+                    const FCu c = fcu(wf, az, a.rdzC[m.dz_off + f - 1], a.dT);
+                    fc = make_float4(c.tr, c.d0c, c.d1c, c.R);
                 }
-                Gc += fo;
             }
-            // apply_bcs! (apply_bcs.jl:4-98)
-            if (m.any_bc) {
-                const FluxBC32* B = a.bcs + m.bc_off + n * 6;
-                const int ii = i - m.Hx, jj = j - m.Hy, kk = k - m.Hz;
-                const float axk = m.dy * dz, ayk = m.dx * dz;
-                if (B[PI_WEST].kind && i == 1 + m.Hx) Gc += getbc32(B[PI_WEST], jj, kk, itn) * dT * axk / volk;
-                if (B[PI_EAST].kind && i == m.Nx + m.Hx) Gc -= getbc32(B[PI_EAST], jj, kk, itn) * dT * axk / volk;
-                if (B[PI_SOUTH].kind && j == 1 + m.Hy) Gc += getbc32(B[PI_SOUTH], ii, kk, itn) * dT * ayk / volk;
-                if (B[PI_NORTH].kind && j == m.Ny + m.Hy) Gc -= getbc32(B[PI_NORTH], ii, kk, itn) * dT * ayk / volk;
-                if (B[PI_BOTTOM].kind && k == bot) Gc += getbc32(B[PI_BOTTOM], ii, jj, itn) * dT * az / volk;
-                if (B[PI_TOP].kind && k == top) Gc -= getbc32(B[PI_TOP], ii, jj, itn) * dT * az / volk;
-            }
-            // particle terms from the fixed-point sums, apply_tendency! (tracer_update.jl:6-13)
-            float plk = 0.0f;
-            if (slot >= 0 && a.pop[cq] > 0) {
-                unsigned long long* pa = a.acc + (long long)slot * G + cq;
-                const long long vv = (long long)*pa;
-                if (vv) { *pa = 0ull; plk = (float)((double)vv * m.fx_unit); }
-            }
-            a.tr_next[n * G + cq] = cc + (Gc + plk / volk);
+            sFC[e] = fc;
+            sW[e] = wf;
+            if (e < LZ * 32) sPop[e] = (i <= m.Nx + m.Hx && f <= bot) ? a.pop[m.cell_off + gid3(m, i, it.z, f)] : 0;
         }
+        __syncthreads();
+        if (m.all_water) z_walk<LZ, false>(a, m, it, sFC, sW, sPop);
+        else z_walk<LZ, true>(a, m, it, sFC, sW, sPop);
+        __syncthreads();
     }
 }
 
