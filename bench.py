@@ -329,13 +329,15 @@ def run_ours(args):
                  "refreshed every 60 steps, dt=30 s")
         scaling = "weak"
     elif args.workload == "config4":
+        from PlanktonIndividuals.batch import member_cost, shard_members
         allm = W.config4()
-        members = allm[rank::ws]
+        members = [allm[q] for q in shard_members([member_cost(w) for w in allm], ws)[rank]]
         wdesc = "config4: 64 members, grids U{64..256}^2 x U{16..32}, populations 2^U(14,20), 1 species, dt=30 s"
         scaling = "strong"
     else:
+        from PlanktonIndividuals.batch import member_cost, shard_members
         allm = W.config5()
-        members = allm[rank::ws]
+        members = [allm[q] for q in shard_members([member_cost(w) for w in allm], ws)[rank]]
         wdesc = "config5: 4096 0D boxes, populations 2^U(8,13), no advection, per-box light phase, dt=60 s"
         scaling = "strong"
     r32 = run_fp32(members, args, dist, local, Clocks)

@@ -306,3 +306,24 @@ class BatchMember:
 
     def set_state(self, individuals, tracers):
         self.batch.set_state(self.m, individuals, tracers)
+
+
+def shard_members(costs, world_size):
+    """Split ensemble members over `world_size` ranks with balanced work: members sorted by cost
+    (largest first) go, one by one, to the rank with the least total so far (ties: lowest rank).
+    `costs` are per-member work estimates (individuals + interior cells). Returns, per rank, the
+    sorted list of member indices. Deterministic, so every rank computes the same partition
+    without communicating."""
+    order = sorted(range(len(costs)), key=lambda m: (-costs[m], m))
+    load = [0.0] * world_size
+    parts = [[] for _ in range(world_size)]
+    for m in order:
+        r = min(range(world_size), key=lambda q: (load[q], q))
+        parts[r].append(m)
+        load[r] += costs[m]
+    return [sorted(p) for p in parts]
+
+
+def member_cost(wl):
+    """Work estimate of a member: active individuals plus interior cells."""
+    return float(sum(wl.N)) + float(wl.grid.Nx * wl.grid.Ny * wl.grid.Nz)
