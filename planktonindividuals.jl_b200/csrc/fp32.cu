@@ -461,6 +461,7 @@ pi_status check_errors(pi_batch* b) {
     }
     BK(cudaStreamSynchronize(b->stream), "synchronize");
     if (e & F32_ERR_FORCING) return bfail(b, PI_ERR_SHAPE, "BoundsError: forcing snapshot not provided for the step time");
+    if (e & F32_ERR_LISTS) return bfail(b, PI_ERR_STATE, "internal error: a division list entry outside its segment");
     return bfail(b, PI_ERR_DOMAIN, "an individual left the halo-padded grid (cell index out of range)");
 }
 
@@ -710,8 +711,10 @@ pi_status pi_batch_set_individuals(pi_batch* b, int32_t member, int32_t sp, cons
             if (!(x >= 0.0 && x <= (double)N[a])) return bfail(b, PI_ERR_PARAM, "pi_set_individuals: position outside [0, N] of an active individual");
             double fl = std::floor(x);
             c[a] = (int)fl;
+            // keep the cell of the FP64 position: an offset that rounds up to 1 becomes the
+            // largest float below 1 instead of moving to the next cell
             float of = (float)(x - fl);
-            if (of >= 1.0f) { c[a] += 1; of = 0.0f; }
+            if (of >= 1.0f) of = 0x1.fffffep-1f;
             o[a][i] = of;
         }
         cell[i] = c[0] + (g.Nx + 1) * (c[1] + (g.Ny + 1) * c[2]);

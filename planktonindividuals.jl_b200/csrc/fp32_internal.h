@@ -25,6 +25,7 @@
 #define F32_ERR_DOMAIN   1u
 #define F32_ERR_CAPACITY 2u
 #define F32_ERR_FORCING  4u
+#define F32_ERR_LISTS    8u     // a division list entry outside its segment (access skipped)
 
 // Slots are processed in tiles of this many consecutive slots of one (member, species) segment.
 #define F32_TILE 1024

@@ -493,7 +493,7 @@ __global__ void k32_assign(Tab32 T, IndDev32 P, const unsigned long long* __rest
 // copy_daughter_individuals! and divide_to_half! (division_death.jl:28-63). Grid: (x, segments).
 __global__ void k32_daughters(Tab32 T, IndDev32 P, const int* __restrict__ divlist,
                               const int* __restrict__ freelist, const uint32_t* __restrict__ ndiv,
-                              const uint32_t* err) {
+                              uint32_t* err) {
     if (stopped(err)) return;
     const int seg = blockIdx.y;
     int mi, s;
@@ -502,7 +502,9 @@ __global__ void k32_daughters(Tab32 T, IndDev32 P, const int* __restrict__ divli
     const long long base = m.slot_off + (long long)s * m.C;
     const uint32_t n = ndiv[seg];
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const long long p = base + divlist[base + k], d = base + freelist[base + k];
+        const int pl = divlist[base + k], dl = freelist[base + k];
+        if (k >= (uint32_t)m.C || pl < 0 || pl >= m.C || dl < 0 || dl >= m.C) { seterr(err, F32_ERR_LISTS); continue; }
+        const long long p = base + pl, d = base + dl;
         // the daughter's slot keeps the cell find_inds! gave it this step
         const int32_t cd = P.cell[d];
         int32_t sc;

@@ -243,3 +243,22 @@ def test_fp32_budget_matches_downloaded_fields(gpu_lib):
         d = batch.get_individuals(0, s)
         C += float(np.sum((d["Bm"] + d["Cq"])[d["ac"]]))
     assert bud["ind_C"] == pytest.approx(C, rel=1e-6)
+
+
+def test_fp32_position_just_below_a_cell_face(gpu_lib):
+    """An uploaded position within an FP32 rounding of the next cell face (z = 1 − 2e-9 in a
+    one-level box) keeps the cell the Float64 position has, and later steps stay in the grid."""
+    wl = W.config5(n_max=1)[0]
+    d = wl.individuals[0]
+    N = wl.N[0]
+    d["z"][:N] = np.minimum(d["z"][:N], 0.5)
+    d["z"][0] = 1.0 - 2e-9
+    d["x"][1] = 1.0 - 1e-9
+    ref, f32 = oracle.from_workload(wl), fp32_model(gpu_lib, wl)
+    vel = VelCache(wl)
+    drive(ref, wl, 5, vel)
+    drive(f32, wl, 5, vel)
+    A, B = ref.get_individuals(0), f32.get_individuals(0)
+    assert np.array_equal(A["ac"], B["ac"])
+    for k in ("xi", "yi", "zi"):
+        assert np.array_equal(A[k][A["ac"]], B[k][B["ac"]]), k
