@@ -21,6 +21,11 @@ the FP32 batched form; the members are split across ranks (scaling "strong").
 Multi-GPU (config 2): the model domain is not partitioned; each rank runs an independent replica
 (scaling "weak") and `value` sums the replicas' individual-steps over the slowest rank's time.
 
+--accuracy reports each output's error of the FP32 batched form against the FP64 form, which the
+GPU parity tests show to be bit-identical to the CPU oracle: config 2 over --acc-steps steps
+(population counts every 100 steps, active-slot and cell mismatches, quota and position errors,
+interior tracer-mass errors) or, with --workload config5, --acc-boxes boxes over 2880 steps.
+
 --impl reference times the reference algorithm's CPU implementation: the reference is Julia
 (absent here), so this is the CPU oracle (a Float64 restatement of TimeStep!) with all host
 threads, on a bounded sample of the same workload (a 128×128×64 sub-domain with the same
@@ -57,6 +62,10 @@ def parse():
     ap.add_argument("--tune-steps", type=int, default=2)
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--accuracy", action="store_true",
+                    help="report the FP32 form's errors against the FP64 form (bit-exact to the CPU oracle)")
+    ap.add_argument("--acc-steps", type=int, default=1000)
+    ap.add_argument("--acc-boxes", type=int, default=16)
     return ap.parse_args()
 
 
@@ -396,6 +405,111 @@ def run_ours(args):
     return out
 
 
+# ------------------------------------------------------------------------------------------
+# FP32 form against the FP64 form (the FP64 form equals the CPU oracle bit for bit)
+# ------------------------------------------------------------------------------------------
+
+def interior_mass(get, g):
+    from PlanktonIndividuals import _abi
+    vol = float(g.Δx) * float(g.Δy) * np.asarray(g.dzF)[g.Hz:g.Hz + g.Nz]
+    out = {}
+    for n, name in enumerate(_abi.tracer_names):
+        a = get(n)[g.Hx:g.Hx + g.Nx, g.Hy:g.Hy + g.Ny, g.Hz:g.Hz + g.Nz]
+        out[name] = float(np.sum(a * vol[None, None, :]))
+    return out
+
+
+def mass_rel(M32, M64):
+    return {k: (abs(M32[k] - M64[k]) / abs(M64[k]) if M64[k] else abs(M32[k])) for k in M64}
+
+
+def fp64_sim(lib, wl, steps):
+    import ctypes as ct
+    from PlanktonIndividuals import _abi
+    from PlanktonIndividuals._native import CModel
+    m = CModel(lib, "pi_", wl.grid, wl.bgc, wl.phyt, wl.nsp, wl.capacity, wl.seed, precision=_abi.PI_FP64)
+    m.set_state(wl.individuals, wl.tracers)
+    nsnap = wl.snapshots_needed(steps + 1)
+    vv = series_arrays(wl, nsnap)
+    u, v, w = (np.asfortranarray(vv[c]) for c in "uvw")
+    dp = lambda a: a.ctypes.data_as(ct.POINTER(ct.c_double))
+    sim = ct.c_void_p()
+    rc = lib.pi_sim_create(m.h, wl.dT, 1, dp(u), dp(v), dp(w), nsnap, wl.dT_vel, dp(wl.parf), wl.parf.shape[2],
+                           wl.dT_PAR, dp(wl.temp), wl.temp.shape[3], wl.dT_temp, ct.byref(sim))
+    assert rc == 0, m._errmsg(m.h)
+    return m, sim, (u, v, w)
+
+
+def fp32_batch(members, steps):
+    from PlanktonIndividuals.batch import Member, PlanktonBatch
+    b = PlanktonBatch([Member(w.grid, w.bgc, w.phyt, w.capacity, w.seed) for w in members], nspecies=members[0].nsp)
+    for m, wl in enumerate(members):
+        b.set_state(m, wl.individuals, wl.tracers)
+        b.set_series(m, vels=series_arrays(wl, wl.snapshots_needed(steps + 1)), ΔT_vel=wl.dT_vel, PARF=wl.parf,
+                     ΔT_PAR=wl.dT_PAR, temp=wl.temp, ΔT_temp=wl.dT_temp)
+    return b
+
+
+def run_accuracy(args):
+    from PlanktonIndividuals import _lib, workloads as W
+    lib = _lib.load()
+    t0 = time.time()
+    if args.workload == "config5":
+        boxes = W.config5(n_max=args.acc_boxes)
+        steps = boxes[0].steps
+        b = fp32_batch(boxes, steps)
+        b.step(boxes[0].dT, steps)
+        c32 = [b.count_active(m, 0) for m in range(len(boxes))]
+        c64, mass = [], []
+        for m, wl in enumerate(boxes):
+            mm, sim, keep = fp64_sim(lib, wl, steps)
+            for _ in range(steps):
+                lib.pi_sim_update(sim, 0, 0)
+            assert lib.pi_synchronize(mm.h) == 0, mm._errmsg(mm.h)
+            c64.append(mm.count_active(0))
+            mass.append(max(mass_rel(interior_mass(lambda n: b.get_tracer(m, n), wl.grid),
+                                     interior_mass(mm.get_tracer, wl.grid)).values()))
+            lib.pi_sim_destroy(sim)
+            mm.close()
+        n0 = [wl.N[0] for wl in boxes]
+        return {"accuracy": "config5", "boxes": len(boxes), "steps": steps, "initial": n0, "fp32": c32, "fp64": c64,
+                "boxes_with_equal_counts": int(sum(int(a == c) for a, c in zip(c32, c64))),
+                "max_count_diff": int(max(abs(a - c) for a, c in zip(c32, c64))),
+                "mean_growth_factor": round(float(np.mean(np.array(c64) / np.array(n0))), 4),
+                "max_tracer_mass_rel_err": float(max(mass)), "seconds": round(time.time() - t0, 1)}
+    wl = W.config2(seed=2)
+    steps = args.acc_steps
+    m64, sim, keep = fp64_sim(lib, wl, steps)
+    b = fp32_batch([wl], steps)
+    hist = []
+    for s0 in range(0, steps, 100):
+        n = min(100, steps - s0)
+        for _ in range(n):
+            assert lib.pi_sim_update(sim, 0, 0) == 0, m64._errmsg(m64.h)
+        assert lib.pi_synchronize(m64.h) == 0, m64._errmsg(m64.h)
+        b.step(wl.dT, n)
+        hist.append({"step": s0 + n, "fp64": [m64.count_active(s) for s in range(wl.nsp)],
+                     "fp32": [b.count_active(0, s) for s in range(wl.nsp)]})
+    rel = mass_rel(interior_mass(lambda n: b.get_tracer(0, n), wl.grid), interior_mass(m64.get_tracer, wl.grid))
+    inds = {}
+    for s in range(wl.nsp):
+        A, B = m64.get_individuals(s), b.get_individuals(0, s)
+        both = A["ac"] & B["ac"]
+        inds[f"sp{s}"] = {
+            "ac_mismatch": int(np.sum(A["ac"] != B["ac"])),
+            "cell_mismatch": int(np.sum(both & ((A["xi"] != B["xi"]) | (A["yi"] != B["yi"]) | (A["zi"] != B["zi"])))),
+            "quota_rel_max": {k: float(np.max(np.abs(A[k][both] - B[k][both]) / np.abs(A[k][both])))
+                              for k in ("Bm", "Cq", "Nq", "Pq", "Chl")},
+            "z_abs_max": float(np.max(np.abs(A["z"][both] - B["z"][both])))}
+    out = {"accuracy": "config2", "steps": steps, "counts_equal_at_every_check": all(h["fp64"] == h["fp32"] for h in hist),
+           "counts": hist, "tracer_mass_rel_err": rel, "max_tracer_mass_rel_err": max(rel.values()),
+           "individuals": inds, "budget_fp32": b.budget(0), "seconds": round(time.time() - t0, 1)}
+    b.close()
+    lib.pi_sim_destroy(sim)
+    m64.close()
+    return out
+
+
 def cpu_sample_workload():
     from PlanktonIndividuals import workloads as W
     # bounded sample of config2: a 128×128×64 sub-domain with the same individual density
@@ -459,7 +573,10 @@ def run_reference(args):
 
 def main():
     args = parse()
-    out = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if args.accuracy:
+        out = run_accuracy(args)
+    else:
+        out = run_reference(args) if args.impl == "reference" else run_ours(args)
     if out is not None:
         print(json.dumps(out))
 
