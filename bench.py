@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--tune-steps", type=int, default=2)
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nx", type=int, default=256, help="config 2 horizontal size (smaller for profiling)")
+    ap.add_argument("--nz", type=int, default=64)
+    ap.add_argument("--n-per-species", type=int, default=2_097_152)
     ap.add_argument("--accuracy", action="store_true",
                     help="report the FP32 form's errors against the FP64 form (bit-exact to the CPU oracle)")
     ap.add_argument("--acc-steps", type=int, default=1000)
@@ -333,9 +336,9 @@ def run_ours(args):
         dist.init_process_group("nccl", device_id=torch.device("cuda", local))
     lib = _lib.load()
     if args.workload == "config2":
-        members = [W.config2(seed=2 + rank)]
-        wdesc = ("config2: 256x256x64 grid, 2 species x 2,097,152 individuals, random-Fourier velocity "
-                 "refreshed every 60 steps, dt=30 s")
+        members = [W.config2(nx=args.nx, nz=args.nz, N_per_species=args.n_per_species, seed=2 + rank)]
+        wdesc = (f"config2: {args.nx}x{args.nx}x{args.nz} grid, 2 species x {args.n_per_species:,} individuals, "
+                 f"random-Fourier velocity refreshed every 60 steps, dt=30 s")
         scaling = "weak"
     elif args.workload == "config4":
         from PlanktonIndividuals.batch import member_cost, shard_members
