@@ -344,7 +344,7 @@ __device__ __forceinline__ void move_one(const MoveArgs& a, const MemberDev& m, 
     is_div = dv2; is_free = !ac2;
 }
 
-__global__ void k32_move(MoveArgs a) {
+__global__ void __launch_bounds__(256, 3) k32_move(MoveArgs a) {
     if (stopped(a.err)) return;
     __shared__ unsigned int sh_d, sh_f;
     const int bs = blockDim.x, ppt = F32_TILE / bs;
@@ -659,7 +659,7 @@ __device__ __forceinline__ void phys_one(const PhysArgs& a, const MemberDev& m, 
     atomicAdd(&a.dcnt[(long long)s * 4 * G + cq], 1u);      // diags num at the (possibly stale) cell
 }
 
-__global__ void k32_physiology(PhysArgs a) {
+__global__ void __launch_bounds__(256, 4) k32_physiology(PhysArgs a) {
     if (stopped(a.err)) return;
     const int bs = blockDim.x, ppt = F32_TILE / bs;
     const uint32_t iter = (uint32_t)(a.st->iteration + 1);
