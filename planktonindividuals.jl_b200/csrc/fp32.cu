@@ -395,9 +395,16 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
         {
             a.items = b->xy_items; a.nitems = b->nxy_items;
             BScope sc(b, "k32_xy");
-            const unsigned grid = (unsigned)std::max(1, b->nxy_items);
-            if (b->tune.ty == 16) k32_xy<16><<<grid, 32 * 20, xy_smem(16), s>>>(a);
-            else if (b->tune.ty == 8) k32_xy<8><<<grid, 32 * 12, xy_smem(8), s>>>(a);
+            // persistent: as many blocks as fit at once, each looping over items with the next
+            // item's loads in flight
+            int per_sm = 1;
+            const int ty = b->tune.ty;
+            if (ty == 16) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k32_xy<16>, 32 * 20, xy_smem(16));
+            else if (ty == 8) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k32_xy<8>, 32 * 12, xy_smem(8));
+            else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k32_xy<4>, 32 * 8, xy_smem(4));
+            const unsigned grid = (unsigned)std::max(1, std::min(b->nxy_items, std::max(1, per_sm) * b->nsm));
+            if (ty == 16) k32_xy<16><<<grid, 32 * 20, xy_smem(16), s>>>(a);
+            else if (ty == 8) k32_xy<8><<<grid, 32 * 12, xy_smem(8), s>>>(a);
             else k32_xy<4><<<grid, 32 * 8, xy_smem(4), s>>>(a);
         }
         {

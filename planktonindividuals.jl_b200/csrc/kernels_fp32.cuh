@@ -777,8 +777,23 @@ struct TrArgs {
 // shuffles). The face coefficients are computed once per face and shared by the 14 tracers.
 // Shared memory [row][tracer][lane]: TA (after x), FY (y face fluxes), TRs (tracer of the rows
 // the y sweep updates).
+// The x-sweep inputs of one item for this thread (its row and column): u and the 14 tracers.
+// A block loops over items and loads the next item's inputs while it works on the current one.
+__device__ __forceinline__ void xy_load(const TrArgs& a, int item, float& u, float* v) {
+    const int4 it = a.items[item];
+    const MemberDev& m = a.T.md[it.x];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int jj = wrap_ax(it.z - 2 + wid, m.Ny, m.Hy, m.ty);
+    const int q = gid3(m, min(it.y - 2 + lane, m.Gx), jj, it.w);
+    u = a.F[it.x].vel1[0][q];
+    const float* __restrict__ src = a.tr + m.cell_off + q;
+#pragma unroll
+    for (int n = 0; n < PI_NTRACERS; ++n) v[n] = src[n * a.Gtot];
+}
+
 template <int TY, bool LM>
-__device__ __forceinline__ void xy_tile(const TrArgs& a, const MemberDev& m, const int4 it, float* sm) {
+__device__ __forceinline__ void xy_tile(const TrArgs& a, const MemberDev& m, const int4 it, float* sm,
+                                        float& pu, float* pv, int next) {
     float* TA = sm;                                        // (TY+4) × 14 × 32
     float* FY = TA + (TY + 4) * PI_NTRACERS * 32;          // (TY+1) × 14 × 32
     float* TRs = FY + (TY + 1) * PI_NTRACERS * 32;         // TY × 14 × 32
@@ -797,8 +812,7 @@ __device__ __forceinline__ void xy_tile(const TrArgs& a, const MemberDev& m, con
         const int i = i0 - 2 + lane;
         const int ic = min(i, m.Gx);
         const float ax = m.dy * dz;
-        const int q = gid3(m, ic, jj, L);
-        const float uw = F.vel1[0][q];
+        const float uw = pu;
         const float ue = __shfl_down_sync(0xffffffffu, uw, 1);
         const FCu fc = fcu(uw, ax, 1.0f / m.dx, dT);
         int l0 = 1, lm1 = 1, lm2 = 1, lp1 = 1;
@@ -810,10 +824,9 @@ __device__ __forceinline__ void xy_tile(const TrArgs& a, const MemberDev& m, con
         const bool east_zero = i == m.Nx + m.Hx && m.tx != PI_PERIODIC;   // fill_halo_east_Gc! (Bounded)
         const float ftr = mk<LM>(ax * ue - ax * uw, lp1, l0);
         const bool store_tr = wid >= 2 && wid < TY + 2;
-        const float* src = a.tr + off + q;
 #pragma unroll
         for (int n = 0; n < PI_NTRACERS; ++n) {
-            const float v = src[n * G];
+            const float v = pv[n];
             const float cm2 = __shfl_up_sync(0xffffffffu, v, 2), cm1 = __shfl_up_sync(0xffffffffu, v, 1);
             const float cp1 = __shfl_down_sync(0xffffffffu, v, 1);
             const float Fw = flux_h<LM>(fc, cm2, cm1, v, cp1, lm2, lm1, l0, lp1);
@@ -824,6 +837,8 @@ __device__ __forceinline__ void xy_tile(const TrArgs& a, const MemberDev& m, con
         }
     }
     __syncthreads();
+    // the registers of this item's x inputs are free: start the next item's loads
+    if (next < a.nitems) xy_load(a, next, pu, pv);
     // ---- y faces j0 + r, r = 0..TY
     const int i = i0 - 2 + lane;
     const bool col = lane >= 2 && lane < 30 && i <= m.Nx + m.Hx;
@@ -869,11 +884,15 @@ template <int TY>
 __global__ void __launch_bounds__(32 * (TY + 4)) k32_xy(TrArgs a) {
     if (stopped(a.err)) return;
     extern __shared__ float sm[];
+    if ((int)blockIdx.x >= a.nitems) return;
+    float pu, pv[PI_NTRACERS];
+    xy_load(a, blockIdx.x, pu, pv);
     for (int item = blockIdx.x; item < a.nitems; item += gridDim.x) {
         const int4 it = a.items[item];
         const MemberDev& m = a.T.md[it.x];
-        if (m.all_water) xy_tile<TY, false>(a, m, it, sm);
-        else xy_tile<TY, true>(a, m, it, sm);
+        const int next = item + gridDim.x;
+        if (m.all_water) xy_tile<TY, false>(a, m, it, sm, pu, pv, next);
+        else xy_tile<TY, true>(a, m, it, sm, pu, pv, next);
     }
 }
 
@@ -901,8 +920,10 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& m, cons
     const int qcol = gid3(m, i, j, 1);
     const BgcDev32& b = a.bgc[it.x];
     const float az = m.dx * m.dy;
-    const float* t = a.tb + n * G + off;
-    const float* c = a.tr + n * G + off;
+    const float* __restrict__ t = a.tb + n * G + off;
+    const float* __restrict__ c = a.tr + n * G + off;
+    const float* __restrict__ trall = a.tr;
+    float* __restrict__ out = a.tr_next + n * G;
     auto lev = [&](int kk) { return qcol + (min(max(kk, top), bot) - 1) * slab; };
     auto fcz = [&](int f) { const float4 v = sFC[(f - k0) * 32 + lane]; FCu r; r.tr = v.x; r.d0c = v.y; r.d1c = v.z; r.R = v.w; return r; };
     auto lmz = [&](int kk) { return LM ? lm32(m, a.lm, i, j, kk) : 1; };
@@ -910,12 +931,15 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& m, cons
     float Ft = flux_v<LM>(fcz(k0), w0, w1, w2, w3, lmz(k0 - 2), lmz(k0 - 1), lmz(k0), lmz(k0 + 1));
     const float ws = n == PI_PFe_bio ? b.w_sink_org : b.w_sink_inorg;
     float sink_prev = (sinks && k0 - 1 > m.Hz) ? c[qcol + (k0 - 2) * slab] : 0.0f;
+    // the two loads of each level are issued one level ahead
+    float cc_next = c[qcol + (k0 - 1) * slab], nw_next = t[lev(k0 + 2)];
     for (int k = k0; k <= kend; ++k) {
         const int f = k + 1;
         const int q = qcol + (k - 1) * slab;
         const long long cq = off + q;
-        const float cc = c[q];
-        const float nw_ = t[lev(k + 2)];
+        const float cc = cc_next;
+        const float nw_ = nw_next;
+        if (k < kend) { cc_next = c[q + slab]; nw_next = t[lev(k + 3)]; }
         const int l1 = lmz(k), l0 = lmz(k + 1);
         w0 = w1; w1 = w2; w2 = w3; w3 = nw_;
         const float Fb = flux_v<LM>(fcz(f), w0, w1, w2, w3, lmz(f - 2), l1, l0, lmz(f + 1));   // zero at the bottom
@@ -947,7 +971,7 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& m, cons
         }
         // tracer_forcing! (tracer_forcings.jl:2-50) on max(0, tracer)
         {
-            auto T = [&](int d) -> float { return d == n ? fmaxf(0.0f, cc) : fmaxf(0.0f, a.tr[d * G + cq]); };
+            auto T = [&](int d) -> float { return d == n ? fmaxf(0.0f, cc) : fmaxf(0.0f, trall[d * G + cq]); };
             float fo = 0.0f;
             switch (n) {
                 case PI_DIC: fo = T(PI_DOC) * b.kDOC * dT; break;
@@ -998,7 +1022,7 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& m, cons
             const long long vv = (long long)*pa;
             if (vv) { *pa = 0ull; plk = (float)((double)vv * m.fx_unit); }
         }
-        a.tr_next[n * G + cq] = cc + (Gc + plk / volk);
+        out[cq] = cc + (Gc + plk / volk);
     }
 }
 
