@@ -64,7 +64,7 @@ struct Tuning {
     int bs_move = 256, bs_phys = 256, bs_assign = 256;
     int persist_move = 0, persist_phys = 0;   // 0: one tile per block; k: k blocks per SM, looping
     int ty = 8;                               // rows of an x-y tracer tile (4, 8 or 16)
-    int lz = 16;                              // levels walked by a z thread (8, 16 or 32)
+    int lz = 32;                              // levels walked by a z thread (8, 16 or 32)
     int wpb_par = 4;
 };
 

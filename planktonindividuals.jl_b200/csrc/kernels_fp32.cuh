@@ -398,10 +398,19 @@ __global__ void k32_par(Tab32 T, const float* __restrict__ dzF, const BgcDev32* 
         const float kc = bgc[it.x].kc, kw = bgc[it.x].kw;
         const long long fcol = m.col_off + (i - 1) + (long long)m.Nx * (j - 1);
         float parf = PARF[fcol];
+        const long long c1 = m.cell_off + gid3(m, i + m.Hx, j + m.Hy, 1 + m.Hz);
+        const long long slab = (long long)m.Gx * m.Gy;
+        // the loads of a level are issued one level ahead (only PARF carries down the column)
+        long long v_n = (long long)chl_acc[c1];
+        int pp_n = pop[c1];
+        float dp_n = diag_par[c1];
         for (int k = 1; k <= m.Nz; ++k) {
             const int kk = k + m.Hz;
-            const long long c = m.cell_off + gid3(m, i + m.Hx, j + m.Hy, kk);
-            const long long v = (long long)chl_acc[c];
+            const long long c = c1 + (k - 1) * slab;
+            const long long v = v_n;
+            const int pp = pp_n;
+            const float dp = dp_n;
+            if (k < m.Nz) { v_n = (long long)chl_acc[c + slab]; pp_n = pop[c + slab]; dp_n = diag_par[c + slab]; }
             if (v) chl_acc[c] = 0ull;
             const float chl = (float)((double)v * m.chl_unit);
             const float dz = dzF[m.dz_off + kk - 1];
@@ -411,8 +420,7 @@ __global__ void k32_par(Tab32 T, const float* __restrict__ dzF, const BgcDev32* 
             const float pv = parf * (1.0f - e) / atten;
             par[c] = pv;
             parf = parf * e;
-            diag_par[c] += pv;
-            const int pp = pop[c];
+            diag_par[c] = dp + pv;
             if (pp > 0) {
                 env[2 * c] = make_float4(tr[PI_NH4 * Gtot + c], tr[PI_NO3 * Gtot + c], tr[PI_PO4 * Gtot + c],
                                          tr[PI_DOC * Gtot + c]);
