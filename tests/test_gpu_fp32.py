@@ -123,6 +123,65 @@ def test_fp32_config2_small_3d_vs_oracle(gpu_lib):
     check_errors(errors_vs_oracle(ref, f32, wl))
 
 
+def _fp32_pair(lib, wl, steps, setup=None):
+    ref, f32 = oracle.from_workload(wl), fp32_model(lib, wl)
+    if setup:
+        setup(ref); setup(f32)
+    vel = VelCache(wl)
+    drive(ref, wl, steps, vel)
+    drive(f32, wl, steps, vel)
+    check_errors(errors_vs_oracle(ref, f32, wl))
+
+
+def test_fp32_landmask_2d_vs_oracle(gpu_lib):
+    from test_gpu_parity_edge import OVER, regrid
+    from PlanktonIndividuals.grids import RectilinearGrid
+    wl = W.config1(n=24, N=1200, steps=30, capacity=4000, phyt_over=OVER)
+    lm = np.ones((24, 24, 1), dtype=bool)
+    lm[5:9, 3:20, :] = False
+    lm[15:17, 10:12, :] = False
+    wl = regrid(wl, RectilinearGrid(size=(24, 24, 1), x=(0.0, 24e3), y=(0.0, 24e3), z=(0.0, -10.0),
+                                    FT=np.float64, landmask=lm))
+    _fp32_pair(gpu_lib, wl, 30)
+
+
+def test_fp32_landmask_3d_vs_oracle(gpu_lib):
+    from test_gpu_parity_edge import OVER, landmask_3d
+    wl = landmask_3d(daylight(W.config2(nx=16, nz=10, N_per_species=900, nsp=1, steps=15, nmodes=12,
+                                        phyt_over=OVER)))
+    _fp32_pair(gpu_lib, wl, 15)
+
+
+def test_fp32_bounded_xy_vs_oracle(gpu_lib):
+    from test_gpu_parity_edge import OVER, regrid
+    from PlanktonIndividuals.grids import Bounded, RectilinearGrid
+    wl = W.config1(n=20, N=900, steps=25, capacity=3000, phyt_over=OVER)
+    wl = regrid(wl, RectilinearGrid(size=(20, 20, 1), x=(0.0, 20e3), y=(0.0, 20e3), z=(0.0, -10.0),
+                                    FT=np.float64, topology=(Bounded, Bounded, Bounded)))
+    _fp32_pair(gpu_lib, wl, 25)
+
+
+def test_fp32_flux_bcs_vs_oracle(gpu_lib):
+    wl = daylight(W.config2(nx=12, nz=6, N_per_species=500, nsp=1, steps=12, nmodes=12))
+    g = wl.grid
+    rng = np.random.default_rng(0)
+    west = np.asfortranarray(rng.uniform(0, 1e-3, (g.Ny, g.Nz)))
+    bottom = np.asfortranarray(rng.uniform(0, 1e-5, (g.Nx, g.Ny, 20)))
+
+    def setup(m):
+        m.set_flux_bc(_abi.tracer_names.index("NO3"), _abi.FACES["top"], _abi.PI_BC_CONST, [1e-4])
+        m.set_flux_bc(_abi.tracer_names.index("DIC"), _abi.FACES["west"], _abi.PI_BC_ARRAY2D, west)
+        m.set_flux_bc(_abi.tracer_names.index("DON"), _abi.FACES["bottom"], _abi.PI_BC_ARRAY3D, bottom, 20)
+    _fp32_pair(gpu_lib, wl, 12, setup)
+
+
+def test_fp32_diffusion_vs_oracle(gpu_lib):
+    from test_gpu_parity_edge import DIFFUSION, OVER
+    wl = daylight(W.config2(nx=12, nz=8, N_per_species=700, nsp=1, steps=15, nmodes=12, phyt_over=OVER))
+    wl.bgc.update(DIFFUSION)
+    _fp32_pair(gpu_lib, wl, 15)
+
+
 def _members(wls):
     return [Member(wl.grid, wl.bgc, wl.phyt, wl.capacity, wl.seed) for wl in wls]
 

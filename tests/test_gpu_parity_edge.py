@@ -1,5 +1,5 @@
-"""Edge cases of the FP64 step, GPU vs oracle with tolerance 0: land mask, Bounded x/y, flux
-boundary conditions, per-species grazing, the Timer and Sizer_Timer division types, capacity
+"""Edge cases of the FP64 step, GPU vs oracle with tolerance 0: land mask (2D and 3D), Bounded
+x/y, flux boundary conditions, tracer and individual diffusion, per-species grazing, the Timer and Sizer_Timer division types, capacity
 overflow, N steps = N/2 + N/2 (checkpoint/resume), and the device-resident update! path."""
 import ctypes as ct
 
@@ -87,6 +87,43 @@ def test_flux_bcs_bitexact(gpu_lib):
         rng = np.random.default_rng(0)
     vel = VelCache(wl)
     drive(ref, wl, 12, vel); drive(gpu, wl, 12, vel)
+    assert compare_states(ref, gpu, 1) == []
+
+
+def landmask_3d(wl, seed=5):
+    """The workload on the same geometry with land: a sloping bottom (deep cells of the western
+    columns) and a block of land through the upper levels; tracers rebuilt on the masked grid."""
+    g = wl.grid
+    lm = np.ones((g.Nx, g.Ny, g.Nz), dtype=bool)
+    for i in range(g.Nx // 2):
+        lm[i, :, g.Nz - 1 - (g.Nx // 2 - i) * g.Nz // g.Nx:] = False
+    lm[g.Nx // 2:g.Nx // 2 + 3, 2:g.Ny - 3, :g.Nz // 2] = False
+    wl.grid = RectilinearGrid(size=(g.Nx, g.Ny, g.Nz), x=(0.0, g.Nx * float(g.Δx)), y=(0.0, g.Ny * float(g.Δy)),
+                              z=(0.0, -float(np.sum(np.asarray(g.dzF)[g.Hz:g.Hz + g.Nz]))), FT=np.float64,
+                              topology=(Periodic, Periodic, Bounded), landmask=lm)
+    wl.tracers = W.make_tracers(wl.grid, np.random.default_rng(seed), no3_gradient_depth=2.0 * g.Nz)
+    return wl
+
+
+DIFFUSION = {"κh": 1.0, "κv": 1e-3, "κhP": 0.5, "κvP": 2e-4}
+
+
+def test_landmask_3d_bitexact(gpu_lib):
+    wl = landmask_3d(daylight(W.config2(nx=16, nz=10, N_per_species=900, nsp=1, steps=15, nmodes=12,
+                                        phyt_over=OVER)))
+    ref, gpu = pair(gpu_lib, wl)
+    vel = VelCache(wl)
+    drive(ref, wl, 15, vel); drive(gpu, wl, 15, vel)
+    assert compare_states(ref, gpu, 1) == []
+
+
+def test_diffusion_bitexact(gpu_lib):
+    """tracer_diffusion! (κh, κv) and the individuals' random walk (κhP, κvP) switched on."""
+    wl = daylight(W.config2(nx=12, nz=8, N_per_species=700, nsp=1, steps=15, nmodes=12, phyt_over=OVER))
+    wl.bgc.update(DIFFUSION)
+    ref, gpu = pair(gpu_lib, wl)
+    vel = VelCache(wl)
+    drive(ref, wl, 15, vel); drive(gpu, wl, 15, vel)
     assert compare_states(ref, gpu, 1) == []
 
 
