@@ -906,131 +906,151 @@ __global__ void __launch_bounds__(32 * (TY + 4)) k32_xy(TrArgs a) {
 
 // z sweep and the rest of tracer_update! for LZ levels of 32 columns: warp y of the block takes
 // tracer y and each lane walks its column keeping the 4-level stencil window of tracer_temp and
-// the flux of the face above the current cell. The face coefficients, the vertical velocity and
-// the cell counts of the block's LZ levels are formed once in shared memory for the 14 tracer
-// warps; as the warps walk the same cells, the forcing terms' reads of the other tracers at a
-// cell hit lines already loaded.
+// the flux of the face above the current cell. What does not depend on the tracer is formed once
+// per item in shared memory for the 14 tracer warps: the face coefficients, the vertical
+// transport term of each cell, the cell counts and the per-level constants (ΔT/vol, ΔT/ΔzC and
+// the fixed-point unit per volume). As the warps walk the same cells, the forcing terms' reads of
+// the other tracers at a cell hit lines already loaded.
+struct ZLev {
+    float dtv;      // ΔT / (Δx Δy ΔzF[k])
+    float sk;       // ΔT / ΔzC (tracer_sinking!)
+    float dz;       // ΔzF[k]
+    float dzn;      // ΔzF[k+1]
+    double fxv;     // mmol per fixed-point unit / (Δx Δy ΔzF[k])
+};
+
+// tracer_forcing! (tracer_forcings.jl:2-50) of the three iron tracers on max(0, tracer)
+__device__ __forceinline__ float fe_forcing(int n, const BgcDev32& b, float dT, float dfe, float poc,
+                                            float dust, float pfeb, float pfei) {
+    if (n == PI_DFe) {
+        const float fe = fmaxf(dfe - b.ligand, 0.0f) * dfe * b.DFeFrac * b.lambda_Fe * dT;
+        return pfeb * b.kPOC * dT - (b.lambda_POC * poc + b.lambda_min + b.lambda_dust * dust) * dfe * b.DFeFrac * dT
+             + pfei * b.kdiss * dT - fe;
+    }
+    if (n == PI_PFe_bio) return poc * dfe * b.DFeFrac * b.lambda_POC * dT - b.kPOC * pfeb * dT;
+    const float fe = fmaxf(dfe - b.ligand, 0.0f) * dfe * b.DFeFrac * b.lambda_Fe * dT;
+    return -pfei * b.kdiss * dT + (b.lambda_min + b.lambda_dust * dust) * dfe * b.DFeFrac * dT + fe;
+}
+
 template <int LZ, bool LM>
-__device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& m, const int4 it, const float4* sFC,
-                                       const float* sW, const int* sPop) {
+__device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& md, const int4 it, const float4* sFC,
+                                       const float* sFtr, const int* sPop, const ZLev* sLev) {
     const int lane = threadIdx.x, n = threadIdx.y;
-    const long long G = a.Gtot;
-    const float dT = a.dT;
+    // member constants in registers: the stores of the walk could otherwise alias them
+    const int Nx = md.Nx, Hx = md.Hx, Hz = md.Hz, Gx = md.Gx, Gy = md.Gy;
     const int i = it.y + lane, j = it.z, k0 = it.w;
-    if (i > m.Nx + m.Hx) return;
-    const int64_t itn = a.st->iteration + 1;
+    if (i > Nx + Hx) return;
+    const long long G = a.Gtot, off = md.cell_off;
+    const float dT = a.dT;
+    const int slab = Gx * Gy;
+    const int top = Hz + 1, bot = md.Nz + Hz;
+    const int kend = min(k0 + LZ - 1, bot);
+    const int qcol = (i - 1) + Gx * (j - 1);             // level 1 of the column, member-local
+    const BgcDev32& b = a.bgc[it.x];
     const int slot = acc_slot(n);
     const bool sinks = n == PI_PFe_inorg || n == PI_Dust || n == PI_PFe_bio;
-    const int top = m.Hz + 1, bot = m.Nz + m.Hz;
-    const int kend = min(k0 + LZ - 1, bot);
-    const long long off = m.cell_off;
-    const int slab = m.Gx * m.Gy;
-    const int qcol = gid3(m, i, j, 1);
-    const BgcDev32& b = a.bgc[it.x];
-    const float az = m.dx * m.dy;
+    const float ws = n == PI_PFe_bio ? b.w_sink_org : b.w_sink_inorg;
+    const bool diffuse = b.kappa_h != 0.0f || b.kappa_v != 0.0f;
+    const bool any_bc = md.any_bc != 0;
+    // tracer_forcing! of the ten nutrient tracers: aS·T(n) + aO·T(dO)
+    float aS = 0.0f, aO = 0.0f;
+    int dO = -1;
+    switch (n) {
+        case PI_DIC: dO = PI_DOC; aO = b.kDOC * dT; break;
+        case PI_DOC: aS = -b.kDOC * dT; dO = PI_POC; aO = b.kPOC * dT; break;
+        case PI_POC: aS = -b.kPOC * dT; break;
+        case PI_NH4: aS = -b.Nit * dT; dO = PI_DON; aO = b.kDON * dT; break;
+        case PI_NO3: dO = PI_NH4; aO = b.Nit * dT; break;
+        case PI_DON: aS = -b.kDON * dT; dO = PI_PON; aO = b.kPON * dT; break;
+        case PI_PON: aS = -b.kPON * dT; break;
+        case PI_PO4: dO = PI_DOP; aO = b.kDOP * dT; break;
+        case PI_DOP: aS = -b.kDOP * dT; dO = PI_POP; aO = b.kPOP * dT; break;
+        case PI_POP: aS = -b.kPOP * dT; break;
+        default: break;
+    }
+    const bool iron = n == PI_DFe || n == PI_PFe_bio || n == PI_PFe_inorg;
     const float* __restrict__ t = a.tb + n * G + off;
     const float* __restrict__ c = a.tr + n * G + off;
-    const float* __restrict__ trall = a.tr;
-    float* __restrict__ out = a.tr_next + n * G;
-    auto lev = [&](int kk) { return qcol + (min(max(kk, top), bot) - 1) * slab; };
-    auto fcz = [&](int f) { const float4 v = sFC[(f - k0) * 32 + lane]; FCu r; r.tr = v.x; r.d0c = v.y; r.d1c = v.z; r.R = v.w; return r; };
-    auto lmz = [&](int kk) { return LM ? lm32(m, a.lm, i, j, kk) : 1; };
-    float w0 = t[lev(k0 - 2)], w1 = t[lev(k0 - 1)], w2 = t[lev(k0)], w3 = t[lev(k0 + 1)];
-    float Ft = flux_v<LM>(fcz(k0), w0, w1, w2, w3, lmz(k0 - 2), lmz(k0 - 1), lmz(k0), lmz(k0 + 1));
-    const float ws = n == PI_PFe_bio ? b.w_sink_org : b.w_sink_inorg;
-    float sink_prev = (sinks && k0 - 1 > m.Hz) ? c[qcol + (k0 - 2) * slab] : 0.0f;
-    // the two loads of each level are issued one level ahead
-    float cc_next = c[qcol + (k0 - 1) * slab], nw_next = t[lev(k0 + 2)];
-    for (int k = k0; k <= kend; ++k) {
-        const int f = k + 1;
-        const int q = qcol + (k - 1) * slab;
-        const long long cq = off + q;
-        const float cc = cc_next;
-        const float nw_ = nw_next;
-        if (k < kend) { cc_next = c[q + slab]; nw_next = t[lev(k + 3)]; }
-        const int l1 = lmz(k), l0 = lmz(k + 1);
-        w0 = w1; w1 = w2; w2 = w3; w3 = nw_;
-        const float Fb = flux_v<LM>(fcz(f), w0, w1, w2, w3, lmz(f - 2), l1, l0, lmz(f + 1));   // zero at the bottom
-        const float dz = a.dzF[m.dz_off + k - 1];
-        const float volk = az * dz;
-        const float ftr = mk<LM>(az * sW[(k - k0) * 32 + lane] - az * sW[(f - k0) * 32 + lane], l0, l1);
-        float Gc = (w1 - dT / volk * (mk<LM>(Ft - Fb, l0, l1) - cc * ftr)) - cc;
+    const float* __restrict__ trm = a.tr + off;           // all tracers of the member
+    const float* __restrict__ co = trm + (dO < 0 ? 0 : dO) * G;
+    float* __restrict__ out = a.tr_next + n * G + off;
+    unsigned long long* __restrict__ acc = a.acc + (slot < 0 ? 0 : slot) * G + off;
+    const uint8_t* __restrict__ lmc = a.lm + off + qcol;
+    auto tl = [&](int kk) { return t[qcol + (min(max(kk, top), bot) - 1) * slab]; };
+    auto lmk = [&](int kk) -> int { return LM ? (int)lmc[(kk - 1) * slab] : 1; };
+    auto fcz = [&](int l) { const float4 v = sFC[l * 32 + lane]; FCu r; r.tr = v.x; r.d0c = v.y; r.d1c = v.z; r.R = v.w; return r; };
+    // stencil windows: w (tracer_temp) and mm (land mask) at levels k-1 .. k+2 of the current cell k
+    float w0 = tl(k0 - 2), w1 = tl(k0 - 1), w2 = tl(k0), w3 = tl(k0 + 1);
+    int mm0 = lmk(k0 - 2), mm1 = lmk(k0 - 1), mm2 = lmk(k0), mm3 = lmk(k0 + 1);
+    float Ft = flux_v<LM>(fcz(0), w0, w1, w2, w3, mm0, mm1, mm2, mm3);
+    int q = qcol + (k0 - 1) * slab;
+    float sink_prev = (sinks && k0 - 1 > Hz) ? c[q - slab] : 0.0f;
+    // the loads of each level are issued one level ahead
+    float cc_next = c[q], nw_next = tl(k0 + 2);
+    for (int k = k0; k <= kend; ++k, q += slab) {
+        const int l = k - k0;
+        const float cc = cc_next, nw = nw_next;
+        if (k < kend) { cc_next = c[q + slab]; nw_next = tl(k + 3); }
+        w0 = w1; w1 = w2; w2 = w3; w3 = nw;
+        if (LM) { mm0 = mm1; mm1 = mm2; mm2 = mm3; mm3 = lmk(k + 2); }
+        const int l1 = mm1, l0 = mm2;                       // land mask of cell k and k+1
+        const float Fb = flux_v<LM>(fcz(l + 1), w0, w1, w2, w3, mm0, mm1, mm2, mm3);   // zero at the bottom
+        const ZLev L = sLev[l];
+        float Gc = (w1 - L.dtv * (mk<LM>(Ft - Fb, l0, l1) - cc * sFtr[l * 32 + lane])) - cc;
         Ft = Fb;
         // tracer_diffusion! (tracer_diffusion.jl:1-21)
-        if (b.kappa_h != 0.0f || b.kappa_v != 0.0f) {
-            const float axk = m.dy * dz, ayk = m.dx * dz;
-            auto dx0 = [&](int ii) { return mulbf(mulbf(c[gid3(m, ii, j, k)] - c[gid3(m, ii - 1, j, k)], lm32(m, a.lm, ii, j, k)), lm32(m, a.lm, ii - 1, j, k)); };
-            auto dy0 = [&](int jj) { return mulbf(mulbf(c[gid3(m, i, jj, k)] - c[gid3(m, i, jj - 1, k)], lm32(m, a.lm, i, jj, k)), lm32(m, a.lm, i, jj - 1, k)); };
-            auto dz0 = [&](int kk) { return mulbf(mulbf(c[gid3(m, i, j, kk - 1)] - c[gid3(m, i, j, kk)], lm32(m, a.lm, i, j, kk)), lm32(m, a.lm, i, j, kk - 1)); };
-            const float fx1 = b.kappa_h * axk * (dx0(i + 1) / m.dx), fx0 = b.kappa_h * axk * (dx0(i) / m.dx);
-            const float fy1 = b.kappa_h * ayk * (dy0(j + 1) / m.dy), fy0 = b.kappa_h * ayk * (dy0(j) / m.dy);
-            const float fz0 = b.kappa_v * az * (dz0(k) / dz), fz1 = b.kappa_v * az * (dz0(k + 1) / a.dzF[m.dz_off + k]);
-            const float ax_ = mulbf(mulbf(fx1 - fx0, lm32(m, a.lm, i + 1, j, k)), l1);
-            const float ay_ = mulbf(mulbf(fy1 - fy0, lm32(m, a.lm, i, j + 1, k)), l1);
+        if (diffuse) {
+            const float dz = L.dz, az = md.dx * md.dy, volk = az * dz;
+            const float axk = md.dy * dz, ayk = md.dx * dz;
+            auto lmq = [&](int dq) -> int { return LM ? (int)lmc[(k - 1) * slab + dq] : 1; };
+            auto dif = [&](int dq, int dp) { return mulbf(mulbf(c[q + dq] - c[q + dp], lmq(dq)), lmq(dp)); };
+            const float fx1 = b.kappa_h * axk * (dif(1, 0) / md.dx), fx0 = b.kappa_h * axk * (dif(0, -1) / md.dx);
+            const float fy1 = b.kappa_h * ayk * (dif(Gx, 0) / md.dy), fy0 = b.kappa_h * ayk * (dif(0, -Gx) / md.dy);
+            const float fz0 = b.kappa_v * az * (dif(-slab, 0) / dz), fz1 = b.kappa_v * az * (dif(0, slab) / L.dzn);
+            const float ax_ = mulbf(mulbf(fx1 - fx0, lmq(1)), l1);
+            const float ay_ = mulbf(mulbf(fy1 - fy0, lmq(Gx)), l1);
             const float az_ = mulbf(mulbf(fz0 - fz1, l0), l1);
             Gc += 1.0f / volk * (ax_ + ay_ + az_) * dT;
         }
         // tracer_sinking! (tracer_sinking.jl:1-42)
         if (sinks) {
-            const float fup = (k - 1 <= m.Hz) ? 0.0f : ws * sink_prev;
+            const float fup = (k - 1 <= Hz) ? 0.0f : ws * sink_prev;
             const float fdn = (k >= bot) ? 0.0f : ws * cc;
-            Gc += (fup - fdn) / a.dzC[m.dz_off + k - m.Hz - 1] * dT;
+            Gc += (fup - fdn) * L.sk;
             sink_prev = cc;
         }
         // tracer_forcing! (tracer_forcings.jl:2-50) on max(0, tracer)
-        {
-            auto T = [&](int d) -> float { return d == n ? fmaxf(0.0f, cc) : fmaxf(0.0f, trall[d * G + cq]); };
-            float fo = 0.0f;
-            switch (n) {
-                case PI_DIC: fo = T(PI_DOC) * b.kDOC * dT; break;
-                case PI_DOC: fo = -T(PI_DOC) * b.kDOC * dT + T(PI_POC) * b.kPOC * dT; break;
-                case PI_POC: fo = -T(PI_POC) * b.kPOC * dT; break;
-                case PI_NH4: fo = T(PI_DON) * b.kDON * dT - T(PI_NH4) * b.Nit * dT; break;
-                case PI_NO3: fo = T(PI_NH4) * b.Nit * dT; break;
-                case PI_DON: fo = -T(PI_DON) * b.kDON * dT + T(PI_PON) * b.kPON * dT; break;
-                case PI_PON: fo = -T(PI_PON) * b.kPON * dT; break;
-                case PI_PO4: fo = T(PI_DOP) * b.kDOP * dT; break;
-                case PI_DOP: fo = -T(PI_DOP) * b.kDOP * dT + T(PI_POP) * b.kPOP * dT; break;
-                case PI_POP: fo = -T(PI_POP) * b.kPOP * dT; break;
-                case PI_DFe: {
-                    const float dfe = T(PI_DFe);
-                    const float fe = fmaxf(dfe - b.ligand, 0.0f) * dfe * b.DFeFrac * b.lambda_Fe * dT;
-                    fo = T(PI_PFe_bio) * b.kPOC * dT
-                       - (b.lambda_POC * T(PI_POC) + b.lambda_min + b.lambda_dust * T(PI_Dust)) * dfe * b.DFeFrac * dT
-                       + T(PI_PFe_inorg) * b.kdiss * dT - fe;
-                    break;
-                }
-                case PI_PFe_bio: fo = T(PI_POC) * T(PI_DFe) * b.DFeFrac * b.lambda_POC * dT - b.kPOC * T(PI_PFe_bio) * dT; break;
-                case PI_PFe_inorg: {
-                    const float dfe = T(PI_DFe);
-                    const float fe = fmaxf(dfe - b.ligand, 0.0f) * dfe * b.DFeFrac * b.lambda_Fe * dT;
-                    fo = -T(PI_PFe_inorg) * b.kdiss * dT + (b.lambda_min + b.lambda_dust * T(PI_Dust)) * dfe * b.DFeFrac * dT + fe;
-                    break;
-                }
-                default: break;
-            }
+        if (!iron) {
+            float fo = aS * fmaxf(0.0f, cc);
+            if (dO >= 0) fo += aO * fmaxf(0.0f, co[q]);
             Gc += fo;
+        } else {
+            const float dfe = fmaxf(0.0f, trm[PI_DFe * G + q]), poc = fmaxf(0.0f, trm[PI_POC * G + q]);
+            const float dust = fmaxf(0.0f, trm[PI_Dust * G + q]);
+            const float pfeb = fmaxf(0.0f, trm[PI_PFe_bio * G + q]), pfei = fmaxf(0.0f, trm[PI_PFe_inorg * G + q]);
+            Gc += fe_forcing(n, b, dT, dfe, poc, dust, pfeb, pfei);
         }
         // apply_bcs! (apply_bcs.jl:4-98)
-        if (m.any_bc) {
-            const FluxBC32* B = a.bcs + m.bc_off + n * 6;
-            const int ii = i - m.Hx, jj = j - m.Hy, kk = k - m.Hz;
-            const float axk = m.dy * dz, ayk = m.dx * dz;
-            if (B[PI_WEST].kind && i == 1 + m.Hx) Gc += getbc32(B[PI_WEST], jj, kk, itn) * dT * axk / volk;
-            if (B[PI_EAST].kind && i == m.Nx + m.Hx) Gc -= getbc32(B[PI_EAST], jj, kk, itn) * dT * axk / volk;
-            if (B[PI_SOUTH].kind && j == 1 + m.Hy) Gc += getbc32(B[PI_SOUTH], ii, kk, itn) * dT * ayk / volk;
-            if (B[PI_NORTH].kind && j == m.Ny + m.Hy) Gc -= getbc32(B[PI_NORTH], ii, kk, itn) * dT * ayk / volk;
+        if (any_bc) {
+            const int64_t itn = a.st->iteration + 1;
+            const FluxBC32* B = a.bcs + md.bc_off + n * 6;
+            const int ii = i - Hx, jj = j - md.Hy, kk = k - Hz;
+            const float dz = L.dz, az = md.dx * md.dy, volk = az * dz;
+            const float axk = md.dy * dz, ayk = md.dx * dz;
+            if (B[PI_WEST].kind && i == 1 + Hx) Gc += getbc32(B[PI_WEST], jj, kk, itn) * dT * axk / volk;
+            if (B[PI_EAST].kind && i == Nx + Hx) Gc -= getbc32(B[PI_EAST], jj, kk, itn) * dT * axk / volk;
+            if (B[PI_SOUTH].kind && j == 1 + md.Hy) Gc += getbc32(B[PI_SOUTH], ii, kk, itn) * dT * ayk / volk;
+            if (B[PI_NORTH].kind && j == md.Ny + md.Hy) Gc -= getbc32(B[PI_NORTH], ii, kk, itn) * dT * ayk / volk;
             if (B[PI_BOTTOM].kind && k == bot) Gc += getbc32(B[PI_BOTTOM], ii, jj, itn) * dT * az / volk;
             if (B[PI_TOP].kind && k == top) Gc -= getbc32(B[PI_TOP], ii, jj, itn) * dT * az / volk;
         }
         // particle terms from the fixed-point sums, apply_tendency! (tracer_update.jl:6-13)
         float plk = 0.0f;
-        if (slot >= 0 && sPop[(k - k0) * 32 + lane] > 0) {
-            unsigned long long* pa = a.acc + (long long)slot * G + cq;
-            const long long vv = (long long)*pa;
-            if (vv) { *pa = 0ull; plk = (float)((double)vv * m.fx_unit); }
+        if (slot >= 0 && sPop[l * 32 + lane] > 0) {
+            const long long vv = (long long)acc[q];
+            if (vv) { acc[q] = 0ull; plk = (float)((double)vv * L.fxv); }
         }
-        out[cq] = cc + (Gc + plk / volk);
+        out[q] = cc + (Gc + plk);
     }
 }
 
@@ -1038,8 +1058,9 @@ template <int LZ>
 __global__ void __launch_bounds__(32 * PI_NTRACERS, 2) k32_ztail(TrArgs a) {
     if (stopped(a.err)) return;
     __shared__ float4 sFC[(LZ + 1) * 32];   // faces k0 .. k0+LZ of the 32 columns
-    __shared__ float sW[(LZ + 1) * 32];     // vertical velocity at those faces
-    __shared__ int sPop[LZ * 32];           // individuals in the cells k0 .. k0+LZ-1
+    __shared__ float sFtr[LZ * 32];         // vertical transport term of the cells k0 .. k0+LZ-1
+    __shared__ int sPop[LZ * 32];           // individuals in those cells
+    __shared__ ZLev sLev[LZ];               // per-level constants
     const int tid = threadIdx.y * 32 + threadIdx.x;
     for (int w = blockIdx.x; w < a.nitems; w += gridDim.x) {
         const int4 it = a.items[w];
@@ -1049,22 +1070,40 @@ __global__ void __launch_bounds__(32 * PI_NTRACERS, 2) k32_ztail(TrArgs a) {
         const float az = m.dx * m.dy;
         for (int e = tid; e < (LZ + 1) * 32; e += 32 * PI_NTRACERS) {
             const int f = k0 + e / 32, i = it.y + (e & 31);
+            const bool col = i <= m.Nx + m.Hx;
             float4 fc = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            float wf = 0.0f;
-            if (i <= m.Nx + m.Hx && f <= bot + 1) {
-                wf = wv[gid3(m, i, it.z, f)];
-                if (f <= bot) {                               // fill_halo_bottom_Gc!: zero flux at the bottom
-                    const FCu c = fcu(wf, az, a.rdzC[m.dz_off + f - 1], a.dT);
-                    fc = make_float4(c.tr, c.d0c, c.d1c, c.R);
+            if (col && f <= bot) {                            // fill_halo_bottom_Gc!: zero flux at the bottom
+                const int q = gid3(m, i, it.z, f);
+                const float wt = wv[q];
+                const FCu c = fcu(wt, az, a.rdzC[m.dz_off + f - 1], a.dT);
+                fc = make_float4(c.tr, c.d0c, c.d1c, c.R);
+                if (e < LZ * 32) {                            // cell f: w at its top and bottom faces
+                    const float ftr = az * wt - az * wv[q + m.Gx * m.Gy];
+                    sFtr[e] = m.all_water ? ftr : mulbf(mulbf(ftr, lm32(m, a.lm, i, it.z, f + 1)), lm32(m, a.lm, i, it.z, f));
+                    sPop[e] = a.pop[m.cell_off + q];
                 }
+            } else if (e < LZ * 32) {
+                sFtr[e] = 0.0f;
+                sPop[e] = 0;
             }
             sFC[e] = fc;
-            sW[e] = wf;
-            if (e < LZ * 32) sPop[e] = (i <= m.Nx + m.Hx && f <= bot) ? a.pop[m.cell_off + gid3(m, i, it.z, f)] : 0;
+        }
+        if (tid < LZ) {
+            const int k = k0 + tid;
+            ZLev L = {0.0f, 0.0f, 1.0f, 1.0f, 0.0};
+            if (k <= bot) {
+                const float dz = a.dzF[m.dz_off + k - 1], volk = az * dz;
+                L.dtv = a.dT / volk;
+                L.sk = a.dT / a.dzC[m.dz_off + k - m.Hz - 1];
+                L.dz = dz;
+                L.dzn = a.dzF[m.dz_off + k];
+                L.fxv = m.fx_unit / (double)volk;
+            }
+            sLev[tid] = L;
         }
         __syncthreads();
-        if (m.all_water) z_walk<LZ, false>(a, m, it, sFC, sW, sPop);
-        else z_walk<LZ, true>(a, m, it, sFC, sW, sPop);
+        if (m.all_water) z_walk<LZ, false>(a, m, it, sFC, sFtr, sPop, sLev);
+        else z_walk<LZ, true>(a, m, it, sFC, sFtr, sPop, sLev);
         __syncthreads();
     }
 }
