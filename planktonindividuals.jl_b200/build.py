@@ -6,8 +6,9 @@ Each translation unit has its own floating-point flags:
   pib200.cu  (FP64 form)  -fmad=false keeps every multiply and add separately rounded so the
                           Float64 path produces the same bits as the CPU oracle, which is compiled
                           with -ffp-contract=off;
-  fp32.cu    (FP32 form)  default contraction: fused multiply-adds are faster and more accurate,
-                          and the FP32 form is compared with the oracle within a tolerance.
+  fp32.cu    (FP32 form)  default contraction and -prec-div=false: fused multiply-adds and the
+                          approximate (2 ulp) division are faster, and the FP32 form is compared
+                          with the oracle within a tolerance.
 """
 import os
 import shutil
@@ -18,7 +19,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "PlanktonIndividuals", "libpib200.so")
 SOURCES = {"pib200.cu": ["-fmad=false", "-Xcompiler", "-ffp-contract=off"],
-           "fp32.cu": []}
+           "fp32.cu": ["-prec-div=false"]}
 DEPS = ["pib200.cu", "kernels_fp64.cuh", "pib200_internal.h", "noalloc.cu", "host_common.h",
         "fp32.cu", "kernels_fp32.cuh", "fp32_internal.h"]
 BUILD_DIR = os.path.join(HERE, "_build")

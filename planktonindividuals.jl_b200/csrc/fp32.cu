@@ -285,7 +285,7 @@ pi_status check_member(const pi_member& mb, int nsp, std::string& msg) {
         if (grid->topo[a] != PI_PERIODIC && grid->topo[a] != PI_BOUNDED) { msg = "topology must be Periodic or Bounded"; return PI_ERR_ARG; }
     if (grid->topo[2] != PI_BOUNDED) { msg = "z must be Bounded (tracer sinking has no Periodic rule)"; return PI_ERR_ARG; }
     long long Gx = grid->Nx + 2LL * grid->Hx, Gy = grid->Ny + 2LL * grid->Hy, Gz = grid->Nz + 2LL * grid->Hz;
-    if (Gx * Gy * Gz >= (1LL << 31) - 2 || (Gx + 1) * (Gy + 1) * (Gz + 1) >= (1LL << 31)) { msg = "grid too large for 32-bit cell indices"; return PI_ERR_ARG; }
+    if (Gx * Gy * Gz >= (1LL << 31) - 2 || f32_bits(Gx) + f32_bits(Gy) + f32_bits(Gz) > 31) { msg = "grid too large for 32-bit cell indices"; return PI_ERR_ARG; }
     if (mb.capacity >= (1LL << 31)) { msg = "capacity must be below 2^31"; return PI_ERR_ARG; }
     for (int s = 0; s < nsp; ++s) {
         const pi_quota_params& p = mb.species[s];
@@ -361,7 +361,7 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
       k32_velhalf<<<dim3(gx, b->nm), 256, 0, s>>>(b->md, b->F, b->errw); }
     {
         MoveArgs a;
-        a.T = b->T; a.P = b->P; a.sp = b->sp; a.bgc = b->bgc; a.F = b->F; a.dzC = b->dzC; a.st = b->st;
+        a.T = b->T; a.P = b->P; a.sp = b->sp; a.bgc = b->bgc; a.F = b->F; a.rdzC = b->rdzC; a.st = b->st;
         a.dT = fdT; a.Gtot = G; a.pop = b->pop; a.pop_sp = b->pop_sp; a.chl_acc = b->chl_acc; a.acc = b->acc;
         a.dcnt = b->dcnt; a.tile_cnt = b->tile_cnt; a.err = b->errw;
         BScope sc(b, "k32_move");
@@ -412,9 +412,10 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
             BScope sc(b, "k32_ztail");
             const unsigned grid = (unsigned)std::max(1, b->nz_items);
             const dim3 blk(32, PI_NTRACERS);
-            if (b->tune.lz == 8) k32_ztail<8><<<grid, blk, 0, s>>>(a);
-            else if (b->tune.lz == 32) k32_ztail<32><<<grid, blk, 0, s>>>(a);
-            else k32_ztail<16><<<grid, blk, 0, s>>>(a);
+            const size_t zs = ztail_smem();
+            if (b->tune.lz == 8) k32_ztail<8><<<grid, blk, zs, s>>>(a);
+            else if (b->tune.lz == 32) k32_ztail<32><<<grid, blk, zs, s>>>(a);
+            else k32_ztail<16><<<grid, blk, zs, s>>>(a);
         }
     }
     { BScope sc(b, "k32_halo");
@@ -537,6 +538,9 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
         d.Gx = g.Gx; d.Gy = g.Gy; d.Gz = g.Gz; d.tx = g.topo[0]; d.ty = g.topo[1]; d.tz = g.topo[2];
         d.all_water = h.all_water; d.any_bc = 0;
         d.dx = (float)g.dx; d.dy = (float)g.dy;
+        d.rdx = 1.0f / d.dx; d.rdy = 1.0f / d.dy;
+        d.cbx = f32_bits(g.Nx); d.cby = f32_bits(g.Ny);
+        d.hbx = f32_bits(g.Gx); d.hby = f32_bits(g.Gy);
         d.cell_off = cell; d.G = g.G; d.col_off = col; d.slot_off = slot; d.C = h.C;
         d.dz_off = lev; d.bc_off = m * PI_NTRACERS * 6; d.seed = h.seed;
         double cmin = 1e300, chlmin = 1e300;
@@ -550,6 +554,8 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
         // 2^40 units per nominal individual: sums of up to ~2^22 individuals per cell fit in 63 bits
         d.fx_unit = cmin * 0x1p-40;
         d.chl_unit = chlmin * 0x1p-40;
+        d.fx_inv = 1.0 / d.fx_unit;
+        d.chl_inv = 1.0 / d.chl_unit;
         bgch.push_back(to_dev(h.bgc));
         for (int k = 0; k < g.Gz; ++k) { dzF.push_back((float)g.dzF[k]); dzC.push_back((float)g.dzC[k]); }
         for (int s = 0; s < nspecies; ++s) {
@@ -660,6 +666,9 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     cudaFuncSetAttribute(k32_xy<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xy_smem(16));
     cudaFuncSetAttribute(k32_xy<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xy_smem(8));
     cudaFuncSetAttribute(k32_xy<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xy_smem(4));
+    cudaFuncSetAttribute(k32_ztail<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ztail_smem());
+    cudaFuncSetAttribute(k32_ztail<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ztail_smem());
+    cudaFuncSetAttribute(k32_ztail<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ztail_smem());
     b->T.md = b->md; b->T.nsp = nspecies; b->T.tiles = b->tiles; b->T.ntiles = b->ntiles; b->T.seg_tile0 = b->seg_tile0;
     st = build_tables(b);
     if (st) return bail(st);
@@ -724,12 +733,12 @@ pi_status pi_batch_set_individuals(pi_batch* b, int32_t member, int32_t sp, cons
             if (of >= 1.0f) of = 0x1.fffffep-1f;
             o[a][i] = of;
         }
-        cell[i] = c[0] + (g.Nx + 1) * (c[1] + (g.Ny + 1) * c[2]);
+        cell[i] = f32_pack(c[0], c[1], c[2], d.cbx, d.cby);
         bool same = true;
         for (int a = 0; a < 3; ++a) same = same && idx[a][i] == c[a] + 1 + Hh[a];
         if (!same) {
             stat[i] = F32_ST_STALE;
-            scell[i] = (int32_t)(in->xi[i] + (g.Gx + 1) * (in->yi[i] + (g.Gy + 1) * in->zi[i]));
+            scell[i] = f32_pack((int)in->xi[i], (int)in->yi[i], (int)in->zi[i], d.hbx, d.hby);
         }
     }
     const long long g0 = d.slot_off + (long long)sp * C;
@@ -774,12 +783,15 @@ pi_status pi_batch_get_individuals(pi_batch* b, int32_t member, int32_t sp, pi_i
     for (long long i = 0; i < C; ++i) {
         const uint8_t fl = flags[i];
         int ci = 0, cj = 0, ck = 0;
-        if (cell[i] >= 0) { ci = cell[i] % (g.Nx + 1); int r = cell[i] / (g.Nx + 1); cj = r % (g.Ny + 1); ck = r / (g.Ny + 1); }
+        const MemberDev& md = b->mdh[member];
+        if (cell[i] >= 0) f32_unpack(cell[i], md.cbx, md.cby, ci, cj, ck);
         const double xyz[3] = { cell[i] < 0 ? 0.0 : ci + (double)o[0][i], cell[i] < 0 ? 0.0 : cj + (double)o[1][i],
                                 cell[i] < 0 ? 0.0 : ck + (double)o[2][i] };
         int64_t xi, yi, zi;
         if (stat[i] & F32_ST_STALE) {
-            xi = scell[i] % (g.Gx + 1); int r = scell[i] / (g.Gx + 1); yi = r % (g.Gy + 1); zi = r / (g.Gy + 1);
+            int a0, a1, a2;
+            f32_unpack(scell[i], md.hbx, md.hby, a0, a1, a2);
+            xi = a0; yi = a1; zi = a2;
         } else if (cell[i] < 0) { xi = g.Hx; yi = g.Hy; zi = g.Hz; }
         else { xi = ci + 1 + g.Hx; yi = cj + 1 + g.Hy; zi = ck + 1 + g.Hz; }
         if (out->x) out->x[i] = xyz[0];

@@ -37,6 +37,9 @@ struct MemberDev {
     int all_water;
     int any_bc;
     float dx, dy;
+    float rdx, rdy;         // 1/dx, 1/dy
+    int cbx, cby;           // bit widths of ci and cj in an interior cell code
+    int hbx, hby;           // bit widths of xi and yi in a find_inds! (halo) cell code
     long long cell_off;     // first cell of the member's halo-padded grid in the batch cell space
     long long G;            // (Nx+2Hx)(Ny+2Hy)(Nz+2Hz)
     long long col_off;      // first of the member's Nx*Ny surface columns
@@ -47,7 +50,23 @@ struct MemberDev {
     uint64_t seed;
     double fx_unit;         // mmol per fixed-point unit of the particle→grid mass sums
     double chl_unit;        // mg Chl per fixed-point unit of the Chl sums
+    double fx_inv;          // 1 / fx_unit
+    double chl_inv;         // 1 / chl_unit
 };
+
+// Cell codes: three indices in bit fields of one int32 (a, b, c from the low bits up, widths of a
+// and b given), so that unpacking takes shifts and masks.
+__host__ __device__ inline int32_t f32_pack(int a, int b, int c, int ba, int bb) {
+    return (int32_t)((unsigned)a | ((unsigned)b << ba) | ((unsigned)c << (ba + bb)));
+}
+__host__ __device__ inline void f32_unpack(int32_t code, int ba, int bb, int& a, int& b, int& c) {
+    const unsigned u = (unsigned)code;
+    a = (int)(u & ((1u << ba) - 1u));
+    b = (int)((u >> ba) & ((1u << bb) - 1u));
+    c = (int)(u >> (ba + bb));
+}
+// bits needed for the values 0..v
+inline int f32_bits(long long v) { int b = 1; while ((1LL << b) <= v) ++b; return b; }
 
 // Forcing of a member for the current step.
 struct MemberForcing {

@@ -48,22 +48,16 @@ __device__ __forceinline__ void seg_of(const Tab32& T, int seg, int& m, int& s) 
 // cells and positions
 // ------------------------------------------------------------------------------------------
 __device__ __forceinline__ void unpack_int(const MemberDev& m, int32_t code, int& ci, int& cj, int& ck) {
-    ci = code % (m.Nx + 1);
-    const int r = code / (m.Nx + 1);
-    cj = r % (m.Ny + 1);
-    ck = r / (m.Ny + 1);
+    f32_unpack(code, m.cbx, m.cby, ci, cj, ck);
 }
 __device__ __forceinline__ int32_t pack_int(const MemberDev& m, int ci, int cj, int ck) {
-    return ci + (m.Nx + 1) * (cj + (m.Ny + 1) * ck);
+    return f32_pack(ci, cj, ck, m.cbx, m.cby);
 }
 __device__ __forceinline__ int32_t pack_halo(const MemberDev& m, int xi, int yi, int zi) {
-    return xi + (m.Gx + 1) * (yi + (m.Gy + 1) * zi);
+    return f32_pack(xi, yi, zi, m.hbx, m.hby);
 }
 __device__ __forceinline__ void unpack_halo(const MemberDev& m, int32_t c, int& xi, int& yi, int& zi) {
-    xi = c % (m.Gx + 1);
-    const int r = c / (m.Gx + 1);
-    yi = r % (m.Gy + 1);
-    zi = r / (m.Gy + 1);
+    f32_unpack(c, m.hbx, m.hby, xi, yi, zi);
 }
 // halo-inclusive member-local cell of an interior position cell (find_inds!, Individuals/utils.jl:2-7)
 __device__ __forceinline__ int q_of(const MemberDev& m, int ci, int cj, int ck) {
@@ -101,14 +95,21 @@ __device__ __forceinline__ void move(Ax1& a, float d, int N, int topo) {
 // index and weight along one axis for a face-centred (own axis) or cell-centred field
 // (interpolation.jl:3-83: x + 1 or x + 0.5 split into trunc and mod)
 __device__ __forceinline__ void axis_iw(const Ax1& a, int H, bool face, int& idx, float& w) {
-    if (face) { idx = a.c + 1 + H; w = a.o; }
-    else if (a.o < 0.5f) { idx = a.c + H; w = a.o + 0.5f; }
-    else { idx = a.c + 1 + H; w = a.o - 0.5f; }
+    if (face) { idx = a.c + 1 + H; w = a.o; return; }
+    const bool lo = a.o < 0.5f;
+    idx = a.c + H + (lo ? 0 : 1);
+    w = lo ? a.o + 0.5f : a.o - 0.5f;
 }
 __device__ __forceinline__ int clampi(int v, int lo, int hi, uint32_t* err) {
     if (v < lo) { seterr(err, F32_ERR_DOMAIN); return lo; }
     if (v > hi) { seterr(err, F32_ERR_DOMAIN); return hi; }
     return v;
+}
+// clamp into [lo, hi], noting an index outside in `bad` (reported once per individual)
+__device__ __forceinline__ int clampb(int v, int lo, int hi, bool& bad) {
+    const int c = min(max(v, lo), hi);
+    bad |= c != v;
+    return c;
 }
 
 // The 8 corner values of one velocity component around a position. The four RK stages of a step
@@ -117,18 +118,32 @@ __device__ __forceinline__ int clampi(int v, int lo, int hi, uint32_t* err) {
 // and the base corner are the same: the values are identical, only the loads are saved.
 struct Corners { const float* f; int q; float v[8]; };
 
-// trilinear interpolation of one velocity component (member-local field pointer)
+// Member constants of the particle kernels, held in registers.
+struct PGeom {
+    int Nx, Ny, Nz, Hx, Hy, Hz, Gx, Gy, Gz, tx, ty, tz, dz_off;
+    float rdx, rdy;
+};
+__device__ __forceinline__ PGeom pgeom(const MemberDev& m) {
+    PGeom g;
+    g.Nx = m.Nx; g.Ny = m.Ny; g.Nz = m.Nz; g.Hx = m.Hx; g.Hy = m.Hy; g.Hz = m.Hz;
+    g.Gx = m.Gx; g.Gy = m.Gy; g.Gz = m.Gz; g.tx = m.tx; g.ty = m.ty; g.tz = m.tz; g.dz_off = m.dz_off;
+    g.rdx = m.rdx; g.rdy = m.rdy;
+    return g;
+}
+
+// trilinear interpolation of one velocity component (member-local field pointer), in grid cells
+// per second
 template <int COMP>
-__device__ __forceinline__ float itpl32(const MemberDev& m, const float* __restrict__ f,
-                                        const float* __restrict__ dzC, const Ax1& X, const Ax1& Y,
-                                        const Ax1& Z, uint32_t* err, Corners& cc) {
+__device__ __forceinline__ float itpl32(const PGeom& m, const float* __restrict__ f,
+                                        const float* __restrict__ rdzC, const Ax1& X, const Ax1& Y,
+                                        const Ax1& Z, bool& bad, Corners& cc) {
     int i, j, k;
     float xd, yd, zd;
     axis_iw(X, m.Hx, COMP == 0, i, xd);
     axis_iw(Y, m.Hy, COMP == 1, j, yd);
     axis_iw(Z, m.Hz, COMP == 2, k, zd);
-    i = clampi(i, 1, m.Gx - 1, err); j = clampi(j, 1, m.Gy - 1, err); k = clampi(k, 1, m.Gz - 1, err);
-    const int q = gid3(m, i, j, k);
+    i = clampb(i, 1, m.Gx - 1, bad); j = clampb(j, 1, m.Gy - 1, bad); k = clampb(k, 1, m.Gz - 1, bad);
+    const int q = (i - 1) + m.Gx * ((j - 1) + m.Gy * (k - 1));
     if (cc.f != f || cc.q != q) {
         const int sy = m.Gx, sz = m.Gx * m.Gy;
         cc.f = f; cc.q = q;
@@ -139,9 +154,9 @@ __device__ __forceinline__ float itpl32(const MemberDev& m, const float* __restr
     const float a0 = (1.0f - xd) * (1.0f - yd), a1 = (1.0f - xd) * yd, a2 = xd * (1.0f - yd), a3 = xd * yd;
     const float lo = a0 * cc.v[0] + a1 * cc.v[1] + a2 * cc.v[2] + a3 * cc.v[3];
     const float hi = a0 * cc.v[4] + a1 * cc.v[5] + a2 * cc.v[6] + a3 * cc.v[7];
-    if (COMP == 0) return ((1.0f - zd) * lo + zd * hi) / m.dx;
-    if (COMP == 1) return ((1.0f - zd) * lo + zd * hi) / m.dy;
-    return (1.0f - zd) * lo / dzC[m.dz_off + k - 1] + zd * hi / dzC[m.dz_off + k];
+    if (COMP == 0) return ((1.0f - zd) * lo + zd * hi) * m.rdx;
+    if (COMP == 1) return ((1.0f - zd) * lo + zd * hi) * m.rdy;
+    return (1.0f - zd) * lo * __ldg(rdzC + m.dz_off + k - 1) + zd * hi * __ldg(rdzC + m.dz_off + k);
 }
 
 // the draws of the FP64 form (same keys, same numbers; lattice values are exact in float)
@@ -156,8 +171,8 @@ __device__ __forceinline__ void draw3f(uint64_t seed, uint32_t iter, uint32_t sp
     r2 = (float)(o[2] >> 8) * 0x1p-24f;
 }
 
-__device__ __forceinline__ void add_fixed(unsigned long long* a, float v, double unit) {
-    const long long x = __double2ll_rn((double)v / unit);
+__device__ __forceinline__ void add_fixed(unsigned long long* a, float v, double inv_unit) {
+    const long long x = __double2ll_rn((double)v * inv_unit);
     if (x) atomicAdd(a, (unsigned long long)x);
 }
 
@@ -235,7 +250,7 @@ struct MoveArgs {
     const SpeciesDev32* sp;        // [member * nsp + species]
     const BgcDev32* bgc;           // [member]
     const MemberForcing* F;
-    const float* dzC;
+    const float* rdzC;             // 1 / ΔzC
     const StepState* st;
     float dT;
     long long Gtot;
@@ -248,8 +263,8 @@ struct MoveArgs {
     uint32_t* err;
 };
 
-__device__ __forceinline__ void move_one(const MoveArgs& a, const MemberDev& m, int mi, int s, long long slot,
-                                         long long g, uint32_t iter, int& is_div, int& is_free) {
+__device__ __forceinline__ void move_one(const MoveArgs& a, const MemberDev& m, const PGeom& pg, int mi, int s,
+                                         long long slot, long long g, uint32_t iter, int& is_div, int& is_free) {
     const IndDev32& P = a.P;
     const uint8_t fl = P.flags[g];
     if (!(fl & F32_AC)) {
@@ -267,47 +282,50 @@ __device__ __forceinline__ void move_one(const MoveArgs& a, const MemberDev& m, 
     int ci, cj, ck;
     unpack_int(m, P.cell[g], ci, cj, ck);
     // ΔzC at the find_inds! zi of the previous step, plus Hz (particle_diffusion.jl:26-28)
-    int zi = ck + 1 + m.Hz;
+    int zi = ck + 1 + pg.Hz;
     if (stt & F32_ST_STALE) { int a0, a1; unpack_halo(m, P.scell[g], a0, a1, zi); }
-    const int kdz = clampi(zi + m.Hz, 1, m.Gz, err);
+    bool bad = false;
+    const int kdz = clampb(zi + pg.Hz, 1, pg.Gz, bad);
     const MemberForcing& f = a.F[mi];
     const Ax1 X0{ci, P.ox[g]}, Y0{cj, P.oy[g]}, Z0{ck, P.oz[g]};
-    const float dT = a.dT;
-    const float* dzC = a.dzC;
+    const float dT = a.dT, hdT = 0.5f * dT;
+    const float* __restrict__ rdzC = a.rdzC;
     Corners cu{nullptr, -1, {}}, cv{nullptr, -1, {}}, cw{nullptr, -1, {}};
-    float u1 = itpl32<0>(m, f.vel0[0], dzC, X0, Y0, Z0, err, cu);
-    float v1 = itpl32<1>(m, f.vel0[1], dzC, X0, Y0, Z0, err, cv);
-    float w1 = itpl32<2>(m, f.vel0[2], dzC, X0, Y0, Z0, err, cw);
+    float u1 = itpl32<0>(pg, f.vel0[0], rdzC, X0, Y0, Z0, bad, cu);
+    float v1 = itpl32<1>(pg, f.vel0[1], rdzC, X0, Y0, Z0, bad, cv);
+    float w1 = itpl32<2>(pg, f.vel0[2], rdzC, X0, Y0, Z0, bad, cw);
     float u2 = u1, v2 = v1, w2 = w1;
     Ax1 X = X0, Y = Y0, Z = Z0;
-    move(X, 0.5f * u1 * dT, m.Nx, m.tx); move(Y, 0.5f * v1 * dT, m.Ny, m.ty); move(Z, -(0.5f * w1 * dT), m.Nz, m.tz);
-    u1 = itpl32<0>(m, f.velh[0], dzC, X, Y, Z, err, cu); v1 = itpl32<1>(m, f.velh[1], dzC, X, Y, Z, err, cv);
-    w1 = itpl32<2>(m, f.velh[2], dzC, X, Y, Z, err, cw);
+    move(X, u1 * hdT, pg.Nx, pg.tx); move(Y, v1 * hdT, pg.Ny, pg.ty); move(Z, -(w1 * hdT), pg.Nz, pg.tz);
+    u1 = itpl32<0>(pg, f.velh[0], rdzC, X, Y, Z, bad, cu); v1 = itpl32<1>(pg, f.velh[1], rdzC, X, Y, Z, bad, cv);
+    w1 = itpl32<2>(pg, f.velh[2], rdzC, X, Y, Z, bad, cw);
     u2 += u1 * 2.0f; v2 += v1 * 2.0f; w2 += w1 * 2.0f;
     X = X0; Y = Y0; Z = Z0;
-    move(X, 0.5f * u1 * dT, m.Nx, m.tx); move(Y, 0.5f * v1 * dT, m.Ny, m.ty); move(Z, -(0.5f * w1 * dT), m.Nz, m.tz);
-    u1 = itpl32<0>(m, f.velh[0], dzC, X, Y, Z, err, cu); v1 = itpl32<1>(m, f.velh[1], dzC, X, Y, Z, err, cv);
-    w1 = itpl32<2>(m, f.velh[2], dzC, X, Y, Z, err, cw);
+    move(X, u1 * hdT, pg.Nx, pg.tx); move(Y, v1 * hdT, pg.Ny, pg.ty); move(Z, -(w1 * hdT), pg.Nz, pg.tz);
+    u1 = itpl32<0>(pg, f.velh[0], rdzC, X, Y, Z, bad, cu); v1 = itpl32<1>(pg, f.velh[1], rdzC, X, Y, Z, bad, cv);
+    w1 = itpl32<2>(pg, f.velh[2], rdzC, X, Y, Z, bad, cw);
     u2 += u1 * 2.0f; v2 += v1 * 2.0f; w2 += w1 * 2.0f;
     X = X0; Y = Y0; Z = Z0;
-    move(X, u1 * dT, m.Nx, m.tx); move(Y, v1 * dT, m.Ny, m.ty); move(Z, -(w1 * dT), m.Nz, m.tz);
-    u1 = itpl32<0>(m, f.vel1[0], dzC, X, Y, Z, err, cu); v1 = itpl32<1>(m, f.vel1[1], dzC, X, Y, Z, err, cv);
-    w1 = itpl32<2>(m, f.vel1[2], dzC, X, Y, Z, err, cw);
-    u2 = (u2 + u1) / 6.0f; v2 = (v2 + v1) / 6.0f; w2 = (w2 + w1) / 6.0f;
+    move(X, u1 * dT, pg.Nx, pg.tx); move(Y, v1 * dT, pg.Ny, pg.ty); move(Z, -(w1 * dT), pg.Nz, pg.tz);
+    u1 = itpl32<0>(pg, f.vel1[0], rdzC, X, Y, Z, bad, cu); v1 = itpl32<1>(pg, f.vel1[1], rdzC, X, Y, Z, bad, cv);
+    w1 = itpl32<2>(pg, f.vel1[2], rdzC, X, Y, Z, bad, cw);
+    const float sixth = 1.0f / 6.0f;
+    u2 = (u2 + u1) * sixth; v2 = (v2 + v1) * sixth; w2 = (w2 + w1) * sixth;
     X = X0; Y = Y0; Z = Z0;
-    move(X, u2 * dT, m.Nx, m.tx); move(Y, v2 * dT, m.Ny, m.ty); move(Z, -(w2 * dT), m.Nz, m.tz);
+    move(X, u2 * dT, pg.Nx, pg.tx); move(Y, v2 * dT, pg.Ny, pg.ty); move(Z, -(w2 * dT), pg.Nz, pg.tz);
     // random-walk diffusion (particle_diffusion.jl:16-33); a zero κ moves nothing
     const BgcDev32& b = a.bgc[mi];
     if (b.kappa_hP != 0.0f || b.kappa_vP != 0.0f) {
         float r0, r1, r2;
         draw3f(m.seed, iter, (uint32_t)s, PI_DRAW_DIFFUSION, (uint32_t)slot, r0, r1, r2);
-        move(X, (r0 - 0.5f) * 2.0f * sqrtf(b.kappa_hP * dT) / m.dx, m.Nx, m.tx);
-        move(Y, (r1 - 0.5f) * 2.0f * sqrtf(b.kappa_hP * dT) / m.dy, m.Ny, m.ty);
-        move(Z, (r2 - 0.5f) * 2.0f * sqrtf(b.kappa_vP * dT) / dzC[m.dz_off + kdz - 1], m.Nz, m.tz);
+        move(X, (r0 - 0.5f) * 2.0f * sqrtf(b.kappa_hP * dT) * pg.rdx, pg.Nx, pg.tx);
+        move(Y, (r1 - 0.5f) * 2.0f * sqrtf(b.kappa_hP * dT) * pg.rdy, pg.Ny, pg.ty);
+        move(Z, (r2 - 0.5f) * 2.0f * sqrtf(b.kappa_vP * dT) * __ldg(rdzC + pg.dz_off + kdz - 1), pg.Nz, pg.tz);
     }
-    if (X.c < 0 || X.c > m.Nx) { seterr(err, F32_ERR_DOMAIN); X.c = X.c < 0 ? 0 : m.Nx; X.o = 0.0f; }
-    if (Y.c < 0 || Y.c > m.Ny) { seterr(err, F32_ERR_DOMAIN); Y.c = Y.c < 0 ? 0 : m.Ny; Y.o = 0.0f; }
-    if (Z.c < 0 || Z.c > m.Nz) { seterr(err, F32_ERR_DOMAIN); Z.c = Z.c < 0 ? 0 : m.Nz; Z.o = 0.0f; }
+    if (X.c < 0 || X.c > pg.Nx) { bad = true; X.c = X.c < 0 ? 0 : pg.Nx; X.o = 0.0f; }
+    if (Y.c < 0 || Y.c > pg.Ny) { bad = true; Y.c = Y.c < 0 ? 0 : pg.Ny; Y.o = 0.0f; }
+    if (Z.c < 0 || Z.c > pg.Nz) { bad = true; Z.c = Z.c < 0 ? 0 : pg.Nz; Z.o = 0.0f; }
+    if (bad) seterr(err, F32_ERR_DOMAIN);
     P.ox[g] = X.o; P.oy[g] = Y.o; P.oz[g] = Z.o;
     P.cell[g] = pack_int(m, X.c, Y.c, Z.c);
     const int q = q_of(m, X.c, Y.c, Z.c);
@@ -316,7 +334,7 @@ __device__ __forceinline__ void move_one(const MoveArgs& a, const MemberDev& m, 
     const bool inside = X.c < m.Nx && Y.c < m.Ny && Z.c < m.Nz;
     atomicAdd(&a.pop[cq], 1);
     if (a.pop_sp) atomicAdd(&a.pop_sp[(long long)s * G + cq], 1);
-    if (inside) add_fixed(&a.chl_acc[cq], P.Chl[g], m.chl_unit);
+    if (inside) add_fixed(&a.chl_acc[cq], P.Chl[g], m.chl_inv);
     // previous step's decisions (plankton_update.jl:5-16, division_death.jl:2-25)
     const int gz = (fl & F32_GRAZ) != 0, mt = (fl & F32_MORT) != 0, dv = (fl & F32_DVID) != 0;
     const int ac1 = !gz, ac2 = ac1 && !mt, dv2 = dv && ac2;
@@ -331,7 +349,7 @@ __device__ __forceinline__ void move_one(const MoveArgs& a, const MemberDev& m, 
         const float fN = kind == 1 ? p.grazFracN : p.mortFracN;
         const float fP = kind == 1 ? p.grazFracP : p.mortFracP;
         const float Bm = P.Bm[g], Cq = P.Cq[g], Nq = P.Nq[g], Pq = P.Pq[g];
-        const double u = m.fx_unit;
+        const double u = m.fx_inv;
         add_fixed(&a.acc[ACC_DOC * G + cq], (Bm + Cq) * fC, u);
         add_fixed(&a.acc[ACC_DON * G + cq], (Bm * p.R_NC + Nq) * fN, u);
         add_fixed(&a.acc[ACC_DOP * G + cq], (Bm * p.R_PC + Pq) * fP, u);
@@ -347,6 +365,7 @@ __device__ __forceinline__ void move_one(const MoveArgs& a, const MemberDev& m, 
 __global__ void __launch_bounds__(256, 3) k32_move(MoveArgs a) {
     if (stopped(a.err)) return;
     __shared__ unsigned int sh_d, sh_f;
+    __shared__ PGeom sg;
     const int bs = blockDim.x, ppt = F32_TILE / bs;
     const uint32_t iter = (uint32_t)(a.st->iteration + 1);
     for (int t = blockIdx.x; t < a.T.ntiles; t += gridDim.x) {
@@ -354,13 +373,15 @@ __global__ void __launch_bounds__(256, 3) k32_move(MoveArgs a) {
         int mi, s;
         seg_of(a.T, tl.x, mi, s);
         const MemberDev& m = a.T.md[mi];
+        if (threadIdx.x == 0) sg = pgeom(m);
+        __syncthreads();
         const long long base = m.slot_off + (long long)s * m.C;
         unsigned int nd = 0, nf = 0;
         for (int p = 0; p < ppt; ++p) {
             const long long slot = (long long)tl.y + p * bs + threadIdx.x;
             if (slot < m.C) {
                 int d, f;
-                move_one(a, m, mi, s, slot, base + slot, iter, d, f);
+                move_one(a, m, sg, mi, s, slot, base + slot, iter, d, f);
                 nd += d; nf += f;
             }
         }
@@ -657,7 +678,7 @@ __device__ __forceinline__ void phys_one(const PhysArgs& a, const MemberDev& m, 
     P.flags[g] = (uint8_t)(F32_AC | (dg ? F32_GRAZ : 0) | (dm ? F32_MORT : 0) | (dd ? F32_DVID : 0));
     // calc_consume_kernel! (consume_loss.jl:2-9): only individuals binned this step reach the grid
     if (ac0 && inside) {
-        const double u = m.fx_unit;
+        const double u = m.fx_inv;
         add_fixed(&a.acc[ACC_DIC * G + cq], (resp - PS) * dT, u);
         add_fixed(&a.acc[ACC_DOC * G + cq], (exu - VDOC) * dT, u);
         add_fixed(&a.acc[ACC_NH4 * G + cq], -VNH4 * dT, u);
@@ -718,23 +739,26 @@ __device__ __forceinline__ float psid0(float d0, float dn, const FCu& f) {
 template <bool LM>
 __device__ __forceinline__ float mk(float x, int ma, int mb) { return LM ? mulbf(mulbf(x, ma), mb) : x; }
 
-// adv_flux_x / adv_flux_y at a face from c[f-2], c[f-1], c[f], c[f+1] and the landmask there
+// adv_flux_x / adv_flux_y at a face from c[f-2], c[f-1], c[f], c[f+1] and the landmask there; the
+// upwind side is selected, not branched on (a zero transport gives a zero flux either way)
 template <bool LM>
 __device__ __forceinline__ float flux_h(const FCu& f, float cm2, float cm1, float c0, float cp1,
                                         int lm2, int lm1, int l0, int lp1) {
     const float d0 = mk<LM>(c0 - cm1, l0, lm1);
-    if (f.tr > 0.0f) return f.tr * (cm1 + psid0(d0, mk<LM>(cm1 - cm2, lm1, lm2), f));
-    if (f.tr < 0.0f) return f.tr * (c0 - psid0(d0, mk<LM>(cp1 - c0, lp1, l0), f));
-    return 0.0f;
+    const bool pos = f.tr > 0.0f;
+    const float dn = pos ? mk<LM>(cm1 - cm2, lm1, lm2) : mk<LM>(cp1 - c0, lp1, l0);
+    const float ps = psid0(d0, dn, f);
+    return f.tr * (pos ? cm1 + ps : c0 - ps);
 }
 // adv_flux_z at face k from c[k-2], c[k-1], c[k], c[k+1] (the index grows downward)
 template <bool LM>
 __device__ __forceinline__ float flux_v(const FCu& f, float cm2, float cm1, float c0, float cp1,
                                         int lm2, int lm1, int l0, int lp1) {
     const float d0 = mk<LM>(cm1 - c0, l0, lm1);
-    if (f.tr > 0.0f) return f.tr * (c0 + psid0(d0, mk<LM>(c0 - cp1, lp1, l0), f));
-    if (f.tr < 0.0f) return f.tr * (cm1 - psid0(d0, mk<LM>(cm2 - cm1, lm1, lm2), f));
-    return 0.0f;
+    const bool pos = f.tr > 0.0f;
+    const float dn = pos ? mk<LM>(c0 - cp1, lp1, l0) : mk<LM>(cm2 - cm1, lm1, lm2);
+    const float ps = psid0(d0, dn, f);
+    return f.tr * (pos ? c0 + ps : cm1 - ps);
 }
 __device__ __forceinline__ int wrap_ax(int a, int N, int H, int topo) {
     if (topo == PI_PERIODIC) { while (a < H + 1) a += N; while (a > N + H) a -= N; return a; }
@@ -932,9 +956,37 @@ __device__ __forceinline__ float fe_forcing(int n, const BgcDev32& b, float dT, 
     return -pfei * b.kdiss * dT + (b.lambda_min + b.lambda_dust * dust) * dfe * b.DFeFrac * dT + fe;
 }
 
-template <int LZ, bool LM>
+// Asynchronous global → shared copies (cp.async): a warp's z walk reads the inputs of each level
+// from a ring of ZS levels filled ahead of it, so ZS - 1 levels of loads are in flight while it
+// computes. A lane reads back only what it copied itself, which wait_group makes visible to it.
+__device__ __forceinline__ void cpa4(float* sdst, const float* gsrc) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n"
+                 :: "r"((unsigned)__cvta_generic_to_shared(sdst)), "l"(gsrc) : "memory");
+}
+// 8 bytes, or zeros without reading when `on` is false
+__device__ __forceinline__ void cpa8(unsigned long long* sdst, const unsigned long long* gsrc, bool on) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n"
+                 :: "r"((unsigned)__cvta_generic_to_shared(sdst)), "l"(gsrc), "r"(on ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpa_wait() { asm volatile("cp.async.wait_group %0;\n" :: "n"(N) : "memory"); }
+
+#define ZS 4                              // levels of a z walk ring (power of two)
+// One warp's ring: own tracer c, tracer_temp t two levels below, up to four other tracers the
+// forcing reads, and the particle sum of the cell.
+struct ZRing {
+    float c[ZS][32];
+    float t[ZS][32];
+    float x[4][ZS][32];
+    unsigned long long acc[ZS][32];
+};
+
+// NUT: the ten nutrient tracers (linear forcing, particle sums); otherwise the three iron tracers
+// and dust (iron forcing, sinking). GEN: diffusion or flux boundary conditions are switched on.
+template <int LZ, bool LM, bool NUT, bool GEN>
 __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& md, const int4 it, const float4* sFC,
-                                       const float* sFtr, const int* sPop, const ZLev* sLev) {
+                                       const float* sFtr, const int* sPop, const ZLev* sLev, ZRing& R) {
     const int lane = threadIdx.x, n = threadIdx.y;
     // member constants in registers: the stores of the walk could otherwise alias them
     const int Nx = md.Nx, Hx = md.Hx, Hz = md.Hz, Gx = md.Gx, Gy = md.Gy;
@@ -947,91 +999,119 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& md, con
     const int kend = min(k0 + LZ - 1, bot);
     const int qcol = (i - 1) + Gx * (j - 1);             // level 1 of the column, member-local
     const BgcDev32& b = a.bgc[it.x];
-    const int slot = acc_slot(n);
-    const bool sinks = n == PI_PFe_inorg || n == PI_Dust || n == PI_PFe_bio;
+    const bool sinks = !NUT && n != PI_DFe;
     const float ws = n == PI_PFe_bio ? b.w_sink_org : b.w_sink_inorg;
-    const bool diffuse = b.kappa_h != 0.0f || b.kappa_v != 0.0f;
-    const bool any_bc = md.any_bc != 0;
-    // tracer_forcing! of the ten nutrient tracers: aS·T(n) + aO·T(dO)
+    // tracer_forcing! of the ten nutrient tracers: aS·T(n) + aO·T(x0) (aO = 0 where there is no
+    // second tracer); of the iron tracers: T of DFe, POC, Dust, PFe_bio, PFe_inorg, each the own
+    // tracer (-1) or one of the four others x0..x3
     float aS = 0.0f, aO = 0.0f;
-    int dO = -1;
-    switch (n) {
-        case PI_DIC: dO = PI_DOC; aO = b.kDOC * dT; break;
-        case PI_DOC: aS = -b.kDOC * dT; dO = PI_POC; aO = b.kPOC * dT; break;
-        case PI_POC: aS = -b.kPOC * dT; break;
-        case PI_NH4: aS = -b.Nit * dT; dO = PI_DON; aO = b.kDON * dT; break;
-        case PI_NO3: dO = PI_NH4; aO = b.Nit * dT; break;
-        case PI_DON: aS = -b.kDON * dT; dO = PI_PON; aO = b.kPON * dT; break;
-        case PI_PON: aS = -b.kPON * dT; break;
-        case PI_PO4: dO = PI_DOP; aO = b.kDOP * dT; break;
-        case PI_DOP: aS = -b.kDOP * dT; dO = PI_POP; aO = b.kPOP * dT; break;
-        case PI_POP: aS = -b.kPOP * dT; break;
-        default: break;
+    int xo[4] = { n, n, n, n };
+    // iron forcing: position of the own tracer in (DFe, POC, Dust, PFe_bio, PFe_inorg); the others
+    // keep their order in x0..x3
+    const int pn = n == PI_DFe ? 0 : n == PI_POC ? 1 : n == PI_Dust ? 2 : n == PI_PFe_bio ? 3 : 4;
+    auto fe_at = [](int r) { return r == 0 ? PI_DFe : r == 1 ? PI_POC : r == 2 ? PI_Dust : r == 3 ? PI_PFe_bio : PI_PFe_inorg; };
+    if (NUT) {
+        switch (n) {
+            case PI_DIC: xo[0] = PI_DOC; aO = b.kDOC * dT; break;
+            case PI_DOC: aS = -b.kDOC * dT; xo[0] = PI_POC; aO = b.kPOC * dT; break;
+            case PI_POC: aS = -b.kPOC * dT; break;
+            case PI_NH4: aS = -b.Nit * dT; xo[0] = PI_DON; aO = b.kDON * dT; break;
+            case PI_NO3: xo[0] = PI_NH4; aO = b.Nit * dT; break;
+            case PI_DON: aS = -b.kDON * dT; xo[0] = PI_PON; aO = b.kPON * dT; break;
+            case PI_PON: aS = -b.kPON * dT; break;
+            case PI_PO4: xo[0] = PI_DOP; aO = b.kDOP * dT; break;
+            case PI_DOP: aS = -b.kDOP * dT; xo[0] = PI_POP; aO = b.kPOP * dT; break;
+            case PI_POP: aS = -b.kPOP * dT; break;
+            default: break;
+        }
+    } else {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) xo[e] = fe_at(e < pn ? e : e + 1);
     }
-    const bool iron = n == PI_DFe || n == PI_PFe_bio || n == PI_PFe_inorg;
     const float* __restrict__ t = a.tb + n * G + off;
     const float* __restrict__ c = a.tr + n * G + off;
     const float* __restrict__ trm = a.tr + off;           // all tracers of the member
-    const float* __restrict__ co = trm + (dO < 0 ? 0 : dO) * G;
     float* __restrict__ out = a.tr_next + n * G + off;
-    unsigned long long* __restrict__ acc = a.acc + (slot < 0 ? 0 : slot) * G + off;
+    unsigned long long* __restrict__ acc = a.acc + (NUT ? acc_slot(n) : 0) * G + off;
     const uint8_t* __restrict__ lmc = a.lm + off + qcol;
-    auto tl = [&](int kk) { return t[qcol + (min(max(kk, top), bot) - 1) * slab]; };
+    auto tl = [&](int kk) { return qcol + (min(max(kk, top), bot) - 1) * slab; };
     auto lmk = [&](int kk) -> int { return LM ? (int)lmc[(kk - 1) * slab] : 1; };
     auto fcz = [&](int l) { const float4 v = sFC[l * 32 + lane]; FCu r; r.tr = v.x; r.d0c = v.y; r.d1c = v.z; r.R = v.w; return r; };
+    // ring fill of level kk (an empty group past the end keeps the group count uniform)
+    auto issue = [&](int kk) {
+        if (kk <= kend) {
+            const int sl = (kk - k0) & (ZS - 1);
+            const int qq = qcol + (kk - 1) * slab;
+            cpa4(&R.c[sl][lane], c + qq);
+            cpa4(&R.t[sl][lane], t + tl(kk + 2));
+            if (NUT) {
+                cpa4(&R.x[0][sl][lane], trm + xo[0] * G + qq);
+                cpa8(&R.acc[sl][lane], acc + qq, sPop[(kk - k0) * 32 + lane] > 0);
+            } else if (n != PI_Dust) {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) cpa4(&R.x[e][sl][lane], trm + xo[e] * G + qq);
+            }
+        }
+        cpa_commit();
+    };
+#pragma unroll
+    for (int e = 0; e < ZS - 1; ++e) issue(k0 + e);
     // stencil windows: w (tracer_temp) and mm (land mask) at levels k-1 .. k+2 of the current cell k
-    float w0 = tl(k0 - 2), w1 = tl(k0 - 1), w2 = tl(k0), w3 = tl(k0 + 1);
+    float w0 = t[tl(k0 - 2)], w1 = t[tl(k0 - 1)], w2 = t[tl(k0)], w3 = t[tl(k0 + 1)];
     int mm0 = lmk(k0 - 2), mm1 = lmk(k0 - 1), mm2 = lmk(k0), mm3 = lmk(k0 + 1);
     float Ft = flux_v<LM>(fcz(0), w0, w1, w2, w3, mm0, mm1, mm2, mm3);
     int q = qcol + (k0 - 1) * slab;
     float sink_prev = (sinks && k0 - 1 > Hz) ? c[q - slab] : 0.0f;
-    // the loads of each level are issued one level ahead
-    float cc_next = c[q], nw_next = tl(k0 + 2);
     for (int k = k0; k <= kend; ++k, q += slab) {
-        const int l = k - k0;
-        const float cc = cc_next, nw = nw_next;
-        if (k < kend) { cc_next = c[q + slab]; nw_next = tl(k + 3); }
-        w0 = w1; w1 = w2; w2 = w3; w3 = nw;
+        const int l = k - k0, sl = l & (ZS - 1);
+        issue(k + ZS - 1);
+        cpa_wait<ZS - 1>();
+        const float cc = R.c[sl][lane];
+        w0 = w1; w1 = w2; w2 = w3; w3 = R.t[sl][lane];
         if (LM) { mm0 = mm1; mm1 = mm2; mm2 = mm3; mm3 = lmk(k + 2); }
         const int l1 = mm1, l0 = mm2;                       // land mask of cell k and k+1
         const float Fb = flux_v<LM>(fcz(l + 1), w0, w1, w2, w3, mm0, mm1, mm2, mm3);   // zero at the bottom
         const ZLev L = sLev[l];
         float Gc = (w1 - L.dtv * (mk<LM>(Ft - Fb, l0, l1) - cc * sFtr[l * 32 + lane])) - cc;
         Ft = Fb;
-        // tracer_diffusion! (tracer_diffusion.jl:1-21)
-        if (diffuse) {
-            const float dz = L.dz, az = md.dx * md.dy, volk = az * dz;
-            const float axk = md.dy * dz, ayk = md.dx * dz;
-            auto lmq = [&](int dq) -> int { return LM ? (int)lmc[(k - 1) * slab + dq] : 1; };
-            auto dif = [&](int dq, int dp) { return mulbf(mulbf(c[q + dq] - c[q + dp], lmq(dq)), lmq(dp)); };
-            const float fx1 = b.kappa_h * axk * (dif(1, 0) / md.dx), fx0 = b.kappa_h * axk * (dif(0, -1) / md.dx);
-            const float fy1 = b.kappa_h * ayk * (dif(Gx, 0) / md.dy), fy0 = b.kappa_h * ayk * (dif(0, -Gx) / md.dy);
-            const float fz0 = b.kappa_v * az * (dif(-slab, 0) / dz), fz1 = b.kappa_v * az * (dif(0, slab) / L.dzn);
-            const float ax_ = mulbf(mulbf(fx1 - fx0, lmq(1)), l1);
-            const float ay_ = mulbf(mulbf(fy1 - fy0, lmq(Gx)), l1);
-            const float az_ = mulbf(mulbf(fz0 - fz1, l0), l1);
-            Gc += 1.0f / volk * (ax_ + ay_ + az_) * dT;
+        if (GEN) {
+            // tracer_diffusion! (tracer_diffusion.jl:1-21)
+            if (b.kappa_h != 0.0f || b.kappa_v != 0.0f) {
+                const float dz = L.dz, az = md.dx * md.dy, volk = az * dz;
+                const float axk = md.dy * dz, ayk = md.dx * dz;
+                auto lmq = [&](int dq) -> int { return LM ? (int)lmc[(k - 1) * slab + dq] : 1; };
+                auto dif = [&](int dq, int dp) { return mulbf(mulbf(c[q + dq] - c[q + dp], lmq(dq)), lmq(dp)); };
+                const float fx1 = b.kappa_h * axk * (dif(1, 0) / md.dx), fx0 = b.kappa_h * axk * (dif(0, -1) / md.dx);
+                const float fy1 = b.kappa_h * ayk * (dif(Gx, 0) / md.dy), fy0 = b.kappa_h * ayk * (dif(0, -Gx) / md.dy);
+                const float fz0 = b.kappa_v * az * (dif(-slab, 0) / dz), fz1 = b.kappa_v * az * (dif(0, slab) / L.dzn);
+                const float ax_ = mulbf(mulbf(fx1 - fx0, lmq(1)), l1);
+                const float ay_ = mulbf(mulbf(fy1 - fy0, lmq(Gx)), l1);
+                const float az_ = mulbf(mulbf(fz0 - fz1, l0), l1);
+                Gc += 1.0f / volk * (ax_ + ay_ + az_) * dT;
+            }
         }
-        // tracer_sinking! (tracer_sinking.jl:1-42)
-        if (sinks) {
-            const float fup = (k - 1 <= Hz) ? 0.0f : ws * sink_prev;
-            const float fdn = (k >= bot) ? 0.0f : ws * cc;
-            Gc += (fup - fdn) * L.sk;
-            sink_prev = cc;
-        }
-        // tracer_forcing! (tracer_forcings.jl:2-50) on max(0, tracer)
-        if (!iron) {
-            float fo = aS * fmaxf(0.0f, cc);
-            if (dO >= 0) fo += aO * fmaxf(0.0f, co[q]);
-            Gc += fo;
+        if (NUT) {
+            // tracer_forcing! (tracer_forcings.jl:2-50) on max(0, tracer)
+            Gc += aS * fmaxf(0.0f, cc) + aO * fmaxf(0.0f, R.x[0][sl][lane]);
         } else {
-            const float dfe = fmaxf(0.0f, trm[PI_DFe * G + q]), poc = fmaxf(0.0f, trm[PI_POC * G + q]);
-            const float dust = fmaxf(0.0f, trm[PI_Dust * G + q]);
-            const float pfeb = fmaxf(0.0f, trm[PI_PFe_bio * G + q]), pfei = fmaxf(0.0f, trm[PI_PFe_inorg * G + q]);
-            Gc += fe_forcing(n, b, dT, dfe, poc, dust, pfeb, pfei);
+            // tracer_sinking! (tracer_sinking.jl:1-42)
+            if (sinks) {
+                const float fup = (k - 1 <= Hz) ? 0.0f : ws * sink_prev;
+                const float fdn = (k >= bot) ? 0.0f : ws * cc;
+                Gc += (fup - fdn) * L.sk;
+                sink_prev = cc;
+            }
+            if (n != PI_Dust) {
+                const float x0 = R.x[0][sl][lane], x1 = R.x[1][sl][lane], x2 = R.x[2][sl][lane], x3 = R.x[3][sl][lane];
+                auto T = [&](int e) {
+                    const int sr = e < pn ? e : (e == pn ? -1 : e - 1);
+                    return fmaxf(0.0f, sr < 0 ? cc : sr == 0 ? x0 : sr == 1 ? x1 : sr == 2 ? x2 : x3);
+                };
+                Gc += fe_forcing(n, b, dT, T(0), T(1), T(2), T(3), T(4));
+            }
         }
-        // apply_bcs! (apply_bcs.jl:4-98)
-        if (any_bc) {
+        if (GEN && md.any_bc) {
+            // apply_bcs! (apply_bcs.jl:4-98)
             const int64_t itn = a.st->iteration + 1;
             const FluxBC32* B = a.bcs + md.bc_off + n * 6;
             const int ii = i - Hx, jj = j - md.Hy, kk = k - Hz;
@@ -1044,15 +1124,35 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& md, con
             if (B[PI_BOTTOM].kind && k == bot) Gc += getbc32(B[PI_BOTTOM], ii, jj, itn) * dT * az / volk;
             if (B[PI_TOP].kind && k == top) Gc -= getbc32(B[PI_TOP], ii, jj, itn) * dT * az / volk;
         }
-        // particle terms from the fixed-point sums, apply_tendency! (tracer_update.jl:6-13)
+        // particle terms from the fixed-point sums (zeroed as they are consumed), apply_tendency!
+        // (tracer_update.jl:6-13)
         float plk = 0.0f;
-        if (slot >= 0 && sPop[l * 32 + lane] > 0) {
-            const long long vv = (long long)acc[q];
+        if (NUT) {
+            const long long vv = (long long)R.acc[sl][lane];   // zero where the cell holds no individual
             if (vv) { acc[q] = 0ull; plk = (float)((double)vv * L.fxv); }
         }
         out[q] = cc + (Gc + plk);
     }
+    cpa_wait<0>();
 }
+
+template <int LZ, bool LM>
+__device__ __forceinline__ void z_walk_any(const TrArgs& a, const MemberDev& m, const int4 it, const float4* sFC,
+                                           const float* sFtr, const int* sPop, const ZLev* sLev, ZRing& R) {
+    const BgcDev32& b = a.bgc[it.x];
+    const bool gen = m.any_bc || b.kappa_h != 0.0f || b.kappa_v != 0.0f;
+    const bool nut = acc_slot(threadIdx.y) >= 0;
+    if (nut) {
+        if (gen) z_walk<LZ, LM, true, true>(a, m, it, sFC, sFtr, sPop, sLev, R);
+        else z_walk<LZ, LM, true, false>(a, m, it, sFC, sFtr, sPop, sLev, R);
+    } else {
+        if (gen) z_walk<LZ, LM, false, true>(a, m, it, sFC, sFtr, sPop, sLev, R);
+        else z_walk<LZ, LM, false, false>(a, m, it, sFC, sFtr, sPop, sLev, R);
+    }
+}
+
+// dynamic shared memory of k32_ztail: one ring per tracer warp
+inline size_t ztail_smem() { return sizeof(ZRing) * PI_NTRACERS; }
 
 template <int LZ>
 __global__ void __launch_bounds__(32 * PI_NTRACERS, 2) k32_ztail(TrArgs a) {
@@ -1061,6 +1161,8 @@ __global__ void __launch_bounds__(32 * PI_NTRACERS, 2) k32_ztail(TrArgs a) {
     __shared__ float sFtr[LZ * 32];         // vertical transport term of the cells k0 .. k0+LZ-1
     __shared__ int sPop[LZ * 32];           // individuals in those cells
     __shared__ ZLev sLev[LZ];               // per-level constants
+    extern __shared__ __align__(16) unsigned char zsm[];
+    ZRing* ring = reinterpret_cast<ZRing*>(zsm);
     const int tid = threadIdx.y * 32 + threadIdx.x;
     for (int w = blockIdx.x; w < a.nitems; w += gridDim.x) {
         const int4 it = a.items[w];
@@ -1102,8 +1204,8 @@ __global__ void __launch_bounds__(32 * PI_NTRACERS, 2) k32_ztail(TrArgs a) {
             sLev[tid] = L;
         }
         __syncthreads();
-        if (m.all_water) z_walk<LZ, false>(a, m, it, sFC, sFtr, sPop, sLev);
-        else z_walk<LZ, true>(a, m, it, sFC, sFtr, sPop, sLev);
+        if (m.all_water) z_walk_any<LZ, false>(a, m, it, sFC, sFtr, sPop, sLev, ring[threadIdx.y]);
+        else z_walk_any<LZ, true>(a, m, it, sFC, sFtr, sPop, sLev, ring[threadIdx.y]);
         __syncthreads();
     }
 }
