@@ -15,6 +15,8 @@
 // where the centred gradient is within a few FP32 ulps of zero.
 #pragma once
 
+#include <cstddef>
+
 #include "fp32_internal.h"
 
 namespace p32 {
@@ -116,15 +118,21 @@ __device__ __forceinline__ int clampb(int v, int lo, int hi, bool& bad) {
 // sample points a small fraction of a cell apart, usually from the same field (vel₀ = vel½ = vel₁
 // between velocity refreshes), so a stage reuses the corners of the previous one when the field
 // and the base corner are the same: the values are identical, only the loads are saved.
-struct Corners { const float* f; int q; float v[8]; };
+struct Corners { int fid; int q; float v[8]; };   // fid: which of the step's fields (0 vel₀, 1 vel½, 2 vel₁)
 
 // Member constants of the particle kernels, held in registers.
 struct PGeom {
     int Nx, Ny, Nz, Hx, Hy, Hz, Gx, Gy, Gz, tx, ty, tz, dz_off;
     float rdx, rdy;
+    int fh, f1;     // field ids of vel½ and vel₁ (fields that are the same arrays share an id)
 };
-__device__ __forceinline__ PGeom pgeom(const MemberDev& m) {
+__device__ __forceinline__ bool same3(const float* const* a, const float* const* b) {
+    return a[0] == b[0] && a[1] == b[1] && a[2] == b[2];
+}
+__device__ __forceinline__ PGeom pgeom(const MemberDev& m, const MemberForcing& f) {
     PGeom g;
+    g.fh = same3(f.velh, f.vel0) ? 0 : 1;
+    g.f1 = same3(f.vel1, f.velh) ? g.fh : same3(f.vel1, f.vel0) ? 0 : 2;
     g.Nx = m.Nx; g.Ny = m.Ny; g.Nz = m.Nz; g.Hx = m.Hx; g.Hy = m.Hy; g.Hz = m.Hz;
     g.Gx = m.Gx; g.Gy = m.Gy; g.Gz = m.Gz; g.tx = m.tx; g.ty = m.ty; g.tz = m.tz; g.dz_off = m.dz_off;
     g.rdx = m.rdx; g.rdy = m.rdy;
@@ -134,7 +142,7 @@ __device__ __forceinline__ PGeom pgeom(const MemberDev& m) {
 // trilinear interpolation of one velocity component (member-local field pointer), in grid cells
 // per second
 template <int COMP>
-__device__ __forceinline__ float itpl32(const PGeom& m, const float* __restrict__ f,
+__device__ __forceinline__ float itpl32(const PGeom& m, const float* __restrict__ f, int fid,
                                         const float* __restrict__ rdzC, const Ax1& X, const Ax1& Y,
                                         const Ax1& Z, bool& bad, Corners& cc) {
     int i, j, k;
@@ -144,9 +152,9 @@ __device__ __forceinline__ float itpl32(const PGeom& m, const float* __restrict_
     axis_iw(Z, m.Hz, COMP == 2, k, zd);
     i = clampb(i, 1, m.Gx - 1, bad); j = clampb(j, 1, m.Gy - 1, bad); k = clampb(k, 1, m.Gz - 1, bad);
     const int q = (i - 1) + m.Gx * ((j - 1) + m.Gy * (k - 1));
-    if (cc.f != f || cc.q != q) {
+    if (cc.fid != fid || cc.q != q) {
         const int sy = m.Gx, sz = m.Gx * m.Gy;
-        cc.f = f; cc.q = q;
+        cc.fid = fid; cc.q = q;
         cc.v[0] = __ldg(f + q); cc.v[1] = __ldg(f + q + sy); cc.v[2] = __ldg(f + q + 1); cc.v[3] = __ldg(f + q + 1 + sy);
         cc.v[4] = __ldg(f + q + sz); cc.v[5] = __ldg(f + q + sy + sz); cc.v[6] = __ldg(f + q + 1 + sz);
         cc.v[7] = __ldg(f + q + 1 + sy + sz);
@@ -266,49 +274,52 @@ struct MoveArgs {
 __device__ __forceinline__ void move_one(const MoveArgs& a, const MemberDev& m, const PGeom& pg, int mi, int s,
                                          long long slot, long long g, uint32_t iter, int& is_div, int& is_free) {
     const IndDev32& P = a.P;
-    const uint8_t fl = P.flags[g];
+    // the slot's state in one round trip (the offsets of an inactive slot are read and unused)
+    const uint8_t fl = P.flags[g], stt = P.stat[g];
+    const int32_t code = P.cell[g];
+    const float ox = P.ox[g], oy = P.oy[g], oz = P.oz[g];
     if (!(fl & F32_AC)) {
         // every stage multiplies by ac: the position becomes (0, 0, 0) and the cell (Hx, Hy, Hz)
-        if (P.cell[g] != -1) {
+        if (code != -1) {
             P.cell[g] = -1;
             P.ox[g] = 0.0f; P.oy[g] = 0.0f; P.oz[g] = 0.0f;
         }
-        if (P.stat[g]) P.stat[g] = 0;
+        if (stt) P.stat[g] = 0;
         is_div = 0; is_free = 1;
         return;
     }
     uint32_t* err = a.err;
-    const uint8_t stt = P.stat[g];
     int ci, cj, ck;
-    unpack_int(m, P.cell[g], ci, cj, ck);
+    unpack_int(m, code, ci, cj, ck);
     // ΔzC at the find_inds! zi of the previous step, plus Hz (particle_diffusion.jl:26-28)
     int zi = ck + 1 + pg.Hz;
     if (stt & F32_ST_STALE) { int a0, a1; unpack_halo(m, P.scell[g], a0, a1, zi); }
     bool bad = false;
     const int kdz = clampb(zi + pg.Hz, 1, pg.Gz, bad);
     const MemberForcing& f = a.F[mi];
-    const Ax1 X0{ci, P.ox[g]}, Y0{cj, P.oy[g]}, Z0{ck, P.oz[g]};
+    const Ax1 X0{ci, ox}, Y0{cj, oy}, Z0{ck, oz};
     const float dT = a.dT, hdT = 0.5f * dT;
     const float* __restrict__ rdzC = a.rdzC;
-    Corners cu{nullptr, -1, {}}, cv{nullptr, -1, {}}, cw{nullptr, -1, {}};
-    float u1 = itpl32<0>(pg, f.vel0[0], rdzC, X0, Y0, Z0, bad, cu);
-    float v1 = itpl32<1>(pg, f.vel0[1], rdzC, X0, Y0, Z0, bad, cv);
-    float w1 = itpl32<2>(pg, f.vel0[2], rdzC, X0, Y0, Z0, bad, cw);
+    Corners cu{-1, -1, {}}, cv{-1, -1, {}}, cw{-1, -1, {}};
+    const int fh = pg.fh, f1 = pg.f1;
+    float u1 = itpl32<0>(pg, f.vel0[0], 0, rdzC, X0, Y0, Z0, bad, cu);
+    float v1 = itpl32<1>(pg, f.vel0[1], 0, rdzC, X0, Y0, Z0, bad, cv);
+    float w1 = itpl32<2>(pg, f.vel0[2], 0, rdzC, X0, Y0, Z0, bad, cw);
     float u2 = u1, v2 = v1, w2 = w1;
     Ax1 X = X0, Y = Y0, Z = Z0;
     move(X, u1 * hdT, pg.Nx, pg.tx); move(Y, v1 * hdT, pg.Ny, pg.ty); move(Z, -(w1 * hdT), pg.Nz, pg.tz);
-    u1 = itpl32<0>(pg, f.velh[0], rdzC, X, Y, Z, bad, cu); v1 = itpl32<1>(pg, f.velh[1], rdzC, X, Y, Z, bad, cv);
-    w1 = itpl32<2>(pg, f.velh[2], rdzC, X, Y, Z, bad, cw);
+    u1 = itpl32<0>(pg, f.velh[0], fh, rdzC, X, Y, Z, bad, cu); v1 = itpl32<1>(pg, f.velh[1], fh, rdzC, X, Y, Z, bad, cv);
+    w1 = itpl32<2>(pg, f.velh[2], fh, rdzC, X, Y, Z, bad, cw);
     u2 += u1 * 2.0f; v2 += v1 * 2.0f; w2 += w1 * 2.0f;
     X = X0; Y = Y0; Z = Z0;
     move(X, u1 * hdT, pg.Nx, pg.tx); move(Y, v1 * hdT, pg.Ny, pg.ty); move(Z, -(w1 * hdT), pg.Nz, pg.tz);
-    u1 = itpl32<0>(pg, f.velh[0], rdzC, X, Y, Z, bad, cu); v1 = itpl32<1>(pg, f.velh[1], rdzC, X, Y, Z, bad, cv);
-    w1 = itpl32<2>(pg, f.velh[2], rdzC, X, Y, Z, bad, cw);
+    u1 = itpl32<0>(pg, f.velh[0], fh, rdzC, X, Y, Z, bad, cu); v1 = itpl32<1>(pg, f.velh[1], fh, rdzC, X, Y, Z, bad, cv);
+    w1 = itpl32<2>(pg, f.velh[2], fh, rdzC, X, Y, Z, bad, cw);
     u2 += u1 * 2.0f; v2 += v1 * 2.0f; w2 += w1 * 2.0f;
     X = X0; Y = Y0; Z = Z0;
     move(X, u1 * dT, pg.Nx, pg.tx); move(Y, v1 * dT, pg.Ny, pg.ty); move(Z, -(w1 * dT), pg.Nz, pg.tz);
-    u1 = itpl32<0>(pg, f.vel1[0], rdzC, X, Y, Z, bad, cu); v1 = itpl32<1>(pg, f.vel1[1], rdzC, X, Y, Z, bad, cv);
-    w1 = itpl32<2>(pg, f.vel1[2], rdzC, X, Y, Z, bad, cw);
+    u1 = itpl32<0>(pg, f.vel1[0], f1, rdzC, X, Y, Z, bad, cu); v1 = itpl32<1>(pg, f.vel1[1], f1, rdzC, X, Y, Z, bad, cv);
+    w1 = itpl32<2>(pg, f.vel1[2], f1, rdzC, X, Y, Z, bad, cw);
     const float sixth = 1.0f / 6.0f;
     u2 = (u2 + u1) * sixth; v2 = (v2 + v1) * sixth; w2 = (w2 + w1) * sixth;
     X = X0; Y = Y0; Z = Z0;
@@ -362,7 +373,7 @@ __device__ __forceinline__ void move_one(const MoveArgs& a, const MemberDev& m, 
     is_div = dv2; is_free = !ac2;
 }
 
-__global__ void __launch_bounds__(256, 3) k32_move(MoveArgs a) {
+__global__ void __launch_bounds__(256, 2) k32_move(MoveArgs a) {
     if (stopped(a.err)) return;
     __shared__ unsigned int sh_d, sh_f;
     __shared__ PGeom sg;
@@ -373,7 +384,7 @@ __global__ void __launch_bounds__(256, 3) k32_move(MoveArgs a) {
         int mi, s;
         seg_of(a.T, tl.x, mi, s);
         const MemberDev& m = a.T.md[mi];
-        if (threadIdx.x == 0) sg = pgeom(m);
+        if (threadIdx.x == 0) sg = pgeom(m, a.F[mi]);
         __syncthreads();
         const long long base = m.slot_off + (long long)s * m.C;
         unsigned int nd = 0, nf = 0;
@@ -598,12 +609,14 @@ struct PhysArgs {
 __device__ __forceinline__ void phys_one(const PhysArgs& a, const MemberDev& m, int mi, int s, long long slot,
                                          long long g, uint32_t iter, double tnow) {
     const IndDev32& P = a.P;
-    if (!(P.flags[g] & F32_AC)) return;
-    const uint8_t stt = P.stat[g];
+    // flags, status and cell in one round trip; the quotas are loaded with the environment
+    const uint8_t fl = P.flags[g], stt = P.stat[g];
+    const int32_t code = P.cell[g];
+    if (!(fl & F32_AC)) return;
     const int ac0 = stt & F32_ST_AC0;
     int q;
     if (stt & F32_ST_STALE) { int xi, yi, zi; unpack_halo(m, P.scell[g], xi, yi, zi); q = gid3(m, xi, yi, zi); }
-    else { int ci, cj, ck; unpack_int(m, P.cell[g], ci, cj, ck); q = q_of(m, ci, cj, ck); }
+    else { int ci, cj, ck; unpack_int(m, code, ci, cj, ck); q = q_of(m, ci, cj, ck); }
     const long long cq = m.cell_off + q;
     const long long G = a.Gtot;
     const SpeciesDev32& p = a.sp[mi * a.T.nsp + s];
@@ -959,18 +972,27 @@ __device__ __forceinline__ float fe_forcing(int n, const BgcDev32& b, float dT, 
 // Asynchronous global → shared copies (cp.async): a warp's z walk reads the inputs of each level
 // from a ring of ZS levels filled ahead of it, so ZS - 1 levels of loads are in flight while it
 // computes. A lane reads back only what it copied itself, which wait_group makes visible to it.
-__device__ __forceinline__ void cpa4(float* sdst, const float* gsrc) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n"
-                 :: "r"((unsigned)__cvta_generic_to_shared(sdst)), "l"(gsrc) : "memory");
+__device__ __forceinline__ void cpa4(unsigned sdst, const float* gsrc) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" :: "r"(sdst), "l"(gsrc) : "memory");
 }
 // 8 bytes, or zeros without reading when `on` is false
-__device__ __forceinline__ void cpa8(unsigned long long* sdst, const unsigned long long* gsrc, bool on) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n"
-                 :: "r"((unsigned)__cvta_generic_to_shared(sdst)), "l"(gsrc), "r"(on ? 8 : 0) : "memory");
+__device__ __forceinline__ void cpa8(unsigned sdst, const unsigned long long* gsrc, bool on) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" :: "r"(sdst), "l"(gsrc), "r"(on ? 8 : 0) : "memory");
 }
 __device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cpa_wait() { asm volatile("cp.async.wait_group %0;\n" :: "n"(N) : "memory"); }
+// shared loads ordered after the wait above (volatile asm keeps program order among them)
+__device__ __forceinline__ float lds_f32(unsigned a) {
+    float v;
+    asm volatile("ld.shared.f32 %0, [%1];\n" : "=f"(v) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ unsigned long long lds_u64(unsigned a) {
+    unsigned long long v;
+    asm volatile("ld.shared.u64 %0, [%1];\n" : "=l"(v) : "r"(a));
+    return v;
+}
 
 #define ZS 4                              // levels of a z walk ring (power of two)
 // One warp's ring: own tracer c, tracer_temp t two levels below, up to four other tracers the
@@ -981,6 +1003,8 @@ struct ZRing {
     float x[4][ZS][32];
     unsigned long long acc[ZS][32];
 };
+static_assert(ZS == 4 && offsetof(ZRing, t) == 512 && offsetof(ZRing, x) == 1024 && offsetof(ZRing, acc) == 3072 &&
+              sizeof(ZRing) == 4096, "z walk ring layout");
 
 // NUT: the ten nutrient tracers (linear forcing, particle sums); otherwise the three iron tracers
 // and dust (iron forcing, sinking). GEN: diffusion or flux boundary conditions are switched on.
@@ -1037,20 +1061,30 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& md, con
     auto tl = [&](int kk) { return qcol + (min(max(kk, top), bot) - 1) * slab; };
     auto lmk = [&](int kk) -> int { return LM ? (int)lmc[(kk - 1) * slab] : 1; };
     auto fcz = [&](int l) { const float4 v = sFC[l * 32 + lane]; FCu r; r.tr = v.x; r.d0c = v.y; r.d1c = v.z; r.R = v.w; return r; };
-    // ring fill of level kk (an empty group past the end keeps the group count uniform)
+    // ring addresses of this lane (shared space): stage sl of c at rc + 128 sl, t at rc + 512 +
+    // 128 sl, x[e] at rc + 1024 + 512 e + 128 sl, the particle sum at ra + 256 sl
+    const unsigned rc = (unsigned)__cvta_generic_to_shared(&R.c[0][lane]);
+    const unsigned ra = (unsigned)__cvta_generic_to_shared(&R.acc[0][lane]);
+    const float* __restrict__ x0p = trm + xo[0] * G;
+    const float* __restrict__ x1p = trm + xo[1] * G;
+    const float* __restrict__ x2p = trm + xo[2] * G;
+    const float* __restrict__ x3p = trm + xo[3] * G;
+    // ring fill of level kk; past the last level the last level is copied again into the stage
+    // that level kk would use, which no iteration reads
     auto issue = [&](int kk) {
-        if (kk <= kend) {
-            const int sl = (kk - k0) & (ZS - 1);
-            const int qq = qcol + (kk - 1) * slab;
-            cpa4(&R.c[sl][lane], c + qq);
-            cpa4(&R.t[sl][lane], t + tl(kk + 2));
-            if (NUT) {
-                cpa4(&R.x[0][sl][lane], trm + xo[0] * G + qq);
-                cpa8(&R.acc[sl][lane], acc + qq, sPop[(kk - k0) * 32 + lane] > 0);
-            } else if (n != PI_Dust) {
-#pragma unroll
-                for (int e = 0; e < 4; ++e) cpa4(&R.x[e][sl][lane], trm + xo[e] * G + qq);
-            }
+        const unsigned so = (unsigned)((kk - k0) & (ZS - 1)) * 128u;
+        const int kc = min(kk, kend);
+        const int qq = qcol + (kc - 1) * slab;
+        cpa4(rc + so, c + qq);
+        cpa4(rc + 512u + so, t + tl(kc + 2));
+        if (NUT) {
+            cpa4(rc + 1024u + so, x0p + qq);
+            cpa8(ra + 2u * so, acc + qq, kk <= kend && sPop[(kc - k0) * 32 + lane] > 0);
+        } else if (n != PI_Dust) {
+            cpa4(rc + 1024u + so, x0p + qq);
+            cpa4(rc + 1536u + so, x1p + qq);
+            cpa4(rc + 2048u + so, x2p + qq);
+            cpa4(rc + 2560u + so, x3p + qq);
         }
         cpa_commit();
     };
@@ -1063,11 +1097,12 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& md, con
     int q = qcol + (k0 - 1) * slab;
     float sink_prev = (sinks && k0 - 1 > Hz) ? c[q - slab] : 0.0f;
     for (int k = k0; k <= kend; ++k, q += slab) {
-        const int l = k - k0, sl = l & (ZS - 1);
+        const int l = k - k0;
+        const unsigned so = (unsigned)(l & (ZS - 1)) * 128u;
         issue(k + ZS - 1);
         cpa_wait<ZS - 1>();
-        const float cc = R.c[sl][lane];
-        w0 = w1; w1 = w2; w2 = w3; w3 = R.t[sl][lane];
+        const float cc = lds_f32(rc + so);
+        w0 = w1; w1 = w2; w2 = w3; w3 = lds_f32(rc + 512u + so);
         if (LM) { mm0 = mm1; mm1 = mm2; mm2 = mm3; mm3 = lmk(k + 2); }
         const int l1 = mm1, l0 = mm2;                       // land mask of cell k and k+1
         const float Fb = flux_v<LM>(fcz(l + 1), w0, w1, w2, w3, mm0, mm1, mm2, mm3);   // zero at the bottom
@@ -1092,7 +1127,7 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& md, con
         }
         if (NUT) {
             // tracer_forcing! (tracer_forcings.jl:2-50) on max(0, tracer)
-            Gc += aS * fmaxf(0.0f, cc) + aO * fmaxf(0.0f, R.x[0][sl][lane]);
+            Gc += aS * fmaxf(0.0f, cc) + aO * fmaxf(0.0f, lds_f32(rc + 1024u + so));
         } else {
             // tracer_sinking! (tracer_sinking.jl:1-42)
             if (sinks) {
@@ -1102,7 +1137,8 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& md, con
                 sink_prev = cc;
             }
             if (n != PI_Dust) {
-                const float x0 = R.x[0][sl][lane], x1 = R.x[1][sl][lane], x2 = R.x[2][sl][lane], x3 = R.x[3][sl][lane];
+                const float x0 = lds_f32(rc + 1024u + so), x1 = lds_f32(rc + 1536u + so);
+                const float x2 = lds_f32(rc + 2048u + so), x3 = lds_f32(rc + 2560u + so);
                 auto T = [&](int e) {
                     const int sr = e < pn ? e : (e == pn ? -1 : e - 1);
                     return fmaxf(0.0f, sr < 0 ? cc : sr == 0 ? x0 : sr == 1 ? x1 : sr == 2 ? x2 : x3);
@@ -1128,7 +1164,7 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& md, con
         // (tracer_update.jl:6-13)
         float plk = 0.0f;
         if (NUT) {
-            const long long vv = (long long)R.acc[sl][lane];   // zero where the cell holds no individual
+            const long long vv = (long long)lds_u64(ra + 2u * so);   // zero where the cell holds no individual
             if (vv) { acc[q] = 0ull; plk = (float)((double)vv * L.fxv); }
         }
         out[q] = cc + (Gc + plk);
