@@ -2,7 +2,7 @@
 """Throughput of the PlanktonIndividuals model time step on B200: FP32 batched form vs FP64 plain.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload config2|config4|config5]
+                    [--workload config2|config3|config4|config5]
 
 Default workload: config 2 — 256×256×64 grid (50 m × 50 m × 2 m), 2 species × 2,097,152
 individuals seeded in the top 40 m, divergence-free random-Fourier velocity refreshed every 60
@@ -15,8 +15,14 @@ the C-ABI (pi_create(PI_FP32) + pi_set_velocity/PARF/temp + pi_time_step + pi_co
 host buffers: each step uploads its forcing snapshot from pinned host memory and reads back the
 population counts.
 
+--workload config3 runs the mixed-precision case at scale (512×512×128, 4 species × 16,777,216
+individuals with their own size distributions, dt = 20 s) the same way as config 2.
 --workload config4 / config5 run the batched ensembles (64 uneven 3D members; 4096 0D boxes) in
 the FP32 batched form; the members are split across ranks (scaling "strong").
+
+`step_roofline` relates the whole step to HBM bandwidth with per-unit bytes of the FP32 form:
+106 B per active individual (read and write of its persistent state) and 308 B per interior cell
+(14 tracers read and written, velocities, temperature, PAR, fixed-point sums).
 
 Multi-GPU (config 2): the model domain is not partitioned; each rank runs an independent replica
 (scaling "weak") and `value` sums the replicas' individual-steps over the slowest rank's time.
@@ -24,7 +30,8 @@ Multi-GPU (config 2): the model domain is not partitioned; each rank runs an ind
 --accuracy reports each output's error of the FP32 batched form against the FP64 form, which the
 GPU parity tests show to be bit-identical to the CPU oracle: config 2 over --acc-steps steps
 (population counts every 100 steps, active-slot and cell mismatches, quota and position errors,
-interior tracer-mass errors) or, with --workload config5, --acc-boxes boxes over 2880 steps.
+interior tracer-mass errors), the same for config 3 with --workload config3, or, with --workload
+config5, --acc-boxes boxes over 2880 steps.
 
 --impl reference times the reference algorithm's CPU implementation: the reference is Julia
 (absent here), so this is the CPU oracle (a Float64 restatement of TimeStep!) with all host
@@ -55,16 +62,17 @@ def parse():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="config2", choices=["config2", "config4", "config5"])
+    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "config5"])
     ap.add_argument("--fp64-steps", type=int, default=50)
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--profile-steps", type=int, default=5)
     ap.add_argument("--tune-steps", type=int, default=2)
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--nx", type=int, default=256, help="config 2 horizontal size (smaller for profiling)")
-    ap.add_argument("--nz", type=int, default=64)
-    ap.add_argument("--n-per-species", type=int, default=2_097_152)
+    ap.add_argument("--nx", type=int, default=None, help="config 2/3 horizontal size (smaller for profiling); "
+                    "default 256 (config 2), 512 (config 3)")
+    ap.add_argument("--nz", type=int, default=None, help="default 64 (config 2), 128 (config 3)")
+    ap.add_argument("--n-per-species", type=int, default=None, help="default 2,097,152 (config 2), 16,777,216 (config 3)")
     ap.add_argument("--accuracy", action="store_true",
                     help="report the FP32 form's errors against the FP64 form (bit-exact to the CPU oracle)")
     ap.add_argument("--acc-steps", type=int, default=1000)
@@ -161,9 +169,31 @@ def algorithmic_bytes(name, members, n_active_total, n_slots_total):
     return None
 
 
+_SNAPS = {}
+
+
+def snapshots(wl, nsnap):
+    """Velocity snapshots 0..nsnap-1 of a workload, computed once per run."""
+    have = _SNAPS.setdefault(id(wl), [])
+    while len(have) < nsnap:
+        have.append(wl.velocity(len(have)))
+    return have[:nsnap]
+
+
 def series_arrays(wl, nsnap):
-    snaps = [wl.velocity(i) for i in range(nsnap)]
+    snaps = snapshots(wl, nsnap)
     return {c: np.stack([sn[q] for sn in snaps], axis=-1) for q, c in enumerate("uvw")}
+
+
+B_IND_FP32, B_CELL_FP32 = 106, 308      # algorithmic bytes per active individual / interior cell
+
+
+def step_roofline(n_ind, n_cells, ms_per_step):
+    hbm, kind = measured_peaks()
+    byts = n_ind * B_IND_FP32 + n_cells * B_CELL_FP32
+    ach = byts / (ms_per_step / 1e3) / 1e9
+    return {"bytes_per_step": int(byts), "achieved": round(ach, 1), "peak": hbm, "peak_source": kind,
+            "unit": "GB/s", "frac": round(ach / hbm, 4)}
 
 
 def profile_roofline(prof, members, nact, nslots):
@@ -281,7 +311,7 @@ def run_e2e(wl, args, lib, precision):
     m = CModel(lib, "pi_", wl.grid, wl.bgc, wl.phyt, wl.nsp, wl.capacity, wl.seed, precision=precision)
     m.set_state(wl.individuals, wl.tracers)
     nsnap = wl.snapshots_needed(args.e2e_steps + 2)
-    snaps = [wl.velocity(i) for i in range(nsnap)]
+    snaps = snapshots(wl, nsnap)
     import ctypes as ct
     sp = ct.c_void_p()
     m.lib.pi_get_stream(m.h, ct.byref(sp))
@@ -336,9 +366,18 @@ def run_ours(args):
         dist.init_process_group("nccl", device_id=torch.device("cuda", local))
     lib = _lib.load()
     if args.workload == "config2":
+        args.nx, args.nz = args.nx or 256, args.nz or 64
+        args.n_per_species = args.n_per_species or 2_097_152
         members = [W.config2(nx=args.nx, nz=args.nz, N_per_species=args.n_per_species, seed=2 + rank)]
         wdesc = (f"config2: {args.nx}x{args.nx}x{args.nz} grid, 2 species x {args.n_per_species:,} individuals, "
                  f"random-Fourier velocity refreshed every 60 steps, dt=30 s")
+        scaling = "weak"
+    elif args.workload == "config3":
+        args.nx, args.nz = args.nx or 512, args.nz or 128
+        args.n_per_species = args.n_per_species or 16_777_216
+        members = [W.config3(nx=args.nx, nz=args.nz, N_per_species=args.n_per_species, seed=3 + rank)]
+        wdesc = (f"config3: {args.nx}x{args.nx}x{args.nz} grid, 4 species x {args.n_per_species:,} individuals "
+                 "(lognormal sizes, mu -0.5/0/0.5/1), random-Fourier velocity refreshed every 60 steps, dt=20 s")
         scaling = "weak"
     elif args.workload == "config4":
         from PlanktonIndividuals.batch import member_cost, shard_members
@@ -372,7 +411,7 @@ def run_ours(args):
     value = ind_all / (t_max / 1e3)
     cell_steps = K * Vall / (t_max / 1e3)
     fp64 = e2e = None
-    if args.workload == "config2":
+    if args.workload in ("config2", "config3"):
         if args.fp64_steps > 0:
             fp64 = run_fp64(members[0], args, lib)
         if args.e2e_steps > 0:
@@ -390,7 +429,7 @@ def run_ours(args):
             "scaling": scaling, "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
             "config": {"workload": wdesc, "form": "fp32 batched (CUDA graph, autotuned launch shapes)",
                        "members_per_rank": len(members),
-                       "l2": "inputs larger than L2 (config2 state ~1 GB per model)",
+                       "l2": "inputs larger than L2 (tracer and particle state of every member over 1 GB)",
                        "parallelism": f"{'replicas' if scaling == 'weak' else 'members split'} x{ws}"},
             "cell_steps_per_s": round(cell_steps, 1),
             "individuals": int(r32["n0"]),
@@ -398,8 +437,10 @@ def run_ours(args):
             "fp32_over_fp64": (round(value / ws / fp64["value"], 3) if fp64 else None),
             "kernel_profile_ms_per_step": {k: round(v[1] / P, 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
             "profile_share": {k: round(v[1] / r32["tot_ms"], 4) for k, v in prof.items()},
-            "roofline": r32["roof"], "cpu_baseline": cpu, "e2e": e2e, "clocks": r32["clocks"],
-            "gpu_launches": K * 14,
+            "roofline": r32["roof"],
+            "step_roofline": step_roofline(ind_all / K, Vall, t_max / K),
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": r32["clocks"],
+            "gpu_launches": K * 16,
             "autotune": {"steps": r32["n_tune"], "choices": r32["tune"].strip().splitlines()},
         }
     if dist:
@@ -480,7 +521,7 @@ def run_accuracy(args):
                 "max_count_diff": int(max(abs(a - c) for a, c in zip(c32, c64))),
                 "mean_growth_factor": round(float(np.mean(np.array(c64) / np.array(n0))), 4),
                 "max_tracer_mass_rel_err": float(max(mass)), "seconds": round(time.time() - t0, 1)}
-    wl = W.config2(seed=2)
+    wl = W.config3(seed=3) if args.workload == "config3" else W.config2(seed=2)
     steps = args.acc_steps
     m64, sim, keep = fp64_sim(lib, wl, steps)
     b = fp32_batch([wl], steps)
@@ -504,7 +545,15 @@ def run_accuracy(args):
             "quota_rel_max": {k: float(np.max(np.abs(A[k][both] - B[k][both]) / np.abs(A[k][both])))
                               for k in ("Bm", "Cq", "Nq", "Pq", "Chl")},
             "z_abs_max": float(np.max(np.abs(A["z"][both] - B["z"][both])))}
-    out = {"accuracy": "config2", "steps": steps, "counts_equal_at_every_check": all(h["fp64"] == h["fp32"] for h in hist),
+        # population totals: meaningful also after a decision flip has moved daughters to other slots
+        tot = {}
+        for k in ("Bm", "Cq", "Nq", "Pq", "Chl"):
+            t64, t32 = float(np.sum(A[k][A["ac"]])), float(np.sum(B[k][B["ac"]]))
+            tot[k] = abs(t32 - t64) / abs(t64) if t64 else abs(t32)
+        n64, n32 = int(A["ac"].sum()), int(B["ac"].sum())
+        inds[f"sp{s}"]["count_rel_diff"] = abs(n32 - n64) / n64
+        inds[f"sp{s}"]["total_rel_diff"] = tot
+    out = {"accuracy": args.workload, "steps": steps, "counts_equal_at_every_check": all(h["fp64"] == h["fp32"] for h in hist),
            "counts": hist, "tracer_mass_rel_err": rel, "max_tracer_mass_rel_err": max(rel.values()),
            "individuals": inds, "budget_fp32": b.budget(0), "seconds": round(time.time() - t0, 1)}
     b.close()
