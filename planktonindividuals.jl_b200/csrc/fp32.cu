@@ -119,7 +119,8 @@ struct pi_batch {
     double last_dT = 0.0;
     char* cub_tmp = nullptr;
     size_t cub_bytes = 0;
-    double* stage = nullptr;        // maxG doubles of upload staging
+    double* stage = nullptr;        // 3 × maxG doubles of upload staging
+    cudaEvent_t copied = nullptr;   // recorded after a setter's host→device copies
     double* partial = nullptr;      // budget partials
     unsigned long long* scratch = nullptr;
     // work tables (device) built for the current tuning
@@ -242,6 +243,7 @@ void free_batch(pi_batch* b) {
     b->allocs.clear();
     for (cudaEvent_t e : b->event_pool) cudaEventDestroy(e);
     b->event_pool.clear();
+    if (b->copied) cudaEventDestroy(b->copied);
     if (b->stream) cudaStreamDestroy(b->stream);
     b->stream = nullptr;
 }
@@ -508,6 +510,7 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     if (cudaGetDevice(&b->device) != cudaSuccess) { b->err = "pi_batch_create: no CUDA device"; return bail(PI_ERR_CUDA); }
     cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, b->device);
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) { b->err = "pi_batch_create: stream"; return bail(PI_ERR_CUDA); }
+    if (cudaEventCreateWithFlags(&b->copied, cudaEventDisableTiming) != cudaSuccess) { b->err = "pi_batch_create: event"; return bail(PI_ERR_CUDA); }
     b->nm = nmembers; b->nsp = nspecies; b->nseg = nmembers * nspecies;
     b->mh.resize(nmembers);
     b->mdh.resize(nmembers);
@@ -600,7 +603,7 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     BA(b->tile_cnt, tiles.size()); BA(b->tile_off, tiles.size());
     BA(b->divlist, S); BA(b->freelist, S); BA(b->ndiv, b->nseg);
     for (int a = 0; a < 3; ++a) BA(b->line_off[a], nmembers + 1);
-    BA(b->stage, std::max<long long>(b->maxG, col));
+    BA(b->stage, std::max<long long>(3 * b->maxG, col));
     BA(b->partial, 3 * 1024); BA(b->scratch, 4);
     size_t cb = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, cb, b->tile_cnt, b->tile_off, b->ntiles, b->stream);
@@ -859,16 +862,21 @@ static pi_status vel_copy32(pi_batch* b, int m, const double* u, const double* v
         const double* src[3] = { u, v, w };
         float* dst[3] = { U, V, W };
         for (int c = 0; c < 3; ++c) {
-            size_t n = (size_t)dims[c][0] * dims[c][1] * dims[c][2];
+            const size_t n = (size_t)dims[c][0] * dims[c][1] * dims[c][2];
+            BK(cudaMemcpyAsync(b->stage + c * b->maxG, src[c], n * sizeof(double), cudaMemcpyDefault, s), "upload velocity");
+        }
+        // the caller's buffers are free once the copies are done; the conversion runs on
+        BK(cudaEventRecord(b->copied, s), "record copies");
+        for (int c = 0; c < 3; ++c) {
             BK(cudaMemsetAsync(dst[c], 0, g.G * sizeof(float), s), "clear velocity");
-            BK(cudaMemcpyAsync(b->stage, src[c], n * sizeof(double), cudaMemcpyDefault, s), "upload velocity");
-            k32_scatter_interior<<<std::min<unsigned>(nblk((long long)n, 256), 1024), 256, 0, s>>>(d, dst[c], b->stage, dims[c][0], dims[c][1], dims[c][2]);
+            k32_scatter_interior<<<std::min<unsigned>(nblk((long long)dims[c][0] * dims[c][1] * dims[c][2], 256), 1024), 256, 0, s>>>(
+                d, dst[c], b->stage + c * b->maxG, dims[c][0], dims[c][1], dims[c][2]);
             k32_halo_vel<0><<<std::min<unsigned>(nblk((long long)g.Gy * g.Gz, 128), 1024), 128, 0, s>>>(d, dst[c], c);
             k32_halo_vel<1><<<std::min<unsigned>(nblk((long long)g.Gx * g.Gz, 128), 1024), 128, 0, s>>>(d, dst[c], c);
             k32_halo_vel<2><<<std::min<unsigned>(nblk((long long)g.Gx * g.Gy, 128), 1024), 128, 0, s>>>(d, dst[c], c);
-            BK(cudaGetLastError(), "velocity halo");
-            BK(cudaStreamSynchronize(s), "synchronize");
         }
+        BK(cudaGetLastError(), "velocity halo");
+        BK(cudaEventSynchronize(b->copied), "synchronize");
     } else {
         std::vector<double> Ud, Vd, Wd;
         host_vel_copy(g, u, v, w, Ud, Vd, Wd);
@@ -889,10 +897,10 @@ static pi_status read_forcing(pi_batch* b, int m, MemberForcing& f) {
     BK(cudaStreamSynchronize(b->stream), "synchronize");
     return PI_OK;
 }
-static pi_status write_forcing(pi_batch* b, int m, const MemberForcing& fin) {
-    // a field the host replaced may sit at an address packed before: pack again
+static pi_status write_forcing(pi_batch* b, int m, const MemberForcing& fin, bool velocity = true) {
+    // a velocity the host replaced may sit at an address packed before: pack again
     MemberForcing f = fin;
-    f.pks0 = f.pks1 = nullptr;
+    if (velocity) f.pks0 = f.pks1 = nullptr;
     BK(cudaMemcpyAsync(b->F + m, &f, sizeof f, cudaMemcpyHostToDevice, b->stream), "write forcing");
     BK(cudaStreamSynchronize(b->stream), "synchronize");
     return PI_OK;
@@ -928,9 +936,10 @@ pi_status pi_batch_set_PARF(pi_batch* b, int32_t member, const double* parf) {
     if (!parf) return bfail(b, PI_ERR_ARG, "pi_set_PARF: NULL argument");
     const long long n = (long long)b->mdh[member].Nx * b->mdh[member].Ny;
     BK(cudaMemcpyAsync(b->stage, parf, n * sizeof(double), cudaMemcpyDefault, b->stream), "upload PARF");
+    BK(cudaEventRecord(b->copied, b->stream), "record copies");
     k32_d2f<<<std::min<unsigned>(nblk(n, 256), 1024), 256, 0, b->stream>>>(b->PARF + b->mdh[member].col_off, b->stage, n);
     BK(cudaGetLastError(), "convert PARF");
-    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    BK(cudaEventSynchronize(b->copied), "synchronize");
     return PI_OK;
 }
 
@@ -943,12 +952,13 @@ pi_status pi_batch_set_temp(pi_batch* b, int32_t member, const double* temp) {
     float* dst = b->tempown + d.cell_off;
     // copy_interior!: only the interior is written; the halo stays zero
     BK(cudaMemcpyAsync(b->stage, temp, n * sizeof(double), cudaMemcpyDefault, b->stream), "upload temp");
+    BK(cudaEventRecord(b->copied, b->stream), "record copies");
     k32_scatter_interior<<<std::min<unsigned>(nblk(n, 256), 1024), 256, 0, b->stream>>>(d, dst, b->stage, d.Nx, d.Ny, d.Nz);
     BK(cudaGetLastError(), "scatter temp");
     MemberForcing f;
     if ((e = read_forcing(b, member, f))) return e;
     f.temp = dst;
-    return write_forcing(b, member, f);
+    return write_forcing(b, member, f, false);
 }
 
 pi_status pi_batch_set_flux_bc(pi_batch* b, int32_t member, int32_t tracer, int32_t face, int32_t kind,
