@@ -997,17 +997,21 @@ struct ZLev {
     double fxv;     // mmol per fixed-point unit / (Δx Δy ΔzF[k])
 };
 
-// tracer_forcing! (tracer_forcings.jl:2-50) of the three iron tracers on max(0, tracer)
-__device__ __forceinline__ float fe_forcing(int n, const BgcDev32& b, float dT, float dfe, float poc,
-                                            float dust, float pfeb, float pfei) {
-    if (n == PI_DFe) {
-        const float fe = fmaxf(dfe - b.ligand, 0.0f) * dfe * b.DFeFrac * b.lambda_Fe * dT;
-        return pfeb * b.kPOC * dT - (b.lambda_POC * poc + b.lambda_min + b.lambda_dust * dust) * dfe * b.DFeFrac * dT
-             + pfei * b.kdiss * dT - fe;
-    }
-    if (n == PI_PFe_bio) return poc * dfe * b.DFeFrac * b.lambda_POC * dT - b.kPOC * pfeb * dT;
-    const float fe = fmaxf(dfe - b.ligand, 0.0f) * dfe * b.DFeFrac * b.lambda_Fe * dT;
-    return -pfei * b.kdiss * dT + (b.lambda_min + b.lambda_dust * dust) * dfe * b.DFeFrac * dT + fe;
+// tracer_forcing! (tracer_forcings.jl:2-50) of the three iron tracers on max(0, tracer), with the
+// products of rate constants and ΔT formed once per walk
+struct FeCoef { float kpoc, frac, kdiss, fefe, frac_poc, lig, lpoc, lmin, ldust; };
+__device__ __forceinline__ FeCoef fe_coef(const BgcDev32& b, float dT) {
+    FeCoef c;
+    c.kpoc = b.kPOC * dT; c.frac = b.DFeFrac * dT; c.kdiss = b.kdiss * dT;
+    c.fefe = b.DFeFrac * b.lambda_Fe * dT; c.frac_poc = b.DFeFrac * b.lambda_POC * dT;
+    c.lig = b.ligand; c.lpoc = b.lambda_POC; c.lmin = b.lambda_min; c.ldust = b.lambda_dust;
+    return c;
+}
+__device__ __forceinline__ float fe_forcing(int n, const FeCoef& c, float dfe, float poc, float dust, float pfeb, float pfei) {
+    const float fe = fmaxf(dfe - c.lig, 0.0f) * dfe * c.fefe;
+    if (n == PI_DFe) return pfeb * c.kpoc - (c.lpoc * poc + c.lmin + c.ldust * dust) * dfe * c.frac + pfei * c.kdiss - fe;
+    if (n == PI_PFe_bio) return poc * dfe * c.frac_poc - pfeb * c.kpoc;
+    return -pfei * c.kdiss + (c.lmin + c.ldust * dust) * dfe * c.frac + fe;
 }
 
 // Asynchronous global → shared copies (cp.async): a warp's z walk reads the inputs of each level
@@ -1036,8 +1040,9 @@ __device__ __forceinline__ unsigned long long lds_u64(unsigned a) {
 }
 
 #define ZS 4                              // levels of a z walk ring (power of two)
-// One warp's ring: own tracer c, tracer_temp t two levels below, up to four other tracers the
-// forcing reads, and the particle sum of the cell.
+// One warp's ring: own tracer c, tracer_temp t two levels below, the other tracers the forcing
+// reads and the particle sum of the cell. A nutrient warp uses x[0] and acc; an iron warp reads
+// DFe, POC, Dust, PFe_bio, PFe_inorg into x[0..3] and, for the fifth, the first 512 bytes of acc.
 struct ZRing {
     float c[ZS][32];
     float t[ZS][32];
@@ -1070,11 +1075,7 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& md, con
     // second tracer); of the iron tracers: T of DFe, POC, Dust, PFe_bio, PFe_inorg, each the own
     // tracer (-1) or one of the four others x0..x3
     float aS = 0.0f, aO = 0.0f;
-    int xo[4] = { n, n, n, n };
-    // iron forcing: position of the own tracer in (DFe, POC, Dust, PFe_bio, PFe_inorg); the others
-    // keep their order in x0..x3
-    const int pn = n == PI_DFe ? 0 : n == PI_POC ? 1 : n == PI_Dust ? 2 : n == PI_PFe_bio ? 3 : 4;
-    auto fe_at = [](int r) { return r == 0 ? PI_DFe : r == 1 ? PI_POC : r == 2 ? PI_Dust : r == 3 ? PI_PFe_bio : PI_PFe_inorg; };
+    int xo[5] = { n, PI_POC, PI_Dust, PI_PFe_bio, PI_PFe_inorg };
     if (NUT) {
         switch (n) {
             case PI_DIC: xo[0] = PI_DOC; aO = b.kDOC * dT; break;
@@ -1090,9 +1091,9 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& md, con
             default: break;
         }
     } else {
-#pragma unroll
-        for (int e = 0; e < 4; ++e) xo[e] = fe_at(e < pn ? e : e + 1);
+        xo[0] = PI_DFe;
     }
+    const FeCoef fc = fe_coef(b, dT);
     const float* __restrict__ t = a.tb + n * G + off;
     const float* __restrict__ c = a.tr + n * G + off;
     const float* __restrict__ trm = a.tr + off;           // all tracers of the member
@@ -1103,13 +1104,16 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& md, con
     auto lmk = [&](int kk) -> int { return LM ? (int)lmc[(kk - 1) * slab] : 1; };
     auto fcz = [&](int l) { const float4 v = sFC[l * 32 + lane]; FCu r; r.tr = v.x; r.d0c = v.y; r.d1c = v.z; r.R = v.w; return r; };
     // ring addresses of this lane (shared space): stage sl of c at rc + 128 sl, t at rc + 512 +
-    // 128 sl, x[e] at rc + 1024 + 512 e + 128 sl, the particle sum at ra + 256 sl
+    // 128 sl, x[e] at rc + 1024 + 512 e + 128 sl, the particle sum at ra + 256 sl, the fifth
+    // iron tracer at rx4 + 128 sl
     const unsigned rc = (unsigned)__cvta_generic_to_shared(&R.c[0][lane]);
     const unsigned ra = (unsigned)__cvta_generic_to_shared(&R.acc[0][lane]);
+    const unsigned rx4 = (unsigned)__cvta_generic_to_shared(&R.acc[0][0]) + 4u * lane;   // iron x[4]: 128 B stages
     const float* __restrict__ x0p = trm + xo[0] * G;
     const float* __restrict__ x1p = trm + xo[1] * G;
     const float* __restrict__ x2p = trm + xo[2] * G;
     const float* __restrict__ x3p = trm + xo[3] * G;
+    const float* __restrict__ x4p = trm + xo[4] * G;
     // ring fill of level kk; past the last level the last level is copied again into the stage
     // that level kk would use, which no iteration reads
     auto issue = [&](int kk) {
@@ -1126,6 +1130,7 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& md, con
             cpa4(rc + 1536u + so, x1p + qq);
             cpa4(rc + 2048u + so, x2p + qq);
             cpa4(rc + 2560u + so, x3p + qq);
+            cpa4(rx4 + so, x4p + qq);
         }
         cpa_commit();
     };
@@ -1178,13 +1183,10 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& md, con
                 sink_prev = cc;
             }
             if (n != PI_Dust) {
-                const float x0 = lds_f32(rc + 1024u + so), x1 = lds_f32(rc + 1536u + so);
-                const float x2 = lds_f32(rc + 2048u + so), x3 = lds_f32(rc + 2560u + so);
-                auto T = [&](int e) {
-                    const int sr = e < pn ? e : (e == pn ? -1 : e - 1);
-                    return fmaxf(0.0f, sr < 0 ? cc : sr == 0 ? x0 : sr == 1 ? x1 : sr == 2 ? x2 : x3);
-                };
-                Gc += fe_forcing(n, b, dT, T(0), T(1), T(2), T(3), T(4));
+                const float dfe = fmaxf(0.0f, lds_f32(rc + 1024u + so)), poc = fmaxf(0.0f, lds_f32(rc + 1536u + so));
+                const float dust = fmaxf(0.0f, lds_f32(rc + 2048u + so)), pfeb = fmaxf(0.0f, lds_f32(rc + 2560u + so));
+                const float pfei = fmaxf(0.0f, lds_f32(rx4 + so));
+                Gc += fe_forcing(n, fc, dfe, poc, dust, pfeb, pfei);
             }
         }
         if (GEN && md.any_bc) {

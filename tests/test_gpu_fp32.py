@@ -175,6 +175,12 @@ def test_fp32_flux_bcs_vs_oracle(gpu_lib):
     _fp32_pair(gpu_lib, wl, 12, setup)
 
 
+def test_fp32_iron_and_sinking_vs_oracle(gpu_lib):
+    from test_gpu_parity_edge import OVER, with_iron
+    wl = with_iron(daylight(W.config2(nx=12, nz=10, N_per_species=600, nsp=1, steps=15, nmodes=12, phyt_over=OVER)))
+    _fp32_pair(gpu_lib, wl, 15)
+
+
 def test_fp32_diffusion_vs_oracle(gpu_lib):
     from test_gpu_parity_edge import DIFFUSION, OVER
     wl = daylight(W.config2(nx=12, nz=8, N_per_species=700, nsp=1, steps=15, nmodes=12, phyt_over=OVER))

@@ -107,6 +107,29 @@ def landmask_3d(wl, seed=5):
 
 DIFFUSION = {"κh": 1.0, "κv": 1e-3, "κhP": 0.5, "κvP": 2e-4}
 
+IRON_INIT = {"DFe": 2e-4, "PFe_inorg": 1e-4, "PFe_bio": 5e-5, "Dust": 1e-3}
+
+
+def with_iron(wl, seed=7, lm=None):
+    """Non-zero iron tracers and dust (the workloads start them at zero), so the iron forcing,
+    the sinking of PFe_inorg, PFe_bio and Dust, and the DFe ligand threshold all act."""
+    rng = np.random.default_rng(seed)
+    g = wl.grid
+    for name, v0 in IRON_INIT.items():
+        a = np.asfortranarray(v0 * rng.uniform(0.2, 1.8, g.total_size)) * g.landmask
+        fill_halo_tracer(a, g)
+        wl.tracers[_abi.tracer_names.index(name)] = np.asfortranarray(a)
+    wl.bgc["ligand"] = 2e-4      # DFe above and below the threshold of the scavenging term
+    return wl
+
+
+def test_iron_and_sinking_bitexact(gpu_lib):
+    wl = with_iron(daylight(W.config2(nx=12, nz=10, N_per_species=600, nsp=1, steps=15, nmodes=12, phyt_over=OVER)))
+    ref, gpu = pair(gpu_lib, wl)
+    vel = VelCache(wl)
+    drive(ref, wl, 15, vel); drive(gpu, wl, 15, vel)
+    assert compare_states(ref, gpu, 1) == []
+
 
 def test_landmask_3d_bitexact(gpu_lib):
     wl = landmask_3d(daylight(W.config2(nx=16, nz=10, N_per_species=900, nsp=1, steps=15, nmodes=12,
