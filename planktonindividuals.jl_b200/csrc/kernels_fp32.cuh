@@ -647,12 +647,20 @@ struct PhysArgs {
     const uint32_t* err;
 };
 
+// flags, status and cell of a slot, loaded one slot ahead of its physiology
+struct PHead { int32_t code; uint8_t fl, stt; };
+__device__ __forceinline__ PHead phys_head(const IndDev32& P, long long g, bool valid) {
+    PHead h{-1, 0, 0};
+    if (valid) { h.fl = P.flags[g]; h.stt = P.stat[g]; h.code = P.cell[g]; }
+    return h;
+}
+
 __device__ __forceinline__ void phys_one(const PhysArgs& a, const MemberDev& m, int mi, int s, long long slot,
-                                         long long g, uint32_t iter, double tnow) {
+                                         long long g, uint32_t iter, double tnow, const PHead& hd) {
     const IndDev32& P = a.P;
-    // flags, status and cell in one round trip; the quotas are loaded with the environment
-    const uint8_t fl = P.flags[g], stt = P.stat[g];
-    const int32_t code = P.cell[g];
+    // the quotas are loaded with the environment
+    const uint8_t fl = hd.fl, stt = hd.stt;
+    const int32_t code = hd.code;
     if (!(fl & F32_AC)) return;
     const int ac0 = stt & F32_ST_AC0;
     int q;
@@ -753,9 +761,12 @@ __global__ void __launch_bounds__(256, 4) k32_physiology(PhysArgs a) {
         seg_of(a.T, tl.x, mi, s);
         const MemberDev& m = a.T.md[mi];
         const long long base = m.slot_off + (long long)s * m.C;
-        for (int p = 0; p < ppt; ++p) {
-            const long long slot = (long long)tl.y + p * bs + threadIdx.x;
-            if (slot < m.C) phys_one(a, m, mi, s, slot, base + slot, iter, tnow);
+        long long slot = (long long)tl.y + threadIdx.x;
+        PHead hd = phys_head(a.P, base + slot, slot < m.C);
+        for (int p = 0; p < ppt; ++p, slot += bs) {
+            const PHead cur = hd;
+            if (p + 1 < ppt) hd = phys_head(a.P, base + slot + bs, slot + bs < m.C);
+            if (slot < m.C) phys_one(a, m, mi, s, slot, base + slot, iter, tnow, cur);
         }
     }
 }
