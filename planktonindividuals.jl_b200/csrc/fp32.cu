@@ -63,7 +63,7 @@ struct MemberHost {
 struct Tuning {
     int bs_move = 256, bs_phys = 256, bs_assign = 256;
     int persist_move = 0, persist_phys = 0;   // 0: one tile per block; k: k blocks per SM, looping
-    int ty = 8;                               // rows of an x-y tracer tile (4, 8 or 16)
+    int ty = 8;                               // rows of an x-y tracer tile (4, 8, 16 or 28)
     int lz = 32;                              // levels walked by a z thread (8, 16 or 32)
     int wpb_par = 4;
 };
@@ -407,11 +407,13 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
             // item's loads in flight
             int per_sm = 1;
             const int ty = b->tune.ty;
-            if (ty == 16) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k32_xy<16>, 32 * 20, xy_smem(16));
+            if (ty == 28) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k32_xy<28>, 32 * 32, xy_smem(28));
+            else if (ty == 16) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k32_xy<16>, 32 * 20, xy_smem(16));
             else if (ty == 8) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k32_xy<8>, 32 * 12, xy_smem(8));
             else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k32_xy<4>, 32 * 8, xy_smem(4));
             const unsigned grid = (unsigned)std::max(1, std::min(b->nxy_items, std::max(1, per_sm) * b->nsm));
-            if (ty == 16) k32_xy<16><<<grid, 32 * 20, xy_smem(16), s>>>(a);
+            if (ty == 28) k32_xy<28><<<grid, 32 * 32, xy_smem(28), s>>>(a);
+            else if (ty == 16) k32_xy<16><<<grid, 32 * 20, xy_smem(16), s>>>(a);
             else if (ty == 8) k32_xy<8><<<grid, 32 * 12, xy_smem(8), s>>>(a);
             else k32_xy<4><<<grid, 32 * 8, xy_smem(4), s>>>(a);
         }
@@ -677,6 +679,7 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     ok = ok && cudaMemsetAsync(P.cell, 0xff, S * sizeof(int32_t), s0) == cudaSuccess;
     ok = ok && cudaStreamSynchronize(s0) == cudaSuccess;
     if (!ok) { b->err = "pi_batch_create: device initialisation failed"; return bail(PI_ERR_CUDA); }
+    cudaFuncSetAttribute(k32_xy<28>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xy_smem(28));
     cudaFuncSetAttribute(k32_xy<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xy_smem(16));
     cudaFuncSetAttribute(k32_xy<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xy_smem(8));
     cudaFuncSetAttribute(k32_xy<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xy_smem(4));
@@ -1284,7 +1287,7 @@ pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t k, char* report, siz
         { "k32_physiology", &t.bs_phys, {128, 256, 512, 1024}, "physiology block", 1 },
         { "k32_physiology", &t.persist_phys, {0, 2, 4, 8}, "physiology blocks/SM (0 = one tile per block)", 0 },
         { "k32_assign", &t.bs_assign, {128, 256, 512, 1024}, "assign block", 1 },
-        { "k32_xy", &t.ty, {4, 8, 16}, "x-y tracer tile rows", 0 },
+        { "k32_xy", &t.ty, {4, 8, 16, 28}, "x-y tracer tile rows", 0 },
         { "k32_ztail", &t.lz, {8, 16, 32}, "z levels per thread", 0 },
         { "k32_par", &t.wpb_par, {1, 2, 4, 8}, "par warps/block", 32 },
     };
