@@ -1334,6 +1334,33 @@ __global__ void k32_halo(const MemberDev* __restrict__ md, const long long* __re
     }
 }
 
+// fill_halo_tracer! in one pass when every axis of every member has N >= H: each halo cell then takes
+// the value of the interior cell reached by applying the rule of each axis (periodic: ±N; Bounded:
+// the nearest interior cell), which is what the three sequential passes above produce. Grid:
+// (x blocks, members); every thread walks halo cells of its member, all fields.
+__device__ __forceinline__ int halo_src(int a, int N, int H, int topo) {
+    if (a > H && a <= N + H) return a;
+    if (topo == PI_PERIODIC) return a <= H ? a + N : a - N;
+    return a <= H ? H + 1 : N + H;
+}
+__global__ void k32_halo_direct(const MemberDev* __restrict__ md, long long Gtot, float* __restrict__ f,
+                                int nfields, const uint32_t* err) {
+    if (err && stopped(err)) return;
+    const MemberDev& m = md[blockIdx.y];
+    const int Gx = m.Gx, Gy = m.Gy, Nx = m.Nx, Ny = m.Ny, Nz = m.Nz, Hx = m.Hx, Hy = m.Hy, Hz = m.Hz;
+    const int tx = m.tx, ty = m.ty;
+    const int G = (int)m.G;                                         // below 2^31 (checked at creation)
+    float* __restrict__ c = f + m.cell_off;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < G; q += gridDim.x * blockDim.x) {
+        const int i = q % Gx + 1, r = q / Gx;
+        const int j = r % Gy + 1, k = r / Gy + 1;
+        const int si = halo_src(i, Nx, Hx, tx), sj = halo_src(j, Ny, Hy, ty), sk = halo_src(k, Nz, Hz, PI_BOUNDED);
+        if (si == i && sj == j && sk == k) continue;               // interior
+        const int src = (si - 1) + Gx * ((sj - 1) + Gy * (sk - 1));
+        for (int n = 0; n < nfields; ++n) c[n * Gtot + q] = c[n * Gtot + src];
+    }
+}
+
 // vel₀ .= vel₁ (time_step.jl:174-176), model.iteration += 1, model.t = iteration·ΔT. After a
 // capacity error nothing advances.
 __global__ void k32_end_step(int nm, MemberForcing* __restrict__ F, StepState* st, double dT, const uint32_t* err) {
