@@ -64,7 +64,7 @@ struct Tuning {
     int bs_move = 256, bs_phys = 256, bs_assign = 256;
     int persist_move = 0, persist_phys = 0;   // 0: one tile per block; k: k blocks per SM, looping
     int ty = 8;                               // rows of an x-y tracer tile (4, 8, 16 or 28)
-    int lz = 32;                              // levels walked by a z thread (8, 16 or 32)
+    int lz = 32;                              // levels walked by a z thread (8, 16, 32 or 64)
     int wpb_par = 4;
 };
 
@@ -423,9 +423,10 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
             BScope sc(b, "k32_ztail");
             const unsigned grid = (unsigned)std::max(1, b->nz_items);
             const dim3 blk(32, PI_NTRACERS);
-            const size_t zs = ztail_smem();
+            const size_t zs = ztail_smem(b->tune.lz);
             if (b->tune.lz == 8) k32_ztail<8><<<grid, blk, zs, s>>>(a);
             else if (b->tune.lz == 32) k32_ztail<32><<<grid, blk, zs, s>>>(a);
+            else if (b->tune.lz == 64) k32_ztail<64><<<grid, blk, zs, s>>>(a);
             else k32_ztail<16><<<grid, blk, zs, s>>>(a);
         }
     }
@@ -688,9 +689,10 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     cudaFuncSetAttribute(k32_xy<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xy_smem(16));
     cudaFuncSetAttribute(k32_xy<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xy_smem(8));
     cudaFuncSetAttribute(k32_xy<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xy_smem(4));
-    cudaFuncSetAttribute(k32_ztail<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ztail_smem());
-    cudaFuncSetAttribute(k32_ztail<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ztail_smem());
-    cudaFuncSetAttribute(k32_ztail<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ztail_smem());
+    cudaFuncSetAttribute(k32_ztail<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ztail_smem(8));
+    cudaFuncSetAttribute(k32_ztail<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ztail_smem(16));
+    cudaFuncSetAttribute(k32_ztail<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ztail_smem(32));
+    cudaFuncSetAttribute(k32_ztail<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ztail_smem(64));
     b->T.md = b->md; b->T.nsp = nspecies; b->T.tiles = b->tiles; b->T.ntiles = b->ntiles; b->T.seg_tile0 = b->seg_tile0;
     st = build_tables(b);
     if (st) return bail(st);
@@ -1293,7 +1295,7 @@ pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t k, char* report, siz
         { "k32_physiology", &t.persist_phys, {0, 2, 4, 8}, "physiology blocks/SM (0 = one tile per block)", 0 },
         { "k32_assign", &t.bs_assign, {128, 256, 512, 1024}, "assign block", 1 },
         { "k32_xy", &t.ty, {4, 8, 16, 28}, "x-y tracer tile rows", 0 },
-        { "k32_ztail", &t.lz, {8, 16, 32}, "z levels per thread", 0 },
+        { "k32_ztail", &t.lz, {8, 16, 32, 64}, "z levels per thread", 0 },
         { "k32_par", &t.wpb_par, {1, 2, 4, 8}, "par warps/block", 32 },
     };
     // the largest block each kernel can be launched with (registers per thread)

@@ -1241,18 +1241,22 @@ __device__ __forceinline__ void z_walk_any(const TrArgs& a, const MemberDev& m, 
     }
 }
 
-// dynamic shared memory of k32_ztail: one ring per tracer warp
-inline size_t ztail_smem() { return sizeof(ZRing) * PI_NTRACERS; }
+// dynamic shared memory of k32_ztail: one ring per tracer warp, then the per-item arrays (face
+// coefficients, transport terms, cell counts, per-level constants) of a walk of lz levels
+inline size_t ztail_smem(int lz) {
+    return sizeof(ZRing) * PI_NTRACERS + (size_t)(lz + 1) * 32 * sizeof(float4) + (size_t)lz * 32 * (sizeof(float) + sizeof(int))
+         + (size_t)lz * sizeof(ZLev);
+}
 
 template <int LZ>
 __global__ void __launch_bounds__(32 * PI_NTRACERS, 2) k32_ztail(TrArgs a) {
     if (stopped(a.err)) return;
-    __shared__ float4 sFC[(LZ + 1) * 32];   // faces k0 .. k0+LZ of the 32 columns
-    __shared__ float sFtr[LZ * 32];         // vertical transport term of the cells k0 .. k0+LZ-1
-    __shared__ int sPop[LZ * 32];           // individuals in those cells
-    __shared__ ZLev sLev[LZ];               // per-level constants
     extern __shared__ __align__(16) unsigned char zsm[];
     ZRing* ring = reinterpret_cast<ZRing*>(zsm);
+    float4* sFC = reinterpret_cast<float4*>(zsm + sizeof(ZRing) * PI_NTRACERS);   // faces k0 .. k0+LZ of the 32 columns
+    float* sFtr = reinterpret_cast<float*>(sFC + (LZ + 1) * 32);       // vertical transport term of the cells k0 .. k0+LZ-1
+    int* sPop = reinterpret_cast<int*>(sFtr + LZ * 32);                 // individuals in those cells
+    ZLev* sLev = reinterpret_cast<ZLev*>(sPop + LZ * 32);               // per-level constants
     const int tid = threadIdx.y * 32 + threadIdx.x;
     for (int w = blockIdx.x; w < a.nitems; w += gridDim.x) {
         const int4 it = a.items[w];
