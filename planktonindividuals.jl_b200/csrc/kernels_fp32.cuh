@@ -319,6 +319,7 @@ __device__ __forceinline__ void move_one(const MoveArgs& a, const MemberDev& m, 
     const uint8_t fl = P.flags[g], stt = P.stat[g];
     const int32_t code = P.cell[g];
     const float ox = P.ox[g], oy = P.oy[g], oz = P.oz[g];
+    const float chl = P.Chl[g];             // for the Chl sum, read before this function's stores
     if (!(fl & F32_AC)) {
         // every stage multiplies by ac: the position becomes (0, 0, 0) and the cell (Hx, Hy, Hz)
         if (code != -1) {
@@ -386,7 +387,7 @@ __device__ __forceinline__ void move_one(const MoveArgs& a, const MemberDev& m, 
     const bool inside = X.c < m.Nx && Y.c < m.Ny && Z.c < m.Nz;
     atomicAdd(&a.pop[cq], 1);
     if (a.pop_sp) atomicAdd(&a.pop_sp[(long long)s * G + cq], 1);
-    if (inside) add_fixed(&a.chl_acc[cq], P.Chl[g], m.chl_inv);
+    if (inside) add_fixed(&a.chl_acc[cq], chl, m.chl_inv);
     // previous step's decisions (plankton_update.jl:5-16, division_death.jl:2-25)
     const int gz = (fl & F32_GRAZ) != 0, mt = (fl & F32_MORT) != 0, dv = (fl & F32_DVID) != 0;
     const int ac1 = !gz, ac2 = ac1 && !mt, dv2 = dv && ac2;
