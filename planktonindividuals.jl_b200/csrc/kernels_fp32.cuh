@@ -379,15 +379,17 @@ __device__ __forceinline__ void move_one(const MoveArgs& a, const MemberDev& m, 
     if (Y.c < 0 || Y.c > pg.Ny) { bad = true; Y.c = Y.c < 0 ? 0 : pg.Ny; Y.o = 0.0f; }
     if (Z.c < 0 || Z.c > pg.Nz) { bad = true; Z.c = Z.c < 0 ? 0 : pg.Nz; Z.o = 0.0f; }
     if (bad) seterr(err, F32_ERR_DOMAIN);
+    // everything that reads the member record is formed before the stores below
+    const int32_t code_new = pack_int(m, X.c, Y.c, Z.c);
+    const long long cq = m.cell_off + q_of(m, X.c, Y.c, Z.c);
+    const bool inside = X.c < pg.Nx && Y.c < pg.Ny && Z.c < pg.Nz;
+    const double chl_inv = m.chl_inv, fx_inv = m.fx_inv;
     P.ox[g] = X.o; P.oy[g] = Y.o; P.oz[g] = Z.o;
-    P.cell[g] = pack_int(m, X.c, Y.c, Z.c);
-    const int q = q_of(m, X.c, Y.c, Z.c);
-    const long long cq = m.cell_off + q;
+    P.cell[g] = code_new;
     const long long G = a.Gtot;
-    const bool inside = X.c < m.Nx && Y.c < m.Ny && Z.c < m.Nz;
     atomicAdd(&a.pop[cq], 1);
     if (a.pop_sp) atomicAdd(&a.pop_sp[(long long)s * G + cq], 1);
-    if (inside) add_fixed(&a.chl_acc[cq], chl, m.chl_inv);
+    if (inside) add_fixed(&a.chl_acc[cq], chl, chl_inv);
     // previous step's decisions (plankton_update.jl:5-16, division_death.jl:2-25)
     const int gz = (fl & F32_GRAZ) != 0, mt = (fl & F32_MORT) != 0, dv = (fl & F32_DVID) != 0;
     const int ac1 = !gz, ac2 = ac1 && !mt, dv2 = dv && ac2;
@@ -402,7 +404,7 @@ __device__ __forceinline__ void move_one(const MoveArgs& a, const MemberDev& m, 
         const float fN = kind == 1 ? p.grazFracN : p.mortFracN;
         const float fP = kind == 1 ? p.grazFracP : p.mortFracP;
         const float Bm = P.Bm[g], Cq = P.Cq[g], Nq = P.Nq[g], Pq = P.Pq[g];
-        const double u = m.fx_inv;
+        const double u = fx_inv;
         add_fixed(&a.acc[ACC_DOC * G + cq], (Bm + Cq) * fC, u);
         add_fixed(&a.acc[ACC_DON * G + cq], (Bm * p.R_NC + Nq) * fN, u);
         add_fixed(&a.acc[ACC_DOP * G + cq], (Bm * p.R_PC + Pq) * fP, u);
@@ -687,6 +689,7 @@ __device__ __forceinline__ void phys_one(const PhysArgs& a, const MemberDev& m, 
         popv = (float)(a.pop_sp ? a.pop_sp[(long long)s * G + cq] : a.pop[cq]);
     }
     float Bm = P.Bm[g], Cq = P.Cq[g], Nq = P.Nq[g], Pq = P.Pq[g], Chl = P.Chl[g];
+    const double fx_inv = m.fx_inv;         // read before the stores below
     const float tf = tempFunc_f(Tm, p);
     // calc_inorganic_uptake_kernel! (:48-56)
     const float aI = parv * p.alpha * p.Phi;
@@ -741,7 +744,7 @@ __device__ __forceinline__ void phys_one(const PhysArgs& a, const MemberDev& m, 
     P.flags[g] = (uint8_t)(F32_AC | (dg ? F32_GRAZ : 0) | (dm ? F32_MORT : 0) | (dd ? F32_DVID : 0));
     // calc_consume_kernel! (consume_loss.jl:2-9): only individuals binned this step reach the grid
     if (ac0 && inside) {
-        const double u = m.fx_inv;
+        const double u = fx_inv;
         add_fixed(&a.acc[ACC_DIC * G + cq], (resp - PS) * dT, u);
         add_fixed(&a.acc[ACC_DOC * G + cq], (exu - VDOC) * dT, u);
         add_fixed(&a.acc[ACC_NH4 * G + cq], -VNH4 * dT, u);
