@@ -312,14 +312,26 @@ struct MoveArgs {
     uint32_t* err;
 };
 
+// The slot state k32_move reads first, loaded one slot ahead of its use (the offsets and Chl of an
+// inactive slot are read and unused).
+struct MState { int32_t code; float ox, oy, oz, chl; uint8_t fl, stt; };
+__device__ __forceinline__ MState move_state(const IndDev32& P, long long g, bool valid) {
+    MState S{-1, 0.0f, 0.0f, 0.0f, 0.0f, 0, 0};
+    if (valid) {
+        S.fl = P.flags[g]; S.stt = P.stat[g]; S.code = P.cell[g];
+        S.ox = P.ox[g]; S.oy = P.oy[g]; S.oz = P.oz[g]; S.chl = P.Chl[g];
+    }
+    return S;
+}
+
 __device__ __forceinline__ void move_one(const MoveArgs& a, const MemberDev& m, const PGeom& pg, int mi, int s,
-                                         long long slot, long long g, uint32_t iter, int& is_div, int& is_free) {
+                                         long long slot, long long g, uint32_t iter, const MState& S,
+                                         int& is_div, int& is_free) {
     const IndDev32& P = a.P;
-    // the slot's state in one round trip (the offsets of an inactive slot are read and unused)
-    const uint8_t fl = P.flags[g], stt = P.stat[g];
-    const int32_t code = P.cell[g];
-    const float ox = P.ox[g], oy = P.oy[g], oz = P.oz[g];
-    const float chl = P.Chl[g];             // for the Chl sum, read before this function's stores
+    const uint8_t fl = S.fl, stt = S.stt;
+    const int32_t code = S.code;
+    const float ox = S.ox, oy = S.oy, oz = S.oz;
+    const float chl = S.chl;
     if (!(fl & F32_AC)) {
         // every stage multiplies by ac: the position becomes (0, 0, 0) and the cell (Hx, Hy, Hz)
         if (code != -1) {
@@ -432,11 +444,14 @@ __global__ void __launch_bounds__(256, 2) k32_move(MoveArgs a) {
         __syncthreads();
         const long long base = m.slot_off + (long long)s * m.C;
         unsigned int nd = 0, nf = 0;
-        for (int p = 0; p < ppt; ++p) {
-            const long long slot = (long long)tl.y + p * bs + threadIdx.x;
+        long long slot = (long long)tl.y + threadIdx.x;
+        MState nx = move_state(a.P, base + slot, slot < m.C);
+        for (int p = 0; p < ppt; ++p, slot += bs) {
+            const MState cur = nx;
+            if (p + 1 < ppt) nx = move_state(a.P, base + slot + bs, slot + bs < m.C);
             if (slot < m.C) {
                 int d, f;
-                move_one(a, m, sg, mi, s, slot, base + slot, iter, d, f);
+                move_one(a, m, sg, mi, s, slot, base + slot, iter, cur, d, f);
                 nd += d; nf += f;
             }
         }
