@@ -81,7 +81,7 @@ struct pi_batch {
     std::vector<FluxBC32> bch;
     std::string err;
     std::vector<void*> allocs;
-    long long Gtot = 0, Stot = 0, ncol = 0, maxG = 0, maxcol = 0;
+    long long Gtot = 0, Stot = 0, ncol = 0, maxG = 0, maxcol = 0, maxhalo = 0;
     bool halo_direct = true;        // every member has N >= H on every axis: one-pass halo fill
     int nlev = 0;
     // device
@@ -431,7 +431,8 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
         }
     }
     if (b->halo_direct) { BScope sc(b, "k32_halo");
-      const unsigned gx = std::max(1u, std::min<unsigned>(nblk(b->maxG, 256), std::max(1, b->nsm * 8 / b->nm)));
+      // about 16 blocks per SM over all members, enough for every member's halo cells
+      const unsigned gx = std::max(1u, std::min<unsigned>(nblk(b->maxhalo, 256), std::max(1, b->nsm * 16 / b->nm)));
       k32_halo_direct<<<dim3(gx, b->nm), 256, 0, s>>>(b->md, G, trn, PI_NTRACERS, b->errw);
     } else { BScope sc(b, "k32_halo");
       k32_halo<0><<<std::min<unsigned>(nblk(b->nlines[0], 128), 148 * 8), 128, 0, s>>>(b->md, b->line_off[0], b->nm, G, trn, PI_NTRACERS, b->errw);
@@ -584,6 +585,7 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
         lev += g.Gz;
         b->maxG = std::max(b->maxG, g.G);
         if (g.Nx < g.Hx || g.Ny < g.Hy || g.Nz < g.Hz) b->halo_direct = false;
+        b->maxhalo = std::max(b->maxhalo, g.G - (long long)g.Nx * g.Ny * g.Nz);
         b->maxcol = std::max(b->maxcol, (long long)g.Nx * g.Ny);
     }
     seg_tile0.push_back((int)tiles.size());

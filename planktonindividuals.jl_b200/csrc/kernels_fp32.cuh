@@ -1366,21 +1366,37 @@ __device__ __forceinline__ int halo_src(int a, int N, int H, int topo) {
     if (topo == PI_PERIODIC) return a <= H ? a + N : a - N;
     return a <= H ? H + 1 : N + H;
 }
+// halo cells of a member: the 2Hz halo levels, then the 2Hy halo rows of the interior levels,
+// then the 2Hx halo columns of the interior rows
 __global__ void k32_halo_direct(const MemberDev* __restrict__ md, long long Gtot, float* __restrict__ f,
                                 int nfields, const uint32_t* err) {
     if (err && stopped(err)) return;
     const MemberDev& m = md[blockIdx.y];
     const int Gx = m.Gx, Gy = m.Gy, Nx = m.Nx, Ny = m.Ny, Nz = m.Nz, Hx = m.Hx, Hy = m.Hy, Hz = m.Hz;
     const int tx = m.tx, ty = m.ty;
-    const int G = (int)m.G;                                         // below 2^31 (checked at creation)
+    const int nz = 2 * Hz * Gx * Gy, ny = 2 * Nz * Hy * Gx, n = nz + ny + 2 * Nz * Ny * Hx;   // below 2^31
     float* __restrict__ c = f + m.cell_off;
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < G; q += gridDim.x * blockDim.x) {
-        const int i = q % Gx + 1, r = q / Gx;
-        const int j = r % Gy + 1, k = r / Gy + 1;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        int i, j, k;
+        if (t < nz) {
+            const int kk = t / (Gx * Gy), r = t - kk * (Gx * Gy);
+            k = kk < Hz ? kk + 1 : Nz + kk + 1;
+            j = r / Gx + 1; i = r - (j - 1) * Gx + 1;
+        } else if (t < nz + ny) {
+            const int u = t - nz, kk = u / (2 * Hy * Gx), r = u - kk * (2 * Hy * Gx), jj = r / Gx;
+            k = Hz + 1 + kk;
+            j = jj < Hy ? jj + 1 : Ny + jj + 1;
+            i = r - jj * Gx + 1;
+        } else {
+            const int u = t - nz - ny, kk = u / (2 * Hx * Ny), r = u - kk * (2 * Hx * Ny), jj = r / (2 * Hx);
+            const int ii = r - jj * 2 * Hx;
+            k = Hz + 1 + kk; j = Hy + 1 + jj;
+            i = ii < Hx ? ii + 1 : Nx + ii + 1;
+        }
+        const int q = (i - 1) + Gx * ((j - 1) + Gy * (k - 1));
         const int si = halo_src(i, Nx, Hx, tx), sj = halo_src(j, Ny, Hy, ty), sk = halo_src(k, Nz, Hz, PI_BOUNDED);
-        if (si == i && sj == j && sk == k) continue;               // interior
         const int src = (si - 1) + Gx * ((sj - 1) + Gy * (sk - 1));
-        for (int n = 0; n < nfields; ++n) c[n * Gtot + q] = c[n * Gtot + src];
+        for (int n2 = 0; n2 < nfields; ++n2) c[n2 * Gtot + q] = c[n2 * Gtot + src];
     }
 }
 
