@@ -102,8 +102,6 @@ __device__ __forceinline__ void axis_iw(const Ax1& a, int H, bool face, int& idx
     idx = a.c + H + (lo ? 0 : 1);
     w = lo ? a.o + 0.5f : a.o - 0.5f;
 }
-__device__ __forceinline__ int clampi(int v, int lo, int hi, uint32_t* err) {
-    if (v < lo) { seterr(err, F32_ERR_DOMAIN); return lo; }
     if (v > hi) { seterr(err, F32_ERR_DOMAIN); return hi; }
     return v;
 }
