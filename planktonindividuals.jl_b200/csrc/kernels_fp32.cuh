@@ -102,9 +102,6 @@ __device__ __forceinline__ void axis_iw(const Ax1& a, int H, bool face, int& idx
     idx = a.c + H + (lo ? 0 : 1);
     w = lo ? a.o + 0.5f : a.o - 0.5f;
 }
-    if (v > hi) { seterr(err, F32_ERR_DOMAIN); return hi; }
-    return v;
-}
 // clamp into [lo, hi], noting an index outside in `bad` (reported once per individual)
 __device__ __forceinline__ int clampb(int v, int lo, int hi, bool& bad) {
     const int c = min(max(v, lo), hi);
