@@ -161,6 +161,17 @@ def test_fp32_bounded_xy_vs_oracle(gpu_lib):
     _fp32_pair(gpu_lib, wl, 25)
 
 
+def test_fp32_bounded_xy_3d_vs_oracle(gpu_lib):
+    """Bounded x/y on a 3D grid: every axis has at least H cells, so the halos are filled in one
+    pass from their source cells (the 2D grid above keeps the three sequential passes)."""
+    from test_gpu_parity_edge import OVER, regrid
+    from PlanktonIndividuals.grids import Bounded, RectilinearGrid
+    wl = W.config1(n=16, N=900, steps=20, capacity=3000, phyt_over=OVER)
+    wl = regrid(wl, RectilinearGrid(size=(16, 16, 4), x=(0.0, 16e3), y=(0.0, 16e3), z=(0.0, -40.0),
+                                    FT=np.float64, topology=(Bounded, Bounded, Bounded)))
+    _fp32_pair(gpu_lib, wl, 20)
+
+
 def test_fp32_flux_bcs_vs_oracle(gpu_lib):
     wl = daylight(W.config2(nx=12, nz=6, N_per_species=500, nsp=1, steps=12, nmodes=12))
     g = wl.grid
