@@ -142,7 +142,7 @@ def dist_setup():
 
 
 # ------------------------------------------------------------------------------------------
-# algorithmic bytes per launch (the minimum each kernel must move; see DESIGN.md)
+# algorithmic bytes per launch (the minimum each kernel must move)
 # ------------------------------------------------------------------------------------------
 
 def algorithmic_bytes(name, members, n_active_total, n_slots_total):

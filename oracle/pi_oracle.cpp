@@ -1,8 +1,8 @@
 /*
  * pi_oracle.cpp — CPU oracle for the model time step of PlanktonIndividuals.jl (QuotaMode).
  *
- * TEST INFRASTRUCTURE ONLY. Nothing in the product library links or calls this file; it is the
- * checker the tests, smoke() and the CPU-baseline leg of bench.py compare the CUDA path against.
+ * TEST INFRASTRUCTURE ONLY. Nothing in the product library links or calls this file; it is what
+ * the tests, smoke() and the CPU-baseline leg of bench.py compare the CUDA path against.
  *
  * This is a plain Float64 restatement of the reference's TimeStep! written pass by pass in the
  * order of the Julia kernels, each pass citing the file:line it follows (paths relative to the
