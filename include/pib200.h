@@ -4,8 +4,8 @@
  * The reference has no FFI: its public surface is the Julia API (src/PlanktonIndividuals.jl:7-42)
  * RectilinearGrid → PlanktonModel → PlanktonSimulation → update!, with TimeStep! underneath.
  * Each entry point below names the reference function whose job it takes over. A Julia `ccall`
- * shim and the Python package `PlanktonIndividuals` in this repository bind
- * exactly these symbols.
+ * shim on the reference side and the Python package `PlanktonIndividuals` in this repository
+ * bind exactly these symbols.
  *
  * Conventions
  *  - Arrays cross the boundary as host pointers in Julia column-major order (x fastest), with the
