@@ -60,12 +60,14 @@ struct MemberHost {
     HostBC bcs[PI_NTRACERS][6];
 };
 
+// Defaults: the autotuner's choices on a 256×256×64 model with 4 M individuals (pi_batch_autotune
+// retunes them for other sizes; no result depends on them)
 struct Tuning {
-    int bs_move = 256, bs_phys = 256, bs_assign = 256;
-    int persist_move = 0, persist_phys = 0;   // 0: one tile per block; k: k blocks per SM, looping
-    int ty = 8;                               // rows of an x-y tracer tile (4, 8, 16 or 28)
+    int bs_move = 256, bs_phys = 128, bs_assign = 128;
+    int persist_move = 2, persist_phys = 0;   // 0: one tile per block; k: k blocks per SM, looping
+    int ty = 16;                              // rows of an x-y tracer tile (4, 8, 16 or 28)
     int lz = 32;                              // levels walked by a z thread (8, 16, 32 or 64)
-    int wpb_par = 4;
+    int wpb_par = 2;
 };
 
 }  // namespace
