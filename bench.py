@@ -585,9 +585,8 @@ def cpu_sample_workload():
 
 def cpu_baseline(steps):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle
-    from helpers import VelCache, drive
+    from PlanktonIndividuals.stepping import VelCache, drive
     wl = cpu_sample_workload()
     m = oracle.from_workload(wl)
     vel = VelCache(wl)
@@ -610,9 +609,8 @@ def run_reference(args):
     if rank != 0:
         return None
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle
-    from helpers import VelCache, drive
+    from PlanktonIndividuals.stepping import VelCache, drive
     wl = cpu_sample_workload()
     m = oracle.from_workload(wl)
     vel = VelCache(wl)

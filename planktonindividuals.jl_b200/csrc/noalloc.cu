@@ -15,7 +15,13 @@
 //  - calls whose work overlaps on the GPU (different streams, or host threads racing) race on the
 //    array; serialise them, e.g. on one stream;
 //  - the first call on a device looks up the array's device address (cudaGetSymbolAddress) with
-//    that device current; make that first call before any stream capture.
+//    that device current; make that first call before any stream capture. The address is kept for
+//    the life of the process, so the entry point must not be called again on a device after
+//    cudaDeviceReset (or any other teardown of its primary context);
+//  - the grid's dzF, dzC and land mask are host arrays: the call copies them into the fixed array
+//    on `stream` and waits for that copy (and so for the work queued on the stream before it)
+//    before returning, so the caller may free or change them as soon as the call returns. Only
+//    the three sweeps stay queued.
 #include <cstring>
 #include <mutex>
 
@@ -135,6 +141,7 @@ extern "C" {
 pi_status pi_tracer_advection_noalloc(const pi_grid* grid, const double* c, const double* u,
                                       const double* v, const double* w, double dT, double* Gc,
                                       void* stream) {
+    g_err.clear();
     if (!grid || !c || !u || !v || !w || !Gc || !grid->dzF || !grid->dzC)
         return noalloc_fail(PI_ERR_ARG, "pi_tracer_advection_noalloc: NULL argument");
     if (grid->Nx < 1 || grid->Ny < 1 || grid->Nz < 1 || grid->Hx < 2 || grid->Hy < 2 || grid->Hz < 2)
@@ -176,6 +183,9 @@ pi_status pi_tracer_advection_noalloc(const pi_grid* grid, const double* c, cons
     if (cudaMemcpyAsync(dzF, grid->dzF, Gz * sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess ||
         cudaMemcpyAsync(dzC, grid->dzC, Gz * sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess ||
         (!all_water && cudaMemcpyAsync(lm, grid->landmask, G, cudaMemcpyHostToDevice, st) != cudaSuccess))
+        return noalloc_fail(PI_ERR_CUDA, "pi_tracer_advection_noalloc: copy of grid metrics failed");
+    // the caller's host arrays are released on return: wait until the stream has read them
+    if (cudaStreamSynchronize(st) != cudaSuccess)
         return noalloc_fail(PI_ERR_CUDA, "pi_tracer_advection_noalloc: copy of grid metrics failed");
     DGrid g{grid->Nx, grid->Ny, grid->Nz, grid->Hx, grid->Hy, grid->Hz, (int)Gx, (int)Gy, (int)Gz,
             grid->topo[0], grid->topo[1], grid->topo[2], all_water, grid->dx, grid->dy, dzF, dzC, lm, G};

@@ -1,40 +1,9 @@
 """Shared test helpers: drive a model (native GPU or CPU oracle) through update!-style steps and
 compare states exactly."""
-import math
-
 import numpy as np
 
 from PlanktonIndividuals import _abi
-
-
-def forcing_indices(t, wl, time_offset_i=None):
-    """Snapshot indices (0-based) that update! selects at model time t (update.jl:14-26)."""
-    tv = int(math.floor(t / wl.dT_vel))
-    tp = int(math.floor(t / wl.dT_PAR))
-    tt = int(math.floor(t / wl.dT_temp))
-    return tv, tp, tt
-
-
-class VelCache:
-    def __init__(self, wl):
-        self.wl, self.cache = wl, {}
-
-    def __call__(self, i):
-        if i not in self.cache:
-            self.cache[i] = self.wl.velocity(i)
-        return self.cache[i]
-
-
-def drive(model, wl, steps, vel=None):
-    """update!(sim) with vels, one step at a time through the set_* entry points."""
-    vel = vel or VelCache(wl)
-    for _ in range(steps):
-        _, t = model.get_time()
-        tv, tp, tt = forcing_indices(t, wl)
-        model.set_velocity(*vel(tv))
-        model.set_PARF(wl.parf[:, :, tp])
-        model.set_temp(wl.temp[:, :, :, tt])
-        model.time_step(wl.dT)
+from PlanktonIndividuals.stepping import VelCache, drive, forcing_indices  # noqa: F401
 
 
 def same(a, b):
