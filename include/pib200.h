@@ -211,13 +211,18 @@ pi_status pi_profile_read(pi_model* m, int32_t max, char* names, size_t names_le
  * runtime that owns all device allocations through its own pool, or a loop that must not allocate
  * after start-up). `c`, `u`, `v`, `w` and `Gc` are caller-owned DEVICE pointers to halo-padded
  * fields in the layout of pi_set_tracer, with halos already filled; the grid's dzF, dzC and
- * landmask are host pointers as in pi_create. On return the work is queued on `stream`
- * (a cudaStream_t, NULL for the default stream) and Gc's interior holds tracer_temp − tracer after
- * the x, y and z sweeps of tracer_advection! (multi_dim_adv.jl:111-135); Gc's halo is not written.
+ * landmask are host pointers as in pi_create. The call copies dzF, dzC and landmask into device
+ * memory on `stream` (a cudaStream_t, NULL for the default stream) and waits for that copy, and
+ * so for the work queued on the stream before it, before it returns: the host arrays may be
+ * freed or changed once it has returned. The three sweeps are then queued on `stream`; when they
+ * have run, Gc's interior holds tracer_temp − tracer after the x, y and z sweeps of
+ * tracer_advection! (multi_dim_adv.jl:111-135); Gc's halo is not written.
  * The sweeps' intermediates live in one fixed device array shared by all calls on a device:
  * grids above 524,288 halo-padded cells or 4,096 levels are rejected with PI_ERR_ARG; calls that
  * overlap on the GPU race on that array; the first call on a device looks up its address and
- * should come before any stream capture. Errors are reported by pi_noalloc_last_error. */
+ * should come before any stream capture; the address is kept for the life of the process, so the
+ * call must not be used on a device after cudaDeviceReset. pi_noalloc_last_error gives the
+ * message of the last call (empty after a call that succeeded). */
 pi_status pi_tracer_advection_noalloc(const pi_grid* grid, const double* c, const double* u,
                                       const double* v, const double* w, double dT, double* Gc,
                                       void* stream);
