@@ -40,7 +40,7 @@ typedef int32_t pi_status;
 #define PI_ERR_CAPACITY  4   /* division overflow (QuotaMode/plankton_update.jl:20-22)    */
 #define PI_ERR_CUDA      5   /* CUDA runtime error or no usable device                    */
 #define PI_ERR_TIMEOUT   6   /* a bounded device-side wait gave up                        */
-#define PI_ERR_NAN       7   /* NaN found by pi_check_finite                              */
+#define PI_ERR_NAN       7   /* NaN or Inf found by pi_check_finite                       */
 #define PI_ERR_DOMAIN    8   /* an individual's cell index left the halo-padded grid      */
 #define PI_ERR_NOMEM     9   /* device allocation failed                                  */
 #define PI_ERR_STATE    10   /* call not valid in the handle's current state              */
@@ -165,6 +165,12 @@ pi_status pi_set_time(pi_model* m, int64_t iteration, double t);
 
 /* Number of active individuals of species `sp` (calc_active_individuals, models.jl:157-164). */
 pi_status pi_count_active(pi_model* m, int32_t sp, int64_t* n);
+
+/* NaN/Inf check of the model state: every tracer value (halos included) and every attribute of
+ * the active individuals. Returns PI_ERR_NAN with a message naming the first tracer cell or
+ * individual (1-based, as in the reference) that holds one. No counterpart in the reference, where
+ * a user would test the arrays with any(isnan, ...). */
+pi_status pi_check_finite(pi_model* m);
 
 /* Diagnostics accumulated by TimeStep! since the last reset: PI_DIAG_PAR (sp ignored) or the
  * per-species PI_DIAG_NUM/GRAZ/MORT/DVID fields, (Nx+2Hx)(Ny+2Hy)(Nz+2Hz) each. */
@@ -297,6 +303,8 @@ pi_status pi_batch_set_time(pi_batch* b, int64_t iteration, double t);
 
 /* Active individuals of one member and species (sp = -1: all species; member = -1: all members). */
 pi_status pi_batch_count_active(pi_batch* b, int32_t member, int32_t sp, int64_t* n);
+/* As pi_check_finite for one member. */
+pi_status pi_batch_check_finite(pi_batch* b, int32_t member);
 /* As pi_get_diag / pi_reset_diags. */
 pi_status pi_batch_get_diag(pi_batch* b, int32_t member, int32_t kind, int32_t sp, double* out);
 pi_status pi_batch_reset_diags(pi_batch* b);
@@ -312,6 +320,14 @@ pi_status pi_batch_budget(pi_batch* b, int32_t member, double out[6]);
  * keeps the fastest per kernel. The steps it takes are ordinary steps of the model (results do
  * not depend on launch shapes). `report` (may be NULL) receives one line per choice. */
 pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t steps_per_candidate, char* report, size_t report_len);
+
+/* Storage order (no counterpart in the reference, which stores individuals in slot order): each
+ * (member, species) segment is kept in an order grouped by cell, restored by a counting sort
+ * before the first step after pi_batch_set_individuals and then every `steps` steps (default 32;
+ * 0 = keep the current order). Slots keep their numbers at the boundary and in every result:
+ * draws are keyed by slot number and divisions are assigned in slot order, so the interval changes
+ * only the speed, never a result. */
+pi_status pi_batch_set_sort_interval(pi_batch* b, int32_t steps);
 
 /* As pi_get_stream / pi_profile_enable / pi_profile_read / pi_last_error. */
 pi_status pi_batch_get_stream(pi_batch* b, void** stream);

@@ -229,6 +229,11 @@ class CModel:
         self._check(self._fn("count_active")(self.h, int(sp), ct.byref(n)), "count_active")
         return n.value
 
+    def check_finite(self):
+        """Raises PIError (PI_ERR_NAN) naming the first tracer cell or active individual holding a
+        NaN or Inf."""
+        self._check(self._fn("check_finite")(self.h), "check_finite")
+
     def get_diag(self, kind, sp=0):
         out = np.empty(self.G, dtype=np.float64)
         self._check(self._fn("get_diag")(self.h, int(kind), int(sp), _dptr(out)), "get_diag")

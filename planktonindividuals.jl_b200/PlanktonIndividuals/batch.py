@@ -213,6 +213,16 @@ class PlanktonBatch:
     def synchronize(self):
         self._check(self.lib.pi_batch_synchronize(self.h), "synchronize")
 
+    def check_finite(self, m):
+        """Raises PIError (PI_ERR_NAN) naming the first tracer cell or active individual of member
+        m holding a NaN or Inf."""
+        self._check(self.lib.pi_batch_check_finite(self.h, int(m)), "check_finite")
+
+    def set_sort_interval(self, steps):
+        """Steps between the counting sorts that keep the stored individuals grouped by cell
+        (0: never); changes speed only, no result."""
+        self._check(self.lib.pi_batch_set_sort_interval(self.h, int(steps)), "set_sort_interval")
+
     def autotune(self, ΔT, steps_per_candidate=2):
         buf = ct.create_string_buffer(4096)
         self._check(self.lib.pi_batch_autotune(self.h, float(ΔT), int(steps_per_candidate), buf, 4096), "autotune")

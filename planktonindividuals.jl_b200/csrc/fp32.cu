@@ -4,8 +4,10 @@
 // One step is this sequence of launches, each covering every member:
 //   k32_bind             forcing of the step from device-resident series; vel½ buffer choice
 //   k32_velhalf          vel½ for members whose vel₀ and vel₁ differ
-//   k32_move             RK4 + diffusion + find_inds!, pop/Chl sums, previous decisions, tile counts
+//   k32_move             RK4 + diffusion + find_inds!, pop/Chl sums, previous decisions; dividers
+//                        and newly freed slots marked in bitmaps over logical slots
 //   k32_par              calc_par! down each column
+//   k32_count_tiles      dividers and free slots of every tile of logical slots
 //   scan(tile counts)    division and free-slot offsets of every tile
 //   k32_assign           k-th divider → k-th free slot per (member, species) segment
 //   k32_daughters        copy_daughter_individuals! + divide_to_half!
@@ -15,8 +17,11 @@
 //                        terms and apply_tendency!
 //   k32_halo<x,y,z>      fill_halo_tracer!
 //   k32_end_step         vel₀ ← vel₁, iteration and t
+// Every sort_interval steps (and before the first step after an upload) the slots of every segment
+// are put back in cell order by a counting sort into the second buffer of the individual arrays
+// (k32_sort_count, a scan of the bin populations, k32_sort_scatter).
 // Nothing in a step reads a host value, so the step is captured once as a CUDA graph (one per
-// tracer-buffer parity) and replayed. The results do not depend on block shapes, tile-per-block
+// tracer-buffer parity and individual-buffer parity) and replayed. The results do not depend on block shapes, tile-per-block
 // assignment, tracer tile heights or z walk lengths (integer sums commute; every other value is computed by
 // exactly one thread from the same inputs), which lets the autotuner time real steps.
 #include <cub/device/device_scan.cuh>
@@ -110,7 +115,19 @@ struct pi_batch {
     unsigned long long* acc = nullptr;
     unsigned long long* chl_acc = nullptr;
     float4* env = nullptr;          // 2 per cell: packed environment of occupied cells
-    IndDev32 P{};
+    IndDev32 P{};                   // the current individual buffer (Pbuf[pcur])
+    IndDev32 Pbuf[2]{};
+    int pcur = 0;
+    // storage-order sort
+    unsigned long long* sort_bins = nullptr;    // nbins populations
+    unsigned long long* sort_offs = nullptr;    // their exclusive scan, then the fill cursors
+    long long nbins = 0;
+    char* sort_tmp = nullptr;
+    size_t sort_tmp_bytes = 0;
+    int sort_interval = 32;         // steps between sorts; 0: never
+    long long since_sort = 0;
+    bool need_sort = true;
+    long long nwords = 0;           // words of each logical-slot bitmap
     int ntiles = 0;
     int2* tiles = nullptr;
     int* seg_tile0 = nullptr;
@@ -138,7 +155,7 @@ struct pi_batch {
     float* rdzC = nullptr;
     Tuning tune;
     // graphs
-    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    cudaGraphExec_t gexec[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [tracer buffer][individual buffer]
     double graph_dT = -1.0;
     int use_graph = 1;
     // profiling
@@ -217,7 +234,8 @@ void drain(pi_batch* b) {
 
 void free_graphs(pi_batch* b) {
     for (int p = 0; p < 2; ++p)
-        if (b->gexec[p]) { cudaGraphExecDestroy(b->gexec[p]); b->gexec[p] = nullptr; }
+        for (int q = 0; q < 2; ++q)
+            if (b->gexec[p][q]) { cudaGraphExecDestroy(b->gexec[p][q]); b->gexec[p][q] = nullptr; }
     b->graph_dT = -1.0;
 }
 
@@ -374,7 +392,7 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
         MoveArgs a;
         a.T = b->T; a.P = b->P; a.sp = b->sp; a.bgc = b->bgc; a.F = b->F; a.rdzC = b->rdzC; a.st = b->st;
         a.dT = fdT; a.Gtot = G; a.pop = b->pop; a.pop_sp = b->pop_sp; a.chl_acc = b->chl_acc; a.acc = b->acc;
-        a.dcnt = b->dcnt; a.tile_cnt = b->tile_cnt; a.err = b->errw;
+        a.dcnt = b->dcnt; a.err = b->errw;
         BScope sc(b, "k32_move");
         k32_move<<<tile_grid(b, b->tune.persist_move), b->tune.bs_move, 0, s>>>(a);
     }
@@ -382,12 +400,14 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
       k32_par<<<warp_grid(b->T.nicol, b->tune.wpb_par), 32 * b->tune.wpb_par, 0, s>>>(b->T, b->dzF, b->bgc, b->chl_acc, b->PARF,
                                                                                    b->par, b->diag_par, tr, G, b->F, b->pop,
                                                                                    b->env, b->errw); }
+    { BScope sc(b, "k32_count_tiles");
+      k32_count_tiles<<<nblk((long long)b->ntiles * 32, 256), 256, 0, s>>>(b->T, b->P, b->tile_cnt, b->errw); }
     { BScope sc(b, "cub_scan_tiles");
       size_t tb = b->cub_bytes;
       BK(cub::DeviceScan::ExclusiveSum(b->cub_tmp, tb, b->tile_cnt, b->tile_off, b->ntiles, s), "scan tiles"); }
     { BScope sc(b, "k32_assign");
-      k32_assign<<<tile_grid(b, 0), b->tune.bs_assign, 0, s>>>(b->T, b->P, b->tile_cnt, b->tile_off, b->divlist,
-                                                               b->freelist, b->ndiv, b->st, b->errw); }
+      k32_assign<<<nblk((long long)b->ntiles * 32, b->tune.bs_assign), b->tune.bs_assign, 0, s>>>(
+          b->T, b->P, b->tile_cnt, b->tile_off, b->divlist, b->freelist, b->ndiv, b->st, b->errw); }
     { BScope sc(b, "k32_daughters");
       k32_daughters<<<dim3(4, b->nseg), 128, 0, s>>>(b->T, b->P, b->divlist, b->freelist, b->ndiv, b->errw); }
     {
@@ -448,19 +468,52 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
 
 pi_status capture_graphs(pi_batch* b, double dT) {
     free_graphs(b);
-    for (int p = 0; p < 2; ++p) {
-        cudaGraph_t g = nullptr;
-        BK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-        pi_status st = enqueue_step(b, dT, p);
-        cudaError_t e = cudaStreamEndCapture(b->stream, &g);
-        if (st) { if (g) cudaGraphDestroy(g); return st; }
-        if (e != cudaSuccess) return bcuda(b, e, "end capture");
-        e = cudaGraphInstantiate(&b->gexec[p], g, 0);
-        cudaGraphDestroy(g);
-        if (e != cudaSuccess) return bcuda(b, e, "instantiate graph");
+    pi_status st = PI_OK;
+    for (int q = 0; q < 2 && !st; ++q) {
+        b->P = b->Pbuf[q];
+        for (int p = 0; p < 2; ++p) {
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) { st = bcuda(b, e, "begin capture"); break; }
+            st = enqueue_step(b, dT, p);
+            e = cudaStreamEndCapture(b->stream, &g);
+            if (st) { if (g) cudaGraphDestroy(g); break; }
+            if (e != cudaSuccess) { st = bcuda(b, e, "end capture"); break; }
+            e = cudaGraphInstantiate(&b->gexec[p][q], g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) { st = bcuda(b, e, "instantiate graph"); break; }
+        }
     }
+    b->P = b->Pbuf[b->pcur];
+    if (st) return st;
     b->graph_dT = dT;
     return PI_OK;
+}
+
+// Puts every segment's slots back in cell order (into the other individual buffer).
+pi_status enqueue_sort(pi_batch* b) {
+    cudaStream_t s = b->stream;
+    IndDev32& P = b->Pbuf[b->pcur];
+    IndDev32& Q = b->Pbuf[b->pcur ^ 1];
+    { BScope sc(b, "k32_sort");
+      BK(cudaMemsetAsync(b->sort_bins, 0, (size_t)b->nbins * sizeof(unsigned long long), s), "zero sort bins");
+      k32_sort_count<<<tile_grid(b, 8), 256, 0, s>>>(b->T, P, b->sort_bins);
+      size_t tb = b->sort_tmp_bytes;
+      BK(cub::DeviceScan::ExclusiveSum(b->sort_tmp, tb, b->sort_bins, b->sort_offs, b->nbins, s), "scan sort bins");
+      k32_sort_scatter<<<tile_grid(b, 8), 256, 0, s>>>(b->T, P, Q, b->sort_offs);
+      BK(cudaGetLastError(), "sort launch"); }
+    b->pcur ^= 1;
+    b->P = b->Pbuf[b->pcur];
+    b->since_sort = 0;
+    b->need_sort = false;
+    return PI_OK;
+}
+
+// A sort before the next step when one is due.
+pi_status maybe_sort(pi_batch* b) {
+    if (b->sort_interval <= 0) return PI_OK;
+    if (!b->need_sort && b->since_sort < b->sort_interval) return PI_OK;
+    return enqueue_sort(b);
 }
 
 pi_status check_errors(pi_batch* b) {
@@ -472,8 +525,9 @@ pi_status check_errors(pi_batch* b) {
     if (!e) return PI_OK;
     BK(cudaMemsetAsync(b->errw, 0, sizeof(uint32_t), b->stream), "clear error word");
     if (e & F32_ERR_CAPACITY) {
-        // the step stopped after the decisions: drop the unconsumed loss sums
+        // the step stopped after the decisions: drop the unconsumed loss sums and divider marks
         BK(cudaMemsetAsync(b->acc, 0, (size_t)ACC_N * b->Gtot * sizeof(unsigned long long), b->stream), "clear sums");
+        BK(cudaMemsetAsync(b->P.dvbits, 0, (size_t)b->nwords * sizeof(uint32_t), b->stream), "clear divider marks");
         BK(cudaStreamSynchronize(b->stream), "synchronize");
         // TimeStep! advanced model.iteration and model.t before it threw (time_step.jl:14-15)
         hs.iteration = hs.err_iter;
@@ -486,6 +540,7 @@ pi_status check_errors(pi_batch* b) {
         return bfail(b, PI_ERR_CAPACITY, msg);
     }
     BK(cudaStreamSynchronize(b->stream), "synchronize");
+    if (e & F32_ERR_TIMEOUT) return bfail(b, PI_ERR_TIMEOUT, "a bounded wait for staged tracer data gave up");
     if (e & F32_ERR_FORCING) return bfail(b, PI_ERR_SHAPE, "BoundsError: forcing snapshot not provided for the step time");
     if (e & F32_ERR_LISTS) return bfail(b, PI_ERR_STATE, "internal error: a division list entry outside its segment");
     return bfail(b, PI_ERR_DOMAIN, "an individual left the halo-padded grid (cell index out of range)");
@@ -529,7 +584,7 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     std::vector<float> dzF, dzC;
     std::vector<int2> tiles;
     std::vector<int> seg_tile0;
-    long long cell = 0, slot = 0, col = 0;
+    long long cell = 0, slot = 0, col = 0, words = 0, bins = 0;
     int lev = 0;
     bool any_land = false;
     for (int m = 0; m < nmembers; ++m) {
@@ -562,6 +617,8 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
         d.hbx = f32_bits(g.Gx); d.hby = f32_bits(g.Gy);
         d.cell_off = cell; d.G = g.G; d.col_off = col; d.slot_off = slot; d.C = h.C;
         d.dz_off = lev; d.bc_off = m * PI_NTRACERS * 6; d.seed = h.seed;
+        d.woff = words; d.wps = (h.C + F32_TILE - 1) / F32_TILE * (F32_TILE / 32);
+        d.bin_off = bins;
         double cmin = 1e300, chlmin = 1e300;
         for (int s = 0; s < nspecies; ++s) {
             const pi_quota_params& p = h.sp[s];
@@ -583,6 +640,8 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
         }
         cell += (g.G + 63) / 64 * 64;       // members start on 256-byte boundaries
         slot += (long long)nspecies * h.C;
+        words += (long long)nspecies * d.wps;
+        bins += (long long)nspecies * ((long long)g.Nx * g.Ny * g.Nz + 1);
         col += (long long)g.Nx * g.Ny;
         lev += g.Gz;
         b->maxG = std::max(b->maxG, g.G);
@@ -593,6 +652,7 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     seg_tile0.push_back((int)tiles.size());
     if (tiles.size() >= (size_t)INT32_MAX) { b->err = "pi_batch_create: too many slots"; return bail(PI_ERR_ARG); }
     b->Gtot = cell; b->Stot = slot; b->ncol = col; b->nlev = lev; b->ntiles = (int)tiles.size();
+    b->nwords = words; b->nbins = bins;
     const long long G = b->Gtot, S = b->Stot;
     pi_status st;
 #define BA(ptr, n) do { st = balloc(b, &(ptr), (size_t)(n), #ptr); if (st) return bail(st); } while (0)
@@ -608,9 +668,18 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     for (auto& h : b->mh) if (h.bgc.shared_graz != 1.0) shared = false;
     if (!shared) BA(b->pop_sp, (size_t)nspecies * G);
     BA(b->acc, (size_t)ACC_N * G); BA(b->chl_acc, G); BA(b->env, 2 * G);
+    for (int q = 0; q < 2; ++q) {
+        IndDev32& Pq = b->Pbuf[q];
+        BA(Pq.cell, S); BA(Pq.scell, S); BA(Pq.ox, S); BA(Pq.oy, S); BA(Pq.oz, S); BA(Pq.Bm, S); BA(Pq.Cq, S);
+        BA(Pq.Nq, S); BA(Pq.Pq, S); BA(Pq.Chl, S); BA(Pq.age, S); BA(Pq.gen, S); BA(Pq.flags, S); BA(Pq.stat, S);
+        BA(Pq.lslot, S);
+    }
+    BA(b->Pbuf[0].phys, S); BA(b->Pbuf[0].freebits, words); BA(b->Pbuf[0].dvbits, words);
+    b->Pbuf[1].phys = b->Pbuf[0].phys; b->Pbuf[1].freebits = b->Pbuf[0].freebits; b->Pbuf[1].dvbits = b->Pbuf[0].dvbits;
+    b->pcur = 0;
+    b->P = b->Pbuf[0];
     IndDev32& P = b->P;
-    BA(P.cell, S); BA(P.scell, S); BA(P.ox, S); BA(P.oy, S); BA(P.oz, S); BA(P.Bm, S); BA(P.Cq, S);
-    BA(P.Nq, S); BA(P.Pq, S); BA(P.Chl, S); BA(P.age, S); BA(P.gen, S); BA(P.flags, S); BA(P.stat, S);
+    BA(b->sort_bins, bins); BA(b->sort_offs, bins);
     BA(b->tiles, tiles.size()); BA(b->seg_tile0, seg_tile0.size());
     BA(b->tile_cnt, tiles.size()); BA(b->tile_off, tiles.size());
     BA(b->divlist, S); BA(b->freelist, S); BA(b->ndiv, b->nseg);
@@ -621,6 +690,10 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     cub::DeviceScan::ExclusiveSum(nullptr, cb, b->tile_cnt, b->tile_off, b->ntiles, b->stream);
     b->cub_bytes = cb;
     BA(b->cub_tmp, cb);
+    cb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, cb, b->sort_bins, b->sort_offs, b->nbins, b->stream);
+    b->sort_tmp_bytes = cb;
+    BA(b->sort_tmp, cb);
 #undef BA
     // series and forcing tables
     b->serh.assign(nmembers, MemberSeries{});
@@ -685,8 +758,26 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     for (void* p : { (void*)P.ox, (void*)P.oy, (void*)P.oz, (void*)P.Bm, (void*)P.Cq, (void*)P.Nq, (void*)P.Pq,
                      (void*)P.Chl, (void*)P.age, (void*)P.gen }) Z(p, S * sizeof(float));
     Z(P.flags, S); Z(P.stat, S); Z(P.scell, S * sizeof(int32_t));
-    // constructor state: inactive, find_inds! cell (0, 0, 0) (plankton_generation.jl:3)
+    // constructor state: inactive, find_inds! cell (0, 0, 0) (plankton_generation.jl:3); storage
+    // in logical order; every slot free, no divider
     ok = ok && cudaMemsetAsync(P.cell, 0xff, S * sizeof(int32_t), s0) == cudaSuccess;
+    Z(P.dvbits, words * sizeof(uint32_t));
+    {
+        std::vector<uint32_t> fb(words, 0u);
+        for (int m = 0; m < nmembers; ++m) {
+            const MemberDev& d = b->mdh[m];
+            for (int sp = 0; sp < nspecies; ++sp)
+                for (long long L = 0; L < d.C; ++L) fb[d.woff + sp * d.wps + (L >> 5)] |= 1u << (L & 31);
+        }
+        H2D(P.freebits, fb.data(), words * sizeof(uint32_t));
+        ok = ok && cudaStreamSynchronize(s0) == cudaSuccess;
+    }
+    for (int m = 0; m < nmembers && ok; ++m)
+        for (int sp = 0; sp < nspecies; ++sp) {
+            const MemberDev& d = b->mdh[m];
+            k32_identity_order<<<std::min<unsigned>(nblk(d.C, 256), 1024), 256, 0, s0>>>(P, d.slot_off + sp * d.C, d.C);
+        }
+    ok = ok && cudaGetLastError() == cudaSuccess;
     ok = ok && cudaStreamSynchronize(s0) == cudaSuccess;
     if (!ok) { b->err = "pi_batch_create: device initialisation failed"; return bail(PI_ERR_CUDA); }
     cudaFuncSetAttribute(k32_xy<28>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xy_smem(28));
@@ -780,7 +871,16 @@ pi_status pi_batch_set_individuals(pi_batch* b, int32_t member, int32_t sp, cons
     for (int q = 0; q < 7; ++q) BK(cudaMemcpyAsync(fd[q] + g0, f[q].data(), C * 4, cudaMemcpyHostToDevice, s), "upload individuals");
     BK(cudaMemcpyAsync(P.flags + g0, flags.data(), C, cudaMemcpyHostToDevice, s), "upload individuals");
     BK(cudaMemcpyAsync(P.stat + g0, stat.data(), C, cudaMemcpyHostToDevice, s), "upload individuals");
+    // stored in logical order until the next sort; free-slot bits from ac, no divider marks
+    k32_identity_order<<<std::min<unsigned>(nblk(C, 256), 1024), 256, 0, s>>>(P, g0, C);
+    BK(cudaGetLastError(), "upload individuals");
+    std::vector<uint32_t> fb(d.wps, 0u);
+    for (long long i = 0; i < C; ++i) if (!in->ac[i]) fb[i >> 5] |= 1u << (i & 31);
+    const long long w0 = d.woff + (long long)sp * d.wps;
+    BK(cudaMemcpyAsync(P.freebits + w0, fb.data(), d.wps * sizeof(uint32_t), cudaMemcpyHostToDevice, s), "upload individuals");
+    BK(cudaMemsetAsync(P.dvbits + w0, 0, d.wps * sizeof(uint32_t), s), "upload individuals");
     BK(cudaStreamSynchronize(s), "synchronize");
+    b->need_sort = true;
     return PI_OK;
 }
 
@@ -792,11 +892,12 @@ pi_status pi_batch_get_individuals(pi_batch* b, int32_t member, int32_t sp, pi_i
     const HostGrid& g = h.g;
     const long long C = h.C;
     const long long g0 = b->mdh[member].slot_off + (long long)sp * C;
-    std::vector<int32_t> cell(C), scell(C);
+    std::vector<int32_t> cell(C), scell(C), lslot(C);
     std::vector<float> o[3], f[7];
     std::vector<uint8_t> flags(C), stat(C);
     const IndDev32& P = b->P;
     cudaStream_t s = b->stream;
+    BK(cudaMemcpyAsync(lslot.data(), P.lslot + g0, C * 4, cudaMemcpyDeviceToHost, s), "download individuals");
     BK(cudaMemcpyAsync(cell.data(), P.cell + g0, C * 4, cudaMemcpyDeviceToHost, s), "download individuals");
     BK(cudaMemcpyAsync(scell.data(), P.scell + g0, C * 4, cudaMemcpyDeviceToHost, s), "download individuals");
     const float* od[3] = { P.ox, P.oy, P.oz };
@@ -808,19 +909,27 @@ pi_status pi_batch_get_individuals(pi_batch* b, int32_t member, int32_t sp, pi_i
     BK(cudaStreamSynchronize(s), "synchronize");
     const pi_quota_params& p = h.sp[sp];
     const float cq_ns = (float)p.Cquota * (float)p.Nsuper;
-    for (long long i = 0; i < C; ++i) {
-        const uint8_t fl = flags[i];
+    // stored position k holds logical slot lslot[k]: the outputs are in logical order
+    std::vector<char> seen(C, 0);
+    for (long long k = 0; k < C; ++k) {
+        if (lslot[k] < 0 || lslot[k] >= C || seen[lslot[k]]) return bfail(b, PI_ERR_STATE, "pi_get_individuals: storage order corrupted");
+        seen[lslot[k]] = 1;
+    }
+    for (long long k = 0; k < C; ++k) {
+        const long long i = lslot[k];       // logical slot written from stored position k
+        const uint8_t fl = flags[k];
+        const int32_t code = cell[k];
         int ci = 0, cj = 0, ck = 0;
         const MemberDev& md = b->mdh[member];
-        if (cell[i] >= 0) f32_unpack(cell[i], md.cbx, md.cby, ci, cj, ck);
-        const double xyz[3] = { cell[i] < 0 ? 0.0 : ci + (double)o[0][i], cell[i] < 0 ? 0.0 : cj + (double)o[1][i],
-                                cell[i] < 0 ? 0.0 : ck + (double)o[2][i] };
+        if (code >= 0) f32_unpack(code, md.cbx, md.cby, ci, cj, ck);
+        const double xyz[3] = { code < 0 ? 0.0 : ci + (double)o[0][k], code < 0 ? 0.0 : cj + (double)o[1][k],
+                                code < 0 ? 0.0 : ck + (double)o[2][k] };
         int64_t xi, yi, zi;
-        if (stat[i] & F32_ST_STALE) {
+        if (stat[k] & F32_ST_STALE) {
             int a0, a1, a2;
-            f32_unpack(scell[i], md.hbx, md.hby, a0, a1, a2);
+            f32_unpack(scell[k], md.hbx, md.hby, a0, a1, a2);
             xi = a0; yi = a1; zi = a2;
-        } else if (cell[i] < 0) { xi = g.Hx; yi = g.Hy; zi = g.Hz; }
+        } else if (code < 0) { xi = g.Hx; yi = g.Hy; zi = g.Hz; }
         else { xi = ci + 1 + g.Hx; yi = cj + 1 + g.Hy; zi = ck + 1 + g.Hz; }
         if (out->x) out->x[i] = xyz[0];
         if (out->y) out->y[i] = xyz[1];
@@ -829,8 +938,8 @@ pi_status pi_batch_get_individuals(pi_batch* b, int32_t member, int32_t sp, pi_i
         if (out->yi) out->yi[i] = yi;
         if (out->zi) out->zi[i] = zi;
         double* cols[7] = { out->Bm, out->Cq, out->Nq, out->Pq, out->Chl, out->age, out->gen };
-        for (int q = 0; q < 7; ++q) if (cols[q]) cols[q][i] = (double)f[q][i];
-        if (out->Sz) out->Sz[i] = (double)(f[0][i] / cq_ns);
+        for (int q = 0; q < 7; ++q) if (cols[q]) cols[q][i] = (double)f[q][k];
+        if (out->Sz) out->Sz[i] = (double)(f[0][k] / cq_ns);
         if (out->ac) out->ac[i] = (fl & F32_AC) ? 1 : 0;
         if (out->graz) out->graz[i] = (fl & F32_GRAZ) ? 1.0 : 0.0;
         if (out->mort) out->mort[i] = (fl & F32_MORT) ? 1.0 : 0.0;
@@ -1136,14 +1245,18 @@ pi_status pi_batch_step(pi_batch* b, double dT, int64_t nsteps, int32_t sync) {
     BK(cudaMemsetAsync(&b->st->call_step, 0, sizeof(int64_t), b->stream), "reset call step");
     if (b->profiling || !b->use_graph) {
         for (int64_t i = 0; i < nsteps; ++i) {
+            if ((e = maybe_sort(b))) return e;
             if ((e = enqueue_step(b, dT, b->cur))) return e;
             b->cur ^= 1;
+            b->since_sort += 1;
         }
     } else {
-        if (b->graph_dT != dT || !b->gexec[0]) { if ((e = capture_graphs(b, dT))) return e; }
+        if (b->graph_dT != dT || !b->gexec[0][0]) { if ((e = capture_graphs(b, dT))) return e; }
         for (int64_t i = 0; i < nsteps; ++i) {
-            BK(cudaGraphLaunch(b->gexec[b->cur], b->stream), "graph launch");
+            if ((e = maybe_sort(b))) return e;
+            BK(cudaGraphLaunch(b->gexec[b->cur][b->pcur], b->stream), "graph launch");
             b->cur ^= 1;
+            b->since_sort += 1;
         }
     }
     if (sync) return pi_batch_synchronize(b);
@@ -1208,6 +1321,39 @@ pi_status pi_batch_get_diag(pi_batch* b, int32_t member, int32_t kind, int32_t s
     return PI_OK;
 }
 
+pi_status pi_batch_check_finite(pi_batch* b, int32_t member) {
+    pi_status e = check_mem(b, member, "pi_check_finite");
+    if (e) return e;
+    const MemberDev& d = b->mdh[member];
+    unsigned long long* dq = b->scratch;
+    const unsigned long long none = ~0ull;
+    unsigned long long q = none;
+    for (int n = 0; n < PI_NTRACERS; ++n) {
+        BK(cudaMemcpyAsync(dq, &none, sizeof none, cudaMemcpyHostToDevice, b->stream), "check finite");
+        k32_first_nonfinite<<<std::min<unsigned>(nblk(d.G, 256), 148 * 4), 256, 0, b->stream>>>(
+            b->trbuf[b->cur] + (long long)n * b->Gtot + d.cell_off, d.G, dq);
+        BK(cudaGetLastError(), "check finite");
+        BK(cudaMemcpyAsync(&q, dq, sizeof q, cudaMemcpyDeviceToHost, b->stream), "check finite");
+        BK(cudaStreamSynchronize(b->stream), "synchronize");
+        if (q != none) {
+            const long long c = (long long)q;
+            const long long i = c % d.Gx + 1, j = (c / d.Gx) % d.Gy + 1, k = c / ((long long)d.Gx * d.Gy) + 1;
+            return bfail(b, PI_ERR_NAN, "NaN or Inf in tracer " + std::string(tracer_name(n)) + " at (" + std::to_string(i) +
+                                            ", " + std::to_string(j) + ", " + std::to_string(k) + ")");
+        }
+    }
+    for (int s = 0; s < b->nsp; ++s) {
+        BK(cudaMemcpyAsync(dq, &none, sizeof none, cudaMemcpyHostToDevice, b->stream), "check finite");
+        k32_first_nonfinite_inds<<<std::min<unsigned>(nblk(d.C, 256), 148 * 2), 256, 0, b->stream>>>(b->P, d.slot_off + s * d.C, d.C, dq);
+        BK(cudaGetLastError(), "check finite");
+        BK(cudaMemcpyAsync(&q, dq, sizeof q, cudaMemcpyDeviceToHost, b->stream), "check finite");
+        BK(cudaStreamSynchronize(b->stream), "synchronize");
+        if (q != none)
+            return bfail(b, PI_ERR_NAN, "NaN or Inf in an attribute of individual " + std::to_string(q + 1) + " of species " + std::to_string(s + 1));
+    }
+    return PI_OK;
+}
+
 pi_status pi_batch_reset_diags(pi_batch* b) {
     if (!b) return bfail(b, PI_ERR_ARG, "pi_reset_diags: NULL batch");
     BK(cudaMemsetAsync(b->diag_par, 0, b->Gtot * sizeof(float), b->stream), "reset diags");
@@ -1233,6 +1379,12 @@ pi_status pi_batch_budget(pi_batch* b, int32_t member, double out[6]) {
     BK(cudaMemcpyAsync(h.data(), b->partial, 3 * nb * sizeof(double), cudaMemcpyDeviceToHost, b->stream), "download budget");
     BK(cudaStreamSynchronize(b->stream), "synchronize");
     for (int r = 0; r < 3; ++r) { double s = 0.0; for (int q = 0; q < nb; ++q) s += h[q * 3 + r]; out[3 + r] = s; }
+    return PI_OK;
+}
+
+pi_status pi_batch_set_sort_interval(pi_batch* b, int32_t steps) {
+    if (!b || steps < 0) return bfail(b, PI_ERR_ARG, "pi_batch_set_sort_interval: bad argument");
+    b->sort_interval = steps;
     return PI_OK;
 }
 
@@ -1282,7 +1434,12 @@ pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t k, char* report, siz
         b->prof_names.clear(); b->prof_count.clear(); b->prof_ms.clear();
         b->last_dT = dT;
         if ((e = build_tables(b))) return e;
-        for (int i = 0; i < k; ++i) { if ((e = enqueue_step(b, dT, b->cur))) return e; b->cur ^= 1; }
+        for (int i = 0; i < k; ++i) {
+            if ((e = maybe_sort(b))) return e;
+            if ((e = enqueue_step(b, dT, b->cur))) return e;
+            b->cur ^= 1;
+            b->since_sort += 1;
+        }
         BK(cudaStreamSynchronize(b->stream), "synchronize");
         drain(b);
         if ((e = check_errors(b))) return e;

@@ -26,6 +26,7 @@
 #define F32_ERR_CAPACITY 2u
 #define F32_ERR_FORCING  4u
 #define F32_ERR_LISTS    8u     // a division list entry outside its segment (access skipped)
+#define F32_ERR_TIMEOUT  16u    // a bounded wait for staged data gave up
 
 // Slots are processed in tiles of this many consecutive slots of one (member, species) segment.
 #define F32_TILE 1024
@@ -47,6 +48,9 @@ struct MemberDev {
     long long C;            // capacity per species
     int dz_off;             // first of the member's Gz levels in dzF/dzC
     int bc_off;             // first of the member's 14*6 flux boundary conditions
+    long long woff;         // first word of species 0 in the logical-slot bitmaps
+    long long wps;          // bitmap words per species (32 per tile of F32_TILE slots)
+    long long bin_off;      // first cell-sort bin of species 0 (Nx*Ny*Nz + 1 bins per species)
     uint64_t seed;
     double fx_unit;         // mmol per fixed-point unit of the particle→grid mass sums
     double chl_unit;        // mg Chl per fixed-point unit of the Chl sums
@@ -113,6 +117,13 @@ struct StepState {
 };
 
 // Individuals of all members and species.
+//
+// Storage order. Each (member, species) segment of `capacity` slots is stored in a physical order
+// that a periodic counting sort keeps grouped by cell, so that neighbouring threads read
+// neighbouring velocity corners and add into neighbouring cell sums. Every slot keeps its logical
+// slot number (the reference's array index), which keys its random draws and orders the division
+// bookkeeping, so no result depends on the physical order. Arrays below are indexed by physical
+// position unless stated.
 struct IndDev32 {
     int32_t* cell;          // interior cell of the position: ci + (Nx+1)(cj + (Ny+1) ck); -1 inactive
     int32_t* scell;         // find_inds! cell (xi + (Gx+1)(yi + (Gy+1) zi)) when F32_ST_STALE
@@ -120,6 +131,11 @@ struct IndDev32 {
     float *Bm, *Cq, *Nq, *Pq, *Chl, *age, *gen;
     uint8_t* flags;
     uint8_t* stat;
+    int32_t* lslot;         // logical slot (within the segment) held at this physical position
+    // indexed by logical slot (shared by both physical buffers)
+    int32_t* phys;          // physical position (within the segment) of each logical slot
+    uint32_t* freebits;     // bit set: the logical slot is inactive (MemberDev::woff layout)
+    uint32_t* dvbits;       // bit set: the logical slot divides in this step
 };
 
 struct SpeciesDev32 {

@@ -99,4 +99,11 @@ inline std::string julia_float(double x) {
 }
 
 
+// Tracer names in the reference's order (src/Biogeochemistry/Biogeochemistry.jl:20).
+inline const char* tracer_name(int n) {
+    static const char* names[PI_NTRACERS] = { "DIC", "NH4", "NO3", "PO4", "DFe", "DOC", "DON", "DOP",
+                                              "PFe_inorg", "POC", "PON", "POP", "PFe_bio", "Dust" };
+    return n >= 0 && n < PI_NTRACERS ? names[n] : "?";
+}
+
 }  // namespace pih

@@ -10,7 +10,10 @@
 //    fixed-point integers added with atomics; integer addition commutes, so the sums do not depend
 //    on the order in which individuals are visited and no sort is needed for determinism; pop and
 //    the diagnostic counts are exact integer counts;
-//  - Sz is not stored: it is Bm / (Cquota Nsuper), as update_cellsize_kernel! sets it.
+//  - Sz is not stored: it is Bm / (Cquota Nsuper), as update_cellsize_kernel! sets it;
+//  - individuals are stored in a physical order grouped by cell (kept by a periodic counting sort)
+//    behind their logical slot numbers: draws are keyed by the logical slot and the division
+//    bookkeeping runs on bitmaps over logical slots, so the order changes no result.
 // FP64 is used for the fixed-point conversions, the mass budgets and the DST3FL limiter ratio
 // where the centred gradient is within a few FP32 ulps of zero.
 #pragma once
@@ -303,9 +306,14 @@ struct MoveArgs {
     unsigned long long* chl_acc;   // Gtot
     unsigned long long* acc;       // ACC_N × Gtot
     uint32_t* dcnt;                // nsp × 4 × Gtot: num, graz, mort, dvid
-    unsigned long long* tile_cnt;  // ntiles: (dividers << 32) | free slots
     uint32_t* err;
 };
+
+// bit of logical slot L of species s of member m in a logical-slot bitmap
+__device__ __forceinline__ void slot_bit(const MemberDev& m, int s, int L, long long& w, uint32_t& bit) {
+    w = m.woff + (long long)s * m.wps + (L >> 5);
+    bit = 1u << (L & 31);
+}
 
 // The slot state k32_move reads first, loaded one slot ahead of its use (the offsets and Chl of an
 // inactive slot are read and unused).
@@ -320,8 +328,7 @@ __device__ __forceinline__ MState move_state(const IndDev32& P, long long g, boo
 }
 
 __device__ __forceinline__ void move_one(const MoveArgs& a, const MemberDev& m, const PGeom& pg, int mi, int s,
-                                         long long slot, long long g, uint32_t iter, const MState& S,
-                                         int& is_div, int& is_free) {
+                                         long long g, uint32_t iter, const MState& S) {
     const IndDev32& P = a.P;
     const uint8_t fl = S.fl, stt = S.stt;
     const int32_t code = S.code;
@@ -334,7 +341,6 @@ __device__ __forceinline__ void move_one(const MoveArgs& a, const MemberDev& m, 
             P.ox[g] = 0.0f; P.oy[g] = 0.0f; P.oz[g] = 0.0f;
         }
         if (stt) P.stat[g] = 0;
-        is_div = 0; is_free = 1;
         return;
     }
     uint32_t* err = a.err;
@@ -377,7 +383,7 @@ __device__ __forceinline__ void move_one(const MoveArgs& a, const MemberDev& m, 
     const BgcDev32& b = a.bgc[mi];
     if (b.kappa_hP != 0.0f || b.kappa_vP != 0.0f) {
         float r0, r1, r2;
-        draw3f(m.seed, iter, (uint32_t)s, PI_DRAW_DIFFUSION, (uint32_t)slot, r0, r1, r2);
+        draw3f(m.seed, iter, (uint32_t)s, PI_DRAW_DIFFUSION, (uint32_t)P.lslot[g], r0, r1, r2);
         move(X, (r0 - 0.5f) * 2.0f * sqrtf(b.kappa_hP * dT) * pg.rdx, pg.Nx, pg.tx);
         move(Y, (r1 - 0.5f) * 2.0f * sqrtf(b.kappa_hP * dT) * pg.rdy, pg.Ny, pg.ty);
         move(Z, (r2 - 0.5f) * 2.0f * sqrtf(b.kappa_vP * dT) * __ldg(rdzC + pg.dz_off + kdz - 1), pg.Nz, pg.tz);
@@ -421,12 +427,18 @@ __device__ __forceinline__ void move_one(const MoveArgs& a, const MemberDev& m, 
     }
     P.flags[g] = (uint8_t)((ac2 ? F32_AC : 0) | (dv2 ? F32_DVID : 0));
     P.stat[g] = F32_ST_AC0;
-    is_div = dv2; is_free = !ac2;
+    // division bookkeeping on logical slots: dividers of this step, slots freed by this step's
+    // grazing and mortality (free slots stay marked until a daughter takes them)
+    if (dv2 || !ac2) {
+        long long w;
+        uint32_t bit;
+        slot_bit(m, s, P.lslot[g], w, bit);
+        atomicOr(dv2 ? &P.dvbits[w] : &P.freebits[w], bit);
+    }
 }
 
 __global__ void __launch_bounds__(256, 2) k32_move(MoveArgs a) {
     if (stopped(a.err)) return;
-    __shared__ unsigned int sh_d, sh_f;
     __shared__ PGeom sg;
     const int bs = blockDim.x, ppt = F32_TILE / bs;
     const uint32_t iter = (uint32_t)(a.st->iteration + 1);
@@ -438,25 +450,13 @@ __global__ void __launch_bounds__(256, 2) k32_move(MoveArgs a) {
         if (threadIdx.x == 0) sg = pgeom(m, a.F[mi]);
         __syncthreads();
         const long long base = m.slot_off + (long long)s * m.C;
-        unsigned int nd = 0, nf = 0;
         long long slot = (long long)tl.y + threadIdx.x;
         MState nx = move_state(a.P, base + slot, slot < m.C);
         for (int p = 0; p < ppt; ++p, slot += bs) {
             const MState cur = nx;
             if (p + 1 < ppt) nx = move_state(a.P, base + slot + bs, slot + bs < m.C);
-            if (slot < m.C) {
-                int d, f;
-                move_one(a, m, sg, mi, s, slot, base + slot, iter, cur, d, f);
-                nd += d; nf += f;
-            }
+            if (slot < m.C) move_one(a, m, sg, mi, s, base + slot, iter, cur);
         }
-        if (threadIdx.x == 0) { sh_d = 0; sh_f = 0; }
-        __syncthreads();
-        nd = __reduce_add_sync(0xffffffffu, nd);
-        nf = __reduce_add_sync(0xffffffffu, nf);
-        if ((threadIdx.x & 31) == 0) { atomicAdd(&sh_d, nd); atomicAdd(&sh_f, nf); }
-        __syncthreads();
-        if (threadIdx.x == 0) a.tile_cnt[t] = ((unsigned long long)sh_d << 32) | sh_f;
         __syncthreads();
     }
 }
@@ -518,20 +518,52 @@ __global__ void k32_par(Tab32 T, const float* __restrict__ dzF, const BgcDev32* 
 }
 
 // ------------------------------------------------------------------------------------------
-// (e) division: k-th divider (slot order) → k-th free slot (findall(!ac), ascending), per segment
-// (get_tind!, Individuals/utils.jl:76-86), with the capacity check (plankton_update.jl:18-22).
-// Ranks inside a tile come from warp ballots, tile offsets from the scan of the tile counts.
-// Tiles with neither dividers nor needed free slots do nothing.
+// (e) division: k-th divider (logical slot order) → k-th free logical slot (findall(!ac),
+// ascending), per segment (get_tind!, Individuals/utils.jl:76-86), with the capacity check
+// (plankton_update.jl:18-22). Dividers and free slots are bits of two bitmaps over logical slots;
+// a tile of F32_TILE logical slots is 32 words, one per lane of a warp.
 // ------------------------------------------------------------------------------------------
+
+// (dividers << 32) | free slots of every tile, from the bitmaps. One warp per tile.
+__global__ void k32_count_tiles(Tab32 T, IndDev32 P, unsigned long long* __restrict__ tile_cnt, const uint32_t* err) {
+    if (stopped(err)) return;
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < T.ntiles; t += nw) {
+        const int2 tl = T.tiles[t];
+        int mi, s;
+        seg_of(T, tl.x, mi, s);
+        const MemberDev& m = T.md[mi];
+        const long long w = m.woff + (long long)s * m.wps + (tl.y >> 5) + lane;
+        const unsigned nd = __reduce_add_sync(0xffffffffu, (unsigned)__popc(P.dvbits[w]));
+        const unsigned nf = __reduce_add_sync(0xffffffffu, (unsigned)__popc(P.freebits[w]));
+        if (lane == 0) tile_cnt[t] = ((unsigned long long)nd << 32) | nf;
+    }
+}
+
+// exclusive prefix sum over the lanes of a warp
+__device__ __forceinline__ unsigned warp_exscan(unsigned v) {
+    const int lane = threadIdx.x & 31;
+    unsigned x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    return x - v;
+}
+
+// Lists of the dividers and of the free slots they take, in logical order. One warp per tile;
+// tiles with neither dividers nor needed free slots do nothing. The divider bits are cleared once
+// listed.
 __global__ void k32_assign(Tab32 T, IndDev32 P, const unsigned long long* __restrict__ tile_cnt,
                            const unsigned long long* __restrict__ tile_off, int* __restrict__ divlist,
                            int* __restrict__ freelist, uint32_t* __restrict__ ndiv, StepState* st,
                            uint32_t* err) {
     if (stopped(err)) return;
-    __shared__ unsigned int wd[32], wf[32];
-    const int bs = blockDim.x, ppt = F32_TILE / bs, nwarp = bs >> 5;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < T.ntiles; t += nw) {
         const int2 tl = T.tiles[t];
         const int seg = tl.x;
         int mi, s;
@@ -543,7 +575,7 @@ __global__ void k32_assign(Tab32 T, IndDev32 P, const unsigned long long* __rest
         const unsigned long long tot = tile_off[t1 - 1] + tile_cnt[t1 - 1] - b0;
         const unsigned int tdiv = (unsigned int)(tot >> 32), tfree = (unsigned int)(tot & 0xffffffffull);
         if (tdiv > tfree) {
-            if (t == t0 && threadIdx.x == 0) {
+            if (t == t0 && lane == 0) {
                 ndiv[seg] = 0;
                 if (!(atomicOr(err, F32_ERR_CAPACITY) & F32_ERR_CAPACITY)) {
                     st->err_iter = st->iteration + 1;
@@ -552,39 +584,33 @@ __global__ void k32_assign(Tab32 T, IndDev32 P, const unsigned long long* __rest
             }
             continue;
         }
-        if (t == t0 && threadIdx.x == 0) ndiv[seg] = tdiv;
+        if (t == t0 && lane == 0) ndiv[seg] = tdiv;
         const unsigned long long before = tile_off[t] - b0;
         const unsigned int dbefore = (unsigned int)(before >> 32), fbefore = (unsigned int)(before & 0xffffffffull);
         const unsigned long long c = tile_cnt[t];
-        const bool work = (c >> 32) != 0 || ((c & 0xffffffffull) != 0 && fbefore < tdiv);
-        if (!work) continue;                                        // uniform over the block
-        unsigned int rd = dbefore, rf = fbefore;
-        for (int p = 0; p < ppt; ++p) {
-            const long long slot = (long long)tl.y + p * bs + threadIdx.x;
-            const bool valid = slot < m.C;
-            const uint8_t fl = valid ? P.flags[base + slot] : (uint8_t)F32_AC;
-            const bool isd = (fl & F32_DVID) != 0, isf = !(fl & F32_AC);
-            const unsigned int bd = __ballot_sync(0xffffffffu, isd), bf = __ballot_sync(0xffffffffu, isf);
-            if (lane == 0) { wd[wid] = __popc(bd); wf[wid] = __popc(bf); }
-            __syncthreads();
-            unsigned int pd = 0, pf = 0, sd = 0, sf = 0;
-            for (int w = 0; w < nwarp; ++w) {
-                if (w < wid) { pd += wd[w]; pf += wf[w]; }
-                sd += wd[w]; sf += wf[w];
-            }
-            const unsigned int lt = (1u << lane) - 1u;
-            if (isd) divlist[base + rd + pd + __popc(bd & lt)] = (int)slot;
-            if (isf) {
-                const unsigned int kf = rf + pf + __popc(bf & lt);
-                if (kf < tdiv) freelist[base + kf] = (int)slot;
-            }
-            rd += sd; rf += sf;
-            __syncthreads();
+        const bool wd = (c >> 32) != 0, wf = (c & 0xffffffffull) != 0 && fbefore < tdiv;
+        if (!wd && !wf) continue;                                   // uniform over the warp
+        const long long w = m.woff + (long long)s * m.wps + (tl.y >> 5) + lane;
+        uint32_t dw = wd ? P.dvbits[w] : 0u, fw = wf ? P.freebits[w] : 0u;
+        unsigned rd = dbefore + warp_exscan((unsigned)__popc(dw));
+        unsigned rf = fbefore + warp_exscan((unsigned)__popc(fw));
+        const int L0 = tl.y + lane * 32;
+        while (dw) {
+            const int bpos = __ffs(dw) - 1;
+            dw &= dw - 1u;
+            divlist[base + rd++] = L0 + bpos;
         }
+        while (fw && rf < tdiv) {
+            const int bpos = __ffs(fw) - 1;
+            fw &= fw - 1u;
+            freelist[base + rf++] = L0 + bpos;
+        }
+        if (wd) P.dvbits[w] = 0u;
     }
 }
 
-// copy_daughter_individuals! and divide_to_half! (division_death.jl:28-63). Grid: (x, segments).
+// copy_daughter_individuals! and divide_to_half! (division_death.jl:28-63). The lists hold logical
+// slots; phys gives where each is stored. Grid: (x, segments).
 __global__ void k32_daughters(Tab32 T, IndDev32 P, const int* __restrict__ divlist,
                               const int* __restrict__ freelist, const uint32_t* __restrict__ ndiv,
                               uint32_t* err) {
@@ -598,7 +624,9 @@ __global__ void k32_daughters(Tab32 T, IndDev32 P, const int* __restrict__ divli
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const int pl = divlist[base + k], dl = freelist[base + k];
         if (k >= (uint32_t)m.C || pl < 0 || pl >= m.C || dl < 0 || dl >= m.C) { seterr(err, F32_ERR_LISTS); continue; }
-        const long long p = base + pl, d = base + dl;
+        const int pp = P.phys[base + pl], dp = P.phys[base + dl];
+        if (pp < 0 || pp >= m.C || dp < 0 || dp >= m.C) { seterr(err, F32_ERR_LISTS); continue; }
+        const long long p = base + pp, d = base + dp;
         // the daughter's slot keeps the cell find_inds! gave it this step
         const int32_t cd = P.cell[d];
         int32_t sc;
@@ -615,6 +643,10 @@ __global__ void k32_daughters(Tab32 T, IndDev32 P, const int* __restrict__ divli
         P.age[p] = P.age[p] * 0.0f;
         P.flags[d] = F32_AC | F32_DVID;
         P.stat[d] = (uint8_t)((P.stat[d] & F32_ST_AC0) | F32_ST_STALE);
+        long long w;
+        uint32_t bit;
+        slot_bit(m, s, dl, w, bit);
+        atomicAnd(&P.freebits[w], ~bit);
     }
 }
 
@@ -660,15 +692,15 @@ struct PhysArgs {
     const uint32_t* err;
 };
 
-// flags, status and cell of a slot, loaded one slot ahead of its physiology
-struct PHead { int32_t code; uint8_t fl, stt; };
+// flags, status, cell and logical slot of a slot, loaded one slot ahead of its physiology
+struct PHead { int32_t code, ls; uint8_t fl, stt; };
 __device__ __forceinline__ PHead phys_head(const IndDev32& P, long long g, bool valid) {
-    PHead h{-1, 0, 0};
-    if (valid) { h.fl = P.flags[g]; h.stt = P.stat[g]; h.code = P.cell[g]; }
+    PHead h{-1, 0, 0, 0};
+    if (valid) { h.fl = P.flags[g]; h.stt = P.stat[g]; h.code = P.cell[g]; h.ls = P.lslot[g]; }
     return h;
 }
 
-__device__ __forceinline__ void phys_one(const PhysArgs& a, const MemberDev& m, int mi, int s, long long slot,
+__device__ __forceinline__ void phys_one(const PhysArgs& a, const MemberDev& m, int mi, int s,
                                          long long g, uint32_t iter, double tnow, const PHead& hd) {
     const IndDev32& P = a.P;
     // the quotas are loaded with the environment
@@ -748,7 +780,7 @@ __device__ __forceinline__ void phys_one(const PhysArgs& a, const MemberDev& m, 
     }
     // get_probability! (:95-107)
     float r0, r1, r2;
-    draw3f(m.seed, iter, (uint32_t)s, PI_DRAW_DECISION, (uint32_t)slot, r0, r1, r2);
+    draw3f(m.seed, iter, (uint32_t)s, PI_DRAW_DECISION, (uint32_t)hd.ls, r0, r1, r2);
     const int dg = jl_lessf(r0, graz * dT), dm = jl_lessf(r1, mort * dT), dd = jl_lessf(r2, dv * dT);
     P.Bm[g] = Bm; P.Cq[g] = Cq; P.Nq[g] = Nq; P.Pq[g] = Pq; P.Chl[g] = Chl; P.age[g] = age;
     P.flags[g] = (uint8_t)(F32_AC | (dg ? F32_GRAZ : 0) | (dm ? F32_MORT : 0) | (dd ? F32_DVID : 0));
@@ -780,7 +812,7 @@ __global__ void __launch_bounds__(256, 4) k32_physiology(PhysArgs a) {
         for (int p = 0; p < ppt; ++p, slot += bs) {
             const PHead cur = hd;
             if (p + 1 < ppt) hd = phys_head(a.P, base + slot + bs, slot + bs < m.C);
-            if (slot < m.C) phys_one(a, m, mi, s, slot, base + slot, iter, tnow, cur);
+            if (slot < m.C) phys_one(a, m, mi, s, base + slot, iter, tnow, cur);
         }
     }
 }
@@ -1471,6 +1503,24 @@ __global__ void k32_u2d(double* __restrict__ dst, const uint32_t* __restrict__ s
         dst[q] = (double)src[q];
 }
 
+// Index of the first non-finite value of a[0, n) (atomicMin into *first, which starts at ~0).
+__global__ void k32_first_nonfinite(const float* __restrict__ a, long long n, unsigned long long* first) {
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        if (!isfinite(a[q])) atomicMin(first, (unsigned long long)q);
+}
+
+// First logical slot of a segment whose active individual has a non-finite attribute.
+__global__ void k32_first_nonfinite_inds(IndDev32 P, long long base, long long C, unsigned long long* first) {
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < C; q += (long long)gridDim.x * blockDim.x) {
+        const long long g = base + q;
+        if (!(P.flags[g] & F32_AC)) continue;
+        const float v[10] = { P.ox[g], P.oy[g], P.oz[g], P.Bm[g], P.Cq[g], P.Nq[g], P.Pq[g], P.Chl[g], P.age[g], P.gen[g] };
+        bool bad = false;
+        for (int k = 0; k < 10; ++k) bad |= !isfinite(v[k]);
+        if (bad) atomicMin(first, (unsigned long long)P.lslot[g]);
+    }
+}
+
 // Active individuals of a slot range (calc_active_individuals, models.jl:157-164).
 __global__ void k32_count_active(const uint8_t* __restrict__ flags, long long n, unsigned long long* out) {
     unsigned long long c = 0;
@@ -1512,7 +1562,8 @@ __global__ void k32_budget_inds(MemberDev m, int nsp, const SpeciesDev32* __rest
     double c = 0.0, n = 0.0, p = 0.0;
     const long long S = (long long)nsp * m.C;
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < S; q += (long long)gridDim.x * blockDim.x) {
-        const long long g = m.slot_off + q;
+        // logical slot order, so the sum does not depend on the storage order
+        const long long g = m.slot_off + (q / m.C) * m.C + P.phys[m.slot_off + q];
         if (!(P.flags[g] & F32_AC)) continue;
         const SpeciesDev32& s = sp[q / m.C];
         const double Bm = P.Bm[g];
@@ -1527,6 +1578,74 @@ __global__ void k32_budget_inds(MemberDev m, int nsp, const SpeciesDev32* __rest
         __syncthreads();
     }
     if (threadIdx.x == 0) for (int r = 0; r < 3; ++r) partial[blockIdx.x * 3 + r] = sh[r][0];
+}
+
+// ------------------------------------------------------------------------------------------
+// storage order: counting sort of every segment by cell (a periodic pass between steps)
+// ------------------------------------------------------------------------------------------
+
+// sort bin of a stored slot: its interior cell in x-fastest order, or the last bin when inactive
+__device__ __forceinline__ long long sort_bin(const MemberDev& m, int s, uint8_t fl, int32_t code) {
+    const long long V = (long long)m.Nx * m.Ny * m.Nz;
+    long long b = V;
+    if ((fl & F32_AC) && code >= 0) {
+        int ci, cj, ck;
+        unpack_int(m, code, ci, cj, ck);
+        b = min(ci, m.Nx - 1) + (long long)m.Nx * (min(cj, m.Ny - 1) + (long long)m.Ny * min(ck, m.Nz - 1));
+    }
+    return m.bin_off + (long long)s * (V + 1) + b;
+}
+
+// population of every bin (bins zeroed beforehand)
+__global__ void k32_sort_count(Tab32 T, IndDev32 P, unsigned long long* __restrict__ bins) {
+    for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
+        const int2 tl = T.tiles[t];
+        int mi, s;
+        seg_of(T, tl.x, mi, s);
+        const MemberDev& m = T.md[mi];
+        const long long base = m.slot_off + (long long)s * m.C;
+        for (long long slot = (long long)tl.y + threadIdx.x; slot < min((long long)tl.y + F32_TILE, m.C); slot += blockDim.x) {
+            const long long g = base + slot;
+            atomicAdd(&bins[sort_bin(m, s, P.flags[g], P.cell[g])], 1ull);
+        }
+    }
+}
+
+// Moves every slot from P to Q at the next position of its bin (offs: the exclusive scan of the
+// bin populations over the whole batch, which starts each segment's bins at the segment's first
+// slot) and records where each logical slot went. The order inside a bin is that of the atomics;
+// nothing computed from the individuals depends on it.
+__global__ void k32_sort_scatter(Tab32 T, IndDev32 P, IndDev32 Q, unsigned long long* __restrict__ offs) {
+    for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
+        const int2 tl = T.tiles[t];
+        int mi, s;
+        seg_of(T, tl.x, mi, s);
+        const MemberDev& m = T.md[mi];
+        const long long base = m.slot_off + (long long)s * m.C;
+        for (long long slot = (long long)tl.y + threadIdx.x; slot < min((long long)tl.y + F32_TILE, m.C); slot += blockDim.x) {
+            const long long g = base + slot;
+            const uint8_t fl = P.flags[g];
+            const int32_t code = P.cell[g];
+            const long long np = (long long)atomicAdd(&offs[sort_bin(m, s, fl, code)], 1ull);
+            Q.cell[np] = code; Q.scell[np] = P.scell[g];
+            Q.ox[np] = P.ox[g]; Q.oy[np] = P.oy[g]; Q.oz[np] = P.oz[g];
+            Q.Bm[np] = P.Bm[g]; Q.Cq[np] = P.Cq[g]; Q.Nq[np] = P.Nq[g]; Q.Pq[np] = P.Pq[g];
+            Q.Chl[np] = P.Chl[g]; Q.age[np] = P.age[g]; Q.gen[np] = P.gen[g];
+            Q.flags[np] = fl; Q.stat[np] = P.stat[g];
+            const int L = P.lslot[g];
+            Q.lslot[np] = L;
+            P.phys[base + L] = (int)(np - base);
+        }
+    }
+}
+
+// Storage order equal to the logical order over a slot range (after an upload): lslot and phys
+// are the identity, relative to the segment's first slot.
+__global__ void k32_identity_order(IndDev32 P, long long base, long long C) {
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < C; q += (long long)gridDim.x * blockDim.x) {
+        P.lslot[base + q] = (int)q;
+        P.phys[base + q] = (int)q;
+    }
 }
 
 }  // namespace p32

@@ -1007,6 +1007,23 @@ __global__ void k_halo_vel(DGrid g, double* __restrict__ c, int face_axis) {
 }
 
 // Active individuals of one species (calc_active_individuals, models.jl:157-164).
+// Index of the first non-finite value of a[0, n) (atomicMin into *first, which starts at ~0).
+__global__ void k_first_nonfinite(const double* __restrict__ a, long long n, unsigned long long* first) {
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        if (!isfinite(a[q])) atomicMin(first, (unsigned long long)q);
+}
+
+// First active slot of a species with a non-finite Float64 attribute.
+__global__ void k_first_nonfinite_inds(SpcDev s, long long C, unsigned long long* first) {
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < C; q += (long long)gridDim.x * blockDim.x) {
+        if (!(s.flags[q] & FL_AC)) continue;
+        const double v[11] = { s.x[q], s.y[q], s.z[q], s.Sz[q], s.Bm[q], s.Cq[q], s.Nq[q], s.Pq[q], s.Chl[q], s.gen[q], s.age[q] };
+        bool bad = false;
+        for (int k = 0; k < 11; ++k) bad |= !isfinite(v[k]);
+        if (bad) atomicMin(first, (unsigned long long)q);
+    }
+}
+
 __global__ void k_count_active(const uint8_t* __restrict__ flags, long long C, unsigned long long* out) {
     unsigned long long n = 0;
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < C; q += (long long)gridDim.x * blockDim.x)

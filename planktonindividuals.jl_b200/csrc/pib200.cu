@@ -838,6 +838,38 @@ pi_status pi_count_active(pi_model* m, int32_t sp, int64_t* n) {
     return PI_OK;
 }
 
+pi_status pi_check_finite(pi_model* m) {
+    if (m && m->b32) return fwd32(m, pi_batch_check_finite(m->b32, 0));
+    if (!m) return fail(m, PI_ERR_ARG, "pi_check_finite: NULL model");
+    unsigned long long* d = (unsigned long long*)m->sb.rank64;   // scratch between steps
+    const unsigned long long none = ~0ull;
+    const long long G = m->hg.G;
+    auto first = [&](auto launch, unsigned long long& out) -> pi_status {
+        CK(cudaMemcpyAsync(d, &none, sizeof none, cudaMemcpyHostToDevice, m->stream), "check finite");
+        launch();
+        CK(cudaGetLastError(), "check finite");
+        CK(cudaMemcpyAsync(&out, d, sizeof out, cudaMemcpyDeviceToHost, m->stream), "check finite");
+        CK(cudaStreamSynchronize(m->stream), "synchronize");
+        return PI_OK;
+    };
+    unsigned long long q = none;
+    pi_status e = first([&] { k_first_nonfinite<<<148 * 4, 256, 0, m->stream>>>(m->tr, PI_NTRACERS * G, d); }, q);
+    if (e) return e;
+    if (q != none) {
+        const long long n = (long long)q / G, c = (long long)q % G;
+        const long long i = c % m->hg.Gx + 1, j = (c / m->hg.Gx) % m->hg.Gy + 1, k = c / ((long long)m->hg.Gx * m->hg.Gy) + 1;
+        return fail(m, PI_ERR_NAN, "NaN or Inf in tracer " + std::string(tracer_name((int)n)) + " at (" + std::to_string(i) + ", " +
+                                       std::to_string(j) + ", " + std::to_string(k) + ")");
+    }
+    for (int s = 0; s < m->nsp; ++s) {
+        e = first([&] { k_first_nonfinite_inds<<<148 * 2, 256, 0, m->stream>>>(m->h_spc[s], m->C, d); }, q);
+        if (e) return e;
+        if (q != none)
+            return fail(m, PI_ERR_NAN, "NaN or Inf in an attribute of individual " + std::to_string(q + 1) + " of species " + std::to_string(s + 1));
+    }
+    return PI_OK;
+}
+
 pi_status pi_get_diag(pi_model* m, int32_t kind, int32_t sp, double* out) {
     if (m && m->b32) return fwd32(m, pi_batch_get_diag(m->b32, 0, kind, sp, out));
     if (!m || !out) return fail(m, PI_ERR_ARG, "pi_get_diag: bad argument");
