@@ -12,6 +12,11 @@
 //   k32_assign           k-th divider → k-th free slot per (member, species) segment
 //   k32_daughters        copy_daughter_individuals! + divide_to_half!
 //   k32_physiology       QuotaMode growth, consumption sums, decisions for the next step
+//   k32_tracer           the whole tracer update when no member has tracer diffusion or flux
+//                        boundary conditions: x, y and z sweeps of TMA-staged level tiles, sinking,
+//                        forcing, particle terms, apply_tendency! and the halo fill in one walk
+//                        down the levels
+//   (otherwise, and in the first step after a tracer upload, these three:)
 //   k32_xy               DST3FL x and y sweeps of every tracer on level tiles in shared memory
 //   k32_ztail            z sweep walking columns, then diffusion, sinking, forcing, BCs, particle
 //                        terms and apply_tendency!
@@ -25,6 +30,7 @@
 // assignment, tracer tile heights or z walk lengths (integer sums commute; every other value is computed by
 // exactly one thread from the same inputs), which lets the autotuner time real steps.
 #include <cub/device/device_scan.cuh>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -34,6 +40,7 @@
 #include <vector>
 
 #include "kernels_fp32.cuh"
+#include "kernels_tracer.cuh"
 #include "host_common.h"
 
 using namespace p32;
@@ -73,6 +80,8 @@ struct Tuning {
     int ty = 16;                              // rows of an x-y tracer tile (4, 8, 16 or 28)
     int lz = 32;                              // levels walked by a z thread (8, 16, 32 or 64)
     int wpb_par = 2;
+    int fused = 1;                            // k32_tracer when the batch allows it
+    int lz_fused = 32;                        // levels finished per k32_tracer block
 };
 
 }  // namespace
@@ -153,6 +162,11 @@ struct pi_batch {
     int nz_items = 0;
     float* tb = nullptr;
     float* rdzC = nullptr;
+    int4* trk_items = nullptr;
+    int ntrk_items = 0;
+    int tables_lzf = -1;
+    unsigned char* tmaps = nullptr;  // CUtensorMap per member, [tracer buffer][member], 128 bytes each
+    bool tracers_dirty = true;       // a tracer was uploaded since the last step
     Tuning tune;
     // graphs
     cudaGraphExec_t gexec[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [tracer buffer][individual buffer]
@@ -242,7 +256,53 @@ void free_graphs(pi_batch* b) {
 void free_tables(pi_batch* b) {
     for (void* p : b->table_allocs) cudaFree(p);
     b->table_allocs.clear();
-    b->tables_ty = b->tables_lz = -1;
+    b->tables_ty = b->tables_lz = b->tables_lzf = -1;
+}
+
+// k32_tracer applies when no member has tracer diffusion or flux boundary conditions (k32_ztail's
+// general path), every axis of every member has at least as many cells as halo points (one-pass
+// halo fill), and the tracers' halos are filled (not the first step after an upload).
+bool use_fused(const pi_batch* b) {
+    if (!b->tune.fused || !b->halo_direct || b->tracers_dirty) return false;
+    for (int m = 0; m < b->nm; ++m) {
+        if (b->mdh[m].any_bc) return false;
+        const pi_bgc_params& p = b->mh[m].bgc;
+        if ((float)p.kappa_h != 0.0f || (float)p.kappa_v != 0.0f) return false;
+    }
+    return true;
+}
+
+// TMA descriptors of every member's tracers (x, y, z, tracer) in each tracer buffer, for members
+// whose row pitch is a multiple of 16 bytes; the kernel copies the others with cp.async.
+pi_status build_tensor_maps(pi_batch* b) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return bfail(b, PI_ERR_CUDA, "cuTensorMapEncodeTiled not available");
+        encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    std::vector<CUtensorMap> maps(2 * (size_t)b->nm);
+    memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
+    for (int p = 0; p < 2; ++p)
+        for (int m = 0; m < b->nm; ++m) {
+            const MemberDev& d = b->mdh[m];
+            if (d.Gx % 4 != 0) continue;
+            const cuuint64_t dims[4] = { (cuuint64_t)d.Gx, (cuuint64_t)d.Gy, (cuuint64_t)d.Gz, (cuuint64_t)PI_NTRACERS };
+            const cuuint64_t strides[3] = { (cuuint64_t)d.Gx * 4, (cuuint64_t)d.Gx * d.Gy * 4, (cuuint64_t)b->Gtot * 4 };
+            const cuuint32_t box[4] = { TRK_W, TRK_R, 1, 1 };
+            const cuuint32_t es[4] = { 1, 1, 1, 1 };
+            CUresult r = encode(&maps[(size_t)p * b->nm + m], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+                                (void*)(b->trbuf[p] + d.cell_off), dims, strides, box, es,
+                                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS) return bfail(b, PI_ERR_CUDA, "cuTensorMapEncodeTiled failed for member " + std::to_string(m));
+        }
+    BK(cudaMemcpyAsync(b->tmaps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, b->stream), "upload tensor maps");
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    return PI_OK;
 }
 
 void free_series(MemberHost& h) {
@@ -322,10 +382,10 @@ pi_status check_member(const pi_member& mb, int nsp, std::string& msg) {
 
 // Work tables for the current tuning (tracer tile height, z walk length) on the device.
 pi_status build_tables(pi_batch* b) {
-    const int ty = b->tune.ty, lz = b->tune.lz;
-    if (b->tables_ty == ty && b->tables_lz == lz) return PI_OK;
+    const int ty = b->tune.ty, lz = b->tune.lz, lzf = b->tune.lz_fused;
+    if (b->tables_ty == ty && b->tables_lz == lz && b->tables_lzf == lzf) return PI_OK;
     free_tables(b);
-    std::vector<int4> xy, zz, icol;
+    std::vector<int4> xy, zz, icol, trk;
     for (int m = 0; m < b->nm; ++m) {
         const HostGrid& g = b->mh[m].g;
         for (int L = 1 + g.Hz; L <= g.Nz + g.Hz; ++L)
@@ -336,6 +396,9 @@ pi_status build_tables(pi_batch* b) {
                 for (int i0 = 1 + g.Hx; i0 <= g.Nx + g.Hx; i0 += 32) zz.push_back(make_int4(m, i0, j, k0));
         for (int j = 1; j <= g.Ny; ++j)
             for (int i0 = 1; i0 <= g.Nx; i0 += 32) icol.push_back(make_int4(m, i0, j, 0));
+        for (int k0 = 1 + g.Hz; k0 <= g.Nz + g.Hz; k0 += lzf)
+            for (int j0 = 1 + g.Hy; j0 <= g.Ny + g.Hy; j0 += TRK_TY)
+                for (int i0 = 1 + g.Hx; i0 <= g.Nx + g.Hx; i0 += TRK_TX) trk.push_back(make_int4(m, i0, j0, k0));
     }
     if (xy.size() >= (size_t)INT32_MAX || zz.size() >= (size_t)INT32_MAX) return bfail(b, PI_ERR_ARG, "work tables too large");
     auto up = [&](std::vector<int4>& v, int4** dst, int* n) -> pi_status {
@@ -351,9 +414,10 @@ pi_status build_tables(pi_batch* b) {
     if ((s = up(xy, &b->xy_items, &b->nxy_items))) return s;
     if ((s = up(zz, &b->z_items, &b->nz_items))) return s;
     if ((s = up(icol, &ic, &b->T.nicol))) return s;
+    if ((s = up(trk, &b->trk_items, &b->ntrk_items))) return s;
     b->T.icol = ic;
     BK(cudaStreamSynchronize(b->stream), "synchronize");
-    b->tables_ty = ty; b->tables_lz = lz;
+    b->tables_ty = ty; b->tables_lz = lz; b->tables_lzf = lzf;
     return PI_OK;
 }
 
@@ -375,6 +439,7 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
     const float fdT = (float)dT;
     float* tr = b->trbuf[cur];
     float* trn = b->trbuf[cur ^ 1];
+    const bool fused = use_fused(b);
     BK(cudaMemsetAsync(b->pop, 0, G * sizeof(int), s), "zero pop");
     if (b->pop_sp) BK(cudaMemsetAsync(b->pop_sp, 0, (size_t)b->nsp * G * sizeof(int), s), "zero pop");
     { BScope sc(b, "k32_bind");
@@ -423,6 +488,15 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
         a.T = b->T; a.lm = b->lm; a.dzF = b->dzF; a.dzC = b->dzC; a.rdzC = b->rdzC; a.bgc = b->bgc;
         a.bcs = b->bcs; a.st = b->st; a.F = b->F; a.Gtot = G; a.tr = tr; a.tb = b->tb; a.tr_next = trn;
         a.acc = b->acc; a.pop = b->pop; a.dT = fdT; a.err = b->errw;
+        if (fused) {
+            TrkArgs A;
+            A.a = a;
+            A.a.items = b->trk_items; A.a.nitems = b->ntrk_items;
+            A.maps = b->tmaps + (size_t)cur * b->nm * sizeof(CUtensorMap);
+            A.lz = b->tune.lz_fused;
+            BScope sc(b, "k32_tracer");
+            k32_tracer<<<dim3((unsigned)std::max(1, b->ntrk_items), 2), TRK_THREADS, tracer_smem_bytes(), s>>>(A);
+        } else {
         {
             a.items = b->xy_items; a.nitems = b->nxy_items;
             BScope sc(b, "k32_xy");
@@ -451,8 +525,11 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
             else if (b->tune.lz == 64) k32_ztail<64><<<grid, blk, zs, s>>>(a);
             else k32_ztail<16><<<grid, blk, zs, s>>>(a);
         }
+        }
     }
-    if (b->halo_direct) { BScope sc(b, "k32_halo");
+    if (fused) {
+        // k32_tracer wrote the halo cells with the interior
+    } else if (b->halo_direct) { BScope sc(b, "k32_halo");
       // about 16 blocks per SM over all members, enough for every member's halo cells
       const unsigned gx = std::max(1u, std::min<unsigned>(nblk(b->maxhalo, 256), std::max(1, b->nsm * 16 / b->nm)));
       k32_halo_direct<<<dim3(gx, b->nm), 256, 0, s>>>(b->md, G, trn, PI_NTRACERS, b->errw);
@@ -469,6 +546,8 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
 pi_status capture_graphs(pi_batch* b, double dT) {
     free_graphs(b);
     pi_status st = PI_OK;
+    const bool dirty = b->tracers_dirty;
+    b->tracers_dirty = false;           // the graphs serve the steps with filled tracer halos
     for (int q = 0; q < 2 && !st; ++q) {
         b->P = b->Pbuf[q];
         for (int p = 0; p < 2; ++p) {
@@ -485,6 +564,7 @@ pi_status capture_graphs(pi_batch* b, double dT) {
         }
     }
     b->P = b->Pbuf[b->pcur];
+    b->tracers_dirty = dirty;
     if (st) return st;
     b->graph_dT = dT;
     return PI_OK;
@@ -690,6 +770,7 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     cub::DeviceScan::ExclusiveSum(nullptr, cb, b->tile_cnt, b->tile_off, b->ntiles, b->stream);
     b->cub_bytes = cb;
     BA(b->cub_tmp, cb);
+    BA(b->tmaps, 2 * (size_t)nmembers * sizeof(CUtensorMap));
     cb = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, cb, b->sort_bins, b->sort_offs, b->nbins, b->stream);
     b->sort_tmp_bytes = cb;
@@ -788,6 +869,9 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     cudaFuncSetAttribute(k32_ztail<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ztail_smem(16));
     cudaFuncSetAttribute(k32_ztail<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ztail_smem(32));
     cudaFuncSetAttribute(k32_ztail<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ztail_smem(64));
+    cudaFuncSetAttribute(k32_tracer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tracer_smem_bytes());
+    st = build_tensor_maps(b);
+    if (st) return bail(st);
     b->T.md = b->md; b->T.nsp = nspecies; b->T.tiles = b->tiles; b->T.ntiles = b->ntiles; b->T.seg_tile0 = b->seg_tile0;
     st = build_tables(b);
     if (st) return bail(st);
@@ -957,6 +1041,7 @@ pi_status pi_batch_set_tracer(pi_batch* b, int32_t member, int32_t idx, const do
     k32_d2f<<<std::min<unsigned>(nblk(G, 256), 1024), 256, 0, b->stream>>>(b->trbuf[b->cur] + idx * b->Gtot + b->mdh[member].cell_off, b->stage, G);
     BK(cudaGetLastError(), "convert tracer");
     BK(cudaStreamSynchronize(b->stream), "synchronize");
+    b->tracers_dirty = true;
     return PI_OK;
 }
 
@@ -1098,6 +1183,7 @@ pi_status pi_batch_set_flux_bc(pi_batch* b, int32_t member, int32_t tracer, int3
     if (n && !values) return bfail(b, PI_ERR_ARG, "pi_set_flux_bc: NULL values");
     HostBC& hb = h.bcs[tracer][face];
     BK(cudaStreamSynchronize(b->stream), "synchronize");
+    free_graphs(b);                     // the tracer kernels depend on whether any member has a flux BC
     if (hb.v) { cudaFree(hb.v); hb.v = nullptr; }
     hb.kind = kind; hb.nt = nt;
     if (n) {
@@ -1249,12 +1335,19 @@ pi_status pi_batch_step(pi_batch* b, double dT, int64_t nsteps, int32_t sync) {
             if ((e = enqueue_step(b, dT, b->cur))) return e;
             b->cur ^= 1;
             b->since_sort += 1;
+            b->tracers_dirty = false;
         }
     } else {
         if (b->graph_dT != dT || !b->gexec[0][0]) { if ((e = capture_graphs(b, dT))) return e; }
         for (int64_t i = 0; i < nsteps; ++i) {
             if ((e = maybe_sort(b))) return e;
-            BK(cudaGraphLaunch(b->gexec[b->cur][b->pcur], b->stream), "graph launch");
+            if (b->tracers_dirty) {
+                // the step after a tracer upload maps the halo rows itself (two-kernel path)
+                if ((e = enqueue_step(b, dT, b->cur))) return e;
+                b->tracers_dirty = false;
+            } else {
+                BK(cudaGraphLaunch(b->gexec[b->cur][b->pcur], b->stream), "graph launch");
+            }
             b->cur ^= 1;
             b->since_sort += 1;
         }
@@ -1439,6 +1532,7 @@ pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t k, char* report, siz
             if ((e = enqueue_step(b, dT, b->cur))) return e;
             b->cur ^= 1;
             b->since_sort += 1;
+            b->tracers_dirty = false;
         }
         BK(cudaStreamSynchronize(b->stream), "synchronize");
         drain(b);
@@ -1458,6 +1552,7 @@ pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t k, char* report, siz
         { "k32_xy", &t.ty, {4, 8, 16, 28}, "x-y tracer tile rows", 0 },
         { "k32_ztail", &t.lz, {8, 16, 32, 64}, "z levels per thread", 0 },
         { "k32_par", &t.wpb_par, {1, 2, 4, 8}, "par warps/block", 32 },
+        { "k32_tracer", &t.lz_fused, {16, 32, 64}, "tracer levels per block", 0 },
     };
     // the largest block each kernel can be launched with (registers per thread)
     auto max_threads = [](const char* kernel) -> int {
@@ -1481,7 +1576,7 @@ pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t k, char* report, siz
             double ms = 0.0;
             pi_status e = kernel_ms(kb.kernel, ms);
             if (e) { b->profiling = was; return e; }
-            if (ms < best_ms) { best_ms = ms; best = v; }
+            if (ms > 0.0 && ms < best_ms) { best_ms = ms; best = v; }
         }
         *kb.field = best;
         char line[160];

@@ -360,3 +360,36 @@ def test_storage_order_changes_no_result(gpu_lib):
         for r in runs[1:]:
             assert compare_states(runs[0].member(m), r.member(m), wl.nsp) == [], f"member {m}"
             assert np.array_equal(runs[0].budget(m), r.budget(m))
+
+
+def test_fused_tracer_kernel_equals_two_kernel_path(gpu_lib):
+    """k32_tracer (x, y and z sweeps, sinking, forcing, particle terms and the halo fill in one walk
+    down the levels, tracers staged by TMA or, for row pitches that are not a multiple of 16 bytes,
+    by cp.async) against the two-kernel path (k32_xy + k32_ztail + halo fill), tolerance 0. The
+    second run re-uploads its tracers before every step, which makes that step take the two-kernel
+    path. Members: a 3D land mask, Bounded x/y, iron tracers with sinking, a grid whose rows are not
+    16-byte multiples, and a grid of two x tiles and two runs of levels."""
+    from test_gpu_parity_edge import OVER, landmask_3d, regrid, with_iron
+    from PlanktonIndividuals.grids import Bounded, RectilinearGrid
+    a = with_iron(daylight(W.config2(nx=13, nz=9, N_per_species=800, nsp=1, steps=12, nmodes=12, seed=21, phyt_over=OVER)))
+    b = landmask_3d(daylight(W.config2(nx=16, nz=10, N_per_species=900, nsp=1, steps=12, nmodes=12, seed=22, phyt_over=OVER)))
+    c = W.config1(n=20, N=900, steps=12, capacity=3000, phyt_over=OVER)
+    c = regrid(c, RectilinearGrid(size=(20, 12, 5), x=(0.0, 20e3), y=(0.0, 12e3), z=(0.0, -50.0),
+                                  FT=np.float64, topology=(Bounded, Bounded, Bounded)))
+    d = with_iron(daylight(W.config2(nx=36, nz=40, N_per_species=2000, nsp=1, steps=12, nmodes=12, seed=24, phyt_over=OVER)))
+    wls = [a, b, c, d]
+    assert a.grid.total_size[0] % 4 != 0 and d.grid.total_size[0] % 4 == 0
+    vels = [VelCache(wl) for wl in wls]
+    fused = PlanktonBatch(_members(wls), nspecies=1)
+    plain = PlanktonBatch(_members(wls), nspecies=1)
+    for batch in (fused, plain):
+        for m, wl in enumerate(wls):
+            batch.set_state(m, wl.individuals, wl.tracers)
+    for step in range(12):
+        for m in range(len(wls)):
+            for n in range(_abi.NTRACERS):
+                plain.set_tracer(m, n, plain.get_tracer(m, n))
+        _drive_batch(plain, wls, 1, vels)
+        _drive_batch(fused, wls, 1, vels)
+    for m, wl in enumerate(wls):
+        assert compare_states(plain.member(m), fused.member(m), wl.nsp) == [], f"member {m}"
