@@ -324,7 +324,8 @@ pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t steps_per_candidate,
 /* Storage order (no counterpart in the reference, which stores individuals in slot order): each
  * (member, species) segment is kept in an order grouped by cell, restored by a counting sort
  * before the first step after pi_batch_set_individuals and then every `steps` steps (default 32;
- * 0 = keep the current order). Slots keep their numbers at the boundary and in every result:
+ * 0 = keep the current order). Setting a positive interval starts a new cycle: the next step
+ * sorts first. Slots keep their numbers at the boundary and in every result:
  * draws are keyed by slot number and divisions are assigned in slot order, so the interval changes
  * only the speed, never a result. */
 pi_status pi_batch_set_sort_interval(pi_batch* b, int32_t steps);

@@ -721,7 +721,7 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
         cell += (g.G + 63) / 64 * 64;       // members start on 256-byte boundaries
         slot += (long long)nspecies * h.C;
         words += (long long)nspecies * d.wps;
-        bins += (long long)nspecies * ((long long)g.Nx * g.Ny * g.Nz + 1);
+        bins += (long long)nspecies * ((long long)g.Nx * g.Ny * g.Nz + (h.C + F32_TILE - 1) / F32_TILE);
         col += (long long)g.Nx * g.Ny;
         lev += g.Gz;
         b->maxG = std::max(b->maxG, g.G);
@@ -1478,6 +1478,7 @@ pi_status pi_batch_budget(pi_batch* b, int32_t member, double out[6]) {
 pi_status pi_batch_set_sort_interval(pi_batch* b, int32_t steps) {
     if (!b || steps < 0) return bfail(b, PI_ERR_ARG, "pi_batch_set_sort_interval: bad argument");
     b->sort_interval = steps;
+    b->need_sort = steps > 0;           // a new cycle starts with a sort before the next step
     return PI_OK;
 }
 

@@ -50,7 +50,7 @@ struct MemberDev {
     int bc_off;             // first of the member's 14*6 flux boundary conditions
     long long woff;         // first word of species 0 in the logical-slot bitmaps
     long long wps;          // bitmap words per species (32 per tile of F32_TILE slots)
-    long long bin_off;      // first cell-sort bin of species 0 (Nx*Ny*Nz + 1 bins per species)
+    long long bin_off;      // first cell-sort bin of species 0 (Nx*Ny*Nz + tiles bins per species)
     uint64_t seed;
     double fx_unit;         // mmol per fixed-point unit of the particle→grid mass sums
     double chl_unit;        // mg Chl per fixed-point unit of the Chl sums

@@ -1584,19 +1584,39 @@ __global__ void k32_budget_inds(MemberDev m, int nsp, const SpeciesDev32* __rest
 // storage order: counting sort of every segment by cell (a periodic pass between steps)
 // ------------------------------------------------------------------------------------------
 
-// sort bin of a stored slot: its interior cell in x-fastest order, or the last bin when inactive
-__device__ __forceinline__ long long sort_bin(const MemberDev& m, int s, uint8_t fl, int32_t code) {
+// Sort bin of a stored slot: its interior cell in x-fastest order; an inactive slot goes to one of
+// the bins after the cells, one per tile of F32_TILE stored positions (so inactive slots keep
+// their relative order and no bin collects a whole segment).
+__device__ __forceinline__ long long sort_bin(const MemberDev& m, int s, uint8_t fl, int32_t code, long long slot) {
     const long long V = (long long)m.Nx * m.Ny * m.Nz;
-    long long b = V;
+    const long long per = V + (m.wps >> 5);
+    long long b;
     if ((fl & F32_AC) && code >= 0) {
         int ci, cj, ck;
         unpack_int(m, code, ci, cj, ck);
         b = min(ci, m.Nx - 1) + (long long)m.Nx * (min(cj, m.Ny - 1) + (long long)m.Ny * min(ck, m.Nz - 1));
+    } else {
+        b = V + slot / F32_TILE;
     }
-    return m.bin_off + (long long)s * (V + 1) + b;
+    return m.bin_off + (long long)s * per + b;
 }
 
-// population of every bin (bins zeroed beforehand)
+// Warp-aggregated increment of bin counters: lanes with the same bin add once; each lane gets the
+// counter value before its own increment (the lanes of a bin take consecutive values). All 32
+// lanes call it; lanes with valid = false take no part.
+__device__ __forceinline__ unsigned long long bin_claim(unsigned long long* ctr, long long bin, bool valid) {
+    const int lane = threadIdx.x & 31;
+    const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+    const unsigned long long key = valid ? (unsigned long long)bin : ~0ull;
+    const unsigned peers = __match_any_sync(0xffffffffu, key) & vmask;
+    const int leader = valid ? __ffs(peers) - 1 : lane;
+    unsigned long long base = 0;
+    if (valid && lane == leader) base = atomicAdd(&ctr[bin], (unsigned long long)__popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return base + (unsigned long long)__popc(peers & ((1u << lane) - 1u));
+}
+
+// population of every bin (bins zeroed beforehand); blockDim.x divides F32_TILE
 __global__ void k32_sort_count(Tab32 T, IndDev32 P, unsigned long long* __restrict__ bins) {
     for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
         const int2 tl = T.tiles[t];
@@ -1604,9 +1624,12 @@ __global__ void k32_sort_count(Tab32 T, IndDev32 P, unsigned long long* __restri
         seg_of(T, tl.x, mi, s);
         const MemberDev& m = T.md[mi];
         const long long base = m.slot_off + (long long)s * m.C;
-        for (long long slot = (long long)tl.y + threadIdx.x; slot < min((long long)tl.y + F32_TILE, m.C); slot += blockDim.x) {
-            const long long g = base + slot;
-            atomicAdd(&bins[sort_bin(m, s, P.flags[g], P.cell[g])], 1ull);
+        for (int p = 0; p < F32_TILE / (int)blockDim.x; ++p) {
+            const long long slot = (long long)tl.y + p * blockDim.x + threadIdx.x;
+            const bool valid = slot < m.C;
+            const long long g = base + (valid ? slot : 0);
+            const long long bin = valid ? sort_bin(m, s, P.flags[g], P.cell[g], slot) : 0;
+            bin_claim(bins, bin, valid);
         }
     }
 }
@@ -1622,11 +1645,14 @@ __global__ void k32_sort_scatter(Tab32 T, IndDev32 P, IndDev32 Q, unsigned long 
         seg_of(T, tl.x, mi, s);
         const MemberDev& m = T.md[mi];
         const long long base = m.slot_off + (long long)s * m.C;
-        for (long long slot = (long long)tl.y + threadIdx.x; slot < min((long long)tl.y + F32_TILE, m.C); slot += blockDim.x) {
-            const long long g = base + slot;
+        for (int p = 0; p < F32_TILE / (int)blockDim.x; ++p) {
+            const long long slot = (long long)tl.y + p * blockDim.x + threadIdx.x;
+            const bool valid = slot < m.C;
+            const long long g = base + (valid ? slot : 0);
             const uint8_t fl = P.flags[g];
             const int32_t code = P.cell[g];
-            const long long np = (long long)atomicAdd(&offs[sort_bin(m, s, fl, code)], 1ull);
+            const long long np = (long long)bin_claim(offs, valid ? sort_bin(m, s, fl, code, slot) : 0, valid);
+            if (!valid) continue;
             Q.cell[np] = code; Q.scell[np] = P.scell[g];
             Q.ox[np] = P.ox[g]; Q.oy[np] = P.oy[g]; Q.oz[np] = P.oz[g];
             Q.Bm[np] = P.Bm[g]; Q.Cq[np] = P.Cq[g]; Q.Nq[np] = P.Nq[g]; Q.Pq[np] = P.Pq[g];
