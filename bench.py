@@ -52,6 +52,9 @@ sys.path.insert(0, os.path.join(ROOT, "planktonindividuals.jl_b200"))
 
 import numpy as np  # noqa: E402
 
+from PlanktonIndividuals.accuracy import (fp32_batch, fp32_vs_fp64, fp64_sim,  # noqa: E402,F401
+                                          interior_mass, mass_rel, series_arrays, snapshots)
+
 METRIC = "individual-steps/s (FP32 batched form; FP64 plain form reported beside)"
 SORT_INTERVAL = 32      # steps between the counting sorts that keep individuals grouped by cell
 UNIT = "ind-steps/s"
@@ -168,22 +171,6 @@ def algorithmic_bytes(name, members, n_active_total, n_slots_total):
     if name in ("k_sweep_y", "k_sweep_z"):
         return V * (14 * 8 * 3 + 8)
     return None
-
-
-_SNAPS = {}
-
-
-def snapshots(wl, nsnap):
-    """Velocity snapshots 0..nsnap-1 of a workload, computed once per run."""
-    have = _SNAPS.setdefault(id(wl), [])
-    while len(have) < nsnap:
-        have.append(wl.velocity(len(have)))
-    return have[:nsnap]
-
-
-def series_arrays(wl, nsnap):
-    snaps = snapshots(wl, nsnap)
-    return {c: np.stack([sn[q] for sn in snaps], axis=-1) for q, c in enumerate("uvw")}
 
 
 B_IND_FP32, B_CELL_FP32 = 106, 308      # algorithmic bytes per active individual / interior cell
@@ -480,47 +467,6 @@ def run_ours(args):
 # FP32 form against the FP64 form (the FP64 form equals the CPU oracle bit for bit)
 # ------------------------------------------------------------------------------------------
 
-def interior_mass(get, g):
-    from PlanktonIndividuals import _abi
-    vol = float(g.Δx) * float(g.Δy) * np.asarray(g.dzF)[g.Hz:g.Hz + g.Nz]
-    out = {}
-    for n, name in enumerate(_abi.tracer_names):
-        a = get(n)[g.Hx:g.Hx + g.Nx, g.Hy:g.Hy + g.Ny, g.Hz:g.Hz + g.Nz]
-        out[name] = float(np.sum(a * vol[None, None, :]))
-    return out
-
-
-def mass_rel(M32, M64):
-    return {k: (abs(M32[k] - M64[k]) / abs(M64[k]) if M64[k] else abs(M32[k])) for k in M64}
-
-
-def fp64_sim(lib, wl, steps):
-    import ctypes as ct
-    from PlanktonIndividuals import _abi
-    from PlanktonIndividuals._native import CModel
-    m = CModel(lib, "pi_", wl.grid, wl.bgc, wl.phyt, wl.nsp, wl.capacity, wl.seed, precision=_abi.PI_FP64)
-    m.set_state(wl.individuals, wl.tracers)
-    nsnap = wl.snapshots_needed(steps + 1)
-    vv = series_arrays(wl, nsnap)
-    u, v, w = (np.asfortranarray(vv[c]) for c in "uvw")
-    dp = lambda a: a.ctypes.data_as(ct.POINTER(ct.c_double))
-    sim = ct.c_void_p()
-    rc = lib.pi_sim_create(m.h, wl.dT, 1, dp(u), dp(v), dp(w), nsnap, wl.dT_vel, dp(wl.parf), wl.parf.shape[2],
-                           wl.dT_PAR, dp(wl.temp), wl.temp.shape[3], wl.dT_temp, ct.byref(sim))
-    assert rc == 0, m._errmsg(m.h)
-    return m, sim, (u, v, w)
-
-
-def fp32_batch(members, steps):
-    from PlanktonIndividuals.batch import Member, PlanktonBatch
-    b = PlanktonBatch([Member(w.grid, w.bgc, w.phyt, w.capacity, w.seed) for w in members], nspecies=members[0].nsp)
-    for m, wl in enumerate(members):
-        b.set_state(m, wl.individuals, wl.tracers)
-        b.set_series(m, vels=series_arrays(wl, wl.snapshots_needed(steps + 1)), ΔT_vel=wl.dT_vel, PARF=wl.parf,
-                     ΔT_PAR=wl.dT_PAR, temp=wl.temp, ΔT_temp=wl.dT_temp)
-    return b
-
-
 def run_accuracy(args):
     from PlanktonIndividuals import _lib, workloads as W
     lib = _lib.load()
@@ -549,43 +495,9 @@ def run_accuracy(args):
                 "mean_growth_factor": round(float(np.mean(np.array(c64) / np.array(n0))), 4),
                 "max_tracer_mass_rel_err": float(max(mass)), "seconds": round(time.time() - t0, 1)}
     wl = W.config3(seed=3) if args.workload == "config3" else W.config2(seed=2)
-    steps = args.acc_steps
-    m64, sim, keep = fp64_sim(lib, wl, steps)
-    b = fp32_batch([wl], steps)
-    hist = []
-    for s0 in range(0, steps, 100):
-        n = min(100, steps - s0)
-        for _ in range(n):
-            assert lib.pi_sim_update(sim, 0, 0) == 0, m64._errmsg(m64.h)
-        assert lib.pi_synchronize(m64.h) == 0, m64._errmsg(m64.h)
-        b.step(wl.dT, n)
-        hist.append({"step": s0 + n, "fp64": [m64.count_active(s) for s in range(wl.nsp)],
-                     "fp32": [b.count_active(0, s) for s in range(wl.nsp)]})
-    rel = mass_rel(interior_mass(lambda n: b.get_tracer(0, n), wl.grid), interior_mass(m64.get_tracer, wl.grid))
-    inds = {}
-    for s in range(wl.nsp):
-        A, B = m64.get_individuals(s), b.get_individuals(0, s)
-        both = A["ac"] & B["ac"]
-        inds[f"sp{s}"] = {
-            "ac_mismatch": int(np.sum(A["ac"] != B["ac"])),
-            "cell_mismatch": int(np.sum(both & ((A["xi"] != B["xi"]) | (A["yi"] != B["yi"]) | (A["zi"] != B["zi"])))),
-            "quota_rel_max": {k: float(np.max(np.abs(A[k][both] - B[k][both]) / np.abs(A[k][both])))
-                              for k in ("Bm", "Cq", "Nq", "Pq", "Chl")},
-            "z_abs_max": float(np.max(np.abs(A["z"][both] - B["z"][both])))}
-        # population totals: meaningful also after a decision flip has moved daughters to other slots
-        tot = {}
-        for k in ("Bm", "Cq", "Nq", "Pq", "Chl"):
-            t64, t32 = float(np.sum(A[k][A["ac"]])), float(np.sum(B[k][B["ac"]]))
-            tot[k] = abs(t32 - t64) / abs(t64) if t64 else abs(t32)
-        n64, n32 = int(A["ac"].sum()), int(B["ac"].sum())
-        inds[f"sp{s}"]["count_rel_diff"] = abs(n32 - n64) / n64
-        inds[f"sp{s}"]["total_rel_diff"] = tot
-    out = {"accuracy": args.workload, "steps": steps, "counts_equal_at_every_check": all(h["fp64"] == h["fp32"] for h in hist),
-           "counts": hist, "tracer_mass_rel_err": rel, "max_tracer_mass_rel_err": max(rel.values()),
-           "individuals": inds, "budget_fp32": b.budget(0), "seconds": round(time.time() - t0, 1)}
-    b.close()
-    lib.pi_sim_destroy(sim)
-    m64.close()
+    out = {"accuracy": args.workload}
+    out.update(fp32_vs_fp64(lib, wl, args.acc_steps))
+    out["seconds"] = round(time.time() - t0, 1)
     return out
 
 

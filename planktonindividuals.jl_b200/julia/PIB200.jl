@@ -1,0 +1,268 @@
+# PIB200 — Julia bindings of libpib200 (the C ABI of include/pib200.h) for PlanktonIndividuals.jl.
+#
+# Untested here: this image has no Julia. The module mirrors include/pib200.h one to one (struct
+# layouts, argument order, status codes); the Python package PlanktonIndividuals in this
+# repository binds the same symbols through ctypes and is what the tests exercise.
+#
+# A GPU architecture of PlanktonIndividuals.jl forwards its model calls here:
+#   PlanktonModel(arch, grid; FT, ...)  -> create(grid, bgc, phyt, Nsp, maxN; FT, seed) + set_individuals!/set_tracer!
+#   TimeStep!(model, ΔT, diags)         -> time_step!(m, ΔT)
+#   PlanktonSimulation(model; ...)      -> simulation(m, ΔT, iterations; PARF, temp, vels, ...)
+#   update!(sim; time_offset)           -> update!(s; time_offset)
+#   model.individuals / model.tracers / diags -> get_individuals, get_tracer, get_diag
+module PIB200
+
+export PiGrid, PiBgc, PiQuota, PiIndividuals, PiMember, PIError
+export create, destroy, set_individuals!, get_individuals, set_tracer!, get_tracer
+export set_velocity!, set_PARF!, set_temp!, set_flux_bc!, time_step!, get_time, set_time!
+export count_active, get_diag, reset_diags!, check_finite, simulation, update!, synchronize
+export batch_create, batch_step!, batch_set_sort_interval!
+
+const lib = get(ENV, "LIBPIB200", joinpath(@__DIR__, "..", "PlanktonIndividuals", "libpib200.so"))
+
+# status codes and constants (include/pib200.h)
+const PI_OK = 0
+const PI_ERR_CAPACITY = 4
+const PI_FP64 = Int32(0)
+const PI_FP32 = Int32(1)
+const PI_PERIODIC = Int32(0)
+const PI_BOUNDED = Int32(1)
+const TRACERS = (:DIC, :NH4, :NO3, :PO4, :DFe, :DOC, :DON, :DOP, :PFe_inorg, :POC, :PON, :POP, :PFe_bio, :Dust)
+const DIAG_KINDS = Dict(:PAR => Int32(0), :num => Int32(1), :graz => Int32(2), :mort => Int32(3), :dvid => Int32(4))
+
+struct PiGrid
+    Nx::Int32; Ny::Int32; Nz::Int32
+    Hx::Int32; Hy::Int32; Hz::Int32
+    topo::NTuple{3,Int32}
+    dx::Float64; dy::Float64
+    dzF::Ptr{Float64}; dzC::Ptr{Float64}; landmask::Ptr{UInt8}
+end
+
+# bgc_params_default (src/Parameters/param_default.jl:44-71), field order of pi_bgc_params
+const BGC_KEYS = ("kw", "kc", "kDOC", "Nit", "kDON", "kDOP", "kPOC", "kPON", "kPOP", "κh", "κv", "κhP",
+                  "κvP", "shared_graz", "w_sink_org", "w_sink_inorg", "lambda_POC", "lambda_min",
+                  "kdiss", "lambda_dust", "lambda_Fe", "ligand", "DFeFrac")
+struct PiBgc
+    v::NTuple{23,Float64}
+end
+PiBgc(p::AbstractDict) = PiBgc(ntuple(i -> Float64(p[BGC_KEYS[i]]), 23))
+
+# QuotaMode param_names (src/Individuals/Plankton/QuotaMode/plankton_generation.jl:16-20)
+const QUOTA_KEYS = ("Nsuper", "Cquota", "mean", "var", "Chl2Cint", "α", "Φ", "Topt", "Tmax", "Ea",
+                    "PCmax", "VDOCmax", "VNO3max", "VNH4max", "VPO4max", "KsatDOC", "KsatNH4",
+                    "KsatNO3", "KsatPO4", "Cqmax", "Nqmax", "Pqmax", "Chl2N", "R_NC", "R_PC", "k_mtb",
+                    "respir", "grz_P", "dvid_type", "dvid_P", "dvid_reg", "dvid_reg2", "mort_P",
+                    "mort_reg", "grazFracC", "grazFracN", "grazFracP", "mortFracC", "mortFracN",
+                    "mortFracP")
+struct PiQuota
+    v::NTuple{40,Float64}
+end
+PiQuota(p::AbstractDict, sp::Integer) = PiQuota(ntuple(i -> Float64(p[QUOTA_KEYS[i]][sp]), 40))
+
+struct PiIndividuals
+    x::Ptr{Float64}; y::Ptr{Float64}; z::Ptr{Float64}
+    xi::Ptr{Int64}; yi::Ptr{Int64}; zi::Ptr{Int64}
+    Sz::Ptr{Float64}; Bm::Ptr{Float64}; Cq::Ptr{Float64}; Nq::Ptr{Float64}; Pq::Ptr{Float64}
+    Chl::Ptr{Float64}; gen::Ptr{Float64}; age::Ptr{Float64}
+    ac::Ptr{UInt8}
+    graz::Ptr{Float64}; mort::Ptr{Float64}; dvid::Ptr{Float64}
+end
+
+struct PiMember
+    grid::Ptr{PiGrid}; bgc::Ptr{PiBgc}; species::Ptr{PiQuota}
+    capacity::Int64; seed::UInt64
+end
+
+struct PIError <: Exception
+    code::Int32
+    msg::String
+end
+Base.showerror(io::IO, e::PIError) = print(io, e.msg)
+
+function lasterror(h::Ptr{Cvoid}, batch::Bool)
+    buf = Vector{UInt8}(undef, 1024)
+    if batch
+        ccall((:pi_batch_last_error, lib), Int32, (Ptr{Cvoid}, Ptr{UInt8}, Csize_t), h, buf, length(buf))
+    else
+        ccall((:pi_last_error, lib), Int32, (Ptr{Cvoid}, Ptr{UInt8}, Csize_t), h, buf, length(buf))
+    end
+    unsafe_string(pointer(buf))
+end
+
+# Validation errors carry the reference's ArgumentError texts; other failures are a PIError.
+function check(st::Integer, h::Ptr{Cvoid}; batch::Bool = false)
+    st == PI_OK && return nothing
+    msg = lasterror(h, batch)
+    st in (1, 2, 3, PI_ERR_CAPACITY) && throw(ArgumentError(msg))
+    throw(PIError(Int32(st), msg))
+end
+
+# ---- model -------------------------------------------------------------------------------------
+mutable struct Model
+    h::Ptr{Cvoid}
+    G::NTuple{3,Int}
+    Nsp::Int
+    capacity::Int
+end
+
+topo_code(T) = occursin("Periodic", string(T)) ? PI_PERIODIC : PI_BOUNDED
+
+function pigrid(g, dzF::Vector{Float64}, dzC::Vector{Float64}, lm::Vector{UInt8})
+    PiGrid(g.Nx, g.Ny, g.Nz, g.Hx, g.Hy, g.Hz,
+           (topo_code(g.topology[1]), topo_code(g.topology[2]), topo_code(g.topology[3])),
+           Float64(g.Δx), Float64(g.Δy), pointer(dzF), pointer(dzC), pointer(lm))
+end
+
+"""PlanktonModel(GPU(), grid; FT, max_individuals, bgc_params, phyto) on the B200: allocates the
+model on the current CUDA device (`FT = Float64` → the plain form, `Float32` → the FP32 form)."""
+function create(g, bgc::AbstractDict, phyt::AbstractDict, Nsp::Integer, maxN::Integer; FT = Float64, seed::Integer = 0)
+    dzF, dzC = Float64.(collect(g.dzF)), Float64.(collect(g.dzC))
+    lm = UInt8.(vec(collect(g.landmask)))
+    pg = Ref(pigrid(g, dzF, dzC, lm))
+    pb = Ref(PiBgc(bgc))
+    ps = [PiQuota(phyt, s) for s in 1:Nsp]
+    out = Ref{Ptr{Cvoid}}(C_NULL)
+    st = GC.@preserve dzF dzC lm ccall((:pi_create, lib), Int32,
+        (Ref{PiGrid}, Ref{PiBgc}, Ptr{PiQuota}, Int32, Int64, Int32, UInt64, Ref{Ptr{Cvoid}}),
+        pg, pb, ps, Nsp, maxN, FT === Float32 ? PI_FP32 : PI_FP64, seed, out)
+    check(st, C_NULL)
+    m = Model(out[], (g.Nx + 2g.Hx, g.Ny + 2g.Hy, g.Nz + 2g.Hz), Nsp, maxN)
+    finalizer(destroy, m)
+    m
+end
+
+function destroy(m::Model)
+    m.h != C_NULL && ccall((:pi_destroy, lib), Int32, (Ptr{Cvoid},), m.h)
+    m.h = C_NULL
+    nothing
+end
+
+"""Upload species `sp` (1-based) from a StructArray-like table with the QuotaMode columns."""
+function set_individuals!(m::Model, sp::Integer, d)
+    cols = (Float64.(d.x), Float64.(d.y), Float64.(d.z), Int64.(d.xi), Int64.(d.yi), Int64.(d.zi),
+            Float64.(d.Sz), Float64.(d.Bm), Float64.(d.Cq), Float64.(d.Nq), Float64.(d.Pq),
+            Float64.(d.Chl), Float64.(d.gen), Float64.(d.age), UInt8.(d.ac),
+            Float64.(d.graz), Float64.(d.mort), Float64.(d.dvid))
+    GC.@preserve cols begin
+        pi = Ref(PiIndividuals(map(pointer, cols)...))
+        check(ccall((:pi_set_individuals, lib), Int32, (Ptr{Cvoid}, Int32, Ref{PiIndividuals}), m.h, sp - 1, pi), m.h)
+    end
+end
+
+"""Download species `sp` (1-based) as a NamedTuple of the QuotaMode columns."""
+function get_individuals(m::Model, sp::Integer)
+    C = m.capacity
+    f = ntuple(_ -> zeros(Float64, C), 3); i = ntuple(_ -> zeros(Int64, C), 3)
+    q = ntuple(_ -> zeros(Float64, C), 8); ac = zeros(UInt8, C); dec = ntuple(_ -> zeros(Float64, C), 3)
+    GC.@preserve f i q ac dec begin
+        pi = Ref(PiIndividuals(pointer(f[1]), pointer(f[2]), pointer(f[3]), pointer(i[1]), pointer(i[2]), pointer(i[3]),
+                               map(pointer, q)..., pointer(ac), map(pointer, dec)...))
+        check(ccall((:pi_get_individuals, lib), Int32, (Ptr{Cvoid}, Int32, Ref{PiIndividuals}), m.h, sp - 1, pi), m.h)
+    end
+    (x = f[1], y = f[2], z = f[3], xi = i[1], yi = i[2], zi = i[3], Sz = q[1], Bm = q[2], Cq = q[3], Nq = q[4],
+     Pq = q[5], Chl = q[6], gen = q[7], age = q[8], ac = ac .== 1, graz = dec[1], mort = dec[2], dvid = dec[3])
+end
+
+tracer_index(name::Symbol) = Int32(findfirst(==(name), TRACERS) - 1)
+
+set_tracer!(m::Model, name::Symbol, a::Array{Float64,3}) =
+    check(ccall((:pi_set_tracer, lib), Int32, (Ptr{Cvoid}, Int32, Ptr{Float64}), m.h, tracer_index(name), a), m.h)
+
+function get_tracer(m::Model, name::Symbol)
+    a = zeros(Float64, m.G)
+    check(ccall((:pi_get_tracer, lib), Int32, (Ptr{Cvoid}, Int32, Ptr{Float64}), m.h, tracer_index(name), a), m.h)
+    a
+end
+
+# vel_copy!(vel₁, u, v, w, grid), copyto!(PARF), copy_interior!(temp) (Simulation/update.jl:18-26)
+set_velocity!(m::Model, u, v, w) =
+    check(ccall((:pi_set_velocity, lib), Int32, (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+                m.h, Float64.(u), Float64.(v), Float64.(w)), m.h)
+set_PARF!(m::Model, parf) = check(ccall((:pi_set_PARF, lib), Int32, (Ptr{Cvoid}, Ptr{Float64}), m.h, Float64.(parf)), m.h)
+set_temp!(m::Model, temp) = check(ccall((:pi_set_temp, lib), Int32, (Ptr{Cvoid}, Ptr{Float64}), m.h, Float64.(temp)), m.h)
+
+# set_bc!(model; tracer, pos, bc_value) (HaloRegions/boundary_conditions.jl:21-31)
+const FACES = Dict(:west => 0, :east => 1, :south => 2, :north => 3, :bottom => 4, :top => 5)
+function set_flux_bc!(m::Model, tracer::Symbol, pos::Symbol, value)
+    kind, vals, nt = value isa Number ? (1, [Float64(value)], 0) :
+                     ndims(value) == 2 ? (2, vec(Float64.(value)), 0) : (3, vec(Float64.(value)), size(value, 3))
+    check(ccall((:pi_set_flux_bc, lib), Int32, (Ptr{Cvoid}, Int32, Int32, Int32, Ptr{Float64}, Int64),
+                m.h, tracer_index(tracer), FACES[pos], kind, vals, nt), m.h)
+end
+
+# TimeStep!(model, ΔT, diags) (src/Model/time_step.jl:12-180)
+time_step!(m::Model, ΔT) = check(ccall((:pi_time_step, lib), Int32, (Ptr{Cvoid}, Float64), m.h, ΔT), m.h)
+
+function get_time(m::Model)
+    it = Ref{Int64}(0); t = Ref{Float64}(0)
+    check(ccall((:pi_get_time, lib), Int32, (Ptr{Cvoid}, Ref{Int64}, Ref{Float64}), m.h, it, t), m.h)
+    (iteration = it[], t = t[])
+end
+set_time!(m::Model, it, t) = check(ccall((:pi_set_time, lib), Int32, (Ptr{Cvoid}, Int64, Float64), m.h, it, t), m.h)
+
+function count_active(m::Model, sp::Integer)
+    n = Ref{Int64}(0)
+    check(ccall((:pi_count_active, lib), Int32, (Ptr{Cvoid}, Int32, Ref{Int64}), m.h, sp - 1, n), m.h)
+    n[]
+end
+
+"""diags.tracer.PAR (kind = :PAR) or diags.phytos[sp].num/graz/mort/dvid, halo-padded."""
+function get_diag(m::Model, kind::Symbol, sp::Integer = 1)
+    a = zeros(Float64, m.G)
+    check(ccall((:pi_get_diag, lib), Int32, (Ptr{Cvoid}, Int32, Int32, Ptr{Float64}), m.h, DIAG_KINDS[kind], sp - 1, a), m.h)
+    a
+end
+reset_diags!(m::Model) = check(ccall((:pi_reset_diags, lib), Int32, (Ptr{Cvoid},), m.h), m.h)
+check_finite(m::Model) = check(ccall((:pi_check_finite, lib), Int32, (Ptr{Cvoid},), m.h), m.h)
+synchronize(m::Model) = check(ccall((:pi_synchronize, lib), Int32, (Ptr{Cvoid},), m.h), m.h)
+
+# ---- simulation ---------------------------------------------------------------------------------
+mutable struct Simulation
+    h::Ptr{Cvoid}
+    model::Model
+end
+
+"""PlanktonSimulation(model; ΔT, iterations, PARF, temp, vels, ΔT_vel, ΔT_PAR, ΔT_temp): the
+forcing series are copied to device memory once; vels = (u = …, v = …, w = …) with a 4th
+(snapshot) dimension, or nothing."""
+function simulation(m::Model, ΔT, iterations; PARF, temp, vels = nothing, ΔT_vel = ΔT, ΔT_PAR = 3600.0, ΔT_temp = 3600.0)
+    parf, tp = Float64.(PARF), Float64.(temp)
+    has = vels !== nothing
+    u, v, w = has ? (Float64.(vels.u), Float64.(vels.v), Float64.(vels.w)) : (Float64[], Float64[], Float64[])
+    nvel = has ? size(u, 4) : 0
+    out = Ref{Ptr{Cvoid}}(C_NULL)
+    st = GC.@preserve parf tp u v w ccall((:pi_sim_create, lib), Int32,
+        (Ptr{Cvoid}, Float64, Int64, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Int64, Float64,
+         Ptr{Float64}, Int64, Float64, Ptr{Float64}, Int64, Float64, Ref{Ptr{Cvoid}}),
+        m.h, ΔT, iterations, has ? pointer(u) : C_NULL, has ? pointer(v) : C_NULL, has ? pointer(w) : C_NULL,
+        nvel, ΔT_vel, parf, size(parf, 3), ΔT_PAR, tp, size(tp, 4), ΔT_temp, out)
+    check(st, m.h)
+    s = Simulation(out[], m)
+    finalizer(s) do s
+        s.h != C_NULL && ccall((:pi_sim_destroy, lib), Int32, (Ptr{Cvoid},), s.h)
+        s.h = C_NULL
+    end
+    s
+end
+
+"""update!(sim; time_offset = (vels = false, PARF = false, temp = false)) (src/Simulation/update.jl:11-48)."""
+function update!(s::Simulation; time_offset = (vels = false, PARF = false, temp = false), sync::Bool = true)
+    mask = Int32(time_offset.vels) | (Int32(time_offset.PARF) << 1) | (Int32(time_offset.temp) << 2)
+    check(ccall((:pi_sim_update, lib), Int32, (Ptr{Cvoid}, Int32, Int32), s.h, mask, sync), s.model.h)
+end
+
+# ---- batched FP32 form (ensembles) ----------------------------------------------------------------
+"""One batch of independent FP32 models advanced together; `members` are PiMember records whose
+pointers the caller keeps alive for the call."""
+function batch_create(members::Vector{PiMember}, Nsp::Integer)
+    out = Ref{Ptr{Cvoid}}(C_NULL)
+    st = ccall((:pi_batch_create, lib), Int32, (Ptr{PiMember}, Int32, Int32, Ref{Ptr{Cvoid}}), members, length(members), Nsp, out)
+    check(st, C_NULL; batch = true)
+    out[]
+end
+batch_step!(b::Ptr{Cvoid}, ΔT, n) =
+    check(ccall((:pi_batch_step, lib), Int32, (Ptr{Cvoid}, Float64, Int64, Int32), b, ΔT, n, 1), b; batch = true)
+batch_set_sort_interval!(b::Ptr{Cvoid}, n) =
+    check(ccall((:pi_batch_set_sort_interval, lib), Int32, (Ptr{Cvoid}, Int32), b, n), b; batch = true)
+
+end # module

@@ -96,3 +96,11 @@ def test_batch_create_rejects_bad_members_before_touching_a_device():
     assert rc == _abi.PI_ERR_ARG and "too large" in msg
     rc, _ = _batch_create_status({})
     assert rc in (_abi.PI_OK, _abi.PI_ERR_CUDA)      # a valid member: created, or no device here
+
+
+def test_julia_binding_calls_only_declared_symbols():
+    """The Julia module (untested here: no Julia) binds symbols that include/pib200.h declares."""
+    src = open(os.path.join(ROOT, "planktonindividuals.jl_b200", "julia", "PIB200.jl")).read()
+    called = set(re.findall(r"ccall\(\(:(pi_\w+), lib\)", src))
+    assert len(called) >= 20
+    assert called <= set(declared_symbols())
