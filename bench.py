@@ -68,7 +68,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "config5"])
     ap.add_argument("--fp64-steps", type=int, default=50)
-    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--profile-steps", type=int, default=5)
     ap.add_argument("--tune-steps", type=int, default=2)
     ap.add_argument("--cpu-steps", type=int, default=2)
@@ -299,21 +299,28 @@ def run_fp64(wl, args, lib):
             "ms_per_step": round(ms / K, 4), "cell_steps_per_s": round(K * V / (ms / 1e3), 1), "dtype": "f64"}
 
 
-def run_e2e(wl, args, lib, precision):
-    """The same metric through the C-ABI with host buffers (pinned), one step per call."""
+def run_e2e(wl, args, lib, precision, inputs="f32"):
+    """The same metric through the C-ABI with host buffers (pinned), one step per call: every step
+    uploads its forcing (vel_copy!, copyto!, copy_interior!) from host arrays with the pi_set_*
+    calls (Float32 arrays through the _f32 setters, the reference's arrays when FT = Float32, or
+    Float64 arrays), queues TimeStep! (pi_time_step_async) and reads its population counts back
+    into host memory (pi_count_active_async). The setters return once their host arrays are copied;
+    the copies overlap the step queued before them."""
+    import ctypes as ct
     import torch
     from PlanktonIndividuals._native import CModel
-    g = wl.grid
     m = CModel(lib, "pi_", wl.grid, wl.bgc, wl.phyt, wl.nsp, wl.capacity, wl.seed, precision=precision)
     m.set_state(wl.individuals, wl.tracers)
     nsnap = wl.snapshots_needed(args.e2e_steps + 2)
     snaps = snapshots(wl, nsnap)
-    import ctypes as ct
     sp = ct.c_void_p()
     m.lib.pi_get_stream(m.h, ct.byref(sp))
     stream = torch.cuda.ExternalStream(sp.value)
+    tdt = torch.float32 if inputs == "f32" else torch.float64
+
     def pin(a):
-        out = torch.empty(int(a.size), dtype=torch.float64, pin_memory=True).numpy().reshape(a.shape, order="F")
+        t = torch.empty(int(a.size), dtype=tdt, pin_memory=True)
+        out = t.numpy().reshape(a.shape, order="F")
         out[...] = a
         return out
 
@@ -332,37 +339,49 @@ def run_e2e(wl, args, lib, precision):
         if tt not in tmp_p:
             tmp_p[tt] = pin(np.asfortranarray(wl.temp[:, :, :, tt]))
     h2d = sum(x.nbytes for x in vel_p[0]) + par_p[0].nbytes + tmp_p[0].nbytes
+    counts = torch.zeros((args.e2e_steps + 1) * wl.nsp, dtype=torch.int64, pin_memory=True)
+    cbase = counts.data_ptr()
+    ptr = lambda a: ct.c_void_p(a.ctypes.data)
+    sfx = "_f32" if inputs == "f32" else ""
+    set_vel, set_par, set_tmp = (getattr(m.lib, f"pi_set_{k}{sfx}") for k in ("velocity", "PARF", "temp"))
 
-    def one_step():
-        it, tnow = m.get_time()
+    def check(rc, what):
+        if rc != 0:
+            raise RuntimeError(f"{what}: {m._errmsg(m.h)}")
+
+    def one_step(i):
+        tnow = i * wl.dT
         tv = min(int(np.floor(tnow / wl.dT_vel)), nsnap - 1)
         tp = int(np.floor(tnow / wl.dT_PAR)); tt = int(np.floor(tnow / wl.dT_temp))
-        m.set_velocity(*vel_p[tv])
-        m.set_PARF(par_p[tp])
-        m.set_temp(tmp_p[tt])
-        m.time_step(wl.dT)
-        return sum(m.count_active(s) for s in range(wl.nsp))
+        check(set_vel(m.h, *(ptr(x) for x in vel_p[tv])), "set velocity")
+        check(set_par(m.h, ptr(par_p[tp])), "set PARF")
+        check(set_tmp(m.h, ptr(tmp_p[tt])), "set temp")
+        check(m.lib.pi_time_step_async(m.h, ct.c_double(wl.dT)), "time step")
+        for s in range(wl.nsp):
+            check(m.lib.pi_count_active_async(m.h, s, ct.c_void_p(cbase + 8 * (i * wl.nsp + s))), "count")
 
-    one_step()          # untimed: first launch of the step (graph capture of the FP32 form)
+    one_step(0)          # untimed: first launch of the step (graph capture of the FP32 form)
+    check(m.lib.pi_synchronize(m.h), "synchronize")
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ee0.record(stream)
-    ne = 0
-    for _ in range(args.e2e_steps):
-        ne += one_step()
+    for i in range(1, args.e2e_steps + 1):
+        one_step(i)
     ee1.record(stream)
     ee1.synchronize()
     wall = time.perf_counter() - t0
+    check(m.lib.pi_synchronize(m.h), "synchronize")
     ev_ms = ee0.elapsed_time(ee1)
+    ne = int(counts[wl.nsp:].sum())
     m.close()
     return {"value": round(ne / (ev_ms / 1e3), 1), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": 8 * wl.nsp, "steps": args.e2e_steps,
             "ms_per_step": round(ev_ms / args.e2e_steps, 3), "wall_ms_per_step": round(1e3 * wall / args.e2e_steps, 3),
-            "form": "fp32" if precision else "fp64",
-            "note": "each step uploads its forcing (vel_copy!, copyto!, copy_interior!) from host buffers "
-                    "staged in pinned memory before the timed region, runs pi_time_step and reads the "
-                    "population counts; CUDA events on the model stream bracket the whole loop"}
+            "form": "fp32" if precision else "fp64", "inputs": "float32" if inputs == "f32" else "float64",
+            "note": "each step uploads its forcing from pinned host arrays through pi_set_velocity/PARF/temp"
+                    f"{sfx}, queues pi_time_step_async and reads the population counts with "
+                    "pi_count_active_async; CUDA events on the model stream bracket the loop"}
 
 
 def run_ours(args):
@@ -426,7 +445,9 @@ def run_ours(args):
         if args.fp64_steps > 0:
             fp64 = run_fp64(members[0], args, lib)
         if args.e2e_steps > 0:
-            e2e = run_e2e(members[0], args, lib, _abi.PI_FP32)
+            e2e = run_e2e(members[0], args, lib, _abi.PI_FP32, "f32")
+            e2e["float64_inputs"] = {k: v for k, v in run_e2e(members[0], args, lib, _abi.PI_FP32, "f64").items()
+                                     if k in ("value", "ms_per_step", "wall_ms_per_step", "h2d_bytes_per_step")}
     out = None
     if rank == 0:
         cpu = None

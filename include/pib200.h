@@ -159,6 +159,25 @@ pi_status pi_set_flux_bc(pi_model* m, int32_t tracer, int32_t face, int32_t kind
  * reference's message when divisions exceed the free slots. */
 pi_status pi_time_step(pi_model* m, double dT);
 
+/* The same entry points for a PI_FP32 model fed from Float32 host arrays (the reference's forcing
+ * arrays when FT = Float32, its default); same shapes as the Float64 versions. Like those, each
+ * call has copied the host arrays when it returns; the copies run on a stream of their own and
+ * overlap the steps already queued, and the conversion into the model's fields is queued behind
+ * them. PI_ERR_ARG for a PI_FP64 model. */
+pi_status pi_set_velocity_f32(pi_model* m, const float* u, const float* v, const float* w);
+pi_status pi_set_PARF_f32(pi_model* m, const float* parf);
+pi_status pi_set_temp_f32(pi_model* m, const float* temp);
+
+/* TimeStep! queued on the model's stream without waiting for it (the reference's GPU kernels are
+ * asynchronous too): the call returns once the step is queued; pi_synchronize waits and reports a
+ * capacity overflow or out-of-domain index raised by the queued steps. */
+pi_status pi_time_step_async(pi_model* m, double dT);
+
+/* pi_count_active queued on the model's stream: *n is written when the stream reaches the count
+ * (after the steps queued before it). *n should be page-locked host memory (cudaHostAlloc) for the
+ * call not to wait for the stream. */
+pi_status pi_count_active_async(pi_model* m, int32_t sp, int64_t* n);
+
 /* model.iteration and model.t. */
 pi_status pi_get_time(pi_model* m, int64_t* iteration, double* t);
 pi_status pi_set_time(pi_model* m, int64_t iteration, double t);
@@ -268,7 +287,11 @@ pi_status pi_batch_get_individuals(pi_batch* b, int32_t member, int32_t sp, pi_i
 /* As pi_set_tracer / pi_get_tracer for one member (halo-padded, Float64 at the boundary). */
 pi_status pi_batch_set_tracer(pi_batch* b, int32_t member, int32_t idx, const double* data);
 pi_status pi_batch_get_tracer(pi_batch* b, int32_t member, int32_t idx, double* out);
-/* As pi_set_velocity / pi_set_velocity0 / pi_set_PARF / pi_set_temp / pi_set_flux_bc. */
+/* As pi_set_velocity / pi_set_velocity0 / pi_set_PARF / pi_set_temp / pi_set_flux_bc, and the
+ * Float32-input setters. */
+pi_status pi_batch_set_velocity_f32(pi_batch* b, int32_t member, const float* u, const float* v, const float* w);
+pi_status pi_batch_set_PARF_f32(pi_batch* b, int32_t member, const float* parf);
+pi_status pi_batch_set_temp_f32(pi_batch* b, int32_t member, const float* temp);
 pi_status pi_batch_set_velocity(pi_batch* b, int32_t member, const double* u, const double* v, const double* w);
 pi_status pi_batch_set_velocity0(pi_batch* b, int32_t member, const double* u, const double* v, const double* w);
 pi_status pi_batch_set_PARF(pi_batch* b, int32_t member, const double* parf);
@@ -301,8 +324,10 @@ pi_status pi_batch_synchronize(pi_batch* b);
 pi_status pi_batch_get_time(pi_batch* b, int64_t* iteration, double* t);
 pi_status pi_batch_set_time(pi_batch* b, int64_t iteration, double t);
 
-/* Active individuals of one member and species (sp = -1: all species; member = -1: all members). */
+/* Active individuals of one member and species (sp = -1: all species; member = -1: all members);
+ * the _async form as pi_count_active_async. */
 pi_status pi_batch_count_active(pi_batch* b, int32_t member, int32_t sp, int64_t* n);
+pi_status pi_batch_count_active_async(pi_batch* b, int32_t member, int32_t sp, int64_t* n);
 /* As pi_check_finite for one member. */
 pi_status pi_batch_check_finite(pi_batch* b, int32_t member);
 /* As pi_get_diag / pi_reset_diags. */

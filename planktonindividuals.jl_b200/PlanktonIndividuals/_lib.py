@@ -103,4 +103,7 @@ EXPORTS = ("pi_create", "pi_destroy", "pi_set_individuals", "pi_get_individuals"
            "pi_batch_get_time", "pi_batch_set_time", "pi_batch_count_active", "pi_batch_get_diag",
            "pi_batch_reset_diags", "pi_batch_budget", "pi_batch_autotune", "pi_batch_get_stream",
            "pi_batch_profile_enable", "pi_batch_profile_read", "pi_batch_last_error",
-           "pi_batch_set_sort_interval", "pi_check_finite", "pi_batch_check_finite")
+           "pi_batch_set_sort_interval", "pi_check_finite", "pi_batch_check_finite",
+           "pi_set_velocity_f32", "pi_set_PARF_f32", "pi_set_temp_f32", "pi_time_step_async",
+           "pi_count_active_async", "pi_batch_set_velocity_f32", "pi_batch_set_PARF_f32", "pi_batch_set_temp_f32",
+           "pi_batch_count_active_async")

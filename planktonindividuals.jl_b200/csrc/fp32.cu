@@ -148,8 +148,18 @@ struct pi_batch {
     double last_dT = 0.0;
     char* cub_tmp = nullptr;
     size_t cub_bytes = 0;
-    double* stage = nullptr;        // 3 × maxG doubles of upload staging
+    double* stage = nullptr;        // 3 × maxG doubles of upload staging (synchronous calls)
     cudaEvent_t copied = nullptr;   // recorded after a setter's host→device copies
+    // forcing setters: host→device copies on their own stream into double-buffered staging, so
+    // they overlap the steps already queued; the conversion runs on the model stream
+    cudaStream_t cstream = nullptr;
+    struct Stage { unsigned char* p[2] = {nullptr, nullptr}; cudaEvent_t copied[2] = {nullptr, nullptr};
+                   cudaEvent_t freed[2] = {nullptr, nullptr}; int k = 0; };
+    Stage vst, tst, pst;            // velocity (3 × maxG values), temperature (maxG), PARF (maxcol)
+    // own velocity buffers (0/1) per member, tracked on the host so setters need not wait for the
+    // queued steps: the buffer vel₁ is bound to (-1: a series snapshot), whether a setter bound it
+    // after the last queued step, and the buffer that is vel₀ of the next step (-1: none)
+    std::vector<int> vel1_buf, vel1_pending, vel0_buf;
     double* partial = nullptr;      // budget partials
     unsigned long long* scratch = nullptr;
     // work tables (device) built for the current tuning
@@ -325,6 +335,12 @@ void free_batch(pi_batch* b) {
     for (cudaEvent_t e : b->event_pool) cudaEventDestroy(e);
     b->event_pool.clear();
     if (b->copied) cudaEventDestroy(b->copied);
+    for (pi_batch::Stage* st : { &b->vst, &b->tst, &b->pst })
+        for (int k = 0; k < 2; ++k) {
+            if (st->copied[k]) cudaEventDestroy(st->copied[k]);
+            if (st->freed[k]) cudaEventDestroy(st->freed[k]);
+        }
+    if (b->cstream) cudaStreamDestroy(b->cstream);
     if (b->stream) cudaStreamDestroy(b->stream);
     b->stream = nullptr;
 }
@@ -589,6 +605,16 @@ pi_status enqueue_sort(pi_batch* b) {
     return PI_OK;
 }
 
+// Bookkeeping after a step was queued: the sort cycle and the own velocity buffers (vel₁ of the
+// step is vel₀ of the next).
+void after_step(pi_batch* b) {
+    b->since_sort += 1;
+    for (int m = 0; m < b->nm; ++m) {
+        b->vel0_buf[m] = b->vel1_buf[m];
+        b->vel1_pending[m] = 0;
+    }
+}
+
 // A sort before the next step when one is due.
 pi_status maybe_sort(pi_batch* b) {
     if (b->sort_interval <= 0) return PI_OK;
@@ -656,6 +682,13 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, b->device);
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) { b->err = "pi_batch_create: stream"; return bail(PI_ERR_CUDA); }
     if (cudaEventCreateWithFlags(&b->copied, cudaEventDisableTiming) != cudaSuccess) { b->err = "pi_batch_create: event"; return bail(PI_ERR_CUDA); }
+    if (cudaStreamCreateWithFlags(&b->cstream, cudaStreamNonBlocking) != cudaSuccess) { b->err = "pi_batch_create: stream"; return bail(PI_ERR_CUDA); }
+    for (pi_batch::Stage* st : { &b->vst, &b->tst, &b->pst })
+        for (int k = 0; k < 2; ++k)
+            if (cudaEventCreateWithFlags(&st->copied[k], cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&st->freed[k], cudaEventDisableTiming) != cudaSuccess) {
+                b->err = "pi_batch_create: event"; return bail(PI_ERR_CUDA);
+            }
     b->nm = nmembers; b->nsp = nspecies; b->nseg = nmembers * nspecies;
     b->mh.resize(nmembers);
     b->mdh.resize(nmembers);
@@ -765,6 +798,14 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     BA(b->divlist, S); BA(b->freelist, S); BA(b->ndiv, b->nseg);
     for (int a = 0; a < 3; ++a) BA(b->line_off[a], nmembers + 1);
     BA(b->stage, std::max<long long>(3 * b->maxG, col));
+    for (int k = 0; k < 2; ++k) {
+        BA(b->vst.p[k], 3 * b->maxG * sizeof(double));
+        BA(b->tst.p[k], b->maxG * sizeof(double));
+        BA(b->pst.p[k], std::max<long long>(b->maxcol, 1) * sizeof(double));
+    }
+    b->vel1_buf.assign(nmembers, 1);
+    b->vel1_pending.assign(nmembers, 0);
+    b->vel0_buf.assign(nmembers, 0);
     BA(b->partial, 3 * 1024); BA(b->scratch, 4);
     size_t cb = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, cb, b->tile_cnt, b->tile_off, b->ntiles, b->stream);
@@ -1059,46 +1100,77 @@ pi_status pi_batch_get_tracer(pi_batch* b, int32_t member, int32_t idx, double* 
 
 // Interior velocity snapshot (reference layout) into three halo-padded FP32 member fields
 // (vel_copy!, Simulation/utils.jl:5-34 with fill_halo_vel!).
-static pi_status vel_copy32(pi_batch* b, int m, const double* u, const double* v, const double* w,
-                            float* U, float* V, float* W) {
+}  // extern "C"
+
+// Host → device copies of one setter into the next staging buffer of `st`, on the copy stream; the
+// model stream then waits for them. Returns the buffer. The caller queues its conversion on the
+// model stream, records st.freed[k] after it, and waits for st.copied[k] before returning (the
+// host arrays are free from then on).
+static pi_status stage_copy(pi_batch* b, pi_batch::Stage& st, const void* const* src, const size_t* bytes, int n,
+                            size_t stride, unsigned char** out) {
+    const int k = st.k ^= 1;
+    BK(cudaStreamWaitEvent(b->cstream, st.freed[k], 0), "order staging");
+    for (int c = 0; c < n; ++c)
+        BK(cudaMemcpyAsync(st.p[k] + c * stride, src[c], bytes[c], cudaMemcpyDefault, b->cstream), "upload forcing");
+    BK(cudaEventRecord(st.copied[k], b->cstream), "record copies");
+    BK(cudaStreamWaitEvent(b->stream, st.copied[k], 0), "order conversion");
+    *out = st.p[k];
+    return PI_OK;
+}
+static pi_status stage_done(pi_batch* b, pi_batch::Stage& st) {
+    BK(cudaEventRecord(st.freed[st.k], b->stream), "record conversion");
+    BK(cudaEventSynchronize(st.copied[st.k]), "synchronize copies");
+    return PI_OK;
+}
+
+// vel_copy! (Simulation/utils.jl:5-34 with fill_halo_vel!) of an interior snapshot (reference
+// layout, Float64 or Float32) into three halo-padded FP32 member fields, queued on the model stream.
+template <typename S>
+static pi_status vel_copy32(pi_batch* b, int m, const S* u, const S* v, const S* w, float* U, float* V, float* W) {
     const HostGrid& g = b->mh[m].g;
     const MemberDev& d = b->mdh[m];
     cudaStream_t s = b->stream;
+    int bd[3] = { g.topo[0] == PI_BOUNDED, g.topo[1] == PI_BOUNDED, g.topo[2] == PI_BOUNDED };
+    int dims[3][3] = { { g.Nx + bd[0], g.Ny, g.Nz }, { g.Nx, g.Ny + bd[1], g.Nz }, { g.Nx, g.Ny, g.Nz + bd[2] } };
+    float* dst[3] = { U, V, W };
     if (g.Nx >= g.Hx && g.Ny >= g.Hy && g.Nz >= g.Hz) {
-        int bd[3] = { g.topo[0] == PI_BOUNDED, g.topo[1] == PI_BOUNDED, g.topo[2] == PI_BOUNDED };
-        int dims[3][3] = { { g.Nx + bd[0], g.Ny, g.Nz }, { g.Nx, g.Ny + bd[1], g.Nz }, { g.Nx, g.Ny, g.Nz + bd[2] } };
-        const double* src[3] = { u, v, w };
-        float* dst[3] = { U, V, W };
-        for (int c = 0; c < 3; ++c) {
-            const size_t n = (size_t)dims[c][0] * dims[c][1] * dims[c][2];
-            BK(cudaMemcpyAsync(b->stage + c * b->maxG, src[c], n * sizeof(double), cudaMemcpyDefault, s), "upload velocity");
-        }
-        // the caller's buffers are free once the copies are done; the conversion runs on
-        BK(cudaEventRecord(b->copied, s), "record copies");
+        const void* src[3] = { u, v, w };
+        size_t bytes[3];
+        for (int c = 0; c < 3; ++c) bytes[c] = (size_t)dims[c][0] * dims[c][1] * dims[c][2] * sizeof(S);
+        unsigned char* stg = nullptr;
+        pi_status e = stage_copy(b, b->vst, src, bytes, 3, b->maxG * sizeof(S), &stg);
+        if (e) return e;
         for (int c = 0; c < 3; ++c) {
             BK(cudaMemsetAsync(dst[c], 0, g.G * sizeof(float), s), "clear velocity");
-            k32_scatter_interior<<<std::min<unsigned>(nblk((long long)dims[c][0] * dims[c][1] * dims[c][2], 256), 1024), 256, 0, s>>>(
-                d, dst[c], b->stage + c * b->maxG, dims[c][0], dims[c][1], dims[c][2]);
+            k32_scatter_interior<S><<<std::min<unsigned>(nblk((long long)dims[c][0] * dims[c][1] * dims[c][2], 256), 1024), 256, 0, s>>>(
+                d, dst[c], (const S*)(stg + c * b->maxG * sizeof(S)), dims[c][0], dims[c][1], dims[c][2]);
             k32_halo_vel<0><<<std::min<unsigned>(nblk((long long)g.Gy * g.Gz, 128), 1024), 128, 0, s>>>(d, dst[c], c);
             k32_halo_vel<1><<<std::min<unsigned>(nblk((long long)g.Gx * g.Gz, 128), 1024), 128, 0, s>>>(d, dst[c], c);
             k32_halo_vel<2><<<std::min<unsigned>(nblk((long long)g.Gx * g.Gy, 128), 1024), 128, 0, s>>>(d, dst[c], c);
         }
         BK(cudaGetLastError(), "velocity halo");
-        BK(cudaEventSynchronize(b->copied), "synchronize");
-    } else {
-        std::vector<double> Ud, Vd, Wd;
-        host_vel_copy(g, u, v, w, Ud, Vd, Wd);
-        std::vector<float> tmp(g.G);
-        const std::vector<double>* hv[3] = { &Ud, &Vd, &Wd };
-        float* dst[3] = { U, V, W };
-        for (int c = 0; c < 3; ++c) {
-            for (long long q = 0; q < g.G; ++q) tmp[q] = (float)(*hv[c])[q];
-            BK(cudaMemcpyAsync(dst[c], tmp.data(), g.G * sizeof(float), cudaMemcpyHostToDevice, s), "upload velocity");
-            BK(cudaStreamSynchronize(s), "synchronize");
-        }
+        return stage_done(b, b->vst);
+    }
+    // an axis with fewer cells than halo points: the halo rule of the host grid code, synchronously
+    const size_t n[3] = { (size_t)dims[0][0] * dims[0][1] * dims[0][2], (size_t)dims[1][0] * dims[1][1] * dims[1][2],
+                          (size_t)dims[2][0] * dims[2][1] * dims[2][2] };
+    std::vector<double> hd[3];
+    const S* hs[3] = { u, v, w };
+    for (int c = 0; c < 3; ++c) hd[c].assign(hs[c], hs[c] + n[c]);
+    std::vector<double> Ud, Vd, Wd;
+    host_vel_copy(g, hd[0].data(), hd[1].data(), hd[2].data(), Ud, Vd, Wd);
+    std::vector<float> tmp(g.G);
+    const std::vector<double>* hv[3] = { &Ud, &Vd, &Wd };
+    BK(cudaStreamSynchronize(s), "synchronize");
+    for (int c = 0; c < 3; ++c) {
+        for (long long q = 0; q < g.G; ++q) tmp[q] = (float)(*hv[c])[q];
+        BK(cudaMemcpyAsync(dst[c], tmp.data(), g.G * sizeof(float), cudaMemcpyHostToDevice, s), "upload velocity");
+        BK(cudaStreamSynchronize(s), "synchronize");
     }
     return PI_OK;
 }
+
+extern "C" {
 
 static pi_status read_forcing(pi_batch* b, int m, MemberForcing& f) {
     BK(cudaMemcpyAsync(&f, b->F + m, sizeof f, cudaMemcpyDeviceToHost, b->stream), "read forcing");
@@ -1114,16 +1186,33 @@ static pi_status write_forcing(pi_batch* b, int m, const MemberForcing& fin, boo
     return PI_OK;
 }
 
-pi_status pi_batch_set_velocity(pi_batch* b, int32_t member, const double* u, const double* v, const double* w) {
+}  // extern "C"
+
+// New own vel₁ of a member: the own buffer that the velocity bound by the previous setter does not
+// occupy (that one is vel₀ by the time this step runs), bound on the device in stream order.
+template <typename S>
+static pi_status set_velocity_any(pi_batch* b, int32_t member, const S* u, const S* v, const S* w) {
     pi_status e = check_mem(b, member, "pi_set_velocity");
     if (e) return e;
     if (!u || !v || !w) return bfail(b, PI_ERR_ARG, "pi_set_velocity: NULL argument");
-    MemberForcing f;
-    if ((e = read_forcing(b, member, f))) return e;
-    const int buf = (f.vel0[0] == velown(b, member, 0, 0)) ? 1 : 0;   // the own buffer vel₀ does not alias
-    if ((e = vel_copy32(b, member, u, v, w, velown(b, member, buf, 0), velown(b, member, buf, 1), velown(b, member, buf, 2)))) return e;
-    for (int c = 0; c < 3; ++c) f.vel1[c] = velown(b, member, buf, c);
-    return write_forcing(b, member, f);
+    // a buffer bound since the last queued step is reused; otherwise the one that is not vel₀
+    const int buf = b->vel1_pending[member] ? b->vel1_buf[member] : (b->vel0_buf[member] == 0 ? 1 : 0);
+    float* dst[3] = { velown(b, member, buf, 0), velown(b, member, buf, 1), velown(b, member, buf, 2) };
+    if ((e = vel_copy32<S>(b, member, u, v, w, dst[0], dst[1], dst[2]))) return e;
+    k32_bind_own<<<1, 32, 0, b->stream>>>(b->F, member, dst[0], dst[1], dst[2], nullptr);
+    BK(cudaGetLastError(), "bind velocity");
+    b->vel1_buf[member] = buf;
+    b->vel1_pending[member] = 1;
+    return PI_OK;
+}
+
+extern "C" {
+
+pi_status pi_batch_set_velocity(pi_batch* b, int32_t member, const double* u, const double* v, const double* w) {
+    return set_velocity_any<double>(b, member, u, v, w);
+}
+pi_status pi_batch_set_velocity_f32(pi_batch* b, int32_t member, const float* u, const float* v, const float* w) {
+    return set_velocity_any<float>(b, member, u, v, w);
 }
 
 pi_status pi_batch_set_velocity0(pi_batch* b, int32_t member, const double* u, const double* v, const double* w) {
@@ -1133,41 +1222,60 @@ pi_status pi_batch_set_velocity0(pi_batch* b, int32_t member, const double* u, c
     MemberForcing f;
     if ((e = read_forcing(b, member, f))) return e;
     const int buf = (f.vel1[0] == velown(b, member, 0, 0)) ? 1 : 0;   // the own buffer vel₁ does not alias
-    if ((e = vel_copy32(b, member, u, v, w, velown(b, member, buf, 0), velown(b, member, buf, 1), velown(b, member, buf, 2)))) return e;
+    if ((e = vel_copy32<double>(b, member, u, v, w, velown(b, member, buf, 0), velown(b, member, buf, 1), velown(b, member, buf, 2)))) return e;
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
     for (int c = 0; c < 3; ++c) f.vel0[c] = velown(b, member, buf, c);
+    b->vel0_buf[member] = buf;
     return write_forcing(b, member, f);
 }
 
-pi_status pi_batch_set_PARF(pi_batch* b, int32_t member, const double* parf) {
+}  // extern "C"
+
+template <typename S>
+static pi_status set_PARF_any(pi_batch* b, int32_t member, const S* parf) {
     pi_status e = check_mem(b, member, "pi_set_PARF");
     if (e) return e;
     if (!parf) return bfail(b, PI_ERR_ARG, "pi_set_PARF: NULL argument");
     const long long n = (long long)b->mdh[member].Nx * b->mdh[member].Ny;
-    BK(cudaMemcpyAsync(b->stage, parf, n * sizeof(double), cudaMemcpyDefault, b->stream), "upload PARF");
-    BK(cudaEventRecord(b->copied, b->stream), "record copies");
-    k32_d2f<<<std::min<unsigned>(nblk(n, 256), 1024), 256, 0, b->stream>>>(b->PARF + b->mdh[member].col_off, b->stage, n);
+    const void* src[1] = { parf };
+    const size_t bytes[1] = { n * sizeof(S) };
+    unsigned char* stg = nullptr;
+    if ((e = stage_copy(b, b->pst, src, bytes, 1, 0, &stg))) return e;
+    k32_to_f32<S><<<std::min<unsigned>(nblk(n, 256), 1024), 256, 0, b->stream>>>(b->PARF + b->mdh[member].col_off, (const S*)stg, n);
     BK(cudaGetLastError(), "convert PARF");
-    BK(cudaEventSynchronize(b->copied), "synchronize");
-    return PI_OK;
+    return stage_done(b, b->pst);
 }
 
-pi_status pi_batch_set_temp(pi_batch* b, int32_t member, const double* temp) {
+extern "C" {
+
+pi_status pi_batch_set_PARF(pi_batch* b, int32_t member, const double* parf) { return set_PARF_any<double>(b, member, parf); }
+pi_status pi_batch_set_PARF_f32(pi_batch* b, int32_t member, const float* parf) { return set_PARF_any<float>(b, member, parf); }
+
+}  // extern "C"
+
+// copy_interior!: only the interior is written; the halo stays zero
+template <typename S>
+static pi_status set_temp_any(pi_batch* b, int32_t member, const S* temp) {
     pi_status e = check_mem(b, member, "pi_set_temp");
     if (e) return e;
     if (!temp) return bfail(b, PI_ERR_ARG, "pi_set_temp: NULL argument");
     const MemberDev& d = b->mdh[member];
     const long long n = (long long)d.Nx * d.Ny * d.Nz;
     float* dst = b->tempown + d.cell_off;
-    // copy_interior!: only the interior is written; the halo stays zero
-    BK(cudaMemcpyAsync(b->stage, temp, n * sizeof(double), cudaMemcpyDefault, b->stream), "upload temp");
-    BK(cudaEventRecord(b->copied, b->stream), "record copies");
-    k32_scatter_interior<<<std::min<unsigned>(nblk(n, 256), 1024), 256, 0, b->stream>>>(d, dst, b->stage, d.Nx, d.Ny, d.Nz);
+    const void* src[1] = { temp };
+    const size_t bytes[1] = { n * sizeof(S) };
+    unsigned char* stg = nullptr;
+    if ((e = stage_copy(b, b->tst, src, bytes, 1, 0, &stg))) return e;
+    k32_scatter_interior<S><<<std::min<unsigned>(nblk(n, 256), 1024), 256, 0, b->stream>>>(d, dst, (const S*)stg, d.Nx, d.Ny, d.Nz);
+    k32_bind_own<<<1, 32, 0, b->stream>>>(b->F, member, nullptr, nullptr, nullptr, dst);
     BK(cudaGetLastError(), "scatter temp");
-    MemberForcing f;
-    if ((e = read_forcing(b, member, f))) return e;
-    f.temp = dst;
-    return write_forcing(b, member, f, false);
+    return stage_done(b, b->tst);
 }
+
+extern "C" {
+
+pi_status pi_batch_set_temp(pi_batch* b, int32_t member, const double* temp) { return set_temp_any<double>(b, member, temp); }
+pi_status pi_batch_set_temp_f32(pi_batch* b, int32_t member, const float* temp) { return set_temp_any<float>(b, member, temp); }
 
 pi_status pi_batch_set_flux_bc(pi_batch* b, int32_t member, int32_t tracer, int32_t face, int32_t kind,
                                const double* values, int64_t nt) {
@@ -1240,7 +1348,7 @@ pi_status pi_batch_set_series(pi_batch* b, int32_t member,
     BK(cudaMemsetAsync(h.ser_temp, 0, (size_t)ntemp * g.G * sizeof(float), s), "clear temperature series");
     for (int64_t t = 0; t < ntemp; ++t) {
         BK(cudaMemcpyAsync(b->stage, temp + t * nt3, nt3 * sizeof(double), cudaMemcpyDefault, s), "upload temp");
-        k32_scatter_interior<<<std::min<unsigned>(nblk(nt3, 256), 1024), 256, 0, s>>>(d, h.ser_temp + t * g.G, b->stage, g.Nx, g.Ny, g.Nz);
+        k32_scatter_interior<double><<<std::min<unsigned>(nblk(nt3, 256), 1024), 256, 0, s>>>(d, h.ser_temp + t * g.G, b->stage, g.Nx, g.Ny, g.Nz);
         BK(cudaStreamSynchronize(s), "synchronize");
     }
     BK(cudaGetLastError(), "upload series");
@@ -1250,6 +1358,7 @@ pi_status pi_batch_set_series(pi_batch* b, int32_t member,
     se.has_series = 1; se.has_vel = has_vel; se.time_offset = time_offset;
     BK(cudaMemcpyAsync(b->S + member, &se, sizeof se, cudaMemcpyHostToDevice, s), "upload series table");
     BK(cudaStreamSynchronize(s), "synchronize");
+    if (has_vel) { b->vel1_buf[member] = -1; b->vel1_pending[member] = 0; }   // vel₁ comes from the series
     return PI_OK;
 }
 
@@ -1282,6 +1391,10 @@ pi_status pi_batch_clear_series(pi_batch* b, int32_t member) {
         f.temp = b->tempown + b->mdh[member].cell_off;
     }
     if ((e = write_forcing(b, member, f))) return e;
+    auto own_of = [&](const float* p) { return p == velown(b, member, 0, 0) ? 0 : p == velown(b, member, 1, 0) ? 1 : -1; };
+    b->vel1_buf[member] = own_of(f.vel1[0]);
+    b->vel0_buf[member] = own_of(f.vel0[0]);
+    b->vel1_pending[member] = 0;
     free_series(h);
     float* keep[3] = { se.velh_buf[0], se.velh_buf[1], se.velh_buf[2] };
     se = MemberSeries{};
@@ -1334,7 +1447,7 @@ pi_status pi_batch_step(pi_batch* b, double dT, int64_t nsteps, int32_t sync) {
             if ((e = maybe_sort(b))) return e;
             if ((e = enqueue_step(b, dT, b->cur))) return e;
             b->cur ^= 1;
-            b->since_sort += 1;
+            after_step(b);
             b->tracers_dirty = false;
         }
     } else {
@@ -1349,7 +1462,7 @@ pi_status pi_batch_step(pi_batch* b, double dT, int64_t nsteps, int32_t sync) {
                 BK(cudaGraphLaunch(b->gexec[b->cur][b->pcur], b->stream), "graph launch");
             }
             b->cur ^= 1;
-            b->since_sort += 1;
+            after_step(b);
         }
     }
     if (sync) return pi_batch_synchronize(b);
@@ -1393,6 +1506,24 @@ pi_status pi_batch_count_active(pi_batch* b, int32_t member, int32_t sp, int64_t
     BK(cudaMemcpyAsync(&h, b->scratch, sizeof h, cudaMemcpyDeviceToHost, b->stream), "download count");
     BK(cudaStreamSynchronize(b->stream), "synchronize");
     *n = (int64_t)h;
+    return PI_OK;
+}
+
+pi_status pi_batch_count_active_async(pi_batch* b, int32_t member, int32_t sp, int64_t* out) {
+    if (!b || !out || member < -1 || member >= b->nm || sp < -1 || sp >= b->nsp) return bfail(b, PI_ERR_ARG, "pi_count_active_async: bad argument");
+    long long first, count;
+    if (member < 0) { first = 0; count = b->Stot; }
+    else {
+        const MemberDev& d = b->mdh[member];
+        first = d.slot_off + (sp < 0 ? 0 : (long long)sp * d.C);
+        count = sp < 0 ? (long long)b->nsp * d.C : d.C;
+    }
+    // stream-ordered: the slot is cleared, counted and copied before the next call clears it
+    unsigned long long* slot = b->scratch + 1;
+    BK(cudaMemsetAsync(slot, 0, sizeof *slot, b->stream), "zero count");
+    k32_count_active<<<std::max(1u, std::min<unsigned>(nblk(count, 256), 148 * 4)), 256, 0, b->stream>>>(b->P.flags + first, count, slot);
+    BK(cudaGetLastError(), "k32_count_active");
+    BK(cudaMemcpyAsync(out, slot, sizeof *slot, cudaMemcpyDeviceToHost, b->stream), "download count");
     return PI_OK;
 }
 
@@ -1532,7 +1663,7 @@ pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t k, char* report, siz
             if ((e = maybe_sort(b))) return e;
             if ((e = enqueue_step(b, dT, b->cur))) return e;
             b->cur ^= 1;
-            b->since_sort += 1;
+            after_step(b);
             b->tracers_dirty = false;
         }
         BK(cudaStreamSynchronize(b->stream), "synchronize");

@@ -1450,8 +1450,10 @@ __global__ void k32_copy_if_err(float* __restrict__ dst, const float* __restrict
 // uploads, counts, budgets
 // ------------------------------------------------------------------------------------------
 
-// Interior array (reference layout, x fastest, FP64) into a member's halo-padded FP32 field.
-__global__ void k32_scatter_interior(MemberDev m, float* __restrict__ dst, const double* __restrict__ src,
+// Interior array (reference layout, x fastest, Float64 or Float32) into a member's halo-padded
+// FP32 field.
+template <typename S>
+__global__ void k32_scatter_interior(MemberDev m, float* __restrict__ dst, const S* __restrict__ src,
                                      int nx, int ny, int nz) {
     const long long n = (long long)nx * ny * nz;
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
@@ -1488,6 +1490,22 @@ __global__ void k32_halo_vel(MemberDev m, float* __restrict__ c, int face_axis) 
         if (velrule) { for (int h = N + H + 2; h <= N + 2 * H; ++h) at(h) = face; }
         else { for (int h = 1; h <= H; ++h) at(N + H + h) = ev[h - 1]; }
     }
+}
+
+// A setter's new own velocity (vel₁) and/or temperature of a member, bound on the device in
+// stream order (after the steps already queued); a replaced velocity is packed again.
+__global__ void k32_bind_own(MemberForcing* __restrict__ F, int m, const float* u, const float* v, const float* w,
+                             const float* temp) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    MemberForcing& f = F[m];
+    if (u) { f.vel1[0] = u; f.vel1[1] = v; f.vel1[2] = w; f.pks0 = nullptr; f.pks1 = nullptr; }
+    if (temp) f.temp = temp;
+}
+
+template <typename S>
+__global__ void k32_to_f32(float* __restrict__ dst, const S* __restrict__ src, long long n) {
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        dst[q] = (float)src[q];
 }
 
 __global__ void k32_d2f(float* __restrict__ dst, const double* __restrict__ src, long long n) {

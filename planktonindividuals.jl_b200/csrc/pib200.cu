@@ -762,6 +762,25 @@ pi_status pi_time_step(pi_model* m, double dT) {
     return check_device_errors(m);
 }
 
+pi_status pi_time_step_async(pi_model* m, double dT) {
+    if (m && m->b32) return fwd32(m, pi_batch_step(m->b32, dT, 1, 0));
+    if (!m) return fail(m, PI_ERR_ARG, "pi_time_step_async: NULL model");
+    return enqueue_step(m, dT);
+}
+
+pi_status pi_set_velocity_f32(pi_model* m, const float* u, const float* v, const float* w) {
+    if (m && m->b32) return fwd32(m, pi_batch_set_velocity_f32(m->b32, 0, u, v, w));
+    return fail(m, PI_ERR_ARG, "pi_set_velocity_f32: Float32 forcing is for a PI_FP32 model");
+}
+pi_status pi_set_PARF_f32(pi_model* m, const float* parf) {
+    if (m && m->b32) return fwd32(m, pi_batch_set_PARF_f32(m->b32, 0, parf));
+    return fail(m, PI_ERR_ARG, "pi_set_PARF_f32: Float32 forcing is for a PI_FP32 model");
+}
+pi_status pi_set_temp_f32(pi_model* m, const float* temp) {
+    if (m && m->b32) return fwd32(m, pi_batch_set_temp_f32(m->b32, 0, temp));
+    return fail(m, PI_ERR_ARG, "pi_set_temp_f32: Float32 forcing is for a PI_FP32 model");
+}
+
 pi_status pi_get_stream(pi_model* m, void** stream) {
     if (m && m->b32) return fwd32(m, pi_batch_get_stream(m->b32, stream));
     if (!m || !stream) return fail(m, PI_ERR_ARG, "pi_get_stream: NULL argument");
@@ -867,6 +886,20 @@ pi_status pi_check_finite(pi_model* m) {
         if (q != none)
             return fail(m, PI_ERR_NAN, "NaN or Inf in an attribute of individual " + std::to_string(q + 1) + " of species " + std::to_string(s + 1));
     }
+    return PI_OK;
+}
+
+pi_status pi_count_active_async(pi_model* m, int32_t sp, int64_t* n) {
+    if (m && m->b32) {
+        if (sp < 0 || sp >= m->nsp) return fail(m, PI_ERR_ARG, "pi_count_active_async: bad argument");
+        return fwd32(m, pi_batch_count_active_async(m->b32, 0, sp, n));
+    }
+    if (!m || !n || sp < 0 || sp >= m->nsp) return fail(m, PI_ERR_ARG, "pi_count_active_async: bad argument");
+    unsigned long long* d = (unsigned long long*)m->sb.rank64;   // scratch between steps, stream-ordered
+    CK(cudaMemsetAsync(d, 0, sizeof *d, m->stream), "zero count");
+    k_count_active<<<148 * 2, 256, 0, m->stream>>>(m->h_spc[sp].flags, m->C, d);
+    CK(cudaGetLastError(), "k_count_active");
+    CK(cudaMemcpyAsync(n, d, sizeof *d, cudaMemcpyDeviceToHost, m->stream), "download count");
     return PI_OK;
 }
 

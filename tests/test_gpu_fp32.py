@@ -393,3 +393,42 @@ def test_fused_tracer_kernel_equals_two_kernel_path(gpu_lib):
         _drive_batch(fused, wls, 1, vels)
     for m, wl in enumerate(wls):
         assert compare_states(plain.member(m), fused.member(m), wl.nsp) == [], f"member {m}"
+
+
+def test_async_float32_setters_equal_sync_path(gpu_lib):
+    """The overlapped input path of an FP32 model (pi_set_velocity/PARF/temp_f32 from Float32 host
+    arrays, copies on their own stream; pi_time_step_async; pi_count_active_async) against the
+    synchronous Float64 path, tolerance 0: a Float32 array is what the device makes of the Float64
+    one. The velocity changes every third step, sometimes twice between two steps, to exercise the
+    choice of the velocity buffer that the queued steps are not using."""
+    import ctypes as ct
+    import torch
+    wl = daylight(W.config2(nx=16, nz=8, N_per_species=1500, steps=16, nmodes=12, seed=61))
+    wl.dT_vel = 3 * wl.dT
+    vel = VelCache(wl)
+    a, b = fp32_model(gpu_lib, wl), fp32_model(gpu_lib, wl)
+    f32 = lambda x: np.asfortranarray(np.asarray(x, dtype=np.float32))
+    p = lambda x: ct.c_void_p(x.ctypes.data)
+    counts = torch.zeros(16 * wl.nsp, dtype=torch.int64, pin_memory=True)
+    keep = []
+    for i in range(16):
+        t = i * wl.dT
+        tv, tp, tt = int(t // wl.dT_vel), int(t // wl.dT_PAR), int(t // wl.dT_temp)
+        a.set_velocity(*vel(tv)); a.set_PARF(wl.parf[:, :, tp]); a.set_temp(wl.temp[:, :, :, tt])
+        a.time_step(wl.dT)
+        if i % 5 == 2:      # a velocity replaced before the step: the second one counts
+            junk = tuple(f32(x * 0.5) for x in vel(tv))
+            keep.append(junk)
+            assert gpu_lib.pi_set_velocity_f32(b.h, *(p(x) for x in junk)) == 0
+        u, v, w = (f32(x) for x in vel(tv))
+        par, tmp = f32(wl.parf[:, :, tp]), f32(wl.temp[:, :, :, tt])
+        keep.append((u, v, w, par, tmp))
+        assert gpu_lib.pi_set_velocity_f32(b.h, p(u), p(v), p(w)) == 0
+        assert gpu_lib.pi_set_PARF_f32(b.h, p(par)) == 0
+        assert gpu_lib.pi_set_temp_f32(b.h, p(tmp)) == 0
+        assert gpu_lib.pi_time_step_async(b.h, ct.c_double(wl.dT)) == 0
+        for s in range(wl.nsp):
+            assert gpu_lib.pi_count_active_async(b.h, s, ct.c_void_p(counts.data_ptr() + 8 * (i * wl.nsp + s))) == 0
+    assert gpu_lib.pi_synchronize(b.h) == 0
+    assert compare_states(a, b, wl.nsp) == []
+    assert [int(c) for c in counts[-wl.nsp:]] == [a.count_active(s) for s in range(wl.nsp)]
