@@ -514,7 +514,9 @@ def run_accuracy(args):
                 "boxes_with_equal_counts": int(sum(int(a == c) for a, c in zip(c32, c64))),
                 "max_count_diff": int(max(abs(a - c) for a, c in zip(c32, c64))),
                 "mean_growth_factor": round(float(np.mean(np.array(c64) / np.array(n0))), 4),
-                "max_tracer_mass_rel_err": float(max(mass)), "seconds": round(time.time() - t0, 1)}
+                "max_tracer_mass_rel_err": float(max(mass)),
+                "guard_band": dict(zip(("recomputed", "changed"), b.guard_stats())),
+                "seconds": round(time.time() - t0, 1)}
     wl = W.config3(seed=3) if args.workload == "config3" else W.config2(seed=2)
     out = {"accuracy": args.workload}
     out.update(fp32_vs_fp64(lib, wl, args.acc_steps))

@@ -346,6 +346,12 @@ pi_status pi_batch_budget(pi_batch* b, int32_t member, double out[6]);
  * not depend on launch shapes). `report` (may be NULL) receives one line per choice. */
 pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t steps_per_candidate, char* report, size_t report_len);
 
+/* Guard band of the FP32 form's decisions (no counterpart in the reference): a grazing, mortality
+ * or division draw within 1e-5 (relative) of its threshold p·ΔT is decided with p recomputed in
+ * Float64 from the individual's state. Counts since the batch was created: decisions recomputed
+ * and, of those, decisions that the Float32 probability would have taken the other way. */
+pi_status pi_batch_guard_stats(pi_batch* b, int64_t* recomputed, int64_t* changed);
+
 /* Storage order (no counterpart in the reference, which stores individuals in slot order): each
  * (member, species) segment is kept in an order grouped by cell, restored by a counting sort
  * before the first step after pi_batch_set_individuals and then every `steps` steps (default 32;

@@ -218,6 +218,12 @@ class PlanktonBatch:
         m holding a NaN or Inf."""
         self._check(self.lib.pi_batch_check_finite(self.h, int(m)), "check_finite")
 
+    def guard_stats(self):
+        """(decisions recomputed in Float64 near their threshold, decisions that changed)."""
+        r, c = ct.c_int64(), ct.c_int64()
+        self._check(self.lib.pi_batch_guard_stats(self.h, ct.byref(r), ct.byref(c)), "guard_stats")
+        return r.value, c.value
+
     def set_sort_interval(self, steps):
         """Steps between the counting sorts that keep the stored individuals grouped by cell
         (0: never); changes speed only, no result."""

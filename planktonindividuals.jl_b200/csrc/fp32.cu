@@ -103,6 +103,8 @@ struct pi_batch {
     // device
     MemberDev* md = nullptr;
     SpeciesDev32* sp = nullptr;
+    SpeciesDec64* dec64 = nullptr;
+    unsigned long long* guard = nullptr;    // guard band: decisions recomputed, decisions changed
     BgcDev32* bgc = nullptr;
     FluxBC32* bcs = nullptr;
     MemberForcing* F = nullptr;
@@ -495,7 +497,7 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
         PhysArgs a;
         a.T = b->T; a.P = b->P; a.sp = b->sp; a.F = b->F; a.st = b->st; a.dT = fdT; a.Gtot = G; a.tr = tr;
         a.par = b->par; a.pop = b->pop; a.pop_sp = b->pop_sp; a.env = b->env; a.acc = b->acc; a.dcnt = b->dcnt;
-        a.err = b->errw;
+        a.err = b->errw; a.dec64 = b->dec64; a.guard = b->guard;
         BScope sc(b, "k32_physiology");
         k32_physiology<<<tile_grid(b, b->tune.persist_phys), b->tune.bs_phys, 0, s>>>(a);
     }
@@ -693,6 +695,7 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     b->mh.resize(nmembers);
     b->mdh.resize(nmembers);
     std::vector<SpeciesDev32> sph;
+    std::vector<SpeciesDec64> dech;
     std::vector<BgcDev32> bgch;
     std::vector<float> dzF, dzC;
     std::vector<int2> tiles;
@@ -738,6 +741,8 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
             cmin = std::min(cmin, p.Cquota * p.Nsuper);
             if (p.Chl2Cint > 0.0) chlmin = std::min(chlmin, p.Chl2Cint * p.Cquota * p.Nsuper);
             sph.push_back(to_dev(p));
+            dech.push_back(SpeciesDec64{p.grz_P, p.mort_P, p.mort_reg, p.dvid_P, p.dvid_reg, p.dvid_reg2,
+                                        p.Cquota * p.Nsuper, (int)p.dvid_type});
         }
         if (chlmin > 1e299) chlmin = cmin;
         // 2^40 units per nominal individual: sums of up to ~2^22 individuals per cell fit in 63 bits
@@ -769,7 +774,7 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     const long long G = b->Gtot, S = b->Stot;
     pi_status st;
 #define BA(ptr, n) do { st = balloc(b, &(ptr), (size_t)(n), #ptr); if (st) return bail(st); } while (0)
-    BA(b->md, nmembers); BA(b->sp, sph.size()); BA(b->bgc, nmembers); BA(b->bcs, (size_t)nmembers * PI_NTRACERS * 6);
+    BA(b->md, nmembers); BA(b->sp, sph.size()); BA(b->dec64, dech.size()); BA(b->guard, 2); BA(b->bgc, nmembers); BA(b->bcs, (size_t)nmembers * PI_NTRACERS * 6);
     BA(b->F, nmembers); BA(b->S, nmembers); BA(b->st, 1); BA(b->errw, 1);
     BA(b->trbuf[0], PI_NTRACERS * G); BA(b->trbuf[1], PI_NTRACERS * G); BA(b->tb, PI_NTRACERS * G);
     BA(b->par, G); BA(b->diag_par, G); BA(b->PARF, std::max<long long>(col, 1));
@@ -851,6 +856,8 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     auto Z = [&](void* d, size_t n) { ok = ok && cudaMemsetAsync(d, 0, n, s0) == cudaSuccess; };
     H2D(b->md, b->mdh.data(), nmembers * sizeof(MemberDev));
     H2D(b->sp, sph.data(), sph.size() * sizeof(SpeciesDev32));
+    H2D(b->dec64, dech.data(), dech.size() * sizeof(SpeciesDec64));
+    Z(b->guard, 2 * sizeof(unsigned long long));
     H2D(b->bgc, bgch.data(), bgch.size() * sizeof(BgcDev32));
     H2D(b->bcs, b->bch.data(), b->bch.size() * sizeof(FluxBC32));
     H2D(b->F, Fh.data(), nmembers * sizeof(MemberForcing));
@@ -1603,6 +1610,16 @@ pi_status pi_batch_budget(pi_batch* b, int32_t member, double out[6]) {
     BK(cudaMemcpyAsync(h.data(), b->partial, 3 * nb * sizeof(double), cudaMemcpyDeviceToHost, b->stream), "download budget");
     BK(cudaStreamSynchronize(b->stream), "synchronize");
     for (int r = 0; r < 3; ++r) { double s = 0.0; for (int q = 0; q < nb; ++q) s += h[q * 3 + r]; out[3 + r] = s; }
+    return PI_OK;
+}
+
+pi_status pi_batch_guard_stats(pi_batch* b, int64_t* recomputed, int64_t* changed) {
+    if (!b) return bfail(b, PI_ERR_ARG, "pi_batch_guard_stats: NULL batch");
+    unsigned long long h[2] = {0, 0};
+    BK(cudaMemcpyAsync(h, b->guard, sizeof h, cudaMemcpyDeviceToHost, b->stream), "read guard counts");
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    if (recomputed) *recomputed = (int64_t)h[0];
+    if (changed) *changed = (int64_t)h[1];
     return PI_OK;
 }
 

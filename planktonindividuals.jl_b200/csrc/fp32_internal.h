@@ -148,6 +148,12 @@ struct SpeciesDev32 {
     float OGT_rate;         // exp(-Ea / (R (Topt + 273.15))), a constant of the species
 };
 
+// Float64 parameters of the decision probabilities, for the guard band of k32_physiology.
+struct SpeciesDec64 {
+    double grz_P, mort_P, mort_reg, dvid_P, dvid_reg, dvid_reg2, CqNs;   // CqNs = Cquota·Nsuper
+    int dvid_type;
+};
+
 struct BgcDev32 {
     float kw, kc, kDOC, Nit, kDON, kDOP, kPOC, kPON, kPOP;
     float kappa_h, kappa_v, kappa_hP, kappa_vP;

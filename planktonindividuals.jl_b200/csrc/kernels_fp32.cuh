@@ -690,7 +690,24 @@ struct PhysArgs {
     unsigned long long* acc;
     uint32_t* dcnt;
     const uint32_t* err;
+    const SpeciesDec64* dec64;  // [member * nsp + species]
+    unsigned long long* guard;  // [0] decisions recomputed in Float64, [1] of those, decisions changed
 };
+
+// Guard band of the decisions (get_probability!, division_death_probability.jl:95-107): a draw
+// within this relative distance of p·ΔT in Float32 takes the decision from p recomputed in Float64
+// from the individual's Float32 state, which removes the rounding of the probability formulas
+// (a few Float32 ulps) from the comparison.
+#define F32_GUARD_REL 1.0e-5f
+
+__device__ __forceinline__ double shape_dec_d(double x, double xmax, double k, int pw) {
+    const double fx = fmax(0.0, fmin(1.0, 1.0 - x / xmax));
+    const double p = pw == 2 ? fx * fx : (fx * fx) * (fx * fx);
+    return p / (k + p);
+}
+__device__ __forceinline__ bool near_threshold(float r, float t) {
+    return fabsf(r - t) <= F32_GUARD_REL * fabsf(t);
+}
 
 // flags, status, cell and logical slot of a slot, loaded one slot ahead of its physiology
 struct PHead { int32_t code, ls; uint8_t fl, stt; };
@@ -781,7 +798,27 @@ __device__ __forceinline__ void phys_one(const PhysArgs& a, const MemberDev& m, 
     // get_probability! (:95-107)
     float r0, r1, r2;
     draw3f(m.seed, iter, (uint32_t)s, PI_DRAW_DECISION, (uint32_t)hd.ls, r0, r1, r2);
-    const int dg = jl_lessf(r0, graz * dT), dm = jl_lessf(r1, mort * dT), dd = jl_lessf(r2, dv * dT);
+    int dg = jl_lessf(r0, graz * dT), dm = jl_lessf(r1, mort * dT), dd = jl_lessf(r2, dv * dT);
+    if (near_threshold(r0, graz * dT) || near_threshold(r1, mort * dT) || near_threshold(r2, dv * dT)) {
+        // the same probabilities in Float64 from the Float32 state (the constants are the Float32
+        // literals of the reference's formulas)
+        const SpeciesDec64& q = a.dec64[mi * a.T.nsp + s];
+        const double dTd = (double)dT, Sz64 = (double)Bm / q.CqNs;
+        const double g64 = (double)popv * q.grz_P;
+        const double m64 = q.mort_P * shape_dec_d(Sz64, q.mort_reg, (double)1.0e-5f, 4);
+        double d64;
+        if (q.dvid_type == 1) d64 = q.dvid_P * (1.0 - shape_dec_d(Sz64, q.dvid_reg, (double)2.0e-3f, 2));
+        else {
+            const double h = fmod(tnow, 86400.0) / 3600.0;
+            if (q.dvid_type == 2) d64 = q.dvid_P * (1.0 - shape_dec_d(h, q.dvid_reg, (double)1.0e-5f, 4));
+            else d64 = q.dvid_P * (1.0 - shape_dec_d(Sz64, q.dvid_reg, (double)1.0e-3f, 4)) *
+                       (1.0 - shape_dec_d(h, q.dvid_reg2, (double)1.0e-5f, 4));
+        }
+        const int dg2 = (double)r0 < g64 * dTd, dm2 = (double)r1 < m64 * dTd, dd2 = (double)r2 < d64 * dTd;
+        atomicAdd(&a.guard[0], 1ull);
+        if (dg2 != dg || dm2 != dm || dd2 != dd) atomicAdd(&a.guard[1], 1ull);
+        dg = dg2; dm = dm2; dd = dd2;
+    }
     P.Bm[g] = Bm; P.Cq[g] = Cq; P.Nq[g] = Nq; P.Pq[g] = Pq; P.Chl[g] = Chl; P.age[g] = age;
     P.flags[g] = (uint8_t)(F32_AC | (dg ? F32_GRAZ : 0) | (dm ? F32_MORT : 0) | (dd ? F32_DVID : 0));
     // calc_consume_kernel! (consume_loss.jl:2-9): only individuals binned this step reach the grid
