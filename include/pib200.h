@@ -61,8 +61,15 @@ enum {
 enum { PI_WEST = 0, PI_EAST, PI_SOUTH, PI_NORTH, PI_BOTTOM, PI_TOP };
 enum { PI_BC_NONE = 0, PI_BC_CONST, PI_BC_ARRAY2D, PI_BC_ARRAY3D };
 
-/* Diagnostics kept by TimeStep! (src/Diagnostics/diagnostics_struct.jl:23-105 defaults). */
-enum { PI_DIAG_PAR = 0, PI_DIAG_NUM, PI_DIAG_GRAZ, PI_DIAG_MORT, PI_DIAG_DVID };
+/* Diagnostics kept by TimeStep! (src/Diagnostics/diagnostics_struct.jl:23-105): the defaults,
+ * and the optional ones of PlanktonDiagnostics(model; tracer, phytoplankton) enabled with
+ * pi_set_diags: PI_DIAG_TRACER + tracer index (diags.tracer[name], time_step.jl:168-172) and
+ * PI_DIAG_PROC + process index (diags.phytos[sp][process], diags_spcs!,
+ * Diagnostics/diagnostics_kernels.jl:14-33) in QuotaMode's order below. */
+enum { PI_DIAG_PAR = 0, PI_DIAG_NUM, PI_DIAG_GRAZ, PI_DIAG_MORT, PI_DIAG_DVID,
+       PI_DIAG_TRACER = 16, PI_DIAG_PROC = 32 };
+enum { PI_PROC_PS = 0, PI_PROC_BS, PI_PROC_VDOC, PI_PROC_VNH4, PI_PROC_VNO3, PI_PROC_VPO4, PI_PROC_resp,
+       PI_PROC_exu, PI_PROC_Bm, PI_PROC_Cq, PI_PROC_Nq, PI_PROC_Pq, PI_PROC_Chl, PI_NPROC };
 
 /* RectilinearGrid (src/Grids/rectilinear_grid.jl:1-25). Metrics are passed as the reference
  * stores them after construction (rectilinear_grid.jl:57-122), halos included. */
@@ -196,6 +203,14 @@ pi_status pi_check_finite(pi_model* m);
 pi_status pi_get_diag(pi_model* m, int32_t kind, int32_t sp, double* out);
 pi_status pi_reset_diags(pi_model* m);
 
+/* PlanktonDiagnostics(model; tracer = (...), phytoplankton = (...)) beyond the defaults: bit n of
+ * tracer_mask adds diags.tracer for tracer n, bit q of proc_mask adds process q of every species
+ * (PI_PROC_*), read with pi_get_diag(PI_DIAG_TRACER + n / PI_DIAG_PROC + q). Each added field is
+ * the sum over steps of the tracer field (halos included) after the tracer update, or of
+ * proc·ac at every individual's find_inds! cell after the species' update, as TimeStep! adds
+ * them. Enabling (again) starts the added fields at zero; pi_reset_diags clears them too. */
+pi_status pi_set_diags(pi_model* m, uint32_t tracer_mask, uint32_t proc_mask);
+
 /* PlanktonSimulation(model; ΔT, iterations, PARF, temp, vels, ΔT_vel, ΔT_PAR, ΔT_temp)
  * (src/Simulation/simulations.jl:98-142) with the shape and time-step validation of
  * src/Simulation/utils.jl:213-304. The forcing series are copied to device memory once:
@@ -328,6 +343,10 @@ pi_status pi_batch_set_time(pi_batch* b, int64_t iteration, double t);
  * the _async form as pi_count_active_async. */
 pi_status pi_batch_count_active(pi_batch* b, int32_t member, int32_t sp, int64_t* n);
 pi_status pi_batch_count_active_async(pi_batch* b, int32_t member, int32_t sp, int64_t* n);
+/* As pi_set_diags, for every member. The FP32 form adds the tracer fields in Float32 (the
+ * reference's diagnostics arrays have the model's FT) and the processes as 64-bit fixed-point sums
+ * (exact and independent of the order individuals are visited in). */
+pi_status pi_batch_set_diags(pi_batch* b, uint32_t tracer_mask, uint32_t proc_mask);
 /* As pi_check_finite for one member. */
 pi_status pi_batch_check_finite(pi_batch* b, int32_t member);
 /* As pi_get_diag / pi_reset_diags. */

@@ -83,8 +83,9 @@ struct Species {
     dvec Sz, Bm, Cq, Nq, Pq, Chl, gen, age;
     std::vector<uint8_t> ac;
     dvec PS, VDOC, VNH4, VNO3, VPO4, rChl, resp, BS, exu, graz, mort, dvid;
-    /* diagnostics (diags.phytos[sp]) */
+    /* diagnostics (diags.phytos[sp]): defaults and the optional QuotaMode processes */
     dvec d_num, d_graz, d_mort, d_dvid;
+    std::vector<dvec> d_proc;            /* PI_NPROC fields when enabled */
 };
 
 struct FluxBC { int kind = PI_BC_NONE; dvec v; int64_t nt = 0; };
@@ -107,6 +108,8 @@ struct orc_model {
     dvec tNH4, tNO3, tPO4, tDOC, tDFe, tpar, tT, tpop, tdpar, tidc;
     std::vector<int64_t> tidc_int;
     dvec d_PAR;
+    uint32_t tr_mask = 0, proc_mask = 0;  /* optional diagnostics (PlanktonDiagnostics keywords) */
+    std::vector<dvec> d_tr;               /* 14 fields when any tracer is enabled */
     FluxBC bc[PI_NTRACERS][6];
     int64_t iteration;
     double t;
@@ -623,6 +626,13 @@ bool plankton_update(orc_model* m, Species& s, int spi, double dT, double t) {
         m->plk[PI_NO3][c] += jl_mulb(-s.VNO3[i] * dT, ac);
         m->plk[PI_PO4][c] += jl_mulb(-s.VPO4[i] * dT, ac);
     }
+    /* diags_spcs! (Diagnostics/diagnostics_kernels.jl:14-33), QuotaMode processes */
+    if (m->proc_mask) {
+        const dvec* procs[PI_NPROC] = { &s.PS, &s.BS, &s.VDOC, &s.VNH4, &s.VNO3, &s.VPO4, &s.resp, &s.exu,
+                                        &s.Bm, &s.Cq, &s.Nq, &s.Pq, &s.Chl };
+        for (int q = 0; q < PI_NPROC; ++q)
+            if (m->proc_mask & (1u << q)) diags_proc(m, s, s.d_proc[q], procs[q]);
+    }
     diags_proc(m, s, s.d_num, nullptr);
     return true;
 }
@@ -1108,6 +1118,9 @@ int orc_time_step(orc_model* m, double dT) {
     if (!ok) return PI_ERR_CAPACITY;
     tracer_update(m, dT);
     for (size_t q = 0; q < g.G; ++q) m->d_PAR[q] += m->par[q];                  /* :167 */
+    for (int n = 0; n < PI_NTRACERS; ++n)                                          /* :168-172 */
+        if (m->tr_mask & (1u << n))
+            for (size_t q = 0; q < g.G; ++q) m->d_tr[n][q] += m->tr[n][q];
     m->u0 = m->u1; m->v0 = m->v1; m->w0 = m->w1;                                  /* :174-177 */
     m->par0 = m->par;
     if (m->err_flags & ERR_DOMAIN) { m->err = "an individual left the halo-padded grid"; return PI_ERR_DOMAIN; }
@@ -1130,11 +1143,26 @@ int orc_count_active(orc_model* m, int32_t sp, int64_t* n) {
     return PI_OK;
 }
 
+/* PlanktonDiagnostics(model; tracer, phytoplankton) optional fields: enabling clears them. */
+int orc_set_diags(orc_model* m, uint32_t tr_mask, uint32_t proc_mask) {
+    if (!m || tr_mask >> PI_NTRACERS || proc_mask >> PI_NPROC) return PI_ERR_ARG;
+    m->tr_mask = tr_mask; m->proc_mask = proc_mask;
+    m->d_tr.assign(tr_mask ? PI_NTRACERS : 0, dvec(tr_mask ? m->g.G : 0, 0.0));
+    for (Species& S : m->sp) S.d_proc.assign(proc_mask ? PI_NPROC : 0, dvec(proc_mask ? m->g.G : 0, 0.0));
+    return PI_OK;
+}
+
 int orc_get_diag(orc_model* m, int32_t kind, int32_t sp, double* out) {
     if (!m || !out) return PI_ERR_ARG;
     const dvec* f = nullptr;
     if (kind == PI_DIAG_PAR) f = &m->d_PAR;
-    else {
+    else if (kind >= PI_DIAG_TRACER && kind < PI_DIAG_TRACER + PI_NTRACERS) {
+        if (!(m->tr_mask & (1u << (kind - PI_DIAG_TRACER)))) return PI_ERR_ARG;
+        f = &m->d_tr[kind - PI_DIAG_TRACER];
+    } else if (kind >= PI_DIAG_PROC && kind < PI_DIAG_PROC + PI_NPROC) {
+        if (sp < 0 || sp >= m->nsp || !(m->proc_mask & (1u << (kind - PI_DIAG_PROC)))) return PI_ERR_ARG;
+        f = &m->sp[sp].d_proc[kind - PI_DIAG_PROC];
+    } else {
         if (sp < 0 || sp >= m->nsp) return PI_ERR_ARG;
         Species& S = m->sp[sp];
         f = kind == PI_DIAG_NUM ? &S.d_num : kind == PI_DIAG_GRAZ ? &S.d_graz

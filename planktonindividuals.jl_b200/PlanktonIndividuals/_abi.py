@@ -14,6 +14,9 @@ NTRACERS = len(tracer_names)
 FACES = {"west": 0, "east": 1, "south": 2, "north": 3, "bottom": 4, "top": 5}
 PI_BC_NONE, PI_BC_CONST, PI_BC_ARRAY2D, PI_BC_ARRAY3D = 0, 1, 2, 3
 PI_DIAG_PAR, PI_DIAG_NUM, PI_DIAG_GRAZ, PI_DIAG_MORT, PI_DIAG_DVID = 0, 1, 2, 3, 4
+PI_DIAG_TRACER, PI_DIAG_PROC = 16, 32
+# QuotaMode processes of diags_spcs! (src/Diagnostics/diagnostics_kernels.jl:22-23), in PI_PROC_* order
+PROC_NAMES = ("PS", "BS", "VDOC", "VNH4", "VNO3", "VPO4", "resp", "exu", "Bm", "Cq", "Nq", "Pq", "Chl")
 
 _dp = ct.POINTER(ct.c_double)
 _i64p = ct.POINTER(ct.c_int64)

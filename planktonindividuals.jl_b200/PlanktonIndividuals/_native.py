@@ -229,6 +229,11 @@ class CModel:
         self._check(self._fn("count_active")(self.h, int(sp), ct.byref(n)), "count_active")
         return n.value
 
+    def set_diags(self, tracer_mask=0, proc_mask=0):
+        """PlanktonDiagnostics(model; tracer, phytoplankton) beyond the defaults: bit n of
+        tracer_mask adds tracer n, bit q of proc_mask the QuotaMode process q (PROC_NAMES)."""
+        self._check(self._fn("set_diags")(self.h, ct.c_uint32(tracer_mask), ct.c_uint32(proc_mask)), "set_diags")
+
     def check_finite(self):
         """Raises PIError (PI_ERR_NAN) naming the first tracer cell or active individual holding a
         NaN or Inf."""

@@ -213,6 +213,10 @@ class PlanktonBatch:
     def synchronize(self):
         self._check(self.lib.pi_batch_synchronize(self.h), "synchronize")
 
+    def set_diags(self, tracer_mask=0, proc_mask=0):
+        """Optional diagnostics of every member (bits as pi_batch_set_diags)."""
+        self._check(self.lib.pi_batch_set_diags(self.h, ct.c_uint32(tracer_mask), ct.c_uint32(proc_mask)), "set_diags")
+
     def check_finite(self, m):
         """Raises PIError (PI_ERR_NAN) naming the first tracer cell or active individual of member
         m holding a NaN or Inf."""

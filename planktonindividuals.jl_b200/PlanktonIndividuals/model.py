@@ -148,35 +148,77 @@ class PlanktonModel:
 class PlanktonDiagnostics:
     """PlanktonDiagnostics(model; tracer, phytoplankton, iteration_interval)
     (diagnostics_struct.jl:23-105). The default diagnostics (PAR and num/graz/mort/dvid per
-    species) are accumulated on the device by every step; fields download on access."""
+    species) and the requested ones — tracer fields (any of the 14 tracer names) and QuotaMode
+    processes (PS, BS, VDOC, VNH4, VNO3, VPO4, resp, exu, Bm, Cq, Nq, Pq, Chl) — are accumulated on
+    the device by every step; fields download on access."""
+
+    DEFAULT = ("num", "graz", "mort", "dvid", "ptc")
 
     def __init__(self, model, tracer=(), phytoplankton=("num", "graz", "mort", "dvid", "ptc"),
                  abiotic_particle=("num",), iteration_interval=1):
-        extra = [p for p in phytoplankton if p not in ("num", "graz", "mort", "dvid", "ptc")]
-        if tracer or extra:
-            raise NotImplementedError("only the default diagnostics (PAR, num, graz, mort, dvid) are implemented")
+        if not isinstance(tracer, tuple) or not isinstance(phytoplankton, tuple):
+            raise ValueError("tracer and phytoplankton must be Tuples")
+        # diag_avail (diagnostics_struct.jl:115-136): names available for QuotaMode
+        for t in tracer:
+            if t not in tracer_names and t != "PAR":
+                raise ValueError(f"{t} is not one of the diagnostics")
+        for p in phytoplankton:
+            if p not in self.DEFAULT and p not in _abi.PROC_NAMES:
+                raise ValueError(f"{p} is not one of the diagnostics")
+        for a in abiotic_particle:
+            if a != "num":
+                raise ValueError(f"{a} is not one of the diagnostics")
         self._model = model
         self.iteration_interval = iteration_interval
         nat = model._native
+        tmask = 0
+        for t in tracer:
+            if t in tracer_names:
+                tmask |= 1 << tracer_names.index(t)
+        pmask = 0
+        for p in phytoplankton:
+            if p in _abi.PROC_NAMES:
+                pmask |= 1 << _abi.PROC_NAMES.index(p)
+        nat.set_diags(tmask, pmask)
         G = model.grid.total_size
+        procs = tuple(dict.fromkeys(tuple(phytoplankton) + self.DEFAULT))
 
         class _Sp:
             def __init__(self, s):
                 self.s = s
+
+            def keys(self):
+                return procs
 
             def __getattr__(self, k):
                 kinds = {"num": _abi.PI_DIAG_NUM, "graz": _abi.PI_DIAG_GRAZ,
                          "mort": _abi.PI_DIAG_MORT, "dvid": _abi.PI_DIAG_DVID}
                 if k == "ptc":
                     return np.zeros(G, order="F")
-                if k not in kinds:
-                    raise AttributeError(k)
-                return nat.get_diag(kinds[k], self.s)
+                if k in kinds:
+                    return nat.get_diag(kinds[k], self.s)
+                if k in procs:
+                    return nat.get_diag(_abi.PI_DIAG_PROC + _abi.PROC_NAMES.index(k), self.s)
+                raise AttributeError(k)
+
+            def __getitem__(self, k):
+                return getattr(self, k)
+
+        names = tuple(t for t in tracer if t in tracer_names) + ("PAR",)
 
         class _Tr:
-            @property
-            def PAR(self):
-                return nat.get_diag(_abi.PI_DIAG_PAR, 0)
+            def keys(self):
+                return names
+
+            def __getattr__(self, k):
+                if k == "PAR":
+                    return nat.get_diag(_abi.PI_DIAG_PAR, 0)
+                if k in names:
+                    return nat.get_diag(_abi.PI_DIAG_TRACER + tracer_names.index(k), 0)
+                raise AttributeError(k)
+
+            def __getitem__(self, k):
+                return getattr(self, k)
 
         self.tracer = _Tr()
         self.phytos = _Attrs({f"sp{s + 1}": _Sp(s) for s in range(model.phyto.Nsp)})

@@ -104,6 +104,10 @@ struct pi_batch {
     MemberDev* md = nullptr;
     SpeciesDev32* sp = nullptr;
     SpeciesDec64* dec64 = nullptr;
+    // optional diagnostics (pi_batch_set_diags)
+    uint32_t tr_mask = 0, proc_mask = 0;
+    float* diag_tr = nullptr;                // 14 × Gtot
+    unsigned long long* diag_proc = nullptr; // nsp × PI_NPROC × Gtot, fixed point
     unsigned long long* guard = nullptr;    // guard band: decisions recomputed, decisions changed
     BgcDev32* bgc = nullptr;
     FluxBC32* bcs = nullptr;
@@ -498,6 +502,7 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
         a.T = b->T; a.P = b->P; a.sp = b->sp; a.F = b->F; a.st = b->st; a.dT = fdT; a.Gtot = G; a.tr = tr;
         a.par = b->par; a.pop = b->pop; a.pop_sp = b->pop_sp; a.env = b->env; a.acc = b->acc; a.dcnt = b->dcnt;
         a.err = b->errw; a.dec64 = b->dec64; a.guard = b->guard;
+        a.dproc = b->diag_proc; a.pmask = b->proc_mask;
         BScope sc(b, "k32_physiology");
         k32_physiology<<<tile_grid(b, b->tune.persist_phys), b->tune.bs_phys, 0, s>>>(a);
     }
@@ -556,6 +561,7 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
       k32_halo<1><<<std::min<unsigned>(nblk(b->nlines[1], 128), 148 * 8), 128, 0, s>>>(b->md, b->line_off[1], b->nm, G, trn, PI_NTRACERS, b->errw);
       k32_halo<2><<<std::min<unsigned>(nblk(b->nlines[2], 128), 148 * 8), 128, 0, s>>>(b->md, b->line_off[2], b->nm, G, trn, PI_NTRACERS, b->errw); }
     k32_copy_if_err<<<148 * 4, 256, 0, s>>>(trn, tr, (long long)PI_NTRACERS * G, b->errw);
+    if (b->tr_mask) k32_diag_tracers<<<148 * 4, 256, 0, s>>>(b->diag_tr, trn, b->tr_mask, G, b->errw);
     k32_end_step<<<nblk(b->nm, 128), 128, 0, s>>>(b->nm, b->F, b->st, dT, b->errw);
     BK(cudaGetLastError(), "step launch");
     return PI_OK;
@@ -1534,6 +1540,20 @@ pi_status pi_batch_count_active_async(pi_batch* b, int32_t member, int32_t sp, i
     return PI_OK;
 }
 
+pi_status pi_batch_set_diags(pi_batch* b, uint32_t tracer_mask, uint32_t proc_mask) {
+    if (!b || tracer_mask >> PI_NTRACERS || proc_mask >> PI_NPROC) return bfail(b, PI_ERR_ARG, "pi_set_diags: bad argument");
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    pi_status e;
+    if (tracer_mask && !b->diag_tr && (e = balloc(b, &b->diag_tr, (size_t)PI_NTRACERS * b->Gtot, "tracer diagnostics"))) return e;
+    if (proc_mask && !b->diag_proc && (e = balloc(b, &b->diag_proc, (size_t)b->nsp * PI_NPROC * b->Gtot, "process diagnostics"))) return e;
+    if (b->diag_tr) BK(cudaMemsetAsync(b->diag_tr, 0, (size_t)PI_NTRACERS * b->Gtot * sizeof(float), b->stream), "clear diagnostics");
+    if (b->diag_proc) BK(cudaMemsetAsync(b->diag_proc, 0, (size_t)b->nsp * PI_NPROC * b->Gtot * 8, b->stream), "clear diagnostics");
+    BK(cudaStreamSynchronize(b->stream), "synchronize");
+    b->tr_mask = tracer_mask; b->proc_mask = proc_mask;
+    free_graphs(b);                     // the captured steps read the masks
+    return PI_OK;
+}
+
 pi_status pi_batch_get_diag(pi_batch* b, int32_t member, int32_t kind, int32_t sp, double* out) {
     pi_status e = check_mem(b, member, "pi_get_diag");
     if (e) return e;
@@ -1542,7 +1562,16 @@ pi_status pi_batch_get_diag(pi_batch* b, int32_t member, int32_t kind, int32_t s
     const long long G = d.G;
     const unsigned grid = std::min<unsigned>(nblk(G, 256), 1024);
     if (kind == PI_DIAG_PAR) k32_f2d<<<grid, 256, 0, b->stream>>>(b->stage, b->diag_par + d.cell_off, G);
-    else {
+    else if (kind >= PI_DIAG_TRACER && kind < PI_DIAG_TRACER + PI_NTRACERS) {
+        if (!(b->tr_mask >> (kind - PI_DIAG_TRACER) & 1u)) return bfail(b, PI_ERR_ARG, "pi_get_diag: tracer diagnostic not enabled");
+        k32_f2d<<<grid, 256, 0, b->stream>>>(b->stage, b->diag_tr + (long long)(kind - PI_DIAG_TRACER) * b->Gtot + d.cell_off, G);
+    } else if (kind >= PI_DIAG_PROC && kind < PI_DIAG_PROC + PI_NPROC) {
+        const int q = kind - PI_DIAG_PROC;
+        if (sp < 0 || sp >= b->nsp || !(b->proc_mask >> q & 1u))
+            return bfail(b, PI_ERR_ARG, "pi_get_diag: process diagnostic not enabled or bad species");
+        k32_fx2d<<<grid, 256, 0, b->stream>>>(b->stage, b->diag_proc + ((long long)sp * PI_NPROC + q) * b->Gtot + d.cell_off, G,
+                                              proc_unit(d, q));
+    } else {
         if (sp < 0 || sp >= b->nsp || kind < PI_DIAG_NUM || kind > PI_DIAG_DVID) return bfail(b, PI_ERR_ARG, "pi_get_diag: bad kind/species");
         k32_u2d<<<grid, 256, 0, b->stream>>>(b->stage, b->dcnt + ((long long)sp * 4 + (kind - PI_DIAG_NUM)) * b->Gtot + d.cell_off, G);
     }
@@ -1589,6 +1618,8 @@ pi_status pi_batch_reset_diags(pi_batch* b) {
     if (!b) return bfail(b, PI_ERR_ARG, "pi_reset_diags: NULL batch");
     BK(cudaMemsetAsync(b->diag_par, 0, b->Gtot * sizeof(float), b->stream), "reset diags");
     BK(cudaMemsetAsync(b->dcnt, 0, (size_t)b->nsp * 4 * b->Gtot * sizeof(uint32_t), b->stream), "reset diags");
+    if (b->diag_tr) BK(cudaMemsetAsync(b->diag_tr, 0, (size_t)PI_NTRACERS * b->Gtot * sizeof(float), b->stream), "reset diags");
+    if (b->diag_proc) BK(cudaMemsetAsync(b->diag_proc, 0, (size_t)b->nsp * PI_NPROC * b->Gtot * 8, b->stream), "reset diags");
     BK(cudaStreamSynchronize(b->stream), "synchronize");
     return PI_OK;
 }

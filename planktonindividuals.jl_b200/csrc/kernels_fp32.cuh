@@ -692,7 +692,16 @@ struct PhysArgs {
     const uint32_t* err;
     const SpeciesDec64* dec64;  // [member * nsp + species]
     unsigned long long* guard;  // [0] decisions recomputed in Float64, [1] of those, decisions changed
+    unsigned long long* dproc;  // optional process diagnostics, fixed point: (species * PI_NPROC + q) * Gtot
+    uint32_t pmask;             // enabled processes (PI_PROC_* bits)
 };
+
+// Fixed-point units of the process diagnostics: rates (mmol s⁻¹) in the mass unit per minute,
+// Bm, Cq, Nq and Pq in the mass unit, Chl in the Chl unit (so a sum over any set of individuals is
+// exact in 64 bits and independent of the order).
+__host__ __device__ inline double proc_unit(const MemberDev& m, int q) {
+    return q < PI_PROC_Bm ? m.fx_unit / 60.0 : q < PI_PROC_Chl ? m.fx_unit : m.chl_unit;
+}
 
 // Guard band of the decisions (get_probability!, division_death_probability.jl:95-107): a draw
 // within this relative distance of p·ΔT in Float32 takes the decision from p recomputed in Float64
@@ -831,6 +840,12 @@ __device__ __forceinline__ void phys_one(const PhysArgs& a, const MemberDev& m, 
         add_fixed(&a.acc[ACC_PO4 * G + cq], -VPO4 * dT, u);
     }
     atomicAdd(&a.dcnt[(long long)s * 4 * G + cq], 1u);      // diags num at the (possibly stale) cell
+    // diags_spcs! (Diagnostics/diagnostics_kernels.jl:14-33) at the same cell
+    if (a.pmask) {
+        const float v[PI_NPROC] = { PS, BS, VDOC, VNH4, VNO3, VPO4, resp, exu, Bm, Cq, Nq, Pq, Chl };
+        for (int q = 0; q < PI_NPROC; ++q)
+            if (a.pmask >> q & 1u) add_fixed(&a.dproc[((long long)s * PI_NPROC + q) * G + cq], v[q], 1.0 / proc_unit(m, q));
+    }
 }
 
 __global__ void __launch_bounds__(256, 4) k32_physiology(PhysArgs a) {
@@ -1574,6 +1589,21 @@ __global__ void k32_first_nonfinite_inds(IndDev32 P, long long base, long long C
         for (int k = 0; k < 10; ++k) bad |= !isfinite(v[k]);
         if (bad) atomicMin(first, (unsigned long long)P.lslot[g]);
     }
+}
+
+// diags.tracer[name] .+= tracer (time_step.jl:168-172) for the enabled tracers, halos included.
+__global__ void k32_diag_tracers(float* __restrict__ d, const float* __restrict__ tr, uint32_t mask, long long Gtot,
+                                 const uint32_t* err) {
+    if (stopped(err)) return;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < (long long)PI_NTRACERS * Gtot;
+         q += (long long)gridDim.x * blockDim.x)
+        if (mask >> (q / Gtot) & 1u) d[q] = d[q] + tr[q];
+}
+
+// fixed-point sums to Float64 values
+__global__ void k32_fx2d(double* __restrict__ dst, const unsigned long long* __restrict__ src, long long n, double unit) {
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        dst[q] = (double)(long long)src[q] * unit;
 }
 
 // Active individuals of a slot range (calc_active_individuals, models.jl:157-164).

@@ -398,7 +398,7 @@ __global__ void k_physiology(DGrid g, SpcDev P, pi_quota_params p, long long C, 
                              const double* __restrict__ par, const double* __restrict__ temp,
                              const uint32_t* __restrict__ off, const uint32_t* __restrict__ gid_sorted,
                              const int32_t* __restrict__ pos, double* __restrict__ contrib,
-                             double* __restrict__ d_num, const uint32_t* err) {
+                             double* __restrict__ d_num, double* __restrict__ procv, const uint32_t* err) {
     long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= C) return;
     if (*err & PI_DEVERR_CAPACITY) return;
@@ -516,8 +516,54 @@ __global__ void k_physiology(DGrid g, SpcDev P, pi_quota_params p, long long C, 
         K[3] = jl_mulb(-VNO3 * dT, ac);
         K[4] = jl_mulb(-VPO4 * dT, ac);
     }
+    // diags_spcs! values of the slot (PI_PROC_* order), summed per cell in slot order later
+    if (procv) {
+        const double v[PI_NPROC] = { PS, BS, VDOC, VNH4, VNO3, VPO4, resp, exu, Bm, Cq, Nq, Pq, Chl };
+        for (int q = 0; q < PI_NPROC; ++q) procv[(long long)q * C + slot] = v[q];
+    }
     // diags_proc!(num, ac, ac) at the slot's (possibly stale) cell
     atomicAdd(&d_num[c], 1.0);
+}
+
+// diags_spcs! (Diagnostics/diagnostics_kernels.jl:14-33): the cell of every slot active after the
+// species' update (its find_inds! cell), G for the others, for a stable sort by cell.
+__global__ void k_diag_keys(DGrid g, SpcDev P, long long C, uint32_t* __restrict__ key, uint32_t* __restrict__ val,
+                            const uint32_t* err) {
+    const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= C) return;
+    uint32_t k = (uint32_t)g.G;
+    if (!(*err & PI_DEVERR_CAPACITY) && (P.flags[slot] & FL_AC)) {
+        int xi, yi, zi;
+        unpack_cell(g, P.cell[slot], xi, yi, zi);
+        k = (uint32_t)gidx(g, xi, yi, zi);
+    }
+    key[slot] = k;
+    val[slot] = (uint32_t)slot;
+}
+
+// d[cell] += value of each of the cell's slots in ascending slot order (the sorted run of the
+// cell), for the enabled processes; one thread per run.
+__global__ void k_diag_sum(long long C, long long G, const uint32_t* __restrict__ key, const uint32_t* __restrict__ val,
+                           const double* __restrict__ procv, uint32_t mask, double* __restrict__ d) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= C) return;
+    const uint32_t c = key[i];
+    if (c >= (uint32_t)G || (i > 0 && key[i - 1] == c)) return;
+    for (int q = 0; q < PI_NPROC; ++q) {
+        if (!(mask >> q & 1u)) continue;
+        double x = d[(long long)q * G + c];
+        for (long long j = i; j < C && key[j] == c; ++j) x = x + procv[(long long)q * C + val[j]];
+        d[(long long)q * G + c] = x;
+    }
+}
+
+// diags.tracer[name] .+= tracer (time_step.jl:168-172) for the enabled tracers, halos included.
+__global__ void k_diag_tracers(double* __restrict__ d, const double* __restrict__ tr, uint32_t mask, long long G,
+                               const uint32_t* err) {
+    if (*err & PI_DEVERR_CAPACITY) return;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < (long long)PI_NTRACERS * G;
+         q += (long long)gridDim.x * blockDim.x)
+        if (mask >> (q / G) & 1u) d[q] = d[q] + tr[q];
 }
 
 // ------------------------------------------------------------------------------------------

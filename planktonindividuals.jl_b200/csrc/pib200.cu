@@ -78,6 +78,14 @@ struct pi_model {
     const double* temp = nullptr;
     double* diag_par = nullptr;  // G
     double* diag_sp = nullptr;   // nsp × 4 × G (num, graz, mort, dvid)
+    // optional diagnostics (pi_set_diags)
+    uint32_t tr_mask = 0, proc_mask = 0;
+    double* diag_tr = nullptr;   // 14 × G
+    double* diag_proc = nullptr; // nsp × PI_NPROC × G
+    double* procv = nullptr;     // PI_NPROC × C values of the species being updated
+    uint32_t *dkey = nullptr, *dkey_s = nullptr, *dval = nullptr, *dval_s = nullptr;
+    void* dsort_tmp = nullptr;
+    size_t dsort_bytes = 0;
     double* dzF = nullptr;
     double* dzC = nullptr;
     uint8_t* lm = nullptr;
@@ -294,8 +302,18 @@ pi_status enqueue_step(pi_model* m, double dT) {
                                                  shared, trp + PI_NH4 * G, trp + PI_NO3 * G,
                                                  trp + PI_PO4 * G, trp + PI_DOC * G, m->par, m->temp,
                                                  sb.off, sb.gid_sorted, sb.pos, sb.contrib,
-                                                 dsp + 0 * G, sb.err);
+                                                 dsp + 0 * G, m->proc_mask ? m->procv : nullptr, sb.err);
         CK(cudaGetLastError(), "k_physiology"); }
+        if (m->proc_mask) {
+            ProfScope ps_(m, "k_diag_proc");
+            k_diag_keys<<<nblk(C, BS), BS, 0, st>>>(g, m->h_spc[s], C, m->dkey, m->dval, sb.err);
+            size_t db = m->dsort_bytes;
+            CK(cub::DeviceRadixSort::SortPairs(m->dsort_tmp, db, m->dkey, m->dkey_s, m->dval, m->dval_s, (int64_t)C,
+                                               0, m->key_bits, st), "sort diagnostics by cell");
+            k_diag_sum<<<nblk(C, BS), BS, 0, st>>>(C, G, m->dkey_s, m->dval_s, m->procv, m->proc_mask,
+                                                   m->diag_proc + (size_t)s * PI_NPROC * G);
+            CK(cudaGetLastError(), "k_diag_proc");
+        }
     }
     {
         { ProfScope ps_(m, "k_sweep_x");
@@ -327,6 +345,10 @@ pi_status enqueue_step(pi_model* m, double dT) {
         CK(cudaGetLastError(), "k_halo"); }
         k_copy_if_err<<<148 * 4, 256, 0, st>>>(m->tr_next, m->tr, PI_NTRACERS * G, sb.err);
         CK(cudaGetLastError(), "k_copy_if_err");
+        if (m->tr_mask) {
+            k_diag_tracers<<<148 * 4, 256, 0, st>>>(m->diag_tr, m->tr_next, m->tr_mask, G, sb.err);
+            CK(cudaGetLastError(), "k_diag_tracers");
+        }
     }
     std::swap(m->tr, m->tr_next);
     for (int c = 0; c < 3; ++c) m->vel0[c] = m->vel1[c];    // vel₀ .= vel₁ (time_step.jl:174-176)
@@ -903,13 +925,45 @@ pi_status pi_count_active_async(pi_model* m, int32_t sp, int64_t* n) {
     return PI_OK;
 }
 
+pi_status pi_set_diags(pi_model* m, uint32_t tracer_mask, uint32_t proc_mask) {
+    if (m && m->b32) return fwd32(m, pi_batch_set_diags(m->b32, tracer_mask, proc_mask));
+    if (!m || tracer_mask >> PI_NTRACERS || proc_mask >> PI_NPROC) return fail(m, PI_ERR_ARG, "pi_set_diags: bad argument");
+    const long long G = m->hg.G, C = m->C;
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    if (tracer_mask && !m->diag_tr) { pi_status e = dalloc(m, &m->diag_tr, (size_t)PI_NTRACERS * G, "tracer diagnostics"); if (e) return e; }
+    if (proc_mask && !m->diag_proc) {
+        pi_status e;
+        if ((e = dalloc(m, &m->diag_proc, (size_t)m->nsp * PI_NPROC * G, "process diagnostics"))) return e;
+        if ((e = dalloc(m, &m->procv, (size_t)PI_NPROC * C, "process values"))) return e;
+        for (uint32_t** p : { &m->dkey, &m->dkey_s, &m->dval, &m->dval_s })
+            if ((e = dalloc(m, p, (size_t)C, "diagnostic sort"))) return e;
+        size_t db = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, db, m->dkey, m->dkey_s, m->dval, m->dval_s, (int64_t)C, 0, m->key_bits, m->stream);
+        unsigned char* tmp = nullptr;
+        if ((e = dalloc(m, &tmp, std::max<size_t>(db, 1), "diagnostic sort"))) return e;
+        m->dsort_tmp = tmp; m->dsort_bytes = db;
+    }
+    if (m->diag_tr) CK(cudaMemsetAsync(m->diag_tr, 0, (size_t)PI_NTRACERS * G * sizeof(double), m->stream), "clear diagnostics");
+    if (m->diag_proc) CK(cudaMemsetAsync(m->diag_proc, 0, (size_t)m->nsp * PI_NPROC * G * sizeof(double), m->stream), "clear diagnostics");
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    m->tr_mask = tracer_mask; m->proc_mask = proc_mask;
+    return PI_OK;
+}
+
 pi_status pi_get_diag(pi_model* m, int32_t kind, int32_t sp, double* out) {
     if (m && m->b32) return fwd32(m, pi_batch_get_diag(m->b32, 0, kind, sp, out));
     if (!m || !out) return fail(m, PI_ERR_ARG, "pi_get_diag: bad argument");
     const long long G = m->hg.G;
     const double* src = nullptr;
     if (kind == PI_DIAG_PAR) src = m->diag_par;
-    else {
+    else if (kind >= PI_DIAG_TRACER && kind < PI_DIAG_TRACER + PI_NTRACERS) {
+        if (!(m->tr_mask >> (kind - PI_DIAG_TRACER) & 1u)) return fail(m, PI_ERR_ARG, "pi_get_diag: tracer diagnostic not enabled");
+        src = m->diag_tr + (size_t)(kind - PI_DIAG_TRACER) * G;
+    } else if (kind >= PI_DIAG_PROC && kind < PI_DIAG_PROC + PI_NPROC) {
+        if (sp < 0 || sp >= m->nsp || !(m->proc_mask >> (kind - PI_DIAG_PROC) & 1u))
+            return fail(m, PI_ERR_ARG, "pi_get_diag: process diagnostic not enabled or bad species");
+        src = m->diag_proc + ((size_t)sp * PI_NPROC + (kind - PI_DIAG_PROC)) * G;
+    } else {
         if (sp < 0 || sp >= m->nsp || kind < PI_DIAG_NUM || kind > PI_DIAG_DVID) return fail(m, PI_ERR_ARG, "pi_get_diag: bad kind/species");
         src = m->diag_sp + ((size_t)sp * 4 + (kind - PI_DIAG_NUM)) * G;
     }
@@ -924,6 +978,8 @@ pi_status pi_reset_diags(pi_model* m) {
     const long long G = m->hg.G;
     CK(cudaMemsetAsync(m->diag_par, 0, G * sizeof(double), m->stream), "reset diags");
     CK(cudaMemsetAsync(m->diag_sp, 0, 4 * m->nsp * G * sizeof(double), m->stream), "reset diags");
+    if (m->diag_tr) CK(cudaMemsetAsync(m->diag_tr, 0, (size_t)PI_NTRACERS * G * sizeof(double), m->stream), "reset diags");
+    if (m->diag_proc) CK(cudaMemsetAsync(m->diag_proc, 0, (size_t)m->nsp * PI_NPROC * G * sizeof(double), m->stream), "reset diags");
     CK(cudaStreamSynchronize(m->stream), "synchronize");
     return PI_OK;
 }
