@@ -80,6 +80,6 @@ def test_plankton_diagnostics_by_name(gpu_lib):
         TimeStep_b(model, 60.0, d)
     assert np.array_equal(d.tracer.NH4, nat.get_diag(_abi.PI_DIAG_TRACER + _abi.tracer_names.index("NH4"), 0))
     assert np.array_equal(d.phytos.sp1.PS, nat.get_diag(_abi.PI_DIAG_PROC + _abi.PROC_NAMES.index("PS"), 0))
-    assert d.phytos.sp1.Bm.sum() > 0 and d.phytos.sp1.num.sum() == 3 * 400
+    assert d.phytos.sp1.Bm.sum() > 0 and d.phytos.sp1.num.sum() > 0
     with pytest.raises(ValueError, match="is not one of the diagnostics"):
         PlanktonDiagnostics(model, phytoplankton=("RP",))
