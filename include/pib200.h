@@ -228,6 +228,11 @@ pi_status pi_sim_create(pi_model* m, double dT, int64_t iterations,
  * vels/PARF/temp time offsets. Runs asynchronously on the model's stream unless `sync`. */
 pi_status pi_sim_update(pi_sim* s, int32_t time_offset, int32_t sync);
 
+/* Steps first .. first+n-1 (1-based, update!'s loop index i, which the time_offset indexing
+ * uses) of update!(sim; time_offset): an update! split into parts, for example to write outputs
+ * after every step (write_output!, src/Simulation/update.jl:30). */
+pi_status pi_sim_update_steps(pi_sim* s, int64_t first, int64_t n, int32_t time_offset, int32_t sync);
+
 pi_status pi_sim_destroy(pi_sim* s);
 
 /* Blocks until all work queued on the model's stream is done and reports any device-side error
@@ -333,6 +338,9 @@ pi_status pi_batch_clear_series(pi_batch* b, int32_t member);
  * queueing; pi_batch_synchronize reports errors. A division overflow in any member stops the
  * whole batch at that step with PI_ERR_CAPACITY and the reference's message. */
 pi_status pi_batch_step(pi_batch* b, double dT, int64_t nsteps, int32_t sync);
+/* As pi_batch_step, with the step index within the update! call (time_offset indexing) starting
+ * at `first` (1-based) instead of 1. */
+pi_status pi_batch_step_from(pi_batch* b, double dT, int64_t first, int64_t nsteps, int32_t sync);
 pi_status pi_batch_synchronize(pi_batch* b);
 
 /* model.iteration and model.t (shared by all members). */

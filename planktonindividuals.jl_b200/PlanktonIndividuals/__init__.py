@@ -19,6 +19,7 @@ from .model import PlanktonDiagnostics, PlanktonModel, TimeStep_b, phyto_setup
 from .parameters import (bgc_params_default, default_PARF, default_temperature, default_tracer_init,
                          phyt_params_default, update_bgc_params, update_phyt_params)
 from .simulation import PlanktonSimulation, synchronize, update_b
+from .output import PlanktonOutputWriter, write_output_b
 from .batch import BatchMember, Member, PlanktonBatch
 from . import units
 
@@ -28,4 +29,4 @@ __all__ = ["RectilinearGrid", "Periodic", "Bounded", "PlanktonModel", "PlanktonS
            "bgc_params_default", "phyt_params_default", "update_bgc_params", "update_phyt_params",
            "default_PARF", "default_temperature", "default_tracer_init", "interior", "units",
            "CapacityError", "PIError", "ΔxC", "ΔyC", "ΔzC", "ΔxF", "ΔyF", "ΔzF", "Ax", "Ay", "Az",
-           "volume", "PlanktonBatch", "Member", "BatchMember"]
+           "volume", "PlanktonBatch", "Member", "BatchMember", "PlanktonOutputWriter", "write_output_b"]

@@ -25,9 +25,8 @@ class PlanktonSimulation:
 
     def __init__(self, model, *, ΔT, iterations, PARF=None, temp=None, diags=None, vels=None,
                  ΔT_vel=None, ΔT_PAR=3600.0, ΔT_temp=3600.0, output_writer=None):
-        if output_writer is not None:
-            raise NotImplementedError("output writers are not implemented")
         FT = model.FT
+        self.output_writer = output_writer
         g = model.grid
         self.model = model
         self.ΔT = float(FT(ΔT))
@@ -95,16 +94,27 @@ class PlanktonSimulation:
 
 def update_b(sim, time_offset=None, sync=True):
     """update!(sim; time_offset) (src/Simulation/update.jl:11-48). `sync=False` returns once the
-    steps are queued on the GPU; call `synchronize(sim.model)` to wait and collect errors."""
+    steps are queued on the GPU; call `synchronize(sim.model)` to wait and collect errors. With an
+    output writer, every step is followed by write_output! (update.jl:30), so the steps run one
+    call each."""
     to = time_offset or {}
     mask = (1 if to.get("vels") else 0) | (2 if to.get("PARF") else 0) | (4 if to.get("temp") else 0)
     nat = sim.model._native
-    rc = nat.lib.pi_sim_update(sim._h, mask, 1 if sync else 0)
-    if rc != PI_OK:
-        msg = nat._errmsg(nat.h)
-        if rc == 4:
-            raise CapacityError(rc, msg)
-        raise PIError(rc, msg)
+
+    def check(rc):
+        if rc != PI_OK:
+            msg = nat._errmsg(nat.h)
+            if rc == 4:
+                raise CapacityError(rc, msg)
+            raise PIError(rc, msg)
+
+    if sim.output_writer is None:
+        check(nat.lib.pi_sim_update(sim._h, mask, 1 if sync else 0))
+        return
+    from .output import write_output_b
+    for i in range(1, sim.iterations + 1):
+        check(nat.lib.pi_sim_update_steps(sim._h, ct.c_int64(i), ct.c_int64(1), mask, 1))
+        write_output_b(sim.output_writer, sim.model, sim.diags)
 
 
 def synchronize(model):

@@ -183,6 +183,7 @@ struct pi_batch {
     int tables_lzf = -1;
     unsigned char* tmaps = nullptr;  // CUtensorMap per member, [tracer buffer][member], 128 bytes each
     bool tracers_dirty = true;       // a tracer was uploaded since the last step
+    int64_t call_step0 = 0;          // source of the call-step copy (kept alive for the async copy)
     Tuning tune;
     // graphs
     cudaGraphExec_t gexec[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [tracer buffer][individual buffer]
@@ -1434,8 +1435,12 @@ pi_status pi_batch_synchronize(pi_batch* b) {
 }
 
 pi_status pi_batch_step(pi_batch* b, double dT, int64_t nsteps, int32_t sync) {
+    return pi_batch_step_from(b, dT, 1, nsteps, sync);
+}
+
+pi_status pi_batch_step_from(pi_batch* b, double dT, int64_t first, int64_t nsteps, int32_t sync) {
     if (!b) return bfail(b, PI_ERR_ARG, "pi_batch_step: NULL batch");
-    if (!(dT > 0) || nsteps < 0) return bfail(b, PI_ERR_ARG, "pi_batch_step: ΔT must be positive and nsteps >= 0");
+    if (!(dT > 0) || nsteps < 0 || first < 1) return bfail(b, PI_ERR_ARG, "pi_batch_step: ΔT must be positive, nsteps >= 0 and first >= 1");
     pi_status e = build_tables(b);
     if (e) return e;
     bool any3d = false;
@@ -1454,7 +1459,9 @@ pi_status pi_batch_step(pi_batch* b, double dT, int64_t nsteps, int32_t sync) {
                                                           std::to_string(it + nsteps) + " needs more");
     }
     b->last_dT = dT;
-    BK(cudaMemsetAsync(&b->st->call_step, 0, sizeof(int64_t), b->stream), "reset call step");
+    // the step index within the update! call, for the time_offset series indexing
+    b->call_step0 = first - 1;
+    BK(cudaMemcpyAsync(&b->st->call_step, &b->call_step0, sizeof(int64_t), cudaMemcpyHostToDevice, b->stream), "set call step");
     if (b->profiling || !b->use_graph) {
         for (int64_t i = 0; i < nsteps; ++i) {
             if ((e = maybe_sort(b))) return e;

@@ -1067,15 +1067,21 @@ pi_status pi_sim_create(pi_model* m, double dT, int64_t iterations,
 
 pi_status pi_sim_update(pi_sim* s, int32_t time_offset, int32_t sync) {
     if (!s || !s->m) return PI_ERR_ARG;
+    return pi_sim_update_steps(s, 1, s->iterations, time_offset, sync);
+}
+
+pi_status pi_sim_update_steps(pi_sim* s, int64_t first, int64_t n, int32_t time_offset, int32_t sync) {
+    if (!s || !s->m) return PI_ERR_ARG;
     pi_model* m = s->m;
+    if (first < 1 || n < 0) return fail(m, PI_ERR_ARG, "pi_sim_update_steps: first >= 1 and n >= 0 required");
     if (s->fp32) {
         pi_status st = pi_batch_set_time_offset(m->b32, 0, time_offset);
         if (st) return fwd32(m, st);
-        return fwd32(m, pi_batch_step(m->b32, s->dT, s->iterations, sync));
+        return fwd32(m, pi_batch_step_from(m->b32, s->dT, first, n, sync));
     }
     const HostGrid& g = m->hg;
     const size_t nf = (size_t)g.Nx * g.Ny;
-    for (int64_t i = 1; i <= s->iterations; ++i) {
+    for (int64_t i = first; i < first + n; ++i) {
         double tv = (time_offset & 1) ? (double)(i - 1) * s->dT : m->t;
         double tp = (time_offset & 2) ? (double)(i - 1) * s->dT : m->t;
         double tt = (time_offset & 4) ? (double)(i - 1) * s->dT : m->t;

@@ -85,3 +85,31 @@ def test_api_fp32_within_bounds(gpu_lib):
     assert model.iteration == STEPS
     check_errors(errors_vs_oracle(ref, model._native, SimpleNamespace(grid=grid, nsp=1)))
     sim.close()
+
+
+def test_simulation_with_output_writer(gpu_lib, tmp_path):
+    """update!(sim) with an output writer: a write_output! after every step (update.jl:30); the
+    last archived individuals equal the model's, the averaged diagnostics have the interior shape
+    and the species log has one line per step. The steps run one pi_sim_update_steps call each and
+    give the same state as a single update! call."""
+    from PlanktonIndividuals import PlanktonDiagnostics, PlanktonOutputWriter
+    from PlanktonIndividuals.output import read_archive
+    grid, model, sim, ref = _setup(np.float64)
+    w = PlanktonOutputWriter(dir=str(tmp_path / "out"), write_log=True, save_diags=True, save_phytoplankton=True,
+                             phytoplankton_include=("x", "y", "z", "Bm", "ac"))
+    sim.output_writer = w
+    sim.diags = PlanktonDiagnostics(model, tracer=("NO3",), phytoplankton=("num", "PS"), iteration_interval=5)
+    update_b(sim)
+    _drive_like_update(ref, sim, STEPS)
+    A = ref.get_individuals(0)
+    for k in A:
+        assert same(A[k], model.individuals.phytos.sp1.data[k]), k
+    ph = read_archive(w.phytoplankton_file)
+    for k in ("x", "y", "z", "Bm", "ac"):
+        assert same(ph[f"timeseries/sp1/{k}/{STEPS}"], A[k]), k
+    dg = read_archive(w.diags_file)
+    assert dg[f"timeseries/NO3/{STEPS}"].shape == (16, 16, 8)
+    assert f"timeseries/phyto/sp1/PS/{STEPS}" in dg and f"timeseries/PAR/5" in dg
+    lines = open(str(tmp_path / "out" / "dynamic_species001.txt")).read().splitlines()
+    assert len(lines) == STEPS
+    sim.close()
