@@ -31,7 +31,8 @@ Multi-GPU (config 2): the model domain is not partitioned; each rank runs an ind
 GPU parity tests show to be bit-identical to the CPU oracle: config 2 over --acc-steps steps
 (population counts every 100 steps, active-slot and cell mismatches, quota and position errors,
 interior tracer-mass errors), the same for config 3 with --workload config3, or, with --workload
-config5, --acc-boxes boxes over 2880 steps.
+config5, --acc-boxes boxes over 2880 steps, or with --workload config4 the first --acc-boxes
+ensemble members over 500 steps (per-member counts and tracer-mass errors).
 
 --impl reference times the reference algorithm's CPU implementation: the reference is Julia
 (absent here), so this is the CPU oracle (a Float64 restatement of TimeStep!) with all host
@@ -492,8 +493,8 @@ def run_accuracy(args):
     from PlanktonIndividuals import _lib, workloads as W
     lib = _lib.load()
     t0 = time.time()
-    if args.workload == "config5":
-        boxes = W.config5(n_max=args.acc_boxes)
+    if args.workload in ("config4", "config5"):
+        boxes = W.config5(n_max=args.acc_boxes) if args.workload == "config5" else W.config4(n_max=args.acc_boxes)
         steps = boxes[0].steps
         b = fp32_batch(boxes, steps)
         b.step(boxes[0].dT, steps)
@@ -510,8 +511,9 @@ def run_accuracy(args):
             lib.pi_sim_destroy(sim)
             mm.close()
         n0 = [wl.N[0] for wl in boxes]
-        return {"accuracy": "config5", "boxes": len(boxes), "steps": steps, "initial": n0, "fp32": c32, "fp64": c64,
-                "boxes_with_equal_counts": int(sum(int(a == c) for a, c in zip(c32, c64))),
+        return {"accuracy": args.workload, "members": len(boxes), "steps": steps, "initial": n0, "fp32": c32, "fp64": c64,
+                "members_with_equal_counts": int(sum(int(a == c) for a, c in zip(c32, c64))),
+                "max_tracer_mass_rel_err_per_member": [float(x) for x in mass],
                 "max_count_diff": int(max(abs(a - c) for a, c in zip(c32, c64))),
                 "mean_growth_factor": round(float(np.mean(np.array(c64) / np.array(n0))), 4),
                 "max_tracer_mass_rel_err": float(max(mass)),
