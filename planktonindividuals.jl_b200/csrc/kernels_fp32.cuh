@@ -468,6 +468,7 @@ __global__ void __launch_bounds__(256, 2) k32_move(MoveArgs a) {
 // For every interior cell holding individuals it also packs the environment physiology gathers
 // (find_NPT!, utils.jl:14-25: NH4, NO3, PO4, DOC, par, temperature, pop) into one 32-byte record,
 // so an individual reads one sector instead of seven.
+#define PAR_CH 8      // levels whose loads are issued together (the column walk is a latency chain)
 __global__ void k32_par(Tab32 T, const float* __restrict__ dzF, const BgcDev32* __restrict__ bgc,
                         unsigned long long* __restrict__ chl_acc, float* __restrict__ PARF,
                         float* __restrict__ par, float* __restrict__ diag_par, const float* __restrict__ tr,
@@ -486,31 +487,49 @@ __global__ void k32_par(Tab32 T, const float* __restrict__ dzF, const BgcDev32* 
         float parf = PARF[fcol];
         const long long c1 = m.cell_off + gid3(m, i + m.Hx, j + m.Hy, 1 + m.Hz);
         const long long slab = (long long)m.Gx * m.Gy;
-        // the loads of a level are issued one level ahead (only PARF carries down the column)
-        long long v_n = (long long)chl_acc[c1];
-        int pp_n = pop[c1];
-        float dp_n = diag_par[c1];
-        for (int k = 1; k <= m.Nz; ++k) {
-            const int kk = k + m.Hz;
-            const long long c = c1 + (k - 1) * slab;
-            const long long v = v_n;
-            const int pp = pp_n;
-            const float dp = dp_n;
-            if (k < m.Nz) { v_n = (long long)chl_acc[c + slab]; pp_n = pop[c + slab]; dp_n = diag_par[c + slab]; }
-            if (v) chl_acc[c] = 0ull;
-            const float chl = (float)((double)v * m.chl_unit);
-            const float dz = dzF[m.dz_off + kk - 1];
-            const float volk = m.dx * m.dy * dz;
-            const float atten = (chl / volk * kc + kw) * dz;
-            const float e = expf(-atten);
-            const float pv = parf * (1.0f - e) / atten;
-            par[c] = pv;
-            parf = parf * e;
-            diag_par[c] = dp + pv;
-            if (pp > 0) {
+        const float* __restrict__ temp = F[it.x].temp;
+        const float areaf = m.dx * m.dy;
+        for (int k0 = 1; k0 <= m.Nz; k0 += PAR_CH) {
+            // the loads of PAR_CH levels first (only PARF carries down the column)
+            long long v[PAR_CH];
+            int pp[PAR_CH];
+            float dp[PAR_CH], dz[PAR_CH];
+#pragma unroll
+            for (int e = 0; e < PAR_CH; ++e) {
+                const int k = k0 + e;
+                const long long c = c1 + (k - 1) * slab;
+                const bool in = k <= m.Nz;
+                v[e] = in ? (long long)chl_acc[c] : 0;
+                pp[e] = in ? pop[c] : 0;
+                dp[e] = in ? diag_par[c] : 0.0f;
+                dz[e] = in ? dzF[m.dz_off + k + m.Hz - 1] : 1.0f;
+            }
+            float pvs[PAR_CH];
+#pragma unroll
+            for (int e = 0; e < PAR_CH; ++e) {
+                const int k = k0 + e;
+                if (k > m.Nz) { pvs[e] = 0.0f; continue; }
+                const long long c = c1 + (k - 1) * slab;
+                if (v[e]) chl_acc[c] = 0ull;
+                const float chl = (float)((double)v[e] * m.chl_unit);
+                const float volk = areaf * dz[e];
+                const float atten = (chl / volk * kc + kw) * dz[e];
+                const float ex = expf(-atten);
+                const float pv = parf * (1.0f - ex) / atten;
+                par[c] = pv;
+                parf = parf * ex;
+                diag_par[c] = dp[e] + pv;
+                pvs[e] = pv;
+            }
+            // environment records of the occupied cells of these levels
+#pragma unroll
+            for (int e = 0; e < PAR_CH; ++e) {
+                const int k = k0 + e;
+                if (k > m.Nz || pp[e] <= 0) continue;
+                const long long c = c1 + (k - 1) * slab;
                 env[2 * c] = make_float4(tr[PI_NH4 * Gtot + c], tr[PI_NO3 * Gtot + c], tr[PI_PO4 * Gtot + c],
                                          tr[PI_DOC * Gtot + c]);
-                env[2 * c + 1] = make_float4(pv, F[it.x].temp[c - m.cell_off], (float)pp, 0.0f);
+                env[2 * c + 1] = make_float4(pvs[e], temp[c - m.cell_off], (float)pp[e], 0.0f);
             }
         }
         PARF[fcol] = parf;
