@@ -29,7 +29,6 @@
 // tracer-buffer parity and individual-buffer parity) and replayed. The results do not depend on block shapes, tile-per-block
 // assignment, tracer tile heights or z walk lengths (integer sums commute; every other value is computed by
 // exactly one thread from the same inputs), which lets the autotuner time real steps.
-#include <cub/device/device_scan.cuh>
 #include <cudaTypedefs.h>
 
 #include <algorithm>
@@ -137,8 +136,7 @@ struct pi_batch {
     unsigned long long* sort_bins = nullptr;    // nbins populations
     unsigned long long* sort_offs = nullptr;    // their exclusive scan, then the fill cursors
     long long nbins = 0;
-    char* sort_tmp = nullptr;
-    size_t sort_tmp_bytes = 0;
+    unsigned long long* sort_sums = nullptr;    // chunk sums of the bin scan
     int sort_interval = 32;         // steps between sorts; 0: never
     long long since_sort = 0;
     bool need_sort = true;
@@ -152,8 +150,6 @@ struct pi_batch {
     long long* line_off[3] = {nullptr, nullptr, nullptr};
     long long nlines[3] = {0, 0, 0};
     double last_dT = 0.0;
-    char* cub_tmp = nullptr;
-    size_t cub_bytes = 0;
     double* stage = nullptr;        // 3 × maxG doubles of upload staging (synchronous calls)
     cudaEvent_t copied = nullptr;   // recorded after a setter's host→device copies
     // forcing setters: host→device copies on their own stream into double-buffered staging, so
@@ -490,9 +486,8 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
                                                                                    b->env, b->errw); }
     { BScope sc(b, "k32_count_tiles");
       k32_count_tiles<<<nblk((long long)b->ntiles * 32, 256), 256, 0, s>>>(b->T, b->P, b->tile_cnt, b->errw); }
-    { BScope sc(b, "cub_scan_tiles");
-      size_t tb = b->cub_bytes;
-      BK(cub::DeviceScan::ExclusiveSum(b->cub_tmp, tb, b->tile_cnt, b->tile_off, b->ntiles, s), "scan tiles"); }
+    { BScope sc(b, "k32_scan_tiles");
+      k32_scan_tiles<<<std::min(b->nseg, 65535), 1024, 0, s>>>(b->T, b->tile_cnt, b->tile_off, b->nseg, b->errw); }
     { BScope sc(b, "k32_assign");
       k32_assign<<<nblk((long long)b->ntiles * 32, b->tune.bs_assign), b->tune.bs_assign, 0, s>>>(
           b->T, b->P, b->tile_cnt, b->tile_off, b->divlist, b->freelist, b->ndiv, b->st, b->errw); }
@@ -603,8 +598,10 @@ pi_status enqueue_sort(pi_batch* b) {
     { BScope sc(b, "k32_sort");
       BK(cudaMemsetAsync(b->sort_bins, 0, (size_t)b->nbins * sizeof(unsigned long long), s), "zero sort bins");
       k32_sort_count<<<tile_grid(b, 8), 256, 0, s>>>(b->T, P, b->sort_bins);
-      size_t tb = b->sort_tmp_bytes;
-      BK(cub::DeviceScan::ExclusiveSum(b->sort_tmp, tb, b->sort_bins, b->sort_offs, b->nbins, s), "scan sort bins");
+      const long long nch = (b->nbins + 1024 * SCAN_PER - 1) / (1024 * SCAN_PER);
+      k32_scan_sums<<<(unsigned)nch, 1024, 0, s>>>(b->sort_bins, b->nbins, b->sort_sums);
+      k32_scan_chunks<<<1, 1024, 0, s>>>(b->sort_sums, nch);
+      k32_scan_apply<<<(unsigned)nch, 1024, 0, s>>>(b->sort_bins, b->nbins, b->sort_sums, b->sort_offs);
       k32_sort_scatter<<<tile_grid(b, 8), 256, 0, s>>>(b->T, P, Q, b->sort_offs);
       BK(cudaGetLastError(), "sort launch"); }
     b->pcur ^= 1;
@@ -819,15 +816,8 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     b->vel1_pending.assign(nmembers, 0);
     b->vel0_buf.assign(nmembers, 0);
     BA(b->partial, 3 * 1024); BA(b->scratch, 4);
-    size_t cb = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, cb, b->tile_cnt, b->tile_off, b->ntiles, b->stream);
-    b->cub_bytes = cb;
-    BA(b->cub_tmp, cb);
     BA(b->tmaps, 2 * (size_t)nmembers * sizeof(CUtensorMap));
-    cb = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, cb, b->sort_bins, b->sort_offs, b->nbins, b->stream);
-    b->sort_tmp_bytes = cb;
-    BA(b->sort_tmp, cb);
+    BA(b->sort_sums, (b->nbins + 1024 * SCAN_PER - 1) / (1024 * SCAN_PER));
 #undef BA
     // series and forcing tables
     b->serh.assign(nmembers, MemberSeries{});

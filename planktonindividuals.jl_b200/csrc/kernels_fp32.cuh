@@ -560,6 +560,106 @@ __global__ void k32_count_tiles(Tab32 T, IndDev32 P, unsigned long long* __restr
     }
 }
 
+// ---- exclusive prefix sums of 64-bit counts (block-wide, 1024 threads) ----------------------
+// inclusive scan over the lanes of a warp
+__device__ __forceinline__ unsigned long long warp_inscan64(unsigned long long x) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    return x;
+}
+// Exclusive scan of v over the block (blockDim.x == 1024); returns the thread's prefix and the
+// block total in *total. sh holds 33 values.
+__device__ __forceinline__ unsigned long long block_exscan64(unsigned long long v, unsigned long long* sh,
+                                                             unsigned long long* total) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const unsigned long long inc = warp_inscan64(v);
+    if (lane == 31) sh[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+        const unsigned long long w = sh[lane];
+        const unsigned long long wi = warp_inscan64(w);
+        sh[lane] = wi - w;
+        if (lane == 31) sh[32] = wi;
+    }
+    __syncthreads();
+    const unsigned long long out = sh[wid] + inc - v;
+    *total = sh[32];
+    __syncthreads();
+    return out;
+}
+
+// Exclusive scan of the tile counts within each (member, species) segment: one block of 1024
+// threads per segment.
+__global__ void __launch_bounds__(1024) k32_scan_tiles(Tab32 T, const unsigned long long* __restrict__ tile_cnt,
+                                                       unsigned long long* __restrict__ tile_off, int nseg,
+                                                       const uint32_t* err) {
+    if (stopped(err)) return;
+    __shared__ unsigned long long sh[33];
+    for (int seg = blockIdx.x; seg < nseg; seg += gridDim.x) {
+        const int t0 = T.seg_tile0[seg], t1 = T.seg_tile0[seg + 1];
+        unsigned long long run = 0;
+        for (int base = t0; base < t1; base += 1024) {
+            const int t = base + threadIdx.x;
+            const unsigned long long v = t < t1 ? tile_cnt[t] : 0ull;
+            unsigned long long tot;
+            const unsigned long long ex = block_exscan64(v, sh, &tot);
+            if (t < t1) tile_off[t] = run + ex;
+            run += tot;
+        }
+    }
+}
+
+// Exclusive scan of n 64-bit values in three passes (chunks of 1024 × PER values): chunk sums,
+// a scan of the chunk sums in one block, then each chunk's scan from its offset.
+#define SCAN_PER 8
+__global__ void __launch_bounds__(1024) k32_scan_sums(const unsigned long long* __restrict__ in, long long n,
+                                                      unsigned long long* __restrict__ sums) {
+    __shared__ unsigned long long sh[33];
+    const long long base = (long long)blockIdx.x * 1024 * SCAN_PER;
+    unsigned long long v = 0;
+    for (int e = 0; e < SCAN_PER; ++e) {
+        const long long q = base + (long long)e * 1024 + threadIdx.x;
+        if (q < n) v += in[q];
+    }
+    unsigned long long tot;
+    block_exscan64(v, sh, &tot);
+    if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+__global__ void __launch_bounds__(1024) k32_scan_chunks(unsigned long long* __restrict__ sums, long long nchunks) {
+    __shared__ unsigned long long sh[33];
+    unsigned long long run = 0;
+    for (long long b = 0; b < nchunks; b += 1024) {
+        const long long q = b + threadIdx.x;
+        const unsigned long long v = q < nchunks ? sums[q] : 0ull;
+        unsigned long long tot;
+        const unsigned long long ex = block_exscan64(v, sh, &tot);
+        if (q < nchunks) sums[q] = run + ex;
+        run += tot;
+    }
+}
+__global__ void __launch_bounds__(1024) k32_scan_apply(const unsigned long long* __restrict__ in, long long n,
+                                                       const unsigned long long* __restrict__ sums,
+                                                       unsigned long long* __restrict__ out) {
+    __shared__ unsigned long long sh[33];
+    const long long base = (long long)blockIdx.x * 1024 * SCAN_PER;
+    // each thread takes PER consecutive values so that the chunk is scanned in order
+    const long long q0 = base + (long long)threadIdx.x * SCAN_PER;
+    unsigned long long loc[SCAN_PER], v = 0;
+#pragma unroll
+    for (int e = 0; e < SCAN_PER; ++e) { loc[e] = q0 + e < n ? in[q0 + e] : 0ull; v += loc[e]; }
+    unsigned long long tot;
+    unsigned long long run = sums[blockIdx.x] + block_exscan64(v, sh, &tot);
+#pragma unroll
+    for (int e = 0; e < SCAN_PER; ++e) {
+        if (q0 + e < n) out[q0 + e] = run;
+        run += loc[e];
+    }
+}
+
 // exclusive prefix sum over the lanes of a warp
 __device__ __forceinline__ unsigned warp_exscan(unsigned v) {
     const int lane = threadIdx.x & 31;
