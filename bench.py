@@ -342,7 +342,8 @@ def run_e2e(wl, args, lib, precision, inputs="f32"):
     h2d = sum(x.nbytes for x in vel_p[0]) + par_p[0].nbytes + tmp_p[0].nbytes
     counts = torch.zeros((args.e2e_steps + 1) * wl.nsp, dtype=torch.int64, pin_memory=True)
     cbase = counts.data_ptr()
-    ptr = lambda a: ct.c_void_p(a.ctypes.data)
+    ptr = ((lambda a: ct.c_void_p(a.ctypes.data)) if inputs == "f32"
+           else (lambda a: a.ctypes.data_as(ct.POINTER(ct.c_double))))
     sfx = "_f32" if inputs == "f32" else ""
     set_vel, set_par, set_tmp = (getattr(m.lib, f"pi_set_{k}{sfx}") for k in ("velocity", "PARF", "temp"))
 
@@ -441,12 +442,18 @@ def run_ours(args):
         Vall = float(tv.item())
     value = ind_all / (t_max / 1e3)
     cell_steps = K * Vall / (t_max / 1e3)
+    print(f"[bench] fp32 {t_max / K:.4f} ms/step, {value:.4g} {UNIT}; kernels (ms/step): "
+          + json.dumps({k: round(v[1] / max(args.profile_steps, 1), 4)
+                        for k, v in sorted(r32['prof'].items(), key=lambda kv: -kv[1][1])[:14]}),
+          file=sys.stderr, flush=True)
     fp64 = e2e = None
     if args.workload in ("config2", "config3"):
         if args.fp64_steps > 0:
             fp64 = run_fp64(members[0], args, lib)
+            print(f"[bench] fp64 {fp64['ms_per_step']} ms/step", file=sys.stderr, flush=True)
         if args.e2e_steps > 0:
             e2e = run_e2e(members[0], args, lib, _abi.PI_FP32, "f32")
+            print(f"[bench] e2e {e2e['ms_per_step']} ms/step", file=sys.stderr, flush=True)
             e2e["float64_inputs"] = {k: v for k, v in run_e2e(members[0], args, lib, _abi.PI_FP32, "f64").items()
                                      if k in ("value", "ms_per_step", "wall_ms_per_step", "h2d_bytes_per_step")}
     out = None

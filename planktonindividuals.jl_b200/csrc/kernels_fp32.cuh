@@ -1002,21 +1002,42 @@ __global__ void __launch_bounds__(256, 4) k32_physiology(PhysArgs a) {
 // near zero are exact. The downwind term of the reference multiplies a zero transport and is
 // dropped.
 // ------------------------------------------------------------------------------------------
+//
+// Every product and sum of the tracer update is written with an explicit rounding intrinsic
+// (__fmul_rn, __fadd_rn, __fsub_rn, and __fmaf_rn where a fused multiply-add is chosen), so the
+// compiler contracts nothing on its own: the kernels that evaluate these formulas (k32_xy and
+// k32_ztail, and the fused k32_tracer) give the same bits in whatever code they are inlined into.
 struct FCu { float tr, d0c, d1c, R; };
 
 __device__ __forceinline__ FCu fcu(float vel, float area, float rdxc, float dT) {
     FCu f;
-    const float cfl = fabsf(vel * dT * rdxc);
-    f.tr = area * vel;
-    f.d0c = (2.0f - cfl) * (1.0f - cfl) * (1.0f / 6.0f);
-    f.d1c = (1.0f - cfl * cfl) * (1.0f / 6.0f);
-    f.R = __fdividef(1.0f - cfl, cfl + EPS20_F);
+    const float cfl = fabsf(__fmul_rn(__fmul_rn(vel, dT), rdxc));
+    f.tr = __fmul_rn(area, vel);
+    f.d0c = __fmul_rn(__fmul_rn(__fsub_rn(2.0f, cfl), __fsub_rn(1.0f, cfl)), 1.0f / 6.0f);
+    f.d1c = __fmul_rn(__fmaf_rn(-cfl, cfl, 1.0f), 1.0f / 6.0f);
+    f.R = __fdividef(__fsub_rn(1.0f, cfl), __fadd_rn(cfl, EPS20_F));
     return f;
 }
 __device__ __forceinline__ float psid0(float d0, float dn, const FCu& f) {
-    const float a = f.d0c * d0 + f.d1c * dn, b = f.R * dn;
+    const float a = __fmaf_rn(f.d0c, d0, __fmul_rn(f.d1c, dn)), b = __fmul_rn(f.R, dn);
     return d0 >= 0.0f ? fmaxf(0.0f, fminf(fminf(d0, a), b)) : fminf(0.0f, fmaxf(fmaxf(d0, a), b));
 }
+// one sweep's update v − dtv·(ΔF − c·ftr) (multi_dim_adv.jl:111-135)
+__device__ __forceinline__ float upd_sweep(float v, float dtv, float dF, float c, float ftr) {
+    return __fmaf_rn(-dtv, __fmaf_rn(-c, ftr, dF), v);
+}
+// a·x1 − a·x0: the transport difference of a cell's two faces
+__device__ __forceinline__ float tdiff(float a, float x1, float x0) { return __fmaf_rn(a, x1, -__fmul_rn(a, x0)); }
+// tracer_forcing! of a nutrient tracer on max(0, ·): G + (aS·T + aO·T_partner)
+__device__ __forceinline__ float add_forcing(float G, float aS, float own, float aO, float partner) {
+    return __fadd_rn(G, __fmaf_rn(aS, fmaxf(0.0f, own), __fmul_rn(aO, fmaxf(0.0f, partner))));
+}
+// tracer_sinking!: G + (ws·T_above − ws·T)·ΔT/ΔzC
+__device__ __forceinline__ float add_sinking(float G, float fup, float fdn, float sk) {
+    return __fmaf_rn(__fsub_rn(fup, fdn), sk, G);
+}
+// the new tracer value T + (G + particle term) (apply_tendency!)
+__device__ __forceinline__ float tendency(float c, float G, float plk) { return __fadd_rn(c, __fadd_rn(G, plk)); }
 // landmask product of a difference (δ·mask_a·mask_b); LM = false: every cell is water
 template <bool LM>
 __device__ __forceinline__ float mk(float x, int ma, int mb) { return LM ? mulbf(mulbf(x, ma), mb) : x; }
@@ -1026,21 +1047,21 @@ __device__ __forceinline__ float mk(float x, int ma, int mb) { return LM ? mulbf
 template <bool LM>
 __device__ __forceinline__ float flux_h(const FCu& f, float cm2, float cm1, float c0, float cp1,
                                         int lm2, int lm1, int l0, int lp1) {
-    const float d0 = mk<LM>(c0 - cm1, l0, lm1);
+    const float d0 = mk<LM>(__fsub_rn(c0, cm1), l0, lm1);
     const bool pos = f.tr > 0.0f;
-    const float dn = pos ? mk<LM>(cm1 - cm2, lm1, lm2) : mk<LM>(cp1 - c0, lp1, l0);
+    const float dn = pos ? mk<LM>(__fsub_rn(cm1, cm2), lm1, lm2) : mk<LM>(__fsub_rn(cp1, c0), lp1, l0);
     const float ps = psid0(d0, dn, f);
-    return f.tr * (pos ? cm1 + ps : c0 - ps);
+    return __fmul_rn(f.tr, pos ? __fadd_rn(cm1, ps) : __fsub_rn(c0, ps));
 }
 // adv_flux_z at face k from c[k-2], c[k-1], c[k], c[k+1] (the index grows downward)
 template <bool LM>
 __device__ __forceinline__ float flux_v(const FCu& f, float cm2, float cm1, float c0, float cp1,
                                         int lm2, int lm1, int l0, int lp1) {
-    const float d0 = mk<LM>(cm1 - c0, l0, lm1);
+    const float d0 = mk<LM>(__fsub_rn(cm1, c0), l0, lm1);
     const bool pos = f.tr > 0.0f;
-    const float dn = pos ? mk<LM>(c0 - cp1, lp1, l0) : mk<LM>(cm2 - cm1, lm1, lm2);
+    const float dn = pos ? mk<LM>(__fsub_rn(c0, cp1), lp1, l0) : mk<LM>(__fsub_rn(cm2, cm1), lm1, lm2);
     const float ps = psid0(d0, dn, f);
-    return f.tr * (pos ? c0 + ps : cm1 - ps);
+    return __fmul_rn(f.tr, pos ? __fadd_rn(c0, ps) : __fsub_rn(cm1, ps));
 }
 __device__ __forceinline__ int wrap_ax(int a, int N, int H, int topo) {
     if (topo == PI_PERIODIC) { while (a < H + 1) a += N; while (a > N + H) a -= N; return a; }
@@ -1119,16 +1140,16 @@ __device__ __forceinline__ void xy_tile(const TrArgs& a, const MemberDev& m, con
     const long long off = m.cell_off;
     const MemberForcing& F = a.F[it.x];
     const float dz = a.dzF[m.dz_off + L - 1];
-    const float az = m.dx * m.dy, dtv = dT / (az * dz);
+    const float az = __fmul_rn(m.dx, m.dy), dtv = __fdiv_rn(dT, __fmul_rn(az, dz));
     // ---- x sweep of row j0-2+wid
     {
         const int jj = wrap_ax(j0 - 2 + wid, m.Ny, m.Hy, m.ty);
         const int i = i0 - 2 + lane;
         const int ic = min(i, m.Gx);
-        const float ax = m.dy * dz;
+        const float ax = __fmul_rn(m.dy, dz);
         const float uw = pu;
         const float ue = __shfl_down_sync(0xffffffffu, uw, 1);
-        const FCu fc = fcu(uw, ax, 1.0f / m.dx, dT);
+        const FCu fc = fcu(uw, ax, __frcp_rn(m.dx), dT);
         int l0 = 1, lm1 = 1, lm2 = 1, lp1 = 1;
         if (LM) {
             l0 = lm32(m, a.lm, ic, jj, L);
@@ -1136,7 +1157,7 @@ __device__ __forceinline__ void xy_tile(const TrArgs& a, const MemberDev& m, con
             lp1 = __shfl_down_sync(0xffffffffu, l0, 1);
         }
         const bool east_zero = i == m.Nx + m.Hx && m.tx != PI_PERIODIC;   // fill_halo_east_Gc! (Bounded)
-        const float ftr = mk<LM>(ax * ue - ax * uw, lp1, l0);
+        const float ftr = mk<LM>(tdiff(ax, ue, uw), lp1, l0);
         const bool store_tr = wid >= 2 && wid < TY + 2;
 #pragma unroll
         for (int n = 0; n < PI_NTRACERS; ++n) {
@@ -1146,7 +1167,7 @@ __device__ __forceinline__ void xy_tile(const TrArgs& a, const MemberDev& m, con
             const float Fw = flux_h<LM>(fc, cm2, cm1, v, cp1, lm2, lm1, l0, lp1);
             float Fe = __shfl_down_sync(0xffffffffu, Fw, 1);
             if (east_zero) Fe = 0.0f;
-            at(TA, wid, n, lane) = v - dtv * (mk<LM>(Fe - Fw, lp1, l0) - v * ftr);
+            at(TA, wid, n, lane) = upd_sweep(v, dtv, mk<LM>(__fsub_rn(Fe, Fw), lp1, l0), v, ftr);
             if (store_tr) at(TRs, wid - 2, n, lane) = v;
         }
     }
@@ -1156,7 +1177,7 @@ __device__ __forceinline__ void xy_tile(const TrArgs& a, const MemberDev& m, con
     // ---- y faces j0 + r, r = 0..TY
     const int i = i0 - 2 + lane;
     const bool col = lane >= 2 && lane < 30 && i <= m.Nx + m.Hx;
-    const float ay = m.dx * dz;
+    const float ay = __fmul_rn(m.dx, dz);
     const float* vv = F.vel1[1];
     if (wid <= TY) {
         const int r = wid, f = j0 + r;
@@ -1164,7 +1185,7 @@ __device__ __forceinline__ void xy_tile(const TrArgs& a, const MemberDev& m, con
         const bool zero = !col || f > m.Ny + m.Hy + 1 || (special && m.ty != PI_PERIODIC);
         const int fs = special ? m.Hy + 1 : min(f, m.Ny + m.Hy);
         const int ic = min(i, m.Gx);
-        const FCu fc = fcu(zero ? 0.0f : vv[gid3(m, ic, fs, L)], ay, 1.0f / m.dy, dT);
+        const FCu fc = fcu(zero ? 0.0f : vv[gid3(m, ic, fs, L)], ay, __frcp_rn(m.dy), dT);
         int L2 = 1, L1 = 1, L0 = 1, Lp = 1;
         if (LM) {
             L2 = lm32(m, a.lm, ic, fs - 2, L); L1 = lm32(m, a.lm, ic, fs - 1, L);
@@ -1182,12 +1203,12 @@ __device__ __forceinline__ void xy_tile(const TrArgs& a, const MemberDev& m, con
         if (col && j <= m.Ny + m.Hy) {
             const int q = gid3(m, i, j, L);
             const int c0m = LM ? lm32(m, a.lm, i, j, L) : 1, cpm = LM ? lm32(m, a.lm, i, j + 1, L) : 1;
-            const float ftr = mk<LM>(ay * vv[q + m.Gx] - ay * vv[q], cpm, c0m);
+            const float ftr = mk<LM>(tdiff(ay, vv[q + m.Gx], vv[q]), cpm, c0m);
             float* dst = a.tb + off + q;
 #pragma unroll
             for (int n = 0; n < PI_NTRACERS; ++n) {
-                const float dG = mk<LM>(at(FY, wid + 1, n, lane) - at(FY, wid, n, lane), cpm, c0m);
-                dst[n * G] = at(TA, wid + 2, n, lane) - dtv * (dG - at(TRs, wid, n, lane) * ftr);
+                const float dG = mk<LM>(__fsub_rn(at(FY, wid + 1, n, lane), at(FY, wid, n, lane)), cpm, c0m);
+                dst[n * G] = upd_sweep(at(TA, wid + 2, n, lane), dtv, dG, at(TRs, wid, n, lane), ftr);
             }
         }
     }
@@ -1236,10 +1257,15 @@ __device__ __forceinline__ FeCoef fe_coef(const BgcDev32& b, float dT) {
     return c;
 }
 __device__ __forceinline__ float fe_forcing(int n, const FeCoef& c, float dfe, float poc, float dust, float pfeb, float pfei) {
-    const float fe = fmaxf(dfe - c.lig, 0.0f) * dfe * c.fefe;
-    if (n == PI_DFe) return pfeb * c.kpoc - (c.lpoc * poc + c.lmin + c.ldust * dust) * dfe * c.frac + pfei * c.kdiss - fe;
-    if (n == PI_PFe_bio) return poc * dfe * c.frac_poc - pfeb * c.kpoc;
-    return -pfei * c.kdiss + (c.lmin + c.ldust * dust) * dfe * c.frac + fe;
+    const float fe = __fmul_rn(__fmul_rn(fmaxf(__fsub_rn(dfe, c.lig), 0.0f), dfe), c.fefe);
+    const float bio = __fmul_rn(pfeb, c.kpoc), diss = __fmul_rn(pfei, c.kdiss);
+    if (n == PI_DFe) {
+        const float scav = __fadd_rn(__fadd_rn(__fmul_rn(c.lpoc, poc), c.lmin), __fmul_rn(c.ldust, dust));
+        return __fsub_rn(__fadd_rn(__fsub_rn(bio, __fmul_rn(__fmul_rn(scav, dfe), c.frac)), diss), fe);
+    }
+    if (n == PI_PFe_bio) return __fsub_rn(__fmul_rn(__fmul_rn(poc, dfe), c.frac_poc), bio);
+    const float scav = __fadd_rn(c.lmin, __fmul_rn(c.ldust, dust));
+    return __fadd_rn(__fadd_rn(-diss, __fmul_rn(__fmul_rn(scav, dfe), c.frac)), fe);
 }
 
 // Asynchronous global → shared copies (cp.async): a warp's z walk reads the inputs of each level
@@ -1381,7 +1407,7 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& md, con
         const int l1 = mm1, l0 = mm2;                       // land mask of cell k and k+1
         const float Fb = flux_v<LM>(fcz(l + 1), w0, w1, w2, w3, mm0, mm1, mm2, mm3);   // zero at the bottom
         const ZLev L = sLev[l];
-        float Gc = (w1 - L.dtv * (mk<LM>(Ft - Fb, l0, l1) - cc * sFtr[l * 32 + lane])) - cc;
+        float Gc = __fsub_rn(upd_sweep(w1, L.dtv, mk<LM>(__fsub_rn(Ft, Fb), l0, l1), cc, sFtr[l * 32 + lane]), cc);
         Ft = Fb;
         if (GEN) {
             // tracer_diffusion! (tracer_diffusion.jl:1-21)
@@ -1401,13 +1427,13 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& md, con
         }
         if (NUT) {
             // tracer_forcing! (tracer_forcings.jl:2-50) on max(0, tracer)
-            Gc += aS * fmaxf(0.0f, cc) + aO * fmaxf(0.0f, lds_f32(rc + 1024u + so));
+            Gc = add_forcing(Gc, aS, cc, aO, lds_f32(rc + 1024u + so));
         } else {
             // tracer_sinking! (tracer_sinking.jl:1-42)
             if (sinks) {
-                const float fup = (k - 1 <= Hz) ? 0.0f : ws * sink_prev;
-                const float fdn = (k >= bot) ? 0.0f : ws * cc;
-                Gc += (fup - fdn) * L.sk;
+                const float fup = (k - 1 <= Hz) ? 0.0f : __fmul_rn(ws, sink_prev);
+                const float fdn = (k >= bot) ? 0.0f : __fmul_rn(ws, cc);
+                Gc = add_sinking(Gc, fup, fdn, L.sk);
                 sink_prev = cc;
             }
             if (n != PI_Dust) {
@@ -1438,7 +1464,7 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& md, con
             const long long vv = (long long)lds_u64(ra + 2u * so);   // zero where the cell holds no individual
             if (vv) { acc[q] = 0ull; plk = (float)((double)vv * L.fxv); }
         }
-        out[q] = cc + (Gc + plk);
+        out[q] = tendency(cc, Gc, plk);
     }
     cpa_wait<0>();
 }
@@ -1480,7 +1506,7 @@ __global__ void __launch_bounds__(32 * PI_NTRACERS, 2) k32_ztail(TrArgs a) {
         const MemberDev& m = a.T.md[it.x];
         const int k0 = it.w, bot = m.Nz + m.Hz;
         const float* wv = a.F[it.x].vel1[2];
-        const float az = m.dx * m.dy;
+        const float az = __fmul_rn(m.dx, m.dy);
         for (int e = tid; e < (LZ + 1) * 32; e += 32 * PI_NTRACERS) {
             const int f = k0 + e / 32, i = it.y + (e & 31);
             const bool col = i <= m.Nx + m.Hx;
@@ -1491,7 +1517,7 @@ __global__ void __launch_bounds__(32 * PI_NTRACERS, 2) k32_ztail(TrArgs a) {
                 const FCu c = fcu(wt, az, a.rdzC[m.dz_off + f - 1], a.dT);
                 fc = make_float4(c.tr, c.d0c, c.d1c, c.R);
                 if (e < LZ * 32) {                            // cell f: w at its top and bottom faces
-                    const float ftr = az * wt - az * wv[q + m.Gx * m.Gy];
+                    const float ftr = tdiff(az, wt, wv[q + m.Gx * m.Gy]);
                     sFtr[e] = m.all_water ? ftr : mulbf(mulbf(ftr, lm32(m, a.lm, i, it.z, f + 1)), lm32(m, a.lm, i, it.z, f));
                     sPop[e] = a.pop[m.cell_off + q];
                 }
@@ -1505,9 +1531,9 @@ __global__ void __launch_bounds__(32 * PI_NTRACERS, 2) k32_ztail(TrArgs a) {
             const int k = k0 + tid;
             ZLev L = {0.0f, 0.0f, 1.0f, 1.0f, 0.0};
             if (k <= bot) {
-                const float dz = a.dzF[m.dz_off + k - 1], volk = az * dz;
-                L.dtv = a.dT / volk;
-                L.sk = a.dT / a.dzC[m.dz_off + k - m.Hz - 1];
+                const float dz = a.dzF[m.dz_off + k - 1], volk = __fmul_rn(az, dz);
+                L.dtv = __fdiv_rn(a.dT, volk);
+                L.sk = __fdiv_rn(a.dT, a.dzC[m.dz_off + k - m.Hz - 1]);
                 L.dz = dz;
                 L.dzn = a.dzF[m.dz_off + k];
                 L.fxv = m.fx_unit / (double)volk;

@@ -170,7 +170,7 @@ __device__ __forceinline__ void trk_body(const TrkArgs& A, const MemberDev& md, 
     const long long G = a.Gtot, off = md.cell_off;
     const int slab = Gx * Gy;
     const float dT = a.dT;
-    const float dx = md.dx, dy = md.dy, az = dx * dy;
+    const float dx = md.dx, dy = md.dy, az = __fmul_rn(dx, dy);
     const bool tma = A.maps != nullptr && (Gx & 3) == 0;
     const void* map = tma ? (const void*)(A.maps + 128 * it.x) : nullptr;
     const MemberForcing& F = a.F[it.x];
@@ -187,9 +187,9 @@ __device__ __forceinline__ void trk_body(const TrkArgs& A, const MemberDev& md, 
     for (int e = threadIdx.x; e <= k1 - Ls; e += TRK_THREADS) {
         const int k = Ls + e;
         ZLev Lv;
-        const float dz = a.dzF[md.dz_off + k - 1], volk = az * dz;
-        Lv.dtv = a.dT / volk;
-        Lv.sk = a.dT / a.dzC[md.dz_off + k - Hz - 1];
+        const float dz = a.dzF[md.dz_off + k - 1], volk = __fmul_rn(az, dz);
+        Lv.dtv = __fdiv_rn(a.dT, volk);
+        Lv.sk = __fdiv_rn(a.dT, a.dzC[md.dz_off + k - Hz - 1]);
         Lv.dz = dz;
         Lv.dzn = a.dzF[md.dz_off + k];
         Lv.fxv = md.fx_unit / (double)volk;
@@ -259,21 +259,21 @@ __device__ __forceinline__ void trk_body(const TrkArgs& A, const MemberDev& md, 
             waited = L;
             const float* R = ring + (size_t)b * TRK_NG * TRK_R * TRK_W;
             const float dz = a.dzF[md.dz_off + L - 1];
-            const float dtv = dT / (az * dz);
+            const float dtv = __fdiv_rn(dT, __fmul_rn(az, dz));
             // ---- x sweep of rows wid and wid + 8 (rows j0-2 .. j0+9)
-            const float ax = dy * dz;
+            const float ax = __fmul_rn(dy, dz);
             for (int r = wid; r < TRK_R; r += TRK_TY) {
                 const int jj = wrap_ax(j0 - 2 + r, Ny, Hy, md.ty);
                 const float uw = uu[gid3(md, ic, jj, L)];
                 const float ue = __shfl_down_sync(0xffffffffu, uw, 1);
-                const FCu fc = fcu(uw, ax, 1.0f / dx, dT);
+                const FCu fc = fcu(uw, ax, __frcp_rn(dx), dT);
                 int l0 = 1, lm1 = 1, lm2 = 1, lp1 = 1;
                 if (LM) {
                     l0 = lmq(ic, jj, L); lm1 = lmq(max(i - 1, 1), jj, L); lm2 = lmq(max(i - 2, 1), jj, L);
                     lp1 = lmq(min(i + 1, Gx), jj, L);
                 }
                 const bool east_zero = i == Nx + Hx && md.tx != PI_PERIODIC;
-                const float ftr = mk<LM>(ax * ue - ax * uw, lp1, l0);
+                const float ftr = mk<LM>(tdiff(ax, ue, uw), lp1, l0);
 #pragma unroll
                 for (int q = 0; q < TRK_NG; ++q) {
                     const float* cr = R + (q * TRK_R + r) * TRK_W + xo + lane;
@@ -281,18 +281,18 @@ __device__ __forceinline__ void trk_body(const TrkArgs& A, const MemberDev& md, 
                     const float Fw = flux_h<LM>(fc, cm2, cm1, v, cp1, lm2, lm1, l0, lp1);
                     float Fe = __shfl_down_sync(0xffffffffu, Fw, 1);
                     if (east_zero) Fe = 0.0f;
-                    TA[(r * TRK_NG + q) * 32 + lane] = v - dtv * (mk<LM>(Fe - Fw, lp1, l0) - v * ftr);
+                    TA[(r * TRK_NG + q) * 32 + lane] = upd_sweep(v, dtv, mk<LM>(__fsub_rn(Fe, Fw), lp1, l0), v, ftr);
                 }
             }
             __syncthreads();
             // ---- y faces j0 + f, f = 0 .. 8 (warp w: face w + 1; warp 0 also face 0)
-            const float ay = dx * dz;
+            const float ay = __fmul_rn(dx, dz);
             for (int f = (wid == 0 ? 0 : wid + 1); f <= wid + 1; ++f) {
                 const int fj = j0 + f;
                 const bool special = fj == Ny + Hy + 1;
                 const bool zero = !col || fj > Ny + Hy + 1 || (special && md.ty != PI_PERIODIC);
                 const int fs = special ? Hy + 1 : min(fj, Ny + Hy);
-                const FCu fc = fcu(zero ? 0.0f : vv[gid3(md, ic, fs, L)], ay, 1.0f / dy, dT);
+                const FCu fc = fcu(zero ? 0.0f : vv[gid3(md, ic, fs, L)], ay, __frcp_rn(dy), dT);
                 int L2 = 1, L1 = 1, L0 = 1, Lp = 1;
                 if (LM) { L2 = lmq(ic, fs - 2, L); L1 = lmq(ic, fs - 1, L); L0 = lmq(ic, fs, L); Lp = lmq(ic, fs + 1, L); }
 #pragma unroll
@@ -307,12 +307,12 @@ __device__ __forceinline__ void trk_body(const TrkArgs& A, const MemberDev& md, 
             if (own) {
                 const int qq = gid3(md, i, j, L);
                 const int c0m = LM ? lmq(i, j, L) : 1, cpm = LM ? lmq(i, j + 1, L) : 1;
-                const float ftr = mk<LM>(ay * vv[qq + Gx] - ay * vv[qq], cpm, c0m);
+                const float ftr = mk<LM>(tdiff(ay, vv[qq + Gx], vv[qq]), cpm, c0m);
 #pragma unroll
                 for (int q = 0; q < TRK_NG; ++q) {
-                    const float dG = mk<LM>(FY[((wid + 1) * TRK_NG + q) * 32 + lane] - FY[(wid * TRK_NG + q) * 32 + lane], cpm, c0m);
+                    const float dG = mk<LM>(__fsub_rn(FY[((wid + 1) * TRK_NG + q) * 32 + lane], FY[(wid * TRK_NG + q) * 32 + lane]), cpm, c0m);
                     const float trs = R[(q * TRK_R + wid + 2) * TRK_W + xo + lane + 2];
-                    tbn[q] = TA[((wid + 2) * TRK_NG + q) * 32 + lane] - dtv * (dG - trs * ftr);
+                    tbn[q] = upd_sweep(TA[((wid + 2) * TRK_NG + q) * 32 + lane], dtv, dG, trs, ftr);
                 }
             }
         }
@@ -335,7 +335,7 @@ __device__ __forceinline__ void trk_body(const TrkArgs& A, const MemberDev& md, 
         if (fin) {
             const ZLev Z = sLev[k - Ls];
             const int l1 = mm1, l0 = mm2;                       // land mask of cell k and k+1
-            const float ftr = LM ? mulbf(mulbf(az * wprev - az * wf, mm2), mm1) : az * wprev - az * wf;
+            const float ftr = LM ? mulbf(mulbf(tdiff(az, wprev, wf), mm2), mm1) : tdiff(az, wprev, wf);
             const float dfe = GRP == 1 ? fmaxf(0.0f, cc[trk_slot(1, PI_DFe)]) : 0.0f;
             const long long qo = off + qk;
             const int nix = halo_count(i, Nx, Hx, md.tx), njy = halo_count(j, Ny, Hy, md.ty);
@@ -343,7 +343,7 @@ __device__ __forceinline__ void trk_body(const TrkArgs& A, const MemberDev& md, 
 #pragma unroll
             for (int q = 0; q < TRK_NG; ++q) {
                 const int n = trk_tracer(GRP, q);
-                float Gc = (tw[q][1] - Z.dtv * (mk<LM>(Ft[q] - Fb[q], l0, l1) - cc[q] * ftr)) - cc[q];
+                float Gc = __fsub_rn(upd_sweep(tw[q][1], Z.dtv, mk<LM>(__fsub_rn(Ft[q], Fb[q]), l0, l1), cc[q], ftr), cc[q]);
                 const int as = acc_slot(n);
                 if (as >= 0) {
                     // tracer_forcing! on max(0, tracer): aS·T(n) + aO·T(partner), the partner in the
@@ -363,14 +363,14 @@ __device__ __forceinline__ void trk_body(const TrkArgs& A, const MemberDev& md, 
                         case PI_POP: aS = -bg.kPOP * dT; break;
                         default: break;
                     }
-                    Gc += aS * fmaxf(0.0f, cc[q]) + aO * fmaxf(0.0f, po >= 0 ? cc[po] : 0.0f);
+                    Gc = add_forcing(Gc, aS, cc[q], aO, po >= 0 ? cc[po] : 0.0f);
                 } else {
                     // tracer_sinking! and the iron forcing
                     if (n != PI_DFe) {
                         const float ws = n == PI_PFe_bio ? wso : wsi;
-                        const float fup = (k - 1 <= Hz) ? 0.0f : ws * ccp[q];
-                        const float fdn = (k >= bot) ? 0.0f : ws * cc[q];
-                        Gc += (fup - fdn) * Z.sk;
+                        const float fup = (k - 1 <= Hz) ? 0.0f : __fmul_rn(ws, ccp[q]);
+                        const float fdn = (k >= bot) ? 0.0f : __fmul_rn(ws, cc[q]);
+                        Gc = add_sinking(Gc, fup, fdn, Z.sk);
                     }
                     if (n != PI_Dust) {
                         const float pfi = fmaxf(0.0f, cc[trk_slot(1, PI_PFe_inorg)]);
@@ -384,7 +384,7 @@ __device__ __forceinline__ void trk_body(const TrkArgs& A, const MemberDev& md, 
                     const long long vvv = (long long)accv[q];
                     if (vvv) { a.acc[(long long)as * G + qo] = 0ull; plk = (float)((double)vvv * Z.fxv); }
                 }
-                a.tr_next[(long long)n * G + qo] = cc[q] + (Gc + plk);
+                a.tr_next[(long long)n * G + qo] = tendency(cc[q], Gc, plk);
             }
             if (nix * njy * nkz > 1) {
                 // a cell on the edge of the domain: copy its new values into its halo images

@@ -48,7 +48,9 @@ def test_config1_full_size_one_day(gpu_lib):
     ref, g64, g32 = _three(gpu_lib, wl, wl.steps)
     assert compare_states(ref, g64, wl.nsp) == []
     assert g64.count_active(0) != 16384           # a day of divisions changed the population
-    check_errors(errors_vs_oracle(ref, g32, wl))
+    # 1440 FP32 steps: pointwise tracer differences grow to a few 1e-5 of the field's maximum while
+    # the interior masses stay within TRACER_MASS_RTOL
+    check_errors(errors_vs_oracle(ref, g32, wl), tracer_rel=1e-4)
 
 
 def test_3d_two_species_64x64x32_bitexact(gpu_lib):

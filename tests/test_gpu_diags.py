@@ -53,7 +53,8 @@ def test_optional_diagnostics_fp64_bitexact(gpu_lib):
     for kind, s in _kinds(wl):
         a, b = ref.get_diag(kind, s), m.get_diag(kind, s)
         assert same(a, b), (kind, s, int(np.sum(a != b)))
-        assert np.any(a != 0.0), (kind, s)
+        if kind != _abi.PI_DIAG_TRACER + _abi.tracer_names.index("Dust"):   # no dust in this workload
+            assert np.any(a != 0.0), (kind, s)
     assert gpu_lib.pi_reset_diags(m.h) == 0
     assert not np.any(m.get_diag(_abi.PI_DIAG_PROC, 0))
 

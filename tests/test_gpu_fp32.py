@@ -77,7 +77,10 @@ def errors_vs_oracle(ref, f32, wl):
     return out
 
 
-def check_errors(e):
+def check_errors(e, tracer_rel=1e-5):
+    """The FP32 bar: counts and active slots identical, cells identical for >= 99.5 %, positions within
+    1e-3 cells, quotas within 1e-4 relative, each tracer within tracer_rel of its largest value
+    (1e-5 for runs of tens of steps) and interior tracer masses within TRACER_MASS_RTOL."""
     print({k: v for k, v in e.items() if k != "mass_rel"})
     print("tracer mass relative error:", {k: f"{v:.2e}" for k, v in e["mass_rel"].items()})
     assert e["count_fp32"] == e["count_fp64"]
@@ -85,7 +88,7 @@ def check_errors(e):
     assert e["cell_mismatch_frac"] <= 5e-3
     assert e["pos_abs"] <= 1e-3
     assert e["quota_rel"] <= 1e-4
-    assert e["tracer_rel_max"] <= 1e-5
+    assert e["tracer_rel_max"] <= tracer_rel
     assert max(e["mass_rel"].values()) <= TRACER_MASS_RTOL
 
 
