@@ -366,6 +366,8 @@ pi_status pi_batch_reset_diags(pi_batch* b);
  * active individuals' C (Bm+Cq), N (Bm·R_NC+Nq) and P (Bm·R_PC+Pq). No counterpart in the
  * reference, which has no budget call. */
 pi_status pi_batch_budget(pi_batch* b, int32_t member, double out[6]);
+/* The same budgets for a model of either precision (a PI_FP32 model is member 0 of its batch). */
+pi_status pi_get_budget(pi_model* m, double out[6]);
 
 /* Launch-shape autotuner (no counterpart in the reference): times `steps_per_candidate` real
  * steps of ΔT for each candidate block size, tiles-per-block mode and sweep segment length, and

@@ -104,6 +104,7 @@ def declare(lib, prefix):
         "set_time": (ct.c_int32, [P, ct.c_int64, ct.c_double]),
         "count_active": (ct.c_int32, [P, ct.c_int32, _i64p]),
         "get_diag": (ct.c_int32, [P, ct.c_int32, ct.c_int32, _dp]),
+        "get_budget": (ct.c_int32, [P, _dp]),
         "last_error": (ct.c_int32, [P, ct.c_char_p, ct.c_size_t]),
     }
     for name, (res, args) in protos.items():

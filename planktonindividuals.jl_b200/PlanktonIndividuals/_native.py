@@ -234,6 +234,13 @@ class CModel:
         tracer_mask adds tracer n, bit q of proc_mask the QuotaMode process q (PROC_NAMES)."""
         self._check(self._fn("set_diags")(self.h, ct.c_uint32(tracer_mask), ct.c_uint32(proc_mask)), "set_diags")
 
+    def budget(self):
+        """Mass budgets (mmol): interior tracer C, N, P and the active individuals' C, N, P
+        (pi_get_budget)."""
+        out = np.zeros(6, dtype=np.float64)
+        self._check(self._fn("get_budget")(self.h, _dptr(out)), "get_budget")
+        return out
+
     def check_finite(self):
         """Raises PIError (PI_ERR_NAN) naming the first tracer cell or active individual holding a
         NaN or Inf."""

@@ -1070,6 +1070,47 @@ __global__ void k_first_nonfinite_inds(SpcDev s, long long C, unsigned long long
     }
 }
 
+// Mass budgets (no counterpart in the reference): block partials of the interior Σ vol·c of the
+// carbon (DIC+DOC+POC), nitrogen (NH4+NO3+DON+PON) and phosphorus (PO4+DOP+POP) tracers, and of the
+// active individuals' C (Bm+Cq), N (Bm·R_NC+Nq) and P (Bm·R_PC+Pq). Each block sums a fixed set of
+// cells (slots) in a fixed order, so the result does not depend on the run.
+__device__ __forceinline__ void block_sum3(double c, double n, double p, double* partial) {
+    __shared__ double sh[3][256];
+    sh[0][threadIdx.x] = c; sh[1][threadIdx.x] = n; sh[2][threadIdx.x] = p;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) for (int r = 0; r < 3; ++r) sh[r][threadIdx.x] += sh[r][threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) for (int r = 0; r < 3; ++r) partial[blockIdx.x * 3 + r] = sh[r][0];
+}
+__global__ void __launch_bounds__(256) k_budget_cells(DGrid g, const double* __restrict__ tr, double* __restrict__ partial) {
+    double c = 0.0, n = 0.0, p = 0.0;
+    const long long V = (long long)g.Nx * g.Ny * g.Nz, G = g.G;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < V; q += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(q % g.Nx) + 1 + g.Hx;
+        const long long r = q / g.Nx;
+        const int j = (int)(r % g.Ny) + 1 + g.Hy, k = (int)(r / g.Ny) + 1 + g.Hz;
+        const long long cq = gidx(g, i, j, k);
+        const double vol = g.dx * g.dy * g.dzF[k - 1];
+        c += vol * (tr[PI_DIC * G + cq] + tr[PI_DOC * G + cq] + tr[PI_POC * G + cq]);
+        n += vol * (tr[PI_NH4 * G + cq] + tr[PI_NO3 * G + cq] + tr[PI_DON * G + cq] + tr[PI_PON * G + cq]);
+        p += vol * (tr[PI_PO4 * G + cq] + tr[PI_DOP * G + cq] + tr[PI_POP * G + cq]);
+    }
+    block_sum3(c, n, p, partial);
+}
+__global__ void __launch_bounds__(256) k_budget_inds(SpcDev s, long long C, double R_NC, double R_PC, double* __restrict__ partial) {
+    double c = 0.0, n = 0.0, p = 0.0;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < C; q += (long long)gridDim.x * blockDim.x) {
+        if (!(s.flags[q] & FL_AC)) continue;
+        const double Bm = s.Bm[q];
+        c += Bm + s.Cq[q];
+        n += Bm * R_NC + s.Nq[q];
+        p += Bm * R_PC + s.Pq[q];
+    }
+    block_sum3(c, n, p, partial);
+}
+
 __global__ void k_count_active(const uint8_t* __restrict__ flags, long long C, unsigned long long* out) {
     unsigned long long n = 0;
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < C; q += (long long)gridDim.x * blockDim.x)

@@ -83,6 +83,7 @@ struct pi_model {
     double* diag_tr = nullptr;   // 14 × G
     double* diag_proc = nullptr; // nsp × PI_NPROC × G
     double* procv = nullptr;     // PI_NPROC × C values of the species being updated
+    double* budget_part = nullptr;   // 3 × 512 block partials of pi_get_budget
     uint32_t *dkey = nullptr, *dkey_s = nullptr, *dval = nullptr, *dval_s = nullptr;
     void* dsort_tmp = nullptr;
     size_t dsort_bytes = 0;
@@ -969,6 +970,30 @@ pi_status pi_get_diag(pi_model* m, int32_t kind, int32_t sp, double* out) {
     }
     CK(cudaMemcpyAsync(out, src, G * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download diag");
     CK(cudaStreamSynchronize(m->stream), "synchronize");
+    return PI_OK;
+}
+
+pi_status pi_get_budget(pi_model* m, double out[6]) {
+    if (m && m->b32) return fwd32(m, pi_batch_budget(m->b32, 0, out));
+    if (!m || !out) return fail(m, PI_ERR_ARG, "pi_get_budget: NULL argument");
+    const int nb = 512;
+    if (!m->budget_part) { pi_status e = dalloc(m, &m->budget_part, 3 * nb, "budget partials"); if (e) return e; }
+    std::vector<double> h(3 * nb);
+    auto collect = [&](double* dst) -> pi_status {
+        CK(cudaGetLastError(), "budget");
+        CK(cudaMemcpyAsync(h.data(), m->budget_part, 3 * nb * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download budget");
+        CK(cudaStreamSynchronize(m->stream), "synchronize");
+        for (int r = 0; r < 3; ++r) { double x = 0.0; for (int q = 0; q < nb; ++q) x += h[q * 3 + r]; dst[r] += x; }
+        return PI_OK;
+    };
+    for (int r = 0; r < 6; ++r) out[r] = 0.0;
+    k_budget_cells<<<nb, 256, 0, m->stream>>>(m->dg, m->tr, m->budget_part);
+    pi_status e = collect(out);
+    if (e) return e;
+    for (int s = 0; s < m->nsp; ++s) {
+        k_budget_inds<<<nb, 256, 0, m->stream>>>(m->h_spc[s], m->C, m->sp[s].R_NC, m->sp[s].R_PC, m->budget_part);
+        if ((e = collect(out + 3))) return e;
+    }
     return PI_OK;
 }
 

@@ -15,7 +15,7 @@ module PIB200
 export PiGrid, PiBgc, PiQuota, PiIndividuals, PiMember, PIError
 export create, destroy, set_individuals!, get_individuals, set_tracer!, get_tracer
 export set_velocity!, set_PARF!, set_temp!, set_flux_bc!, time_step!, get_time, set_time!
-export count_active, get_diag, reset_diags!, check_finite, simulation, update!, synchronize
+export count_active, get_diag, reset_diags!, check_finite, budget, simulation, update!, synchronize
 export batch_create, batch_step!, batch_set_sort_interval!
 
 const lib = get(ENV, "LIBPIB200", joinpath(@__DIR__, "..", "PlanktonIndividuals", "libpib200.so"))
@@ -214,6 +214,13 @@ function get_diag(m::Model, kind::Symbol, sp::Integer = 1)
 end
 reset_diags!(m::Model) = check(ccall((:pi_reset_diags, lib), Int32, (Ptr{Cvoid},), m.h), m.h)
 check_finite(m::Model) = check(ccall((:pi_check_finite, lib), Int32, (Ptr{Cvoid},), m.h), m.h)
+
+"""Mass budgets (mmol): interior tracer C, N, P, then the active individuals' C, N, P."""
+function budget(m::Model)
+    out = zeros(Float64, 6)
+    check(ccall((:pi_get_budget, lib), Int32, (Ptr{Cvoid}, Ptr{Float64}), m.h, out), m.h)
+    return out
+end
 synchronize(m::Model) = check(ccall((:pi_synchronize, lib), Int32, (Ptr{Cvoid},), m.h), m.h)
 
 # ---- simulation ---------------------------------------------------------------------------------

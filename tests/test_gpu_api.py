@@ -113,3 +113,26 @@ def test_simulation_with_output_writer(gpu_lib, tmp_path):
     lines = open(str(tmp_path / "out" / "dynamic_species001.txt")).read().splitlines()
     assert len(lines) == STEPS
     sim.close()
+
+
+@pytest.mark.parametrize("FT", [np.float64, np.float32])
+def test_model_budget_matches_downloaded_state(gpu_lib, FT):
+    """pi_get_budget on a model handle (either precision): the interior tracer C, N, P and the
+    active individuals' C, N, P equal the sums over the downloaded fields and attributes."""
+    grid, model, sim, _ = _setup(FT)
+    update_b(sim)
+    bud = model._native.budget()
+    g = grid
+    vol = float(g.Δx) * float(g.Δy) * np.asarray(g.dzF)[g.Hz:g.Hz + g.Nz]
+    inner = lambda a: np.asarray(a, dtype=np.float64)[g.Hx:g.Hx + g.Nx, g.Hy:g.Hy + g.Ny, g.Hz:g.Hz + g.Nz]
+    tot = lambda names: sum(float(np.sum(inner(model.tracers[n].data) * vol)) for n in names)
+    d = {k: np.asarray(v, dtype=np.float64) for k, v in model.individuals.phytos.sp1.data.items()}
+    ac = np.asarray(model.individuals.phytos.sp1.data["ac"], dtype=bool)
+    p = model.phyto.params
+    R_NC, R_PC = float(np.ravel(p["R_NC"])[0]), float(np.ravel(p["R_PC"])[0])
+    want = [tot(("DIC", "DOC", "POC")), tot(("NH4", "NO3", "DON", "PON")), tot(("PO4", "DOP", "POP")),
+            float(np.sum((d["Bm"] + d["Cq"])[ac])), float(np.sum((d["Bm"] * R_NC + d["Nq"])[ac])),
+            float(np.sum((d["Bm"] * R_PC + d["Pq"])[ac]))]
+    rel = 1e-12 if FT is np.float64 else 1e-6
+    for a, b in zip(bud, want):
+        assert a == pytest.approx(b, rel=rel)
