@@ -176,9 +176,47 @@ __device__ __forceinline__ void draw3f(uint64_t seed, uint32_t iter, uint32_t sp
     r2 = (float)(o[2] >> 8) * 0x1p-24f;
 }
 
+__device__ __forceinline__ unsigned long long to_fixed(float v, double inv_unit) {
+    return (unsigned long long)__double2ll_rn((double)v * inv_unit);
+}
 __device__ __forceinline__ void add_fixed(unsigned long long* a, float v, double inv_unit) {
-    const long long x = __double2ll_rn((double)v * inv_unit);
-    if (x) atomicAdd(a, (unsigned long long)x);
+    const unsigned long long x = to_fixed(v, inv_unit);
+    if (x) atomicAdd(a, x);
+}
+
+// Warp-segmented sums for the particle → grid scatters. In the cell-sorted storage order the
+// individuals of one cell sit in adjacent slots, so the lanes of a warp form runs of equal cell
+// keys; each run's first lane adds the run's total with one integer atomic instead of one atomic
+// per individual. Sums are integers (counts, fixed-point masses), so the result is the same
+// whatever the runs are. All 32 lanes call these with converged control flow; a key of -1 takes
+// no part.
+struct WarpRuns {
+    bool head;      // first lane of its run
+    bool dup;       // some run in the warp is longer than one lane (warp-uniform)
+    int end;        // last lane of this lane's run
+};
+__device__ __forceinline__ WarpRuns warp_runs(long long key) {
+    const int lane = threadIdx.x & 31;
+    const long long prev = __shfl_up_sync(0xffffffffu, key, 1);
+    WarpRuns R;
+    R.head = lane == 0 || prev != key;
+    const unsigned heads = __ballot_sync(0xffffffffu, R.head);
+    const unsigned after = lane == 31 ? 0u : heads & ~((2u << lane) - 1u);
+    R.end = after ? __ffs(after) - 2 : 31;
+    R.dup = heads != 0xffffffffu;
+    return R;
+}
+// the total of v over the lanes from this lane to the end of its run (the run's total at its head)
+template <typename T>
+__device__ __forceinline__ T run_sum(T v, const WarpRuns& R) {
+    if (!R.dup) return v;
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const T y = __shfl_down_sync(0xffffffffu, v, o);
+        if (lane + o <= R.end) v += y;
+    }
+    return v;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -327,9 +365,15 @@ __device__ __forceinline__ MState move_state(const IndDev32& P, long long g, boo
     return S;
 }
 
-__device__ __forceinline__ void move_one(const MoveArgs& a, const MemberDev& m, const PGeom& pg, int mi, int s,
-                                         long long g, uint32_t iter, const MState& S) {
+// What k32_move adds to the grid for one slot: the cell (-1: nothing), a packed count
+// (pop | grazed << 8 | dead << 16 | dividing << 24; a warp's run sums stay below 256 per field) and
+// the Chl sum in fixed point (interior cells only).
+struct MoveOut { long long cq; uint32_t cnt; unsigned long long chl; };
+
+__device__ __forceinline__ MoveOut move_one(const MoveArgs& a, const MemberDev& m, const PGeom& pg, int mi, int s,
+                                            long long g, uint32_t iter, const MState& S) {
     const IndDev32& P = a.P;
+    MoveOut out{-1, 0u, 0ull};
     const uint8_t fl = S.fl, stt = S.stt;
     const int32_t code = S.code;
     const float ox = S.ox, oy = S.oy, oz = S.oz;
@@ -341,7 +385,7 @@ __device__ __forceinline__ void move_one(const MoveArgs& a, const MemberDev& m, 
             P.ox[g] = 0.0f; P.oy[g] = 0.0f; P.oz[g] = 0.0f;
         }
         if (stt) P.stat[g] = 0;
-        return;
+        return out;
     }
     uint32_t* err = a.err;
     int ci, cj, ck;
@@ -400,16 +444,13 @@ __device__ __forceinline__ void move_one(const MoveArgs& a, const MemberDev& m, 
     P.ox[g] = X.o; P.oy[g] = Y.o; P.oz[g] = Z.o;
     P.cell[g] = code_new;
     const long long G = a.Gtot;
-    atomicAdd(&a.pop[cq], 1);
-    if (a.pop_sp) atomicAdd(&a.pop_sp[(long long)s * G + cq], 1);
-    if (inside) add_fixed(&a.chl_acc[cq], chl, chl_inv);
     // previous step's decisions (plankton_update.jl:5-16, division_death.jl:2-25)
     const int gz = (fl & F32_GRAZ) != 0, mt = (fl & F32_MORT) != 0, dv = (fl & F32_DVID) != 0;
     const int ac1 = !gz, ac2 = ac1 && !mt, dv2 = dv && ac2;
-    uint32_t* dc = a.dcnt + (long long)s * 4 * G + cq;
-    if (gz) atomicAdd(dc + 1 * G, 1u);
-    if (ac1 && mt) atomicAdd(dc + 2 * G, 1u);
-    if (dv2) atomicAdd(dc + 3 * G, 1u);
+    // pop, the Chl sum and the graz/mort/dvid diagnostics counts, added by scatter_move
+    out.cq = cq;
+    out.cnt = 1u | (gz ? 1u << 8 : 0u) | (ac1 && mt ? 1u << 16 : 0u) | (dv2 ? 1u << 24 : 0u);
+    out.chl = inside ? to_fixed(chl, chl_inv) : 0ull;
     const int kind = gz ? 1 : (ac1 && mt) ? 2 : 0;
     if (kind && inside) {
         const SpeciesDev32& p = a.sp[mi * a.T.nsp + s];
@@ -435,6 +476,25 @@ __device__ __forceinline__ void move_one(const MoveArgs& a, const MemberDev& m, 
         slot_bit(m, s, P.lslot[g], w, bit);
         atomicOr(dv2 ? &P.dvbits[w] : &P.freebits[w], bit);
     }
+    return out;
+}
+
+// k32_move's grid sums of one warp (segment s of one member): one atomic per run of a cell
+__device__ __forceinline__ void scatter_move(const MoveArgs& a, int s, const MoveOut& o) {
+    const WarpRuns R = warp_runs(o.cq);
+    const uint32_t c = run_sum(o.cnt, R);
+    const unsigned long long chl = run_sum(o.chl, R);
+    if (R.head && o.cq >= 0) {
+        const long long G = a.Gtot, cq = o.cq;
+        const int np = (int)(c & 0xffu);
+        atomicAdd(&a.pop[cq], np);
+        if (a.pop_sp) atomicAdd(&a.pop_sp[(long long)s * G + cq], np);
+        if (chl) atomicAdd(&a.chl_acc[cq], chl);
+        uint32_t* dc = a.dcnt + (long long)s * 4 * G + cq;
+        if (c >> 8 & 0xffu) atomicAdd(dc + 1 * G, c >> 8 & 0xffu);
+        if (c >> 16 & 0xffu) atomicAdd(dc + 2 * G, c >> 16 & 0xffu);
+        if (c >> 24) atomicAdd(dc + 3 * G, c >> 24);
+    }
 }
 
 __global__ void __launch_bounds__(256, 2) k32_move(MoveArgs a) {
@@ -455,7 +515,9 @@ __global__ void __launch_bounds__(256, 2) k32_move(MoveArgs a) {
         for (int p = 0; p < ppt; ++p, slot += bs) {
             const MState cur = nx;
             if (p + 1 < ppt) nx = move_state(a.P, base + slot + bs, slot + bs < m.C);
-            if (slot < m.C) move_one(a, m, sg, mi, s, base + slot, iter, cur);
+            MoveOut o{-1, 0u, 0ull};
+            if (slot < m.C) o = move_one(a, m, sg, mi, s, base + slot, iter, cur);
+            scatter_move(a, s, o);
         }
         __syncthreads();
     }
@@ -845,13 +907,19 @@ __device__ __forceinline__ PHead phys_head(const IndDev32& P, long long g, bool 
     return h;
 }
 
-__device__ __forceinline__ void phys_one(const PhysArgs& a, const MemberDev& m, int mi, int s,
-                                         long long g, uint32_t iter, double tnow, const PHead& hd) {
+// What k32_physiology adds to the grid for one slot: the cell (-1: nothing; the diagnostics count
+// num is added there) and the consumption of DIC, DOC, NH4, NO3, PO4 in fixed point (zero unless
+// the individual was binned this step into an interior cell).
+struct PhysOut { long long cq; unsigned long long v[5]; };
+
+__device__ __forceinline__ PhysOut phys_one(const PhysArgs& a, const MemberDev& m, int mi, int s,
+                                            long long g, uint32_t iter, double tnow, const PHead& hd) {
     const IndDev32& P = a.P;
+    PhysOut out{-1, {0ull, 0ull, 0ull, 0ull, 0ull}};
     // the quotas are loaded with the environment
     const uint8_t fl = hd.fl, stt = hd.stt;
     const int32_t code = hd.code;
-    if (!(fl & F32_AC)) return;
+    if (!(fl & F32_AC)) return out;
     const int ac0 = stt & F32_ST_AC0;
     int q;
     if (stt & F32_ST_STALE) { int xi, yi, zi; unpack_halo(m, P.scell[g], xi, yi, zi); q = gid3(m, xi, yi, zi); }
@@ -950,20 +1018,38 @@ __device__ __forceinline__ void phys_one(const PhysArgs& a, const MemberDev& m, 
     P.Bm[g] = Bm; P.Cq[g] = Cq; P.Nq[g] = Nq; P.Pq[g] = Pq; P.Chl[g] = Chl; P.age[g] = age;
     P.flags[g] = (uint8_t)(F32_AC | (dg ? F32_GRAZ : 0) | (dm ? F32_MORT : 0) | (dd ? F32_DVID : 0));
     // calc_consume_kernel! (consume_loss.jl:2-9): only individuals binned this step reach the grid
+    out.cq = cq;                // diags num at the (possibly stale) cell
     if (ac0 && inside) {
         const double u = fx_inv;
-        add_fixed(&a.acc[ACC_DIC * G + cq], (resp - PS) * dT, u);
-        add_fixed(&a.acc[ACC_DOC * G + cq], (exu - VDOC) * dT, u);
-        add_fixed(&a.acc[ACC_NH4 * G + cq], -VNH4 * dT, u);
-        add_fixed(&a.acc[ACC_NO3 * G + cq], -VNO3 * dT, u);
-        add_fixed(&a.acc[ACC_PO4 * G + cq], -VPO4 * dT, u);
+        out.v[0] = to_fixed((resp - PS) * dT, u);
+        out.v[1] = to_fixed((exu - VDOC) * dT, u);
+        out.v[2] = to_fixed(-VNH4 * dT, u);
+        out.v[3] = to_fixed(-VNO3 * dT, u);
+        out.v[4] = to_fixed(-VPO4 * dT, u);
     }
-    atomicAdd(&a.dcnt[(long long)s * 4 * G + cq], 1u);      // diags num at the (possibly stale) cell
     // diags_spcs! (Diagnostics/diagnostics_kernels.jl:14-33) at the same cell
     if (a.pmask) {
         const float v[PI_NPROC] = { PS, BS, VDOC, VNH4, VNO3, VPO4, resp, exu, Bm, Cq, Nq, Pq, Chl };
         for (int q = 0; q < PI_NPROC; ++q)
             if (a.pmask >> q & 1u) add_fixed(&a.dproc[((long long)s * PI_NPROC + q) * G + cq], v[q], 1.0 / proc_unit(m, q));
+    }
+    return out;
+}
+
+// k32_physiology's grid sums of one warp (segment s of one member): one atomic per run of a cell
+__device__ __forceinline__ void scatter_phys(const PhysArgs& a, int s, const PhysOut& o) {
+    const WarpRuns R = warp_runs(o.cq);
+    const int n = (int)run_sum(o.cq >= 0 ? 1u : 0u, R);
+    unsigned long long v[5];
+#pragma unroll
+    for (int e = 0; e < 5; ++e) v[e] = run_sum(o.v[e], R);
+    if (R.head && o.cq >= 0) {
+        const long long G = a.Gtot, cq = o.cq;
+        atomicAdd(&a.dcnt[(long long)s * 4 * G + cq], (uint32_t)n);
+        const int slot_of[5] = { ACC_DIC, ACC_DOC, ACC_NH4, ACC_NO3, ACC_PO4 };
+#pragma unroll
+        for (int e = 0; e < 5; ++e)
+            if (v[e]) atomicAdd(&a.acc[(long long)slot_of[e] * G + cq], v[e]);
     }
 }
 
@@ -983,7 +1069,9 @@ __global__ void __launch_bounds__(256, 4) k32_physiology(PhysArgs a) {
         for (int p = 0; p < ppt; ++p, slot += bs) {
             const PHead cur = hd;
             if (p + 1 < ppt) hd = phys_head(a.P, base + slot + bs, slot + bs < m.C);
-            if (slot < m.C) phys_one(a, m, mi, s, base + slot, iter, tnow, cur);
+            PhysOut o{-1, {0ull, 0ull, 0ull, 0ull, 0ull}};
+            if (slot < m.C) o = phys_one(a, m, mi, s, base + slot, iter, tnow, cur);
+            scatter_phys(a, s, o);
         }
     }
 }
