@@ -16,6 +16,7 @@ export PiGrid, PiBgc, PiQuota, PiIndividuals, PiMember, PIError
 export create, destroy, set_individuals!, get_individuals, set_tracer!, get_tracer
 export set_velocity!, set_PARF!, set_temp!, set_flux_bc!, time_step!, get_time, set_time!
 export count_active, get_diag, reset_diags!, check_finite, budget, simulation, update!, synchronize
+export set_velocity_f32!, set_PARF_f32!, set_temp_f32!, time_step_async!, count_active_async!, set_diags!
 export batch_create, batch_step!, batch_set_sort_interval!
 
 const lib = get(ENV, "LIBPIB200", joinpath(@__DIR__, "..", "PlanktonIndividuals", "libpib200.so"))
@@ -29,6 +30,10 @@ const PI_PERIODIC = Int32(0)
 const PI_BOUNDED = Int32(1)
 const TRACERS = (:DIC, :NH4, :NO3, :PO4, :DFe, :DOC, :DON, :DOP, :PFe_inorg, :POC, :PON, :POP, :PFe_bio, :Dust)
 const DIAG_KINDS = Dict(:PAR => Int32(0), :num => Int32(1), :graz => Int32(2), :mort => Int32(3), :dvid => Int32(4))
+# optional diagnostics: PI_DIAG_TRACER + tracer index, PI_DIAG_PROC + process index
+const PI_DIAG_TRACER = Int32(16)
+const PI_DIAG_PROC = Int32(32)
+const PROCS = (:PS, :BS, :VDOC, :VNH4, :VNO3, :VPO4, :resp, :exu, :Bm, :Cq, :Nq, :Pq, :Chl)
 
 struct PiGrid
     Nx::Int32; Ny::Int32; Nz::Int32
@@ -181,6 +186,16 @@ set_velocity!(m::Model, u, v, w) =
 set_PARF!(m::Model, parf) = check(ccall((:pi_set_PARF, lib), Int32, (Ptr{Cvoid}, Ptr{Float64}), m.h, Float64.(parf)), m.h)
 set_temp!(m::Model, temp) = check(ccall((:pi_set_temp, lib), Int32, (Ptr{Cvoid}, Ptr{Float64}), m.h, Float64.(temp)), m.h)
 
+# The same uploads from Float32 arrays (the reference's arrays when FT = Float32), for a model
+# created with FT = Float32: the copies are queued on the model's copy stream and overlap the step
+# queued before them; the arrays may be reused when the call returns.
+set_velocity_f32!(m::Model, u::Array{Float32}, v::Array{Float32}, w::Array{Float32}) =
+    check(ccall((:pi_set_velocity_f32, lib), Int32, (Ptr{Cvoid}, Ptr{Float32}, Ptr{Float32}, Ptr{Float32}), m.h, u, v, w), m.h)
+set_PARF_f32!(m::Model, parf::Array{Float32}) =
+    check(ccall((:pi_set_PARF_f32, lib), Int32, (Ptr{Cvoid}, Ptr{Float32}), m.h, parf), m.h)
+set_temp_f32!(m::Model, temp::Array{Float32}) =
+    check(ccall((:pi_set_temp_f32, lib), Int32, (Ptr{Cvoid}, Ptr{Float32}), m.h, temp), m.h)
+
 # set_bc!(model; tracer, pos, bc_value) (HaloRegions/boundary_conditions.jl:21-31)
 const FACES = Dict(:west => 0, :east => 1, :south => 2, :north => 3, :bottom => 4, :top => 5)
 function set_flux_bc!(m::Model, tracer::Symbol, pos::Symbol, value)
@@ -192,6 +207,11 @@ end
 
 # TimeStep!(model, ΔT, diags) (src/Model/time_step.jl:12-180)
 time_step!(m::Model, ΔT) = check(ccall((:pi_time_step, lib), Int32, (Ptr{Cvoid}, Float64), m.h, ΔT), m.h)
+# queues the step and returns; errors of the step are reported by the next synchronize
+time_step_async!(m::Model, ΔT) = check(ccall((:pi_time_step_async, lib), Int32, (Ptr{Cvoid}, Float64), m.h, ΔT), m.h)
+# queues the count of species sp into n (which must stay valid until synchronize)
+count_active_async!(m::Model, sp::Integer, n::Base.RefValue{Int64}) =
+    check(ccall((:pi_count_active_async, lib), Int32, (Ptr{Cvoid}, Int32, Ptr{Int64}), m.h, sp - 1, n), m.h)
 
 function get_time(m::Model)
     it = Ref{Int64}(0); t = Ref{Float64}(0)
@@ -206,11 +226,34 @@ function count_active(m::Model, sp::Integer)
     n[]
 end
 
-"""diags.tracer.PAR (kind = :PAR) or diags.phytos[sp].num/graz/mort/dvid, halo-padded."""
+"""diags.tracer.PAR / diags.tracer[name] (kind = :PAR or a tracer name) or
+diags.phytos[sp].num/graz/mort/dvid/<process>, halo-padded. Tracers and processes must have been
+enabled with set_diags!."""
 function get_diag(m::Model, kind::Symbol, sp::Integer = 1)
+    k = haskey(DIAG_KINDS, kind) ? DIAG_KINDS[kind] :
+        kind in TRACERS ? PI_DIAG_TRACER + tracer_index(kind) :
+        kind in PROCS ? PI_DIAG_PROC + Int32(findfirst(==(kind), PROCS) - 1) :
+        throw(ArgumentError("$kind is not one of the diagnostics"))
     a = zeros(Float64, m.G)
-    check(ccall((:pi_get_diag, lib), Int32, (Ptr{Cvoid}, Int32, Int32, Ptr{Float64}), m.h, DIAG_KINDS[kind], sp - 1, a), m.h)
+    check(ccall((:pi_get_diag, lib), Int32, (Ptr{Cvoid}, Int32, Int32, Ptr{Float64}), m.h, k, sp - 1, a), m.h)
     a
+end
+
+"""PlanktonDiagnostics(model; tracer = (...), phytoplankton = (...)): adds the named tracer fields
+and QuotaMode processes to the diagnostics the step accumulates."""
+function set_diags!(m::Model; tracer = (), phytoplankton = ())
+    tm = UInt32(0); pm = UInt32(0)
+    for n in tracer
+        n === :PAR && continue
+        tm |= UInt32(1) << tracer_index(n)
+    end
+    for p in phytoplankton
+        p in keys(DIAG_KINDS) && continue
+        q = findfirst(==(p), PROCS)
+        q === nothing && throw(ArgumentError("$p is not one of the diagnostics"))
+        pm |= UInt32(1) << (q - 1)
+    end
+    check(ccall((:pi_set_diags, lib), Int32, (Ptr{Cvoid}, UInt32, UInt32), m.h, tm, pm), m.h)
 end
 reset_diags!(m::Model) = check(ccall((:pi_reset_diags, lib), Int32, (Ptr{Cvoid},), m.h), m.h)
 check_finite(m::Model) = check(ccall((:pi_check_finite, lib), Int32, (Ptr{Cvoid},), m.h), m.h)
