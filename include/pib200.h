@@ -381,6 +381,12 @@ pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t steps_per_candidate,
  * and, of those, decisions that the Float32 probability would have taken the other way. */
 pi_status pi_batch_guard_stats(pi_batch* b, int64_t* recomputed, int64_t* changed);
 
+/* Tracer update kernels (no counterpart in the reference; pi_batch_autotune chooses): fused = 1
+ * runs the single kernel that sweeps x, y and z and finishes the tracer update per column run of
+ * `levels` levels (8, 16, 32 or 64), where every member allows it (no tracer diffusion, no flux
+ * boundary conditions, at least as many cells as halo points on each axis); fused = 0 runs the x-y
+ * kernel, the z kernel and the halo fill. Results are identical either way. */
+pi_status pi_batch_set_tracer_kernel(pi_batch* b, int32_t fused, int32_t levels);
 /* Storage order (no counterpart in the reference, which stores individuals in slot order): each
  * (member, species) segment is kept in an order grouped by cell, restored by a counting sort
  * before the first step after pi_batch_set_individuals and then every `steps` steps (default 32;

@@ -210,6 +210,11 @@ class PlanktonBatch:
     def step(self, ΔT, nsteps=1, sync=True):
         self._check(self.lib.pi_batch_step(self.h, float(ΔT), int(nsteps), 1 if sync else 0), "step")
 
+    def set_tracer_kernel(self, fused, levels=32):
+        """Tracer update kernels: fused (one kernel per column run of `levels` levels) or the x-y
+        and z kernels with the halo fill (pi_batch_set_tracer_kernel); results are identical."""
+        self._check(self.lib.pi_batch_set_tracer_kernel(self.h, 1 if fused else 0, int(levels)), "set_tracer_kernel")
+
     def synchronize(self):
         self._check(self.lib.pi_batch_synchronize(self.h), "synchronize")
 

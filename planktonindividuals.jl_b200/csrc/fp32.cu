@@ -79,7 +79,8 @@ struct Tuning {
     int ty = 16;                              // rows of an x-y tracer tile (4, 8, 16 or 28)
     int lz = 32;                              // levels walked by a z thread (8, 16, 32 or 64)
     int wpb_par = 2;
-    int fused = 1;                            // k32_tracer when the batch allows it
+    int fused = 0;                            // k32_tracer when the batch allows it (the autotuner
+                                              // picks it where it beats k32_xy + k32_ztail + halo fill)
     int lz_fused = 32;                        // levels finished per k32_tracer block
 };
 
@@ -1651,6 +1652,15 @@ pi_status pi_batch_guard_stats(pi_batch* b, int64_t* recomputed, int64_t* change
     return PI_OK;
 }
 
+pi_status pi_batch_set_tracer_kernel(pi_batch* b, int32_t fused, int32_t levels) {
+    if (!b || (fused != 0 && fused != 1) || (levels != 8 && levels != 16 && levels != 32 && levels != 64))
+        return bfail(b, PI_ERR_ARG, "pi_batch_set_tracer_kernel: fused must be 0 or 1 and levels 8, 16, 32 or 64");
+    b->tune.fused = fused;
+    b->tune.lz_fused = levels;
+    free_graphs(b);
+    return PI_OK;
+}
+
 pi_status pi_batch_set_sort_interval(pi_batch* b, int32_t steps) {
     if (!b || steps < 0) return bfail(b, PI_ERR_ARG, "pi_batch_set_sort_interval: bad argument");
     b->sort_interval = steps;
@@ -1698,6 +1708,7 @@ pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t k, char* report, siz
     if (!b || !(dT > 0) || k < 1) return bfail(b, PI_ERR_ARG, "pi_batch_autotune: bad argument");
     const int was = b->profiling;
     std::string rep;
+    // average time per step of the kernels named (a name, or several separated by '|')
     auto kernel_ms = [&](const char* name, double& out) -> pi_status {
         pi_status e;
         b->profiling = 1;
@@ -1715,7 +1726,9 @@ pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t k, char* report, siz
         drain(b);
         if ((e = check_errors(b))) return e;
         out = 0.0;
-        for (size_t q = 0; q < b->prof_names.size(); ++q) if (b->prof_names[q] == name) out = b->prof_ms[q] / k;
+        const std::string names = std::string("|") + name + "|";
+        for (size_t q = 0; q < b->prof_names.size(); ++q)
+            if (names.find("|" + b->prof_names[q] + "|") != std::string::npos) out += b->prof_ms[q] / k;
         return PI_OK;
     };
     struct Knob { const char* kernel; int* field; std::vector<int> values; const char* label; int threads_per_value; };
@@ -1729,7 +1742,6 @@ pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t k, char* report, siz
         { "k32_xy", &t.ty, {4, 8, 16, 28}, "x-y tracer tile rows", 0 },
         { "k32_ztail", &t.lz, {8, 16, 32, 64}, "z levels per thread", 0 },
         { "k32_par", &t.wpb_par, {1, 2, 4, 8}, "par warps/block", 32 },
-        { "k32_tracer", &t.lz_fused, {16, 32, 64}, "tracer levels per block", 0 },
     };
     // the largest block each kernel can be launched with (registers per thread)
     auto max_threads = [](const char* kernel) -> int {
@@ -1743,6 +1755,9 @@ pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t k, char* report, siz
         return fa.maxThreadsPerBlock;
     };
     free_graphs(b);
+    // the knobs of the two-kernel tracer path are tuned on that path
+    const int fused0 = t.fused;
+    t.fused = 0;
     for (auto& kb : knobs) {
         int best = *kb.field;
         double best_ms = 1e300;
@@ -1758,6 +1773,27 @@ pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t k, char* report, siz
         *kb.field = best;
         char line[160];
         snprintf(line, sizeof line, "%s = %d (%.4f ms)\n", kb.label, best, best_ms);
+        rep += line;
+    }
+    // tracer path: k32_tracer (levels per block tuned) against k32_xy + k32_ztail + halo fill
+    double two = 0.0;
+    pi_status e0 = kernel_ms("k32_xy|k32_ztail|k32_halo", two);
+    if (e0) { b->profiling = was; return e0; }
+    t.fused = 1;
+    int best_lz = t.lz_fused;
+    double fused_ms = 1e300;
+    for (int v : {8, 16, 32, 64}) {
+        t.lz_fused = v;
+        double ms = 0.0;
+        if ((e0 = kernel_ms("k32_tracer", ms))) { b->profiling = was; return e0; }
+        if (ms > 0.0 && ms < fused_ms) { fused_ms = ms; best_lz = v; }
+    }
+    t.lz_fused = best_lz;
+    t.fused = (fused_ms < two) ? 1 : (fused_ms < 1e300 ? 0 : fused0);
+    {
+        char line[200];
+        snprintf(line, sizeof line, "tracer path = %s (fused %.4f ms at %d levels per block, two-kernel %.4f ms)\n",
+                 t.fused ? "k32_tracer" : "k32_xy + k32_ztail", fused_ms < 1e300 ? fused_ms : 0.0, best_lz, two);
         rep += line;
     }
     b->profiling = was;

@@ -385,6 +385,8 @@ def test_fused_tracer_kernel_equals_two_kernel_path(gpu_lib):
     vels = [VelCache(wl) for wl in wls]
     fused = PlanktonBatch(_members(wls), nspecies=1)
     plain = PlanktonBatch(_members(wls), nspecies=1)
+    fused.set_tracer_kernel(True, 32)
+    plain.set_tracer_kernel(False)
     for batch in (fused, plain):
         for m, wl in enumerate(wls):
             batch.set_state(m, wl.individuals, wl.tracers)
