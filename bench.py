@@ -220,6 +220,7 @@ def run_fp32(members, args, dist, local, clocks_cls):
     n_tune = b.get_time()[0]
     b.step(dT, Wm)
     n0 = b.count_active()
+    it0 = b.get_time()[0]
     # the timed steps start a storage-order cycle: they include one counting sort per SORT_INTERVAL
     # steps, the first before their first step
     b.set_sort_interval(SORT_INTERVAL)
@@ -240,6 +241,8 @@ def run_fp32(members, args, dist, local, clocks_cls):
     b.synchronize()
     ms = e0.elapsed_time(e1)
     n1 = b.count_active()
+    if b.get_time()[0] != it0 + K:
+        raise RuntimeError(f"the timed region advanced the model by {b.get_time()[0] - it0} steps, not {K}")
     prof = {}
     if args.profile_steps > 0:
         b.set_sort_interval(SORT_INTERVAL)          # the profiled steps include one sort

@@ -122,7 +122,6 @@ struct pi_batch {
     uint8_t* lm = nullptr;
     float* velown = nullptr;        // 6 planes of Gtot: buffer b, component c at (b*3+c)*Gtot
     float* velh = nullptr;          // 3 planes of Gtot
-    float4* pkpool = nullptr;       // 9 planes of Gtot: packed set k, component c at (k*3+c)*Gtot
     float* tempown = nullptr;       // Gtot
     uint32_t* dcnt = nullptr;
     int* pop = nullptr;
@@ -470,9 +469,6 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
     { BScope sc(b, "k32_velhalf");
       const unsigned gx = fgx;
       k32_velhalf<<<dim3(gx, b->nm), 256, 0, s>>>(b->md, b->F, b->errw); }
-    { BScope sc(b, "k32_pack");
-      k32_pack_bind<<<nblk(b->nm, 128), 128, 0, s>>>(b->nm, b->F, b->errw);
-      k32_pack<<<dim3(std::max(1u, fgx / 4), b->nm, 9), 256, 0, s>>>(b->md, b->F, b->errw); }
     {
         MoveArgs a;
         a.T = b->T; a.P = b->P; a.sp = b->sp; a.bgc = b->bgc; a.F = b->F; a.rdzC = b->rdzC; a.st = b->st;
@@ -785,7 +781,7 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     BA(b->par, G); BA(b->diag_par, G); BA(b->PARF, std::max<long long>(col, 1));
     BA(b->dzF, lev); BA(b->dzC, lev); BA(b->rdzC, lev);
     if (any_land) BA(b->lm, G);
-    BA(b->velown, 6 * G); BA(b->velh, 3 * G); BA(b->tempown, G); BA(b->pkpool, 9 * G);
+    BA(b->velown, 6 * G); BA(b->velh, 3 * G); BA(b->tempown, G);
     BA(b->dcnt, (size_t)nspecies * 4 * G); BA(b->pop, G);
     bool shared = true;
     for (auto& h : b->mh) if (h.bgc.shared_graz != 1.0) shared = false;
@@ -831,11 +827,6 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
             Fh[m].velh[c] = b->serh[m].velh_buf[c];
         }
         Fh[m].temp = b->tempown + b->mdh[m].cell_off;
-        for (int k = 0; k < 3; ++k)
-            for (int c = 0; c < 3; ++c) Fh[m].pkset[k][c] = b->pkpool + (long long)(k * 3 + c) * G + b->mdh[m].cell_off;
-        for (int c = 0; c < 3; ++c) Fh[m].pk0[c] = Fh[m].pk1[c] = Fh[m].pkh[c] = Fh[m].pkset[0][c];
-        Fh[m].pks0 = Fh[m].pks1 = nullptr;
-        Fh[m].pk_rebuild = 0;
         b->serh[m].dT_vel = b->serh[m].dT_PAR = b->serh[m].dT_temp = 1.0;
     }
     b->bch.assign((size_t)nmembers * PI_NTRACERS * 6, FluxBC32{PI_BC_NONE, 0, 0, 0, nullptr});
@@ -1182,10 +1173,7 @@ static pi_status read_forcing(pi_batch* b, int m, MemberForcing& f) {
     BK(cudaStreamSynchronize(b->stream), "synchronize");
     return PI_OK;
 }
-static pi_status write_forcing(pi_batch* b, int m, const MemberForcing& fin, bool velocity = true) {
-    // a velocity the host replaced may sit at an address packed before: pack again
-    MemberForcing f = fin;
-    if (velocity) f.pks0 = f.pks1 = nullptr;
+static pi_status write_forcing(pi_batch* b, int m, const MemberForcing& f) {
     BK(cudaMemcpyAsync(b->F + m, &f, sizeof f, cudaMemcpyHostToDevice, b->stream), "write forcing");
     BK(cudaStreamSynchronize(b->stream), "synchronize");
     return PI_OK;

@@ -78,15 +78,6 @@ struct MemberForcing {
     const float* vel1[3];   // halo-padded velocity of this step
     const float* velh[3];   // (vel0 + vel1) / 2, or vel1 itself when vel0 and vel1 are the same field
     const float* temp;      // halo-padded temperature
-    // xy-quad copies of the three velocities for the particle kernel: element q of a component f
-    // is (f[q], f[q+Gx], f[q+1], f[q+1+Gx]), the 4 corners of the cell column face at one level
-    const float4* pk0[3];
-    const float4* pk1[3];
-    const float4* pkh[3];
-    const float* pks0;      // vel0[0] / vel1[0] that pk0 / pk1 were packed from (NULL: not packed)
-    const float* pks1;
-    float4* pkset[3][3];    // the member's three packed sets [set][component]
-    int pk_rebuild;         // bits 0, 1, 2: pack vel0, vel1, velh in this step
 };
 
 // Forcing time series resident on the device (PlanktonSimulation's arrays), or none.

@@ -139,8 +139,11 @@ __device__ __forceinline__ PGeom pgeom(const MemberDev& m, const MemberForcing& 
 
 // trilinear interpolation of one velocity component (member-local field pointer), in grid cells
 // per second
+// The 8 corner values come from the component's own halo-padded field: in the cell-sorted
+// storage order the lanes of a warp sit in neighbouring cells, so the corner loads of a warp
+// share sectors and the fields (12 bytes per cell) stay in L2.
 template <int COMP>
-__device__ __forceinline__ float itpl32(const PGeom& m, const float4* __restrict__ pk, int fid,
+__device__ __forceinline__ float itpl32(const PGeom& m, const float* __restrict__ fld, int fid,
                                         const float* __restrict__ rdzC, const Ax1& X, const Ax1& Y,
                                         const Ax1& Z, bool& bad, Corners& cc) {
     int i, j, k;
@@ -151,10 +154,11 @@ __device__ __forceinline__ float itpl32(const PGeom& m, const float4* __restrict
     i = clampb(i, 1, m.Gx - 1, bad); j = clampb(j, 1, m.Gy - 1, bad); k = clampb(k, 1, m.Gz - 1, bad);
     const int q = (i - 1) + m.Gx * ((j - 1) + m.Gy * (k - 1));
     if (cc.fid != fid || cc.q != q) {
-        const float4 lo = __ldg(pk + q), hi = __ldg(pk + q + m.Gx * m.Gy);     // levels k and k+1
+        const float* __restrict__ p = fld + q;                 // (i, j, k); level k+1 one slab on
+        const int sy = m.Gx, sz = m.Gx * m.Gy;
         cc.fid = fid; cc.q = q;
-        cc.v[0] = lo.x; cc.v[1] = lo.y; cc.v[2] = lo.z; cc.v[3] = lo.w;
-        cc.v[4] = hi.x; cc.v[5] = hi.y; cc.v[6] = hi.z; cc.v[7] = hi.w;
+        cc.v[0] = __ldg(p); cc.v[1] = __ldg(p + sy); cc.v[2] = __ldg(p + 1); cc.v[3] = __ldg(p + 1 + sy);
+        cc.v[4] = __ldg(p + sz); cc.v[5] = __ldg(p + sz + sy); cc.v[6] = __ldg(p + sz + 1); cc.v[7] = __ldg(p + sz + 1 + sy);
     }
     const float a0 = (1.0f - xd) * (1.0f - yd), a1 = (1.0f - xd) * yd, a2 = xd * (1.0f - yd), a3 = xd * yd;
     const float lo = a0 * cc.v[0] + a1 * cc.v[1] + a2 * cc.v[2] + a3 * cc.v[3];
@@ -187,29 +191,31 @@ __device__ __forceinline__ void add_fixed(unsigned long long* a, float v, double
 // Warp-segmented sums for the particle → grid scatters. In the cell-sorted storage order the
 // individuals of one cell sit in adjacent slots, so the lanes of a warp form runs of equal cell
 // keys; each run's first lane adds the run's total with one integer atomic instead of one atomic
-// per individual. Sums are integers (counts, fixed-point masses), so the result is the same
-// whatever the runs are. All 32 lanes call these with converged control flow; a key of -1 takes
-// no part.
+// per individual. A warp whose runs are short (more than 16 runs in 32 lanes) adds per lane: the
+// shuffles of the segmented sums would cost more than the atomics they save. Sums are integers
+// (counts, fixed-point masses), so the result is the same either way. All 32 lanes call these
+// with converged control flow; a key of -1 takes no part.
 struct WarpRuns {
-    bool head;      // first lane of its run
-    bool dup;       // some run in the warp is longer than one lane (warp-uniform)
+    bool head;      // this lane adds: the first lane of its run, or every lane when not aggregating
+    bool agg;       // the warp adds per run (warp-uniform)
     int end;        // last lane of this lane's run
 };
 __device__ __forceinline__ WarpRuns warp_runs(long long key) {
     const int lane = threadIdx.x & 31;
     const long long prev = __shfl_up_sync(0xffffffffu, key, 1);
     WarpRuns R;
-    R.head = lane == 0 || prev != key;
-    const unsigned heads = __ballot_sync(0xffffffffu, R.head);
+    const bool head = lane == 0 || prev != key;
+    const unsigned heads = __ballot_sync(0xffffffffu, head);
     const unsigned after = lane == 31 ? 0u : heads & ~((2u << lane) - 1u);
     R.end = after ? __ffs(after) - 2 : 31;
-    R.dup = heads != 0xffffffffu;
+    R.agg = __popc(heads) <= 16;
+    R.head = R.agg ? head : true;
     return R;
 }
 // the total of v over the lanes from this lane to the end of its run (the run's total at its head)
 template <typename T>
 __device__ __forceinline__ T run_sum(T v, const WarpRuns& R) {
-    if (!R.dup) return v;
+    if (!R.agg) return v;
     const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -279,48 +285,6 @@ __global__ void k32_velhalf(const MemberDev* __restrict__ md, const MemberForcin
         h0[q] = (f.vel0[0][q] + f.vel1[0][q]) * 0.5f;
         h1[q] = (f.vel0[1][q] + f.vel1[1][q]) * 0.5f;
         h2[q] = (f.vel0[2][q] + f.vel1[2][q]) * 0.5f;
-    }
-}
-
-// Which packed sets this step's velocities need (one thread per member). vel₀'s set is the one
-// packed from vel₁ last step (k32_end_step rotates it) unless the host replaced a field; vel₁
-// shares it when the field is the same array, else it is packed into another set; vel½ is packed
-// whenever it is a field of its own (recomputed in the steps where vel₀ ≠ vel₁).
-__global__ void k32_pack_bind(int nm, MemberForcing* __restrict__ F, const uint32_t* err) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= nm || stopped(err)) return;
-    MemberForcing f = F[m];
-    auto set_of = [&](const float4* p) { for (int k = 0; k < 3; ++k) if (f.pkset[k][0] == p) return k; return -1; };
-    int rb = 0;
-    int s0 = set_of(f.pk0[0]);
-    if (s0 < 0 || f.pks0 != f.vel0[0]) { if (s0 < 0) s0 = 0; rb |= 1; f.pks0 = f.vel0[0]; }
-    int s1 = s0;
-    if (f.vel1[0] == f.vel0[0]) f.pks1 = f.pks0;
-    else { s1 = (s0 + 1) % 3; rb |= 2; f.pks1 = f.vel1[0]; }
-    int sh = s1;
-    if (f.velh[0] != f.vel1[0]) { sh = s0 != s1 ? 3 - s0 - s1 : (s0 + 1) % 3; rb |= 4; }
-    for (int c = 0; c < 3; ++c) { f.pk0[c] = f.pkset[s0][c]; f.pk1[c] = f.pkset[s1][c]; f.pkh[c] = f.pkset[sh][c]; }
-    f.pk_rebuild = rb;
-    F[m] = f;
-}
-
-// Packing of the sets marked above. Grid: (x blocks, members, 9 = role × component).
-__global__ void k32_pack(const MemberDev* __restrict__ md, const MemberForcing* __restrict__ F, const uint32_t* err) {
-    const int m = blockIdx.y, role = blockIdx.z / 3, c = blockIdx.z % 3;
-    if (stopped(err)) return;
-    const MemberForcing& f = F[m];
-    if (!((f.pk_rebuild >> role) & 1)) return;
-    const float* __restrict__ src = role == 0 ? f.vel0[c] : role == 1 ? f.vel1[c] : f.velh[c];
-    float4* __restrict__ dst = f.pkset[0][0];
-    for (int k = 0; k < 3; ++k) {
-        const float4* want = role == 0 ? f.pk0[c] : role == 1 ? f.pk1[c] : f.pkh[c];
-        if (f.pkset[k][c] == want) dst = f.pkset[k][c];
-    }
-    const long long G = md[m].G, sy = md[m].Gx;
-    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < G; q += (long long)gridDim.x * blockDim.x) {
-        const long long q1 = q + 1 < G ? q + 1 : G - 1, qy = q + sy < G ? q + sy : G - 1;
-        const long long q1y = q + 1 + sy < G ? q + 1 + sy : G - 1;
-        dst[q] = make_float4(src[q], src[qy], src[q1], src[q1y]);
     }
 }
 
@@ -401,24 +365,24 @@ __device__ __forceinline__ MoveOut move_one(const MoveArgs& a, const MemberDev& 
     const float* __restrict__ rdzC = a.rdzC;
     Corners cu{-1, -1, {}}, cv{-1, -1, {}}, cw{-1, -1, {}};
     const int fh = pg.fh, f1 = pg.f1;
-    float u1 = itpl32<0>(pg, f.pk0[0], 0, rdzC, X0, Y0, Z0, bad, cu);
-    float v1 = itpl32<1>(pg, f.pk0[1], 0, rdzC, X0, Y0, Z0, bad, cv);
-    float w1 = itpl32<2>(pg, f.pk0[2], 0, rdzC, X0, Y0, Z0, bad, cw);
+    float u1 = itpl32<0>(pg, f.vel0[0], 0, rdzC, X0, Y0, Z0, bad, cu);
+    float v1 = itpl32<1>(pg, f.vel0[1], 0, rdzC, X0, Y0, Z0, bad, cv);
+    float w1 = itpl32<2>(pg, f.vel0[2], 0, rdzC, X0, Y0, Z0, bad, cw);
     float u2 = u1, v2 = v1, w2 = w1;
     Ax1 X = X0, Y = Y0, Z = Z0;
     move(X, u1 * hdT, pg.Nx, pg.tx); move(Y, v1 * hdT, pg.Ny, pg.ty); move(Z, -(w1 * hdT), pg.Nz, pg.tz);
-    u1 = itpl32<0>(pg, f.pkh[0], fh, rdzC, X, Y, Z, bad, cu); v1 = itpl32<1>(pg, f.pkh[1], fh, rdzC, X, Y, Z, bad, cv);
-    w1 = itpl32<2>(pg, f.pkh[2], fh, rdzC, X, Y, Z, bad, cw);
+    u1 = itpl32<0>(pg, f.velh[0], fh, rdzC, X, Y, Z, bad, cu); v1 = itpl32<1>(pg, f.velh[1], fh, rdzC, X, Y, Z, bad, cv);
+    w1 = itpl32<2>(pg, f.velh[2], fh, rdzC, X, Y, Z, bad, cw);
     u2 += u1 * 2.0f; v2 += v1 * 2.0f; w2 += w1 * 2.0f;
     X = X0; Y = Y0; Z = Z0;
     move(X, u1 * hdT, pg.Nx, pg.tx); move(Y, v1 * hdT, pg.Ny, pg.ty); move(Z, -(w1 * hdT), pg.Nz, pg.tz);
-    u1 = itpl32<0>(pg, f.pkh[0], fh, rdzC, X, Y, Z, bad, cu); v1 = itpl32<1>(pg, f.pkh[1], fh, rdzC, X, Y, Z, bad, cv);
-    w1 = itpl32<2>(pg, f.pkh[2], fh, rdzC, X, Y, Z, bad, cw);
+    u1 = itpl32<0>(pg, f.velh[0], fh, rdzC, X, Y, Z, bad, cu); v1 = itpl32<1>(pg, f.velh[1], fh, rdzC, X, Y, Z, bad, cv);
+    w1 = itpl32<2>(pg, f.velh[2], fh, rdzC, X, Y, Z, bad, cw);
     u2 += u1 * 2.0f; v2 += v1 * 2.0f; w2 += w1 * 2.0f;
     X = X0; Y = Y0; Z = Z0;
     move(X, u1 * dT, pg.Nx, pg.tx); move(Y, v1 * dT, pg.Ny, pg.ty); move(Z, -(w1 * dT), pg.Nz, pg.tz);
-    u1 = itpl32<0>(pg, f.pk1[0], f1, rdzC, X, Y, Z, bad, cu); v1 = itpl32<1>(pg, f.pk1[1], f1, rdzC, X, Y, Z, bad, cv);
-    w1 = itpl32<2>(pg, f.pk1[2], f1, rdzC, X, Y, Z, bad, cw);
+    u1 = itpl32<0>(pg, f.vel1[0], f1, rdzC, X, Y, Z, bad, cu); v1 = itpl32<1>(pg, f.vel1[1], f1, rdzC, X, Y, Z, bad, cv);
+    w1 = itpl32<2>(pg, f.vel1[2], f1, rdzC, X, Y, Z, bad, cw);
     const float sixth = 1.0f / 6.0f;
     u2 = (u2 + u1) * sixth; v2 = (v2 + v1) * sixth; w2 = (w2 + w1) * sixth;
     X = X0; Y = Y0; Z = Z0;
@@ -1718,8 +1682,7 @@ __global__ void k32_end_step(int nm, MemberForcing* __restrict__ F, StepState* s
     if (stopped(err)) return;
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m < nm) {
-        for (int c = 0; c < 3; ++c) { F[m].vel0[c] = F[m].vel1[c]; F[m].pk0[c] = F[m].pk1[c]; }
-        F[m].pks0 = F[m].pks1;
+        for (int c = 0; c < 3; ++c) F[m].vel0[c] = F[m].vel1[c];
     }
     if (m == 0) { st->iteration += 1; st->t = (double)st->iteration * dT; st->call_step += 1; }
 }
@@ -1778,12 +1741,12 @@ __global__ void k32_halo_vel(MemberDev m, float* __restrict__ c, int face_axis) 
 }
 
 // A setter's new own velocity (vel₁) and/or temperature of a member, bound on the device in
-// stream order (after the steps already queued); a replaced velocity is packed again.
+// stream order (after the steps already queued).
 __global__ void k32_bind_own(MemberForcing* __restrict__ F, int m, const float* u, const float* v, const float* w,
                              const float* temp) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     MemberForcing& f = F[m];
-    if (u) { f.vel1[0] = u; f.vel1[1] = v; f.vel1[2] = w; f.pks0 = nullptr; f.pks1 = nullptr; }
+    if (u) { f.vel1[0] = u; f.vel1[1] = v; f.vel1[2] = w; }
     if (temp) f.temp = temp;
 }
 
