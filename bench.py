@@ -161,8 +161,9 @@ def algorithmic_bytes(name, members, n_active_total, n_slots_total):
         return V * (2 * 14 * 4 + 8)
     if name == "k32_move":
         # active: cell, 3 offsets, flags, stat, Chl read; cell, offsets, flags, stat written;
-        # pop (4) and Chl (8) sums; inactive slots: flags and cell read
-        return n_active_total * (4 + 12 + 1 + 1 + 4 + 4 + 12 + 1 + 1 + 4 + 8) + inactive * 5
+        # pop (4) and Chl (8) sums; inactive slots: flags and cell read; the velocity field
+        # (u, v, w: 12 bytes per cell) read once
+        return n_active_total * (4 + 12 + 1 + 1 + 4 + 4 + 12 + 1 + 1 + 4 + 8) + inactive * 5 + V * 12
     if name == "k32_physiology":
         # flags, stat, cell, Bm..age read; Bm..age, flags written; 7 gathers; 5 consumption sums
         return n_active_total * (1 + 1 + 4 + 24 + 24 + 1 + 7 * 4 + 5 * 8) + inactive * 1
@@ -183,6 +184,19 @@ def step_roofline(n_ind, n_cells, ms_per_step):
     ach = byts / (ms_per_step / 1e3) / 1e9
     return {"bytes_per_step": int(byts), "achieved": round(ach, 1), "peak": hbm, "peak_source": kind,
             "unit": "GB/s", "frac": round(ach / hbm, 4)}
+
+
+def gpu_launches(prof, P, K, workload):
+    """Own kernels launched in K timed steps, from the kernels one profiled step launched: one per
+    profiled scope, except the halo fill (three passes in the 0D boxes, whose N < H) and the
+    storage-order sort (count, three scan passes, scatter; once per SORT_INTERVAL steps), plus
+    k32_copy_if_err and k32_end_step in every step."""
+    per_step = 2
+    for name, (n, _) in prof.items():
+        if name == "k32_sort":
+            continue
+        per_step += (3 if (name == "k32_halo" and workload == "config5") else 1) * n // P
+    return K * per_step + 5 * (-(-K // SORT_INTERVAL))
 
 
 def profile_roofline(prof, members, nact, nslots):
@@ -252,8 +266,8 @@ def run_fp32(members, args, dist, local, clocks_cls):
         b.profile_enable(False)
         if "k32_sort" in prof:
             # a sort runs once per SORT_INTERVAL steps: its share of a step
-            n, ms = prof["k32_sort"]
-            prof["k32_sort"] = (n, ms / n / SORT_INTERVAL * args.profile_steps)
+            n_sort, ms_sort = prof["k32_sort"]
+            prof["k32_sort"] = (n_sort, ms_sort / n_sort / SORT_INTERVAL * args.profile_steps)
     nslots = sum(w.capacity * w.nsp for w in members)
     roof, tot = profile_roofline(prof, members, b.count_active(), nslots) if prof else (None, 1.0)
     budgets = b.budget(0)
@@ -483,9 +497,7 @@ def run_ours(args):
             "roofline": r32["roof"],
             "step_roofline": step_roofline(ind_all / K, Vall, t_max / K),
             "cpu_baseline": cpu, "e2e": e2e, "clocks": r32["clocks"],
-            # own kernels per step: 13 with k32_tracer; the 0D boxes take the two-kernel tracer path
-            # and three halo passes (16); plus two per storage-order sort
-            "gpu_launches": K * (16 if args.workload == "config5" else 13) + 2 * (-(-K // SORT_INTERVAL)),
+            "gpu_launches": gpu_launches(prof, P, K, args.workload),
             "sort_interval": SORT_INTERVAL,
             "autotune": {"steps": r32["n_tune"], "choices": r32["tune"].strip().splitlines()},
         }
