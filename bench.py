@@ -72,7 +72,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--profile-steps", type=int, default=5)
     ap.add_argument("--tune-steps", type=int, default=2)
-    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-steps", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nx", type=int, default=None, help="config 2/3 horizontal size (smaller for profiling); "
                     "default 256 (config 2), 512 (config 3)")

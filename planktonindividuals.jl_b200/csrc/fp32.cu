@@ -79,6 +79,7 @@ struct Tuning {
     int ty = 16;                              // rows of an x-y tracer tile (4, 8, 16 or 28)
     int lz = 32;                              // levels walked by a z thread (8, 16, 32 or 64)
     int wpb_par = 2;
+    int occ_move = 2, occ_phys = 4;           // register fit of k32_move / k32_physiology (blocks of 256 per SM)
     int fused = 0;                            // k32_tracer when the batch allows it (the autotuner
                                               // picks it where it beats k32_xy + k32_ztail + halo fill)
     int lz_fused = 32;                        // levels finished per k32_tracer block
@@ -475,7 +476,10 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
         a.dT = fdT; a.Gtot = G; a.pop = b->pop; a.pop_sp = b->pop_sp; a.chl_acc = b->chl_acc; a.acc = b->acc;
         a.dcnt = b->dcnt; a.err = b->errw;
         BScope sc(b, "k32_move");
-        k32_move<<<tile_grid(b, b->tune.persist_move), b->tune.bs_move, 0, s>>>(a);
+        const unsigned g = tile_grid(b, b->tune.persist_move);
+        if (b->tune.occ_move == 4) k32_move<4><<<g, b->tune.bs_move, 0, s>>>(a);
+        else if (b->tune.occ_move == 3) k32_move<3><<<g, b->tune.bs_move, 0, s>>>(a);
+        else k32_move<2><<<g, b->tune.bs_move, 0, s>>>(a);
     }
     { BScope sc(b, "k32_par");
       k32_par<<<warp_grid(b->T.nicol, b->tune.wpb_par), 32 * b->tune.wpb_par, 0, s>>>(b->T, b->dzF, b->bgc, b->chl_acc, b->PARF,
@@ -497,7 +501,10 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
         a.err = b->errw; a.dec64 = b->dec64; a.guard = b->guard;
         a.dproc = b->diag_proc; a.pmask = b->proc_mask;
         BScope sc(b, "k32_physiology");
-        k32_physiology<<<tile_grid(b, b->tune.persist_phys), b->tune.bs_phys, 0, s>>>(a);
+        const unsigned g = tile_grid(b, b->tune.persist_phys);
+        if (b->tune.occ_phys == 4) k32_physiology<4><<<g, b->tune.bs_phys, 0, s>>>(a);
+        else if (b->tune.occ_phys == 3) k32_physiology<3><<<g, b->tune.bs_phys, 0, s>>>(a);
+        else k32_physiology<2><<<g, b->tune.bs_phys, 0, s>>>(a);
     }
     {
         TrArgs a;
@@ -1722,8 +1729,10 @@ pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t k, char* report, siz
     struct Knob { const char* kernel; int* field; std::vector<int> values; const char* label; int threads_per_value; };
     Tuning& t = b->tune;
     std::vector<Knob> knobs = {
+        { "k32_move", &t.occ_move, {2, 3, 4}, "move register fit (blocks of 256 per SM)", 0 },
         { "k32_move", &t.bs_move, {128, 256, 512, 1024}, "move block", 1 },
         { "k32_move", &t.persist_move, {0, 2, 4, 8}, "move blocks/SM (0 = one tile per block)", 0 },
+        { "k32_physiology", &t.occ_phys, {2, 3, 4}, "physiology register fit (blocks of 256 per SM)", 0 },
         { "k32_physiology", &t.bs_phys, {128, 256, 512, 1024}, "physiology block", 1 },
         { "k32_physiology", &t.persist_phys, {0, 2, 4, 8}, "physiology blocks/SM (0 = one tile per block)", 0 },
         { "k32_assign", &t.bs_assign, {128, 256, 512, 1024}, "assign block", 1 },
@@ -1735,8 +1744,8 @@ pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t k, char* report, siz
     auto max_threads = [](const char* kernel) -> int {
         cudaFuncAttributes fa{};
         const void* f = nullptr;
-        if (!strcmp(kernel, "k32_move")) f = (const void*)k32_move;
-        else if (!strcmp(kernel, "k32_physiology")) f = (const void*)k32_physiology;
+        if (!strcmp(kernel, "k32_move")) f = (const void*)k32_move<2>;
+        else if (!strcmp(kernel, "k32_physiology")) f = (const void*)k32_physiology<2>;
         else if (!strcmp(kernel, "k32_assign")) f = (const void*)k32_assign;
         else if (!strcmp(kernel, "k32_par")) f = (const void*)k32_par;
         if (!f || cudaFuncGetAttributes(&fa, f) != cudaSuccess) return 256;

@@ -461,7 +461,10 @@ __device__ __forceinline__ void scatter_move(const MoveArgs& a, int s, const Mov
     }
 }
 
-__global__ void __launch_bounds__(256, 2) k32_move(MoveArgs a) {
+// MINB: blocks of 256 threads per SM the registers are fitted for (2: 128 registers, 3: 80, 4: 64);
+// the autotuner picks the variant.
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k32_move(MoveArgs a) {
     if (stopped(a.err)) return;
     __shared__ PGeom sg;
     const int bs = blockDim.x, ppt = F32_TILE / bs;
@@ -1017,7 +1020,8 @@ __device__ __forceinline__ void scatter_phys(const PhysArgs& a, int s, const Phy
     }
 }
 
-__global__ void __launch_bounds__(256, 4) k32_physiology(PhysArgs a) {
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k32_physiology(PhysArgs a) {
     if (stopped(a.err)) return;
     const int bs = blockDim.x, ppt = F32_TILE / bs;
     const uint32_t iter = (uint32_t)(a.st->iteration + 1);
