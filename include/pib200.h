@@ -279,6 +279,12 @@ pi_status pi_last_error(pi_model* m, char* buf, size_t len);
 /* Static description of a status code. */
 const char* pi_status_string(pi_status code);
 
+/* Self-test of the bounded device-side waits (no counterpart in the reference): a kernel waits on
+ * an mbarrier that nothing arrives on, with the same helper the tracer kernel's staging waits use,
+ * and gives up after limit_ns (at most 2 s). *gave_up = 1 and *waited_ns >= limit_ns show that a
+ * wait that cannot complete ends with an error status and leaves the context usable. */
+pi_status pi_selftest_bounded_wait(int64_t limit_ns, int32_t* gave_up, int64_t* waited_ns);
+
 /* ---------------------------------------------------------------------------------------------
  * Batched FP32 form. A batch holds independent members, each a PlanktonModel of its own (grid,
  * parameters, capacity, individuals, tracers, forcing, seed), that are advanced together: every

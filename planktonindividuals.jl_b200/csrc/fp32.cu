@@ -1647,6 +1647,22 @@ pi_status pi_batch_guard_stats(pi_batch* b, int64_t* recomputed, int64_t* change
     return PI_OK;
 }
 
+pi_status pi_selftest_bounded_wait(int64_t limit_ns, int32_t* gave_up, int64_t* waited_ns) {
+    if (limit_ns <= 0 || limit_ns > 2000000000LL || !gave_up || !waited_ns) return PI_ERR_ARG;
+    int* d = nullptr;
+    if (cudaMalloc(&d, 16) != cudaSuccess) return PI_ERR_NOMEM;
+    k32_wait_selftest<<<1, 32>>>((unsigned long long)limit_ns, d, (unsigned long long*)(d + 2));
+    int h[4] = {0, 0, 0, 0};
+    cudaError_t e = cudaMemcpy(h, d, 16, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return PI_ERR_CUDA;
+    *gave_up = h[0];
+    unsigned long long w = 0;
+    memcpy(&w, h + 2, sizeof w);
+    *waited_ns = (int64_t)w;
+    return PI_OK;
+}
+
 pi_status pi_batch_set_tracer_kernel(pi_batch* b, int32_t fused, int32_t levels) {
     if (!b || (fused != 0 && fused != 1) || (levels != 8 && levels != 16 && levels != 32 && levels != 64))
         return bfail(b, PI_ERR_ARG, "pi_batch_set_tracer_kernel: fused must be 0 or 1 and levels 8, 16, 32 or 64");

@@ -89,14 +89,28 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
     asm volatile("mov.u64 %0, %globaltimer;\n" : "=l"(t));
     return t;
 }
-// Bounded wait on an mbarrier phase (one second at most); false when it gave up.
-__device__ __forceinline__ bool mbar_wait(unsigned addr, unsigned parity) {
+// Bounded wait on an mbarrier phase (one second at most by default); false when it gave up.
+__device__ __forceinline__ bool mbar_wait(unsigned addr, unsigned parity, unsigned long long limit_ns = 1000000000ull) {
     if (mbar_try_wait(addr, parity)) return true;
     const unsigned long long t0 = globaltimer_ns();
     do {
         if (mbar_try_wait(addr, parity)) return true;
-    } while (globaltimer_ns() - t0 < 1000000000ull);
+    } while (globaltimer_ns() - t0 < limit_ns);
     return false;
+}
+
+// Self-test of the bounded wait: one thread waits on an mbarrier that nothing arrives on, with the
+// given limit, and records whether it gave up (1) and how long it waited.
+__global__ void k32_wait_selftest(unsigned long long limit_ns, int* gave_up, unsigned long long* waited_ns) {
+    __shared__ __align__(8) unsigned long long bar;
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const unsigned a = (unsigned)__cvta_generic_to_shared(&bar);
+    mbar_init(a, 1u);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    const unsigned long long t0 = globaltimer_ns();
+    const bool ok = mbar_wait(a, 0u, limit_ns);
+    *waited_ns = globaltimer_ns() - t0;
+    *gave_up = ok ? 0 : 1;
 }
 
 // The cells an interior cell a (1-based, along one axis of N >= H cells with H halo points) stands

@@ -14,7 +14,7 @@ import pytest
 import oracle
 from PlanktonIndividuals import _abi, workloads as W
 from PlanktonIndividuals._native import CModel, PIError
-from helpers import compare_states
+from helpers import VelCache, compare_states, drive
 
 pytestmark = pytest.mark.gpu
 
@@ -68,4 +68,20 @@ def test_domain_error_above_cfl_one(gpu_lib, precision):
     assert e_ref.value.code == e_gpu.value.code == _abi.PI_ERR_DOMAIN
     if precision == _abi.PI_FP64:
         assert compare_states(ref, m, wl.nsp) == []
+    m.close()
+
+
+def test_bounded_wait_gives_up_and_context_stays_usable(gpu_lib):
+    """A device-side wait on an mbarrier that nothing arrives on (the helper the tracer kernel's
+    staging waits use) gives up after its limit and reports it; the context runs a step afterwards."""
+    import ctypes as ct
+    gave, waited = ct.c_int32(-1), ct.c_int64(0)
+    assert gpu_lib.pi_selftest_bounded_wait(ct.c_int64(20_000_000), ct.byref(gave), ct.byref(waited)) == 0
+    assert gave.value == 1
+    assert 20_000_000 <= waited.value < 1_000_000_000
+    wl = W.config1(n=16, N=256, steps=2)
+    m = CModel(gpu_lib, "pi_", wl.grid, wl.bgc, wl.phyt, wl.nsp, wl.capacity, wl.seed, precision=_abi.PI_FP32)
+    m.set_state(wl.individuals, wl.tracers)
+    drive(m, wl, 2, VelCache(wl))
+    assert m.count_active(0) > 0
     m.close()
