@@ -350,7 +350,7 @@ def test_storage_order_changes_no_result(gpu_lib):
     (draws are keyed by slot number, divisions assigned in slot order)."""
     wls = _uneven_members()
     runs = []
-    for interval in (0, 1, 7):
+    for interval in (0, 1, 7, 32):
         batch = PlanktonBatch(_members(wls), nspecies=2)
         batch.set_sort_interval(interval)
         for m, wl in enumerate(wls):
