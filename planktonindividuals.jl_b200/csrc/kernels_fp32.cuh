@@ -867,10 +867,14 @@ __device__ __forceinline__ bool near_threshold(float r, float t) {
 }
 
 // flags, status, cell and logical slot of a slot, loaded one slot ahead of its physiology
-struct PHead { int32_t code, ls; uint8_t fl, stt; };
+// and, for an active slot, its quotas and age (so only the environment gather waits in phys_one)
+struct PHead { int32_t code, ls; uint8_t fl, stt; float Bm, Cq, Nq, Pq, Chl, age; };
 __device__ __forceinline__ PHead phys_head(const IndDev32& P, long long g, bool valid) {
-    PHead h{-1, 0, 0, 0};
-    if (valid) { h.fl = P.flags[g]; h.stt = P.stat[g]; h.code = P.cell[g]; h.ls = P.lslot[g]; }
+    PHead h{-1, 0, 0, 0, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    if (valid) {
+        h.fl = P.flags[g]; h.stt = P.stat[g]; h.code = P.cell[g]; h.ls = P.lslot[g];
+        if (h.fl & F32_AC) { h.Bm = P.Bm[g]; h.Cq = P.Cq[g]; h.Nq = P.Nq[g]; h.Pq = P.Pq[g]; h.Chl = P.Chl[g]; h.age = P.age[g]; }
+    }
     return h;
 }
 
@@ -910,7 +914,7 @@ __device__ __forceinline__ PhysOut phys_one(const PhysArgs& a, const MemberDev& 
         Tm = a.F[mi].temp[q];
         popv = (float)(a.pop_sp ? a.pop_sp[(long long)s * G + cq] : a.pop[cq]);
     }
-    float Bm = P.Bm[g], Cq = P.Cq[g], Nq = P.Nq[g], Pq = P.Pq[g], Chl = P.Chl[g];
+    float Bm = hd.Bm, Cq = hd.Cq, Nq = hd.Nq, Pq = hd.Pq, Chl = hd.Chl;
     const double fx_inv = m.fx_inv;         // read before the stores below
     const float tf = tempFunc_f(Tm, p);
     // calc_inorganic_uptake_kernel! (:48-56)
@@ -946,7 +950,7 @@ __device__ __forceinline__ PhysOut phys_one(const PhysArgs& a, const MemberDev& 
     // update_biomass_kernel! (:146-154)
     Bm += dT * BS; Cq -= dT * (BS + exu); Nq -= dT * BS * p.R_NC; Pq -= dT * BS * p.R_PC;
     Chl += dT * BS * p.R_NC * rChl;
-    const float age = P.age[g] + dT / 3600.0f;
+    const float age = hd.age + dT / 3600.0f;
     // update_cellsize_kernel! (:163-166) and the probabilities (division_death_probability.jl:7-68)
     const float Sz = Bm / (p.Cquota * p.Nsuper);
     const float graz = popv * p.grz_P;
@@ -1168,23 +1172,35 @@ struct TrArgs {
 // shuffles). The face coefficients are computed once per face and shared by the 14 tracers.
 // Shared memory [row][tracer][lane]: TA (after x), FY (y face fluxes), TRs (tracer of the rows
 // the y sweep updates).
-// The x-sweep inputs of one item for this thread (its row and column): u and the 14 tracers.
-// A block loops over items and loads the next item's inputs while it works on the current one.
-__device__ __forceinline__ void xy_load(const TrArgs& a, int item, float& u, float* v) {
+// The inputs of one item for this thread (its row and column): u and the 14 tracers of the x
+// sweep, and the y velocities it reads later — v at its y face j0 + wid (x) and at the two faces
+// of its row (y, z; in range whenever the row is updated). A block loops over items and loads the
+// next item's inputs while it works on the current one.
+__device__ __forceinline__ void xy_load(const TrArgs& a, int item, float& u, float* v, float3& vy) {
     const int4 it = a.items[item];
     const MemberDev& m = a.T.md[it.x];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int jj = wrap_ax(it.z - 2 + wid, m.Ny, m.Hy, m.ty);
-    const int q = gid3(m, min(it.y - 2 + lane, m.Gx), jj, it.w);
-    u = a.F[it.x].vel1[0][q];
+    const int ic = min(it.y - 2 + lane, m.Gx);
+    const int q = gid3(m, ic, jj, it.w);
+    const MemberForcing& F = a.F[it.x];
+    u = F.vel1[0][q];
     const float* __restrict__ src = a.tr + m.cell_off + q;
 #pragma unroll
     for (int n = 0; n < PI_NTRACERS; ++n) v[n] = src[n * a.Gtot];
+    const int f = it.z + wid;
+    const int fs = f == m.Ny + m.Hy + 1 ? m.Hy + 1 : min(f, m.Ny + m.Hy);
+    const int jr = min(f, m.Gy - 1);
+    const float* __restrict__ vv = F.vel1[1];
+    vy.x = vv[gid3(m, ic, fs, it.w)];
+    const int qr = gid3(m, ic, jr, it.w);
+    vy.y = vv[qr];
+    vy.z = vv[qr + m.Gx];
 }
 
 template <int TY, bool LM>
 __device__ __forceinline__ void xy_tile(const TrArgs& a, const MemberDev& m, const int4 it, float* sm,
-                                        float& pu, float* pv, int next) {
+                                        float& pu, float* pv, float3& pvy, int next) {
     float* TA = sm;                                        // (TY+4) × 14 × 32
     float* FY = TA + (TY + 4) * PI_NTRACERS * 32;          // (TY+1) × 14 × 32
     float* TRs = FY + (TY + 1) * PI_NTRACERS * 32;         // TY × 14 × 32
@@ -1194,7 +1210,6 @@ __device__ __forceinline__ void xy_tile(const TrArgs& a, const MemberDev& m, con
     const float dT = a.dT;
     const int i0 = it.y, j0 = it.z, L = it.w;
     const long long off = m.cell_off;
-    const MemberForcing& F = a.F[it.x];
     const float dz = a.dzF[m.dz_off + L - 1];
     const float az = __fmul_rn(m.dx, m.dy), dtv = __fdiv_rn(dT, __fmul_rn(az, dz));
     // ---- x sweep of row j0-2+wid
@@ -1229,19 +1244,19 @@ __device__ __forceinline__ void xy_tile(const TrArgs& a, const MemberDev& m, con
     }
     __syncthreads();
     // the registers of this item's x inputs are free: start the next item's loads
-    if (next < a.nitems) xy_load(a, next, pu, pv);
+    const float3 vy = pvy;
+    if (next < a.nitems) xy_load(a, next, pu, pv, pvy);
     // ---- y faces j0 + r, r = 0..TY
     const int i = i0 - 2 + lane;
     const bool col = lane >= 2 && lane < 30 && i <= m.Nx + m.Hx;
     const float ay = __fmul_rn(m.dx, dz);
-    const float* vv = F.vel1[1];
     if (wid <= TY) {
         const int r = wid, f = j0 + r;
         const bool special = f == m.Ny + m.Hy + 1;
         const bool zero = !col || f > m.Ny + m.Hy + 1 || (special && m.ty != PI_PERIODIC);
         const int fs = special ? m.Hy + 1 : min(f, m.Ny + m.Hy);
         const int ic = min(i, m.Gx);
-        const FCu fc = fcu(zero ? 0.0f : vv[gid3(m, ic, fs, L)], ay, __frcp_rn(m.dy), dT);
+        const FCu fc = fcu(zero ? 0.0f : vy.x, ay, __frcp_rn(m.dy), dT);
         int L2 = 1, L1 = 1, L0 = 1, Lp = 1;
         if (LM) {
             L2 = lm32(m, a.lm, ic, fs - 2, L); L1 = lm32(m, a.lm, ic, fs - 1, L);
@@ -1259,7 +1274,7 @@ __device__ __forceinline__ void xy_tile(const TrArgs& a, const MemberDev& m, con
         if (col && j <= m.Ny + m.Hy) {
             const int q = gid3(m, i, j, L);
             const int c0m = LM ? lm32(m, a.lm, i, j, L) : 1, cpm = LM ? lm32(m, a.lm, i, j + 1, L) : 1;
-            const float ftr = mk<LM>(tdiff(ay, vv[q + m.Gx], vv[q]), cpm, c0m);
+            const float ftr = mk<LM>(tdiff(ay, vy.z, vy.y), cpm, c0m);
             float* dst = a.tb + off + q;
 #pragma unroll
             for (int n = 0; n < PI_NTRACERS; ++n) {
@@ -1277,13 +1292,14 @@ __global__ void __launch_bounds__(32 * (TY + 4)) k32_xy(TrArgs a) {
     extern __shared__ float sm[];
     if ((int)blockIdx.x >= a.nitems) return;
     float pu, pv[PI_NTRACERS];
-    xy_load(a, blockIdx.x, pu, pv);
+    float3 pvy;
+    xy_load(a, blockIdx.x, pu, pv, pvy);
     for (int item = blockIdx.x; item < a.nitems; item += gridDim.x) {
         const int4 it = a.items[item];
         const MemberDev& m = a.T.md[it.x];
         const int next = item + gridDim.x;
-        if (m.all_water) xy_tile<TY, false>(a, m, it, sm, pu, pv, next);
-        else xy_tile<TY, true>(a, m, it, sm, pu, pv, next);
+        if (m.all_water) xy_tile<TY, false>(a, m, it, sm, pu, pv, pvy, next);
+        else xy_tile<TY, true>(a, m, it, sm, pu, pv, pvy, next);
     }
 }
 
