@@ -393,6 +393,13 @@ pi_status pi_batch_guard_stats(pi_batch* b, int64_t* recomputed, int64_t* change
  * boundary conditions, at least as many cells as halo points on each axis); fused = 0 runs the x-y
  * kernel, the z kernel and the halo fill. Results are identical either way. */
 pi_status pi_batch_set_tracer_kernel(pi_batch* b, int32_t fused, int32_t levels);
+/* One launch-shape option (no counterpart in the reference; pi_batch_autotune sets them all):
+ * "move_block" 128|256, "move_fit" 2|3|4 (register fit: blocks of 256 per SM),
+ * "move_blocks_per_sm" 0|2|4|8 (0: one tile per block), the same three for "physiology_",
+ * "xy_rows" 4|8|16|28, "z_levels" 8|16|32|64, "par_warps" 1|2|4|8, "tracer_fused" 0|1,
+ * "tracer_fused_levels" 8|16|32|64, "xy_beside_particles" 0|1 (the x-y tracer kernel on a second
+ * graph branch beside the particle kernels). Results are identical for every choice. */
+pi_status pi_batch_set_option(pi_batch* b, const char* name, int32_t value);
 /* Storage order (no counterpart in the reference, which stores individuals in slot order): each
  * (member, species) segment is kept in an order grouped by cell, restored by a counting sort
  * before the first step after pi_batch_set_individuals and then every `steps` steps (default 32;

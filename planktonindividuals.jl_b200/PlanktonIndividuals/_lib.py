@@ -107,4 +107,4 @@ EXPORTS = ("pi_create", "pi_destroy", "pi_set_individuals", "pi_get_individuals"
            "pi_set_velocity_f32", "pi_set_PARF_f32", "pi_set_temp_f32", "pi_time_step_async",
            "pi_count_active_async", "pi_batch_set_velocity_f32", "pi_batch_set_PARF_f32", "pi_batch_set_temp_f32",
            "pi_batch_count_active_async", "pi_batch_guard_stats",
-           "pi_set_diags", "pi_batch_set_diags", "pi_sim_update_steps", "pi_batch_step_from", "pi_get_budget", "pi_batch_set_tracer_kernel", "pi_selftest_bounded_wait")
+           "pi_set_diags", "pi_batch_set_diags", "pi_sim_update_steps", "pi_batch_step_from", "pi_get_budget", "pi_batch_set_tracer_kernel", "pi_selftest_bounded_wait", "pi_batch_set_option")

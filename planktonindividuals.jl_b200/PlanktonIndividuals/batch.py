@@ -215,6 +215,11 @@ class PlanktonBatch:
         and z kernels with the halo fill (pi_batch_set_tracer_kernel); results are identical."""
         self._check(self.lib.pi_batch_set_tracer_kernel(self.h, 1 if fused else 0, int(levels)), "set_tracer_kernel")
 
+    def set_option(self, name, value):
+        """One launch-shape option by name (pi_batch_set_option); results are identical for every
+        choice."""
+        self._check(self.lib.pi_batch_set_option(self.h, name.encode(), int(value)), "set_option")
+
     def synchronize(self):
         self._check(self.lib.pi_batch_synchronize(self.h), "synchronize")
 

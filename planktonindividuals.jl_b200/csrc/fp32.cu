@@ -81,6 +81,7 @@ struct Tuning {
     int lz = 32;                              // levels walked by a z thread (8, 16, 32 or 64)
     int wpb_par = 2;
     int occ_move = 2, occ_phys = 4;           // register fit of k32_move / k32_physiology (blocks of 256 per SM)
+    int concurrent = 0;                       // k32_xy on a second branch beside the particle kernels
     int fused = 0;                            // k32_tracer when the batch allows it (the autotuner
                                               // picks it where it beats k32_xy + k32_ztail + halo fill)
     int lz_fused = 32;                        // levels finished per k32_tracer block
@@ -157,6 +158,8 @@ struct pi_batch {
     // forcing setters: host→device copies on their own stream into double-buffered staging, so
     // they overlap the steps already queued; the conversion runs on the model stream
     cudaStream_t cstream = nullptr;
+    cudaStream_t s2 = nullptr;                 // second branch of a step (k32_xy beside the particle kernels)
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     struct Stage { unsigned char* p[2] = {nullptr, nullptr}; cudaEvent_t copied[2] = {nullptr, nullptr};
                    cudaEvent_t freed[2] = {nullptr, nullptr}; int k = 0; };
     Stage vst, tst, pst;            // velocity (3 × maxG values), temperature (maxG), PARF (maxcol)
@@ -233,14 +236,15 @@ struct BScope {
     pi_batch* b;
     pi_batch::Mark mk;
     bool on;
-    BScope(pi_batch* b_, const char* name) : b(b_), on(b_->profiling != 0) {
+    cudaStream_t st;
+    BScope(pi_batch* b_, const char* name, cudaStream_t s_ = nullptr) : b(b_), on(b_->profiling != 0), st(s_ ? s_ : b_->stream) {
         if (!on) return;
         mk.name = name; mk.a = take_event(b); mk.b = take_event(b);
-        cudaEventRecord(mk.a, b->stream);
+        cudaEventRecord(mk.a, st);
     }
     ~BScope() {
         if (!on) return;
-        cudaEventRecord(mk.b, b->stream);
+        cudaEventRecord(mk.b, st);
         b->marks.push_back(mk);
     }
 };
@@ -345,6 +349,9 @@ void free_batch(pi_batch* b) {
             if (st->copied[k]) cudaEventDestroy(st->copied[k]);
             if (st->freed[k]) cudaEventDestroy(st->freed[k]);
         }
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->ev_join) cudaEventDestroy(b->ev_join);
+    if (b->s2) cudaStreamDestroy(b->s2);
     if (b->cstream) cudaStreamDestroy(b->cstream);
     if (b->stream) cudaStreamDestroy(b->stream);
     b->stream = nullptr;
@@ -471,6 +478,38 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
     { BScope sc(b, "k32_velhalf");
       const unsigned gx = fgx;
       k32_velhalf<<<dim3(gx, b->nm), 256, 0, s>>>(b->md, b->F, b->errw); }
+    TrArgs ta;
+    ta.T = b->T; ta.lm = b->lm; ta.dzF = b->dzF; ta.dzC = b->dzC; ta.rdzC = b->rdzC; ta.bgc = b->bgc;
+    ta.bcs = b->bcs; ta.st = b->st; ta.F = b->F; ta.Gtot = G; ta.tr = tr; ta.tb = b->tb; ta.tr_next = trn;
+    ta.acc = b->acc; ta.pop = b->pop; ta.dT = fdT; ta.err = b->errw;
+    ta.halo_in_walk = b->halo_direct ? 1 : 0;
+    // k32_xy reads the tracers at the start of the step and this step's u and v only, so it can run
+    // on a second branch beside the particle kernels; k32_ztail joins the two
+    auto launch_xy = [&](cudaStream_t st) {
+        TrArgs a = ta;
+        a.items = b->xy_items; a.nitems = b->nxy_items;
+        BScope sc(b, "k32_xy", st);
+        // persistent: as many blocks as fit at once, each looping over items with the next
+        // item's loads in flight
+        int per_sm = 1;
+        const int ty = b->tune.ty;
+        if (ty == 28) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k32_xy<28>, 32 * 32, xy_smem(28));
+        else if (ty == 16) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k32_xy<16>, 32 * 20, xy_smem(16));
+        else if (ty == 8) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k32_xy<8>, 32 * 12, xy_smem(8));
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k32_xy<4>, 32 * 8, xy_smem(4));
+        const unsigned grid = (unsigned)std::max(1, std::min(b->nxy_items, std::max(1, per_sm) * b->nsm));
+        if (ty == 28) k32_xy<28><<<grid, 32 * 32, xy_smem(28), st>>>(a);
+        else if (ty == 16) k32_xy<16><<<grid, 32 * 20, xy_smem(16), st>>>(a);
+        else if (ty == 8) k32_xy<8><<<grid, 32 * 12, xy_smem(8), st>>>(a);
+        else k32_xy<4><<<grid, 32 * 8, xy_smem(4), st>>>(a);
+    };
+    const bool branch = !fused && b->tune.concurrent;
+    if (branch) {
+        BK(cudaEventRecord(b->ev_fork, s), "fork");
+        BK(cudaStreamWaitEvent(b->s2, b->ev_fork, 0), "fork");
+        launch_xy(b->s2);
+        BK(cudaEventRecord(b->ev_join, b->s2), "join");
+    }
     {
         MoveArgs a;
         a.T = b->T; a.P = b->P; a.sp = b->sp; a.bgc = b->bgc; a.F = b->F; a.rdzC = b->rdzC; a.st = b->st;
@@ -508,11 +547,7 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
         else k32_physiology<2><<<g, b->tune.bs_phys, 0, s>>>(a);
     }
     {
-        TrArgs a;
-        a.T = b->T; a.lm = b->lm; a.dzF = b->dzF; a.dzC = b->dzC; a.rdzC = b->rdzC; a.bgc = b->bgc;
-        a.bcs = b->bcs; a.st = b->st; a.F = b->F; a.Gtot = G; a.tr = tr; a.tb = b->tb; a.tr_next = trn;
-        a.acc = b->acc; a.pop = b->pop; a.dT = fdT; a.err = b->errw;
-        a.halo_in_walk = b->halo_direct ? 1 : 0;
+        TrArgs a = ta;
         if (fused) {
             TrkArgs A;
             A.a = a;
@@ -522,23 +557,8 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
             BScope sc(b, "k32_tracer");
             k32_tracer<<<dim3((unsigned)std::max(1, b->ntrk_items), 2), TRK_THREADS, tracer_smem_bytes(), s>>>(A);
         } else {
-        {
-            a.items = b->xy_items; a.nitems = b->nxy_items;
-            BScope sc(b, "k32_xy");
-            // persistent: as many blocks as fit at once, each looping over items with the next
-            // item's loads in flight
-            int per_sm = 1;
-            const int ty = b->tune.ty;
-            if (ty == 28) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k32_xy<28>, 32 * 32, xy_smem(28));
-            else if (ty == 16) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k32_xy<16>, 32 * 20, xy_smem(16));
-            else if (ty == 8) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k32_xy<8>, 32 * 12, xy_smem(8));
-            else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k32_xy<4>, 32 * 8, xy_smem(4));
-            const unsigned grid = (unsigned)std::max(1, std::min(b->nxy_items, std::max(1, per_sm) * b->nsm));
-            if (ty == 28) k32_xy<28><<<grid, 32 * 32, xy_smem(28), s>>>(a);
-            else if (ty == 16) k32_xy<16><<<grid, 32 * 20, xy_smem(16), s>>>(a);
-            else if (ty == 8) k32_xy<8><<<grid, 32 * 12, xy_smem(8), s>>>(a);
-            else k32_xy<4><<<grid, 32 * 8, xy_smem(4), s>>>(a);
-        }
+        if (branch) BK(cudaStreamWaitEvent(s, b->ev_join, 0), "join");
+        else launch_xy(s);
         {
             a.items = b->z_items; a.nitems = b->nz_items;
             BScope sc(b, "k32_ztail");
@@ -690,7 +710,10 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
     cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, b->device);
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) { b->err = "pi_batch_create: stream"; return bail(PI_ERR_CUDA); }
     if (cudaEventCreateWithFlags(&b->copied, cudaEventDisableTiming) != cudaSuccess) { b->err = "pi_batch_create: event"; return bail(PI_ERR_CUDA); }
-    if (cudaStreamCreateWithFlags(&b->cstream, cudaStreamNonBlocking) != cudaSuccess) { b->err = "pi_batch_create: stream"; return bail(PI_ERR_CUDA); }
+    if (cudaStreamCreateWithFlags(&b->cstream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->s2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) != cudaSuccess) { b->err = "pi_batch_create: stream"; return bail(PI_ERR_CUDA); }
     for (pi_batch::Stage* st : { &b->vst, &b->tst, &b->pst })
         for (int k = 0; k < 2; ++k)
             if (cudaEventCreateWithFlags(&st->copied[k], cudaEventDisableTiming) != cudaSuccess ||
@@ -1660,6 +1683,34 @@ pi_status pi_selftest_bounded_wait(int64_t limit_ns, int32_t* gave_up, int64_t* 
     return PI_OK;
 }
 
+pi_status pi_batch_set_option(pi_batch* b, const char* name, int32_t value) {
+    if (!b || !name) return bfail(b, PI_ERR_ARG, "pi_batch_set_option: NULL argument");
+    struct Opt { const char* name; int Tuning::*field; std::vector<int> values; };
+    static const Opt opts[] = {
+        { "move_block", &Tuning::bs_move, {128, 256} },
+        { "move_fit", &Tuning::occ_move, {2, 3, 4} },
+        { "move_blocks_per_sm", &Tuning::persist_move, {0, 2, 4, 8} },
+        { "physiology_block", &Tuning::bs_phys, {128, 256} },
+        { "physiology_fit", &Tuning::occ_phys, {2, 3, 4} },
+        { "physiology_blocks_per_sm", &Tuning::persist_phys, {0, 2, 4, 8} },
+        { "xy_rows", &Tuning::ty, {4, 8, 16, 28} },
+        { "z_levels", &Tuning::lz, {8, 16, 32, 64} },
+        { "par_warps", &Tuning::wpb_par, {1, 2, 4, 8} },
+        { "tracer_fused", &Tuning::fused, {0, 1} },
+        { "tracer_fused_levels", &Tuning::lz_fused, {8, 16, 32, 64} },
+        { "xy_beside_particles", &Tuning::concurrent, {0, 1} },
+    };
+    for (const Opt& o : opts) {
+        if (strcmp(o.name, name)) continue;
+        if (std::find(o.values.begin(), o.values.end(), (int)value) == o.values.end())
+            return bfail(b, PI_ERR_ARG, std::string("pi_batch_set_option: value not allowed for ") + name);
+        b->tune.*o.field = value;
+        free_graphs(b);
+        return PI_OK;
+    }
+    return bfail(b, PI_ERR_ARG, std::string("pi_batch_set_option: unknown option ") + name);
+}
+
 pi_status pi_batch_set_tracer_kernel(pi_batch* b, int32_t fused, int32_t levels) {
     if (!b || (fused != 0 && fused != 1) || (levels != 8 && levels != 16 && levels != 32 && levels != 64))
         return bfail(b, PI_ERR_ARG, "pi_batch_set_tracer_kernel: fused must be 0 or 1 and levels 8, 16, 32 or 64");
@@ -1716,13 +1767,16 @@ pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t k, char* report, siz
     if (!b || !(dT > 0) || k < 1) return bfail(b, PI_ERR_ARG, "pi_batch_autotune: bad argument");
     const int was = b->profiling;
     std::string rep;
-    // average time per step of the kernels named (a name, or several separated by '|')
+    // average time per step of the kernels named (a name, or several separated by '|'; "step": the
+    // whole step, start to end on the batch stream)
+    cudaEvent_t st0 = take_event(b), st1 = take_event(b);
     auto kernel_ms = [&](const char* name, double& out) -> pi_status {
         pi_status e;
         b->profiling = 1;
         b->prof_names.clear(); b->prof_count.clear(); b->prof_ms.clear();
         b->last_dT = dT;
         if ((e = build_tables(b))) return e;
+        BK(cudaEventRecord(st0, b->stream), "tuning event");
         for (int i = 0; i < k; ++i) {
             if ((e = maybe_sort(b))) return e;
             if ((e = enqueue_step(b, dT, b->cur))) return e;
@@ -1730,10 +1784,17 @@ pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t k, char* report, siz
             after_step(b);
             b->tracers_dirty = false;
         }
+        BK(cudaEventRecord(st1, b->stream), "tuning event");
         BK(cudaStreamSynchronize(b->stream), "synchronize");
         drain(b);
         if ((e = check_errors(b))) return e;
         out = 0.0;
+        if (!strcmp(name, "step")) {
+            float ms = 0.f;
+            BK(cudaEventElapsedTime(&ms, st0, st1), "tuning event");
+            out = ms / k;
+            return PI_OK;
+        }
         const std::string names = std::string("|") + name + "|";
         for (size_t q = 0; q < b->prof_names.size(); ++q)
             if (names.find("|" + b->prof_names[q] + "|") != std::string::npos) out += b->prof_ms[q] / k;
@@ -1800,6 +1861,21 @@ pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t k, char* report, siz
     }
     t.lz_fused = best_lz;
     t.fused = (fused_ms < two) ? 1 : (fused_ms < 1e300 ? 0 : fused0);
+    // with the x-y/z kernels: k32_xy beside the particle kernels or after them (whole step timed)
+    if (!t.fused) {
+        double best_ms = 1e300;
+        int best = t.concurrent;
+        for (int v : {0, 1}) {
+            t.concurrent = v;
+            double ms = 0.0;
+            if ((e0 = kernel_ms("step", ms))) { b->profiling = was; return e0; }
+            if (ms > 0.0 && ms < best_ms) { best_ms = ms; best = v; }
+        }
+        t.concurrent = best;
+        char line[160];
+        snprintf(line, sizeof line, "x-y kernel beside the particle kernels = %d (%.4f ms per step)\n", best, best_ms);
+        rep += line;
+    }
     {
         char line[200];
         snprintf(line, sizeof line, "tracer path = %s (fused %.4f ms at %d levels per block, two-kernel %.4f ms)\n",
@@ -1808,6 +1884,8 @@ pi_status pi_batch_autotune(pi_batch* b, double dT, int32_t k, char* report, siz
     }
     b->profiling = was;
     b->prof_names.clear(); b->prof_count.clear(); b->prof_ms.clear();
+    b->event_pool.push_back(st0);
+    b->event_pool.push_back(st1);
     pi_status e = build_tables(b);
     if (e) return e;
     if (report && report_len) {

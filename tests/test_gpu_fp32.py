@@ -15,7 +15,7 @@ import pytest
 
 import oracle
 from PlanktonIndividuals import _abi, workloads as W
-from PlanktonIndividuals._native import CModel, CapacityError
+from PlanktonIndividuals._native import CModel, CapacityError, PIError
 from PlanktonIndividuals.batch import Member, PlanktonBatch
 from helpers import VelCache, compare_states, drive
 
@@ -437,3 +437,23 @@ def test_async_float32_setters_equal_sync_path(gpu_lib):
     assert gpu_lib.pi_synchronize(b.h) == 0
     assert compare_states(a, b, wl.nsp) == []
     assert [int(c) for c in counts[-wl.nsp:]] == [a.count_active(s) for s in range(wl.nsp)]
+
+
+def test_launch_options_change_no_result(gpu_lib):
+    """Every launch-shape option (register fits, blocks per SM, tile rows, z walk length, PAR warps,
+    the x-y kernel on a second graph branch beside the particle kernels) gives the same bits."""
+    wls = _uneven_members()
+    runs = []
+    for opts in ({}, {"xy_beside_particles": 1, "move_fit": 3, "physiology_fit": 2, "xy_rows": 8,
+                      "z_levels": 16, "par_warps": 4, "move_blocks_per_sm": 0, "physiology_blocks_per_sm": 2}):
+        batch = PlanktonBatch(_members(wls), nspecies=2)
+        for k, v in opts.items():
+            batch.set_option(k, v)
+        for m, wl in enumerate(wls):
+            batch.set_state(m, wl.individuals, wl.tracers)
+        _drive_batch(batch, wls, 15, [VelCache(wl) for wl in wls])
+        runs.append(batch)
+    for m, wl in enumerate(wls):
+        assert compare_states(runs[0].member(m), runs[1].member(m), wl.nsp) == [], f"member {m}"
+    with pytest.raises(PIError):
+        runs[0].set_option("xy_rows", 5)
