@@ -111,7 +111,7 @@ def fp32_vs_fp64(lib, wl, steps, check_every=100):
         inds = {f"sp{s}": individual_errors(m64.get_individuals(s), b.get_individuals(0, s)) for s in range(wl.nsp)}
         return {"steps": steps, "counts_equal_at_every_check": all(h["fp64"] == h["fp32"] for h in hist),
                 "counts": hist, "tracer_mass_rel_err": rel, "max_tracer_mass_rel_err": max(rel.values()),
-                "individuals": inds, "budget_fp32": list(b.budget(0)),
+                "individuals": inds, "budget_fp32": b.budget(0),
                 "guard_band": dict(zip(("recomputed", "changed"), b.guard_stats()))}
     finally:
         b.close()
