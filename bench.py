@@ -199,6 +199,13 @@ def gpu_launches(prof, P, K, workload):
     return K * per_step + 5 * (-(-K // SORT_INTERVAL))
 
 
+# DRAM traffic per launch measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum, one pass,
+# --clock-control none) on config 2 (256x256x64, 2 x 2,097,152 individuals), per interior cell or per
+# active individual; a launch's traffic is this figure times its units
+MEASURED_TRAFFIC = {"k32_xy": ("cell", 113.0), "k32_ztail": ("cell", 214.4),
+                    "k32_move": ("active", 78.0), "k32_physiology": ("active", 123.8)}
+
+
 def profile_roofline(prof, members, nact, nslots):
     tot_ms = sum(v[1] for v in prof.values())
     order = sorted(prof, key=lambda k: -prof[k][1])
@@ -209,10 +216,17 @@ def profile_roofline(prof, members, nact, nslots):
         if byts:
             per_launch_ms = prof[dom][1] / prof[dom][0]
             ach = byts / (per_launch_ms / 1e3) / 1e9
+            traffic = None
+            if dom in MEASURED_TRAFFIC:
+                unit, per = MEASURED_TRAFFIC[dom]
+                V = sum(w.grid.Nx * w.grid.Ny * w.grid.Nz for w in members)
+                traffic = int(per * (V if unit == "cell" else nact))
             roof = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": hbm,
                     "peak_source": peak_kind, "unit": "GB/s", "frac": round(ach / hbm, 4),
-                    "traffic": None, "algorithmic_bytes_per_launch": int(byts),
-                    "avg_launch_ms": round(per_launch_ms, 4)}
+                    "traffic": traffic, "algorithmic_bytes_per_launch": int(byts),
+                    "avg_launch_ms": round(per_launch_ms, 4),
+                    "traffic_source": "ncu dram bytes per " + MEASURED_TRAFFIC[dom][0] + " on config 2, times this launch's units"
+                    if traffic else None}
             break
     return roof, tot_ms
 
