@@ -8,7 +8,7 @@
 //                        and newly freed slots marked in bitmaps over logical slots
 //   k32_par              calc_par! down each column
 //   k32_count_tiles      dividers and free slots of every tile of logical slots
-//   k32_scan_tiles       division and free-slot offsets of every tile (block scan per segment)
+//   scan(tile counts)    division and free-slot offsets of every tile
 //   k32_assign           k-th divider → k-th free slot per (member, species) segment
 //   k32_daughters        copy_daughter_individuals! + divide_to_half!
 //   k32_physiology       QuotaMode growth, consumption sums, decisions for the next step
@@ -16,12 +16,11 @@
 //                        boundary conditions: x, y and z sweeps of TMA-staged level tiles, sinking,
 //                        forcing, particle terms, apply_tendency! and the halo fill in one walk
 //                        down the levels
-//   (otherwise, and in the first step after a tracer upload:)
+//   (otherwise, and in the first step after a tracer upload, these three:)
 //   k32_xy               DST3FL x and y sweeps of every tracer on level tiles in shared memory
 //   k32_ztail            z sweep walking columns, then diffusion, sinking, forcing, BCs, particle
-//                        terms and apply_tendency!; with N >= H on every axis of every member it
-//                        also writes the halo images of the cells it finishes
-//   k32_halo<x,y,z>      fill_halo_tracer! in three passes (members with N < H on some axis)
+//                        terms and apply_tendency!
+//   k32_halo<x,y,z>      fill_halo_tracer!
 //   k32_end_step         vel₀ ← vel₁, iteration and t
 // Every sort_interval steps (and before the first step after an upload) the slots of every segment
 // are put back in cell order by a counting sort into the second buffer of the individual arrays
@@ -100,7 +99,7 @@ struct pi_batch {
     std::vector<FluxBC32> bch;
     std::string err;
     std::vector<void*> allocs;
-    long long Gtot = 0, Stot = 0, ncol = 0, maxG = 0, maxcol = 0;
+    long long Gtot = 0, Stot = 0, ncol = 0, maxG = 0, maxcol = 0, maxhalo = 0;
     bool halo_direct = true;        // every member has N >= H on every axis: one-pass halo fill
     int nlev = 0;
     // device
@@ -482,7 +481,6 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
     ta.T = b->T; ta.lm = b->lm; ta.dzF = b->dzF; ta.dzC = b->dzC; ta.rdzC = b->rdzC; ta.bgc = b->bgc;
     ta.bcs = b->bcs; ta.st = b->st; ta.F = b->F; ta.Gtot = G; ta.tr = tr; ta.tb = b->tb; ta.tr_next = trn;
     ta.acc = b->acc; ta.pop = b->pop; ta.dT = fdT; ta.err = b->errw;
-    ta.halo_in_walk = b->halo_direct ? 1 : 0;
     // k32_xy reads the tracers at the start of the step and this step's u and v only, so it can run
     // on a second branch beside the particle kernels; k32_ztail joins the two
     auto launch_xy = [&](cudaStream_t st) {
@@ -572,8 +570,12 @@ pi_status enqueue_step(pi_batch* b, double dT, int cur) {
         }
         }
     }
-    if (fused || b->halo_direct) {
-        // k32_tracer or k32_ztail wrote the halo cells with the interior
+    if (fused) {
+        // k32_tracer wrote the halo cells with the interior
+    } else if (b->halo_direct) { BScope sc(b, "k32_halo");
+      // about 16 blocks per SM over all members, enough for every member's halo cells
+      const unsigned gx = std::max(1u, std::min<unsigned>(nblk(b->maxhalo, 256), std::max(1, b->nsm * 16 / b->nm)));
+      k32_halo_direct<<<dim3(gx, b->nm), 256, 0, s>>>(b->md, G, trn, PI_NTRACERS, b->errw);
     } else { BScope sc(b, "k32_halo");
       k32_halo<0><<<std::min<unsigned>(nblk(b->nlines[0], 128), 148 * 8), 128, 0, s>>>(b->md, b->line_off[0], b->nm, G, trn, PI_NTRACERS, b->errw);
       k32_halo<1><<<std::min<unsigned>(nblk(b->nlines[1], 128), 148 * 8), 128, 0, s>>>(b->md, b->line_off[1], b->nm, G, trn, PI_NTRACERS, b->errw);
@@ -793,6 +795,7 @@ pi_status pi_batch_create(const pi_member* members, int32_t nmembers, int32_t ns
         lev += g.Gz;
         b->maxG = std::max(b->maxG, g.G);
         if (g.Nx < g.Hx || g.Ny < g.Hy || g.Nz < g.Hz) b->halo_direct = false;
+        b->maxhalo = std::max(b->maxhalo, g.G - (long long)g.Nx * g.Ny * g.Nz);
         b->maxcol = std::max(b->maxcol, (long long)g.Nx * g.Ny);
     }
     seg_tile0.push_back((int)tiles.size());

@@ -1164,7 +1164,6 @@ struct TrArgs {
     const int* pop;
     float dT;
     const uint32_t* err;
-    int halo_in_walk;           // k32_ztail also writes the halo images of the cells it finishes
 };
 
 // x and y sweeps of all 14 tracers on one level of a tile of 28 columns × TY rows. Warp w holds
@@ -1366,20 +1365,6 @@ __device__ __forceinline__ unsigned long long lds_u64(unsigned a) {
     return v;
 }
 
-// The cells an interior cell a (1-based, along one axis of N >= H cells with H halo points) stands
-// for after the halo fill: itself (t = 0), then its periodic images in the halo, or the halo points
-// a Bounded edge cell is copied to.
-__device__ __forceinline__ int halo_count(int a, int N, int H, int topo) {
-    if (topo == PI_PERIODIC) return 1 + (a - H <= H ? 1 : 0) + (a - H > N - H ? 1 : 0);
-    return 1 + (a == H + 1 ? H : 0) + (a == N + H ? H : 0);
-}
-__device__ __forceinline__ int halo_image(int a, int N, int H, int topo, int t) {
-    if (t == 0) return a;
-    if (topo == PI_PERIODIC) return (t == 1 && a - H <= H) ? a + N : a - N;
-    if (a == H + 1 && t <= H) return t;
-    return N + H + t - (a == H + 1 ? H : 0);
-}
-
 #define ZS 4                              // levels of a z walk ring (power of two)
 // One warp's ring: own tracer c, tracer_temp t two levels below, the other tracers the forcing
 // reads and the particle sum of the cell. A nutrient warp uses x[0] and acc; an iron warp reads
@@ -1551,22 +1536,7 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& md, con
             const long long vv = (long long)lds_u64(ra + 2u * so);   // zero where the cell holds no individual
             if (vv) { acc[q] = 0ull; plk = (float)((double)vv * L.fxv); }
         }
-        const float nv = tendency(cc, Gc, plk);
-        out[q] = nv;
-        if (a.halo_in_walk) {
-            // fill_halo_tracer! for an edge cell: its periodic images or Bounded copies
-            const int nix = halo_count(i, Nx, Hx, md.tx), njy = halo_count(j, md.Ny, md.Hy, md.ty);
-            const int nkz = halo_count(k, md.Nz, Hz, PI_BOUNDED);
-            if (nix * njy * nkz > 1) {
-#pragma unroll 1
-                for (int c3 = 0; c3 < nkz; ++c3)
-                    for (int b3 = 0; b3 < njy; ++b3)
-                        for (int a3 = 0; a3 < nix; ++a3)
-                            if (a3 | b3 | c3)
-                                out[gid3(md, halo_image(i, Nx, Hx, md.tx, a3), halo_image(j, md.Ny, md.Hy, md.ty, b3),
-                                         halo_image(k, md.Nz, Hz, PI_BOUNDED, c3))] = nv;
-            }
-        }
+        out[q] = tendency(cc, Gc, plk);
     }
     cpa_wait<0>();
 }
@@ -1683,6 +1653,48 @@ __global__ void k32_halo(const MemberDev* __restrict__ md, const long long* __re
     }
 }
 
+// fill_halo_tracer! in one pass when every axis of every member has N >= H: each halo cell then takes
+// the value of the interior cell reached by applying the rule of each axis (periodic: ±N; Bounded:
+// the nearest interior cell), which is what the three sequential passes above produce. Grid:
+// (x blocks, members); every thread walks halo cells of its member, all fields.
+__device__ __forceinline__ int halo_src(int a, int N, int H, int topo) {
+    if (a > H && a <= N + H) return a;
+    if (topo == PI_PERIODIC) return a <= H ? a + N : a - N;
+    return a <= H ? H + 1 : N + H;
+}
+// halo cells of a member: the 2Hz halo levels, then the 2Hy halo rows of the interior levels,
+// then the 2Hx halo columns of the interior rows
+__global__ void k32_halo_direct(const MemberDev* __restrict__ md, long long Gtot, float* __restrict__ f,
+                                int nfields, const uint32_t* err) {
+    if (err && stopped(err)) return;
+    const MemberDev& m = md[blockIdx.y];
+    const int Gx = m.Gx, Gy = m.Gy, Nx = m.Nx, Ny = m.Ny, Nz = m.Nz, Hx = m.Hx, Hy = m.Hy, Hz = m.Hz;
+    const int tx = m.tx, ty = m.ty;
+    const int nz = 2 * Hz * Gx * Gy, ny = 2 * Nz * Hy * Gx, n = nz + ny + 2 * Nz * Ny * Hx;   // below 2^31
+    float* __restrict__ c = f + m.cell_off;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        int i, j, k;
+        if (t < nz) {
+            const int kk = t / (Gx * Gy), r = t - kk * (Gx * Gy);
+            k = kk < Hz ? kk + 1 : Nz + kk + 1;
+            j = r / Gx + 1; i = r - (j - 1) * Gx + 1;
+        } else if (t < nz + ny) {
+            const int u = t - nz, kk = u / (2 * Hy * Gx), r = u - kk * (2 * Hy * Gx), jj = r / Gx;
+            k = Hz + 1 + kk;
+            j = jj < Hy ? jj + 1 : Ny + jj + 1;
+            i = r - jj * Gx + 1;
+        } else {
+            const int u = t - nz - ny, kk = u / (2 * Hx * Ny), r = u - kk * (2 * Hx * Ny), jj = r / (2 * Hx);
+            const int ii = r - jj * 2 * Hx;
+            k = Hz + 1 + kk; j = Hy + 1 + jj;
+            i = ii < Hx ? ii + 1 : Nx + ii + 1;
+        }
+        const int q = (i - 1) + Gx * ((j - 1) + Gy * (k - 1));
+        const int si = halo_src(i, Nx, Hx, tx), sj = halo_src(j, Ny, Hy, ty), sk = halo_src(k, Nz, Hz, PI_BOUNDED);
+        const int src = (si - 1) + Gx * ((sj - 1) + Gy * (sk - 1));
+        for (int n2 = 0; n2 < nfields; ++n2) c[n2 * Gtot + q] = c[n2 * Gtot + src];
+    }
+}
 
 // vel₀ .= vel₁ (time_step.jl:174-176), model.iteration += 1, model.t = iteration·ΔT. After a
 // capacity error nothing advances.

@@ -113,6 +113,19 @@ __global__ void k32_wait_selftest(unsigned long long limit_ns, int* gave_up, uns
     *gave_up = ok ? 0 : 1;
 }
 
+// The cells an interior cell a (1-based, along one axis of N >= H cells with H halo points) stands
+// for after the halo fill: itself (t = 0), then its periodic images in the halo, or the halo points
+// a Bounded edge cell is copied to.
+__device__ __forceinline__ int halo_count(int a, int N, int H, int topo) {
+    if (topo == PI_PERIODIC) return 1 + (a - H <= H ? 1 : 0) + (a - H > N - H ? 1 : 0);
+    return 1 + (a == H + 1 ? H : 0) + (a == N + H ? H : 0);
+}
+__device__ __forceinline__ int halo_image(int a, int N, int H, int topo, int t) {
+    if (t == 0) return a;
+    if (topo == PI_PERIODIC) return (t == 1 && a - H <= H) ? a + N : a - N;
+    if (a == H + 1 && t <= H) return t;
+    return N + H + t - (a == H + 1 ? H : 0);
+}
 
 struct TrkArgs {
     TrArgs a;
