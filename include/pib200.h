@@ -70,6 +70,10 @@ enum { PI_DIAG_PAR = 0, PI_DIAG_NUM, PI_DIAG_GRAZ, PI_DIAG_MORT, PI_DIAG_DVID,
        PI_DIAG_TRACER = 16, PI_DIAG_PROC = 32 };
 enum { PI_PROC_PS = 0, PI_PROC_BS, PI_PROC_VDOC, PI_PROC_VNH4, PI_PROC_VNO3, PI_PROC_VPO4, PI_PROC_resp,
        PI_PROC_exu, PI_PROC_Bm, PI_PROC_Cq, PI_PROC_Nq, PI_PROC_Pq, PI_PROC_Chl, PI_NPROC };
+/* The processes of a CarbonMode model (diags_spcs!, diagnostics_kernels.jl:16-17), the same
+ * PI_DIAG_PROC + q kinds and proc_mask bits. */
+enum { PI_CPROC_PS = 0, PI_CPROC_BS, PI_CPROC_RP, PI_CPROC_RS, PI_CPROC_TD, PI_CPROC_Bm, PI_CPROC_Bd,
+       PI_CPROC_Chl, PI_NCPROC };
 
 /* RectilinearGrid (src/Grids/rectilinear_grid.jl:1-25). Metrics are passed as the reference
  * stores them after construction (rectilinear_grid.jl:57-122), halos included. */
@@ -104,16 +108,28 @@ typedef struct {
     double mort_P, mort_reg, grazFracC, grazFracN, grazFracP, mortFracC, mortFracN, mortFracP;
 } pi_quota_params;
 
+/* CarbonMode phytoplankton parameters of one species, in the reference's param_names order
+ * (src/Individuals/Plankton/CarbonMode/plankton_generation.jl:13-15); thermal = 1 switches on
+ * thermal damage and repair, is_bact = 1 makes photosynthesis independent of light. */
+typedef struct {
+    double Nsuper, Cquota, mean, var, alpha, Phi, Topt, Tmax, Ea, PCmax, Chl2C, respir, f_T2B;
+    double grz_P, dvid_type, dvid_P, dvid_reg, dvid_reg2, mort_P, mort_reg, grazFracC, mortFracC;
+    double thermal, is_bact;
+} pi_carbon_params;
+
 /* The persistent per-individual state of one species (QuotaMode struct-of-arrays,
- * plankton_generation.jl:2-13). Every array is `capacity` long. graz/mort/dvid carry the 0/1
- * decisions drawn at the end of a step and applied at the start of the next. For
- * pi_set_individuals every member is required; for pi_get_individuals NULL members are skipped. */
+ * plankton_generation.jl:2-13; CarbonMode, CarbonMode/plankton_generation.jl:2-11, keeps Bd, the
+ * damaged biomass, and no Cq, Nq, Pq). Every array is `capacity` long. graz/mort/dvid carry the
+ * 0/1 decisions drawn at the end of a step and applied at the start of the next. For
+ * pi_set_individuals every member the mode uses is required (Bd: CarbonMode only; Cq, Nq, Pq:
+ * QuotaMode only); for pi_get_individuals NULL members are skipped. */
 typedef struct {
     double  *x, *y, *z;
     int64_t *xi, *yi, *zi;
     double  *Sz, *Bm, *Cq, *Nq, *Pq, *Chl, *gen, *age;
     uint8_t *ac;
     double  *graz, *mort, *dvid;
+    double  *Bd;
 } pi_individuals;
 
 typedef struct pi_model pi_model;
@@ -126,6 +142,14 @@ typedef struct pi_sim   pi_sim;
 pi_status pi_create(const pi_grid* grid, const pi_bgc_params* bgc,
                     const pi_quota_params* species, int32_t nspecies, int64_t capacity,
                     int32_t precision, uint64_t seed, pi_model** out);
+
+/* PlanktonModel(arch, grid; mode = CarbonMode(), ...): as pi_create with CarbonMode species
+ * (src/Individuals/Plankton/CarbonMode/). Built in the FP64 form (precision PI_FP64; PI_FP32 is
+ * refused with PI_ERR_ARG). The other calls work as for a QuotaMode model; pi_get_budget reports
+ * the individuals' carbon as ΣBm and no individual N or P. */
+pi_status pi_create_carbon(const pi_grid* grid, const pi_bgc_params* bgc,
+                           const pi_carbon_params* species, int32_t nspecies, int64_t capacity,
+                           int32_t precision, uint64_t seed, pi_model** out);
 
 /* Releases every device allocation of the handle. */
 pi_status pi_destroy(pi_model* m);

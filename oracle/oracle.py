@@ -56,8 +56,8 @@ FIELDS = {"par": 0, "Chl": 1, "pop": 2, "u1": 31, "v1": 32, "w1": 33, "u0": 34, 
 class OracleModel(CModel):
     """Same methods as the product's native model, backed by the CPU oracle."""
 
-    def __init__(self, grid, bgc_params, phyt_params, nsp, capacity, seed):
-        super().__init__(load(), "orc_", grid, bgc_params, phyt_params, nsp, capacity, seed)
+    def __init__(self, grid, bgc_params, phyt_params, nsp, capacity, seed, mode="quota"):
+        super().__init__(load(), "orc_", grid, bgc_params, phyt_params, nsp, capacity, seed, mode=mode)
 
     def get_field(self, name_or_idx):
         which = FIELDS.get(name_or_idx, name_or_idx)
@@ -78,7 +78,7 @@ class OracleModel(CModel):
 
 
 def from_workload(wl):
-    m = OracleModel(wl.grid, wl.bgc, wl.phyt, wl.nsp, wl.capacity, wl.seed)
+    m = OracleModel(wl.grid, wl.bgc, wl.phyt, wl.nsp, wl.capacity, wl.seed, mode=getattr(wl, "mode", "quota"))
     m.set_state(wl.individuals, wl.tracers)
     return m
 

@@ -52,6 +52,8 @@ const double F_1em1  = (double)1.0e-1f;    /* 1.0f-1   */
 const double F_2em3  = (double)2.0e-3f;    /* 2.0f-3   */
 const double F_1em3  = (double)1.0e-3f;    /* 1.0f-3   */
 const double F_1em5  = (double)1.0e-5f;    /* 1.0f-5   */
+const double F_1em6  = (double)1.0e-6f;    /* 1.0f-6   */
+const double F_0p99  = (double)0.99f;      /* 0.99f0   */
 const double F_THMAX = (double)1.0e20f;    /* θmax = 1.0f20, DST3FL.jl:2 */
 const double F_1em20 = (double)1.0e-20f;   /* 1.0f-20  */
 
@@ -86,6 +88,11 @@ struct Species {
     /* diagnostics (diags.phytos[sp]): defaults and the optional QuotaMode processes */
     dvec d_num, d_graz, d_mort, d_dvid;
     std::vector<dvec> d_proc;            /* PI_NPROC fields when enabled */
+    /* CarbonMode species (CarbonMode/plankton_generation.jl:2-11): damaged biomass and the rates
+     * of repair, respiration and thermal damage (PS and BS are shared with QuotaMode) */
+    int carbon = 0;
+    pi_carbon_params cp{};
+    dvec Bd, RP, RS, TD;
 };
 
 struct FluxBC { int kind = PI_BC_NONE; dvec v; int64_t nt = 0; };
@@ -563,8 +570,28 @@ void diags_proc(orc_model* m, Species& s, dvec& d, const dvec* proc) {
     }
 }
 
+/* The capacity error of plankton_update! (plankton_update.jl:21): Julia prints the Float64 day
+ * with the shortest digits that round-trip. */
+std::string capacity_message(double t) {
+    char num[64];
+    double d = t / 86400.0;
+    for (int p = 1; p <= 17; ++p) { snprintf(num, sizeof num, "%.*g", p, d); if (strtod(num, nullptr) == d) break; }
+    std::string ns(num);
+    if (ns.find('e') != std::string::npos) {
+        std::string mant = ns.substr(0, ns.find('e')), ex = ns.substr(ns.find('e') + 1);
+        if (mant.find('.') == std::string::npos) mant += ".0";
+        ns = mant + "e" + std::to_string(atoi(ex.c_str()));
+    } else if (ns.find('.') == std::string::npos) {
+        ns += ".0";
+    }
+    return "number of individual exceeds the capacity at timestep " + ns + " days";
+}
+
+bool plankton_update_carbon(orc_model* m, Species& s, int spi, double dT, double t);
+
 /* plankton_update!, QuotaMode/plankton_update.jl:1-34 */
 bool plankton_update(orc_model* m, Species& s, int spi, double dT, double t) {
+    if (s.carbon) return plankton_update_carbon(m, s, spi, dT, t);
     const pi_quota_params& p = s.p;
     int64_t C = m->C;
     diags_proc(m, s, s.d_graz, &s.graz);
@@ -580,19 +607,7 @@ bool plankton_update(orc_model* m, Species& s, int spi, double dT, double t) {
         if (!s.ac[i]) free_slots.push_back(i + 1);                          /* 1-based */
     }
     if (dvidnum > (double)free_slots.size()) {
-        /* Julia prints the Float64 with the shortest digits that round-trip */
-        char num[64];
-        double d = t / 86400.0;
-        for (int p = 1; p <= 17; ++p) { snprintf(num, sizeof num, "%.*g", p, d); if (strtod(num, nullptr) == d) break; }
-        std::string ns(num);
-        if (ns.find('e') != std::string::npos) {
-            std::string mant = ns.substr(0, ns.find('e')), ex = ns.substr(ns.find('e') + 1);
-            if (mant.find('.') == std::string::npos) mant += ".0";
-            ns = mant + "e" + std::to_string(atoi(ex.c_str()));
-        } else if (ns.find('.') == std::string::npos) {
-            ns += ".0";
-        }
-        m->err = "number of individual exceeds the capacity at timestep " + ns + " days";
+        m->err = capacity_message(t);
         m->err_flags |= ERR_CAPACITY;
         return false;
     }
@@ -631,6 +646,162 @@ bool plankton_update(orc_model* m, Species& s, int spi, double dT, double t) {
         const dvec* procs[PI_NPROC] = { &s.PS, &s.BS, &s.VDOC, &s.VNH4, &s.VNO3, &s.VPO4, &s.resp, &s.exu,
                                         &s.Bm, &s.Cq, &s.Nq, &s.Pq, &s.Chl };
         for (int q = 0; q < PI_NPROC; ++q)
+            if (m->proc_mask & (1u << q)) diags_proc(m, s, s.d_proc[q], procs[q]);
+    }
+    diags_proc(m, s, s.d_num, nullptr);
+    return true;
+}
+
+/* ---------------------------------------------------------------------------------------- */
+/* CarbonMode physiology, src/Individuals/Plankton/CarbonMode/ (all files)                   */
+/* ---------------------------------------------------------------------------------------- */
+
+inline double c_tempFunc_PS(double T, const pi_carbon_params& p) {   /* CarbonMode/growth_kernels.jl:2-9 */
+    double x = T - p.Topt, xmax = p.Tmax - p.Topt;
+    double regT = shape_func_dec(x, xmax, F_1em1, 4);
+    double k = pi_exp(-p.Ea / (F_RGAS * (T + F_T0))) * regT;
+    k = jl_max(0.0, k);
+    double OGT_rate = pi_exp(-p.Ea / (F_RGAS * (p.Topt + F_T0)));
+    return jl_min(1.0, k / OGT_rate);
+}
+inline double c_tempFunc(double T, const pi_carbon_params& p) {      /* :12-17 */
+    double k = pi_exp(-p.Ea / (F_RGAS * (T + F_T0)));
+    k = jl_max(0.0, k);
+    double OGT_rate = pi_exp(-p.Ea / (F_RGAS * (p.Topt + F_T0)));
+    return jl_min(1.0, k / OGT_rate);
+}
+inline double c_gamma(double Bm, double Bd, const pi_carbon_params& p) {   /* gamma_alloc, :22-26 */
+    double g = jl_mulb(Bd / jl_max(F_1em30, Bm), jl_isless(0.0, Bd));
+    return jl_mulb(jl_min(1.0, g), p.thermal == 1.0);
+}
+
+/* plankton_growth!, CarbonMode/plankton_growth.jl:2-29, with the kernels of growth_kernels.jl */
+void plankton_growth_carbon(orc_model* m, Species& s, int spi, double dT, double t) {
+    const pi_carbon_params& p = s.cp;
+    int64_t C = m->C;
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < C; ++i) {
+        int ac = s.ac[i];
+        double par = m->tpar[i], T = m->tT[i], pop = m->tpop[i];
+        double Bm = s.Bm[i], Bd = s.Bd[i], Chl = s.Chl[i];
+        /* calc_PS! (calc_photosynthesis, :29-36) */
+        double aI = par * p.alpha * p.Phi;
+        double PCm = p.PCmax * (c_tempFunc(T, p) * p.thermal + c_tempFunc_PS(T, p) * (1.0 - p.thermal));
+        double light = 1.0 - pi_exp(-aI / jl_max(F_1em30, PCm) * Chl / jl_max(F_1em30, Bm));
+        double PS = PCm * jl_max(0.0, Bm - Bd) * (light * (1.0 - p.is_bact) + p.is_bact);
+        s.PS[i] = jl_mulb(PS, ac);
+        /* calc_BS!, calc_repair! (:55-64) */
+        s.BS[i] = s.PS[i] * (1.0 - c_gamma(Bm, Bd, p));
+        s.RP[i] = s.PS[i] * c_gamma(Bm, Bd, p);
+        /* calc_thermal_damage! (:69-75) */
+        double TD = jl_mulb(jl_mulb(jl_mulb((T - p.Topt) * p.f_T2B * (Bm - Bd), jl_isless(p.Topt, T)),
+                                    jl_isless(Bd, Bm)), p.thermal == 1.0);
+        s.TD[i] = jl_max(0.0, jl_min(TD, (Bm - Bd) / dT));
+        /* calc_respir! (:82-85) */
+        s.RS[i] = jl_mulb(p.respir * Bm * c_tempFunc(T, p), ac);
+        /* update_quotas! (:92-97) */
+        s.Bm[i] += (s.BS[i] - s.RS[i]) * dT;
+        s.Bd[i] += (s.TD[i] - s.RP[i]) * dT;
+        s.age[i] += jl_mulb(dT / 3600.0, ac);
+        /* update_cellsize! (:104-108) */
+        s.Sz[i] = s.Bm[i] / (p.Cquota * p.Nsuper);
+        s.Chl[i] = s.Bm[i] * p.Chl2C;
+        /* calc_graz_quadratic!, calc_dvid!, calc_thermal_mort! or calc_mort!
+         * (division_death_probability.jl:26-30, 49-52, 60-77) */
+        s.graz[i] = jl_mulb(pop * p.grz_P, ac);
+        double dv;
+        int ty = (int)p.dvid_type;
+        if (ty == 1) dv = p.dvid_P * shape_func_inc(s.Sz[i], p.dvid_reg, F_2em3, 2);
+        else if (ty == 2) dv = p.dvid_P * shape_func_inc(fmod(t, 86400.0) / 3600.0, p.dvid_reg, F_1em5, 4);
+        else dv = p.dvid_P * shape_func_inc(s.Sz[i], p.dvid_reg, F_1em3, 4)
+                  * shape_func_inc(fmod(t, 86400.0) / 3600.0, p.dvid_reg2, F_1em5, 4);
+        s.dvid[i] = jl_mulb(dv, ac);
+        if (p.thermal == 1.0)
+            s.mort[i] = jl_mulb(p.mort_P * shape_func_inc(s.Bd[i] / jl_max(F_1em30, s.Bm[i]), F_0p99, F_1em6, 4), ac);
+        else
+            s.mort[i] = jl_mulb(p.mort_P * shape_func_dec(s.Sz[i], p.mort_reg, F_1em5, 4), ac);
+    }
+    /* get_probability!, division_death_probability.jl:95-107 */
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < C; ++i) {
+        double r0, r1, r2;
+        pi_draw3(m->seed, (uint32_t)m->iteration, (uint32_t)spi, PI_DRAW_DECISION, (uint32_t)i, &r0, &r1, &r2);
+        m->rx[i] = r0; m->ry[i] = r1; m->rz[i] = r2;
+    }
+    for (int64_t i = 0; i < C; ++i) {
+        int ac = s.ac[i];
+        s.graz[i] = (double)(jl_isless(m->rx[i], s.graz[i] * dT) && ac);
+        s.mort[i] = (double)(jl_isless(m->ry[i], s.mort[i] * dT) && ac);
+        s.dvid[i] = (double)(jl_isless(m->rz[i], s.dvid[i] * dT) && ac);
+    }
+}
+
+/* calc_loss_kernel!, CarbonMode/consume_loss.jl:12-16, then inactivate! */
+void calc_loss_carbon(orc_model* m, Species& s, const dvec& loss, double fC) {
+    for (int64_t i = 0; i < m->C; ++i) {
+        size_t c = cell_of(m, s, i);
+        int ac = s.ac[i];
+        double Bm = s.Bm[i], l = loss[i];
+        m->plk[PI_DOC][c] += jl_mulb(Bm * fC, ac) * l;
+        m->plk[PI_POC][c] += jl_mulb(Bm * (1.0 - fC), ac) * l;
+    }
+    for (int64_t i = 0; i < m->C; ++i) s.ac[i] = (uint8_t)(s.ac[i] && jl_isless(loss[i], 1.0));
+}
+
+std::string capacity_message(double t);
+
+/* plankton_update!, CarbonMode/plankton_update.jl:1-32 */
+bool plankton_update_carbon(orc_model* m, Species& s, int spi, double dT, double t) {
+    const pi_carbon_params& p = s.cp;
+    int64_t C = m->C;
+    diags_proc(m, s, s.d_graz, &s.graz);
+    calc_loss_carbon(m, s, s.graz, p.grazFracC);                          /* grazing!   */
+    diags_proc(m, s, s.d_mort, &s.mort);
+    calc_loss_carbon(m, s, s.mort, p.mortFracC);                          /* mortality! */
+    for (int64_t i = 0; i < C; ++i) s.dvid[i] = jl_mulb(s.dvid[i], s.ac[i]);
+    diags_proc(m, s, s.d_dvid, &s.dvid);
+    double dvidnum = 0.0;
+    std::vector<int64_t> free_slots;
+    for (int64_t i = 0; i < C; ++i) {
+        dvidnum += s.dvid[i] * (double)s.ac[i];
+        if (!s.ac[i]) free_slots.push_back(i + 1);
+    }
+    if (dvidnum > (double)free_slots.size()) {
+        m->err = capacity_message(t);
+        m->err_flags |= ERR_CAPACITY;
+        return false;
+    }
+    /* divide!, CarbonMode/division_death.jl:62-69: copy_daughter_individuals! (:28-45) copies
+     * x, y, z, Sz, Bm, Chl, gen, ac and dvid (not Bd, not age); divide_to_half! (:49-57) halves
+     * Sz, Bm, Bd and Chl of every divider and daughter */
+    double acc = 0.0;
+    for (int64_t i = 0; i < C; ++i) { acc += s.dvid[i]; m->tidc[i] = acc; m->tidc_int[i] = (int64_t)acc; }
+    for (int64_t i = 0; i < C; ++i)
+        if (s.dvid[i] == 1.0) s.idx[i] = free_slots[(size_t)m->tidc_int[i] - 1];
+    for (int64_t i = 0; i < C; ++i)
+        if (s.dvid[i] == 1.0 && s.idx[i] != 0) {
+            int64_t d = s.idx[i] - 1;
+            s.x[d] = s.x[i]; s.y[d] = s.y[i]; s.z[d] = s.z[i];
+            s.Sz[d] = s.Sz[i]; s.Bm[d] = s.Bm[i]; s.Chl[d] = s.Chl[i]; s.gen[d] = s.gen[i];
+            s.ac[d] = s.ac[i]; s.dvid[d] = s.dvid[i];
+        }
+    for (int64_t i = 0; i < C; ++i) {
+        double f = (2.0 - s.dvid[i]) / 2.0;
+        s.Sz[i] *= f; s.Bm[i] *= f; s.Bd[i] *= f; s.Chl[i] *= f;
+        s.gen[i] += s.dvid[i];
+        s.age[i] *= (1.0 - s.dvid[i]);
+    }
+    for (int64_t i = 0; i < C; ++i) s.idx[i] = 0;
+    plankton_growth_carbon(m, s, spi, dT, t);
+    /* calc_consume_kernel!, CarbonMode/consume_loss.jl:2-5 */
+    for (int64_t i = 0; i < C; ++i) {
+        size_t c = cell_of(m, s, i);
+        m->plk[PI_DIC][c] += jl_mulb((s.RS[i] - s.PS[i]) * dT, s.ac[i]);
+    }
+    /* diags_spcs! (Diagnostics/diagnostics_kernels.jl:14-33), CarbonMode processes */
+    if (m->proc_mask) {
+        const dvec* procs[PI_NCPROC] = { &s.PS, &s.BS, &s.RP, &s.RS, &s.TD, &s.Bm, &s.Bd, &s.Chl };
+        for (int q = 0; q < PI_NCPROC; ++q)
             if (m->proc_mask & (1u << q)) diags_proc(m, s, s.d_proc[q], procs[q]);
     }
     diags_proc(m, s, s.d_num, nullptr);
@@ -955,6 +1126,33 @@ int orc_create(const pi_grid* grid, const pi_bgc_params* bgc, const pi_quota_par
     return PI_OK;
 }
 
+/* A CarbonMode model: the QuotaMode setup with the shared parameters filled in, then the species
+ * switched to CarbonMode (their Cq, Nq, Pq stay zero). */
+int orc_create_carbon(const pi_grid* grid, const pi_bgc_params* bgc, const pi_carbon_params* species,
+                      int32_t nspecies, int64_t capacity, uint64_t seed, orc_model** out) {
+    if (!species || nspecies < 1) { g_create_err = "orc_create_carbon: bad argument"; return PI_ERR_ARG; }
+    std::vector<pi_quota_params> q((size_t)nspecies);
+    for (int s = 0; s < nspecies; ++s) {
+        const pi_carbon_params& c = species[s];
+        pi_quota_params& p = q[s];
+        memset(&p, 0, sizeof p);
+        p.Nsuper = c.Nsuper; p.Cquota = c.Cquota; p.mean = c.mean; p.var = c.var; p.alpha = c.alpha;
+        p.Phi = c.Phi; p.Topt = c.Topt; p.Tmax = c.Tmax; p.Ea = c.Ea; p.PCmax = c.PCmax; p.respir = c.respir;
+        p.grz_P = c.grz_P; p.dvid_type = c.dvid_type; p.dvid_P = c.dvid_P; p.dvid_reg = c.dvid_reg;
+        p.dvid_reg2 = c.dvid_reg2; p.mort_P = c.mort_P; p.mort_reg = c.mort_reg;
+        p.grazFracC = c.grazFracC; p.mortFracC = c.mortFracC;
+    }
+    int st = orc_create(grid, bgc, q.data(), nspecies, capacity, seed, out);
+    if (st) return st;
+    for (int s = 0; s < nspecies; ++s) {
+        Species& S = (*out)->sp[s];
+        S.carbon = 1;
+        S.cp = species[s];
+        for (dvec* v : { &S.Bd, &S.RP, &S.RS, &S.TD }) v->assign((size_t)capacity, 0.0);
+    }
+    return PI_OK;
+}
+
 int orc_destroy(orc_model* m) { delete m; return PI_OK; }
 
 int orc_set_individuals(orc_model* m, int32_t sp, const pi_individuals* in) {
@@ -964,10 +1162,16 @@ int orc_set_individuals(orc_model* m, int32_t sp, const pi_individuals* in) {
     auto cp = [&](dvec& d, const double* s) { d.assign(s, s + C); };
     cp(S.x, in->x); cp(S.y, in->y); cp(S.z, in->z);
     S.xi.assign(in->xi, in->xi + C); S.yi.assign(in->yi, in->yi + C); S.zi.assign(in->zi, in->zi + C);
-    cp(S.Sz, in->Sz); cp(S.Bm, in->Bm); cp(S.Cq, in->Cq); cp(S.Nq, in->Nq); cp(S.Pq, in->Pq);
+    cp(S.Sz, in->Sz); cp(S.Bm, in->Bm);
+    for (auto pr : { std::make_pair(&S.Cq, in->Cq), std::make_pair(&S.Nq, in->Nq), std::make_pair(&S.Pq, in->Pq) }) {
+        if (pr.second) cp(*pr.first, pr.second);
+        else if (S.carbon) pr.first->assign(C, 0.0);
+        else return PI_ERR_ARG;
+    }
     cp(S.Chl, in->Chl); cp(S.gen, in->gen); cp(S.age, in->age);
     S.ac.assign(in->ac, in->ac + C);
     cp(S.graz, in->graz); cp(S.mort, in->mort); cp(S.dvid, in->dvid);
+    if (S.carbon) { if (in->Bd) cp(S.Bd, in->Bd); else S.Bd.assign(C, 0.0); }
     return PI_OK;
 }
 
@@ -982,6 +1186,7 @@ int orc_get_individuals(orc_model* m, int32_t sp, pi_individuals* out) {
     cp(out->Chl, S.Chl); cp(out->gen, S.gen); cp(out->age, S.age);
     if (out->ac) std::copy(S.ac.begin(), S.ac.end(), out->ac);
     cp(out->graz, S.graz); cp(out->mort, S.mort); cp(out->dvid, S.dvid);
+    if (S.carbon) cp(out->Bd, S.Bd);
     return PI_OK;
 }
 

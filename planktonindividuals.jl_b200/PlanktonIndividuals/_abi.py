@@ -65,6 +65,24 @@ class pi_quota_params(ct.Structure):
     _fields_ = [(c, ct.c_double) for c, _ in QUOTA_FIELDS]
 
 
+# CarbonMode param_names (src/Individuals/Plankton/CarbonMode/plankton_generation.jl:13-15)
+CARBON_FIELDS = [("Nsuper", "Nsuper"), ("Cquota", "Cquota"), ("mean", "mean"), ("var", "var"),
+                 ("alpha", "α"), ("Phi", "Φ"), ("Topt", "Topt"), ("Tmax", "Tmax"), ("Ea", "Ea"),
+                 ("PCmax", "PCmax"), ("Chl2C", "Chl2C"), ("respir", "respir"), ("f_T2B", "f_T2B"),
+                 ("grz_P", "grz_P"), ("dvid_type", "dvid_type"), ("dvid_P", "dvid_P"),
+                 ("dvid_reg", "dvid_reg"), ("dvid_reg2", "dvid_reg2"), ("mort_P", "mort_P"),
+                 ("mort_reg", "mort_reg"), ("grazFracC", "grazFracC"), ("mortFracC", "mortFracC"),
+                 ("thermal", "thermal"), ("is_bact", "is_bact")]
+
+
+class pi_carbon_params(ct.Structure):
+    _fields_ = [(c, ct.c_double) for c, _ in CARBON_FIELDS]
+
+
+# CarbonMode processes of diags_spcs! (diagnostics_kernels.jl:16-17), in PI_CPROC_* order
+CARBON_PROC_NAMES = ("PS", "BS", "RP", "RS", "TD", "Bm", "Bd", "Chl")
+
+
 IND_DOUBLE = ("x", "y", "z", "Sz", "Bm", "Cq", "Nq", "Pq", "Chl", "gen", "age", "graz", "mort", "dvid")
 IND_INT = ("xi", "yi", "zi")
 
@@ -75,7 +93,8 @@ class pi_individuals(ct.Structure):
                 ("Sz", _dp), ("Bm", _dp), ("Cq", _dp), ("Nq", _dp), ("Pq", _dp),
                 ("Chl", _dp), ("gen", _dp), ("age", _dp),
                 ("ac", _u8p),
-                ("graz", _dp), ("mort", _dp), ("dvid", _dp)]
+                ("graz", _dp), ("mort", _dp), ("dvid", _dp),
+                ("Bd", _dp)]
 
 
 class pi_member(ct.Structure):
@@ -105,13 +124,15 @@ def declare(lib, prefix):
         "count_active": (ct.c_int32, [P, ct.c_int32, _i64p]),
         "get_diag": (ct.c_int32, [P, ct.c_int32, ct.c_int32, _dp]),
         "get_budget": (ct.c_int32, [P, _dp]),
+        "create_carbon": (ct.c_int32, [ct.POINTER(pi_grid), ct.POINTER(pi_bgc_params),
+                                       ct.POINTER(pi_carbon_params), ct.c_int32, ct.c_int64]),
         "last_error": (ct.c_int32, [P, ct.c_char_p, ct.c_size_t]),
     }
     for name, (res, args) in protos.items():
         fn = getattr(lib, prefix + name, None)
         if fn is None:
             continue
-        if name == "create":
+        if name in ("create", "create_carbon"):
             if prefix == "pi_":
                 args = args + [ct.c_int32, ct.c_uint64, ct.POINTER(P)]
             else:

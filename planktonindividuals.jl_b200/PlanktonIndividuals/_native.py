@@ -58,10 +58,11 @@ def make_bgc_struct(params):
     return b
 
 
-def make_species_structs(phyt_params, nsp):
-    arr = (pi_quota_params * nsp)()
+def make_species_structs(phyt_params, nsp, mode="quota"):
+    carbon = mode == "carbon"
+    arr = ((_abi.pi_carbon_params if carbon else pi_quota_params) * nsp)()
     for s in range(nsp):
-        for cname, key in QUOTA_FIELDS:
+        for cname, key in (_abi.CARBON_FIELDS if carbon else QUOTA_FIELDS):
             v = phyt_params[key]
             v = v[s] if hasattr(v, "__len__") else v
             setattr(arr[s], cname, float(v))
@@ -72,17 +73,21 @@ class CModel:
     """One model handle of a library exporting `<prefix>create` ... `<prefix>last_error`."""
 
     def __init__(self, lib, prefix, grid, bgc_params, phyt_params, nsp, capacity, seed,
-                 precision=None):
+                 precision=None, mode="quota"):
+        """mode: "quota" (QuotaMode) or "carbon" (CarbonMode, `<prefix>create_carbon`)."""
+        if mode not in ("quota", "carbon"):
+            raise ValueError(f"mode must be 'quota' or 'carbon', not {mode!r}")
         self.lib = _abi.declare(lib, prefix)
         self.prefix = prefix
+        self.mode = mode
         self.grid = grid
         self.nsp = int(nsp)
         self.capacity = int(capacity)
         g, self._keep = make_grid_struct(grid)
         b = make_bgc_struct(bgc_params)
-        sp = make_species_structs(phyt_params, self.nsp)
+        sp = make_species_structs(phyt_params, self.nsp, mode)
         h = ct.c_void_p()
-        fn = self._fn("create")
+        fn = self._fn("create_carbon" if mode == "carbon" else "create")
         if precision is None:
             rc = fn(ct.byref(g), ct.byref(b), sp, self.nsp, self.capacity, ct.c_uint64(seed), ct.byref(h))
         else:
@@ -132,7 +137,10 @@ class CModel:
         C = self.capacity
         keep = {}
         st = pi_individuals()
-        for k in IND_DOUBLE:
+        carbon = self.mode == "carbon"
+        for k in IND_DOUBLE + (("Bd",) if carbon else ()):
+            if carbon and k in ("Cq", "Nq", "Pq", "Bd") and k not in data:
+                continue                      # CarbonMode keeps no quotas; Bd defaults to zero
             a = np.ascontiguousarray(data[k], dtype=np.float64)
             if a.shape != (C,):
                 raise ValueError(f"individual attribute {k} must have length {C}")
@@ -151,11 +159,13 @@ class CModel:
 
     def get_individuals(self, sp):
         C = self.capacity
-        out = {k: np.empty(C, dtype=np.float64) for k in IND_DOUBLE}
+        carbon = self.mode == "carbon"
+        names = tuple(k for k in IND_DOUBLE if not (carbon and k in ("Cq", "Nq", "Pq"))) + (("Bd",) if carbon else ())
+        out = {k: np.empty(C, dtype=np.float64) for k in names}
         out.update({k: np.empty(C, dtype=np.int64) for k in IND_INT})
         out["ac"] = np.empty(C, dtype=np.uint8)
         st = pi_individuals()
-        for k in IND_DOUBLE:
+        for k in names:
             setattr(st, k, _dptr(out[k]))
         for k in IND_INT:
             setattr(st, k, out[k].ctypes.data_as(ct.POINTER(ct.c_int64)))

@@ -1,6 +1,6 @@
 """Architectures and physiology modes (src/Architectures.jl, src/PlanktonIndividuals.jl:59-83).
-Only GPU() and QuotaMode() are implemented; the others exist so that code naming them fails
-with a clear message."""
+GPU() with QuotaMode() (both precisions) and CarbonMode() (Float64) are implemented; the other
+modes exist so that code naming them fails with a clear message."""
 
 
 class Architecture:
@@ -33,7 +33,10 @@ class QuotaMode(AbstractMode):
 
 
 class CarbonMode(AbstractMode):
-    pass
+    """Carbon only: biomass, damaged biomass and Chl (src/Individuals/Plankton/CarbonMode/)."""
+
+    def __repr__(self):
+        return "CarbonMode()"
 
 
 class MacroMolecularMode(AbstractMode):

@@ -52,6 +52,33 @@ def initialize_plankton(grid, p, s, N, C, rng):
     return d
 
 
+def initialize_plankton_carbon(grid, p, s, N, C, rng):
+    """initialize_plankton! of CarbonMode (CarbonMode/plankton_generation.jl:33-56) for species s:
+    Sz = max(1, N(mean, var)), Bm = Cquota·Sz·Nsuper, Chl = Bm·Chl2C, Bd = 0."""
+    if N > C:
+        raise ValueError("PlanktonModel: number of individuals exceeds max_individuals")
+    d = empty_individuals(C)
+    for k in ("Cq", "Nq", "Pq"):
+        del d[k]
+    ac = np.zeros(C, dtype=bool)
+    ac[:N] = True
+    mean, var = species_param(p, "mean", s), species_param(p, "var", s)
+    Cquota, Nsuper, Chl2C = (species_param(p, k, s) for k in ("Cquota", "Nsuper", "Chl2C"))
+    Sz = rng.standard_normal(C)
+    x, y, z = rng.random(C), rng.random(C), rng.random(C)
+    d["ac"] = ac
+    d["gen"][:N] = 1.0
+    d["x"] = (x * grid.Nx) * ac
+    d["y"] = (y * grid.Ny) * ac
+    d["z"] = (z * grid.Nz) * ac
+    d["Sz"] = np.maximum(1.0, Sz * var + mean) * ac
+    d["Bm"] = Cquota * d["Sz"] * Nsuper
+    d["Chl"] = d["Bm"] * Chl2C
+    d["Bd"] = np.zeros(C, dtype=np.float64)
+    mask_individuals(d, grid, N)
+    return d
+
+
 def mask_individuals(d, grid, N):
     """mask_individuals! (Individuals/utils.jl:89-100)."""
     ac = d["ac"][:N]

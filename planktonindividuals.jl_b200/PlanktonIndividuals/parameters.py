@@ -54,7 +54,19 @@ def bgc_params_default(FT=np.float32):
 
 
 def phyt_params_default(N=1, mode=None):
-    """phyt_params_default(N, QuotaMode()) (param_default.jl:235-284); one list entry per species."""
+    """phyt_params_default(N, QuotaMode()) (param_default.jl:235-284) or, for CarbonMode(),
+    param_default.jl:290-320; one list entry per species."""
+    from .architectures import CarbonMode
+    if isinstance(mode, CarbonMode) or mode is CarbonMode:
+        params = {
+            "Nsuper": [1], "Cquota": [1.8e-11], "mean": [1.2], "var": [0.3], "Chl2C": [0.10],
+            "α": [2.0e-2], "Φ": [4.0e-5], "Topt": [27.0], "Tmax": [30.0], "Ea": [5.3e4],
+            "PCmax": [4.2e-5], "respir": [1.2e-6], "f_T2B": [2.7e-6], "grz_P": [0.0],
+            "dvid_P": [5e-5], "dvid_type": [1], "dvid_reg": [1.9], "dvid_reg2": [12.0],
+            "mort_P": [5e-5], "mort_reg": [0.5], "grazFracC": [0.7], "mortFracC": [0.5],
+            "thermal": [1.0], "is_bact": [0.0],
+        }
+        return params if N == 1 else {k: [v[0]] * N for k, v in params.items()}
     params = {
         "Nsuper": [1], "Cquota": [1.8e-11], "mean": [1.2], "var": [0.3], "Chl2Cint": [0.10],
         "α": [2.0e-2], "Φ": [4.0e-5], "Topt": [27.0], "Tmax": [30.0], "Ea": [5.3e4],

@@ -49,6 +49,7 @@ class Workload:
     dT_temp: float
     seed: int
     meta: dict = field(default_factory=dict)
+    mode: str = "quota"           # physiology: "quota" (QuotaMode) or "carbon" (CarbonMode)
 
     def velocity(self, t):
         return self.vel_fn(t)
@@ -234,6 +235,39 @@ def config2(nx=256, nz=64, N_per_species=2_097_152, nsp=2, steps=1000, dT=30.0, 
     n_vel = int(np.ceil(steps / 60)) + 1
     return _finish("config2", grid, nsp, [N_per_species] * nsp, C, phyt_over, None, dT, steps, rng,
                    vel, n_vel, 60 * dT, zmax, [0.0] * nsp, 0.2, seed, no3_grad=2.0 * nz)
+
+
+def carbon(nx=16, nz=8, N_per_species=2000, nsp=2, steps=30, dT=60.0, seed=11, nmodes=16,
+           capacity=None, phyt_over=None, temp=None, bd_frac=0.0):
+    """CarbonMode workload on a config-2-like 3D grid (nx×nx×nz, 50 m × 50 m × 2 m): individuals
+    from CarbonMode's initialize_plankton! rule, optionally with damaged biomass Bd = Bm·U(0,
+    bd_frac); `temp` (°C, scalar or interior array) replaces the default temperature so that the
+    thermal damage and repair terms (T > Topt) can be exercised."""
+    from .architectures import CarbonMode
+    from .init import initialize_plankton_carbon
+    rng = np.random.default_rng(seed)
+    grid = RectilinearGrid(size=(nx, nx, nz), x=(0.0, nx * 50.0), y=(0.0, nx * 50.0),
+                           z=(0.0, -2.0 * nz), FT=np.float64, topology=(Periodic, Periodic, Bounded))
+    vel = FourierVelocity(grid, nmodes=nmodes, rms=0.05, seed=seed)
+    C = capacity or 2 * N_per_species
+    bgc = update_bgc_params({}, np.float64)
+    phyt = update_phyt_params(phyt_over or {}, np.float64, N=nsp, mode=CarbonMode())
+    inds = []
+    for s in range(nsp):
+        d = initialize_plankton_carbon(grid, phyt, s, N_per_species, C, rng)
+        if bd_frac:
+            d["Bd"] = d["Bm"] * rng.uniform(0.0, bd_frac, C) * d["ac"]
+        inds.append(d)
+    trs = make_tracers(grid, rng, no3_gradient_depth=2.0 * nz)
+    hours = int(np.ceil(steps * dT / 3600.0)) + 1
+    parf = diel_parf(grid.Nx, grid.Ny, hours)
+    tmp = default_temperature(grid, dT, steps)
+    if temp is not None:
+        tmp = np.asfortranarray(np.broadcast_to(np.asarray(temp, dtype=np.float64)[..., None] if np.ndim(temp) == 3
+                                                else np.float64(temp), tmp.shape).copy())
+    n_vel = int(np.ceil(steps / 60)) + 1
+    return Workload("carbon", grid, bgc, phyt, nsp, C, [N_per_species] * nsp, inds, trs, dT, steps,
+                    60 * dT, n_vel, vel, parf, 3600.0, tmp, 3600.0, seed, mode="carbon")
 
 
 def config3(nx=512, nz=128, N_per_species=16_777_216, nsp=4, steps=1000, dT=20.0, seed=3,
