@@ -268,11 +268,12 @@ __global__ void k_par(DGrid g, const SpcDev* __restrict__ spc, long long C,
 
 // Applies last step's grazing/mortality decisions, writes the loss contributions of the
 // individuals lost, the division/free flags for the slot scan and the graz/mort/dvid diags.
+// carbon: CarbonMode losses (CarbonMode/consume_loss.jl:12-16): DOC and POC from Bm only.
 __global__ void k_decide(DGrid g, SpcDev P, pi_quota_params p, long long C, int s,
                          const int32_t* __restrict__ pos, double* __restrict__ loss,
                          uint8_t* __restrict__ evk, unsigned long long* __restrict__ flag64,
                          double* __restrict__ d_graz, double* __restrict__ d_mort,
-                         double* __restrict__ d_dvid, uint32_t* err) {
+                         double* __restrict__ d_dvid, uint32_t* err, int carbon) {
     long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= C) return;
     if (*err & PI_DEVERR_CAPACITY) return;
@@ -296,14 +297,21 @@ __global__ void k_decide(DGrid g, SpcDev P, pi_quota_params p, long long C, int 
             double fC = kind == 1 ? p.grazFracC : p.mortFracC;
             double fN = kind == 1 ? p.grazFracN : p.mortFracN;
             double fP = kind == 1 ? p.grazFracP : p.mortFracP;
-            double Bm = P.Bm[slot], Cq = P.Cq[slot], Nq = P.Nq[slot], Pq = P.Pq[slot];
             double* L = loss + e * 6;
+            if (carbon) {
+                const double Bm = P.Bm[slot];
+                L[0] = jl_mulb(Bm * fC, 1) * 1.0;                     // DOC
+                L[3] = jl_mulb(Bm * (1.0 - fC), 1) * 1.0;             // POC
+                L[1] = 0.0; L[2] = 0.0; L[4] = 0.0; L[5] = 0.0;
+            } else {
+            double Bm = P.Bm[slot], Cq = P.Cq[slot], Nq = P.Nq[slot], Pq = P.Pq[slot];
             L[0] = jl_mulb((Bm + Cq) * fC, 1) * 1.0;                  // DOC
             L[1] = jl_mulb((Bm * p.R_NC + Nq) * fN, 1) * 1.0;         // DON
             L[2] = jl_mulb((Bm * p.R_PC + Pq) * fP, 1) * 1.0;         // DOP
             L[3] = jl_mulb((Bm + Cq) * (1.0 - fC), 1) * 1.0;          // POC
             L[4] = jl_mulb((Bm * p.R_NC + Nq) * (1.0 - fN), 1) * 1.0; // PON
             L[5] = jl_mulb((Bm * p.R_PC + Pq) * (1.0 - fP), 1) * 1.0; // POP
+            }
         }
     }
     P.flags[slot] = (uint8_t)((ac2 ? FL_AC : 0) | (dv2 ? FL_DVID : 0));
@@ -340,14 +348,26 @@ __global__ void k_lists(const unsigned long long* __restrict__ flag64,
 
 // copy_daughter_individuals! then divide_to_half! for the dividers and their daughters
 // (division_death.jl:28-63). Other slots are unchanged by divide_to_half (factor 1, +0, ×1).
+// CarbonMode (CarbonMode/division_death.jl:28-57): x, y, z, Sz, Bm, Chl and gen are copied, Bd is
+// not — the daughter halves the damaged biomass its slot held before.
 __global__ void k_daughters(SpcDev P, const int32_t* __restrict__ divlist,
                             const int32_t* __restrict__ freelist, const uint32_t* ndiv,
-                            const uint32_t* err) {
+                            const uint32_t* err, int carbon) {
     if (*err & PI_DEVERR_CAPACITY) return;
     uint32_t n = *ndiv;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         long long p = divlist[k], d = freelist[k];
         const double h = (2.0 - 1.0) / 2.0;
+        if (carbon) {
+            double Sz = P.Sz[p], Bm = P.Bm[p], Chl = P.Chl[p], gen = P.gen[p];
+            P.x[d] = P.x[p]; P.y[d] = P.y[p]; P.z[d] = P.z[p];
+            P.Sz[d] = Sz * h; P.Bm[d] = Bm * h; P.Bd[d] = P.Bd[d] * h; P.Chl[d] = Chl * h;
+            P.gen[d] = gen + 1.0; P.age[d] = P.age[d] * (1.0 - 1.0);
+            P.flags[d] = FL_AC | FL_DVID;
+            P.Sz[p] = Sz * h; P.Bm[p] = Bm * h; P.Bd[p] = P.Bd[p] * h; P.Chl[p] = Chl * h;
+            P.gen[p] = gen + 1.0; P.age[p] = P.age[p] * (1.0 - 1.0);
+            continue;
+        }
         double Sz = P.Sz[p], Bm = P.Bm[p], Cq = P.Cq[p], Nq = P.Nq[p], Pq = P.Pq[p], Chl = P.Chl[p];
         double gen = P.gen[p];
         P.x[d] = P.x[p]; P.y[d] = P.y[p]; P.z[d] = P.z[p];
@@ -522,6 +542,116 @@ __global__ void k_physiology(DGrid g, SpcDev P, pi_quota_params p, long long C, 
         for (int q = 0; q < PI_NPROC; ++q) procv[(long long)q * C + slot] = v[q];
     }
     // diags_proc!(num, ac, ac) at the slot's (possibly stale) cell
+    atomicAdd(&d_num[c], 1.0);
+}
+
+// ------------------------------------------------------------------------------------------
+// CarbonMode physiology — CarbonMode/plankton_growth.jl:2-29, growth_kernels.jl:2-120,
+// division_death_probability.jl:7-107, calc_consume! (consume_loss.jl:2-5)
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ double c_tempFunc_PS(double T, const pi_carbon_params& p) {
+    double x = T - p.Topt, xmax = p.Tmax - p.Topt;
+    double regT = shape_dec(x, xmax, F_1em1, 4);
+    double k = pi_exp(-p.Ea / (F_RGAS * (T + F_T0))) * regT;
+    k = jl_max(0.0, k);
+    double OGT_rate = pi_exp(-p.Ea / (F_RGAS * (p.Topt + F_T0)));
+    return jl_min(1.0, k / OGT_rate);
+}
+__device__ __forceinline__ double c_tempFunc(double T, const pi_carbon_params& p) {
+    double k = pi_exp(-p.Ea / (F_RGAS * (T + F_T0)));
+    k = jl_max(0.0, k);
+    double OGT_rate = pi_exp(-p.Ea / (F_RGAS * (p.Topt + F_T0)));
+    return jl_min(1.0, k / OGT_rate);
+}
+// gamma_alloc (growth_kernels.jl:22-26)
+__device__ __forceinline__ double c_gamma(double Bm, double Bd, const pi_carbon_params& p) {
+    double gm = jl_mulb(Bd / jl_max(F_1em30, Bm), jl_isless(0.0, Bd));
+    return jl_mulb(jl_min(1.0, gm), p.thermal == 1.0);
+}
+
+__global__ void k_physiology_carbon(DGrid g, SpcDev P, pi_carbon_params p, long long C, int s,
+                                    double dT, double t, uint64_t seed, uint32_t iter, int shared_graz,
+                                    const double* __restrict__ par, const double* __restrict__ temp,
+                                    const uint32_t* __restrict__ off, const uint32_t* __restrict__ gid_sorted,
+                                    const int32_t* __restrict__ pos, double* __restrict__ contrib,
+                                    double* __restrict__ d_num, double* __restrict__ procv, const uint32_t* err) {
+    long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= C) return;
+    if (*err & PI_DEVERR_CAPACITY) return;
+    uint8_t f = P.flags[slot];
+    int ac = f & FL_AC;
+    int ac0 = P.stat[slot] & ST_AC0;
+    long long e = ac0 ? pos[(long long)s * C + slot] : -1;
+    if (!ac) {
+        // inactive after this step's deaths: every rate is 0 and the state keeps its values
+        if (ac0) {
+            double* K = contrib + e * 5;
+            K[0] = 0.0; K[1] = 0.0; K[2] = 0.0; K[3] = 0.0; K[4] = 0.0;
+        }
+        return;
+    }
+    int xi, yi, zi;
+    unpack_cell(g, P.cell[slot], xi, yi, zi);
+    int c = gidx(g, xi, yi, zi);
+    double parv = 0.0, T = 0.0, pop = 0.0;
+    if (ac0) {
+        parv = par[c]; T = temp[c];
+        if (shared_graz) {
+            pop = (double)(off[c + 1] - off[c]);
+        } else {
+            uint32_t n = 0;
+            for (uint32_t q = off[c]; q < off[c + 1]; ++q) n += (gid_sorted[q] / (uint32_t)C) == (uint32_t)s;
+            pop = (double)n;
+        }
+    }
+    double Bm = P.Bm[slot], Bd = P.Bd[slot], Chl = P.Chl[slot], age = P.age[slot];
+    // calc_PS! (calc_photosynthesis, growth_kernels.jl:29-36)
+    double aI = parv * p.alpha * p.Phi;
+    double PCm = p.PCmax * (c_tempFunc(T, p) * p.thermal + c_tempFunc_PS(T, p) * (1.0 - p.thermal));
+    double light = 1.0 - pi_exp(-aI / jl_max(F_1em30, PCm) * Chl / jl_max(F_1em30, Bm));
+    double PS = jl_mulb(PCm * jl_max(0.0, Bm - Bd) * (light * (1.0 - p.is_bact) + p.is_bact), ac);
+    // calc_BS!, calc_repair! (:55-64), calc_thermal_damage! (:69-75), calc_respir! (:82-85)
+    double BS = PS * (1.0 - c_gamma(Bm, Bd, p));
+    double RP = PS * c_gamma(Bm, Bd, p);
+    double TD = jl_mulb(jl_mulb(jl_mulb((T - p.Topt) * p.f_T2B * (Bm - Bd), jl_isless(p.Topt, T)),
+                                jl_isless(Bd, Bm)), p.thermal == 1.0);
+    TD = jl_max(0.0, jl_min(TD, (Bm - Bd) / dT));
+    double RS = jl_mulb(p.respir * Bm * c_tempFunc(T, p), ac);
+    // update_quotas! (:92-97), update_cellsize! (:104-108)
+    Bm += (BS - RS) * dT;
+    Bd += (TD - RP) * dT;
+    age += jl_mulb(dT / 3600.0, ac);
+    double Sz = Bm / (p.Cquota * p.Nsuper);
+    Chl = Bm * p.Chl2C;
+    // probabilities (division_death_probability.jl:26-30, 49-52, 60-77)
+    double graz = jl_mulb(pop * p.grz_P, ac);
+    double dv;
+    int ty = (int)p.dvid_type;
+    if (ty == 1) dv = p.dvid_P * shape_inc(Sz, p.dvid_reg, F_2em3, 2);
+    else if (ty == 2) dv = p.dvid_P * shape_inc(fmod(t, 86400.0) / 3600.0, p.dvid_reg, F_1em5, 4);
+    else dv = p.dvid_P * shape_inc(Sz, p.dvid_reg, F_1em3, 4) * shape_inc(fmod(t, 86400.0) / 3600.0, p.dvid_reg2, F_1em5, 4);
+    double dvid = jl_mulb(dv, ac);
+    double mort = p.thermal == 1.0 ? jl_mulb(p.mort_P * shape_inc(Bd / jl_max(F_1em30, Bm), F_0p99, F_1em6, 4), ac)
+                                   : jl_mulb(p.mort_P * shape_dec(Sz, p.mort_reg, F_1em5, 4), ac);
+    // get_probability! (:95-107)
+    double r0, r1, r2;
+    pi_draw3(seed, iter, (uint32_t)s, PI_DRAW_DECISION, (uint32_t)slot, &r0, &r1, &r2);
+    int dg = jl_isless(r0, graz * dT) && ac;
+    int dm = jl_isless(r1, mort * dT) && ac;
+    int dd = jl_isless(r2, dvid * dT) && ac;
+    P.Bm[slot] = Bm; P.Bd[slot] = Bd; P.Chl[slot] = Chl; P.age[slot] = age; P.Sz[slot] = Sz;
+    P.flags[slot] = (uint8_t)(FL_AC | (dg ? FL_GRAZ : 0) | (dm ? FL_MORT : 0) | (dd ? FL_DVID : 0));
+    // calc_consume_kernel!: DIC only
+    if (ac0) {
+        double* K = contrib + e * 5;
+        K[0] = jl_mulb((RS - PS) * dT, ac);
+        K[1] = 0.0; K[2] = 0.0; K[3] = 0.0; K[4] = 0.0;
+    }
+    // diags_spcs! values of the slot (PI_CPROC_* order)
+    if (procv) {
+        const double v[PI_NCPROC] = { PS, BS, RP, RS, TD, Bm, Bd, Chl };
+        for (int q = 0; q < PI_NCPROC; ++q) procv[(long long)q * C + slot] = v[q];
+    }
     atomicAdd(&d_num[c], 1.0);
 }
 

@@ -52,6 +52,8 @@ struct pi_model {
     uint64_t seed = 0;
     int precision = PI_FP64;
     pi_batch* b32 = nullptr;     // PI_FP32: the model is a batch of one member
+    int carbon = 0;              // CarbonMode species (pi_create_carbon)
+    std::vector<pi_carbon_params> cp;
     int64_t iteration = 0;
     double t = 0.0;
     double last_dT = 0.0;
@@ -285,7 +287,7 @@ pi_status enqueue_step(pi_model* m, double dT) {
         double* dsp = m->diag_sp + (size_t)s * 4 * G;
         { ProfScope ps_(m, "k_decide");
         k_decide<<<nblk(C, BS), BS, 0, st>>>(g, m->h_spc[s], m->sp[s], C, s, sb.pos, sb.loss, sb.evk,
-                                             sb.flag64, dsp + 1 * G, dsp + 2 * G, dsp + 3 * G, sb.err);
+                                             sb.flag64, dsp + 1 * G, dsp + 2 * G, dsp + 3 * G, sb.err, m->carbon);
         CK(cudaGetLastError(), "k_decide"); }
         tb = m->cub_bytes;
         { ProfScope ps_(m, "cub_scan_slots");
@@ -295,9 +297,14 @@ pi_status enqueue_step(pi_model* m, double dT) {
                                             sb.err, sb.err_iter, m->iteration);
         CK(cudaGetLastError(), "k_lists"); }
         { ProfScope ps_(m, "k_daughters");
-        k_daughters<<<148 * 4, 256, 0, st>>>(m->h_spc[s], sb.divlist, sb.freelist, sb.ndiv, sb.err);
+        k_daughters<<<148 * 4, 256, 0, st>>>(m->h_spc[s], sb.divlist, sb.freelist, sb.ndiv, sb.err, m->carbon);
         CK(cudaGetLastError(), "k_daughters"); }
         const double* trp = m->tr;
+        if (m->carbon) { ProfScope ps_(m, "k_physiology");
+        k_physiology_carbon<<<nblk(C, BS), BS, 0, st>>>(g, m->h_spc[s], m->cp[s], C, s, dT, m->t, m->seed, iter,
+                                                        shared, m->par, m->temp, sb.off, sb.gid_sorted, sb.pos,
+                                                        sb.contrib, dsp + 0 * G, m->proc_mask ? m->procv : nullptr, sb.err);
+        CK(cudaGetLastError(), "k_physiology_carbon"); } else
         { ProfScope ps_(m, "k_physiology");
         k_physiology<<<nblk(C, BS), BS, 0, st>>>(g, m->h_spc[s], m->sp[s], C, s, dT, m->t, m->seed, iter,
                                                  shared, trp + PI_NH4 * G, trp + PI_NO3 * G,
@@ -572,6 +579,46 @@ pi_status pi_create(const pi_grid* grid, const pi_bgc_params* bgc, const pi_quot
     return PI_OK;
 }
 
+pi_status pi_create_carbon(const pi_grid* grid, const pi_bgc_params* bgc, const pi_carbon_params* species,
+                           int32_t nspecies, int64_t capacity, int32_t precision, uint64_t seed, pi_model** out) {
+    if (!out) return fail(nullptr, PI_ERR_ARG, "pi_create_carbon: out is NULL");
+    *out = nullptr;
+    if (!species || nspecies < 1) return fail(nullptr, PI_ERR_ARG, "pi_create_carbon: NULL species or nspecies < 1");
+    if (precision != PI_FP64)
+        return fail(nullptr, PI_ERR_ARG, "pi_create_carbon: CarbonMode is built in the FP64 form only (precision PI_FP64)");
+    // the QuotaMode setup with the parameters both modes share; the species then switch to CarbonMode
+    std::vector<pi_quota_params> q((size_t)nspecies);
+    for (int s = 0; s < nspecies; ++s) {
+        const pi_carbon_params& c = species[s];
+        pi_quota_params& p = q[s];
+        memset(&p, 0, sizeof p);
+        p.Nsuper = c.Nsuper; p.Cquota = c.Cquota; p.mean = c.mean; p.var = c.var; p.alpha = c.alpha;
+        p.Phi = c.Phi; p.Topt = c.Topt; p.Tmax = c.Tmax; p.Ea = c.Ea; p.PCmax = c.PCmax; p.respir = c.respir;
+        p.grz_P = c.grz_P; p.dvid_type = c.dvid_type; p.dvid_P = c.dvid_P; p.dvid_reg = c.dvid_reg;
+        p.dvid_reg2 = c.dvid_reg2; p.mort_P = c.mort_P; p.mort_reg = c.mort_reg;
+        p.grazFracC = c.grazFracC; p.mortFracC = c.mortFracC;
+    }
+    pi_status st = pi_create(grid, bgc, q.data(), nspecies, capacity, PI_FP64, seed, out);
+    if (st) return st;
+    pi_model* m = *out;
+    m->carbon = 1;
+    m->cp.assign(species, species + nspecies);
+    for (int s = 0; s < nspecies; ++s) {
+        SpcDev& P = m->h_spc[s];
+        if ((st = dalloc(m, &P.Bd, (size_t)capacity, "damaged biomass")) ||
+            cudaMemsetAsync(P.Bd, 0, (size_t)capacity * sizeof(double), m->stream) != cudaSuccess) {
+            pi_destroy(m); *out = nullptr;
+            return fail(nullptr, st ? st : PI_ERR_CUDA, "pi_create_carbon: device allocation failed");
+        }
+    }
+    if (cudaMemcpyAsync(m->d_spc, m->h_spc.data(), nspecies * sizeof(SpcDev), cudaMemcpyHostToDevice, m->stream) != cudaSuccess ||
+        cudaStreamSynchronize(m->stream) != cudaSuccess) {
+        pi_destroy(m); *out = nullptr;
+        return fail(nullptr, PI_ERR_CUDA, "pi_create_carbon: device initialisation failed");
+    }
+    return PI_OK;
+}
+
 pi_status pi_destroy(pi_model* m) {
     if (!m) return PI_OK;
     if (m->b32) {
@@ -593,7 +640,9 @@ pi_status pi_set_individuals(pi_model* m, int32_t sp, const pi_individuals* in) 
     if (!m || !in || sp < 0 || sp >= m->nsp) return fail(m, PI_ERR_ARG, "pi_set_individuals: bad argument");
     const double* dcols[] = { in->x, in->y, in->z, in->Sz, in->Bm, in->Cq, in->Nq, in->Pq, in->Chl, in->gen, in->age,
                               in->graz, in->mort, in->dvid };
-    for (const double* p : dcols) if (!p) return fail(m, PI_ERR_ARG, "pi_set_individuals: NULL attribute");
+    for (int q = 0; q < 14; ++q)
+        if (!dcols[q] && !(m->carbon && q >= 5 && q <= 7))        // CarbonMode keeps no quotas
+            return fail(m, PI_ERR_ARG, "pi_set_individuals: NULL attribute");
     if (!in->xi || !in->yi || !in->zi || !in->ac) return fail(m, PI_ERR_ARG, "pi_set_individuals: NULL attribute");
     const long long C = m->C;
     const HostGrid& g = m->hg;
@@ -613,7 +662,11 @@ pi_status pi_set_individuals(pi_model* m, int32_t sp, const pi_individuals* in) 
     const SpcDev& P = m->h_spc[sp];
     double* dptr[] = { P.x, P.y, P.z, P.Sz, P.Bm, P.Cq, P.Nq, P.Pq, P.Chl, P.gen, P.age };
     for (int q = 0; q < 11; ++q)
-        CK(cudaMemcpyAsync(dptr[q], dcols[q], C * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload individuals");
+        if (dcols[q]) CK(cudaMemcpyAsync(dptr[q], dcols[q], C * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload individuals");
+    if (m->carbon) {
+        if (in->Bd) CK(cudaMemcpyAsync(P.Bd, in->Bd, C * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload individuals");
+        else CK(cudaMemsetAsync(P.Bd, 0, C * sizeof(double), m->stream), "upload individuals");
+    }
     CK(cudaMemcpyAsync(P.flags, flags.data(), C, cudaMemcpyHostToDevice, m->stream), "upload flags");
     CK(cudaMemcpyAsync(P.cell, cell.data(), C * sizeof(int32_t), cudaMemcpyHostToDevice, m->stream), "upload cells");
     CK(cudaMemsetAsync(P.stat, 0, C, m->stream), "reset step status");
@@ -630,6 +683,7 @@ pi_status pi_get_individuals(pi_model* m, int32_t sp, pi_individuals* out) {
     const double* dptr[] = { P.x, P.y, P.z, P.Sz, P.Bm, P.Cq, P.Nq, P.Pq, P.Chl, P.gen, P.age };
     for (int q = 0; q < 11; ++q)
         if (hptr[q]) CK(cudaMemcpyAsync(hptr[q], dptr[q], C * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download individuals");
+    if (m->carbon && out->Bd) CK(cudaMemcpyAsync(out->Bd, P.Bd, C * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download individuals");
     std::vector<uint8_t> flags(C);
     std::vector<int32_t> cell(C);
     CK(cudaMemcpyAsync(flags.data(), P.flags, C, cudaMemcpyDeviceToHost, m->stream), "download flags");
@@ -928,7 +982,8 @@ pi_status pi_count_active_async(pi_model* m, int32_t sp, int64_t* n) {
 
 pi_status pi_set_diags(pi_model* m, uint32_t tracer_mask, uint32_t proc_mask) {
     if (m && m->b32) return fwd32(m, pi_batch_set_diags(m->b32, tracer_mask, proc_mask));
-    if (!m || tracer_mask >> PI_NTRACERS || proc_mask >> PI_NPROC) return fail(m, PI_ERR_ARG, "pi_set_diags: bad argument");
+    if (!m || tracer_mask >> PI_NTRACERS || proc_mask >> (m->carbon ? (int)PI_NCPROC : (int)PI_NPROC))
+        return fail(m, PI_ERR_ARG, "pi_set_diags: bad argument");
     const long long G = m->hg.G, C = m->C;
     CK(cudaStreamSynchronize(m->stream), "synchronize");
     if (tracer_mask && !m->diag_tr) { pi_status e = dalloc(m, &m->diag_tr, (size_t)PI_NTRACERS * G, "tracer diagnostics"); if (e) return e; }

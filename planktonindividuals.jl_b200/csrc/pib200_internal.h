@@ -19,6 +19,8 @@
 #define F_2em3  ((double)2.0e-3f)
 #define F_1em3  ((double)1.0e-3f)
 #define F_1em5  ((double)1.0e-5f)
+#define F_1em6  ((double)1.0e-6f)
+#define F_0p99  ((double)0.99f)
 #define F_THMAX ((double)1.0e20f)
 #define F_1em20 ((double)1.0e-20f)
 
@@ -66,6 +68,7 @@ __host__ __device__ __forceinline__ void unpack_cell(const DGrid& g, int32_t c, 
 // Device pointers of one species (FP64 plain form).
 struct SpcDev {
     double *x, *y, *z, *Sz, *Bm, *Cq, *Nq, *Pq, *Chl, *gen, *age;
+    double* Bd;         // CarbonMode damaged biomass (NULL for QuotaMode)
     uint8_t* flags;
     int32_t* cell;      // packed (xi, yi, zi)
     uint8_t* stat;      // ST_* bits of the current step
