@@ -5,8 +5,8 @@ import numpy as np
 from . import _abi, _lib
 from ._abi import NTRACERS, PI_FP32, PI_FP64, tracer_names
 from ._native import CModel
-from .architectures import GPU, QuotaMode
-from .init import generate_tracers, initialize_plankton
+from .architectures import GPU, CarbonMode, QuotaMode
+from .init import generate_tracers, initialize_plankton, initialize_plankton_carbon
 from .parameters import (bgc_params_default, default_tracer_init, phyt_params_default,
                          update_bgc_params, update_phyt_params)
 
@@ -62,16 +62,21 @@ class PlanktonModel:
                  max_candidates=25, seed=0, initial_state=None):
         if not isinstance(arch, GPU) and arch is not GPU:
             raise ValueError("PlanktonModel: this implementation runs on GPU() only (no CPU fallback)")
-        if mode is not None and not isinstance(mode, QuotaMode) and mode is not QuotaMode:
-            raise NotImplementedError(f"{mode}: only QuotaMode() is implemented")
+        if mode is CarbonMode:
+            mode = CarbonMode()
+        carbon = isinstance(mode, CarbonMode)
+        if mode is not None and not carbon and not isinstance(mode, QuotaMode) and mode is not QuotaMode:
+            raise NotImplementedError(f"{mode}: QuotaMode() and CarbonMode() are implemented")
         if abiotic is not None:
             raise NotImplementedError("abiotic particles are not implemented")
         FT = np.dtype(FT).type
         if FT not in (np.float32, np.float64):
             raise ValueError("FT must be Float32 or Float64")
+        if carbon and FT is not np.float64:
+            raise NotImplementedError("CarbonMode() is built in the FP64 form: use FT = Float64")
         self.FT = FT
         self.arch = GPU()
-        self.mode = QuotaMode()
+        self.mode = mode if carbon else QuotaMode()
         self.grid = grid
         self.max_candidates = max_candidates
         if bgc_params is None:
@@ -80,8 +85,9 @@ class PlanktonModel:
             bgc_final = update_bgc_params(bgc_params, FT)
         else:
             raise ValueError("Phytoplankton parameters must be either Nothing or Dict!")
+        pmode = self.mode
         if phyto is None:
-            phyto = phyto_setup(update_phyt_params({}, FT, N=1), [2 ** 10], 1)
+            phyto = phyto_setup(update_phyt_params({}, FT, N=1, mode=pmode), [2 ** 10], 1)
         elif isinstance(phyto, phyto_setup):
             if max(phyto.N) > max_individuals:
                 raise ValueError("maximum(phyto.N) ≤ max_individuals")
@@ -89,9 +95,9 @@ class PlanktonModel:
                 raise ValueError(f"PlanktonModel: `phyto`: The length of `N` must be {phyto.Nsp}, the same as "
                                  f"`Nsp`, each species has its own initial condition")
             if phyto.params is None:
-                phyto.params = update_phyt_params({}, FT, N=phyto.Nsp)
+                phyto.params = update_phyt_params({}, FT, N=phyto.Nsp, mode=pmode)
             elif isinstance(phyto.params, dict):
-                phyto.params = update_phyt_params(phyto.params, FT, N=phyto.Nsp)
+                phyto.params = update_phyt_params(phyto.params, FT, N=phyto.Nsp, mode=pmode)
             else:
                 raise ValueError("Phytoplankton parameters must be either Nothing or Dict!")
         else:
@@ -103,11 +109,11 @@ class PlanktonModel:
         lib = _lib.load()
         precision = PI_FP64 if FT is np.float64 else PI_FP32
         self._native = CModel(lib, "pi_", grid, bgc_final, phyto.params, nsp, max_individuals,
-                              seed, precision=precision)
+                              seed, precision=precision, mode="carbon" if carbon else "quota")
         if initial_state is None:
             rng = np.random.default_rng(seed)
-            inds = [initialize_plankton(grid, phyto.params, s, phyto.N[s], max_individuals, rng)
-                    for s in range(nsp)]
+            init = initialize_plankton_carbon if carbon else initialize_plankton
+            inds = [init(grid, phyto.params, s, phyto.N[s], max_individuals, rng) for s in range(nsp)]
             trs = generate_tracers(grid, tracer_initial or default_tracer_init(), rng)
         else:
             inds, trs = initial_state
@@ -140,7 +146,7 @@ class PlanktonModel:
 
     def __repr__(self):
         return (f"PlanktonModel:\n├── floating point data type: {np.dtype(self.FT).name}\n"
-                f"├── grid: {self.grid!r}\n├── QuotaMode() is selected for phytoplankton physiology\n"
+                f"├── grid: {self.grid!r}\n├── {self.mode!r} is selected for phytoplankton physiology\n"
                 f"├── phytoplankton: {self.phyto.Nsp} species with {self.count_active()} individuals for each species\n"
                 f"└── maximum number of individuals: {self.max_individuals} per species")
 
@@ -148,9 +154,10 @@ class PlanktonModel:
 class PlanktonDiagnostics:
     """PlanktonDiagnostics(model; tracer, phytoplankton, iteration_interval)
     (diagnostics_struct.jl:23-105). The default diagnostics (PAR and num/graz/mort/dvid per
-    species) and the requested ones — tracer fields (any of the 14 tracer names) and QuotaMode
-    processes (PS, BS, VDOC, VNH4, VNO3, VPO4, resp, exu, Bm, Cq, Nq, Pq, Chl) — are accumulated on
-    the device by every step; fields download on access."""
+    species) and the requested ones — tracer fields (any of the 14 tracer names) and the mode's
+    processes (QuotaMode: PS, BS, VDOC, VNH4, VNO3, VPO4, resp, exu, Bm, Cq, Nq, Pq, Chl; CarbonMode:
+    PS, BS, RP, RS, TD, Bm, Bd, Chl) — are accumulated on the device by every step; fields download
+    on access."""
 
     DEFAULT = ("num", "graz", "mort", "dvid", "ptc")
 
@@ -158,12 +165,13 @@ class PlanktonDiagnostics:
                  abiotic_particle=("num",), iteration_interval=1):
         if not isinstance(tracer, tuple) or not isinstance(phytoplankton, tuple):
             raise ValueError("tracer and phytoplankton must be Tuples")
-        # diag_avail (diagnostics_struct.jl:115-136): names available for QuotaMode
+        # diag_avail (diagnostics_struct.jl:115-136): names available for the model's mode
+        proc_names = _abi.CARBON_PROC_NAMES if isinstance(model.mode, CarbonMode) else _abi.PROC_NAMES
         for t in tracer:
             if t not in tracer_names and t != "PAR":
                 raise ValueError(f"{t} is not one of the diagnostics")
         for p in phytoplankton:
-            if p not in self.DEFAULT and p not in _abi.PROC_NAMES:
+            if p not in self.DEFAULT and p not in proc_names:
                 raise ValueError(f"{p} is not one of the diagnostics")
         for a in abiotic_particle:
             if a != "num":
@@ -177,8 +185,8 @@ class PlanktonDiagnostics:
                 tmask |= 1 << tracer_names.index(t)
         pmask = 0
         for p in phytoplankton:
-            if p in _abi.PROC_NAMES:
-                pmask |= 1 << _abi.PROC_NAMES.index(p)
+            if p in proc_names:
+                pmask |= 1 << proc_names.index(p)
         nat.set_diags(tmask, pmask)
         G = model.grid.total_size
         procs = tuple(dict.fromkeys(tuple(phytoplankton) + self.DEFAULT))
@@ -198,7 +206,7 @@ class PlanktonDiagnostics:
                 if k in kinds:
                     return nat.get_diag(kinds[k], self.s)
                 if k in procs:
-                    return nat.get_diag(_abi.PI_DIAG_PROC + _abi.PROC_NAMES.index(k), self.s)
+                    return nat.get_diag(_abi.PI_DIAG_PROC + proc_names.index(k), self.s)
                 raise AttributeError(k)
 
             def __getitem__(self, k):

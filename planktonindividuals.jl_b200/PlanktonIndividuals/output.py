@@ -132,19 +132,24 @@ def write_diags(diags, path, t, it, ncounts, grid):
     diags.reset()
 
 
-def write_species_dynamics(t, phytos, filepath):
-    """write_species_dynamics for QuotaMode (write_outputs.jl:98-117): one line per species file."""
+def write_species_dynamics(t, phytos, filepath, carbon=False):
+    """write_species_dynamics for QuotaMode (write_outputs.jl:98-117) or CarbonMode (:142-157): one
+    line per species file."""
     for i, sp in enumerate(phytos.keys(), start=1):
         d = phytos[sp].data
         ac = np.asarray(d["ac"], dtype=bool)
         pop = int(ac.sum())
-        ave = {k: (float(np.sum(np.asarray(d[k])[ac])) / pop if pop else float("nan"))
-               for k in ("gen", "age", "Sz", "Bm", "Cq", "Nq", "Pq", "Chl")}
+        keys = ("gen", "age", "Sz", "Bm") if carbon else ("gen", "age", "Sz", "Bm", "Cq", "Nq", "Pq", "Chl")
+        ave = {k: (float(np.sum(np.asarray(d[k])[ac])) / pop if pop else float("nan")) for k in keys}
         day, hour = t // 86400, (t % 86400) / 3600
         with open(os.path.join(filepath, "dynamic_species%03d.txt" % i), "a") as f:
-            f.write("%3.0f  %2.2f  %6.0f  %1.2f  %1.2f  %1.2f  %.8E  %.8E  %.8E  %.8E  %.8E\n" %
-                    (day, hour, pop, ave["gen"], ave["age"], ave["Sz"], ave["Bm"], ave["Cq"], ave["Nq"],
-                     ave["Pq"], ave["Chl"]))
+            if carbon:
+                f.write("%3.0f  %2.2f  %6.0f  %1.2f  %1.2f  %1.2f  %.8E\n" %
+                        (day, hour, pop, ave["gen"], ave["age"], ave["Sz"], ave["Bm"]))
+            else:
+                f.write("%3.0f  %2.2f  %6.0f  %1.2f  %1.2f  %1.2f  %.8E  %.8E  %.8E  %.8E  %.8E\n" %
+                        (day, hour, pop, ave["gen"], ave["age"], ave["Sz"], ave["Bm"], ave["Cq"], ave["Nq"],
+                         ave["Pq"], ave["Chl"]))
 
 
 def write_output_b(writer, model, diags):
@@ -154,7 +159,8 @@ def write_output_b(writer, model, diags):
     t, it = model.t, model.iteration
     phytos = model.individuals.phytos
     if writer.write_log:
-        write_species_dynamics(t, phytos, writer.filepath)
+        from .architectures import CarbonMode
+        write_species_dynamics(t, phytos, writer.filepath, carbon=isinstance(getattr(model, "mode", None), CarbonMode))
     if writer.save_diags and it % diags.iteration_interval == 0:
         if _filesize(writer.diags_file) >= writer.max_filesize:
             writer.diags_file, writer.part_diags = _next_part(writer.diags_file, writer.part_diags)

@@ -74,3 +74,41 @@ def test_carbon_fp32_is_refused(gpu_lib):
         CModel(gpu_lib, "pi_", wl.grid, wl.bgc, wl.phyt, wl.nsp, wl.capacity, wl.seed, precision=_abi.PI_FP32,
                mode="carbon")
     assert "FP64 form only" in str(ei.value)
+
+
+def test_carbon_drop_in_api_bitexact(gpu_lib):
+    """PlanktonModel(GPU(), grid; FT = Float64, mode = CarbonMode()) → PlanktonSimulation →
+    update!, with PlanktonDiagnostics of CarbonMode processes by name, against the oracle from the
+    model's own initial state; FT = Float32 is refused."""
+    import math
+    from PlanktonIndividuals import (GPU, CarbonMode, PlanktonDiagnostics, PlanktonModel, PlanktonSimulation,
+                                     RectilinearGrid, default_PARF, phyto_setup, tracer_names, update_b)
+    grid = RectilinearGrid(size=(12, 12, 6), x=(0.0, 600.0), y=(0.0, 600.0), z=(0.0, -12.0), FT=np.float64)
+    params = {"dvid_P": 1e-3, "mort_P": 5e-4, "grz_P": 2e-5}
+    model = PlanktonModel(GPU(), grid, FT=np.float64, mode=CarbonMode(), max_individuals=4000,
+                          phyto=phyto_setup(dict(params), [1500], 1), seed=5)
+    diags = PlanktonDiagnostics(model, tracer=("DIC",), phytoplankton=("num", "PS", "RS", "Bm"))
+    fv = W.FourierVelocity(grid, nmodes=12, rms=0.02, seed=3)
+    snaps = [fv(i) for i in range(2)]
+    vels = {c: np.stack([s[q] for s in snaps], axis=-1) for q, c in enumerate("uvw")}
+    parf = np.asfortranarray(np.roll(default_PARF(grid, 60.0, 20), -10, axis=2))
+    ref = oracle.OracleModel(grid, model.bgc_params, model.phyto.params, 1, 4000, 5, mode="carbon")
+    ref.set_state([dict(model.individuals.phytos.sp1.data)], [model.tracers[n].data for n in tracer_names])
+    ref.set_diags(1 << tracer_names.index("DIC"), (1 << 0) | (1 << 3) | (1 << 5))
+    sim = PlanktonSimulation(model, ΔT=60.0, iterations=20, PARF=parf, vels=vels, ΔT_vel=600.0, diags=diags)
+    inp = sim.input
+    for _ in range(20):
+        _, t = ref.get_time()
+        tv, tp, tt = (int(math.floor(t / inp[k])) for k in ("ΔT_vel", "ΔT_PAR", "ΔT_temp"))
+        ref.set_velocity(*(np.asfortranarray(np.asarray(inp["vels"][c])[..., tv]) for c in "uvw"))
+        ref.set_PARF(inp["PARF"][:, :, tp])
+        ref.set_temp(inp["temp"][:, :, :, tt])
+        ref.time_step(60.0)
+    update_b(sim)
+    assert compare_states(ref, model._native, 1) == []
+    assert same(ref.get_diag(_abi.PI_DIAG_PROC + 0, 0), diags.phytos.sp1.PS)
+    assert same(ref.get_diag(_abi.PI_DIAG_PROC + 3, 0), diags.phytos.sp1.RS)
+    assert same(ref.get_diag(_abi.PI_DIAG_TRACER + tracer_names.index("DIC"), 0), diags.tracer.DIC)
+    with pytest.raises(NotImplementedError):
+        PlanktonModel(GPU(), grid, FT=np.float32, mode=CarbonMode(), max_individuals=100,
+                      phyto=phyto_setup(None, [10], 1))
