@@ -13,7 +13,7 @@
 module PIB200
 
 export PiGrid, PiBgc, PiQuota, PiIndividuals, PiMember, PIError
-export create, destroy, set_individuals!, get_individuals, set_tracer!, get_tracer
+export create, create_carbon, destroy, set_individuals!, get_individuals, set_tracer!, get_tracer
 export set_velocity!, set_PARF!, set_temp!, set_flux_bc!, time_step!, get_time, set_time!
 export count_active, get_diag, reset_diags!, check_finite, budget, simulation, update!, synchronize
 export set_velocity_f32!, set_PARF_f32!, set_temp_f32!, time_step_async!, count_active_async!, set_diags!
@@ -34,6 +34,8 @@ const DIAG_KINDS = Dict(:PAR => Int32(0), :num => Int32(1), :graz => Int32(2), :
 const PI_DIAG_TRACER = Int32(16)
 const PI_DIAG_PROC = Int32(32)
 const PROCS = (:PS, :BS, :VDOC, :VNH4, :VNO3, :VPO4, :resp, :exu, :Bm, :Cq, :Nq, :Pq, :Chl)
+const CPROCS = (:PS, :BS, :RP, :RS, :TD, :Bm, :Bd, :Chl)      # CarbonMode processes
+procs(m) = m.carbon ? CPROCS : PROCS
 
 struct PiGrid
     Nx::Int32; Ny::Int32; Nz::Int32
@@ -64,6 +66,15 @@ struct PiQuota
 end
 PiQuota(p::AbstractDict, sp::Integer) = PiQuota(ntuple(i -> Float64(p[QUOTA_KEYS[i]][sp]), 40))
 
+# CarbonMode param_names (src/Individuals/Plankton/CarbonMode/plankton_generation.jl:13-15)
+const CARBON_KEYS = ("Nsuper", "Cquota", "mean", "var", "α", "Φ", "Topt", "Tmax", "Ea", "PCmax", "Chl2C",
+                     "respir", "f_T2B", "grz_P", "dvid_type", "dvid_P", "dvid_reg", "dvid_reg2", "mort_P",
+                     "mort_reg", "grazFracC", "mortFracC", "thermal", "is_bact")
+struct PiCarbon
+    v::NTuple{24,Float64}
+end
+PiCarbon(p::AbstractDict, sp::Integer) = PiCarbon(ntuple(i -> Float64(p[CARBON_KEYS[i]][sp]), 24))
+
 struct PiIndividuals
     x::Ptr{Float64}; y::Ptr{Float64}; z::Ptr{Float64}
     xi::Ptr{Int64}; yi::Ptr{Int64}; zi::Ptr{Int64}
@@ -71,6 +82,7 @@ struct PiIndividuals
     Chl::Ptr{Float64}; gen::Ptr{Float64}; age::Ptr{Float64}
     ac::Ptr{UInt8}
     graz::Ptr{Float64}; mort::Ptr{Float64}; dvid::Ptr{Float64}
+    Bd::Ptr{Float64}            # CarbonMode damaged biomass (C_NULL for QuotaMode)
 end
 
 struct PiMember
@@ -108,6 +120,7 @@ mutable struct Model
     G::NTuple{3,Int}
     Nsp::Int
     capacity::Int
+    carbon::Bool
 end
 
 topo_code(T) = occursin("Periodic", string(T)) ? PI_PERIODIC : PI_BOUNDED
@@ -131,7 +144,25 @@ function create(g, bgc::AbstractDict, phyt::AbstractDict, Nsp::Integer, maxN::In
         (Ref{PiGrid}, Ref{PiBgc}, Ptr{PiQuota}, Int32, Int64, Int32, UInt64, Ref{Ptr{Cvoid}}),
         pg, pb, ps, Nsp, maxN, FT === Float32 ? PI_FP32 : PI_FP64, seed, out)
     check(st, C_NULL)
-    m = Model(out[], (g.Nx + 2g.Hx, g.Ny + 2g.Hy, g.Nz + 2g.Hz), Nsp, maxN)
+    m = Model(out[], (g.Nx + 2g.Hx, g.Ny + 2g.Hy, g.Nz + 2g.Hz), Nsp, maxN, false)
+    finalizer(destroy, m)
+    m
+end
+
+"""PlanktonModel(GPU(), grid; FT = Float64, mode = CarbonMode(), ...): CarbonMode species, built in
+the FP64 form only."""
+function create_carbon(g, bgc::AbstractDict, phyt::AbstractDict, Nsp::Integer, maxN::Integer; seed::Integer = 0)
+    dzF, dzC = Float64.(collect(g.dzF)), Float64.(collect(g.dzC))
+    lm = UInt8.(vec(collect(g.landmask)))
+    pg = Ref(pigrid(g, dzF, dzC, lm))
+    pb = Ref(PiBgc(bgc))
+    ps = [PiCarbon(phyt, s) for s in 1:Nsp]
+    out = Ref{Ptr{Cvoid}}(C_NULL)
+    st = GC.@preserve dzF dzC lm ccall((:pi_create_carbon, lib), Int32,
+        (Ref{PiGrid}, Ref{PiBgc}, Ptr{PiCarbon}, Int32, Int64, Int32, UInt64, Ref{Ptr{Cvoid}}),
+        pg, pb, ps, Nsp, maxN, PI_FP64, seed, out)
+    check(st, C_NULL)
+    m = Model(out[], (g.Nx + 2g.Hx, g.Ny + 2g.Hy, g.Nz + 2g.Hz), Nsp, maxN, true)
     finalizer(destroy, m)
     m
 end
@@ -142,14 +173,18 @@ function destroy(m::Model)
     nothing
 end
 
-"""Upload species `sp` (1-based) from a StructArray-like table with the QuotaMode columns."""
+"""Upload species `sp` (1-based) from a StructArray-like table with the mode's columns
+(QuotaMode: Cq, Nq, Pq; CarbonMode: Bd)."""
 function set_individuals!(m::Model, sp::Integer, d)
+    C = m.capacity
+    quota = m.carbon ? (zeros(Float64, C), zeros(Float64, C), zeros(Float64, C)) :
+                       (Float64.(d.Cq), Float64.(d.Nq), Float64.(d.Pq))
+    bd = m.carbon ? Float64.(d.Bd) : Float64[]
     cols = (Float64.(d.x), Float64.(d.y), Float64.(d.z), Int64.(d.xi), Int64.(d.yi), Int64.(d.zi),
-            Float64.(d.Sz), Float64.(d.Bm), Float64.(d.Cq), Float64.(d.Nq), Float64.(d.Pq),
-            Float64.(d.Chl), Float64.(d.gen), Float64.(d.age), UInt8.(d.ac),
-            Float64.(d.graz), Float64.(d.mort), Float64.(d.dvid))
-    GC.@preserve cols begin
-        pi = Ref(PiIndividuals(map(pointer, cols)...))
+            Float64.(d.Sz), Float64.(d.Bm), quota..., Float64.(d.Chl), Float64.(d.gen), Float64.(d.age),
+            UInt8.(d.ac), Float64.(d.graz), Float64.(d.mort), Float64.(d.dvid))
+    GC.@preserve cols bd begin
+        pi = Ref(PiIndividuals(map(pointer, cols)..., m.carbon ? pointer(bd) : Ptr{Float64}(C_NULL)))
         check(ccall((:pi_set_individuals, lib), Int32, (Ptr{Cvoid}, Int32, Ref{PiIndividuals}), m.h, sp - 1, pi), m.h)
     end
 end
@@ -159,13 +194,16 @@ function get_individuals(m::Model, sp::Integer)
     C = m.capacity
     f = ntuple(_ -> zeros(Float64, C), 3); i = ntuple(_ -> zeros(Int64, C), 3)
     q = ntuple(_ -> zeros(Float64, C), 8); ac = zeros(UInt8, C); dec = ntuple(_ -> zeros(Float64, C), 3)
-    GC.@preserve f i q ac dec begin
+    bd = zeros(Float64, C)
+    GC.@preserve f i q ac dec bd begin
         pi = Ref(PiIndividuals(pointer(f[1]), pointer(f[2]), pointer(f[3]), pointer(i[1]), pointer(i[2]), pointer(i[3]),
-                               map(pointer, q)..., pointer(ac), map(pointer, dec)...))
+                               map(pointer, q)..., pointer(ac), map(pointer, dec)..., pointer(bd)))
         check(ccall((:pi_get_individuals, lib), Int32, (Ptr{Cvoid}, Int32, Ref{PiIndividuals}), m.h, sp - 1, pi), m.h)
     end
-    (x = f[1], y = f[2], z = f[3], xi = i[1], yi = i[2], zi = i[3], Sz = q[1], Bm = q[2], Cq = q[3], Nq = q[4],
-     Pq = q[5], Chl = q[6], gen = q[7], age = q[8], ac = ac .== 1, graz = dec[1], mort = dec[2], dvid = dec[3])
+    m.carbon ? (x = f[1], y = f[2], z = f[3], xi = i[1], yi = i[2], zi = i[3], Sz = q[1], Bm = q[2], Bd = bd,
+                Chl = q[6], gen = q[7], age = q[8], ac = ac .== 1, graz = dec[1], mort = dec[2], dvid = dec[3]) :
+               (x = f[1], y = f[2], z = f[3], xi = i[1], yi = i[2], zi = i[3], Sz = q[1], Bm = q[2], Cq = q[3], Nq = q[4],
+                Pq = q[5], Chl = q[6], gen = q[7], age = q[8], ac = ac .== 1, graz = dec[1], mort = dec[2], dvid = dec[3])
 end
 
 tracer_index(name::Symbol) = Int32(findfirst(==(name), TRACERS) - 1)
@@ -232,7 +270,7 @@ enabled with set_diags!."""
 function get_diag(m::Model, kind::Symbol, sp::Integer = 1)
     k = haskey(DIAG_KINDS, kind) ? DIAG_KINDS[kind] :
         kind in TRACERS ? PI_DIAG_TRACER + tracer_index(kind) :
-        kind in PROCS ? PI_DIAG_PROC + Int32(findfirst(==(kind), PROCS) - 1) :
+        kind in procs(m) ? PI_DIAG_PROC + Int32(findfirst(==(kind), procs(m)) - 1) :
         throw(ArgumentError("$kind is not one of the diagnostics"))
     a = zeros(Float64, m.G)
     check(ccall((:pi_get_diag, lib), Int32, (Ptr{Cvoid}, Int32, Int32, Ptr{Float64}), m.h, k, sp - 1, a), m.h)
@@ -249,7 +287,7 @@ function set_diags!(m::Model; tracer = (), phytoplankton = ())
     end
     for p in phytoplankton
         p in keys(DIAG_KINDS) && continue
-        q = findfirst(==(p), PROCS)
+        q = findfirst(==(p), procs(m))
         q === nothing && throw(ArgumentError("$p is not one of the diagnostics"))
         pm |= UInt32(1) << (q - 1)
     end
