@@ -583,10 +583,21 @@ __global__ void k_physiology_carbon(DGrid g, SpcDev P, pi_carbon_params p, long 
     int ac0 = P.stat[slot] & ST_AC0;
     long long e = ac0 ? pos[(long long)s * C + slot] : -1;
     if (!ac) {
-        // inactive after this step's deaths: every rate is 0 and the state keeps its values
+        // inactive after this step's deaths: every rate that carries ac is 0. Thermal damage does
+        // not (growth_kernels.jl:69-75), and an individual killed in this step gathered its
+        // temperature while it was active, so its damaged biomass still grows by TD·ΔT; the
+        // state of a slot inactive before the step keeps its values (T = 0 gives TD = 0).
         if (ac0) {
             double* K = contrib + e * 5;
             K[0] = 0.0; K[1] = 0.0; K[2] = 0.0; K[3] = 0.0; K[4] = 0.0;
+            int xi, yi, zi;
+            unpack_cell(g, P.cell[slot], xi, yi, zi);
+            const double T = temp[gidx(g, xi, yi, zi)];
+            const double Bm = P.Bm[slot], Bd = P.Bd[slot];
+            double TD = jl_mulb(jl_mulb(jl_mulb((T - p.Topt) * p.f_T2B * (Bm - Bd), jl_isless(p.Topt, T)),
+                                        jl_isless(Bd, Bm)), p.thermal == 1.0);
+            TD = jl_max(0.0, jl_min(TD, (Bm - Bd) / dT));
+            P.Bd[slot] = Bd + (TD - 0.0) * dT;           // RP = PS·γ = 0 (PS carries ac)
         }
         return;
     }
