@@ -866,14 +866,33 @@ __device__ __forceinline__ bool near_threshold(float r, float t) {
     return fabsf(r - t) <= F32_GUARD_REL * fabsf(t);
 }
 
-// flags, status, cell and logical slot of a slot, loaded one slot ahead of its physiology
-// and, for an active slot, its quotas and age (so only the environment gather waits in phys_one)
-struct PHead { int32_t code, ls; uint8_t fl, stt; float Bm, Cq, Nq, Pq, Chl, age; };
-__device__ __forceinline__ PHead phys_head(const IndDev32& P, long long g, bool valid) {
-    PHead h{-1, 0, 0, 0, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+// flags, status, cell and logical slot of a slot, loaded one slot ahead of its physiology, and,
+// for an active slot, its quotas and age and, when it was binned this step into an interior cell
+// (not a stale cell), the environment record of that cell: phys_one then waits on no load.
+struct PHead {
+    int32_t code, ls;
+    uint8_t fl, stt;
+    int env;                    // e0, e1 hold the environment record
+    float Bm, Cq, Nq, Pq, Chl, age;
+    float4 e0, e1;
+};
+__device__ __forceinline__ PHead phys_head(const IndDev32& P, long long g, bool valid, const MemberDev& m,
+                                           const float4* __restrict__ envr) {
+    PHead h{-1, 0, 0, 0, 0, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, {}, {}};
     if (valid) {
         h.fl = P.flags[g]; h.stt = P.stat[g]; h.code = P.cell[g]; h.ls = P.lslot[g];
-        if (h.fl & F32_AC) { h.Bm = P.Bm[g]; h.Cq = P.Cq[g]; h.Nq = P.Nq[g]; h.Pq = P.Pq[g]; h.Chl = P.Chl[g]; h.age = P.age[g]; }
+        if (h.fl & F32_AC) {
+            h.Bm = P.Bm[g]; h.Cq = P.Cq[g]; h.Nq = P.Nq[g]; h.Pq = P.Pq[g]; h.Chl = P.Chl[g]; h.age = P.age[g];
+            if ((h.stt & F32_ST_AC0) && !(h.stt & F32_ST_STALE)) {
+                int ci, cj, ck;
+                unpack_int(m, h.code, ci, cj, ck);
+                if (ci < m.Nx && cj < m.Ny && ck < m.Nz) {
+                    const long long cq = m.cell_off + q_of(m, ci, cj, ck);
+                    h.e0 = envr[2 * cq]; h.e1 = envr[2 * cq + 1];
+                    h.env = 1;
+                }
+            }
+        }
     }
     return h;
 }
@@ -893,16 +912,25 @@ __device__ __forceinline__ PhysOut phys_one(const PhysArgs& a, const MemberDev& 
     if (!(fl & F32_AC)) return out;
     const int ac0 = stt & F32_ST_AC0;
     int q;
-    if (stt & F32_ST_STALE) { int xi, yi, zi; unpack_halo(m, P.scell[g], xi, yi, zi); q = gid3(m, xi, yi, zi); }
-    else { int ci, cj, ck; unpack_int(m, code, ci, cj, ck); q = q_of(m, ci, cj, ck); }
+    bool inside;
+    if (stt & F32_ST_STALE) {
+        int xi, yi, zi;
+        unpack_halo(m, P.scell[g], xi, yi, zi);
+        q = gid3(m, xi, yi, zi);
+        inside = interior_q(m, q);
+    } else {
+        int ci, cj, ck;
+        unpack_int(m, code, ci, cj, ck);
+        q = q_of(m, ci, cj, ck);
+        inside = ci < m.Nx && cj < m.Ny && ck < m.Nz;
+    }
     const long long cq = m.cell_off + q;
     const long long G = a.Gtot;
     const SpeciesDev32& p = a.sp[mi * a.T.nsp + s];
     const float dT = a.dT;
     float NH4 = 0.0f, NO3 = 0.0f, PO4 = 0.0f, DOC = 0.0f, parv = 0.0f, Tm = 0.0f, popv = 0.0f;
-    const bool inside = interior_q(m, q);
     if (ac0 && inside) {
-        const float4 e0 = a.env[2 * cq], e1 = a.env[2 * cq + 1];
+        const float4 e0 = hd.env ? hd.e0 : a.env[2 * cq], e1 = hd.env ? hd.e1 : a.env[2 * cq + 1];
         NH4 = fmaxf(0.0f, e0.x); NO3 = fmaxf(0.0f, e0.y); PO4 = fmaxf(0.0f, e0.z); DOC = fmaxf(0.0f, e0.w);
         parv = e1.x; Tm = e1.y;
         popv = a.pop_sp ? (float)a.pop_sp[(long long)s * G + cq] : e1.z;
@@ -1037,10 +1065,10 @@ __global__ void __launch_bounds__(256, MINB) k32_physiology(PhysArgs a) {
         const MemberDev& m = a.T.md[mi];
         const long long base = m.slot_off + (long long)s * m.C;
         long long slot = (long long)tl.y + threadIdx.x;
-        PHead hd = phys_head(a.P, base + slot, slot < m.C);
+        PHead hd = phys_head(a.P, base + slot, slot < m.C, m, a.env);
         for (int p = 0; p < ppt; ++p, slot += bs) {
             const PHead cur = hd;
-            if (p + 1 < ppt) hd = phys_head(a.P, base + slot + bs, slot + bs < m.C);
+            if (p + 1 < ppt) hd = phys_head(a.P, base + slot + bs, slot + bs < m.C, m, a.env);
             PhysOut o{-1, {0ull, 0ull, 0ull, 0ull, 0ull}};
             if (slot < m.C) o = phys_one(a, m, mi, s, base + slot, iter, tnow, cur);
             scatter_phys(a, s, o);
