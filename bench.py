@@ -274,6 +274,9 @@ def run_fp32(members, args, dist, local, clocks_cls):
     prof = {}
     if args.profile_steps > 0:
         b.set_sort_interval(SORT_INTERVAL)          # the profiled steps include one sort
+        # each kernel timed on its own: the x-y tracer kernel in line with the particle kernels
+        # (results are the same either way)
+        b.set_option("xy_beside_particles", 0)
         b.profile_enable(True)
         b.step(dT, args.profile_steps)
         prof = b.profile_read()
