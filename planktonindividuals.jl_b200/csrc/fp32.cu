@@ -448,10 +448,7 @@ pi_status build_tables(pi_batch* b) {
     return PI_OK;
 }
 
-size_t xy_smem(int ty) {
-    const int f = ty == 28 ? XYSmem<28>::floats : ty == 16 ? XYSmem<16>::floats : ty == 8 ? XYSmem<8>::floats : XYSmem<4>::floats;
-    return (size_t)f * sizeof(float);
-}
+size_t xy_smem(int ty) { return (size_t)(3 * ty + 5) * PI_NTRACERS * 32 * sizeof(float); }
 
 float* velown(pi_batch* b, int m, int buf, int c) { return b->velown + ((long long)(buf * 3 + c)) * b->Gtot + b->mdh[m].cell_off; }
 

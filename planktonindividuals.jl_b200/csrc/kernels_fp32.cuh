@@ -1194,18 +1194,12 @@ struct TrArgs {
     const uint32_t* err;
 };
 
-// x and y sweeps of all 14 tracers on one level of a tile of 28 columns × TY rows. In the x sweep
-// warp w holds row j0-2+w (TY+4 rows: the y sweep reads two rows on each side, outside the domain
-// through the halo-fill map) and lane l column i0-2+l (28 cells and two halo columns on each side,
-// exchanged by shuffles), all 14 tracers per thread; it leaves the x-updated values (TA) and the
-// tracers of the rows the y sweep updates (TRs) in shared memory, and the warps of the y faces
-// leave each face's coefficients once for all tracers (FC, with the faces that carry no flux
-// marked in FZ) and each row's transport term (FTR). The y sweep then walks each tracer down the
-// columns (warp w: tracers w, w + TY + 4, ...; lane l: column i0-2+l) with the four rows a face
-// reads in registers, so each x-updated value is read once.
-// Shared memory: TA [row][tracer][lane], TRs [row][tracer][lane], FC [face][lane] (float4),
-// FTR [row][lane], FZ [face][lane], and with a land mask LMF [face][lane] (the four mask bits of a
-// face) and LMR [row][lane] (the mask of the row and the row above).
+// x and y sweeps of all 14 tracers on one level of a tile of 28 columns × TY rows. Warp w holds
+// row j0-2+w (TY+4 rows: the y sweep reads two rows on each side, outside the domain through the
+// halo-fill map), lane l column i0-2+l (28 cells and two halo columns on each side, exchanged by
+// shuffles). The face coefficients are computed once per face and shared by the 14 tracers.
+// Shared memory [row][tracer][lane]: TA (after x), FY (y face fluxes), TRs (tracer of the rows
+// the y sweep updates).
 // The inputs of one item for this thread (its row and column): u and the 14 tracers of the x
 // sweep, and the y velocities it reads later — v at its y face j0 + wid (x) and at the two faces
 // of its row (y, z; in range whenever the row is updated). A block loops over items and loads the
@@ -1232,27 +1226,12 @@ __device__ __forceinline__ void xy_load(const TrArgs& a, int item, float& u, flo
     vy.z = vv[qr + m.Gx];
 }
 
-template <int TY>
-struct XYSmem {
-    static constexpr int ta = 0;                                        // (TY+4) × 14 × 32 floats
-    static constexpr int trs = ta + (TY + 4) * PI_NTRACERS * 32;        // TY × 14 × 32 floats
-    static constexpr int fc = trs + TY * PI_NTRACERS * 32;              // (TY+1) × 32 float4
-    static constexpr int ftr = fc + (TY + 1) * 32 * 4;                  // TY × 32 floats
-    static constexpr int fz = ftr + TY * 32;                            // (TY+1) × 32 bytes, then LMF, LMR
-    static constexpr int floats = fz + ((TY + 1) * 32 * 2 + TY * 32 + 3) / 4;
-};
-
 template <int TY, bool LM>
 __device__ __forceinline__ void xy_tile(const TrArgs& a, const MemberDev& m, const int4 it, float* sm,
                                         float& pu, float* pv, float3& pvy, int next) {
-    using SM = XYSmem<TY>;
-    float* TA = sm + SM::ta;
-    float* TRs = sm + SM::trs;
-    float4* FC = reinterpret_cast<float4*>(sm + SM::fc);
-    float* FTR = sm + SM::ftr;
-    unsigned char* FZ = reinterpret_cast<unsigned char*>(sm + SM::fz);
-    unsigned char* LMF = FZ + (TY + 1) * 32;
-    unsigned char* LMR = LMF + (TY + 1) * 32;
+    float* TA = sm;                                        // (TY+4) × 14 × 32
+    float* FY = TA + (TY + 4) * PI_NTRACERS * 32;          // (TY+1) × 14 × 32
+    float* TRs = FY + (TY + 1) * PI_NTRACERS * 32;         // TY × 14 × 32
     auto at = [](float* base, int r, int n, int l) -> float& { return base[(r * PI_NTRACERS + n) * 32 + l]; };
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const long long G = a.Gtot;
@@ -1291,66 +1270,45 @@ __device__ __forceinline__ void xy_tile(const TrArgs& a, const MemberDev& m, con
             if (store_tr) at(TRs, wid - 2, n, lane) = v;
         }
     }
-    // ---- what the y sweep shares between tracers: face j0 + wid (wid <= TY) and row j0 + wid
-    // (wid < TY), from the y velocities loaded with this item
+    __syncthreads();
+    // the registers of this item's x inputs are free: start the next item's loads
+    const float3 vy = pvy;
+    if (next < a.nitems) xy_load(a, next, pu, pv, pvy);
+    // ---- y faces j0 + r, r = 0..TY
     const int i = i0 - 2 + lane;
     const bool col = lane >= 2 && lane < 30 && i <= m.Nx + m.Hx;
     const float ay = __fmul_rn(m.dx, dz);
-    const int ic = min(i, m.Gx);
     if (wid <= TY) {
-        const int f = j0 + wid;
+        const int r = wid, f = j0 + r;
         const bool special = f == m.Ny + m.Hy + 1;
         const bool zero = !col || f > m.Ny + m.Hy + 1 || (special && m.ty != PI_PERIODIC);
         const int fs = special ? m.Hy + 1 : min(f, m.Ny + m.Hy);
-        const FCu fc = fcu(zero ? 0.0f : pvy.x, ay, __frcp_rn(m.dy), dT);
-        FC[wid * 32 + lane] = make_float4(fc.tr, fc.d0c, fc.d1c, fc.R);
-        FZ[wid * 32 + lane] = zero ? 1 : 0;
+        const int ic = min(i, m.Gx);
+        const FCu fc = fcu(zero ? 0.0f : vy.x, ay, __frcp_rn(m.dy), dT);
+        int L2 = 1, L1 = 1, L0 = 1, Lp = 1;
         if (LM) {
-            const int L2 = lm32(m, a.lm, ic, fs - 2, L), L1 = lm32(m, a.lm, ic, fs - 1, L);
-            const int L0 = lm32(m, a.lm, ic, fs, L), Lp = lm32(m, a.lm, ic, fs + 1, L);
-            LMF[wid * 32 + lane] = (unsigned char)(L2 | (L1 << 1) | (L0 << 2) | (Lp << 3));
+            L2 = lm32(m, a.lm, ic, fs - 2, L); L1 = lm32(m, a.lm, ic, fs - 1, L);
+            L0 = lm32(m, a.lm, ic, fs, L); Lp = lm32(m, a.lm, ic, fs + 1, L);
         }
+#pragma unroll
+        for (int n = 0; n < PI_NTRACERS; ++n)
+            at(FY, r, n, lane) = zero ? 0.0f : flux_h<LM>(fc, at(TA, r, n, lane), at(TA, r + 1, n, lane), at(TA, r + 2, n, lane),
+                                                          at(TA, r + 3, n, lane), L2, L1, L0, Lp);
     }
+    __syncthreads();
+    // ---- y update of row j0 + wid
     if (wid < TY) {
         const int j = j0 + wid;
         if (col && j <= m.Ny + m.Hy) {
+            const int q = gid3(m, i, j, L);
             const int c0m = LM ? lm32(m, a.lm, i, j, L) : 1, cpm = LM ? lm32(m, a.lm, i, j + 1, L) : 1;
-            FTR[wid * 32 + lane] = mk<LM>(tdiff(ay, pvy.z, pvy.y), cpm, c0m);
-            if (LM) LMR[wid * 32 + lane] = (unsigned char)(c0m | (cpm << 1));
-        }
-    }
-    __syncthreads();
-    // the registers of this item's inputs are free: start the next item's loads
-    if (next < a.nitems) xy_load(a, next, pu, pv, pvy);
-    // ---- y sweep: each tracer walks the rows of its column
-    float* dstc = a.tb + off;
-    for (int n = wid; n < PI_NTRACERS; n += TY + 4) {
-        float c0 = at(TA, 0, n, lane), c1 = at(TA, 1, n, lane), c2 = at(TA, 2, n, lane);
-        float Fprev = 0.0f;
-#pragma unroll 4
-        for (int f = 0; f <= TY; ++f) {
-            const float c3 = at(TA, f + 3, n, lane);
-            float F = 0.0f;
-            if (!FZ[f * 32 + lane]) {
-                const float4 q = FC[f * 32 + lane];
-                FCu fc;
-                fc.tr = q.x; fc.d0c = q.y; fc.d1c = q.z; fc.R = q.w;
-                int L2 = 1, L1 = 1, L0 = 1, Lp = 1;
-                if (LM) { const int b = LMF[f * 32 + lane]; L2 = b & 1; L1 = (b >> 1) & 1; L0 = (b >> 2) & 1; Lp = (b >> 3) & 1; }
-                F = flux_h<LM>(fc, c0, c1, c2, c3, L2, L1, L0, Lp);
+            const float ftr = mk<LM>(tdiff(ay, vy.z, vy.y), cpm, c0m);
+            float* dst = a.tb + off + q;
+#pragma unroll
+            for (int n = 0; n < PI_NTRACERS; ++n) {
+                const float dG = mk<LM>(__fsub_rn(at(FY, wid + 1, n, lane), at(FY, wid, n, lane)), cpm, c0m);
+                dst[n * G] = upd_sweep(at(TA, wid + 2, n, lane), dtv, dG, at(TRs, wid, n, lane), ftr);
             }
-            if (f > 0) {
-                // row j0 + f - 1: faces f - 1 and f, x-updated value c1 (row f + 1 of TA)
-                const int r = f - 1, j = j0 + r;
-                if (col && j <= m.Ny + m.Hy) {
-                    int c0m = 1, cpm = 1;
-                    if (LM) { const int b = LMR[r * 32 + lane]; c0m = b & 1; cpm = (b >> 1) & 1; }
-                    const float dG = mk<LM>(__fsub_rn(F, Fprev), cpm, c0m);
-                    dstc[(long long)n * G + gid3(m, i, j, L)] = upd_sweep(c1, dtv, dG, at(TRs, r, n, lane), FTR[r * 32 + lane]);
-                }
-            }
-            Fprev = F;
-            c0 = c1; c1 = c2; c2 = c3;
         }
     }
     __syncthreads();
@@ -1359,7 +1317,7 @@ __device__ __forceinline__ void xy_tile(const TrArgs& a, const MemberDev& m, con
 template <int TY>
 __global__ void __launch_bounds__(32 * (TY + 4)) k32_xy(TrArgs a) {
     if (stopped(a.err)) return;
-    extern __shared__ __align__(16) float sm[];
+    extern __shared__ float sm[];
     if ((int)blockIdx.x >= a.nitems) return;
     float pu, pv[PI_NTRACERS];
     float3 pvy;
