@@ -96,6 +96,13 @@ __device__ __forceinline__ void move(Ax1& a, float d, int N, int topo) {
     if (a.o >= 1.0f) { a.c += 1; a.o = 0.0f; }
     bc_axis(a, N, topo);
 }
+// move() to an RK stage position, which is only sampled: a position left outside [0, N] by a
+// displacement above one domain length (CFL far above 1) is noted in `bad` and held at the edge,
+// so every corner index of the interpolation stays inside the halo-padded grid (H >= 2)
+__device__ __forceinline__ void move_stage(Ax1& a, float d, int N, int topo, bool& bad) {
+    move(a, d, N, topo);
+    if (a.c < 0 || a.c > N) { bad = true; a.c = a.c < 0 ? 0 : N; a.o = 0.0f; }
+}
 
 // index and weight along one axis for a face-centred (own axis) or cell-centred field
 // (interpolation.jl:3-83: x + 1 or x + 0.5 split into trunc and mod)
@@ -112,11 +119,14 @@ __device__ __forceinline__ int clampb(int v, int lo, int hi, bool& bad) {
     return c;
 }
 
-// The 8 corner values of one velocity component around a position. The four RK stages of a step
-// sample points a small fraction of a cell apart, usually from the same field (vel₀ = vel½ = vel₁
-// between velocity refreshes), so a stage reuses the corners of the previous one when the field
-// and the base corner are the same: the values are identical, only the loads are saved.
-struct Corners { int fid; int q; float v[8]; };   // fid: which of the step's fields (0 vel₀, 1 vel½, 2 vel₁)
+// One velocity component around a position, as the coefficients of its trilinear interpolant in
+// grid cells per second: v(xd, yd, zd) = c0 + xd·cx + yd·cy + zd·cz + xd·yd·cxy + xd·zd·cxz +
+// yd·zd·cyz + xd·yd·zd·cxyz, formed from the 8 corner values (each divided by its ΔxC, ΔyC or ΔzC,
+// interpolation.jl:23-50) when they are loaded. The four RK stages of a step sample points a small
+// fraction of a cell apart, usually from the same field (vel₀ = vel½ = vel₁ between velocity
+// refreshes), so a stage reuses the coefficients of the previous one when the field and the base
+// corner are the same: only the loads and the setup are saved.
+struct Corners { int fid; int q; float c0, cx, cy, cz, cxy, cxz, cyz, cxyz; };   // fid: 0 vel₀, 1 vel½, 2 vel₁
 
 // Member constants of the particle kernels, held in registers.
 struct PGeom {
@@ -142,30 +152,41 @@ __device__ __forceinline__ PGeom pgeom(const MemberDev& m, const MemberForcing& 
 // The 8 corner values come from the component's own halo-padded field: in the cell-sorted
 // storage order the lanes of a warp sit in neighbouring cells, so the corner loads of a warp
 // share sectors and the fields (12 bytes per cell) stay in L2.
+// Every position passed here lies in [0, N] on each axis (uploads are validated, stored positions
+// are clamped, stage positions pass through move_stage), so with H >= 2 the base corner (i, j, k)
+// satisfies 1 <= i <= Gx - 1 (likewise j, k) and needs no clamp.
 template <int COMP>
 __device__ __forceinline__ float itpl32(const PGeom& m, const float* __restrict__ fld, int fid,
                                         const float* __restrict__ rdzC, const Ax1& X, const Ax1& Y,
-                                        const Ax1& Z, bool& bad, Corners& cc) {
+                                        const Ax1& Z, Corners& cc) {
     int i, j, k;
     float xd, yd, zd;
     axis_iw(X, m.Hx, COMP == 0, i, xd);
     axis_iw(Y, m.Hy, COMP == 1, j, yd);
     axis_iw(Z, m.Hz, COMP == 2, k, zd);
-    i = clampb(i, 1, m.Gx - 1, bad); j = clampb(j, 1, m.Gy - 1, bad); k = clampb(k, 1, m.Gz - 1, bad);
     const int q = (i - 1) + m.Gx * ((j - 1) + m.Gy * (k - 1));
     if (cc.fid != fid || cc.q != q) {
         const float* __restrict__ p = fld + q;                 // (i, j, k); level k+1 one slab on
         const int sy = m.Gx, sz = m.Gx * m.Gy;
         cc.fid = fid; cc.q = q;
-        cc.v[0] = __ldg(p); cc.v[1] = __ldg(p + sy); cc.v[2] = __ldg(p + 1); cc.v[3] = __ldg(p + 1 + sy);
-        cc.v[4] = __ldg(p + sz); cc.v[5] = __ldg(p + sz + sy); cc.v[6] = __ldg(p + sz + 1); cc.v[7] = __ldg(p + sz + 1 + sy);
+        // corners v_abc at (i + a, j + b, k + c), in cells per second
+        float s0 = m.rdx, s1 = m.rdx;
+        if (COMP == 1) { s0 = m.rdy; s1 = m.rdy; }
+        if (COMP == 2) { s0 = __ldg(rdzC + m.dz_off + k - 1); s1 = __ldg(rdzC + m.dz_off + k); }
+        const float v000 = __ldg(p) * s0, v010 = __ldg(p + sy) * s0, v100 = __ldg(p + 1) * s0, v110 = __ldg(p + 1 + sy) * s0;
+        const float v001 = __ldg(p + sz) * s1, v011 = __ldg(p + sz + sy) * s1, v101 = __ldg(p + sz + 1) * s1,
+                    v111 = __ldg(p + sz + 1 + sy) * s1;
+        cc.c0 = v000;
+        cc.cx = v100 - v000; cc.cy = v010 - v000; cc.cz = v001 - v000;
+        cc.cxy = (v110 - v100) - (v010 - v000);
+        cc.cxz = (v101 - v100) - (v001 - v000);
+        cc.cyz = (v011 - v010) - (v001 - v000);
+        cc.cxyz = ((v111 - v110) - (v101 - v100)) - ((v011 - v010) - (v001 - v000));
     }
-    const float a0 = (1.0f - xd) * (1.0f - yd), a1 = (1.0f - xd) * yd, a2 = xd * (1.0f - yd), a3 = xd * yd;
-    const float lo = a0 * cc.v[0] + a1 * cc.v[1] + a2 * cc.v[2] + a3 * cc.v[3];
-    const float hi = a0 * cc.v[4] + a1 * cc.v[5] + a2 * cc.v[6] + a3 * cc.v[7];
-    if (COMP == 0) return ((1.0f - zd) * lo + zd * hi) * m.rdx;
-    if (COMP == 1) return ((1.0f - zd) * lo + zd * hi) * m.rdy;
-    return (1.0f - zd) * lo * __ldg(rdzC + m.dz_off + k - 1) + zd * hi * __ldg(rdzC + m.dz_off + k);
+    const float ty = fmaf(zd, cc.cxyz, cc.cxy);
+    const float tx = fmaf(zd, cc.cxz, fmaf(yd, ty, cc.cx));
+    const float tz = fmaf(zd, cc.cyz, cc.cy);
+    return fmaf(zd, cc.cz, fmaf(yd, tz, fmaf(xd, tx, cc.c0)));
 }
 
 // the draws of the FP64 form (same keys, same numbers; lattice values are exact in float)
@@ -363,26 +384,26 @@ __device__ __forceinline__ MoveOut move_one(const MoveArgs& a, const MemberDev& 
     const Ax1 X0{ci, ox}, Y0{cj, oy}, Z0{ck, oz};
     const float dT = a.dT, hdT = 0.5f * dT;
     const float* __restrict__ rdzC = a.rdzC;
-    Corners cu{-1, -1, {}}, cv{-1, -1, {}}, cw{-1, -1, {}};
+    Corners cu{-1, -1}, cv{-1, -1}, cw{-1, -1};
     const int fh = pg.fh, f1 = pg.f1;
-    float u1 = itpl32<0>(pg, f.vel0[0], 0, rdzC, X0, Y0, Z0, bad, cu);
-    float v1 = itpl32<1>(pg, f.vel0[1], 0, rdzC, X0, Y0, Z0, bad, cv);
-    float w1 = itpl32<2>(pg, f.vel0[2], 0, rdzC, X0, Y0, Z0, bad, cw);
+    float u1 = itpl32<0>(pg, f.vel0[0], 0, rdzC, X0, Y0, Z0, cu);
+    float v1 = itpl32<1>(pg, f.vel0[1], 0, rdzC, X0, Y0, Z0, cv);
+    float w1 = itpl32<2>(pg, f.vel0[2], 0, rdzC, X0, Y0, Z0, cw);
     float u2 = u1, v2 = v1, w2 = w1;
     Ax1 X = X0, Y = Y0, Z = Z0;
-    move(X, u1 * hdT, pg.Nx, pg.tx); move(Y, v1 * hdT, pg.Ny, pg.ty); move(Z, -(w1 * hdT), pg.Nz, pg.tz);
-    u1 = itpl32<0>(pg, f.velh[0], fh, rdzC, X, Y, Z, bad, cu); v1 = itpl32<1>(pg, f.velh[1], fh, rdzC, X, Y, Z, bad, cv);
-    w1 = itpl32<2>(pg, f.velh[2], fh, rdzC, X, Y, Z, bad, cw);
+    move_stage(X, u1 * hdT, pg.Nx, pg.tx, bad); move_stage(Y, v1 * hdT, pg.Ny, pg.ty, bad); move_stage(Z, -(w1 * hdT), pg.Nz, pg.tz, bad);
+    u1 = itpl32<0>(pg, f.velh[0], fh, rdzC, X, Y, Z, cu); v1 = itpl32<1>(pg, f.velh[1], fh, rdzC, X, Y, Z, cv);
+    w1 = itpl32<2>(pg, f.velh[2], fh, rdzC, X, Y, Z, cw);
     u2 += u1 * 2.0f; v2 += v1 * 2.0f; w2 += w1 * 2.0f;
     X = X0; Y = Y0; Z = Z0;
-    move(X, u1 * hdT, pg.Nx, pg.tx); move(Y, v1 * hdT, pg.Ny, pg.ty); move(Z, -(w1 * hdT), pg.Nz, pg.tz);
-    u1 = itpl32<0>(pg, f.velh[0], fh, rdzC, X, Y, Z, bad, cu); v1 = itpl32<1>(pg, f.velh[1], fh, rdzC, X, Y, Z, bad, cv);
-    w1 = itpl32<2>(pg, f.velh[2], fh, rdzC, X, Y, Z, bad, cw);
+    move_stage(X, u1 * hdT, pg.Nx, pg.tx, bad); move_stage(Y, v1 * hdT, pg.Ny, pg.ty, bad); move_stage(Z, -(w1 * hdT), pg.Nz, pg.tz, bad);
+    u1 = itpl32<0>(pg, f.velh[0], fh, rdzC, X, Y, Z, cu); v1 = itpl32<1>(pg, f.velh[1], fh, rdzC, X, Y, Z, cv);
+    w1 = itpl32<2>(pg, f.velh[2], fh, rdzC, X, Y, Z, cw);
     u2 += u1 * 2.0f; v2 += v1 * 2.0f; w2 += w1 * 2.0f;
     X = X0; Y = Y0; Z = Z0;
-    move(X, u1 * dT, pg.Nx, pg.tx); move(Y, v1 * dT, pg.Ny, pg.ty); move(Z, -(w1 * dT), pg.Nz, pg.tz);
-    u1 = itpl32<0>(pg, f.vel1[0], f1, rdzC, X, Y, Z, bad, cu); v1 = itpl32<1>(pg, f.vel1[1], f1, rdzC, X, Y, Z, bad, cv);
-    w1 = itpl32<2>(pg, f.vel1[2], f1, rdzC, X, Y, Z, bad, cw);
+    move_stage(X, u1 * dT, pg.Nx, pg.tx, bad); move_stage(Y, v1 * dT, pg.Ny, pg.ty, bad); move_stage(Z, -(w1 * dT), pg.Nz, pg.tz, bad);
+    u1 = itpl32<0>(pg, f.vel1[0], f1, rdzC, X, Y, Z, cu); v1 = itpl32<1>(pg, f.vel1[1], f1, rdzC, X, Y, Z, cv);
+    w1 = itpl32<2>(pg, f.vel1[2], f1, rdzC, X, Y, Z, cw);
     const float sixth = 1.0f / 6.0f;
     u2 = (u2 + u1) * sixth; v2 = (v2 + v1) * sixth; w2 = (w2 + w1) * sixth;
     X = X0; Y = Y0; Z = Z0;
@@ -445,6 +466,7 @@ __device__ __forceinline__ MoveOut move_one(const MoveArgs& a, const MemberDev& 
 
 // k32_move's grid sums of one warp (segment s of one member): one atomic per run of a cell
 __device__ __forceinline__ void scatter_move(const MoveArgs& a, int s, const MoveOut& o) {
+    if (__all_sync(0xffffffffu, o.cq < 0)) return;      // a warp of inactive slots adds nothing
     const WarpRuns R = warp_runs(o.cq);
     const uint32_t c = run_sum(o.cnt, R);
     const unsigned long long chl = run_sum(o.chl, R);
@@ -876,11 +898,19 @@ struct PHead {
     float Bm, Cq, Nq, Pq, Chl, age;
     float4 e0, e1;
 };
-__device__ __forceinline__ PHead phys_head(const IndDev32& P, long long g, bool valid, const MemberDev& m,
+// The first level of a slot's loads (flags, status, cell, logical slot): the loads of phys_head
+// depend on them, so k32_physiology issues these two slots ahead and phys_head one slot ahead.
+struct PPre { int32_t code, ls; uint8_t fl, stt; };
+__device__ __forceinline__ PPre phys_pre(const IndDev32& P, long long g, bool valid) {
+    PPre r{-1, 0, 0, 0};
+    if (valid) { r.fl = P.flags[g]; r.stt = P.stat[g]; r.code = P.cell[g]; r.ls = P.lslot[g]; }
+    return r;
+}
+__device__ __forceinline__ PHead phys_head(const IndDev32& P, long long g, const PPre& pre, const MemberDev& m,
                                            const float4* __restrict__ envr) {
     PHead h{-1, 0, 0, 0, 0, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, {}, {}};
-    if (valid) {
-        h.fl = P.flags[g]; h.stt = P.stat[g]; h.code = P.cell[g]; h.ls = P.lslot[g];
+    {
+        h.fl = pre.fl; h.stt = pre.stt; h.code = pre.code; h.ls = pre.ls;
         if (h.fl & F32_AC) {
             h.Bm = P.Bm[g]; h.Cq = P.Cq[g]; h.Nq = P.Nq[g]; h.Pq = P.Pq[g]; h.Chl = P.Chl[g]; h.age = P.age[g];
             if ((h.stt & F32_ST_AC0) && !(h.stt & F32_ST_STALE)) {
@@ -1037,6 +1067,7 @@ __device__ __forceinline__ PhysOut phys_one(const PhysArgs& a, const MemberDev& 
 
 // k32_physiology's grid sums of one warp (segment s of one member): one atomic per run of a cell
 __device__ __forceinline__ void scatter_phys(const PhysArgs& a, int s, const PhysOut& o) {
+    if (__all_sync(0xffffffffu, o.cq < 0)) return;      // a warp of inactive slots adds nothing
     const WarpRuns R = warp_runs(o.cq);
     const int n = (int)run_sum(o.cq >= 0 ? 1u : 0u, R);
     unsigned long long v[5];
@@ -1065,10 +1096,14 @@ __global__ void __launch_bounds__(256, MINB) k32_physiology(PhysArgs a) {
         const MemberDev& m = a.T.md[mi];
         const long long base = m.slot_off + (long long)s * m.C;
         long long slot = (long long)tl.y + threadIdx.x;
-        PHead hd = phys_head(a.P, base + slot, slot < m.C, m, a.env);
+        PHead hd = phys_head(a.P, base + slot, phys_pre(a.P, base + slot, slot < m.C), m, a.env);
+        PPre pre = phys_pre(a.P, base + slot + bs, 1 < ppt && slot + bs < m.C);
         for (int p = 0; p < ppt; ++p, slot += bs) {
             const PHead cur = hd;
-            if (p + 1 < ppt) hd = phys_head(a.P, base + slot + bs, slot + bs < m.C, m, a.env);
+            if (p + 1 < ppt) {
+                hd = phys_head(a.P, base + slot + bs, pre, m, a.env);
+                pre = phys_pre(a.P, base + slot + 2 * bs, p + 2 < ppt && slot + 2 * bs < m.C);
+            }
             PhysOut o{-1, {0ull, 0ull, 0ull, 0ull, 0ull}};
             if (slot < m.C) o = phys_one(a, m, mi, s, base + slot, iter, tnow, cur);
             scatter_phys(a, s, o);
