@@ -75,17 +75,33 @@ enum { PI_PROC_PS = 0, PI_PROC_BS, PI_PROC_VDOC, PI_PROC_VNH4, PI_PROC_VNO3, PI_
 enum { PI_CPROC_PS = 0, PI_CPROC_BS, PI_CPROC_RP, PI_CPROC_RS, PI_CPROC_TD, PI_CPROC_Bm, PI_CPROC_Bd,
        PI_CPROC_Chl, PI_NCPROC };
 
-/* RectilinearGrid (src/Grids/rectilinear_grid.jl:1-25). Metrics are passed as the reference
- * stores them after construction (rectilinear_grid.jl:57-122), halos included. */
+/* The horizontal metrics of a LatLonGrid (src/Grids/lat_lon_grid.jl:1-45, built by
+ * LatLonGrid :57-170 or LoadLatLonGrid :196-316), as the reference stores them: halos included,
+ * Julia column-major. ΔxC, ΔyC, ΔxF, ΔyF, Ax, Ay, Az and volume read these arrays
+ * (Grids/areas_volumes_spacings.jl:27-38) where a RectilinearGrid uses Δx, Δy and dzF. */
+typedef struct {
+    const double *dxC, *dyC;    /* (Nx+2Hx)(Ny+2Hy): center-to-center spacings, m          */
+    const double *dxF, *dyF;    /* (Nx+2Hx)(Ny+2Hy): face-to-face spacings, m              */
+    const double *Az;           /* (Nx+2Hx)(Ny+2Hy): area of a horizontal face, m²          */
+    const double *Ax, *Ay;      /* (Nx+2Hx)(Ny+2Hy)(Nz+2Hz): areas of the x and y faces, m² */
+    const double *Vol;          /* (Nx+2Hx)(Ny+2Hy)(Nz+2Hz): cell volumes, m³               */
+} pi_grid_metrics;
+
+/* RectilinearGrid (src/Grids/rectilinear_grid.jl:1-25) or, with `metrics`, LatLonGrid
+ * (src/Grids/lat_lon_grid.jl:1-45). Metrics are passed as the reference stores them after
+ * construction (rectilinear_grid.jl:57-122), halos included. */
 typedef struct {
     int32_t Nx, Ny, Nz;
     int32_t Hx, Hy, Hz;
     int32_t topo[3];            /* PI_PERIODIC or PI_BOUNDED for x, y, z                   */
-    double  dx, dy;             /* Δx, Δy                                                  */
+    double  dx, dy;             /* Δx, Δy (RectilinearGrid; unused with metrics)           */
     const double*  dzF;         /* Nz+2Hz, g.dzF                                           */
     const double*  dzC;         /* Nz+2Hz, g.dzC                                           */
     const uint8_t* landmask;    /* (Nx+2Hx)(Ny+2Hy)(Nz+2Hz) with halos (Grids/utils.jl:92-129),
                                    NULL = all water                                        */
+    const pi_grid_metrics* metrics;   /* NULL: RectilinearGrid. Otherwise the LatLonGrid
+                                         arrays (FP64 form only; the FP32 form and
+                                         pi_tracer_advection_noalloc return PI_ERR_ARG) */
 } pi_grid;
 
 /* Biogeochemical parameters, names and meaning of bgc_params_default

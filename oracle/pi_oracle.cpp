@@ -71,10 +71,19 @@ struct Grid {
     }
     inline double dzF1(long k) const { return dzF[k - 1]; }
     inline double dzC1(long k) const { return dzC[k - 1]; }
-    inline double vol(long k) const { return dx * dy * dzF1(k); }      /* volume = Δx*Δy*dzF[k] */
-    inline double Axk(long k) const { return dy * dzF1(k); }           /* Ax = Δy*dzF[k] */
-    inline double Ayk(long k) const { return dx * dzF1(k); }           /* Ay = Δx*dzF[k] */
-    inline double Az() const { return dx * dy; }                        /* Az = Δx*Δy     */
+    /* LatLonGrid (lat_lon_grid.jl:1-45): the stored arrays; empty for a RectilinearGrid */
+    bool ll = false;
+    dvec mdxC, mdyC, mdxF, mdyF, mAz, mAx, mAy, mVol;
+    inline size_t id2(long i, long j) const { return (size_t)(i - 1) + (size_t)Gx * (size_t)(j - 1); }
+    /* Grids/areas_volumes_spacings.jl:9-38, 1-based halo-inclusive indices */
+    inline double dxC(long i, long j) const { return ll ? mdxC[id2(i, j)] : dx; }
+    inline double dyC(long i, long j) const { return ll ? mdyC[id2(i, j)] : dy; }
+    inline double dxF(long i, long j) const { return ll ? mdxF[id2(i, j)] : dx; }
+    inline double dyF(long i, long j) const { return ll ? mdyF[id2(i, j)] : dy; }
+    inline double vol(long i, long j, long k) const { return ll ? mVol[id(i, j, k)] : dx * dy * dzF1(k); }  /* Δx*Δy*dzF[k] */
+    inline double Axk(long i, long j, long k) const { return ll ? mAx[id(i, j, k)] : dy * dzF1(k); }      /* Δy*dzF[k] */
+    inline double Ayk(long i, long j, long k) const { return ll ? mAy[id(i, j, k)] : dx * dzF1(k); }      /* Δx*dzF[k] */
+    inline double Az(long i, long j) const { return ll ? mAz[id2(i, j)] : dx * dy; }                      /* Δx*Δy */
     inline int L(long i, long j, long k) const { return lm[id(i, j, k)]; }
 };
 
@@ -238,18 +247,18 @@ double itpl(orc_model* m, const dvec& f, int comp, double x, double y, double z,
     double w101 = xd * (1.0 - yd) * zd;
     double w110 = xd * yd * (1.0 - zd);
     double w111 = xd * yd * zd;
-    double d0, d1;   /* ΔxC / ΔyC are constant; ΔzC depends on the corner's k */
-    if (comp == 0) { d0 = g.dx; d1 = g.dx; }
-    else if (comp == 1) { d0 = g.dy; d1 = g.dy; }
-    else { d0 = g.dzC1(k); d1 = g.dzC1(k + 1); }
-    return w000 * f[g.id(i, j, k)] / d0
-         + w001 * f[g.id(i, j, k + 1)] / d1
-         + w010 * f[g.id(i, j + 1, k)] / d0
-         + w011 * f[g.id(i, j + 1, k + 1)] / d1
-         + w100 * f[g.id(i + 1, j, k)] / d0
-         + w101 * f[g.id(i + 1, j, k + 1)] / d1
-         + w110 * f[g.id(i + 1, j + 1, k)] / d0
-         + w111 * f[g.id(i + 1, j + 1, k + 1)] / d1;
+    /* each corner is divided by ΔxC, ΔyC or ΔzC at that corner (interpolation.jl:23-50) */
+    auto D = [&](long a, long b, long c) -> double {
+        return comp == 0 ? g.dxC(i + a, j + b) : comp == 1 ? g.dyC(i + a, j + b) : g.dzC1(k + c);
+    };
+    return w000 * f[g.id(i, j, k)] / D(0, 0, 0)
+         + w001 * f[g.id(i, j, k + 1)] / D(0, 0, 1)
+         + w010 * f[g.id(i, j + 1, k)] / D(0, 1, 0)
+         + w011 * f[g.id(i, j + 1, k + 1)] / D(0, 1, 1)
+         + w100 * f[g.id(i + 1, j, k)] / D(1, 0, 0)
+         + w101 * f[g.id(i + 1, j, k + 1)] / D(1, 0, 1)
+         + w110 * f[g.id(i + 1, j + 1, k)] / D(1, 1, 0)
+         + w111 * f[g.id(i + 1, j + 1, k + 1)] / D(1, 1, 1);
 }
 
 /* vel_interpolate_kernel!, particle_advection_kernels.jl:26-31 */
@@ -343,8 +352,12 @@ void particle_diffusion(orc_model* m, Species& s, int spi, double dT) {
     #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < C; ++i) {   /* calc_diffusion_kernel!, :2-8; ΔzC at zi+Hz of the stored zi */
         long kk = clampi(m, (long)s.zi[i] + g.Hz, 1, g.Gz);
-        m->rx[i] = m->rx[i] * sqrt(kx * dT) / g.dx;
-        m->ry[i] = m->ry[i] * sqrt(ky * dT) / g.dy;
+        /* ΔxC/ΔyC at (xi+Hx, yi+Hy) of the stored indices; the reference reads past the array
+           there when x = Nx exactly, which is held at the last column here */
+        long ii = std::min<long>(std::max<long>((long)s.xi[i] + g.Hx, 1), g.Gx);
+        long jj = std::min<long>(std::max<long>((long)s.yi[i] + g.Hy, 1), g.Gy);
+        m->rx[i] = m->rx[i] * sqrt(kx * dT) / g.dxC(ii, jj);
+        m->ry[i] = m->ry[i] * sqrt(ky * dT) / g.dyC(ii, jj);
         m->rz[i] = m->rz[i] * sqrt(kz * dT) / g.dzC1(kk);
     }
     for (int64_t i = 0; i < C; ++i) {
@@ -394,7 +407,7 @@ void calc_par(orc_model* m, int ki) {          /* utils.jl:55-63 */
             long ii = i + g.Hx, jj = j + g.Hy, kk = ki + g.Hz;
             size_t c = g.id(ii, jj, kk);
             size_t f = (size_t)(i - 1) + (size_t)g.Nx * (size_t)(j - 1);
-            double atten = (m->Chl[c] / g.vol(kk) * m->bgc.kc + m->bgc.kw) * g.dzF1(kk);
+            double atten = (m->Chl[c] / g.vol(ii, jj, kk) * m->bgc.kc + m->bgc.kw) * g.dzF1(kk);
             m->par[c] = m->PARF[f] * (1.0 - pi_exp(-atten)) / atten;
             m->PARF[f] = m->PARF[f] * pi_exp(-atten);
         }
@@ -839,8 +852,8 @@ inline double psi_lim(double cfl, double th) {
 /* adv_flux_x/y/z, DST3FL.jl:63-73 */
 double adv_flux_x(const Grid& g, const Ops& o, long i, long j, long k, const dvec& u, const dvec& c, double dT) {
     double uu = u[g.id(i, j, k)];
-    double cfl = fabs(uu * dT / g.dx);
-    double tr = g.Axk(k) * uu;
+    double cfl = fabs(uu * dT / g.dxC(i, j));
+    double tr = g.Axk(i, j, k) * uu;
     double d0 = o.dx0(c, i, j, k);
     double psp = psi_lim(cfl, theta(o.dxm(c, i, j, k), d0));
     double psm = psi_lim(cfl, theta(o.dxp(c, i, j, k), d0));
@@ -849,8 +862,8 @@ double adv_flux_x(const Grid& g, const Ops& o, long i, long j, long k, const dve
 }
 double adv_flux_y(const Grid& g, const Ops& o, long i, long j, long k, const dvec& v, const dvec& c, double dT) {
     double vv = v[g.id(i, j, k)];
-    double cfl = fabs(vv * dT / g.dy);
-    double tr = g.Ayk(k) * vv;
+    double cfl = fabs(vv * dT / g.dyC(i, j));
+    double tr = g.Ayk(i, j, k) * vv;
     double d0 = o.dy0(c, i, j, k);
     double psp = psi_lim(cfl, theta(o.dym(c, i, j, k), d0));
     double psm = psi_lim(cfl, theta(o.dyp(c, i, j, k), d0));
@@ -860,7 +873,7 @@ double adv_flux_y(const Grid& g, const Ops& o, long i, long j, long k, const dve
 double adv_flux_z(const Grid& g, const Ops& o, long i, long j, long k, const dvec& w, const dvec& c, double dT) {
     double ww = w[g.id(i, j, k)];
     double cfl = fabs(ww * dT / g.dzC1(k));
-    double tr = g.Az() * ww;
+    double tr = g.Az(i, j) * ww;
     double d0 = o.dz0(c, i, j, k);
     double psp = psi_lim(cfl, theta(o.dzm(c, i, j, k), d0));   /* Ψz⁺ uses θz⁺ = δz⁻/δz⁰ */
     double psm = psi_lim(cfl, theta(o.dzp(c, i, j, k), d0));   /* Ψz⁻ uses θz⁻ = δz⁺/δz⁰ */
@@ -900,15 +913,15 @@ void tracer_advection(orc_model* m, double dT) {
                         double dG;
                         if (dir == 0) {
                             dG = o.dxp(Gc, i, j, k);
-                            ftr = jl_mulb(jl_mulb(g.Axk(k) * vel[g.id(i + 1, j, k)] - g.Axk(k) * vel[q], g.L(i + 1, j, k)), g.L(i, j, k));
+                            ftr = jl_mulb(jl_mulb(g.Axk(i + 1, j, k) * vel[g.id(i + 1, j, k)] - g.Axk(i, j, k) * vel[q], g.L(i + 1, j, k)), g.L(i, j, k));
                         } else if (dir == 1) {
                             dG = o.dyp(Gc, i, j, k);
-                            ftr = jl_mulb(jl_mulb(g.Ayk(k) * vel[g.id(i, j + 1, k)] - g.Ayk(k) * vel[q], g.L(i, j + 1, k)), g.L(i, j, k));
+                            ftr = jl_mulb(jl_mulb(g.Ayk(i, j + 1, k) * vel[g.id(i, j + 1, k)] - g.Ayk(i, j, k) * vel[q], g.L(i, j + 1, k)), g.L(i, j, k));
                         } else {
                             dG = o.dzp(Gc, i, j, k);
-                            ftr = jl_mulb(jl_mulb(g.Az() * vel[q] - g.Az() * vel[g.id(i, j, k + 1)], g.L(i, j, k + 1)), g.L(i, j, k));
+                            ftr = jl_mulb(jl_mulb(g.Az(i, j) * vel[q] - g.Az(i, j) * vel[g.id(i, j, k + 1)], g.L(i, j, k + 1)), g.L(i, j, k));
                         }
-                        ct[q] -= dT / g.vol(k) * (dG - c[q] * ftr);
+                        ct[q] -= dT / g.vol(i, j, k) * (dG - c[q] * ftr);
                     }
         }
         for (int n = 0; n < PI_NTRACERS; ++n) fill_halo_tracer(g, m->tt[n]);
@@ -928,16 +941,16 @@ void tracer_diffusion(orc_model* m, double dT) {
     for (int n = 0; n < PI_NTRACERS; ++n) {
         const dvec& c = m->tr[n];
         dvec& Gc = m->Gcs[n];
-        auto fx = [&](long i, long j, long k) { return kx * g.Axk(k) * (o.dx0(c, i, j, k) / g.dx); };
-        auto fy = [&](long i, long j, long k) { return ky * g.Ayk(k) * (o.dy0(c, i, j, k) / g.dy); };
-        auto fz = [&](long i, long j, long k) { return kz * g.Az() * (o.dz0(c, i, j, k) / g.dzF1(k)); };
+        auto fx = [&](long i, long j, long k) { return kx * g.Axk(i, j, k) * (o.dx0(c, i, j, k) / g.dxF(i, j)); };
+        auto fy = [&](long i, long j, long k) { return ky * g.Ayk(i, j, k) * (o.dy0(c, i, j, k) / g.dyF(i, j)); };
+        auto fz = [&](long i, long j, long k) { return kz * g.Az(i, j) * (o.dz0(c, i, j, k) / g.dzF1(k)); };
         for (long k = g.Hz + 1; k <= g.Hz + g.Nz; ++k)
             for (long j = g.Hy + 1; j <= g.Hy + g.Ny; ++j)
                 for (long i = g.Hx + 1; i <= g.Hx + g.Nx; ++i) {
                     double ax = jl_mulb(jl_mulb(fx(i + 1, j, k) - fx(i, j, k), g.L(i + 1, j, k)), g.L(i, j, k));
                     double ay = jl_mulb(jl_mulb(fy(i, j + 1, k) - fy(i, j, k), g.L(i, j + 1, k)), g.L(i, j, k));
                     double az = jl_mulb(jl_mulb(fz(i, j, k) - fz(i, j, k + 1), g.L(i, j, k + 1)), g.L(i, j, k));
-                    double lap = 1.0 / g.vol(k) * (ax + ay + az);
+                    double lap = 1.0 / g.vol(i, j, k) * (ax + ay + az);
                     size_t q = g.id(i, j, k);
                     Gc[q] = Gc[q] + lap * dT;
                 }
@@ -1019,27 +1032,27 @@ void apply_bcs(orc_model* m, double dT) {
         const FluxBC* b = m->bc[n];
         if (b[PI_WEST].kind) for (long k = 1; k <= g.Nz; ++k) for (long j = 1; j <= g.Ny; ++j) {
             long jj = j + g.Hy, kk = k + g.Hz;
-            Gc[g.id(1 + g.Hx, jj, kk)] += getbc(b[PI_WEST], g.Ny, g.Nz, j, k, it) * dT * g.Axk(kk) / g.vol(kk);
+            Gc[g.id(1 + g.Hx, jj, kk)] += getbc(b[PI_WEST], g.Ny, g.Nz, j, k, it) * dT * g.Axk(1 + g.Hx, jj, kk) / g.vol(1 + g.Hx, jj, kk);
         }
         if (b[PI_EAST].kind) for (long k = 1; k <= g.Nz; ++k) for (long j = 1; j <= g.Ny; ++j) {
             long jj = j + g.Hy, kk = k + g.Hz;
-            Gc[g.id(g.Nx + g.Hx, jj, kk)] -= getbc(b[PI_EAST], g.Ny, g.Nz, j, k, it) * dT * g.Axk(kk) / g.vol(kk);
+            Gc[g.id(g.Nx + g.Hx, jj, kk)] -= getbc(b[PI_EAST], g.Ny, g.Nz, j, k, it) * dT * g.Axk(g.Nx + g.Hx, jj, kk) / g.vol(g.Nx + g.Hx, jj, kk);
         }
         if (b[PI_SOUTH].kind) for (long k = 1; k <= g.Nz; ++k) for (long i = 1; i <= g.Nx; ++i) {
             long ii = i + g.Hx, kk = k + g.Hz;
-            Gc[g.id(ii, 1 + g.Hy, kk)] += getbc(b[PI_SOUTH], g.Nx, g.Nz, i, k, it) * dT * g.Ayk(kk) / g.vol(kk);
+            Gc[g.id(ii, 1 + g.Hy, kk)] += getbc(b[PI_SOUTH], g.Nx, g.Nz, i, k, it) * dT * g.Ayk(ii, 1 + g.Hy, kk) / g.vol(ii, 1 + g.Hy, kk);
         }
         if (b[PI_NORTH].kind) for (long k = 1; k <= g.Nz; ++k) for (long i = 1; i <= g.Nx; ++i) {
             long ii = i + g.Hx, kk = k + g.Hz;
-            Gc[g.id(ii, g.Ny + g.Hy, kk)] -= getbc(b[PI_NORTH], g.Nx, g.Nz, i, k, it) * dT * g.Ayk(kk) / g.vol(kk);
+            Gc[g.id(ii, g.Ny + g.Hy, kk)] -= getbc(b[PI_NORTH], g.Nx, g.Nz, i, k, it) * dT * g.Ayk(ii, g.Ny + g.Hy, kk) / g.vol(ii, g.Ny + g.Hy, kk);
         }
         if (b[PI_BOTTOM].kind) for (long j = 1; j <= g.Ny; ++j) for (long i = 1; i <= g.Nx; ++i) {
             long ii = i + g.Hx, jj = j + g.Hy, kk = g.Nz + g.Hz;
-            Gc[g.id(ii, jj, kk)] += getbc(b[PI_BOTTOM], g.Nx, g.Ny, i, j, it) * dT * g.Az() / g.vol(kk);
+            Gc[g.id(ii, jj, kk)] += getbc(b[PI_BOTTOM], g.Nx, g.Ny, i, j, it) * dT * g.Az(ii, jj) / g.vol(ii, jj, kk);
         }
         if (b[PI_TOP].kind) for (long j = 1; j <= g.Ny; ++j) for (long i = 1; i <= g.Nx; ++i) {
             long ii = i + g.Hx, jj = j + g.Hy, kk = 1 + g.Hz;
-            Gc[g.id(ii, jj, kk)] -= getbc(b[PI_TOP], g.Nx, g.Ny, i, j, it) * dT * g.Az() / g.vol(kk);
+            Gc[g.id(ii, jj, kk)] -= getbc(b[PI_TOP], g.Nx, g.Ny, i, j, it) * dT * g.Az(ii, jj) / g.vol(ii, jj, kk);
         }
     }
 }
@@ -1053,7 +1066,7 @@ void apply_tendency(orc_model* m) {
             for (long j = g.Hy + 1; j <= g.Hy + g.Ny; ++j)
                 for (long i = g.Hx + 1; i <= g.Hx + g.Nx; ++i) {
                     size_t q = g.id(i, j, k);
-                    m->tr[n][q] += m->Gcs[n][q] + m->plk[n][q] / g.vol(k);
+                    m->tr[n][q] += m->Gcs[n][q] + m->plk[n][q] / g.vol(i, j, k);
                 }
 }
 
@@ -1097,6 +1110,18 @@ int orc_create(const pi_grid* grid, const pi_bgc_params* bgc, const pi_quota_par
     g.G = (size_t)g.Gx * g.Gy * g.Gz;
     g.lm.assign(g.G, 1);
     if (grid->landmask) g.lm.assign(grid->landmask, grid->landmask + g.G);
+    if (const pi_grid_metrics* mt = grid->metrics) {          /* LatLonGrid */
+        const size_t G2 = (size_t)g.Gx * g.Gy;
+        const double* a2[5] = { mt->dxC, mt->dyC, mt->dxF, mt->dyF, mt->Az };
+        const double* a3[3] = { mt->Ax, mt->Ay, mt->Vol };
+        for (const double* p : a2) if (!p) { delete m; g_create_err = "orc_create: LatLonGrid metrics incomplete"; return PI_ERR_ARG; }
+        for (const double* p : a3) if (!p) { delete m; g_create_err = "orc_create: LatLonGrid metrics incomplete"; return PI_ERR_ARG; }
+        g.ll = true;
+        g.mdxC.assign(mt->dxC, mt->dxC + G2); g.mdyC.assign(mt->dyC, mt->dyC + G2);
+        g.mdxF.assign(mt->dxF, mt->dxF + G2); g.mdyF.assign(mt->dyF, mt->dyF + G2);
+        g.mAz.assign(mt->Az, mt->Az + G2);
+        g.mAx.assign(mt->Ax, mt->Ax + g.G); g.mAy.assign(mt->Ay, mt->Ay + g.G); g.mVol.assign(mt->Vol, mt->Vol + g.G);
+    }
     m->bgc = *bgc; m->nsp = nspecies; m->C = capacity; m->seed = seed;
     m->sp.resize(nspecies);
     size_t C = (size_t)capacity;

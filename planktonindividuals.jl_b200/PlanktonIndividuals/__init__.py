@@ -13,8 +13,8 @@ All numerical work runs in libpib200.so (CUDA); there is no CPU fallback.
 from ._abi import tracer_names
 from ._native import CapacityError, PIError
 from .architectures import CPU, GPU, CarbonMode, IronEnergyMode, MacroMolecularMode, QuotaMode
-from .grids import (Ax, Ay, Az, Bounded, Periodic, RectilinearGrid, interior, volume, ΔxC, ΔxF,
-                    ΔyC, ΔyF, ΔzC, ΔzF)
+from .grids import (Ax, Ay, Az, Bounded, LatLonGrid, LoadLatLonGrid, Periodic, RectilinearGrid, interior,
+                    volume, ΔxC, ΔxF, ΔyC, ΔyF, ΔzC, ΔzF)
 from .model import PlanktonDiagnostics, PlanktonModel, TimeStep_b, phyto_setup
 from .parameters import (bgc_params_default, default_PARF, default_temperature, default_tracer_init,
                          phyt_params_default, update_bgc_params, update_phyt_params)
@@ -23,7 +23,7 @@ from .output import PlanktonOutputWriter, write_output_b
 from .batch import BatchMember, Member, PlanktonBatch
 from . import units
 
-__all__ = ["RectilinearGrid", "Periodic", "Bounded", "PlanktonModel", "PlanktonSimulation",
+__all__ = ["RectilinearGrid", "LatLonGrid", "LoadLatLonGrid", "Periodic", "Bounded", "PlanktonModel", "PlanktonSimulation",
            "PlanktonDiagnostics", "update_b", "TimeStep_b", "synchronize", "phyto_setup", "GPU", "CPU",
            "QuotaMode", "CarbonMode", "MacroMolecularMode", "IronEnergyMode", "tracer_names",
            "bgc_params_default", "phyt_params_default", "update_bgc_params", "update_phyt_params",

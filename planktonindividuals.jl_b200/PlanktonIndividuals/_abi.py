@@ -23,12 +23,18 @@ _i64p = ct.POINTER(ct.c_int64)
 _u8p = ct.POINTER(ct.c_uint8)
 
 
+class pi_grid_metrics(ct.Structure):
+    _fields_ = [("dxC", _dp), ("dyC", _dp), ("dxF", _dp), ("dyF", _dp), ("Az", _dp),
+                ("Ax", _dp), ("Ay", _dp), ("Vol", _dp)]
+
+
 class pi_grid(ct.Structure):
     _fields_ = [("Nx", ct.c_int32), ("Ny", ct.c_int32), ("Nz", ct.c_int32),
                 ("Hx", ct.c_int32), ("Hy", ct.c_int32), ("Hz", ct.c_int32),
                 ("topo", ct.c_int32 * 3),
                 ("dx", ct.c_double), ("dy", ct.c_double),
-                ("dzF", _dp), ("dzC", _dp), ("landmask", _u8p)]
+                ("dzF", _dp), ("dzC", _dp), ("landmask", _u8p),
+                ("metrics", ct.POINTER(pi_grid_metrics))]
 
 
 # bgc_params_default keys (src/Parameters/param_default.jl:44-71) in struct order

@@ -8,7 +8,7 @@ import ctypes as ct
 import numpy as np
 
 from . import _abi
-from ._abi import (IND_DOUBLE, IND_INT, NTRACERS, PI_OK, pi_bgc_params, pi_grid, pi_individuals,
+from ._abi import (IND_DOUBLE, IND_INT, NTRACERS, PI_OK, pi_bgc_params, pi_grid, pi_grid_metrics, pi_individuals,
                    pi_quota_params, BGC_FIELDS, QUOTA_FIELDS)
 
 
@@ -48,6 +48,15 @@ def make_grid_struct(grid):
     g.dzF = _dptr(keep[0])
     g.dzC = _dptr(keep[1])
     g.landmask = keep[2].ctypes.data_as(ct.POINTER(ct.c_uint8))
+    if getattr(grid, "is_latlon", False):
+        # LatLonGrid: the metric arrays as the reference stores them (halos included)
+        mt = pi_grid_metrics()
+        for name in ("dxC", "dyC", "dxF", "dyF", "Az", "Ax", "Ay", "Vol"):
+            arr = np.asfortranarray(getattr(grid, name), dtype=np.float64)
+            keep.append(arr)
+            setattr(mt, name, _dptr(arr))
+        keep.append(mt)
+        g.metrics = ct.pointer(mt)
     return g, keep
 
 

@@ -30,11 +30,12 @@ def series_arrays(wl, nsnap):
 
 def interior_mass(get, g):
     """Σ tracer · volume over the interior, per tracer (get(n) returns tracer n with halos)."""
-    vol = float(g.Δx) * float(g.Δy) * np.asarray(g.dzF)[g.Hz:g.Hz + g.Nz]
+    from .grids import cell_volumes
+    vol = cell_volumes(g)[g.Hx:g.Hx + g.Nx, g.Hy:g.Hy + g.Ny, g.Hz:g.Hz + g.Nz]
     out = {}
     for n, name in enumerate(_abi.tracer_names):
         a = get(n)[g.Hx:g.Hx + g.Nx, g.Hy:g.Hy + g.Ny, g.Hz:g.Hz + g.Nz]
-        out[name] = float(np.sum(a * vol[None, None, :]))
+        out[name] = float(np.sum(a * vol))
     return out
 
 

@@ -74,6 +74,8 @@ class PlanktonModel:
             raise ValueError("FT must be Float32 or Float64")
         if carbon and FT is not np.float64:
             raise NotImplementedError("CarbonMode() is built in the FP64 form: use FT = Float64")
+        if getattr(grid, "is_latlon", False) and FT is not np.float64:
+            raise NotImplementedError("LatLonGrid is built in the FP64 form: use FT = Float64")
         self.FT = FT
         self.arch = GPU()
         self.mode = mode if carbon else QuotaMode()

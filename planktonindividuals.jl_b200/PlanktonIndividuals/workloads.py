@@ -22,7 +22,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from ._abi import tracer_names
-from .grids import Bounded, Periodic, RectilinearGrid, fill_halo_tracer
+from .grids import Bounded, LatLonGrid, Periodic, RectilinearGrid, fill_halo_tracer
 from .init import empty_individuals
 from .parameters import default_temperature, update_bgc_params, update_phyt_params
 
@@ -268,6 +268,50 @@ def carbon(nx=16, nz=8, N_per_species=2000, nsp=2, steps=30, dT=60.0, seed=11, n
     n_vel = int(np.ceil(steps / 60)) + 1
     return Workload("carbon", grid, bgc, phyt, nsp, C, [N_per_species] * nsp, inds, trs, dT, steps,
                     60 * dT, n_vel, vel, parf, 3600.0, tmp, 3600.0, seed, mode="carbon")
+
+
+def latlon_streamfunction_velocity(grid, cfl=0.2, dT=600.0, seed=0):
+    """Divergence-free flow on a LatLonGrid from a corner streamfunction ψ of volume transport:
+    U = −(ψ[i, j+1] − ψ[i, j]), V = ψ[i+1, j] − ψ[i, j] per level, u = U/Ax and v = V/Ay at the
+    faces, w = 0, so every cell's transports sum to zero up to rounding. ψ vanishes on Bounded
+    edges (no flow through them) and is periodic in x when x is Periodic. Scaled so the largest
+    Courant number |u|ΔT/ΔxC, |v|ΔT/ΔyC is `cfl`."""
+    rng = np.random.default_rng(seed)
+    Nx, Ny, Nz, Hx, Hy, Hz = grid.Nx, grid.Ny, grid.Nz, grid.Hx, grid.Hy, grid.Hz
+    px = grid.topo[0] == Periodic.code
+    xs = np.arange(Nx + 1, dtype=np.float64)[:, None]
+    ys = np.arange(Ny + 1, dtype=np.float64)[None, :]
+    fx = np.sin(2 * np.pi * xs / Nx + rng.uniform(0, 2 * np.pi)) if px else np.sin(np.pi * xs / Nx)
+    psi2 = fx * np.sin(np.pi * ys / Ny) + 0.3 * np.sin(2 * np.pi * xs / Nx) * np.sin(2 * np.pi * ys / Ny)
+    prof = 1.0 + 0.5 * np.cos(np.pi * (np.arange(Nz) + 0.5) / Nz)
+    nxu = Nx + (0 if px else 1)
+    U = np.zeros((nxu, Ny, Nz)); V = np.zeros((Nx, Ny + 1, Nz))
+    for k in range(Nz):
+        psi = psi2 * prof[k]
+        U[:, :, k] = -(psi[:nxu, 1:] - psi[:nxu, :-1])
+        V[:, :, k] = psi[1:, :] - psi[:-1, :]
+    Ax = grid.Ax[Hx:Hx + nxu, Hy:Hy + Ny, Hz:Hz + Nz]
+    Ay = grid.Ay[Hx:Hx + Nx, Hy:Hy + Ny + 1, Hz:Hz + Nz]
+    u, v = U / Ax, V / Ay
+    dxc = grid.dxC[Hx:Hx + nxu, Hy:Hy + Ny][:, :, None]
+    dyc = grid.dyC[Hx:Hx + Nx, Hy:Hy + Ny + 1][:, :, None]
+    s = cfl / max(np.max(np.abs(u) * dT / dxc), np.max(np.abs(v) * dT / dyc))
+    w = np.zeros((Nx, Ny, Nz + 1))
+    return np.asfortranarray(u * s), np.asfortranarray(v * s), np.asfortranarray(w)
+
+
+def latlon(nx=24, ny=20, nz=6, lon=(-10.0, -7.6), lat=(30.0, 32.0), dz=10.0, N_per_species=3000, nsp=2,
+           steps=20, dT=600.0, seed=12, capacity=None, phyt_over=None, bgc_over=None, landmask=None, cfl=0.2):
+    """QuotaMode on a LatLonGrid (src/Grids/lat_lon_grid.jl): nx×ny×nz cells over `lon` × `lat`
+    degrees and nz levels of dz metres, individuals seeded in the top half, a steady
+    divergence-free transport streamfunction flow (latlon_streamfunction_velocity)."""
+    rng = np.random.default_rng(seed)
+    grid = LatLonGrid(size=(nx, ny, nz), lat=lat, lon=lon, z=(0.0, -dz * nz), FT=np.float64, landmask=landmask)
+    u, v, w = latlon_streamfunction_velocity(grid, cfl=cfl, dT=dT, seed=seed)
+    C = capacity or 2 * N_per_species
+    return _finish("latlon", grid, nsp, [N_per_species] * nsp, C, phyt_over, bgc_over, dT, steps, rng,
+                   lambda t: (u, v, w), 1, dT * steps, max(1, nz // 2), [0.0] * nsp, 0.2, seed,
+                   no3_grad=dz * nz)
 
 
 def config3(nx=512, nz=128, N_per_species=16_777_216, nsp=4, steps=1000, dT=20.0, seed=3,

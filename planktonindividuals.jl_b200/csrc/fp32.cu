@@ -395,6 +395,7 @@ pi_status check_member(const pi_member& mb, int nsp, std::string& msg) {
     for (int a = 0; a < 3; ++a)
         if (grid->topo[a] != PI_PERIODIC && grid->topo[a] != PI_BOUNDED) { msg = "topology must be Periodic or Bounded"; return PI_ERR_ARG; }
     if (grid->topo[2] != PI_BOUNDED) { msg = "z must be Bounded (tracer sinking has no Periodic rule)"; return PI_ERR_ARG; }
+    if (grid->metrics) { msg = "LatLonGrid is built in the FP64 form only (precision PI_FP64)"; return PI_ERR_ARG; }
     long long Gx = grid->Nx + 2LL * grid->Hx, Gy = grid->Ny + 2LL * grid->Hy, Gz = grid->Nz + 2LL * grid->Hz;
     if (Gx * Gy * Gz >= (1LL << 31) - 2 || f32_bits(Gx) + f32_bits(Gy) + f32_bits(Gz) > 31) { msg = "grid too large for 32-bit cell indices"; return PI_ERR_ARG; }
     if (mb.capacity >= (1LL << 31)) { msg = "capacity must be below 2^31"; return PI_ERR_ARG; }

@@ -21,7 +21,25 @@ __device__ __forceinline__ int clamp_idx(long long v, int lo, int hi, uint32_t* 
 
 __device__ __forceinline__ double dzF1(const DGrid& g, int k) { return g.dzF[k - 1]; }
 __device__ __forceinline__ double dzC1(const DGrid& g, int k) { return g.dzC[k - 1]; }
+// Grids/areas_volumes_spacings.jl:9-38 with 1-based halo-inclusive indices: a RectilinearGrid
+// forms them from Δx, Δy and dzF (in the reference's operation order), a LatLonGrid reads its arrays
+__device__ __forceinline__ int gidx2(const DGrid& g, int i, int j) { return (i - 1) + g.Gx * (j - 1); }
+__device__ __forceinline__ double vol(const DGrid& g, int i, int j, int k) {
+    return g.mVol ? g.mVol[(i - 1) + (long long)g.Gx * ((j - 1) + (long long)g.Gy * (k - 1))] : g.dx * g.dy * dzF1(g, k);
+}
+// volume of a RectilinearGrid cell at level k (pi_tracer_advection_noalloc takes only these)
 __device__ __forceinline__ double vol(const DGrid& g, int k) { return g.dx * g.dy * dzF1(g, k); }
+__device__ __forceinline__ double Axm(const DGrid& g, int i, int j, int k) {
+    return g.mAx ? g.mAx[(i - 1) + (long long)g.Gx * ((j - 1) + (long long)g.Gy * (k - 1))] : g.dy * dzF1(g, k);
+}
+__device__ __forceinline__ double Aym(const DGrid& g, int i, int j, int k) {
+    return g.mAy ? g.mAy[(i - 1) + (long long)g.Gx * ((j - 1) + (long long)g.Gy * (k - 1))] : g.dx * dzF1(g, k);
+}
+__device__ __forceinline__ double Azm(const DGrid& g, int i, int j) { return g.mAz ? g.mAz[gidx2(g, i, j)] : g.dx * g.dy; }
+__device__ __forceinline__ double dxCm(const DGrid& g, int i, int j) { return g.mdxC ? g.mdxC[gidx2(g, i, j)] : g.dx; }
+__device__ __forceinline__ double dyCm(const DGrid& g, int i, int j) { return g.mdyC ? g.mdyC[gidx2(g, i, j)] : g.dy; }
+__device__ __forceinline__ double dxFm(const DGrid& g, int i, int j) { return g.mdxF ? g.mdxF[gidx2(g, i, j)] : g.dx; }
+__device__ __forceinline__ double dyFm(const DGrid& g, int i, int j) { return g.mdyF ? g.mdyF[gidx2(g, i, j)] : g.dy; }
 __device__ __forceinline__ int lmask(const DGrid& g, int i, int j, int k) {
     return g.all_water ? 1 : (int)g.lm[gidx(g, i, j, k)];
 }
@@ -72,12 +90,12 @@ __device__ __forceinline__ double itpl(const DGrid& g, const double* __restrict_
     double w101 = xd * (1.0 - yd) * zd;
     double w110 = xd * yd * (1.0 - zd);
     double w111 = xd * yd * zd;
-    double d0, d1;
-    if (COMP == 0) { d0 = g.dx; d1 = g.dx; }
-    else if (COMP == 1) { d0 = g.dy; d1 = g.dy; }
-    else { d0 = dzC1(g, k); d1 = dzC1(g, k + 1); }
-    return w000 * c000 / d0 + w001 * c001 / d1 + w010 * c010 / d0 + w011 * c011 / d1
-         + w100 * c100 / d0 + w101 * c101 / d1 + w110 * c110 / d0 + w111 * c111 / d1;
+    // each corner divided by ΔxC, ΔyC or ΔzC at that corner (interpolation.jl:23-50)
+    auto D = [&](int a, int b, int c) -> double {
+        return COMP == 0 ? dxCm(g, i + a, j + b) : COMP == 1 ? dyCm(g, i + a, j + b) : dzC1(g, k + c);
+    };
+    return w000 * c000 / D(0, 0, 0) + w001 * c001 / D(0, 0, 1) + w010 * c010 / D(0, 1, 0) + w011 * c011 / D(0, 1, 1)
+         + w100 * c100 / D(1, 0, 0) + w101 * c101 / D(1, 0, 1) + w110 * c110 / D(1, 1, 0) + w111 * c111 / D(1, 1, 1);
 }
 
 
@@ -151,8 +169,11 @@ __device__ __forceinline__ void particle_step(const DGrid& g, const SpcDev& P, i
     double r0, r1, r2;
     pi_draw3(seed, iter, (uint32_t)s, PI_DRAW_DIFFUSION, (uint32_t)slot, &r0, &r1, &r2);
     r0 = (r0 - 0.5) * 2.0; r1 = (r1 - 0.5) * 2.0; r2 = (r2 - 0.5) * 2.0;
-    r0 = r0 * sqrt(kappa_h * dT) / g.dx;
-    r1 = r1 * sqrt(kappa_h * dT) / g.dy;
+    // ΔxC/ΔyC at (xi+Hx, yi+Hy) of the stored indices (particle_diffusion.jl:4-5); the reference
+    // reads past the metric array there when x = Nx exactly, which is held at the last column here
+    const int dxi = min(max(oxi + g.Hx, 1), g.Gx), dyi = min(max(oyi + g.Hy, 1), g.Gy);
+    r0 = r0 * sqrt(kappa_h * dT) / dxCm(g, dxi, dyi);
+    r1 = r1 * sqrt(kappa_h * dT) / dyCm(g, dxi, dyi);
     r2 = r2 * sqrt(kappa_v * dT) / dzC1(g, kdz);
     x = x + jl_mulb(r0, ac); y = y + jl_mulb(r1, ac); z = z + jl_mulb(r2, ac);
     x = jl_mulb(bc_pos(x, NX, g.tx), ac); y = jl_mulb(bc_pos(y, NY, g.ty), ac); z = jl_mulb(bc_pos(z, NZ, g.tz), ac);
@@ -251,7 +272,7 @@ __global__ void k_par(DGrid g, const SpcDev* __restrict__ spc, long long C,
             int s = (int)(gd / C);
             chl += spc[s].Chl[gd - (long long)s * C];
         }
-        double atten = (chl / vol(g, kk) * kc + kw) * dzF1(g, kk);
+        double atten = (chl / vol(g, ii, jj, kk) * kc + kw) * dzF1(g, kk);
         double e = pi_exp(-atten);
         double pv = parf * (1.0 - e) / atten;
         par[c] = pv;
@@ -824,12 +845,11 @@ __global__ void __launch_bounds__(32 * SWX_WARPS) k_sweep_x(DGrid g, const doubl
     const bool zero_face = !has_face || (special && g.tx != PI_PERIODIC);
     const int fs = special ? g.Hx + 1 : f;           // face whose stencil gives the flux
     const long long G = g.G;
-    const double ax = g.dy * dzF1(g, k);
     const int qf = gidx(g, has_face ? fs : i0, j, k);
     FaceCoef fc{};
     int lm2 = 1, lm1 = 1, l0 = 1, lp1 = 1;
     if (!zero_face) {
-        fc = face_coef(u[qf], ax, g.dx, dT);
+        fc = face_coef(u[qf], Axm(g, fs, j, k), dxCm(g, fs, j), dT);
         lm2 = lmask(g, fs - 2, j, k); lm1 = lmask(g, fs - 1, j, k); l0 = lmask(g, fs, j, k); lp1 = lmask(g, fs + 1, j, k);
     }
     const int qc = gidx(g, has_cell ? f : i0, j, k);
@@ -837,8 +857,8 @@ __global__ void __launch_bounds__(32 * SWX_WARPS) k_sweep_x(DGrid g, const doubl
     int cl0 = 1, clp = 1;
     if (has_cell) {
         cl0 = lmask(g, f, j, k); clp = lmask(g, f + 1, j, k);
-        ftr = jl_mulb(jl_mulb(ax * u[qc + 1] - ax * u[qc], clp), cl0);
-        dtv = dT / vol(g, k);
+        ftr = jl_mulb(jl_mulb(Axm(g, f + 1, j, k) * u[qc + 1] - Axm(g, f, j, k) * u[qc], clp), cl0);
+        dtv = dT / vol(g, f, j, k);
     }
 #pragma unroll 2
     for (int n = 0; n < PI_NTRACERS; ++n) {
@@ -862,11 +882,11 @@ __global__ void __launch_bounds__(32 * SWX_WARPS) k_sweep_x(DGrid g, const doubl
 #define SWY_TY 4
 __device__ __forceinline__ double yface_flux(const DGrid& g, const double* __restrict__ c,
                                              const double* __restrict__ v, int i, int f, int k,
-                                             double ay, double dT) {
+                                             double dT) {
     const bool special = f == g.Ny + g.Hy + 1;
     if (special && g.ty != PI_PERIODIC) return 0.0;            // fill_halo_north_Gc! (Bounded)
     const int fs = special ? g.Hy + 1 : f;                      // periodic: Gc[N+H+1] = Gc[H+1]
-    FaceCoef fc = face_coef(v[gidx(g, i, fs, k)], ay, g.dy, dT);
+    FaceCoef fc = face_coef(v[gidx(g, i, fs, k)], Aym(g, i, fs, k), dyCm(g, i, fs), dT);
     int r0 = gidx(g, i, wrap_axis(fs - 2, g.Ny, g.Hy, g.ty), k), r1 = gidx(g, i, wrap_axis(fs - 1, g.Ny, g.Hy, g.ty), k);
     int r2 = gidx(g, i, wrap_axis(fs, g.Ny, g.Hy, g.ty), k), r3 = gidx(g, i, wrap_axis(fs + 1, g.Ny, g.Hy, g.ty), k);
     return flux_xy_c(fc, c[r0], c[r1], c[r2], c[r3], lmask(g, i, fs - 2, k), lmask(g, i, fs - 1, k),
@@ -885,17 +905,17 @@ __global__ void __launch_bounds__(32 * SWY_TY, 8) k_sweep_y(DGrid g, const doubl
     if (i > g.Nx + g.Hx || j0 > g.Ny + g.Hy) return;
     const int jend = min(j0 + SWY_L - 1, g.Ny + g.Hy);
     const long long G = g.G;
-    const double ay = g.dx * dzF1(g, k);
-    const double dtv = dT / vol(g, k);
+    const double dtv0 = dT / vol(g, i, j0, k);      // the same for every row of a RectilinearGrid
 #pragma unroll 1
     for (int t = 0; t < PI_NTRACERS; ++t) {
         const double* c = tta + t * G;
-        double Ft = yface_flux(g, c, v, i, j0, k, ay, dT);
+        double Ft = yface_flux(g, c, v, i, j0, k, dT);
         for (int jj = j0; jj <= jend; ++jj) {
-            double Fb = yface_flux(g, c, v, i, jj + 1, k, ay, dT);
+            double Fb = yface_flux(g, c, v, i, jj + 1, k, dT);
             const int q = gidx(g, i, jj, k);
             const int cl0 = lmask(g, i, jj, k), clp = lmask(g, i, jj + 1, k);
-            const double ftr = jl_mulb(jl_mulb(ay * v[q + g.Gx] - ay * v[q], clp), cl0);
+            const double dtv = g.mVol ? dT / vol(g, i, jj, k) : dtv0;
+            const double ftr = jl_mulb(jl_mulb(Aym(g, i, jj + 1, k) * v[q + g.Gx] - Aym(g, i, jj, k) * v[q], clp), cl0);
             double dG = jl_mulb(jl_mulb(Fb - Ft, clp), cl0);
             ttb[t * G + q] = c[q] - dtv * (dG - tr[t * G + q] * ftr);
             Ft = Fb;
@@ -962,7 +982,7 @@ __global__ void __launch_bounds__(32 * SWZ_TZ, 8) k_sweep_z(DGrid g, const doubl
     if (i > g.Nx + g.Hx || k0 > g.Nz + g.Hz) return;
     const int kend = min(k0 + SWZ_L - 1, g.Nz + g.Hz);
     const long long G = g.G;
-    const double az = g.dx * g.dy;
+    const double az = Azm(g, i, j);
     const int slab = g.Gx * g.Gy;
     const int qcol = gidx(g, i, j, 1);
 #pragma unroll 1
@@ -976,7 +996,7 @@ __global__ void __launch_bounds__(32 * SWZ_TZ, 8) k_sweep_z(DGrid g, const doubl
             const double ftr = jl_mulb(jl_mulb(az * w[q] - az * w[q + slab], clp), cl0);
             const double dG = jl_mulb(jl_mulb(Ft - Fb, clp), cl0);
             const double cc = tr[t * G + q];
-            const double ct = c[q] - dT / vol(g, k) * (dG - cc * ftr);
+            const double ct = c[q] - dT / vol(g, i, j, k) * (dG - cc * ftr);
             gadv[t * G + q] = ct - cc;                          // calc_tracer_tendency!
             Ft = Fb;
         }
@@ -999,7 +1019,7 @@ __global__ void __launch_bounds__(128, 6) k_tracer_tail(ZFinalArgs a) {
     double Gc[PI_NTRACERS];
 #pragma unroll
     for (int t = 0; t < PI_NTRACERS; ++t) Gc[t] = a.gadv[t * G + q];
-    z_final_cell(a, i, j, k, q, vol(g, k), Gc);
+    z_final_cell(a, i, j, k, q, vol(g, i, j, k), Gc);
 }
 
 // The rest of tracer_update! for one interior cell, given its advective tendency Gc.
@@ -1007,13 +1027,12 @@ __device__ __forceinline__ void z_final_cell(const ZFinalArgs& a, int i, int j, 
     const DGrid& g = a.g;
     const long long G = g.G;
     const double dT = a.dT;
-    const double az = g.dx * g.dy;
+    const double az = Azm(g, i, j);
     const int slab = g.Gx * g.Gy;
     const pi_bgc_params& b = a.b;
     // tracer_diffusion! (κ∇², tracer_diffusion.jl:1-21) on the original tracer
     if (a.diffuse) {
         double kx = b.kappa_h, ky = b.kappa_h, kz = b.kappa_v;
-        double axk = g.dy * dzF1(g, k), ayk = g.dx * dzF1(g, k);
         int li = lmask(g, i, j, k);
 #pragma unroll
         for (int n = 0; n < PI_NTRACERS; ++n) {
@@ -1021,8 +1040,8 @@ __device__ __forceinline__ void z_final_cell(const ZFinalArgs& a, int i, int j, 
             auto dx0 = [&](int ii) { return jl_mulb(jl_mulb(c[gidx(g, ii, j, k)] - c[gidx(g, ii - 1, j, k)], lmask(g, ii, j, k)), lmask(g, ii - 1, j, k)); };
             auto dy0 = [&](int jj) { return jl_mulb(jl_mulb(c[gidx(g, i, jj, k)] - c[gidx(g, i, jj - 1, k)], lmask(g, i, jj, k)), lmask(g, i, jj - 1, k)); };
             auto dz0 = [&](int kk) { return jl_mulb(jl_mulb(c[gidx(g, i, j, kk - 1)] - c[gidx(g, i, j, kk)], lmask(g, i, j, kk)), lmask(g, i, j, kk - 1)); };
-            double fx1 = kx * axk * (dx0(i + 1) / g.dx), fx0 = kx * axk * (dx0(i) / g.dx);
-            double fy1 = ky * ayk * (dy0(j + 1) / g.dy), fy0 = ky * ayk * (dy0(j) / g.dy);
+            double fx1 = kx * Axm(g, i + 1, j, k) * (dx0(i + 1) / dxFm(g, i + 1, j)), fx0 = kx * Axm(g, i, j, k) * (dx0(i) / dxFm(g, i, j));
+            double fy1 = ky * Aym(g, i, j + 1, k) * (dy0(j + 1) / dyFm(g, i, j + 1)), fy0 = ky * Aym(g, i, j, k) * (dy0(j) / dyFm(g, i, j));
             double fz0 = kz * az * (dz0(k) / dzF1(g, k)), fz1 = kz * az * (dz0(k + 1) / dzF1(g, k + 1));
             double ax_ = jl_mulb(jl_mulb(fx1 - fx0, lmask(g, i + 1, j, k)), li);
             double ay_ = jl_mulb(jl_mulb(fy1 - fy0, lmask(g, i, j + 1, k)), li);
@@ -1071,7 +1090,7 @@ __device__ __forceinline__ void z_final_cell(const ZFinalArgs& a, int i, int j, 
     // apply_bcs! (apply_bcs.jl:4-98), faces in the reference's order
     if (a.any_bc) {
         int ii = i - g.Hx, jj = j - g.Hy, kk = k - g.Hz;
-        double axk = g.dy * dzF1(g, k), ayk = g.dx * dzF1(g, k);
+        double axk = Axm(g, i, j, k), ayk = Aym(g, i, j, k);
 #pragma unroll
         for (int n = 0; n < PI_NTRACERS; ++n) {
             const FluxBCDev* B = a.bcs + n * 6;
@@ -1233,7 +1252,7 @@ __global__ void __launch_bounds__(256) k_budget_cells(DGrid g, const double* __r
         const long long r = q / g.Nx;
         const int j = (int)(r % g.Ny) + 1 + g.Hy, k = (int)(r / g.Ny) + 1 + g.Hz;
         const long long cq = gidx(g, i, j, k);
-        const double vol = g.dx * g.dy * g.dzF[k - 1];
+        const double vol = pib::vol(g, i, j, k);
         c += vol * (tr[PI_DIC * G + cq] + tr[PI_DOC * G + cq] + tr[PI_POC * G + cq]);
         n += vol * (tr[PI_NH4 * G + cq] + tr[PI_NO3 * G + cq] + tr[PI_DON * G + cq] + tr[PI_PON * G + cq]);
         p += vol * (tr[PI_PO4 * G + cq] + tr[PI_DOP * G + cq] + tr[PI_POP * G + cq]);

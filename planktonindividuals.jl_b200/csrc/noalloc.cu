@@ -151,6 +151,8 @@ pi_status pi_tracer_advection_noalloc(const pi_grid* grid, const double* c, cons
         return noalloc_fail(PI_ERR_ARG, "pi_tracer_advection_noalloc: x/y Periodic or Bounded, z Bounded");
     if (grid->Nx < grid->Hx || grid->Ny < grid->Hy || grid->Nz < grid->Hz)
         return noalloc_fail(PI_ERR_ARG, "pi_tracer_advection_noalloc: every axis needs at least as many cells as halo points");
+    if (grid->metrics)
+        return noalloc_fail(PI_ERR_ARG, "pi_tracer_advection_noalloc: RectilinearGrid only (metrics must be NULL)");
     long long Gx = grid->Nx + 2LL * grid->Hx, Gy = grid->Ny + 2LL * grid->Hy, Gz = grid->Nz + 2LL * grid->Hz;
     long long G = Gx * Gy * Gz;
     if (G > PI_NOALLOC_MAX_CELLS || Gz > PI_NOALLOC_MAX_GZ)

@@ -92,6 +92,8 @@ struct pi_model {
     double* dzF = nullptr;
     double* dzC = nullptr;
     uint8_t* lm = nullptr;
+    double* met = nullptr;           // LatLonGrid metrics: dxC, dyC, dxF, dyF, Az (Gx·Gy each), Ax, Ay, Vol (G each)
+    std::vector<double> met_host;    // their host copy, the source of the upload
     StepBufs sb{};
     uint32_t* iota = nullptr;    // nsp·C
     void* cub_tmp = nullptr;
@@ -442,6 +444,12 @@ pi_status pi_create(const pi_grid* grid, const pi_bgc_params* bgc, const pi_quot
     long long Gx = grid->Nx + 2LL * grid->Hx, Gy = grid->Ny + 2LL * grid->Hy, Gz = grid->Nz + 2LL * grid->Hz;
     if (Gx * Gy * Gz >= (1LL << 31) - 2 || (Gx + 1) * (Gy + 1) * (Gz + 1) >= (1LL << 31))
         return fail(nullptr, PI_ERR_ARG, "pi_create: grid too large for 32-bit cell indices");
+    if (const pi_grid_metrics* mt = grid->metrics) {
+        if (precision != PI_FP64)
+            return fail(nullptr, PI_ERR_ARG, "pi_create: LatLonGrid is built in the FP64 form only (precision PI_FP64)");
+        if (!mt->dxC || !mt->dyC || !mt->dxF || !mt->dyF || !mt->Az || !mt->Ax || !mt->Ay || !mt->Vol)
+            return fail(nullptr, PI_ERR_ARG, "pi_create: LatLonGrid metrics: every array is required");
+    }
     if ((long long)nspecies * capacity >= (1LL << 31))
         return fail(nullptr, PI_ERR_ARG, "pi_create: nspecies × capacity must be below 2^31");
     for (int s = 0; s < nspecies; ++s) {
@@ -501,6 +509,15 @@ pi_status pi_create(const pi_grid* grid, const pi_bgc_params* bgc, const pi_quot
     pi_status st;
 #define ALB(ptr, n) do { st = dalloc(m, &(ptr), (size_t)(n), #ptr); if (st) return bail(st); } while (0)
     ALB(m->dzF, Gz); ALB(m->dzC, Gz); ALB(m->lm, G);
+    const long long G2 = Gx * Gy;
+    if (const pi_grid_metrics* mt = grid->metrics) {
+        ALB(m->met, 5 * G2 + 3 * G);
+        m->met_host.resize((size_t)(5 * G2 + 3 * G));
+        const double* a2[5] = { mt->dxC, mt->dyC, mt->dxF, mt->dyF, mt->Az };
+        const double* a3[3] = { mt->Ax, mt->Ay, mt->Vol };
+        for (int e = 0; e < 5; ++e) std::copy(a2[e], a2[e] + G2, m->met_host.begin() + e * G2);
+        for (int e = 0; e < 3; ++e) std::copy(a3[e], a3[e] + G, m->met_host.begin() + 5 * G2 + e * G);
+    }
     ALB(m->tr, PI_NTRACERS * G); ALB(m->tr_next, PI_NTRACERS * G);
     ALB(m->tta, PI_NTRACERS * G); ALB(m->ttb, PI_NTRACERS * G);
     for (int b = 0; b < 2; ++b) for (int c = 0; c < 3; ++c) ALB(m->velbuf[b][c], G);
@@ -529,6 +546,8 @@ pi_status pi_create(const pi_grid* grid, const pi_bgc_params* bgc, const pi_quot
     ok = ok && cudaMemcpyAsync(m->dzF, hg.dzF.data(), Gz * sizeof(double), cudaMemcpyHostToDevice, s0) == cudaSuccess;
     ok = ok && cudaMemcpyAsync(m->dzC, hg.dzC.data(), Gz * sizeof(double), cudaMemcpyHostToDevice, s0) == cudaSuccess;
     ok = ok && cudaMemcpyAsync(m->lm, hg.lm.data(), G, cudaMemcpyHostToDevice, s0) == cudaSuccess;
+    if (m->met)
+        ok = ok && cudaMemcpyAsync(m->met, m->met_host.data(), m->met_host.size() * sizeof(double), cudaMemcpyHostToDevice, s0) == cudaSuccess;
     ok = ok && cudaMemcpyAsync(m->d_spc, m->h_spc.data(), nspecies * sizeof(SpcDev), cudaMemcpyHostToDevice, s0) == cudaSuccess;
     for (void* p : { (void*)m->tr, (void*)m->tr_next, (void*)m->tta, (void*)m->ttb })
         ok = ok && cudaMemsetAsync(p, 0, PI_NTRACERS * G * sizeof(double), s0) == cudaSuccess;
@@ -572,7 +591,13 @@ pi_status pi_create(const pi_grid* grid, const pi_bgc_params* bgc, const pi_quot
     st = dalloc(m, (char**)&m->cub_tmp, m->cub_bytes, "cub scratch");
     if (st) return bail(st);
     m->dg = DGrid{hg.Nx, hg.Ny, hg.Nz, hg.Hx, hg.Hy, hg.Hz, hg.Gx, hg.Gy, hg.Gz,
-                  hg.topo[0], hg.topo[1], hg.topo[2], all_water, hg.dx, hg.dy, m->dzF, m->dzC, m->lm, G};
+                  hg.topo[0], hg.topo[1], hg.topo[2], all_water, hg.dx, hg.dy, m->dzF, m->dzC, m->lm, G,
+                  nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    if (m->met) {
+        double* b = m->met;
+        m->dg.mdxC = b; m->dg.mdyC = b + G2; m->dg.mdxF = b + 2 * G2; m->dg.mdyF = b + 3 * G2; m->dg.mAz = b + 4 * G2;
+        m->dg.mAx = b + 5 * G2; m->dg.mAy = b + 5 * G2 + G; m->dg.mVol = b + 5 * G2 + 2 * G;
+    }
     st = upload_bcs(m);
     if (st) return bail(st);
     *out = m;

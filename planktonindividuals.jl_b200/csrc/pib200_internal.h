@@ -48,6 +48,9 @@ struct DGrid {
     const double* dzC;     // Gz
     const uint8_t* lm;     // G
     long long G;
+    // LatLonGrid metrics (lat_lon_grid.jl:1-45), null for a RectilinearGrid: dxC, dyC, dxF, dyF,
+    // Az over the Gx·Gy columns, Ax, Ay, Vol over the G cells
+    const double *mdxC, *mdyC, *mdxF, *mdyF, *mAz, *mAx, *mAy, *mVol;
 };
 
 __host__ __device__ __forceinline__ int gidx(const DGrid& g, int i, int j, int k) {

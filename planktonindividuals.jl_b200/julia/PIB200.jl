@@ -43,6 +43,13 @@ struct PiGrid
     topo::NTuple{3,Int32}
     dx::Float64; dy::Float64
     dzF::Ptr{Float64}; dzC::Ptr{Float64}; landmask::Ptr{UInt8}
+    metrics::Ptr{Cvoid}          # Ptr{PiGridMetrics} for a LatLonGrid, C_NULL for a RectilinearGrid
+end
+
+# pi_grid_metrics: the arrays a LatLonGrid stores (src/Grids/lat_lon_grid.jl:1-45), halos included
+struct PiGridMetrics
+    dxC::Ptr{Float64}; dyC::Ptr{Float64}; dxF::Ptr{Float64}; dyF::Ptr{Float64}; Az::Ptr{Float64}
+    Ax::Ptr{Float64}; Ay::Ptr{Float64}; Vol::Ptr{Float64}
 end
 
 # bgc_params_default (src/Parameters/param_default.jl:44-71), field order of pi_bgc_params
@@ -125,10 +132,18 @@ end
 
 topo_code(T) = occursin("Periodic", string(T)) ? PI_PERIODIC : PI_BOUNDED
 
-function pigrid(g, dzF::Vector{Float64}, dzC::Vector{Float64}, lm::Vector{UInt8})
+function pigrid(g, dzF::Vector{Float64}, dzC::Vector{Float64}, lm::Vector{UInt8}, met::Ptr{Cvoid} = C_NULL)
     PiGrid(g.Nx, g.Ny, g.Nz, g.Hx, g.Hy, g.Hz,
            (topo_code(g.topology[1]), topo_code(g.topology[2]), topo_code(g.topology[3])),
-           Float64(g.Î”x), Float64(g.Î”y), pointer(dzF), pointer(dzC), pointer(lm))
+           Float64(g.Î”x), Float64(g.Î”y), pointer(dzF), pointer(dzC), pointer(lm), met)
+end
+
+# The LatLonGrid arrays as Float64 vectors (kept alive by the caller) and their pi_grid_metrics;
+# a RectilinearGrid (no dxC field) gives nothing.
+function metric_arrays(g)
+    hasproperty(g, :dxC) || return (Vector{Float64}[], nothing)
+    arrs = [Float64.(vec(collect(getproperty(g, s)))) for s in (:dxC, :dyC, :dxF, :dyF, :Az, :Ax, :Ay, :Vol)]
+    (arrs, Ref(PiGridMetrics(map(pointer, arrs)...)))
 end
 
 """PlanktonModel(GPU(), grid; FT, max_individuals, bgc_params, phyto) on the B200: allocates the
@@ -136,11 +151,12 @@ model on the current CUDA device (`FT = Float64` â†’ the plain form, `Float32` â
 function create(g, bgc::AbstractDict, phyt::AbstractDict, Nsp::Integer, maxN::Integer; FT = Float64, seed::Integer = 0)
     dzF, dzC = Float64.(collect(g.dzF)), Float64.(collect(g.dzC))
     lm = UInt8.(vec(collect(g.landmask)))
-    pg = Ref(pigrid(g, dzF, dzC, lm))
+    marr, mref = metric_arrays(g)
+    pg = Ref(pigrid(g, dzF, dzC, lm, mref === nothing ? C_NULL : Ptr{Cvoid}(Base.unsafe_convert(Ptr{PiGridMetrics}, mref))))
     pb = Ref(PiBgc(bgc))
     ps = [PiQuota(phyt, s) for s in 1:Nsp]
     out = Ref{Ptr{Cvoid}}(C_NULL)
-    st = GC.@preserve dzF dzC lm ccall((:pi_create, lib), Int32,
+    st = GC.@preserve dzF dzC lm marr mref ccall((:pi_create, lib), Int32,
         (Ref{PiGrid}, Ref{PiBgc}, Ptr{PiQuota}, Int32, Int64, Int32, UInt64, Ref{Ptr{Cvoid}}),
         pg, pb, ps, Nsp, maxN, FT === Float32 ? PI_FP32 : PI_FP64, seed, out)
     check(st, C_NULL)
@@ -154,11 +170,12 @@ the FP64 form only."""
 function create_carbon(g, bgc::AbstractDict, phyt::AbstractDict, Nsp::Integer, maxN::Integer; seed::Integer = 0)
     dzF, dzC = Float64.(collect(g.dzF)), Float64.(collect(g.dzC))
     lm = UInt8.(vec(collect(g.landmask)))
-    pg = Ref(pigrid(g, dzF, dzC, lm))
+    marr, mref = metric_arrays(g)
+    pg = Ref(pigrid(g, dzF, dzC, lm, mref === nothing ? C_NULL : Ptr{Cvoid}(Base.unsafe_convert(Ptr{PiGridMetrics}, mref))))
     pb = Ref(PiBgc(bgc))
     ps = [PiCarbon(phyt, s) for s in 1:Nsp]
     out = Ref{Ptr{Cvoid}}(C_NULL)
-    st = GC.@preserve dzF dzC lm ccall((:pi_create_carbon, lib), Int32,
+    st = GC.@preserve dzF dzC lm marr mref ccall((:pi_create_carbon, lib), Int32,
         (Ref{PiGrid}, Ref{PiBgc}, Ptr{PiCarbon}, Int32, Int64, Int32, UInt64, Ref{Ptr{Cvoid}}),
         pg, pb, ps, Nsp, maxN, PI_FP64, seed, out)
     check(st, C_NULL)
