@@ -1450,6 +1450,14 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& md, con
     // member constants in registers: the stores of the walk could otherwise alias them
     const int Nx = md.Nx, Hx = md.Hx, Hz = md.Hz, Gx = md.Gx, Gy = md.Gy;
     const int i = it.y + lane, j = it.z, k0 = it.w;
+    // levels of the walk where any of the 32 columns holds an individual: only those have
+    // particle sums to read and zero (a warp-uniform test; the others skip the sum's copy)
+    uint64_t occm = 0;
+    if (NUT) {
+#pragma unroll 4
+        for (int l = 0; l < LZ; ++l)
+            if (__ballot_sync(0xffffffffu, sPop[l * 32 + lane] > 0)) occm |= 1ull << l;
+    }
     if (i > Nx + Hx) return;
     const long long G = a.Gtot, off = md.cell_off;
     const float dT = a.dT;
@@ -1483,6 +1491,8 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& md, con
         xo[0] = PI_DFe;
     }
     const FeCoef fc = fe_coef(b, dT);
+    // POC, PON and POP force on themselves only: their partner term reads the own value (aO = 0)
+    const bool partner = !NUT || xo[0] != n;
     const float* __restrict__ t = a.tb + n * G + off;
     const float* __restrict__ c = a.tr + n * G + off;
     const float* __restrict__ trm = a.tr + off;           // all tracers of the member
@@ -1503,23 +1513,23 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& md, con
     const float* __restrict__ x2p = trm + xo[2] * G;
     const float* __restrict__ x3p = trm + xo[3] * G;
     const float* __restrict__ x4p = trm + xo[4] * G;
-    // ring fill of level kk; past the last level the last level is copied again into the stage
-    // that level kk would use, which no iteration reads
+    // ring fill of level kk (nothing past the last level: an empty group keeps the wait count)
     auto issue = [&](int kk) {
-        const unsigned so = (unsigned)((kk - k0) & (ZS - 1)) * 128u;
-        const int kc = min(kk, kend);
-        const int qq = qcol + (kc - 1) * slab;
-        cpa4(rc + so, c + qq);
-        cpa4(rc + 512u + so, t + tl(kc + 2));
-        if (NUT) {
-            cpa4(rc + 1024u + so, x0p + qq);
-            cpa8(ra + 2u * so, acc + qq, kk <= kend && sPop[(kc - k0) * 32 + lane] > 0);
-        } else if (n != PI_Dust) {
-            cpa4(rc + 1024u + so, x0p + qq);
-            cpa4(rc + 1536u + so, x1p + qq);
-            cpa4(rc + 2048u + so, x2p + qq);
-            cpa4(rc + 2560u + so, x3p + qq);
-            cpa4(rx4 + so, x4p + qq);
+        if (kk <= kend) {                                     // warp-uniform
+            const unsigned so = (unsigned)((kk - k0) & (ZS - 1)) * 128u;
+            const int qq = qcol + (kk - 1) * slab;
+            cpa4(rc + so, c + qq);
+            cpa4(rc + 512u + so, t + tl(kk + 2));
+            if (NUT) {
+                if (partner) cpa4(rc + 1024u + so, x0p + qq);
+                if (occm >> (kk - k0) & 1ull) cpa8(ra + 2u * so, acc + qq, sPop[(kk - k0) * 32 + lane] > 0);
+            } else if (n != PI_Dust) {
+                cpa4(rc + 1024u + so, x0p + qq);
+                cpa4(rc + 1536u + so, x1p + qq);
+                cpa4(rc + 2048u + so, x2p + qq);
+                cpa4(rc + 2560u + so, x3p + qq);
+                cpa4(rx4 + so, x4p + qq);
+            }
         }
         cpa_commit();
     };
@@ -1562,7 +1572,7 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& md, con
         }
         if (NUT) {
             // tracer_forcing! (tracer_forcings.jl:2-50) on max(0, tracer)
-            Gc = add_forcing(Gc, aS, cc, aO, lds_f32(rc + 1024u + so));
+            Gc = add_forcing(Gc, aS, cc, aO, partner ? lds_f32(rc + 1024u + so) : cc);
         } else {
             // tracer_sinking! (tracer_sinking.jl:1-42)
             if (sinks) {
@@ -1595,7 +1605,7 @@ __device__ __forceinline__ void z_walk(const TrArgs& a, const MemberDev& md, con
         // particle terms from the fixed-point sums (zeroed as they are consumed), apply_tendency!
         // (tracer_update.jl:6-13)
         float plk = 0.0f;
-        if (NUT) {
+        if (NUT && (occm >> l & 1ull)) {
             const long long vv = (long long)lds_u64(ra + 2u * so);   // zero where the cell holds no individual
             if (vv) { acc[q] = 0ull; plk = (float)((double)vv * L.fxv); }
         }
