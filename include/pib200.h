@@ -74,6 +74,12 @@ enum { PI_PROC_PS = 0, PI_PROC_BS, PI_PROC_VDOC, PI_PROC_VNH4, PI_PROC_VNO3, PI_
  * PI_DIAG_PROC + q kinds and proc_mask bits. */
 enum { PI_CPROC_PS = 0, PI_CPROC_BS, PI_CPROC_RP, PI_CPROC_RS, PI_CPROC_TD, PI_CPROC_Bm, PI_CPROC_Bd,
        PI_CPROC_Chl, PI_NCPROC };
+/* The processes of a MacroMolecularMode model, in the order of plank_avail_diags
+ * (Diagnostics/diagnostics_struct.jl:148-149). diags_spcs! (diagnostics_kernels.jl:20-21) lists
+ * VNH4 as :VHN4 and has no :exu, so those two fields are kept and stay zero, as there. */
+enum { PI_MPROC_PS = 0, PI_MPROC_VDOC, PI_MPROC_VNH4, PI_MPROC_VNO3, PI_MPROC_VPO4, PI_MPROC_resp,
+       PI_MPROC_rChl, PI_MPROC_S_PRO, PI_MPROC_S_DNA, PI_MPROC_S_RNA, PI_MPROC_exu, PI_MPROC_CH,
+       PI_MPROC_NST, PI_MPROC_PST, PI_MPROC_PRO, PI_MPROC_DNA, PI_MPROC_RNA, PI_MPROC_Chl, PI_NMPROC };
 
 /* The horizontal metrics of a LatLonGrid (src/Grids/lat_lon_grid.jl:1-45, built by
  * LatLonGrid :57-170 or LoadLatLonGrid :196-316), as the reference stores them: halos included,
@@ -133,6 +139,16 @@ typedef struct {
     double thermal, is_bact;
 } pi_carbon_params;
 
+/* MacroMolecularMode phytoplankton parameters of one species, in the reference's param_names
+ * order (src/Individuals/Plankton/MacroMolecularMode/plankton_generation.jl:17-23). */
+typedef struct {
+    double Nsuper, C_DNA, var, PRO2DNA, RNA2DNA, CH2DNA, Chl2DNA, alpha, Phi, Topt, Tmax, Ea;
+    double PCmax, VDOCmax, VNO3max, VNH4max, VPO4max, KsatDOC, KsatNH4, KsatNO3, KsatPO4;
+    double CHmax, NSTmax, PSTmax, Chl2N, R_NC_PRO, R_NC_DNA, R_NC_RNA, R_PC_DNA, R_PC_RNA, respir;
+    double k_pro, k_sat_pro, k_rna, k_sat_rna, k_dna, k_sat_dna;
+    double dvid_P, grz_P, mort_P, mort_reg, grazFracC, grazFracN, grazFracP, mortFracC, mortFracN, mortFracP;
+} pi_macro_params;
+
 /* The persistent per-individual state of one species (QuotaMode struct-of-arrays,
  * plankton_generation.jl:2-13; CarbonMode, CarbonMode/plankton_generation.jl:2-11, keeps Bd, the
  * damaged biomass, and no Cq, Nq, Pq). Every array is `capacity` long. graz/mort/dvid carry the
@@ -146,6 +162,8 @@ typedef struct {
     uint8_t *ac;
     double  *graz, *mort, *dvid;
     double  *Bd;
+    double  *PRO, *DNA, *RNA, *CH, *NST, *PST;   /* MacroMolecularMode only (protein, DNA, RNA,
+                                                  carbohydrate/lipid, N and P reserves) */
 } pi_individuals;
 
 typedef struct pi_model pi_model;
@@ -166,6 +184,15 @@ pi_status pi_create(const pi_grid* grid, const pi_bgc_params* bgc,
 pi_status pi_create_carbon(const pi_grid* grid, const pi_bgc_params* bgc,
                            const pi_carbon_params* species, int32_t nspecies, int64_t capacity,
                            int32_t precision, uint64_t seed, pi_model** out);
+
+/* PlanktonModel(arch, grid; mode = MacroMolecularMode(), ...): as pi_create with MacroMolecularMode
+ * species (src/Individuals/Plankton/MacroMolecularMode/): individuals carry PRO, DNA, RNA, CH, NST,
+ * PST, Chl, gen and age (Sz, Bm and the quotas are not used). Built in the FP64 form (precision
+ * PI_FP64; PI_FP32 is refused with PI_ERR_ARG). pi_get_budget reports the individuals' carbon,
+ * nitrogen and phosphorus from total_C/N/P_biomass (plankton_generation.jl:82-93). */
+pi_status pi_create_macro(const pi_grid* grid, const pi_bgc_params* bgc,
+                          const pi_macro_params* species, int32_t nspecies, int64_t capacity,
+                          int32_t precision, uint64_t seed, pi_model** out);
 
 /* Releases every device allocation of the handle. */
 pi_status pi_destroy(pi_model* m);

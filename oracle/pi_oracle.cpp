@@ -56,6 +56,8 @@ const double F_1em6  = (double)1.0e-6f;    /* 1.0f-6   */
 const double F_0p99  = (double)0.99f;      /* 0.99f0   */
 const double F_THMAX = (double)1.0e20f;    /* θmax = 1.0f20, DST3FL.jl:2 */
 const double F_1em20 = (double)1.0e-20f;   /* 1.0f-20  */
+const double F_5em2  = (double)0.05f;      /* 0.05f0   */
+const double F_CHL   = (double)893.49f;    /* 893.49f0 (mg Chl per mmol, MacroMolecularMode) */
 
 const uint32_t ERR_DOMAIN = 1u, ERR_CAPACITY = 2u;
 
@@ -102,6 +104,11 @@ struct Species {
     int carbon = 0;
     pi_carbon_params cp{};
     dvec Bd, RP, RS, TD;
+    /* MacroMolecularMode species (MacroMolecularMode/plankton_generation.jl:2-15): protein, DNA,
+     * RNA, carbohydrate/lipid, N and P reserves, and the synthesis rates */
+    int macro = 0;
+    pi_macro_params mp{};
+    dvec PRO, DNA, RNA, CH, NST, PST, S_PRO, S_DNA, S_RNA;
 };
 
 struct FluxBC { int kind = PI_BC_NONE; dvec v; int64_t nt = 0; };
@@ -601,10 +608,12 @@ std::string capacity_message(double t) {
 }
 
 bool plankton_update_carbon(orc_model* m, Species& s, int spi, double dT, double t);
+bool plankton_update_macro(orc_model* m, Species& s, int spi, double dT, double t);
 
 /* plankton_update!, QuotaMode/plankton_update.jl:1-34 */
 bool plankton_update(orc_model* m, Species& s, int spi, double dT, double t) {
     if (s.carbon) return plankton_update_carbon(m, s, spi, dT, t);
+    if (s.macro) return plankton_update_macro(m, s, spi, dT, t);
     const pi_quota_params& p = s.p;
     int64_t C = m->C;
     diags_proc(m, s, s.d_graz, &s.graz);
@@ -816,6 +825,216 @@ bool plankton_update_carbon(orc_model* m, Species& s, int spi, double dT, double
         const dvec* procs[PI_NCPROC] = { &s.PS, &s.BS, &s.RP, &s.RS, &s.TD, &s.Bm, &s.Bd, &s.Chl };
         for (int q = 0; q < PI_NCPROC; ++q)
             if (m->proc_mask & (1u << q)) diags_proc(m, s, s.d_proc[q], procs[q]);
+    }
+    diags_proc(m, s, s.d_num, nullptr);
+    return true;
+}
+
+/* ---------------------------------------------------------------------------------------- */
+/* MacroMolecularMode physiology, src/Individuals/Plankton/MacroMolecularMode/ (all files)      */
+/* ---------------------------------------------------------------------------------------- */
+
+inline double m_tempFunc_PS(double T, const pi_macro_params& p) {   /* MacroMolecularMode/growth_kernels.jl:2-9 */
+    double x = T - p.Topt, xmax = p.Tmax - p.Topt;
+    double regT = shape_func_dec(x, xmax, F_4em2, 4);
+    double k = pi_exp(-p.Ea / (F_RGAS * (T + F_T0))) * regT;
+    k = jl_max(0.0, k);
+    double OGT_rate = pi_exp(-p.Ea / (F_RGAS * (p.Topt + F_T0)));
+    return jl_min(1.0, k / OGT_rate);
+}
+inline double m_tempFunc(double T, const pi_macro_params& p) {      /* :12-17 */
+    double k = pi_exp(-p.Ea / (F_RGAS * (T + F_T0)));
+    k = jl_max(0.0, k);
+    double OGT_rate = pi_exp(-p.Ea / (F_RGAS * (p.Topt + F_T0)));
+    return jl_min(1.0, k / OGT_rate);
+}
+/* total_C/N/P_biomass, MacroMolecularMode/plankton_generation.jl:82-93 */
+inline double m_totC(double PRO, double DNA, double RNA, double CH, double Chl) {
+    return PRO + DNA + RNA + CH + Chl / F_CHL * 55.0;
+}
+inline double m_totN(double PRO, double DNA, double RNA, double NST, double Chl, const pi_macro_params& p) {
+    return PRO * p.R_NC_PRO + DNA * p.R_NC_DNA + RNA * p.R_NC_RNA + NST + Chl / F_CHL * 4.0;
+}
+inline double m_totP(double DNA, double RNA, double PST, const pi_macro_params& p) {
+    return DNA * p.R_PC_DNA + RNA * p.R_PC_RNA + PST;
+}
+
+/* plankton_growth!, MacroMolecularMode/plankton_growth.jl:2-28, with the kernels of
+ * growth_kernels.jl:1-200 and division_death_probability.jl:37-40, 49-52, 84-87. Every slot is
+ * updated: the synthesis and exudation terms carry no ac, so the state of an inactive slot keeps
+ * changing as in the reference (its temperature, light and nutrients are zero unless it was
+ * active when they were gathered). */
+void plankton_growth_macro(orc_model* m, Species& s, int spi, double dT) {
+    const pi_macro_params& p = s.mp;
+    int64_t C = m->C;
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < C; ++i) {
+        int ac = s.ac[i];
+        double NH4 = m->tNH4[i], NO3 = m->tNO3[i], PO4 = m->tPO4[i], DOC = m->tDOC[i];
+        double par = m->tpar[i], T = m->tT[i], pop = m->tpop[i];
+        double PRO = s.PRO[i], DNA = s.DNA[i], RNA = s.RNA[i], CH = s.CH[i], NST = s.NST[i], PST = s.PST[i];
+        double Chl = s.Chl[i];
+        /* calc_inorganic_uptake_kernel! (:45-54): calc_PS (:20-25), calc_NP_uptake (:28-42) */
+        double aI = par * p.alpha * p.Phi;
+        double PCm = p.PCmax * m_tempFunc_PS(T, p);
+        double PS = PCm * (1.0 - pi_exp(-aI / jl_max(F_1em30, PCm) * Chl / jl_max(F_1em30, PRO))) * PRO;
+        PS = jl_mulb(PS, ac);
+        double N_tot = m_totN(PRO, DNA, RNA, NST, Chl, p), P_tot = m_totP(DNA, RNA, PST, p);
+        double R_NST = NST / jl_max(F_1em30, N_tot), R_PST = PST / jl_max(F_1em30, P_tot);
+        double regQN = shape_func_dec(R_NST, p.NSTmax, F_1em4, 4), regQP = shape_func_dec(R_PST, p.PSTmax, F_1em4, 4);
+        double VNH4 = jl_mulb(p.VNH4max * regQN * NH4 / jl_max(F_1em30, NH4 + p.KsatNH4) * m_tempFunc(T, p) * PRO, ac);
+        double VNO3 = jl_mulb(p.VNO3max * regQN * NO3 / jl_max(F_1em30, NO3 + p.KsatNO3) * m_tempFunc(T, p) * PRO, ac);
+        double VPO4 = jl_mulb(p.VPO4max * regQP * PO4 / jl_max(F_1em30, PO4 + p.KsatPO4) * m_tempFunc(T, p) * PRO, ac);
+        VNH4 = jl_min(VNH4, NH4 / dT / jl_max(1.0, pop));
+        VNO3 = jl_min(VNO3, NO3 / dT / jl_max(1.0, pop));
+        VPO4 = jl_min(VPO4, PO4 / dT / jl_max(1.0, pop));
+        /* update_quotas_1_kernel! (:63-67) */
+        CH += PS * dT; PST += VPO4 * dT; NST += (VNH4 + VNO3) * dT;
+        /* calc_organic_uptake_kernel! (:82-90): calc_DOC_uptake (:73-80) */
+        double R_CH = CH / jl_max(F_1em30, m_totC(PRO, DNA, RNA, CH, Chl));
+        double regQ = shape_func_dec(R_CH, p.CHmax, F_1em4, 4);
+        double VN = p.VDOCmax * regQ * DOC / jl_max(F_1em30, DOC + p.KsatDOC) * m_tempFunc(T, p) * PRO;
+        double VDOC = jl_mulb(jl_min(VN, DOC / dT / jl_max(1.0, pop)), ac);
+        VDOC = jl_mulb(VDOC, jl_isless(F_5em2, PS / (VDOC + PS)));
+        /* calc_ρChl_kernel! (:98-103) */
+        double rChl = jl_mulb(jl_mulb(PS / jl_max(F_1em30, PRO) / jl_max(F_1em30, par * p.alpha * p.Phi * Chl / jl_max(F_1em30, PRO)),
+                                      jl_isless(F_1em1, par)), ac);
+        /* calc_respir_kernel! (:111-114) */
+        double resp = jl_mulb(p.respir * PRO * m_tempFunc(T, p), ac);
+        /* update_quotas_2_kernel! (:124-130) */
+        CH = CH + (VDOC - resp) * dT;
+        PRO = PRO - jl_max(0.0, 0.0 - CH);
+        NST = NST + jl_max(0.0, 0.0 - CH) * p.R_NC_PRO;
+        CH = CH + jl_max(0.0, 0.0 - CH);
+        /* calc_BS_kernel! (:136-152) */
+        double tf = m_tempFunc(T, p);
+        double limit_PRO = jl_min(CH / (CH + p.k_sat_pro * p.Nsuper), NST / (NST + p.k_sat_pro * p.Nsuper * p.R_NC_PRO));
+        double limit_DNA = jl_min(jl_min(CH / (CH + p.k_sat_dna * p.Nsuper), NST / (NST + p.k_sat_dna * p.Nsuper * p.R_NC_DNA)),
+                                  PST / (PST + p.k_sat_dna * p.Nsuper * p.R_PC_DNA));
+        double limit_RNA = jl_min(jl_min(CH / (CH + p.k_sat_rna * p.Nsuper), NST / (NST + p.k_sat_rna * p.Nsuper * p.R_NC_RNA)),
+                                  PST / (PST + p.k_sat_rna * p.Nsuper * p.R_PC_RNA));
+        double S_PRO = p.k_pro * RNA * limit_PRO * tf;
+        double S_DNA = jl_mulb(p.k_dna * PRO * limit_DNA * tf, jl_isless(DNA / (p.C_DNA * p.Nsuper), 2.0));
+        double S_RNA = p.k_rna * PRO * limit_RNA * tf;
+        /* update_biomass_kernel! (:159-171) */
+        PRO += dT * S_PRO;
+        DNA += dT * S_DNA;
+        RNA += dT * S_RNA;
+        CH -= dT * (S_PRO + S_DNA + S_RNA + S_PRO * rChl);
+        NST -= dT * (S_PRO * p.R_NC_PRO + S_DNA * p.R_NC_DNA + S_RNA * p.R_NC_RNA + S_PRO * rChl * 4.0 / 55.0);
+        PST -= dT * (S_DNA * p.R_PC_DNA + S_RNA * p.R_PC_RNA);
+        Chl += dT * S_PRO * rChl * F_CHL / 55.0;
+        s.age[i] += jl_mulb(dT / 3600.0, ac);
+        /* calc_exudation_kernel! (:179-183), update_CH_kernel! (:190-193) */
+        double exu = jl_max(0.0, CH - p.CHmax * m_totC(PRO, DNA, RNA, CH, Chl));
+        CH -= exu;
+        s.PS[i] = PS; s.VNH4[i] = VNH4; s.VNO3[i] = VNO3; s.VPO4[i] = VPO4; s.VDOC[i] = VDOC;
+        s.rChl[i] = rChl; s.resp[i] = resp; s.S_PRO[i] = S_PRO; s.S_DNA[i] = S_DNA; s.S_RNA[i] = S_RNA;
+        s.exu[i] = exu;
+        s.PRO[i] = PRO; s.DNA[i] = DNA; s.RNA[i] = RNA; s.CH[i] = CH; s.NST[i] = NST; s.PST[i] = PST; s.Chl[i] = Chl;
+        /* calc_graz_quadratic!, calc_MM_mort!, calc_MM_dvid! (division_death_probability.jl:37-40,
+         * 49-52, 84-87) */
+        s.graz[i] = jl_mulb(pop * p.grz_P, ac);
+        s.mort[i] = jl_mulb(p.mort_P * shape_func_inc(s.age[i], p.mort_reg, F_1em4, 4), ac);
+        s.dvid[i] = jl_mulb(p.dvid_P, jl_isless(2.0, DNA / (p.C_DNA * p.Nsuper)));
+    }
+    /* get_probability!, division_death_probability.jl:95-107 */
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < C; ++i) {
+        double r0, r1, r2;
+        pi_draw3(m->seed, (uint32_t)m->iteration, (uint32_t)spi, PI_DRAW_DECISION, (uint32_t)i, &r0, &r1, &r2);
+        m->rx[i] = r0; m->ry[i] = r1; m->rz[i] = r2;
+    }
+    for (int64_t i = 0; i < C; ++i) {
+        int ac = s.ac[i];
+        s.graz[i] = (double)(jl_isless(m->rx[i], s.graz[i] * dT) && ac);
+        s.mort[i] = (double)(jl_isless(m->ry[i], s.mort[i] * dT) && ac);
+        s.dvid[i] = (double)(jl_isless(m->rz[i], s.dvid[i] * dT) && ac);
+    }
+}
+
+/* calc_loss_kernel!, MacroMolecularMode/consume_loss.jl:14-24, then inactivate! */
+void calc_loss_macro(orc_model* m, Species& s, const dvec& loss, double fC, double fN, double fP) {
+    const pi_macro_params& p = s.mp;
+    for (int64_t i = 0; i < m->C; ++i) {
+        size_t c = cell_of(m, s, i);
+        int ac = s.ac[i];
+        double l = loss[i];
+        double tC = m_totC(s.PRO[i], s.DNA[i], s.RNA[i], s.CH[i], s.Chl[i]);
+        double tN = m_totN(s.PRO[i], s.DNA[i], s.RNA[i], s.NST[i], s.Chl[i], p);
+        double tP = m_totP(s.DNA[i], s.RNA[i], s.PST[i], p);
+        m->plk[PI_DOC][c] += jl_mulb(tC * fC, ac) * l;
+        m->plk[PI_DON][c] += jl_mulb(tN * fN, ac) * l;
+        m->plk[PI_DOP][c] += jl_mulb(tP * fP, ac) * l;
+        m->plk[PI_POC][c] += jl_mulb(tC * (1.0 - fC), ac) * l;
+        m->plk[PI_PON][c] += jl_mulb(tN * (1.0 - fN), ac) * l;
+        m->plk[PI_POP][c] += jl_mulb(tP * (1.0 - fP), ac) * l;
+    }
+    for (int64_t i = 0; i < m->C; ++i) s.ac[i] = (uint8_t)(s.ac[i] && jl_isless(loss[i], 1.0));
+}
+
+/* plankton_update!, MacroMolecularMode/plankton_update.jl:1-33 */
+bool plankton_update_macro(orc_model* m, Species& s, int spi, double dT, double t) {
+    const pi_macro_params& p = s.mp;
+    int64_t C = m->C;
+    diags_proc(m, s, s.d_graz, &s.graz);
+    calc_loss_macro(m, s, s.graz, p.grazFracC, p.grazFracN, p.grazFracP);   /* grazing!   */
+    diags_proc(m, s, s.d_mort, &s.mort);
+    calc_loss_macro(m, s, s.mort, p.mortFracC, p.mortFracN, p.mortFracP);   /* mortality! */
+    for (int64_t i = 0; i < C; ++i) s.dvid[i] = jl_mulb(s.dvid[i], s.ac[i]);
+    diags_proc(m, s, s.d_dvid, &s.dvid);
+    double dvidnum = 0.0;
+    std::vector<int64_t> free_slots;
+    for (int64_t i = 0; i < C; ++i) {
+        dvidnum += s.dvid[i] * (double)s.ac[i];
+        if (!s.ac[i]) free_slots.push_back(i + 1);
+    }
+    if (dvidnum > (double)free_slots.size()) {
+        m->err = capacity_message(t);
+        m->err_flags |= ERR_CAPACITY;
+        return false;
+    }
+    /* divide!, MacroMolecularMode/division_death.jl:70-78: copy_daughter_individuals! (:28-46)
+     * copies x, y, z, PRO, DNA, RNA, CH, NST, PST, Chl, gen, ac and dvid (not age);
+     * divide_to_half! (:51-62) halves the seven biomass pools of every divider and daughter */
+    double acc = 0.0;
+    for (int64_t i = 0; i < C; ++i) { acc += s.dvid[i]; m->tidc[i] = acc; m->tidc_int[i] = (int64_t)acc; }
+    for (int64_t i = 0; i < C; ++i)
+        if (s.dvid[i] == 1.0) s.idx[i] = free_slots[(size_t)m->tidc_int[i] - 1];
+    for (int64_t i = 0; i < C; ++i)
+        if (s.dvid[i] == 1.0 && s.idx[i] != 0) {
+            int64_t d = s.idx[i] - 1;
+            s.x[d] = s.x[i]; s.y[d] = s.y[i]; s.z[d] = s.z[i];
+            s.PRO[d] = s.PRO[i]; s.DNA[d] = s.DNA[i]; s.RNA[d] = s.RNA[i]; s.CH[d] = s.CH[i];
+            s.NST[d] = s.NST[i]; s.PST[d] = s.PST[i]; s.Chl[d] = s.Chl[i]; s.gen[d] = s.gen[i];
+            s.ac[d] = s.ac[i]; s.dvid[d] = s.dvid[i];
+        }
+    for (int64_t i = 0; i < C; ++i) {
+        double f = (2.0 - s.dvid[i]) / 2.0;
+        s.PRO[i] *= f; s.DNA[i] *= f; s.RNA[i] *= f; s.CH[i] *= f; s.NST[i] *= f; s.PST[i] *= f; s.Chl[i] *= f;
+        s.gen[i] += s.dvid[i];
+        s.age[i] *= (1.0 - s.dvid[i]);
+    }
+    for (int64_t i = 0; i < C; ++i) s.idx[i] = 0;
+    plankton_growth_macro(m, s, spi, dT);
+    /* calc_consume_kernel!, MacroMolecularMode/consume_loss.jl:2-9 */
+    for (int64_t i = 0; i < C; ++i) {
+        size_t c = cell_of(m, s, i);
+        int ac = s.ac[i];
+        m->plk[PI_DIC][c] += jl_mulb((s.resp[i] - s.PS[i]) * dT, ac);
+        m->plk[PI_DOC][c] += jl_mulb((s.exu[i] - s.VDOC[i]) * dT, ac);
+        m->plk[PI_NH4][c] += jl_mulb(-s.VNH4[i] * dT, ac);
+        m->plk[PI_NO3][c] += jl_mulb(-s.VNO3[i] * dT, ac);
+        m->plk[PI_PO4][c] += jl_mulb(-s.VPO4[i] * dT, ac);
+    }
+    /* diags_spcs! (Diagnostics/diagnostics_kernels.jl:20-21): VNH4 (listed there as :VHN4) and
+     * exu are not accumulated */
+    if (m->proc_mask) {
+        const dvec* procs[PI_NMPROC] = { &s.PS, &s.VDOC, nullptr, &s.VNO3, &s.VPO4, &s.resp, &s.rChl, &s.S_PRO,
+                                         &s.S_DNA, &s.S_RNA, nullptr, &s.CH, &s.NST, &s.PST, &s.PRO, &s.DNA,
+                                         &s.RNA, &s.Chl };
+        for (int q = 0; q < PI_NMPROC; ++q)
+            if ((m->proc_mask & (1u << q)) && procs[q]) diags_proc(m, s, s.d_proc[q], procs[q]);
     }
     diags_proc(m, s, s.d_num, nullptr);
     return true;
@@ -1178,6 +1397,34 @@ int orc_create_carbon(const pi_grid* grid, const pi_bgc_params* bgc, const pi_ca
     return PI_OK;
 }
 
+/* A MacroMolecularMode model: the QuotaMode setup with the shared parameters, then the species
+ * switched to MacroMolecularMode (Sz, Bm and the quotas stay zero). */
+int orc_create_macro(const pi_grid* grid, const pi_bgc_params* bgc, const pi_macro_params* species,
+                     int32_t nspecies, int64_t capacity, uint64_t seed, orc_model** out) {
+    if (!species || nspecies < 1) { g_create_err = "orc_create_macro: bad argument"; return PI_ERR_ARG; }
+    std::vector<pi_quota_params> q((size_t)nspecies);
+    for (int s = 0; s < nspecies; ++s) {
+        const pi_macro_params& c = species[s];
+        pi_quota_params& p = q[s];
+        memset(&p, 0, sizeof p);
+        p.Nsuper = c.Nsuper; p.var = c.var; p.alpha = c.alpha; p.Phi = c.Phi; p.Topt = c.Topt; p.Tmax = c.Tmax;
+        p.Ea = c.Ea; p.PCmax = c.PCmax; p.respir = c.respir; p.grz_P = c.grz_P; p.dvid_type = 1.0;
+        p.dvid_P = c.dvid_P; p.mort_P = c.mort_P; p.mort_reg = c.mort_reg;
+        p.grazFracC = c.grazFracC; p.grazFracN = c.grazFracN; p.grazFracP = c.grazFracP;
+        p.mortFracC = c.mortFracC; p.mortFracN = c.mortFracN; p.mortFracP = c.mortFracP;
+    }
+    int st = orc_create(grid, bgc, q.data(), nspecies, capacity, seed, out);
+    if (st) return st;
+    for (int s = 0; s < nspecies; ++s) {
+        Species& S = (*out)->sp[s];
+        S.macro = 1;
+        S.mp = species[s];
+        for (dvec* v : { &S.PRO, &S.DNA, &S.RNA, &S.CH, &S.NST, &S.PST, &S.S_PRO, &S.S_DNA, &S.S_RNA })
+            v->assign((size_t)capacity, 0.0);
+    }
+    return PI_OK;
+}
+
 int orc_destroy(orc_model* m) { delete m; return PI_OK; }
 
 int orc_set_individuals(orc_model* m, int32_t sp, const pi_individuals* in) {
@@ -1187,11 +1434,18 @@ int orc_set_individuals(orc_model* m, int32_t sp, const pi_individuals* in) {
     auto cp = [&](dvec& d, const double* s) { d.assign(s, s + C); };
     cp(S.x, in->x); cp(S.y, in->y); cp(S.z, in->z);
     S.xi.assign(in->xi, in->xi + C); S.yi.assign(in->yi, in->yi + C); S.zi.assign(in->zi, in->zi + C);
+    if (S.macro) {
+        const double* cols[6] = { in->PRO, in->DNA, in->RNA, in->CH, in->NST, in->PST };
+        dvec* dst[6] = { &S.PRO, &S.DNA, &S.RNA, &S.CH, &S.NST, &S.PST };
+        for (int q = 0; q < 6; ++q) { if (!cols[q]) return PI_ERR_ARG; cp(*dst[q], cols[q]); }
+        for (dvec* v : { &S.Sz, &S.Bm, &S.Cq, &S.Nq, &S.Pq }) v->assign(C, 0.0);
+    } else {
     cp(S.Sz, in->Sz); cp(S.Bm, in->Bm);
     for (auto pr : { std::make_pair(&S.Cq, in->Cq), std::make_pair(&S.Nq, in->Nq), std::make_pair(&S.Pq, in->Pq) }) {
         if (pr.second) cp(*pr.first, pr.second);
         else if (S.carbon) pr.first->assign(C, 0.0);
         else return PI_ERR_ARG;
+    }
     }
     cp(S.Chl, in->Chl); cp(S.gen, in->gen); cp(S.age, in->age);
     S.ac.assign(in->ac, in->ac + C);
@@ -1212,6 +1466,10 @@ int orc_get_individuals(orc_model* m, int32_t sp, pi_individuals* out) {
     if (out->ac) std::copy(S.ac.begin(), S.ac.end(), out->ac);
     cp(out->graz, S.graz); cp(out->mort, S.mort); cp(out->dvid, S.dvid);
     if (S.carbon) cp(out->Bd, S.Bd);
+    if (S.macro) {
+        cp(out->PRO, S.PRO); cp(out->DNA, S.DNA); cp(out->RNA, S.RNA);
+        cp(out->CH, S.CH); cp(out->NST, S.NST); cp(out->PST, S.PST);
+    }
     return PI_OK;
 }
 
@@ -1375,10 +1633,11 @@ int orc_count_active(orc_model* m, int32_t sp, int64_t* n) {
 
 /* PlanktonDiagnostics(model; tracer, phytoplankton) optional fields: enabling clears them. */
 int orc_set_diags(orc_model* m, uint32_t tr_mask, uint32_t proc_mask) {
-    if (!m || tr_mask >> PI_NTRACERS || proc_mask >> PI_NPROC) return PI_ERR_ARG;
+    const int nproc = m ? (m->sp[0].macro ? (int)PI_NMPROC : m->sp[0].carbon ? (int)PI_NCPROC : (int)PI_NPROC) : 0;
+    if (!m || tr_mask >> PI_NTRACERS || proc_mask >> nproc) return PI_ERR_ARG;
     m->tr_mask = tr_mask; m->proc_mask = proc_mask;
     m->d_tr.assign(tr_mask ? PI_NTRACERS : 0, dvec(tr_mask ? m->g.G : 0, 0.0));
-    for (Species& S : m->sp) S.d_proc.assign(proc_mask ? PI_NPROC : 0, dvec(proc_mask ? m->g.G : 0, 0.0));
+    for (Species& S : m->sp) S.d_proc.assign(proc_mask ? nproc : 0, dvec(proc_mask ? m->g.G : 0, 0.0));
     return PI_OK;
 }
 
@@ -1389,8 +1648,9 @@ int orc_get_diag(orc_model* m, int32_t kind, int32_t sp, double* out) {
     else if (kind >= PI_DIAG_TRACER && kind < PI_DIAG_TRACER + PI_NTRACERS) {
         if (!(m->tr_mask & (1u << (kind - PI_DIAG_TRACER)))) return PI_ERR_ARG;
         f = &m->d_tr[kind - PI_DIAG_TRACER];
-    } else if (kind >= PI_DIAG_PROC && kind < PI_DIAG_PROC + PI_NPROC) {
+    } else if (kind >= PI_DIAG_PROC && kind < PI_DIAG_PROC + PI_NMPROC) {
         if (sp < 0 || sp >= m->nsp || !(m->proc_mask & (1u << (kind - PI_DIAG_PROC)))) return PI_ERR_ARG;
+        if ((size_t)(kind - PI_DIAG_PROC) >= m->sp[sp].d_proc.size()) return PI_ERR_ARG;
         f = &m->sp[sp].d_proc[kind - PI_DIAG_PROC];
     } else {
         if (sp < 0 || sp >= m->nsp) return PI_ERR_ARG;

@@ -88,6 +88,31 @@ class pi_carbon_params(ct.Structure):
 # CarbonMode processes of diags_spcs! (diagnostics_kernels.jl:16-17), in PI_CPROC_* order
 CARBON_PROC_NAMES = ("PS", "BS", "RP", "RS", "TD", "Bm", "Bd", "Chl")
 
+# MacroMolecularMode param_names (src/Individuals/Plankton/MacroMolecularMode/plankton_generation.jl:17-23)
+MACRO_FIELDS = [("Nsuper", "Nsuper"), ("C_DNA", "C_DNA"), ("var", "var"), ("PRO2DNA", "PRO2DNA"),
+                ("RNA2DNA", "RNA2DNA"), ("CH2DNA", "CH2DNA"), ("Chl2DNA", "Chl2DNA"), ("alpha", "α"),
+                ("Phi", "Φ"), ("Topt", "Topt"), ("Tmax", "Tmax"), ("Ea", "Ea"), ("PCmax", "PCmax"),
+                ("VDOCmax", "VDOCmax"), ("VNO3max", "VNO3max"), ("VNH4max", "VNH4max"),
+                ("VPO4max", "VPO4max"), ("KsatDOC", "KsatDOC"), ("KsatNH4", "KsatNH4"),
+                ("KsatNO3", "KsatNO3"), ("KsatPO4", "KsatPO4"), ("CHmax", "CHmax"), ("NSTmax", "NSTmax"),
+                ("PSTmax", "PSTmax"), ("Chl2N", "Chl2N"), ("R_NC_PRO", "R_NC_PRO"), ("R_NC_DNA", "R_NC_DNA"),
+                ("R_NC_RNA", "R_NC_RNA"), ("R_PC_DNA", "R_PC_DNA"), ("R_PC_RNA", "R_PC_RNA"),
+                ("respir", "respir"), ("k_pro", "k_pro"), ("k_sat_pro", "k_sat_pro"), ("k_rna", "k_rna"),
+                ("k_sat_rna", "k_sat_rna"), ("k_dna", "k_dna"), ("k_sat_dna", "k_sat_dna"),
+                ("dvid_P", "dvid_P"), ("grz_P", "grz_P"), ("mort_P", "mort_P"), ("mort_reg", "mort_reg"),
+                ("grazFracC", "grazFracC"), ("grazFracN", "grazFracN"), ("grazFracP", "grazFracP"),
+                ("mortFracC", "mortFracC"), ("mortFracN", "mortFracN"), ("mortFracP", "mortFracP")]
+
+
+class pi_macro_params(ct.Structure):
+    _fields_ = [(c, ct.c_double) for c, _ in MACRO_FIELDS]
+
+
+# MacroMolecularMode processes in PI_MPROC_* order (plank_avail_diags, diagnostics_struct.jl:148-149)
+MACRO_PROC_NAMES = ("PS", "VDOC", "VNH4", "VNO3", "VPO4", "resp", "ρChl", "S_PRO", "S_DNA", "S_RNA", "exu",
+                    "CH", "NST", "PST", "PRO", "DNA", "RNA", "Chl")
+MACRO_POOLS = ("PRO", "DNA", "RNA", "CH", "NST", "PST")
+
 
 IND_DOUBLE = ("x", "y", "z", "Sz", "Bm", "Cq", "Nq", "Pq", "Chl", "gen", "age", "graz", "mort", "dvid")
 IND_INT = ("xi", "yi", "zi")
@@ -100,7 +125,8 @@ class pi_individuals(ct.Structure):
                 ("Chl", _dp), ("gen", _dp), ("age", _dp),
                 ("ac", _u8p),
                 ("graz", _dp), ("mort", _dp), ("dvid", _dp),
-                ("Bd", _dp)]
+                ("Bd", _dp),
+                ("PRO", _dp), ("DNA", _dp), ("RNA", _dp), ("CH", _dp), ("NST", _dp), ("PST", _dp)]
 
 
 class pi_member(ct.Structure):
@@ -132,13 +158,15 @@ def declare(lib, prefix):
         "get_budget": (ct.c_int32, [P, _dp]),
         "create_carbon": (ct.c_int32, [ct.POINTER(pi_grid), ct.POINTER(pi_bgc_params),
                                        ct.POINTER(pi_carbon_params), ct.c_int32, ct.c_int64]),
+        "create_macro": (ct.c_int32, [ct.POINTER(pi_grid), ct.POINTER(pi_bgc_params),
+                                      ct.POINTER(pi_macro_params), ct.c_int32, ct.c_int64]),
         "last_error": (ct.c_int32, [P, ct.c_char_p, ct.c_size_t]),
     }
     for name, (res, args) in protos.items():
         fn = getattr(lib, prefix + name, None)
         if fn is None:
             continue
-        if name in ("create", "create_carbon"):
+        if name in ("create", "create_carbon", "create_macro"):
             if prefix == "pi_":
                 args = args + [ct.c_int32, ct.c_uint64, ct.POINTER(P)]
             else:

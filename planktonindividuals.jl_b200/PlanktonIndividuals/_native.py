@@ -68,10 +68,11 @@ def make_bgc_struct(params):
 
 
 def make_species_structs(phyt_params, nsp, mode="quota"):
-    carbon = mode == "carbon"
-    arr = ((_abi.pi_carbon_params if carbon else pi_quota_params) * nsp)()
+    struct, fields = {"carbon": (_abi.pi_carbon_params, _abi.CARBON_FIELDS),
+                      "macro": (_abi.pi_macro_params, _abi.MACRO_FIELDS)}.get(mode, (pi_quota_params, QUOTA_FIELDS))
+    arr = (struct * nsp)()
     for s in range(nsp):
-        for cname, key in (_abi.CARBON_FIELDS if carbon else QUOTA_FIELDS):
+        for cname, key in fields:
             v = phyt_params[key]
             v = v[s] if hasattr(v, "__len__") else v
             setattr(arr[s], cname, float(v))
@@ -83,9 +84,10 @@ class CModel:
 
     def __init__(self, lib, prefix, grid, bgc_params, phyt_params, nsp, capacity, seed,
                  precision=None, mode="quota"):
-        """mode: "quota" (QuotaMode) or "carbon" (CarbonMode, `<prefix>create_carbon`)."""
-        if mode not in ("quota", "carbon"):
-            raise ValueError(f"mode must be 'quota' or 'carbon', not {mode!r}")
+        """mode: "quota" (QuotaMode), "carbon" (CarbonMode, `<prefix>create_carbon`) or "macro"
+        (MacroMolecularMode, `<prefix>create_macro`)."""
+        if mode not in ("quota", "carbon", "macro"):
+            raise ValueError(f"mode must be 'quota', 'carbon' or 'macro', not {mode!r}")
         self.lib = _abi.declare(lib, prefix)
         self.prefix = prefix
         self.mode = mode
@@ -96,7 +98,7 @@ class CModel:
         b = make_bgc_struct(bgc_params)
         sp = make_species_structs(phyt_params, self.nsp, mode)
         h = ct.c_void_p()
-        fn = self._fn("create_carbon" if mode == "carbon" else "create")
+        fn = self._fn({"carbon": "create_carbon", "macro": "create_macro"}.get(mode, "create"))
         if precision is None:
             rc = fn(ct.byref(g), ct.byref(b), sp, self.nsp, self.capacity, ct.c_uint64(seed), ct.byref(h))
         else:
@@ -146,10 +148,12 @@ class CModel:
         C = self.capacity
         keep = {}
         st = pi_individuals()
-        carbon = self.mode == "carbon"
-        for k in IND_DOUBLE + (("Bd",) if carbon else ()):
+        carbon, macro = self.mode == "carbon", self.mode == "macro"
+        for k in IND_DOUBLE + (("Bd",) if carbon else ()) + (_abi.MACRO_POOLS if macro else ()):
             if carbon and k in ("Cq", "Nq", "Pq", "Bd") and k not in data:
                 continue                      # CarbonMode keeps no quotas; Bd defaults to zero
+            if macro and k in ("Sz", "Bm", "Cq", "Nq", "Pq"):
+                continue                      # MacroMolecularMode keeps its six pools instead
             a = np.ascontiguousarray(data[k], dtype=np.float64)
             if a.shape != (C,):
                 raise ValueError(f"individual attribute {k} must have length {C}")
@@ -168,8 +172,11 @@ class CModel:
 
     def get_individuals(self, sp):
         C = self.capacity
-        carbon = self.mode == "carbon"
-        names = tuple(k for k in IND_DOUBLE if not (carbon and k in ("Cq", "Nq", "Pq"))) + (("Bd",) if carbon else ())
+        carbon, macro = self.mode == "carbon", self.mode == "macro"
+        if macro:
+            names = tuple(k for k in IND_DOUBLE if k not in ("Sz", "Bm", "Cq", "Nq", "Pq")) + _abi.MACRO_POOLS
+        else:
+            names = tuple(k for k in IND_DOUBLE if not (carbon and k in ("Cq", "Nq", "Pq"))) + (("Bd",) if carbon else ())
         out = {k: np.empty(C, dtype=np.float64) for k in names}
         out.update({k: np.empty(C, dtype=np.int64) for k in IND_INT})
         out["ac"] = np.empty(C, dtype=np.uint8)

@@ -1,6 +1,6 @@
 """Architectures and physiology modes (src/Architectures.jl, src/PlanktonIndividuals.jl:59-83).
-GPU() with QuotaMode() (both precisions) and CarbonMode() (Float64) are implemented; the other
-modes exist so that code naming them fails with a clear message."""
+GPU() with QuotaMode() (both precisions), CarbonMode() and MacroMolecularMode() (Float64) are
+implemented; IronEnergyMode exists so that code naming it fails with a clear message."""
 
 
 class Architecture:
@@ -40,7 +40,11 @@ class CarbonMode(AbstractMode):
 
 
 class MacroMolecularMode(AbstractMode):
-    pass
+    """Protein, DNA, RNA, carbohydrate/lipid and N/P reserves
+    (src/Individuals/Plankton/MacroMolecularMode/)."""
+
+    def __repr__(self):
+        return "MacroMolecularMode()"
 
 
 class IronEnergyMode(AbstractMode):

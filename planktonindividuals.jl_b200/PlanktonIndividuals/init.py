@@ -79,6 +79,45 @@ def initialize_plankton_carbon(grid, p, s, N, C, rng):
     return d
 
 
+def initialize_plankton_macro(grid, p, s, N, C, rng):
+    """initialize_plankton! of MacroMolecularMode (MacroMolecularMode/plankton_generation.jl:40-79)
+    for species s: DNA in C_DNA·Nsuper·(1, 1 + var), RNA, PRO in (1 ± var) times their ratio to
+    DNA, CH in (1 ± var)·DNA·CH2DNA, NST = U(1 ± var)·CH·16/106, PST = U(1 ± var)·CH/106,
+    Chl = DNA·Chl2DNA·893.49/55."""
+    if N > C:
+        raise ValueError("PlanktonModel: number of individuals exceeds max_individuals")
+    d = empty_individuals(C)
+    for k in ("Sz", "Bm", "Cq", "Nq", "Pq"):
+        del d[k]
+    ac = np.zeros(C, dtype=bool)
+    ac[:N] = True
+    var, C_DNA, Nsuper = (species_param(p, k, s) for k in ("var", "C_DNA", "Nsuper"))
+    RNA2DNA, PRO2DNA, CH2DNA, Chl2DNA = (species_param(p, k, s) for k in ("RNA2DNA", "PRO2DNA", "CH2DNA", "Chl2DNA"))
+    DNA, RNA, PRO = rng.random(C), rng.random(C), rng.random(C)
+    x, y, z = rng.random(C), rng.random(C), rng.random(C)
+    CH, NST, PST = rng.random(C), rng.random(C), rng.random(C)
+    d["ac"] = ac
+    d["gen"][:N] = 1.0
+    DNA = DNA * var + 1.0
+    RNA = RNA * var * 2.0 + 1.0 - var
+    PRO = PRO * var * 2.0 + 1.0 - var
+    CH = CH * var * 2.0 + 1.0 - var
+    NST = NST * var * 2.0 + 1.0 - var
+    PST = PST * var * 2.0 + 1.0 - var
+    d["x"] = (x * grid.Nx) * ac
+    d["y"] = (y * grid.Ny) * ac
+    d["z"] = (z * grid.Nz) * ac
+    d["DNA"] = DNA * C_DNA * Nsuper * ac
+    d["RNA"] = RNA * C_DNA * Nsuper * ac * RNA2DNA
+    d["PRO"] = PRO * C_DNA * Nsuper * ac * PRO2DNA
+    d["CH"] = CH * d["DNA"] * CH2DNA
+    d["NST"] = NST * d["CH"] * np.float32(16.0) / np.float32(106.0)
+    d["PST"] = PST * d["CH"] / np.float32(106.0)
+    d["Chl"] = d["DNA"] * Chl2DNA * np.float32(893.49) / 55.0
+    mask_individuals(d, grid, N)
+    return d
+
+
 def mask_individuals(d, grid, N):
     """mask_individuals! (Individuals/utils.jl:89-100)."""
     ac = d["ac"][:N]

@@ -5,8 +5,8 @@ import numpy as np
 from . import _abi, _lib
 from ._abi import NTRACERS, PI_FP32, PI_FP64, tracer_names
 from ._native import CModel
-from .architectures import GPU, CarbonMode, QuotaMode
-from .init import generate_tracers, initialize_plankton, initialize_plankton_carbon
+from .architectures import GPU, CarbonMode, MacroMolecularMode, QuotaMode
+from .init import generate_tracers, initialize_plankton, initialize_plankton_carbon, initialize_plankton_macro
 from .parameters import (bgc_params_default, default_tracer_init, phyt_params_default,
                          update_bgc_params, update_phyt_params)
 
@@ -64,9 +64,12 @@ class PlanktonModel:
             raise ValueError("PlanktonModel: this implementation runs on GPU() only (no CPU fallback)")
         if mode is CarbonMode:
             mode = CarbonMode()
+        if mode is MacroMolecularMode:
+            mode = MacroMolecularMode()
         carbon = isinstance(mode, CarbonMode)
-        if mode is not None and not carbon and not isinstance(mode, QuotaMode) and mode is not QuotaMode:
-            raise NotImplementedError(f"{mode}: QuotaMode() and CarbonMode() are implemented")
+        macro = isinstance(mode, MacroMolecularMode)
+        if mode is not None and not carbon and not macro and not isinstance(mode, QuotaMode) and mode is not QuotaMode:
+            raise NotImplementedError(f"{mode}: QuotaMode(), CarbonMode() and MacroMolecularMode() are implemented")
         if abiotic is not None:
             raise NotImplementedError("abiotic particles are not implemented")
         FT = np.dtype(FT).type
@@ -74,11 +77,13 @@ class PlanktonModel:
             raise ValueError("FT must be Float32 or Float64")
         if carbon and FT is not np.float64:
             raise NotImplementedError("CarbonMode() is built in the FP64 form: use FT = Float64")
+        if macro and FT is not np.float64:
+            raise NotImplementedError("MacroMolecularMode() is built in the FP64 form: use FT = Float64")
         if getattr(grid, "is_latlon", False) and FT is not np.float64:
             raise NotImplementedError("LatLonGrid is built in the FP64 form: use FT = Float64")
         self.FT = FT
         self.arch = GPU()
-        self.mode = mode if carbon else QuotaMode()
+        self.mode = mode if (carbon or macro) else QuotaMode()
         self.grid = grid
         self.max_candidates = max_candidates
         if bgc_params is None:
@@ -111,10 +116,10 @@ class PlanktonModel:
         lib = _lib.load()
         precision = PI_FP64 if FT is np.float64 else PI_FP32
         self._native = CModel(lib, "pi_", grid, bgc_final, phyto.params, nsp, max_individuals,
-                              seed, precision=precision, mode="carbon" if carbon else "quota")
+                              seed, precision=precision, mode="carbon" if carbon else "macro" if macro else "quota")
         if initial_state is None:
             rng = np.random.default_rng(seed)
-            init = initialize_plankton_carbon if carbon else initialize_plankton
+            init = initialize_plankton_carbon if carbon else initialize_plankton_macro if macro else initialize_plankton
             inds = [init(grid, phyto.params, s, phyto.N[s], max_individuals, rng) for s in range(nsp)]
             trs = generate_tracers(grid, tracer_initial or default_tracer_init(), rng)
         else:
@@ -158,8 +163,9 @@ class PlanktonDiagnostics:
     (diagnostics_struct.jl:23-105). The default diagnostics (PAR and num/graz/mort/dvid per
     species) and the requested ones — tracer fields (any of the 14 tracer names) and the mode's
     processes (QuotaMode: PS, BS, VDOC, VNH4, VNO3, VPO4, resp, exu, Bm, Cq, Nq, Pq, Chl; CarbonMode:
-    PS, BS, RP, RS, TD, Bm, Bd, Chl) — are accumulated on the device by every step; fields download
-    on access."""
+    PS, BS, RP, RS, TD, Bm, Bd, Chl; MacroMolecularMode: PS, VDOC, VNH4, VNO3, VPO4, resp, ρChl,
+    S_PRO, S_DNA, S_RNA, exu, CH, NST, PST, PRO, DNA, RNA, Chl, of which VNH4 and exu stay zero as
+    in the reference) — are accumulated on the device by every step; fields download on access."""
 
     DEFAULT = ("num", "graz", "mort", "dvid", "ptc")
 
@@ -168,7 +174,8 @@ class PlanktonDiagnostics:
         if not isinstance(tracer, tuple) or not isinstance(phytoplankton, tuple):
             raise ValueError("tracer and phytoplankton must be Tuples")
         # diag_avail (diagnostics_struct.jl:115-136): names available for the model's mode
-        proc_names = _abi.CARBON_PROC_NAMES if isinstance(model.mode, CarbonMode) else _abi.PROC_NAMES
+        proc_names = (_abi.CARBON_PROC_NAMES if isinstance(model.mode, CarbonMode) else
+                      _abi.MACRO_PROC_NAMES if isinstance(model.mode, MacroMolecularMode) else _abi.PROC_NAMES)
         for t in tracer:
             if t not in tracer_names and t != "PAR":
                 raise ValueError(f"{t} is not one of the diagnostics")

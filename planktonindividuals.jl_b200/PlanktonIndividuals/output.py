@@ -159,7 +159,11 @@ def write_output_b(writer, model, diags):
     t, it = model.t, model.iteration
     phytos = model.individuals.phytos
     if writer.write_log:
-        from .architectures import CarbonMode
+        from .architectures import CarbonMode, MacroMolecularMode
+        if isinstance(getattr(model, "mode", None), MacroMolecularMode):
+            # the reference defines write_species_dynamics for QuotaMode, IronEnergyMode and
+            # CarbonMode only (write_outputs.jl:98-157)
+            raise ValueError("write_species_dynamics has no method for MacroMolecularMode (use write_log = false)")
         write_species_dynamics(t, phytos, writer.filepath, carbon=isinstance(getattr(model, "mode", None), CarbonMode))
     if writer.save_diags and it % diags.iteration_interval == 0:
         if _filesize(writer.diags_file) >= writer.max_filesize:

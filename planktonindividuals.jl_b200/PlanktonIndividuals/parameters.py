@@ -54,9 +54,25 @@ def bgc_params_default(FT=np.float32):
 
 
 def phyt_params_default(N=1, mode=None):
-    """phyt_params_default(N, QuotaMode()) (param_default.jl:235-284) or, for CarbonMode(),
-    param_default.jl:290-320; one list entry per species."""
-    from .architectures import CarbonMode
+    """phyt_params_default(N, QuotaMode()) (param_default.jl:235-284), for CarbonMode()
+    param_default.jl:290-320, for MacroMolecularMode() param_default.jl:94-141; one list entry per
+    species."""
+    from .architectures import CarbonMode, MacroMolecularMode
+    if isinstance(mode, MacroMolecularMode) or mode is MacroMolecularMode:
+        params = {
+            "Nsuper": [1], "C_DNA": [1.8e-13], "var": [0.3], "RNA2DNA": [1.73], "PRO2DNA": [34.83],
+            "CH2DNA": [23.3], "Chl2DNA": [3.45], "α": [2.0e-2], "Φ": [4.0e-5], "Topt": [27.0],
+            "Tmax": [30.0], "Ea": [5.3e4], "PCmax": [6.2e-5], "VDOCmax": [0.0], "VNH4max": [6.9e-6],
+            "VNO3max": [6.9e-6], "VPO4max": [1.2e-6], "KsatNH4": [0.005], "KsatNO3": [0.010],
+            "KsatPO4": [0.003], "KsatDOC": [0.0], "NSTmax": [0.12], "PSTmax": [0.70], "CHmax": [0.4],
+            "respir": [1.2e-6], "k_pro": [6.0e-5], "k_sat_pro": [4.5e-13], "k_dna": [1.6e-7],
+            "k_sat_dna": [1.0e-15], "k_rna": [3.0e-7], "k_sat_rna": [1.0e-12], "Chl2N": [3.0],
+            "R_NC_PRO": [1 / 4.5], "R_NC_DNA": [1 / 2.9], "R_PC_DNA": [1 / 11.1], "R_NC_RNA": [1 / 2.8],
+            "R_PC_RNA": [1 / 10.7], "dvid_P": [1.0e-5], "grz_P": [0.0], "mort_P": [5e-5],
+            "mort_reg": [0.5], "grazFracC": [0.7], "grazFracN": [0.7], "grazFracP": [0.7],
+            "mortFracC": [0.5], "mortFracN": [0.5], "mortFracP": [0.5],
+        }
+        return params if N == 1 else {k: [v[0]] * N for k, v in params.items()}
     if isinstance(mode, CarbonMode) or mode is CarbonMode:
         params = {
             "Nsuper": [1], "Cquota": [1.8e-11], "mean": [1.2], "var": [0.3], "Chl2C": [0.10],

@@ -49,7 +49,7 @@ class Workload:
     dT_temp: float
     seed: int
     meta: dict = field(default_factory=dict)
-    mode: str = "quota"           # physiology: "quota" (QuotaMode) or "carbon" (CarbonMode)
+    mode: str = "quota"           # physiology: "quota" (QuotaMode), "carbon" (CarbonMode) or "macro"
 
     def velocity(self, t):
         return self.vel_fn(t)
@@ -268,6 +268,30 @@ def carbon(nx=16, nz=8, N_per_species=2000, nsp=2, steps=30, dT=60.0, seed=11, n
     n_vel = int(np.ceil(steps / 60)) + 1
     return Workload("carbon", grid, bgc, phyt, nsp, C, [N_per_species] * nsp, inds, trs, dT, steps,
                     60 * dT, n_vel, vel, parf, 3600.0, tmp, 3600.0, seed, mode="carbon")
+
+
+def macro(nx=16, nz=8, N_per_species=2000, nsp=2, steps=30, dT=60.0, seed=13, nmodes=16,
+          capacity=None, phyt_over=None, bgc_over=None):
+    """MacroMolecularMode workload on a config-2-like 3D grid (nx×nx×nz, 50 m × 50 m × 2 m):
+    individuals from MacroMolecularMode's initialize_plankton! rule, random-Fourier velocity,
+    default temperature and a diel light cycle."""
+    from .architectures import MacroMolecularMode
+    from .init import initialize_plankton_macro
+    rng = np.random.default_rng(seed)
+    grid = RectilinearGrid(size=(nx, nx, nz), x=(0.0, nx * 50.0), y=(0.0, nx * 50.0),
+                           z=(0.0, -2.0 * nz), FT=np.float64, topology=(Periodic, Periodic, Bounded))
+    vel = FourierVelocity(grid, nmodes=nmodes, rms=0.05, seed=seed)
+    C = capacity or 2 * N_per_species
+    bgc = update_bgc_params(bgc_over or {}, np.float64)
+    phyt = update_phyt_params(phyt_over or {}, np.float64, N=nsp, mode=MacroMolecularMode())
+    inds = [initialize_plankton_macro(grid, phyt, s, N_per_species, C, rng) for s in range(nsp)]
+    trs = make_tracers(grid, rng, no3_gradient_depth=2.0 * nz)
+    hours = int(np.ceil(steps * dT / 3600.0)) + 1
+    parf = diel_parf(grid.Nx, grid.Ny, hours)
+    tmp = default_temperature(grid, dT, steps)
+    n_vel = int(np.ceil(steps / 60)) + 1
+    return Workload("macro", grid, bgc, phyt, nsp, C, [N_per_species] * nsp, inds, trs, dT, steps,
+                    60 * dT, n_vel, vel, parf, 3600.0, tmp, 3600.0, seed, mode="macro")
 
 
 def latlon_streamfunction_velocity(grid, cfl=0.2, dT=600.0, seed=0):

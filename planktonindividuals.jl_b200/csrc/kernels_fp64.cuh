@@ -21,25 +21,30 @@ __device__ __forceinline__ int clamp_idx(long long v, int lo, int hi, uint32_t* 
 
 __device__ __forceinline__ double dzF1(const DGrid& g, int k) { return g.dzF[k - 1]; }
 __device__ __forceinline__ double dzC1(const DGrid& g, int k) { return g.dzC[k - 1]; }
-// Grids/areas_volumes_spacings.jl:9-38 with 1-based halo-inclusive indices: a RectilinearGrid
-// forms them from Δx, Δy and dzF (in the reference's operation order), a LatLonGrid reads its arrays
+// Grids/areas_volumes_spacings.jl:9-38 with 1-based halo-inclusive indices. LL = false: a
+// RectilinearGrid, whose metrics are formed from Δx, Δy and dzF in the reference's operation order;
+// LL = true: a LatLonGrid, whose arrays are read. The kernels that use them are instantiated for
+// both, so the RectilinearGrid code reads no metric array.
 __device__ __forceinline__ int gidx2(const DGrid& g, int i, int j) { return (i - 1) + g.Gx * (j - 1); }
-__device__ __forceinline__ double vol(const DGrid& g, int i, int j, int k) {
-    return g.mVol ? g.mVol[(i - 1) + (long long)g.Gx * ((j - 1) + (long long)g.Gy * (k - 1))] : g.dx * g.dy * dzF1(g, k);
+__device__ __forceinline__ long long gidx3l(const DGrid& g, int i, int j, int k) {
+    return (i - 1) + (long long)g.Gx * ((j - 1) + (long long)g.Gy * (k - 1));
 }
+template <bool LL> __device__ __forceinline__ double vol(const DGrid& g, int i, int j, int k) {
+    return LL ? g.mVol[gidx3l(g, i, j, k)] : g.dx * g.dy * dzF1(g, k);
+}
+template <bool LL> __device__ __forceinline__ double Axm(const DGrid& g, int i, int j, int k) {
+    return LL ? g.mAx[gidx3l(g, i, j, k)] : g.dy * dzF1(g, k);
+}
+template <bool LL> __device__ __forceinline__ double Aym(const DGrid& g, int i, int j, int k) {
+    return LL ? g.mAy[gidx3l(g, i, j, k)] : g.dx * dzF1(g, k);
+}
+template <bool LL> __device__ __forceinline__ double Azm(const DGrid& g, int i, int j) { return LL ? g.mAz[gidx2(g, i, j)] : g.dx * g.dy; }
+template <bool LL> __device__ __forceinline__ double dxCm(const DGrid& g, int i, int j) { return LL ? g.mdxC[gidx2(g, i, j)] : g.dx; }
+template <bool LL> __device__ __forceinline__ double dyCm(const DGrid& g, int i, int j) { return LL ? g.mdyC[gidx2(g, i, j)] : g.dy; }
+template <bool LL> __device__ __forceinline__ double dxFm(const DGrid& g, int i, int j) { return LL ? g.mdxF[gidx2(g, i, j)] : g.dx; }
+template <bool LL> __device__ __forceinline__ double dyFm(const DGrid& g, int i, int j) { return LL ? g.mdyF[gidx2(g, i, j)] : g.dy; }
 // volume of a RectilinearGrid cell at level k (pi_tracer_advection_noalloc takes only these)
 __device__ __forceinline__ double vol(const DGrid& g, int k) { return g.dx * g.dy * dzF1(g, k); }
-__device__ __forceinline__ double Axm(const DGrid& g, int i, int j, int k) {
-    return g.mAx ? g.mAx[(i - 1) + (long long)g.Gx * ((j - 1) + (long long)g.Gy * (k - 1))] : g.dy * dzF1(g, k);
-}
-__device__ __forceinline__ double Aym(const DGrid& g, int i, int j, int k) {
-    return g.mAy ? g.mAy[(i - 1) + (long long)g.Gx * ((j - 1) + (long long)g.Gy * (k - 1))] : g.dx * dzF1(g, k);
-}
-__device__ __forceinline__ double Azm(const DGrid& g, int i, int j) { return g.mAz ? g.mAz[gidx2(g, i, j)] : g.dx * g.dy; }
-__device__ __forceinline__ double dxCm(const DGrid& g, int i, int j) { return g.mdxC ? g.mdxC[gidx2(g, i, j)] : g.dx; }
-__device__ __forceinline__ double dyCm(const DGrid& g, int i, int j) { return g.mdyC ? g.mdyC[gidx2(g, i, j)] : g.dy; }
-__device__ __forceinline__ double dxFm(const DGrid& g, int i, int j) { return g.mdxF ? g.mdxF[gidx2(g, i, j)] : g.dx; }
-__device__ __forceinline__ double dyFm(const DGrid& g, int i, int j) { return g.mdyF ? g.mdyF[gidx2(g, i, j)] : g.dy; }
 __device__ __forceinline__ int lmask(const DGrid& g, int i, int j, int k) {
     return g.all_water ? 1 : (int)g.lm[gidx(g, i, j, k)];
 }
@@ -65,7 +70,7 @@ __device__ __forceinline__ double bc_pos(double x, double xr, int topo) {
 
 // Trilinear interpolation in grid-index units (u_itpl/v_itpl/w_itpl). HALF = 1 samples
 // vel½ = (vel₀ + vel₁) * 0.5 corner by corner, which is the array time_step.jl:17-19 builds.
-template <int COMP, int HALF>
+template <int COMP, int HALF, bool LL>
 __device__ __forceinline__ double itpl(const DGrid& g, const double* __restrict__ f0,
                                        const double* __restrict__ f1, double x, double y,
                                        double z, int ac, uint32_t* err) {
@@ -92,7 +97,7 @@ __device__ __forceinline__ double itpl(const DGrid& g, const double* __restrict_
     double w111 = xd * yd * zd;
     // each corner divided by ΔxC, ΔyC or ΔzC at that corner (interpolation.jl:23-50)
     auto D = [&](int a, int b, int c) -> double {
-        return COMP == 0 ? dxCm(g, i + a, j + b) : COMP == 1 ? dyCm(g, i + a, j + b) : dzC1(g, k + c);
+        return COMP == 0 ? dxCm<LL>(g, i + a, j + b) : COMP == 1 ? dyCm<LL>(g, i + a, j + b) : dzC1(g, k + c);
     };
     return w000 * c000 / D(0, 0, 0) + w001 * c001 / D(0, 0, 1) + w010 * c010 / D(0, 1, 0) + w011 * c011 / D(0, 1, 1)
          + w100 * c100 / D(1, 0, 0) + w101 * c101 / D(1, 0, 1) + w110 * c110 / D(1, 1, 0) + w111 * c111 / D(1, 1, 1);
@@ -117,6 +122,7 @@ struct VelPtrs { const double *u0, *v0, *w0, *uh, *vh, *wh, *u1, *v1, *w1; };
 
 // RK4 + diffusion + find_inds! of one active individual; writes its position, packed cell, binning
 // key and count.
+template <bool LL>
 __device__ __forceinline__ void particle_step(const DGrid& g, const SpcDev& P, int s, long long slot,
                                               long long gid, double dT, uint64_t seed, uint32_t iter,
                                               const VelPtrs& vel, double kappa_h, double kappa_v,
@@ -129,36 +135,36 @@ __device__ __forceinline__ void particle_step(const DGrid& g, const SpcDev& P, i
     const double X = P.x[slot], Y = P.y[slot], Z = P.z[slot];
     const double NX = (double)g.Nx, NY = (double)g.Ny, NZ = (double)g.Nz;
     // stage 1 at vel₀
-    double u1 = jl_mulb(itpl<0, 0>(g, vel.u0, vel.u0, X, Y, Z, ac, err), ac);
-    double v1 = jl_mulb(itpl<1, 0>(g, vel.v0, vel.v0, X, Y, Z, ac, err), ac);
-    double w1 = jl_mulb(itpl<2, 0>(g, vel.w0, vel.w0, X, Y, Z, ac, err), ac);
+    double u1 = jl_mulb(itpl<0, 0, LL>(g, vel.u0, vel.u0, X, Y, Z, ac, err), ac);
+    double v1 = jl_mulb(itpl<1, 0, LL>(g, vel.v0, vel.v0, X, Y, Z, ac, err), ac);
+    double w1 = jl_mulb(itpl<2, 0, LL>(g, vel.w0, vel.w0, X, Y, Z, ac, err), ac);
     double u2 = u1, v2 = v1, w2 = w1;
     double vx = X + jl_mulb(0.5 * u1 * dT, ac);
     double vy = Y + jl_mulb(0.5 * v1 * dT, ac);
     double vz = Z - jl_mulb(0.5 * w1 * dT, ac);
     vx = jl_mulb(bc_pos(vx, NX, g.tx), ac); vy = jl_mulb(bc_pos(vy, NY, g.ty), ac); vz = jl_mulb(bc_pos(vz, NZ, g.tz), ac);
     // stage 2 at vel½
-    u1 = jl_mulb(itpl<0, 0>(g, vel.uh, vel.uh, vx, vy, vz, ac, err), ac);
-    v1 = jl_mulb(itpl<1, 0>(g, vel.vh, vel.vh, vx, vy, vz, ac, err), ac);
-    w1 = jl_mulb(itpl<2, 0>(g, vel.wh, vel.wh, vx, vy, vz, ac, err), ac);
+    u1 = jl_mulb(itpl<0, 0, LL>(g, vel.uh, vel.uh, vx, vy, vz, ac, err), ac);
+    v1 = jl_mulb(itpl<1, 0, LL>(g, vel.vh, vel.vh, vx, vy, vz, ac, err), ac);
+    w1 = jl_mulb(itpl<2, 0, LL>(g, vel.wh, vel.wh, vx, vy, vz, ac, err), ac);
     u2 = u2 + u1 * 2.0; v2 = v2 + v1 * 2.0; w2 = w2 + w1 * 2.0;
     vx = X + jl_mulb(0.5 * u1 * dT, ac);
     vy = Y + jl_mulb(0.5 * v1 * dT, ac);
     vz = Z - jl_mulb(0.5 * w1 * dT, ac);
     vx = jl_mulb(bc_pos(vx, NX, g.tx), ac); vy = jl_mulb(bc_pos(vy, NY, g.ty), ac); vz = jl_mulb(bc_pos(vz, NZ, g.tz), ac);
     // stage 3 at vel½
-    u1 = jl_mulb(itpl<0, 0>(g, vel.uh, vel.uh, vx, vy, vz, ac, err), ac);
-    v1 = jl_mulb(itpl<1, 0>(g, vel.vh, vel.vh, vx, vy, vz, ac, err), ac);
-    w1 = jl_mulb(itpl<2, 0>(g, vel.wh, vel.wh, vx, vy, vz, ac, err), ac);
+    u1 = jl_mulb(itpl<0, 0, LL>(g, vel.uh, vel.uh, vx, vy, vz, ac, err), ac);
+    v1 = jl_mulb(itpl<1, 0, LL>(g, vel.vh, vel.vh, vx, vy, vz, ac, err), ac);
+    w1 = jl_mulb(itpl<2, 0, LL>(g, vel.wh, vel.wh, vx, vy, vz, ac, err), ac);
     u2 = u2 + u1 * 2.0; v2 = v2 + v1 * 2.0; w2 = w2 + w1 * 2.0;
     vx = X + jl_mulb(1.0 * u1 * dT, ac);
     vy = Y + jl_mulb(1.0 * v1 * dT, ac);
     vz = Z - jl_mulb(1.0 * w1 * dT, ac);
     vx = jl_mulb(bc_pos(vx, NX, g.tx), ac); vy = jl_mulb(bc_pos(vy, NY, g.ty), ac); vz = jl_mulb(bc_pos(vz, NZ, g.tz), ac);
     // stage 4 at vel₁
-    u1 = jl_mulb(itpl<0, 0>(g, vel.u1, vel.u1, vx, vy, vz, ac, err), ac);
-    v1 = jl_mulb(itpl<1, 0>(g, vel.v1, vel.v1, vx, vy, vz, ac, err), ac);
-    w1 = jl_mulb(itpl<2, 0>(g, vel.w1, vel.w1, vx, vy, vz, ac, err), ac);
+    u1 = jl_mulb(itpl<0, 0, LL>(g, vel.u1, vel.u1, vx, vy, vz, ac, err), ac);
+    v1 = jl_mulb(itpl<1, 0, LL>(g, vel.v1, vel.v1, vx, vy, vz, ac, err), ac);
+    w1 = jl_mulb(itpl<2, 0, LL>(g, vel.w1, vel.w1, vx, vy, vz, ac, err), ac);
     u2 = u2 + u1; v2 = v2 + v1; w2 = w2 + w1;
     u2 = u2 / 6.0; v2 = v2 / 6.0; w2 = w2 / 6.0;
     double x = X + jl_mulb(1.0 * u2 * dT, ac);
@@ -172,8 +178,8 @@ __device__ __forceinline__ void particle_step(const DGrid& g, const SpcDev& P, i
     // ΔxC/ΔyC at (xi+Hx, yi+Hy) of the stored indices (particle_diffusion.jl:4-5); the reference
     // reads past the metric array there when x = Nx exactly, which is held at the last column here
     const int dxi = min(max(oxi + g.Hx, 1), g.Gx), dyi = min(max(oyi + g.Hy, 1), g.Gy);
-    r0 = r0 * sqrt(kappa_h * dT) / dxCm(g, dxi, dyi);
-    r1 = r1 * sqrt(kappa_h * dT) / dyCm(g, dxi, dyi);
+    r0 = r0 * sqrt(kappa_h * dT) / dxCm<LL>(g, dxi, dyi);
+    r1 = r1 * sqrt(kappa_h * dT) / dyCm<LL>(g, dxi, dyi);
     r2 = r2 * sqrt(kappa_v * dT) / dzC1(g, kdz);
     x = x + jl_mulb(r0, ac); y = y + jl_mulb(r1, ac); z = z + jl_mulb(r2, ac);
     x = jl_mulb(bc_pos(x, NX, g.tx), ac); y = jl_mulb(bc_pos(y, NY, g.ty), ac); z = jl_mulb(bc_pos(z, NZ, g.tz), ac);
@@ -192,6 +198,7 @@ __device__ __forceinline__ void particle_step(const DGrid& g, const SpcDev& P, i
 // their positions end as zeros and their cell is (Hx, Hy, Hz)), and active individuals that were
 // not binned in the previous step (new daughters, uploaded state). The others are moved by
 // k_particles_sorted in cell order.
+template <bool LL>
 __global__ void k_particles(DGrid g, const SpcDev* __restrict__ spc, int nsp, long long C,
                             double dT, uint64_t seed, uint32_t iter, VelPtrs vel,
                             double kappa_h, double kappa_v, uint32_t* __restrict__ cnt,
@@ -214,11 +221,12 @@ __global__ void k_particles(DGrid g, const SpcDev* __restrict__ spc, int nsp, lo
         return;
     }
     if (P.stat[slot] & ST_AC0) return;                // moved by k_particles_sorted
-    particle_step(g, P, s, slot, gid, dT, seed, iter, vel, kappa_h, kappa_v, cnt, key, err);
+    particle_step<LL>(g, P, s, slot, gid, dT, seed, iter, vel, kappa_h, kappa_v, cnt, key, err);
 }
 
 // Cell-order pass: the individuals binned in the previous step (prev_sorted[0 .. off[G]), which
 // were active then) that are still active. Neighbouring threads interpolate in neighbouring cells.
+template <bool LL>
 __global__ void k_particles_sorted(DGrid g, const SpcDev* __restrict__ spc, long long C,
                                    const uint32_t* __restrict__ prev_sorted,
                                    const uint32_t* __restrict__ prev_off, long long Gcells,
@@ -233,7 +241,7 @@ __global__ void k_particles_sorted(DGrid g, const SpcDev* __restrict__ spc, long
     long long slot = gd - (long long)s * C;
     const SpcDev& P = spc[s];
     if (!(P.flags[slot] & FL_AC) || !(P.stat[slot] & ST_AC0)) return;
-    particle_step(g, P, s, slot, gd, dT, seed, iter, vel, kappa_h, kappa_v, cnt, key, err);
+    particle_step<LL>(g, P, s, slot, gd, dT, seed, iter, vel, kappa_h, kappa_v, cnt, key, err);
 }
 
 // pos[gid] = position of gid in the cell-sorted entry list.
@@ -251,6 +259,7 @@ __global__ void k_setpos(const uint32_t* __restrict__ off, long long G,
 // of acc_chl! (utils.jl:33-36) summed per cell in species-then-slot order, and
 // diags.tracer.PAR .+= par (time_step.jl:167).
 // ------------------------------------------------------------------------------------------
+template <bool LL>
 __global__ void k_par(DGrid g, const SpcDev* __restrict__ spc, long long C,
                       const uint32_t* __restrict__ off, const uint32_t* __restrict__ gid_sorted,
                       double* __restrict__ PARF, const double* __restrict__ PARF_src,
@@ -272,7 +281,7 @@ __global__ void k_par(DGrid g, const SpcDev* __restrict__ spc, long long C,
             int s = (int)(gd / C);
             chl += spc[s].Chl[gd - (long long)s * C];
         }
-        double atten = (chl / vol(g, ii, jj, kk) * kc + kw) * dzF1(g, kk);
+        double atten = (chl / vol<LL>(g, ii, jj, kk) * kc + kw) * dzF1(g, kk);
         double e = pi_exp(-atten);
         double pv = parf * (1.0 - e) / atten;
         par[c] = pv;
@@ -287,14 +296,28 @@ __global__ void k_par(DGrid g, const SpcDev* __restrict__ spc, long long C,
 //     consume_loss.jl:17-26, Diagnostics/diagnostics_kernels.jl:4-7
 // ------------------------------------------------------------------------------------------
 
+// total_C/N/P_biomass (MacroMolecularMode/plankton_generation.jl:82-93)
+__host__ __device__ __forceinline__ double m_totC(double PRO, double DNA, double RNA, double CH, double Chl) {
+    return PRO + DNA + RNA + CH + Chl / F_CHL * 55.0;
+}
+__host__ __device__ __forceinline__ double m_totN(double PRO, double DNA, double RNA, double NST, double Chl,
+                                                  const pi_macro_params& p) {
+    return PRO * p.R_NC_PRO + DNA * p.R_NC_DNA + RNA * p.R_NC_RNA + NST + Chl / F_CHL * 4.0;
+}
+__host__ __device__ __forceinline__ double m_totP(double DNA, double RNA, double PST, const pi_macro_params& p) {
+    return DNA * p.R_PC_DNA + RNA * p.R_PC_RNA + PST;
+}
+
 // Applies last step's grazing/mortality decisions, writes the loss contributions of the
 // individuals lost, the division/free flags for the slot scan and the graz/mort/dvid diags.
-// carbon: CarbonMode losses (CarbonMode/consume_loss.jl:12-16): DOC and POC from Bm only.
-__global__ void k_decide(DGrid g, SpcDev P, pi_quota_params p, long long C, int s,
+// mode MODE_CARBON: CarbonMode losses (CarbonMode/consume_loss.jl:12-16), DOC and POC from Bm only;
+// MODE_MACRO: MacroMolecularMode losses (MacroMolecularMode/consume_loss.jl:14-24) from the total
+// C, N and P biomass (mp holds its R_NC_* and R_PC_* ratios).
+__global__ void k_decide(DGrid g, SpcDev P, pi_quota_params p, pi_macro_params mp, long long C, int s,
                          const int32_t* __restrict__ pos, double* __restrict__ loss,
                          uint8_t* __restrict__ evk, unsigned long long* __restrict__ flag64,
                          double* __restrict__ d_graz, double* __restrict__ d_mort,
-                         double* __restrict__ d_dvid, uint32_t* err, int carbon) {
+                         double* __restrict__ d_dvid, uint32_t* err, int mode) {
     long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= C) return;
     if (*err & PI_DEVERR_CAPACITY) return;
@@ -319,11 +342,21 @@ __global__ void k_decide(DGrid g, SpcDev P, pi_quota_params p, long long C, int 
             double fN = kind == 1 ? p.grazFracN : p.mortFracN;
             double fP = kind == 1 ? p.grazFracP : p.mortFracP;
             double* L = loss + e * 6;
-            if (carbon) {
+            if (mode == MODE_CARBON) {
                 const double Bm = P.Bm[slot];
                 L[0] = jl_mulb(Bm * fC, 1) * 1.0;                     // DOC
                 L[3] = jl_mulb(Bm * (1.0 - fC), 1) * 1.0;             // POC
                 L[1] = 0.0; L[2] = 0.0; L[4] = 0.0; L[5] = 0.0;
+            } else if (mode == MODE_MACRO) {
+                const double tC = m_totC(P.PRO[slot], P.DNA[slot], P.RNA[slot], P.CH[slot], P.Chl[slot]);
+                const double tN = m_totN(P.PRO[slot], P.DNA[slot], P.RNA[slot], P.NST[slot], P.Chl[slot], mp);
+                const double tP = m_totP(P.DNA[slot], P.RNA[slot], P.PST[slot], mp);
+                L[0] = jl_mulb(tC * fC, 1) * 1.0;                     // DOC
+                L[1] = jl_mulb(tN * fN, 1) * 1.0;                     // DON
+                L[2] = jl_mulb(tP * fP, 1) * 1.0;                     // DOP
+                L[3] = jl_mulb(tC * (1.0 - fC), 1) * 1.0;             // POC
+                L[4] = jl_mulb(tN * (1.0 - fN), 1) * 1.0;             // PON
+                L[5] = jl_mulb(tP * (1.0 - fP), 1) * 1.0;             // POP
             } else {
             double Bm = P.Bm[slot], Cq = P.Cq[slot], Nq = P.Nq[slot], Pq = P.Pq[slot];
             L[0] = jl_mulb((Bm + Cq) * fC, 1) * 1.0;                  // DOC
@@ -373,13 +406,26 @@ __global__ void k_lists(const unsigned long long* __restrict__ flag64,
 // not — the daughter halves the damaged biomass its slot held before.
 __global__ void k_daughters(SpcDev P, const int32_t* __restrict__ divlist,
                             const int32_t* __restrict__ freelist, const uint32_t* ndiv,
-                            const uint32_t* err, int carbon) {
+                            const uint32_t* err, int mode) {
     if (*err & PI_DEVERR_CAPACITY) return;
     uint32_t n = *ndiv;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         long long p = divlist[k], d = freelist[k];
         const double h = (2.0 - 1.0) / 2.0;
-        if (carbon) {
+        if (mode == MODE_MACRO) {
+            // MacroMolecularMode/division_death.jl:28-62: the seven pools, x, y, z and gen are
+            // copied and halved in both (not age)
+            double* pools[7] = { P.PRO, P.DNA, P.RNA, P.CH, P.NST, P.PST, P.Chl };
+            const double gen = P.gen[p];
+            P.x[d] = P.x[p]; P.y[d] = P.y[p]; P.z[d] = P.z[p];
+#pragma unroll
+            for (int q = 0; q < 7; ++q) { const double v = pools[q][p] * h; pools[q][d] = v; pools[q][p] = v; }
+            P.gen[d] = gen + 1.0; P.age[d] = P.age[d] * (1.0 - 1.0);
+            P.flags[d] = FL_AC | FL_DVID;
+            P.gen[p] = gen + 1.0; P.age[p] = P.age[p] * (1.0 - 1.0);
+            continue;
+        }
+        if (mode == MODE_CARBON) {
             double Sz = P.Sz[p], Bm = P.Bm[p], Chl = P.Chl[p], gen = P.gen[p];
             P.x[d] = P.x[p]; P.y[d] = P.y[p]; P.z[d] = P.z[p];
             P.Sz[d] = Sz * h; P.Bm[d] = Bm * h; P.Bd[d] = P.Bd[d] * h; P.Chl[d] = Chl * h;
@@ -687,6 +733,145 @@ __global__ void k_physiology_carbon(DGrid g, SpcDev P, pi_carbon_params p, long 
     atomicAdd(&d_num[c], 1.0);
 }
 
+// ------------------------------------------------------------------------------------------
+// MacroMolecularMode physiology — MacroMolecularMode/plankton_growth.jl:2-28, growth_kernels.jl:1-200,
+// division_death_probability.jl:37-40, 49-52, 84-107, calc_consume! (consume_loss.jl:2-9)
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ double m_tempFunc_PS(double T, const pi_macro_params& p) {
+    double x = T - p.Topt, xmax = p.Tmax - p.Topt;
+    double regT = shape_dec(x, xmax, F_4em2, 4);
+    double k = pi_exp(-p.Ea / (F_RGAS * (T + F_T0))) * regT;
+    k = jl_max(0.0, k);
+    double OGT_rate = pi_exp(-p.Ea / (F_RGAS * (p.Topt + F_T0)));
+    return jl_min(1.0, k / OGT_rate);
+}
+__device__ __forceinline__ double m_tempFunc(double T, const pi_macro_params& p) {
+    double k = pi_exp(-p.Ea / (F_RGAS * (T + F_T0)));
+    k = jl_max(0.0, k);
+    double OGT_rate = pi_exp(-p.Ea / (F_RGAS * (p.Topt + F_T0)));
+    return jl_min(1.0, k / OGT_rate);
+}
+// Every slot is updated: the synthesis and exudation terms carry no ac, so the state of an
+// inactive slot keeps changing as in the reference, from zero light, temperature and nutrients
+// unless it was active when they were gathered (an individual grazed or dead in this step).
+__global__ void k_physiology_macro(DGrid g, SpcDev P, pi_macro_params p, long long C, int s,
+                                   double dT, uint64_t seed, uint32_t iter, int shared_graz,
+                                   const double* __restrict__ NH4f, const double* __restrict__ NO3f,
+                                   const double* __restrict__ PO4f, const double* __restrict__ DOCf,
+                                   const double* __restrict__ par, const double* __restrict__ temp,
+                                   const uint32_t* __restrict__ off, const uint32_t* __restrict__ gid_sorted,
+                                   const int32_t* __restrict__ pos, double* __restrict__ contrib,
+                                   double* __restrict__ d_num, double* __restrict__ procv, const uint32_t* err) {
+    long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= C) return;
+    if (*err & PI_DEVERR_CAPACITY) return;
+    const int ac = P.flags[slot] & FL_AC;
+    const int ac0 = P.stat[slot] & ST_AC0;
+    int c = -1;
+    double NH4 = 0.0, NO3 = 0.0, PO4 = 0.0, DOC = 0.0, parv = 0.0, T = 0.0, pop = 0.0;
+    if (ac0) {                                         // find_NPT! (utils.jl:14-25), × ac at gathering
+        int xi, yi, zi;
+        unpack_cell(g, P.cell[slot], xi, yi, zi);
+        c = gidx(g, xi, yi, zi);
+        NH4 = jl_max(0.0, NH4f[c]); NO3 = jl_max(0.0, NO3f[c]); PO4 = jl_max(0.0, PO4f[c]); DOC = jl_max(0.0, DOCf[c]);
+        parv = par[c]; T = temp[c];
+        if (shared_graz) {
+            pop = (double)(off[c + 1] - off[c]);
+        } else {
+            uint32_t n = 0;
+            for (uint32_t q = off[c]; q < off[c + 1]; ++q) n += (gid_sorted[q] / (uint32_t)C) == (uint32_t)s;
+            pop = (double)n;
+        }
+    }
+    double PRO = P.PRO[slot], DNA = P.DNA[slot], RNA = P.RNA[slot], CH = P.CH[slot];
+    double NST = P.NST[slot], PST = P.PST[slot], Chl = P.Chl[slot], age = P.age[slot];
+    // calc_inorganic_uptake_kernel! (growth_kernels.jl:45-54): calc_PS (:20-25), calc_NP_uptake (:28-42)
+    double aI = parv * p.alpha * p.Phi;
+    double PCm = p.PCmax * m_tempFunc_PS(T, p);
+    double PS = jl_mulb(PCm * (1.0 - pi_exp(-aI / jl_max(F_1em30, PCm) * Chl / jl_max(F_1em30, PRO))) * PRO, ac);
+    double R_NST = NST / jl_max(F_1em30, m_totN(PRO, DNA, RNA, NST, Chl, p));
+    double R_PST = PST / jl_max(F_1em30, m_totP(DNA, RNA, PST, p));
+    double regQN = shape_dec(R_NST, p.NSTmax, F_1em4, 4), regQP = shape_dec(R_PST, p.PSTmax, F_1em4, 4);
+    double VNH4 = jl_mulb(p.VNH4max * regQN * NH4 / jl_max(F_1em30, NH4 + p.KsatNH4) * m_tempFunc(T, p) * PRO, ac);
+    double VNO3 = jl_mulb(p.VNO3max * regQN * NO3 / jl_max(F_1em30, NO3 + p.KsatNO3) * m_tempFunc(T, p) * PRO, ac);
+    double VPO4 = jl_mulb(p.VPO4max * regQP * PO4 / jl_max(F_1em30, PO4 + p.KsatPO4) * m_tempFunc(T, p) * PRO, ac);
+    VNH4 = jl_min(VNH4, NH4 / dT / jl_max(1.0, pop));
+    VNO3 = jl_min(VNO3, NO3 / dT / jl_max(1.0, pop));
+    VPO4 = jl_min(VPO4, PO4 / dT / jl_max(1.0, pop));
+    // update_quotas_1_kernel! (:63-67)
+    CH += PS * dT; PST += VPO4 * dT; NST += (VNH4 + VNO3) * dT;
+    // calc_organic_uptake_kernel! (:82-90), calc_DOC_uptake (:73-80)
+    double R_CH = CH / jl_max(F_1em30, m_totC(PRO, DNA, RNA, CH, Chl));
+    double regQ = shape_dec(R_CH, p.CHmax, F_1em4, 4);
+    double VN = p.VDOCmax * regQ * DOC / jl_max(F_1em30, DOC + p.KsatDOC) * m_tempFunc(T, p) * PRO;
+    double VDOC = jl_mulb(jl_min(VN, DOC / dT / jl_max(1.0, pop)), ac);
+    VDOC = jl_mulb(VDOC, jl_isless(F_5em2, PS / (VDOC + PS)));
+    // calc_ρChl_kernel! (:98-103), calc_respir_kernel! (:111-114)
+    double rChl = jl_mulb(jl_mulb(PS / jl_max(F_1em30, PRO) / jl_max(F_1em30, parv * p.alpha * p.Phi * Chl / jl_max(F_1em30, PRO)),
+                                  jl_isless(F_1em1, parv)), ac);
+    double resp = jl_mulb(p.respir * PRO * m_tempFunc(T, p), ac);
+    // update_quotas_2_kernel! (:124-130)
+    CH = CH + (VDOC - resp) * dT;
+    PRO = PRO - jl_max(0.0, 0.0 - CH);
+    NST = NST + jl_max(0.0, 0.0 - CH) * p.R_NC_PRO;
+    CH = CH + jl_max(0.0, 0.0 - CH);
+    // calc_BS_kernel! (:136-152)
+    double tf = m_tempFunc(T, p);
+    double limit_PRO = jl_min(CH / (CH + p.k_sat_pro * p.Nsuper), NST / (NST + p.k_sat_pro * p.Nsuper * p.R_NC_PRO));
+    double limit_DNA = jl_min(jl_min(CH / (CH + p.k_sat_dna * p.Nsuper), NST / (NST + p.k_sat_dna * p.Nsuper * p.R_NC_DNA)),
+                              PST / (PST + p.k_sat_dna * p.Nsuper * p.R_PC_DNA));
+    double limit_RNA = jl_min(jl_min(CH / (CH + p.k_sat_rna * p.Nsuper), NST / (NST + p.k_sat_rna * p.Nsuper * p.R_NC_RNA)),
+                              PST / (PST + p.k_sat_rna * p.Nsuper * p.R_PC_RNA));
+    double S_PRO = p.k_pro * RNA * limit_PRO * tf;
+    double S_DNA = jl_mulb(p.k_dna * PRO * limit_DNA * tf, jl_isless(DNA / (p.C_DNA * p.Nsuper), 2.0));
+    double S_RNA = p.k_rna * PRO * limit_RNA * tf;
+    // update_biomass_kernel! (:159-171)
+    PRO += dT * S_PRO;
+    DNA += dT * S_DNA;
+    RNA += dT * S_RNA;
+    CH -= dT * (S_PRO + S_DNA + S_RNA + S_PRO * rChl);
+    NST -= dT * (S_PRO * p.R_NC_PRO + S_DNA * p.R_NC_DNA + S_RNA * p.R_NC_RNA + S_PRO * rChl * 4.0 / 55.0);
+    PST -= dT * (S_DNA * p.R_PC_DNA + S_RNA * p.R_PC_RNA);
+    Chl += dT * S_PRO * rChl * F_CHL / 55.0;
+    age += jl_mulb(dT / 3600.0, ac);
+    // calc_exudation_kernel! (:179-183), update_CH_kernel! (:190-193)
+    double exu = jl_max(0.0, CH - p.CHmax * m_totC(PRO, DNA, RNA, CH, Chl));
+    CH -= exu;
+    // calc_graz_quadratic!, calc_MM_mort!, calc_MM_dvid!, get_probability!
+    double graz = jl_mulb(pop * p.grz_P, ac);
+    double mort = jl_mulb(p.mort_P * shape_inc(age, p.mort_reg, F_1em4, 4), ac);
+    double dvid = jl_mulb(p.dvid_P, jl_isless(2.0, DNA / (p.C_DNA * p.Nsuper)));
+    double r0, r1, r2;
+    pi_draw3(seed, iter, (uint32_t)s, PI_DRAW_DECISION, (uint32_t)slot, &r0, &r1, &r2);
+    int dg = jl_isless(r0, graz * dT) && ac;
+    int dm = jl_isless(r1, mort * dT) && ac;
+    int dd = jl_isless(r2, dvid * dT) && ac;
+    P.PRO[slot] = PRO; P.DNA[slot] = DNA; P.RNA[slot] = RNA; P.CH[slot] = CH;
+    P.NST[slot] = NST; P.PST[slot] = PST; P.Chl[slot] = Chl; P.age[slot] = age;
+    P.flags[slot] = (uint8_t)((ac ? FL_AC : 0) | (dg ? FL_GRAZ : 0) | (dm ? FL_MORT : 0) | (dd ? FL_DVID : 0));
+    // calc_consume_kernel! (consume_loss.jl:2-9) for the individuals binned this step
+    if (ac0) {
+        double* K = contrib + (long long)pos[(long long)s * C + slot] * 5;
+        K[0] = jl_mulb((resp - PS) * dT, ac);
+        K[1] = jl_mulb((exu - VDOC) * dT, ac);
+        K[2] = jl_mulb(-VNH4 * dT, ac);
+        K[3] = jl_mulb(-VNO3 * dT, ac);
+        K[4] = jl_mulb(-VPO4 * dT, ac);
+    }
+    // diags_spcs! (Diagnostics/diagnostics_kernels.jl:20-21) in PI_MPROC_* order: VNH4 (listed
+    // there as :VHN4) and exu are never accumulated
+    if (procv) {
+        const double v[PI_NMPROC] = { PS, VDOC, 0.0, VNO3, VPO4, resp, rChl, S_PRO, S_DNA, S_RNA, 0.0,
+                                      CH, NST, PST, PRO, DNA, RNA, Chl };
+        for (int q = 0; q < PI_NMPROC; ++q) procv[(long long)q * C + slot] = v[q];
+    }
+    if (ac) {
+        int xi, yi, zi;
+        unpack_cell(g, P.cell[slot], xi, yi, zi);
+        atomicAdd(&d_num[gidx(g, xi, yi, zi)], 1.0);
+    }
+}
+
 // diags_spcs! (Diagnostics/diagnostics_kernels.jl:14-33): the cell of every slot active after the
 // species' update (its find_inds! cell), G for the others, for a stable sort by cell.
 __global__ void k_diag_keys(DGrid g, SpcDev P, long long C, uint32_t* __restrict__ key, uint32_t* __restrict__ val,
@@ -711,7 +896,7 @@ __global__ void k_diag_sum(long long C, long long G, const uint32_t* __restrict_
     if (i >= C) return;
     const uint32_t c = key[i];
     if (c >= (uint32_t)G || (i > 0 && key[i - 1] == c)) return;
-    for (int q = 0; q < PI_NPROC; ++q) {
+    for (int q = 0; q < PI_MAXPROC; ++q) {
         if (!(mask >> q & 1u)) continue;
         double x = d[(long long)q * G + c];
         for (long long j = i; j < C && key[j] == c; ++j) x = x + procv[(long long)q * C + val[j]];
@@ -827,6 +1012,7 @@ __device__ __forceinline__ double flux_z_c(const FaceCoef& f, double cm2, double
 // flux of its cell comes from lane l + 1 by shuffle. The face after the last interior cell follows
 // fill_halo_Gcs!: the periodic image of face H+1, or zero when Bounded.
 #define SWX_WARPS 4
+template <bool LL>
 __global__ void __launch_bounds__(32 * SWX_WARPS) k_sweep_x(DGrid g, const double* __restrict__ tr,
                                                             double* __restrict__ tta,
                                                             const double* __restrict__ u, double dT,
@@ -845,11 +1031,12 @@ __global__ void __launch_bounds__(32 * SWX_WARPS) k_sweep_x(DGrid g, const doubl
     const bool zero_face = !has_face || (special && g.tx != PI_PERIODIC);
     const int fs = special ? g.Hx + 1 : f;           // face whose stencil gives the flux
     const long long G = g.G;
+    const double ax = g.dy * dzF1(g, k);             // Ax of a RectilinearGrid
     const int qf = gidx(g, has_face ? fs : i0, j, k);
     FaceCoef fc{};
     int lm2 = 1, lm1 = 1, l0 = 1, lp1 = 1;
     if (!zero_face) {
-        fc = face_coef(u[qf], Axm(g, fs, j, k), dxCm(g, fs, j), dT);
+        fc = face_coef(u[qf], LL ? Axm<LL>(g, fs, j, k) : ax, dxCm<LL>(g, fs, j), dT);
         lm2 = lmask(g, fs - 2, j, k); lm1 = lmask(g, fs - 1, j, k); l0 = lmask(g, fs, j, k); lp1 = lmask(g, fs + 1, j, k);
     }
     const int qc = gidx(g, has_cell ? f : i0, j, k);
@@ -857,8 +1044,8 @@ __global__ void __launch_bounds__(32 * SWX_WARPS) k_sweep_x(DGrid g, const doubl
     int cl0 = 1, clp = 1;
     if (has_cell) {
         cl0 = lmask(g, f, j, k); clp = lmask(g, f + 1, j, k);
-        ftr = jl_mulb(jl_mulb(Axm(g, f + 1, j, k) * u[qc + 1] - Axm(g, f, j, k) * u[qc], clp), cl0);
-        dtv = dT / vol(g, f, j, k);
+        ftr = jl_mulb(jl_mulb((LL ? Axm<LL>(g, f + 1, j, k) : ax) * u[qc + 1] - (LL ? Axm<LL>(g, f, j, k) : ax) * u[qc], clp), cl0);
+        dtv = dT / vol<LL>(g, f, j, k);
     }
 #pragma unroll 2
     for (int n = 0; n < PI_NTRACERS; ++n) {
@@ -880,19 +1067,21 @@ __global__ void __launch_bounds__(32 * SWX_WARPS) k_sweep_x(DGrid g, const doubl
 // halo fill of tracer_temp produces.
 #define SWY_L 8
 #define SWY_TY 4
+template <bool LL>
 __device__ __forceinline__ double yface_flux(const DGrid& g, const double* __restrict__ c,
                                              const double* __restrict__ v, int i, int f, int k,
-                                             double dT) {
+                                             double ay, double dT) {
     const bool special = f == g.Ny + g.Hy + 1;
     if (special && g.ty != PI_PERIODIC) return 0.0;            // fill_halo_north_Gc! (Bounded)
     const int fs = special ? g.Hy + 1 : f;                      // periodic: Gc[N+H+1] = Gc[H+1]
-    FaceCoef fc = face_coef(v[gidx(g, i, fs, k)], Aym(g, i, fs, k), dyCm(g, i, fs), dT);
+    FaceCoef fc = face_coef(v[gidx(g, i, fs, k)], LL ? Aym<LL>(g, i, fs, k) : ay, dyCm<LL>(g, i, fs), dT);
     int r0 = gidx(g, i, wrap_axis(fs - 2, g.Ny, g.Hy, g.ty), k), r1 = gidx(g, i, wrap_axis(fs - 1, g.Ny, g.Hy, g.ty), k);
     int r2 = gidx(g, i, wrap_axis(fs, g.Ny, g.Hy, g.ty), k), r3 = gidx(g, i, wrap_axis(fs + 1, g.Ny, g.Hy, g.ty), k);
     return flux_xy_c(fc, c[r0], c[r1], c[r2], c[r3], lmask(g, i, fs - 2, k), lmask(g, i, fs - 1, k),
                      lmask(g, i, fs, k), lmask(g, i, fs + 1, k));
 }
 
+template <bool LL>
 __global__ void __launch_bounds__(32 * SWY_TY, 8) k_sweep_y(DGrid g, const double* __restrict__ tr,
                                                          const double* __restrict__ tta,
                                                          double* __restrict__ ttb,
@@ -905,17 +1094,20 @@ __global__ void __launch_bounds__(32 * SWY_TY, 8) k_sweep_y(DGrid g, const doubl
     if (i > g.Nx + g.Hx || j0 > g.Ny + g.Hy) return;
     const int jend = min(j0 + SWY_L - 1, g.Ny + g.Hy);
     const long long G = g.G;
-    const double dtv0 = dT / vol(g, i, j0, k);      // the same for every row of a RectilinearGrid
+    // the face area and ΔT/volume of a RectilinearGrid are the same for every row
+    const double ay = g.dx * dzF1(g, k);
+    const double dtv0 = dT / vol<false>(g, i, j0, k);
 #pragma unroll 1
     for (int t = 0; t < PI_NTRACERS; ++t) {
         const double* c = tta + t * G;
-        double Ft = yface_flux(g, c, v, i, j0, k, dT);
+        double Ft = yface_flux<LL>(g, c, v, i, j0, k, ay, dT);
         for (int jj = j0; jj <= jend; ++jj) {
-            double Fb = yface_flux(g, c, v, i, jj + 1, k, dT);
+            double Fb = yface_flux<LL>(g, c, v, i, jj + 1, k, ay, dT);
             const int q = gidx(g, i, jj, k);
             const int cl0 = lmask(g, i, jj, k), clp = lmask(g, i, jj + 1, k);
-            const double dtv = g.mVol ? dT / vol(g, i, jj, k) : dtv0;
-            const double ftr = jl_mulb(jl_mulb(Aym(g, i, jj + 1, k) * v[q + g.Gx] - Aym(g, i, jj, k) * v[q], clp), cl0);
+            const double dtv = LL ? dT / vol<LL>(g, i, jj, k) : dtv0;
+            const double ayp = LL ? Aym<LL>(g, i, jj + 1, k) : ay, ay0 = LL ? Aym<LL>(g, i, jj, k) : ay;
+            const double ftr = jl_mulb(jl_mulb(ayp * v[q + g.Gx] - ay0 * v[q], clp), cl0);
             double dG = jl_mulb(jl_mulb(Fb - Ft, clp), cl0);
             ttb[t * G + q] = c[q] - dtv * (dG - tr[t * G + q] * ftr);
             Ft = Fb;
@@ -970,6 +1162,7 @@ __device__ __forceinline__ double zface_flux(const DGrid& g, const double* __res
                     lmask(g, i, j, f - 1), lmask(g, i, j, f), lmask(g, i, j, f + 1));
 }
 
+template <bool LL>
 __global__ void __launch_bounds__(32 * SWZ_TZ, 8) k_sweep_z(DGrid g, const double* __restrict__ tr,
                                                          const double* __restrict__ ttb,
                                                          double* __restrict__ gadv,
@@ -982,7 +1175,7 @@ __global__ void __launch_bounds__(32 * SWZ_TZ, 8) k_sweep_z(DGrid g, const doubl
     if (i > g.Nx + g.Hx || k0 > g.Nz + g.Hz) return;
     const int kend = min(k0 + SWZ_L - 1, g.Nz + g.Hz);
     const long long G = g.G;
-    const double az = Azm(g, i, j);
+    const double az = Azm<LL>(g, i, j);
     const int slab = g.Gx * g.Gy;
     const int qcol = gidx(g, i, j, 1);
 #pragma unroll 1
@@ -996,17 +1189,19 @@ __global__ void __launch_bounds__(32 * SWZ_TZ, 8) k_sweep_z(DGrid g, const doubl
             const double ftr = jl_mulb(jl_mulb(az * w[q] - az * w[q + slab], clp), cl0);
             const double dG = jl_mulb(jl_mulb(Ft - Fb, clp), cl0);
             const double cc = tr[t * G + q];
-            const double ct = c[q] - dT / vol(g, i, j, k) * (dG - cc * ftr);
+            const double ct = c[q] - dT / vol<LL>(g, i, j, k) * (dG - cc * ftr);
             gadv[t * G + q] = ct - cc;                          // calc_tracer_tendency!
             Ft = Fb;
         }
     }
 }
 
+template <bool LL>
 __device__ __forceinline__ void z_final_cell(const ZFinalArgs& a, int i, int j, int k, int q, double volk, double* Gc);
 
 // Per interior cell: diffusion, sinking, forcing, flux BCs, particle terms and apply_tendency!
 // on top of the advective tendency of k_sweep_z (tracer_update.jl:22-43).
+template <bool LL>
 __global__ void __launch_bounds__(128, 6) k_tracer_tail(ZFinalArgs a) {
     const DGrid& g = a.g;
     if (*a.err & PI_DEVERR_CAPACITY) return;
@@ -1019,15 +1214,16 @@ __global__ void __launch_bounds__(128, 6) k_tracer_tail(ZFinalArgs a) {
     double Gc[PI_NTRACERS];
 #pragma unroll
     for (int t = 0; t < PI_NTRACERS; ++t) Gc[t] = a.gadv[t * G + q];
-    z_final_cell(a, i, j, k, q, vol(g, i, j, k), Gc);
+    z_final_cell<LL>(a, i, j, k, q, vol<LL>(g, i, j, k), Gc);
 }
 
 // The rest of tracer_update! for one interior cell, given its advective tendency Gc.
+template <bool LL>
 __device__ __forceinline__ void z_final_cell(const ZFinalArgs& a, int i, int j, int k, int q, double volk, double* Gc) {
     const DGrid& g = a.g;
     const long long G = g.G;
     const double dT = a.dT;
-    const double az = Azm(g, i, j);
+    const double az = Azm<LL>(g, i, j);
     const int slab = g.Gx * g.Gy;
     const pi_bgc_params& b = a.b;
     // tracer_diffusion! (κ∇², tracer_diffusion.jl:1-21) on the original tracer
@@ -1040,8 +1236,8 @@ __device__ __forceinline__ void z_final_cell(const ZFinalArgs& a, int i, int j, 
             auto dx0 = [&](int ii) { return jl_mulb(jl_mulb(c[gidx(g, ii, j, k)] - c[gidx(g, ii - 1, j, k)], lmask(g, ii, j, k)), lmask(g, ii - 1, j, k)); };
             auto dy0 = [&](int jj) { return jl_mulb(jl_mulb(c[gidx(g, i, jj, k)] - c[gidx(g, i, jj - 1, k)], lmask(g, i, jj, k)), lmask(g, i, jj - 1, k)); };
             auto dz0 = [&](int kk) { return jl_mulb(jl_mulb(c[gidx(g, i, j, kk - 1)] - c[gidx(g, i, j, kk)], lmask(g, i, j, kk)), lmask(g, i, j, kk - 1)); };
-            double fx1 = kx * Axm(g, i + 1, j, k) * (dx0(i + 1) / dxFm(g, i + 1, j)), fx0 = kx * Axm(g, i, j, k) * (dx0(i) / dxFm(g, i, j));
-            double fy1 = ky * Aym(g, i, j + 1, k) * (dy0(j + 1) / dyFm(g, i, j + 1)), fy0 = ky * Aym(g, i, j, k) * (dy0(j) / dyFm(g, i, j));
+            double fx1 = kx * Axm<LL>(g, i + 1, j, k) * (dx0(i + 1) / dxFm<LL>(g, i + 1, j)), fx0 = kx * Axm<LL>(g, i, j, k) * (dx0(i) / dxFm<LL>(g, i, j));
+            double fy1 = ky * Aym<LL>(g, i, j + 1, k) * (dy0(j + 1) / dyFm<LL>(g, i, j + 1)), fy0 = ky * Aym<LL>(g, i, j, k) * (dy0(j) / dyFm<LL>(g, i, j));
             double fz0 = kz * az * (dz0(k) / dzF1(g, k)), fz1 = kz * az * (dz0(k + 1) / dzF1(g, k + 1));
             double ax_ = jl_mulb(jl_mulb(fx1 - fx0, lmask(g, i + 1, j, k)), li);
             double ay_ = jl_mulb(jl_mulb(fy1 - fy0, lmask(g, i, j + 1, k)), li);
@@ -1090,7 +1286,7 @@ __device__ __forceinline__ void z_final_cell(const ZFinalArgs& a, int i, int j, 
     // apply_bcs! (apply_bcs.jl:4-98), faces in the reference's order
     if (a.any_bc) {
         int ii = i - g.Hx, jj = j - g.Hy, kk = k - g.Hz;
-        double axk = Axm(g, i, j, k), ayk = Aym(g, i, j, k);
+        double axk = Axm<LL>(g, i, j, k), ayk = Aym<LL>(g, i, j, k);
 #pragma unroll
         for (int n = 0; n < PI_NTRACERS; ++n) {
             const FluxBCDev* B = a.bcs + n * 6;
@@ -1226,6 +1422,10 @@ __global__ void k_first_nonfinite_inds(SpcDev s, long long C, unsigned long long
         const double v[11] = { s.x[q], s.y[q], s.z[q], s.Sz[q], s.Bm[q], s.Cq[q], s.Nq[q], s.Pq[q], s.Chl[q], s.gen[q], s.age[q] };
         bool bad = false;
         for (int k = 0; k < 11; ++k) bad |= !isfinite(v[k]);
+        if (s.PRO) {                                  // MacroMolecularMode pools
+            const double w[6] = { s.PRO[q], s.DNA[q], s.RNA[q], s.CH[q], s.NST[q], s.PST[q] };
+            for (int k = 0; k < 6; ++k) bad |= !isfinite(w[k]);
+        }
         if (bad) atomicMin(first, (unsigned long long)q);
     }
 }
@@ -1252,7 +1452,7 @@ __global__ void __launch_bounds__(256) k_budget_cells(DGrid g, const double* __r
         const long long r = q / g.Nx;
         const int j = (int)(r % g.Ny) + 1 + g.Hy, k = (int)(r / g.Ny) + 1 + g.Hz;
         const long long cq = gidx(g, i, j, k);
-        const double vol = pib::vol(g, i, j, k);
+        const double vol = g.mVol ? pib::vol<true>(g, i, j, k) : pib::vol<false>(g, i, j, k);
         c += vol * (tr[PI_DIC * G + cq] + tr[PI_DOC * G + cq] + tr[PI_POC * G + cq]);
         n += vol * (tr[PI_NH4 * G + cq] + tr[PI_NO3 * G + cq] + tr[PI_DON * G + cq] + tr[PI_PON * G + cq]);
         p += vol * (tr[PI_PO4 * G + cq] + tr[PI_DOP * G + cq] + tr[PI_POP * G + cq]);
@@ -1267,6 +1467,18 @@ __global__ void __launch_bounds__(256) k_budget_inds(SpcDev s, long long C, doub
         c += Bm + s.Cq[q];
         n += Bm * R_NC + s.Nq[q];
         p += Bm * R_PC + s.Pq[q];
+    }
+    block_sum3(c, n, p, partial);
+}
+
+// MacroMolecularMode individuals: total_C/N/P_biomass (plankton_generation.jl:82-93) of the active ones
+__global__ void __launch_bounds__(256) k_budget_inds_macro(SpcDev s, long long C, pi_macro_params mp, double* __restrict__ partial) {
+    double c = 0.0, n = 0.0, p = 0.0;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < C; q += (long long)gridDim.x * blockDim.x) {
+        if (!(s.flags[q] & FL_AC)) continue;
+        c += m_totC(s.PRO[q], s.DNA[q], s.RNA[q], s.CH[q], s.Chl[q]);
+        n += m_totN(s.PRO[q], s.DNA[q], s.RNA[q], s.NST[q], s.Chl[q], mp);
+        p += m_totP(s.DNA[q], s.RNA[q], s.PST[q], mp);
     }
     block_sum3(c, n, p, partial);
 }

@@ -54,6 +54,9 @@ struct pi_model {
     pi_batch* b32 = nullptr;     // PI_FP32: the model is a batch of one member
     int carbon = 0;              // CarbonMode species (pi_create_carbon)
     std::vector<pi_carbon_params> cp;
+    int macro = 0;               // MacroMolecularMode species (pi_create_macro)
+    std::vector<pi_macro_params> mp;
+    int mode() const { return macro ? MODE_MACRO : carbon ? MODE_CARBON : MODE_QUOTA; }
     int64_t iteration = 0;
     double t = 0.0;
     double last_dT = 0.0;
@@ -83,8 +86,8 @@ struct pi_model {
     // optional diagnostics (pi_set_diags)
     uint32_t tr_mask = 0, proc_mask = 0;
     double* diag_tr = nullptr;   // 14 × G
-    double* diag_proc = nullptr; // nsp × PI_NPROC × G
-    double* procv = nullptr;     // PI_NPROC × C values of the species being updated
+    double* diag_proc = nullptr; // nsp × PI_MAXPROC × G
+    double* procv = nullptr;     // PI_MAXPROC × C values of the species being updated
     double* budget_part = nullptr;   // 3 × 512 block partials of pi_get_budget
     uint32_t *dkey = nullptr, *dkey_s = nullptr, *dval = nullptr, *dval_s = nullptr;
     void* dsort_tmp = nullptr;
@@ -258,12 +261,13 @@ pi_status enqueue_step(pi_model* m, double dT) {
     CK(cudaGetLastError(), "k_velhalf"); }
     VelPtrs vp{m->vel0[0], m->vel0[1], m->vel0[2], m->velh[0], m->velh[1], m->velh[2],
                m->vel1[0], m->vel1[1], m->vel1[2]};
+    const bool ll = m->met != nullptr;      // LatLonGrid: the kernels that read grid metrics take their arrays
     { ProfScope ps_(m, "k_particles_sorted");
-    k_particles_sorted<<<nblk(NC, 128), 128, 0, st>>>(g, m->d_spc, C, sb.gid_sorted, sb.off, G, dT, m->seed, iter, vp,
+    (ll ? k_particles_sorted<true> : k_particles_sorted<false>)<<<nblk(NC, 128), 128, 0, st>>>(g, m->d_spc, C, sb.gid_sorted, sb.off, G, dT, m->seed, iter, vp,
                                                       m->bgc.kappa_hP, m->bgc.kappa_vP, sb.cnt, sb.key, sb.err);
     CK(cudaGetLastError(), "k_particles_sorted"); }
     { ProfScope ps_(m, "k_particles");
-    k_particles<<<nblk(NC, BS), BS, 0, st>>>(g, m->d_spc, m->nsp, C, dT, m->seed, iter, vp,
+    (ll ? k_particles<true> : k_particles<false>)<<<nblk(NC, BS), BS, 0, st>>>(g, m->d_spc, m->nsp, C, dT, m->seed, iter, vp,
                                              m->bgc.kappa_hP, m->bgc.kappa_vP, sb.cnt, sb.key,
                                              (uint32_t)G, sb.err);
     CK(cudaGetLastError(), "k_particles"); }
@@ -280,7 +284,7 @@ pi_status enqueue_step(pi_model* m, double dT) {
     {
         dim3 grid(nblk(g.Nx, 128), g.Ny);
         ProfScope ps_(m, "k_par");
-        k_par<<<grid, 128, 0, st>>>(g, m->d_spc, C, sb.off, sb.gid_sorted, m->PARF, m->PARF, m->par,
+        (ll ? k_par<true> : k_par<false>)<<<grid, 128, 0, st>>>(g, m->d_spc, C, sb.off, sb.gid_sorted, m->PARF, m->PARF, m->par,
                                     m->diag_par, m->bgc.kc, m->bgc.kw, sb.err);
         CK(cudaGetLastError(), "k_par");
     }
@@ -288,8 +292,9 @@ pi_status enqueue_step(pi_model* m, double dT) {
     for (int s = 0; s < m->nsp; ++s) {
         double* dsp = m->diag_sp + (size_t)s * 4 * G;
         { ProfScope ps_(m, "k_decide");
-        k_decide<<<nblk(C, BS), BS, 0, st>>>(g, m->h_spc[s], m->sp[s], C, s, sb.pos, sb.loss, sb.evk,
-                                             sb.flag64, dsp + 1 * G, dsp + 2 * G, dsp + 3 * G, sb.err, m->carbon);
+        const pi_macro_params mpz = m->macro ? m->mp[s] : pi_macro_params{};
+        k_decide<<<nblk(C, BS), BS, 0, st>>>(g, m->h_spc[s], m->sp[s], mpz, C, s, sb.pos, sb.loss, sb.evk,
+                                             sb.flag64, dsp + 1 * G, dsp + 2 * G, dsp + 3 * G, sb.err, m->mode());
         CK(cudaGetLastError(), "k_decide"); }
         tb = m->cub_bytes;
         { ProfScope ps_(m, "cub_scan_slots");
@@ -299,9 +304,16 @@ pi_status enqueue_step(pi_model* m, double dT) {
                                             sb.err, sb.err_iter, m->iteration);
         CK(cudaGetLastError(), "k_lists"); }
         { ProfScope ps_(m, "k_daughters");
-        k_daughters<<<148 * 4, 256, 0, st>>>(m->h_spc[s], sb.divlist, sb.freelist, sb.ndiv, sb.err, m->carbon);
+        k_daughters<<<148 * 4, 256, 0, st>>>(m->h_spc[s], sb.divlist, sb.freelist, sb.ndiv, sb.err, m->mode());
         CK(cudaGetLastError(), "k_daughters"); }
         const double* trp = m->tr;
+        if (m->macro) { ProfScope ps_(m, "k_physiology");
+        k_physiology_macro<<<nblk(C, BS), BS, 0, st>>>(g, m->h_spc[s], m->mp[s], C, s, dT, m->seed, iter, shared,
+                                                       trp + PI_NH4 * G, trp + PI_NO3 * G, trp + PI_PO4 * G,
+                                                       trp + PI_DOC * G, m->par, m->temp, sb.off, sb.gid_sorted,
+                                                       sb.pos, sb.contrib, dsp + 0 * G,
+                                                       m->proc_mask ? m->procv : nullptr, sb.err);
+        CK(cudaGetLastError(), "k_physiology_macro"); } else
         if (m->carbon) { ProfScope ps_(m, "k_physiology");
         k_physiology_carbon<<<nblk(C, BS), BS, 0, st>>>(g, m->h_spc[s], m->cp[s], C, s, dT, m->t, m->seed, iter,
                                                         shared, m->par, m->temp, sb.off, sb.gid_sorted, sb.pos,
@@ -321,16 +333,16 @@ pi_status enqueue_step(pi_model* m, double dT) {
             CK(cub::DeviceRadixSort::SortPairs(m->dsort_tmp, db, m->dkey, m->dkey_s, m->dval, m->dval_s, (int64_t)C,
                                                0, m->key_bits, st), "sort diagnostics by cell");
             k_diag_sum<<<nblk(C, BS), BS, 0, st>>>(C, G, m->dkey_s, m->dval_s, m->procv, m->proc_mask,
-                                                   m->diag_proc + (size_t)s * PI_NPROC * G);
+                                                   m->diag_proc + (size_t)s * PI_MAXPROC * G);
             CK(cudaGetLastError(), "k_diag_proc");
         }
     }
     {
         { ProfScope ps_(m, "k_sweep_x");
-        k_sweep_x<<<dim3(nblk(nblk(g.Nx, 31), SWX_WARPS), g.Ny, g.Nz), 32 * SWX_WARPS, 0, st>>>(g, m->tr, m->tta, m->vel1[0], dT, sb.err);
+        (ll ? k_sweep_x<true> : k_sweep_x<false>)<<<dim3(nblk(nblk(g.Nx, 31), SWX_WARPS), g.Ny, g.Nz), 32 * SWX_WARPS, 0, st>>>(g, m->tr, m->tta, m->vel1[0], dT, sb.err);
         CK(cudaGetLastError(), "k_sweep_x"); }
         { ProfScope ps_(m, "k_sweep_y");
-        k_sweep_y<<<dim3(nblk(g.Nx, 32), nblk(nblk(g.Ny, SWY_L), SWY_TY), g.Nz), dim3(32, SWY_TY), 0, st>>>(g, m->tr, m->tta, m->ttb, m->vel1[1], dT, sb.err);
+        (ll ? k_sweep_y<true> : k_sweep_y<false>)<<<dim3(nblk(g.Nx, 32), nblk(nblk(g.Ny, SWY_L), SWY_TY), g.Nz), dim3(32, SWY_TY), 0, st>>>(g, m->tr, m->tta, m->ttb, m->vel1[1], dT, sb.err);
         CK(cudaGetLastError(), "k_sweep_y"); }
         ZFinalArgs za;
         za.g = g; za.tr = m->tr; za.ttb = m->ttb; za.tr_next = m->tr_next; za.w = m->vel1[2];
@@ -341,11 +353,11 @@ pi_status enqueue_step(pi_model* m, double dT) {
         za.loss = sb.loss; za.contrib = sb.contrib; za.nsp = m->nsp; za.err = sb.err;
         za.gadv = m->tta;      // the x-sweep output is no longer needed
         { ProfScope ps_(m, "k_sweep_z");
-        k_sweep_z<<<dim3(nblk(g.Nx, 32), g.Ny, nblk(nblk(g.Nz, SWZ_L), SWZ_TZ)), dim3(32, SWZ_TZ), 0, st>>>(
+        (ll ? k_sweep_z<true> : k_sweep_z<false>)<<<dim3(nblk(g.Nx, 32), g.Ny, nblk(nblk(g.Nz, SWZ_L), SWZ_TZ)), dim3(32, SWZ_TZ), 0, st>>>(
             g, m->tr, m->ttb, m->tta, m->vel1[2], dT, sb.err);
         CK(cudaGetLastError(), "k_sweep_z"); }
         { ProfScope ps_(m, "k_tracer_tail");
-        k_tracer_tail<<<dim3(nblk(g.Nx, 128), g.Ny, g.Nz), 128, 0, st>>>(za);
+        (ll ? k_tracer_tail<true> : k_tracer_tail<false>)<<<dim3(nblk(g.Nx, 128), g.Ny, g.Nz), 128, 0, st>>>(za);
         CK(cudaGetLastError(), "k_tracer_tail"); }
         // tracers are only replaced when the step completed (a capacity error leaves them)
         { ProfScope ps_(m, "k_halo");
@@ -644,6 +656,49 @@ pi_status pi_create_carbon(const pi_grid* grid, const pi_bgc_params* bgc, const 
     return PI_OK;
 }
 
+pi_status pi_create_macro(const pi_grid* grid, const pi_bgc_params* bgc, const pi_macro_params* species,
+                          int32_t nspecies, int64_t capacity, int32_t precision, uint64_t seed, pi_model** out) {
+    if (!out) return fail(nullptr, PI_ERR_ARG, "pi_create_macro: out is NULL");
+    *out = nullptr;
+    if (!species || nspecies < 1) return fail(nullptr, PI_ERR_ARG, "pi_create_macro: NULL species or nspecies < 1");
+    if (precision != PI_FP64)
+        return fail(nullptr, PI_ERR_ARG, "pi_create_macro: MacroMolecularMode is built in the FP64 form only (precision PI_FP64)");
+    // the QuotaMode setup with the parameters both modes share; the species then switch to
+    // MacroMolecularMode (dvid_type 1 only passes the shared validation, division is by DNA)
+    std::vector<pi_quota_params> q((size_t)nspecies);
+    for (int s = 0; s < nspecies; ++s) {
+        const pi_macro_params& c = species[s];
+        pi_quota_params& p = q[s];
+        memset(&p, 0, sizeof p);
+        p.Nsuper = c.Nsuper; p.var = c.var; p.alpha = c.alpha; p.Phi = c.Phi; p.Topt = c.Topt; p.Tmax = c.Tmax;
+        p.Ea = c.Ea; p.PCmax = c.PCmax; p.respir = c.respir; p.grz_P = c.grz_P; p.dvid_type = 1.0;
+        p.dvid_P = c.dvid_P; p.mort_P = c.mort_P; p.mort_reg = c.mort_reg;
+        p.grazFracC = c.grazFracC; p.grazFracN = c.grazFracN; p.grazFracP = c.grazFracP;
+        p.mortFracC = c.mortFracC; p.mortFracN = c.mortFracN; p.mortFracP = c.mortFracP;
+    }
+    pi_status st = pi_create(grid, bgc, q.data(), nspecies, capacity, PI_FP64, seed, out);
+    if (st) return st;
+    pi_model* m = *out;
+    m->macro = 1;
+    m->mp.assign(species, species + nspecies);
+    for (int s = 0; s < nspecies; ++s) {
+        SpcDev& P = m->h_spc[s];
+        double** pools[6] = { &P.PRO, &P.DNA, &P.RNA, &P.CH, &P.NST, &P.PST };
+        for (double** pp : pools)
+            if ((st = dalloc(m, pp, (size_t)capacity, "macromolecular pools")) ||
+                cudaMemsetAsync(*pp, 0, (size_t)capacity * sizeof(double), m->stream) != cudaSuccess) {
+                pi_destroy(m); *out = nullptr;
+                return fail(nullptr, st ? st : PI_ERR_CUDA, "pi_create_macro: device allocation failed");
+            }
+    }
+    if (cudaMemcpyAsync(m->d_spc, m->h_spc.data(), nspecies * sizeof(SpcDev), cudaMemcpyHostToDevice, m->stream) != cudaSuccess ||
+        cudaStreamSynchronize(m->stream) != cudaSuccess) {
+        pi_destroy(m); *out = nullptr;
+        return fail(nullptr, PI_ERR_CUDA, "pi_create_macro: device initialisation failed");
+    }
+    return PI_OK;
+}
+
 pi_status pi_destroy(pi_model* m) {
     if (!m) return PI_OK;
     if (m->b32) {
@@ -665,9 +720,14 @@ pi_status pi_set_individuals(pi_model* m, int32_t sp, const pi_individuals* in) 
     if (!m || !in || sp < 0 || sp >= m->nsp) return fail(m, PI_ERR_ARG, "pi_set_individuals: bad argument");
     const double* dcols[] = { in->x, in->y, in->z, in->Sz, in->Bm, in->Cq, in->Nq, in->Pq, in->Chl, in->gen, in->age,
                               in->graz, in->mort, in->dvid };
-    for (int q = 0; q < 14; ++q)
-        if (!dcols[q] && !(m->carbon && q >= 5 && q <= 7))        // CarbonMode keeps no quotas
-            return fail(m, PI_ERR_ARG, "pi_set_individuals: NULL attribute");
+    const double* mcols[6] = { in->PRO, in->DNA, in->RNA, in->CH, in->NST, in->PST };
+    for (int q = 0; q < 14; ++q) {
+        // CarbonMode keeps no quotas; MacroMolecularMode no Sz, Bm or quotas, but its six pools
+        const bool unused = (m->carbon && q >= 5 && q <= 7) || (m->macro && q >= 3 && q <= 7);
+        if (!dcols[q] && !unused) return fail(m, PI_ERR_ARG, "pi_set_individuals: NULL attribute");
+    }
+    if (m->macro)
+        for (const double* c : mcols) if (!c) return fail(m, PI_ERR_ARG, "pi_set_individuals: NULL attribute");
     if (!in->xi || !in->yi || !in->zi || !in->ac) return fail(m, PI_ERR_ARG, "pi_set_individuals: NULL attribute");
     const long long C = m->C;
     const HostGrid& g = m->hg;
@@ -687,7 +747,13 @@ pi_status pi_set_individuals(pi_model* m, int32_t sp, const pi_individuals* in) 
     const SpcDev& P = m->h_spc[sp];
     double* dptr[] = { P.x, P.y, P.z, P.Sz, P.Bm, P.Cq, P.Nq, P.Pq, P.Chl, P.gen, P.age };
     for (int q = 0; q < 11; ++q)
-        if (dcols[q]) CK(cudaMemcpyAsync(dptr[q], dcols[q], C * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload individuals");
+        if (dcols[q] && !(m->macro && q >= 3 && q <= 7))
+            CK(cudaMemcpyAsync(dptr[q], dcols[q], C * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload individuals");
+    if (m->macro) {
+        double* mptr[6] = { P.PRO, P.DNA, P.RNA, P.CH, P.NST, P.PST };
+        for (int q = 0; q < 6; ++q)
+            CK(cudaMemcpyAsync(mptr[q], mcols[q], C * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload individuals");
+    }
     if (m->carbon) {
         if (in->Bd) CK(cudaMemcpyAsync(P.Bd, in->Bd, C * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload individuals");
         else CK(cudaMemsetAsync(P.Bd, 0, C * sizeof(double), m->stream), "upload individuals");
@@ -709,6 +775,12 @@ pi_status pi_get_individuals(pi_model* m, int32_t sp, pi_individuals* out) {
     for (int q = 0; q < 11; ++q)
         if (hptr[q]) CK(cudaMemcpyAsync(hptr[q], dptr[q], C * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download individuals");
     if (m->carbon && out->Bd) CK(cudaMemcpyAsync(out->Bd, P.Bd, C * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download individuals");
+    if (m->macro) {
+        double* mh[6] = { out->PRO, out->DNA, out->RNA, out->CH, out->NST, out->PST };
+        const double* md[6] = { P.PRO, P.DNA, P.RNA, P.CH, P.NST, P.PST };
+        for (int q = 0; q < 6; ++q)
+            if (mh[q]) CK(cudaMemcpyAsync(mh[q], md[q], C * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download individuals");
+    }
     std::vector<uint8_t> flags(C);
     std::vector<int32_t> cell(C);
     CK(cudaMemcpyAsync(flags.data(), P.flags, C, cudaMemcpyDeviceToHost, m->stream), "download flags");
@@ -1007,15 +1079,15 @@ pi_status pi_count_active_async(pi_model* m, int32_t sp, int64_t* n) {
 
 pi_status pi_set_diags(pi_model* m, uint32_t tracer_mask, uint32_t proc_mask) {
     if (m && m->b32) return fwd32(m, pi_batch_set_diags(m->b32, tracer_mask, proc_mask));
-    if (!m || tracer_mask >> PI_NTRACERS || proc_mask >> (m->carbon ? (int)PI_NCPROC : (int)PI_NPROC))
+    if (!m || tracer_mask >> PI_NTRACERS || proc_mask >> (m->macro ? (int)PI_NMPROC : m->carbon ? (int)PI_NCPROC : (int)PI_NPROC))
         return fail(m, PI_ERR_ARG, "pi_set_diags: bad argument");
     const long long G = m->hg.G, C = m->C;
     CK(cudaStreamSynchronize(m->stream), "synchronize");
     if (tracer_mask && !m->diag_tr) { pi_status e = dalloc(m, &m->diag_tr, (size_t)PI_NTRACERS * G, "tracer diagnostics"); if (e) return e; }
     if (proc_mask && !m->diag_proc) {
         pi_status e;
-        if ((e = dalloc(m, &m->diag_proc, (size_t)m->nsp * PI_NPROC * G, "process diagnostics"))) return e;
-        if ((e = dalloc(m, &m->procv, (size_t)PI_NPROC * C, "process values"))) return e;
+        if ((e = dalloc(m, &m->diag_proc, (size_t)m->nsp * PI_MAXPROC * G, "process diagnostics"))) return e;
+        if ((e = dalloc(m, &m->procv, (size_t)PI_MAXPROC * C, "process values"))) return e;
         for (uint32_t** p : { &m->dkey, &m->dkey_s, &m->dval, &m->dval_s })
             if ((e = dalloc(m, p, (size_t)C, "diagnostic sort"))) return e;
         size_t db = 0;
@@ -1025,7 +1097,7 @@ pi_status pi_set_diags(pi_model* m, uint32_t tracer_mask, uint32_t proc_mask) {
         m->dsort_tmp = tmp; m->dsort_bytes = db;
     }
     if (m->diag_tr) CK(cudaMemsetAsync(m->diag_tr, 0, (size_t)PI_NTRACERS * G * sizeof(double), m->stream), "clear diagnostics");
-    if (m->diag_proc) CK(cudaMemsetAsync(m->diag_proc, 0, (size_t)m->nsp * PI_NPROC * G * sizeof(double), m->stream), "clear diagnostics");
+    if (m->diag_proc) CK(cudaMemsetAsync(m->diag_proc, 0, (size_t)m->nsp * PI_MAXPROC * G * sizeof(double), m->stream), "clear diagnostics");
     CK(cudaStreamSynchronize(m->stream), "synchronize");
     m->tr_mask = tracer_mask; m->proc_mask = proc_mask;
     return PI_OK;
@@ -1040,10 +1112,10 @@ pi_status pi_get_diag(pi_model* m, int32_t kind, int32_t sp, double* out) {
     else if (kind >= PI_DIAG_TRACER && kind < PI_DIAG_TRACER + PI_NTRACERS) {
         if (!(m->tr_mask >> (kind - PI_DIAG_TRACER) & 1u)) return fail(m, PI_ERR_ARG, "pi_get_diag: tracer diagnostic not enabled");
         src = m->diag_tr + (size_t)(kind - PI_DIAG_TRACER) * G;
-    } else if (kind >= PI_DIAG_PROC && kind < PI_DIAG_PROC + PI_NPROC) {
+    } else if (kind >= PI_DIAG_PROC && kind < PI_DIAG_PROC + PI_MAXPROC) {
         if (sp < 0 || sp >= m->nsp || !(m->proc_mask >> (kind - PI_DIAG_PROC) & 1u))
             return fail(m, PI_ERR_ARG, "pi_get_diag: process diagnostic not enabled or bad species");
-        src = m->diag_proc + ((size_t)sp * PI_NPROC + (kind - PI_DIAG_PROC)) * G;
+        src = m->diag_proc + ((size_t)sp * PI_MAXPROC + (kind - PI_DIAG_PROC)) * G;
     } else {
         if (sp < 0 || sp >= m->nsp || kind < PI_DIAG_NUM || kind > PI_DIAG_DVID) return fail(m, PI_ERR_ARG, "pi_get_diag: bad kind/species");
         src = m->diag_sp + ((size_t)sp * 4 + (kind - PI_DIAG_NUM)) * G;
@@ -1071,7 +1143,8 @@ pi_status pi_get_budget(pi_model* m, double out[6]) {
     pi_status e = collect(out);
     if (e) return e;
     for (int s = 0; s < m->nsp; ++s) {
-        k_budget_inds<<<nb, 256, 0, m->stream>>>(m->h_spc[s], m->C, m->sp[s].R_NC, m->sp[s].R_PC, m->budget_part);
+        if (m->macro) k_budget_inds_macro<<<nb, 256, 0, m->stream>>>(m->h_spc[s], m->C, m->mp[s], m->budget_part);
+        else k_budget_inds<<<nb, 256, 0, m->stream>>>(m->h_spc[s], m->C, m->sp[s].R_NC, m->sp[s].R_PC, m->budget_part);
         if ((e = collect(out + 3))) return e;
     }
     return PI_OK;
@@ -1084,7 +1157,7 @@ pi_status pi_reset_diags(pi_model* m) {
     CK(cudaMemsetAsync(m->diag_par, 0, G * sizeof(double), m->stream), "reset diags");
     CK(cudaMemsetAsync(m->diag_sp, 0, 4 * m->nsp * G * sizeof(double), m->stream), "reset diags");
     if (m->diag_tr) CK(cudaMemsetAsync(m->diag_tr, 0, (size_t)PI_NTRACERS * G * sizeof(double), m->stream), "reset diags");
-    if (m->diag_proc) CK(cudaMemsetAsync(m->diag_proc, 0, (size_t)m->nsp * PI_NPROC * G * sizeof(double), m->stream), "reset diags");
+    if (m->diag_proc) CK(cudaMemsetAsync(m->diag_proc, 0, (size_t)m->nsp * PI_MAXPROC * G * sizeof(double), m->stream), "reset diags");
     CK(cudaStreamSynchronize(m->stream), "synchronize");
     return PI_OK;
 }

@@ -16,6 +16,8 @@
 #define F_1em4  ((double)1.0e-4f)
 #define F_1em2  ((double)1.0e-2f)
 #define F_1em1  ((double)1.0e-1f)
+#define F_5em2  ((double)0.05f)
+#define F_CHL   ((double)893.49f)      // mg Chl per mmol (MacroMolecularMode)
 #define F_2em3  ((double)2.0e-3f)
 #define F_1em3  ((double)1.0e-3f)
 #define F_1em5  ((double)1.0e-5f)
@@ -23,6 +25,14 @@
 #define F_0p99  ((double)0.99f)
 #define F_THMAX ((double)1.0e20f)
 #define F_1em20 ((double)1.0e-20f)
+
+// physiology modes of an FP64 model
+#define MODE_QUOTA  0
+#define MODE_CARBON 1
+#define MODE_MACRO  2
+
+// process diagnostics of the largest mode (MacroMolecularMode): sizes of the per-species buffers
+#define PI_MAXPROC PI_NMPROC
 
 // Device error word bits (sticky until pi_synchronize reads and clears them).
 #define PI_DEVERR_DOMAIN   1u
@@ -72,6 +82,8 @@ __host__ __device__ __forceinline__ void unpack_cell(const DGrid& g, int32_t c, 
 struct SpcDev {
     double *x, *y, *z, *Sz, *Bm, *Cq, *Nq, *Pq, *Chl, *gen, *age;
     double* Bd;         // CarbonMode damaged biomass (NULL for QuotaMode)
+    // MacroMolecularMode pools (NULL otherwise): protein, DNA, RNA, carbohydrate/lipid, N and P reserves
+    double *PRO, *DNA, *RNA, *CH, *NST, *PST;
     uint8_t* flags;
     int32_t* cell;      // packed (xi, yi, zi)
     uint8_t* stat;      // ST_* bits of the current step

@@ -13,7 +13,7 @@
 module PIB200
 
 export PiGrid, PiBgc, PiQuota, PiIndividuals, PiMember, PIError
-export create, create_carbon, destroy, set_individuals!, get_individuals, set_tracer!, get_tracer
+export create, create_carbon, create_macro, destroy, set_individuals!, get_individuals, set_tracer!, get_tracer
 export set_velocity!, set_PARF!, set_temp!, set_flux_bc!, time_step!, get_time, set_time!
 export count_active, get_diag, reset_diags!, check_finite, budget, simulation, update!, synchronize
 export set_velocity_f32!, set_PARF_f32!, set_temp_f32!, time_step_async!, count_active_async!, set_diags!
@@ -35,7 +35,10 @@ const PI_DIAG_TRACER = Int32(16)
 const PI_DIAG_PROC = Int32(32)
 const PROCS = (:PS, :BS, :VDOC, :VNH4, :VNO3, :VPO4, :resp, :exu, :Bm, :Cq, :Nq, :Pq, :Chl)
 const CPROCS = (:PS, :BS, :RP, :RS, :TD, :Bm, :Bd, :Chl)      # CarbonMode processes
-procs(m) = m.carbon ? CPROCS : PROCS
+# MacroMolecularMode processes (PI_MPROC_* order); VNH4 and exu stay zero as in the reference
+const MPROCS = (:PS, :VDOC, :VNH4, :VNO3, :VPO4, :resp, :ρChl, :S_PRO, :S_DNA, :S_RNA, :exu, :CH, :NST, :PST,
+                :PRO, :DNA, :RNA, :Chl)
+procs(m) = m.mm ? MPROCS : m.carbon ? CPROCS : PROCS
 
 struct PiGrid
     Nx::Int32; Ny::Int32; Nz::Int32
@@ -82,6 +85,18 @@ struct PiCarbon
 end
 PiCarbon(p::AbstractDict, sp::Integer) = PiCarbon(ntuple(i -> Float64(p[CARBON_KEYS[i]][sp]), 24))
 
+# MacroMolecularMode param_names (src/Individuals/Plankton/MacroMolecularMode/plankton_generation.jl:17-23)
+const MACRO_KEYS = ("Nsuper", "C_DNA", "var", "PRO2DNA", "RNA2DNA", "CH2DNA", "Chl2DNA", "α", "Φ", "Topt", "Tmax",
+                    "Ea", "PCmax", "VDOCmax", "VNO3max", "VNH4max", "VPO4max", "KsatDOC", "KsatNH4", "KsatNO3",
+                    "KsatPO4", "CHmax", "NSTmax", "PSTmax", "Chl2N", "R_NC_PRO", "R_NC_DNA", "R_NC_RNA", "R_PC_DNA",
+                    "R_PC_RNA", "respir", "k_pro", "k_sat_pro", "k_rna", "k_sat_rna", "k_dna", "k_sat_dna",
+                    "dvid_P", "grz_P", "mort_P", "mort_reg", "grazFracC", "grazFracN", "grazFracP", "mortFracC",
+                    "mortFracN", "mortFracP")
+struct PiMacro
+    v::NTuple{47,Float64}
+end
+PiMacro(p::AbstractDict, sp::Integer) = PiMacro(ntuple(i -> Float64(p[MACRO_KEYS[i]][sp]), 47))
+
 struct PiIndividuals
     x::Ptr{Float64}; y::Ptr{Float64}; z::Ptr{Float64}
     xi::Ptr{Int64}; yi::Ptr{Int64}; zi::Ptr{Int64}
@@ -90,6 +105,8 @@ struct PiIndividuals
     ac::Ptr{UInt8}
     graz::Ptr{Float64}; mort::Ptr{Float64}; dvid::Ptr{Float64}
     Bd::Ptr{Float64}            # CarbonMode damaged biomass (C_NULL for QuotaMode)
+    PRO::Ptr{Float64}; DNA::Ptr{Float64}; RNA::Ptr{Float64}    # MacroMolecularMode pools (C_NULL otherwise)
+    CH::Ptr{Float64}; NST::Ptr{Float64}; PST::Ptr{Float64}
 end
 
 struct PiMember
@@ -128,6 +145,7 @@ mutable struct Model
     Nsp::Int
     capacity::Int
     carbon::Bool
+    mm::Bool                 # MacroMolecularMode
 end
 
 topo_code(T) = occursin("Periodic", string(T)) ? PI_PERIODIC : PI_BOUNDED
@@ -160,7 +178,7 @@ function create(g, bgc::AbstractDict, phyt::AbstractDict, Nsp::Integer, maxN::In
         (Ref{PiGrid}, Ref{PiBgc}, Ptr{PiQuota}, Int32, Int64, Int32, UInt64, Ref{Ptr{Cvoid}}),
         pg, pb, ps, Nsp, maxN, FT === Float32 ? PI_FP32 : PI_FP64, seed, out)
     check(st, C_NULL)
-    m = Model(out[], (g.Nx + 2g.Hx, g.Ny + 2g.Hy, g.Nz + 2g.Hz), Nsp, maxN, false)
+    m = Model(out[], (g.Nx + 2g.Hx, g.Ny + 2g.Hy, g.Nz + 2g.Hz), Nsp, maxN, false, false)
     finalizer(destroy, m)
     m
 end
@@ -179,7 +197,26 @@ function create_carbon(g, bgc::AbstractDict, phyt::AbstractDict, Nsp::Integer, m
         (Ref{PiGrid}, Ref{PiBgc}, Ptr{PiCarbon}, Int32, Int64, Int32, UInt64, Ref{Ptr{Cvoid}}),
         pg, pb, ps, Nsp, maxN, PI_FP64, seed, out)
     check(st, C_NULL)
-    m = Model(out[], (g.Nx + 2g.Hx, g.Ny + 2g.Hy, g.Nz + 2g.Hz), Nsp, maxN, true)
+    m = Model(out[], (g.Nx + 2g.Hx, g.Ny + 2g.Hy, g.Nz + 2g.Hz), Nsp, maxN, true, false)
+    finalizer(destroy, m)
+    m
+end
+
+"""PlanktonModel(GPU(), grid; FT = Float64, mode = MacroMolecularMode(), ...): MacroMolecularMode
+species (individuals carry PRO, DNA, RNA, CH, NST, PST, Chl), built in the FP64 form only."""
+function create_macro(g, bgc::AbstractDict, phyt::AbstractDict, Nsp::Integer, maxN::Integer; seed::Integer = 0)
+    dzF, dzC = Float64.(collect(g.dzF)), Float64.(collect(g.dzC))
+    lm = UInt8.(vec(collect(g.landmask)))
+    marr, mref = metric_arrays(g)
+    pg = Ref(pigrid(g, dzF, dzC, lm, mref === nothing ? C_NULL : Ptr{Cvoid}(Base.unsafe_convert(Ptr{PiGridMetrics}, mref))))
+    pb = Ref(PiBgc(bgc))
+    ps = [PiMacro(phyt, s) for s in 1:Nsp]
+    out = Ref{Ptr{Cvoid}}(C_NULL)
+    st = GC.@preserve dzF dzC lm marr mref ccall((:pi_create_macro, lib), Int32,
+        (Ref{PiGrid}, Ref{PiBgc}, Ptr{PiMacro}, Int32, Int64, Int32, UInt64, Ref{Ptr{Cvoid}}),
+        pg, pb, ps, Nsp, maxN, PI_FP64, seed, out)
+    check(st, C_NULL)
+    m = Model(out[], (g.Nx + 2g.Hx, g.Ny + 2g.Hy, g.Nz + 2g.Hz), Nsp, maxN, false, true)
     finalizer(destroy, m)
     m
 end
@@ -191,17 +228,20 @@ function destroy(m::Model)
 end
 
 """Upload species `sp` (1-based) from a StructArray-like table with the mode's columns
-(QuotaMode: Cq, Nq, Pq; CarbonMode: Bd)."""
+(QuotaMode: Sz, Bm, Cq, Nq, Pq; CarbonMode: Sz, Bm, Bd; MacroMolecularMode: PRO, DNA, RNA, CH, NST, PST)."""
 function set_individuals!(m::Model, sp::Integer, d)
     C = m.capacity
-    quota = m.carbon ? (zeros(Float64, C), zeros(Float64, C), zeros(Float64, C)) :
-                       (Float64.(d.Cq), Float64.(d.Nq), Float64.(d.Pq))
+    z() = zeros(Float64, C)
+    szbm = m.mm ? (z(), z()) : (Float64.(d.Sz), Float64.(d.Bm))
+    quota = (m.carbon || m.mm) ? (z(), z(), z()) : (Float64.(d.Cq), Float64.(d.Nq), Float64.(d.Pq))
     bd = m.carbon ? Float64.(d.Bd) : Float64[]
+    pools = m.mm ? map(k -> Float64.(getproperty(d, k)), (:PRO, :DNA, :RNA, :CH, :NST, :PST)) : ()
     cols = (Float64.(d.x), Float64.(d.y), Float64.(d.z), Int64.(d.xi), Int64.(d.yi), Int64.(d.zi),
-            Float64.(d.Sz), Float64.(d.Bm), quota..., Float64.(d.Chl), Float64.(d.gen), Float64.(d.age),
+            szbm..., quota..., Float64.(d.Chl), Float64.(d.gen), Float64.(d.age),
             UInt8.(d.ac), Float64.(d.graz), Float64.(d.mort), Float64.(d.dvid))
-    GC.@preserve cols bd begin
-        pi = Ref(PiIndividuals(map(pointer, cols)..., m.carbon ? pointer(bd) : Ptr{Float64}(C_NULL)))
+    GC.@preserve cols bd pools begin
+        pp = m.mm ? map(pointer, pools) : ntuple(_ -> Ptr{Float64}(C_NULL), 6)
+        pi = Ref(PiIndividuals(map(pointer, cols)..., m.carbon ? pointer(bd) : Ptr{Float64}(C_NULL), pp...))
         check(ccall((:pi_set_individuals, lib), Int32, (Ptr{Cvoid}, Int32, Ref{PiIndividuals}), m.h, sp - 1, pi), m.h)
     end
 end
@@ -212,11 +252,15 @@ function get_individuals(m::Model, sp::Integer)
     f = ntuple(_ -> zeros(Float64, C), 3); i = ntuple(_ -> zeros(Int64, C), 3)
     q = ntuple(_ -> zeros(Float64, C), 8); ac = zeros(UInt8, C); dec = ntuple(_ -> zeros(Float64, C), 3)
     bd = zeros(Float64, C)
-    GC.@preserve f i q ac dec bd begin
+    pools = ntuple(_ -> zeros(Float64, C), 6)
+    GC.@preserve f i q ac dec bd pools begin
         pi = Ref(PiIndividuals(pointer(f[1]), pointer(f[2]), pointer(f[3]), pointer(i[1]), pointer(i[2]), pointer(i[3]),
-                               map(pointer, q)..., pointer(ac), map(pointer, dec)..., pointer(bd)))
+                               map(pointer, q)..., pointer(ac), map(pointer, dec)..., pointer(bd), map(pointer, pools)...))
         check(ccall((:pi_get_individuals, lib), Int32, (Ptr{Cvoid}, Int32, Ref{PiIndividuals}), m.h, sp - 1, pi), m.h)
     end
+    m.mm && return (x = f[1], y = f[2], z = f[3], xi = i[1], yi = i[2], zi = i[3], PRO = pools[1], DNA = pools[2],
+                       RNA = pools[3], CH = pools[4], NST = pools[5], PST = pools[6], Chl = q[6], gen = q[7], age = q[8],
+                       ac = ac .== 1, graz = dec[1], mort = dec[2], dvid = dec[3])
     m.carbon ? (x = f[1], y = f[2], z = f[3], xi = i[1], yi = i[2], zi = i[3], Sz = q[1], Bm = q[2], Bd = bd,
                 Chl = q[6], gen = q[7], age = q[8], ac = ac .== 1, graz = dec[1], mort = dec[2], dvid = dec[3]) :
                (x = f[1], y = f[2], z = f[3], xi = i[1], yi = i[2], zi = i[3], Sz = q[1], Bm = q[2], Cq = q[3], Nq = q[4],
