@@ -1207,6 +1207,56 @@ __device__ __forceinline__ float getbc32(const FluxBC32& b, int a, int c, int64_
     return b.v[(a - 1) + (long long)b.n1 * ((c - 1) + (long long)b.n2 * (t - 1))];
 }
 
+// Pairs of FP32 values — the same cell of tracers 2p and 2p+1 — in one 64-bit register, for the
+// packed FP32 instructions of sm_100 (add/sub/mul/fma .rn.f32x2). Each half is rounded exactly as the
+// scalar __fadd_rn, __fsub_rn, __fmul_rn and __fmaf_rn, so the packed x-y tile gives the same bits
+// as xy_tile while issuing one instruction for two tracers.
+typedef unsigned long long fx2;
+__device__ __forceinline__ fx2 fx2_of(float lo, float hi) {
+    fx2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void fx2_split(fx2 v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ fx2 fx2_add(fx2 a, fx2 b) { fx2 d; asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b)); return d; }
+__device__ __forceinline__ fx2 fx2_sub(fx2 a, fx2 b) { fx2 d; asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b)); return d; }
+__device__ __forceinline__ fx2 fx2_mul(fx2 a, fx2 b) { fx2 d; asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b)); return d; }
+__device__ __forceinline__ fx2 fx2_fma(fx2 a, fx2 b, fx2 c) {
+    fx2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ fx2 fx2_neg(fx2 a) { return a ^ 0x8000000080000000ull; }   // exact sign flips
+
+// the face coefficients of one face for both halves
+struct FCu2 { fx2 tr, d0c, d1c, R; bool pos; };
+__device__ __forceinline__ FCu2 fcu2(const FCu& f) {
+    FCu2 g;
+    g.tr = fx2_of(f.tr, f.tr); g.d0c = fx2_of(f.d0c, f.d0c); g.d1c = fx2_of(f.d1c, f.d1c); g.R = fx2_of(f.R, f.R);
+    g.pos = f.tr > 0.0f;
+    return g;
+}
+// flux_h of an all-water face for two tracers: the upwind operands are selected first (the
+// selected difference and the sum c0 − ψ = c0 + (−ψ) are the same IEEE operations), the limiter
+// (min/max, no packed form) runs per half
+__device__ __forceinline__ fx2 flux_h2(const FCu2& f, fx2 cm2, fx2 cm1, fx2 c0, fx2 cp1) {
+    const fx2 d0 = fx2_sub(c0, cm1);
+    const fx2 dn = f.pos ? fx2_sub(cm1, cm2) : fx2_sub(cp1, c0);
+    const fx2 a = fx2_fma(f.d0c, d0, fx2_mul(f.d1c, dn)), b = fx2_mul(f.R, dn);
+    float d0l, d0h, al, ah, bl, bh;
+    fx2_split(d0, d0l, d0h); fx2_split(a, al, ah); fx2_split(b, bl, bh);
+    const float pl = d0l >= 0.0f ? fmaxf(0.0f, fminf(fminf(d0l, al), bl)) : fminf(0.0f, fmaxf(fmaxf(d0l, al), bl));
+    const float ph = d0h >= 0.0f ? fmaxf(0.0f, fminf(fminf(d0h, ah), bh)) : fminf(0.0f, fmaxf(fmaxf(d0h, ah), bh));
+    const fx2 ps = fx2_of(pl, ph);
+    return fx2_mul(f.tr, f.pos ? fx2_add(cm1, ps) : fx2_add(c0, fx2_neg(ps)));
+}
+// upd_sweep for two tracers: v − dtv·(ΔF − c·ftr)
+__device__ __forceinline__ fx2 upd_sweep2(fx2 v, fx2 ndtv, fx2 dF, fx2 c, fx2 ftr) {
+    return fx2_fma(ndtv, fx2_fma(fx2_neg(c), ftr, dF), v);
+}
+
 struct TrArgs {
     Tab32 T;
     const int4* items;          // k32_xy: {member, i0, j0, level}; k32_ztail: {member, i0, j, k0}
@@ -1349,6 +1399,92 @@ __device__ __forceinline__ void xy_tile(const TrArgs& a, const MemberDev& m, con
     __syncthreads();
 }
 
+// xy_tile for an all-water member with the 14 tracers handled as 7 packed pairs: the same tile,
+// threads and operations, with shared memory laid out [row][pair][lane] of 64-bit pairs so that a
+// lane reads or writes both tracers of a pair with one access.
+template <int TY>
+__device__ __forceinline__ void xy_tile_pk(const TrArgs& a, const MemberDev& m, const int4 it, float* sm,
+                                           float& pu, float* pv, float3& pvy, int next) {
+    constexpr int NP = PI_NTRACERS / 2;
+    fx2* TA = reinterpret_cast<fx2*>(sm);                 // (TY+4) × 7 × 32
+    fx2* FY = TA + (TY + 4) * NP * 32;                     // (TY+1) × 7 × 32
+    fx2* TRs = FY + (TY + 1) * NP * 32;                    // TY × 7 × 32
+    auto at = [](fx2* base, int r, int p, int l) -> fx2& { return base[(r * NP + p) * 32 + l]; };
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const long long G = a.Gtot;
+    const float dT = a.dT;
+    const int i0 = it.y, j0 = it.z, L = it.w;
+    const long long off = m.cell_off;
+    const float dz = a.dzF[m.dz_off + L - 1];
+    const float az = __fmul_rn(m.dx, m.dy), dtv = __fdiv_rn(dT, __fmul_rn(az, dz));
+    const fx2 ndtv = fx2_of(-dtv, -dtv);
+    // ---- x sweep of row j0-2+wid
+    {
+        const int i = i0 - 2 + lane;
+        const float ax = __fmul_rn(m.dy, dz);
+        const float uw = pu;
+        const float ue = __shfl_down_sync(0xffffffffu, uw, 1);
+        const FCu2 fc = fcu2(fcu(uw, ax, __frcp_rn(m.dx), dT));
+        const bool east_zero = i == m.Nx + m.Hx && m.tx != PI_PERIODIC;   // fill_halo_east_Gc! (Bounded)
+        const float ftr1 = tdiff(ax, ue, uw);
+        const fx2 ftr = fx2_of(ftr1, ftr1);
+        const bool store_tr = wid >= 2 && wid < TY + 2;
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+            const float v0 = pv[2 * p], v1 = pv[2 * p + 1];
+            const fx2 v = fx2_of(v0, v1);
+            const fx2 cm2 = fx2_of(__shfl_up_sync(0xffffffffu, v0, 2), __shfl_up_sync(0xffffffffu, v1, 2));
+            const fx2 cm1 = fx2_of(__shfl_up_sync(0xffffffffu, v0, 1), __shfl_up_sync(0xffffffffu, v1, 1));
+            const fx2 cp1 = fx2_of(__shfl_down_sync(0xffffffffu, v0, 1), __shfl_down_sync(0xffffffffu, v1, 1));
+            const fx2 Fw = flux_h2(fc, cm2, cm1, v, cp1);
+            float wl, wh;
+            fx2_split(Fw, wl, wh);
+            fx2 Fe = fx2_of(__shfl_down_sync(0xffffffffu, wl, 1), __shfl_down_sync(0xffffffffu, wh, 1));
+            if (east_zero) Fe = 0ull;
+            at(TA, wid, p, lane) = upd_sweep2(v, ndtv, fx2_sub(Fe, Fw), v, ftr);
+            if (store_tr) at(TRs, wid - 2, p, lane) = v;
+        }
+    }
+    __syncthreads();
+    // the registers of this item's x inputs are free: start the next item's loads
+    const float3 vy = pvy;
+    if (next < a.nitems) xy_load(a, next, pu, pv, pvy);
+    // ---- y faces j0 + r, r = 0..TY
+    const int i = i0 - 2 + lane;
+    const bool col = lane >= 2 && lane < 30 && i <= m.Nx + m.Hx;
+    const float ay = __fmul_rn(m.dx, dz);
+    if (wid <= TY) {
+        const int r = wid, f = j0 + r;
+        const bool special = f == m.Ny + m.Hy + 1;
+        const bool zero = !col || f > m.Ny + m.Hy + 1 || (special && m.ty != PI_PERIODIC);
+        const FCu2 fc = fcu2(fcu(zero ? 0.0f : vy.x, ay, __frcp_rn(m.dy), dT));
+#pragma unroll
+        for (int p = 0; p < NP; ++p)
+            at(FY, r, p, lane) = zero ? 0ull : flux_h2(fc, at(TA, r, p, lane), at(TA, r + 1, p, lane), at(TA, r + 2, p, lane),
+                                                      at(TA, r + 3, p, lane));
+    }
+    __syncthreads();
+    // ---- y update of row j0 + wid
+    if (wid < TY) {
+        const int j = j0 + wid;
+        if (col && j <= m.Ny + m.Hy) {
+            const int q = gid3(m, i, j, L);
+            const float ftr1 = tdiff(ay, vy.z, vy.y);
+            const fx2 ftr = fx2_of(ftr1, ftr1);
+            float* dst = a.tb + off + q;
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                const fx2 dG = fx2_sub(at(FY, wid + 1, p, lane), at(FY, wid, p, lane));
+                float lo, hi;
+                fx2_split(upd_sweep2(at(TA, wid + 2, p, lane), ndtv, dG, at(TRs, wid, p, lane), ftr), lo, hi);
+                dst[(2 * p) * G] = lo;
+                dst[(2 * p + 1) * G] = hi;
+            }
+        }
+    }
+    __syncthreads();
+}
+
 template <int TY>
 __global__ void __launch_bounds__(32 * (TY + 4)) k32_xy(TrArgs a) {
     if (stopped(a.err)) return;
@@ -1361,7 +1497,7 @@ __global__ void __launch_bounds__(32 * (TY + 4)) k32_xy(TrArgs a) {
         const int4 it = a.items[item];
         const MemberDev& m = a.T.md[it.x];
         const int next = item + gridDim.x;
-        if (m.all_water) xy_tile<TY, false>(a, m, it, sm, pu, pv, pvy, next);
+        if (m.all_water) xy_tile_pk<TY>(a, m, it, sm, pu, pv, pvy, next);
         else xy_tile<TY, true>(a, m, it, sm, pu, pv, pvy, next);
     }
 }
