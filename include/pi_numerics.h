@@ -192,7 +192,10 @@ PI_HD void pi_philox4x32_10(const uint32_t ctr_in[4], const uint32_t key_in[2], 
 
 /* Draw purposes: one Philox block gives the three draws of one call site for one slot. */
 enum { PI_DRAW_DIFFUSION = 0,   /* rnd.x, rnd.y, rnd.z of particle_diffusion!          */
-       PI_DRAW_DECISION  = 1 }; /* rnd.x, rnd.y, rnd.z of get_probability! (graz, mort, dvid) */
+       PI_DRAW_DECISION  = 1,   /* rnd.x, rnd.y, rnd.z of get_probability! (graz, mort, dvid) */
+       PI_DRAW_ABIO_DIFFUSION = 2,   /* particle_diffusion! of abiotic species `species`     */
+       PI_DRAW_ABIO_BC   = 3,   /* rnd_3d of particles_from_bcs! (abiotic species, cell)    */
+       PI_DRAW_RELEASE   = 4 }; /* rnd.x of get_release_probability! (release pair, slot)   */
 
 /* Three uniforms in [0, 1) on the 2^-24 lattice for (seed, iteration, species, purpose, slot). */
 PI_HD void pi_draw3(uint64_t seed, uint32_t iteration, uint32_t species, uint32_t purpose,

@@ -67,6 +67,10 @@ enum { PI_BC_NONE = 0, PI_BC_CONST, PI_BC_ARRAY2D, PI_BC_ARRAY3D };
  * PI_DIAG_PROC + process index (diags.phytos[sp][process], diags_spcs!,
  * Diagnostics/diagnostics_kernels.jl:14-33) in QuotaMode's order below. */
 enum { PI_DIAG_PAR = 0, PI_DIAG_NUM, PI_DIAG_GRAZ, PI_DIAG_MORT, PI_DIAG_DVID,
+       PI_DIAG_PTC,        /* diags.phytos[sp].ptc: Σ ptc·ac per cell (time_step.jl:140-149), kept
+                              while the model has abiotic species                               */
+       PI_DIAG_ABIO_NUM,   /* diags.abiotics[sa].num (time_step.jl:151-158): sp is the abiotic
+                              species                                                            */
        PI_DIAG_TRACER = 16, PI_DIAG_PROC = 32 };
 enum { PI_PROC_PS = 0, PI_PROC_BS, PI_PROC_VDOC, PI_PROC_VNH4, PI_PROC_VNO3, PI_PROC_VPO4, PI_PROC_resp,
        PI_PROC_exu, PI_PROC_Bm, PI_PROC_Cq, PI_PROC_Nq, PI_PROC_Pq, PI_PROC_Chl, PI_NPROC };
@@ -164,6 +168,8 @@ typedef struct {
     double  *Bd;
     double  *PRO, *DNA, *RNA, *CH, *NST, *PST;   /* MacroMolecularMode only (protein, DNA, RNA,
                                                   carbohydrate/lipid, N and P reserves) */
+    double  *ptc;                                /* abiotic particles held (every mode); NULL on
+                                                  pi_set_individuals sets zeros */
 } pi_individuals;
 
 typedef struct pi_model pi_model;
@@ -227,6 +233,48 @@ pi_status pi_set_temp(pi_model* m, const double* temp);
  * the face's (n1, n2) array; PI_BC_ARRAY3D reads (n1, n2, nt), indexed by model.iteration. */
 pi_status pi_set_flux_bc(pi_model* m, int32_t tracer, int32_t face, int32_t kind,
                          const double* values, int64_t nt);
+
+/* Abiotic particles (src/Individuals/Abiotic/): the parameters of construct_abiotic_particle
+ * (particle_generation.jl:1-22) in its param_names order; defaults in abiotic_params_default
+ * (src/Parameters/param_default.jl:329-343). */
+typedef struct {
+    double Nsuper, Rd, release_P, sz_min, Ktr;
+} pi_abiotic_params;
+
+/* The state of one abiotic species (particle_generation.jl:2-5), `capacity` long: positions in
+ * grid-spacing units, the halo-inclusive cell indices of the last find_inds! and the activity
+ * flag. pi_set_abiotic_particles requires x, y, z and ac; NULL xi, yi, zi are taken as find_inds!
+ * of the positions (the state initialize_abiotic_particle! leaves, particle_generation.jl:24-35).
+ * For pi_get_abiotic_particles NULL members are skipped. */
+typedef struct {
+    double  *x, *y, *z;
+    int64_t *xi, *yi, *zi;
+    uint8_t *ac;
+} pi_abiotic_particles;
+
+/* PlanktonModel(...; abiotic = abiotic_setup(params, N, Nsa, Palat(intac, release)),
+ * max_candidates) (src/Model/models.jl:99-146) for a PI_FP64 model (PI_FP32 is refused with
+ * PI_ERR_ARG): `nsa` abiotic species, all inactive until pi_set_abiotic_particles. Palat's pairs
+ * are 0-based (phytoplankton species, abiotic species) index pairs, 2·n_intac and 2·n_release
+ * int32 values, applied in the order given: intac by particle_interaction! and release by
+ * particle_release! (time_step.jl:121-137). max_ptc[sp] is phytoplankton species sp's max_ptc
+ * parameter, NaN for a mode whose parameters have none (QuotaMode, CarbonMode and
+ * MacroMolecularMode): there the reference's merge kernel fails on the field access, and here
+ * the step that would merge a particle into such a species returns PI_ERR_PARAM. Called once,
+ * before the first step. */
+pi_status pi_set_abiotics(pi_model* m, int32_t nsa, const pi_abiotic_params* params,
+                          int32_t n_intac, const int32_t* intac, int32_t n_release, const int32_t* release,
+                          int32_t max_candidates, const double* max_ptc);
+pi_status pi_set_abiotic_particles(pi_model* m, int32_t sa, const pi_abiotic_particles* in);
+pi_status pi_get_abiotic_particles(pi_model* m, int32_t sa, pi_abiotic_particles* out);
+/* Active abiotic particles of species sa (calc_active_individuals, models.jl:157-164). */
+pi_status pi_count_abiotic(pi_model* m, int32_t sa, int64_t* n);
+
+/* set_bc_particle!(model; sa, pos, bc_value) (HaloRegions/boundary_conditions.jl:33-41): the flux
+ * of particles through one face of abiotic species sa that particles_from_bcs! turns into new
+ * particles (Abiotic/particle_interaction.jl:138-239), with pi_set_flux_bc's kinds and layout. */
+pi_status pi_set_abiotic_bc(pi_model* m, int32_t sa, int32_t face, int32_t kind,
+                            const double* values, int64_t nt);
 
 /* TimeStep!(model, ΔT, diags) (src/Model/time_step.jl:12-180), QuotaMode physiology. Advances
  * model.iteration by one and model.t to iteration·ΔT. Returns PI_ERR_CAPACITY with the

@@ -109,9 +109,23 @@ struct Species {
     int macro = 0;
     pi_macro_params mp{};
     dvec PRO, DNA, RNA, CH, NST, PST, S_PRO, S_DNA, S_RNA;
+    /* abiotic particles held (ptc, every mode's plankton_generation.jl) and their diagnostic */
+    dvec ptc, d_ptc;
 };
 
 struct FluxBC { int kind = PI_BC_NONE; dvec v; int64_t nt = 0; };
+
+/* One abiotic species, construct_abiotic_particle (Abiotic/particle_generation.jl:1-22): the
+ * positions, the find_inds! cells and the activity flag of `capacity` slots, its parameters, the
+ * particle flux boundary conditions (abiotic_particle.bc) and diags.abiotics[sa].num. */
+struct Abiotic {
+    pi_abiotic_params p{};
+    dvec x, y, z;
+    std::vector<int64_t> xi, yi, zi;
+    std::vector<uint8_t> ac;
+    FluxBC bc[6];
+    dvec d_num;
+};
 
 }  // namespace
 
@@ -134,6 +148,14 @@ struct orc_model {
     uint32_t tr_mask = 0, proc_mask = 0;  /* optional diagnostics (PlanktonDiagnostics keywords) */
     std::vector<dvec> d_tr;               /* 14 fields when any tracer is enabled */
     FluxBC bc[PI_NTRACERS][6];
+    /* abiotic particles (abiotic_setup): species, Palat pairs (phytoplankton, abiotic), the
+     * candidate table intac (max_candidates × capacity, timestepper.jl:52) and max_ptc per
+     * phytoplankton species (NaN: the mode has no such parameter) */
+    std::vector<Abiotic> ab;
+    std::vector<std::pair<int, int>> pal_intac, pal_release;
+    int maxc = 25;
+    dvec max_ptc;
+    std::vector<int64_t> intac;
     int64_t iteration;
     double t;
     uint32_t err_flags;
@@ -269,7 +291,8 @@ double itpl(orc_model* m, const dvec& f, int comp, double x, double y, double z,
 }
 
 /* vel_interpolate_kernel!, particle_advection_kernels.jl:26-31 */
-void vel_interpolate(orc_model* m, Species& s, const dvec& X, const dvec& Y, const dvec& Z,
+template <class P>
+void vel_interpolate(orc_model* m, P& s, const dvec& X, const dvec& Y, const dvec& Z,
                      const dvec& U, const dvec& V, const dvec& W) {
     int64_t C = m->C;
     #pragma omp parallel for schedule(static)
@@ -282,7 +305,8 @@ void vel_interpolate(orc_model* m, Species& s, const dvec& X, const dvec& Y, con
 }
 
 /* calc_coord_kernel!, particle_advection_kernels.jl:40-45 */
-void calc_coord(orc_model* m, Species& s, dvec& oX, dvec& oY, dvec& oZ,
+template <class P>
+void calc_coord(orc_model* m, P& s, dvec& oX, dvec& oY, dvec& oZ,
                 const dvec& U, const dvec& V, const dvec& W, double dT, double weight) {
     int64_t C = m->C;
     #pragma omp parallel for schedule(static)
@@ -296,7 +320,8 @@ void calc_coord(orc_model* m, Species& s, dvec& oX, dvec& oY, dvec& oZ,
 }
 
 /* particle_boundaries_kernel!, particle_advection_kernels.jl:13-17 */
-void particle_boundaries(orc_model* m, Species& s, dvec& X, dvec& Y, dvec& Z) {
+template <class P>
+void particle_boundaries(orc_model* m, P& s, dvec& X, dvec& Y, dvec& Z) {
     const Grid& g = m->g;
     int64_t C = m->C;
     #pragma omp parallel for schedule(static)
@@ -309,7 +334,8 @@ void particle_boundaries(orc_model* m, Species& s, dvec& X, dvec& Y, dvec& Z) {
 }
 
 /* particle_advection!, particle_advection.jl:2-56 (RK4) */
-void particle_advection(orc_model* m, Species& s, double dT) {
+template <class P>
+void particle_advection(orc_model* m, P& s, double dT) {
     int64_t C = m->C;
     vel_interpolate(m, s, s.x, s.y, s.z, m->u0, m->v0, m->w0);
     for (int64_t i = 0; i < C; ++i) { m->vu2[i] = m->vu1[i]; m->vv2[i] = m->vv1[i]; m->vw2[i] = m->vw1[i]; }
@@ -345,13 +371,14 @@ void particle_advection(orc_model* m, Species& s, double dT) {
 }
 
 /* particle_diffusion!, particle_diffusion.jl:16-33 */
-void particle_diffusion(orc_model* m, Species& s, int spi, double dT) {
+template <class P>
+void particle_diffusion(orc_model* m, P& s, int spi, double dT, uint32_t purpose = PI_DRAW_DIFFUSION) {
     const Grid& g = m->g;
     int64_t C = m->C;
     double kx = m->bgc.kappa_hP, ky = m->bgc.kappa_hP, kz = m->bgc.kappa_vP;
     #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < C; ++i)
-        pi_draw3(m->seed, (uint32_t)m->iteration, (uint32_t)spi, PI_DRAW_DIFFUSION, (uint32_t)i,
+        pi_draw3(m->seed, (uint32_t)m->iteration, (uint32_t)spi, purpose, (uint32_t)i,
                  &m->rx[i], &m->ry[i], &m->rz[i]);
     for (int64_t i = 0; i < C; ++i) {
         m->rx[i] = (m->rx[i] - 0.5) * 2.0; m->ry[i] = (m->ry[i] - 0.5) * 2.0; m->rz[i] = (m->rz[i] - 0.5) * 2.0;
@@ -380,7 +407,8 @@ void particle_diffusion(orc_model* m, Species& s, int spi, double dT) {
 /* Particle-grid coupling, src/Individuals/utils.jl                                            */
 /* ---------------------------------------------------------------------------------------- */
 
-void find_inds(orc_model* m, Species& s) {     /* utils.jl:2-7 */
+template <class P>
+void find_inds(orc_model* m, P& s) {     /* utils.jl:2-7 */
     const Grid& g = m->g;
     #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < m->C; ++i) {
@@ -391,7 +419,8 @@ void find_inds(orc_model* m, Species& s) {     /* utils.jl:2-7 */
     }
 }
 
-inline size_t cell_of(orc_model* m, const Species& s, int64_t i) {
+template <class P>
+inline size_t cell_of(orc_model* m, const P& s, int64_t i) {
     const Grid& g = m->g;
     long a = clampi(m, (long)s.xi[i], 1, g.Gx);
     long b = clampi(m, (long)s.yi[i], 1, g.Gy);
@@ -1302,6 +1331,181 @@ void tracer_update(orc_model* m, double dT) {
 
 void zero(dvec& v) { std::fill(v.begin(), v.end(), 0.0); }
 
+/* ---------------------------------------------------------------------------------------- */
+/* Abiotic particles, src/Individuals/Abiotic/particle_interaction.jl                          */
+/* ---------------------------------------------------------------------------------------- */
+
+/* The capacity error of particle_release! and particles_from_bcs! (:128-130, :252-271). */
+std::string abiotic_capacity_message(double t) {
+    const std::string s = capacity_message(t);
+    return "number of abiotic particles exceeds the capacity at timestep " + s.substr(s.find("timestep ") + 9);
+}
+
+/* particles_from_bcs!, :252-271, with calc_particle_bcs! (:142-229). A boundary cell of a face
+ * with a particle flux becomes a particle when rnd·sz_min·Nsuper < flux·ΔT·area (rnd one draw per
+ * cell and step). The faces write in the order top, bottom, east, west, north, south, so a later
+ * face decides a cell two faces share (edges; top and bottom when Nz = 1). New particles take the
+ * free slots in ascending order, cells in column-major order (findall), at cell − halo − 0.4 on
+ * each axis, computed in Float32 (Int − Float32 promotes to Float32, :239-244). Their cell indices
+ * stay as the slot held them until find_inds!. */
+int particles_from_bcs(orc_model* m, Abiotic& a, int sa, double dT) {
+    const Grid& g = m->g;
+    const int64_t it = m->iteration;
+    const FluxBC* b = a.bc;
+    bool any = false;
+    for (int f = 0; f < 6; ++f) any = any || b[f].kind != PI_BC_NONE;
+    if (!any) return PI_OK;
+    std::vector<uint8_t> flag(g.G, 0);
+    auto set = [&](long i, long j, long k, double flux, double area) {
+        double r0, r1, r2;
+        pi_draw3(m->seed, (uint32_t)it, (uint32_t)sa, PI_DRAW_ABIO_BC, (uint32_t)g.id(i, j, k), &r0, &r1, &r2);
+        flag[g.id(i, j, k)] = (uint8_t)jl_isless(r0 * a.p.sz_min * a.p.Nsuper, flux * dT * area);
+    };
+    if (b[PI_TOP].kind) for (long j = 1; j <= g.Ny; ++j) for (long i = 1; i <= g.Nx; ++i)
+        set(i + g.Hx, j + g.Hy, 1 + g.Hz, getbc(b[PI_TOP], g.Nx, g.Ny, i, j, it), g.Az(i + g.Hx, j + g.Hy));
+    if (b[PI_BOTTOM].kind) for (long j = 1; j <= g.Ny; ++j) for (long i = 1; i <= g.Nx; ++i)
+        set(i + g.Hx, j + g.Hy, g.Nz + g.Hz, getbc(b[PI_BOTTOM], g.Nx, g.Ny, i, j, it), g.Az(i + g.Hx, j + g.Hy));
+    if (b[PI_EAST].kind) for (long k = 1; k <= g.Nz; ++k) for (long j = 1; j <= g.Ny; ++j)
+        set(g.Nx + g.Hx, j + g.Hy, k + g.Hz, getbc(b[PI_EAST], g.Ny, g.Nz, j, k, it), g.Axk(g.Nx + g.Hx, j + g.Hy, k + g.Hz));
+    if (b[PI_WEST].kind) for (long k = 1; k <= g.Nz; ++k) for (long j = 1; j <= g.Ny; ++j)
+        set(1 + g.Hx, j + g.Hy, k + g.Hz, getbc(b[PI_WEST], g.Ny, g.Nz, j, k, it), g.Axk(1 + g.Hx, j + g.Hy, k + g.Hz));
+    if (b[PI_NORTH].kind) for (long k = 1; k <= g.Nz; ++k) for (long i = 1; i <= g.Nx; ++i)
+        set(i + g.Hx, g.Ny + g.Hy, k + g.Hz, getbc(b[PI_NORTH], g.Nx, g.Nz, i, k, it), g.Ayk(i + g.Hx, g.Ny + g.Hy, k + g.Hz));
+    if (b[PI_SOUTH].kind) for (long k = 1; k <= g.Nz; ++k) for (long i = 1; i <= g.Nx; ++i)
+        set(i + g.Hx, 1 + g.Hy, k + g.Hz, getbc(b[PI_SOUTH], g.Nx, g.Nz, i, k, it), g.Ayk(i + g.Hx, 1 + g.Hy, k + g.Hz));
+    size_t n = 0;
+    for (size_t q = 0; q < g.G; ++q) n += flag[q];
+    if (n == 0) return PI_OK;                                          /* sum(tr_temp) == 0 */
+    std::vector<int64_t> freel;
+    for (int64_t k = 0; k < m->C; ++k) if (!a.ac[k]) freel.push_back(k);
+    if (n > freel.size()) { m->err = abiotic_capacity_message(m->t); return PI_ERR_CAPACITY; }
+    size_t r = 0;
+    for (size_t q = 0; q < g.G; ++q) {
+        if (!flag[q]) continue;
+        const long i = (long)(q % (size_t)g.Gx) + 1, j = (long)((q / (size_t)g.Gx) % (size_t)g.Gy) + 1;
+        const long k = (long)(q / ((size_t)g.Gx * (size_t)g.Gy)) + 1;
+        const int64_t d = freel[r++];
+        a.ac[d] = 1;
+        a.x[d] = (double)((float)(i - g.Hx) - 0.4f);
+        a.y[d] = (double)((float)(j - g.Hy) - 0.4f);
+        a.z[d] = (double)((float)(k - g.Hz) - 0.4f);
+    }
+    return PI_OK;
+}
+
+/* calc_distance, :3-15: the distance in metres of two particles whose find_inds! cells are equal
+ * (ΔxF, ΔyF, ΔzF at the first one's cell), else 1.0f20. dx^2.0f0 is Float64^Float64 with an
+ * integral exponent, which Julia evaluates as the integer power. */
+inline double calc_distance(const Grid& g, int64_t xi1, int64_t yi1, int64_t zi1, double x1, double y1, double z1,
+                            int64_t xi2, int64_t yi2, int64_t zi2, double x2, double y2, double z2) {
+    if (xi1 == xi2 && yi1 == yi2 && zi1 == zi2) {
+        const double dx = (x1 - x2) * g.dxF(xi1, yi1);
+        const double dy = (y1 - y2) * g.dyF(xi1, yi1);
+        const double dz = (z1 - z2) * g.dzF1(zi1);
+        return sqrt(pi_pow_int(dx, 2) + pi_pow_int(dy, 2) + pi_pow_int(dz, 2));
+    }
+    return (double)1.0e20f;
+}
+
+/* particle_interaction!, :18-81, as a single-threaded run of its kernels leaves it.
+ * calc_interaction_kernel! (:24-40) writes intac[(i % max_candidates) + 1, k] = i for every
+ * active phytoplankton i (1-based, ascending) within Rd of active particle k, so an entry ends
+ * with the largest such i; merge_particle_kernel! (:50-66) walks the particles in ascending k,
+ * each merging into its first candidate whose ptc is below max_ptc (ptc += 1, the particle
+ * inactive). This is the reference's scan over every pair. */
+int particle_interaction(orc_model* m, Species& pl, Abiotic& a, int sp) {
+    const Grid& g = m->g;
+    const int64_t C = m->C, K = m->maxc;
+    std::fill(m->intac.begin(), m->intac.end(), 0);                    /* reset_interaction! */
+    for (int64_t i = 0; i < C; ++i) {
+        if (!pl.ac[i]) continue;
+        for (int64_t k = 0; k < C; ++k) {
+            if (!a.ac[k]) continue;
+            const double dist = calc_distance(g, pl.xi[i], pl.yi[i], pl.zi[i], pl.x[i], pl.y[i], pl.z[i],
+                                              a.xi[k], a.yi[k], a.zi[k], a.x[k], a.y[k], a.z[k]);
+            if (dist < a.p.Rd) m->intac[(size_t)k * (size_t)K + (size_t)((i + 1) % K)] = i + 1;
+        }
+    }
+    for (int64_t k = 0; k < C; ++k) {
+        if (!a.ac[k]) continue;
+        for (int64_t j = 0; j < K; ++j) {
+            const int64_t pid = m->intac[(size_t)k * (size_t)K + (size_t)j];
+            if (pid <= 0) continue;
+            const double mp = m->max_ptc[sp];
+            if (mp != mp) { m->err = "type NamedTuple has no field max_ptc"; return PI_ERR_PARAM; }
+            if (pl.ptc[pid - 1] < mp) { pl.ptc[pid - 1] += 1.0; a.ac[k] = 0; break; }
+        }
+    }
+    return PI_OK;
+}
+
+/* particle_release!, :124-137, with get_release_probability! (:85-91), get_tind! (utils.jl:76-86)
+ * and release_abiotic_particle_kernel! (:93-101). An active phytoplankton releases one particle
+ * when rnd.x < release_P·ΔT·ptc; releasers take the free particle slots in ascending order. The
+ * particle goes to the phytoplankton's position plus (rnd.x, rnd.y, rnd.z): rnd.x is the release
+ * draw, rnd.y and rnd.z still hold the mortality and division draws of the last species'
+ * get_probability! (calc_release_position!, :109-122, is not called). Its cell indices stay as
+ * the slot held them until the next find_inds!. */
+int particle_release(orc_model* m, Species& pl, Abiotic& a, int pair, double dT) {
+    const int64_t C = m->C;
+    std::vector<uint8_t> R((size_t)C, 0);
+    dvec rx((size_t)C);
+    int64_t nrel = 0;
+    for (int64_t i = 0; i < C; ++i) {
+        double r1, r2;
+        pi_draw3(m->seed, (uint32_t)m->iteration, (uint32_t)pair, PI_DRAW_RELEASE, (uint32_t)i, &rx[i], &r1, &r2);
+        R[i] = (uint8_t)(jl_isless(rx[i], a.p.release_P * dT * pl.ptc[i]) && pl.ac[i]);
+        nrel += R[i];
+    }
+    std::vector<int64_t> freel;
+    for (int64_t k = 0; k < C; ++k) if (!a.ac[k]) freel.push_back(k);
+    if (nrel > (int64_t)freel.size()) { m->err = abiotic_capacity_message(m->t); return PI_ERR_CAPACITY; }
+    size_t r = 0;
+    for (int64_t i = 0; i < C; ++i) {
+        if (!R[i]) continue;
+        double d0, dy, dz;
+        pi_draw3(m->seed, (uint32_t)m->iteration, (uint32_t)(m->nsp - 1), PI_DRAW_DECISION, (uint32_t)i, &d0, &dy, &dz);
+        const int64_t d = freel[r++];
+        a.ac[d] = 1;
+        a.x[d] = pl.x[i] + rx[i];
+        a.y[d] = pl.y[i] + dy;
+        a.z[d] = pl.z[i] + dz;
+        pl.ptc[i] -= 1.0;
+    }
+    return PI_OK;
+}
+
+/* The abiotic phase before the phytoplankton (time_step.jl:24-39). */
+int abiotic_update(orc_model* m, double dT) {
+    for (size_t sa = 0; sa < m->ab.size(); ++sa) {
+        Abiotic& a = m->ab[sa];
+        int st = particles_from_bcs(m, a, (int)sa, dT);
+        if (st) return st;
+        particle_advection(m, a, dT);
+        particle_diffusion(m, a, (int)sa, dT, PI_DRAW_ABIO_DIFFUSION);
+        find_inds(m, a);
+    }
+    return PI_OK;
+}
+
+/* Interaction, release and their diagnostics after the phytoplankton (time_step.jl:120-158). */
+int abiotic_exchange(orc_model* m, double dT) {
+    if (m->ab.empty()) return PI_OK;
+    for (const auto& pr : m->pal_intac) {
+        int st = particle_interaction(m, m->sp[pr.first], m->ab[pr.second], pr.first);
+        if (st) return st;
+    }
+    for (size_t q = 0; q < m->pal_release.size(); ++q) {
+        const auto& pr = m->pal_release[q];
+        int st = particle_release(m, m->sp[pr.first], m->ab[pr.second], (int)q, dT);
+        if (st) return st;
+    }
+    for (Species& S : m->sp) diags_proc(m, S, S.d_ptc, &S.ptc);
+    for (Abiotic& a : m->ab)
+        for (int64_t k = 0; k < m->C; ++k) a.d_num[cell_of(m, a, k)] += (double)(a.ac[k] && a.ac[k]);
+    return PI_OK;
+}
+
 }  // namespace
 
 /* ============================================================================================ */
@@ -1349,10 +1553,10 @@ int orc_create(const pi_grid* grid, const pi_bgc_params* bgc, const pi_quota_par
         S.p = species[s];
         for (dvec* v : { &S.x, &S.y, &S.z, &S.Sz, &S.Bm, &S.Cq, &S.Nq, &S.Pq, &S.Chl, &S.gen, &S.age,
                          &S.PS, &S.VDOC, &S.VNH4, &S.VNO3, &S.VPO4, &S.rChl, &S.resp, &S.BS, &S.exu,
-                         &S.graz, &S.mort, &S.dvid }) v->assign(C, 0.0);
+                         &S.graz, &S.mort, &S.dvid, &S.ptc }) v->assign(C, 0.0);
         S.xi.assign(C, 0); S.yi.assign(C, 0); S.zi.assign(C, 0); S.idx.assign(C, 0);
         S.ac.assign(C, 0);
-        for (dvec* v : { &S.d_num, &S.d_graz, &S.d_mort, &S.d_dvid }) v->assign(g.G, 0.0);
+        for (dvec* v : { &S.d_num, &S.d_graz, &S.d_mort, &S.d_dvid, &S.d_ptc }) v->assign(g.G, 0.0);
     }
     m->tr.assign(PI_NTRACERS, dvec(g.G, 0.0));
     m->Gcs.assign(PI_NTRACERS, dvec(g.G, 0.0));
@@ -1451,6 +1655,7 @@ int orc_set_individuals(orc_model* m, int32_t sp, const pi_individuals* in) {
     S.ac.assign(in->ac, in->ac + C);
     cp(S.graz, in->graz); cp(S.mort, in->mort); cp(S.dvid, in->dvid);
     if (S.carbon) { if (in->Bd) cp(S.Bd, in->Bd); else S.Bd.assign(C, 0.0); }
+    if (in->ptc) cp(S.ptc, in->ptc); else S.ptc.assign(C, 0.0);
     return PI_OK;
 }
 
@@ -1470,6 +1675,78 @@ int orc_get_individuals(orc_model* m, int32_t sp, pi_individuals* out) {
         cp(out->PRO, S.PRO); cp(out->DNA, S.DNA); cp(out->RNA, S.RNA);
         cp(out->CH, S.CH); cp(out->NST, S.NST); cp(out->PST, S.PST);
     }
+    cp(out->ptc, S.ptc);
+    return PI_OK;
+}
+
+/* abiotic_setup / Palat / max_candidates of PlanktonModel (models.jl:99-146) */
+int orc_set_abiotics(orc_model* m, int32_t nsa, const pi_abiotic_params* params, int32_t n_intac, const int32_t* intac,
+                     int32_t n_release, const int32_t* release, int32_t max_candidates, const double* max_ptc) {
+    if (!m || nsa < 1 || !params || max_candidates < 1 || !max_ptc || n_intac < 0 || n_release < 0 ||
+        (n_intac && !intac) || (n_release && !release) || !m->ab.empty()) return PI_ERR_ARG;
+    for (int32_t q = 0; q < n_intac + n_release; ++q) {
+        const int32_t* pr = q < n_intac ? intac + 2 * q : release + 2 * (q - n_intac);
+        if (pr[0] < 0 || pr[0] >= m->nsp || pr[1] < 0 || pr[1] >= nsa) return PI_ERR_ARG;
+    }
+    const size_t C = (size_t)m->C;
+    m->ab.resize((size_t)nsa);
+    for (int32_t a = 0; a < nsa; ++a) {
+        Abiotic& A = m->ab[a];
+        A.p = params[a];
+        for (dvec* v : { &A.x, &A.y, &A.z }) v->assign(C, 0.0);
+        A.xi.assign(C, 0); A.yi.assign(C, 0); A.zi.assign(C, 0);
+        A.ac.assign(C, 0);
+        A.d_num.assign(m->g.G, 0.0);
+    }
+    for (int32_t q = 0; q < n_intac; ++q) m->pal_intac.emplace_back(intac[2 * q], intac[2 * q + 1]);
+    for (int32_t q = 0; q < n_release; ++q) m->pal_release.emplace_back(release[2 * q], release[2 * q + 1]);
+    m->maxc = max_candidates;
+    m->max_ptc.assign(max_ptc, max_ptc + m->nsp);
+    m->intac.assign((size_t)max_candidates * C, 0);
+    return PI_OK;
+}
+
+int orc_set_abiotic_particles(orc_model* m, int32_t sa, const pi_abiotic_particles* in) {
+    if (!m || sa < 0 || sa >= (int32_t)m->ab.size() || !in || !in->x || !in->y || !in->z || !in->ac) return PI_ERR_ARG;
+    Abiotic& A = m->ab[sa];
+    const size_t C = (size_t)m->C;
+    A.x.assign(in->x, in->x + C); A.y.assign(in->y, in->y + C); A.z.assign(in->z, in->z + C);
+    A.ac.assign(in->ac, in->ac + C);
+    for (auto pr : { std::make_pair(&A.xi, in->xi), std::make_pair(&A.yi, in->yi), std::make_pair(&A.zi, in->zi) }) {
+        if (pr.second) pr.first->assign(pr.second, pr.second + C);
+        else pr.first->assign(C, 0);
+    }
+    return PI_OK;
+}
+
+int orc_get_abiotic_particles(orc_model* m, int32_t sa, pi_abiotic_particles* out) {
+    if (!m || sa < 0 || sa >= (int32_t)m->ab.size() || !out) return PI_ERR_ARG;
+    const Abiotic& A = m->ab[sa];
+    auto cp = [&](double* d, const dvec& s) { if (d) std::copy(s.begin(), s.end(), d); };
+    auto ci = [&](int64_t* d, const std::vector<int64_t>& s) { if (d) std::copy(s.begin(), s.end(), d); };
+    cp(out->x, A.x); cp(out->y, A.y); cp(out->z, A.z);
+    ci(out->xi, A.xi); ci(out->yi, A.yi); ci(out->zi, A.zi);
+    if (out->ac) std::copy(A.ac.begin(), A.ac.end(), out->ac);
+    return PI_OK;
+}
+
+int orc_count_abiotic(orc_model* m, int32_t sa, int64_t* n) {
+    if (!m || sa < 0 || sa >= (int32_t)m->ab.size() || !n) return PI_ERR_ARG;
+    int64_t c = 0;
+    for (uint8_t a : m->ab[sa].ac) c += a;
+    *n = c;
+    return PI_OK;
+}
+
+int orc_set_abiotic_bc(orc_model* m, int32_t sa, int32_t face, int32_t kind, const double* values, int64_t nt) {
+    if (!m || sa < 0 || sa >= (int32_t)m->ab.size() || face < 0 || face > 5 || kind < 0 || kind > 3) return PI_ERR_ARG;
+    const Grid& g = m->g;
+    FluxBC& b = m->ab[sa].bc[face];
+    b.kind = kind; b.nt = nt; b.v.clear();
+    size_t n1 = face <= PI_EAST ? g.Ny : g.Nx, n2 = face <= PI_NORTH ? g.Nz : g.Ny;
+    size_t n = kind == PI_BC_CONST ? 1 : kind == PI_BC_ARRAY2D ? n1 * n2 : kind == PI_BC_ARRAY3D ? n1 * n2 * (size_t)nt : 0;
+    if (n && !values) return PI_ERR_ARG;
+    if (n) b.v.assign(values, values + n);
     return PI_OK;
 }
 
@@ -1559,7 +1836,7 @@ int orc_set_flux_bc(orc_model* m, int32_t tracer, int32_t face, int32_t kind, co
     return PI_OK;
 }
 
-/* TimeStep!, Model/time_step.jl:12-180 (QuotaMode, no abiotic particles) */
+/* TimeStep!, Model/time_step.jl:12-180 */
 int orc_time_step(orc_model* m, double dT) {
     if (!m) return PI_ERR_ARG;
     const Grid& g = m->g;
@@ -1574,6 +1851,7 @@ int orc_time_step(orc_model* m, double dT) {
     for (int n = 0; n < PI_NTRACERS; ++n) zero(m->plk[n]);                        /* :21-22 */
     zero(m->Chl);
     bool ok = true;
+    if (int st = abiotic_update(m, dT)) return st;                                 /* :24-39 */
     if (m->bgc.shared_graz == 1.0) {
         zero(m->pop);
         for (int s = 0; s < m->nsp; ++s) {
@@ -1604,6 +1882,7 @@ int orc_time_step(orc_model* m, double dT) {
         }
     }
     if (!ok) return PI_ERR_CAPACITY;
+    if (int st = abiotic_exchange(m, dT)) return st;                               /* :120-158 */
     tracer_update(m, dT);
     for (size_t q = 0; q < g.G; ++q) m->d_PAR[q] += m->par[q];                  /* :167 */
     for (int n = 0; n < PI_NTRACERS; ++n)                                          /* :168-172 */
@@ -1652,11 +1931,15 @@ int orc_get_diag(orc_model* m, int32_t kind, int32_t sp, double* out) {
         if (sp < 0 || sp >= m->nsp || !(m->proc_mask & (1u << (kind - PI_DIAG_PROC)))) return PI_ERR_ARG;
         if ((size_t)(kind - PI_DIAG_PROC) >= m->sp[sp].d_proc.size()) return PI_ERR_ARG;
         f = &m->sp[sp].d_proc[kind - PI_DIAG_PROC];
+    } else if (kind == PI_DIAG_ABIO_NUM) {
+        if (sp < 0 || sp >= (int32_t)m->ab.size()) return PI_ERR_ARG;
+        f = &m->ab[sp].d_num;
     } else {
         if (sp < 0 || sp >= m->nsp) return PI_ERR_ARG;
         Species& S = m->sp[sp];
         f = kind == PI_DIAG_NUM ? &S.d_num : kind == PI_DIAG_GRAZ ? &S.d_graz
-          : kind == PI_DIAG_MORT ? &S.d_mort : kind == PI_DIAG_DVID ? &S.d_dvid : nullptr;
+          : kind == PI_DIAG_MORT ? &S.d_mort : kind == PI_DIAG_DVID ? &S.d_dvid
+          : kind == PI_DIAG_PTC ? &S.d_ptc : nullptr;
     }
     if (!f) return PI_ERR_ARG;
     std::copy(f->begin(), f->end(), out);

@@ -15,9 +15,11 @@ from ._native import CapacityError, PIError
 from .architectures import CPU, GPU, CarbonMode, IronEnergyMode, MacroMolecularMode, QuotaMode
 from .grids import (Ax, Ay, Az, Bounded, LatLonGrid, LoadLatLonGrid, Periodic, RectilinearGrid, interior,
                     volume, ΔxC, ΔxF, ΔyC, ΔyF, ΔzC, ΔzF)
-from .model import PlanktonDiagnostics, PlanktonModel, TimeStep_b, phyto_setup
-from .parameters import (bgc_params_default, default_PARF, default_temperature, default_tracer_init,
-                         phyt_params_default, update_bgc_params, update_phyt_params)
+from .model import (Palat, PlanktonDiagnostics, PlanktonModel, TimeStep_b, abiotic_setup, phyto_setup,
+                    set_bc_b, set_bc_particle_b)
+from .parameters import (abiotic_params_default, bgc_params_default, default_PARF, default_temperature,
+                         default_tracer_init, phyt_params_default, update_abiotic_params, update_bgc_params,
+                         update_phyt_params)
 from .simulation import PlanktonSimulation, synchronize, update_b
 from .output import PlanktonOutputWriter, write_output_b
 from .batch import BatchMember, Member, PlanktonBatch
@@ -29,4 +31,6 @@ __all__ = ["RectilinearGrid", "LatLonGrid", "LoadLatLonGrid", "Periodic", "Bound
            "bgc_params_default", "phyt_params_default", "update_bgc_params", "update_phyt_params",
            "default_PARF", "default_temperature", "default_tracer_init", "interior", "units",
            "CapacityError", "PIError", "ΔxC", "ΔyC", "ΔzC", "ΔxF", "ΔyF", "ΔzF", "Ax", "Ay", "Az",
-           "volume", "PlanktonBatch", "Member", "BatchMember", "PlanktonOutputWriter", "write_output_b"]
+           "volume", "PlanktonBatch", "Member", "BatchMember", "PlanktonOutputWriter", "write_output_b",
+           "abiotic_setup", "Palat", "abiotic_params_default", "update_abiotic_params", "set_bc_b",
+           "set_bc_particle_b"]

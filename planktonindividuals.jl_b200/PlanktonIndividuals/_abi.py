@@ -14,7 +14,10 @@ NTRACERS = len(tracer_names)
 FACES = {"west": 0, "east": 1, "south": 2, "north": 3, "bottom": 4, "top": 5}
 PI_BC_NONE, PI_BC_CONST, PI_BC_ARRAY2D, PI_BC_ARRAY3D = 0, 1, 2, 3
 PI_DIAG_PAR, PI_DIAG_NUM, PI_DIAG_GRAZ, PI_DIAG_MORT, PI_DIAG_DVID = 0, 1, 2, 3, 4
+PI_DIAG_PTC, PI_DIAG_ABIO_NUM = 5, 6
 PI_DIAG_TRACER, PI_DIAG_PROC = 16, 32
+# draw purposes of include/pi_numerics.h
+PI_DRAW_DIFFUSION, PI_DRAW_DECISION, PI_DRAW_ABIO_DIFFUSION, PI_DRAW_ABIO_BC, PI_DRAW_RELEASE = 0, 1, 2, 3, 4
 # QuotaMode processes of diags_spcs! (src/Diagnostics/diagnostics_kernels.jl:22-23), in PI_PROC_* order
 PROC_NAMES = ("PS", "BS", "VDOC", "VNH4", "VNO3", "VPO4", "resp", "exu", "Bm", "Cq", "Nq", "Pq", "Chl")
 
@@ -126,7 +129,20 @@ class pi_individuals(ct.Structure):
                 ("ac", _u8p),
                 ("graz", _dp), ("mort", _dp), ("dvid", _dp),
                 ("Bd", _dp),
-                ("PRO", _dp), ("DNA", _dp), ("RNA", _dp), ("CH", _dp), ("NST", _dp), ("PST", _dp)]
+                ("PRO", _dp), ("DNA", _dp), ("RNA", _dp), ("CH", _dp), ("NST", _dp), ("PST", _dp),
+                ("ptc", _dp)]
+
+
+# construct_abiotic_particle's param_names (src/Individuals/Abiotic/particle_generation.jl:7)
+ABIOTIC_FIELDS = ("Nsuper", "Rd", "release_P", "sz_min", "Ktr")
+
+
+class pi_abiotic_params(ct.Structure):
+    _fields_ = [(k, ct.c_double) for k in ABIOTIC_FIELDS]
+
+
+class pi_abiotic_particles(ct.Structure):
+    _fields_ = [("x", _dp), ("y", _dp), ("z", _dp), ("xi", _i64p), ("yi", _i64p), ("zi", _i64p), ("ac", _u8p)]
 
 
 class pi_member(ct.Structure):
@@ -161,6 +177,12 @@ def declare(lib, prefix):
         "create_macro": (ct.c_int32, [ct.POINTER(pi_grid), ct.POINTER(pi_bgc_params),
                                       ct.POINTER(pi_macro_params), ct.c_int32, ct.c_int64]),
         "last_error": (ct.c_int32, [P, ct.c_char_p, ct.c_size_t]),
+        "set_abiotics": (ct.c_int32, [P, ct.c_int32, ct.POINTER(pi_abiotic_params), ct.c_int32,
+                                      ct.POINTER(ct.c_int32), ct.c_int32, ct.POINTER(ct.c_int32), ct.c_int32, _dp]),
+        "set_abiotic_particles": (ct.c_int32, [P, ct.c_int32, ct.POINTER(pi_abiotic_particles)]),
+        "get_abiotic_particles": (ct.c_int32, [P, ct.c_int32, ct.POINTER(pi_abiotic_particles)]),
+        "count_abiotic": (ct.c_int32, [P, ct.c_int32, _i64p]),
+        "set_abiotic_bc": (ct.c_int32, [P, ct.c_int32, ct.c_int32, ct.c_int32, _dp, ct.c_int64]),
     }
     for name, (res, args) in protos.items():
         fn = getattr(lib, prefix + name, None)

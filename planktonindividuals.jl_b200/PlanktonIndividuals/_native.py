@@ -91,6 +91,8 @@ class CModel:
         self.lib = _abi.declare(lib, prefix)
         self.prefix = prefix
         self.mode = mode
+        self.precision = _abi.PI_FP64 if precision is None else int(precision)
+        self.nsa = 0
         self.grid = grid
         self.nsp = int(nsp)
         self.capacity = int(capacity)
@@ -168,6 +170,12 @@ class CModel:
         ac = np.ascontiguousarray(data["ac"], dtype=np.uint8)
         keep["ac"] = ac
         st.ac = ac.ctypes.data_as(ct.POINTER(ct.c_uint8))
+        if data.get("ptc") is not None:           # abiotic particles held; zeros when absent
+            a = np.ascontiguousarray(data["ptc"], dtype=np.float64)
+            if a.shape != (C,):
+                raise ValueError(f"individual attribute ptc must have length {C}")
+            keep["ptc"] = a
+            st.ptc = _dptr(a)
         self._check(self._fn("set_individuals")(self.h, int(sp), ct.byref(st)), "set_individuals")
 
     def get_individuals(self, sp):
@@ -177,6 +185,8 @@ class CModel:
             names = tuple(k for k in IND_DOUBLE if k not in ("Sz", "Bm", "Cq", "Nq", "Pq")) + _abi.MACRO_POOLS
         else:
             names = tuple(k for k in IND_DOUBLE if not (carbon and k in ("Cq", "Nq", "Pq"))) + (("Bd",) if carbon else ())
+        if self.precision == _abi.PI_FP64:
+            names = names + ("ptc",)
         out = {k: np.empty(C, dtype=np.float64) for k in names}
         out.update({k: np.empty(C, dtype=np.int64) for k in IND_INT})
         out["ac"] = np.empty(C, dtype=np.uint8)
@@ -276,6 +286,77 @@ class CModel:
         out = np.empty(self.G, dtype=np.float64)
         self._check(self._fn("get_diag")(self.h, int(kind), int(sp), _dptr(out)), "get_diag")
         return out.reshape(self.gshape, order="F")
+
+    # ---- abiotic particles (src/Individuals/Abiotic/) --------------------------------------------
+    def set_abiotics(self, params, nsa, intac=(), release=(), max_candidates=25, max_ptc=None):
+        """abiotic_setup(params, N, Nsa, Palat(intac, release)) and max_candidates of PlanktonModel:
+        params maps each of ABIOTIC_FIELDS to nsa values; intac and release are (phytoplankton
+        species, abiotic species) 0-based pairs; max_ptc holds each phytoplankton species'
+        max_ptc (NaN where the mode has none, the default)."""
+        ps = (_abi.pi_abiotic_params * nsa)()
+        for a in range(nsa):
+            for k in _abi.ABIOTIC_FIELDS:
+                setattr(ps[a], k, float(np.asarray(params[k], dtype=np.float64).ravel()[a]))
+        def pairs(lst):
+            arr = (ct.c_int32 * max(1, 2 * len(lst)))()
+            for q, (p, a) in enumerate(lst):
+                arr[2 * q], arr[2 * q + 1] = int(p), int(a)
+            return arr
+        mp = np.full(self.nsp, np.nan) if max_ptc is None else np.asarray(max_ptc, dtype=np.float64)
+        mp = np.ascontiguousarray(mp)
+        self._keep.append(mp)
+        self._check(self._fn("set_abiotics")(self.h, int(nsa), ps, len(intac), pairs(intac), len(release),
+                                             pairs(release), int(max_candidates), _dptr(mp)), "set_abiotics")
+        self.nsa = nsa
+
+    def set_abiotic_particles(self, sa, data):
+        C = self.capacity
+        st = _abi.pi_abiotic_particles()
+        keep = []
+        for k in ("x", "y", "z"):
+            a = np.ascontiguousarray(data[k], dtype=np.float64)
+            if a.shape != (C,):
+                raise ValueError(f"abiotic attribute {k} must have length {C}")
+            keep.append(a)
+            setattr(st, k, _dptr(a))
+        for k in IND_INT:
+            if data.get(k) is not None:
+                a = np.ascontiguousarray(data[k], dtype=np.int64)
+                keep.append(a)
+                setattr(st, k, a.ctypes.data_as(ct.POINTER(ct.c_int64)))
+        ac = np.ascontiguousarray(data["ac"], dtype=np.uint8)
+        keep.append(ac)
+        st.ac = ac.ctypes.data_as(ct.POINTER(ct.c_uint8))
+        self._check(self._fn("set_abiotic_particles")(self.h, int(sa), ct.byref(st)), "set_abiotic_particles")
+
+    def get_abiotic_particles(self, sa):
+        C = self.capacity
+        out = {k: np.empty(C, dtype=np.float64) for k in ("x", "y", "z")}
+        out.update({k: np.empty(C, dtype=np.int64) for k in IND_INT})
+        out["ac"] = np.empty(C, dtype=np.uint8)
+        st = _abi.pi_abiotic_particles()
+        for k in ("x", "y", "z"):
+            setattr(st, k, _dptr(out[k]))
+        for k in IND_INT:
+            setattr(st, k, out[k].ctypes.data_as(ct.POINTER(ct.c_int64)))
+        st.ac = out["ac"].ctypes.data_as(ct.POINTER(ct.c_uint8))
+        self._check(self._fn("get_abiotic_particles")(self.h, int(sa), ct.byref(st)), "get_abiotic_particles")
+        out["ac"] = out["ac"].astype(bool)
+        return out
+
+    def count_abiotic(self, sa):
+        n = ct.c_int64()
+        self._check(self._fn("count_abiotic")(self.h, int(sa), ct.byref(n)), "count_abiotic")
+        return n.value
+
+    def set_abiotic_bc(self, sa, face, kind, values=None, nt=0):
+        if values is None:
+            p = ct.POINTER(ct.c_double)()
+        else:
+            values = np.asfortranarray(np.atleast_1d(np.asarray(values, dtype=np.float64)))
+            self._keep.append(values)
+            p = _dptr(values.ravel(order="F"))
+        self._check(self._fn("set_abiotic_bc")(self.h, int(sa), int(face), int(kind), p, int(nt)), "set_abiotic_bc")
 
     def set_state(self, individuals, tracers):
         """Upload a full initial state: individuals = list (per species) of attribute dicts,

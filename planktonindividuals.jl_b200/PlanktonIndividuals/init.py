@@ -128,6 +128,21 @@ def mask_individuals(d, grid, N):
     d["ac"][:N] = lm & ac
 
 
+def initialize_abiotic_particle(grid, N, C, rng):
+    """initialize_abiotic_particle! (src/Individuals/Abiotic/particle_generation.jl:24-35): N active
+    particles at uniform positions in the domain, masked by land; cell indices zero as constructed."""
+    if N > C:
+        raise ValueError("PlanktonModel: number of abiotic particles exceeds max_individuals")
+    ac = np.zeros(C, dtype=bool)
+    ac[:N] = True
+    x, y, z = rng.random(C), rng.random(C), rng.random(C)
+    d = {"x": (x * grid.Nx) * ac, "y": (y * grid.Ny) * ac, "z": (z * grid.Nz) * ac, "ac": ac}
+    for k in ("xi", "yi", "zi"):
+        d[k] = np.zeros(C, dtype=np.int64)
+    mask_individuals(d, grid, N)
+    return d
+
+
 def generate_tracers(grid, source, rng):
     """generate_tracers for a NamedTuple-style source {initial_condition, rand_noise}: each tracer
     is its value times a draw from lower:1.0e-4:upper, masked by land, halos filled."""

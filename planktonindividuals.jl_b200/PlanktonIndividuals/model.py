@@ -6,9 +6,10 @@ from . import _abi, _lib
 from ._abi import NTRACERS, PI_FP32, PI_FP64, tracer_names
 from ._native import CModel
 from .architectures import GPU, CarbonMode, MacroMolecularMode, QuotaMode
-from .init import generate_tracers, initialize_plankton, initialize_plankton_carbon, initialize_plankton_macro
-from .parameters import (bgc_params_default, default_tracer_init, phyt_params_default,
-                         update_bgc_params, update_phyt_params)
+from .init import (generate_tracers, initialize_abiotic_particle, initialize_plankton, initialize_plankton_carbon,
+                   initialize_plankton_macro)
+from .parameters import (abiotic_params_default, bgc_params_default, default_tracer_init, phyt_params_default,
+                         update_abiotic_params, update_bgc_params, update_phyt_params)
 
 
 class phyto_setup:
@@ -18,6 +19,26 @@ class phyto_setup:
         self.params = params
         self.N = list(N)
         self.Nsp = int(Nsp)
+
+
+class Palat:
+    """Palat(intac, release) (src/PlanktonIndividuals.jl:118-121): the (phytoplankton, abiotic)
+    species name pairs that interact (particle_interaction!) and release (particle_release!), e.g.
+    Palat([("sp1", "sa1")], [("sp1", "sa1")])."""
+
+    def __init__(self, intac=(), release=()):
+        self.intac = [tuple(p) for p in intac]
+        self.release = [tuple(p) for p in release]
+
+
+class abiotic_setup:
+    """abiotic_setup(params, N, Nsa, palat) (src/PlanktonIndividuals.jl:122-127)."""
+
+    def __init__(self, params=None, N=(2 ** 10,), Nsa=1, palat=None):
+        self.params = params
+        self.N = list(N)
+        self.Nsa = int(Nsa)
+        self.palat = palat if palat is not None else Palat()
 
 
 class _Attrs(dict):
@@ -35,11 +56,24 @@ class phytoplankton:
         return _Attrs(self._model._native.get_individuals(self._s))
 
 
+class abiotic_particle:
+    """abiotic_particle{data, p, bc} of one abiotic species (src/PlanktonIndividuals.jl:100-105);
+    `data` (x, y, z, xi, yi, zi, ac) is downloaded from the device on access."""
+
+    def __init__(self, model, a, p):
+        self._model, self._a, self.p = model, a, p
+
+    @property
+    def data(self):
+        return _Attrs(self._model._native.get_abiotic_particles(self._a))
+
+
 class individuals:
-    def __init__(self, model, params, nsp):
+    def __init__(self, model, params, nsp, abiotic_params=None, nsa=0):
         self.phytos = _Attrs({f"sp{s + 1}": phytoplankton(model, s, _Attrs(
             {k: (v[s] if hasattr(v, "__len__") else v) for k, v in params.items()})) for s in range(nsp)})
-        self.abiotics = _Attrs()
+        self.abiotics = _Attrs({f"sa{a + 1}": abiotic_particle(model, a, _Attrs(
+            {k: v[a] for k, v in abiotic_params.items()})) for a in range(nsa)})
 
 
 class _Field:
@@ -70,8 +104,6 @@ class PlanktonModel:
         macro = isinstance(mode, MacroMolecularMode)
         if mode is not None and not carbon and not macro and not isinstance(mode, QuotaMode) and mode is not QuotaMode:
             raise NotImplementedError(f"{mode}: QuotaMode(), CarbonMode() and MacroMolecularMode() are implemented")
-        if abiotic is not None:
-            raise NotImplementedError("abiotic particles are not implemented")
         FT = np.dtype(FT).type
         if FT not in (np.float32, np.float64):
             raise ValueError("FT must be Float32 or Float64")
@@ -81,6 +113,22 @@ class PlanktonModel:
             raise NotImplementedError("MacroMolecularMode() is built in the FP64 form: use FT = Float64")
         if getattr(grid, "is_latlon", False) and FT is not np.float64:
             raise NotImplementedError("LatLonGrid is built in the FP64 form: use FT = Float64")
+        if abiotic is not None:                                  # models.jl:99-117
+            if not isinstance(abiotic, abiotic_setup):
+                raise ValueError("PlanktonModel:`abiotic` must be either Nothing or `abiotic_setup`!")
+            if FT is not np.float64:
+                raise NotImplementedError("abiotic particles are built in the FP64 form: use FT = Float64")
+            if max(abiotic.N) > max_individuals:
+                raise ValueError("maximum(abiotic.N) ≤ max_individuals")
+            if len(abiotic.N) != abiotic.Nsa:
+                raise ValueError(f"PlanktonModel: `abiotic`: The length of `N` must be {abiotic.Nsa}, the same as "
+                                 f"`Nsa`, each species has its own initial condition")
+            if abiotic.params is None:
+                abiotic.params = update_abiotic_params(abiotic_params_default(abiotic.Nsa), FT, N=abiotic.Nsa)
+            elif isinstance(abiotic.params, dict):
+                abiotic.params = update_abiotic_params(abiotic.params, FT, N=abiotic.Nsa)
+            else:
+                raise ValueError("Abiotic parameters must be either Nothing or Dict!")
         self.FT = FT
         self.arch = GPU()
         self.mode = mode if (carbon or macro) else QuotaMode()
@@ -111,7 +159,20 @@ class PlanktonModel:
             raise ValueError("PlanktonModel:`phyto` must be either Nothing or `phyto_setup`!")
         self.bgc_params = bgc_final
         self.phyto = phyto
+        self.abiotic = abiotic
         nsp = phyto.Nsp
+        pal_intac, pal_release = [], []
+        if abiotic is not None:                                  # models.jl:121-143
+            sps = [f"sp{s + 1}" for s in range(nsp)]
+            sas = [f"sa{a + 1}" for a in range(abiotic.Nsa)]
+            for lst, out in ((abiotic.palat.intac, pal_intac), (abiotic.palat.release, pal_release)):
+                for pr in lst:
+                    sp, sa = (str(q).lstrip(":") for q in pr)
+                    if sp not in sps:
+                        raise ValueError(f"Abiotic: {sp} is not generated")
+                    if sa not in sas:
+                        raise ValueError(f"Abiotic: {sa} is not generated")
+                    out.append((sps.index(sp), sas.index(sa)))
         self.max_individuals = int(max_individuals)
         lib = _lib.load()
         precision = PI_FP64 if FT is np.float64 else PI_FP32
@@ -125,9 +186,21 @@ class PlanktonModel:
         else:
             inds, trs = initial_state
         self._native.set_state(inds, trs)
+        nsa = 0
+        if abiotic is not None:
+            nsa = abiotic.Nsa
+            # max_ptc exists only where the mode's parameters define it (IronEnergyMode); NaN
+            # otherwise, where a merge raises as the reference's field access does
+            mp = phyto.params.get("max_ptc")
+            max_ptc = [float(mp[s]) for s in range(nsp)] if mp is not None else [float("nan")] * nsp
+            self._native.set_abiotics(abiotic.params, nsa, pal_intac, pal_release, max_candidates, max_ptc)
+            if initial_state is None:
+                for a in range(nsa):
+                    self._native.set_abiotic_particles(a, initialize_abiotic_particle(grid, abiotic.N[a],
+                                                                                      max_individuals, rng))
         if t:
             self._native.set_time(0, float(t))
-        self.individuals = individuals(self, phyto.params, nsp)
+        self.individuals = individuals(self, phyto.params, nsp, abiotic.params if abiotic else None, nsa)
         self.tracers = _Attrs({name: _Field(self, n) for n, name in enumerate(tracer_names)})
 
     @property
@@ -141,6 +214,10 @@ class PlanktonModel:
     def count_active(self):
         """calc_active_individuals (models.jl:157-164)."""
         return [self._native.count_active(s) for s in range(self.phyto.Nsp)]
+
+    def count_abiotic(self):
+        """calc_active_individuals of the abiotic species (models.jl:170-176)."""
+        return [self._native.count_abiotic(a) for a in range(self._native.nsa)]
 
     def set_velocity(self, u, v, w):
         self._native.set_velocity(u, v, w)
@@ -210,8 +287,10 @@ class PlanktonDiagnostics:
             def __getattr__(self, k):
                 kinds = {"num": _abi.PI_DIAG_NUM, "graz": _abi.PI_DIAG_GRAZ,
                          "mort": _abi.PI_DIAG_MORT, "dvid": _abi.PI_DIAG_DVID}
-                if k == "ptc":
-                    return np.zeros(G, order="F")
+                if k == "ptc":                   # time_step.jl:140-149: kept only with abiotic particles
+                    if not nat.nsa:
+                        return np.zeros(G, order="F")
+                    return nat.get_diag(_abi.PI_DIAG_PTC, self.s)
                 if k in kinds:
                     return nat.get_diag(kinds[k], self.s)
                 if k in procs:
@@ -239,12 +318,62 @@ class PlanktonDiagnostics:
 
         self.tracer = _Tr()
         self.phytos = _Attrs({f"sp{s + 1}": _Sp(s) for s in range(model.phyto.Nsp)})
-        self.abiotics = _Attrs()
+        anames = tuple(abiotic_particle)
+
+        class _Sa:
+            def __init__(self, a):
+                self.a = a
+
+            def keys(self):
+                return anames
+
+            def __getattr__(self, k):
+                if k == "num":
+                    return nat.get_diag(_abi.PI_DIAG_ABIO_NUM, self.a)
+                raise AttributeError(k)
+
+            def __getitem__(self, k):
+                return getattr(self, k)
+
+        self.abiotics = _Attrs({f"sa{a + 1}": _Sa(a) for a in range(nat.nsa)})
 
     def reset(self):
         r = self._model._native.lib.pi_reset_diags(self._model._native.h)
         if r:
             raise RuntimeError("pi_reset_diags failed")
+
+
+def _bc_kind(model, pos, bc_value):
+    if pos not in _abi.FACES:
+        raise ValueError(f"pos must be one of {tuple(_abi.FACES)}")
+    if np.ndim(bc_value) == 0:
+        return _abi.FACES[pos], _abi.PI_BC_CONST, [float(bc_value)], 0
+    a = np.asfortranarray(np.asarray(bc_value, dtype=np.float64))
+    if a.ndim == 2:
+        return _abi.FACES[pos], _abi.PI_BC_ARRAY2D, a, 0
+    if a.ndim == 3:
+        return _abi.FACES[pos], _abi.PI_BC_ARRAY3D, a, a.shape[2]
+    raise ValueError("bc_value must be a Number, a 2D or a 3D array")
+
+
+def set_bc_b(model, *, tracer, pos, bc_value):
+    """set_bc!(model; tracer, pos, bc_value) (src/Biogeochemistry/HaloRegions/boundary_conditions.jl:21-31):
+    a constant, a face array (n1, n2) or a time series (n1, n2, nt) indexed by model.iteration."""
+    tracer = str(tracer).lstrip(":")
+    if tracer not in tracer_names:
+        raise ValueError(f"{tracer} is not a tracer")
+    face, kind, v, nt = _bc_kind(model, str(pos).lstrip(":"), bc_value)
+    model._native.set_flux_bc(tracer_names.index(tracer), face, kind, v, nt)
+
+
+def set_bc_particle_b(model, *, sa, pos, bc_value):
+    """set_bc_particle!(model; sa, pos, bc_value) (boundary_conditions.jl:33-41): the particle flux
+    of abiotic species `sa` through a face, turned into particles by particles_from_bcs!."""
+    sa = str(sa).lstrip(":")
+    if sa not in model.individuals.abiotics:
+        raise ValueError(f"Abiotic: {sa} is not generated")
+    face, kind, v, nt = _bc_kind(model, str(pos).lstrip(":"), bc_value)
+    model._native.set_abiotic_bc(int(sa[2:]) - 1, face, kind, v, nt)
 
 
 def TimeStep_b(model, ΔT, diags=None):

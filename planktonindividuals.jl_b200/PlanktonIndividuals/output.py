@@ -128,6 +128,10 @@ def write_diags(diags, path, t, it, ncounts, grid):
     for sp in diags.phytos.keys():
         for proc in diags.phytos[sp].keys():
             items.append((f"timeseries/phyto/{sp}/{proc}/{it}", _interior(diags.phytos[sp][proc], grid) / ncounts))
+    abiotics = getattr(diags, "abiotics", {})
+    for sa in abiotics.keys():
+        for proc in abiotics[sa].keys():
+            items.append((f"timeseries/abiotic/{sa}/{proc}/{it}", _interior(abiotics[sa][proc], grid) / ncounts))
     _append(path, items)
     diags.reset()
 

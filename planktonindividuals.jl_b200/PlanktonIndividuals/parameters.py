@@ -121,6 +121,23 @@ def update_phyt_params(tmp, FT=np.float32, *, N=1, mode=None):
     return parameters
 
 
+def abiotic_params_default(N=1):
+    """abiotic_params_default(N) (src/Parameters/param_default.jl:329-343)."""
+    params = {"Nsuper": [1.0], "Rd": [1.0e-4], "release_P": [1.0e-6], "sz_min": [1.0e-3], "Ktr": [0.0e-5]}
+    return {k: v * N for k, v in params.items()}
+
+
+def update_abiotic_params(tmp, FT=np.float32, *, N=1):
+    """update_abiotic_params (src/Parameters/param_update.jl:57-69)."""
+    FT = np.dtype(FT).type
+    parameters = abiotic_params_default(N)
+    for key in tmp:
+        if key not in parameters:
+            raise ValueError(f"PARAM: abiotic parameter not found {key}")
+        parameters[key] = [FT(v) for v in np.atleast_1d(tmp[key])]
+    return parameters
+
+
 def default_tracer_init():
     """default_tracer_init() (tracer_fields.jl:41-45)."""
     init = dict(DIC=20.0, NH4=0.5, NO3=0.8, PO4=0.10, DFe=1.0e-6, DOC=10.0, DON=0.1, DOP=0.05,

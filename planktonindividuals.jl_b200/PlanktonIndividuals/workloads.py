@@ -402,3 +402,60 @@ def config5(n_boxes=4096, steps=2880, dT=60.0, seed=5, n_max=None):
         wl.parf = diel_parf(1, 1, hours, peak=1000.0, phase=phase)
         out.append(wl)
     return out
+
+
+def abiotic(nx=16, nz=8, N_per_species=1500, nsp=2, N_abiotic=(2000, 1000), steps=20, dT=60.0, seed=17,
+            nmodes=16, capacity=None, Rd=(12.0, 20.0), release_P=(2.0e-3, 1.0e-3), max_ptc=(25.0, 2.0),
+            top_flux=2.0e-9, max_candidates=25, topology=None):
+    """QuotaMode with abiotic particles on a config-2-like 3D grid (nx×nx×nz, 50 m × 50 m × 2 m):
+    two abiotic species from initialize_abiotic_particle!, interaction pairs (sp1, sa1) and
+    (sp2, sa2), release pair (sp1, sa1), particle fluxes into sa2 through the top (constant), the
+    east face (a face array) and the south face (a time series). Interaction radii and release
+    probabilities are raised from the defaults (Rd = 1e-4 m) so that merges and releases happen
+    every step; max_ptc is given per phytoplankton species as IronEnergyMode's parameter would be.
+    The abiotic setup is in `wl.abiotic` (see configure_abiotics)."""
+    from .init import initialize_abiotic_particle
+    rng = np.random.default_rng(seed)
+    topology = topology or (Periodic, Periodic, Bounded)
+    grid = RectilinearGrid(size=(nx, nx, nz), x=(0.0, nx * 50.0), y=(0.0, nx * 50.0),
+                           z=(0.0, -2.0 * nz), FT=np.float64, topology=topology)
+    vel = FourierVelocity(grid, nmodes=nmodes, rms=0.05, seed=seed)
+    C = capacity or 2 * N_per_species
+    n_vel = int(np.ceil(steps / 60)) + 1
+    vel_fn = vel
+    if grid.topo[0] == Bounded.code or grid.topo[1] == Bounded.code:
+        def vel_fn(t, _v=vel, _bx=grid.topo[0] == Bounded.code, _by=grid.topo[1] == Bounded.code):
+            u, v, w = _v(t)                  # the periodic field, its first face repeated on Bounded axes
+            if _bx:
+                u = np.asfortranarray(np.concatenate([u, u[:1]], axis=0))
+            if _by:
+                v = np.asfortranarray(np.concatenate([v, v[:, :1]], axis=1))
+            return u, v, w
+    wl = _finish("abiotic", grid, nsp, [N_per_species] * nsp, C, None, None, dT, steps, rng, vel_fn, n_vel, 60 * dT,
+                 nz, [0.0] * nsp, 0.2, seed, no3_grad=2.0 * nz)
+    nsa = len(N_abiotic)
+    params = {"Nsuper": [1.0] * nsa, "Rd": list(Rd)[:nsa], "release_P": list(release_P)[:nsa],
+              "sz_min": [1.0e-3] * nsa, "Ktr": [0.0] * nsa}
+    from ._abi import FACES, PI_BC_ARRAY2D, PI_BC_ARRAY3D, PI_BC_CONST
+    sa_bc = min(1, nsa - 1)
+    bcs = [(sa_bc, FACES["top"], PI_BC_CONST, [top_flux], 0),
+           (sa_bc, FACES["east"], PI_BC_ARRAY2D, np.asfortranarray(rng.random((grid.Ny, grid.Nz)) * 5.0e-8), 0),
+           (sa_bc, FACES["south"], PI_BC_ARRAY3D, np.asfortranarray(rng.random((grid.Nx, grid.Nz, steps + 1)) * 5.0e-8),
+            steps + 1)]
+    wl.abiotic = dict(params=params, nsa=nsa,
+                      intac=[(s, min(s, nsa - 1)) for s in range(nsp)], release=[(0, 0)],
+                      max_candidates=max_candidates, max_ptc=list(max_ptc)[:nsp],
+                      particles=[initialize_abiotic_particle(grid, N_abiotic[a], C, rng) for a in range(nsa)],
+                      bcs=bcs)
+    return wl
+
+
+def configure_abiotics(model, wl):
+    """Applies `wl.abiotic` to a model handle (the oracle's or the library's)."""
+    a = wl.abiotic
+    model.set_abiotics(a["params"], a["nsa"], a["intac"], a["release"], a["max_candidates"], a["max_ptc"])
+    for s, d in enumerate(a["particles"]):
+        model.set_abiotic_particles(s, d)
+    for (sa, face, kind, values, nt) in a["bcs"]:
+        model.set_abiotic_bc(sa, face, kind, values, nt)
+    return model

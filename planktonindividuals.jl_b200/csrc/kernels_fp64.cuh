@@ -1,4 +1,5 @@
-// FP64 plain-form kernels of the model time step (QuotaMode, no abiotic particles).
+// FP64 plain-form kernels of the model time step (the abiotic particles' own kernels are in
+// kernels_abiotic.cuh).
 //
 // Every arithmetic expression below is written in the operation order of the reference Julia
 // code it cites, and the library is compiled with -fmad=false, so each result is the same IEEE
@@ -120,10 +121,12 @@ __global__ void k_velhalf(long long G, const double* __restrict__ u0, const doub
 
 struct VelPtrs { const double *u0, *v0, *w0, *uh, *vh, *wh, *u1, *v1, *w1; };
 
-// RK4 + diffusion + find_inds! of one active individual; writes its position, packed cell, binning
-// key and count.
-template <bool LL>
-__device__ __forceinline__ void particle_step(const DGrid& g, const SpcDev& P, int s, long long slot,
+// RK4 + diffusion + find_inds! of one active particle at `slot` of the columns x, y, z, cell of P
+// (a phytoplankton species, SpcDev, or an abiotic species, AbioDev, whose steps are the same
+// kernels, time_step.jl:29-38); the diffusion draw is keyed by (dsp, purpose). BIN: writes the
+// binning key and count of a phytoplankton individual.
+template <bool LL, bool BIN = true, class PV>
+__device__ __forceinline__ void particle_step(const DGrid& g, const PV& P, uint32_t dsp, uint32_t purpose, long long slot,
                                               long long gid, double dT, uint64_t seed, uint32_t iter,
                                               const VelPtrs& vel, double kappa_h, double kappa_v,
                                               uint32_t* __restrict__ cnt, uint32_t* __restrict__ key,
@@ -173,7 +176,7 @@ __device__ __forceinline__ void particle_step(const DGrid& g, const SpcDev& P, i
     x = jl_mulb(bc_pos(x, NX, g.tx), ac); y = jl_mulb(bc_pos(y, NY, g.ty), ac); z = jl_mulb(bc_pos(z, NZ, g.tz), ac);
     // diffusion: rnd ∈ [0,1) → (rnd - 0.5) * 2 → · √(κΔT) / Δ
     double r0, r1, r2;
-    pi_draw3(seed, iter, (uint32_t)s, PI_DRAW_DIFFUSION, (uint32_t)slot, &r0, &r1, &r2);
+    pi_draw3(seed, iter, dsp, purpose, (uint32_t)slot, &r0, &r1, &r2);
     r0 = (r0 - 0.5) * 2.0; r1 = (r1 - 0.5) * 2.0; r2 = (r2 - 0.5) * 2.0;
     // ΔxC/ΔyC at (xi+Hx, yi+Hy) of the stored indices (particle_diffusion.jl:4-5); the reference
     // reads past the metric array there when x = Nx exactly, which is held at the last column here
@@ -189,9 +192,11 @@ __device__ __forceinline__ void particle_step(const DGrid& g, const SpcDev& P, i
     int yi = clamp_idx(jl_trunc(jl_mulb(y + 1.0, ac)) + g.Hy, 1, g.Gy, err);
     int zi = clamp_idx(jl_trunc(jl_mulb(z + 1.0, ac)) + g.Hz, 1, g.Gz, err);
     P.cell[slot] = pack_cell(g, xi, yi, zi);
-    int c = gidx(g, xi, yi, zi);
-    key[gid] = (uint32_t)c;
-    atomicAdd(&cnt[c], 1u);
+    if (BIN) {
+        int c = gidx(g, xi, yi, zi);
+        key[gid] = (uint32_t)c;
+        atomicAdd(&cnt[c], 1u);
+    }
 }
 
 // Slot-order pass over every (species, slot): inactive slots (every stage multiplies by ac, so
@@ -221,7 +226,8 @@ __global__ void k_particles(DGrid g, const SpcDev* __restrict__ spc, int nsp, lo
         return;
     }
     if (P.stat[slot] & ST_AC0) return;                // moved by k_particles_sorted
-    particle_step<LL>(g, P, s, slot, gid, dT, seed, iter, vel, kappa_h, kappa_v, cnt, key, err);
+    particle_step<LL>(g, P, (uint32_t)s, PI_DRAW_DIFFUSION, slot, gid, dT, seed, iter, vel, kappa_h, kappa_v, cnt, key,
+                      err);
 }
 
 // Cell-order pass: the individuals binned in the previous step (prev_sorted[0 .. off[G]), which
@@ -241,7 +247,8 @@ __global__ void k_particles_sorted(DGrid g, const SpcDev* __restrict__ spc, long
     long long slot = gd - (long long)s * C;
     const SpcDev& P = spc[s];
     if (!(P.flags[slot] & FL_AC) || !(P.stat[slot] & ST_AC0)) return;
-    particle_step<LL>(g, P, s, slot, gd, dT, seed, iter, vel, kappa_h, kappa_v, cnt, key, err);
+    particle_step<LL>(g, P, (uint32_t)s, PI_DRAW_DIFFUSION, slot, gd, dT, seed, iter, vel, kappa_h, kappa_v, cnt, key,
+                      err);
 }
 
 // pos[gid] = position of gid in the cell-sorted entry list.
@@ -378,7 +385,8 @@ __global__ void k_decide(DGrid g, SpcDev P, pi_quota_params p, pi_macro_params m
 __global__ void k_lists(const unsigned long long* __restrict__ flag64,
                         const unsigned long long* __restrict__ rank64, long long C,
                         int32_t* __restrict__ divlist, int32_t* __restrict__ freelist,
-                        uint32_t* ndiv, uint32_t* err, int64_t* err_iter, int64_t iter) {
+                        uint32_t* ndiv, uint32_t* err, int64_t* err_iter, int64_t iter,
+                        uint32_t errbits = PI_DEVERR_CAPACITY) {
     long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= C) return;
     if (*err & PI_DEVERR_CAPACITY) return;
@@ -388,7 +396,7 @@ __global__ void k_lists(const unsigned long long* __restrict__ flag64,
         if (slot == 0) { *ndiv = 0; *err_iter = iter; }
         __threadfence();
         // every thread sees the same totals; one flag write is enough but all are harmless
-        if (slot == 0) set_err(err, PI_DEVERR_CAPACITY);
+        if (slot == 0) set_err(err, errbits);
         return;
     }
     if (slot == 0) *ndiv = (uint32_t)tdiv;

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "kernels_fp64.cuh"
+#include "kernels_abiotic.cuh"
 #include "host_common.h"
 
 using namespace pib;
@@ -105,6 +106,26 @@ struct pi_model {
     DevBC bcs[PI_NTRACERS][6];
     FluxBCDev* d_bcs = nullptr;
     int any_bc = 0;
+    // abiotic particles (pi_set_abiotics): species, their particle flux boundary conditions, the
+    // Palat pairs, the candidate rows intac (max_candidates per particle slot) and the scratch of
+    // the cell binning, boundary creation and free-slot lists
+    int nsa = 0;
+    std::vector<pi_abiotic_params> ap;
+    std::vector<AbioDev> h_ab;
+    std::vector<DevBC> abc;                 // nsa × 6
+    std::vector<std::pair<int, int>> pal_intac, pal_release;
+    int maxc = 25;
+    std::vector<double> max_ptc;
+    int32_t* intac = nullptr;
+    double* diag_ptc = nullptr;             // nsp × G
+    double* diag_abn = nullptr;             // nsa × G
+    uint32_t *akey = nullptr, *akey_s = nullptr, *aval = nullptr, *aval_s = nullptr;   // C each
+    uint32_t *pkey = nullptr, *pkey_s = nullptr, *pval = nullptr, *pval_s = nullptr;   // C each
+    uint32_t *cflag = nullptr, *crank = nullptr;                                        // G each
+    uint32_t *afl = nullptr, *afr = nullptr;                                            // C each
+    int32_t* afree = nullptr;                                                           // C
+    void* atmp = nullptr;
+    size_t abytes = 0;
     // optional per-kernel event timing
     int profiling = 0;
     struct Mark { const char* name; cudaEvent_t a, b; };
@@ -174,6 +195,8 @@ void free_all(pi_model* m) {
     for (int n = 0; n < PI_NTRACERS; ++n)
         for (int f = 0; f < 6; ++f)
             if (m->bcs[n][f].v) { cudaFree(m->bcs[n][f].v); m->bcs[n][f].v = nullptr; }
+    for (DevBC& b : m->abc)
+        if (b.v) { cudaFree(b.v); b.v = nullptr; }
 }
 
 inline unsigned nblk(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
@@ -227,12 +250,122 @@ pi_status check_device_errors(pi_model* m) {
     if (!err) return PI_OK;
     CK(cudaMemsetAsync(m->sb.err, 0, sizeof(uint32_t), m->stream), "clear error word");
     CK(cudaStreamSynchronize(m->stream), "synchronize");
+    if (err & PI_DEVERR_MAXPTC)     // merge_particle_kernel! reads plank_p.max_ptc (particle_interaction.jl:58)
+        return fail(m, PI_ERR_PARAM, "type NamedTuple has no field max_ptc");
     if (err & PI_DEVERR_CAPACITY) {
         double tf = (double)it * m->last_dT;    // model.t of the failing step
-        return fail(m, PI_ERR_CAPACITY, "number of individual exceeds the capacity at timestep " +
-                                            julia_float(tf / 86400.0) + " days");
+        return fail(m, PI_ERR_CAPACITY, std::string(err & PI_DEVERR_ABIO ? "number of abiotic particles" : "number of individual") +
+                                            " exceeds the capacity at timestep " + julia_float(tf / 86400.0) + " days");
     }
     return fail(m, PI_ERR_DOMAIN, "an individual left the halo-padded grid (cell index out of range)");
+}
+
+// The abiotic phase before the phytoplankton (time_step.jl:24-39): for each abiotic species,
+// particles_from_bcs! (particle_interaction.jl:252-271), then the particle step.
+pi_status enqueue_abiotic_update(pi_model* m, double dT, const VelPtrs& vp) {
+    const DGrid& g = m->dg;
+    const long long G = g.G, C = m->C;
+    const uint32_t iter = (uint32_t)m->iteration;
+    cudaStream_t st = m->stream;
+    StepBufs& sb = m->sb;
+    const bool ll = m->met != nullptr;
+    const int BS = 256;
+    for (int sa = 0; sa < m->nsa; ++sa) {
+        const AbioDev& A = m->h_ab[sa];
+        const DevBC* B = &m->abc[(size_t)sa * 6];
+        bool any = false;
+        for (int f = 0; f < 6; ++f) any = any || B[f].kind != PI_BC_NONE;
+        if (any) {
+            ProfScope ps_(m, "k_abio_bcs");
+            CK(cudaMemsetAsync(m->cflag, 0, G * sizeof(uint32_t), st), "zero tr_temp");
+            const HostGrid& hg = m->hg;
+            const pi_abiotic_params& p = m->ap[sa];
+            auto face = [&](int f) -> FluxBCDev {
+                FluxBCDev d;
+                d.kind = B[f].kind; d.nt = B[f].nt; d.v = B[f].v;
+                d.n1 = f <= PI_EAST ? hg.Ny : hg.Nx;
+                d.n2 = f <= PI_NORTH ? hg.Nz : hg.Ny;
+                return d;
+            };
+            const long long nxy = (long long)hg.Nx * hg.Ny, nyz = (long long)hg.Ny * hg.Nz, nxz = (long long)hg.Nx * hg.Nz;
+#define ABIO_FACE(F, N) if (B[F].kind) (ll ? k_abio_bc_face<true, F> : k_abio_bc_face<false, F>)<<<nblk(N, BS), BS, 0, st>>>( \
+                g, face(F), p.sz_min, p.Nsuper, dT, m->seed, m->iteration, sa, m->cflag, sb.err)
+            ABIO_FACE(PI_TOP, nxy); ABIO_FACE(PI_BOTTOM, nxy); ABIO_FACE(PI_EAST, nyz);
+            ABIO_FACE(PI_WEST, nyz); ABIO_FACE(PI_NORTH, nxz); ABIO_FACE(PI_SOUTH, nxz);
+#undef ABIO_FACE
+            CK(cudaGetLastError(), "k_abio_bc_face");
+            size_t tb = m->abytes;
+            CK(cub::DeviceScan::ExclusiveSum(m->atmp, tb, m->cflag, m->crank, (int)G, st), "scan boundary cells");
+            k_abio_free_flags<<<nblk(C, BS), BS, 0, st>>>(A, C, m->afl);
+            tb = m->abytes;
+            CK(cub::DeviceScan::ExclusiveSum(m->atmp, tb, m->afl, m->afr, (int)C, st), "scan free particle slots");
+            k_abio_free_list<<<nblk(C, BS), BS, 0, st>>>(m->afl, m->afr, C, m->afree);
+            k_abio_place<<<nblk(G, BS), BS, 0, st>>>(g, A, C, m->cflag, m->crank, m->afl, m->afr, m->afree, sb.err,
+                                                      sb.err_iter, m->iteration);
+            CK(cudaGetLastError(), "k_abio_place");
+        }
+        ProfScope ps_(m, "k_abio_move");
+        (ll ? k_abio_move<true> : k_abio_move<false>)<<<nblk(C, 128), 128, 0, st>>>(g, A, C, sa, dT, m->seed, iter, vp,
+                                                                                     m->bgc.kappa_hP, m->bgc.kappa_vP, sb.err);
+        CK(cudaGetLastError(), "k_abio_move");
+    }
+    return PI_OK;
+}
+
+// The interaction, the release and their diagnostics after the phytoplankton (time_step.jl:120-158).
+pi_status enqueue_abiotic_exchange(pi_model* m, double dT) {
+    const DGrid& g = m->dg;
+    const long long G = g.G, C = m->C;
+    const uint32_t iter = (uint32_t)m->iteration;
+    cudaStream_t st = m->stream;
+    StepBufs& sb = m->sb;
+    const bool ll = m->met != nullptr;
+    const int BS = 256;
+    for (const auto& pr : m->pal_intac) {
+        ProfScope ps_(m, "k_interact");
+        const SpcDev& P = m->h_spc[pr.first];
+        const AbioDev& A = m->h_ab[pr.second];
+        k_diag_keys<<<nblk(C, BS), BS, 0, st>>>(g, P, C, m->pkey, m->pval, sb.err);
+        k_abio_keys<<<nblk(C, BS), BS, 0, st>>>(g, A, C, m->akey, m->aval, sb.err);
+        size_t tb = m->abytes;
+        CK(cub::DeviceRadixSort::SortPairs(m->atmp, tb, m->pkey, m->pkey_s, m->pval, m->pval_s, (int64_t)C, 0, m->key_bits, st),
+           "sort phytoplankton by cell");
+        tb = m->abytes;
+        CK(cub::DeviceRadixSort::SortPairs(m->atmp, tb, m->akey, m->akey_s, m->aval, m->aval_s, (int64_t)C, 0, m->key_bits, st),
+           "sort particles by cell");
+        (ll ? k_interact<true> : k_interact<false>)<<<nblk(C, 128), 128, 0, st>>>(
+            g, P, A, C, m->pkey_s, m->pval_s, m->akey_s, m->aval_s, m->ap[pr.second].Rd, m->maxc, m->max_ptc[pr.first],
+            m->intac, sb.err, sb.err_iter, m->iteration);
+        CK(cudaGetLastError(), "k_interact");
+    }
+    for (size_t q = 0; q < m->pal_release.size(); ++q) {
+        ProfScope ps_(m, "k_release");
+        const auto& pr = m->pal_release[q];
+        const SpcDev& P = m->h_spc[pr.first];
+        const AbioDev& A = m->h_ab[pr.second];
+        k_release_flags<<<nblk(C, BS), BS, 0, st>>>(P, A, C, m->ap[pr.second].release_P, dT, m->seed, iter, (int)q,
+                                                    sb.flag64, sb.err);
+        size_t tb = m->cub_bytes;
+        CK(cub::DeviceScan::ExclusiveSum(m->cub_tmp, tb, sb.flag64, sb.rank64, (int64_t)C, st), "scan release flags");
+        k_lists<<<nblk(C, BS), BS, 0, st>>>(sb.flag64, sb.rank64, C, sb.divlist, sb.freelist, sb.ndiv, sb.err, sb.err_iter,
+                                            m->iteration, PI_DEVERR_CAPACITY | PI_DEVERR_ABIO);
+        k_release<<<148 * 2, 256, 0, st>>>(P, A, sb.divlist, sb.freelist, sb.ndiv, m->seed, iter, (int)q, m->nsp - 1, sb.err);
+        CK(cudaGetLastError(), "k_release");
+    }
+    {
+        ProfScope ps_(m, "k_abio_diags");
+        for (int s = 0; s < m->nsp; ++s) {          // diags.phytos[sp].ptc in ascending slot order per cell
+            k_diag_keys<<<nblk(C, BS), BS, 0, st>>>(g, m->h_spc[s], C, m->pkey, m->pval, sb.err);
+            size_t tb = m->abytes;
+            CK(cub::DeviceRadixSort::SortPairs(m->atmp, tb, m->pkey, m->pkey_s, m->pval, m->pval_s, (int64_t)C, 0, m->key_bits, st),
+               "sort phytoplankton by cell");
+            k_diag_sum<<<nblk(C, BS), BS, 0, st>>>(C, G, m->pkey_s, m->pval_s, m->h_spc[s].ptc, 1u, m->diag_ptc + (size_t)s * G);
+        }
+        for (int sa = 0; sa < m->nsa; ++sa)
+            k_abio_num<<<nblk(C, BS), BS, 0, st>>>(g, m->h_ab[sa], C, m->diag_abn + (size_t)sa * G, sb.err);
+        CK(cudaGetLastError(), "k_abio_diags");
+    }
+    return PI_OK;
 }
 
 // Enqueues one TimeStep! on the model's stream (no synchronisation).
@@ -244,6 +377,11 @@ pi_status enqueue_step(pi_model* m, double dT) {
                 return fail(m, PI_ERR_SHAPE, "BoundsError: time-dependent flux boundary condition has " +
                                                  std::to_string(m->bcs[n][f].nt) + " snapshots, step " +
                                                  std::to_string(m->iteration + 1) + " needs one more");
+    for (const DevBC& b : m->abc)
+        if (b.kind == PI_BC_ARRAY3D && b.nt < m->iteration + 1)
+            return fail(m, PI_ERR_SHAPE, "BoundsError: time-dependent particle flux boundary condition has " +
+                                             std::to_string(b.nt) + " snapshots, step " + std::to_string(m->iteration + 1) +
+                                             " needs one more");
     m->iteration += 1;
     m->t = (double)m->iteration * dT;
     m->last_dT = dT;
@@ -262,6 +400,7 @@ pi_status enqueue_step(pi_model* m, double dT) {
     VelPtrs vp{m->vel0[0], m->vel0[1], m->vel0[2], m->velh[0], m->velh[1], m->velh[2],
                m->vel1[0], m->vel1[1], m->vel1[2]};
     const bool ll = m->met != nullptr;      // LatLonGrid: the kernels that read grid metrics take their arrays
+    if (m->nsa) { pi_status e = enqueue_abiotic_update(m, dT, vp); if (e) return e; }
     { ProfScope ps_(m, "k_particles_sorted");
     (ll ? k_particles_sorted<true> : k_particles_sorted<false>)<<<nblk(NC, 128), 128, 0, st>>>(g, m->d_spc, C, sb.gid_sorted, sb.off, G, dT, m->seed, iter, vp,
                                                       m->bgc.kappa_hP, m->bgc.kappa_vP, sb.cnt, sb.key, sb.err);
@@ -337,6 +476,7 @@ pi_status enqueue_step(pi_model* m, double dT) {
             CK(cudaGetLastError(), "k_diag_proc");
         }
     }
+    if (m->nsa) { pi_status e = enqueue_abiotic_exchange(m, dT); if (e) return e; }
     {
         { ProfScope ps_(m, "k_sweep_x");
         (ll ? k_sweep_x<true> : k_sweep_x<false>)<<<dim3(nblk(nblk(g.Nx, 31), SWX_WARPS), g.Ny, g.Nz), 32 * SWX_WARPS, 0, st>>>(g, m->tr, m->tta, m->vel1[0], dT, sb.err);
@@ -549,7 +689,7 @@ pi_status pi_create(const pi_grid* grid, const pi_bgc_params* bgc, const pi_quot
         SpcDev& P = m->h_spc[s];
         ALB(P.x, C); ALB(P.y, C); ALB(P.z, C); ALB(P.Sz, C); ALB(P.Bm, C); ALB(P.Cq, C); ALB(P.Nq, C);
         ALB(P.Pq, C); ALB(P.Chl, C); ALB(P.gen, C); ALB(P.age, C); ALB(P.flags, C); ALB(P.cell, C);
-        ALB(P.stat, C);
+        ALB(P.stat, C); ALB(P.ptc, C);
     }
     ALB(m->d_spc, nspecies);
 #undef ALB
@@ -575,7 +715,7 @@ pi_status pi_create(const pi_grid* grid, const pi_bgc_params* bgc, const pi_quot
     ok = ok && cudaMemsetAsync(sb.err_iter, 0, sizeof(int64_t), s0) == cudaSuccess;
     for (int s = 0; s < nspecies; ++s) {
         const SpcDev& P = m->h_spc[s];
-        for (double* p : { P.x, P.y, P.z, P.Sz, P.Bm, P.Cq, P.Nq, P.Pq, P.Chl, P.gen, P.age })
+        for (double* p : { P.x, P.y, P.z, P.Sz, P.Bm, P.Cq, P.Nq, P.Pq, P.Chl, P.gen, P.age, P.ptc })
             ok = ok && cudaMemsetAsync(p, 0, C * sizeof(double), s0) == cudaSuccess;
         ok = ok && cudaMemsetAsync(P.flags, 0, C, s0) == cudaSuccess;
         ok = ok && cudaMemsetAsync(P.stat, 0, C, s0) == cudaSuccess;
@@ -758,6 +898,8 @@ pi_status pi_set_individuals(pi_model* m, int32_t sp, const pi_individuals* in) 
         if (in->Bd) CK(cudaMemcpyAsync(P.Bd, in->Bd, C * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload individuals");
         else CK(cudaMemsetAsync(P.Bd, 0, C * sizeof(double), m->stream), "upload individuals");
     }
+    if (in->ptc) CK(cudaMemcpyAsync(P.ptc, in->ptc, C * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload individuals");
+    else CK(cudaMemsetAsync(P.ptc, 0, C * sizeof(double), m->stream), "upload individuals");
     CK(cudaMemcpyAsync(P.flags, flags.data(), C, cudaMemcpyHostToDevice, m->stream), "upload flags");
     CK(cudaMemcpyAsync(P.cell, cell.data(), C * sizeof(int32_t), cudaMemcpyHostToDevice, m->stream), "upload cells");
     CK(cudaMemsetAsync(P.stat, 0, C, m->stream), "reset step status");
@@ -775,6 +917,7 @@ pi_status pi_get_individuals(pi_model* m, int32_t sp, pi_individuals* out) {
     for (int q = 0; q < 11; ++q)
         if (hptr[q]) CK(cudaMemcpyAsync(hptr[q], dptr[q], C * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download individuals");
     if (m->carbon && out->Bd) CK(cudaMemcpyAsync(out->Bd, P.Bd, C * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download individuals");
+    if (out->ptc) CK(cudaMemcpyAsync(out->ptc, P.ptc, C * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download individuals");
     if (m->macro) {
         double* mh[6] = { out->PRO, out->DNA, out->RNA, out->CH, out->NST, out->PST };
         const double* md[6] = { P.PRO, P.DNA, P.RNA, P.CH, P.NST, P.PST };
@@ -926,6 +1069,141 @@ pi_status pi_set_flux_bc(pi_model* m, int32_t tracer, int32_t face, int32_t kind
         CK(cudaMemcpyAsync(b.v, values, n * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload bc");
     }
     return upload_bcs(m);
+}
+
+pi_status pi_set_abiotics(pi_model* m, int32_t nsa, const pi_abiotic_params* params, int32_t n_intac, const int32_t* intac,
+                          int32_t n_release, const int32_t* release, int32_t max_candidates, const double* max_ptc) {
+    if (m && m->b32) return fail(m, PI_ERR_ARG, "pi_set_abiotics: abiotic particles are built in the FP64 form only");
+    if (!m || nsa < 1 || !params || max_candidates < 1 || !max_ptc || n_intac < 0 || n_release < 0 ||
+        (n_intac && !intac) || (n_release && !release))
+        return fail(m, PI_ERR_ARG, "pi_set_abiotics: bad argument");
+    if (m->nsa) return fail(m, PI_ERR_STATE, "pi_set_abiotics: the model already has abiotic particles");
+    for (int32_t q = 0; q < n_intac + n_release; ++q) {       // models.jl:127-142
+        const int32_t* pr = q < n_intac ? intac + 2 * q : release + 2 * (q - n_intac);
+        if (pr[0] < 0 || pr[0] >= m->nsp) return fail(m, PI_ERR_ARG, "Abiotic: sp" + std::to_string(pr[0] + 1) + " is not generated");
+        if (pr[1] < 0 || pr[1] >= nsa) return fail(m, PI_ERR_ARG, "Abiotic: sa" + std::to_string(pr[1] + 1) + " is not generated");
+    }
+    const long long C = m->C, G = m->hg.G;
+    if ((double)max_candidates * (double)C > 9.0e18) return fail(m, PI_ERR_ARG, "pi_set_abiotics: max_candidates too large");
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    pi_status e;
+    std::vector<AbioDev> ab((size_t)nsa);
+    for (AbioDev& A : ab) {
+        if ((e = dalloc(m, &A.x, C, "abiotic particles")) || (e = dalloc(m, &A.y, C, "abiotic particles")) ||
+            (e = dalloc(m, &A.z, C, "abiotic particles")) || (e = dalloc(m, &A.ac, C, "abiotic particles")) ||
+            (e = dalloc(m, &A.cell, C, "abiotic particles")))
+            return e;
+        for (double* p : { A.x, A.y, A.z }) CK(cudaMemsetAsync(p, 0, C * sizeof(double), m->stream), "zero abiotic particles");
+        CK(cudaMemsetAsync(A.ac, 0, C, m->stream), "zero abiotic particles");
+        CK(cudaMemsetAsync(A.cell, 0, C * sizeof(int32_t), m->stream), "zero abiotic particles");   // (0, 0, 0) as constructed
+    }
+    if ((e = dalloc(m, &m->intac, (size_t)max_candidates * C, "interaction candidates")) ||
+        (e = dalloc(m, &m->diag_ptc, (size_t)m->nsp * G, "ptc diagnostics")) ||
+        (e = dalloc(m, &m->diag_abn, (size_t)nsa * G, "abiotic diagnostics")) ||
+        (e = dalloc(m, &m->cflag, G, "boundary cells")) || (e = dalloc(m, &m->crank, G, "boundary cells")) ||
+        (e = dalloc(m, &m->afl, C, "free particle slots")) || (e = dalloc(m, &m->afr, C, "free particle slots")) ||
+        (e = dalloc(m, &m->afree, C, "free particle slots")))
+        return e;
+    for (uint32_t** p : { &m->akey, &m->akey_s, &m->aval, &m->aval_s, &m->pkey, &m->pkey_s, &m->pval, &m->pval_s })
+        if ((e = dalloc(m, p, (size_t)C, "cell binning"))) return e;
+    size_t b1 = 0, b2 = 0, b3 = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, b1, m->akey, m->akey_s, m->aval, m->aval_s, (int64_t)C, 0, m->key_bits, m->stream);
+    cub::DeviceScan::ExclusiveSum(nullptr, b2, m->cflag, m->crank, (int)G, m->stream);
+    cub::DeviceScan::ExclusiveSum(nullptr, b3, m->afl, m->afr, (int)C, m->stream);
+    m->abytes = std::max(b1, std::max(b2, b3));
+    unsigned char* tmp = nullptr;
+    if ((e = dalloc(m, &tmp, std::max<size_t>(m->abytes, 1), "abiotic scratch"))) return e;
+    m->atmp = tmp;
+    CK(cudaMemsetAsync(m->diag_ptc, 0, (size_t)m->nsp * G * sizeof(double), m->stream), "zero diagnostics");
+    CK(cudaMemsetAsync(m->diag_abn, 0, (size_t)nsa * G * sizeof(double), m->stream), "zero diagnostics");
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    m->h_ab = ab;
+    m->ap.assign(params, params + nsa);
+    m->abc.assign((size_t)nsa * 6, DevBC{});
+    for (int32_t q = 0; q < n_intac; ++q) m->pal_intac.emplace_back(intac[2 * q], intac[2 * q + 1]);
+    for (int32_t q = 0; q < n_release; ++q) m->pal_release.emplace_back(release[2 * q], release[2 * q + 1]);
+    m->maxc = max_candidates;
+    m->max_ptc.assign(max_ptc, max_ptc + m->nsp);
+    m->nsa = nsa;
+    return PI_OK;
+}
+
+pi_status pi_set_abiotic_particles(pi_model* m, int32_t sa, const pi_abiotic_particles* in) {
+    if (!m || sa < 0 || sa >= m->nsa || !in || !in->x || !in->y || !in->z || !in->ac)
+        return fail(m, PI_ERR_ARG, "pi_set_abiotic_particles: bad argument");
+    const long long C = m->C;
+    const HostGrid& g = m->hg;
+    std::vector<int32_t> cell((size_t)C);
+    for (long long k = 0; k < C; ++k) {
+        if (in->ac[k] > 1) return fail(m, PI_ERR_PARAM, "pi_set_abiotic_particles: ac must be 0 or 1");
+        const int64_t xi = in->xi ? in->xi[k] : 0, yi = in->yi ? in->yi[k] : 0, zi = in->zi ? in->zi[k] : 0;
+        if (xi < 0 || xi > g.Gx || yi < 0 || yi > g.Gy || zi < 0 || zi > g.Gz)
+            return fail(m, PI_ERR_PARAM, "pi_set_abiotic_particles: xi/yi/zi outside 0..G");
+        cell[k] = pack_cell(m->dg, (int)xi, (int)yi, (int)zi);
+    }
+    const AbioDev& A = m->h_ab[sa];
+    CK(cudaMemcpyAsync(A.x, in->x, C * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload abiotic particles");
+    CK(cudaMemcpyAsync(A.y, in->y, C * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload abiotic particles");
+    CK(cudaMemcpyAsync(A.z, in->z, C * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload abiotic particles");
+    CK(cudaMemcpyAsync(A.ac, in->ac, C, cudaMemcpyHostToDevice, m->stream), "upload abiotic particles");
+    CK(cudaMemcpyAsync(A.cell, cell.data(), C * sizeof(int32_t), cudaMemcpyHostToDevice, m->stream), "upload abiotic particles");
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    return PI_OK;
+}
+
+pi_status pi_get_abiotic_particles(pi_model* m, int32_t sa, pi_abiotic_particles* out) {
+    if (!m || sa < 0 || sa >= m->nsa || !out) return fail(m, PI_ERR_ARG, "pi_get_abiotic_particles: bad argument");
+    const long long C = m->C;
+    const AbioDev& A = m->h_ab[sa];
+    double* hp[3] = { out->x, out->y, out->z };
+    const double* dp[3] = { A.x, A.y, A.z };
+    for (int q = 0; q < 3; ++q)
+        if (hp[q]) CK(cudaMemcpyAsync(hp[q], dp[q], C * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download abiotic particles");
+    if (out->ac) CK(cudaMemcpyAsync(out->ac, A.ac, C, cudaMemcpyDeviceToHost, m->stream), "download abiotic particles");
+    std::vector<int32_t> cell((size_t)C);
+    CK(cudaMemcpyAsync(cell.data(), A.cell, C * sizeof(int32_t), cudaMemcpyDeviceToHost, m->stream), "download abiotic particles");
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    for (long long k = 0; k < C; ++k) {
+        int xi, yi, zi;
+        unpack_cell(m->dg, cell[k], xi, yi, zi);
+        if (out->xi) out->xi[k] = xi;
+        if (out->yi) out->yi[k] = yi;
+        if (out->zi) out->zi[k] = zi;
+    }
+    return PI_OK;
+}
+
+pi_status pi_count_abiotic(pi_model* m, int32_t sa, int64_t* n) {
+    if (!m || !n || sa < 0 || sa >= m->nsa) return fail(m, PI_ERR_ARG, "pi_count_abiotic: bad argument");
+    unsigned long long* d = (unsigned long long*)m->sb.rank64;   // scratch between steps
+    unsigned long long h = 0;
+    CK(cudaMemsetAsync(d, 0, sizeof h, m->stream), "zero count");
+    k_count_active<<<148 * 2, 256, 0, m->stream>>>(m->h_ab[sa].ac, m->C, d);
+    CK(cudaGetLastError(), "k_count_active");
+    CK(cudaMemcpyAsync(&h, d, sizeof h, cudaMemcpyDeviceToHost, m->stream), "download count");
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    *n = (int64_t)h;
+    return PI_OK;
+}
+
+pi_status pi_set_abiotic_bc(pi_model* m, int32_t sa, int32_t face, int32_t kind, const double* values, int64_t nt) {
+    if (!m || sa < 0 || sa >= m->nsa || face < 0 || face > 5 || kind < 0 || kind > 3)
+        return fail(m, PI_ERR_ARG, "pi_set_abiotic_bc: bad argument");
+    const HostGrid& g = m->hg;
+    size_t n1 = face <= PI_EAST ? g.Ny : g.Nx, n2 = face <= PI_NORTH ? g.Nz : g.Ny;
+    size_t n = kind == PI_BC_CONST ? 1 : kind == PI_BC_ARRAY2D ? n1 * n2 : kind == PI_BC_ARRAY3D ? n1 * n2 * (size_t)std::max<int64_t>(nt, 0) : 0;
+    if (kind == PI_BC_ARRAY3D && nt < 1) return fail(m, PI_ERR_SHAPE, "BC: time-dependent flux needs nt >= 1");
+    if (n && !values) return fail(m, PI_ERR_ARG, "pi_set_abiotic_bc: NULL values");
+    CK(cudaStreamSynchronize(m->stream), "synchronize");
+    DevBC& b = m->abc[(size_t)sa * 6 + face];
+    if (b.v) { cudaFree(b.v); b.v = nullptr; }
+    b.kind = kind; b.nt = nt;
+    if (n) {
+        CK(cudaMalloc(&b.v, n * sizeof(double)), "bc values");
+        CK(cudaMemcpyAsync(b.v, values, n * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload bc");
+        CK(cudaStreamSynchronize(m->stream), "synchronize");
+    }
+    return PI_OK;
 }
 
 pi_status pi_time_step(pi_model* m, double dT) {
@@ -1116,6 +1394,10 @@ pi_status pi_get_diag(pi_model* m, int32_t kind, int32_t sp, double* out) {
         if (sp < 0 || sp >= m->nsp || !(m->proc_mask >> (kind - PI_DIAG_PROC) & 1u))
             return fail(m, PI_ERR_ARG, "pi_get_diag: process diagnostic not enabled or bad species");
         src = m->diag_proc + ((size_t)sp * PI_MAXPROC + (kind - PI_DIAG_PROC)) * G;
+    } else if (kind == PI_DIAG_PTC || kind == PI_DIAG_ABIO_NUM) {
+        const int n = kind == PI_DIAG_PTC ? m->nsp : m->nsa;
+        if (sp < 0 || sp >= n || !m->nsa) return fail(m, PI_ERR_ARG, "pi_get_diag: no abiotic particles or bad species");
+        src = (kind == PI_DIAG_PTC ? m->diag_ptc : m->diag_abn) + (size_t)sp * G;
     } else {
         if (sp < 0 || sp >= m->nsp || kind < PI_DIAG_NUM || kind > PI_DIAG_DVID) return fail(m, PI_ERR_ARG, "pi_get_diag: bad kind/species");
         src = m->diag_sp + ((size_t)sp * 4 + (kind - PI_DIAG_NUM)) * G;
@@ -1158,6 +1440,8 @@ pi_status pi_reset_diags(pi_model* m) {
     CK(cudaMemsetAsync(m->diag_sp, 0, 4 * m->nsp * G * sizeof(double), m->stream), "reset diags");
     if (m->diag_tr) CK(cudaMemsetAsync(m->diag_tr, 0, (size_t)PI_NTRACERS * G * sizeof(double), m->stream), "reset diags");
     if (m->diag_proc) CK(cudaMemsetAsync(m->diag_proc, 0, (size_t)m->nsp * PI_MAXPROC * G * sizeof(double), m->stream), "reset diags");
+    if (m->diag_ptc) CK(cudaMemsetAsync(m->diag_ptc, 0, (size_t)m->nsp * G * sizeof(double), m->stream), "reset diags");
+    if (m->diag_abn) CK(cudaMemsetAsync(m->diag_abn, 0, (size_t)m->nsa * G * sizeof(double), m->stream), "reset diags");
     CK(cudaStreamSynchronize(m->stream), "synchronize");
     return PI_OK;
 }

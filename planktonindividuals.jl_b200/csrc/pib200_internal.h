@@ -37,6 +37,8 @@
 // Device error word bits (sticky until pi_synchronize reads and clears them).
 #define PI_DEVERR_DOMAIN   1u
 #define PI_DEVERR_CAPACITY 2u
+#define PI_DEVERR_ABIO     4u   // with CAPACITY: the overflow was of abiotic particle slots
+#define PI_DEVERR_MAXPTC   8u   // with CAPACITY: a merge into a species without max_ptc
 
 // Per-individual flag byte: ac plus the three 0/1 decisions carried to the next step.
 #define FL_AC   1u
@@ -84,9 +86,18 @@ struct SpcDev {
     double* Bd;         // CarbonMode damaged biomass (NULL for QuotaMode)
     // MacroMolecularMode pools (NULL otherwise): protein, DNA, RNA, carbohydrate/lipid, N and P reserves
     double *PRO, *DNA, *RNA, *CH, *NST, *PST;
+    double* ptc;        // abiotic particles held (every mode)
     uint8_t* flags;
     int32_t* cell;      // packed (xi, yi, zi)
     uint8_t* stat;      // ST_* bits of the current step
+};
+
+// One abiotic species (Abiotic/particle_generation.jl:2-5): positions, activity and the packed
+// find_inds! cell of `capacity` slots.
+struct AbioDev {
+    double *x, *y, *z;
+    uint8_t* ac;
+    int32_t* cell;
 };
 
 struct SpcParams {      // pi_quota_params on the device
