@@ -18,6 +18,7 @@ export set_velocity!, set_PARF!, set_temp!, set_flux_bc!, time_step!, get_time, 
 export count_active, get_diag, reset_diags!, check_finite, budget, simulation, update!, synchronize
 export set_velocity_f32!, set_PARF_f32!, set_temp_f32!, time_step_async!, count_active_async!, set_diags!
 export batch_create, batch_step!, batch_set_sort_interval!
+export set_abiotics!, set_abiotic_particles!, get_abiotic_particles, count_abiotic, set_bc_particle!
 
 const lib = get(ENV, "LIBPIB200", joinpath(@__DIR__, "..", "PlanktonIndividuals", "libpib200.so"))
 
@@ -29,7 +30,8 @@ const PI_FP32 = Int32(1)
 const PI_PERIODIC = Int32(0)
 const PI_BOUNDED = Int32(1)
 const TRACERS = (:DIC, :NH4, :NO3, :PO4, :DFe, :DOC, :DON, :DOP, :PFe_inorg, :POC, :PON, :POP, :PFe_bio, :Dust)
-const DIAG_KINDS = Dict(:PAR => Int32(0), :num => Int32(1), :graz => Int32(2), :mort => Int32(3), :dvid => Int32(4))
+const DIAG_KINDS = Dict(:PAR => Int32(0), :num => Int32(1), :graz => Int32(2), :mort => Int32(3), :dvid => Int32(4),
+                        :ptc => Int32(5), :abiotic_num => Int32(6))   # abiotic_num: sp is the abiotic species
 # optional diagnostics: PI_DIAG_TRACER + tracer index, PI_DIAG_PROC + process index
 const PI_DIAG_TRACER = Int32(16)
 const PI_DIAG_PROC = Int32(32)
@@ -107,6 +109,19 @@ struct PiIndividuals
     Bd::Ptr{Float64}            # CarbonMode damaged biomass (C_NULL for QuotaMode)
     PRO::Ptr{Float64}; DNA::Ptr{Float64}; RNA::Ptr{Float64}    # MacroMolecularMode pools (C_NULL otherwise)
     CH::Ptr{Float64}; NST::Ptr{Float64}; PST::Ptr{Float64}
+    ptc::Ptr{Float64}           # abiotic particles held (every mode); C_NULL uploads zeros
+end
+
+# construct_abiotic_particle's parameters (Abiotic/particle_generation.jl:7) and one species' state
+struct PiAbiotic
+    Nsuper::Float64; Rd::Float64; release_P::Float64; sz_min::Float64; Ktr::Float64
+end
+const ABIOTIC_KEYS = ("Nsuper", "Rd", "release_P", "sz_min", "Ktr")
+PiAbiotic(p::AbstractDict, sa::Integer) = PiAbiotic(ntuple(i -> Float64(p[ABIOTIC_KEYS[i]][sa]), 5)...)
+struct PiAbioticParticles
+    x::Ptr{Float64}; y::Ptr{Float64}; z::Ptr{Float64}
+    xi::Ptr{Int64}; yi::Ptr{Int64}; zi::Ptr{Int64}
+    ac::Ptr{UInt8}
 end
 
 struct PiMember
@@ -239,9 +254,11 @@ function set_individuals!(m::Model, sp::Integer, d)
     cols = (Float64.(d.x), Float64.(d.y), Float64.(d.z), Int64.(d.xi), Int64.(d.yi), Int64.(d.zi),
             szbm..., quota..., Float64.(d.Chl), Float64.(d.gen), Float64.(d.age),
             UInt8.(d.ac), Float64.(d.graz), Float64.(d.mort), Float64.(d.dvid))
-    GC.@preserve cols bd pools begin
+    ptc = hasproperty(d, :ptc) ? Float64.(d.ptc) : Float64[]
+    GC.@preserve cols bd pools ptc begin
         pp = m.mm ? map(pointer, pools) : ntuple(_ -> Ptr{Float64}(C_NULL), 6)
-        pi = Ref(PiIndividuals(map(pointer, cols)..., m.carbon ? pointer(bd) : Ptr{Float64}(C_NULL), pp...))
+        pi = Ref(PiIndividuals(map(pointer, cols)..., m.carbon ? pointer(bd) : Ptr{Float64}(C_NULL), pp...,
+                               isempty(ptc) ? Ptr{Float64}(C_NULL) : pointer(ptc)))
         check(ccall((:pi_set_individuals, lib), Int32, (Ptr{Cvoid}, Int32, Ref{PiIndividuals}), m.h, sp - 1, pi), m.h)
     end
 end
@@ -253,18 +270,21 @@ function get_individuals(m::Model, sp::Integer)
     q = ntuple(_ -> zeros(Float64, C), 8); ac = zeros(UInt8, C); dec = ntuple(_ -> zeros(Float64, C), 3)
     bd = zeros(Float64, C)
     pools = ntuple(_ -> zeros(Float64, C), 6)
-    GC.@preserve f i q ac dec bd pools begin
+    ptc = zeros(Float64, C)      # stays zero for a Float32 model, which keeps no abiotic particles
+    GC.@preserve f i q ac dec bd pools ptc begin
         pi = Ref(PiIndividuals(pointer(f[1]), pointer(f[2]), pointer(f[3]), pointer(i[1]), pointer(i[2]), pointer(i[3]),
-                               map(pointer, q)..., pointer(ac), map(pointer, dec)..., pointer(bd), map(pointer, pools)...))
+                               map(pointer, q)..., pointer(ac), map(pointer, dec)..., pointer(bd), map(pointer, pools)...,
+                               pointer(ptc)))
         check(ccall((:pi_get_individuals, lib), Int32, (Ptr{Cvoid}, Int32, Ref{PiIndividuals}), m.h, sp - 1, pi), m.h)
     end
     m.mm && return (x = f[1], y = f[2], z = f[3], xi = i[1], yi = i[2], zi = i[3], PRO = pools[1], DNA = pools[2],
                        RNA = pools[3], CH = pools[4], NST = pools[5], PST = pools[6], Chl = q[6], gen = q[7], age = q[8],
-                       ac = ac .== 1, graz = dec[1], mort = dec[2], dvid = dec[3])
+                       ac = ac .== 1, graz = dec[1], mort = dec[2], dvid = dec[3], ptc = ptc)
     m.carbon ? (x = f[1], y = f[2], z = f[3], xi = i[1], yi = i[2], zi = i[3], Sz = q[1], Bm = q[2], Bd = bd,
-                Chl = q[6], gen = q[7], age = q[8], ac = ac .== 1, graz = dec[1], mort = dec[2], dvid = dec[3]) :
+                Chl = q[6], gen = q[7], age = q[8], ac = ac .== 1, graz = dec[1], mort = dec[2], dvid = dec[3], ptc = ptc) :
                (x = f[1], y = f[2], z = f[3], xi = i[1], yi = i[2], zi = i[3], Sz = q[1], Bm = q[2], Cq = q[3], Nq = q[4],
-                Pq = q[5], Chl = q[6], gen = q[7], age = q[8], ac = ac .== 1, graz = dec[1], mort = dec[2], dvid = dec[3])
+                Pq = q[5], Chl = q[6], gen = q[7], age = q[8], ac = ac .== 1, graz = dec[1], mort = dec[2], dvid = dec[3],
+                ptc = ptc)
 end
 
 tracer_index(name::Symbol) = Int32(findfirst(==(name), TRACERS) - 1)
@@ -302,6 +322,56 @@ function set_flux_bc!(m::Model, tracer::Symbol, pos::Symbol, value)
                      ndims(value) == 2 ? (2, vec(Float64.(value)), 0) : (3, vec(Float64.(value)), size(value, 3))
     check(ccall((:pi_set_flux_bc, lib), Int32, (Ptr{Cvoid}, Int32, Int32, Int32, Ptr{Float64}, Int64),
                 m.h, tracer_index(tracer), FACES[pos], kind, vals, nt), m.h)
+end
+
+# abiotic = abiotic_setup(params, N, Nsa, Palat(intac, release)) and max_candidates of PlanktonModel
+# (models.jl:99-146), FP64 models: pairs are (phytoplankton, abiotic) species indices (1-based);
+# max_ptc per phytoplankton species, NaN for modes without that parameter (a merge then fails).
+function set_abiotics!(m::Model, params::AbstractDict, Nsa::Integer; intac = (), release = (),
+                       max_candidates::Integer = 25, max_ptc = fill(NaN, m.Nsp))
+    ps = [PiAbiotic(params, a) for a in 1:Nsa]
+    ia = Int32[v - 1 for p in intac for v in p]; ra = Int32[v - 1 for p in release for v in p]
+    mp = Float64.(collect(max_ptc))
+    check(ccall((:pi_set_abiotics, lib), Int32,
+                (Ptr{Cvoid}, Int32, Ptr{PiAbiotic}, Int32, Ptr{Int32}, Int32, Ptr{Int32}, Int32, Ptr{Float64}),
+                m.h, Nsa, ps, length(intac), ia, length(release), ra, max_candidates, mp), m.h)
+end
+
+"""Upload abiotic species `sa` (1-based): x, y, z, ac and optionally xi, yi, zi."""
+function set_abiotic_particles!(m::Model, sa::Integer, d)
+    cols = (Float64.(d.x), Float64.(d.y), Float64.(d.z))
+    cells = hasproperty(d, :xi) ? (Int64.(d.xi), Int64.(d.yi), Int64.(d.zi)) : ()
+    ac = UInt8.(d.ac)
+    GC.@preserve cols cells ac begin
+        cp = isempty(cells) ? ntuple(_ -> Ptr{Int64}(C_NULL), 3) : map(pointer, cells)
+        pa = Ref(PiAbioticParticles(map(pointer, cols)..., cp..., pointer(ac)))
+        check(ccall((:pi_set_abiotic_particles, lib), Int32, (Ptr{Cvoid}, Int32, Ref{PiAbioticParticles}), m.h, sa - 1, pa), m.h)
+    end
+end
+
+"""model.individuals.abiotics[sa].data (1-based sa) as a NamedTuple."""
+function get_abiotic_particles(m::Model, sa::Integer)
+    C = m.capacity
+    f = ntuple(_ -> zeros(Float64, C), 3); i = ntuple(_ -> zeros(Int64, C), 3); ac = zeros(UInt8, C)
+    GC.@preserve f i ac begin
+        pa = Ref(PiAbioticParticles(map(pointer, f)..., map(pointer, i)..., pointer(ac)))
+        check(ccall((:pi_get_abiotic_particles, lib), Int32, (Ptr{Cvoid}, Int32, Ref{PiAbioticParticles}), m.h, sa - 1, pa), m.h)
+    end
+    (x = f[1], y = f[2], z = f[3], xi = i[1], yi = i[2], zi = i[3], ac = ac .== 1)
+end
+
+function count_abiotic(m::Model, sa::Integer)
+    n = Ref{Int64}(0)
+    check(ccall((:pi_count_abiotic, lib), Int32, (Ptr{Cvoid}, Int32, Ref{Int64}), m.h, sa - 1, n), m.h)
+    n[]
+end
+
+# set_bc_particle!(model; sa, pos, bc_value) (HaloRegions/boundary_conditions.jl:33-41)
+function set_bc_particle!(m::Model, sa::Integer, pos::Symbol, value)
+    kind, vals, nt = value isa Number ? (1, [Float64(value)], 0) :
+                     ndims(value) == 2 ? (2, vec(Float64.(value)), 0) : (3, vec(Float64.(value)), size(value, 3))
+    check(ccall((:pi_set_abiotic_bc, lib), Int32, (Ptr{Cvoid}, Int32, Int32, Int32, Ptr{Float64}, Int64),
+                m.h, sa - 1, FACES[pos], kind, vals, nt), m.h)
 end
 
 # TimeStep!(model, ΔT, diags) (src/Model/time_step.jl:12-180)
