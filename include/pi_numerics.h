@@ -24,6 +24,11 @@
  *    compensated power-by-squaring path (`pow_body`: Dekker two-product with an error term carried
  *    beside each square, one fused multiply-add at the end). The reference raises to 4.0f0 and
  *    2.0f0 in its shape functions (src/Individuals/utils.jl:109-137); this restates that method.
+ *  - pi_log: x = m·2^e by frexp (exact) with m in [√½, √2), then log x = e·ln2 + 2·atanh(s),
+ *    s = (m − 1)/(m + 1), the atanh by its odd Taylor series through s^25 (|s| < 0.1716, truncation
+ *    < 1e-20) in Horner form, ln2 split as in pi_exp. pi_pow(x, y) = pi_exp(y·pi_log(x)) for x >= 0,
+ *    for the reference's non-integer powers (Sz^(2/3), IronEnergyMode/growth_kernels.jl:48);
+ *    agreement with Julia's correctly rounded pow is to a few ulp and not pinned.
  *  - Julia semantics: `min`/`max` propagate NaN and order -0.0 < 0.0; `isless` orders NaN last;
  *    `x * b::Bool` is `ifelse(b, x, copysign(0, x))`; `mod(x, 1)` is `rem` moved into [0, 1).
  */
@@ -64,6 +69,12 @@ PI_HD double jl_min(double x, double y) {
 }
 
 /* Julia isless on floats: total order -Inf < ... < -0.0 < 0.0 < ... < Inf < NaN. */
+/* isequal(x, y): NaN equals NaN, -0.0 differs from 0.0 */
+PI_HD int jl_isequal(double x, double y) {
+    if (x != x || y != y) return (x != x) && (y != y);
+    return x == y && signbit(x) == signbit(y);
+}
+
 PI_HD int jl_isless(double x, double y) {
     if (pi_isnan(x)) return 0;
     if (pi_isnan(y)) return 1;
@@ -133,6 +144,29 @@ PI_HD double pi_exp(double x) {
     if (k > 1023) { p = p * 0x1p1023; k -= 1023; }
     if (k < -1022) { p = p * 0x1p-1022; k += 1022; }
     return p * pi_pow2i(k);
+}
+
+PI_HD double pi_log(double x) {
+    if (pi_isnan(x) || x < 0.0) return NAN;
+    if (x == 0.0) return -INFINITY;
+    if (x == INFINITY) return x;
+    int e = 0;
+    double m = frexp(x, &e);                          /* x = m·2^e, m in [0.5, 1) */
+    if (m < 0x1.6a09e667f3bcdp-1) { m = m * 2.0; e -= 1; }
+    const double ln2_hi = 0x1.62e42fee00000p-1, ln2_lo = 0x1.a39ef35793c76p-33;
+    double f = m - 1.0, s = f / (2.0 + f), z = s * s;
+    double t = 1.0 / 25.0;
+    t = t * z + 1.0 / 23.0; t = t * z + 1.0 / 21.0; t = t * z + 1.0 / 19.0; t = t * z + 1.0 / 17.0;
+    t = t * z + 1.0 / 15.0; t = t * z + 1.0 / 13.0; t = t * z + 1.0 / 11.0; t = t * z + 1.0 / 9.0;
+    t = t * z + 1.0 / 7.0; t = t * z + 1.0 / 5.0; t = t * z + 1.0 / 3.0;
+    double lm = 2.0 * s + 2.0 * s * (z * t);
+    double ed = (double)e;
+    return ed * ln2_hi + (lm + ed * ln2_lo);
+}
+
+PI_HD double pi_pow(double x, double y) {
+    if (x == 0.0) return y > 0.0 ? 0.0 : (y == 0.0 ? 1.0 : INFINITY);
+    return pi_exp(y * pi_log(x));
 }
 
 /* ------------------------------------------------------------------------------------------ */

@@ -84,6 +84,13 @@ enum { PI_CPROC_PS = 0, PI_CPROC_BS, PI_CPROC_RP, PI_CPROC_RS, PI_CPROC_TD, PI_C
 enum { PI_MPROC_PS = 0, PI_MPROC_VDOC, PI_MPROC_VNH4, PI_MPROC_VNO3, PI_MPROC_VPO4, PI_MPROC_resp,
        PI_MPROC_rChl, PI_MPROC_S_PRO, PI_MPROC_S_DNA, PI_MPROC_S_RNA, PI_MPROC_exu, PI_MPROC_CH,
        PI_MPROC_NST, PI_MPROC_PST, PI_MPROC_PRO, PI_MPROC_DNA, PI_MPROC_RNA, PI_MPROC_Chl, PI_NMPROC };
+/* The processes of an IronEnergyMode model (diags_spcs!, diagnostics_kernels.jl:22-23, without
+ * :ptc, which is PI_DIAG_PTC): 32 fields, all bits of proc_mask. */
+enum { PI_IPROC_PS = 0, PI_IPROC_CF, PI_IPROC_ECF, PI_IPROC_RS, PI_IPROC_ERS, PI_IPROC_NR, PI_IPROC_ENR,
+       PI_IPROC_NF, PI_IPROC_ENF, PI_IPROC_BS, PI_IPROC_VNH4, PI_IPROC_VNO3, PI_IPROC_VPO4, PI_IPROC_VFe,
+       PI_IPROC_PS2ST, PI_IPROC_ST2PS, PI_IPROC_NR2ST, PI_IPROC_ST2NR, PI_IPROC_NF2ST, PI_IPROC_ST2NF,
+       PI_IPROC_Bm, PI_IPROC_exEn, PI_IPROC_CH, PI_IPROC_qNO3, PI_IPROC_qNH4, PI_IPROC_qP, PI_IPROC_qFe,
+       PI_IPROC_qFePS, PI_IPROC_qFeNR, PI_IPROC_qFeNF, PI_IPROC_Chl, PI_IPROC_tdark, PI_NIPROC };
 
 /* The horizontal metrics of a LatLonGrid (src/Grids/lat_lon_grid.jl:1-45, built by
  * LatLonGrid :57-170 or LoadLatLonGrid :196-316), as the reference stores them: halos included,
@@ -153,6 +160,17 @@ typedef struct {
     double dvid_P, grz_P, mort_P, mort_reg, grazFracC, grazFracN, grazFracP, mortFracC, mortFracN, mortFracP;
 } pi_macro_params;
 
+/* IronEnergyMode phytoplankton parameters of one species, in the reference's param_names order
+ * (src/Individuals/Plankton/IronEnergyMode/plankton_generation.jl:27-36). */
+typedef struct {
+    double Nsuper, Cquota, SA, mean, var, Chl2Cint, alpha, Topt, Tmax, Ea, is_nr, is_croc, is_tric;
+    double PCmax, VNO3max, VNH4max, VPO4max, k_cf, k_rs, k_nr, k_nf, k_mtb, e_cf, e_rs, e_nr, e_nf;
+    double k_Fe_ST2PS, k_Fe_PS2ST, k_Fe_ST2NR, k_Fe_NR2ST, k_Fe_ST2NF, k_Fe_NF2ST;
+    double KfePS, KfeNR, KfeNF, KsatNH4, KsatNO3, KsatPO4, KSAFe, CHmax, qNH4max, qNO3max, qPmax, qFemax;
+    double Chl2N, R_NC, R_PC, NF_clock, grz_P, dvid_type, dvid_P, dvid_reg, dvid_reg2, mort_P, mort_reg;
+    double grazFracC, grazFracN, grazFracP, grazFracFe, mortFracC, mortFracN, mortFracP, mortFracFe, max_ptc;
+} pi_iron_params;
+
 /* The persistent per-individual state of one species (QuotaMode struct-of-arrays,
  * plankton_generation.jl:2-13; CarbonMode, CarbonMode/plankton_generation.jl:2-11, keeps Bd, the
  * damaged biomass, and no Cq, Nq, Pq). Every array is `capacity` long. graz/mort/dvid carry the
@@ -170,6 +188,10 @@ typedef struct {
                                                   carbohydrate/lipid, N and P reserves) */
     double  *ptc;                                /* abiotic particles held (every mode); NULL on
                                                   pi_set_individuals sets zeros */
+    double  *qNO3, *qNH4, *qP, *qFe, *qFePS, *qFeNR, *qFeNF, *exEn, *tdark;   /* IronEnergyMode
+                                                  only, with CH: N, P and Fe (storage, photosystem,
+                                                  nitrate reductase, nitrogenase) quotas, excess
+                                                  energy and the time since sunset */
 } pi_individuals;
 
 typedef struct pi_model pi_model;
@@ -199,6 +221,16 @@ pi_status pi_create_carbon(const pi_grid* grid, const pi_bgc_params* bgc,
 pi_status pi_create_macro(const pi_grid* grid, const pi_bgc_params* bgc,
                           const pi_macro_params* species, int32_t nspecies, int64_t capacity,
                           int32_t precision, uint64_t seed, pi_model** out);
+
+/* PlanktonModel(arch, grid; mode = IronEnergyMode(), ...): as pi_create with IronEnergyMode species
+ * (src/Individuals/Plankton/IronEnergyMode/): individuals carry Sz, Bm, CH, qNO3, qNH4, qP, qFe,
+ * qFePS, qFeNR, qFeNF, exEn, Chl, tdark, gen and age; the step also reads DFe and the change of PAR
+ * since the previous step, and its consumption and losses reach DFe and PFe_bio. Built in the FP64
+ * form (precision PI_FP64; PI_FP32 is refused with PI_ERR_ARG). pi_get_budget reports the
+ * individuals' C (Bm + CH), N (Bm·R_NC + qNO3 + qNH4) and P (Bm·R_PC + qP). */
+pi_status pi_create_iron(const pi_grid* grid, const pi_bgc_params* bgc,
+                         const pi_iron_params* species, int32_t nspecies, int64_t capacity,
+                         int32_t precision, uint64_t seed, pi_model** out);
 
 /* Releases every device allocation of the handle. */
 pi_status pi_destroy(pi_model* m);

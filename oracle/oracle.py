@@ -44,6 +44,10 @@ def load():
         _lib.orc_exp.argtypes = [ct.c_double]
         _lib.orc_pow_int.restype = ct.c_double
         _lib.orc_pow_int.argtypes = [ct.c_double, ct.c_int]
+        for name in ("orc_log", "orc_pow"):
+            getattr(_lib, name).restype = ct.c_double
+        _lib.orc_log.argtypes = [ct.c_double]
+        _lib.orc_pow.argtypes = [ct.c_double, ct.c_double]
         _lib.orc_draw3.restype = None
         _lib.orc_draw3.argtypes = [ct.c_uint64, ct.c_uint32, ct.c_uint32, ct.c_uint32, ct.c_uint32, dp]
         _lib.orc_num_threads.restype = ct.c_int
@@ -89,6 +93,14 @@ def pi_exp(x):
 
 def pow_int(x, n):
     return load().orc_pow_int(float(x), int(n))
+
+
+def pi_log(x):
+    return load().orc_log(float(x))
+
+
+def pi_pow(x, y):
+    return load().orc_pow(float(x), float(y))
 
 
 def draw3(seed, iteration, species, purpose, slot):

@@ -111,6 +111,12 @@ struct Species {
     dvec PRO, DNA, RNA, CH, NST, PST, S_PRO, S_DNA, S_RNA;
     /* abiotic particles held (ptc, every mode's plankton_generation.jl) and their diagnostic */
     dvec ptc, d_ptc;
+    /* IronEnergyMode species (IronEnergyMode/plankton_generation.jl:2-22; CH and RS are shared with
+     * the fields above): N, P and Fe quotas, excess energy, time since sunset, and the rates */
+    int iron = 0;
+    pi_iron_params ipp{};
+    dvec qNO3, qNH4, qP, qFe, qFePS, qFeNR, qFeNF, exEn, tdark;
+    dvec CF, ECF, NF, ENF, VFe, PS2ST, ST2PS, NR2ST, ST2NR, NF2ST, ST2NF, ERS, NR, ENR;
 };
 
 struct FluxBC { int kind = PI_BC_NONE; dvec v; int64_t nt = 0; };
@@ -638,9 +644,11 @@ std::string capacity_message(double t) {
 
 bool plankton_update_carbon(orc_model* m, Species& s, int spi, double dT, double t);
 bool plankton_update_macro(orc_model* m, Species& s, int spi, double dT, double t);
+bool plankton_update_iron(orc_model* m, Species& s, int spi, double dT, double t);
 
 /* plankton_update!, QuotaMode/plankton_update.jl:1-34 */
 bool plankton_update(orc_model* m, Species& s, int spi, double dT, double t) {
+    if (s.iron) return plankton_update_iron(m, s, spi, dT, t);
     if (s.carbon) return plankton_update_carbon(m, s, spi, dT, t);
     if (s.macro) return plankton_update_macro(m, s, spi, dT, t);
     const pi_quota_params& p = s.p;
@@ -1074,6 +1082,246 @@ bool plankton_update_macro(orc_model* m, Species& s, int spi, double dT, double 
 /* ---------------------------------------------------------------------------------------- */
 
 /* Difference operators with landmask, Advection/operaters.jl:1-14 */
+/* ---------------------------------------------------------------------------------------- */
+/* IronEnergyMode physiology, src/Individuals/Plankton/IronEnergyMode/ (all files)           */
+/* ---------------------------------------------------------------------------------------- */
+
+inline double i_tempFunc_CF(double T, const pi_iron_params& p) {   /* growth_kernels.jl:2-9 */
+    double x = T - p.Topt, xmax = p.Tmax - p.Topt;
+    double regT = shape_func_dec(x, xmax, F_4em2, 4);
+    double k = pi_exp(-p.Ea / (F_RGAS * (T + F_T0))) * regT;
+    k = jl_max(0.0, k);
+    double OGT_rate = pi_exp(-p.Ea / (F_RGAS * (p.Topt + F_T0)));
+    return jl_min(1.0, k / OGT_rate);
+}
+inline double i_tempFunc(double T, const pi_iron_params& p) {      /* :12-17 */
+    double k = pi_exp(-p.Ea / (F_RGAS * (T + F_T0)));
+    k = jl_max(0.0, k);
+    double OGT_rate = pi_exp(-p.Ea / (F_RGAS * (p.Topt + F_T0)));
+    return jl_min(1.0, k / OGT_rate);
+}
+/* the Fe quota sum, qFe + qFePS + qFeNF + qFeNR in the reference's order (:46, consume_loss.jl:28) */
+inline double i_feq(double qFe, double qFePS, double qFeNR, double qFeNF) { return qFe + qFePS + qFeNF + qFeNR; }
+
+/* plankton_growth! (plankton_growth.jl:2-26), one pass per kernel in the reference's order */
+void plankton_growth_iron(orc_model* m, Species& s, int spi, double dT, double t) {
+    const pi_iron_params& p = s.ipp;
+    const int64_t C = m->C;
+    const double nfx = p.is_croc + p.is_tric;
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < C; ++i) {
+        const int ac = s.ac[i];
+        const double NH4 = m->tNH4[i], NO3 = m->tNO3[i], PO4 = m->tPO4[i], DFe = m->tDFe[i];
+        const double par = m->tpar[i], dpar = m->tdpar[i], T = m->tT[i], pop = m->tpop[i];
+        const double Bm = s.Bm[i], Sz = s.Sz[i];
+        double CH = s.CH[i], qNH4 = s.qNH4[i], qNO3 = s.qNO3[i], qP = s.qP[i], qFe = s.qFe[i];
+        const double qFePS = s.qFePS[i], qFeNR = s.qFeNR[i], qFeNF = s.qFeNF[i], Chl = s.Chl[i];
+        /* calc_trs_uptake_kernel! (growth_kernels.jl:56-66) with calc_NH4/NO3/P/Fe_uptake (:20-53) */
+        double reg = shape_func_dec(qNH4 / jl_max(F_1em30, Bm + CH), p.qNH4max, F_1em4, 2);
+        double VNH4 = jl_mulb(p.VNH4max * reg * NH4 / jl_max(F_1em30, NH4 + p.KsatNH4) * i_tempFunc(T, p) * Bm, ac);
+        VNH4 = jl_min(VNH4, NH4 / dT / jl_max(1.0, pop)) * p.is_nr;
+        reg = shape_func_dec(qNO3 / jl_max(F_1em30, Bm + CH), p.qNO3max, F_1em4, 2);
+        double VNO3 = jl_mulb(p.VNO3max * reg * NO3 / jl_max(F_1em30, NO3 + p.KsatNO3) * i_tempFunc(T, p) * Bm, ac);
+        VNO3 = jl_min(VNO3, NO3 / dT / jl_max(1.0, pop)) * p.is_nr;
+        reg = shape_func_dec((qP + Bm * p.R_PC) / jl_max(F_1em30, Bm + CH), p.qPmax, F_1em4, 2);
+        double VPO4 = jl_mulb(p.VPO4max * reg * PO4 / jl_max(F_1em30, PO4 + p.KsatPO4) * i_tempFunc(T, p) * Bm, ac);
+        VPO4 = jl_min(VPO4, PO4 / dT / jl_max(1.0, pop));
+        reg = shape_func_dec(i_feq(qFe, qFePS, qFeNR, qFeNF) / jl_max(F_1em30, Bm + CH), p.qFemax, F_1em4, 2);
+        const double SA = p.SA * pi_pow(Sz, (double)(2.0f / 3.0f));
+        double VFe = jl_mulb(p.KSAFe * SA * DFe * reg * p.Nsuper * i_tempFunc(T, p), ac);
+        VFe = jl_min(VFe, DFe / dT / jl_max(1.0, pop));
+        /* update_state_1_kernel! (:73-79) */
+        qP += VPO4 * dT; qNO3 += VNO3 * dT; qNH4 += VNH4 * dT; qFe += VFe * dT;
+        /* calc_PS (:87-93) */
+        const double aI = par * p.alpha * Chl / jl_max(F_1em30, Bm);
+        const double Qfe_ps = qFePS / jl_max(F_1em30, Bm + CH);
+        const double PS = p.PCmax * (1.0 - pi_exp(-aI)) * Bm * (Qfe_ps / jl_max(F_1em30, Qfe_ps + p.KfePS));
+        /* calc_respir (:106-111) */
+        double RS = jl_mulb(CH * p.k_rs * i_tempFunc(T, p), ac);
+        RS = jl_min(RS, CH / dT);
+        double ERS = jl_mulb(RS * p.e_rs, ac);
+        /* calc_CF (:125-131) */
+        reg = shape_func_dec(CH / jl_max(F_1em30, Bm + CH), p.CHmax, F_1em4, 2);
+        double CF = jl_mulb(p.k_cf * reg * i_tempFunc_CF(T, p) * Bm, ac);
+        double ECF = jl_mulb(CF * p.e_cf, ac);
+        /* calc_NR (:145-155) */
+        reg = shape_func_dec(qNH4 / jl_max(F_1em30, Bm + CH), p.qNH4max, F_1em4, 2);
+        const double Qfe_NR = qFeNR / jl_max(F_1em30, Bm + CH);
+        double NR = jl_mulb(p.k_nr * reg * qNO3 * (Qfe_NR / jl_max(F_1em30, Qfe_NR + p.KfeNR)) * i_tempFunc(T, p), ac);
+        NR = jl_min(NR, qNO3 / dT);
+        double ENR = jl_mulb(NR * p.e_nr, ac);
+        NR = NR * p.is_nr; ENR = ENR * p.is_nr;
+        /* calc_NF (:167-176) */
+        const double Qfe_NF = qFeNF / jl_max(F_1em30, Bm + CH);
+        double NF = jl_mulb(p.k_nf * reg * (Qfe_NF / jl_max(F_1em30, Qfe_NF + p.KfeNF)) * i_tempFunc(T, p) * Bm, ac);
+        double ENF = jl_mulb(NF * p.e_nf, ac);
+        NF = NF * nfx; ENF = ENF * nfx;
+        /* energy_alloc (:190-197) and energy_allocation_kernel! (:198-206) */
+        const double ECFt = jl_min(PS, ECF);
+        const double ENFt = jl_min(ENF, PS + ERS - ECFt) * nfx;
+        const double ENRt = jl_min(ENR, PS + ERS - ECFt) * p.is_nr;
+        const double ERSt = jl_min(ERS, jl_max(0.0, ECFt + ENFt + ENRt - PS));
+        const double exEn = jl_max(0.0, PS - ECFt - ENFt - ENRt);
+        ERS = ERSt; ECF = ECFt; ENF = ENFt; ENR = ENRt;
+        RS = ERS / p.e_rs; CF = ECF / p.e_cf; NF = ENF / p.e_nf; NR = ENR / p.e_nr;
+        /* update_state_2_kernel! (:213-219) */
+        CH += (CF - RS) * dT;
+        qNO3 += -NR * dT;
+        qNH4 += NR * dT;
+        qNH4 += NF * dT;
+        /* calc_ρChl_kernel! (:227-231) and calc_BS_kernel! (:239-243) */
+        const double rChl = jl_mulb(jl_mulb(p.Chl2N / jl_max(F_1em30, par * p.alpha * Chl / Bm), jl_isless(F_1em1, par)), ac);
+        const double BS = jl_mulb(jl_min(jl_min(CH, qNH4 / p.R_NC), qP / p.R_PC) * p.k_mtb, ac);
+        /* iron_alloc (:251-283): Bool·Bool is a Bool, Bool + Bool an Int */
+        const int pos_dpar = jl_isless(0.0, dpar), neg_dpar = jl_isless(dpar, 0.0), dark = jl_isequal(0.0, par);
+        const int light = jl_isless(0.0, par), early = jl_isless(s.tdark[i], p.NF_clock), late = jl_isless(p.NF_clock, s.tdark[i]);
+        double ST2PS = jl_mulb(p.k_Fe_ST2PS * qFe, pos_dpar);
+        double PS2ST = p.k_Fe_PS2ST * qFePS * (double)(neg_dpar + dark);
+        double ST2NR = jl_mulb(jl_mulb(p.k_Fe_ST2NR * qFe, dark), early) * p.is_nr;
+        double NR2ST = p.k_Fe_NR2ST * qFeNR * (double)((dark & late) + light) * p.is_nr;
+        const double ST2NF_cr = jl_mulb(jl_mulb(p.k_Fe_ST2NF * qFe, dark), early);
+        const double NF2ST_cr = p.k_Fe_NF2ST * qFeNF * (double)((dark & late) + light);
+        const double ST2NF_tr = jl_mulb(p.k_Fe_ST2NF * qFe, pos_dpar);
+        const double NF2ST_tr = p.k_Fe_NF2ST * qFeNF * (double)(neg_dpar + dark);
+        double ST2NF = ST2NF_cr * p.is_croc + ST2NF_tr * p.is_tric;
+        double NF2ST = NF2ST_cr * p.is_croc + NF2ST_tr * p.is_tric;
+        ST2PS = jl_min(ST2PS, qFe / dT);
+        PS2ST = jl_min(PS2ST, qFePS / dT);
+        ST2NR = jl_min(ST2NR, qFe / dT - ST2PS);
+        NR2ST = jl_min(NR2ST, qFeNR / dT);
+        ST2NF = jl_min(ST2NF, qFe / dT - ST2PS);
+        NF2ST = jl_min(NF2ST, qFeNF / dT);
+        /* update_biomass_kernel! (:296-312), update_cellsize_kernel! (:322-325) */
+        const double Bm1 = Bm + dT * BS;
+        CH -= dT * BS;
+        qNH4 -= dT * BS * p.R_NC;
+        qP -= dT * BS * p.R_PC;
+        s.Chl[i] = Chl + dT * BS * p.R_NC * rChl;
+        s.age[i] = s.age[i] + jl_mulb(dT / 3600.0, ac);
+        s.qFe[i] = qFe + dT * (PS2ST - ST2PS + NR2ST - ST2NR + NF2ST - ST2NF);
+        s.qFePS[i] = qFePS + dT * (ST2PS - PS2ST);
+        s.qFeNR[i] = qFeNR + dT * (ST2NR - NR2ST);
+        s.qFeNF[i] = qFeNF + dT * (ST2NF - NF2ST);
+        s.Bm[i] = Bm1; s.CH[i] = CH; s.qNH4[i] = qNH4; s.qNO3[i] = qNO3; s.qP[i] = qP;
+        s.Sz[i] = Bm1 / (p.Cquota * p.Nsuper);
+        /* update_tdark_kernel! (:333-337): 1.0f0 − Bool is a Float32 */
+        s.tdark[i] = s.tdark[i] * (1.0 - (double)light) + jl_mulb(dT, dark);
+        s.exEn[i] = exEn;
+        s.PS[i] = PS; s.CF[i] = CF; s.ECF[i] = ECF; s.RS[i] = RS; s.ERS[i] = ERS; s.NR[i] = NR; s.ENR[i] = ENR;
+        s.NF[i] = NF; s.ENF[i] = ENF; s.BS[i] = BS; s.VNH4[i] = VNH4; s.VNO3[i] = VNO3; s.VPO4[i] = VPO4; s.VFe[i] = VFe;
+        s.PS2ST[i] = PS2ST; s.ST2PS[i] = ST2PS; s.NR2ST[i] = NR2ST; s.ST2NR[i] = ST2NR; s.NF2ST[i] = NF2ST; s.ST2NF[i] = ST2NF;
+        s.rChl[i] = rChl;
+        /* calc_graz_quadratic!, calc_mort!, calc_dvid! (division_death_probability.jl:7-68) */
+        s.graz[i] = jl_mulb(pop * p.grz_P, ac);
+        s.mort[i] = jl_mulb(p.mort_P * shape_func_dec(s.Sz[i], p.mort_reg, F_1em5, 4), ac);
+        double dv;
+        const int ty = (int)p.dvid_type;
+        if (ty == 1) dv = p.dvid_P * shape_func_inc(s.Sz[i], p.dvid_reg, F_2em3, 2);
+        else if (ty == 2) dv = p.dvid_P * shape_func_inc(fmod(t, 86400.0) / 3600.0, p.dvid_reg, F_1em5, 4);
+        else dv = p.dvid_P * shape_func_inc(s.Sz[i], p.dvid_reg, F_1em3, 4)
+                  * shape_func_inc(fmod(t, 86400.0) / 3600.0, p.dvid_reg2, F_1em5, 4);
+        s.dvid[i] = jl_mulb(dv, ac);
+    }
+    /* get_probability! (division_death_probability.jl:95-107) */
+    for (int64_t i = 0; i < C; ++i) {
+        double r0, r1, r2;
+        pi_draw3(m->seed, (uint32_t)m->iteration, (uint32_t)spi, PI_DRAW_DECISION, (uint32_t)i, &r0, &r1, &r2);
+        const int ac = s.ac[i];
+        s.graz[i] = (double)(jl_isless(r0, s.graz[i] * dT) && ac);
+        s.mort[i] = (double)(jl_isless(r1, s.mort[i] * dT) && ac);
+        s.dvid[i] = (double)(jl_isless(r2, s.dvid[i] * dT) && ac);
+    }
+}
+
+/* calc_loss_kernel! (IronEnergyMode/consume_loss.jl:17-32), then inactivate! */
+void calc_loss_iron(orc_model* m, Species& s, const dvec& loss, double fC, double fN, double fP, double fFe) {
+    const pi_iron_params& p = s.ipp;
+    for (int64_t i = 0; i < m->C; ++i) {
+        size_t c = cell_of(m, s, i);
+        int ac = s.ac[i];
+        const double l = loss[i], Bm = s.Bm[i], CH = s.CH[i], qP = s.qP[i];
+        const double fe = i_feq(s.qFe[i], s.qFePS[i], s.qFeNR[i], s.qFeNF[i]);
+        m->plk[PI_NH4][c] += jl_mulb(s.qNH4[i], ac) * l;
+        m->plk[PI_NO3][c] += jl_mulb(s.qNO3[i], ac) * l;
+        m->plk[PI_DOC][c] += jl_mulb((Bm + CH) * fC, ac) * l;
+        m->plk[PI_DON][c] += jl_mulb(Bm * p.R_NC * fN, ac) * l;
+        m->plk[PI_DOP][c] += jl_mulb((Bm * p.R_PC + qP) * fP, ac) * l;
+        m->plk[PI_DFe][c] += jl_mulb(fe * fFe, ac) * l;
+        m->plk[PI_POC][c] += jl_mulb((Bm + CH) * (1.0 - fC), ac) * l;
+        m->plk[PI_PON][c] += jl_mulb(Bm * p.R_NC * (1.0 - fN), ac) * l;
+        m->plk[PI_POP][c] += jl_mulb((Bm * p.R_PC + qP) * (1.0 - fP), ac) * l;
+        m->plk[PI_PFe_bio][c] += jl_mulb(fe * (1.0 - fFe), ac) * l;
+    }
+    for (int64_t i = 0; i < m->C; ++i) s.ac[i] = (uint8_t)(s.ac[i] && jl_isless(loss[i], 1.0));
+}
+
+/* plankton_update! (IronEnergyMode/plankton_update.jl:1-33) */
+bool plankton_update_iron(orc_model* m, Species& s, int spi, double dT, double t) {
+    const pi_iron_params& p = s.ipp;
+    const int64_t C = m->C;
+    diags_proc(m, s, s.d_graz, &s.graz);
+    calc_loss_iron(m, s, s.graz, p.grazFracC, p.grazFracN, p.grazFracP, p.grazFracFe);
+    diags_proc(m, s, s.d_mort, &s.mort);
+    calc_loss_iron(m, s, s.mort, p.mortFracC, p.mortFracN, p.mortFracP, p.mortFracFe);
+    for (int64_t i = 0; i < C; ++i) s.dvid[i] = jl_mulb(s.dvid[i], s.ac[i]);
+    diags_proc(m, s, s.d_dvid, &s.dvid);
+    double dvidnum = 0.0;
+    std::vector<int64_t> free_slots;
+    for (int64_t i = 0; i < C; ++i) {
+        dvidnum += s.dvid[i] * (double)s.ac[i];
+        if (!s.ac[i]) free_slots.push_back(i + 1);
+    }
+    if (dvidnum > (double)free_slots.size()) {
+        m->err = capacity_message(t);
+        m->err_flags |= ERR_CAPACITY;
+        return false;
+    }
+    /* divide! (division_death.jl:84-92): copy_daughter_individuals! (:44-70), divide_to_half! (:73-82) */
+    double acc = 0.0;
+    for (int64_t i = 0; i < C; ++i) { acc += s.dvid[i]; m->tidc[i] = acc; m->tidc_int[i] = (int64_t)acc; }
+    for (int64_t i = 0; i < C; ++i)
+        if (s.dvid[i] == 1.0) s.idx[i] = free_slots[(size_t)m->tidc_int[i] - 1];
+    dvec* copied[] = { &s.x, &s.y, &s.z, &s.Sz, &s.Bm, &s.CH, &s.qNO3, &s.qNH4, &s.qP, &s.qFe, &s.qFePS,
+                       &s.qFeNR, &s.qFeNF, &s.exEn, &s.Chl, &s.gen };
+    for (int64_t i = 0; i < C; ++i)
+        if (s.dvid[i] == 1.0 && s.idx[i] != 0) {
+            const int64_t d = s.idx[i] - 1;
+            for (dvec* v : copied) (*v)[d] = (*v)[i];
+            s.ac[d] = s.ac[i]; s.dvid[d] = s.dvid[i]; s.tdark[d] = s.tdark[i];
+        }
+    dvec* halved[] = { &s.Sz, &s.Bm, &s.CH, &s.qNO3, &s.qNH4, &s.qP, &s.qFe, &s.qFePS, &s.qFeNR, &s.qFeNF,
+                       &s.exEn, &s.Chl };
+    for (int64_t i = 0; i < C; ++i) {
+        const double f = (2.0 - s.dvid[i]) / 2.0;
+        for (dvec* v : halved) (*v)[i] *= f;
+        s.gen[i] += s.dvid[i];
+        s.age[i] *= (1.0 - s.dvid[i]);
+    }
+    for (int64_t i = 0; i < C; ++i) s.idx[i] = 0;
+    plankton_growth_iron(m, s, spi, dT, t);
+    /* calc_consume_kernel! (consume_loss.jl:2-9) */
+    for (int64_t i = 0; i < C; ++i) {
+        size_t c = cell_of(m, s, i);
+        int ac = s.ac[i];
+        m->plk[PI_DIC][c] += jl_mulb((s.RS[i] - s.PS[i]) * dT, ac);
+        m->plk[PI_NH4][c] += jl_mulb(-s.VNH4[i] * dT, ac);
+        m->plk[PI_NO3][c] += jl_mulb(-s.VNO3[i] * dT, ac);
+        m->plk[PI_PO4][c] += jl_mulb(-s.VPO4[i] * dT, ac);
+        m->plk[PI_DFe][c] += jl_mulb(-s.VFe[i] * dT, ac);
+    }
+    /* diags_spcs! (Diagnostics/diagnostics_kernels.jl:22-31), the IronEnergyMode processes */
+    if (m->proc_mask) {
+        const dvec* procs[PI_NIPROC] = { &s.PS, &s.CF, &s.ECF, &s.RS, &s.ERS, &s.NR, &s.ENR, &s.NF, &s.ENF, &s.BS,
+                                         &s.VNH4, &s.VNO3, &s.VPO4, &s.VFe, &s.PS2ST, &s.ST2PS, &s.NR2ST, &s.ST2NR,
+                                         &s.NF2ST, &s.ST2NF, &s.Bm, &s.exEn, &s.CH, &s.qNO3, &s.qNH4, &s.qP, &s.qFe,
+                                         &s.qFePS, &s.qFeNR, &s.qFeNF, &s.Chl, &s.tdark };
+        for (int q = 0; q < PI_NIPROC; ++q)
+            if (m->proc_mask & (1u << q)) diags_proc(m, s, s.d_proc[q], procs[q]);
+    }
+    diags_proc(m, s, s.d_num, nullptr);
+    return true;
+}
+
 struct Ops {
     const Grid& g;
     inline double dxp(const dvec& c, long i, long j, long k) const { return jl_mulb(jl_mulb(c[g.id(i + 1, j, k)] - c[g.id(i, j, k)], g.L(i + 1, j, k)), g.L(i, j, k)); }
@@ -1629,6 +1877,37 @@ int orc_create_macro(const pi_grid* grid, const pi_bgc_params* bgc, const pi_mac
     return PI_OK;
 }
 
+/* An IronEnergyMode model: the QuotaMode setup with the shared parameters, then the species switched
+ * to IronEnergyMode (their Cq, Nq, Pq stay zero). */
+int orc_create_iron(const pi_grid* grid, const pi_bgc_params* bgc, const pi_iron_params* species,
+                    int32_t nspecies, int64_t capacity, uint64_t seed, orc_model** out) {
+    if (!species || nspecies < 1) { g_create_err = "orc_create_iron: bad argument"; return PI_ERR_ARG; }
+    std::vector<pi_quota_params> q((size_t)nspecies);
+    for (int s = 0; s < nspecies; ++s) {
+        const pi_iron_params& c = species[s];
+        pi_quota_params& p = q[s];
+        memset(&p, 0, sizeof p);
+        p.Nsuper = c.Nsuper; p.Cquota = c.Cquota; p.mean = c.mean; p.var = c.var; p.Chl2Cint = c.Chl2Cint;
+        p.alpha = c.alpha; p.Topt = c.Topt; p.Tmax = c.Tmax; p.Ea = c.Ea; p.PCmax = c.PCmax;
+        p.R_NC = c.R_NC; p.R_PC = c.R_PC; p.grz_P = c.grz_P; p.dvid_type = c.dvid_type; p.dvid_P = c.dvid_P;
+        p.dvid_reg = c.dvid_reg; p.dvid_reg2 = c.dvid_reg2; p.mort_P = c.mort_P; p.mort_reg = c.mort_reg;
+        p.grazFracC = c.grazFracC; p.grazFracN = c.grazFracN; p.grazFracP = c.grazFracP;
+        p.mortFracC = c.mortFracC; p.mortFracN = c.mortFracN; p.mortFracP = c.mortFracP;
+    }
+    int st = orc_create(grid, bgc, q.data(), nspecies, capacity, seed, out);
+    if (st) return st;
+    for (int s = 0; s < nspecies; ++s) {
+        Species& S = (*out)->sp[s];
+        S.iron = 1;
+        S.ipp = species[s];
+        for (dvec* v : { &S.CH, &S.RS, &S.qNO3, &S.qNH4, &S.qP, &S.qFe, &S.qFePS, &S.qFeNR, &S.qFeNF, &S.exEn, &S.tdark,
+                         &S.CF, &S.ECF, &S.NF, &S.ENF, &S.VFe, &S.PS2ST, &S.ST2PS, &S.NR2ST, &S.ST2NR, &S.NF2ST,
+                         &S.ST2NF, &S.ERS, &S.NR, &S.ENR })
+            v->assign((size_t)capacity, 0.0);
+    }
+    return PI_OK;
+}
+
 int orc_destroy(orc_model* m) { delete m; return PI_OK; }
 
 int orc_set_individuals(orc_model* m, int32_t sp, const pi_individuals* in) {
@@ -1647,7 +1926,7 @@ int orc_set_individuals(orc_model* m, int32_t sp, const pi_individuals* in) {
     cp(S.Sz, in->Sz); cp(S.Bm, in->Bm);
     for (auto pr : { std::make_pair(&S.Cq, in->Cq), std::make_pair(&S.Nq, in->Nq), std::make_pair(&S.Pq, in->Pq) }) {
         if (pr.second) cp(*pr.first, pr.second);
-        else if (S.carbon) pr.first->assign(C, 0.0);
+        else if (S.carbon || S.iron) pr.first->assign(C, 0.0);
         else return PI_ERR_ARG;
     }
     }
@@ -1656,6 +1935,13 @@ int orc_set_individuals(orc_model* m, int32_t sp, const pi_individuals* in) {
     cp(S.graz, in->graz); cp(S.mort, in->mort); cp(S.dvid, in->dvid);
     if (S.carbon) { if (in->Bd) cp(S.Bd, in->Bd); else S.Bd.assign(C, 0.0); }
     if (in->ptc) cp(S.ptc, in->ptc); else S.ptc.assign(C, 0.0);
+    if (S.iron) {
+        const double* cols[8] = { in->CH, in->qNO3, in->qNH4, in->qP, in->qFe, in->qFePS, in->qFeNR, in->qFeNF };
+        dvec* dst[8] = { &S.CH, &S.qNO3, &S.qNH4, &S.qP, &S.qFe, &S.qFePS, &S.qFeNR, &S.qFeNF };
+        for (int q = 0; q < 8; ++q) { if (!cols[q]) return PI_ERR_ARG; cp(*dst[q], cols[q]); }
+        if (in->exEn) cp(S.exEn, in->exEn); else S.exEn.assign(C, 0.0);
+        if (in->tdark) cp(S.tdark, in->tdark); else S.tdark.assign(C, 0.0);
+    }
     return PI_OK;
 }
 
@@ -1676,6 +1962,11 @@ int orc_get_individuals(orc_model* m, int32_t sp, pi_individuals* out) {
         cp(out->CH, S.CH); cp(out->NST, S.NST); cp(out->PST, S.PST);
     }
     cp(out->ptc, S.ptc);
+    if (S.iron) {
+        cp(out->CH, S.CH); cp(out->qNO3, S.qNO3); cp(out->qNH4, S.qNH4); cp(out->qP, S.qP); cp(out->qFe, S.qFe);
+        cp(out->qFePS, S.qFePS); cp(out->qFeNR, S.qFeNR); cp(out->qFeNF, S.qFeNF); cp(out->exEn, S.exEn);
+        cp(out->tdark, S.tdark);
+    }
     return PI_OK;
 }
 
@@ -1912,8 +2203,9 @@ int orc_count_active(orc_model* m, int32_t sp, int64_t* n) {
 
 /* PlanktonDiagnostics(model; tracer, phytoplankton) optional fields: enabling clears them. */
 int orc_set_diags(orc_model* m, uint32_t tr_mask, uint32_t proc_mask) {
-    const int nproc = m ? (m->sp[0].macro ? (int)PI_NMPROC : m->sp[0].carbon ? (int)PI_NCPROC : (int)PI_NPROC) : 0;
-    if (!m || tr_mask >> PI_NTRACERS || proc_mask >> nproc) return PI_ERR_ARG;
+    const int nproc = m ? (m->sp[0].iron ? (int)PI_NIPROC : m->sp[0].macro ? (int)PI_NMPROC
+                           : m->sp[0].carbon ? (int)PI_NCPROC : (int)PI_NPROC) : 0;
+    if (!m || tr_mask >> PI_NTRACERS || (nproc < 32 && proc_mask >> nproc)) return PI_ERR_ARG;
     m->tr_mask = tr_mask; m->proc_mask = proc_mask;
     m->d_tr.assign(tr_mask ? PI_NTRACERS : 0, dvec(tr_mask ? m->g.G : 0, 0.0));
     for (Species& S : m->sp) S.d_proc.assign(proc_mask ? nproc : 0, dvec(proc_mask ? m->g.G : 0, 0.0));
@@ -1927,7 +2219,7 @@ int orc_get_diag(orc_model* m, int32_t kind, int32_t sp, double* out) {
     else if (kind >= PI_DIAG_TRACER && kind < PI_DIAG_TRACER + PI_NTRACERS) {
         if (!(m->tr_mask & (1u << (kind - PI_DIAG_TRACER)))) return PI_ERR_ARG;
         f = &m->d_tr[kind - PI_DIAG_TRACER];
-    } else if (kind >= PI_DIAG_PROC && kind < PI_DIAG_PROC + PI_NMPROC) {
+    } else if (kind >= PI_DIAG_PROC && kind < PI_DIAG_PROC + PI_NIPROC) {
         if (sp < 0 || sp >= m->nsp || !(m->proc_mask & (1u << (kind - PI_DIAG_PROC)))) return PI_ERR_ARG;
         if ((size_t)(kind - PI_DIAG_PROC) >= m->sp[sp].d_proc.size()) return PI_ERR_ARG;
         f = &m->sp[sp].d_proc[kind - PI_DIAG_PROC];
@@ -1963,6 +2255,8 @@ int orc_num_threads(void) {
 /* Numeric primitives exposed for tests of the shared header. */
 double orc_exp(double x) { return pi_exp(x); }
 double orc_pow_int(double x, int n) { return pi_pow_int(x, n); }
+double orc_log(double x) { return pi_log(x); }
+double orc_pow(double x, double y) { return pi_pow(x, y); }
 void orc_draw3(uint64_t seed, uint32_t it, uint32_t sp, uint32_t purpose, uint32_t slot, double* r) {
     pi_draw3(seed, it, sp, purpose, slot, &r[0], &r[1], &r[2]);
 }

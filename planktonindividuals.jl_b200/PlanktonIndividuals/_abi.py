@@ -116,6 +116,26 @@ MACRO_PROC_NAMES = ("PS", "VDOC", "VNH4", "VNO3", "VPO4", "resp", "ρChl", "S_PR
                     "CH", "NST", "PST", "PRO", "DNA", "RNA", "Chl")
 MACRO_POOLS = ("PRO", "DNA", "RNA", "CH", "NST", "PST")
 
+# IronEnergyMode param_names (src/Individuals/Plankton/IronEnergyMode/plankton_generation.jl:27-36)
+IRON_FIELDS = [(c, {"alpha": "α"}.get(c, c)) for c in (
+    "Nsuper", "Cquota", "SA", "mean", "var", "Chl2Cint", "alpha", "Topt", "Tmax", "Ea", "is_nr", "is_croc", "is_tric",
+    "PCmax", "VNO3max", "VNH4max", "VPO4max", "k_cf", "k_rs", "k_nr", "k_nf", "k_mtb", "e_cf", "e_rs", "e_nr", "e_nf",
+    "k_Fe_ST2PS", "k_Fe_PS2ST", "k_Fe_ST2NR", "k_Fe_NR2ST", "k_Fe_ST2NF", "k_Fe_NF2ST",
+    "KfePS", "KfeNR", "KfeNF", "KsatNH4", "KsatNO3", "KsatPO4", "KSAFe", "CHmax", "qNH4max", "qNO3max", "qPmax", "qFemax",
+    "Chl2N", "R_NC", "R_PC", "NF_clock", "grz_P", "dvid_type", "dvid_P", "dvid_reg", "dvid_reg2", "mort_P", "mort_reg",
+    "grazFracC", "grazFracN", "grazFracP", "grazFracFe", "mortFracC", "mortFracN", "mortFracP", "mortFracFe", "max_ptc")]
+
+
+class pi_iron_params(ct.Structure):
+    _fields_ = [(c, ct.c_double) for c, _ in IRON_FIELDS]
+
+
+# IronEnergyMode processes in PI_IPROC_* order (diags_spcs!, diagnostics_kernels.jl:22-23, :ptc aside)
+IRON_PROC_NAMES = ("PS", "CF", "ECF", "RS", "ERS", "NR", "ENR", "NF", "ENF", "BS", "VNH4", "VNO3", "VPO4", "VFe",
+                   "PS2ST", "ST2PS", "NR2ST", "ST2NR", "NF2ST", "ST2NF", "Bm", "exEn", "CH", "qNO3", "qNH4", "qP",
+                   "qFe", "qFePS", "qFeNR", "qFeNF", "Chl", "tdark")
+IRON_POOLS = ("CH", "qNO3", "qNH4", "qP", "qFe", "qFePS", "qFeNR", "qFeNF", "exEn", "tdark")
+
 
 IND_DOUBLE = ("x", "y", "z", "Sz", "Bm", "Cq", "Nq", "Pq", "Chl", "gen", "age", "graz", "mort", "dvid")
 IND_INT = ("xi", "yi", "zi")
@@ -130,7 +150,9 @@ class pi_individuals(ct.Structure):
                 ("graz", _dp), ("mort", _dp), ("dvid", _dp),
                 ("Bd", _dp),
                 ("PRO", _dp), ("DNA", _dp), ("RNA", _dp), ("CH", _dp), ("NST", _dp), ("PST", _dp),
-                ("ptc", _dp)]
+                ("ptc", _dp),
+                ("qNO3", _dp), ("qNH4", _dp), ("qP", _dp), ("qFe", _dp), ("qFePS", _dp), ("qFeNR", _dp),
+                ("qFeNF", _dp), ("exEn", _dp), ("tdark", _dp)]
 
 
 # construct_abiotic_particle's param_names (src/Individuals/Abiotic/particle_generation.jl:7)
@@ -176,6 +198,8 @@ def declare(lib, prefix):
                                        ct.POINTER(pi_carbon_params), ct.c_int32, ct.c_int64]),
         "create_macro": (ct.c_int32, [ct.POINTER(pi_grid), ct.POINTER(pi_bgc_params),
                                       ct.POINTER(pi_macro_params), ct.c_int32, ct.c_int64]),
+        "create_iron": (ct.c_int32, [ct.POINTER(pi_grid), ct.POINTER(pi_bgc_params),
+                                     ct.POINTER(pi_iron_params), ct.c_int32, ct.c_int64]),
         "last_error": (ct.c_int32, [P, ct.c_char_p, ct.c_size_t]),
         "set_abiotics": (ct.c_int32, [P, ct.c_int32, ct.POINTER(pi_abiotic_params), ct.c_int32,
                                       ct.POINTER(ct.c_int32), ct.c_int32, ct.POINTER(ct.c_int32), ct.c_int32, _dp]),
@@ -188,7 +212,7 @@ def declare(lib, prefix):
         fn = getattr(lib, prefix + name, None)
         if fn is None:
             continue
-        if name in ("create", "create_carbon", "create_macro"):
+        if name in ("create", "create_carbon", "create_macro", "create_iron"):
             if prefix == "pi_":
                 args = args + [ct.c_int32, ct.c_uint64, ct.POINTER(P)]
             else:

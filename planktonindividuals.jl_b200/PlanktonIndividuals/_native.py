@@ -69,7 +69,8 @@ def make_bgc_struct(params):
 
 def make_species_structs(phyt_params, nsp, mode="quota"):
     struct, fields = {"carbon": (_abi.pi_carbon_params, _abi.CARBON_FIELDS),
-                      "macro": (_abi.pi_macro_params, _abi.MACRO_FIELDS)}.get(mode, (pi_quota_params, QUOTA_FIELDS))
+                      "macro": (_abi.pi_macro_params, _abi.MACRO_FIELDS),
+                      "iron": (_abi.pi_iron_params, _abi.IRON_FIELDS)}.get(mode, (pi_quota_params, QUOTA_FIELDS))
     arr = (struct * nsp)()
     for s in range(nsp):
         for cname, key in fields:
@@ -84,10 +85,10 @@ class CModel:
 
     def __init__(self, lib, prefix, grid, bgc_params, phyt_params, nsp, capacity, seed,
                  precision=None, mode="quota"):
-        """mode: "quota" (QuotaMode), "carbon" (CarbonMode, `<prefix>create_carbon`) or "macro"
-        (MacroMolecularMode, `<prefix>create_macro`)."""
-        if mode not in ("quota", "carbon", "macro"):
-            raise ValueError(f"mode must be 'quota', 'carbon' or 'macro', not {mode!r}")
+        """mode: "quota" (QuotaMode), "carbon" (CarbonMode, `<prefix>create_carbon`), "macro"
+        (MacroMolecularMode, `<prefix>create_macro`) or "iron" (IronEnergyMode, `<prefix>create_iron`)."""
+        if mode not in ("quota", "carbon", "macro", "iron"):
+            raise ValueError(f"mode must be 'quota', 'carbon', 'macro' or 'iron', not {mode!r}")
         self.lib = _abi.declare(lib, prefix)
         self.prefix = prefix
         self.mode = mode
@@ -100,7 +101,7 @@ class CModel:
         b = make_bgc_struct(bgc_params)
         sp = make_species_structs(phyt_params, self.nsp, mode)
         h = ct.c_void_p()
-        fn = self._fn({"carbon": "create_carbon", "macro": "create_macro"}.get(mode, "create"))
+        fn = self._fn({"carbon": "create_carbon", "macro": "create_macro", "iron": "create_iron"}.get(mode, "create"))
         if precision is None:
             rc = fn(ct.byref(g), ct.byref(b), sp, self.nsp, self.capacity, ct.c_uint64(seed), ct.byref(h))
         else:
@@ -150,10 +151,13 @@ class CModel:
         C = self.capacity
         keep = {}
         st = pi_individuals()
-        carbon, macro = self.mode == "carbon", self.mode == "macro"
-        for k in IND_DOUBLE + (("Bd",) if carbon else ()) + (_abi.MACRO_POOLS if macro else ()):
+        carbon, macro, iron = self.mode == "carbon", self.mode == "macro", self.mode == "iron"
+        for k in IND_DOUBLE + (("Bd",) if carbon else ()) + (_abi.MACRO_POOLS if macro else ()) + \
+                (_abi.IRON_POOLS if iron else ()):
             if carbon and k in ("Cq", "Nq", "Pq", "Bd") and k not in data:
                 continue                      # CarbonMode keeps no quotas; Bd defaults to zero
+            if iron and (k in ("Cq", "Nq", "Pq") or (k in ("exEn", "tdark") and k not in data)):
+                continue                      # IronEnergyMode keeps its own quotas instead
             if macro and k in ("Sz", "Bm", "Cq", "Nq", "Pq"):
                 continue                      # MacroMolecularMode keeps its six pools instead
             a = np.ascontiguousarray(data[k], dtype=np.float64)
@@ -183,6 +187,8 @@ class CModel:
         carbon, macro = self.mode == "carbon", self.mode == "macro"
         if macro:
             names = tuple(k for k in IND_DOUBLE if k not in ("Sz", "Bm", "Cq", "Nq", "Pq")) + _abi.MACRO_POOLS
+        elif self.mode == "iron":
+            names = tuple(k for k in IND_DOUBLE if k not in ("Cq", "Nq", "Pq")) + _abi.IRON_POOLS
         else:
             names = tuple(k for k in IND_DOUBLE if not (carbon and k in ("Cq", "Nq", "Pq"))) + (("Bd",) if carbon else ())
         if self.precision == _abi.PI_FP64:

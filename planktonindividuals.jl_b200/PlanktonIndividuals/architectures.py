@@ -1,6 +1,6 @@
 """Architectures and physiology modes (src/Architectures.jl, src/PlanktonIndividuals.jl:59-83).
-GPU() with QuotaMode() (both precisions), CarbonMode() and MacroMolecularMode() (Float64) are
-implemented; IronEnergyMode exists so that code naming it fails with a clear message."""
+GPU() with QuotaMode() (both precisions), CarbonMode(), MacroMolecularMode() and IronEnergyMode()
+(Float64) are implemented."""
 
 
 class Architecture:
@@ -48,4 +48,8 @@ class MacroMolecularMode(AbstractMode):
 
 
 class IronEnergyMode(AbstractMode):
-    pass
+    """Energy budget with N, P and Fe quotas, iron allocation to photosynthesis, nitrate reduction
+    and nitrogen fixation (src/Individuals/Plankton/IronEnergyMode/)."""
+
+    def __repr__(self):
+        return "IronEnergyMode()"

@@ -79,6 +79,45 @@ def initialize_plankton_carbon(grid, p, s, N, C, rng):
     return d
 
 
+def initialize_plankton_iron(grid, p, s, N, C, rng):
+    """initialize_plankton! of IronEnergyMode (IronEnergyMode/plankton_generation.jl:53-95) for species
+    s: Sz = max(1, N(mean, var)), Bm = Cquota·Sz·Nsuper, CH, qNO3, qNH4, qP, qFe uniform up to a tenth
+    of their maxima, the iron split 0.4 / 0.3 / 0.3 between photosystem, nitrate reductase and
+    nitrogenase as the species has them, Chl = Bm·Chl2Cint."""
+    if N > C:
+        raise ValueError("PlanktonModel: number of individuals exceeds max_individuals")
+    d = empty_individuals(C)
+    for k in ("Cq", "Nq", "Pq"):
+        del d[k]
+    ac = np.zeros(C, dtype=bool)
+    ac[:N] = True
+    g = lambda k: species_param(p, k, s)
+    CHmax, qNO3max, qNH4max = g("CHmax") * 0.1, g("qNO3max") * 0.1, g("qNH4max") * 0.1
+    pqmax, feqmax = g("qPmax") * 0.1, g("qFemax") * 0.1
+    Sz = rng.standard_normal(C)
+    x, y, z = rng.random(C), rng.random(C), rng.random(C)
+    CH, qNO3, qNH4, qP, qFe = (rng.random(C) for _ in range(5))
+    d["ac"] = ac
+    d["gen"][:N] = 1.0
+    d["x"], d["y"], d["z"] = (x * grid.Nx) * ac, (y * grid.Ny) * ac, (z * grid.Nz) * ac
+    d["Sz"] = np.maximum(1.0, Sz * g("var") + g("mean")) * ac
+    d["Bm"] = g("Cquota") * d["Sz"] * g("Nsuper")
+    d["CH"] = CH * CHmax * d["Bm"]
+    d["qNO3"] = qNO3 * (qNO3max * (d["Bm"] + d["CH"]))
+    d["qNH4"] = qNH4 * (qNH4max * (d["Bm"] + d["CH"]))
+    d["qP"] = qP * (pqmax * (d["Bm"] + d["CH"]))
+    fe = qFe * (feqmax * (d["Bm"] + d["CH"]))
+    d["qFePS"] = fe * 0.4
+    d["qFeNR"] = fe * 0.3 * g("is_nr")
+    d["qFeNF"] = fe * 0.3 * (g("is_croc") + g("is_tric"))
+    d["qFe"] = fe - (d["qFePS"] + d["qFeNR"] + d["qFeNF"])
+    d["Chl"] = d["Bm"] * g("Chl2Cint")
+    d["exEn"] = np.zeros(C)
+    d["tdark"] = np.zeros(C)
+    mask_individuals(d, grid, N)
+    return d
+
+
 def initialize_plankton_macro(grid, p, s, N, C, rng):
     """initialize_plankton! of MacroMolecularMode (MacroMolecularMode/plankton_generation.jl:40-79)
     for species s: DNA in C_DNA·Nsuper·(1, 1 + var), RNA, PRO in (1 ± var) times their ratio to

@@ -5,9 +5,9 @@ import numpy as np
 from . import _abi, _lib
 from ._abi import NTRACERS, PI_FP32, PI_FP64, tracer_names
 from ._native import CModel
-from .architectures import GPU, CarbonMode, MacroMolecularMode, QuotaMode
+from .architectures import GPU, CarbonMode, IronEnergyMode, MacroMolecularMode, QuotaMode
 from .init import (generate_tracers, initialize_abiotic_particle, initialize_plankton, initialize_plankton_carbon,
-                   initialize_plankton_macro)
+                   initialize_plankton_iron, initialize_plankton_macro)
 from .parameters import (abiotic_params_default, bgc_params_default, default_tracer_init, phyt_params_default,
                          update_abiotic_params, update_bgc_params, update_phyt_params)
 
@@ -100,10 +100,14 @@ class PlanktonModel:
             mode = CarbonMode()
         if mode is MacroMolecularMode:
             mode = MacroMolecularMode()
+        if mode is IronEnergyMode:
+            mode = IronEnergyMode()
         carbon = isinstance(mode, CarbonMode)
         macro = isinstance(mode, MacroMolecularMode)
-        if mode is not None and not carbon and not macro and not isinstance(mode, QuotaMode) and mode is not QuotaMode:
-            raise NotImplementedError(f"{mode}: QuotaMode(), CarbonMode() and MacroMolecularMode() are implemented")
+        iron = isinstance(mode, IronEnergyMode)
+        if mode is not None and not (carbon or macro or iron) and not isinstance(mode, QuotaMode) and mode is not QuotaMode:
+            raise NotImplementedError(f"{mode}: QuotaMode(), CarbonMode(), MacroMolecularMode() and IronEnergyMode() "
+                                      f"are implemented")
         FT = np.dtype(FT).type
         if FT not in (np.float32, np.float64):
             raise ValueError("FT must be Float32 or Float64")
@@ -111,6 +115,8 @@ class PlanktonModel:
             raise NotImplementedError("CarbonMode() is built in the FP64 form: use FT = Float64")
         if macro and FT is not np.float64:
             raise NotImplementedError("MacroMolecularMode() is built in the FP64 form: use FT = Float64")
+        if iron and FT is not np.float64:
+            raise NotImplementedError("IronEnergyMode() is built in the FP64 form: use FT = Float64")
         if getattr(grid, "is_latlon", False) and FT is not np.float64:
             raise NotImplementedError("LatLonGrid is built in the FP64 form: use FT = Float64")
         if abiotic is not None:                                  # models.jl:99-117
@@ -131,7 +137,7 @@ class PlanktonModel:
                 raise ValueError("Abiotic parameters must be either Nothing or Dict!")
         self.FT = FT
         self.arch = GPU()
-        self.mode = mode if (carbon or macro) else QuotaMode()
+        self.mode = mode if (carbon or macro or iron) else QuotaMode()
         self.grid = grid
         self.max_candidates = max_candidates
         if bgc_params is None:
@@ -177,10 +183,12 @@ class PlanktonModel:
         lib = _lib.load()
         precision = PI_FP64 if FT is np.float64 else PI_FP32
         self._native = CModel(lib, "pi_", grid, bgc_final, phyto.params, nsp, max_individuals,
-                              seed, precision=precision, mode="carbon" if carbon else "macro" if macro else "quota")
+                              seed, precision=precision,
+                              mode="carbon" if carbon else "macro" if macro else "iron" if iron else "quota")
         if initial_state is None:
             rng = np.random.default_rng(seed)
-            init = initialize_plankton_carbon if carbon else initialize_plankton_macro if macro else initialize_plankton
+            init = (initialize_plankton_carbon if carbon else initialize_plankton_macro if macro else
+                    initialize_plankton_iron if iron else initialize_plankton)
             inds = [init(grid, phyto.params, s, phyto.N[s], max_individuals, rng) for s in range(nsp)]
             trs = generate_tracers(grid, tracer_initial or default_tracer_init(), rng)
         else:
@@ -252,7 +260,8 @@ class PlanktonDiagnostics:
             raise ValueError("tracer and phytoplankton must be Tuples")
         # diag_avail (diagnostics_struct.jl:115-136): names available for the model's mode
         proc_names = (_abi.CARBON_PROC_NAMES if isinstance(model.mode, CarbonMode) else
-                      _abi.MACRO_PROC_NAMES if isinstance(model.mode, MacroMolecularMode) else _abi.PROC_NAMES)
+                      _abi.MACRO_PROC_NAMES if isinstance(model.mode, MacroMolecularMode) else
+                      _abi.IRON_PROC_NAMES if isinstance(model.mode, IronEnergyMode) else _abi.PROC_NAMES)
         for t in tracer:
             if t not in tracer_names and t != "PAR":
                 raise ValueError(f"{t} is not one of the diagnostics")

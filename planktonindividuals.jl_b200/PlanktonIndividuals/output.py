@@ -163,7 +163,11 @@ def write_output_b(writer, model, diags):
     t, it = model.t, model.iteration
     phytos = model.individuals.phytos
     if writer.write_log:
-        from .architectures import CarbonMode, MacroMolecularMode
+        from .architectures import CarbonMode, IronEnergyMode, MacroMolecularMode
+        if isinstance(getattr(model, "mode", None), IronEnergyMode):
+            # write_species_dynamics for IronEnergyMode (write_outputs.jl:118-141) reads data.En,
+            # which IronEnergyMode individuals do not have (their field is exEn)
+            raise ValueError("type has no field En: write_species_dynamics fails for IronEnergyMode (use write_log = false)")
         if isinstance(getattr(model, "mode", None), MacroMolecularMode):
             # the reference defines write_species_dynamics for QuotaMode, IronEnergyMode and
             # CarbonMode only (write_outputs.jl:98-157)

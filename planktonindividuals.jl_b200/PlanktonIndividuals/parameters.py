@@ -57,7 +57,24 @@ def phyt_params_default(N=1, mode=None):
     """phyt_params_default(N, QuotaMode()) (param_default.jl:235-284), for CarbonMode()
     param_default.jl:290-320, for MacroMolecularMode() param_default.jl:94-141; one list entry per
     species."""
-    from .architectures import CarbonMode, MacroMolecularMode
+    from .architectures import CarbonMode, IronEnergyMode, MacroMolecularMode
+    if isinstance(mode, IronEnergyMode) or mode is IronEnergyMode:          # param_default.jl:156-228
+        params = {
+            "Nsuper": [1], "Cquota": [1.8e-11], "SA": [0.18], "mean": [1.2], "var": [0.3], "Chl2Cint": [0.10],
+            "α": [4.5e-2], "Topt": [27.0], "Tmax": [30.0], "Ea": [5.3e4], "is_nr": [1.0], "is_croc": [0.0],
+            "is_tric": [0.0], "PCmax": [7.8e-8], "VNH4max": [6.9e-6], "VNO3max": [6.9e-6], "VPO4max": [1.2e-6],
+            "k_cf": [1.0e-5], "k_rs": [1.5e-6], "k_nr": [2.8e-6], "k_nf": [2.8e-6], "k_mtb": [3.5e-5],
+            "e_cf": [9.0], "e_rs": [5.0], "e_nf": [8.0], "e_nr": [10.0], "k_Fe_ST2PS": [2.4e-5],
+            "k_Fe_PS2ST": [1.2e-6], "k_Fe_ST2NR": [1.2e-5], "k_Fe_NR2ST": [1.2e-5], "k_Fe_ST2NF": [1.2e-5],
+            "k_Fe_NF2ST": [1.2e-5], "KfePS": [3.0e-6], "KfeNR": [2.0e-6], "KfeNF": [5.0e-6], "KsatNH4": [0.005],
+            "KsatNO3": [0.010], "KsatPO4": [0.003], "KSAFe": [2.77e-19], "qNO3max": [0.25], "qNH4max": [0.25],
+            "qPmax": [0.02], "qFemax": [2.0e-5], "CHmax": [0.4], "Chl2N": [3.0], "R_NC": [16 / 106],
+            "R_PC": [1 / 106], "NF_clock": [21600.0], "grz_P": [0.0], "dvid_P": [1e-4], "dvid_type": [1],
+            "dvid_reg": [2.5], "dvid_reg2": [12.0], "mort_P": [5e-5], "mort_reg": [0.5], "grazFracC": [0.7],
+            "grazFracN": [0.7], "grazFracP": [0.7], "grazFracFe": [0.1], "mortFracC": [0.5], "mortFracN": [0.5],
+            "mortFracP": [0.5], "mortFracFe": [0.1], "max_ptc": [25],
+        }
+        return params if N == 1 else {k: [v[0]] * N for k, v in params.items()}
     if isinstance(mode, MacroMolecularMode) or mode is MacroMolecularMode:
         params = {
             "Nsuper": [1], "C_DNA": [1.8e-13], "var": [0.3], "RNA2DNA": [1.73], "PRO2DNA": [34.83],

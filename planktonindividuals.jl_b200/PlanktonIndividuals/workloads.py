@@ -294,6 +294,33 @@ def macro(nx=16, nz=8, N_per_species=2000, nsp=2, steps=30, dT=60.0, seed=13, nm
                     60 * dT, n_vel, vel, parf, 3600.0, tmp, 3600.0, seed, mode="macro")
 
 
+def iron(nx=16, nz=8, N_per_species=2000, nsp=2, steps=40, dT=120.0, seed=19, nmodes=16,
+         capacity=None, phyt_over=None, bgc_over=None, start_hour=17.5, DFe=1.0e-3):
+    """IronEnergyMode workload on a config-2-like 3D grid (nx×nx×nz, 50 m × 50 m × 2 m):
+    individuals from IronEnergyMode's initialize_plankton! rule, random-Fourier velocity, default
+    temperature, DFe ≈ `DFe` (±10 %), and the diel light cycle from `start_hour` (17:30: the
+    first hour lit, then night, so that a run of more than 30 steps of 120 s crosses sunset)."""
+    from .architectures import IronEnergyMode
+    from .init import initialize_plankton_iron
+    rng = np.random.default_rng(seed)
+    grid = RectilinearGrid(size=(nx, nx, nz), x=(0.0, nx * 50.0), y=(0.0, nx * 50.0),
+                           z=(0.0, -2.0 * nz), FT=np.float64, topology=(Periodic, Periodic, Bounded))
+    vel = FourierVelocity(grid, nmodes=nmodes, rms=0.05, seed=seed)
+    C = capacity or 2 * N_per_species
+    bgc = update_bgc_params(bgc_over or {}, np.float64)
+    phyt = update_phyt_params(phyt_over or {}, np.float64, N=nsp, mode=IronEnergyMode())
+    inds = [initialize_plankton_iron(grid, phyt, s, N_per_species, C, rng) for s in range(nsp)]
+    trs = make_tracers(grid, rng, no3_gradient_depth=2.0 * nz)
+    trs[tracer_names.index("DFe")] = np.asfortranarray(DFe * rng.uniform(0.9, 1.1, grid.total_size))
+    fill_halo_tracer(trs[tracer_names.index("DFe")], grid)
+    hours = int(np.ceil(steps * dT / 3600.0)) + 1
+    parf = diel_parf(grid.Nx, grid.Ny, hours, phase=(start_hour - 0.5) * 3600.0)
+    tmp = default_temperature(grid, dT, steps)
+    n_vel = int(np.ceil(steps / 60)) + 1
+    return Workload("iron", grid, bgc, phyt, nsp, C, [N_per_species] * nsp, inds, trs, dT, steps,
+                    60 * dT, n_vel, vel, parf, 3600.0, tmp, 3600.0, seed, mode="iron")
+
+
 def latlon_streamfunction_velocity(grid, cfl=0.2, dT=600.0, seed=0):
     """Divergence-free flow on a LatLonGrid from a corner streamfunction ψ of volume transport:
     U = −(ψ[i, j+1] − ψ[i, j]), V = ψ[i+1, j] − ψ[i, j] per level, u = U/Ax and v = V/Ay at the

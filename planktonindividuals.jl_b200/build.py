@@ -20,7 +20,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "PlanktonIndividuals", "libpib200.so")
 SOURCES = {"pib200.cu": ["-fmad=false", "-Xcompiler", "-ffp-contract=off"],
            "fp32.cu": ["-prec-div=false"]}
-DEPS = ["pib200.cu", "kernels_fp64.cuh", "kernels_abiotic.cuh", "pib200_internal.h", "noalloc.cu", "host_common.h",
+DEPS = ["pib200.cu", "kernels_fp64.cuh", "kernels_abiotic.cuh", "kernels_iron.cuh", "pib200_internal.h", "noalloc.cu", "host_common.h",
         "fp32.cu", "kernels_fp32.cuh", "fp32_internal.h", "kernels_tracer.cuh"]
 BUILD_DIR = os.path.join(HERE, "_build")
 

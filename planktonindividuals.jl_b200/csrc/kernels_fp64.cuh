@@ -320,7 +320,7 @@ __host__ __device__ __forceinline__ double m_totP(double DNA, double RNA, double
 // mode MODE_CARBON: CarbonMode losses (CarbonMode/consume_loss.jl:12-16), DOC and POC from Bm only;
 // MODE_MACRO: MacroMolecularMode losses (MacroMolecularMode/consume_loss.jl:14-24) from the total
 // C, N and P biomass (mp holds its R_NC_* and R_PC_* ratios).
-__global__ void k_decide(DGrid g, SpcDev P, pi_quota_params p, pi_macro_params mp, long long C, int s,
+__global__ void k_decide(DGrid g, SpcDev P, pi_quota_params p, pi_macro_params mp, pi_iron_params ip, long long C, int s,
                          const int32_t* __restrict__ pos, double* __restrict__ loss,
                          uint8_t* __restrict__ evk, unsigned long long* __restrict__ flag64,
                          double* __restrict__ d_graz, double* __restrict__ d_mort,
@@ -348,6 +348,23 @@ __global__ void k_decide(DGrid g, SpcDev P, pi_quota_params p, pi_macro_params m
             double fC = kind == 1 ? p.grazFracC : p.mortFracC;
             double fN = kind == 1 ? p.grazFracN : p.mortFracN;
             double fP = kind == 1 ? p.grazFracP : p.mortFracP;
+            if (mode == MODE_IRON) {
+                // IronEnergyMode/consume_loss.jl:17-32: NH4, NO3, DOC, DON, DOP, DFe, POC, PON, POP, PFe_bio
+                double* L = loss + e * 10;
+                const double fFe = kind == 1 ? ip.grazFracFe : ip.mortFracFe;
+                const double Bm = P.Bm[slot], CH = P.CH[slot], qP = P.qP[slot];
+                const double fe = P.qFe[slot] + P.qFePS[slot] + P.qFeNF[slot] + P.qFeNR[slot];
+                L[0] = jl_mulb(P.qNH4[slot], 1) * 1.0;
+                L[1] = jl_mulb(P.qNO3[slot], 1) * 1.0;
+                L[2] = jl_mulb((Bm + CH) * fC, 1) * 1.0;
+                L[3] = jl_mulb(Bm * ip.R_NC * fN, 1) * 1.0;
+                L[4] = jl_mulb((Bm * ip.R_PC + qP) * fP, 1) * 1.0;
+                L[5] = jl_mulb(fe * fFe, 1) * 1.0;
+                L[6] = jl_mulb((Bm + CH) * (1.0 - fC), 1) * 1.0;
+                L[7] = jl_mulb(Bm * ip.R_NC * (1.0 - fN), 1) * 1.0;
+                L[8] = jl_mulb((Bm * ip.R_PC + qP) * (1.0 - fP), 1) * 1.0;
+                L[9] = jl_mulb(fe * (1.0 - fFe), 1) * 1.0;
+            } else {
             double* L = loss + e * 6;
             if (mode == MODE_CARBON) {
                 const double Bm = P.Bm[slot];
@@ -372,6 +389,7 @@ __global__ void k_decide(DGrid g, SpcDev P, pi_quota_params p, pi_macro_params m
             L[3] = jl_mulb((Bm + Cq) * (1.0 - fC), 1) * 1.0;          // POC
             L[4] = jl_mulb((Bm * p.R_NC + Nq) * (1.0 - fN), 1) * 1.0; // PON
             L[5] = jl_mulb((Bm * p.R_PC + Pq) * (1.0 - fP), 1) * 1.0; // POP
+            }
             }
         }
     }
@@ -420,6 +438,19 @@ __global__ void k_daughters(SpcDev P, const int32_t* __restrict__ divlist,
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         long long p = divlist[k], d = freelist[k];
         const double h = (2.0 - 1.0) / 2.0;
+        if (mode == MODE_IRON) {
+            // IronEnergyMode/division_death.jl:44-82: x, y, z, tdark and gen copied; Sz, Bm, CH, the
+            // quotas, exEn and Chl copied and halved in both; age not copied
+            double* pools[12] = { P.Sz, P.Bm, P.CH, P.qNO3, P.qNH4, P.qP, P.qFe, P.qFePS, P.qFeNR, P.qFeNF, P.exEn, P.Chl };
+            const double gen = P.gen[p];
+            P.x[d] = P.x[p]; P.y[d] = P.y[p]; P.z[d] = P.z[p]; P.tdark[d] = P.tdark[p];
+#pragma unroll
+            for (int q = 0; q < 12; ++q) { const double v = pools[q][p] * h; pools[q][d] = v; pools[q][p] = v; }
+            P.gen[d] = gen + 1.0; P.age[d] = P.age[d] * (1.0 - 1.0);
+            P.flags[d] = FL_AC | FL_DVID;
+            P.gen[p] = gen + 1.0; P.age[p] = P.age[p] * (1.0 - 1.0);
+            continue;
+        }
         if (mode == MODE_MACRO) {
             // MacroMolecularMode/division_death.jl:28-62: the seven pools, x, y, z and gen are
             // copied and halved in both (not age)
@@ -1204,12 +1235,12 @@ __global__ void __launch_bounds__(32 * SWZ_TZ, 8) k_sweep_z(DGrid g, const doubl
     }
 }
 
-template <bool LL>
+template <bool LL, bool IRON>
 __device__ __forceinline__ void z_final_cell(const ZFinalArgs& a, int i, int j, int k, int q, double volk, double* Gc);
 
 // Per interior cell: diffusion, sinking, forcing, flux BCs, particle terms and apply_tendency!
 // on top of the advective tendency of k_sweep_z (tracer_update.jl:22-43).
-template <bool LL>
+template <bool LL, bool IRON = false>
 __global__ void __launch_bounds__(128, 6) k_tracer_tail(ZFinalArgs a) {
     const DGrid& g = a.g;
     if (*a.err & PI_DEVERR_CAPACITY) return;
@@ -1222,11 +1253,11 @@ __global__ void __launch_bounds__(128, 6) k_tracer_tail(ZFinalArgs a) {
     double Gc[PI_NTRACERS];
 #pragma unroll
     for (int t = 0; t < PI_NTRACERS; ++t) Gc[t] = a.gadv[t * G + q];
-    z_final_cell<LL>(a, i, j, k, q, vol<LL>(g, i, j, k), Gc);
+    z_final_cell<LL, IRON>(a, i, j, k, q, vol<LL>(g, i, j, k), Gc);
 }
 
 // The rest of tracer_update! for one interior cell, given its advective tendency Gc.
-template <bool LL>
+template <bool LL, bool IRON>
 __device__ __forceinline__ void z_final_cell(const ZFinalArgs& a, int i, int j, int k, int q, double volk, double* Gc) {
     const DGrid& g = a.g;
     const long long G = g.G;
@@ -1309,6 +1340,7 @@ __device__ __forceinline__ void z_final_cell(const ZFinalArgs& a, int i, int j, 
     // plk: per-cell particle losses and consumption in reference summation order
     double plk_DIC = 0.0, plk_NH4 = 0.0, plk_NO3 = 0.0, plk_PO4 = 0.0, plk_DOC = 0.0;
     double plk_DON = 0.0, plk_DOP = 0.0, plk_POC = 0.0, plk_PON = 0.0, plk_POP = 0.0;
+    double plk_DFe = 0.0, plk_PFe = 0.0;         // IronEnergyMode only
     {
         uint32_t p0 = a.off[q], p1 = a.off[q + 1];
         uint32_t p = p0;
@@ -1319,13 +1351,20 @@ __device__ __forceinline__ void z_final_cell(const ZFinalArgs& a, int i, int j, 
             for (int pass = 1; pass <= 2; ++pass)
                 for (uint32_t r = p; r < e; ++r)
                     if (a.evk[r] == pass) {
-                        const double* L = a.loss + (long long)r * 6;
-                        plk_DOC += L[0]; plk_DON += L[1]; plk_DOP += L[2];
-                        plk_POC += L[3]; plk_PON += L[4]; plk_POP += L[5];
+                        if (IRON) {                  // NH4, NO3, DOC, DON, DOP, DFe, POC, PON, POP, PFe_bio
+                            const double* L = a.loss + (long long)r * 10;
+                            plk_NH4 += L[0]; plk_NO3 += L[1]; plk_DOC += L[2]; plk_DON += L[3]; plk_DOP += L[4];
+                            plk_DFe += L[5]; plk_POC += L[6]; plk_PON += L[7]; plk_POP += L[8]; plk_PFe += L[9];
+                        } else {
+                            const double* L = a.loss + (long long)r * 6;
+                            plk_DOC += L[0]; plk_DON += L[1]; plk_DOP += L[2];
+                            plk_POC += L[3]; plk_PON += L[4]; plk_POP += L[5];
+                        }
                     }
             for (uint32_t r = p; r < e; ++r) {
                 const double* K = a.contrib + (long long)r * 5;
-                plk_DIC += K[0]; plk_DOC += K[1]; plk_NH4 += K[2]; plk_NO3 += K[3]; plk_PO4 += K[4];
+                if (IRON) { plk_DIC += K[0]; plk_NH4 += K[1]; plk_NO3 += K[2]; plk_PO4 += K[3]; plk_DFe += K[4]; }
+                else { plk_DIC += K[0]; plk_DOC += K[1]; plk_NH4 += K[2]; plk_NO3 += K[3]; plk_PO4 += K[4]; }
             }
             p = e;
         }
@@ -1335,7 +1374,8 @@ __device__ __forceinline__ void z_final_cell(const ZFinalArgs& a, int i, int j, 
     for (int n = 0; n < PI_NTRACERS; ++n) {
         double pk = n == PI_DIC ? plk_DIC : n == PI_NH4 ? plk_NH4 : n == PI_NO3 ? plk_NO3 : n == PI_PO4 ? plk_PO4
                   : n == PI_DOC ? plk_DOC : n == PI_DON ? plk_DON : n == PI_DOP ? plk_DOP : n == PI_POC ? plk_POC
-                  : n == PI_PON ? plk_PON : n == PI_POP ? plk_POP : 0.0;
+                  : n == PI_PON ? plk_PON : n == PI_POP ? plk_POP
+                  : (IRON && n == PI_DFe) ? plk_DFe : (IRON && n == PI_PFe_bio) ? plk_PFe : 0.0;
         a.tr_next[n * G + q] = a.tr[n * G + q] + (Gc[n] + pk / volk);
     }
 }

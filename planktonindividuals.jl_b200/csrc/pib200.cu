@@ -24,6 +24,7 @@
 
 #include "kernels_fp64.cuh"
 #include "kernels_abiotic.cuh"
+#include "kernels_iron.cuh"
 #include "host_common.h"
 
 using namespace pib;
@@ -57,7 +58,10 @@ struct pi_model {
     std::vector<pi_carbon_params> cp;
     int macro = 0;               // MacroMolecularMode species (pi_create_macro)
     std::vector<pi_macro_params> mp;
-    int mode() const { return macro ? MODE_MACRO : carbon ? MODE_CARBON : MODE_QUOTA; }
+    int iron = 0;                // IronEnergyMode species (pi_create_iron)
+    std::vector<pi_iron_params> ipp;
+    double* par0 = nullptr;      // G: par of the previous step (timestepper.par₀), IronEnergyMode only
+    int mode() const { return iron ? MODE_IRON : macro ? MODE_MACRO : carbon ? MODE_CARBON : MODE_QUOTA; }
     int64_t iteration = 0;
     double t = 0.0;
     double last_dT = 0.0;
@@ -432,7 +436,8 @@ pi_status enqueue_step(pi_model* m, double dT) {
         double* dsp = m->diag_sp + (size_t)s * 4 * G;
         { ProfScope ps_(m, "k_decide");
         const pi_macro_params mpz = m->macro ? m->mp[s] : pi_macro_params{};
-        k_decide<<<nblk(C, BS), BS, 0, st>>>(g, m->h_spc[s], m->sp[s], mpz, C, s, sb.pos, sb.loss, sb.evk,
+        const pi_iron_params ipz = m->iron ? m->ipp[s] : pi_iron_params{};
+        k_decide<<<nblk(C, BS), BS, 0, st>>>(g, m->h_spc[s], m->sp[s], mpz, ipz, C, s, sb.pos, sb.loss, sb.evk,
                                              sb.flag64, dsp + 1 * G, dsp + 2 * G, dsp + 3 * G, sb.err, m->mode());
         CK(cudaGetLastError(), "k_decide"); }
         tb = m->cub_bytes;
@@ -446,6 +451,13 @@ pi_status enqueue_step(pi_model* m, double dT) {
         k_daughters<<<148 * 4, 256, 0, st>>>(m->h_spc[s], sb.divlist, sb.freelist, sb.ndiv, sb.err, m->mode());
         CK(cudaGetLastError(), "k_daughters"); }
         const double* trp = m->tr;
+        if (m->iron) { ProfScope ps_(m, "k_physiology");
+        k_physiology_iron<<<nblk(C, BS), BS, 0, st>>>(g, m->h_spc[s], m->ipp[s], C, s, dT, m->t, m->seed, iter, shared,
+                                                      trp + PI_NH4 * G, trp + PI_NO3 * G, trp + PI_PO4 * G,
+                                                      trp + PI_DFe * G, m->par, m->par0, m->temp, sb.off, sb.gid_sorted,
+                                                      sb.pos, sb.contrib, dsp + 0 * G,
+                                                      m->proc_mask ? m->procv : nullptr, sb.err);
+        CK(cudaGetLastError(), "k_physiology_iron"); } else
         if (m->macro) { ProfScope ps_(m, "k_physiology");
         k_physiology_macro<<<nblk(C, BS), BS, 0, st>>>(g, m->h_spc[s], m->mp[s], C, s, dT, m->seed, iter, shared,
                                                        trp + PI_NH4 * G, trp + PI_NO3 * G, trp + PI_PO4 * G,
@@ -497,7 +509,8 @@ pi_status enqueue_step(pi_model* m, double dT) {
             g, m->tr, m->ttb, m->tta, m->vel1[2], dT, sb.err);
         CK(cudaGetLastError(), "k_sweep_z"); }
         { ProfScope ps_(m, "k_tracer_tail");
-        (ll ? k_tracer_tail<true> : k_tracer_tail<false>)<<<dim3(nblk(g.Nx, 128), g.Ny, g.Nz), 128, 0, st>>>(za);
+        (m->iron ? (ll ? k_tracer_tail<true, true> : k_tracer_tail<false, true>)
+                 : (ll ? k_tracer_tail<true, false> : k_tracer_tail<false, false>))<<<dim3(nblk(g.Nx, 128), g.Ny, g.Nz), 128, 0, st>>>(za);
         CK(cudaGetLastError(), "k_tracer_tail"); }
         // tracers are only replaced when the step completed (a capacity error leaves them)
         { ProfScope ps_(m, "k_halo");
@@ -514,6 +527,7 @@ pi_status enqueue_step(pi_model* m, double dT) {
     }
     std::swap(m->tr, m->tr_next);
     for (int c = 0; c < 3; ++c) m->vel0[c] = m->vel1[c];    // vel₀ .= vel₁ (time_step.jl:174-176)
+    if (m->par0) CK(cudaMemcpyAsync(m->par0, m->par, G * sizeof(double), cudaMemcpyDeviceToDevice, st), "par₀ .= par");
     return PI_OK;
 }
 
@@ -796,6 +810,50 @@ pi_status pi_create_carbon(const pi_grid* grid, const pi_bgc_params* bgc, const 
     return PI_OK;
 }
 
+pi_status pi_create_iron(const pi_grid* grid, const pi_bgc_params* bgc, const pi_iron_params* species,
+                         int32_t nspecies, int64_t capacity, int32_t precision, uint64_t seed, pi_model** out) {
+    if (!out) return fail(nullptr, PI_ERR_ARG, "pi_create_iron: out is NULL");
+    *out = nullptr;
+    if (!species || nspecies < 1) return fail(nullptr, PI_ERR_ARG, "pi_create_iron: NULL species or nspecies < 1");
+    if (precision != PI_FP64)
+        return fail(nullptr, PI_ERR_ARG, "pi_create_iron: IronEnergyMode is built in the FP64 form only (precision PI_FP64)");
+    // the QuotaMode setup with the parameters both modes share; the species then switch to IronEnergyMode
+    std::vector<pi_quota_params> q((size_t)nspecies);
+    for (int s = 0; s < nspecies; ++s) {
+        const pi_iron_params& c = species[s];
+        pi_quota_params& p = q[s];
+        memset(&p, 0, sizeof p);
+        p.Nsuper = c.Nsuper; p.Cquota = c.Cquota; p.mean = c.mean; p.var = c.var; p.Chl2Cint = c.Chl2Cint;
+        p.alpha = c.alpha; p.Topt = c.Topt; p.Tmax = c.Tmax; p.Ea = c.Ea; p.PCmax = c.PCmax;
+        p.R_NC = c.R_NC; p.R_PC = c.R_PC; p.grz_P = c.grz_P; p.dvid_type = c.dvid_type; p.dvid_P = c.dvid_P;
+        p.dvid_reg = c.dvid_reg; p.dvid_reg2 = c.dvid_reg2; p.mort_P = c.mort_P; p.mort_reg = c.mort_reg;
+        p.grazFracC = c.grazFracC; p.grazFracN = c.grazFracN; p.grazFracP = c.grazFracP;
+        p.mortFracC = c.mortFracC; p.mortFracN = c.mortFracN; p.mortFracP = c.mortFracP;
+    }
+    pi_status st = pi_create(grid, bgc, q.data(), nspecies, capacity, PI_FP64, seed, out);
+    if (st) return st;
+    pi_model* m = *out;
+    m->iron = 1;
+    m->ipp.assign(species, species + nspecies);
+    const long long NC = (long long)nspecies * capacity;
+    bool ok = dalloc(m, &m->par0, (size_t)m->hg.G, "previous PAR") == PI_OK &&
+              cudaMemsetAsync(m->par0, 0, (size_t)m->hg.G * sizeof(double), m->stream) == cudaSuccess &&
+              dalloc(m, &m->sb.loss, (size_t)(10 * NC), "iron loss records") == PI_OK;     // ten tracers per record
+    for (int s = 0; s < nspecies && ok; ++s) {
+        SpcDev& P = m->h_spc[s];
+        double** pools[10] = { &P.CH, &P.qNO3, &P.qNH4, &P.qP, &P.qFe, &P.qFePS, &P.qFeNR, &P.qFeNF, &P.exEn, &P.tdark };
+        for (double** pp : pools)
+            ok = ok && dalloc(m, pp, (size_t)capacity, "iron-energy pools") == PI_OK &&
+                 cudaMemsetAsync(*pp, 0, (size_t)capacity * sizeof(double), m->stream) == cudaSuccess;
+    }
+    if (!ok || cudaMemcpyAsync(m->d_spc, m->h_spc.data(), nspecies * sizeof(SpcDev), cudaMemcpyHostToDevice, m->stream) != cudaSuccess ||
+        cudaStreamSynchronize(m->stream) != cudaSuccess) {
+        pi_destroy(m); *out = nullptr;
+        return fail(nullptr, PI_ERR_CUDA, "pi_create_iron: device allocation or initialisation failed");
+    }
+    return PI_OK;
+}
+
 pi_status pi_create_macro(const pi_grid* grid, const pi_bgc_params* bgc, const pi_macro_params* species,
                           int32_t nspecies, int64_t capacity, int32_t precision, uint64_t seed, pi_model** out) {
     if (!out) return fail(nullptr, PI_ERR_ARG, "pi_create_macro: out is NULL");
@@ -863,11 +921,14 @@ pi_status pi_set_individuals(pi_model* m, int32_t sp, const pi_individuals* in) 
     const double* mcols[6] = { in->PRO, in->DNA, in->RNA, in->CH, in->NST, in->PST };
     for (int q = 0; q < 14; ++q) {
         // CarbonMode keeps no quotas; MacroMolecularMode no Sz, Bm or quotas, but its six pools
-        const bool unused = (m->carbon && q >= 5 && q <= 7) || (m->macro && q >= 3 && q <= 7);
+        const bool unused = ((m->carbon || m->iron) && q >= 5 && q <= 7) || (m->macro && q >= 3 && q <= 7);
         if (!dcols[q] && !unused) return fail(m, PI_ERR_ARG, "pi_set_individuals: NULL attribute");
     }
     if (m->macro)
         for (const double* c : mcols) if (!c) return fail(m, PI_ERR_ARG, "pi_set_individuals: NULL attribute");
+    const double* icols[10] = { in->CH, in->qNO3, in->qNH4, in->qP, in->qFe, in->qFePS, in->qFeNR, in->qFeNF, in->exEn, in->tdark };
+    if (m->iron)
+        for (int q = 0; q < 8; ++q) if (!icols[q]) return fail(m, PI_ERR_ARG, "pi_set_individuals: NULL attribute");
     if (!in->xi || !in->yi || !in->zi || !in->ac) return fail(m, PI_ERR_ARG, "pi_set_individuals: NULL attribute");
     const long long C = m->C;
     const HostGrid& g = m->hg;
@@ -899,6 +960,13 @@ pi_status pi_set_individuals(pi_model* m, int32_t sp, const pi_individuals* in) 
         else CK(cudaMemsetAsync(P.Bd, 0, C * sizeof(double), m->stream), "upload individuals");
     }
     if (in->ptc) CK(cudaMemcpyAsync(P.ptc, in->ptc, C * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload individuals");
+    if (m->iron) {
+        double* iptr[10] = { P.CH, P.qNO3, P.qNH4, P.qP, P.qFe, P.qFePS, P.qFeNR, P.qFeNF, P.exEn, P.tdark };
+        for (int q = 0; q < 10; ++q) {
+            if (icols[q]) CK(cudaMemcpyAsync(iptr[q], icols[q], C * sizeof(double), cudaMemcpyHostToDevice, m->stream), "upload individuals");
+            else CK(cudaMemsetAsync(iptr[q], 0, C * sizeof(double), m->stream), "upload individuals");   // exEn, tdark
+        }
+    }
     else CK(cudaMemsetAsync(P.ptc, 0, C * sizeof(double), m->stream), "upload individuals");
     CK(cudaMemcpyAsync(P.flags, flags.data(), C, cudaMemcpyHostToDevice, m->stream), "upload flags");
     CK(cudaMemcpyAsync(P.cell, cell.data(), C * sizeof(int32_t), cudaMemcpyHostToDevice, m->stream), "upload cells");
@@ -918,6 +986,12 @@ pi_status pi_get_individuals(pi_model* m, int32_t sp, pi_individuals* out) {
         if (hptr[q]) CK(cudaMemcpyAsync(hptr[q], dptr[q], C * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download individuals");
     if (m->carbon && out->Bd) CK(cudaMemcpyAsync(out->Bd, P.Bd, C * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download individuals");
     if (out->ptc) CK(cudaMemcpyAsync(out->ptc, P.ptc, C * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download individuals");
+    if (m->iron) {
+        double* ih[10] = { out->CH, out->qNO3, out->qNH4, out->qP, out->qFe, out->qFePS, out->qFeNR, out->qFeNF, out->exEn, out->tdark };
+        const double* id[10] = { P.CH, P.qNO3, P.qNH4, P.qP, P.qFe, P.qFePS, P.qFeNR, P.qFeNF, P.exEn, P.tdark };
+        for (int q = 0; q < 10; ++q)
+            if (ih[q]) CK(cudaMemcpyAsync(ih[q], id[q], C * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "download individuals");
+    }
     if (m->macro) {
         double* mh[6] = { out->PRO, out->DNA, out->RNA, out->CH, out->NST, out->PST };
         const double* md[6] = { P.PRO, P.DNA, P.RNA, P.CH, P.NST, P.PST };
@@ -1357,7 +1431,8 @@ pi_status pi_count_active_async(pi_model* m, int32_t sp, int64_t* n) {
 
 pi_status pi_set_diags(pi_model* m, uint32_t tracer_mask, uint32_t proc_mask) {
     if (m && m->b32) return fwd32(m, pi_batch_set_diags(m->b32, tracer_mask, proc_mask));
-    if (!m || tracer_mask >> PI_NTRACERS || proc_mask >> (m->macro ? (int)PI_NMPROC : m->carbon ? (int)PI_NCPROC : (int)PI_NPROC))
+    const int nproc = !m ? 0 : m->iron ? (int)PI_NIPROC : m->macro ? (int)PI_NMPROC : m->carbon ? (int)PI_NCPROC : (int)PI_NPROC;
+    if (!m || tracer_mask >> PI_NTRACERS || (nproc < 32 && proc_mask >> nproc))
         return fail(m, PI_ERR_ARG, "pi_set_diags: bad argument");
     const long long G = m->hg.G, C = m->C;
     CK(cudaStreamSynchronize(m->stream), "synchronize");
@@ -1425,7 +1500,8 @@ pi_status pi_get_budget(pi_model* m, double out[6]) {
     pi_status e = collect(out);
     if (e) return e;
     for (int s = 0; s < m->nsp; ++s) {
-        if (m->macro) k_budget_inds_macro<<<nb, 256, 0, m->stream>>>(m->h_spc[s], m->C, m->mp[s], m->budget_part);
+        if (m->iron) k_budget_inds_iron<<<nb, 256, 0, m->stream>>>(m->h_spc[s], m->C, m->ipp[s].R_NC, m->ipp[s].R_PC, m->budget_part);
+        else if (m->macro) k_budget_inds_macro<<<nb, 256, 0, m->stream>>>(m->h_spc[s], m->C, m->mp[s], m->budget_part);
         else k_budget_inds<<<nb, 256, 0, m->stream>>>(m->h_spc[s], m->C, m->sp[s].R_NC, m->sp[s].R_PC, m->budget_part);
         if ((e = collect(out + 3))) return e;
     }

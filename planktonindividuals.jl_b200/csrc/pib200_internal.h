@@ -30,9 +30,10 @@
 #define MODE_QUOTA  0
 #define MODE_CARBON 1
 #define MODE_MACRO  2
+#define MODE_IRON   3
 
 // process diagnostics of the largest mode (MacroMolecularMode): sizes of the per-species buffers
-#define PI_MAXPROC PI_NMPROC
+#define PI_MAXPROC PI_NIPROC     // the most processes of any mode (IronEnergyMode's 32)
 
 // Device error word bits (sticky until pi_synchronize reads and clears them).
 #define PI_DEVERR_DOMAIN   1u
@@ -87,6 +88,8 @@ struct SpcDev {
     // MacroMolecularMode pools (NULL otherwise): protein, DNA, RNA, carbohydrate/lipid, N and P reserves
     double *PRO, *DNA, *RNA, *CH, *NST, *PST;
     double* ptc;        // abiotic particles held (every mode)
+    // IronEnergyMode quotas, excess energy and time since sunset (NULL otherwise; CH above)
+    double *qNO3, *qNH4, *qP, *qFe, *qFePS, *qFeNR, *qFeNF, *exEn, *tdark;
     uint8_t* flags;
     int32_t* cell;      // packed (xi, yi, zi)
     uint8_t* stat;      // ST_* bits of the current step

@@ -106,3 +106,20 @@ def test_draws_lattice_and_keys():
     # uniformity on a sample
     s = np.array([oracle.draw3(5, 1, 0, 1, i)[0] for i in range(20000)])
     assert abs(s.mean() - 0.5) < 0.01 and abs(s.var() - 1 / 12) < 0.005
+
+
+def test_log_and_pow_error_bounds():
+    """pi_log within 2 ulp of libm's log over [1e-300, 1e300]; pi_pow(x, y) within 8 ulp of
+    libm's pow for the reference's non-integer exponent 2f0/3f0 and others on positive bases."""
+    rng = np.random.default_rng(5)
+    xs = np.concatenate([10.0 ** rng.uniform(-300, 300, 3000), rng.uniform(0.5, 2.0, 3000),
+                         [1.0, 2.0, 0.5, math.sqrt(0.5), math.sqrt(2.0), 5e-324]])
+    worst = max(abs(oracle.pi_log(x) - math.log(x)) / math.ulp(math.log(x)) if x != 1.0 else 0.0 for x in xs)
+    assert worst <= 2.0
+    assert oracle.pi_log(1.0) == 0.0 and oracle.pi_log(0.0) == -math.inf and math.isnan(oracle.pi_log(-1.0))
+    y23 = float(np.float32(2.0) / np.float32(3.0))
+    for y in (y23, 0.5, 1.7, -0.3):
+        bases = rng.uniform(0.0, 20.0, 2000)
+        worst = max(abs(oracle.pi_pow(x, y) - x ** y) / math.ulp(x ** y) for x in bases if x > 0)
+        assert worst <= 8.0, (y, worst)
+    assert oracle.pi_pow(0.0, y23) == 0.0 and oracle.pi_pow(8.0, 1.0 / 3.0) == pytest.approx(2.0, rel=1e-15)
