@@ -13,7 +13,7 @@
 module PIB200
 
 export PiGrid, PiBgc, PiQuota, PiIndividuals, PiMember, PIError
-export create, create_carbon, create_macro, destroy, set_individuals!, get_individuals, set_tracer!, get_tracer
+export create, create_carbon, create_macro, create_iron, destroy, set_individuals!, get_individuals, set_tracer!, get_tracer
 export set_velocity!, set_PARF!, set_temp!, set_flux_bc!, time_step!, get_time, set_time!
 export count_active, get_diag, reset_diags!, check_finite, budget, simulation, update!, synchronize
 export set_velocity_f32!, set_PARF_f32!, set_temp_f32!, time_step_async!, count_active_async!, set_diags!
@@ -110,6 +110,8 @@ struct PiIndividuals
     PRO::Ptr{Float64}; DNA::Ptr{Float64}; RNA::Ptr{Float64}    # MacroMolecularMode pools (C_NULL otherwise)
     CH::Ptr{Float64}; NST::Ptr{Float64}; PST::Ptr{Float64}
     ptc::Ptr{Float64}           # abiotic particles held (every mode); C_NULL uploads zeros
+    qNO3::Ptr{Float64}; qNH4::Ptr{Float64}; qP::Ptr{Float64}; qFe::Ptr{Float64}     # IronEnergyMode (C_NULL otherwise)
+    qFePS::Ptr{Float64}; qFeNR::Ptr{Float64}; qFeNF::Ptr{Float64}; exEn::Ptr{Float64}; tdark::Ptr{Float64}
 end
 
 # construct_abiotic_particle's parameters (Abiotic/particle_generation.jl:7) and one species' state
@@ -217,6 +219,39 @@ function create_carbon(g, bgc::AbstractDict, phyt::AbstractDict, Nsp::Integer, m
     m
 end
 
+# IronEnergyMode parameters in param_names order (IronEnergyMode/plankton_generation.jl:27-36)
+const IRON_KEYS = ("Nsuper", "Cquota", "SA", "mean", "var", "Chl2Cint", "α", "Topt", "Tmax", "Ea", "is_nr", "is_croc",
+    "is_tric", "PCmax", "VNO3max", "VNH4max", "VPO4max", "k_cf", "k_rs", "k_nr", "k_nf", "k_mtb", "e_cf", "e_rs",
+    "e_nr", "e_nf", "k_Fe_ST2PS", "k_Fe_PS2ST", "k_Fe_ST2NR", "k_Fe_NR2ST", "k_Fe_ST2NF", "k_Fe_NF2ST", "KfePS",
+    "KfeNR", "KfeNF", "KsatNH4", "KsatNO3", "KsatPO4", "KSAFe", "CHmax", "qNH4max", "qNO3max", "qPmax", "qFemax",
+    "Chl2N", "R_NC", "R_PC", "NF_clock", "grz_P", "dvid_type", "dvid_P", "dvid_reg", "dvid_reg2", "mort_P",
+    "mort_reg", "grazFracC", "grazFracN", "grazFracP", "grazFracFe", "mortFracC", "mortFracN", "mortFracP",
+    "mortFracFe", "max_ptc")
+struct PiIron
+    v::NTuple{64,Float64}
+end
+PiIron(p::AbstractDict, sp::Integer) = PiIron(ntuple(i -> Float64(p[IRON_KEYS[i]][sp]), 64))
+
+"""PlanktonModel(GPU(), grid; FT = Float64, mode = IronEnergyMode(), ...): IronEnergyMode species, built
+in the FP64 form only. Its individual columns (CH, qNO3, qNH4, qP, qFe, qFePS, qFeNR, qFeNF, exEn,
+tdark) are the PiIndividuals members of those names."""
+function create_iron(g, bgc::AbstractDict, phyt::AbstractDict, Nsp::Integer, maxN::Integer; seed::Integer = 0)
+    dzF, dzC = Float64.(collect(g.dzF)), Float64.(collect(g.dzC))
+    lm = UInt8.(vec(collect(g.landmask)))
+    marr, mref = metric_arrays(g)
+    pg = Ref(pigrid(g, dzF, dzC, lm, mref === nothing ? C_NULL : Ptr{Cvoid}(Base.unsafe_convert(Ptr{PiGridMetrics}, mref))))
+    pb = Ref(PiBgc(bgc))
+    ps = [PiIron(phyt, s) for s in 1:Nsp]
+    out = Ref{Ptr{Cvoid}}(C_NULL)
+    st = GC.@preserve dzF dzC lm marr mref ccall((:pi_create_iron, lib), Int32,
+        (Ref{PiGrid}, Ref{PiBgc}, Ptr{PiIron}, Int32, Int64, Int32, UInt64, Ref{Ptr{Cvoid}}),
+        pg, pb, ps, Nsp, maxN, PI_FP64, seed, out)
+    check(st, C_NULL)
+    m = Model(out[], (g.Nx + 2g.Hx, g.Ny + 2g.Hy, g.Nz + 2g.Hz), Nsp, maxN, false, false)
+    finalizer(destroy, m)
+    m
+end
+
 """PlanktonModel(GPU(), grid; FT = Float64, mode = MacroMolecularMode(), ...): MacroMolecularMode
 species (individuals carry PRO, DNA, RNA, CH, NST, PST, Chl), built in the FP64 form only."""
 function create_macro(g, bgc::AbstractDict, phyt::AbstractDict, Nsp::Integer, maxN::Integer; seed::Integer = 0)
@@ -258,7 +293,7 @@ function set_individuals!(m::Model, sp::Integer, d)
     GC.@preserve cols bd pools ptc begin
         pp = m.mm ? map(pointer, pools) : ntuple(_ -> Ptr{Float64}(C_NULL), 6)
         pi = Ref(PiIndividuals(map(pointer, cols)..., m.carbon ? pointer(bd) : Ptr{Float64}(C_NULL), pp...,
-                               isempty(ptc) ? Ptr{Float64}(C_NULL) : pointer(ptc)))
+                               isempty(ptc) ? Ptr{Float64}(C_NULL) : pointer(ptc), ntuple(_ -> Ptr{Float64}(C_NULL), 9)...))
         check(ccall((:pi_set_individuals, lib), Int32, (Ptr{Cvoid}, Int32, Ref{PiIndividuals}), m.h, sp - 1, pi), m.h)
     end
 end
@@ -274,7 +309,7 @@ function get_individuals(m::Model, sp::Integer)
     GC.@preserve f i q ac dec bd pools ptc begin
         pi = Ref(PiIndividuals(pointer(f[1]), pointer(f[2]), pointer(f[3]), pointer(i[1]), pointer(i[2]), pointer(i[3]),
                                map(pointer, q)..., pointer(ac), map(pointer, dec)..., pointer(bd), map(pointer, pools)...,
-                               pointer(ptc)))
+                               pointer(ptc), ntuple(_ -> Ptr{Float64}(C_NULL), 9)...))
         check(ccall((:pi_get_individuals, lib), Int32, (Ptr{Cvoid}, Int32, Ref{PiIndividuals}), m.h, sp - 1, pi), m.h)
     end
     m.mm && return (x = f[1], y = f[2], z = f[3], xi = i[1], yi = i[2], zi = i[3], PRO = pools[1], DNA = pools[2],
