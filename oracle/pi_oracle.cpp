@@ -1,5 +1,6 @@
 /*
- * pi_oracle.cpp — CPU oracle for the model time step of PlanktonIndividuals.jl (QuotaMode).
+ * pi_oracle.cpp — CPU oracle for the model time step of PlanktonIndividuals.jl (QuotaMode,
+ * CarbonMode, MacroMolecularMode and IronEnergyMode physiology; abiotic particles).
  *
  * TEST INFRASTRUCTURE ONLY. Nothing in the product library links or calls this file; it is what
  * the tests, smoke() and the CPU-baseline leg of bench.py compare the CUDA path against.
